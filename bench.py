@@ -1,0 +1,279 @@
+"""Benchmark of the B200 intra RD core.
+
+Default workload (1080p 4:2:0 luma, quality 60 -> qindex 70, QM level 6): one
+step is one batched RDO level over the whole frame -- every 8x8 luma block x
+13 intra modes x 5 transform types (the 2-D-scan set IDTX, DCT_DCT, ADST_ADST,
+ADST_DCT, DCT_ADST) = 2,106,000 candidate chains (predict -> residual ->
+forward transform + quant + QM -> trellis -> inverse -> SATD distortion ->
+coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
+
+  value  MPix/s of the device-resident launch (inputs already in HBM)
+  e2e    MPix/s through the public host C ABI (mt_candidate_chain): host
+         planes + candidate list copied in, results copied out, every step
+
+``--impl reference`` times the CPU restatement of the reference (the oracle;
+the Rust reference cannot be built here) on all host cores over a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, QIDX, QM_LEVEL = 1920, 1080, 70, 6
+MODES = list(range(13))
+MPIX = W * H / 1e6
+
+
+def make_workload(seed=3):
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    rgb = synth.generate_rgb(W, H, seed, sigma=4.0, variant="1080p")
+    src = synth.rgb_to_luma(rgb)
+    rec = synth.synthetic_recon(src, seed + 1000)
+    cands = synth.level_candidates(W, H, MODES, abi.TX_2D_SCAN_TYPES, seed=seed)
+    cdfs = synth.synthetic_cdfs(seed)
+    q = mt.quant_new(QIDX, 8, QM_LEVEL)
+    qm = mt.qm_row(QM_LEVEL, 0, 8)
+    # lambdas of the luma proxy at qindex 70 4:2:0 (mode_lambda_q(dc_q) x weight,
+    # luma_satd_scale = satd_base 1.25, bridge K_PART_LAMBDA / k_satd * 7.130643)
+    dcq = float(q.dc_q)
+    mlam = 0.009005174719460433 * dcq * dcq * (3.3 + 0.0015 * dcq) * 0.8
+    k_satd = 24.5 + (21.3 - 24.5) * (QIDX - 28.0) / (81.0 - 28.0)
+    prm = mt.chain_params(W, H, trellis_lambda0=0.05, mode_lambda=mlam, satd_scale=1.25,
+                          satd_bridge=2.775 / k_satd * 7.130643)
+    return dict(src=src, rec=rec, cands=cands, cdfs=cdfs, q=q, qm=qm, prm=prm, rgb=rgb)
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([v.strip() for v in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 4 + i and s[4 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_rate(wl, sample, threads):
+    """Oracle throughput (candidates/s) over a bounded slice of the candidates."""
+    from oracle import pyoracle as po
+
+    cands = wl["cands"][:sample]
+    t0 = time.perf_counter()
+    po.candidate_chain(wl["src"], wl["rec"], wl["prm"], wl["q"], wl["qm"], wl["cdfs"], cands, threads=threads)
+    dt = time.perf_counter() - t0
+    return len(cands) / dt, dt
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import build as obuild
+
+    obuild.build()
+    wl = make_workload()
+    threads = os.cpu_count() or 1
+    n_all = len(wl["cands"])
+    sample = n_all  # the whole level: ~1.5 s on 8 cores
+    for _ in range(args.warmup):
+        cpu_rate(wl, min(sample, 50_000), threads)
+    times = []
+    for _ in range(args.steps):
+        rate, dt = cpu_rate(wl, sample, threads)
+        times.append(dt)
+    step_s = float(np.mean(times))
+    value = MPIX / step_s
+    line = {
+        "impl": "reference", "metric": "MPix/s (8x8 RDO level, 1080p luma)", "value": round(value, 4),
+        "unit": "MPix/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32+f32", "data": "synthetic",
+        "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
+                   "candidates": n_all},
+        "cpu_baseline": {"value": round(value, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                         "sample": f"all {n_all} candidates of the level per step"},
+        "e2e": {"value": round(value, 4), "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mt.load()
+    wl = make_workload()
+    cands = wl["cands"]
+    n = len(cands)
+    costs = mt.coef_costs(wl["cdfs"])
+    # device-resident inputs (replicas: every rank encodes its own frame; no collective on the data path)
+    d_src = torch.from_numpy(wl["src"].astype(np.int16)).to(dev)
+    d_rec = torch.from_numpy(wl["rec"].astype(np.int16)).to(dev)
+    d_qm = torch.from_numpy(wl["qm"]).to(dev)
+    d_costs = torch.from_numpy(np.frombuffer(bytes(costs), np.uint8).copy()).to(dev)
+    d_cands = torch.from_numpy(cands.view(np.uint8).copy()).to(dev)
+    d_res = torch.empty(n * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def launch():
+        mt.candidate_chain_device(d_src, d_rec, wl["prm"], wl["q"], d_qm, d_costs, d_cands, n, d_res,
+                                  stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        launch()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush between timed launches (outside the events)
+            ev[i][0].record(stream)
+            launch()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    kernel_ms = [a.elapsed_time(b) for a, b in ev]
+    step_ms = float(np.mean(kernel_ms))
+    t = torch.tensor([step_ms], device=dev)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    step_ms = float(t.item())
+    value = world * MPIX / (step_ms / 1e3)
+
+    # e2e through the host ABI: copies in and out inside the timed region
+    src, rec = wl["src"], wl["rec"]
+    e2e_times = []
+    for i in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res, _, _ = mt.candidate_chain(src, rec, wl["prm"], wl["q"], wl["qm"], costs, cands)
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_times))
+    h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + cands.nbytes
+    d2h = n * abi.RESULT_DTYPE.itemsize
+
+    # roofline of the chain kernel against HBM: algorithmic bytes per launch =
+    # candidate record 16 B + result 32 B + source 64 x 2 B + neighbour edges
+    # (up to 33) x 2 B per candidate
+    alg_bytes = n * (16 + 32 + 128 + 66)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import build as obuild
+
+        obuild.build()
+        threads = os.cpu_count() or 1
+        rate, dt = cpu_rate(wl, n, threads)
+        cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+               "sample": f"the whole level, {n} candidates ({dt:.2f} s)"}
+
+    line = {
+        "metric": "MPix/s (8x8 RDO level, 1080p luma)", "value": round(value, 3), "unit": "MPix/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f32",
+        "data": "synthetic",
+        "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
+                   "candidates": n, "parallelism": f"replicas x{world}", "l2": "flushed between timed launches"},
+        "e2e": {"value": round(world * MPIX / e2e_s, 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 5), "traffic": None,
+                     "kernel": "chain8_kernel", "alg_bytes_per_launch": alg_bytes},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

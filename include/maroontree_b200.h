@@ -1,0 +1,212 @@
+/*
+ * maroontree_b200 — C ABI of the B200 intra rate-distortion core.
+ *
+ * These entry points are what a host encoder's FFI crate binds in place of the
+ * reference's CPU kernel dispatch tables.  Every function takes plain pointers
+ * and sizes; no torch or CUDA types appear in the signatures.  Device entry
+ * points (mt_*_device) take device pointers and a cudaStream_t passed as
+ * `void*` (NULL = legacy default stream); host entry points (mt_* without the
+ * suffix) take host buffers and do the copies themselves.
+ *
+ * Reference interfaces replaced (paths inside awxkee/maroontree):
+ *   mt_quant_init / mt_quant_init_chroma  src/quant.rs:351-418  Quant::new_with_qm /
+ *                                         Quant::new_chroma_with_delta_qm
+ *   mt_coef_costs_build                   src/rate.rs:58-80 CoefCostTables::build +
+ *                                         src/cost.rs:156-190 cdf_cost_with_table
+ *   mt_candidate_chain[_device]           the per-candidate chain of the luma mode
+ *                                         search, src/coder/partition_search.rs:467-530
+ *                                         (predict_nd -> residual_pred -> DctDispatch ->
+ *                                         trellis_optimize -> IdctDispatch ->
+ *                                         luma_partition_distortion + luma_bits + mode bits
+ *                                         -> partition_rd::rd_cost), batched over candidates
+ *   mt_fwd_txfm_quant[_device]            src/dct.rs:2416-2950 DctDispatch::*_t
+ *   mt_inv_txfm_dequant[_device]          src/idct.rs:90-160 IdctDispatch
+ *   mt_trellis_optimize[_device]          src/trellis.rs:944-1030 trellis_optimize
+ *   mt_intra_predict[_device]             src/intrapred.rs:322-398 IntraPredDispatch::predict_nd_ad,
+ *                                         src/intrapred.rs:1740-1790 dc_pred
+ */
+#ifndef MAROONTREE_B200_H
+#define MAROONTREE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error codes (src/err.rs:146-173 EncodeError, one negative code per variant
+ * this boundary can raise, plus device failures). */
+#define MT_OK 0
+#define MT_ERR_INVALID_INPUT (-2)
+#define MT_ERR_UNSUPPORTED (-3)
+#define MT_ERR_DEVICE (-10)
+#define MT_ERR_ALLOC (-11)
+
+/* Intra prediction modes, AV1 numbering (src/intrapred.rs:54-79). */
+#define MT_DC_PRED 0
+#define MT_V_PRED 1
+#define MT_H_PRED 2
+#define MT_D45_PRED 3
+#define MT_D135_PRED 4
+#define MT_D113_PRED 5
+#define MT_D157_PRED 6
+#define MT_D203_PRED 7
+#define MT_D67_PRED 8
+#define MT_SMOOTH_PRED 9
+#define MT_SMOOTH_V_PRED 10
+#define MT_SMOOTH_H_PRED 11
+#define MT_PAETH_PRED 12
+
+/* Transform types in the 7-type intra set index order used by the reference
+ * (src/cost.rs:100-103: IDTX=0, DCT_DCT=1, V_DCT=2, H_DCT=3, ADST_ADST=4,
+ * ADST_DCT=5, DCT_ADST=6).  ADST_DCT = ADST down the columns, DCT along rows. */
+#define MT_TX_IDTX 0
+#define MT_TX_DCT_DCT 1
+#define MT_TX_V_DCT 2
+#define MT_TX_H_DCT 3
+#define MT_TX_ADST_ADST 4
+#define MT_TX_ADST_DCT 5
+#define MT_TX_DCT_ADST 6
+
+/* Quantiser state of one plane (src/quant.rs:327-343 Quant). */
+typedef struct mt_quant {
+  int32_t dc_q, ac_q;           /* dequant steps */
+  int32_t q_mult_dc, q_mult_ac; /* round(65536 / step) */
+  int32_t rmin, rmax, cmin, cmax, cf_max; /* inverse-transform clips */
+  int32_t qm_level;             /* 0..14, 15 = flat */
+  int32_t qm_chroma;
+  int32_t qidx;
+} mt_quant;
+
+/* One (transform class, plane) slice of an immutable decision CDF snapshot
+ * (src/coder/cdfs.rs Cdfs fields), AV1 inverse-CDF form: entry s is
+ * 32768 * P(symbol > s); the last entry of each CDF is 0. */
+typedef struct mt_coef_cdfs {
+  uint16_t txb_skip[13][2];
+  uint16_t base_tok[42][4];
+  uint16_t br_tok[21][4];
+  uint16_t eob_base[4][3];
+  uint16_t eob_hi[11][2];
+  uint16_t eob_bin[11];   /* eob_pt CDF of this size; unused tail = 0 */
+  uint16_t dc_sign[3][2];
+  uint16_t txtp[13][16];  /* intra tx-type CDF per y mode; unused tail = 0 */
+} mt_coef_cdfs;
+
+/* Bit costs of the same slice, each entry cdf_cost_with_table(cdf, s)
+ * (src/cost.rs:184-190) and br_cum the cumulative base-range ladder
+ * (src/cost.rs:214-241).  Built on the host by mt_coef_costs_build. */
+typedef struct mt_coef_costs {
+  float txb_skip[13][2];
+  float base_tok[42][4];
+  float br_cum[21][13];
+  float eob_base[4][3];
+  float eob_hi[11][2];
+  float eob_bin[11];
+  float dc_sign[3][2];
+  float txtp[13][16];
+} mt_coef_costs;
+
+/* One candidate of the batched chain: block position, intra mode (+ angle
+ * delta), transform type and neighbour availability. */
+typedef struct mt_candidate {
+  uint16_t px, py;       /* luma sample position of the block */
+  uint8_t mode;          /* MT_*_PRED */
+  int8_t angle_delta;    /* -3..3, directional modes only */
+  uint8_t tx_type;       /* MT_TX_* */
+  uint8_t flags;         /* bit0 have_tr, bit1 have_bl, bit2 filter_type */
+  uint8_t dcs_ctx;       /* dc_sign context 0..2 */
+  uint8_t skip_ctx;      /* txb_skip context 0..12 */
+  uint16_t reserved;
+  float mode_bits;       /* LossyTile::mode_bits(px, py, mode) of the caller */
+} mt_candidate;
+
+#define MT_CAND_HAVE_TR 1u
+#define MT_CAND_HAVE_BL 2u
+#define MT_CAND_FILTER_TYPE 4u
+
+/* Batch-wide parameters of the chain. */
+typedef struct mt_chain_params {
+  int32_t tx_size;        /* square luma transform size: 8 (4, 16 reserved) */
+  int32_t bd;             /* bit depth (8) */
+  int32_t frame_w, frame_h; /* padded plane size, also the prediction frame bounds */
+  int32_t stride;         /* samples per row of src and recon */
+  float trellis_lambda0;  /* lambda0 * prdo of trellis_optimize; <= 0 disables */
+  float mode_lambda;      /* mlam * prdo, the rd_cost lambda */
+  float satd_scale;       /* partition_rd::luma_satd_scale(base_q, subsampled) */
+  float satd_bridge;      /* K_PART_LAMBDA / k_satd * proxy_luma_scale; 0 = bridge off */
+  int32_t use_skip_bits;  /* 1: skip_bits below replace the txb_skip CDF cost */
+  float skip_bits[2];     /* (all_zero = 1, all_zero = 0) */
+} mt_chain_params;
+
+/* Per-candidate outputs. */
+typedef struct mt_candidate_result {
+  float distortion;       /* luma_partition_distortion */
+  float bits;             /* luma_bits + mode_bits */
+  float cost;             /* rd_cost(distortion, mode_lambda, bits) */
+  uint32_t satd;          /* raw SATD of the reconstruction */
+  int32_t eob;            /* last nonzero scan index after trellis, -1 if none */
+  uint32_t reserved[3];
+} mt_candidate_result;
+
+/* ---- host-side helpers ---------------------------------------------------- */
+
+/* Quant::new_with_qm(base_q_idx, bd, qm_level) for 8-bit luma. */
+int mt_quant_init(uint8_t base_q_idx, uint8_t bd, uint8_t qm_level, mt_quant* out);
+/* Quant::new_chroma_with_delta_qm(base_q_idx, dc_delta, ac_delta, bd, qm_level). */
+int mt_quant_init_chroma(uint8_t base_q_idx, int32_t dc_delta, int32_t ac_delta, uint8_t bd,
+                         uint8_t qm_level, mt_quant* out);
+/* Inverse QM weight row for a w x h transform (qm_row, src/quant.rs:83-89), or
+ * NULL when the level is flat.  Points into a static table. */
+const uint8_t* mt_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h);
+/* Default diagonal scan of a square transform of size n (4, 8, 16, 32). */
+const uint16_t* mt_default_scan(int32_t n);
+/* CoefCostTables-style bit costs of one CDF slice. */
+int mt_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
+
+/* ---- batched kernels ------------------------------------------------------ */
+
+/* The candidate chain over n candidates.  src/recon: u16 planes of
+ * frame_h x stride samples.  qm_row: inverse QM weights of the transform size
+ * (tx_size^2 bytes, column-major rc = x*h + y) or NULL when flat.
+ * levels_out (optional, n * tx_size^2 int32): final quantised levels,
+ * column-major.  recon_out (optional, n * tx_size^2 int32): reconstructed
+ * samples (prediction + inverse residual, clamped), row-major. */
+int mt_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm,
+                       const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                       const mt_candidate* cands, int32_t n, mt_candidate_result* results,
+                       int32_t* levels_out, int32_t* recon_out);
+int mt_candidate_chain_device(const uint16_t* d_src, const uint16_t* d_recon,
+                              const mt_chain_params* prm, const mt_quant* quant,
+                              const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                              const mt_candidate* d_cands, int32_t n,
+                              mt_candidate_result* d_results, int32_t* d_levels_out,
+                              int32_t* d_recon_out, void* stream);
+
+/* Forward transform + quantisation of n residual blocks (row-major int32,
+ * tx_size^2 each) with one tx type per block: levels (column-major int32) and
+ * f32 quantisation targets, with the QM applied as DctDispatch does. */
+int mt_fwd_txfm_quant_device(const int32_t* d_resid, const uint8_t* d_tx_types, int32_t n,
+                             int32_t tx_size, const mt_quant* quant, const uint8_t* d_qm_row,
+                             int32_t* d_levels, float* d_targets, void* stream);
+/* Inverse transform + dequantisation of n level blocks -> row-major residual. */
+int mt_inv_txfm_dequant_device(const int32_t* d_levels, const uint8_t* d_tx_types, int32_t n,
+                               int32_t tx_size, const mt_quant* quant, const uint8_t* d_qm_row,
+                               int32_t* d_resid, void* stream);
+/* trellis_optimize over n blocks in place (levels), one scan for all. */
+int mt_trellis_optimize_device(int32_t* d_levels, const float* d_targets, int32_t n,
+                               int32_t tx_size, float dc_q, float ac_q, float lambda0,
+                               void* stream);
+/* Intra prediction of n candidates (mode/angle/flags from the candidate
+ * records) into pred_out (n * tx_size^2 int32, row-major). */
+int mt_intra_predict_device(const uint16_t* d_recon, const mt_chain_params* prm,
+                            const mt_candidate* d_cands, int32_t n, int32_t* d_pred_out,
+                            void* stream);
+
+/* Library version string. */
+const char* mt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAROONTREE_B200_H */

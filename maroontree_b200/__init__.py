@@ -1,0 +1,101 @@
+"""maroontree_b200: B200-native intra rate-distortion core of the maroontree AVIF
+encoder, behind a C ABI (``include/maroontree_b200.h``).
+
+Python here is a thin host mirror over that ABI (ctypes); the arithmetic runs
+in the sm_100a kernels of ``csrc/``.  There is no CPU fallback: the calls raise
+when the library or a CUDA device is missing.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCosts, Quant, load, ptr)
+
+__all__ = [
+    "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
+    "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
+    "candidate_chain_device", "MtError",
+]
+
+
+class MtError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what} failed with code {code}")
+        self.code = code
+
+
+def _check(rc, what):
+    if rc != abi.MT_OK:
+        raise MtError(rc, what)
+
+
+def quant_new(base_q_idx, bd=8, qm_level=15):
+    """``Quant::new_with_qm`` (src/quant.rs:351-373)."""
+    q = Quant()
+    _check(load().mt_quant_init(base_q_idx, bd, qm_level, C.byref(q)), "mt_quant_init")
+    return q
+
+
+def quant_new_chroma(base_q_idx, dc_delta, ac_delta, bd=8, qm_level=15):
+    """``Quant::new_chroma_with_delta_qm`` (src/quant.rs:393-418)."""
+    q = Quant()
+    _check(load().mt_quant_init_chroma(base_q_idx, dc_delta, ac_delta, bd, qm_level, C.byref(q)),
+           "mt_quant_init_chroma")
+    return q
+
+
+def qm_row(level, chroma, n):
+    """Inverse QM weights of an n x n transform as a numpy array, or None when flat."""
+    p = load().mt_qm_row(level, chroma, n, n)
+    if not p:
+        return None
+    return np.ctypeslib.as_array((C.c_uint8 * (n * n)).from_address(p)).copy()
+
+
+def default_scan(n):
+    p = load().mt_default_scan(n)
+    return np.ctypeslib.as_array((C.c_uint16 * (n * n)).from_address(p)).copy()
+
+
+def coef_costs(cdfs):
+    out = CoefCosts()
+    _check(load().mt_coef_costs_build(C.byref(cdfs), C.byref(out)), "mt_coef_costs_build")
+    return out
+
+
+def chain_params(frame_w, frame_h, stride=None, tx_size=8, trellis_lambda0=0.05, mode_lambda=1.0,
+                 satd_scale=1.25, satd_bridge=0.0, skip_bits=None):
+    p = ChainParams()
+    p.tx_size, p.bd, p.frame_w, p.frame_h = tx_size, 8, frame_w, frame_h
+    p.stride = stride if stride is not None else frame_w
+    p.trellis_lambda0, p.mode_lambda, p.satd_scale, p.satd_bridge = trellis_lambda0, mode_lambda, satd_scale, satd_bridge
+    if skip_bits is not None:
+        p.use_skip_bits = 1
+        p.skip_bits[0], p.skip_bits[1] = skip_bits
+    return p
+
+
+def candidate_chain(src, recon, prm, quant, qmrow, costs, cands, want_levels=False, want_recon=False):
+    """Evaluate the candidate chain with host buffers (copies in and out)."""
+    lib = load()
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    cands = np.ascontiguousarray(cands, CANDIDATE_DTYPE)
+    n = len(cands)
+    N = prm.tx_size * prm.tx_size
+    res = np.zeros(n, RESULT_DTYPE)
+    lv = np.zeros((n, N), np.int32) if want_levels else None
+    ro = np.zeros((n, N), np.int32) if want_recon else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(lib.mt_candidate_chain(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                                  ptr(cands), n, ptr(res), ptr(lv), ptr(ro)), "mt_candidate_chain")
+    return res, lv, ro
+
+
+def candidate_chain_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_cands, n, d_res, d_lv=None, d_ro=None,
+                           stream=0):
+    """Device-pointer form: arguments are torch CUDA tensors (or raw addresses)."""
+    _check(load().mt_candidate_chain_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
+                                            ptr(d_costs), ptr(d_cands), n, ptr(d_res), ptr(d_lv), ptr(d_ro),
+                                            stream or None), "mt_candidate_chain_device")

@@ -1,0 +1,136 @@
+"""ctypes mirror of ``include/maroontree_b200.h`` plus numpy record dtypes for the
+batched arrays.  Loads the in-tree ``_lib/libmaroontree_b200.so``; there is no
+fallback, a missing library raises."""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libmaroontree_b200.so")
+
+MT_OK = 0
+MT_ERR_INVALID_INPUT = -2
+MT_ERR_UNSUPPORTED = -3
+MT_ERR_DEVICE = -10
+MT_ERR_ALLOC = -11
+
+# intra modes (src/intrapred.rs:54-79)
+DC_PRED, V_PRED, H_PRED, D45_PRED, D135_PRED, D113_PRED, D157_PRED, D203_PRED, D67_PRED = range(9)
+SMOOTH_PRED, SMOOTH_V_PRED, SMOOTH_H_PRED, PAETH_PRED = 9, 10, 11, 12
+# 7-type intra transform set order (src/cost.rs:100-103)
+TX_IDTX, TX_DCT_DCT, TX_V_DCT, TX_H_DCT, TX_ADST_ADST, TX_ADST_DCT, TX_DCT_ADST = range(7)
+TX_2D_SCAN_TYPES = (TX_IDTX, TX_DCT_DCT, TX_ADST_ADST, TX_ADST_DCT, TX_DCT_ADST)
+
+CAND_HAVE_TR, CAND_HAVE_BL, CAND_FILTER_TYPE = 1, 2, 4
+
+
+class Quant(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in (
+        "dc_q", "ac_q", "q_mult_dc", "q_mult_ac", "rmin", "rmax", "cmin", "cmax", "cf_max",
+        "qm_level", "qm_chroma", "qidx")]
+
+
+class CoefCdfs(C.Structure):
+    _fields_ = [
+        ("txb_skip", (C.c_uint16 * 2) * 13),
+        ("base_tok", (C.c_uint16 * 4) * 42),
+        ("br_tok", (C.c_uint16 * 4) * 21),
+        ("eob_base", (C.c_uint16 * 3) * 4),
+        ("eob_hi", (C.c_uint16 * 2) * 11),
+        ("eob_bin", C.c_uint16 * 11),
+        ("dc_sign", (C.c_uint16 * 2) * 3),
+        ("txtp", (C.c_uint16 * 16) * 13),
+    ]
+
+
+class CoefCosts(C.Structure):
+    _fields_ = [
+        ("txb_skip", (C.c_float * 2) * 13),
+        ("base_tok", (C.c_float * 4) * 42),
+        ("br_cum", (C.c_float * 13) * 21),
+        ("eob_base", (C.c_float * 3) * 4),
+        ("eob_hi", (C.c_float * 2) * 11),
+        ("eob_bin", C.c_float * 11),
+        ("dc_sign", (C.c_float * 2) * 3),
+        ("txtp", (C.c_float * 16) * 13),
+    ]
+
+
+class ChainParams(C.Structure):
+    _fields_ = [
+        ("tx_size", C.c_int32), ("bd", C.c_int32), ("frame_w", C.c_int32), ("frame_h", C.c_int32),
+        ("stride", C.c_int32), ("trellis_lambda0", C.c_float), ("mode_lambda", C.c_float),
+        ("satd_scale", C.c_float), ("satd_bridge", C.c_float), ("use_skip_bits", C.c_int32),
+        ("skip_bits", C.c_float * 2),
+    ]
+
+
+CANDIDATE_DTYPE = np.dtype([
+    ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"),
+    ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "<u2"), ("mode_bits", "<f4"),
+])
+RESULT_DTYPE = np.dtype([
+    ("distortion", "<f4"), ("bits", "<f4"), ("cost", "<f4"), ("satd", "<u4"), ("eob", "<i4"),
+    ("reserved", "<u4", (3,)),
+])
+assert CANDIDATE_DTYPE.itemsize == 16 and RESULT_DTYPE.itemsize == 32
+
+_P = C.c_void_p
+
+
+def _bind(lib):
+    sig = {
+        "mt_version": (C.c_char_p, []),
+        "mt_quant_init": (C.c_int, [C.c_uint8, C.c_uint8, C.c_uint8, C.POINTER(Quant)]),
+        "mt_quant_init_chroma": (C.c_int, [C.c_uint8, C.c_int32, C.c_int32, C.c_uint8, C.c_uint8, C.POINTER(Quant)]),
+        "mt_qm_row": (_P, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "mt_default_scan": (_P, [C.c_int32]),
+        "mt_coef_costs_build": (C.c_int, [C.POINTER(CoefCdfs), C.POINTER(CoefCosts)]),
+        "mt_candidate_chain": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
+                                         _P, C.c_int32, _P, _P, _P]),
+        "mt_candidate_chain_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
+                                                C.c_int32, _P, _P, _P, _P]),
+        "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
+        "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
+        "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
+        "mt_intra_predict_device": (C.c_int, [_P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises OSError when it is missing or broken)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"maroontree_b200: CUDA library not built ({LIB_PATH}); run python -m maroontree_b200.build")
+        _lib = _bind(C.CDLL(LIB_PATH))
+    return _lib
+
+
+EXPORTED_SYMBOLS = (
+    "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
+    "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_fwd_txfm_quant_device",
+    "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
+)
+
+
+def ptr(a):
+    """Address of a numpy array, torch tensor, ctypes object or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    if isinstance(a, int):
+        return a
+    return C.addressof(a)

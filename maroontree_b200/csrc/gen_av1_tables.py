@@ -1,0 +1,87 @@
+"""Generate ``av1_tables.h``: the normative AV1 data tables the intra RD path needs.
+
+The tables are AV1 specification data (the dav1d runtime forms the reference
+vendors), not algorithm: dequantiser lookups (``Dc_Qlookup``/``Ac_Qlookup``),
+inverse quantisation-matrix weights, default coefficient scans and the
+coefficient-base context offsets.  They must be identical to the reference's
+for byte parity, so this script reads them out of the reference's Rust sources
+once and writes a C header that is committed; nothing at run time reads the
+reference.
+
+Usage (from the repository root, with the reference checkout available)::
+
+    python maroontree_b200/csrc/gen_av1_tables.py <reference-root>
+
+Source locations (reference paths):
+  src/coef_q.rs     DC_QLOOKUP_8, AC_QLOOKUP_8, SCAN_16X16, SCAN_32X32
+  src/tables.rs     SCAN_8X8, SCAN_4X4, LO_CTX_OFF, LO_CTX_OFF_WLH, LO_CTX_OFF_WGH
+  src/qm_tables.rs  AV1_IQM  ([15][2][3344] u8)
+"""
+import os
+import re
+import sys
+
+TABLES = [
+    # (file, rust name, C name, C type)
+    ("src/coef_q.rs", "DC_QLOOKUP_8", "MT_DC_QLOOKUP_8", "uint16_t"),
+    ("src/coef_q.rs", "AC_QLOOKUP_8", "MT_AC_QLOOKUP_8", "uint16_t"),
+    ("src/skip_tables.rs", "SCAN_4X4", "MT_SCAN_4X4", "uint16_t"),
+    ("src/tables.rs", "SCAN_8X8", "MT_SCAN_8X8", "uint16_t"),
+    ("src/coef_q.rs", "SCAN_16X16", "MT_SCAN_16X16", "uint16_t"),
+    ("src/coef_q.rs", "SCAN_32X32", "MT_SCAN_32X32", "uint16_t"),
+    ("src/tables.rs", "LO_CTX_OFF", "MT_LO_CTX_OFF", "uint8_t"),
+    ("src/tables.rs", "LO_CTX_OFF_WLH", "MT_LO_CTX_OFF_WLH", "uint8_t"),
+    ("src/tables.rs", "LO_CTX_OFF_WGH", "MT_LO_CTX_OFF_WGH", "uint8_t"),
+    ("src/qm_tables.rs", "AV1_IQM", "MT_AV1_IQM", "uint8_t"),
+]
+
+
+def extract(path, name):
+    text = open(path, encoding="utf-8").read()
+    m = re.search(r"static\s+" + re.escape(name) + r"\s*:\s*([^=]+)=\s*\[", text)
+    if not m:
+        raise SystemExit(f"{name} not found in {path}")
+    i = m.end() - 1
+    depth = 0
+    j = i
+    while True:
+        c = text[j]
+        if c == "[":
+            depth += 1
+        elif c == "]":
+            depth -= 1
+            if depth == 0:
+                break
+        j += 1
+    body = re.sub(r"//[^\n]*", "", text[i : j + 1])
+    nums = [int(v) for v in re.findall(r"-?\d+", body)]
+    dims = [int(d) for d in re.findall(r";\s*([A-Z_0-9]+|\d+)\s*\]", m.group(1)) if d.isdigit()]
+    return nums, m.group(1).strip()
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "av1_tables.h")
+    lines = [
+        "/* Generated by gen_av1_tables.py: normative AV1 tables (dequantiser lookups,",
+        " * inverse quantisation matrices, default scans, coefficient-base context",
+        " * offsets).  Do not edit. */",
+        "#pragma once",
+        "#include <stdint.h>",
+        "",
+    ]
+    for rel, rname, cname, ctype in TABLES:
+        nums, decl = extract(os.path.join(ref, rel), rname)
+        lines.append(f"/* {rel} {rname}: {decl} ({len(nums)} values) */")
+        lines.append(f"#define {cname}_LEN {len(nums)}")
+        lines.append(f"static const {ctype} {cname}[{len(nums)}] = {{")
+        for k in range(0, len(nums), 24):
+            lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
+        lines.append("};")
+        lines.append("")
+    open(out, "w").write("\n".join(lines))
+    print("wrote", out)
+
+
+if __name__ == "__main__":
+    main()

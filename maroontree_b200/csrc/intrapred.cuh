@@ -1,0 +1,233 @@
+// Device AV1 intra prediction for one block per thread (src/intrapred.rs:1357-1810
+// semantics): edge gathering with the reference's availability and fill rules,
+// corner/edge filtering, 2x edge upsampling, directional zones 1-3, PAETH,
+// SMOOTH*, and DC.  Edges live in a per-thread array with logical origin 2
+// (indices -2 .. 2*(bw+bh)), the reference's IntraEdge layout.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/maroontree_b200.h"
+#include "common.cuh"
+
+namespace mtd {
+
+__constant__ int16_t kDrDeriv[44] = {0,  1023, 0,  547, 372, 0,  0,  273, 215, 0,  178, 151, 0,  132, 116,
+                                     0,  102,  0,  90,  80,  0,  71, 64,  0,   57, 51,  0,   45, 0,   40,
+                                     35, 0,    31, 27,  0,   23, 19, 0,   15,  0,  11,  0,   7,  3};
+__constant__ int16_t kSmW8[8] = {255, 197, 146, 105, 73, 50, 37, 32};
+
+constexpr int kEdgeOrigin = 2;
+constexpr int kEdgeCap8 = 2 + 2 * 16 + 4;  // bw = bh = 8: upsampled reach 2*16
+
+__device__ __forceinline__ int edge_strength(int w, int h, bool ft, int delta) {
+  const int d = abs(delta), wh = w + h;
+  int s = 0;
+  if (!ft) {
+    if (wh <= 8) s = d >= 56;
+    else if (wh <= 16) s = d >= 40;
+    else if (wh <= 24) s = d >= 32 ? 3 : (d >= 16 ? 2 : (d >= 8 ? 1 : 0));
+    else if (wh <= 32) s = d >= 32 ? 3 : (d >= 4 ? 2 : (d >= 1 ? 1 : 0));
+    else s = d >= 1 ? 3 : 0;
+  } else {
+    if (wh <= 8) s = d >= 64 ? 2 : (d >= 40 ? 1 : 0);
+    else if (wh <= 16) s = d >= 48 ? 2 : (d >= 20 ? 1 : 0);
+    else if (wh <= 24) s = d >= 4 ? 3 : 0;
+    else s = d >= 1 ? 3 : 0;
+  }
+  return s;
+}
+
+// 5-tap edge smoothing of positions 0..size-2 from the unfiltered window
+// src[k] = edge[k-1] with clamped reads (src/intrapred.rs:977-1012).
+template <int CAP>
+__device__ __forceinline__ void filter_edge(int32_t* e, int size, int strength) {
+  if (strength == 0) return;
+  int32_t k0, k1, k2;  // symmetric taps: (k0, k1, k2, k1, k0)
+  if (strength == 1) { k0 = 0; k1 = 4; k2 = 8; }
+  else if (strength == 2) { k0 = 0; k1 = 5; k2 = 6; }
+  else { k0 = 2; k1 = 4; k2 = 4; }
+  int32_t src[CAP];
+  for (int i = 0; i < size; i++) src[i] = e[kEdgeOrigin + i - 1];
+  const int last = size - 1;
+  for (int o = 0; o < size - 1; o++) {
+    const int32_t a = src[max(o - 1, 0)], b = src[min(max(o, 0), last)], c = src[min(o + 1, last)];
+    const int32_t d = src[min(o + 2, last)], f = src[min(o + 3, last)];
+    e[kEdgeOrigin + o] = (k0 * a + k1 * b + k2 * c + k1 * d + k0 * f + 8) >> 4;
+  }
+}
+
+// 2x upsampling of num_px edge samples (src/intrapred.rs:1026-1048).
+template <int CAP>
+__device__ __forceinline__ void upsample_edge(int32_t* e, int num_px, int32_t maxv) {
+  int32_t in[CAP];
+  in[0] = e[kEdgeOrigin - 1];
+  in[1] = e[kEdgeOrigin - 1];
+  for (int i = 0; i < num_px; i++) in[i + 2] = e[kEdgeOrigin + i];
+  in[num_px + 2] = e[kEdgeOrigin + num_px - 1];
+  e[kEdgeOrigin - 2] = in[0];
+  for (int i = 0; i < num_px; i++) {
+    const int32_t v = -in[i] + 9 * in[i + 1] + 9 * in[i + 2] - in[i + 3];
+    e[kEdgeOrigin + 2 * i - 1] = clampi((v + 8) >> 4, 0, maxv);
+    e[kEdgeOrigin + 2 * i] = in[i + 2];
+  }
+}
+
+// DC predictor (src/intrapred.rs:1740-1789) for square power-of-two blocks.
+__device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, int stride, int ox, int oy, int n,
+                                              int log2n, int bd) {
+  const bool top = oy > 0, left = ox > 0;
+  int32_t sum = 0;
+  if (top)
+    for (int x = 0; x < n; x++) sum += rec[(size_t)(oy - 1) * stride + ox + x];
+  if (left)
+    for (int y = 0; y < n; y++) sum += rec[(size_t)(oy + y) * stride + ox - 1];
+  if (top && left) return (n + sum) >> (log2n + 1);
+  if (top || left) return ((n >> 1) + sum) >> log2n;
+  return 1 << (bd - 1);
+}
+
+// Prediction of an 8x8 block into out[64] (row-major).
+__device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
+                         int delta, bool have_tr, bool have_bl, bool ft, int bd, int32_t* __restrict__ out) {
+  constexpr int bw = 8, bh = 8, edge_len = 16;
+  if (mode == MT_DC_PRED) {
+    const int32_t d = dc_pred_sq(rec, stride, ox, oy, 8, 3, bd);
+    for (int i = 0; i < 64; i++) out[i] = d;
+    return;
+  }
+  int32_t A[kEdgeCap8], L[kEdgeCap8];
+  for (int i = 0; i < kEdgeCap8; i++) A[i] = L[i] = 0;
+  const bool have_top = oy > 0, have_left = ox > 0;
+  const int32_t base = 1 << (bd - 1);
+  const uint16_t* up = rec + (size_t)(oy - 1) * stride + ox;     // valid when have_top
+  const uint16_t* lf = rec + (size_t)oy * stride + ox - 1;       // valid when have_left
+  if (have_top) {
+    for (int i = 0; i < bw; i++) A[kEdgeOrigin + i] = up[i];
+  } else {
+    const int32_t fill = have_left ? (int32_t)lf[0] : base - 1;
+    for (int i = 0; i < edge_len; i++) A[kEdgeOrigin + i] = fill;
+  }
+  if (have_left) {
+    for (int j = 0; j < bh; j++) L[kEdgeOrigin + j] = lf[(size_t)j * stride];
+  } else {
+    const int32_t fill = have_top ? (int32_t)up[0] : base + 1;
+    for (int i = 0; i < edge_len; i++) L[kEdgeOrigin + i] = fill;
+  }
+  const int32_t corner =
+      have_left ? (have_top ? (int32_t)up[-1] : (int32_t)lf[0]) : (have_top ? (int32_t)up[0] : base);
+  A[kEdgeOrigin - 1] = corner;
+  L[kEdgeOrigin - 1] = corner;
+  if (have_top) {
+    const int px_have = have_tr ? min(bw, max(fw - (ox + bw), 0)) : 0;
+    for (int i = 0; i < px_have; i++) A[kEdgeOrigin + bw + i] = up[bw + i];
+    const int32_t fill = A[kEdgeOrigin + bw + px_have - 1];
+    for (int i = bw + px_have; i < edge_len; i++) A[kEdgeOrigin + i] = fill;
+  }
+  if (have_left) {
+    const int px_have = have_bl ? min(bh, max(fh - (oy + bh), 0)) : 0;
+    for (int i = 0; i < px_have; i++) L[kEdgeOrigin + bh + i] = lf[(size_t)(bh + i) * stride];
+    const int32_t fill = L[kEdgeOrigin + bh + px_have - 1];
+    for (int i = bh + px_have; i < edge_len; i++) L[kEdgeOrigin + i] = fill;
+  }
+  const bool directional = mode >= MT_V_PRED && mode <= MT_D67_PRED;
+  if (directional) {
+    const int base_angle[9] = {0, 90, 180, 45, 135, 113, 157, 203, 67};
+    const int angle = base_angle[mode] + delta * 3;
+    int up_a = 0, up_l = 0;
+    if (angle != 90 && angle != 180) {
+      // edge_len 16 < 24: no corner filter for 8x8.
+      filter_edge<kEdgeCap8>(A, bw + 1 + (angle < 90 ? bh : 0), edge_strength(bw, bh, ft, angle - 90));
+      filter_edge<kEdgeCap8>(L, bh + 1 + (angle > 180 ? bw : 0), edge_strength(bh, bw, ft, angle - 180));
+      const int da = abs(angle - 90), dl = abs(angle - 180);
+      const int lim = ft ? 8 : 16;
+      up_a = (da != 0 && da < 40 && bw + bh <= lim);
+      up_l = (dl != 0 && dl < 40 && bw + bh <= lim);
+      const int32_t maxv = (1 << bd) - 1;
+      if (up_a) upsample_edge<kEdgeCap8>(A, bw + (angle < 90 ? bh : 0), maxv);
+      if (up_l) upsample_edge<kEdgeCap8>(L, bh + (angle > 180 ? bw : 0), maxv);
+    }
+    const int32_t* a = A + kEdgeOrigin;  // logical index 0
+    const int32_t* l = L + kEdgeOrigin;
+    if (angle == 90) {
+      for (int y = 0; y < bh; y++)
+        for (int x = 0; x < bw; x++) out[y * bw + x] = a[x];
+    } else if (angle == 180) {
+      for (int y = 0; y < bh; y++)
+        for (int x = 0; x < bw; x++) out[y * bw + x] = l[y];
+    } else if (angle < 90) {
+      const int dx = kDrDeriv[angle >> 1];
+      const int max_base_x = (edge_len - 1) << up_a;
+      const int frac_bits = 6 - up_a, inc = 1 << up_a;
+      for (int y = 0; y < bh; y++) {
+        const int xpos = dx * (y + 1);
+        const int shift = ((xpos << up_a) & 0x3f) >> 1;
+        const int b0 = xpos >> frac_bits;
+        for (int x = 0; x < bw; x++) {
+          const int b = b0 + x * inc;
+          out[y * bw + x] = b < max_base_x ? (a[b] * (32 - shift) + a[b + 1] * shift + 16) >> 5 : a[max_base_x];
+        }
+      }
+    } else if (angle > 180) {
+      const int dy = kDrDeriv[(270 - angle) >> 1];
+      const int max_base_y = (edge_len - 1) << up_l;
+      const int frac_bits = 6 - up_l, inc = 1 << up_l;
+      for (int y = 0; y < bh; y++)
+        for (int x = 0; x < bw; x++) {
+          const int ypos = dy * (x + 1);
+          const int shift = ((ypos << up_l) & 0x3f) >> 1;
+          const int b = (ypos >> frac_bits) + y * inc;
+          out[y * bw + x] = b >= max_base_y ? l[max_base_y] : (l[b] * (32 - shift) + l[b + 1] * shift + 16) >> 5;
+        }
+    } else {
+      const int dy = kDrDeriv[(angle - 90) >> 1];
+      const int dx = kDrDeriv[(180 - angle) >> 1];
+      for (int y = 0; y < bh; y++) {
+        const int t = (y + 1) * dx - 64;
+        const int x0 = t <= 0 ? 0 : min((t + 63) >> 6, bw);
+        const int xpos0 = (x0 << 6) - (y + 1) * dx;
+        const int ba0 = xpos0 >> (6 - up_a);
+        const int sha = ((xpos0 * (1 << up_a)) & 0x3f) >> 1;
+        for (int x = 0; x < bw; x++) {
+          if (x < x0) {
+            const int ypos = (y << 6) - (x + 1) * dy;
+            const int b = ypos >> (6 - up_l);
+            const int sh = ((ypos * (1 << up_l)) & 0x3f) >> 1;
+            out[y * bw + x] = (l[b] * (32 - sh) + l[b + 1] * sh + 16) >> 5;
+          } else {
+            const int b = ba0 + (x - x0) * (1 << up_a);
+            out[y * bw + x] = (a[b] * (32 - sha) + a[b + 1] * sha + 16) >> 5;
+          }
+        }
+      }
+    }
+    return;
+  }
+  const int32_t* a = A + kEdgeOrigin;
+  const int32_t* l = L + kEdgeOrigin;
+  if (mode == MT_PAETH_PRED) {
+    for (int y = 0; y < bh; y++)
+      for (int x = 0; x < bw; x++) {
+        const int32_t lv = l[y], tv = a[x], b = lv + tv - corner;
+        const int32_t ld = abs(lv - b), td = abs(tv - b), cd = abs(corner - b);
+        out[y * bw + x] = (ld <= td && ld <= cd) ? lv : (td <= cd ? tv : corner);
+      }
+  } else if (mode == MT_SMOOTH_PRED) {
+    const int32_t right = a[bw - 1], bottom = l[bh - 1];
+    for (int y = 0; y < bh; y++)
+      for (int x = 0; x < bw; x++) {
+        const int32_t wv = kSmW8[y], wh = kSmW8[x];
+        const int32_t p = wv * a[x] + (256 - wv) * bottom + wh * l[y] + (256 - wh) * right;
+        out[y * bw + x] = (p + 256) >> 9;
+      }
+  } else if (mode == MT_SMOOTH_V_PRED) {
+    const int32_t bottom = l[bh - 1];
+    for (int y = 0; y < bh; y++)
+      for (int x = 0; x < bw; x++) out[y * bw + x] = (kSmW8[y] * a[x] + (256 - kSmW8[y]) * bottom + 128) >> 8;
+  } else {  // SMOOTH_H
+    const int32_t right = a[bw - 1];
+    for (int y = 0; y < bh; y++)
+      for (int x = 0; x < bw; x++) out[y * bw + x] = (kSmW8[x] * l[y] + (256 - kSmW8[x]) * right + 128) >> 8;
+  }
+}
+
+}  // namespace mtd

@@ -1,0 +1,69 @@
+/*
+ * Oracle: CPU restatement of the reference's intra RD kernels, used ONLY as the
+ * checker of the CUDA path (tests, smoke, the bench's CPU-baseline leg).  It is
+ * test infrastructure, not part of the product; nothing in maroontree_b200/
+ * links or calls it.
+ *
+ * Each function follows the reference (awxkee/maroontree) file:line named in
+ * its comment, in the arithmetic order of the x86-64 build with AVX2+FMA
+ * detected at run time (the AVX2 float sites are named where they differ from
+ * the scalar Rust).  Integer arithmetic wraps (built with -fwrapv) like Rust
+ * release builds; floats are IEEE binary32 without contraction
+ * (-ffp-contract=off) except where the AVX2 reference uses an explicit FMA.
+ */
+#ifndef MT_ORACLE_H
+#define MT_ORACLE_H
+#include <stdint.h>
+#include "../include/maroontree_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int or_quant_init(uint8_t base_q_idx, uint8_t bd, uint8_t qm_level, mt_quant* out);
+int or_quant_init_chroma(uint8_t base_q_idx, int32_t dc_delta, int32_t ac_delta, uint8_t bd,
+                         uint8_t qm_level, mt_quant* out);
+const uint8_t* or_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h);
+const uint16_t* or_default_scan(int32_t n);
+
+/* dct.rs: forward transform + quantisation of one n x n block (n = 8). */
+void or_fwd_txfm_quant(const int32_t* resid, int32_t tx_type, int32_t n, const mt_quant* q,
+                       const uint8_t* qm_row, int32_t* levels, float* targets);
+/* idct.rs: dequantisation + inverse transform of one block. */
+void or_inv_txfm_dequant(const int32_t* levels, int32_t tx_type, int32_t n, const mt_quant* q,
+                         const uint8_t* qm_row, int32_t* resid);
+/* trellis.rs:944 trellis_optimize (AVX2 step-A order). */
+void or_trellis_optimize(int32_t* cf, const float* tf, float dc_q, float ac_q,
+                         const uint16_t* scan, int32_t n, float lambda0);
+/* intrapred.rs:1357 intra_predict_nd_ad_impl (non-DC modes) and :1740 dc_pred. */
+void or_intra_predict(const uint16_t* recon, int32_t stride, int32_t ox, int32_t oy, int32_t bw,
+                      int32_t bh, int32_t mode, int32_t angle_delta, int32_t have_tr,
+                      int32_t have_bl, int32_t fw, int32_t fh, int32_t filter_type, int32_t bd,
+                      int32_t* out);
+int32_t or_dc_pred(const uint16_t* recon, int32_t stride, int32_t ox, int32_t oy, int32_t w,
+                   int32_t h, int32_t bd);
+/* partition_rd.rs:86 luma_satd_scalar. */
+uint64_t or_luma_satd(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w,
+                      int32_t h, int32_t max_value, const int32_t* pred, const int32_t* resid);
+/* cost.rs:156 cost_q_table / cdf_cost_with_table. */
+float or_cdf_cost(const uint16_t* cdf, int32_t s);
+/* rate.rs:149 real_block_bits_bounded (bound = +inf) for a square luma block. */
+float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int32_t cls,
+                         const mt_coef_cdfs* cdfs, int32_t skip_ctx, int32_t dcs_ctx,
+                         int32_t y_mode, int32_t txtp, int32_t use_skip_bits,
+                         const float* skip_bits);
+/* rate.rs:58 CoefCostTables::build and the other per-symbol costs. */
+void or_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
+/* The candidate chain of partition_search.rs:467-530, per candidate. */
+int or_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm,
+                       const mt_quant* quant, const uint8_t* qm_row, const mt_coef_cdfs* cdfs,
+                       const mt_candidate* cands, int32_t n, mt_candidate_result* results,
+                       int32_t* levels_out, int32_t* recon_out, int32_t threads);
+
+int or_edge_filter_strength(int w, int h, int filter_type, int delta);
+int or_use_edge_upsample(int w, int h, int filter_type, int delta);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

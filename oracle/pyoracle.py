@@ -1,0 +1,142 @@
+"""ctypes bindings of the oracle library (test infrastructure: the CPU checker
+of the CUDA path; see oracle.h).  Only tests, ``__graft_entry__.smoke`` and the
+bench's CPU-baseline leg load this."""
+import ctypes as C
+import os
+
+import numpy as np
+
+from maroontree_b200 import abi
+
+from . import build as _build
+
+_lib = None
+_P = C.c_void_p
+
+
+def load():
+    global _lib
+    if _lib is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            path = _build.build()
+        lib = C.CDLL(path)
+        sig = {
+            "or_quant_init": (C.c_int, [C.c_uint8, C.c_uint8, C.c_uint8, C.POINTER(abi.Quant)]),
+            "or_quant_init_chroma": (C.c_int, [C.c_uint8, C.c_int32, C.c_int32, C.c_uint8, C.c_uint8,
+                                               C.POINTER(abi.Quant)]),
+            "or_qm_row": (_P, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+            "or_default_scan": (_P, [C.c_int32]),
+            "or_fwd_txfm_quant": (None, [_P, C.c_int32, C.c_int32, C.POINTER(abi.Quant), _P, _P, _P]),
+            "or_inv_txfm_dequant": (None, [_P, C.c_int32, C.c_int32, C.POINTER(abi.Quant), _P, _P]),
+            "or_trellis_optimize": (None, [_P, _P, C.c_float, C.c_float, _P, C.c_int32, C.c_float]),
+            "or_intra_predict": (None, [_P] + [C.c_int32] * 13 + [_P]),
+            "or_dc_pred": (C.c_int32, [_P] + [C.c_int32] * 6),
+            "or_luma_satd": (C.c_uint64, [_P] + [C.c_int32] * 6 + [_P, _P]),
+            "or_cdf_cost": (C.c_float, [_P, C.c_int32]),
+            "or_real_block_bits": (C.c_float, [_P, _P, C.c_int32, C.c_int32, C.POINTER(abi.CoefCdfs), C.c_int32,
+                                               C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
+            "or_edge_filter_strength": (C.c_int, [C.c_int] * 4),
+            "or_use_edge_upsample": (C.c_int, [C.c_int] * 4),
+            "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
+            "or_candidate_chain": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), C.POINTER(abi.Quant), _P,
+                                             C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def p(a):
+    return None if a is None else a.ctypes.data
+
+
+def quant_new(qidx, bd=8, qm_level=15):
+    q = abi.Quant()
+    assert load().or_quant_init(qidx, bd, qm_level, C.byref(q)) == 0
+    return q
+
+
+def quant_new_chroma(qidx, dc_delta, ac_delta, bd=8, qm_level=15):
+    q = abi.Quant()
+    assert load().or_quant_init_chroma(qidx, dc_delta, ac_delta, bd, qm_level, C.byref(q)) == 0
+    return q
+
+
+def qm_row(level, chroma, n):
+    a = load().or_qm_row(level, chroma, n, n)
+    if not a:
+        return None
+    return np.ctypeslib.as_array((C.c_uint8 * (n * n)).from_address(a)).copy()
+
+
+def default_scan(n):
+    a = load().or_default_scan(n)
+    return np.ctypeslib.as_array((C.c_uint16 * (n * n)).from_address(a)).copy()
+
+
+def fwd_txfm_quant(resid, tx_type, q, qm):
+    resid = np.ascontiguousarray(resid, np.int32).reshape(-1)
+    n = int(round(len(resid) ** 0.5))
+    cf = np.zeros(n * n, np.int32)
+    tf = np.zeros(n * n, np.float32)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    load().or_fwd_txfm_quant(p(resid), tx_type, n, C.byref(q), p(qm), p(cf), p(tf))
+    return cf, tf
+
+
+def inv_txfm_dequant(levels, tx_type, q, qm):
+    levels = np.ascontiguousarray(levels, np.int32).reshape(-1)
+    n = int(round(len(levels) ** 0.5))
+    out = np.zeros(n * n, np.int32)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    load().or_inv_txfm_dequant(p(levels), tx_type, n, C.byref(q), p(qm), p(out))
+    return out
+
+
+def trellis_optimize(cf, tf, dc_q, ac_q, scan, lambda0):
+    cf = np.ascontiguousarray(cf, np.int32).copy()
+    tf = np.ascontiguousarray(tf, np.float32)
+    scan = np.ascontiguousarray(scan, np.uint16)
+    load().or_trellis_optimize(p(cf), p(tf), dc_q, ac_q, p(scan), len(scan), lambda0)
+    return cf
+
+
+def intra_predict(recon, ox, oy, bw, bh, mode, delta=0, have_tr=False, have_bl=False, filter_type=False, bd=8,
+                  fw=None, fh=None):
+    recon = np.ascontiguousarray(recon, np.uint16)
+    h, w = recon.shape
+    out = np.zeros(bw * bh, np.int32)
+    load().or_intra_predict(p(recon), w, ox, oy, bw, bh, mode, delta, int(have_tr), int(have_bl),
+                            fw if fw is not None else w, fh if fh is not None else h, int(filter_type), bd, p(out))
+    return out.reshape(bh, bw)
+
+
+def cdf_cost(cdf, s):
+    cdf = np.ascontiguousarray(cdf, np.uint16)
+    return load().or_cdf_cost(p(cdf), s)
+
+
+def coef_costs(cdfs):
+    out = abi.CoefCosts()
+    load().or_coef_costs_build(C.byref(cdfs), C.byref(out))
+    return out
+
+
+def candidate_chain(src, recon, prm, q, qm, cdfs, cands, want_levels=False, want_recon=False, threads=1):
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    cands = np.ascontiguousarray(cands, abi.CANDIDATE_DTYPE)
+    n = len(cands)
+    N = prm.tx_size * prm.tx_size
+    res = np.zeros(n, abi.RESULT_DTYPE)
+    lv = np.zeros((n, N), np.int32) if want_levels else None
+    ro = np.zeros((n, N), np.int32) if want_recon else None
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    rc = load().or_candidate_chain(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(cands), n,
+                                   p(res), p(lv), p(ro), threads)
+    assert rc == 0, rc
+    return res, lv, ro
