@@ -139,6 +139,10 @@ typedef struct mt_chain_params {
   float skip_bits[2];     /* (all_zero = 1, all_zero = 0) */
 } mt_chain_params;
 
+/* eob value of a candidate the kernel rejected (block outside the frame, or a
+ * mode / type / context index out of range); its other outputs are zero. */
+#define MT_EOB_INVALID (-2)
+
 /* Per-candidate outputs. */
 typedef struct mt_candidate_result {
   float distortion;       /* luma_partition_distortion */

@@ -9,227 +9,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "intrapred.cuh"
-#include "txfm8.cuh"
+#include "chain8.cuh"
 
 namespace mtd {
-
-__constant__ uint8_t kScan8[64] = {0,  8,  1,  2,  9,  16, 24, 17, 10, 3,  4,  11, 18, 25, 32, 40,
-                                   33, 26, 19, 12, 5,  6,  13, 20, 27, 34, 41, 48, 56, 49, 42, 35,
-                                   28, 21, 14, 7,  15, 22, 29, 36, 43, 50, 57, 58, 51, 44, 37, 30,
-                                   23, 31, 38, 45, 52, 59, 60, 53, 46, 39, 47, 54, 61, 62, 55, 63};
-// Coefficient-base position offsets for square transforms, [min(y,4)][min(x,4)].
-__constant__ uint8_t kLoCtxOff[25] = {0, 1, 6, 6, 21, 1, 6, 6, 21, 21, 6, 6, 21, 21, 21,
-                                      6, 21, 21, 21, 21, 21, 21, 21, 21, 21};
-// Static per-level trellis rate (src/cost.rs:70-75).
-__constant__ float kCoefRateLut[64] = {
-    0.9f,  2.7f,  3.6f,  5.3f,  5.3f,  5.3f,  6.6f,  6.6f,  6.6f,  7.9f,  7.9f,  7.9f,  9.2f,
-    9.2f,  9.2f,  11.5f, 13.5f, 13.5f, 15.5f, 15.5f, 15.5f, 15.5f, 17.5f, 17.5f, 17.5f, 17.5f,
-    17.5f, 17.5f, 17.5f, 17.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f,
-    19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f,
-    21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f};
-
-__device__ __forceinline__ float coef_rate_bits(uint32_t level) {
-  if (level < 64) return kCoefRateLut[level];
-  float b = 4.0f;
-  const int32_t total_br = min((int32_t)level - 3, 12);
-  b = __fadd_rn(b, __fmul_rn((float)(total_br / 3 + 1), 1.3f));
-  if (level >= 15) b = __fadd_rn(b, __fadd_rn(__fmul_rn(2.0f, (float)(32 - __clz(level - 15 + 1))), -1.0f));
-  return b;
-}
-__device__ __forceinline__ float golomb_cost(uint32_t v) { return (float)(2 * (32 - __clz(v + 1)) - 1); }
-__device__ __forceinline__ uint8_t level_byte(uint32_t m) {
-  return m == 0 ? 0 : (m <= 2 ? (uint8_t)(m * 0x41) : (uint8_t)(min(m, 15u) + 0xC0));
-}
-
-// One trellis round-down lane in the AVX2 FMA form (src/avx/trellis.rs:79-118)
-// or the scalar fallback form (src/avx/trellis.rs:139-161): returns true when
-// the level should drop by one.
-__device__ __forceinline__ bool round_down_fma(float at, int32_t li, float q2, float lambda) {
-  const int32_t ldi = max(li - 1, 0);
-  const float el = __fsub_rn(at, (float)li), ed = __fsub_rn(at, (float)ldi);
-  const float cl = __fmaf_rn(q2, __fmul_rn(el, el), __fmul_rn(lambda, kCoefRateLut[li]));
-  const float cd = __fmaf_rn(q2, __fmul_rn(ed, ed), __fmul_rn(lambda, kCoefRateLut[ldi]));
-  return cd < cl;
-}
-__device__ __forceinline__ bool round_down_plain(float at, uint32_t l, float q2, float lambda) {
-  const float el = __fsub_rn(at, (float)l), ed = __fsub_rn(at, (float)(l - 1));
-  const float cl = __fadd_rn(__fmul_rn(q2, __fmul_rn(el, el)), __fmul_rn(lambda, coef_rate_bits(l)));
-  const float cd = __fadd_rn(__fmul_rn(q2, __fmul_rn(ed, ed)), __fmul_rn(lambda, coef_rate_bits(l - 1)));
-  return cd < cl;
-}
-
-// trellis_optimize (src/trellis.rs:944-1030) over the 8x8 default scan, with
-// step A in the pinned AVX2 chunking (8-wide, then 4-wide, then scalar tail;
-// a chunk holding a level >= 64 takes the scalar form for all its lanes).
-__device__ void trellis8(int32_t* cf, const float* tf, float dc_q, float ac_q, float lambda) {
-  const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
-  int eob_idx = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) { eob_idx = i; break; }
-  if (eob_idx < 0) return;
-  const int m = eob_idx + 1;
-  int i = 0;
-  for (int w = 8; w >= 4; w >>= 1) {
-    while (i + w <= m) {
-      bool big = false;
-      for (int k = 0; k < w; k++) big |= uabs(cf[kScan8[i + k]]) > 63;
-      uint32_t mask = 0;
-      for (int k = 0; k < w; k++) {
-        const int rc = kScan8[i + k];
-        const int32_t c = cf[rc];
-        const float q2 = rc == 0 ? dq2 : aq2;
-        const float at = fabsf(tf[rc]);
-        if (big) {
-          if (c != 0 && round_down_plain(at, uabs(c), q2, lambda)) mask |= 1u << k;
-        } else if (round_down_fma(at, (int32_t)uabs(c), q2, lambda)) {
-          mask |= 1u << k;
-        }
-      }
-      for (int k = 0; k < w; k++)
-        if (mask >> k & 1) {
-          const int rc = kScan8[i + k];
-          const int32_t c = cf[rc];
-          if (c != 0) cf[rc] = c < 0 ? c + 1 : c - 1;
-        }
-      i += w;
-    }
-  }
-  for (; i < m; i++) {
-    const int rc = kScan8[i];
-    const int32_t c = cf[rc];
-    if (c != 0 && round_down_plain(fabsf(tf[rc]), uabs(c), rc == 0 ? dq2 : aq2, lambda))
-      cf[rc] = c < 0 ? c + 1 : c - 1;
-  }
-  // Suffix sums of the zeroing distortion, exact right-to-left order.
-  float suf[65];
-  suf[m] = 0.0f;
-  for (int e = m - 1; e >= 0; e--) {
-    const int rc = kScan8[e];
-    const float at = fabsf(tf[rc]);
-    suf[e] = __fadd_rn(suf[e + 1], __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
-  }
-  int best_e = -1;
-  float best = __int_as_float(0x7f800000);
-  float pre = 0.0f;
-  for (int e = 0; e < m; e++) {
-    const int rc = kScan8[e];
-    const float at = fabsf(tf[rc]);
-    const uint32_t l = uabs(cf[rc]);
-    const float ecur = __fsub_rn(at, (float)l);
-    const float dcur = __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(ecur, ecur));
-    if (l != 0) {
-      const int bin = e < 2 ? e : 32 - __clz(e);
-      const int extra = bin > 1 ? bin - 2 : 0;
-      const float sig = __fadd_rn(__fmul_rn((float)bin, 0.9f), __fadd_rn((float)extra, 2.0f));
-      const float c = __fadd_rn(__fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, sig)), suf[e + 1]);
-      if (c < best) { best = c; best_e = e; }
-    }
-    pre = __fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, coef_rate_bits(l)));
-  }
-  const float skip = __fadd_rn(suf[0], __fmul_rn(lambda, 1.0f));
-  const int keep = (best_e < 0 || skip < best) ? 0 : best_e + 1;
-  for (int e = keep; e < m; e++) cf[kScan8[e]] = 0;
-}
-
-// Coefficient rate of an 8x8 luma block (src/rate.rs:149-291) from the
-// host-built bit costs; float additions in the reference's order.
-__device__ float rate8(const int32_t* cf, const mt_coef_costs& C, int skip_ctx, int dcs, int mode, int tx,
-                       bool use_skip_bits, float skip1, float skip0, int* eob_out) {
-  int eob = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) { eob = i; break; }
-  *eob_out = eob;
-  if (eob < 0) return use_skip_bits ? skip1 : C.txb_skip[skip_ctx][1];
-  float bits = use_skip_bits ? skip0 : C.txb_skip[skip_ctx][0];
-  bits = __fadd_rn(bits, C.txtp[mode][tx]);
-  const float* dcs_c = C.dc_sign[dcs];
-  auto hi_tok = [&](uint32_t m, int bc) -> float {
-    float h = C.br_cum[bc][min((int32_t)m - 3, 12)];
-    if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
-    return h;
-  };
-  if (eob == 0) {
-    const uint32_t m = uabs(cf[0]), mm = min(m, 3u);
-    bits = __fadd_rn(bits, C.eob_bin[0]);
-    bits = __fadd_rn(bits, C.eob_base[0][mm - 1]);
-    if (mm == 3) bits = __fadd_rn(bits, hi_tok(m, 0));
-    return __fadd_rn(bits, dcs_c[cf[0] < 0]);
-  }
-  const int eob_bin = eob < 2 ? eob : 32 - __clz(eob);
-  bits = __fadd_rn(bits, C.eob_bin[eob_bin]);
-  if (eob_bin > 1) {
-    const int nb = eob_bin - 2;
-    bits = __fadd_rn(bits, C.eob_hi[eob_bin][(eob >> nb) & 1]);
-    bits = __fadd_rn(bits, (float)nb);
-  }
-  uint8_t lv[100];
-  for (int i = 0; i < 100; i++) lv[i] = 0;
-  const int ctx_e = 1 + (eob > 8) + (eob > 16);
-  {
-    const int rc = kScan8[eob];
-    const int ex = rc >> 3, ey = rc & 7;
-    const uint32_t m = uabs(cf[rc]);
-    const uint32_t tok = min(m, 3u) - 1;
-    bits = __fadd_rn(bits, C.eob_base[ctx_e][tok]);
-    if (tok == 2) bits = __fadd_rn(bits, hi_tok(m, (ex | ey) > 1 ? 14 : 7));
-    lv[ex * 8 + ey] = level_byte(m);
-  }
-  int ac_nz = 1;
-  for (int i = eob - 1; i >= 1; i--) {
-    const int rc = kScan8[i];
-    const int x = rc >> 3, y = rc & 7;
-    const uint32_t hm = (uint32_t)lv[x * 8 + y + 1] + lv[(x + 1) * 8 + y] + lv[(x + 1) * 8 + y + 1];
-    const uint32_t mag = hm + lv[x * 8 + y + 2] + lv[(x + 2) * 8 + y];
-    const int ctx = kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
-    const uint32_t m = uabs(cf[rc]);
-    const uint32_t tok = min(m, 3u);
-    bits = __fadd_rn(bits, C.base_tok[ctx][tok]);
-    if (tok == 3) {
-      const uint32_t hmag = hm & 63;
-      const int bc = ((y | x) > 1 ? 14 : 7) + (hmag > 12 ? 6 : (int)((hmag + 1) >> 1));
-      bits = __fadd_rn(bits, C.br_cum[bc][min((int32_t)m - 3, 12)]);
-      if (m >= 15) bits = __fadd_rn(bits, golomb_cost(m - 15));
-    }
-    if (m != 0) {
-      lv[x * 8 + y] = level_byte(m);
-      ac_nz++;
-    }
-  }
-  const uint32_t dm = uabs(cf[0]), dtok = min(dm, 3u);
-  bits = __fadd_rn(bits, C.base_tok[0][dtok]);
-  if (dtok == 3) {
-    const uint32_t mag = ((uint32_t)lv[1] + lv[8] + lv[9]) & 63;
-    bits = __fadd_rn(bits, hi_tok(dm, mag > 12 ? 6 : (int)((mag + 1) >> 1)));
-  }
-  if (cf[0] != 0) bits = __fadd_rn(bits, dcs_c[cf[0] < 0]);
-  for (int k = 0; k < ac_nz; k++) bits = __fadd_rn(bits, 1.0f);
-  return bits;
-}
-
-// Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
-__device__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const int32_t* pred,
-                          const int32_t* rr, int32_t maxv) {
-  uint32_t satd = 0;
-  for (int ty = 0; ty < 8; ty += 4)
-    for (int tx = 0; tx < 8; tx += 4) {
-      int32_t r[4][4];
-      for (int y = 0; y < 4; y++) {
-        int32_t d[4];
-        for (int x = 0; x < 4; x++) {
-          const int i = (ty + y) * 8 + tx + x;
-          d[x] = (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv);
-        }
-        const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
-        r[y][0] = e + g; r[y][1] = f + h; r[y][2] = f - h; r[y][3] = e - g;
-      }
-      for (int x = 0; x < 4; x++) {
-        const int32_t e = r[0][x] + r[2][x], f = r[0][x] - r[2][x], g = r[1][x] + r[3][x], h = r[1][x] - r[3][x];
-        satd += uabs(e + g) + uabs(f + h) + uabs(f - h) + uabs(e - g);
-      }
-    }
-  return satd;
-}
 
 struct ChainArgs {
   mt_chain_params p;
@@ -257,35 +39,19 @@ __global__ void __launch_bounds__(128) chain8_kernel(const uint16_t* __restrict_
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   const mt_candidate cd = cands[idx];
-  const mt_chain_params& p = a.p;
-  const int32_t maxv = (1 << p.bd) - 1;
-  int32_t pred[64], cf[64], rr[64];
-  float tf[64];
-  predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
-           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred);
-  for (int y = 0; y < 8; y++)
-    for (int x = 0; x < 8; x++)
-      rr[y * 8 + x] = (int32_t)src[(size_t)(cd.py + y) * p.stride + cd.px + x] - pred[y * 8 + x];
-  fwd8x8(rr, cd.tx_type, a.q, cf, tf);
-  const bool two_d = cd.tx_type == MT_TX_DCT_DCT || cd.tx_type >= MT_TX_ADST_ADST;
-  if (a.has_qm && two_d) apply_qm(cf, tf, sQm, 64);
-  if (p.trellis_lambda0 > 0.0f) trellis8(cf, tf, (float)a.q.dc_q, (float)a.q.ac_q, a.trellis_lambda);
-  inv8x8(cf, cd.tx_type, a.q, a.has_qm ? sQm : nullptr, rr);
-  const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv);
-  const float qstep = (float)a.q.ac_q;
-  float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
-  if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
-  int eob;
-  const float cbits = rate8(cf, sC, cd.skip_ctx, cd.dcs_ctx, cd.mode, cd.tx_type, p.use_skip_bits != 0,
-                            p.skip_bits[0], p.skip_bits[1], &eob);
-  const float bits = __fadd_rn(cbits, cd.mode_bits);
+  const int32_t maxv = (1 << a.p.bd) - 1;
+  if (!cand_ok(cd, a.p.frame_w, a.p.frame_h)) {
+    mt_candidate_result bad = {};
+    bad.eob = MT_EOB_INVALID;
+    res[idx] = bad;
+    return;
+  }
+  Work8 w;
   mt_candidate_result r;
-  r.distortion = price;
-  r.bits = bits;
-  r.cost = __fadd_rn(price, __fmul_rn(p.mode_lambda, bits));
-  r.satd = satd;
-  r.eob = eob;
-  r.reserved[0] = r.reserved[1] = r.reserved[2] = 0;
+  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+  const int32_t* pred = w.pred();
+  const int32_t* cf = w.cf();
+  const int32_t* rr = w.rr();
   res[idx] = r;
   if (lv_out) {
     int4* o = reinterpret_cast<int4*>(lv_out + (size_t)idx * 64);
@@ -300,14 +66,17 @@ __global__ void __launch_bounds__(128) chain8_kernel(const uint16_t* __restrict_
   }
 }
 
+
 // Standalone kernels of the chain's stages, one block per thread.
 __global__ void fwd8_kernel(const int32_t* __restrict__ resid, const uint8_t* __restrict__ types, int n, mt_quant q,
                             const uint8_t* __restrict__ qm_row, int32_t* __restrict__ levels,
                             float* __restrict__ targets) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  int32_t r[64], cf[64];
-  float tf[64];
+  Work8 w;
+  int32_t* r = w.rr();
+  int32_t* cf = w.cf();
+  float* tf = w.tf();
   for (int i = 0; i < 64; i++) r[i] = resid[(size_t)idx * 64 + i];
   const int tx = types[idx];
   fwd8x8(r, tx, q, cf, tf);
@@ -321,7 +90,9 @@ __global__ void inv8_kernel(const int32_t* __restrict__ levels, const uint8_t* _
                             const uint8_t* __restrict__ qm_row, int32_t* __restrict__ out) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  int32_t cf[64], o[64];
+  Work8 w;
+  int32_t* cf = w.cf();
+  int32_t* o = w.rr();
   for (int i = 0; i < 64; i++) cf[i] = levels[(size_t)idx * 64 + i];
   inv8x8(cf, types[idx], q, qm_row, o);
   for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = o[i];
@@ -330,8 +101,9 @@ __global__ void trellis8_kernel(int32_t* __restrict__ levels, const float* __res
                                 float ac_q, float lambda) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  int32_t cf[64];
-  float tf[64];
+  Work8 w;
+  int32_t* cf = w.cf();
+  float* tf = w.tf();
   for (int i = 0; i < 64; i++) {
     cf[i] = levels[(size_t)idx * 64 + i];
     tf[i] = targets[(size_t)idx * 64 + i];
@@ -344,7 +116,12 @@ __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   const mt_candidate cd = cands[idx];
-  int32_t pr[64];
+  Work8 w;
+  int32_t* pr = w.pred();
+  if (!cand_ok(cd, p.frame_w, p.frame_h)) {
+    for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = 0;
+    return;
+  }
   predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
            (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pr);
   for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = pr[i];
