@@ -40,7 +40,9 @@ def make_workload(seed=3):
     rgb = synth.generate_rgb(W, H, seed, sigma=4.0, variant="1080p")
     src = synth.rgb_to_luma(rgb)
     rec = synth.synthetic_recon(src, seed + 1000)
-    cands = synth.level_candidates(W, H, MODES, abi.TX_2D_SCAN_TYPES, seed=seed)
+    blocks = synth.level_blocks(W, H, seed=seed)
+    combos = synth.level_combos(MODES, abi.TX_2D_SCAN_TYPES)
+    cands = synth.candidates_of_level(blocks, combos)
     cdfs = synth.synthetic_cdfs(seed)
     q = mt.quant_new(QIDX, 8, QM_LEVEL)
     qm = mt.qm_row(QM_LEVEL, 0, 8)
@@ -51,7 +53,7 @@ def make_workload(seed=3):
     k_satd = 24.5 + (21.3 - 24.5) * (QIDX - 28.0) / (81.0 - 28.0)
     prm = mt.chain_params(W, H, trellis_lambda0=0.05, mode_lambda=mlam, satd_scale=1.25,
                           satd_bridge=2.775 / k_satd * 7.130643)
-    return dict(src=src, rec=rec, cands=cands, cdfs=cdfs, q=q, qm=qm, prm=prm, rgb=rgb)
+    return dict(src=src, rec=rec, blocks=blocks, combos=combos, cands=cands, cdfs=cdfs, q=q, qm=qm, prm=prm, rgb=rgb)
 
 
 class ClockSampler:
@@ -165,22 +167,24 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     mt.load()
     wl = make_workload()
-    cands = wl["cands"]
-    n = len(cands)
+    blocks, combos = wl["blocks"], wl["combos"]
+    nb, nc = len(blocks), len(combos)
+    n = nb * nc
     costs = mt.coef_costs(wl["cdfs"])
     # device-resident inputs (replicas: every rank encodes its own frame; no collective on the data path)
-    d_src = torch.from_numpy(wl["src"].astype(np.int16)).to(dev)
-    d_rec = torch.from_numpy(wl["rec"].astype(np.int16)).to(dev)
-    d_qm = torch.from_numpy(wl["qm"]).to(dev)
-    d_costs = torch.from_numpy(np.frombuffer(bytes(costs), np.uint8).copy()).to(dev)
-    d_cands = torch.from_numpy(cands.view(np.uint8).copy()).to(dev)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d_src, d_rec, d_qm = t(wl["src"]), t(wl["rec"]), t(wl["qm"])
+    d_costs = t(np.frombuffer(bytes(costs), np.uint8))
+    d_blocks, d_combos = t(blocks), t(combos)
+    d_best = torch.empty(nb * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     d_res = torch.empty(n * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_keys = torch.empty(nb * 8, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
     def launch():
-        mt.candidate_chain_device(d_src, d_rec, wl["prm"], wl["q"], d_qm, d_costs, d_cands, n, d_res,
-                                  stream=stream.cuda_stream)
+        mt.rdo_level8_device(d_src, d_rec, wl["prm"], wl["q"], d_qm, d_costs, d_blocks, nb, d_combos, nc, d_best,
+                             d_res, d_keys, stream=stream.cuda_stream)
 
     for _ in range(max(args.warmup, 3)):
         launch()
@@ -204,22 +208,23 @@ def run_ours(args):
     step_ms = float(t.item())
     value = world * MPIX / (step_ms / 1e3)
 
-    # e2e through the host ABI: copies in and out inside the timed region
+    # e2e through the host ABI (mt_rdo_level8): planes, block and combo lists
+    # copied in and the per-block winners copied out inside the timed region
     src, rec = wl["src"], wl["rec"]
     e2e_times = []
     for i in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res, _, _ = mt.candidate_chain(src, rec, wl["prm"], wl["q"], wl["qm"], costs, cands)
+        best, _ = mt.rdo_level8(src, rec, wl["prm"], wl["q"], wl["qm"], costs, blocks, combos)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = float(np.median(e2e_times))
-    h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + cands.nbytes
-    d2h = n * abi.RESULT_DTYPE.itemsize
+    h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + blocks.nbytes + combos.nbytes
+    d2h = nb * abi.BEST_DTYPE.itemsize
 
-    # roofline of the chain kernel against HBM: algorithmic bytes per launch =
-    # candidate record 16 B + result 32 B + source 64 x 2 B + neighbour edges
-    # (up to 33) x 2 B per candidate
-    alg_bytes = n * (16 + 32 + 128 + 66)
+    # roofline of the level kernel against HBM: algorithmic bytes per launch =
+    # per candidate the result record (32 B) + source block (64 x 2 B) +
+    # neighbour edges (up to 33 x 2 B); per block its record (60 B)
+    alg_bytes = n * (32 + 128 + 66) + nb * 60
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -234,7 +239,7 @@ def run_ours(args):
 
         obuild.build()
         threads = os.cpu_count() or 1
-        rate, dt = cpu_rate(wl, n, threads)
+        rate, dt = cpu_rate(wl, n, threads)  # the same candidates, combo-major
         cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
                "sample": f"the whole level, {n} candidates ({dt:.2f} s)"}
 
@@ -244,13 +249,14 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f32",
         "data": "synthetic",
         "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
-                   "candidates": n, "parallelism": f"replicas x{world}", "l2": "flushed between timed launches"},
+                   "candidates": n, "blocks": nb, "combos": nc, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed launches"},
         "e2e": {"value": round(world * MPIX / e2e_s, 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 5), "traffic": None,
-                     "kernel": "chain8_kernel", "alg_bytes_per_launch": alg_bytes},
-        "gpu_launches": args.steps,
+                     "kernel": "level8_kernel", "alg_bytes_per_launch": alg_bytes},
+        "gpu_launches": 2 * args.steps,  # level8_kernel + level8_finalize_kernel per step
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }

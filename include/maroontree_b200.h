@@ -24,6 +24,11 @@
  *   mt_trellis_optimize[_device]          src/trellis.rs:944-1030 trellis_optimize
  *   mt_intra_predict[_device]             src/intrapred.rs:322-398 IntraPredDispatch::predict_nd_ad,
  *                                         src/intrapred.rs:1740-1790 dc_pred
+ *   mt_rdo_level8[_device]                the batched form of the same chain over a whole
+ *                                         partition level: the per-block candidate loops of
+ *                                         src/coder/partition_search.rs:467-530 (and the
+ *                                         emitter's mode x type trials, e.g. :4320-4390) with
+ *                                         their "if cost < best" selection
  */
 #ifndef MAROONTREE_B200_H
 #define MAROONTREE_B200_H
@@ -153,6 +158,35 @@ typedef struct mt_candidate_result {
   uint32_t reserved[3];
 } mt_candidate_result;
 
+/* One 8x8 block of an RDO level: position, neighbour availability, contexts
+ * and the caller's mode-signalling bits for each of the 13 luma modes. */
+typedef struct mt_block8 {
+  uint16_t px, py;
+  uint8_t flags;          /* MT_CAND_* bits */
+  uint8_t dcs_ctx;        /* dc_sign context 0..2 */
+  uint8_t skip_ctx;       /* txb_skip context 0..12 */
+  uint8_t reserved;
+  float mode_bits[13];    /* LossyTile::mode_bits(px, py, m) for m = 0..12 */
+} mt_block8;
+
+/* One (mode, angle delta, transform type) candidate of every block. */
+typedef struct mt_combo {
+  uint8_t mode;
+  int8_t angle_delta;
+  uint8_t tx_type;
+  uint8_t reserved;
+} mt_combo;
+
+/* Per-block winner of a level: the lowest rd cost over the combos, ties to
+ * the earlier combo (the reference's strict-< scan in candidate order). */
+typedef struct mt_block_best {
+  int32_t combo;          /* index into the combo list, -1 if none evaluated */
+  float cost, distortion, bits;
+  uint32_t satd;
+  int32_t eob;
+  uint32_t reserved[2];
+} mt_block_best;
+
 /* ---- host-side helpers ---------------------------------------------------- */
 
 /* Quant::new_with_qm(base_q_idx, bd, qm_level) for 8-bit luma. */
@@ -180,12 +214,32 @@ int mt_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chai
                        const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
                        const mt_candidate* cands, int32_t n, mt_candidate_result* results,
                        int32_t* levels_out, int32_t* recon_out);
+/* Device form.  d_scratch (optional, mt_candidate_chain_scratch_bytes(n)
+ * bytes) lets the launch bucket the candidates by code path first; results
+ * are identical with or without it. */
 int mt_candidate_chain_device(const uint16_t* d_src, const uint16_t* d_recon,
                               const mt_chain_params* prm, const mt_quant* quant,
                               const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                               const mt_candidate* d_cands, int32_t n,
                               mt_candidate_result* d_results, int32_t* d_levels_out,
-                              int32_t* d_recon_out, void* stream);
+                              int32_t* d_recon_out, void* d_scratch, void* stream);
+size_t mt_candidate_chain_scratch_bytes(int32_t n);
+
+/* One batched RDO level: every combo of every block (ncombos * nblocks chain
+ * evaluations in one launch) and the per-block best.  Host form: host
+ * buffers in and out; results_out (optional) receives all
+ * ncombos * nblocks results, combo-major (index combo * nblocks + block). */
+int mt_rdo_level8(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm,
+                  const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                  const mt_block8* blocks, int32_t nblocks, const mt_combo* combos,
+                  int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out);
+/* Device form: d_results (ncombos * nblocks) and d_keys (nblocks * 8 bytes)
+ * are caller-provided working storage; d_best receives the winners. */
+int mt_rdo_level8_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
+                         int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
+                         void* d_keys, void* stream);
 
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and

@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "MtError",
 ]
 
 
@@ -94,8 +94,36 @@ def candidate_chain(src, recon, prm, quant, qmrow, costs, cands, want_levels=Fal
 
 
 def candidate_chain_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_cands, n, d_res, d_lv=None, d_ro=None,
-                           stream=0):
+                           d_scratch=None, stream=0):
     """Device-pointer form: arguments are torch CUDA tensors (or raw addresses)."""
     _check(load().mt_candidate_chain_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
                                             ptr(d_costs), ptr(d_cands), n, ptr(d_res), ptr(d_lv), ptr(d_ro),
-                                            stream or None), "mt_candidate_chain_device")
+                                            ptr(d_scratch), stream or None), "mt_candidate_chain_device")
+
+
+def chain_scratch_bytes(n):
+    return load().mt_candidate_chain_scratch_bytes(n)
+
+
+def rdo_level8(src, recon, prm, quant, qmrow, costs, blocks, combos, want_results=False):
+    """One batched RDO level with host buffers: per-block best (and optionally
+    every candidate result, combo-major)."""
+    lib = load()
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.BLOCK8_DTYPE)
+    combos = np.ascontiguousarray(combos, abi.COMBO_DTYPE)
+    best = np.zeros(len(blocks), abi.BEST_DTYPE)
+    res = np.zeros(len(blocks) * len(combos), RESULT_DTYPE) if want_results else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(lib.mt_rdo_level8(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                             ptr(blocks), len(blocks), ptr(combos), len(combos), ptr(best), ptr(res)),
+           "mt_rdo_level8")
+    return best, res
+
+
+def rdo_level8_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_blocks, nblocks, d_combos, ncombos, d_best,
+                      d_results, d_keys, stream=0):
+    _check(load().mt_rdo_level8_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
+                                       ptr(d_costs), ptr(d_blocks), nblocks, ptr(d_combos), ncombos, ptr(d_best),
+                                       ptr(d_results), ptr(d_keys), stream or None), "mt_rdo_level8_device")

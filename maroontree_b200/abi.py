@@ -14,6 +14,7 @@ MT_ERR_INVALID_INPUT = -2
 MT_ERR_UNSUPPORTED = -3
 MT_ERR_DEVICE = -10
 MT_ERR_ALLOC = -11
+MT_EOB_INVALID = -2
 
 # intra modes (src/intrapred.rs:54-79)
 DC_PRED, V_PRED, H_PRED, D45_PRED, D135_PRED, D113_PRED, D157_PRED, D203_PRED, D67_PRED = range(9)
@@ -66,6 +67,17 @@ class ChainParams(C.Structure):
     ]
 
 
+BLOCK8_DTYPE = np.dtype([
+    ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
+    ("mode_bits", "<f4", (13,)),
+])
+COMBO_DTYPE = np.dtype([("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"), ("reserved", "u1")])
+BEST_DTYPE = np.dtype([
+    ("combo", "<i4"), ("cost", "<f4"), ("distortion", "<f4"), ("bits", "<f4"), ("satd", "<u4"), ("eob", "<i4"),
+    ("reserved", "<u4", (2,)),
+])
+assert BLOCK8_DTYPE.itemsize == 60 and COMBO_DTYPE.itemsize == 4 and BEST_DTYPE.itemsize == 32
+
 CANDIDATE_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"),
     ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "<u2"), ("mode_bits", "<f4"),
@@ -90,7 +102,12 @@ def _bind(lib):
         "mt_candidate_chain": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                          _P, C.c_int32, _P, _P, _P]),
         "mt_candidate_chain_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
-                                                C.c_int32, _P, _P, _P, _P]),
+                                                C.c_int32, _P, _P, _P, _P, _P]),
+        "mt_candidate_chain_scratch_bytes": (C.c_size_t, [C.c_int32]),
+        "mt_rdo_level8": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                                    C.c_int32, _P, C.c_int32, _P, _P]),
+        "mt_rdo_level8_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
+                                           _P, C.c_int32, _P, _P, _P, _P]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -118,7 +135,8 @@ def load():
 
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
-    "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_fwd_txfm_quant_device",
+    "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
+    "mt_rdo_level8", "mt_rdo_level8_device", "mt_fwd_txfm_quant_device",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
 )
 

@@ -13,10 +13,15 @@
 #include "av1_tables.h"
 
 namespace mth {
+size_t chain8_scratch_bytes(int n);
 cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
                           const mt_candidate* cands, int n, mt_candidate_result* res, int32_t* lv, int32_t* ro,
-                          cudaStream_t st);
+                          void* scratch, cudaStream_t st);
+cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                          float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                          const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
+                          mt_candidate_result* res, unsigned long long* keys, mt_block_best* best, cudaStream_t st);
 cudaError_t launch_fwd8(const int32_t* resid, const uint8_t* types, int n, const mt_quant& q, const uint8_t* qm,
                         int32_t* levels, float* targets, cudaStream_t st);
 cudaError_t launch_inv8(const int32_t* levels, const uint8_t* types, int n, const mt_quant& q, const uint8_t* qm,
@@ -181,17 +186,85 @@ static int check_chain(const mt_chain_params* prm, const mt_quant* q, int32_t n)
   return MT_OK;
 }
 
+size_t mt_candidate_chain_scratch_bytes(int32_t n) { return n > 0 ? mth::chain8_scratch_bytes(n) : 0; }
+
 int mt_candidate_chain_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
                               const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                               const mt_candidate* d_cands, int32_t n, mt_candidate_result* d_results,
-                              int32_t* d_levels_out, int32_t* d_recon_out, void* stream) {
+                              int32_t* d_levels_out, int32_t* d_recon_out, void* d_scratch, void* stream) {
   int rc = check_chain(prm, quant, n);
   if (rc != MT_OK) return rc;
   if (n == 0) return MT_OK;
   if (!d_src || !d_recon || !d_costs || !d_cands || !d_results) return MT_ERR_INVALID_INPUT;
   float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
   cudaError_t e = mth::launch_chain8(d_src, d_recon, *prm, *quant, tl, d_qm_row, d_costs, d_cands, n, d_results,
-                                     d_levels_out, d_recon_out, as_stream(stream));
+                                     d_levels_out, d_recon_out, d_scratch, as_stream(stream));
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_rdo_level8_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
+                         mt_block_best* d_best, mt_candidate_result* d_results, void* d_keys, void* stream) {
+  int rc = check_chain(prm, quant, 0);
+  if (rc != MT_OK) return rc;
+  if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
+  if (nblocks == 0 || ncombos == 0) return MT_OK;
+  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_INVALID_INPUT;
+  if (!d_src || !d_recon || !d_costs || !d_blocks || !d_combos || !d_best || !d_results || !d_keys)
+    return MT_ERR_INVALID_INPUT;
+  float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
+  cudaError_t e = mth::launch_level8(d_src, d_recon, *prm, *quant, tl, d_qm_row, d_costs, d_blocks, nblocks, d_combos,
+                                     ncombos, d_results, static_cast<unsigned long long*>(d_keys), d_best,
+                                     as_stream(stream));
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_rdo_level8(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
+                  const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
+                  const mt_combo* combos, int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out) {
+  int rc = check_chain(prm, quant, 0);
+  if (rc != MT_OK) return rc;
+  if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
+  if (nblocks == 0 || ncombos == 0) return MT_OK;
+  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_INVALID_INPUT;
+  if (!src || !recon || !costs || !blocks || !combos || !best_out) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
+  const size_t nres = (size_t)nblocks * ncombos;
+  size_t off_src = 0, off_rec = align256(plane), off_cost = off_rec + align256(plane);
+  size_t off_qm = off_cost + align256(sizeof(mt_coef_costs));
+  size_t off_blk = off_qm + 256;
+  size_t off_cmb = off_blk + align256((size_t)nblocks * sizeof(mt_block8));
+  size_t off_best = off_cmb + align256((size_t)ncombos * sizeof(mt_combo));
+  size_t off_key = off_best + align256((size_t)nblocks * sizeof(mt_block_best));
+  size_t off_res = off_key + align256((size_t)nblocks * 8);
+  size_t total = off_res + align256(nres * sizeof(mt_candidate_result));
+  std::lock_guard<std::mutex> lock(g_ws.mu);
+  char* base = (char*)g_ws.get(total);
+  if (!base) return MT_ERR_ALLOC;
+  cudaStream_t st = 0;
+  cudaError_t e = cudaSuccess;
+  auto cp = [&](size_t off, const void* h, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + off, h, bytes, cudaMemcpyHostToDevice, st);
+  };
+  cp(off_src, src, plane);
+  cp(off_rec, recon, plane);
+  cp(off_cost, costs, sizeof(mt_coef_costs));
+  if (qm_row) cp(off_qm, qm_row, 64);
+  cp(off_blk, blocks, (size_t)nblocks * sizeof(mt_block8));
+  cp(off_cmb, combos, (size_t)ncombos * sizeof(mt_combo));
+  if (e != cudaSuccess) return MT_ERR_DEVICE;
+  float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
+  e = mth::launch_level8((const uint16_t*)(base + off_src), (const uint16_t*)(base + off_rec), *prm, *quant, tl,
+                         qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
+                         (const mt_block8*)(base + off_blk), nblocks, (const mt_combo*)(base + off_cmb), ncombos,
+                         (mt_candidate_result*)(base + off_res), (unsigned long long*)(base + off_key),
+                         (mt_block_best*)(base + off_best), st);
+  if (e != cudaSuccess) return MT_ERR_DEVICE;
+  e = cudaMemcpyAsync(best_out, base + off_best, (size_t)nblocks * sizeof(mt_block_best), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && results_out)
+    e = cudaMemcpyAsync(results_out, base + off_res, nres * sizeof(mt_candidate_result), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
@@ -210,7 +283,8 @@ int mt_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chai
   size_t off_res = off_cand + align256((size_t)n * sizeof(mt_candidate));
   size_t off_lv = off_res + align256((size_t)n * sizeof(mt_candidate_result));
   size_t off_ro = off_lv + (levels_out ? align256(blk) : 0);
-  size_t total = off_ro + (recon_out ? align256(blk) : 0);
+  size_t off_scr = off_ro + (recon_out ? align256(blk) : 0);
+  size_t total = off_scr + align256(mth::chain8_scratch_bytes(n));
   std::lock_guard<std::mutex> lock(g_ws.mu);
   char* base = (char*)g_ws.get(total);
   if (!base) return MT_ERR_ALLOC;
@@ -230,7 +304,7 @@ int mt_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chai
                          qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
                          (const mt_candidate*)(base + off_cand), n, (mt_candidate_result*)(base + off_res),
                          levels_out ? (int32_t*)(base + off_lv) : nullptr,
-                         recon_out ? (int32_t*)(base + off_ro) : nullptr, st);
+                         recon_out ? (int32_t*)(base + off_ro) : nullptr, base + off_scr, st);
   if (e != cudaSuccess) return MT_ERR_DEVICE;
   e = cudaMemcpyAsync(results, base + off_res, (size_t)n * sizeof(mt_candidate_result), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && levels_out) e = cudaMemcpyAsync(levels_out, base + off_lv, blk, cudaMemcpyDeviceToHost, st);

@@ -1,11 +1,15 @@
-// Batched luma candidate chain for 8x8 blocks (the per-candidate body of the
-// reference's luma mode search, src/coder/partition_search.rs:467-530):
-//   predict -> residual -> forward transform + quantisation (+QM)
-//   -> trellis_optimize -> dequantisation + inverse transform
-//   -> SATD distortion (luma_partition_distortion) and coefficient rate
-//   -> rd_cost = D + lambda * (bits + mode bits).
-// One thread evaluates one candidate; the batch-wide tables (bit costs, scan,
-// QM row) are staged once per CTA in shared memory.
+// Kernels of the batched 8x8 luma candidate chain.
+//
+//  * chain8_kernel: an arbitrary candidate list.  The launcher first buckets
+//    the candidates by (transform type, mode, angle delta) into a permutation
+//    (counting sort, 3 small kernels) so that each warp runs one code path.
+//  * level8_kernel: one whole RDO level -- every (block, combo) pair of a block
+//    list and a combo list (mode, angle delta, transform type), enumerated so a
+//    warp holds one combo over 32 consecutive blocks -- with the per-block
+//    argmin under the reference's comparison (strict <, first in evaluation
+//    order wins) folded in through a 64-bit atomicMin on (cost bits, combo).
+//  * stage kernels (forward, inverse, trellis, prediction) for the
+//    kernel-level entry points.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -20,26 +24,81 @@ struct ChainArgs {
   int has_qm;
 };
 
-__global__ void __launch_bounds__(128) chain8_kernel(const uint16_t* __restrict__ src,
-                                                     const uint16_t* __restrict__ rec, ChainArgs a,
-                                                     const uint8_t* __restrict__ qm_row,
-                                                     const mt_coef_costs* __restrict__ costs,
-                                                     const mt_candidate* __restrict__ cands, int n,
-                                                     mt_candidate_result* __restrict__ res,
-                                                     int32_t* __restrict__ lv_out, int32_t* __restrict__ rec_out) {
+constexpr int kThreads = 128;
+constexpr int kBuckets = 1024;
+
+__device__ __forceinline__ int bucket_of(const mt_candidate& c) {
+  const int t = min((int)c.tx_type, 7), m = min((int)c.mode, 15), d = min(max(c.angle_delta + 3, 0), 7);
+  return (t * 16 + m) * 8 + d;
+}
+
+__global__ void bucket_count_kernel(const mt_candidate* __restrict__ cands, int n, int* __restrict__ hist) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&hist[bucket_of(cands[i])], 1);
+}
+// Exclusive scan of the 1024 bucket counts into the scatter cursors (one CTA).
+__global__ void bucket_scan_kernel(const int* __restrict__ hist, int* __restrict__ cursor) {
+  __shared__ int s[kBuckets];
+  const int t = threadIdx.x;  // 1024 threads
+  s[t] = hist[t];
+  __syncthreads();
+  for (int off = 1; off < kBuckets; off <<= 1) {
+    const int v = t >= off ? s[t - off] : 0;
+    __syncthreads();
+    s[t] += v;
+    __syncthreads();
+  }
+  cursor[t] = s[t] - hist[t];
+}
+__global__ void bucket_scatter_kernel(const mt_candidate* __restrict__ cands, int n, int* __restrict__ cursor,
+                                      int* __restrict__ perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) perm[atomicAdd(&cursor[bucket_of(cands[i])], 1)] = i;
+}
+
+__device__ __forceinline__ void stage_tables(const mt_coef_costs* __restrict__ costs, const uint8_t* __restrict__ qm_row,
+                                             int has_qm, mt_coef_costs& sC, uint8_t* sQm) {
+  const float* g = reinterpret_cast<const float*>(costs);
+  float* s = reinterpret_cast<float*>(&sC);
+  for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+  if (threadIdx.x < 64) sQm[threadIdx.x] = has_qm ? qm_row[threadIdx.x] : 32;
+  __syncthreads();
+}
+
+__device__ __forceinline__ void store_blocks(Work8& w, int32_t maxv, int32_t* lv_out, int32_t* rec_out, size_t slot) {
+  const int16_t* cf = w.cf();
+  const int16_t* pred = w.pred();
+  const int16_t* rr = w.rr();
+  if (lv_out) {
+    int4* o = reinterpret_cast<int4*>(lv_out + slot * 64);
+#pragma unroll
+    for (int i = 0; i < 16; i++) o[i] = make_int4(cf[4 * i], cf[4 * i + 1], cf[4 * i + 2], cf[4 * i + 3]);
+  }
+  if (rec_out) {
+    int4* o = reinterpret_cast<int4*>(rec_out + slot * 64);
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+      o[i] = make_int4(clampi(pred[4 * i] + rr[4 * i], 0, maxv), clampi(pred[4 * i + 1] + rr[4 * i + 1], 0, maxv),
+                       clampi(pred[4 * i + 2] + rr[4 * i + 2], 0, maxv),
+                       clampi(pred[4 * i + 3] + rr[4 * i + 3], 0, maxv));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) chain8_kernel(const uint16_t* __restrict__ src,
+                                                          const uint16_t* __restrict__ rec, ChainArgs a,
+                                                          const uint8_t* __restrict__ qm_row,
+                                                          const mt_coef_costs* __restrict__ costs,
+                                                          const mt_candidate* __restrict__ cands,
+                                                          const int* __restrict__ perm, int n,
+                                                          mt_candidate_result* __restrict__ res,
+                                                          int32_t* __restrict__ lv_out, int32_t* __restrict__ rec_out) {
   __shared__ mt_coef_costs sC;
   __shared__ uint8_t sQm[64];
-  {
-    const float* g = reinterpret_cast<const float*>(costs);
-    float* s = reinterpret_cast<float*>(&sC);
-    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
-    if (threadIdx.x < 64) sQm[threadIdx.x] = a.has_qm ? qm_row[threadIdx.x] : 32;
-  }
-  __syncthreads();
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n) return;
+  stage_tables(costs, qm_row, a.has_qm, sC, sQm);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int idx = perm ? perm[t] : t;
   const mt_candidate cd = cands[idx];
-  const int32_t maxv = (1 << a.p.bd) - 1;
   if (!cand_ok(cd, a.p.frame_w, a.p.frame_h)) {
     mt_candidate_result bad = {};
     bad.eob = MT_EOB_INVALID;
@@ -49,33 +108,87 @@ __global__ void __launch_bounds__(128) chain8_kernel(const uint16_t* __restrict_
   Work8 w;
   mt_candidate_result r;
   chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
-  const int32_t* pred = w.pred();
-  const int32_t* cf = w.cf();
-  const int32_t* rr = w.rr();
   res[idx] = r;
-  if (lv_out) {
-    int4* o = reinterpret_cast<int4*>(lv_out + (size_t)idx * 64);
-    for (int i = 0; i < 16; i++) o[i] = make_int4(cf[4 * i], cf[4 * i + 1], cf[4 * i + 2], cf[4 * i + 3]);
-  }
-  if (rec_out) {
-    int4* o = reinterpret_cast<int4*>(rec_out + (size_t)idx * 64);
-    for (int i = 0; i < 16; i++)
-      o[i] = make_int4(clampi(pred[4 * i] + rr[4 * i], 0, maxv), clampi(pred[4 * i + 1] + rr[4 * i + 1], 0, maxv),
-                       clampi(pred[4 * i + 2] + rr[4 * i + 2], 0, maxv),
-                       clampi(pred[4 * i + 3] + rr[4 * i + 3], 0, maxv));
-  }
+  store_blocks(w, (1 << a.p.bd) - 1, lv_out, rec_out, (size_t)idx);
 }
 
+// Candidate (combo c, block b) for thread t: warps take 32 consecutive blocks
+// of one combo.
+__global__ void __launch_bounds__(kThreads) level8_kernel(const uint16_t* __restrict__ src,
+                                                          const uint16_t* __restrict__ rec, ChainArgs a,
+                                                          const uint8_t* __restrict__ qm_row,
+                                                          const mt_coef_costs* __restrict__ costs,
+                                                          const mt_block8* __restrict__ blocks, int nblocks,
+                                                          const mt_combo* __restrict__ combos, int ncombos,
+                                                          mt_candidate_result* __restrict__ res,
+                                                          unsigned long long* __restrict__ best_key) {
+  __shared__ mt_coef_costs sC;
+  __shared__ uint8_t sQm[64];
+  stage_tables(costs, qm_row, a.has_qm, sC, sQm);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
+  if (c >= ncombos) return;
+  const mt_block8& bk = blocks[b];
+  const mt_combo cb = combos[c];
+  mt_candidate cd;
+  cd.px = bk.px;
+  cd.py = bk.py;
+  cd.mode = cb.mode;
+  cd.angle_delta = cb.angle_delta;
+  cd.tx_type = cb.tx_type;
+  cd.flags = bk.flags;
+  cd.dcs_ctx = bk.dcs_ctx;
+  cd.skip_ctx = bk.skip_ctx;
+  cd.reserved = 0;
+  cd.mode_bits = cb.mode <= MT_PAETH_PRED ? bk.mode_bits[cb.mode] : 0.0f;
+  const size_t slot = (size_t)c * nblocks + b;
+  if (!cand_ok(cd, a.p.frame_w, a.p.frame_h)) {
+    mt_candidate_result bad = {};
+    bad.eob = MT_EOB_INVALID;
+    res[slot] = bad;
+    return;
+  }
+  Work8 w;
+  mt_candidate_result r;
+  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+  res[slot] = r;
+  // Costs are non-negative finite floats, so their bit patterns order like
+  // the values; ties go to the lower combo index (evaluated first).
+  const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c;
+  atomicMin(&best_key[b], key);
+}
 
-// Standalone kernels of the chain's stages, one block per thread.
+__global__ void level8_finalize_kernel(const unsigned long long* __restrict__ best_key, int nblocks,
+                                       const mt_candidate_result* __restrict__ res, mt_block_best* __restrict__ best) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblocks) return;
+  const unsigned long long k = best_key[b];
+  mt_block_best o = {};
+  if (k == ~0ull) {
+    o.combo = -1;
+    o.eob = MT_EOB_INVALID;
+  } else {
+    const int c = (int)(k & 0xffffffffu);
+    const mt_candidate_result r = res[(size_t)c * nblocks + b];
+    o.combo = c;
+    o.cost = r.cost;
+    o.distortion = r.distortion;
+    o.bits = r.bits;
+    o.satd = r.satd;
+    o.eob = r.eob;
+  }
+  best[b] = o;
+}
+
+// Standalone stage kernels, one block per thread.
 __global__ void fwd8_kernel(const int32_t* __restrict__ resid, const uint8_t* __restrict__ types, int n, mt_quant q,
                             const uint8_t* __restrict__ qm_row, int32_t* __restrict__ levels,
                             float* __restrict__ targets) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   Work8 w;
-  int32_t* r = w.rr();
-  int32_t* cf = w.cf();
+  int32_t* r = w.w + 64;   // int32 residual at [64, 128)
+  int32_t* cf = w.w + 128; // int32 levels at [128, 192)
   float* tf = w.tf();
   for (int i = 0; i < 64; i++) r[i] = resid[(size_t)idx * 64 + i];
   const int tx = types[idx];
@@ -91,8 +204,8 @@ __global__ void inv8_kernel(const int32_t* __restrict__ levels, const uint8_t* _
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   Work8 w;
-  int32_t* cf = w.cf();
-  int32_t* o = w.rr();
+  int32_t* cf = w.w;        // int32 levels at [0, 64)
+  int32_t* o = w.w + 64;    // int32 output at [64, 128)
   for (int i = 0; i < 64; i++) cf[i] = levels[(size_t)idx * 64 + i];
   inv8x8(cf, types[idx], q, qm_row, o);
   for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = o[i];
@@ -102,13 +215,13 @@ __global__ void trellis8_kernel(int32_t* __restrict__ levels, const float* __res
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   Work8 w;
-  int32_t* cf = w.cf();
+  int32_t* cf = w.w + 132;  // int32 levels at [132, 196)
   float* tf = w.tf();
   for (int i = 0; i < 64; i++) {
     cf[i] = levels[(size_t)idx * 64 + i];
     tf[i] = targets[(size_t)idx * 64 + i];
   }
-  trellis8(cf, tf, dc_q, ac_q, lambda);
+  trellis8(cf, tf, w.suf(), dc_q, ac_q, lambda);
   for (int i = 0; i < 64; i++) levels[(size_t)idx * 64 + i] = cf[i];
 }
 __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p, const mt_candidate* __restrict__ cands,
@@ -117,7 +230,7 @@ __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p
   if (idx >= n) return;
   const mt_candidate cd = cands[idx];
   Work8 w;
-  int32_t* pr = w.pred();
+  int16_t* pr = w.pred();
   if (!cand_ok(cd, p.frame_w, p.frame_h)) {
     for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = 0;
     return;
@@ -131,20 +244,55 @@ __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p
 
 // Host launchers used by the C ABI (capi.cu).
 namespace mth {
-cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
-                          float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
-                          const mt_candidate* cands, int n, mt_candidate_result* res, int32_t* lv, int32_t* ro,
-                          cudaStream_t st) {
+static mtd::ChainArgs make_args(const mt_chain_params& p, const mt_quant& q, float tl, const uint8_t* qm) {
   mtd::ChainArgs a;
   a.p = p;
   a.q = q;
-  a.trellis_lambda = trellis_lambda;
-  a.has_qm = qm_row != nullptr;
-  const int threads = 128;
-  const int blocks = (n + threads - 1) / threads;
-  if (blocks > 0) mtd::chain8_kernel<<<blocks, threads, 0, st>>>(src, rec, a, qm_row, costs, cands, n, res, lv, ro);
+  a.trellis_lambda = tl;
+  a.has_qm = qm != nullptr;
+  return a;
+}
+
+size_t chain8_scratch_bytes(int n) { return (size_t)2 * mtd::kBuckets * sizeof(int) + (size_t)n * sizeof(int); }
+
+cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                          float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                          const mt_candidate* cands, int n, mt_candidate_result* res, int32_t* lv, int32_t* ro,
+                          void* scratch, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int blocks = (n + mtd::kThreads - 1) / mtd::kThreads;
+  int* perm = nullptr;
+  if (scratch) {
+    int* hist = static_cast<int*>(scratch);
+    int* cursor = hist + mtd::kBuckets;
+    perm = cursor + mtd::kBuckets;
+    cudaError_t e = cudaMemsetAsync(hist, 0, mtd::kBuckets * sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    mtd::bucket_count_kernel<<<blocks, mtd::kThreads, 0, st>>>(cands, n, hist);
+    mtd::bucket_scan_kernel<<<1, mtd::kBuckets, 0, st>>>(hist, cursor);
+    mtd::bucket_scatter_kernel<<<blocks, mtd::kThreads, 0, st>>>(cands, n, cursor, perm);
+  }
+  mtd::chain8_kernel<<<blocks, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row), qm_row,
+                                                       costs, cands, perm, n, res, lv, ro);
   return cudaGetLastError();
 }
+
+cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                          float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                          const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
+                          mt_candidate_result* res, unsigned long long* keys, mt_block_best* best, cudaStream_t st) {
+  if (nblocks <= 0 || ncombos <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(keys, 0xff, (size_t)nblocks * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  const long long total = (long long)nblocks * ncombos;
+  const long long grid = (total + mtd::kThreads - 1) / mtd::kThreads;
+  mtd::level8_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+                                                               qm_row, costs, blocks, nblocks, combos, ncombos, res,
+                                                               keys);
+  mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fwd8(const int32_t* resid, const uint8_t* types, int n, const mt_quant& q, const uint8_t* qm,
                         int32_t* levels, float* targets, cudaStream_t st) {
   const int blocks = (n + 127) / 128;

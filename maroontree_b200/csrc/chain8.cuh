@@ -1,5 +1,17 @@
-// Device functions of the 8x8 candidate chain: trellis, rate walk, SATD and
-// the per-candidate driver.  Shared by the kernels in chain.cu.
+// Device functions of the 8x8 luma candidate chain (the per-candidate body of
+// the reference's luma mode search, src/coder/partition_search.rs:467-530):
+//   predict -> residual -> forward transform + quantisation (+QM)
+//   -> trellis_optimize -> dequantisation + inverse transform
+//   -> SATD distortion (luma_partition_distortion) and coefficient rate
+//   -> rd_cost = D + lambda * (bits + mode bits).
+//
+// Execution model: one thread evaluates one candidate; launches arrange the
+// candidates so that a warp runs one (mode, transform type) pair over 32
+// blocks.  Every loop over scan positions runs on a warp-uniform index (the
+// warp maximum of the per-lane bound, lanes past their own bound predicated
+// off), so scan tables are constant-cache broadcasts and the per-thread
+// arrays are read and written with the same offset in every lane (coalesced
+// local memory).
 #pragma once
 #include <stdint.h>
 
@@ -8,10 +20,15 @@
 
 namespace mtd {
 
+// Default 8x8 scan (scan index -> rc = x*8 + y) and its inverse.
 __constant__ uint8_t kScan8[64] = {0,  8,  1,  2,  9,  16, 24, 17, 10, 3,  4,  11, 18, 25, 32, 40,
                                    33, 26, 19, 12, 5,  6,  13, 20, 27, 34, 41, 48, 56, 49, 42, 35,
                                    28, 21, 14, 7,  15, 22, 29, 36, 43, 50, 57, 58, 51, 44, 37, 30,
                                    23, 31, 38, 45, 52, 59, 60, 53, 46, 39, 47, 54, 61, 62, 55, 63};
+__constant__ uint8_t kIScan8[64] = {0,  2,  3,  9,  10, 20, 21, 35, 1,  4,  8,  11, 19, 22, 34, 36,
+                                    5,  7,  12, 18, 23, 33, 37, 48, 6,  13, 17, 24, 32, 38, 47, 49,
+                                    14, 16, 25, 31, 39, 46, 50, 57, 15, 26, 30, 40, 45, 51, 56, 58,
+                                    27, 29, 41, 44, 52, 55, 59, 62, 28, 42, 43, 53, 54, 60, 61, 63};
 // Coefficient-base position offsets for square transforms, [min(y,4)][min(x,4)].
 __constant__ uint8_t kLoCtxOff[25] = {0, 1, 6, 6, 21, 1, 6, 6, 21, 21, 6, 6, 21, 21, 21,
                                       6, 21, 21, 21, 21, 21, 21, 21, 21, 21};
@@ -23,6 +40,11 @@ __constant__ float kCoefRateLut[64] = {
     19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 19.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f,
     21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f, 21.5f};
 
+// Warp maximum over the lanes currently executing this call site; every lane
+// gets a bound >= its own value.
+__device__ __forceinline__ int warp_max(int v) { return __reduce_max_sync(__activemask(), v); }
+
+// Static per-level bit estimate (src/cost.rs:50-68); >= 64 takes the closed form.
 __device__ __forceinline__ float coef_rate_bits(uint32_t level) {
   if (level < 64) return kCoefRateLut[level];
   float b = 4.0f;
@@ -32,13 +54,13 @@ __device__ __forceinline__ float coef_rate_bits(uint32_t level) {
   return b;
 }
 __device__ __forceinline__ float golomb_cost(uint32_t v) { return (float)(2 * (32 - __clz(v + 1)) - 1); }
-__device__ __forceinline__ uint8_t level_byte(uint32_t m) {
-  return m == 0 ? 0 : (m <= 2 ? (uint8_t)(m * 0x41) : (uint8_t)(min(m, 15u) + 0xC0));
+// The byte the coefficient coder keeps per position (src/tables.rs:365-373).
+__device__ __forceinline__ uint32_t level_byte(uint32_t m) {
+  return m == 0 ? 0u : (m <= 2 ? m * 0x41u : min(m, 15u) + 0xC0u);
 }
 
-// One trellis round-down lane in the AVX2 FMA form (src/avx/trellis.rs:79-118)
-// or the scalar fallback form (src/avx/trellis.rs:139-161): returns true when
-// the level should drop by one.
+// Round-down decision of one coefficient: the AVX2 FMA lane form
+// (src/avx/trellis.rs:79-118) or the scalar form (src/avx/trellis.rs:139-161).
 __device__ __forceinline__ bool round_down_fma(float at, int32_t li, float q2, float lambda) {
   const int32_t ldi = max(li - 1, 0);
   const float el = __fsub_rn(at, (float)li), ed = __fsub_rn(at, (float)ldi);
@@ -53,52 +75,69 @@ __device__ __forceinline__ bool round_down_plain(float at, uint32_t l, float q2,
   return cd < cl;
 }
 
-// trellis_optimize (src/trellis.rs:944-1030) over the 8x8 default scan, with
-// step A in the pinned AVX2 chunking (8-wide, then 4-wide, then scalar tail;
-// a chunk holding a level >= 64 takes the scalar form for all its lanes).
-__device__ void trellis8(int32_t* cf, const float* tf, float dc_q, float ac_q, float lambda) {
+// One chunk of the trellis step A at scan positions [base, base + width).
+template <typename C>
+__device__ __forceinline__ void round_down_chunk(C* cf, const float* tf, int base, int width, float dq2, float aq2,
+                                                 float lambda) {
+  bool big = false;
+  for (int k = 0; k < width; k++) big |= uabs(cf[kScan8[base + k]]) > 63u;
+  uint32_t mask = 0;
+  for (int k = 0; k < width; k++) {
+    const int rc = kScan8[base + k];
+    const int32_t c = cf[rc];
+    const float q2 = rc == 0 ? dq2 : aq2;
+    const float at = fabsf(tf[rc]);
+    const bool dn = big ? (c != 0 && round_down_plain(at, uabs(c), q2, lambda))
+                        : round_down_fma(at, (int32_t)uabs(c), q2, lambda);
+    mask |= (uint32_t)dn << k;
+  }
+  for (int k = 0; k < width; k++) {
+    const int rc = kScan8[base + k];
+    const int32_t c = cf[rc];
+    if ((mask >> k & 1) && c != 0) cf[rc] = (C)(c < 0 ? c + 1 : c - 1);
+  }
+}
+
+// trellis_optimize (src/trellis.rs:944-1030) over the 8x8 default scan with
+// step A in the pinned AVX2 chunking (8-wide chunks, one 4-wide chunk, scalar
+// tail; a chunk holding a level >= 64 takes the scalar form in all lanes).
+// `suf` is scratch for 65 floats.  Returns the final EOB scan index (-1 when
+// every level is zero).
+template <typename C>
+__device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda) {
   const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
   int eob_idx = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) { eob_idx = i; break; }
-  if (eob_idx < 0) return;
+  for (int i = 0; i < 64; i++)
+    if (cf[kScan8[i]] != 0) eob_idx = i;
   const int m = eob_idx + 1;
-  int i = 0;
-  for (int w = 8; w >= 4; w >>= 1) {
-    while (i + w <= m) {
-      bool big = false;
-      for (int k = 0; k < w; k++) big |= uabs(cf[kScan8[i + k]]) > 63;
-      uint32_t mask = 0;
-      for (int k = 0; k < w; k++) {
-        const int rc = kScan8[i + k];
-        const int32_t c = cf[rc];
-        const float q2 = rc == 0 ? dq2 : aq2;
-        const float at = fabsf(tf[rc]);
-        if (big) {
-          if (c != 0 && round_down_plain(at, uabs(c), q2, lambda)) mask |= 1u << k;
-        } else if (round_down_fma(at, (int32_t)uabs(c), q2, lambda)) {
-          mask |= 1u << k;
-        }
+  const int M = warp_max(m);
+  if (m == 0) return -1;
+  const int full8 = m & ~7;
+  const bool has4 = (m - full8) >= 4;
+  for (int base = 0; base < M; base += 8) {
+    if (base >= m) continue;
+    if (base < full8) {
+      round_down_chunk(cf, tf, base, 8, dq2, aq2, lambda);
+    } else {
+      int s = base;
+      if (has4) {
+        round_down_chunk(cf, tf, base, 4, dq2, aq2, lambda);
+        s += 4;
       }
-      for (int k = 0; k < w; k++)
-        if (mask >> k & 1) {
-          const int rc = kScan8[i + k];
-          const int32_t c = cf[rc];
-          if (c != 0) cf[rc] = c < 0 ? c + 1 : c - 1;
-        }
-      i += w;
+      for (int k = 0; k < 4; k++) {
+        const int e = s + k;
+        if (e >= m) break;
+        const int rc = kScan8[e];
+        const int32_t c = cf[rc];
+        if (c != 0 && round_down_plain(fabsf(tf[rc]), uabs(c), rc == 0 ? dq2 : aq2, lambda))
+          cf[rc] = (C)(c < 0 ? c + 1 : c - 1);
+      }
     }
   }
-  for (; i < m; i++) {
-    const int rc = kScan8[i];
-    const int32_t c = cf[rc];
-    if (c != 0 && round_down_plain(fabsf(tf[rc]), uabs(c), rc == 0 ? dq2 : aq2, lambda))
-      cf[rc] = c < 0 ? c + 1 : c - 1;
-  }
-  // Suffix sums of the zeroing distortion, exact right-to-left order.
-  float suf[65];
+  // Suffix sums of the zeroing distortion in exact right-to-left order.
   suf[m] = 0.0f;
-  for (int e = m - 1; e >= 0; e--) {
+  for (int e = M - 1; e >= 0; e--) {
+    if (e >= m) continue;
     const int rc = kScan8[e];
     const float at = fabsf(tf[rc]);
     suf[e] = __fadd_rn(suf[e + 1], __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
@@ -106,7 +145,8 @@ __device__ void trellis8(int32_t* cf, const float* tf, float dc_q, float ac_q, f
   int best_e = -1;
   float best = __int_as_float(0x7f800000);
   float pre = 0.0f;
-  for (int e = 0; e < m; e++) {
+  for (int e = 0; e < M; e++) {
+    if (e >= m) continue;
     const int rc = kScan8[e];
     const float at = fabsf(tf[rc]);
     const uint32_t l = uabs(cf[rc]);
@@ -117,84 +157,96 @@ __device__ void trellis8(int32_t* cf, const float* tf, float dc_q, float ac_q, f
       const int extra = bin > 1 ? bin - 2 : 0;
       const float sig = __fadd_rn(__fmul_rn((float)bin, 0.9f), __fadd_rn((float)extra, 2.0f));
       const float c = __fadd_rn(__fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, sig)), suf[e + 1]);
-      if (c < best) { best = c; best_e = e; }
+      if (c < best) {
+        best = c;
+        best_e = e;
+      }
     }
     pre = __fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, coef_rate_bits(l)));
   }
-  const float skip = __fadd_rn(suf[0], __fmul_rn(lambda, 1.0f));
+  const float skip = __fadd_rn(suf[0], lambda);
   const int keep = (best_e < 0 || skip < best) ? 0 : best_e + 1;
-  for (int e = keep; e < m; e++) cf[kScan8[e]] = 0;
+  for (int e = 0; e < M; e++)
+    if (e >= keep && e < m) cf[kScan8[e]] = 0;
+  return keep - 1;
 }
 
-// Coefficient rate of an 8x8 luma block (src/rate.rs:149-291) from the
-// host-built bit costs; float additions in the reference's order.
-__device__ float rate8(const int32_t* cf, const mt_coef_costs& C, int skip_ctx, int dcs, int mode, int tx,
-                       bool use_skip_bits, float skip1, float skip0, int* eob_out) {
-  int eob = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) { eob = i; break; }
-  *eob_out = eob;
-  if (eob < 0) return use_skip_bits ? skip1 : C.txb_skip[skip_ctx][1];
-  float bits = use_skip_bits ? skip0 : C.txb_skip[skip_ctx][0];
-  bits = __fadd_rn(bits, C.txtp[mode][tx]);
-  const float* dcs_c = C.dc_sign[dcs];
-  auto hi_tok = [&](uint32_t m, int bc) -> float {
-    float h = C.br_cum[bc][min((int32_t)m - 3, 12)];
-    if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
-    return h;
-  };
+// Coefficient bits of an 8x8 luma block (src/rate.rs:149-291) from the
+// host-built bit costs, float additions in the reference's order.  The
+// reference walks the scan backwards keeping a level map; a position's
+// neighbour holds its level exactly when the neighbour's scan index is above
+// the current one (positions past the padded 8x8 plane read zero), so the
+// contexts are formed from the final levels and the inverse scan instead.
+template <typename C>
+__device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ctx, int dcs, int mode, int tx,
+                       bool use_skip_bits, float skip1, float skip0) {
+  const int E = warp_max(eob);
+  if (eob < 0) return use_skip_bits ? skip1 : T.txb_skip[skip_ctx][1];
+  float bits = use_skip_bits ? skip0 : T.txb_skip[skip_ctx][0];
+  bits = __fadd_rn(bits, T.txtp[mode][tx]);
+  const float* dcs_c = T.dc_sign[dcs];
   if (eob == 0) {
     const uint32_t m = uabs(cf[0]), mm = min(m, 3u);
-    bits = __fadd_rn(bits, C.eob_bin[0]);
-    bits = __fadd_rn(bits, C.eob_base[0][mm - 1]);
-    if (mm == 3) bits = __fadd_rn(bits, hi_tok(m, 0));
+    bits = __fadd_rn(bits, T.eob_bin[0]);
+    bits = __fadd_rn(bits, T.eob_base[0][mm - 1]);
+    if (mm == 3) {
+      float h = T.br_cum[0][min((int32_t)m - 3, 12)];
+      if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+      bits = __fadd_rn(bits, h);
+    }
     return __fadd_rn(bits, dcs_c[cf[0] < 0]);
   }
   const int eob_bin = eob < 2 ? eob : 32 - __clz(eob);
-  bits = __fadd_rn(bits, C.eob_bin[eob_bin]);
+  bits = __fadd_rn(bits, T.eob_bin[eob_bin]);
   if (eob_bin > 1) {
     const int nb = eob_bin - 2;
-    bits = __fadd_rn(bits, C.eob_hi[eob_bin][(eob >> nb) & 1]);
+    bits = __fadd_rn(bits, T.eob_hi[eob_bin][(eob >> nb) & 1]);
     bits = __fadd_rn(bits, (float)nb);
   }
-  uint8_t lv[100];
-  for (int i = 0; i < 100; i++) lv[i] = 0;
   const int ctx_e = 1 + (eob > 8) + (eob > 16);
   {
     const int rc = kScan8[eob];
     const int ex = rc >> 3, ey = rc & 7;
     const uint32_t m = uabs(cf[rc]);
     const uint32_t tok = min(m, 3u) - 1;
-    bits = __fadd_rn(bits, C.eob_base[ctx_e][tok]);
-    if (tok == 2) bits = __fadd_rn(bits, hi_tok(m, (ex | ey) > 1 ? 14 : 7));
-    lv[ex * 8 + ey] = level_byte(m);
+    bits = __fadd_rn(bits, T.eob_base[ctx_e][tok]);
+    if (tok == 2) {
+      float h = T.br_cum[(ex | ey) > 1 ? 14 : 7][min((int32_t)m - 3, 12)];
+      if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+      bits = __fadd_rn(bits, h);
+    }
   }
+  // Neighbour level of plane index p (x*8 + y + offset) seen from scan index i.
+  auto nb = [&](int p, int i) -> uint32_t {
+    return (p < 64 && (int)kIScan8[p] > i) ? level_byte(uabs(cf[p])) : 0u;
+  };
   int ac_nz = 1;
-  for (int i = eob - 1; i >= 1; i--) {
+  for (int i = E - 1; i >= 1; i--) {
+    if (i >= eob) continue;
     const int rc = kScan8[i];
     const int x = rc >> 3, y = rc & 7;
-    const uint32_t hm = (uint32_t)lv[x * 8 + y + 1] + lv[(x + 1) * 8 + y] + lv[(x + 1) * 8 + y + 1];
-    const uint32_t mag = hm + lv[x * 8 + y + 2] + lv[(x + 2) * 8 + y];
+    const int p = x * 8 + y;
+    const uint32_t hm = nb(p + 1, i) + nb(p + 8, i) + nb(p + 9, i);
+    const uint32_t mag = hm + nb(p + 2, i) + nb(p + 16, i);
     const int ctx = kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
     const uint32_t m = uabs(cf[rc]);
     const uint32_t tok = min(m, 3u);
-    bits = __fadd_rn(bits, C.base_tok[ctx][tok]);
+    bits = __fadd_rn(bits, T.base_tok[ctx][tok]);
     if (tok == 3) {
       const uint32_t hmag = hm & 63;
       const int bc = ((y | x) > 1 ? 14 : 7) + (hmag > 12 ? 6 : (int)((hmag + 1) >> 1));
-      bits = __fadd_rn(bits, C.br_cum[bc][min((int32_t)m - 3, 12)]);
+      bits = __fadd_rn(bits, T.br_cum[bc][min((int32_t)m - 3, 12)]);
       if (m >= 15) bits = __fadd_rn(bits, golomb_cost(m - 15));
     }
-    if (m != 0) {
-      lv[x * 8 + y] = level_byte(m);
-      ac_nz++;
-    }
+    ac_nz += m != 0;
   }
   const uint32_t dm = uabs(cf[0]), dtok = min(dm, 3u);
-  bits = __fadd_rn(bits, C.base_tok[0][dtok]);
+  bits = __fadd_rn(bits, T.base_tok[0][dtok]);
   if (dtok == 3) {
-    const uint32_t mag = ((uint32_t)lv[1] + lv[8] + lv[9]) & 63;
-    bits = __fadd_rn(bits, hi_tok(dm, mag > 12 ? 6 : (int)((mag + 1) >> 1)));
+    const uint32_t mag = (level_byte(uabs(cf[1])) + level_byte(uabs(cf[8])) + level_byte(uabs(cf[9]))) & 63;
+    float h = T.br_cum[mag > 12 ? 6 : (int)((mag + 1) >> 1)][min((int32_t)dm - 3, 12)];
+    if (dm >= 15) h = __fadd_rn(h, golomb_cost(dm - 15));
+    bits = __fadd_rn(bits, h);
   }
   if (cf[0] != 0) bits = __fadd_rn(bits, dcs_c[cf[0] < 0]);
   for (int k = 0; k < ac_nz; k++) bits = __fadd_rn(bits, 1.0f);
@@ -202,21 +254,30 @@ __device__ float rate8(const int32_t* cf, const mt_coef_costs& C, int skip_ctx, 
 }
 
 // Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
-__device__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const int32_t* pred,
-                          const int32_t* rr, int32_t maxv) {
+template <typename P, typename R>
+__device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
+                                          const R* rr, int32_t maxv) {
   uint32_t satd = 0;
+#pragma unroll
   for (int ty = 0; ty < 8; ty += 4)
+#pragma unroll
     for (int tx = 0; tx < 8; tx += 4) {
       int32_t r[4][4];
+#pragma unroll
       for (int y = 0; y < 4; y++) {
         int32_t d[4];
+#pragma unroll
         for (int x = 0; x < 4; x++) {
           const int i = (ty + y) * 8 + tx + x;
           d[x] = (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv);
         }
         const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
-        r[y][0] = e + g; r[y][1] = f + h; r[y][2] = f - h; r[y][3] = e - g;
+        r[y][0] = e + g;
+        r[y][1] = f + h;
+        r[y][2] = f - h;
+        r[y][3] = e - g;
       }
+#pragma unroll
       for (int x = 0; x < 4; x++) {
         const int32_t e = r[0][x] + r[2][x], f = r[0][x] - r[2][x], g = r[1][x] + r[3][x], h = r[1][x] - r[3][x];
         satd += uabs(e + g) + uabs(f + h) + uabs(f - h) + uabs(e - g);
@@ -236,44 +297,53 @@ __device__ __forceinline__ bool cand_ok(const mt_candidate& c, int fw, int fh) {
 // allocation.  NVVM -O3 (CUDA 12.9, sm_100a) was seen to give two separate
 // per-thread arrays that are both live across an inlined transform the same
 // local-memory slot (the residual input and the level output); a single
-// allocation cannot be split that way.
+// allocation cannot be split that way.  Sample-domain arrays are int16:
+// for 8-bit video every prediction, residual, level and inverse output fits.
 struct Work8 {
-  int32_t arena[256];
-  __device__ __forceinline__ int32_t* pred() { return arena; }
-  __device__ __forceinline__ int32_t* cf() { return arena + 64; }
-  __device__ __forceinline__ int32_t* rr() { return arena + 128; }
-  __device__ __forceinline__ float* tf() { return reinterpret_cast<float*>(arena + 192); }
+  int32_t w[228];
+  __device__ __forceinline__ float* tf() { return reinterpret_cast<float*>(w); }
+  __device__ __forceinline__ float* suf() { return reinterpret_cast<float*>(w + 64); }
+  __device__ __forceinline__ int16_t* pred() { return reinterpret_cast<int16_t*>(w + 132); }
+  __device__ __forceinline__ int16_t* rr() { return reinterpret_cast<int16_t*>(w + 164); }
+  __device__ __forceinline__ int16_t* cf() { return reinterpret_cast<int16_t*>(w + 196); }
 };
 
-// Evaluate one candidate (src/coder/partition_search.rs:467-530).  Leaves the
-// final levels (column-major) in w.cf(), the prediction in w.pred() and the
-// reconstruction residual in w.rr().
+// Evaluate one candidate.  Leaves the final levels (column-major) in w.cf(),
+// the prediction in w.pred() and the inverse residual in w.rr().
 __device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
                                            const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
-                                           const uint8_t* qm, const mt_coef_costs& C, const mt_candidate& cd,
+                                           const uint8_t* qm, const mt_coef_costs& T, const mt_candidate& cd,
                                            mt_candidate_result& r, Work8& w) {
   const int32_t maxv = (1 << p.bd) - 1;
-  int32_t* pred = w.pred();
-  int32_t* cf = w.cf();
-  int32_t* rr = w.rr();
+  int16_t* pred = w.pred();
+  int16_t* cf = w.cf();
+  int16_t* rr = w.rr();
   float* tf = w.tf();
   predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
            (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred);
+#pragma unroll
   for (int y = 0; y < 8; y++)
+#pragma unroll
     for (int x = 0; x < 8; x++)
-      rr[y * 8 + x] = (int32_t)src[(size_t)(cd.py + y) * p.stride + cd.px + x] - pred[y * 8 + x];
+      rr[y * 8 + x] = (int16_t)((int32_t)src[(size_t)(cd.py + y) * p.stride + cd.px + x] - pred[y * 8 + x]);
   fwd8x8(rr, cd.tx_type, q, cf, tf);
   const bool two_d = cd.tx_type == MT_TX_DCT_DCT || cd.tx_type >= MT_TX_ADST_ADST;
   if (qm && two_d) apply_qm(cf, tf, qm, 64);
-  if (p.trellis_lambda0 > 0.0f) trellis8(cf, tf, (float)q.dc_q, (float)q.ac_q, trellis_lambda);
+  int eob;
+  if (p.trellis_lambda0 > 0.0f) {
+    eob = trellis8(cf, tf, w.suf(), (float)q.dc_q, (float)q.ac_q, trellis_lambda);
+  } else {
+    eob = -1;
+    for (int i = 0; i < 64; i++)
+      if (cf[kScan8[i]] != 0) eob = i;
+  }
   inv8x8(cf, cd.tx_type, q, qm, rr);
   const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv);
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
-  int eob;
-  const float cbits = rate8(cf, C, cd.skip_ctx, cd.dcs_ctx, cd.mode, cd.tx_type, p.use_skip_bits != 0,
-                            p.skip_bits[0], p.skip_bits[1], &eob);
+  const float cbits = rate8(cf, eob, T, cd.skip_ctx, cd.dcs_ctx, cd.mode, cd.tx_type, p.use_skip_bits != 0,
+                            p.skip_bits[0], p.skip_bits[1]);
   const float bits = __fadd_rn(cbits, cd.mode_bits);
   r.distortion = price;
   r.bits = bits;

@@ -87,12 +87,13 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
 }
 
 // Prediction of an 8x8 block into out[64] (row-major).
+template <typename O>
 __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
-                         int delta, bool have_tr, bool have_bl, bool ft, int bd, int32_t* __restrict__ out) {
+                         int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out) {
   constexpr int bw = 8, bh = 8, edge_len = 16;
   if (mode == MT_DC_PRED) {
     const int32_t d = dc_pred_sq(rec, stride, ox, oy, 8, 3, bd);
-    for (int i = 0; i < 64; i++) out[i] = d;
+    for (int i = 0; i < 64; i++) out[i] = (O)(d);
     return;
   }
   int32_t A[kEdgeCap8], L[kEdgeCap8];
@@ -150,10 +151,10 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
     const int32_t* l = L + kEdgeOrigin;
     if (angle == 90) {
       for (int y = 0; y < bh; y++)
-        for (int x = 0; x < bw; x++) out[y * bw + x] = a[x];
+        for (int x = 0; x < bw; x++) out[y * bw + x] = (O)(a[x]);
     } else if (angle == 180) {
       for (int y = 0; y < bh; y++)
-        for (int x = 0; x < bw; x++) out[y * bw + x] = l[y];
+        for (int x = 0; x < bw; x++) out[y * bw + x] = (O)(l[y]);
     } else if (angle < 90) {
       const int dx = kDrDeriv[angle >> 1];
       const int max_base_x = (edge_len - 1) << up_a;
@@ -164,7 +165,7 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
         const int b0 = xpos >> frac_bits;
         for (int x = 0; x < bw; x++) {
           const int b = b0 + x * inc;
-          out[y * bw + x] = b < max_base_x ? (a[b] * (32 - shift) + a[b + 1] * shift + 16) >> 5 : a[max_base_x];
+          out[y * bw + x] = (O)(b < max_base_x ? (a[b] * (32 - shift) + a[b + 1] * shift + 16) >> 5 : a[max_base_x]);
         }
       }
     } else if (angle > 180) {
@@ -176,7 +177,7 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
           const int ypos = dy * (x + 1);
           const int shift = ((ypos << up_l) & 0x3f) >> 1;
           const int b = (ypos >> frac_bits) + y * inc;
-          out[y * bw + x] = b >= max_base_y ? l[max_base_y] : (l[b] * (32 - shift) + l[b + 1] * shift + 16) >> 5;
+          out[y * bw + x] = (O)(b >= max_base_y ? l[max_base_y] : (l[b] * (32 - shift) + l[b + 1] * shift + 16) >> 5);
         }
     } else {
       const int dy = kDrDeriv[(angle - 90) >> 1];
@@ -192,10 +193,10 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
             const int ypos = (y << 6) - (x + 1) * dy;
             const int b = ypos >> (6 - up_l);
             const int sh = ((ypos * (1 << up_l)) & 0x3f) >> 1;
-            out[y * bw + x] = (l[b] * (32 - sh) + l[b + 1] * sh + 16) >> 5;
+            out[y * bw + x] = (O)((l[b] * (32 - sh) + l[b + 1] * sh + 16) >> 5);
           } else {
             const int b = ba0 + (x - x0) * (1 << up_a);
-            out[y * bw + x] = (a[b] * (32 - sha) + a[b + 1] * sha + 16) >> 5;
+            out[y * bw + x] = (O)((a[b] * (32 - sha) + a[b + 1] * sha + 16) >> 5);
           }
         }
       }
@@ -209,7 +210,7 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
       for (int x = 0; x < bw; x++) {
         const int32_t lv = l[y], tv = a[x], b = lv + tv - corner;
         const int32_t ld = abs(lv - b), td = abs(tv - b), cd = abs(corner - b);
-        out[y * bw + x] = (ld <= td && ld <= cd) ? lv : (td <= cd ? tv : corner);
+        out[y * bw + x] = (O)((ld <= td && ld <= cd) ? lv : (td <= cd ? tv : corner));
       }
   } else if (mode == MT_SMOOTH_PRED) {
     const int32_t right = a[bw - 1], bottom = l[bh - 1];
@@ -217,16 +218,16 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
       for (int x = 0; x < bw; x++) {
         const int32_t wv = kSmW8[y], wh = kSmW8[x];
         const int32_t p = wv * a[x] + (256 - wv) * bottom + wh * l[y] + (256 - wh) * right;
-        out[y * bw + x] = (p + 256) >> 9;
+        out[y * bw + x] = (O)((p + 256) >> 9);
       }
   } else if (mode == MT_SMOOTH_V_PRED) {
     const int32_t bottom = l[bh - 1];
     for (int y = 0; y < bh; y++)
-      for (int x = 0; x < bw; x++) out[y * bw + x] = (kSmW8[y] * a[x] + (256 - kSmW8[y]) * bottom + 128) >> 8;
+      for (int x = 0; x < bw; x++) out[y * bw + x] = (O)((kSmW8[y] * a[x] + (256 - kSmW8[y]) * bottom + 128) >> 8);
   } else {  // SMOOTH_H
     const int32_t right = a[bw - 1];
     for (int y = 0; y < bh; y++)
-      for (int x = 0; x < bw; x++) out[y * bw + x] = (kSmW8[x] * l[y] + (256 - kSmW8[x]) * right + 128) >> 8;
+      for (int x = 0; x < bw; x++) out[y * bw + x] = (O)((kSmW8[x] * l[y] + (256 - kSmW8[x]) * right + 128) >> 8);
   }
 }
 

@@ -158,7 +158,8 @@ __device__ __forceinline__ int row_kind(int tx) {
 // column-major levels and f32 targets (src/dct.rs:279-301, :1222-1293 for the
 // 2-D types; :328-370 V/H_DCT; :1586-1611 IDTX).  The QM step of the 2-D types
 // is applied by the caller.
-__device__ void fwd8x8(const int32_t* __restrict__ in, int tx, const mt_quant& q, int32_t* __restrict__ cf,
+template <typename I, typename C>
+__device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* __restrict__ cf,
                        float* __restrict__ tf) {
   if (tx == MT_TX_IDTX) {
 #pragma unroll 8
@@ -169,7 +170,7 @@ __device__ void fwd8x8(const int32_t* __restrict__ in, int tx, const mt_quant& q
       tf[rc] = __fdiv_rn((float)num, (float)qd);
       const int32_t am = (int32_t)uabs(num);
       const int32_t level = (am + qd / 2) / qd;
-      cf[rc] = am < qd ? 0 : (num < 0 ? -level : level);
+      cf[rc] = (C)(am < qd ? 0 : (num < 0 ? -level : level));
     }
     return;
   }
@@ -201,7 +202,9 @@ __device__ void fwd8x8(const int32_t* __restrict__ in, int tx, const mt_quant& q
 #pragma unroll
       for (int x = 0; x < 8; x++) {
         const int rc = y + x * 8;
-        quant_fullstep(t[y * 8 + x], rc == 0 ? q.q_mult_dc : q.q_mult_ac, &cf[rc], &tf[rc]);
+        int32_t lv;
+        quant_fullstep(t[y * 8 + x], rc == 0 ? q.q_mult_dc : q.q_mult_ac, &lv, &tf[rc]);
+        cf[rc] = (C)lv;
       }
     return;
   }
@@ -223,7 +226,7 @@ __device__ void fwd8x8(const int32_t* __restrict__ in, int tx, const mt_quant& q
     for (int u = 0; u < 8; u++) {
       const int idx = u * 8 + r;
       const int32_t m = idx == 0 ? q.q_mult_dc : q.q_mult_ac;
-      cf[idx] = quant_q16(v[u], m);
+      cf[idx] = (C)quant_q16(v[u], m);
       tf[idx] = __fmul_rn(__fmul_rn((float)v[u], (float)m), 1.0f / 65536.0f);
     }
   }
@@ -232,7 +235,8 @@ __device__ void fwd8x8(const int32_t* __restrict__ in, int tx, const mt_quant& q
 // Forward QM scale (1024 + w/2)/w / 32 (src/dct.rs:93-104) and the AVX2
 // re-quantisation of the pinned x86 build (src/avx/qmatrix.rs:34-71): scale the
 // target, round half away from zero by truncate + fraction test.
-__device__ __forceinline__ void apply_qm(int32_t* cf, float* tf, const uint8_t* iw, int n) {
+template <typename C>
+__device__ __forceinline__ void apply_qm(C* cf, float* tf, const uint8_t* iw, int n) {
   for (int i = 0; i < n; i++) {
     const int w = iw[i];
     const float scale = __fdiv_rn((float)((1024 + w / 2) / w), 32.0f);
@@ -241,15 +245,16 @@ __device__ __forceinline__ void apply_qm(int32_t* cf, float* tf, const uint8_t* 
     const float tr = truncf(x);
     const float frac = fabsf(__fsub_rn(x, tr));
     const float step = frac >= 0.5f ? copysignf(1.0f, x) : 0.0f;
-    cf[i] = (int32_t)__fadd_rn(tr, step);
+    cf[i] = (C)(int32_t)__fadd_rn(tr, step);
   }
 }
 
 // Dequantisation (src/idct.rs:1562-1590) and the 8x8 inverse transforms
 // (src/idct.rs:1572-1824): tmp[y*8+x] = coeff[y + x*8]; row pass, (t+1)>>1 with
 // the column clip, column pass, (t+8)>>4.
-__device__ void inv8x8(const int32_t* __restrict__ cf, int tx, const mt_quant& q, const uint8_t* __restrict__ qm,
-                       int32_t* __restrict__ out) {
+template <typename C, typename O>
+__device__ void inv8x8(const C* __restrict__ cf, int tx, const mt_quant& q, const uint8_t* __restrict__ qm,
+                       O* __restrict__ out) {
   const bool flat = tx == MT_TX_IDTX || tx == MT_TX_V_DCT || tx == MT_TX_H_DCT;
   const uint8_t* w = flat ? nullptr : qm;
   int32_t t[64];
@@ -287,7 +292,7 @@ __device__ void inv8x8(const int32_t* __restrict__ cf, int tx, const mt_quant& q
     }
   }
 #pragma unroll
-  for (int i = 0; i < 64; i++) out[i] = (t[i] + 8) >> 4;
+  for (int i = 0; i < 64; i++) out[i] = (O)((t[i] + 8) >> 4);
 }
 
 }  // namespace mtd

@@ -166,3 +166,59 @@ def level_candidates(fw, fh, modes, tx_types, deltas=(0,), n=8, seed=0):
     out["skip_ctx"] = 0
     out["mode_bits"] = (rng.random(len(out)) * 6 + 1).astype(np.float32)
     return out
+
+
+def level_blocks(fw, fh, n=8, seed=0):
+    """Block records of one 8x8 level (raster order) with deterministic
+    neighbour flags, contexts and mode-signalling bits."""
+    rng = np.random.default_rng(seed)
+    bys, bxs = np.meshgrid(np.arange(0, fh - n + 1, n), np.arange(0, fw - n + 1, n), indexing="ij")
+    px, py = bxs.ravel(), bys.ravel()
+    out = np.zeros(len(px), abi.BLOCK8_DTYPE)
+    out["px"], out["py"] = px, py
+    out["flags"] = [block_flags(int(x), int(y), fw, fh, n) for x, y in zip(px, py)]
+    out["dcs_ctx"] = rng.integers(0, 3, size=len(px))
+    out["skip_ctx"] = 0
+    out["mode_bits"] = (rng.random((len(px), 13)) * 6 + 1).astype(np.float32)
+    return out
+
+
+def level_combos(modes, tx_types, deltas=(0,)):
+    """(mode, angle delta, tx type) combos in the reference's evaluation order
+    (mode, then delta, then type)."""
+    rows = []
+    for m in modes:
+        ds = deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)
+        for d in ds:
+            for t in tx_types:
+                rows.append((m, d, t, 0))
+    return _combos(rows)
+
+
+def _combos(rows):
+    out = np.zeros(len(rows), abi.COMBO_DTYPE)
+    for i, (m, d, t, _) in enumerate(rows):
+        out[i] = (m, d, t, 0)
+    return out
+
+
+def candidates_of_level(blocks, combos):
+    """The candidate list a level launch evaluates, combo-major (index c * nblocks + b)."""
+    nb, nc = len(blocks), len(combos)
+    out = np.zeros(nb * nc, abi.CANDIDATE_DTYPE)
+    out["px"] = np.tile(blocks["px"], nc)
+    out["py"] = np.tile(blocks["py"], nc)
+    out["mode"] = np.repeat(combos["mode"], nb)
+    out["angle_delta"] = np.repeat(combos["angle_delta"], nb)
+    out["tx_type"] = np.repeat(combos["tx_type"], nb)
+    out["flags"] = np.tile(blocks["flags"], nc)
+    out["dcs_ctx"] = np.tile(blocks["dcs_ctx"], nc)
+    out["skip_ctx"] = np.tile(blocks["skip_ctx"], nc)
+    out["mode_bits"] = blocks["mode_bits"][np.tile(np.arange(nb), nc), np.repeat(combos["mode"], nb)]
+    return out
+
+
+def best_of_level(results, nblocks, ncombos):
+    """Per-block argmin of combo-major results with the first-minimum rule."""
+    cost = results["cost"].reshape(ncombos, nblocks)
+    return np.argmin(cost, axis=0)

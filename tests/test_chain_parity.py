@@ -92,11 +92,15 @@ def test_chain_device_api_and_empty_batch(mt_lib, oracle_lib, cuda):
     d_costs = torch.from_numpy(np.frombuffer(bytes(costs), np.uint8).copy()).to(dev)
     d_cands = torch.from_numpy(cands.view(np.uint8)).to(dev)
     d_res = torch.zeros(len(cands) * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    b, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, cands, threads=8)
     mt_lib.candidate_chain_device(d_src, d_rec, prm, q, d_qm, d_costs, d_cands, len(cands), d_res)
     torch.cuda.synchronize()
-    a = d_res.cpu().numpy().view(abi.RESULT_DTYPE)
-    b, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, cands, threads=8)
-    assert a.tobytes() == b.tobytes()
+    assert d_res.cpu().numpy().tobytes() == b.tobytes()
+    d_scr = torch.zeros(mt_lib.chain_scratch_bytes(len(cands)), dtype=torch.uint8, device=dev)
+    d_res.zero_()
+    mt_lib.candidate_chain_device(d_src, d_rec, prm, q, d_qm, d_costs, d_cands, len(cands), d_res, d_scratch=d_scr)
+    torch.cuda.synchronize()
+    assert d_res.cpu().numpy().tobytes() == b.tobytes()
     mt_lib.candidate_chain_device(d_src, d_rec, prm, q, d_qm, d_costs, d_cands, 0, d_res)
 
 
