@@ -45,6 +45,7 @@ extern "C" {
 #define MT_OK 0
 #define MT_ERR_INVALID_INPUT (-2)
 #define MT_ERR_UNSUPPORTED (-3)
+#define MT_ERR_TOO_LARGE (-4)
 #define MT_ERR_DEVICE (-10)
 #define MT_ERR_ALLOC (-11)
 
@@ -240,6 +241,27 @@ int mt_rdo_level8_device(const uint16_t* d_src, const uint16_t* d_recon, const m
                          const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
                          int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
                          void* d_keys, void* stream);
+
+/* Allocation-free form of mt_rdo_level8_device.  No counterpart in the
+ * reference: it exists for callers that cannot give this library device
+ * memory on demand (a fixed GPU-memory budget owned by another framework's
+ * pool, or a real-time thread that must not call the driver's allocator).
+ * The caller passes only inputs and the per-block output; the call allocates
+ * nothing and needs no working storage: its per-block argmin keys live in a
+ * file-scope device array of MT_NOALLOC_MAX_BLOCKS entries (1 MiB held on
+ * every device that loads the library until exit), and each block's winner is
+ * re-evaluated to fill d_best, which equals mt_rdo_level8_device's d_best.
+ * More than MT_NOALLOC_MAX_BLOCKS blocks returns MT_ERR_TOO_LARGE.  The first
+ * call on a device looks up that array's device address (once per device, with
+ * the device current); make that first call before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must not be
+ * issued. */
+#define MT_NOALLOC_MAX_BLOCKS 131072
+int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_t* d_recon,
+                                 const mt_chain_params* prm, const mt_quant* quant,
+                                 const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                                 const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
+                                 int32_t ncombos, mt_block_best* d_best, void* stream);
 
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and

@@ -12,6 +12,8 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libmaroontree_b200.so")
 MT_OK = 0
 MT_ERR_INVALID_INPUT = -2
 MT_ERR_UNSUPPORTED = -3
+MT_ERR_TOO_LARGE = -4
+MT_NOALLOC_MAX_BLOCKS = 131072
 MT_ERR_DEVICE = -10
 MT_ERR_ALLOC = -11
 MT_EOB_INVALID = -2
@@ -108,6 +110,8 @@ def _bind(lib):
                                     C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_rdo_level8_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
                                            _P, C.c_int32, _P, _P, _P, _P]),
+        "mt_rdo_level8_device_noalloc": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
+                                                   C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -136,7 +140,7 @@ def load():
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
-    "mt_rdo_level8", "mt_rdo_level8_device", "mt_fwd_txfm_quant_device",
+    "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
 )
 
