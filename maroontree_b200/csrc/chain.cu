@@ -25,6 +25,11 @@ struct ChainArgs {
 };
 
 constexpr int kThreads = 128;
+// Minimum resident CTAs per SM requested from the register allocator.
+#ifndef MT_CHAIN_MIN_BLOCKS
+#define MT_CHAIN_MIN_BLOCKS 3
+#endif
+constexpr int kMinBlocks = MT_CHAIN_MIN_BLOCKS;
 constexpr int kBuckets = 1024;
 
 __device__ __forceinline__ int bucket_of(const mt_candidate& c) {
@@ -57,11 +62,16 @@ __global__ void bucket_scatter_kernel(const mt_candidate* __restrict__ cands, in
 }
 
 __device__ __forceinline__ void stage_tables(const mt_coef_costs* __restrict__ costs, const uint8_t* __restrict__ qm_row,
-                                             int has_qm, mt_coef_costs& sC, uint8_t* sQm) {
+                                             int has_qm, mt_coef_costs& sC, uint8_t* sQm, float* sQs, float* sLut) {
   const float* g = reinterpret_cast<const float*>(costs);
   float* s = reinterpret_cast<float*>(&sC);
   for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
-  if (threadIdx.x < 64) sQm[threadIdx.x] = has_qm ? qm_row[threadIdx.x] : 32;
+  if (threadIdx.x < 64) {
+    const int w = has_qm ? qm_row[threadIdx.x] : 32;
+    sQm[threadIdx.x] = (uint8_t)w;
+    sQs[threadIdx.x] = fwd_qm_scale(w);
+    sLut[threadIdx.x] = kCoefRateLut[threadIdx.x];
+  }
   __syncthreads();
 }
 
@@ -84,7 +94,7 @@ __device__ __forceinline__ void store_blocks(Work8& w, int32_t maxv, int32_t* lv
   }
 }
 
-__global__ void __launch_bounds__(kThreads) chain8_kernel(const uint16_t* __restrict__ src,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) chain8_kernel(const uint16_t* __restrict__ src,
                                                           const uint16_t* __restrict__ rec, ChainArgs a,
                                                           const uint8_t* __restrict__ qm_row,
                                                           const mt_coef_costs* __restrict__ costs,
@@ -94,7 +104,9 @@ __global__ void __launch_bounds__(kThreads) chain8_kernel(const uint16_t* __rest
                                                           int32_t* __restrict__ lv_out, int32_t* __restrict__ rec_out) {
   __shared__ mt_coef_costs sC;
   __shared__ uint8_t sQm[64];
-  stage_tables(costs, qm_row, a.has_qm, sC, sQm);
+  __shared__ float sQs[64];
+  __shared__ float sLut[64];
+  stage_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const int idx = perm ? perm[t] : t;
@@ -105,16 +117,17 @@ __global__ void __launch_bounds__(kThreads) chain8_kernel(const uint16_t* __rest
     res[idx] = bad;
     return;
   }
-  Work8 w;
+  int32_t store[kWork8Words];
+  Work8 w{store};
   mt_candidate_result r;
-  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[idx] = r;
   store_blocks(w, (1 << a.p.bd) - 1, lv_out, rec_out, (size_t)idx);
 }
 
 // Candidate (combo c, block b) for thread t: warps take 32 consecutive blocks
 // of one combo.
-__global__ void __launch_bounds__(kThreads) level8_kernel(const uint16_t* __restrict__ src,
+__global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint16_t* __restrict__ src,
                                                           const uint16_t* __restrict__ rec, ChainArgs a,
                                                           const uint8_t* __restrict__ qm_row,
                                                           const mt_coef_costs* __restrict__ costs,
@@ -124,7 +137,9 @@ __global__ void __launch_bounds__(kThreads) level8_kernel(const uint16_t* __rest
                                                           unsigned long long* __restrict__ best_key) {
   __shared__ mt_coef_costs sC;
   __shared__ uint8_t sQm[64];
-  stage_tables(costs, qm_row, a.has_qm, sC, sQm);
+  __shared__ float sQs[64];
+  __shared__ float sLut[64];
+  stage_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
   if (c >= ncombos) return;
@@ -148,9 +163,10 @@ __global__ void __launch_bounds__(kThreads) level8_kernel(const uint16_t* __rest
     res[slot] = bad;
     return;
   }
-  Work8 w;
+  int32_t store[kWork8Words];
+  Work8 w{store};
   mt_candidate_result r;
-  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[slot] = r;
   // Costs are non-negative finite floats, so their bit patterns order like
   // the values; ties go to the lower combo index (evaluated first).
@@ -186,14 +202,19 @@ __global__ void fwd8_kernel(const int32_t* __restrict__ resid, const uint8_t* __
                             float* __restrict__ targets) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  Work8 w;
+  int32_t store[kWork8Words + 64];
+  Work8 w{store};
   int32_t* r = w.w + 64;   // int32 residual at [64, 128)
   int32_t* cf = w.w + 128; // int32 levels at [128, 192)
   float* tf = w.tf();
   for (int i = 0; i < 64; i++) r[i] = resid[(size_t)idx * 64 + i];
   const int tx = types[idx];
-  fwd8x8(r, tx, q, cf, tf);
-  if (qm_row && (tx == MT_TX_DCT_DCT || tx >= MT_TX_ADST_ADST)) apply_qm(cf, tf, qm_row, 64);
+  fwd8x8(r, tx, q, cf, tf, store + kWork8Words);
+  if (qm_row && (tx == MT_TX_DCT_DCT || tx >= MT_TX_ADST_ADST)) {
+    float qs[64];
+    for (int i = 0; i < 64; i++) qs[i] = fwd_qm_scale(qm_row[i]);
+    apply_qm(cf, tf, qs, 64);
+  }
   for (int i = 0; i < 64; i++) {
     levels[(size_t)idx * 64 + i] = cf[i];
     targets[(size_t)idx * 64 + i] = tf[i];
@@ -203,25 +224,30 @@ __global__ void inv8_kernel(const int32_t* __restrict__ levels, const uint8_t* _
                             const uint8_t* __restrict__ qm_row, int32_t* __restrict__ out) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  Work8 w;
+  int32_t store[kWork8Words + 64];
+  Work8 w{store};
   int32_t* cf = w.w;        // int32 levels at [0, 64)
   int32_t* o = w.w + 64;    // int32 output at [64, 128)
   for (int i = 0; i < 64; i++) cf[i] = levels[(size_t)idx * 64 + i];
-  inv8x8(cf, types[idx], q, qm_row, o);
+  inv8x8(cf, types[idx], q, qm_row, o, store + kWork8Words);
   for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = o[i];
 }
 __global__ void trellis8_kernel(int32_t* __restrict__ levels, const float* __restrict__ targets, int n, float dc_q,
                                 float ac_q, float lambda) {
+  __shared__ float sLut[64];
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) sLut[i] = kCoefRateLut[i];
+  __syncthreads();
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
-  Work8 w;
+  int32_t store[kWork8Words];
+  Work8 w{store};
   int32_t* cf = w.w + 132;  // int32 levels at [132, 196)
   float* tf = w.tf();
   for (int i = 0; i < 64; i++) {
     cf[i] = levels[(size_t)idx * 64 + i];
     tf[i] = targets[(size_t)idx * 64 + i];
   }
-  trellis8(cf, tf, w.suf(), dc_q, ac_q, lambda);
+  trellis8(cf, tf, w.suf(), dc_q, ac_q, lambda, sLut);
   for (int i = 0; i < 64; i++) levels[(size_t)idx * 64 + i] = cf[i];
 }
 __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p, const mt_candidate* __restrict__ cands,
@@ -229,14 +255,15 @@ __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n) return;
   const mt_candidate cd = cands[idx];
-  Work8 w;
+  int32_t store[kWork8Words];
+  Work8 w{store};
   int16_t* pr = w.pred();
   if (!cand_ok(cd, p.frame_w, p.frame_h)) {
     for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = 0;
     return;
   }
   predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
-           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pr);
+           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pr, w.edges());
   for (int i = 0; i < 64; i++) out[(size_t)idx * 64 + i] = pr[i];
 }
 

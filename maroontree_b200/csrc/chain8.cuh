@@ -75,38 +75,52 @@ __device__ __forceinline__ bool round_down_plain(float at, uint32_t l, float q2,
   return cd < cl;
 }
 
-// One chunk of the trellis step A at scan positions [base, base + width).
-template <typename C>
-__device__ __forceinline__ void round_down_chunk(C* cf, const float* tf, int base, int width, float dq2, float aq2,
-                                                 float lambda) {
+// One chunk of the trellis step A at scan positions [base, base + W).  The
+// chunk's levels and targets are read once; decisions use the values at the
+// start of the chunk (scan positions are distinct, as in the AVX2 gather).
+// `lut` is the static per-level rate table in shared memory (per-lane
+// indices, so it must not sit in the constant cache).
+template <int W, typename C>
+__device__ __forceinline__ void round_down_chunk(C* cf, const float* tf, int base, float dq2, float aq2, float lambda,
+                                                 const float* lut) {
+  int32_t c[W];
+  float at[W];
+  int rc[W];
   bool big = false;
-  for (int k = 0; k < width; k++) big |= uabs(cf[kScan8[base + k]]) > 63u;
-  uint32_t mask = 0;
-  for (int k = 0; k < width; k++) {
-    const int rc = kScan8[base + k];
-    const int32_t c = cf[rc];
-    const float q2 = rc == 0 ? dq2 : aq2;
-    const float at = fabsf(tf[rc]);
-    const bool dn = big ? (c != 0 && round_down_plain(at, uabs(c), q2, lambda))
-                        : round_down_fma(at, (int32_t)uabs(c), q2, lambda);
-    mask |= (uint32_t)dn << k;
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    rc[k] = kScan8[base + k];
+    c[k] = cf[rc[k]];
+    at[k] = fabsf(tf[rc[k]]);
+    big |= uabs(c[k]) > 63u;
   }
-  for (int k = 0; k < width; k++) {
-    const int rc = kScan8[base + k];
-    const int32_t c = cf[rc];
-    if ((mask >> k & 1) && c != 0) cf[rc] = (C)(c < 0 ? c + 1 : c - 1);
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    const float q2 = rc[k] == 0 ? dq2 : aq2;
+    bool dn;
+    if (big) {
+      dn = c[k] != 0 && round_down_plain(at[k], uabs(c[k]), q2, lambda);
+    } else {
+      const int32_t li = (int32_t)uabs(c[k]), ldi = max(li - 1, 0);
+      const float el = __fsub_rn(at[k], (float)li), ed = __fsub_rn(at[k], (float)ldi);
+      const float cl = __fmaf_rn(q2, __fmul_rn(el, el), __fmul_rn(lambda, lut[li]));
+      const float cd = __fmaf_rn(q2, __fmul_rn(ed, ed), __fmul_rn(lambda, lut[ldi]));
+      dn = cd < cl;
+    }
+    if (dn && c[k] != 0) cf[rc[k]] = (C)(c[k] < 0 ? c[k] + 1 : c[k] - 1);
   }
 }
 
 // trellis_optimize (src/trellis.rs:944-1030) over the 8x8 default scan with
 // step A in the pinned AVX2 chunking (8-wide chunks, one 4-wide chunk, scalar
 // tail; a chunk holding a level >= 64 takes the scalar form in all lanes).
-// `suf` is scratch for 65 floats.  Returns the final EOB scan index (-1 when
-// every level is zero).
+// `suf` is scratch for 65 floats, `lut` the shared-memory rate table.
+// Returns the final EOB scan index (-1 when every level is zero).
 template <typename C>
-__device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda) {
+__device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda, const float* lut) {
   const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
   int eob_idx = -1;
+#pragma unroll 8
   for (int i = 0; i < 64; i++)
     if (cf[kScan8[i]] != 0) eob_idx = i;
   const int m = eob_idx + 1;
@@ -117,11 +131,11 @@ __device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac
   for (int base = 0; base < M; base += 8) {
     if (base >= m) continue;
     if (base < full8) {
-      round_down_chunk(cf, tf, base, 8, dq2, aq2, lambda);
+      round_down_chunk<8>(cf, tf, base, dq2, aq2, lambda, lut);
     } else {
       int s = base;
       if (has4) {
-        round_down_chunk(cf, tf, base, 4, dq2, aq2, lambda);
+        round_down_chunk<4>(cf, tf, base, dq2, aq2, lambda, lut);
         s += 4;
       }
       for (int k = 0; k < 4; k++) {
@@ -136,11 +150,13 @@ __device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac
   }
   // Suffix sums of the zeroing distortion in exact right-to-left order.
   suf[m] = 0.0f;
+  float acc = 0.0f;
   for (int e = M - 1; e >= 0; e--) {
     if (e >= m) continue;
     const int rc = kScan8[e];
     const float at = fabsf(tf[rc]);
-    suf[e] = __fadd_rn(suf[e + 1], __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
+    acc = __fadd_rn(acc, __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
+    suf[e] = acc;
   }
   int best_e = -1;
   float best = __int_as_float(0x7f800000);
@@ -152,17 +168,18 @@ __device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac
     const uint32_t l = uabs(cf[rc]);
     const float ecur = __fsub_rn(at, (float)l);
     const float dcur = __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(ecur, ecur));
+    const float base_c = __fadd_rn(pre, dcur);
     if (l != 0) {
       const int bin = e < 2 ? e : 32 - __clz(e);
       const int extra = bin > 1 ? bin - 2 : 0;
       const float sig = __fadd_rn(__fmul_rn((float)bin, 0.9f), __fadd_rn((float)extra, 2.0f));
-      const float c = __fadd_rn(__fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, sig)), suf[e + 1]);
+      const float c = __fadd_rn(__fadd_rn(base_c, __fmul_rn(lambda, sig)), suf[e + 1]);
       if (c < best) {
         best = c;
         best_e = e;
       }
     }
-    pre = __fadd_rn(__fadd_rn(pre, dcur), __fmul_rn(lambda, coef_rate_bits(l)));
+    pre = __fadd_rn(base_c, __fmul_rn(lambda, l < 64 ? lut[l] : coef_rate_bits(l)));
   }
   const float skip = __fadd_rn(suf[0], lambda);
   const int keep = (best_e < 0 || skip < best) ? 0 : best_e + 1;
@@ -172,14 +189,12 @@ __device__ int trellis8(C* cf, const float* tf, float* suf, float dc_q, float ac
 }
 
 // Coefficient bits of an 8x8 luma block (src/rate.rs:149-291) from the
-// host-built bit costs, float additions in the reference's order.  The
-// reference walks the scan backwards keeping a level map; a position's
-// neighbour holds its level exactly when the neighbour's scan index is above
-// the current one (positions past the padded 8x8 plane read zero), so the
-// contexts are formed from the final levels and the inverse scan instead.
+// host-built bit costs, float additions in the reference's order, with the
+// reference's level map (stride 8, reads past the 8x8 plane land in the
+// zeroed tail) kept in the 80-byte scratch `lv`.
 template <typename C>
 __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ctx, int dcs, int mode, int tx,
-                       bool use_skip_bits, float skip1, float skip0) {
+                       bool use_skip_bits, float skip1, float skip0, uint8_t* lv) {
   const int E = warp_max(eob);
   if (eob < 0) return use_skip_bits ? skip1 : T.txb_skip[skip_ctx][1];
   float bits = use_skip_bits ? skip0 : T.txb_skip[skip_ctx][0];
@@ -203,6 +218,9 @@ __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
     bits = __fadd_rn(bits, T.eob_hi[eob_bin][(eob >> nb) & 1]);
     bits = __fadd_rn(bits, (float)nb);
   }
+  uint32_t* lv32 = reinterpret_cast<uint32_t*>(lv);
+#pragma unroll
+  for (int i = 0; i < 20; i++) lv32[i] = 0;
   const int ctx_e = 1 + (eob > 8) + (eob > 16);
   {
     const int rc = kScan8[eob];
@@ -215,19 +233,15 @@ __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
       if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
       bits = __fadd_rn(bits, h);
     }
+    lv[rc] = (uint8_t)level_byte(m);
   }
-  // Neighbour level of plane index p (x*8 + y + offset) seen from scan index i.
-  auto nb = [&](int p, int i) -> uint32_t {
-    return (p < 64 && (int)kIScan8[p] > i) ? level_byte(uabs(cf[p])) : 0u;
-  };
   int ac_nz = 1;
   for (int i = E - 1; i >= 1; i--) {
     if (i >= eob) continue;
     const int rc = kScan8[i];
     const int x = rc >> 3, y = rc & 7;
-    const int p = x * 8 + y;
-    const uint32_t hm = nb(p + 1, i) + nb(p + 8, i) + nb(p + 9, i);
-    const uint32_t mag = hm + nb(p + 2, i) + nb(p + 16, i);
+    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + 8] + lv[rc + 9];
+    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 16];
     const int ctx = kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
     const uint32_t m = uabs(cf[rc]);
     const uint32_t tok = min(m, 3u);
@@ -238,12 +252,13 @@ __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
       bits = __fadd_rn(bits, T.br_cum[bc][min((int32_t)m - 3, 12)]);
       if (m >= 15) bits = __fadd_rn(bits, golomb_cost(m - 15));
     }
+    lv[rc] = (uint8_t)level_byte(m);
     ac_nz += m != 0;
   }
   const uint32_t dm = uabs(cf[0]), dtok = min(dm, 3u);
   bits = __fadd_rn(bits, T.base_tok[0][dtok]);
   if (dtok == 3) {
-    const uint32_t mag = (level_byte(uabs(cf[1])) + level_byte(uabs(cf[8])) + level_byte(uabs(cf[9]))) & 63;
+    const uint32_t mag = ((uint32_t)lv[1] + lv[8] + lv[9]) & 63;
     float h = T.br_cum[mag > 12 ? 6 : (int)((mag + 1) >> 1)][min((int32_t)dm - 3, 12)];
     if (dm >= 15) h = __fadd_rn(h, golomb_cost(dm - 15));
     bits = __fadd_rn(bits, h);
@@ -253,14 +268,19 @@ __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
   return bits;
 }
 
+#ifndef MT_SATD_UNROLL
+#define MT_SATD_UNROLL 1
+#endif
+constexpr int kSatdUnroll = MT_SATD_UNROLL;
+
 // Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
 template <typename P, typename R>
 __device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
                                           const R* rr, int32_t maxv) {
   uint32_t satd = 0;
-#pragma unroll
+#pragma unroll kSatdUnroll
   for (int ty = 0; ty < 8; ty += 4)
-#pragma unroll
+#pragma unroll kSatdUnroll
     for (int tx = 0; tx < 8; tx += 4) {
       int32_t r[4][4];
 #pragma unroll
@@ -293,57 +313,67 @@ __device__ __forceinline__ bool cand_ok(const mt_candidate& c, int fw, int fh) {
          c.angle_delta >= -3 && c.angle_delta <= 3 && c.dcs_ctx < 3 && c.skip_ctx < 13;
 }
 
-// Per-thread working set of one 8x8 candidate, carved out of ONE local
-// allocation.  NVVM -O3 (CUDA 12.9, sm_100a) was seen to give two separate
-// per-thread arrays that are both live across an inlined transform the same
-// local-memory slot (the residual input and the level output); a single
-// allocation cannot be split that way.  Sample-domain arrays are int16:
-// for 8-bit video every prediction, residual, level and inverse output fits.
+// Per-thread working set of one 8x8 candidate: a view onto ONE block of
+// kWork8Words 32-bit words (a single local array, or one thread's slice of a
+// shared-memory arena).  NVVM -O3 (CUDA 12.9, sm_100a) was seen to give two
+// separate per-thread local arrays that are both live across an inlined
+// transform the same slot (the residual input and the level output); one
+// allocation cannot be split that way.  Sample-domain arrays are int16: for
+// 8-bit video every prediction, residual, level and inverse output fits.
+// Layout (words): [0,64) tf | [64,132) suf, later the rate walk's level map |
+// [132,164) pred | [164,196) rr | [196,228) cf.  During prediction, before
+// tf and suf are live, [0,114) holds the two edges and the filter temporary.
+constexpr int kWork8Words = 228;
 struct Work8 {
-  int32_t w[228];
+  int32_t* w;
   __device__ __forceinline__ float* tf() { return reinterpret_cast<float*>(w); }
   __device__ __forceinline__ float* suf() { return reinterpret_cast<float*>(w + 64); }
+  __device__ __forceinline__ int32_t* edges() { return w; }
   __device__ __forceinline__ int16_t* pred() { return reinterpret_cast<int16_t*>(w + 132); }
   __device__ __forceinline__ int16_t* rr() { return reinterpret_cast<int16_t*>(w + 164); }
   __device__ __forceinline__ int16_t* cf() { return reinterpret_cast<int16_t*>(w + 196); }
 };
 
 // Evaluate one candidate.  Leaves the final levels (column-major) in w.cf(),
-// the prediction in w.pred() and the inverse residual in w.rr().
+// the prediction in w.pred() and the inverse residual in w.rr().  (Compiling
+// one path per transform type raised register use to the cap and was no
+// faster, so the type stays a run-time value.)
 __device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
                                            const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
-                                           const uint8_t* qm, const mt_coef_costs& T, const mt_candidate& cd,
-                                           mt_candidate_result& r, Work8& w) {
+                                           const uint8_t* qm, const float* qs, const float* lut,
+                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
+                                           Work8& w) {
   const int32_t maxv = (1 << p.bd) - 1;
   int16_t* pred = w.pred();
   int16_t* cf = w.cf();
   int16_t* rr = w.rr();
   float* tf = w.tf();
   predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
-           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred);
+           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, w.edges());
 #pragma unroll
   for (int y = 0; y < 8; y++)
 #pragma unroll
     for (int x = 0; x < 8; x++)
       rr[y * 8 + x] = (int16_t)((int32_t)src[(size_t)(cd.py + y) * p.stride + cd.px + x] - pred[y * 8 + x]);
-  fwd8x8(rr, cd.tx_type, q, cf, tf);
-  const bool two_d = cd.tx_type == MT_TX_DCT_DCT || cd.tx_type >= MT_TX_ADST_ADST;
-  if (qm && two_d) apply_qm(cf, tf, qm, 64);
+  const int TX = cd.tx_type;
+  fwd8x8(rr, TX, q, cf, tf, reinterpret_cast<int32_t*>(w.suf()));
+  const bool two_d = TX == MT_TX_DCT_DCT || TX >= MT_TX_ADST_ADST;
+  if (two_d && qm) apply_qm(cf, tf, qs, 64);
   int eob;
   if (p.trellis_lambda0 > 0.0f) {
-    eob = trellis8(cf, tf, w.suf(), (float)q.dc_q, (float)q.ac_q, trellis_lambda);
+    eob = trellis8(cf, tf, w.suf(), (float)q.dc_q, (float)q.ac_q, trellis_lambda, lut);
   } else {
     eob = -1;
     for (int i = 0; i < 64; i++)
       if (cf[kScan8[i]] != 0) eob = i;
   }
-  inv8x8(cf, cd.tx_type, q, qm, rr);
+  inv8x8(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
   const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv);
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
-  const float cbits = rate8(cf, eob, T, cd.skip_ctx, cd.dcs_ctx, cd.mode, cd.tx_type, p.use_skip_bits != 0,
-                            p.skip_bits[0], p.skip_bits[1]);
+  const float cbits = rate8(cf, eob, T, cd.skip_ctx, cd.dcs_ctx, cd.mode, TX, p.use_skip_bits != 0, p.skip_bits[0],
+                            p.skip_bits[1], reinterpret_cast<uint8_t*>(w.suf()));
   const float bits = __fadd_rn(cbits, cd.mode_bits);
   r.distortion = price;
   r.bits = bits;

@@ -39,14 +39,12 @@ __device__ __forceinline__ int edge_strength(int w, int h, bool ft, int delta) {
 
 // 5-tap edge smoothing of positions 0..size-2 from the unfiltered window
 // src[k] = edge[k-1] with clamped reads (src/intrapred.rs:977-1012).
-template <int CAP>
-__device__ __forceinline__ void filter_edge(int32_t* e, int size, int strength) {
+__device__ __forceinline__ void filter_edge(int32_t* e, int size, int strength, int32_t* src) {
   if (strength == 0) return;
   int32_t k0, k1, k2;  // symmetric taps: (k0, k1, k2, k1, k0)
   if (strength == 1) { k0 = 0; k1 = 4; k2 = 8; }
   else if (strength == 2) { k0 = 0; k1 = 5; k2 = 6; }
   else { k0 = 2; k1 = 4; k2 = 4; }
-  int32_t src[CAP];
   for (int i = 0; i < size; i++) src[i] = e[kEdgeOrigin + i - 1];
   const int last = size - 1;
   for (int o = 0; o < size - 1; o++) {
@@ -57,9 +55,7 @@ __device__ __forceinline__ void filter_edge(int32_t* e, int size, int strength) 
 }
 
 // 2x upsampling of num_px edge samples (src/intrapred.rs:1026-1048).
-template <int CAP>
-__device__ __forceinline__ void upsample_edge(int32_t* e, int num_px, int32_t maxv) {
-  int32_t in[CAP];
+__device__ __forceinline__ void upsample_edge(int32_t* e, int num_px, int32_t maxv, int32_t* in) {
   in[0] = e[kEdgeOrigin - 1];
   in[1] = e[kEdgeOrigin - 1];
   for (int i = 0; i < num_px; i++) in[i + 2] = e[kEdgeOrigin + i];
@@ -86,18 +82,23 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
   return 1 << (bd - 1);
 }
 
-// Prediction of an 8x8 block into out[64] (row-major).
+// Prediction of an 8x8 block into out[64] (row-major).  `scratch` holds
+// 3 * kEdgeCap8 words: the above and left edges and a filter temporary.
 template <typename O>
 __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
-                         int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out) {
+                         int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out,
+                         int32_t* __restrict__ scratch) {
   constexpr int bw = 8, bh = 8, edge_len = 16;
   if (mode == MT_DC_PRED) {
     const int32_t d = dc_pred_sq(rec, stride, ox, oy, 8, 3, bd);
     for (int i = 0; i < 64; i++) out[i] = (O)(d);
     return;
   }
-  int32_t A[kEdgeCap8], L[kEdgeCap8];
-  for (int i = 0; i < kEdgeCap8; i++) A[i] = L[i] = 0;
+  // Every edge entry the predictor reads is written below (logical -1 ..
+  // 15, and -2 .. 30 once upsampled), so the arrays are not cleared.
+  int32_t* A = scratch;
+  int32_t* L = scratch + kEdgeCap8;
+  int32_t* tmp = scratch + 2 * kEdgeCap8;
   const bool have_top = oy > 0, have_left = ox > 0;
   const int32_t base = 1 << (bd - 1);
   const uint16_t* up = rec + (size_t)(oy - 1) * stride + ox;     // valid when have_top
@@ -137,15 +138,15 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
     int up_a = 0, up_l = 0;
     if (angle != 90 && angle != 180) {
       // edge_len 16 < 24: no corner filter for 8x8.
-      filter_edge<kEdgeCap8>(A, bw + 1 + (angle < 90 ? bh : 0), edge_strength(bw, bh, ft, angle - 90));
-      filter_edge<kEdgeCap8>(L, bh + 1 + (angle > 180 ? bw : 0), edge_strength(bh, bw, ft, angle - 180));
+      filter_edge(A, bw + 1 + (angle < 90 ? bh : 0), edge_strength(bw, bh, ft, angle - 90), tmp);
+      filter_edge(L, bh + 1 + (angle > 180 ? bw : 0), edge_strength(bh, bw, ft, angle - 180), tmp);
       const int da = abs(angle - 90), dl = abs(angle - 180);
       const int lim = ft ? 8 : 16;
       up_a = (da != 0 && da < 40 && bw + bh <= lim);
       up_l = (dl != 0 && dl < 40 && bw + bh <= lim);
       const int32_t maxv = (1 << bd) - 1;
-      if (up_a) upsample_edge<kEdgeCap8>(A, bw + (angle < 90 ? bh : 0), maxv);
-      if (up_l) upsample_edge<kEdgeCap8>(L, bh + (angle > 180 ? bw : 0), maxv);
+      if (up_a) upsample_edge(A, bw + (angle < 90 ? bh : 0), maxv, tmp);
+      if (up_l) upsample_edge(L, bh + (angle > 180 ? bw : 0), maxv, tmp);
     }
     const int32_t* a = A + kEdgeOrigin;  // logical index 0
     const int32_t* l = L + kEdgeOrigin;

@@ -54,11 +54,16 @@ __device__ __forceinline__ bool noalloc_candidate(const mt_block8& bk, const mt_
 
 __device__ __forceinline__ void noalloc_tables(const mt_coef_costs* __restrict__ costs,
                                                const uint8_t* __restrict__ qm_row, int has_qm, mt_coef_costs& sC,
-                                               uint8_t* sQm) {
+                                               uint8_t* sQm, float* sQs, float* sLut) {
   const float* g = reinterpret_cast<const float*>(costs);
   float* s = reinterpret_cast<float*>(&sC);
   for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
-  if (threadIdx.x < 64) sQm[threadIdx.x] = has_qm ? qm_row[threadIdx.x] : 32;
+  if (threadIdx.x < 64) {
+    const int w = has_qm ? qm_row[threadIdx.x] : 32;
+    sQm[threadIdx.x] = (uint8_t)w;
+    sQs[threadIdx.x] = mtd::fwd_qm_scale(w);
+    sLut[threadIdx.x] = mtd::kCoefRateLut[threadIdx.x];
+  }
   __syncthreads();
 }
 
@@ -70,16 +75,19 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_keys_kernel(
     int nblocks, const mt_combo* __restrict__ combos, int ncombos, unsigned long long* __restrict__ keys) {
   __shared__ mt_coef_costs sC;
   __shared__ uint8_t sQm[64];
-  noalloc_tables(costs, qm_row, a.has_qm, sC, sQm);
+  __shared__ float sQs[64];
+  __shared__ float sLut[64];
+  noalloc_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
   if (c >= ncombos) return;
   mt_candidate cd;
   noalloc_candidate(blocks[b], combos[c], cd);
   if (!mtd::cand_ok(cd, a.p.frame_w, a.p.frame_h)) return;
-  mtd::Work8 w;
+  int32_t store[mtd::kWork8Words];
+  mtd::Work8 w{store};
   mt_candidate_result r;
-  mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+  mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   atomicMin(&keys[b], ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c);
 }
 
@@ -91,7 +99,9 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_winner_kernel(
     mt_block_best* __restrict__ best) {
   __shared__ mt_coef_costs sC;
   __shared__ uint8_t sQm[64];
-  noalloc_tables(costs, qm_row, a.has_qm, sC, sQm);
+  __shared__ float sQs[64];
+  __shared__ float sLut[64];
+  noalloc_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nblocks) return;
   const unsigned long long k = keys[b];
@@ -103,9 +113,10 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_winner_kernel(
     const int c = (int)(k & 0xffffffffu);
     mt_candidate cd;
     noalloc_candidate(blocks[b], combos[c], cd);
-    mtd::Work8 w;
+    int32_t store[mtd::kWork8Words];
+  mtd::Work8 w{store};
     mt_candidate_result r;
-    mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sC, cd, r, w);
+    mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
     o.combo = c;
     o.cost = r.cost;
     o.distortion = r.distortion;

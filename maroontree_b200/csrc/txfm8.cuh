@@ -13,6 +13,19 @@
 
 namespace mtd {
 
+// Unroll depth of the 8-iteration row/column loops of the 8x8 transforms and
+// of the 64-element sweeps.  Rolled loops keep one candidate's path small
+// enough for the instruction caches, which measured faster than
+// straight-line code (the kernel is bound by instruction fetch otherwise).
+#ifndef MT_TX_UNROLL
+#define MT_TX_UNROLL 1
+#endif
+#ifndef MT_VEC_UNROLL
+#define MT_VEC_UNROLL 8
+#endif
+constexpr int kTxUnroll = MT_TX_UNROLL;
+constexpr int kVecUnroll = MT_VEC_UNROLL;
+
 // Q16 butterfly multiply with rounding (src/dct.rs:60-67).
 __device__ __forceinline__ int32_t mul_q16(int32_t d, int32_t c) {
   return (int32_t)(((int64_t)d * (int64_t)c + 32768) >> 16);
@@ -63,14 +76,18 @@ __constant__ int16_t kAdst8Fwd[64] = {
     -1681, -5764, -569, 5542,  2732,  -4479, 4479,  2732,  -5542, -569,  5764,  -1681, -5108,
     3675,  5109,  -569, -4479, 5544,  -1682, -3675, 5766,  -2732, 5545,  -3675, 569,   2732,
     -5109, 5766,  -4480, 1682, 5766,  -5544, 5109,  -4477, 3675,  -2730, 1682,  -567};
+// The reference accumulates in i64.  For residuals of 8-bit samples
+// (|r| <= 255) no partial sum of either pass leaves +-2^31 (row sums of |A|
+// are <= 29550, column outputs <= ~6.2k), so the i32 accumulation here is the
+// same value.
 __device__ __forceinline__ void fadst8(int32_t* v) {
   int32_t o[8];
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    int64_t acc = 0;
+    int32_t acc = 2048;
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc += (int64_t)kAdst8Fwd[i * 8 + j] * (int64_t)v[j];
-    o[i] = (int32_t)((acc + 2048) >> 12);
+    for (int j = 0; j < 8; j++) acc += (int32_t)kAdst8Fwd[i * 8 + j] * v[j];
+    o[i] = acc >> 12;
   }
 #pragma unroll
   for (int i = 0; i < 8; i++) v[i] = o[i];
@@ -160,7 +177,7 @@ __device__ __forceinline__ int row_kind(int tx) {
 // is applied by the caller.
 template <typename I, typename C>
 __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* __restrict__ cf,
-                       float* __restrict__ tf) {
+                       float* __restrict__ tf, int32_t* __restrict__ t) {
   if (tx == MT_TX_IDTX) {
 #pragma unroll 8
     for (int i = 0; i < 64; i++) {
@@ -174,13 +191,12 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
     }
     return;
   }
-  int32_t t[64];
-#pragma unroll
+#pragma unroll kVecUnroll
   for (int i = 0; i < 64; i++) t[i] = in[i];
   if (tx == MT_TX_V_DCT || tx == MT_TX_H_DCT) {
     const bool vert = tx == MT_TX_V_DCT;
     if (vert) {
-#pragma unroll
+#pragma unroll kTxUnroll
       for (int x = 0; x < 8; x++) {
         int32_t v[8];
 #pragma unroll
@@ -190,7 +206,7 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
         for (int y = 0; y < 8; y++) t[y * 8 + x] = v[y] * 2;
       }
     } else {
-#pragma unroll
+#pragma unroll kTxUnroll
       for (int y = 0; y < 8; y++) {
         fdct8(t + y * 8);
 #pragma unroll
@@ -199,7 +215,7 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
     }
 #pragma unroll
     for (int y = 0; y < 8; y++)
-#pragma unroll
+#pragma unroll kTxUnroll
       for (int x = 0; x < 8; x++) {
         const int rc = y + x * 8;
         int32_t lv;
@@ -209,7 +225,7 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
     return;
   }
   const int ck = col_kind(tx), rk = row_kind(tx);
-#pragma unroll
+#pragma unroll kTxUnroll
   for (int x = 0; x < 8; x++) {
     int32_t v[8];
 #pragma unroll
@@ -218,7 +234,7 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
 #pragma unroll
     for (int r = 0; r < 8; r++) t[r * 8 + x] = v[r];
   }
-#pragma unroll
+#pragma unroll kTxUnroll
   for (int r = 0; r < 8; r++) {
     int32_t* v = t + r * 8;
     if (rk == 1) fdct8(v); else fadst8(v);
@@ -235,12 +251,15 @@ __device__ void fwd8x8(const I* __restrict__ in, int tx, const mt_quant& q, C* _
 // Forward QM scale (1024 + w/2)/w / 32 (src/dct.rs:93-104) and the AVX2
 // re-quantisation of the pinned x86 build (src/avx/qmatrix.rs:34-71): scale the
 // target, round half away from zero by truncate + fraction test.
+// Forward QM scale of an inverse weight w (src/dct.rs:93-104); exact in f32.
+__device__ __forceinline__ float fwd_qm_scale(int w) { return __fmul_rn((float)((1024 + w / 2) / w), 1.0f / 32.0f); }
+
+// `scale` holds fwd_qm_scale of each position's inverse weight.
 template <typename C>
-__device__ __forceinline__ void apply_qm(C* cf, float* tf, const uint8_t* iw, int n) {
+__device__ __forceinline__ void apply_qm(C* cf, float* tf, const float* scale, int n) {
+#pragma unroll 8
   for (int i = 0; i < n; i++) {
-    const int w = iw[i];
-    const float scale = __fdiv_rn((float)((1024 + w / 2) / w), 32.0f);
-    const float x = __fmul_rn(tf[i], scale);
+    const float x = __fmul_rn(tf[i], scale[i]);
     tf[i] = x;
     const float tr = truncf(x);
     const float frac = fabsf(__fsub_rn(x, tr));
@@ -254,44 +273,45 @@ __device__ __forceinline__ void apply_qm(C* cf, float* tf, const uint8_t* iw, in
 // the column clip, column pass, (t+8)>>4.
 template <typename C, typename O>
 __device__ void inv8x8(const C* __restrict__ cf, int tx, const mt_quant& q, const uint8_t* __restrict__ qm,
-                       O* __restrict__ out) {
+                       O* __restrict__ out, int32_t* __restrict__ t) {
   const bool flat = tx == MT_TX_IDTX || tx == MT_TX_V_DCT || tx == MT_TX_H_DCT;
   const uint8_t* w = flat ? nullptr : qm;
-  int32_t t[64];
 #pragma unroll 8
   for (int rc = 0; rc < 64; rc++) {
     const int32_t l = cf[rc];
     const int32_t base = rc == 0 ? q.dc_q : q.ac_q;
     const int32_t step = w ? ((base * (int32_t)w[rc] + 16) >> 5) : base;
-    int32_t mag = (int32_t)(((uint64_t)uabs(l) * (uint64_t)(uint32_t)step) & 0xffffffull);
+    // Low 24 bits of |l| * step: the 32-bit product has the same low 24 bits
+    // as the reference's 64-bit one.
+    int32_t mag = (int32_t)((uabs(l) * (uint32_t)step) & 0xffffffu);
     mag = min(mag, q.cf_max + (l < 0 ? 1 : 0));
     const int y = rc & 7, x = rc >> 3;
     t[y * 8 + x] = l == 0 ? 0 : (l < 0 ? -mag : mag);
   }
   const int ck = col_kind(tx), rk = row_kind(tx);
   if (rk == 0) {
-#pragma unroll
+#pragma unroll kVecUnroll
     for (int i = 0; i < 64; i++) t[i] *= 2;
   } else {
-#pragma unroll
+#pragma unroll kTxUnroll
     for (int y = 0; y < 8; y++) {
       if (rk == 1) idct8s(t + y * 8, 1, q.rmin, q.rmax);
       else iadst8s(t + y * 8, 1, q.rmin, q.rmax);
     }
   }
-#pragma unroll
+#pragma unroll kVecUnroll
   for (int i = 0; i < 64; i++) t[i] = clampi((t[i] + 1) >> 1, q.cmin, q.cmax);
   if (ck == 0) {
-#pragma unroll
+#pragma unroll kVecUnroll
     for (int i = 0; i < 64; i++) t[i] *= 2;
   } else {
-#pragma unroll
+#pragma unroll kTxUnroll
     for (int x = 0; x < 8; x++) {
       if (ck == 1) idct8s(t + x, 8, q.cmin, q.cmax);
       else iadst8s(t + x, 8, q.cmin, q.cmax);
     }
   }
-#pragma unroll
+#pragma unroll kVecUnroll
   for (int i = 0; i < 64; i++) out[i] = (O)((t[i] + 8) >> 4);
 }
 
