@@ -29,6 +29,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 W, H, QIDX, QM_LEVEL = 1920, 1080, 70, 6
+# From one ncu capture of level8_kernel on this workload
+# (ncu --set full -k regex:level8_kernel ... python bench.py --steps 1 --warmup 3 --no-cpu):
+NCU_DRAM_BYTES_PER_LAUNCH = 52_023_040 + 781_145_856  # dram__bytes_read.sum + dram__bytes_write.sum
+NCU_WARP_INSTS_PER_LAUNCH = 1_298_978_611  # smsp__inst_executed.sum
+ISSUE_PEAK_PER_CLK = 148 * 4  # SMs x schedulers, one warp-instruction each per clock
 MODES = list(range(13))
 MPIX = W * H / 1e6
 
@@ -232,6 +237,9 @@ def run_ours(args):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    clk_mhz = peaks.get("sm_max_mhz", 1965.0)
+    issue_peak = ISSUE_PEAK_PER_CLK * clk_mhz * 1e6
+    issue_rate = NCU_WARP_INSTS_PER_LAUNCH / (step_ms / 1e3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -254,8 +262,12 @@ def run_ours(args):
         "e2e": {"value": round(world * MPIX / e2e_s, 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 5), "traffic": None,
-                     "kernel": "level8_kernel", "alg_bytes_per_launch": alg_bytes},
+                     "frac": round(achieved / hbm_peak, 5), "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
+                     "kernel": "level8_kernel", "alg_bytes_per_launch": alg_bytes,
+                     "note": "integer/FP32 issue-bound kernel; see issue_roofline"},
+        "issue_roofline": {"achieved_ginst_s": round(issue_rate / 1e9, 1),
+                           "peak_ginst_s": round(issue_peak / 1e9, 1), "frac": round(issue_rate / issue_peak, 4),
+                           "inst_per_launch": NCU_WARP_INSTS_PER_LAUNCH, "sm_clock_mhz": clk_mhz},
         "gpu_launches": 2 * args.steps,  # level8_kernel + level8_finalize_kernel per step
         "clocks": clk.summary(),
         "cpu_baseline": cpu,

@@ -283,6 +283,34 @@ int mt_intra_predict_device(const uint16_t* d_recon, const mt_chain_params* prm,
                             const mt_candidate* d_cands, int32_t n, int32_t* d_pred_out,
                             void* stream);
 
+/* Colour conversion + padding (src/encoder.rs:113-127, :370-410, :532-604
+ * and src/dispatch.rs:113-131): interleaved 8-bit RGB (w x h x 3) -> the
+ * coder's padded u16 planes.  sub = 0 (4:4:4) or 2 (4:2:0).  Padded sizes from
+ * mt_padded_plane_dims: luma align8(w) x align8(h), chroma that >> sub. */
+int mt_padded_plane_dims(int32_t w, int32_t h, int32_t sub, int32_t* pw, int32_t* ph, int32_t* pcw,
+                         int32_t* pch);
+int mt_csc_rgb8(const uint8_t* rgb, int32_t w, int32_t h, int32_t sub, uint16_t* y, uint16_t* cb,
+                uint16_t* cr);
+int mt_csc_rgb8_device(const uint8_t* d_rgb, int32_t w, int32_t h, int32_t sub, uint16_t* d_y,
+                       uint16_t* d_cb, uint16_t* d_cr, void* stream);
+
+/* Deblocking of one plane (src/loopfilter.rs:482-648 filter_plane_impl, with
+ * the dav1d loop filter of src/loopfilter.rs:98-292), as src/coder/frame_deblock.rs
+ * drives it per plane.  px: the padded plane (w x h u16, w and h multiples of 4),
+ * filtered in place; only edges inside the visible vis_w x vis_h window are
+ * filtered.  bw4 / bh4: block width / height in 4-sample units per 4x4 cell
+ * (row-major, nc4 cells per row, ceil(vis_h/4) rows; entries >= 1).  vedge4 /
+ * hedge4: 1 where a block starts at that cell column / row, or NULL for the
+ * alignment rule (col % bw4 == 0, row % bh4 == 0).  level 0..63 (0 = no
+ * filtering), sharp 0..7, is_luma selects the 4/8/16 (luma) or 4/6 (chroma)
+ * widths.  bd must be 8. */
+int mt_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,
+                     const uint8_t* bh4, const uint8_t* vedge4, const uint8_t* hedge4, int32_t nc4, int32_t level,
+                     int32_t sharp, int32_t is_luma, int32_t bd);
+int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* d_bw4,
+                            const uint8_t* d_bh4, const uint8_t* d_vedge4, const uint8_t* d_hedge4, int32_t nc4,
+                            int32_t level, int32_t sharp, int32_t is_luma, int32_t bd, void* stream);
+
 /* Library version string. */
 const char* mt_version(void);
 

@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "MtError",
 ]
 
 
@@ -127,3 +127,49 @@ def rdo_level8_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_blocks, nbloc
     _check(load().mt_rdo_level8_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
                                        ptr(d_costs), ptr(d_blocks), nblocks, ptr(d_combos), ncombos, ptr(d_best),
                                        ptr(d_results), ptr(d_keys), stream or None), "mt_rdo_level8_device")
+
+
+def padded_plane_dims(w, h, sub):
+    v = [C.c_int32() for _ in range(4)]
+    _check(load().mt_padded_plane_dims(w, h, sub, *[C.byref(x) for x in v]), "mt_padded_plane_dims")
+    return tuple(x.value for x in v)
+
+
+def csc_rgb8(rgb, sub):
+    """Interleaved u8 RGB (h, w, 3) -> padded (Y, Cb, Cr) u16 planes; sub 0 = 4:4:4, 2 = 4:2:0."""
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    h, w = rgb.shape[:2]
+    pw, ph, pcw, pch = padded_plane_dims(w, h, sub)
+    y = np.zeros((ph, pw), np.uint16)
+    cb = np.zeros((pch, pcw), np.uint16)
+    cr = np.zeros((pch, pcw), np.uint16)
+    _check(load().mt_csc_rgb8(ptr(rgb), w, h, sub, ptr(y), ptr(cb), ptr(cr)), "mt_csc_rgb8")
+    return y, cb, cr
+
+
+def _u8_map(m, nr4, nc4):
+    if m is None:
+        return None
+    m = np.asarray(m)
+    if m.ndim != 2 or m.shape[0] < nr4 or m.shape[1] != nc4:
+        raise ValueError(f"block map shape {m.shape}: need at least {nr4} rows of {nc4} cells")
+    return np.ascontiguousarray(m[:nr4], np.uint8)
+
+
+def deblock_plane(px, vis_w, vis_h, bw4, bh4, level, sharp, is_luma, vedge4=None, hedge4=None, bd=8):
+    """``filter_plane`` (src/loopfilter.rs:482-648) on a copy of ``px``.
+
+    px: (h, w) u16 padded plane; bw4 / bh4: (>= ceil(vis_h/4), nc4) u8 block
+    width / height maps in 4-sample units; vedge4 / hedge4: optional block
+    start flags (None = alignment rule).  Returns the filtered plane."""
+    out = np.array(px, dtype=np.uint16, copy=True, order="C")
+    h, w = out.shape
+    nr4 = (vis_h + 3) // 4
+    nc4 = np.asarray(bw4).shape[-1]
+    bw4 = _u8_map(bw4, nr4, nc4)
+    bh4 = _u8_map(bh4, nr4, nc4)
+    ve = _u8_map(vedge4, nr4, nc4)
+    he = _u8_map(hedge4, nr4, nc4)
+    _check(load().mt_deblock_plane(ptr(out), w, h, vis_w, vis_h, ptr(bw4), ptr(bh4), ptr(ve), ptr(he), nc4, level,
+                                   sharp, int(bool(is_luma)), bd), "mt_deblock_plane")
+    return out

@@ -112,6 +112,13 @@ def _bind(lib):
                                            _P, C.c_int32, _P, _P, _P, _P]),
         "mt_rdo_level8_device_noalloc": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
                                                    C.c_int32, _P, C.c_int32, _P, _P]),
+        "mt_padded_plane_dims": (C.c_int, [C.c_int32, C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
+        "mt_csc_rgb8": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
+        "mt_csc_rgb8_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P]),
+        "mt_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "mt_deblock_plane_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
+                                              C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -141,6 +148,7 @@ EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
+    "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
 )
 

@@ -1,0 +1,343 @@
+// Deblocking of one plane (src/loopfilter.rs:98-648, the dav1d loop-filter
+// port driven per superblock row).
+//
+// Order.  The reference walks superblock rows top to bottom; in each it filters
+// every vertical edge (per row of samples, left to right), then every
+// horizontal edge (per column, top to bottom).  A line of samples across a
+// vertical edge only touches its own row, and one across a horizontal edge
+// only its own column, so the reference's result is fixed by two orders: along
+// each row, vertical edges left to right; along each column, horizontal edges
+// top to bottom -- plus the interleaving of the two directions per superblock
+// row.  A horizontal edge reaches at most 6 rows below itself (the 16-wide
+// luma filter), so only a 16-wide horizontal edge on the last 4-row of a
+// superblock row reaches the next superblock row, whose vertical edges the
+// reference filters after it.  No AV1 block geometry puts one there (a block
+// >= 16 rows high starts on a multiple of 16 rows); without one, two
+// frame-wide passes -- all vertical edges, then all horizontal edges -- give
+// the reference's samples.  mt_deblock_plane rejects maps that have one.
+//
+// Parallelism.  One thread filters one line across one edge.  Two edges of one
+// direction whose taps overlap (possible only with edge maps that do not
+// follow the block sizes: AV1 geometry keeps the taps of neighbouring edges
+// apart, 1+2 < 4, 3+4 < 8, 6+7 < 16 samples) must run in the reference's order:
+// such edges form runs of consecutive overlapping edges, and the thread of a
+// run's first edge filters the whole run in order while the others return.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/maroontree_b200.h"
+
+namespace {
+
+struct LfLimits {
+  int e, i, h;
+};
+
+__host__ __device__ inline LfLimits lf_limits(int level, int sharp) {
+  int i = level;
+  if (sharp > 0) {
+    i >>= (sharp + 3) >> 2;
+    i = i < 9 - sharp ? i : 9 - sharp;
+  }
+  i = i > 1 ? i : 1;
+  return {2 * (level + 2) + i, i, level >> 4};
+}
+
+__device__ __forceinline__ int clip3(int v, int lo, int hi) { return max(lo, min(v, hi)); }
+
+// One line of the filter across an edge at dst[0] (samples dst[k * sb]).
+__device__ __forceinline__ void lf_line(uint16_t* __restrict__ dst, long sb, const LfLimits L, int wd, int bd) {
+  const int bm8 = bd - 8;
+  const int f_flat = 1 << bm8;
+  const int e = L.e << bm8, il = L.i << bm8, ht = L.h << bm8;
+  const int px_max = (1 << bd) - 1;
+  const int clip_lo = -128 * (1 << bm8), clip_hi = 128 * (1 << bm8) - 1;
+  auto g = [&](int k) -> int { return dst[k * sb]; };
+  auto put = [&](int k, int v) { dst[k * sb] = (uint16_t)v; };
+  const int p1 = g(-2), p0 = g(-1), q0 = g(0), q1 = g(1);
+  bool fm = abs(p1 - p0) <= il && abs(q1 - q0) <= il && abs(p0 - q0) * 2 + (abs(p1 - q1) >> 1) <= e;
+  int p2 = 0, q2 = 0, p3 = 0, q3 = 0;
+  if (wd > 4) {
+    p2 = g(-3);
+    q2 = g(2);
+    fm = fm && abs(p2 - p1) <= il && abs(q2 - q1) <= il;
+    if (wd > 6) {
+      p3 = g(-4);
+      q3 = g(3);
+      fm = fm && abs(p3 - p2) <= il && abs(q3 - q2) <= il;
+    }
+  }
+  if (!fm) return;
+  bool flat8in = false;
+  if (wd >= 6)
+    flat8in = abs(p2 - p0) <= f_flat && abs(p1 - p0) <= f_flat && abs(q1 - q0) <= f_flat && abs(q2 - q0) <= f_flat;
+  if (wd >= 8) flat8in = flat8in && abs(p3 - p0) <= f_flat && abs(q3 - q0) <= f_flat;
+  if (wd >= 16 && flat8in) {
+    const int p6 = g(-7), p5 = g(-6), p4 = g(-5), q4 = g(4), q5 = g(5), q6 = g(6);
+    const bool flat8out = abs(p6 - p0) <= f_flat && abs(p5 - p0) <= f_flat && abs(p4 - p0) <= f_flat &&
+                          abs(q4 - q0) <= f_flat && abs(q5 - q0) <= f_flat && abs(q6 - q0) <= f_flat;
+    if (flat8out) {
+      put(-6, (p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8) >> 4);
+      put(-5, (p6 * 5 + p5 * 2 + p4 * 2 + p3 * 2 + p2 + p1 + p0 + q0 + q1 + 8) >> 4);
+      put(-4, (p6 * 4 + p5 + p4 * 2 + p3 * 2 + p2 * 2 + p1 + p0 + q0 + q1 + q2 + 8) >> 4);
+      put(-3, (p6 * 3 + p5 + p4 + p3 * 2 + p2 * 2 + p1 * 2 + p0 + q0 + q1 + q2 + q3 + 8) >> 4);
+      put(-2, (p6 * 2 + p5 + p4 + p3 + p2 * 2 + p1 * 2 + p0 * 2 + q0 + q1 + q2 + q3 + q4 + 8) >> 4);
+      put(-1, (p6 + p5 + p4 + p3 + p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + q2 + q3 + q4 + q5 + 8) >> 4);
+      put(0, (p5 + p4 + p3 + p2 + p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + q3 + q4 + q5 + q6 + 8) >> 4);
+      put(1, (p4 + p3 + p2 + p1 + p0 + q0 * 2 + q1 * 2 + q2 * 2 + q3 + q4 + q5 + q6 + q6 + 8) >> 4);
+      put(2, (p3 + p2 + p1 + p0 + q0 + q1 * 2 + q2 * 2 + q3 * 2 + q4 + q5 + q6 + q6 + q6 + 8) >> 4);
+      put(3, (p2 + p1 + p0 + q0 + q1 + q2 * 2 + q3 * 2 + q4 * 2 + q5 + q6 + q6 + q6 + q6 + 8) >> 4);
+      put(4, (p1 + p0 + q0 + q1 + q2 + q3 * 2 + q4 * 2 + q5 * 2 + q6 * 5 + 8) >> 4);
+      put(5, (p0 + q0 + q1 + q2 + q3 + q4 * 2 + q5 * 2 + q6 * 7 + 8) >> 4);
+      return;
+    }
+  }
+  if (wd >= 8 && flat8in) {
+    put(-3, (p3 * 3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3);
+    put(-2, (p3 * 2 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3);
+    put(-1, (p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3);
+    put(0, (p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3);
+    put(1, (p1 + p0 + q0 + 2 * q1 + q2 + q3 + q3 + 4) >> 3);
+    put(2, (p0 + q0 + q1 + 2 * q2 + q3 + q3 + q3 + 4) >> 3);
+  } else if (wd == 6 && flat8in) {
+    put(-2, (p2 * 3 + 2 * p1 + 2 * p0 + q0 + 4) >> 3);
+    put(-1, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
+    put(0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3);
+    put(1, (p0 + 2 * q0 + 2 * q1 + 2 * q2 + q2 + 4) >> 3);
+  } else {
+    const bool hev = abs(p1 - p0) > ht || abs(q1 - q0) > ht;
+    int fv = hev ? clip3(p1 - q1, clip_lo, clip_hi) : 0;
+    fv = clip3(3 * (q0 - p0) + fv, clip_lo, clip_hi);
+    const int f1 = min(fv + 4, clip_hi) >> 3;
+    const int f2 = min(fv + 3, clip_hi) >> 3;
+    put(-1, clip3(p0 + f2, 0, px_max));
+    put(0, clip3(q0 - f1, 0, px_max));
+    if (!hev) {
+      const int f = (f1 + 1) >> 1;
+      put(-2, clip3(p1 + f, 0, px_max));
+      put(1, clip3(q1 - f, 0, px_max));
+    }
+  }
+}
+
+// Filter width class of a block dimension in 4-sample units
+// (src/loopfilter.rs:396-412): luma 4/8/16, chroma 4/6.
+__host__ __device__ __forceinline__ int lf_cls(int d, bool luma) {
+  return luma ? (d == 1 ? 0 : (d == 2 ? 1 : 2)) : (d >= 2);
+}
+__host__ __device__ __forceinline__ int lf_wd(int wcls, bool luma) { return luma ? 4 << wcls : 4 + 2 * wcls; }
+// Samples a filter of width wd reads before / after the edge (it writes fewer).
+__host__ __device__ __forceinline__ int lf_reach_lo(int wd) {
+  return wd == 16 ? 7 : (wd == 8 ? 4 : (wd == 6 ? 3 : 2));
+}
+__host__ __device__ __forceinline__ int lf_reach_hi(int wd) {
+  return wd == 16 ? 6 : (wd == 8 ? 3 : (wd == 6 ? 2 : 1));
+}
+
+// The edges of one row of cells (vertical edges, i = 4x4 column) or one
+// column of cells (horizontal edges, i = 4x4 row): cell i sits at
+// map[base + i * step], the block before the edge at map[base + (i-1) * step].
+struct EdgeLine {
+  const uint8_t* dim;   // block extent across the edge, in 4-sample units
+  const uint8_t* flag;  // block-start flags, or null for the alignment rule
+  long base, step;
+  int n4;               // cells along the line inside the visible window
+  int len;              // samples along the line in the padded plane
+  bool luma;
+};
+
+// Filter width of the edge at cell i, 0 where none is filtered: outside
+// 1..n4-1, no block start there, or taps that would leave the row / plane (the
+// reference indexes outside its row there; no AV1 geometry reaches it).
+__host__ __device__ __forceinline__ int edge_wd(const EdgeLine& e, int i) {
+  if (i < 1 || i >= e.n4) return 0;
+  const long idx = e.base + (long)i * e.step;
+  const int cur = e.dim[idx];
+  if (cur == 0) return 0;
+  const bool present = e.flag ? e.flag[idx] != 0 : (i % cur == 0);
+  if (!present) return 0;
+  const int prev = e.dim[idx - e.step];
+  const int a = lf_cls(cur, e.luma), b = lf_cls(prev, e.luma);
+  const int wd = lf_wd(a < b ? a : b, e.luma);
+  if (4 * i - lf_reach_lo(wd) < 0 || 4 * i + lf_reach_hi(wd) >= e.len) return 0;
+  return wd;
+}
+
+// Do the taps of edges i < k (widths wi, wk) share a sample?
+__host__ __device__ __forceinline__ bool taps_overlap(int i, int wi, int k, int wk) {
+  return 4 * i + lf_reach_hi(wi) >= 4 * k - lf_reach_lo(wk);
+}
+
+// Window of edge widths for cells i-6 .. i+3 (taps reach at most 3 cells).
+struct EdgeWindow {
+  int wd[10];
+  __device__ __forceinline__ int at(int d) const { return wd[d + 6]; }  // d in -6..3
+};
+
+// Does the edge at offset d (-3..0) of the window overlap a neighbour within 3 cells?
+__device__ __forceinline__ bool window_involved(const EdgeWindow& w, int i, int d) {
+  const int wd = w.at(d);
+  for (int k = d - 3; k <= d + 3; k++) {
+    if (k == d || k < -6 || k > 3) continue;
+    const int wk = w.at(k);
+    if (!wk) continue;
+    if (k < d ? taps_overlap(i + k, wk, i + d, wd) : taps_overlap(i + d, wd, i + k, wk)) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ bool involved_at(const EdgeLine& e, int i, int wd) {
+  for (int k = i - 3; k <= i + 3; k++) {
+    if (k == i) continue;
+    const int wk = edge_wd(e, k);
+    if (!wk) continue;
+    if (k < i ? taps_overlap(k, wk, i, wd) : taps_overlap(i, wd, k, wk)) return true;
+  }
+  return false;
+}
+
+// Filters the line across edge i of e (and, when i heads a run of
+// overlapping edges, the rest of the run in order).  line0 points at the
+// line's sample at along-position 0; stride is the along-line sample stride.
+__device__ __forceinline__ void filter_edge_line(const EdgeLine& e, int i, uint16_t* __restrict__ line0, long stride,
+                                                 const LfLimits L, int bd) {
+  EdgeWindow w;
+#pragma unroll
+  for (int d = -6; d <= 3; d++) w.wd[d + 6] = edge_wd(e, i + d);
+  const int wd = w.at(0);
+  if (!wd) return;
+  if (!window_involved(w, i, 0)) {
+    lf_line(line0 + (long)4 * i * stride, stride, L, wd, bd);
+    return;
+  }
+  // Part of a run: only the run's first edge proceeds.
+  for (int d = -1; d >= -3; d--) {
+    if (w.at(d)) {
+      if (window_involved(w, i, d)) return;
+      break;
+    }
+  }
+  int cur = i, cw = wd;
+  while (true) {
+    lf_line(line0 + (long)4 * cur * stride, stride, L, cw, bd);
+    int nxt = 0, nw = 0;
+    for (int k = cur + 1; k <= cur + 3; k++) {
+      const int wk = edge_wd(e, k);
+      if (wk) {
+        nxt = k;
+        nw = wk;
+        break;
+      }
+    }
+    if (!nw || !involved_at(e, nxt, nw)) return;
+    cur = nxt;
+    cw = nw;
+  }
+}
+
+struct PlaneArgs {
+  int w, h, w4, h4, nc4, bd, luma;
+  LfLimits L;
+};
+
+// Vertical edges: thread (sample row y, edge column c4).
+__global__ void lf_vert_kernel(uint16_t* __restrict__ px, PlaneArgs a, const uint8_t* __restrict__ bw4,
+                               const uint8_t* __restrict__ vedge4) {
+  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  if (c4 >= a.w4) return;
+  const EdgeLine e{bw4, vedge4, (long)(y >> 2) * a.nc4, 1, a.w4, a.w, a.luma != 0};
+  filter_edge_line(e, c4, px + (size_t)y * a.w, 1, a.L, a.bd);
+}
+
+// Horizontal edges: thread (sample column x, edge row r4).
+__global__ void lf_horz_kernel(uint16_t* __restrict__ px, PlaneArgs a, const uint8_t* __restrict__ bh4,
+                               const uint8_t* __restrict__ hedge4) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r4 = blockIdx.y;
+  if (x >= a.w4 * 4) return;
+  const EdgeLine e{bh4, hedge4, (long)(x >> 2), a.nc4, a.h4, a.h, a.luma != 0};
+  filter_edge_line(e, r4, px + x, a.w, a.L, a.bd);
+}
+
+int check_plane(int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, int32_t nc4, int32_t level, int32_t sharp,
+                int32_t bd) {
+  if (w <= 0 || h <= 0 || (w & 3) || (h & 3)) return MT_ERR_INVALID_INPUT;
+  if (vis_w <= 0 || vis_h <= 0 || vis_w > w || vis_h > h) return MT_ERR_INVALID_INPUT;
+  if (nc4 < (vis_w + 3) / 4 || level < 0 || level > 63 || sharp < 0 || sharp > 7) return MT_ERR_INVALID_INPUT;
+  if (bd != 8) return MT_ERR_UNSUPPORTED;
+  return MT_OK;
+}
+
+// A 16-wide horizontal edge on the last 4-row of a 64-row superblock row
+// (the only edge the two-pass order would filter out of the reference's order).
+bool has_superblock_crossing(int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bh4,
+                             const uint8_t* hedge4, int32_t nc4) {
+  const int w4 = (vis_w + 3) / 4, h4 = (vis_h + 3) / 4;
+  (void)w;
+  for (int t = 16; t < h4; t += 16)
+    for (int c4 = 0; c4 < w4; c4++) {
+      const EdgeLine e{bh4, hedge4, (long)c4, nc4, h4, h, true};
+      if (edge_wd(e, t - 1) == 16) return true;
+    }
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* d_bw4,
+                            const uint8_t* d_bh4, const uint8_t* d_vedge4, const uint8_t* d_hedge4, int32_t nc4,
+                            int32_t level, int32_t sharp, int32_t is_luma, int32_t bd, void* stream) {
+  int rc = check_plane(w, h, vis_w, vis_h, nc4, level, sharp, bd);
+  if (rc != MT_OK) return rc;
+  if (level == 0) return MT_OK;
+  if (!d_px || !d_bw4 || !d_bh4) return MT_ERR_INVALID_INPUT;
+  PlaneArgs a;
+  a.w = w;
+  a.h = h;
+  a.w4 = (vis_w + 3) / 4;
+  a.h4 = (vis_h + 3) / 4;
+  a.nc4 = nc4;
+  a.bd = bd;
+  a.luma = is_luma;
+  a.L = lf_limits(level, sharp);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int T = 128;
+  if (a.w4 > 1) lf_vert_kernel<<<dim3((a.w4 + T - 1) / T, a.h4 * 4), T, 0, st>>>(d_px, a, d_bw4, d_vedge4);
+  if (a.h4 > 1) lf_horz_kernel<<<dim3((a.w4 * 4 + T - 1) / T, a.h4), T, 0, st>>>(d_px, a, d_bh4, d_hedge4);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,
+                     const uint8_t* bh4, const uint8_t* vedge4, const uint8_t* hedge4, int32_t nc4, int32_t level,
+                     int32_t sharp, int32_t is_luma, int32_t bd) {
+  int rc = check_plane(w, h, vis_w, vis_h, nc4, level, sharp, bd);
+  if (rc != MT_OK) return rc;
+  if (level == 0) return MT_OK;
+  if (!px || !bw4 || !bh4) return MT_ERR_INVALID_INPUT;
+  if (is_luma && has_superblock_crossing(w, h, vis_w, vis_h, bh4, hedge4, nc4)) return MT_ERR_UNSUPPORTED;
+  const int nr4 = (vis_h + 3) / 4;
+  const size_t n_px = (size_t)w * h * 2, n_map = (size_t)nr4 * nc4;
+  const size_t o_bw = (n_px + 255) & ~(size_t)255, o_bh = o_bw + ((n_map + 255) & ~(size_t)255);
+  const size_t o_ve = o_bh + ((n_map + 255) & ~(size_t)255), o_he = o_ve + ((n_map + 255) & ~(size_t)255);
+  const size_t total = o_he + n_map;
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  cudaError_t e = cudaMemcpy(d, px, n_px, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_bw, bw4, n_map, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_bh, bh4, n_map, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && vedge4) e = cudaMemcpy(d + o_ve, vedge4, n_map, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && hedge4) e = cudaMemcpy(d + o_he, hedge4, n_map, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = mt_deblock_plane_device((uint16_t*)d, w, h, vis_w, vis_h, d + o_bw, d + o_bh, vedge4 ? d + o_ve : nullptr,
+                                 hedge4 ? d + o_he : nullptr, nc4, level, sharp, is_luma, bd, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(px, d, n_px, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+}  // extern "C"

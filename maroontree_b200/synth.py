@@ -222,3 +222,117 @@ def best_of_level(results, nblocks, ncombos):
     """Per-block argmin of combo-major results with the first-minimum rule."""
     cost = results["cost"].reshape(ncombos, nblocks)
     return np.argmin(cost, axis=0)
+
+
+# ---------------------------------------------------------------------------
+# Block geometry and reconstructions for the in-loop filters.
+
+def partition_maps(nc4, nr4, seed, sb4=16, split_bias=0.55):
+    """Random AV1-shaped block geometry over an nr4 x nc4 grid of 4x4 cells.
+
+    Each sb4 x sb4 superblock is partitioned recursively with the AV1
+    partition types (NONE, SPLIT, HORZ, VERT, HORZ_4, VERT_4 and the 3-way
+    HORZ_A/B, VERT_A/B); blocks are clipped to the grid.  Returns
+    (bw4, bh4, vedge4, hedge4, block_id): u8 block width / height in 4-sample
+    units per cell, u8 flags where a block starts at the cell's column / row,
+    and an int32 block index per cell."""
+    rng = np.random.default_rng(seed)
+    bw4 = np.zeros((nr4, nc4), np.uint8)
+    bh4 = np.zeros((nr4, nc4), np.uint8)
+    ve = np.zeros((nr4, nc4), np.uint8)
+    he = np.zeros((nr4, nc4), np.uint8)
+    bid = np.full((nr4, nc4), -1, np.int32)
+    count = [0]
+
+    def put(r, c, h, w):
+        if r >= nr4 or c >= nc4:
+            return
+        r1, c1 = min(r + h, nr4), min(c + w, nc4)
+        bw4[r:r1, c:c1] = w
+        bh4[r:r1, c:c1] = h
+        ve[r:r1, c] = 1
+        he[r, c:c1] = 1
+        bid[r:r1, c:c1] = count[0]
+        count[0] += 1
+
+    def node(r, c, s):
+        if r >= nr4 or c >= nc4:
+            return
+        kinds = ["none"]
+        if s > 1:
+            kinds += ["split", "horz", "vert", "horz_a", "horz_b", "vert_a", "vert_b"]
+        if s >= 4:
+            kinds += ["horz_4", "vert_4"]
+        if s > 1 and rng.random() < split_bias:
+            kind = "split"
+        else:
+            kind = kinds[int(rng.integers(len(kinds)))]
+        hs = s // 2
+        if kind == "none":
+            put(r, c, s, s)
+        elif kind == "split":
+            for dr in (0, hs):
+                for dc in (0, hs):
+                    node(r + dr, c + dc, hs)
+        elif kind == "horz":
+            put(r, c, hs, s)
+            put(r + hs, c, hs, s)
+        elif kind == "vert":
+            put(r, c, s, hs)
+            put(r, c + hs, s, hs)
+        elif kind == "horz_4":
+            for k in range(4):
+                put(r + k * s // 4, c, s // 4, s)
+        elif kind == "vert_4":
+            for k in range(4):
+                put(r, c + k * s // 4, s, s // 4)
+        elif kind == "horz_a":
+            put(r, c, hs, hs)
+            put(r, c + hs, hs, hs)
+            put(r + hs, c, hs, s)
+        elif kind == "horz_b":
+            put(r, c, hs, s)
+            put(r + hs, c, hs, hs)
+            put(r + hs, c + hs, hs, hs)
+        elif kind == "vert_a":
+            put(r, c, hs, hs)
+            put(r + hs, c, hs, hs)
+            put(r, c + hs, s, hs)
+        else:  # vert_b
+            put(r, c, s, hs)
+            put(r, c + hs, hs, hs)
+            put(r + hs, c + hs, hs, hs)
+
+    for r in range(0, nr4, sb4):
+        for c in range(0, nc4, sb4):
+            node(r, c, sb4)
+    return bw4, bh4, ve, he, bid
+
+
+def blocky_plane(w, h, block_id, seed, maxv=255):
+    """A reconstruction-like plane: per block a flat level, a gentle ramp or
+    texture, with small steps between neighbouring blocks, so that every branch
+    of the loop filter (flat 16 / flat 8 / 6 / narrow with and without high
+    edge variance, and rejected lines) is reached."""
+    rng = np.random.default_rng(seed)
+    nb = int(block_id.max()) + 1
+    base = np.clip(128 + np.cumsum(rng.integers(-6, 7, nb)), 16, maxv - 16)
+    style = rng.integers(0, 5, nb)
+    gx = rng.integers(-2, 3, nb)
+    gy = rng.integers(-2, 3, nb)
+    cell = np.repeat(np.repeat(block_id, 4, axis=0), 4, axis=1)
+    ch, cw = cell.shape
+    full = np.zeros((h, w), np.int64)
+    bidp = np.full((h, w), 0, np.int64)
+    bidp[:min(h, ch), :min(w, cw)] = cell[:min(h, ch), :min(w, cw)]
+    bidp[bidp < 0] = 0
+    yy, xx = np.mgrid[0:h, 0:w]
+    b = bidp
+    v = base[b].astype(np.int64)
+    s = style[b]
+    v = v + np.where(s == 1, rng.integers(-1, 2, (h, w)), 0)
+    v = v + np.where(s == 2, (gx[b] * (xx % 16) + gy[b] * (yy % 16)) // 4, 0)
+    v = v + np.where(s == 3, rng.integers(-12, 13, (h, w)), 0)
+    v = v + np.where(s == 4, rng.integers(-3, 4, (h, w)), 0)
+    full[:] = np.clip(v, 0, maxv)
+    return full.astype(np.uint16)

@@ -60,6 +60,13 @@ int or_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chai
                        const mt_candidate* cands, int32_t n, mt_candidate_result* results,
                        int32_t* levels_out, int32_t* recon_out, int32_t threads);
 
+/* encoder.rs CSC + dispatch.rs padding: interleaved RGB -> padded Y/Cb/Cr
+ * (sub 0 = 4:4:4, 2 = 4:2:0). */
+int or_csc_rgb8(const uint8_t* rgb, int32_t w, int32_t h, int32_t sub, uint16_t* y, uint16_t* cb, uint16_t* cr);
+/* loopfilter.rs filter_plane (scalar path, per superblock row order). */
+int or_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,
+                     const uint8_t* bh4, const uint8_t* vedge4, const uint8_t* hedge4, int32_t nc4, int32_t level,
+                     int32_t sharp, int32_t is_luma, int32_t sb_rows4, int32_t bd);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 

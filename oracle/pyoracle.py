@@ -38,6 +38,9 @@ def load():
                                                C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
             "or_edge_filter_strength": (C.c_int, [C.c_int] * 4),
             "or_use_edge_upsample": (C.c_int, [C.c_int] * 4),
+            "or_csc_rgb8": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
+            "or_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
+                                           C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
             "or_candidate_chain": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), C.POINTER(abi.Quant), _P,
                                              C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
@@ -140,3 +143,28 @@ def candidate_chain(src, recon, prm, q, qm, cdfs, cands, want_levels=False, want
                                    p(res), p(lv), p(ro), threads)
     assert rc == 0, rc
     return res, lv, ro
+
+
+def csc_rgb8(rgb, sub):
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    h, w = rgb.shape[:2]
+    pw, ph = (w + 7) & ~7, (h + 7) & ~7
+    pcw, pch = (pw >> 1, ph >> 1) if sub == 2 else (pw, ph)
+    y = np.zeros((ph, pw), np.uint16)
+    cb = np.zeros((pch, pcw), np.uint16)
+    cr = np.zeros((pch, pcw), np.uint16)
+    assert load().or_csc_rgb8(p(rgb), w, h, sub, p(y), p(cb), p(cr)) == 0
+    return y, cb, cr
+
+
+def deblock_plane(px, vis_w, vis_h, bw4, bh4, level, sharp, is_luma, vedge4=None, hedge4=None, sb_rows4=16, bd=8):
+    out = np.array(px, dtype=np.uint16, copy=True, order="C")
+    h, w = out.shape
+    bw4 = np.ascontiguousarray(bw4, np.uint8)
+    bh4 = np.ascontiguousarray(bh4, np.uint8)
+    nc4 = bw4.shape[1]
+    ve = None if vedge4 is None else np.ascontiguousarray(vedge4, np.uint8)
+    he = None if hedge4 is None else np.ascontiguousarray(hedge4, np.uint8)
+    assert load().or_deblock_plane(p(out), w, h, vis_w, vis_h, p(bw4), p(bh4), p(ve), p(he), nc4, level, sharp,
+                                   int(bool(is_luma)), sb_rows4, bd) == 0
+    return out

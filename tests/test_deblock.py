@@ -1,0 +1,180 @@
+"""Deblocking filter (src/loopfilter.rs filter_plane, as src/coder/frame_deblock.rs
+drives it per plane): oracle known answers and order properties on the CPU,
+bit-exact GPU parity with the oracle on AV1-shaped block geometry, on the
+reference's own mixed-geometry pattern (edges whose taps overlap), at 1080p,
+and through the device entry point on a stream."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from maroontree_b200 import synth
+
+
+def _geometry(vis_w, vis_h, seed):
+    w, h = (vis_w + 7) & ~7, (vis_h + 7) & ~7
+    bw, bh, ve, he, bid = synth.partition_maps(w // 4, h // 4, seed)
+    return w, h, bw, bh, ve, he, synth.blocky_plane(w, h, bid, seed)
+
+
+def _mixed_geometry():
+    """The edge-map pattern of the reference's batch-coalescing test
+    (src/loopfilter.rs tests): block sizes and edge flags that ignore each
+    other, so neighbouring edges' taps overlap."""
+    W, H = 264, 88
+    nc4, nr4 = W // 4, H // 4
+    r4, c4 = np.mgrid[0:nr4, 0:nc4]
+    sizes = np.array([1, 2, 4, 8], np.uint8)
+    bw = sizes[(r4 + 2 * c4) & 3]
+    bh = sizes[(2 * r4 + c4) & 3]
+    ve = ((c4 >= 2) & (c4 + 2 < nc4) & ((3 * r4 + c4) % 5 <= 2)).astype(np.uint8)
+    he = ((r4 >= 2) & (r4 + 2 < nr4) & ((r4 + 3 * c4) % 5 <= 2)).astype(np.uint8)
+    i = np.arange(W * H)
+    img = ((((i % W) // 8 + (i // W) // 8) & 31) * 4 + 64).astype(np.uint16).reshape(H, W)
+    return W, H, bw, bh, ve, he, img
+
+
+def test_oracle_explicit_edge_at_unaligned_origin(oracle_lib):
+    """An explicitly flagged vertical edge at x = 12 inside 8-wide blocks is
+    filtered; under the alignment rule (12/4 = 3 is not a multiple of 2) it is not."""
+    w, h = 32, 4
+    px = np.full((h, w), 110, np.uint16)
+    px[:, :12] = 100
+    bw = np.full((1, w // 4), 2, np.uint8)
+    bh = np.ones((1, w // 4), np.uint8)
+    ve = np.zeros((1, w // 4), np.uint8)
+    ve[0, 3] = 1
+    out = oracle_lib.deblock_plane(px, w, h, bw, bh, 32, 7, True, ve, None)
+    assert not np.array_equal(out, px)
+    assert np.array_equal(out[:, :8], px[:, :8]) and np.array_equal(out[:, 16:], px[:, 16:])
+    assert np.array_equal(oracle_lib.deblock_plane(px, w, h, bw, bh, 32, 7, True), px)
+
+
+def test_oracle_wide_filter_known_answer(oracle_lib):
+    """A 1-step edge between two 16-wide flat blocks at level 32 takes the
+    16-wide smoothing filter: (sum of the 15-tap window + 8) >> 4 per sample."""
+    w, h = 32, 4
+    px = np.full((h, w), 101, np.uint16)
+    px[:, :16] = 100
+    bw = np.full((1, 8), 4, np.uint8)
+    out = oracle_lib.deblock_plane(px, w, h, bw, bw, 32, 0, True)
+    row = out[0, 10:22].tolist()
+    # p5..q5 of p = 100 x7, q = 101 x7 under the 16-wide taps (AV1 spec 7.14.6.4).
+    window = [100] * 7 + [101] * 7
+    taps = [
+        [7, 2, 2, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0, 0], [5, 2, 2, 2, 1, 1, 1, 1, 1, 0, 0, 0, 0, 0],
+        [4, 1, 2, 2, 2, 1, 1, 1, 1, 1, 0, 0, 0, 0], [3, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 0, 0, 0],
+        [2, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 0, 0], [1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1, 0],
+        [0, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 1, 1], [0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 1, 2],
+        [0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 1, 1, 3], [0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 1, 4],
+        [0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 2, 5], [0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 2, 2, 7],
+    ]
+    expect = [(sum(t * v for t, v in zip(tp, window)) + 8) >> 4 for tp in taps]
+    assert row == expect
+    assert np.all(out == out[0:1])
+
+
+def test_oracle_level_zero_is_identity(oracle_lib):
+    w, h, bw, bh, ve, he, px = _geometry(77, 45, 3)
+    assert np.array_equal(oracle_lib.deblock_plane(px, 77, 45, bw, bh, 0, 0, True, ve, he), px)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_oracle_two_pass_order_equals_superblock_order(oracle_lib, seed):
+    """On AV1-shaped geometry, filtering all vertical edges then all horizontal
+    edges (one superblock row spanning the frame) gives the reference's
+    per-superblock-row samples: the order the GPU passes use."""
+    rng = np.random.default_rng(seed)
+    vis_w, vis_h = int(rng.integers(8, 260)), int(rng.integers(8, 300))
+    w, h, bw, bh, ve, he, px = _geometry(vis_w, vis_h, seed)
+    luma = seed % 3 != 0
+    level, sharp = int(rng.choice([8, 24, 40, 63])), int(rng.integers(0, 8))
+    flags = (ve, he) if seed % 2 else (None, None)
+    sb = oracle_lib.deblock_plane(px, vis_w, vis_h, bw, bh, level, sharp, luma, *flags, sb_rows4=16 if luma else 8)
+    whole = oracle_lib.deblock_plane(px, vis_w, vis_h, bw, bh, level, sharp, luma, *flags, sb_rows4=1 << 20)
+    assert np.array_equal(sb, whole)
+    assert not np.array_equal(sb, px)
+
+
+def test_deblock_rejects_bad_input(mt_lib):
+    from maroontree_b200 import MtError, abi
+
+    w, h, bw, bh, ve, he, px = _geometry(64, 64, 1)
+    with pytest.raises(MtError):
+        mt_lib.deblock_plane(px, 64, 64, bw, bh, 64, 0, True)
+    with pytest.raises(MtError):
+        mt_lib.deblock_plane(px, 64, 64, bw, bh, 10, 8, True)
+    with pytest.raises(MtError):
+        mt_lib.deblock_plane(px, 65, 64, bw, bh, 10, 0, True)
+    lib = mt_lib.load()
+    odd = np.zeros((6, 6), np.uint16)
+    m = np.ones((2, 2), np.uint8)
+    assert lib.mt_deblock_plane(odd.ctypes.data, 6, 6, 6, 6, m.ctypes.data, m.ctypes.data, None, None, 2, 10, 0, 1,
+                                8) == abi.MT_ERR_INVALID_INPUT
+    assert lib.mt_deblock_plane(odd.ctypes.data, 8, 8, 8, 8, m.ctypes.data, m.ctypes.data, None, None, 2, 10, 0, 1,
+                                10) == abi.MT_ERR_UNSUPPORTED
+
+
+def test_deblock_rejects_superblock_crossing_edge(mt_lib):
+    """A 16-wide horizontal edge on the last 4-row of a 64-row superblock row
+    (outside AV1 block geometry) is refused by the host entry point, which
+    checks the maps before touching the device."""
+    from maroontree_b200 import MtError, abi
+
+    w, h = 64, 128
+    nc4, nr4 = w // 4, h // 4
+    bw = np.full((nr4, nc4), 4, np.uint8)
+    bh = np.full((nr4, nc4), 4, np.uint8)
+    he = np.zeros((nr4, nc4), np.uint8)
+    he[15, 4] = 1
+    px = np.full((h, w), 100, np.uint16)
+    with pytest.raises(MtError) as ei:
+        mt_lib.deblock_plane(px, w, h, bw, bh, 30, 0, True, None, he)
+    assert ei.value.code == abi.MT_ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("seed", range(16))
+def test_deblock_matches_oracle(mt_lib, oracle_lib, cuda, seed):
+    rng = np.random.default_rng(1000 + seed)
+    vis_w, vis_h = int(rng.integers(1, 400)), int(rng.integers(1, 300))
+    w, h, bw, bh, ve, he, px = _geometry(vis_w, vis_h, 1000 + seed)
+    luma = seed % 4 != 0
+    level, sharp = int(rng.choice([1, 6, 16, 31, 47, 63])), int(rng.integers(0, 8))
+    flags = (ve, he) if seed % 2 else (None, None)
+    want = oracle_lib.deblock_plane(px, vis_w, vis_h, bw, bh, level, sharp, luma, *flags, sb_rows4=16 if luma else 8)
+    got = mt_lib.deblock_plane(px, vis_w, vis_h, bw, bh, level, sharp, luma, *flags)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level,sharp", [(32, 7), (63, 0), (12, 3)])
+def test_deblock_overlapping_taps_match_oracle(mt_lib, oracle_lib, cuda, level, sharp):
+    W, H, bw, bh, ve, he, img = _mixed_geometry()
+    want = oracle_lib.deblock_plane(img, W, H, bw, bh, level, sharp, True, ve, he)
+    got = mt_lib.deblock_plane(img, W, H, bw, bh, level, sharp, True, ve, he)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("luma", [True, False])
+def test_deblock_1080p_device_entry(mt_lib, oracle_lib, cuda, luma):
+    """Full-size planes through mt_deblock_plane_device on a side stream."""
+    import torch
+
+    from maroontree_b200 import abi
+
+    vis_w, vis_h = (1920, 1080) if luma else (960, 540)
+    w, h, bw, bh, ve, he, px = _geometry(vis_w, vis_h, 77 + luma)
+    level = 36 if luma else 20
+    want = oracle_lib.deblock_plane(px, vis_w, vis_h, bw, bh, level, 2, luma, ve, he, sb_rows4=16 if luma else 8)
+    d_px = torch.from_numpy(px.astype(np.int16)).cuda()
+    maps = [torch.from_numpy(np.ascontiguousarray(m)).cuda() for m in (bw, bh, ve, he)]
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        rc = mt_lib.load().mt_deblock_plane_device(d_px.data_ptr(), w, h, vis_w, vis_h, *[m.data_ptr() for m in maps],
+                                                    bw.shape[1], level, 2, int(luma), 8, C.c_void_p(s.cuda_stream))
+    s.synchronize()
+    assert rc == abi.MT_OK
+    got = d_px.cpu().numpy().view(np.uint16)
+    assert np.array_equal(got, want)
