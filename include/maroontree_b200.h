@@ -311,6 +311,61 @@ int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w,
                             const uint8_t* d_bh4, const uint8_t* d_vedge4, const uint8_t* d_hedge4, int32_t nc4,
                             int32_t level, int32_t sharp, int32_t is_luma, int32_t bd, void* stream);
 
+/* Frame CDEF (src/coder/frame_cdef.rs:49-520 frame_cdef, with the filter,
+ * direction search and 12-strength candidate evaluation of src/cdef.rs), in
+ * the configuration the encoder ships: weighted-SSE decision metric
+ * (src/rd_sse.rs weighted_sse, AVX2 order src/avx/rd.rs:767-848, scale 1),
+ * 40 per-mille margin, directional-variance gate 15000, chroma weight 1, CDEF
+ * bits priced with the frame lambda_d.
+ *
+ * Planes: luma w8 x h8 (multiples of 8), chroma (w8 >> sub_x) x (h8 >> sub_y)
+ * (absent when mono), all u16 row-major; recon planes are filtered in place.
+ * skip8: one byte per luma 8x8 block ((w8/8) x (h8/8), 1 = skip block, which
+ * CDEF leaves untouched).  The caller gates CDEF as the reference does (no
+ * IntraBC, CDEF enabled, base_q_idx != 0). */
+typedef struct mt_cdef_params {
+  int32_t w8, h8;          /* padded luma plane */
+  int32_t disp_w, disp_h;  /* visible luma size (w8 - 8 < disp_w <= w8) */
+  int32_t sub_x, sub_y;    /* chroma subsampling shifts: (1,1) 4:2:0, (1,0) 4:2:2, (0,0) 4:4:4 */
+  int32_t mono;            /* 1: luma only */
+  int32_t base_q_idx;      /* 1..255 */
+  int32_t bd;              /* 8 */
+  int32_t slow;            /* 1: Speed::Slow or slower (two-stage strength search) */
+} mt_cdef_params;
+
+typedef struct mt_cdef_decision {
+  int32_t bits;            /* cdef_bits 0..3, or -1: CDEF off for the frame (planes unchanged) */
+  int32_t damping;         /* signalled damping 3..6 */
+  int32_t n_strengths;     /* entries in strengths (1 << bits), 0 when bits == -1 */
+  int32_t unit_cols, unit_rows;  /* the 64x64 unit grid */
+  uint8_t strengths[8][4]; /* per entry: luma pri, luma sec, chroma pri, chroma sec */
+} mt_cdef_decision;
+
+/* Per-block directions / variances and the per-64x64-unit distortion of all
+ * 12 strength pairs (index sec_idx * 4 + pri_idx over pri {0,1,2,4}, sec
+ * {0,1,2}): src/coder/frame_cdef.rs:600-820 cdef_luma_unit_dists_all /
+ * cdef_chroma_unit_sse_all.  dirs / vars: (h8/8) x (w8/8); tables:
+ * unit_rows x unit_cols x 12 int64 (u / v tables ignored when mono). */
+int mt_cdef_tables_device(const uint16_t* d_y, const uint16_t* d_u, const uint16_t* d_v, const uint16_t* d_src_y,
+                          const uint16_t* d_src_u, const uint16_t* d_src_v, const uint8_t* d_skip8,
+                          const mt_cdef_params* prm, uint8_t* d_dirs, int32_t* d_vars, int64_t* d_luma_tab,
+                          int64_t* d_u_tab, int64_t* d_v_tab, void* stream);
+/* Device working storage mt_cdef_frame_device needs. */
+size_t mt_cdef_scratch_bytes(const mt_cdef_params* prm);
+/* The whole frame CDEF: tables on the device, the strength search on the host
+ * (the stream is synchronised once to read the tables), then the filter
+ * applied to the recon planes on the stream.  grid: host buffer of
+ * unit_cols * unit_rows bytes (the per-unit strength index; zeros unless bits
+ * > 0), may be NULL. */
+int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint16_t* d_src_y,
+                         const uint16_t* d_src_u, const uint16_t* d_src_v, const uint8_t* d_skip8,
+                         const mt_cdef_params* prm, void* d_scratch, mt_cdef_decision* out, uint8_t* grid,
+                         void* stream);
+/* Host-buffer form of mt_cdef_frame_device. */
+int mt_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* src_y, const uint16_t* src_u,
+                  const uint16_t* src_v, const uint8_t* skip8, const mt_cdef_params* prm, mt_cdef_decision* out,
+                  uint8_t* grid);
+
 /* Library version string. */
 const char* mt_version(void);
 

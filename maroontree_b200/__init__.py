@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "cdef_params", "cdef_frame", "MtError",
 ]
 
 
@@ -173,3 +173,35 @@ def deblock_plane(px, vis_w, vis_h, bw4, bh4, level, sharp, is_luma, vedge4=None
     _check(load().mt_deblock_plane(ptr(out), w, h, vis_w, vis_h, ptr(bw4), ptr(bh4), ptr(ve), ptr(he), nc4, level,
                                    sharp, int(bool(is_luma)), bd), "mt_deblock_plane")
     return out
+
+
+def cdef_params(disp_w, disp_h, sub_x, sub_y, base_q_idx, mono=False, slow=True, bd=8):
+    """``mt_cdef_params`` of a frame whose padded planes are align8(disp)."""
+    p = abi.CdefParams()
+    p.w8, p.h8 = (disp_w + 7) & ~7, (disp_h + 7) & ~7
+    p.disp_w, p.disp_h, p.sub_x, p.sub_y = disp_w, disp_h, sub_x, sub_y
+    p.mono, p.base_q_idx, p.bd, p.slow = int(mono), base_q_idx, bd, int(slow)
+    return p
+
+
+def _decision_dict(d, grid):
+    n = d.n_strengths
+    return {"bits": d.bits, "damping": d.damping, "unit_cols": d.unit_cols, "unit_rows": d.unit_rows,
+            "strengths": [tuple(d.strengths[e]) for e in range(n)], "grid": grid}
+
+
+def cdef_frame(recon, src, skip8, prm):
+    """``frame_cdef`` (src/coder/frame_cdef.rs:49-520) on copies of the recon
+    planes.  recon / src: [Y] or [Y, U, V] u16 planes; skip8: (h8/8, w8/8) u8.
+    Returns (filtered planes, decision dict)."""
+    mono = bool(prm.mono)
+    out = [np.array(p, dtype=np.uint16, copy=True, order="C") for p in recon]
+    src = [np.ascontiguousarray(p, np.uint16) for p in src]
+    skip8 = np.ascontiguousarray(skip8, np.uint8)
+    nu = ((prm.w8 + 63) // 64) * ((prm.h8 + 63) // 64)
+    grid = np.zeros(nu, np.uint8)
+    d = abi.CdefDecision()
+    ch = (lambda a, i: None) if mono else (lambda a, i: ptr(a[i]))
+    _check(load().mt_cdef_frame(ptr(out[0]), ch(out, 1), ch(out, 2), ptr(src[0]), ch(src, 1), ch(src, 2), ptr(skip8),
+                                C.byref(prm), C.byref(d), ptr(grid)), "mt_cdef_frame")
+    return out, _decision_dict(d, grid)

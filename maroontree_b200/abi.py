@@ -69,6 +69,20 @@ class ChainParams(C.Structure):
     ]
 
 
+class CdefParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "disp_w", "disp_h", "sub_x", "sub_y", "mono", "base_q_idx",
+                                         "bd", "slow")]
+
+
+class CdefDecision(C.Structure):
+    _fields_ = [
+        ("bits", C.c_int32), ("damping", C.c_int32), ("n_strengths", C.c_int32), ("unit_cols", C.c_int32),
+        ("unit_rows", C.c_int32), ("strengths", (C.c_uint8 * 4) * 8),
+    ]
+
+
+assert C.sizeof(CdefParams) == 40 and C.sizeof(CdefDecision) == 52
+
 BLOCK8_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
     ("mode_bits", "<f4", (13,)),
@@ -119,6 +133,10 @@ def _bind(lib):
                                        C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "mt_deblock_plane_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                               C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
+        "mt_cdef_tables_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams)] + [_P] * 6),
+        "mt_cdef_scratch_bytes": (C.c_size_t, [C.POINTER(CdefParams)]),
+        "mt_cdef_frame_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams), _P, C.POINTER(CdefDecision), _P, _P]),
+        "mt_cdef_frame": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams), C.POINTER(CdefDecision), _P]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -149,6 +167,7 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
+    "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
 )
 

@@ -336,3 +336,38 @@ def blocky_plane(w, h, block_id, seed, maxv=255):
     v = v + np.where(s == 4, rng.integers(-3, 4, (h, w)), 0)
     full[:] = np.clip(v, 0, maxv)
     return full.astype(np.uint16)
+
+
+def cdef_inputs(disp_w, disp_h, sub_x, sub_y, mono, seed, skip_frac=0.3):
+    """Source and reconstruction planes plus a per-8x8 skip map for the frame
+    CDEF: luma from the synthetic RGB image, chroma a contrast-reduced copy of
+    it; the reconstruction adds seeded error whose amplitude varies per 64x64
+    unit (0 .. 12, with or without block-edge ringing), so that CDEF helps some units and
+    not others.  Planes are edge-padded to multiples of 8."""
+    w8, h8 = (disp_w + 7) & ~7, (disp_h + 7) & ~7
+    rng = np.random.default_rng(seed)
+    y = rgb_to_luma(generate_rgb(disp_w, disp_h, seed)).astype(np.int32)
+    y = np.pad(y, ((0, h8 - disp_h), (0, w8 - disp_w)), mode="edge")
+    planes = [y]
+    if not mono:
+        sub = y[::1 << sub_y, ::1 << sub_x]
+        planes.append(np.clip(128 + (sub - 128) // 3, 0, 255))
+        planes.append(np.clip(128 - (sub - 128) // 4, 0, 255))
+    src, rec = [], []
+    uc, ur = (w8 + 63) // 64, (h8 + 63) // 64
+    amp_u = rng.choice([0, 1, 2, 4, 7, 12], size=(ur, uc))
+    ring_u = rng.choice([0, 1, 3], size=(ur, uc))
+    for k, p in enumerate(planes):
+        sx, sy = (0, 0) if k == 0 else (sub_x, sub_y)
+        h, w = p.shape
+        yy, xx = np.mgrid[0:h, 0:w]
+        amp = amp_u[(yy << sy) // 64, (xx << sx) // 64]
+        noise = np.round(rng.uniform(-1, 1, size=p.shape) * amp).astype(np.int32)
+        ring = np.where(((xx % (8 >> sx)) == 0) | ((yy % (8 >> sy)) == 0),
+                        ring_u[(yy << sy) // 64, (xx << sx) // 64] * amp // 2, 0)
+        src.append(p.astype(np.uint16))
+        rec.append(np.clip(p + noise + ring, 0, 255).astype(np.uint16))
+    skip8 = (rng.random((h8 // 8, w8 // 8)) < skip_frac).astype(np.uint8)
+    if uc * ur > 1:
+        skip8[:8, :8] = 1  # one all-skip unit
+    return src, rec, skip8

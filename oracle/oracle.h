@@ -67,6 +67,12 @@ int or_csc_rgb8(const uint8_t* rgb, int32_t w, int32_t h, int32_t sub, uint16_t*
 int or_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,
                      const uint8_t* bh4, const uint8_t* vedge4, const uint8_t* hedge4, int32_t nc4, int32_t level,
                      int32_t sharp, int32_t is_luma, int32_t sb_rows4, int32_t bd);
+/* frame_cdef.rs frame_cdef: tables (optional outputs), decision, apply in place. */
+int or_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* sy, const uint16_t* su, const uint16_t* sv,
+                  const uint8_t* skip8, const mt_cdef_params* prm, mt_cdef_decision* out, uint8_t* grid,
+                  int64_t* luma_tab, int64_t* u_tab, int64_t* v_tab, uint8_t* dirs, int32_t* vars);
+float or_weighted_sse(const int32_t* err, int32_t w, int32_t h);
+float or_cdef_frame_lambda(int32_t qidx, int32_t bd, int32_t sub_x, int32_t sub_y);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 

@@ -39,6 +39,9 @@ def load():
             "or_edge_filter_strength": (C.c_int, [C.c_int] * 4),
             "or_use_edge_upsample": (C.c_int, [C.c_int] * 4),
             "or_csc_rgb8": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P]),
+            "or_cdef_frame": (C.c_int, [_P] * 7 + [C.POINTER(abi.CdefParams), C.POINTER(abi.CdefDecision)] + [_P] * 6),
+            "or_weighted_sse": (C.c_float, [_P, C.c_int32, C.c_int32]),
+            "or_cdef_frame_lambda": (C.c_float, [C.c_int32] * 4),
             "or_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
@@ -168,3 +171,31 @@ def deblock_plane(px, vis_w, vis_h, bw4, bh4, level, sharp, is_luma, vedge4=None
     assert load().or_deblock_plane(p(out), w, h, vis_w, vis_h, p(bw4), p(bh4), p(ve), p(he), nc4, level, sharp,
                                    int(bool(is_luma)), sb_rows4, bd) == 0
     return out
+
+
+def weighted_sse(err):
+    err = np.ascontiguousarray(err, np.int32)
+    h, w = err.shape
+    return load().or_weighted_sse(p(err), w, h)
+
+
+def cdef_frame(recon, src, skip8, prm):
+    """Returns (filtered planes, decision dict, tables dict)."""
+    mono = bool(prm.mono)
+    out = [np.array(x, dtype=np.uint16, copy=True, order="C") for x in recon]
+    src = [np.ascontiguousarray(x, np.uint16) for x in src]
+    skip8 = np.ascontiguousarray(skip8, np.uint8)
+    uc, ur = (prm.w8 + 63) // 64, (prm.h8 + 63) // 64
+    nb = (prm.w8 // 8) * (prm.h8 // 8)
+    grid = np.zeros(uc * ur, np.uint8)
+    tabs = [np.zeros((ur * uc, 12), np.int64) for _ in range(3)]
+    dirs = np.zeros(nb, np.uint8)
+    vars_ = np.zeros(nb, np.int32)
+    d = abi.CdefDecision()
+    ch = (lambda a, i: None) if mono else (lambda a, i: p(a[i]))
+    assert load().or_cdef_frame(p(out[0]), ch(out, 1), ch(out, 2), p(src[0]), ch(src, 1), ch(src, 2), p(skip8),
+                                C.byref(prm), C.byref(d), p(grid), p(tabs[0]), p(tabs[1]), p(tabs[2]), p(dirs),
+                                p(vars_)) == 0
+    dec = {"bits": d.bits, "damping": d.damping, "unit_cols": d.unit_cols, "unit_rows": d.unit_rows,
+           "strengths": [tuple(d.strengths[e]) for e in range(d.n_strengths)], "grid": grid}
+    return out, dec, {"luma": tabs[0], "u": tabs[1], "v": tabs[2], "dirs": dirs, "vars": vars_}
