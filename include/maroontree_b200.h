@@ -311,6 +311,33 @@ int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w,
                             const uint8_t* d_bh4, const uint8_t* d_vedge4, const uint8_t* d_hedge4, int32_t nc4,
                             int32_t level, int32_t sharp, int32_t is_luma, int32_t bd, void* stream);
 
+/* Frame deblocking as src/coder/frame_deblock.rs:206-224 (frame_deblock)
+ * drives it: luma from the luma TRANSFORM-block maps with explicit block-start
+ * flags (16 4-rows per superblock), then, when luma is filtered and a chroma
+ * level is non-zero, U and V from chroma geometry derived from the luma
+ * PREDICTION-block maps (src/coder/frame_deblock.rs:87-152: size >> subsampling,
+ * clamped to 1..8 cells, alignment-rule edges).  Maps: (h8/4) x (w8/4) u8 cells
+ * of the luma grid.  Sharpness is the shipped 7. */
+typedef struct mt_deblock_frame_params {
+  int32_t w8, h8;          /* padded luma plane (multiples of 8) */
+  int32_t disp_w, disp_h;  /* visible luma size */
+  int32_t sub_x, sub_y;    /* chroma subsampling shifts */
+  int32_t mono;
+  int32_t bd;              /* 8 */
+} mt_deblock_frame_params;
+/* loop_filter_levels / loop_filter_sharpness (src/obu.rs:306-334, shipped
+ * tuning): the frame's luma and chroma levels and the sharpness. */
+int mt_loop_filter_levels(int32_t base_q_idx, int32_t sub_x, int32_t sub_y, int32_t* lvl_y, int32_t* lvl_uv,
+                          int32_t* sharp);
+size_t mt_deblock_frame_scratch_bytes(const mt_deblock_frame_params* prm);
+int mt_deblock_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint8_t* d_blk4,
+                            const uint8_t* d_blk4h, const uint8_t* d_blk4v, const uint8_t* d_blk4t,
+                            const uint8_t* d_pblk4, const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm,
+                            int32_t lvl_y, int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream);
+int mt_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,
+                     const uint8_t* blk4v, const uint8_t* blk4t, const uint8_t* pblk4, const uint8_t* pblk4h,
+                     const mt_deblock_frame_params* prm, int32_t lvl_y, int32_t lvl_u, int32_t lvl_v);
+
 /* Frame CDEF (src/coder/frame_cdef.rs:49-520 frame_cdef, with the filter,
  * direction search and 12-strength candidate evaluation of src/cdef.rs), in
  * the configuration the encoder ships: weighted-SSE decision metric

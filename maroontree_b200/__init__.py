@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "cdef_params", "cdef_frame", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
 ]
 
 
@@ -205,3 +205,29 @@ def cdef_frame(recon, src, skip8, prm):
     _check(load().mt_cdef_frame(ptr(out[0]), ch(out, 1), ch(out, 2), ptr(src[0]), ch(src, 1), ch(src, 2), ptr(skip8),
                                 C.byref(prm), C.byref(d), ptr(grid)), "mt_cdef_frame")
     return out, _decision_dict(d, grid)
+
+
+def loop_filter_levels(base_q_idx, sub_x, sub_y):
+    """``loop_filter_levels`` / ``loop_filter_sharpness`` (src/obu.rs:306-334): (lvl_y, lvl_uv, sharp)."""
+    a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+    _check(load().mt_loop_filter_levels(base_q_idx, sub_x, sub_y, C.byref(a), C.byref(b), C.byref(c)),
+           "mt_loop_filter_levels")
+    return a.value, b.value, c.value
+
+
+def deblock_frame(planes, disp_w, disp_h, sub_x, sub_y, tx_maps, pred_maps, lvl_y, lvl_u, lvl_v, mono=False):
+    """``frame_deblock`` (src/coder/frame_deblock.rs:206-224) on copies of the planes.
+
+    tx_maps: (blk4, blk4h, blk4v, blk4t) luma transform-block maps with block
+    start flags; pred_maps: (pblk4, pblk4h) luma prediction-block sizes; all
+    (h8/4, w8/4) u8."""
+    out = [np.array(p, dtype=np.uint16, copy=True, order="C") for p in planes]
+    g = abi.DeblockFrameParams()
+    g.w8, g.h8 = out[0].shape[1], out[0].shape[0]
+    g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = disp_w, disp_h, sub_x, sub_y, int(mono), 8
+    tm = [np.ascontiguousarray(m, np.uint8) for m in tx_maps]
+    pm = [np.ascontiguousarray(m, np.uint8) for m in pred_maps]
+    ch = (lambda i: None) if mono else (lambda i: ptr(out[i]))
+    _check(load().mt_deblock_frame(ptr(out[0]), ch(1), ch(2), *[ptr(m) for m in tm], *[ptr(m) for m in pm],
+                                   C.byref(g), lvl_y, lvl_u, lvl_v), "mt_deblock_frame")
+    return out

@@ -69,6 +69,10 @@ class ChainParams(C.Structure):
     ]
 
 
+class DeblockFrameParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "disp_w", "disp_h", "sub_x", "sub_y", "mono", "bd")]
+
+
 class CdefParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "disp_w", "disp_h", "sub_x", "sub_y", "mono", "base_q_idx",
                                          "bd", "slow")]
@@ -133,6 +137,10 @@ def _bind(lib):
                                        C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "mt_deblock_plane_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                               C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P]),
+        "mt_loop_filter_levels": (C.c_int, [C.c_int32] * 3 + [C.POINTER(C.c_int32)] * 3),
+        "mt_deblock_frame_scratch_bytes": (C.c_size_t, [C.POINTER(DeblockFrameParams)]),
+        "mt_deblock_frame_device": (C.c_int, [_P] * 9 + [C.POINTER(DeblockFrameParams)] + [C.c_int32] * 3 + [_P, _P]),
+        "mt_deblock_frame": (C.c_int, [_P] * 9 + [C.POINTER(DeblockFrameParams)] + [C.c_int32] * 3),
         "mt_cdef_tables_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams)] + [_P] * 6),
         "mt_cdef_scratch_bytes": (C.c_size_t, [C.POINTER(CdefParams)]),
         "mt_cdef_frame_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams), _P, C.POINTER(CdefDecision), _P, _P]),
@@ -167,6 +175,7 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
+    "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
 )

@@ -23,7 +23,10 @@
 // such edges form runs of consecutive overlapping edges, and the thread of a
 // run's first edge filters the whole run in order while the others return.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "../../include/maroontree_b200.h"
 
@@ -283,9 +286,56 @@ bool has_superblock_crossing(int32_t w, int32_t h, int32_t vis_w, int32_t vis_h,
   return false;
 }
 
+// Chroma deblocking geometry (src/coder/frame_deblock.rs:87-152, variant 1):
+// per chroma 4x4 cell, the covering luma PREDICTION block's size >> subsampling,
+// at least 1 and at most 8 (32 px, the largest chroma transform); edges by the
+// alignment rule.
+__global__ void chroma_geom_kernel(const uint8_t* __restrict__ pbw4, const uint8_t* __restrict__ pbh4, int nc4,
+                                   int cnc4, int cnr4, int ss_hor, int ss_ver, uint8_t* __restrict__ cbw4,
+                                   uint8_t* __restrict__ cbh4) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= cnc4 * cnr4) return;
+  const int cr = i / cnc4, cc = i - cr * cnc4;
+  const long li = (long)(cr << ss_ver) * nc4 + (cc << ss_hor);
+  cbw4[i] = (uint8_t)min(max(pbw4[li] >> ss_hor, 1), 8);
+  cbh4[i] = (uint8_t)min(max(pbh4[li] >> ss_ver, 1), 8);
+}
+
+int check_frame(const mt_deblock_frame_params* p) {
+  if (!p) return MT_ERR_INVALID_INPUT;
+  if (p->w8 <= 0 || p->h8 <= 0 || (p->w8 & 7) || (p->h8 & 7)) return MT_ERR_INVALID_INPUT;
+  if (p->disp_w <= p->w8 - 8 || p->disp_w > p->w8 || p->disp_h <= p->h8 - 8 || p->disp_h > p->h8)
+    return MT_ERR_INVALID_INPUT;
+  if (p->sub_x < 0 || p->sub_x > 1 || p->sub_y < 0 || p->sub_y > p->sub_x) return MT_ERR_INVALID_INPUT;
+  if (p->bd != 8) return MT_ERR_UNSUPPORTED;
+  return MT_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int mt_loop_filter_levels(int32_t base_q_idx, int32_t sub_x, int32_t sub_y, int32_t* lvl_y, int32_t* lvl_uv,
+                          int32_t* sharp) {
+  if (base_q_idx < 0 || base_q_idx > 255 || sub_x < 0 || sub_x > 1 || sub_y < 0 || sub_y > 1)
+    return MT_ERR_INVALID_INPUT;
+  const int q = base_q_idx;
+  const int sub = sub_x + sub_y;
+  const float uv_scale = sub == 2 ? 0.5f : 1.0f;
+  const int ly = std::min(std::max((int)roundf((float)(q / 8) * 1.0f), 0), 40);
+  int luv = 0;
+  if (ly > 0) luv = std::min(std::max(std::max((int)roundf((float)(q / 10) * uv_scale), 1), 0), 32);
+  if (lvl_y) *lvl_y = ly;
+  if (lvl_uv) *lvl_uv = luv;
+  if (sharp) *sharp = 7;
+  return MT_OK;
+}
+
+size_t mt_deblock_frame_scratch_bytes(const mt_deblock_frame_params* prm) {
+  if (check_frame(prm) != MT_OK) return 0;
+  const size_t n = (size_t)((prm->w8 >> prm->sub_x) / 4) * ((prm->h8 >> prm->sub_y) / 4);
+  return 2 * ((n + 255) & ~(size_t)255);
+}
 
 int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* d_bw4,
                             const uint8_t* d_bh4, const uint8_t* d_vedge4, const uint8_t* d_hedge4, int32_t nc4,
@@ -308,6 +358,83 @@ int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w,
   if (a.w4 > 1) lf_vert_kernel<<<dim3((a.w4 + T - 1) / T, a.h4 * 4), T, 0, st>>>(d_px, a, d_bw4, d_vedge4);
   if (a.h4 > 1) lf_horz_kernel<<<dim3((a.w4 * 4 + T - 1) / T, a.h4), T, 0, st>>>(d_px, a, d_bh4, d_hedge4);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_deblock_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint8_t* d_blk4,
+                            const uint8_t* d_blk4h, const uint8_t* d_blk4v, const uint8_t* d_blk4t,
+                            const uint8_t* d_pblk4, const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm,
+                            int32_t lvl_y, int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream) {
+  int rc = check_frame(prm);
+  if (rc != MT_OK) return rc;
+  if (lvl_y < 0 || lvl_y > 63 || lvl_u < 0 || lvl_u > 63 || lvl_v < 0 || lvl_v > 63) return MT_ERR_INVALID_INPUT;
+  const int sharp = 7;
+  const int nc4 = prm->w8 / 4;
+  if (lvl_y > 0) {
+    rc = mt_deblock_plane_device(d_y, prm->w8, prm->h8, prm->disp_w, prm->disp_h, d_blk4, d_blk4h, d_blk4v, d_blk4t,
+                                 nc4, lvl_y, sharp, 1, prm->bd, stream);
+    if (rc != MT_OK) return rc;
+  }
+  if (prm->mono || lvl_y <= 0 || (lvl_u <= 0 && lvl_v <= 0)) return MT_OK;
+  if (!d_pblk4 || !d_pblk4h || !d_scratch || !d_u || !d_v) return MT_ERR_INVALID_INPUT;
+  const int cw8 = prm->w8 >> prm->sub_x, ch8 = prm->h8 >> prm->sub_y;
+  const int cnc4 = cw8 / 4, cnr4 = ch8 / 4;
+  const size_t n = (size_t)cnc4 * cnr4;
+  uint8_t* cbw4 = static_cast<uint8_t*>(d_scratch);
+  uint8_t* cbh4 = cbw4 + ((n + 255) & ~(size_t)255);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  chroma_geom_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pblk4, d_pblk4h, nc4, cnc4, cnr4, prm->sub_x,
+                                                                  prm->sub_y, cbw4, cbh4);
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_DEVICE;
+  const int vis_w = (prm->disp_w + (1 << prm->sub_x) - 1) >> prm->sub_x;
+  const int vis_h = (prm->disp_h + (1 << prm->sub_y) - 1) >> prm->sub_y;
+  if (lvl_u > 0) {
+    rc = mt_deblock_plane_device(d_u, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4, lvl_u, sharp, 0,
+                                 prm->bd, stream);
+    if (rc != MT_OK) return rc;
+  }
+  if (lvl_v > 0)
+    rc = mt_deblock_plane_device(d_v, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4, lvl_v, sharp, 0,
+                                 prm->bd, stream);
+  return rc;
+}
+
+int mt_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,
+                     const uint8_t* blk4v, const uint8_t* blk4t, const uint8_t* pblk4, const uint8_t* pblk4h,
+                     const mt_deblock_frame_params* prm, int32_t lvl_y, int32_t lvl_u, int32_t lvl_v) {
+  int rc = check_frame(prm);
+  if (rc != MT_OK) return rc;
+  if (!y || !blk4 || !blk4h || !blk4v || !blk4t) return MT_ERR_INVALID_INPUT;
+  const bool chroma = !prm->mono && lvl_y > 0 && (lvl_u > 0 || lvl_v > 0);
+  if (chroma && (!u || !v || !pblk4 || !pblk4h)) return MT_ERR_INVALID_INPUT;
+  const int nc4 = prm->w8 / 4, nr4 = prm->h8 / 4;
+  if (lvl_y > 0 && has_superblock_crossing(prm->w8, prm->h8, prm->disp_w, prm->disp_h, blk4h, blk4t, nc4))
+    return MT_ERR_UNSUPPORTED;
+  const size_t ny = (size_t)prm->w8 * prm->h8 * 2, nm = (size_t)nc4 * nr4;
+  const size_t nc = chroma ? (size_t)(prm->w8 >> prm->sub_x) * (prm->h8 >> prm->sub_y) * 2 : 0;
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t o_y = 0, o_u = up(ny), o_v = o_u + up(nc), o_m = o_v + up(nc), o_s = o_m + 6 * up(nm);
+  const size_t total = o_s + mt_deblock_frame_scratch_bytes(prm);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const uint8_t* maps[6] = {blk4, blk4h, blk4v, blk4t, pblk4, pblk4h};
+  cudaError_t e = cudaMemcpy(d + o_y, y, ny, cudaMemcpyHostToDevice);
+  for (int k = 0; k < 6 && e == cudaSuccess; k++)
+    if (maps[k] && (k < 4 || chroma)) e = cudaMemcpy(d + o_m + k * up(nm), maps[k], nm, cudaMemcpyHostToDevice);
+  if (chroma && e == cudaSuccess) e = cudaMemcpy(d + o_u, u, nc, cudaMemcpyHostToDevice);
+  if (chroma && e == cudaSuccess) e = cudaMemcpy(d + o_v, v, nc, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    auto m = [&](int k) { return (const uint8_t*)(d + o_m + k * up(nm)); };
+    rc = mt_deblock_frame_device((uint16_t*)(d + o_y), chroma ? (uint16_t*)(d + o_u) : nullptr,
+                                 chroma ? (uint16_t*)(d + o_v) : nullptr, m(0), m(1), m(2), m(3),
+                                 chroma ? m(4) : nullptr, chroma ? m(5) : nullptr, prm, lvl_y, chroma ? lvl_u : 0,
+                                 chroma ? lvl_v : 0, d + o_s, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(y, d + o_y, ny, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && chroma && e == cudaSuccess) e = cudaMemcpy(u, d + o_u, nc, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && chroma && e == cudaSuccess) e = cudaMemcpy(v, d + o_v, nc, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
 int mt_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,

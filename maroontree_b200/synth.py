@@ -371,3 +371,37 @@ def cdef_inputs(disp_w, disp_h, sub_x, sub_y, mono, seed, skip_frac=0.3):
     if uc * ur > 1:
         skip8[:8, :8] = 1  # one all-skip unit
     return src, rec, skip8
+
+
+def transform_maps(bw4, bh4, block_id, seed, split_p=0.4):
+    """Luma transform-block maps inside the prediction blocks of
+    ``partition_maps``: each block of at least 8x8 is split into a 2x2 grid of
+    transforms with probability split_p (tx_depth 1).  Returns (tw4, th4,
+    tv4, tt4) like the prediction maps."""
+    rng = np.random.default_rng(seed)
+    nr4, nc4 = bw4.shape
+    tw, th = bw4.copy(), bh4.copy()
+    tv = np.zeros_like(bw4)
+    tt = np.zeros_like(bw4)
+    nb = int(block_id.max()) + 1
+    split = rng.random(nb) < split_p
+    seen = np.zeros(nb, bool)
+    for r in range(nr4):
+        for c in range(nc4):
+            b = block_id[r, c]
+            if b < 0 or seen[b]:
+                continue
+            seen[b] = True
+            w, h = int(bw4[r, c]), int(bh4[r, c])
+            sw, sh = (w // 2, h // 2) if (split[b] and w >= 2 and h >= 2) else (w, h)
+            for dr in range(0, h, sh):
+                for dc in range(0, w, sw):
+                    r0, c0 = r + dr, c + dc
+                    if r0 >= nr4 or c0 >= nc4:
+                        continue
+                    r1, c1 = min(r0 + sh, nr4), min(c0 + sw, nc4)
+                    tw[r0:r1, c0:c1] = sw
+                    th[r0:r1, c0:c1] = sh
+                    tv[r0:r1, c0] = 1
+                    tt[r0, c0:c1] = 1
+    return tw, th, tv, tt

@@ -67,6 +67,10 @@ int or_csc_rgb8(const uint8_t* rgb, int32_t w, int32_t h, int32_t sub, uint16_t*
 int or_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* bw4,
                      const uint8_t* bh4, const uint8_t* vedge4, const uint8_t* hedge4, int32_t nc4, int32_t level,
                      int32_t sharp, int32_t is_luma, int32_t sb_rows4, int32_t bd);
+void or_loop_filter_levels(int32_t base_q_idx, int32_t sub, int32_t* lvl_y, int32_t* lvl_uv, int32_t* sharp);
+int or_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,
+                     const uint8_t* blk4v, const uint8_t* blk4t, const uint8_t* pblk4, const uint8_t* pblk4h,
+                     const mt_deblock_frame_params* g, int32_t lvl_y, int32_t lvl_u, int32_t lvl_v);
 /* frame_cdef.rs frame_cdef: tables (optional outputs), decision, apply in place. */
 int or_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* sy, const uint16_t* su, const uint16_t* sv,
                   const uint8_t* skip8, const mt_cdef_params* prm, mt_cdef_decision* out, uint8_t* grid,

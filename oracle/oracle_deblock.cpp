@@ -5,8 +5,12 @@
 //   luma_cls / chroma_cls src/loopfilter.rs:396-412
 //   filter_plane_impl     src/loopfilter.rs:482-648 (per superblock row: vertical
 //                         edges, then horizontal edges; scalar edge path)
+//   frame_deblock         src/coder/frame_deblock.rs:87-224, src/obu.rs:306-334
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
+
+#include <vector>
 
 #include "oracle.h"
 
@@ -177,5 +181,58 @@ extern "C" int or_deblock_plane(uint16_t* px, int32_t w, int32_t h, int32_t vis_
       }
     }
   }
+  return MT_OK;
+}
+
+// src/obu.rs:306-334 with the shipped tuning (lf_level_scale 1, lf_uv_level_scale
+// 1, lf_uv_level_scale_420 0.5, lf_sharpness 7; src/tuning.rs:764-767).
+extern "C" void or_loop_filter_levels(int32_t base_q_idx, int32_t sub, int32_t* lvl_y, int32_t* lvl_uv,
+                                      int32_t* sharp) {
+  const int q = base_q_idx;
+  const float uv_scale = sub == 2 ? 0.5f : 1.0f;
+  int ly = (int)roundf((float)(q / 8) * 1.0f);
+  ly = ly < 0 ? 0 : (ly > 40 ? 40 : ly);
+  int luv = 0;
+  if (ly > 0) {
+    luv = (int)roundf((float)(q / 10) * uv_scale);
+    if (luv < 1) luv = 1;
+    luv = luv > 32 ? 32 : luv;
+  }
+  *lvl_y = ly;
+  *lvl_uv = luv;
+  *sharp = 7;
+}
+
+// src/coder/frame_deblock.rs:87-224: frame_deblock with chroma_deblock_geom
+// (cdblk_variant 1: prediction geometry, alignment-rule chroma edges).
+extern "C" int or_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,
+                                const uint8_t* blk4v, const uint8_t* blk4t, const uint8_t* pblk4,
+                                const uint8_t* pblk4h, const mt_deblock_frame_params* g, int32_t lvl_y,
+                                int32_t lvl_u, int32_t lvl_v) {
+  const int nc4 = g->w8 / 4;
+  if (lvl_y > 0)
+    or_deblock_plane(y, g->w8, g->h8, g->disp_w, g->disp_h, blk4, blk4h, blk4v, blk4t, nc4, lvl_y, 7, 1, 16, g->bd);
+  if (g->mono || lvl_y <= 0 || (lvl_u <= 0 && lvl_v <= 0)) return MT_OK;
+  const int ss_hor = g->sub_x, ss_ver = g->sub_y;
+  const int cw8 = g->w8 >> ss_hor, ch8 = g->h8 >> ss_ver;
+  const int cnc4 = cw8 / 4, cnr4 = ch8 / 4;
+  std::vector<uint8_t> cbw4(cnc4 * cnr4), cbh4(cnc4 * cnr4);
+  for (int cr = 0; cr < cnr4; cr++)
+    for (int cc = 0; cc < cnc4; cc++) {
+      const int li = (cr << ss_ver) * nc4 + (cc << ss_hor), ci = cr * cnc4 + cc;
+      int sw = pblk4[li] >> ss_hor, sh = pblk4h[li] >> ss_ver;
+      sw = sw < 1 ? 1 : (sw > 8 ? 8 : sw);
+      sh = sh < 1 ? 1 : (sh > 8 ? 8 : sh);
+      cbw4[ci] = (uint8_t)sw;
+      cbh4[ci] = (uint8_t)sh;
+    }
+  const int vis_w = (g->disp_w + (1 << ss_hor) - 1) >> ss_hor, vis_h = (g->disp_h + (1 << ss_ver) - 1) >> ss_ver;
+  const int sb_rows4 = 16 >> ss_ver;
+  if (lvl_u > 0)
+    or_deblock_plane(u, cw8, ch8, vis_w, vis_h, cbw4.data(), cbh4.data(), nullptr, nullptr, cnc4, lvl_u, 7, 0,
+                     sb_rows4, g->bd);
+  if (lvl_v > 0)
+    or_deblock_plane(v, cw8, ch8, vis_w, vis_h, cbw4.data(), cbh4.data(), nullptr, nullptr, cnc4, lvl_v, 7, 0,
+                     sb_rows4, g->bd);
   return MT_OK;
 }

@@ -42,6 +42,8 @@ def load():
             "or_cdef_frame": (C.c_int, [_P] * 7 + [C.POINTER(abi.CdefParams), C.POINTER(abi.CdefDecision)] + [_P] * 6),
             "or_weighted_sse": (C.c_float, [_P, C.c_int32, C.c_int32]),
             "or_cdef_frame_lambda": (C.c_float, [C.c_int32] * 4),
+            "or_loop_filter_levels": (None, [C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 3),
+            "or_deblock_frame": (C.c_int, [_P] * 9 + [C.POINTER(abi.DeblockFrameParams)] + [C.c_int32] * 3),
             "or_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
@@ -199,3 +201,22 @@ def cdef_frame(recon, src, skip8, prm):
     dec = {"bits": d.bits, "damping": d.damping, "unit_cols": d.unit_cols, "unit_rows": d.unit_rows,
            "strengths": [tuple(d.strengths[e]) for e in range(d.n_strengths)], "grid": grid}
     return out, dec, {"luma": tabs[0], "u": tabs[1], "v": tabs[2], "dirs": dirs, "vars": vars_}
+
+
+def loop_filter_levels(base_q_idx, sub):
+    a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
+    load().or_loop_filter_levels(base_q_idx, sub, C.byref(a), C.byref(b), C.byref(c))
+    return a.value, b.value, c.value
+
+
+def deblock_frame(planes, disp_w, disp_h, sub_x, sub_y, tx_maps, pred_maps, lvl_y, lvl_u, lvl_v, mono=False):
+    out = [np.array(x, dtype=np.uint16, copy=True, order="C") for x in planes]
+    g = abi.DeblockFrameParams()
+    g.w8, g.h8 = out[0].shape[1], out[0].shape[0]
+    g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = disp_w, disp_h, sub_x, sub_y, int(mono), 8
+    tm = [np.ascontiguousarray(m, np.uint8) for m in tx_maps]
+    pm = [np.ascontiguousarray(m, np.uint8) for m in pred_maps]
+    ch = (lambda i: None) if mono else (lambda i: p(out[i]))
+    assert load().or_deblock_frame(p(out[0]), ch(1), ch(2), *[p(m) for m in tm], *[p(m) for m in pm], C.byref(g),
+                                   lvl_y, lvl_u, lvl_v) == 0
+    return out

@@ -178,3 +178,44 @@ def test_deblock_1080p_device_entry(mt_lib, oracle_lib, cuda, luma):
     assert rc == abi.MT_OK
     got = d_px.cpu().numpy().view(np.uint16)
     assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("q,sub,want", [(70, 2, (8, 4, 7)), (255, 0, (31, 25, 7)), (5, 2, (0, 0, 7)), (9, 2, (1, 1, 7)),
+                                        (120, 1, (15, 12, 7)), (0, 0, (0, 0, 7))])
+def test_loop_filter_levels_known_answers(mt_lib, oracle_lib, q, sub, want):
+    """src/obu.rs:306-334: luma round(q/8) (max 40); chroma round((q/10) x 0.5
+    in 4:2:0, x 1 otherwise), at least 1 while luma filters (max 32)."""
+    sx, sy = (1, 1) if sub == 2 else ((1, 0) if sub == 1 else (0, 0))
+    assert mt_lib.loop_filter_levels(q, sx, sy) == want
+    assert oracle_lib.loop_filter_levels(q, sub) == want
+
+
+def test_loop_filter_levels_all_q_match_oracle(mt_lib, oracle_lib):
+    for q in range(256):
+        for sx, sy in ((0, 0), (1, 0), (1, 1)):
+            assert mt_lib.loop_filter_levels(q, sx, sy) == oracle_lib.loop_filter_levels(q, sx + sy)
+
+
+def _frame_inputs(disp_w, disp_h, sx, sy, mono, seed):
+    w8, h8 = (disp_w + 7) & ~7, (disp_h + 7) & ~7
+    pw, ph, pv, pt, bid = synth.partition_maps(w8 // 4, h8 // 4, seed)
+    tx = synth.transform_maps(pw, ph, bid, seed + 1)
+    planes = [synth.blocky_plane(w8, h8, bid, seed)]
+    if not mono:
+        cb = bid[::1 << sy, ::1 << sx]
+        planes += [synth.blocky_plane(w8 >> sx, h8 >> sy, cb, seed + 2), synth.blocky_plane(w8 >> sx, h8 >> sy, cb, seed + 3)]
+    return planes, tx, (pw, ph)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("disp_w,disp_h,sx,sy,mono,q", [
+    (64, 64, 1, 1, False, 70), (203, 117, 1, 1, False, 180), (130, 90, 1, 0, False, 120), (97, 131, 0, 0, False, 255),
+    (150, 70, 1, 1, True, 100), (1920, 1080, 1, 1, False, 70)])
+def test_deblock_frame_matches_oracle(mt_lib, oracle_lib, cuda, disp_w, disp_h, sx, sy, mono, q):
+    planes, tx, pred = _frame_inputs(disp_w, disp_h, sx, sy, mono, disp_w + q)
+    ly, luv, _ = mt_lib.loop_filter_levels(q, sx, sy)
+    want = oracle_lib.deblock_frame(planes, disp_w, disp_h, sx, sy, tx, pred, ly, luv, luv, mono)
+    got = mt_lib.deblock_frame(planes, disp_w, disp_h, sx, sy, tx, pred, ly, luv, luv, mono)
+    for a, b, c in zip(got, want, planes):
+        assert np.array_equal(a, b)
+        assert not np.array_equal(b, c)
