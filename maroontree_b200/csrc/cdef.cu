@@ -732,31 +732,56 @@ void decide(const mt_cdef_params* p, const Geo& g, const int64_t* ltab, const in
     total_off += d_off[u];
   }
   const size_t n_pairs = nl * nc;
-  auto d_pair = [&](size_t pp, int u) { return ly[(pp / nc) * nu + u] + lc[(pp % nc) * nu + u]; };
+  // d_pair(p, u) for every pair, row-major by pair (n_pairs x nu).
+  std::vector<int64_t> dp(n_pairs * nu);
+  for (size_t pp = 0; pp < n_pairs; pp++) {
+    const int64_t* a = &ly[(pp / nc) * nu];
+    const int64_t* b = &lc[(pp % nc) * nu];
+    int64_t* r = &dp[pp * nu];
+    for (int u = 0; u < nu; u++) r[u] = a[u] + b[u];
+  }
+  auto d_pair = [&](size_t pp, int u) { return dp[pp * nu + u]; };
+  // Units that never signal contribute d_off whatever the entry.
+  std::vector<int> sig_units;
+  int64_t unsig_off = 0;
+  for (int u = 0; u < nu; u++) {
+    if (signaled[u])
+      sig_units.push_back(u);
+    else
+      unsig_off += d_off[u];
+  }
   size_t global_entry = 0;
   int64_t prefix[4] = {INT64_MAX, INT64_MAX, INT64_MAX, INT64_MAX};
   for (size_t pp = 0; pp < n_pairs; pp++) {
-    int64_t t = 0;
-    for (int u = 0; u < nu; u++) t += signaled[u] ? d_pair(pp, u) : d_off[u];
+    const int64_t* r = &dp[pp * nu];
+    int64_t t = unsig_off;
+    for (int u : sig_units) t += r[u];
     if (t < prefix[0]) {
       prefix[0] = t;
       global_entry = pp;
     }
   }
-  std::vector<int64_t> cur_min = d_off;
+  // Greedy set construction on the signalled units (compacted copies).
+  const size_t ns = sig_units.size();
+  std::vector<int64_t> cm(ns), th(ns), off(ns), dps(n_pairs * ns);
+  for (size_t k = 0; k < ns; k++) {
+    const int u = sig_units[k];
+    cm[k] = d_off[u];
+    th[k] = thr[u];
+    off[k] = d_off[u];
+  }
+  for (size_t pp = 0; pp < n_pairs; pp++)
+    for (size_t k = 0; k < ns; k++) dps[pp * ns + k] = dp[pp * nu + sig_units[k]];
   std::vector<size_t> entries = {0};
   while (entries.size() < 8) {
     size_t best_p = 0;
     int64_t best_tot = INT64_MAX;
     for (size_t pp = 0; pp < n_pairs; pp++) {
-      int64_t tot = 0;
-      for (int u = 0; u < nu; u++) {
-        if (!signaled[u]) {
-          tot += d_off[u];
-          continue;
-        }
-        const int64_t b = std::min(cur_min[u], d_pair(pp, u));
-        tot += b >= thr[u] ? d_off[u] : b;
+      const int64_t* r = &dps[pp * ns];
+      int64_t tot = unsig_off;
+      for (size_t k = 0; k < ns; k++) {
+        const int64_t b = cm[k] < r[k] ? cm[k] : r[k];
+        tot += b >= th[k] ? off[k] : b;
       }
       if (tot < best_tot) {
         best_tot = tot;
@@ -764,7 +789,8 @@ void decide(const mt_cdef_params* p, const Geo& g, const int64_t* ltab, const in
       }
     }
     entries.push_back(best_p);
-    for (int u = 0; u < nu; u++) cur_min[u] = std::min(cur_min[u], d_pair(best_p, u));
+    const int64_t* r = &dps[best_p * ns];
+    for (size_t k = 0; k < ns; k++) cm[k] = std::min(cm[k], r[k]);
     const size_t n = entries.size();
     if ((n & (n - 1)) == 0) prefix[__builtin_ctzll(n)] = best_tot;
   }

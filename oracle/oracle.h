@@ -52,6 +52,10 @@ float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int
                          const mt_coef_cdfs* cdfs, int32_t skip_ctx, int32_t dcs_ctx,
                          int32_t y_mode, int32_t txtp, int32_t use_skip_bits,
                          const float* skip_bits);
+/* rate.rs:149 real_block_bits_bounded for any w x h (txtp_mode < 0: no txtp symbol). */
+float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
+                            const mt_coef_cdfs* cdfs, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
+                            int32_t txtp, int32_t use_skip_bits, const float* skip_bits);
 /* rate.rs:58 CoefCostTables::build and the other per-symbol costs. */
 void or_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
 /* The candidate chain of partition_search.rs:467-530, per candidate. */

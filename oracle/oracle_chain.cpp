@@ -933,13 +933,15 @@ float hi_tok_cost(uint32_t m, const uint16_t* br) {
 
 extern "C" {
 
-// rate.rs:149-291 real_block_bits_bounded for a square w == h luma block, with
-// the CDF costs evaluated directly (the CoefCostTables cache at rate.rs:58-80
-// holds the same values).
-float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int32_t cls,
-                         const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t y_mode,
-                         int32_t txtp, int32_t use_skip_bits, const float* skip_bits) {
-  const int N = n * n;
+// rate.rs:149-291 real_block_bits_bounded (bound = +inf) for a w x h block,
+// with the CDF costs evaluated directly (the CoefCostTables cache at
+// rate.rs:58-80 holds the same values).  txtp_mode < 0: no transform-type
+// symbol (chroma, TX_32X32).  Contexts: the square, w < h or w > h lo-context
+// offset table (src/tables.rs:354-360, :456-472).
+float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
+                            const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
+                            int32_t txtp, int32_t use_skip_bits, const float* skip_bits) {
+  const int N = w * h;
   int eob = -1;
   for (int i = N - 1; i >= 0; i--)
     if (cf[scan[i]] != 0) {
@@ -948,7 +950,7 @@ float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int
     }
   if (eob < 0) return use_skip_bits ? skip_bits[0] : or_cdf_cost(c->txb_skip[skip_ctx], 1);
   float bits = use_skip_bits ? skip_bits[1] : or_cdf_cost(c->txb_skip[skip_ctx], 0);
-  if (cls < 3) bits += or_cdf_cost(c->txtp[y_mode], txtp);  // TX_32X32 codes no txtp
+  if (txtp_mode >= 0) bits += or_cdf_cost(c->txtp[txtp_mode], txtp);
   const uint16_t* dc_sign = c->dc_sign[dcs_ctx];
   if (eob == 0) {
     uint32_t m = uabs(cf[0]);
@@ -966,15 +968,19 @@ float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int
     bits += or_cdf_cost(c->eob_hi[eob_bin], (eob >> nbits) & 1);
     bits += (float)nbits;
   }
-  const int h = n, stride = h;
+  static const uint8_t kOffWlh[25] = {0, 11, 11, 11, 11, 11, 11, 11, 11, 11, 6, 6, 21,
+                                        21, 21, 6, 21, 21, 21, 21, 21, 21, 21, 21, 21};
+  static const uint8_t kOffWgh[25] = {0, 16, 6, 6, 21, 16, 16, 6, 21, 21, 16, 16, 21,
+                                        21, 21, 16, 16, 21, 21, 21, 16, 16, 21, 21, 21};
+  const int stride = h;
   const int log2h = __builtin_ctz((unsigned)h);
-  std::vector<uint8_t> levels((size_t)(n + 2) * (n + 2), 0);
+  std::vector<uint8_t> levels((size_t)(w + 2) * (h + 2), 0);
   auto lo_ctx = [&](int x, int y, uint32_t* hi_mag) -> int {
     auto g = [&](int dx, int dy) -> uint32_t { return levels[(size_t)(x + dx) * stride + (y + dy)]; };
     uint32_t hm = g(0, 1) + g(1, 0) + g(1, 1);
     uint32_t mag = hm + g(0, 2) + g(2, 0);
     int yy = y < 4 ? y : 4, xx = x < 4 ? x : 4;
-    int off = MT_LO_CTX_OFF[yy * 5 + xx];
+    int off = w < h ? kOffWlh[yy * 5 + xx] : (w > h ? kOffWgh[yy * 5 + xx] : MT_LO_CTX_OFF[yy * 5 + xx]);
     *hi_mag = hm;
     return off + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
   };
@@ -1036,6 +1042,14 @@ float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int
   if (cf[0] != 0) bits += or_cdf_cost(dc_sign, cf[0] < 0 ? 1 : 0);
   for (int k = 0; k < ac_nonzero; k++) bits += 1.0f;
   return bits;
+}
+
+// The square luma form the candidate chain prices (TX_32X32 codes no txtp).
+float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int32_t cls,
+                         const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t y_mode,
+                         int32_t txtp, int32_t use_skip_bits, const float* skip_bits) {
+  return or_real_block_bits_wh(cf, scan, n, n, c, skip_ctx, dcs_ctx, cls < 3 ? y_mode : -1, txtp, use_skip_bits,
+                               skip_bits);
 }
 
 // rate.rs:58-80 CoefCostTables::build plus the per-symbol costs of the other

@@ -44,6 +44,8 @@ def load():
             "or_cdef_frame_lambda": (C.c_float, [C.c_int32] * 4),
             "or_loop_filter_levels": (None, [C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 3),
             "or_deblock_frame": (C.c_int, [_P] * 9 + [C.POINTER(abi.DeblockFrameParams)] + [C.c_int32] * 3),
+            "or_real_block_bits_wh": (C.c_float, [_P, _P, C.c_int32, C.c_int32, C.POINTER(abi.CoefCdfs)] +
+                                      [C.c_int32] * 5 + [_P]),
             "or_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
@@ -220,3 +222,11 @@ def deblock_frame(planes, disp_w, disp_h, sub_x, sub_y, tx_maps, pred_maps, lvl_
     assert load().or_deblock_frame(p(out[0]), ch(1), ch(2), *[p(m) for m in tm], *[p(m) for m in pm], C.byref(g),
                                    lvl_y, lvl_u, lvl_v) == 0
     return out
+
+
+def real_block_bits_wh(cf, scan, w, h, cdfs, skip_ctx, dcs_ctx, txtp_mode=-1, txtp=0, skip_bits=None):
+    cf = np.ascontiguousarray(cf, np.int32)
+    scan = np.ascontiguousarray(scan, np.uint16)
+    sb = None if skip_bits is None else np.ascontiguousarray(skip_bits, np.float32)
+    return load().or_real_block_bits_wh(p(cf), p(scan), w, h, C.byref(cdfs), skip_ctx, dcs_ctx, txtp_mode, txtp,
+                                        int(sb is not None), None if sb is None else p(sb))
