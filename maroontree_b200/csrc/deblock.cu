@@ -48,78 +48,124 @@ __host__ __device__ inline LfLimits lf_limits(int level, int sharp) {
 
 __device__ __forceinline__ int clip3(int v, int lo, int hi) { return max(lo, min(v, hi)); }
 
-// One line of the filter across an edge at dst[0] (samples dst[k * sb]).
-__device__ __forceinline__ void lf_line(uint16_t* __restrict__ dst, long sb, const LfLimits L, int wd, int bd) {
+// One line of the filter across an edge (src/loopfilter.rs:98-292): v[7 + k]
+// holds the sample k places past the edge (v[6] = p0, v[7] = q0); WD is the
+// filter width, so only v[7 - reach .. 7 + reach) is read.
+template <int WD>
+__device__ __forceinline__ void lf_core(int (&v)[14], const LfLimits L, int bd) {
   const int bm8 = bd - 8;
   const int f_flat = 1 << bm8;
   const int e = L.e << bm8, il = L.i << bm8, ht = L.h << bm8;
   const int px_max = (1 << bd) - 1;
   const int clip_lo = -128 * (1 << bm8), clip_hi = 128 * (1 << bm8) - 1;
-  auto g = [&](int k) -> int { return dst[k * sb]; };
-  auto put = [&](int k, int v) { dst[k * sb] = (uint16_t)v; };
-  const int p1 = g(-2), p0 = g(-1), q0 = g(0), q1 = g(1);
+  const int p1 = v[5], p0 = v[6], q0 = v[7], q1 = v[8];
   bool fm = abs(p1 - p0) <= il && abs(q1 - q0) <= il && abs(p0 - q0) * 2 + (abs(p1 - q1) >> 1) <= e;
   int p2 = 0, q2 = 0, p3 = 0, q3 = 0;
-  if (wd > 4) {
-    p2 = g(-3);
-    q2 = g(2);
+  if (WD > 4) {
+    p2 = v[4];
+    q2 = v[9];
     fm = fm && abs(p2 - p1) <= il && abs(q2 - q1) <= il;
-    if (wd > 6) {
-      p3 = g(-4);
-      q3 = g(3);
+    if (WD > 6) {
+      p3 = v[3];
+      q3 = v[10];
       fm = fm && abs(p3 - p2) <= il && abs(q3 - q2) <= il;
     }
   }
   if (!fm) return;
   bool flat8in = false;
-  if (wd >= 6)
+  if (WD >= 6)
     flat8in = abs(p2 - p0) <= f_flat && abs(p1 - p0) <= f_flat && abs(q1 - q0) <= f_flat && abs(q2 - q0) <= f_flat;
-  if (wd >= 8) flat8in = flat8in && abs(p3 - p0) <= f_flat && abs(q3 - q0) <= f_flat;
-  if (wd >= 16 && flat8in) {
-    const int p6 = g(-7), p5 = g(-6), p4 = g(-5), q4 = g(4), q5 = g(5), q6 = g(6);
+  if (WD >= 8) flat8in = flat8in && abs(p3 - p0) <= f_flat && abs(q3 - q0) <= f_flat;
+  if (WD >= 16 && flat8in) {
+    const int p6 = v[0], p5 = v[1], p4 = v[2], q4 = v[11], q5 = v[12], q6 = v[13];
     const bool flat8out = abs(p6 - p0) <= f_flat && abs(p5 - p0) <= f_flat && abs(p4 - p0) <= f_flat &&
                           abs(q4 - q0) <= f_flat && abs(q5 - q0) <= f_flat && abs(q6 - q0) <= f_flat;
     if (flat8out) {
-      put(-6, (p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8) >> 4);
-      put(-5, (p6 * 5 + p5 * 2 + p4 * 2 + p3 * 2 + p2 + p1 + p0 + q0 + q1 + 8) >> 4);
-      put(-4, (p6 * 4 + p5 + p4 * 2 + p3 * 2 + p2 * 2 + p1 + p0 + q0 + q1 + q2 + 8) >> 4);
-      put(-3, (p6 * 3 + p5 + p4 + p3 * 2 + p2 * 2 + p1 * 2 + p0 + q0 + q1 + q2 + q3 + 8) >> 4);
-      put(-2, (p6 * 2 + p5 + p4 + p3 + p2 * 2 + p1 * 2 + p0 * 2 + q0 + q1 + q2 + q3 + q4 + 8) >> 4);
-      put(-1, (p6 + p5 + p4 + p3 + p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + q2 + q3 + q4 + q5 + 8) >> 4);
-      put(0, (p5 + p4 + p3 + p2 + p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + q3 + q4 + q5 + q6 + 8) >> 4);
-      put(1, (p4 + p3 + p2 + p1 + p0 + q0 * 2 + q1 * 2 + q2 * 2 + q3 + q4 + q5 + q6 + q6 + 8) >> 4);
-      put(2, (p3 + p2 + p1 + p0 + q0 + q1 * 2 + q2 * 2 + q3 * 2 + q4 + q5 + q6 + q6 + q6 + 8) >> 4);
-      put(3, (p2 + p1 + p0 + q0 + q1 + q2 * 2 + q3 * 2 + q4 * 2 + q5 + q6 + q6 + q6 + q6 + 8) >> 4);
-      put(4, (p1 + p0 + q0 + q1 + q2 + q3 * 2 + q4 * 2 + q5 * 2 + q6 * 5 + 8) >> 4);
-      put(5, (p0 + q0 + q1 + q2 + q3 + q4 * 2 + q5 * 2 + q6 * 7 + 8) >> 4);
+      v[1] = (p6 * 7 + p5 * 2 + p4 * 2 + p3 + p2 + p1 + p0 + q0 + 8) >> 4;
+      v[2] = (p6 * 5 + p5 * 2 + p4 * 2 + p3 * 2 + p2 + p1 + p0 + q0 + q1 + 8) >> 4;
+      v[3] = (p6 * 4 + p5 + p4 * 2 + p3 * 2 + p2 * 2 + p1 + p0 + q0 + q1 + q2 + 8) >> 4;
+      v[4] = (p6 * 3 + p5 + p4 + p3 * 2 + p2 * 2 + p1 * 2 + p0 + q0 + q1 + q2 + q3 + 8) >> 4;
+      v[5] = (p6 * 2 + p5 + p4 + p3 + p2 * 2 + p1 * 2 + p0 * 2 + q0 + q1 + q2 + q3 + q4 + 8) >> 4;
+      v[6] = (p6 + p5 + p4 + p3 + p2 + p1 * 2 + p0 * 2 + q0 * 2 + q1 + q2 + q3 + q4 + q5 + 8) >> 4;
+      v[7] = (p5 + p4 + p3 + p2 + p1 + p0 * 2 + q0 * 2 + q1 * 2 + q2 + q3 + q4 + q5 + q6 + 8) >> 4;
+      v[8] = (p4 + p3 + p2 + p1 + p0 + q0 * 2 + q1 * 2 + q2 * 2 + q3 + q4 + q5 + q6 + q6 + 8) >> 4;
+      v[9] = (p3 + p2 + p1 + p0 + q0 + q1 * 2 + q2 * 2 + q3 * 2 + q4 + q5 + q6 + q6 + q6 + 8) >> 4;
+      v[10] = (p2 + p1 + p0 + q0 + q1 + q2 * 2 + q3 * 2 + q4 * 2 + q5 + q6 + q6 + q6 + q6 + 8) >> 4;
+      v[11] = (p1 + p0 + q0 + q1 + q2 + q3 * 2 + q4 * 2 + q5 * 2 + q6 * 5 + 8) >> 4;
+      v[12] = (p0 + q0 + q1 + q2 + q3 + q4 * 2 + q5 * 2 + q6 * 7 + 8) >> 4;
       return;
     }
   }
-  if (wd >= 8 && flat8in) {
-    put(-3, (p3 * 3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3);
-    put(-2, (p3 * 2 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3);
-    put(-1, (p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3);
-    put(0, (p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3);
-    put(1, (p1 + p0 + q0 + 2 * q1 + q2 + q3 + q3 + 4) >> 3);
-    put(2, (p0 + q0 + q1 + 2 * q2 + q3 + q3 + q3 + 4) >> 3);
-  } else if (wd == 6 && flat8in) {
-    put(-2, (p2 * 3 + 2 * p1 + 2 * p0 + q0 + 4) >> 3);
-    put(-1, (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3);
-    put(0, (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3);
-    put(1, (p0 + 2 * q0 + 2 * q1 + 2 * q2 + q2 + 4) >> 3);
+  if (WD >= 8 && flat8in) {
+    v[4] = (p3 * 3 + 2 * p2 + p1 + p0 + q0 + 4) >> 3;
+    v[5] = (p3 * 2 + p2 + 2 * p1 + p0 + q0 + q1 + 4) >> 3;
+    v[6] = (p3 + p2 + p1 + 2 * p0 + q0 + q1 + q2 + 4) >> 3;
+    v[7] = (p2 + p1 + p0 + 2 * q0 + q1 + q2 + q3 + 4) >> 3;
+    v[8] = (p1 + p0 + q0 + 2 * q1 + q2 + q3 + q3 + 4) >> 3;
+    v[9] = (p0 + q0 + q1 + 2 * q2 + q3 + q3 + q3 + 4) >> 3;
+  } else if (WD == 6 && flat8in) {
+    v[5] = (p2 * 3 + 2 * p1 + 2 * p0 + q0 + 4) >> 3;
+    v[6] = (p2 + 2 * p1 + 2 * p0 + 2 * q0 + q1 + 4) >> 3;
+    v[7] = (p1 + 2 * p0 + 2 * q0 + 2 * q1 + q2 + 4) >> 3;
+    v[8] = (p0 + 2 * q0 + 2 * q1 + 2 * q2 + q2 + 4) >> 3;
   } else {
     const bool hev = abs(p1 - p0) > ht || abs(q1 - q0) > ht;
     int fv = hev ? clip3(p1 - q1, clip_lo, clip_hi) : 0;
     fv = clip3(3 * (q0 - p0) + fv, clip_lo, clip_hi);
     const int f1 = min(fv + 4, clip_hi) >> 3;
     const int f2 = min(fv + 3, clip_hi) >> 3;
-    put(-1, clip3(p0 + f2, 0, px_max));
-    put(0, clip3(q0 - f1, 0, px_max));
+    v[6] = clip3(p0 + f2, 0, px_max);
+    v[7] = clip3(q0 - f1, 0, px_max);
     if (!hev) {
       const int f = (f1 + 1) >> 1;
-      put(-2, clip3(p1 + f, 0, px_max));
-      put(1, clip3(q1 - f, 0, px_max));
+      v[5] = clip3(p1 + f, 0, px_max);
+      v[8] = clip3(q1 - f, 0, px_max);
     }
+  }
+}
+
+// Samples a filter of width WD reads / writes on each side: reads
+// [7 - RLO, 7 + RHI], writes [7 - WLO, 7 + WHI].
+template <int WD> struct Reach;
+template <> struct Reach<4> { static constexpr int RLO = 2, RHI = 1, WLO = 2, WHI = 1; };
+template <> struct Reach<6> { static constexpr int RLO = 3, RHI = 2, WLO = 2, WHI = 1; };
+template <> struct Reach<8> { static constexpr int RLO = 4, RHI = 3, WLO = 3, WHI = 2; };
+template <> struct Reach<16> { static constexpr int RLO = 7, RHI = 6, WLO = 6, WHI = 5; };
+
+// One line across a vertical edge at row[x0] (samples contiguous).
+template <int WD>
+__device__ __forceinline__ void lf_row(uint16_t* __restrict__ row, const LfLimits L, int bd) {
+  using R = Reach<WD>;
+  int v[14];
+#pragma unroll
+  for (int k = -R::RLO; k <= R::RHI; k++) v[7 + k] = row[k];
+  lf_core<WD>(v, L, bd);
+#pragma unroll
+  for (int k = -R::WLO; k <= R::WHI; k++) row[k] = (uint16_t)v[7 + k];
+}
+
+// Four columns (x0 .. x0 + 3) across a horizontal edge at row y0: 8-byte row
+// loads and stores (col points at sample (x0, y0), 8-byte aligned).
+template <int WD>
+__device__ __forceinline__ void lf_cols4(uint16_t* __restrict__ col, long stride, const LfLimits L, int bd) {
+  using R = Reach<WD>;
+  int v[4][14];
+#pragma unroll
+  for (int k = -R::RLO; k <= R::RHI; k++) {
+    const uint2 q = *reinterpret_cast<const uint2*>(col + k * stride);
+    v[0][7 + k] = q.x & 0xffff;
+    v[1][7 + k] = q.x >> 16;
+    v[2][7 + k] = q.y & 0xffff;
+    v[3][7 + k] = q.y >> 16;
+  }
+#pragma unroll
+  for (int l = 0; l < 4; l++) lf_core<WD>(v[l], L, bd);
+#pragma unroll
+  for (int k = -R::WLO; k <= R::WHI; k++) {
+    uint2 q;
+    q.x = (unsigned)v[0][7 + k] | ((unsigned)v[1][7 + k] << 16);
+    q.y = (unsigned)v[2][7 + k] | ((unsigned)v[3][7 + k] << 16);
+    *reinterpret_cast<uint2*>(col + k * stride) = q;
   }
 }
 
@@ -199,43 +245,41 @@ __device__ __forceinline__ bool involved_at(const EdgeLine& e, int i, int wd) {
   return false;
 }
 
-// Filters the line across edge i of e (and, when i heads a run of
-// overlapping edges, the rest of the run in order).  line0 points at the
-// line's sample at along-position 0; stride is the along-line sample stride.
-__device__ __forceinline__ void filter_edge_line(const EdgeLine& e, int i, uint16_t* __restrict__ line0, long stride,
-                                                 const LfLimits L, int bd) {
+// Is the edge at cell i filtered by this thread, and which edges follow it?
+// Returns the width of edge i when this thread owns it (0 otherwise); *run is
+// set when i heads a run of edges whose taps overlap (the thread then filters
+// the whole run in order, see run_next).
+__device__ __forceinline__ int own_edge(const EdgeLine& e, int i, bool* run) {
   EdgeWindow w;
 #pragma unroll
   for (int d = -6; d <= 3; d++) w.wd[d + 6] = edge_wd(e, i + d);
   const int wd = w.at(0);
-  if (!wd) return;
-  if (!window_involved(w, i, 0)) {
-    lf_line(line0 + (long)4 * i * stride, stride, L, wd, bd);
-    return;
-  }
+  *run = false;
+  if (!wd) return 0;
+  if (!window_involved(w, i, 0)) return wd;
   // Part of a run: only the run's first edge proceeds.
+#pragma unroll
   for (int d = -1; d >= -3; d--) {
     if (w.at(d)) {
-      if (window_involved(w, i, d)) return;
+      if (window_involved(w, i, d)) return 0;
       break;
     }
   }
-  int cur = i, cw = wd;
-  while (true) {
-    lf_line(line0 + (long)4 * cur * stride, stride, L, cw, bd);
-    int nxt = 0, nw = 0;
-    for (int k = cur + 1; k <= cur + 3; k++) {
-      const int wk = edge_wd(e, k);
-      if (wk) {
-        nxt = k;
-        nw = wk;
-        break;
-      }
+  *run = true;
+  return wd;
+}
+
+// The edge after cur in its run, or 0 (with its width in *nw).
+__device__ __forceinline__ int run_next(const EdgeLine& e, int cur, int* nw) {
+  for (int k = cur + 1; k <= cur + 3; k++) {
+    const int wk = edge_wd(e, k);
+    if (wk) {
+      *nw = involved_at(e, k, wk) ? wk : 0;
+      return *nw ? k : 0;
     }
-    if (!nw || !involved_at(e, nxt, nw)) return;
-    cur = nxt;
-    cw = nw;
   }
+  *nw = 0;
+  return 0;
 }
 
 struct PlaneArgs {
@@ -243,24 +287,70 @@ struct PlaneArgs {
   LfLimits L;
 };
 
-// Vertical edges: thread (sample row y, edge column c4).
-__global__ void lf_vert_kernel(uint16_t* __restrict__ px, PlaneArgs a, const uint8_t* __restrict__ bw4,
-                               const uint8_t* __restrict__ vedge4) {
-  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = blockIdx.y;
-  if (c4 >= a.w4) return;
-  const EdgeLine e{bw4, vedge4, (long)(y >> 2) * a.nc4, 1, a.w4, a.w, a.luma != 0};
-  filter_edge_line(e, c4, px + (size_t)y * a.w, 1, a.L, a.bd);
+__device__ __forceinline__ void vert_cell(uint16_t* __restrict__ px, const PlaneArgs& a, int r4, int c4, int wd) {
+  uint16_t* base = px + (size_t)(r4 * 4) * a.w + c4 * 4;
+#pragma unroll 1
+  for (int l = 0; l < 4; l++) {
+    uint16_t* row = base + (size_t)l * a.w;
+    switch (wd) {
+      case 4: lf_row<4>(row, a.L, a.bd); break;
+      case 6: lf_row<6>(row, a.L, a.bd); break;
+      case 8: lf_row<8>(row, a.L, a.bd); break;
+      default: lf_row<16>(row, a.L, a.bd); break;
+    }
+  }
 }
 
-// Horizontal edges: thread (sample column x, edge row r4).
-__global__ void lf_horz_kernel(uint16_t* __restrict__ px, PlaneArgs a, const uint8_t* __restrict__ bh4,
-                               const uint8_t* __restrict__ hedge4) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void horz_cell(uint16_t* __restrict__ px, const PlaneArgs& a, int r4, int c4, int wd) {
+  uint16_t* col = px + (size_t)(r4 * 4) * a.w + c4 * 4;
+  switch (wd) {
+    case 4: lf_cols4<4>(col, a.w, a.L, a.bd); break;
+    case 6: lf_cols4<6>(col, a.w, a.L, a.bd); break;
+    case 8: lf_cols4<8>(col, a.w, a.L, a.bd); break;
+    default: lf_cols4<16>(col, a.w, a.L, a.bd); break;
+  }
+}
+
+// Vertical edges: one thread per 4x4 cell (edge column c4, cell row r4),
+// filtering the cell's four rows.
+__global__ void __launch_bounds__(128) lf_vert_kernel(uint16_t* __restrict__ px, PlaneArgs a,
+                                                      const uint8_t* __restrict__ bw4,
+                                                      const uint8_t* __restrict__ vedge4) {
+  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
   const int r4 = blockIdx.y;
-  if (x >= a.w4 * 4) return;
-  const EdgeLine e{bh4, hedge4, (long)(x >> 2), a.nc4, a.h4, a.h, a.luma != 0};
-  filter_edge_line(e, r4, px + x, a.w, a.L, a.bd);
+  if (c4 >= a.w4) return;
+  const EdgeLine e{bw4, vedge4, (long)r4 * a.nc4, 1, a.w4, a.w, a.luma != 0};
+  bool run;
+  int wd = own_edge(e, c4, &run);
+  if (!wd) return;
+  int cur = c4;
+  while (true) {
+    vert_cell(px, a, r4, cur, wd);
+    if (!run) return;
+    cur = run_next(e, cur, &wd);
+    if (!cur) return;
+  }
+}
+
+// Horizontal edges: one thread per 4x4 cell (cell column c4, edge row r4),
+// filtering the cell's four columns with 8-byte row accesses.
+__global__ void __launch_bounds__(128) lf_horz_kernel(uint16_t* __restrict__ px, PlaneArgs a,
+                                                      const uint8_t* __restrict__ bh4,
+                                                      const uint8_t* __restrict__ hedge4) {
+  const int c4 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r4 = blockIdx.y;
+  if (c4 >= a.w4) return;
+  const EdgeLine e{bh4, hedge4, (long)c4, a.nc4, a.h4, a.h, a.luma != 0};
+  bool run;
+  int wd = own_edge(e, r4, &run);
+  if (!wd) return;
+  int cur = r4;
+  while (true) {
+    horz_cell(px, a, cur, c4, wd);
+    if (!run) return;
+    cur = run_next(e, cur, &wd);
+    if (!cur) return;
+  }
 }
 
 int check_plane(int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, int32_t nc4, int32_t level, int32_t sharp,
@@ -344,6 +434,7 @@ int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w,
   if (rc != MT_OK) return rc;
   if (level == 0) return MT_OK;
   if (!d_px || !d_bw4 || !d_bh4) return MT_ERR_INVALID_INPUT;
+  if (reinterpret_cast<uintptr_t>(d_px) & 7) return MT_ERR_INVALID_INPUT;  // 8-byte row accesses
   PlaneArgs a;
   a.w = w;
   a.h = h;
@@ -355,8 +446,8 @@ int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w,
   a.L = lf_limits(level, sharp);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int T = 128;
-  if (a.w4 > 1) lf_vert_kernel<<<dim3((a.w4 + T - 1) / T, a.h4 * 4), T, 0, st>>>(d_px, a, d_bw4, d_vedge4);
-  if (a.h4 > 1) lf_horz_kernel<<<dim3((a.w4 * 4 + T - 1) / T, a.h4), T, 0, st>>>(d_px, a, d_bh4, d_hedge4);
+  if (a.w4 > 1) lf_vert_kernel<<<dim3((a.w4 + T - 1) / T, a.h4), T, 0, st>>>(d_px, a, d_bw4, d_vedge4);
+  if (a.h4 > 1) lf_horz_kernel<<<dim3((a.w4 + T - 1) / T, a.h4), T, 0, st>>>(d_px, a, d_bh4, d_hedge4);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
