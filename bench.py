@@ -8,8 +8,15 @@ forward transform + quant + QM -> trellis -> inverse -> SATD distortion ->
 coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
 
   value  MPix/s of the device-resident launch (inputs already in HBM)
-  e2e    MPix/s through the public host C ABI (mt_candidate_chain): host
-         planes + candidate list copied in, results copied out, every step
+  e2e    MPix/s through the public host C ABI (mt_rdo_level8): host planes,
+         block and combo lists copied in, per-block winners copied out, every
+         step
+
+The line also carries ``frame_filters``: the frame-wide kernels of the same
+1080p 4:2:0 frame (colour conversion + padding, deblocking of the three
+planes, CDEF tables + strength search + apply) timed on the device with CUDA
+events after an L2 flush, with their algorithmic bytes against the measured
+HBM copy bandwidth.
 
 ``--impl reference`` times the CPU restatement of the reference (the oracle;
 the Rust reference cannot be built here) on all host cores over a bounded
@@ -157,6 +164,105 @@ def run_reference(args):
     return 0
 
 
+def measure_filters(dev, wl, hbm_peak, reps=5):
+    """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    lib = mt.load()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    t16 = lambda a: torch.from_numpy(np.ascontiguousarray(a).astype(np.int16)).to(dev)
+    t8 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.uint8)).to(dev)
+
+    def timed(fn, reset=None):
+        ms = []
+        for i in range(reps + 2):
+            if reset:
+                reset()
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            rc = fn()
+            b.record()
+            torch.cuda.synchronize()
+            assert rc == 0, rc
+            if i >= 2:
+                ms.append(a.elapsed_time(b))
+        return float(np.median(ms))
+
+    def entry(ms, nbytes, what):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return {"ms": round(ms, 4), "alg_bytes": int(nbytes), "achieved_gbs": round(gbs, 1),
+                "frac_hbm": round(gbs / hbm_peak, 4), "bytes": what}
+
+    out = {}
+    # colour conversion + padding (RGB -> padded Y / Cb / Cr)
+    pw, ph, pcw, pch = mt.padded_plane_dims(W, H, 2)
+    d_rgb = t8(wl["rgb"])
+    y = torch.empty((ph, pw), dtype=torch.int16, device=dev)
+    cb = torch.empty((pch, pcw), dtype=torch.int16, device=dev)
+    cr = torch.empty_like(cb)
+    ms = timed(lambda: lib.mt_csc_rgb8_device(d_rgb.data_ptr(), W, H, 2, y.data_ptr(), cb.data_ptr(), cr.data_ptr(),
+                                              None))
+    out["csc"] = entry(ms, W * H * 3 + (pw * ph + 2 * pcw * pch) * 2, "3 B/px in + 2 B per output sample")
+    # deblocking of the three planes (frame_deblock at the shipped levels)
+    pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
+    tx = synth.transform_maps(pwm, phm, bid, 8)
+    planes = [synth.blocky_plane(pw, ph, bid, 7), synth.blocky_plane(pcw, pch, bid[::2, ::2], 8),
+              synth.blocky_plane(pcw, pch, bid[::2, ::2], 9)]
+    d0 = [t16(p) for p in planes]
+    dp = [p.clone() for p in d0]
+    maps = [t8(m) for m in list(tx) + [pwm, phm]]
+    g = abi.DeblockFrameParams()
+    g.w8, g.h8, g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = pw, ph, W, H, 1, 1, 0, 8
+    scr = torch.empty(max(1, lib.mt_deblock_frame_scratch_bytes(C.byref(g))), dtype=torch.uint8, device=dev)
+    ly, luv, _ = mt.loop_filter_levels(QIDX, 1, 1)
+
+    def reset_db():
+        for a, b in zip(dp, d0):
+            a.copy_(b)
+
+    ms = timed(lambda: lib.mt_deblock_frame_device(*[p.data_ptr() for p in dp], *[m.data_ptr() for m in maps],
+                                                   C.byref(g), ly, luv, luv, scr.data_ptr(), None), reset_db)
+    samples = pw * ph + 2 * pcw * pch
+    out["deblock"] = entry(ms, 4 * samples, "2 B read + 2 B write per sample (3 planes, both edge directions)")
+    out["deblock"]["levels"] = [ly, luv, luv]
+    # CDEF: the table pass alone (device events) and the whole frame (host search inside)
+    src, rec, skip = synth.cdef_inputs(W, H, 1, 1, False, 3)
+    prm = mt.cdef_params(W, H, 1, 1, QIDX)
+    r0 = [t16(p) for p in rec]
+    rr = [p.clone() for p in r0]
+    ss = [t16(p) for p in src]
+    sk = t8(skip)
+    nb, nu = skip.size, ((prm.w8 + 63) // 64) * ((prm.h8 + 63) // 64)
+    dirs = torch.empty(nb, dtype=torch.uint8, device=dev)
+    vars_ = torch.empty(nb, dtype=torch.int32, device=dev)
+    tabs = [torch.empty((nu, 12), dtype=torch.int64, device=dev) for _ in range(3)]
+    ms_tab = timed(lambda: lib.mt_cdef_tables_device(*[p.data_ptr() for p in rr], *[p.data_ptr() for p in ss],
+                                                     sk.data_ptr(), C.byref(prm), dirs.data_ptr(), vars_.data_ptr(),
+                                                     *[t.data_ptr() for t in tabs], None))
+    cscr = torch.empty(lib.mt_cdef_scratch_bytes(C.byref(prm)), dtype=torch.uint8, device=dev)
+    dec = abi.CdefDecision()
+
+    def reset_cdef():
+        for a, b in zip(rr, r0):
+            a.copy_(b)
+
+    ms_frame = timed(lambda: lib.mt_cdef_frame_device(*[p.data_ptr() for p in rr], *[p.data_ptr() for p in ss],
+                                                      sk.data_ptr(), C.byref(prm), cscr.data_ptr(), C.byref(dec), None,
+                                                      None), reset_cdef)
+    out["cdef_tables"] = entry(ms_tab, 4 * samples, "2 B recon + 2 B source read per sample")
+    out["cdef_tables"]["bound"] = "issue (12 candidate filters + weighted SSE per sample)"
+    out["cdef_frame"] = entry(ms_frame, 6 * samples, "tables + apply: 2 B recon + 2 B source + 2 B write")
+    out["cdef_frame"]["cdef_bits"] = dec.bits
+    out["workload"] = "1920x1080 4:2:0, qindex 70; L2 flushed before each timed call"
+    return out
+
+
 def run_ours(args):
     import torch
     import maroontree_b200 as mt
@@ -241,6 +347,8 @@ def run_ours(args):
     issue_peak = ISSUE_PEAK_PER_CLK * clk_mhz * 1e6
     issue_rate = NCU_WARP_INSTS_PER_LAUNCH / (step_ms / 1e3)
 
+    filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import build as obuild
@@ -268,6 +376,7 @@ def run_ours(args):
         "issue_roofline": {"achieved_ginst_s": round(issue_rate / 1e9, 1),
                            "peak_ginst_s": round(issue_peak / 1e9, 1), "frac": round(issue_rate / issue_peak, 4),
                            "inst_per_launch": NCU_WARP_INSTS_PER_LAUNCH, "sm_clock_mhz": clk_mhz},
+        "frame_filters": filters,
         "gpu_launches": 2 * args.steps,  # level8_kernel + level8_finalize_kernel per step
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
