@@ -289,7 +289,7 @@ def run_ours(args):
     d_blocks, d_combos = t(blocks), t(combos)
     d_best = torch.empty(nb * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     d_res = torch.empty(n * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-    d_keys = torch.empty(nb * 8, dtype=torch.uint8, device=dev)
+    d_keys = torch.empty(mt.rdo_level8_scratch_bytes(nb, nc), dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 

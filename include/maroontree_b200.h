@@ -229,18 +229,25 @@ size_t mt_candidate_chain_scratch_bytes(int32_t n);
 /* One batched RDO level: every combo of every block (ncombos * nblocks chain
  * evaluations in one launch) and the per-block best.  Host form: host
  * buffers in and out; results_out (optional) receives all
- * ncombos * nblocks results, combo-major (index combo * nblocks + block). */
+ * ncombos * nblocks results, combo-major (index combo * nblocks + block).
+ * Consecutive combos with the same (mode, angle delta) share one prediction,
+ * so list each mode's transform types together.  At most MT_LEVEL_MAX_COMBOS
+ * combos (13 modes x 7 deltas x 16 types is 1456), else MT_ERR_TOO_LARGE. */
+#define MT_LEVEL_MAX_COMBOS 2048
 int mt_rdo_level8(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm,
                   const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
                   const mt_block8* blocks, int32_t nblocks, const mt_combo* combos,
                   int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out);
-/* Device form: d_results (ncombos * nblocks) and d_keys (nblocks * 8 bytes)
- * are caller-provided working storage; d_best receives the winners. */
+/* Device form: d_results (ncombos * nblocks records) and d_scratch
+ * (mt_rdo_level8_scratch_bytes: the per-block argmin keys, the run table and
+ * one 64-byte prediction per (mode, delta, block)) are caller-provided;
+ * d_best receives the winners. */
 int mt_rdo_level8_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                          const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
                          int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
-                         void* d_keys, void* stream);
+                         void* d_scratch, void* stream);
+size_t mt_rdo_level8_scratch_bytes(int32_t nblocks, int32_t ncombos);
 
 /* Allocation-free form of mt_rdo_level8_device.  No counterpart in the
  * reference: it exists for callers that cannot give this library device

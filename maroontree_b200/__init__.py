@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "rdo_level8_scratch_bytes", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
 ]
 
 
@@ -122,11 +122,16 @@ def rdo_level8(src, recon, prm, quant, qmrow, costs, blocks, combos, want_result
     return best, res
 
 
+def rdo_level8_scratch_bytes(nblocks, ncombos):
+    """Device working storage ``mt_rdo_level8_device`` needs."""
+    return load().mt_rdo_level8_scratch_bytes(nblocks, ncombos)
+
+
 def rdo_level8_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_blocks, nblocks, d_combos, ncombos, d_best,
-                      d_results, d_keys, stream=0):
+                      d_results, d_scratch, stream=0):
     _check(load().mt_rdo_level8_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
                                        ptr(d_costs), ptr(d_blocks), nblocks, ptr(d_combos), ncombos, ptr(d_best),
-                                       ptr(d_results), ptr(d_keys), stream or None), "mt_rdo_level8_device")
+                                       ptr(d_results), ptr(d_scratch), stream or None), "mt_rdo_level8_device")
 
 
 def padded_plane_dims(w, h, sub):

@@ -128,6 +128,7 @@ def _bind(lib):
                                     C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_rdo_level8_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
                                            _P, C.c_int32, _P, _P, _P, _P]),
+        "mt_rdo_level8_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
         "mt_rdo_level8_device_noalloc": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
                                                    C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_padded_plane_dims": (C.c_int, [C.c_int32, C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
@@ -173,7 +174,7 @@ def load():
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
-    "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
+    "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
     "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",

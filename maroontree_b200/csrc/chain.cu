@@ -31,6 +31,7 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kMinBlocks = MT_CHAIN_MIN_BLOCKS;
 constexpr int kBuckets = 1024;
+constexpr int kLevelMaxCombos = MT_LEVEL_MAX_COMBOS;
 
 __device__ __forceinline__ int bucket_of(const mt_candidate& c) {
   const int t = min((int)c.tx_type, 7), m = min((int)c.mode, 15), d = min(max(c.angle_delta + 3, 0), 7);
@@ -125,26 +126,36 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) chain8_kernel(const uint
   store_blocks(w, (1 << a.p.bd) - 1, lv_out, rec_out, (size_t)idx);
 }
 
-// Candidate (combo c, block b) for thread t: warps take 32 consecutive blocks
-// of one combo.
-__global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint16_t* __restrict__ src,
-                                                          const uint16_t* __restrict__ rec, ChainArgs a,
-                                                          const uint8_t* __restrict__ qm_row,
-                                                          const mt_coef_costs* __restrict__ costs,
-                                                          const mt_block8* __restrict__ blocks, int nblocks,
-                                                          const mt_combo* __restrict__ combos, int ncombos,
-                                                          mt_candidate_result* __restrict__ res,
-                                                          unsigned long long* __restrict__ best_key) {
-  __shared__ mt_coef_costs sC;
-  __shared__ uint8_t sQm[64];
-  __shared__ float sQs[64];
-  __shared__ float sLut[64];
-  stage_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
-  if (c >= ncombos) return;
-  const mt_block8& bk = blocks[b];
-  const mt_combo cb = combos[c];
+// A level runs in three kernels.  Consecutive combos that share (mode, angle
+// delta) form a run; the prediction depends on the run only, so
+//   level8_runs_kernel  finds the runs (one thread),
+//   level8_pred_kernel  predicts each (run, block) once into an 8-bit buffer
+//                       (64 B per item, L2-resident for a 1080p level),
+//   level8_kernel       evaluates the rest of every candidate chain: thread t
+//                       takes combo t / nblocks and block t % nblocks, so a
+//                       warp -- and nearly the whole device at any moment --
+//                       runs one transform type's code path over 32
+//                       consecutive blocks; the per-block argmin folds in
+//                       through a 64-bit atomicMin on (cost bits, combo).
+struct LevelRuns {
+  int nruns;
+  int16_t start[kLevelMaxCombos + 1];  // run r covers combos [start[r], start[r + 1])
+  int16_t run_of[kLevelMaxCombos];
+};
+
+__global__ void level8_runs_kernel(const mt_combo* __restrict__ combos, int ncombos, LevelRuns* __restrict__ runs) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int nr = 0;
+  for (int c = 0; c < ncombos; c++) {
+    if (c == 0 || combos[c].mode != combos[c - 1].mode || combos[c].angle_delta != combos[c - 1].angle_delta)
+      runs->start[nr++] = (int16_t)c;
+    runs->run_of[c] = (int16_t)(nr - 1);
+  }
+  runs->start[nr] = (int16_t)ncombos;
+  runs->nruns = nr;
+}
+
+__device__ __forceinline__ mt_candidate level_candidate(const mt_block8& bk, const mt_combo& cb) {
   mt_candidate cd;
   cd.px = bk.px;
   cd.py = bk.py;
@@ -156,6 +167,56 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint
   cd.skip_ctx = bk.skip_ctx;
   cd.reserved = 0;
   cd.mode_bits = cb.mode <= MT_PAETH_PRED ? bk.mode_bits[cb.mode] : 0.0f;
+  return cd;
+}
+
+// One (run, block) prediction per thread; items past the run count exit.
+__global__ void __launch_bounds__(kThreads) level8_pred_kernel(const uint16_t* __restrict__ rec, ChainArgs a,
+                                                               const mt_block8* __restrict__ blocks, int nblocks,
+                                                               const mt_combo* __restrict__ combos,
+                                                               const LevelRuns* __restrict__ runs,
+                                                               uint4* __restrict__ preds) {
+  const long long wi = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (wi >= (long long)runs->nruns * nblocks) return;
+  const int r = (int)(wi / nblocks), b = (int)(wi - (long long)r * nblocks);
+  mt_candidate cd = level_candidate(blocks[b], combos[runs->start[r]]);
+  cd.tx_type = 0;  // every check but the transform type's
+  if (!cand_ok(cd, a.p.frame_w, a.p.frame_h)) return;
+  int32_t store[kWork8Words];
+  Work8 w{store};
+  chain8_predict(rec, a.p, cd, w);
+  const int16_t* pr = w.pred();
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint32_t v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int o = k * 16 + j * 4;
+      v[j] = (uint32_t)(uint8_t)pr[o] | ((uint32_t)(uint8_t)pr[o + 1] << 8) | ((uint32_t)(uint8_t)pr[o + 2] << 16) |
+             ((uint32_t)(uint8_t)pr[o + 3] << 24);
+    }
+    preds[wi * 4 + k] = make_uint4(v[0], v[1], v[2], v[3]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint16_t* __restrict__ src, ChainArgs a,
+                                                          const uint8_t* __restrict__ qm_row,
+                                                          const mt_coef_costs* __restrict__ costs,
+                                                          const mt_block8* __restrict__ blocks, int nblocks,
+                                                          const mt_combo* __restrict__ combos, int ncombos,
+                                                          const LevelRuns* __restrict__ runs,
+                                                          const uint4* __restrict__ preds,
+                                                          mt_candidate_result* __restrict__ res,
+                                                          unsigned long long* __restrict__ best_key) {
+  __shared__ mt_coef_costs sC;
+  __shared__ uint8_t sQm[64];
+  __shared__ float sQs[64];
+  __shared__ float sLut[64];
+  stage_tables(costs, qm_row, a.has_qm, sC, sQm, sQs, sLut);
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
+  if (c >= ncombos) return;
+  const mt_candidate cd = level_candidate(blocks[b], combos[c]);
   const size_t slot = (size_t)c * nblocks + b;
   if (!cand_ok(cd, a.p.frame_w, a.p.frame_h)) {
     mt_candidate_result bad = {};
@@ -165,11 +226,25 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint
   }
   int32_t store[kWork8Words];
   Work8 w{store};
+  {
+    const uint4* pp = preds + ((size_t)runs->run_of[c] * nblocks + b) * 4;
+    int16_t* pr = w.pred();
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint4 q = pp[k];
+      const uint32_t v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) pr[k * 16 + j * 4 + i] = (int16_t)((v[j] >> (8 * i)) & 0xff);
+    }
+  }
   mt_candidate_result r;
-  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  chain8_tx(src, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[slot] = r;
   // Costs are non-negative finite floats, so their bit patterns order like
-  // the values; ties go to the lower combo index (evaluated first).
+  // the values; ties go to the lower combo index (evaluated first in the
+  // reference's loop).
   const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c;
   atomicMin(&best_key[b], key);
 }
@@ -304,18 +379,45 @@ cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_cha
   return cudaGetLastError();
 }
 
+// Working storage of a level: argmin keys, the run table, the predictions.
+struct LevelLayout {
+  size_t keys, runs, preds, total;
+};
+LevelLayout level_layout(int nblocks, int ncombos) {
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  LevelLayout L;
+  L.keys = 0;
+  L.runs = up((size_t)nblocks * 8);
+  L.preds = L.runs + up(sizeof(mtd::LevelRuns));
+  L.total = L.preds + (size_t)nblocks * ncombos * 64;
+  return L;
+}
+
+size_t level8_scratch_bytes(int nblocks, int ncombos) {
+  if (nblocks <= 0 || ncombos <= 0) return 0;
+  return level_layout(nblocks, ncombos).total;
+}
+
 cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
-                          mt_candidate_result* res, unsigned long long* keys, mt_block_best* best, cudaStream_t st) {
+                          mt_candidate_result* res, void* scratch, mt_block_best* best, cudaStream_t st) {
   if (nblocks <= 0 || ncombos <= 0) return cudaSuccess;
+  const LevelLayout L = level_layout(nblocks, ncombos);
+  uint8_t* s = static_cast<uint8_t*>(scratch);
+  unsigned long long* keys = reinterpret_cast<unsigned long long*>(s + L.keys);
+  mtd::LevelRuns* runs = reinterpret_cast<mtd::LevelRuns*>(s + L.runs);
+  uint4* preds = reinterpret_cast<uint4*>(s + L.preds);
   cudaError_t e = cudaMemsetAsync(keys, 0xff, (size_t)nblocks * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
+  const mtd::ChainArgs args = make_args(p, q, trellis_lambda, qm_row);
   const long long total = (long long)nblocks * ncombos;
   const long long grid = (total + mtd::kThreads - 1) / mtd::kThreads;
-  mtd::level8_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
-                                                               qm_row, costs, blocks, nblocks, combos, ncombos, res,
-                                                               keys);
+  mtd::level8_runs_kernel<<<1, 32, 0, st>>>(combos, ncombos, runs);
+  // At most ncombos runs: pred CTAs past the run count exit at once.
+  mtd::level8_pred_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(rec, args, blocks, nblocks, combos, runs, preds);
+  mtd::level8_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, args, qm_row, costs, blocks, nblocks, combos,
+                                                               ncombos, runs, preds, res, keys);
   mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
   return cudaGetLastError();
 }

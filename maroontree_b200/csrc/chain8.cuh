@@ -338,18 +338,25 @@ struct Work8 {
 // the prediction in w.pred() and the inverse residual in w.rr().  (Compiling
 // one path per transform type raised register use to the cap and was no
 // faster, so the type stays a run-time value.)
-__device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
-                                           const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
-                                           const uint8_t* qm, const float* qs, const float* lut,
-                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
-                                           Work8& w) {
+// Prediction of candidate cd into w.pred() (it depends on the mode, angle
+// delta and neighbour flags only, not on the transform type).
+__device__ __forceinline__ void chain8_predict(const uint16_t* __restrict__ rec, const mt_chain_params& p,
+                                               const mt_candidate& cd, Work8& w) {
+  predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
+           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, w.pred(), w.edges());
+}
+
+// The rest of the chain for candidate cd from the prediction in w.pred()
+// (left intact, so several transform types can share one prediction).
+__device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, const mt_chain_params& p,
+                                          const mt_quant& q, float trellis_lambda, const uint8_t* qm,
+                                          const float* qs, const float* lut, const mt_coef_costs& T,
+                                          const mt_candidate& cd, mt_candidate_result& r, Work8& w) {
   const int32_t maxv = (1 << p.bd) - 1;
   int16_t* pred = w.pred();
   int16_t* cf = w.cf();
   int16_t* rr = w.rr();
   float* tf = w.tf();
-  predict8(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
-           (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, w.edges());
 #pragma unroll
   for (int y = 0; y < 8; y++)
 #pragma unroll
@@ -381,6 +388,15 @@ __device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, con
   r.satd = satd;
   r.eob = eob;
   r.reserved[0] = r.reserved[1] = r.reserved[2] = 0;
+}
+
+__device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
+                                           const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
+                                           const uint8_t* qm, const float* qs, const float* lut,
+                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
+                                           Work8& w) {
+  chain8_predict(rec, p, cd, w);
+  chain8_tx(src, p, q, trellis_lambda, qm, qs, lut, T, cd, r, w);
 }
 
 }  // namespace mtd

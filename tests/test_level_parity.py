@@ -66,7 +66,7 @@ def test_level_device_api_matches_host(mt_lib, oracle_lib, cuda):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_best = torch.zeros(len(blocks) * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     d_res = torch.zeros(len(blocks) * len(combos) * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-    d_keys = torch.zeros(len(blocks) * 8, dtype=torch.uint8, device=dev)
+    d_keys = torch.zeros(mt_lib.rdo_level8_scratch_bytes(len(blocks), len(combos)), dtype=torch.uint8, device=dev)
     mt_lib.rdo_level8_device(t(src), t(rec), prm, q, t(qm), t(np.frombuffer(bytes(costs), np.uint8)), t(blocks),
                              len(blocks), t(combos), len(combos), d_best, d_res, d_keys)
     torch.cuda.synchronize()

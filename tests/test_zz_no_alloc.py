@@ -43,7 +43,7 @@ def _run_both(mt_lib, torch, case):
     # existing entry point: caller-provided working storage
     d_best_ref = torch.zeros(nb * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     d_res = torch.zeros(nb * nc * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-    d_keys = torch.zeros(nb * 8, dtype=torch.uint8, device=dev)
+    d_keys = torch.zeros(mt_lib.rdo_level8_scratch_bytes(nb, nc), dtype=torch.uint8, device=dev)
     mt_lib.rdo_level8_device(d_src, d_rec, prm, q, d_qm, d_costs, d_blocks, nb, d_combos, nc, d_best_ref, d_res,
                              d_keys)
     # allocation-free entry point, called through the C ABI
