@@ -120,7 +120,7 @@ typedef struct mt_candidate {
   uint8_t mode;          /* MT_*_PRED */
   int8_t angle_delta;    /* -3..3, directional modes only */
   uint8_t tx_type;       /* MT_TX_* */
-  uint8_t flags;         /* bit0 have_tr, bit1 have_bl, bit2 filter_type */
+  uint8_t flags;         /* bit0 have_tr, bit1 have_bl, bit2 filter_type, bit3 no trellis */
   uint8_t dcs_ctx;       /* dc_sign context 0..2 */
   uint8_t skip_ctx;      /* txb_skip context 0..12 */
   uint16_t reserved;
@@ -130,10 +130,13 @@ typedef struct mt_candidate {
 #define MT_CAND_HAVE_TR 1u
 #define MT_CAND_HAVE_BL 2u
 #define MT_CAND_FILTER_TYPE 4u
+/* Price the levels as quantised, without trellis_optimize: the reference's
+ * 4x4 IDTX trial in the SPLIT4 pricing (src/coder/lossy_state.rs:2229-2236). */
+#define MT_CAND_NO_TRELLIS 8u
 
 /* Batch-wide parameters of the chain. */
 typedef struct mt_chain_params {
-  int32_t tx_size;        /* square luma transform size: 8 (4, 16 reserved) */
+  int32_t tx_size;        /* square luma transform size: 8, or 4 for the 4x4 level (16 reserved) */
   int32_t bd;             /* bit depth (8) */
   int32_t frame_w, frame_h; /* padded plane size, also the prediction frame bounds */
   int32_t stride;         /* samples per row of src and recon */
@@ -159,8 +162,9 @@ typedef struct mt_candidate_result {
   uint32_t reserved[3];
 } mt_candidate_result;
 
-/* One 8x8 block of an RDO level: position, neighbour availability, contexts
- * and the caller's mode-signalling bits for each of the 13 luma modes. */
+/* One block of an RDO level (8x8 for mt_rdo_level8*, 4x4 for mt_rdo_level4*):
+ * position, neighbour availability, contexts and the caller's
+ * mode-signalling bits for each of the 13 luma modes. */
 typedef struct mt_block8 {
   uint16_t px, py;
   uint8_t flags;          /* MT_CAND_* bits */
@@ -175,8 +179,9 @@ typedef struct mt_combo {
   uint8_t mode;
   int8_t angle_delta;
   uint8_t tx_type;
-  uint8_t reserved;
+  uint8_t flags;          /* MT_COMBO_NO_TRELLIS */
 } mt_combo;
+#define MT_COMBO_NO_TRELLIS 1u
 
 /* Per-block winner of a level: the lowest rd cost over the combos, ties to
  * the earlier combo (the reference's strict-< scan in candidate order). */
@@ -248,6 +253,26 @@ int mt_rdo_level8_device(const uint16_t* d_src, const uint16_t* d_recon, const m
                          int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
                          void* d_scratch, void* stream);
 size_t mt_rdo_level8_scratch_bytes(int32_t nblocks, int32_t ncombos);
+
+/* The same batched level for 4x4 luma blocks (prm->tx_size = 4): the per-4x4
+ * chain the reference's SPLIT4 pricing runs (src/coder/lossy_state.rs:
+ * 2148-2290: predict_nd from the pre-block reconstruction, dct4x4_t /
+ * adst4x4_t / idtx4x4_t, trellis_optimize over SCAN_4X4 -- skipped for combos
+ * flagged MT_COMBO_NO_TRELLIS, as its IDTX trial does --, the 4x4 inverse,
+ * luma_partition_distortion and luma_bits over the TX_4X4 class).  Blocks are
+ * mt_block8 records on the 4-sample grid; qm_row is the 16-entry 4x4 row;
+ * costs the TX_4X4 luma slice; d_scratch is mt_rdo_level4_scratch_bytes
+ * (the per-block argmin keys). */
+int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm,
+                  const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                  const mt_block8* blocks, int32_t nblocks, const mt_combo* combos,
+                  int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out);
+int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
+                         int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
+                         void* d_scratch, void* stream);
+size_t mt_rdo_level4_scratch_bytes(int32_t nblocks, int32_t ncombos);
 
 /* Allocation-free form of mt_rdo_level8_device.  No counterpart in the
  * reference: it exists for callers that cannot give this library device

@@ -15,7 +15,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
     "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
-    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "rdo_level8_scratch_bytes", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
+    "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "rdo_level8_scratch_bytes", "rdo_level4", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
 ]
 
 
@@ -119,6 +119,23 @@ def rdo_level8(src, recon, prm, quant, qmrow, costs, blocks, combos, want_result
     _check(lib.mt_rdo_level8(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
                              ptr(blocks), len(blocks), ptr(combos), len(combos), ptr(best), ptr(res)),
            "mt_rdo_level8")
+    return best, res
+
+
+def rdo_level4(src, recon, prm, quant, qmrow, costs, blocks, combos, want_results=False):
+    """The batched 4x4 level (``mt_rdo_level4``): blocks on the 4-sample grid,
+    prm.tx_size = 4, the 16-entry 4x4 QM row and the TX_4X4 cost slice."""
+    lib = load()
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.BLOCK8_DTYPE)
+    combos = np.ascontiguousarray(combos, abi.COMBO_DTYPE)
+    best = np.zeros(len(blocks), abi.BEST_DTYPE)
+    res = np.zeros(len(blocks) * len(combos), RESULT_DTYPE) if want_results else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(lib.mt_rdo_level4(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                             ptr(blocks), len(blocks), ptr(combos), len(combos), ptr(best), ptr(res)),
+           "mt_rdo_level4")
     return best, res
 
 

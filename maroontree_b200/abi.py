@@ -25,7 +25,8 @@ SMOOTH_PRED, SMOOTH_V_PRED, SMOOTH_H_PRED, PAETH_PRED = 9, 10, 11, 12
 TX_IDTX, TX_DCT_DCT, TX_V_DCT, TX_H_DCT, TX_ADST_ADST, TX_ADST_DCT, TX_DCT_ADST = range(7)
 TX_2D_SCAN_TYPES = (TX_IDTX, TX_DCT_DCT, TX_ADST_ADST, TX_ADST_DCT, TX_DCT_ADST)
 
-CAND_HAVE_TR, CAND_HAVE_BL, CAND_FILTER_TYPE = 1, 2, 4
+CAND_HAVE_TR, CAND_HAVE_BL, CAND_FILTER_TYPE, CAND_NO_TRELLIS = 1, 2, 4, 8
+COMBO_NO_TRELLIS = 1
 
 
 class Quant(C.Structure):
@@ -91,7 +92,7 @@ BLOCK8_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
     ("mode_bits", "<f4", (13,)),
 ])
-COMBO_DTYPE = np.dtype([("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"), ("reserved", "u1")])
+COMBO_DTYPE = np.dtype([("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"), ("flags", "u1")])
 BEST_DTYPE = np.dtype([
     ("combo", "<i4"), ("cost", "<f4"), ("distortion", "<f4"), ("bits", "<f4"), ("satd", "<u4"), ("eob", "<i4"),
     ("reserved", "<u4", (2,)),
@@ -129,6 +130,11 @@ def _bind(lib):
         "mt_rdo_level8_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
                                            _P, C.c_int32, _P, _P, _P, _P]),
         "mt_rdo_level8_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+        "mt_rdo_level4": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                                    C.c_int32, _P, C.c_int32, _P, _P]),
+        "mt_rdo_level4_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
+                                           _P, C.c_int32, _P, _P, _P, _P]),
+        "mt_rdo_level4_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
         "mt_rdo_level8_device_noalloc": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
                                                    C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_padded_plane_dims": (C.c_int, [C.c_int32, C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
@@ -174,7 +180,8 @@ def load():
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
-    "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc", "mt_fwd_txfm_quant_device",
+    "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
+    "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
     "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",

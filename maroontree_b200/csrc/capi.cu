@@ -19,6 +19,10 @@ cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_cha
                           const mt_candidate* cands, int n, mt_candidate_result* res, int32_t* lv, int32_t* ro,
                           void* scratch, cudaStream_t st);
 size_t level8_scratch_bytes(int nblocks, int ncombos);
+cudaError_t launch_level4(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                          float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                          const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
+                          mt_candidate_result* res, void* scratch, mt_block_best* best, cudaStream_t st);
 cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
@@ -180,9 +184,9 @@ int mt_coef_costs_build(const mt_coef_cdfs* c, mt_coef_costs* o) {
   return MT_OK;
 }
 
-static int check_chain(const mt_chain_params* prm, const mt_quant* q, int32_t n) {
+static int check_chain(const mt_chain_params* prm, const mt_quant* q, int32_t n, int32_t tx_size = 8) {
   if (!prm || !q || n < 0) return MT_ERR_INVALID_INPUT;
-  if (prm->tx_size != 8 || prm->bd != 8) return MT_ERR_UNSUPPORTED;
+  if (prm->tx_size != tx_size || prm->bd != 8) return MT_ERR_UNSUPPORTED;
   if (prm->frame_w <= 0 || prm->frame_h <= 0 || prm->stride < prm->frame_w) return MT_ERR_INVALID_INPUT;
   return MT_OK;
 }
@@ -263,6 +267,78 @@ int mt_rdo_level8(const uint16_t* src, const uint16_t* recon, const mt_chain_par
   if (e != cudaSuccess) return MT_ERR_DEVICE;
   float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
   e = mth::launch_level8((const uint16_t*)(base + off_src), (const uint16_t*)(base + off_rec), *prm, *quant, tl,
+                         qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
+                         (const mt_block8*)(base + off_blk), nblocks, (const mt_combo*)(base + off_cmb), ncombos,
+                         (mt_candidate_result*)(base + off_res), base + off_key, (mt_block_best*)(base + off_best),
+                         st);
+  if (e != cudaSuccess) return MT_ERR_DEVICE;
+  e = cudaMemcpyAsync(best_out, base + off_best, (size_t)nblocks * sizeof(mt_block_best), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && results_out)
+    e = cudaMemcpyAsync(results_out, base + off_res, nres * sizeof(mt_candidate_result), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+size_t mt_rdo_level4_scratch_bytes(int32_t nblocks, int32_t ncombos) {
+  if (nblocks <= 0 || ncombos <= 0 || ncombos > MT_LEVEL_MAX_COMBOS) return 0;
+  return (size_t)nblocks * 8;
+}
+
+int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
+                         mt_block_best* d_best, mt_candidate_result* d_results, void* d_scratch, void* stream) {
+  int rc = check_chain(prm, quant, 0, 4);
+  if (rc != MT_OK) return rc;
+  if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
+  if (nblocks == 0 || ncombos == 0) return MT_OK;
+  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_INVALID_INPUT;
+  if (ncombos > MT_LEVEL_MAX_COMBOS) return MT_ERR_TOO_LARGE;
+  if (!d_src || !d_recon || !d_costs || !d_blocks || !d_combos || !d_best || !d_results || !d_scratch)
+    return MT_ERR_INVALID_INPUT;
+  float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
+  cudaError_t e = mth::launch_level4(d_src, d_recon, *prm, *quant, tl, d_qm_row, d_costs, d_blocks, nblocks, d_combos,
+                                     ncombos, d_results, d_scratch, d_best, as_stream(stream));
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
+                  const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
+                  const mt_combo* combos, int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out) {
+  int rc = check_chain(prm, quant, 0, 4);
+  if (rc != MT_OK) return rc;
+  if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
+  if (nblocks == 0 || ncombos == 0) return MT_OK;
+  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_INVALID_INPUT;
+  if (ncombos > MT_LEVEL_MAX_COMBOS) return MT_ERR_TOO_LARGE;
+  if (!src || !recon || !costs || !blocks || !combos || !best_out) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
+  const size_t nres = (size_t)nblocks * ncombos;
+  size_t off_src = 0, off_rec = align256(plane), off_cost = off_rec + align256(plane);
+  size_t off_qm = off_cost + align256(sizeof(mt_coef_costs));
+  size_t off_blk = off_qm + 256;
+  size_t off_cmb = off_blk + align256((size_t)nblocks * sizeof(mt_block8));
+  size_t off_best = off_cmb + align256((size_t)ncombos * sizeof(mt_combo));
+  size_t off_key = off_best + align256((size_t)nblocks * sizeof(mt_block_best));
+  size_t off_res = off_key + align256((size_t)nblocks * 8);
+  size_t total = off_res + align256(nres * sizeof(mt_candidate_result));
+  std::lock_guard<std::mutex> lock(g_ws.mu);
+  char* base = (char*)g_ws.get(total);
+  if (!base) return MT_ERR_ALLOC;
+  cudaStream_t st = 0;
+  cudaError_t e = cudaSuccess;
+  auto cp = [&](size_t off, const void* h, size_t bytes) {
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + off, h, bytes, cudaMemcpyHostToDevice, st);
+  };
+  cp(off_src, src, plane);
+  cp(off_rec, recon, plane);
+  cp(off_cost, costs, sizeof(mt_coef_costs));
+  if (qm_row) cp(off_qm, qm_row, 16);
+  cp(off_blk, blocks, (size_t)nblocks * sizeof(mt_block8));
+  cp(off_cmb, combos, (size_t)ncombos * sizeof(mt_combo));
+  if (e != cudaSuccess) return MT_ERR_DEVICE;
+  float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
+  e = mth::launch_level4((const uint16_t*)(base + off_src), (const uint16_t*)(base + off_rec), *prm, *quant, tl,
                          qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
                          (const mt_block8*)(base + off_blk), nblocks, (const mt_combo*)(base + off_cmb), ncombos,
                          (mt_candidate_result*)(base + off_res), base + off_key, (mt_block_best*)(base + off_best),

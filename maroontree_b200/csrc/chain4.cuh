@@ -1,0 +1,303 @@
+// Device 4x4 luma candidate chain: prediction -> residual -> forward 4x4
+// transform + quantisation (+ QM) -> trellis -> inverse -> SATD distortion ->
+// coefficient rate -> rd cost, one candidate per thread, in the reference's
+// arithmetic (the SPLIT4 pricing of src/coder/lossy_state.rs:2148-2290).  The
+// trellis and rate walk are the 8x8 chain's (chain8.cuh) over the 16-entry
+// default 4x4 scan and the TX_4X4 coefficient class.
+#pragma once
+#include <stdint.h>
+
+#include "chain8.cuh"
+#include "intrapred.cuh"
+#include "txfm4.cuh"
+
+namespace mtd {
+
+// Default 4x4 scan (scan index -> rc = x*4 + y) and its inverse.
+__constant__ uint8_t kScan4[16] = {0, 4, 1, 2, 5, 8, 12, 9, 6, 3, 7, 10, 13, 14, 11, 15};
+
+// One chunk of trellis step A (src/avx/trellis.rs:79-161) at 4x4 scan
+// positions [base, base + W): decisions use the chunk's values at its start.
+template <int W, typename C>
+__device__ __forceinline__ void round_down_chunk4(C* cf, const float* tf, int base, float dq2, float aq2, float lambda,
+                                                  const float* lut) {
+  int32_t c[W];
+  float at[W];
+  int rc[W];
+  bool big = false;
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    rc[k] = kScan4[base + k];
+    c[k] = cf[rc[k]];
+    at[k] = fabsf(tf[rc[k]]);
+    big |= uabs(c[k]) > 63u;
+  }
+#pragma unroll
+  for (int k = 0; k < W; k++) {
+    const float q2 = rc[k] == 0 ? dq2 : aq2;
+    bool dn;
+    if (big) {
+      dn = c[k] != 0 && round_down_plain(at[k], uabs(c[k]), q2, lambda);
+    } else {
+      const int32_t li = (int32_t)uabs(c[k]), ldi = max(li - 1, 0);
+      const float el = __fsub_rn(at[k], (float)li), ed = __fsub_rn(at[k], (float)ldi);
+      const float cl = __fmaf_rn(q2, __fmul_rn(el, el), __fmul_rn(lambda, lut[li]));
+      const float cd = __fmaf_rn(q2, __fmul_rn(ed, ed), __fmul_rn(lambda, lut[ldi]));
+      dn = cd < cl;
+    }
+    if (dn && c[k] != 0) cf[rc[k]] = (C)(c[k] < 0 ? c[k] + 1 : c[k] - 1);
+  }
+}
+
+// trellis_optimize (src/trellis.rs:944-1030) over the 4x4 default scan, step
+// A in the pinned AVX2 chunking (one 8-wide chunk, a 4-wide chunk, scalar
+// tail), then the exact right-to-left suffix sums and the EOB search.
+// `suf` is scratch for 17 floats.  Returns the final EOB scan index.
+template <typename C>
+__device__ int trellis4(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda, const float* lut) {
+  const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
+  int eob_idx = -1;
+#pragma unroll
+  for (int i = 0; i < 16; i++)
+    if (cf[kScan4[i]] != 0) eob_idx = i;
+  const int m = eob_idx + 1;
+  const int M = warp_max(m);
+  if (m == 0) return -1;
+  const int full8 = m & ~7;
+  const bool has4 = (m - full8) >= 4;
+  for (int base = 0; base < M; base += 8) {
+    if (base >= m) continue;
+    if (base < full8) {
+      round_down_chunk4<8>(cf, tf, base, dq2, aq2, lambda, lut);
+    } else {
+      int s = base;
+      if (has4) {
+        round_down_chunk4<4>(cf, tf, base, dq2, aq2, lambda, lut);
+        s += 4;
+      }
+      for (int k = 0; k < 4; k++) {
+        const int e = s + k;
+        if (e >= m) break;
+        const int rc = kScan4[e];
+        const int32_t c = cf[rc];
+        if (c != 0 && round_down_plain(fabsf(tf[rc]), uabs(c), rc == 0 ? dq2 : aq2, lambda))
+          cf[rc] = (C)(c < 0 ? c + 1 : c - 1);
+      }
+    }
+  }
+  suf[m] = 0.0f;
+  float acc = 0.0f;
+  for (int e = M - 1; e >= 0; e--) {
+    if (e >= m) continue;
+    const int rc = kScan4[e];
+    const float at = fabsf(tf[rc]);
+    acc = __fadd_rn(acc, __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
+    suf[e] = acc;
+  }
+  int best_e = -1;
+  float best = __int_as_float(0x7f800000);
+  float pre = 0.0f;
+  for (int e = 0; e < M; e++) {
+    if (e >= m) continue;
+    const int rc = kScan4[e];
+    const float at = fabsf(tf[rc]);
+    const uint32_t l = uabs(cf[rc]);
+    const float ecur = __fsub_rn(at, (float)l);
+    const float dcur = __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(ecur, ecur));
+    const float base_c = __fadd_rn(pre, dcur);
+    if (l != 0) {
+      const int bin = e < 2 ? e : 32 - __clz(e);
+      const int extra = bin > 1 ? bin - 2 : 0;
+      const float sig = __fadd_rn(__fmul_rn((float)bin, 0.9f), __fadd_rn((float)extra, 2.0f));
+      const float c = __fadd_rn(__fadd_rn(base_c, __fmul_rn(lambda, sig)), suf[e + 1]);
+      if (c < best) {
+        best = c;
+        best_e = e;
+      }
+    }
+    pre = __fadd_rn(base_c, __fmul_rn(lambda, l < 64 ? lut[l] : coef_rate_bits(l)));
+  }
+  const float skip = __fadd_rn(suf[0], lambda);
+  const int keep = (best_e < 0 || skip < best) ? 0 : best_e + 1;
+  for (int e = 0; e < M; e++)
+    if (e >= keep && e < m) cf[kScan4[e]] = 0;
+  return keep - 1;
+}
+
+// Coefficient bits of a 4x4 luma block (src/rate.rs:149-291, TX_4X4 class):
+// the reference's level map (stride 4; reads past the block land in the
+// zeroed tail) in the 24-byte scratch `lv`.
+template <typename C>
+__device__ float rate4(const C* cf, int eob, const mt_coef_costs& T, int skip_ctx, int dcs, int mode, int tx,
+                       bool use_skip_bits, float skip1, float skip0, uint8_t* lv) {
+  const int E = warp_max(eob);
+  if (eob < 0) return use_skip_bits ? skip1 : T.txb_skip[skip_ctx][1];
+  float bits = use_skip_bits ? skip0 : T.txb_skip[skip_ctx][0];
+  bits = __fadd_rn(bits, T.txtp[mode][tx]);
+  const float* dcs_c = T.dc_sign[dcs];
+  if (eob == 0) {
+    const uint32_t m = uabs(cf[0]), mm = min(m, 3u);
+    bits = __fadd_rn(bits, T.eob_bin[0]);
+    bits = __fadd_rn(bits, T.eob_base[0][mm - 1]);
+    if (mm == 3) {
+      float h = T.br_cum[0][min((int32_t)m - 3, 12)];
+      if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+      bits = __fadd_rn(bits, h);
+    }
+    return __fadd_rn(bits, dcs_c[cf[0] < 0]);
+  }
+  const int eob_bin = eob < 2 ? eob : 32 - __clz(eob);
+  bits = __fadd_rn(bits, T.eob_bin[eob_bin]);
+  if (eob_bin > 1) {
+    const int nb = eob_bin - 2;
+    bits = __fadd_rn(bits, T.eob_hi[eob_bin][(eob >> nb) & 1]);
+    bits = __fadd_rn(bits, (float)nb);
+  }
+  uint32_t* lv32 = reinterpret_cast<uint32_t*>(lv);
+#pragma unroll
+  for (int i = 0; i < 6; i++) lv32[i] = 0;
+  const int ctx_e = 1 + (eob > 2) + (eob > 4);
+  {
+    const int rc = kScan4[eob];
+    const int ex = rc >> 2, ey = rc & 3;
+    const uint32_t m = uabs(cf[rc]);
+    const uint32_t tok = min(m, 3u) - 1;
+    bits = __fadd_rn(bits, T.eob_base[ctx_e][tok]);
+    if (tok == 2) {
+      float h = T.br_cum[(ex | ey) > 1 ? 14 : 7][min((int32_t)m - 3, 12)];
+      if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+      bits = __fadd_rn(bits, h);
+    }
+    lv[rc] = (uint8_t)level_byte(m);
+  }
+  int ac_nz = 1;
+  for (int i = E - 1; i >= 1; i--) {
+    if (i >= eob) continue;
+    const int rc = kScan4[i];
+    const int x = rc >> 2, y = rc & 3;
+    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + 4] + lv[rc + 5];
+    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 8];
+    const int ctx = kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
+    const uint32_t m = uabs(cf[rc]);
+    const uint32_t tok = min(m, 3u);
+    bits = __fadd_rn(bits, T.base_tok[ctx][tok]);
+    if (tok == 3) {
+      const uint32_t hmag = hm & 63;
+      const int bc = ((y | x) > 1 ? 14 : 7) + (hmag > 12 ? 6 : (int)((hmag + 1) >> 1));
+      bits = __fadd_rn(bits, T.br_cum[bc][min((int32_t)m - 3, 12)]);
+      if (m >= 15) bits = __fadd_rn(bits, golomb_cost(m - 15));
+    }
+    lv[rc] = (uint8_t)level_byte(m);
+    ac_nz += m != 0;
+  }
+  const uint32_t dm = uabs(cf[0]), dtok = min(dm, 3u);
+  bits = __fadd_rn(bits, T.base_tok[0][dtok]);
+  if (dtok == 3) {
+    const uint32_t mag = ((uint32_t)lv[1] + lv[4] + lv[5]) & 63;
+    float h = T.br_cum[mag > 12 ? 6 : (int)((mag + 1) >> 1)][min((int32_t)dm - 3, 12)];
+    if (dm >= 15) h = __fadd_rn(h, golomb_cost(dm - 15));
+    bits = __fadd_rn(bits, h);
+  }
+  if (cf[0] != 0) bits = __fadd_rn(bits, dcs_c[cf[0] < 0]);
+  for (int k = 0; k < ac_nz; k++) bits = __fadd_rn(bits, 1.0f);
+  return bits;
+}
+
+// Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
+template <typename P, typename R>
+__device__ __forceinline__ uint32_t satd4(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
+                                          const R* rr, int32_t maxv) {
+  int32_t r[4][4];
+#pragma unroll
+  for (int y = 0; y < 4; y++) {
+    int32_t d[4];
+#pragma unroll
+    for (int x = 0; x < 4; x++) {
+      const int i = y * 4 + x;
+      d[x] = (int32_t)src[(size_t)(py + y) * stride + px + x] - clampi(pred[i] + rr[i], 0, maxv);
+    }
+    const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
+    r[y][0] = e + g;
+    r[y][1] = f + h;
+    r[y][2] = f - h;
+    r[y][3] = e - g;
+  }
+  uint32_t satd = 0;
+#pragma unroll
+  for (int x = 0; x < 4; x++) {
+    const int32_t e = r[0][x] + r[2][x], f = r[0][x] - r[2][x], g = r[1][x] + r[3][x], h = r[1][x] - r[3][x];
+    satd += uabs(e + g) + uabs(f + h) + uabs(f - h) + uabs(e - g);
+  }
+  return satd;
+}
+
+__device__ __forceinline__ bool cand4_ok(const mt_candidate& c, int fw, int fh) {
+  return c.px + 4 <= fw && c.py + 4 <= fh && c.mode <= MT_PAETH_PRED && c.tx_type <= MT_TX_DCT_ADST &&
+         c.angle_delta >= -3 && c.angle_delta <= 3 && c.dcs_ctx < 3 && c.skip_ctx < 13;
+}
+
+// Per-thread working set of one 4x4 candidate in ONE allocation (the same
+// single-arena rule as the 8x8 chain's Work8).  Layout (words): [0,8) pred |
+// [8,16) rr | [16,24) cf (int16) | [24,40) tf | [40,57) suf, also the rate
+// walk's level map and the transform scratch.  During prediction, before tf
+// and suf are live, [24,90) holds the two edges and the filter temporary.
+constexpr int kWork4Words = 24 + 3 * edge_cap<4>();
+struct Work4 {
+  int32_t* w;
+  __device__ __forceinline__ int16_t* pred() { return reinterpret_cast<int16_t*>(w); }
+  __device__ __forceinline__ int16_t* rr() { return reinterpret_cast<int16_t*>(w + 8); }
+  __device__ __forceinline__ int16_t* cf() { return reinterpret_cast<int16_t*>(w + 16); }
+  __device__ __forceinline__ float* tf() { return reinterpret_cast<float*>(w + 24); }
+  __device__ __forceinline__ float* suf() { return reinterpret_cast<float*>(w + 40); }
+  __device__ __forceinline__ int32_t* edges() { return w + 24; }
+};
+static_assert(kWork4Words >= 57, "4x4 arena too small");
+
+// Evaluate one 4x4 candidate; leaves the final levels in w.cf(), the
+// prediction in w.pred() and the inverse residual in w.rr().
+__device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
+                                           const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
+                                           const uint8_t* qm, const float* qs, const float* lut,
+                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
+                                           Work4& w) {
+  const int32_t maxv = (1 << p.bd) - 1;
+  int16_t* pred = w.pred();
+  int16_t* cf = w.cf();
+  int16_t* rr = w.rr();
+  float* tf = w.tf();
+  predict_sq<4>(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
+                (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, w.edges());
+#pragma unroll
+  for (int y = 0; y < 4; y++)
+#pragma unroll
+    for (int x = 0; x < 4; x++)
+      rr[y * 4 + x] = (int16_t)((int32_t)src[(size_t)(cd.py + y) * p.stride + cd.px + x] - pred[y * 4 + x]);
+  const int TX = cd.tx_type;
+  fwd4x4(rr, TX, q, cf, tf, reinterpret_cast<int32_t*>(w.suf()));
+  const bool two_d = TX == MT_TX_DCT_DCT || TX >= MT_TX_ADST_ADST;
+  if (two_d && qm) apply_qm(cf, tf, qs, 16);
+  int eob;
+  if (p.trellis_lambda0 > 0.0f && !(cd.flags & MT_CAND_NO_TRELLIS)) {
+    eob = trellis4(cf, tf, w.suf(), (float)q.dc_q, (float)q.ac_q, trellis_lambda, lut);
+  } else {
+    eob = -1;
+    for (int i = 0; i < 16; i++)
+      if (cf[kScan4[i]] != 0) eob = i;
+  }
+  inv4x4(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
+  const uint32_t satd = satd4(src, p.stride, cd.px, cd.py, pred, rr, maxv);
+  const float qstep = (float)q.ac_q;
+  float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
+  if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
+  const float cbits = rate4(cf, eob, T, cd.skip_ctx, cd.dcs_ctx, cd.mode, TX, p.use_skip_bits != 0, p.skip_bits[0],
+                            p.skip_bits[1], reinterpret_cast<uint8_t*>(w.suf()));
+  const float bits = __fadd_rn(cbits, cd.mode_bits);
+  r.distortion = price;
+  r.bits = bits;
+  r.cost = __fadd_rn(price, __fmul_rn(p.mode_lambda, bits));
+  r.satd = satd;
+  r.eob = eob;
+  r.reserved[0] = r.reserved[1] = r.reserved[2] = 0;
+}
+
+}  // namespace mtd

@@ -367,7 +367,7 @@ __device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, cons
   const bool two_d = TX == MT_TX_DCT_DCT || TX >= MT_TX_ADST_ADST;
   if (two_d && qm) apply_qm(cf, tf, qs, 64);
   int eob;
-  if (p.trellis_lambda0 > 0.0f) {
+  if (p.trellis_lambda0 > 0.0f && !(cd.flags & MT_CAND_NO_TRELLIS)) {
     eob = trellis8(cf, tf, w.suf(), (float)q.dc_q, (float)q.ac_q, trellis_lambda, lut);
   } else {
     eob = -1;

@@ -15,9 +15,21 @@ __constant__ int16_t kDrDeriv[44] = {0,  1023, 0,  547, 372, 0,  0,  273, 215, 0
                                      0,  102,  0,  90,  80,  0,  71, 64,  0,   57, 51,  0,   45, 0,   40,
                                      35, 0,    31, 27,  0,   23, 19, 0,   15,  0,  11,  0,   7,  3};
 __constant__ int16_t kSmW8[8] = {255, 197, 146, 105, 73, 50, 37, 32};
+__constant__ int16_t kSmW4[4] = {255, 149, 85, 64};
+
+template <int N>
+__device__ __forceinline__ int32_t sm_weight(int i) {
+  return N == 4 ? kSmW4[i] : kSmW8[i];
+}
 
 constexpr int kEdgeOrigin = 2;
-constexpr int kEdgeCap8 = 2 + 2 * 16 + 4;  // bw = bh = 8: upsampled reach 2*16
+// Words of one edge array for an N x N block: origin 2 plus the upsampled
+// reach 2 * (2N) and slack.
+template <int N>
+__host__ __device__ constexpr int edge_cap() {
+  return 2 + 4 * N + 4;
+}
+constexpr int kEdgeCap8 = edge_cap<8>();
 
 __device__ __forceinline__ int edge_strength(int w, int h, bool ft, int delta) {
   const int d = abs(delta), wh = w + h;
@@ -82,23 +94,25 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
   return 1 << (bd - 1);
 }
 
-// Prediction of an 8x8 block into out[64] (row-major).  `scratch` holds
-// 3 * kEdgeCap8 words: the above and left edges and a filter temporary.
-template <typename O>
-__device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
-                         int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out,
-                         int32_t* __restrict__ scratch) {
-  constexpr int bw = 8, bh = 8, edge_len = 16;
+// Prediction of an N x N block (N = 4 or 8) into out[N*N] (row-major).
+// `scratch` holds 3 * edge_cap<N>() words: the above and left edges and a
+// filter temporary.
+template <int N, typename O>
+__device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
+                           int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out,
+                           int32_t* __restrict__ scratch) {
+  static_assert(N == 4 || N == 8, "corner filtering (edge_len >= 24) is not built");
+  constexpr int bw = N, bh = N, edge_len = 2 * N, cap = edge_cap<N>();
   if (mode == MT_DC_PRED) {
-    const int32_t d = dc_pred_sq(rec, stride, ox, oy, 8, 3, bd);
-    for (int i = 0; i < 64; i++) out[i] = (O)(d);
+    const int32_t d = dc_pred_sq(rec, stride, ox, oy, N, N == 4 ? 2 : 3, bd);
+    for (int i = 0; i < N * N; i++) out[i] = (O)(d);
     return;
   }
   // Every edge entry the predictor reads is written below (logical -1 ..
-  // 15, and -2 .. 30 once upsampled), so the arrays are not cleared.
+  // 2N-1, and -2 .. 4N-2 once upsampled), so the arrays are not cleared.
   int32_t* A = scratch;
-  int32_t* L = scratch + kEdgeCap8;
-  int32_t* tmp = scratch + 2 * kEdgeCap8;
+  int32_t* L = scratch + cap;
+  int32_t* tmp = scratch + 2 * cap;
   const bool have_top = oy > 0, have_left = ox > 0;
   const int32_t base = 1 << (bd - 1);
   const uint16_t* up = rec + (size_t)(oy - 1) * stride + ox;     // valid when have_top
@@ -137,7 +151,7 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
     const int angle = base_angle[mode] + delta * 3;
     int up_a = 0, up_l = 0;
     if (angle != 90 && angle != 180) {
-      // edge_len 16 < 24: no corner filter for 8x8.
+      // edge_len <= 16 < 24: no corner filter for 4x4 and 8x8.
       filter_edge(A, bw + 1 + (angle < 90 ? bh : 0), edge_strength(bw, bh, ft, angle - 90), tmp);
       filter_edge(L, bh + 1 + (angle > 180 ? bw : 0), edge_strength(bh, bw, ft, angle - 180), tmp);
       const int da = abs(angle - 90), dl = abs(angle - 180);
@@ -217,19 +231,28 @@ __device__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, i
     const int32_t right = a[bw - 1], bottom = l[bh - 1];
     for (int y = 0; y < bh; y++)
       for (int x = 0; x < bw; x++) {
-        const int32_t wv = kSmW8[y], wh = kSmW8[x];
+        const int32_t wv = sm_weight<N>(y), wh = sm_weight<N>(x);
         const int32_t p = wv * a[x] + (256 - wv) * bottom + wh * l[y] + (256 - wh) * right;
         out[y * bw + x] = (O)((p + 256) >> 9);
       }
   } else if (mode == MT_SMOOTH_V_PRED) {
     const int32_t bottom = l[bh - 1];
     for (int y = 0; y < bh; y++)
-      for (int x = 0; x < bw; x++) out[y * bw + x] = (O)((kSmW8[y] * a[x] + (256 - kSmW8[y]) * bottom + 128) >> 8);
+      for (int x = 0; x < bw; x++)
+        out[y * bw + x] = (O)((sm_weight<N>(y) * a[x] + (256 - sm_weight<N>(y)) * bottom + 128) >> 8);
   } else {  // SMOOTH_H
     const int32_t right = a[bw - 1];
     for (int y = 0; y < bh; y++)
-      for (int x = 0; x < bw; x++) out[y * bw + x] = (O)((kSmW8[x] * l[y] + (256 - kSmW8[x]) * right + 128) >> 8);
+      for (int x = 0; x < bw; x++)
+        out[y * bw + x] = (O)((sm_weight<N>(x) * l[y] + (256 - sm_weight<N>(x)) * right + 128) >> 8);
   }
+}
+
+template <typename O>
+__device__ __forceinline__ void predict8(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy,
+                                         int mode, int delta, bool have_tr, bool have_bl, bool ft, int bd,
+                                         O* __restrict__ out, int32_t* __restrict__ scratch) {
+  predict_sq<8>(rec, stride, fw, fh, ox, oy, mode, delta, have_tr, have_bl, ft, bd, out, scratch);
 }
 
 }  // namespace mtd

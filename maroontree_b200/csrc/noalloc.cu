@@ -44,7 +44,7 @@ __device__ __forceinline__ bool noalloc_candidate(const mt_block8& bk, const mt_
   cd.mode = cb.mode;
   cd.angle_delta = cb.angle_delta;
   cd.tx_type = cb.tx_type;
-  cd.flags = bk.flags;
+  cd.flags = (uint8_t)((bk.flags & ~MT_CAND_NO_TRELLIS) | ((cb.flags & MT_COMBO_NO_TRELLIS) ? MT_CAND_NO_TRELLIS : 0));
   cd.dcs_ctx = bk.dcs_ctx;
   cd.skip_ctx = bk.skip_ctx;
   cd.reserved = 0;

@@ -183,22 +183,23 @@ def level_blocks(fw, fh, n=8, seed=0):
     return out
 
 
-def level_combos(modes, tx_types, deltas=(0,)):
+def level_combos(modes, tx_types, deltas=(0,), no_trellis_types=()):
     """(mode, angle delta, tx type) combos in the reference's evaluation order
-    (mode, then delta, then type)."""
+    (mode, then delta, then type); types in no_trellis_types carry
+    MT_COMBO_NO_TRELLIS."""
     rows = []
     for m in modes:
         ds = deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)
         for d in ds:
             for t in tx_types:
-                rows.append((m, d, t, 0))
+                rows.append((m, d, t, abi.COMBO_NO_TRELLIS if t in no_trellis_types else 0))
     return _combos(rows)
 
 
 def _combos(rows):
     out = np.zeros(len(rows), abi.COMBO_DTYPE)
-    for i, (m, d, t, _) in enumerate(rows):
-        out[i] = (m, d, t, 0)
+    for i, (m, d, t, f) in enumerate(rows):
+        out[i] = (m, d, t, f)
     return out
 
 
@@ -211,7 +212,8 @@ def candidates_of_level(blocks, combos):
     out["mode"] = np.repeat(combos["mode"], nb)
     out["angle_delta"] = np.repeat(combos["angle_delta"], nb)
     out["tx_type"] = np.repeat(combos["tx_type"], nb)
-    out["flags"] = np.tile(blocks["flags"], nc)
+    no_tr = np.where(combos["flags"] & abi.COMBO_NO_TRELLIS, abi.CAND_NO_TRELLIS, 0).astype(np.uint8)
+    out["flags"] = np.tile(blocks["flags"], nc) | np.repeat(no_tr, nb)
     out["dcs_ctx"] = np.tile(blocks["dcs_ctx"], nc)
     out["skip_ctx"] = np.tile(blocks["skip_ctx"], nc)
     out["mode_bits"] = blocks["mode_bits"][np.tile(np.arange(nb), nc), np.repeat(combos["mode"], nb)]

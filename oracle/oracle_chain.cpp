@@ -110,6 +110,23 @@ void fwd_adst8(int32_t* b) {
   memcpy(b, o, sizeof(o));
 }
 
+// dct.rs:1368-1383 ADST4_FWD_Q12 / fwd_adst4_1d.
+const int32_t ADST4_FWD[4][4] = {
+    {1868, 3510, 4730, 5379},
+    {4730, 4730, 0, -4730},
+    {5379, -1868, -4730, 3510},
+    {3510, -5379, 4730, -1868},
+};
+void fwd_adst4(int32_t* b) {
+  int32_t o[4];
+  for (int i = 0; i < 4; i++) {
+    int64_t acc = 0;
+    for (int j = 0; j < 4; j++) acc += (int64_t)ADST4_FWD[i][j] * (int64_t)b[j];
+    o[i] = (int32_t)((acc + 2048) >> 12);
+  }
+  memcpy(b, o, sizeof(o));
+}
+
 // dct.rs:1194-1205 store_quant_target_scalar (AVX2 twin avx/dct.rs:143-166 has the
 // same float order: (c * m) * 2^-16).
 inline void store_quant_target(int32_t* cf, float* tf, int idx, int32_t coeff, int32_t mdc, int32_t mac) {
@@ -189,6 +206,54 @@ void fwd_1d_8x8(const int32_t* in, bool vertical, int32_t mdc, int32_t mac, int3
     for (int x = 0; x < 8; x++) {
       int rc = y + x * 8;
       quant_fullstep(cf, tf, rc, f[y * 8 + x], rc == 0 ? mdc : mac);
+    }
+}
+
+// dct.rs:3076-3100 dct4x4_quant_t_direct and dct.rs:1398-1470 adst4x4 /
+// adstdct4x4 / dctadst4x4 (AVX2 twins avx/dct.rs:717-793, :841-843 run the
+// same columns-then-rows order; their 4x4 normalisation is Q16 unity):
+// columns first, then rows, levels at u*4 + r.
+void fwd_2d_4x4(const int32_t* in, void (*colf)(int32_t*), void (*rowf)(int32_t*), int32_t mdc, int32_t mac,
+                int32_t* cf, float* tf) {
+  int32_t tmp[16];
+  for (int x = 0; x < 4; x++) {
+    int32_t col[4];
+    for (int r = 0; r < 4; r++) col[r] = in[r * 4 + x];
+    colf(col);
+    for (int r = 0; r < 4; r++) tmp[r * 4 + x] = col[r];
+  }
+  for (int r = 0; r < 4; r++) {
+    int32_t row[4];
+    for (int u = 0; u < 4; u++) row[u] = tmp[r * 4 + u];
+    rowf(row);
+    for (int u = 0; u < 4; u++) store_quant_target(cf, tf, u * 4 + r, row[u], mdc, mac);
+  }
+}
+
+// dct.rs:391-431 f1ddct4x4_quant_t_direct (V_DCT / H_DCT): the 1-D DCT x 2 sqrt2
+// (AVX2 avx/dct.rs:933-934 folds it into one Q16 multiply by 185364, the same
+// value), full-step quantisation, transposed storage.
+void fwd_1d_4x4(const int32_t* in, bool vertical, int32_t mdc, int32_t mac, int32_t* cf, float* tf) {
+  int32_t f[16];
+  if (vertical) {
+    for (int x = 0; x < 4; x++) {
+      int32_t col[4];
+      for (int y = 0; y < 4; y++) col[y] = in[y * 4 + x];
+      dct1d_4(col);
+      for (int y = 0; y < 4; y++) f[y * 4 + x] = mul_q16(col[y] * 2, SQRT2_Q16);
+    }
+  } else {
+    for (int y = 0; y < 4; y++) {
+      int32_t row[4];
+      for (int x = 0; x < 4; x++) row[x] = in[y * 4 + x];
+      dct1d_4(row);
+      for (int x = 0; x < 4; x++) f[y * 4 + x] = mul_q16(row[x] * 2, SQRT2_Q16);
+    }
+  }
+  for (int y = 0; y < 4; y++)
+    for (int x = 0; x < 4; x++) {
+      int rc = y + x * 4;
+      quant_fullstep(cf, tf, rc, f[y * 4 + x], rc == 0 ? mdc : mac);
     }
 }
 
@@ -285,6 +350,24 @@ void inv_adst8(int32_t* c, int s, int32_t mn, int32_t mx) {
   c[5 * s] = -(((v6 - v7) * 181 + 128) >> 8);
 }
 
+// idct.rs:2837-2865 inv_adst4_1d (no clamps).
+void inv_adst4(int32_t* c, int s) {
+  int32_t in0 = c[0], in1 = c[s], in2 = c[2 * s], in3 = c[3 * s];
+  int32_t o0 = ((1321 * in0 + (3803 - 4096) * in2 + (2482 - 4096) * in3 + (3344 - 4096) * in1 + 2048) >> 12) + in2 +
+               in3 + in1;
+  int32_t o1 = (((2482 - 4096) * in0 - 1321 * in2 - (3803 - 4096) * in3 + (3344 - 4096) * in1 + 2048) >> 12) + in0 -
+               in3 + in1;
+  int32_t o2 = (209 * (in0 - in2 + in3) + 128) >> 8;
+  int32_t o3 = (((3803 - 4096) * in0 + (2482 - 4096) * in2 - 1321 * in3 - (3344 - 4096) * in1 + 2048) >> 12) + in0 +
+               in2 - in1;
+  c[0] = o0;
+  c[s] = o1;
+  c[2 * s] = o2;
+  c[3 * s] = o3;
+}
+// idct.rs:2719-2748 identity4 step: i + (i * 1697 + 2048) >> 12.
+inline int32_t inv_id4(int32_t i) { return i + ((i * 1697 + 2048) >> 12); }
+
 // idct.rs:1562-1570 IdctDequant::step and the dequant loop shared by every
 // inverse (idct.rs:1581-1590): 24-bit magnitude wrap, cf_max clip.
 void dequant(const int32_t* lv, int n, int h, const mt_quant* q, const uint8_t* qm, int32_t* coeff) {
@@ -339,6 +422,42 @@ void inv_8x8(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* qm
   if (colk == 0)
     for (int i = 0; i < 64; i++) tmp[i] *= 2;
   for (int i = 0; i < 64; i++) out[i] = (tmp[i] + 8) >> 4;
+}
+
+// idct.rs:2719-2948 the 4x4 inverses: rows (kind by type), no inter-pass
+// shift, the column clamp, columns, (t+8)>>4; identity4 rows/columns use the
+// 1697 step; the identity family (IDTX, V_DCT, H_DCT) dequantises flat.
+void inv_4x4(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* qm, int32_t* out) {
+  int32_t coeff[16];
+  const bool flat = (tx == MT_TX_IDTX || tx == MT_TX_V_DCT || tx == MT_TX_H_DCT);
+  dequant(levels, 16, 4, q, flat ? nullptr : qm, coeff);
+  int32_t tmp[16];
+  for (int y = 0; y < 4; y++)
+    for (int x = 0; x < 4; x++) tmp[y * 4 + x] = coeff[y + x * 4];
+  int rowk, colk;  // 0 identity, 1 dct, 2 adst
+  switch (tx) {
+    case MT_TX_IDTX: rowk = 0; colk = 0; break;
+    case MT_TX_DCT_DCT: rowk = 1; colk = 1; break;
+    case MT_TX_V_DCT: rowk = 0; colk = 1; break;
+    case MT_TX_H_DCT: rowk = 1; colk = 0; break;
+    case MT_TX_ADST_ADST: rowk = 2; colk = 2; break;
+    case MT_TX_ADST_DCT: rowk = 1; colk = 2; break;
+    default: rowk = 2; colk = 1; break;  // DCT_ADST
+  }
+  for (int y = 0; y < 4; y++) {
+    if (rowk == 1) inv_dct4(tmp + y * 4, 1, q->rmin, q->rmax);
+    else if (rowk == 2) inv_adst4(tmp + y * 4, 1);
+    else
+      for (int x = 0; x < 4; x++) tmp[y * 4 + x] = inv_id4(tmp[y * 4 + x]);
+  }
+  for (int i = 0; i < 16; i++) tmp[i] = clampi(tmp[i], q->cmin, q->cmax);
+  for (int x = 0; x < 4; x++) {
+    if (colk == 1) inv_dct4(tmp + x, 4, q->cmin, q->cmax);
+    else if (colk == 2) inv_adst4(tmp + x, 4);
+    else
+      for (int y = 0; y < 4; y++) tmp[y * 4 + x] = inv_id4(tmp[y * 4 + x]);
+  }
+  for (int i = 0; i < 16; i++) out[i] = (tmp[i] + 8) >> 4;
 }
 
 // ------------------------------------------------------- cost.rs / trellis
@@ -477,6 +596,25 @@ const uint16_t* or_default_scan(int32_t n) {
 // idtx8x8_t (dc/ac steps, :2918-2924).
 void or_fwd_txfm_quant(const int32_t* resid, int32_t tx, int32_t n, const mt_quant* q,
                        const uint8_t* qm_row, int32_t* cf, float* tf) {
+  if (n == 4) {
+    // DctDispatch::dct4x4_t and the dispatch_qm_ratio_methods family
+    // (dct.rs:2465-2488, :2624-2637, :2876-2880): Q16 multipliers x 8/sqrt(16)
+    // = 2 (RATIO_4X4_Q16); V/H flat (:2510-2523, :2899-2901); IDTX dc/ac steps.
+    const int32_t r4 = 131072;
+    const int32_t mdc = mul_q16(q->q_mult_dc, r4), mac = mul_q16(q->q_mult_ac, r4);
+    switch (tx) {
+      case MT_TX_IDTX: fwd_idtx(resid, 4, 4, q->dc_q, q->ac_q, cf, tf); return;
+      case MT_TX_V_DCT: fwd_1d_4x4(resid, true, q->q_mult_dc, q->q_mult_ac, cf, tf); return;
+      case MT_TX_H_DCT: fwd_1d_4x4(resid, false, q->q_mult_dc, q->q_mult_ac, cf, tf); return;
+      case MT_TX_DCT_DCT: fwd_2d_4x4(resid, dct1d_4, dct1d_4, mdc, mac, cf, tf); break;
+      case MT_TX_ADST_ADST: fwd_2d_4x4(resid, fwd_adst4, fwd_adst4, mdc, mac, cf, tf); break;
+      case MT_TX_ADST_DCT: fwd_2d_4x4(resid, fwd_adst4, dct1d_4, mdc, mac, cf, tf); break;
+      case MT_TX_DCT_ADST: fwd_2d_4x4(resid, dct1d_4, fwd_adst4, mdc, mac, cf, tf); break;
+      default: return;
+    }
+    if (qm_row) apply_qmatrix(cf, tf, qm_row, 16);
+    return;
+  }
   if (n != 8) return;
   switch (tx) {
     case MT_TX_IDTX: fwd_idtx(resid, 8, 8, q->dc_q, q->ac_q, cf, tf); return;
@@ -493,6 +631,7 @@ void or_fwd_txfm_quant(const int32_t* resid, int32_t tx, int32_t n, const mt_qua
 
 void or_inv_txfm_dequant(const int32_t* levels, int32_t tx, int32_t n, const mt_quant* q,
                          const uint8_t* qm_row, int32_t* resid) {
+  if (n == 4) inv_4x4(levels, tx, q, qm_row, resid);
   if (n != 8) return;
   inv_8x8(levels, tx, q, qm_row, resid);
 }
@@ -1097,7 +1236,8 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
       resid[y * n + x] = (int32_t)src[(size_t)(cd.py + y) * p->stride + cd.px + x] - pred[y * n + x];
   or_fwd_txfm_quant(resid, cd.tx_type, n, q, qm, cf, tf);
   const uint16_t* scan = or_default_scan(n);
-  or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, scan, N, p->trellis_lambda0);
+  if (!(cd.flags & MT_CAND_NO_TRELLIS))
+    or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, scan, N, p->trellis_lambda0);
   or_inv_txfm_dequant(cf, cd.tx_type, n, q, qm, rr);
   const int32_t maxv = (1 << p->bd) - 1;
   uint64_t satd = or_luma_satd(src, p->stride, cd.px, cd.py, n, n, maxv, pred, rr);
@@ -1128,7 +1268,7 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
 int or_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chain_params* p, const mt_quant* q,
                        const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_candidate* cands, int32_t n,
                        mt_candidate_result* results, int32_t* levels_out, int32_t* recon_out, int32_t threads) {
-  if (!p || p->tx_size != 8) return MT_ERR_UNSUPPORTED;
+  if (!p || (p->tx_size != 8 && p->tx_size != 4)) return MT_ERR_UNSUPPORTED;
   const int N = p->tx_size * p->tx_size;
   auto work = [&](int lo, int hi) {
     for (int i = lo; i < hi; i++)
