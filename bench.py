@@ -37,9 +37,9 @@ sys.path.insert(0, ROOT)
 
 W, H, QIDX, QM_LEVEL = 1920, 1080, 70, 6
 # From one ncu capture of level8_kernel on this workload
-# (ncu --set full -k regex:level8_kernel ... python bench.py --steps 1 --warmup 3 --no-cpu):
-NCU_DRAM_BYTES_PER_LAUNCH = 52_023_040 + 781_145_856  # dram__bytes_read.sum + dram__bytes_write.sum
-NCU_WARP_INSTS_PER_LAUNCH = 1_298_978_611  # smsp__inst_executed.sum
+# (ncu --set full -k regex:"^level[48]_kernel$" ... python bench.py --steps 1 --warmup 3 --no-cpu):
+NCU_DRAM_BYTES_PER_LAUNCH = 198_752_000 + 1_367_270_000  # dram__bytes_read.sum + dram__bytes_write.sum
+NCU_WARP_INSTS_PER_LAUNCH = 1_224_376_834  # smsp__inst_executed.sum
 ISSUE_PEAK_PER_CLK = 148 * 4  # SMs x schedulers, one warp-instruction each per clock
 MODES = list(range(13))
 MPIX = W * H / 1e6
@@ -162,6 +162,67 @@ def run_reference(args):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def measure_level4(dev, wl, reps=5, cpu=True):
+    """The batched 4x4 level over the same 1080p luma (129,600 4x4 blocks x 13
+    modes x the SPLIT4 trial types DCT, ADST, IDTX-without-trellis, ADST_DCT,
+    DCT_ADST): device time with CUDA events after an L2 flush, and the oracle
+    on all host cores over the same candidates."""
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    q = mt.quant_new(QIDX, 8, QM_LEVEL)
+    qm = mt.qm_row(QM_LEVEL, 0, 4)
+    blocks = synth.level_blocks(W, H, n=4, seed=3)
+    combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX, abi.TX_ADST_DCT,
+                                        abi.TX_DCT_ADST), no_trellis_types=(abi.TX_IDTX,))
+    cdfs = synth.synthetic_cdfs(4, n_eob_bins=5)
+    costs = mt.coef_costs(cdfs)
+    prm = mt.chain_params(W, H, tx_size=4, trellis_lambda0=0.05, mode_lambda=wl["prm"].mode_lambda,
+                          satd_scale=wl["prm"].satd_scale, satd_bridge=wl["prm"].satd_bridge)
+    nb, nc = len(blocks), len(combos)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d = [t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)), t(blocks), t(combos)]
+    d_best = torch.empty(nb * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_res = torch.empty(nb * nc * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_keys = torch.empty(mt.load().mt_rdo_level4_scratch_bytes(nb, nc), dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    import ctypes as C
+
+    def launch():
+        rc = mt.load().mt_rdo_level4_device(d[0].data_ptr(), d[1].data_ptr(), C.byref(prm), C.byref(q),
+                                            d[2].data_ptr(), d[3].data_ptr(), d[4].data_ptr(), nb, d[5].data_ptr(), nc,
+                                            d_best.data_ptr(), d_res.data_ptr(), d_keys.data_ptr(), None)
+        assert rc == 0, rc
+
+    for _ in range(3):
+        launch()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    step = float(np.median(ms))
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "candidates": nb * nc,
+           "workload": "rdo-level-4x4 1920x1080 luma, qindex 70, QM 6, 13 modes x 5 types (IDTX without trellis)"}
+    if cpu:
+        from oracle import pyoracle as po
+
+        cands = synth.candidates_of_level(blocks, combos)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        po.candidate_chain(wl["src"], wl["rec"], prm, q, qm, cdfs, cands, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                               "sample": f"the whole level, {len(cands)} candidates ({dt:.2f} s)"}
+    return out
 
 
 def measure_filters(dev, wl, hbm_peak, reps=5):
@@ -348,6 +409,7 @@ def run_ours(args):
     issue_rate = NCU_WARP_INSTS_PER_LAUNCH / (step_ms / 1e3)
 
     filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
+    level4 = measure_level4(dev, wl, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -377,7 +439,9 @@ def run_ours(args):
                            "peak_ginst_s": round(issue_peak / 1e9, 1), "frac": round(issue_rate / issue_peak, 4),
                            "inst_per_launch": NCU_WARP_INSTS_PER_LAUNCH, "sm_clock_mhz": clk_mhz},
         "frame_filters": filters,
-        "gpu_launches": 2 * args.steps,  # level8_kernel + level8_finalize_kernel per step
+        "level4": level4,
+        # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
+        "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
