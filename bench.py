@@ -270,6 +270,17 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     ms = timed(lambda: lib.mt_csc_rgb8_device(d_rgb.data_ptr(), W, H, 2, y.data_ptr(), cb.data_ptr(), cr.data_ptr(),
                                               None))
     out["csc"] = entry(ms, W * H * 3 + (pw * ph + 2 * pcw * pch) * 2, "3 B/px in + 2 B per output sample")
+    # adaptive-quantisation grid over the padded luma the conversion produced
+    nsb = ((pw + 63) // 64) * ((ph + 63) // 64)
+    cells = torch.empty(nsb * 4, dtype=torch.uint8, device=dev)
+    refs = torch.empty(2 * 64, dtype=torch.float32, device=dev)
+    for tag, q in (("aq_grid", QIDX), ("aq_grid_q116", 116)):
+        ap = mt.aq_params(pw, ph, q)
+        ascr = torch.empty(lib.mt_aq_grid_scratch_bytes(C.byref(ap)), dtype=torch.uint8, device=dev)
+        ms = timed(lambda: lib.mt_aq_grid_device(y.data_ptr(), C.byref(ap), cells.data_ptr(), refs.data_ptr(),
+                                                 ascr.data_ptr(), None))
+        out[tag] = entry(ms, pw * ph * 2, "2 B luma read per sample")
+        out[tag]["bound"] = "launch / per-tile serial means (two kernels; dark protection from qindex 90)"
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)

@@ -425,6 +425,61 @@ int mt_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* src_y, 
                   const uint16_t* src_v, const uint8_t* skip8, const mt_cdef_params* prm, mt_cdef_decision* out,
                   uint8_t* grid);
 
+/* ---- Adaptive quantisation: the per-superblock qindex grid ----
+ * Replaces the frame pre-pass of the reference's tile encoder: for every tile,
+ * tile_ref_activity / tile_ref_picked (src/coder/aq.rs:162-192) and
+ * precompute_aq_grid -> aq_sb_target (src/coder/lossy_state.rs:3796-3963), with
+ * Variance Boost (src/aq_common.rs:58-150), dark-structure protection
+ * (src/aq_common.rs:216-345, DarkAq::on) and the relative step clamp
+ * (src/coder/lossy_state.rs:133-154).  Shipped tuning: aq_slope 5, aq_max_delta
+ * 28, aq_r 1.35, top_ease 1 / knee 20 / width 12, delta_q_res 2 (steps of 4
+ * qindex, at most 12 per superblock).
+ *
+ * The luma plane is the padded source, w8 x h8 u16 row-major (stride w8).
+ * Tiles follow the frame header's uniform spacing for the given log2 counts
+ * (src/coder/tiling.rs:138-147); each tile has at most 64 superblock columns
+ * and 2304 superblocks (the AV1 limits), else MT_ERR_INVALID_INPUT.  The chain
+ * restarts at base_q_idx in every tile. */
+typedef struct mt_aq_params {
+  int32_t w8, h8;           /* padded luma size, multiples of 8, at most 16384 */
+  int32_t tile_cols_log2;   /* the frame's tiling (see mt_tiling_spec_min) */
+  int32_t tile_rows_log2;
+  int32_t base_q_idx;       /* frame base qindex 0..255 */
+  int32_t bd;               /* 8, 10 or 12 */
+  int32_t variance_boost;   /* 1: Variance Boost (octile of the 8x8 variances); 0: classic whole-SB AQ */
+  int32_t dark_aq;          /* 1: dark-structure protection (active from base qindex 90) */
+  int32_t octile;           /* 1..8 (clamped), 6 by default */
+  int32_t boost_only;       /* 1: never coarsen; 0 by default */
+  float strength;           /* Variance Boost strength (negative clamps to 0), 1 by default */
+} mt_aq_params;
+
+/* One superblock of the grid (AqCell, src/coder/aq.rs:325-342). */
+typedef struct mt_aq_cell {
+  uint8_t prev;    /* raster-chain qindex before the superblock */
+  uint8_t newq;    /* the superblock's qindex */
+  int8_t steps;    /* signalled reducedDeltaQIndex, -12..12 */
+  uint8_t target;  /* aq_sb_target, the qindex the steps move toward */
+} mt_aq_cell;
+
+/* The spec-minimum tiling the reference encodes with (plan_tiling with one
+ * target tile, src/coder/tiling.rs:92-136). */
+int mt_tiling_spec_min(int32_t w8, int32_t h8, int32_t* cols_log2, int32_t* rows_log2);
+/* Device working storage mt_aq_grid_device needs. */
+size_t mt_aq_grid_scratch_bytes(const mt_aq_params* prm);
+/* The grid on the stream: d_cells holds (ceil(h8/64) x ceil(w8/64)) cells in
+ * frame raster order; d_tile_refs (may be NULL) two floats per tile in raster
+ * order of tiles: ref_act (tile mean whole-SB log-activity) and ref_pick (tile
+ * mean log octile variance). */
+int mt_aq_grid_device(const uint16_t* d_luma, const mt_aq_params* prm, mt_aq_cell* d_cells, float* d_tile_refs,
+                      void* d_scratch, void* stream);
+/* Host-buffer form of mt_aq_grid_device. */
+int mt_aq_grid(const uint16_t* luma, const mt_aq_params* prm, mt_aq_cell* cells, float* tile_refs);
+/* The dark-protection weight's power for each x: equal to the host C
+ * library's powf(x, 1.2f) for every x in (1, 4.5], the range the weight uses
+ * (72 / (16 + mean) with mean >= 0, clamped to [1, 4.5] after the power);
+ * elsewhere the binary64 power rounded once to binary32. */
+int mt_dark_pow_device(const float* d_x, float* d_out, int64_t n, void* stream);
+
 /* Library version string. */
 const char* mt_version(void);
 

@@ -229,6 +229,56 @@ def cdef_frame(recon, src, skip8, prm):
     return out, _decision_dict(d, grid)
 
 
+def tiling_spec_min(w8, h8):
+    """``plan_tiling(sb_cols, sb_rows, 1)`` (src/coder/tiling.rs:92-136): (cols_log2, rows_log2)."""
+    a, b = C.c_int32(), C.c_int32()
+    _check(load().mt_tiling_spec_min(w8, h8, C.byref(a), C.byref(b)), "mt_tiling_spec_min")
+    return a.value, b.value
+
+
+def aq_params(w8, h8, base_q_idx, bd=8, variance_boost=True, dark_aq=True, octile=6, boost_only=False,
+              strength=1.0, tiling=None):
+    """``mt_aq_params`` with the reference's defaults (adaptive quant, Variance
+    Boost and dark protection on); tiling defaults to the spec minimum."""
+    p = abi.AqParams()
+    p.w8, p.h8 = w8, h8
+    p.tile_cols_log2, p.tile_rows_log2 = tiling if tiling is not None else tiling_spec_min(w8, h8)
+    p.base_q_idx, p.bd, p.variance_boost, p.dark_aq = base_q_idx, bd, int(variance_boost), int(dark_aq)
+    p.octile, p.boost_only, p.strength = octile, int(boost_only), strength
+    return p
+
+
+def aq_grid(luma, prm):
+    """``precompute_aq_grid`` of every tile (src/coder/lossy_state.rs:3937-3963).
+
+    luma: (h8, w8) u16 padded source.  Returns (cells, tile_refs): cells an
+    (sb_rows, sb_cols) array of ``AQ_CELL_DTYPE``, tile_refs (ntiles, 2) f32."""
+    luma = np.ascontiguousarray(luma, np.uint16)
+    assert luma.shape == (prm.h8, prm.w8)
+    sbr, sbc = (prm.h8 + 63) // 64, (prm.w8 + 63) // 64
+    cells = np.zeros((sbr, sbc), abi.AQ_CELL_DTYPE)
+    tc = -(-sbc // -(-sbc // (1 << prm.tile_cols_log2)))
+    tr = -(-sbr // -(-sbr // (1 << prm.tile_rows_log2)))
+    refs = np.zeros((tc * tr, 2), np.float32)
+    _check(load().mt_aq_grid(ptr(luma), C.byref(prm), ptr(cells), ptr(refs)), "mt_aq_grid")
+    return cells, refs
+
+
+def aq_grid_device(d_luma, prm, d_cells, d_tile_refs, d_scratch, stream=0):
+    """Device form: torch tensors (or raw pointers) on the current device."""
+    _check(load().mt_aq_grid_device(ptr(d_luma), C.byref(prm), ptr(d_cells), ptr(d_tile_refs), ptr(d_scratch),
+                                    stream or None), "mt_aq_grid_device")
+
+
+def aq_grid_scratch_bytes(prm):
+    return load().mt_aq_grid_scratch_bytes(C.byref(prm))
+
+
+def dark_pow_device(d_x, d_out, n, stream=0):
+    """The dark-protection weight's power (``powf(x, 1.2f)`` of the C library on (1, 4.5])."""
+    _check(load().mt_dark_pow_device(ptr(d_x), ptr(d_out), n, stream or None), "mt_dark_pow_device")
+
+
 def loop_filter_levels(base_q_idx, sub_x, sub_y):
     """``loop_filter_levels`` / ``loop_filter_sharpness`` (src/obu.rs:306-334): (lvl_y, lvl_uv, sharp)."""
     a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

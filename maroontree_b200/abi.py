@@ -88,6 +88,17 @@ class CdefDecision(C.Structure):
 
 assert C.sizeof(CdefParams) == 40 and C.sizeof(CdefDecision) == 52
 
+
+class AqParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "tile_cols_log2", "tile_rows_log2", "base_q_idx", "bd",
+                                         "variance_boost", "dark_aq", "octile", "boost_only")] + [
+        ("strength", C.c_float)]
+
+
+assert C.sizeof(AqParams) == 44
+
+AQ_CELL_DTYPE = np.dtype([("prev", "u1"), ("newq", "u1"), ("steps", "i1"), ("target", "u1")])
+
 BLOCK8_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
     ("mode_bits", "<f4", (13,)),
@@ -152,6 +163,11 @@ def _bind(lib):
         "mt_cdef_scratch_bytes": (C.c_size_t, [C.POINTER(CdefParams)]),
         "mt_cdef_frame_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams), _P, C.POINTER(CdefDecision), _P, _P]),
         "mt_cdef_frame": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams), C.POINTER(CdefDecision), _P]),
+        "mt_tiling_spec_min": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "mt_aq_grid_scratch_bytes": (C.c_size_t, [C.POINTER(AqParams)]),
+        "mt_aq_grid_device": (C.c_int, [_P, C.POINTER(AqParams), _P, _P, _P, _P]),
+        "mt_aq_grid": (C.c_int, [_P, C.POINTER(AqParams), _P, _P]),
+        "mt_dark_pow_device": (C.c_int, [_P, _P, C.c_int64, _P]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -186,6 +202,7 @@ EXPORTED_SYMBOLS = (
     "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
+    "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
 )
 
 

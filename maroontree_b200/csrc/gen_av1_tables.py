@@ -13,7 +13,7 @@ Usage (from the repository root, with the reference checkout available)::
     python maroontree_b200/csrc/gen_av1_tables.py <reference-root>
 
 Source locations (reference paths):
-  src/coef_q.rs     DC_QLOOKUP_8, AC_QLOOKUP_8, SCAN_16X16, SCAN_32X32
+  src/coef_q.rs     DC_QLOOKUP_8, AC_QLOOKUP_8/10/12, SCAN_16X16, SCAN_32X32
   src/tables.rs     SCAN_8X8, SCAN_4X4, LO_CTX_OFF, LO_CTX_OFF_WLH, LO_CTX_OFF_WGH
   src/qm_tables.rs  AV1_IQM  ([15][2][3344] u8)
 """
@@ -25,6 +25,8 @@ TABLES = [
     # (file, rust name, C name, C type)
     ("src/coef_q.rs", "DC_QLOOKUP_8", "MT_DC_QLOOKUP_8", "uint16_t"),
     ("src/coef_q.rs", "AC_QLOOKUP_8", "MT_AC_QLOOKUP_8", "uint16_t"),
+    ("src/coef_q.rs", "AC_QLOOKUP_10", "MT_AC_QLOOKUP_10", "uint16_t"),
+    ("src/coef_q.rs", "AC_QLOOKUP_12", "MT_AC_QLOOKUP_12", "uint16_t"),
     ("src/skip_tables.rs", "SCAN_4X4", "MT_SCAN_4X4", "uint16_t"),
     ("src/tables.rs", "SCAN_8X8", "MT_SCAN_8X8", "uint16_t"),
     ("src/coef_q.rs", "SCAN_16X16", "MT_SCAN_16X16", "uint16_t"),

@@ -81,6 +81,14 @@ int or_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* sy, con
                   int64_t* luma_tab, int64_t* u_tab, int64_t* v_tab, uint8_t* dirs, int32_t* vars);
 float or_weighted_sse(const int32_t* err, int32_t w, int32_t h);
 float or_cdef_frame_lambda(int32_t qidx, int32_t bd, int32_t sub_x, int32_t sub_y);
+/* aq_common.rs / coder/aq.rs / lossy_state.rs: the adaptive-quantisation grid and its pieces. */
+float or_fast_round(float x);
+float or_dirty_log1pf(float d);
+void or_dark_pow(const float* x, float* out, int64_t n);
+int32_t or_dark_protection(int32_t enabled, int32_t base_q, const uint16_t* yp, int32_t pw, int32_t sb_y, int32_t sb_x,
+                           int32_t width, int32_t height, float scale);
+int or_tiling_spec_min(int32_t w8, int32_t h8, int32_t* cols_log2, int32_t* rows_log2);
+int or_aq_grid(const uint16_t* luma, const mt_aq_params* p, mt_aq_cell* cells, float* refs_out);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 

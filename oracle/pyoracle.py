@@ -49,6 +49,12 @@ def load():
             "or_deblock_plane": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P, _P, _P,
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
+            "or_fast_round": (C.c_float, [C.c_float]),
+            "or_dirty_log1pf": (C.c_float, [C.c_float]),
+            "or_dark_pow": (None, [_P, _P, C.c_int64]),
+            "or_dark_protection": (C.c_int32, [C.c_int32, C.c_int32, _P] + [C.c_int32] * 5 + [C.c_float]),
+            "or_tiling_spec_min": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "or_aq_grid": (C.c_int, [_P, C.POINTER(abi.AqParams), _P, _P]),
             "or_candidate_chain": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), C.POINTER(abi.Quant), _P,
                                              C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
@@ -230,3 +236,36 @@ def real_block_bits_wh(cf, scan, w, h, cdfs, skip_ctx, dcs_ctx, txtp_mode=-1, tx
     sb = None if skip_bits is None else np.ascontiguousarray(skip_bits, np.float32)
     return load().or_real_block_bits_wh(p(cf), p(scan), w, h, C.byref(cdfs), skip_ctx, dcs_ctx, txtp_mode, txtp,
                                         int(sb is not None), None if sb is None else p(sb))
+
+
+def dark_protection(plane, base_q, bd=8, enabled=True, sb_x=0, sb_y=0):
+    """dark_protection over the SB at (sb_x, sb_y) of a u16 plane (src/aq_common.rs:312-345)."""
+    plane = np.ascontiguousarray(plane, np.uint16)
+    h, w = plane.shape
+    scale = np.float32(1.0) / np.float32(1 << (bd - 8))
+    return load().or_dark_protection(int(enabled), base_q, p(plane), w, sb_y, sb_x, w, h, float(scale))
+
+
+def dark_pow(x):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    load().or_dark_pow(p(x), p(out), x.size)
+    return out
+
+
+def tiling_spec_min(w8, h8):
+    a, b = C.c_int32(), C.c_int32()
+    assert load().or_tiling_spec_min(w8, h8, C.byref(a), C.byref(b)) == 0
+    return a.value, b.value
+
+
+def aq_grid(luma, prm):
+    """Returns (cells (sb_rows, sb_cols) AQ_CELL_DTYPE, tile refs (ntiles, 2) f32)."""
+    luma = np.ascontiguousarray(luma, np.uint16)
+    sbr, sbc = (prm.h8 + 63) // 64, (prm.w8 + 63) // 64
+    cells = np.zeros((sbr, sbc), abi.AQ_CELL_DTYPE)
+    tc = -(-sbc // -(-sbc // (1 << prm.tile_cols_log2)))
+    tr = -(-sbr // -(-sbr // (1 << prm.tile_rows_log2)))
+    refs = np.zeros((tc * tr, 2), np.float32)
+    assert load().or_aq_grid(p(luma), C.byref(prm), p(cells), p(refs)) == 0
+    return cells, refs
