@@ -239,13 +239,17 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     t8 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.uint8)).to(dev)
 
     def timed(fn, reset=None):
+        # The GPU is kept busy (L2 flush, then a ~100 us spin) while the host
+        # enqueues the start event, the call's launches and the end event, so
+        # the events bracket device time, not the host's launch latency.
         ms = []
         for i in range(reps + 2):
             if reset:
                 reset()
-            flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
+            flush.zero_()
+            torch.cuda._sleep(200_000)
             a.record()
             rc = fn()
             b.record()

@@ -40,6 +40,9 @@ constexpr int kMaxTileSbs = 2304;   // AV1 MAX_TILE_AREA / (64 * 64)
 constexpr int kMaxChunks = (kMaxTileSbs + kChunk - 1) / kChunk;
 constexpr int kDarkMinQ = 90;       // DarkAq::on (src/aq_common.rs:206-212)
 
+// Ac_Qlookup at 8 / 10 / 12 bits (src/coef_q.rs), for the relative step clamp.
+__device__ const uint16_t kAcQ[3][256] = {{MT_AC_QLOOKUP_8_LIST}, {MT_AC_QLOOKUP_10_LIST}, {MT_AC_QLOOKUP_12_LIST}};
+
 struct AqGeom {
   int w8, h8, sb_cols, sb_rows;
   int tc_size, tr_size;      // tile size in superblocks (uniform spacing)
@@ -47,7 +50,6 @@ struct AqGeom {
   int chunks_per_tile;       // chunk slots per tile: ceil(tc_size * tr_size / 32)
   int base_q, bd, vb, dark, octile, boost_only;
   float strength;
-  uint16_t ac_q[256];
 };
 
 struct SbStat {
@@ -69,7 +71,7 @@ __device__ __forceinline__ int32_t to_i32(float v) { return __float2int_rz(v); }
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 
 // aq_common.rs:89-109 dirty_log1pf, f_fmlaf unfused (multiply, round, add, round).
-__device__ float dirty_log1pf(float d) {
+__device__ __forceinline__ float dirty_log1pf(float d) {
   const uint32_t ix = __float_as_uint(__fadd_rn(1.0f, d));
   const int32_t n = (int32_t)((ix & 0x7f800000u) >> 23) - 0x7f;
   const float mant = __uint_as_float((ix & 0x007fffffu) | 0x3f800000u);
@@ -85,16 +87,15 @@ __device__ float dirty_log1pf(float d) {
 }
 
 // powf(x, 1.2f) as the host C library rounds it: the binary64 power rounded
-// once, except on the listed inputs where the library's result is taken.
+// once, except on the listed inputs where the library's result is taken (a
+// bucket of at most 15 entries, found through the 4096-float bucket index).
 __device__ float dark_pow(float x) {
   const uint32_t u = __float_as_uint(x);
-  int lo = 0, hi = MT_DARK_POW_N;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (kDarkPowX[mid] < u) lo = mid + 1;
-    else hi = mid;
+  if (u > MT_DARK_POW_BASE && u <= MT_DARK_POW_BASE + ((uint32_t)(MT_DARK_POW_NB - 1) << MT_DARK_POW_SHIFT)) {
+    const uint32_t b = (u - MT_DARK_POW_BASE) >> MT_DARK_POW_SHIFT;
+    for (int i = kDarkPowB[b], e = kDarkPowB[b + 1]; i < e; i++)
+      if (kDarkPowX[i] == u) return __uint_as_float(kDarkPowR[i]);
   }
-  if (lo < MT_DARK_POW_N && kDarkPowX[lo] == u) return __uint_as_float(kDarkPowR[lo]);
   return __double2float_rn(pow((double)x, (double)1.2f));
 }
 
@@ -112,6 +113,13 @@ __device__ __forceinline__ int warp_sum_i(int v) {
   return v;
 }
 
+__device__ __forceinline__ int lap_at(const uint16_t (*p)[64], int r, int c) {
+  return 4 * (int)p[r][c] - p[r - 1][c] - p[r + 1][c] - p[r][c - 1] - p[r][c + 1];
+}
+__device__ __forceinline__ int lap_at(const int32_t (*p)[32], int r, int c) {
+  return 4 * p[r][c] - p[r - 1][c] - p[r + 1][c] - p[r][c - 1] - p[r][c + 1];
+}
+
 __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__ luma, const AqGeom g,
                                                     SbStat* __restrict__ stats, uint32_t* __restrict__ counters,
                                                     int n_counters) {
@@ -120,7 +128,7 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
   __shared__ float s_var[64];
   __shared__ uint32_t s_bsum[64], s_bssq[64];
   __shared__ int s_red[2][8];
-  __shared__ float s_pick;
+  __shared__ float s_pick, s_wgt;
   const int tid = threadIdx.x;
   const int sb = blockIdx.x;
   if (sb == 0)
@@ -128,6 +136,8 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
   const int sbr = sb / g.sb_cols, sbc = sb - sbr * g.sb_cols;
   const int y0 = sbr * 64, x0 = sbc * 64;
   const int h = min(g.h8 - y0, 64), w = min(g.w8 - x0, 64);  // multiples of 8
+  const int bd = g.bd;
+  const bool dark_on = g.dark && g.base_q >= kDarkMinQ;
   // Stage: 64 rows x 8 segments of 8 samples, two segments per thread.
 #pragma unroll
   for (int k = 0; k < 2; k++) {
@@ -160,9 +170,17 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
       s_var[b] = valid ? var_of((long long)s, q, 64) : __int_as_float(0x7fc00000);
     }
   }
+  // 2x box sums for the dark statistics (value = Q * scale / 4).
+  const int hh = h >> 1, ww = w >> 1;
+  if (dark_on)
+    for (int i = tid; i < hh * ww; i += 256) {
+      const int y = i / ww, x = i - y * ww;
+      s_half[y][x] = (int)s_px[2 * y][2 * x] + s_px[2 * y][2 * x + 1] + s_px[2 * y + 1][2 * x] +
+                     s_px[2 * y + 1][2 * x + 1];
+    }
   __syncthreads();
-  const int bd = g.bd;
   const int nblk = (h >> 3) * (w >> 3);
+  const float scale = __fdiv_rn(1.0f, (float)(1u << (bd - 8)));
   float act = 0.0f, pick_log = 0.0f;
   if (tid < 32) {
     // Whole-SB moments from the block moments (exact).
@@ -191,9 +209,9 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
     // smaller values is <= k and whose count of smaller-or-equal values is > k.
     const int k = min(g.octile * 8 - 1, 63);
     int lt0 = 0, le0 = 0, lt1 = 0, le1 = 0;
+#pragma unroll 16
     for (int j = 0; j < 64; j++) {
-      float vj = s_var[j];
-      if (vj != vj) vj = fill;
+      const float vj = __shfl_sync(0xffffffffu, j < 32 ? v0 : v1, j & 31);
       lt0 += vj < v0;
       le0 += vj <= v0;
       lt1 += vj < v1;
@@ -205,32 +223,33 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
     const float var_scale = __fdiv_rn(1.0f, (float)(1u << (2 * (bd - 8))));
     pick_log = dirty_log1pf(__fmul_rn(s_pick, var_scale));
   }
-  // Dark-structure protection.
+  // Dark-structure protection (src/aq_common.rs:262-345).
   int dark = 0;
-  if (g.dark && g.base_q >= kDarkMinQ) {
-    const float scale = __fdiv_rn(1.0f, (float)(1u << (bd - 8)));
-    // Full-resolution |Laplacian| over the interior, in integer sample units.
-    int lf = 0;
+  if (dark_on) {
+    if (tid == 32) {
+      // The weight's power, started early: its table walk overlaps the Laplacians.
+      // The sample sum is exact in f32 at every depth (< 2^24 sample units):
+      // sum(px * scale) = S * scale.
+      float mean;
+      {
+        long long s = 0;
+        for (int b = 0; b < 64; b++) s += s_bsum[b];
+        mean = __fdiv_rn(__fmul_rn(__ll2float_rn(s), scale), (float)(h * w));
+      }
+      const float x = __fdiv_rn(72.0f, __fadd_rn(16.0f, mean));
+      s_wgt = x > 1.0f ? clampf(dark_pow(x), 1.0f, 4.5f) : 1.0f;
+    }
+    // |Laplacian| sums in integer units of the sample scale (full) and of a quarter of it (half).
+    int lf = 0, lh = 0;
     const int iw = w - 2, ni = (h - 2) * iw;
     for (int i = tid; i < ni; i += 256) {
       const int r = 1 + i / iw, c = 1 + i % iw;
-      const int L = 4 * (int)s_px[r][c] - s_px[r - 1][c] - s_px[r + 1][c] - s_px[r][c - 1] - s_px[r][c + 1];
-      lf += abs(L);
+      lf += abs(lap_at(s_px, r, c));
     }
-    // 2x box sums (value = Q * scale / 4).
-    const int hh = h >> 1, ww = w >> 1;
-    for (int i = tid; i < hh * ww; i += 256) {
-      const int y = i / ww, x = i % ww;
-      s_half[y][x] = (int)s_px[2 * y][2 * x] + s_px[2 * y][2 * x + 1] + s_px[2 * y + 1][2 * x] +
-                     s_px[2 * y + 1][2 * x + 1];
-    }
-    __syncthreads();
-    int lh = 0;
     const int hw = ww - 2, nh = (hh - 2) * hw;
     for (int i = tid; i < nh; i += 256) {
       const int r = 1 + i / hw, c = 1 + i % hw;
-      const int L = 4 * s_half[r][c] - s_half[r - 1][c] - s_half[r + 1][c] - s_half[r][c - 1] - s_half[r][c + 1];
-      lh += abs(L);
+      lh += abs(lap_at(s_half, r, c));
     }
     lf = warp_sum_i(lf);
     lh = warp_sum_i(lh);
@@ -240,24 +259,21 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
     }
     __syncthreads();
     if (tid == 0) {
-      long long tf = 0, th = 0, sum = 0;
+      long long tf = 0, th = 0;
       for (int i = 0; i < 8; i++) {
         tf += s_red[0][i];
         th += s_red[1][i];
       }
-      for (int b = 0; b < 64; b++) sum += s_bsum[b];
-      // The sample sum is exact in f32 at every depth (< 2^24 sample units).
-      const float mean = __fdiv_rn(__fmul_rn(__ll2float_rn(sum), scale), (float)(h * w));
+      // Every partial sum of the reference's f32 loop is an integer multiple of
+      // the unit below 2^24 units, hence exact, when the integer total is; else
+      // (busy 12-bit content) the loop is re-run in the reference's order.
       float sf, sh;
       if (tf < (1 << 24)) {
         sf = __fmul_rn(__ll2float_rn(tf), scale);
-      } else {  // 12-bit, very busy: the reference's sequential f32 sum
+      } else {
         sf = 0.0f;
         for (int r = 1; r + 1 < h; r++)
-          for (int c = 1; c + 1 < w; c++) {
-            const int L = 4 * (int)s_px[r][c] - s_px[r - 1][c] - s_px[r + 1][c] - s_px[r][c - 1] - s_px[r][c + 1];
-            sf = __fadd_rn(sf, __fmul_rn((float)abs(L), scale));
-          }
+          for (int c = 1; c + 1 < w; c++) sf = __fadd_rn(sf, __fmul_rn((float)abs(lap_at(s_px, r, c)), scale));
       }
       const float qs = __fmul_rn(scale, 0.25f);
       if (th < (1 << 24)) {
@@ -265,17 +281,13 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
       } else {
         sh = 0.0f;
         for (int r = 1; r + 1 < hh; r++)
-          for (int c = 1; c + 1 < ww; c++) {
-            const int L = 4 * s_half[r][c] - s_half[r - 1][c] - s_half[r + 1][c] - s_half[r][c - 1] - s_half[r][c + 1];
-            sh = __fadd_rn(sh, __fmul_rn((float)abs(L), qs));
-          }
+          for (int c = 1; c + 1 < ww; c++) sh = __fadd_rn(sh, __fmul_rn((float)abs(lap_at(s_half, r, c)), qs));
       }
       const float lap_full = __fdiv_rn(sf, (float)((h - 2) * (w - 2)));
       const float lap_half = __fdiv_rn(sh, (float)((hh - 2) * (ww - 2)));
       const float mid = __fsqrt_rn(__fmul_rn(lap_full, lap_half));
       if (mid > 0.0f) {
-        const float wgt = clampf(dark_pow(__fdiv_rn(72.0f, __fadd_rn(16.0f, mean))), 1.0f, 4.5f);
-        const float darkness = __fsub_rn(wgt, 1.0f);
+        const float darkness = __fsub_rn(s_wgt, 1.0f);
         if (darkness > 0.0f) {
           const float ds = dirty_log1pf(__fmul_rn(mid, darkness));
           dark = to_i32(fast_round(fmaxf(fminf(__fmul_rn(ds, 4.0f), 16.0f), 0.0f)));
@@ -293,15 +305,21 @@ __global__ void __launch_bounds__(256) aq_sb_kernel(const uint16_t* __restrict__
   }
 }
 
-// clamp_aq_delta_relative (lossy_state.rs:133-154), aq_r 1.35.
-__device__ int32_t clamp_delta_relative(const AqGeom& g, int32_t base_q, int32_t delta) {
+// The frame constants aq_sb_target reads.
+struct TargetConsts {
+  int base_q, vb, boost_only;
+  float strength, mid_t, low_log, boost_slope, cut_slope, ease;
+};
+
+// clamp_aq_delta_relative (lossy_state.rs:133-154), aq_r 1.35; acq = Ac_Qlookup.
+__device__ __forceinline__ int32_t clamp_delta_relative(const uint16_t* acq, int32_t base_q, int32_t delta) {
   if (delta == 0) return 0;
   const float r = delta > 0 ? 1.35f : fmaxf(1.35f, 1.05f);
-  const float base_step = (float)g.ac_q[min(max(base_q, 1), 255)];
+  const float base_step = (float)acq[min(max(base_q, 1), 255)];
   const float lo = __fdiv_rn(base_step, r), hi = __fmul_rn(base_step, r);
   int32_t d = delta;
   while (d != 0) {
-    const float s = (float)g.ac_q[min(max(base_q + d, 1), 255)];
+    const float s = (float)acq[min(max(base_q + d, 1), 255)];
     if (s >= lo && s <= hi) break;
     d -= d > 0 ? 1 : -1;
   }
@@ -309,29 +327,25 @@ __device__ int32_t clamp_delta_relative(const AqGeom& g, int32_t base_q, int32_t
 }
 
 // aq_sb_target (lossy_state.rs:3796-3902) from the superblock's statistics.
-__device__ int32_t sb_target(const AqGeom& g, const SbStat& st, float ref_act, float ref_pick) {
-  const int32_t base_q = g.base_q;
+__device__ __forceinline__ int32_t sb_target(const TargetConsts& k, const uint16_t* acq, const SbStat& st,
+                                             float ref_act, float ref_pick) {
+  const int32_t base_q = k.base_q;
   const int32_t dark = st.dark;
   int32_t delta;
-  if (g.vb) {
+  if (k.vb) {
     if (st.filled == 0) return base_q;
     // variance_boost_delta (aq_common.rs:115-150), cut_wide_t 0.
-    const float mid_t = clampf(__fdiv_rn(__fsub_rn((float)base_q, 48.0f), 48.0f), 0.0f, 1.0f);
-    const float strength = fmaxf(g.strength, 0.0f);
     const float v_log = st.pick_log;
-    const float low_log = __fadd_rn(__fmul_rn(0.5f, mid_t), 5.549076f);
-    const float boost_slope = __fadd_rn(5.0f, __fmul_rn(1.5f, mid_t));
-    const float cut_slope = __fadd_rn(6.0f, __fmul_rn(2.0f, mid_t));
     int32_t vb_delta;
-    if (v_log < low_log) {
-      const float d = fminf(__fmul_rn(__fmul_rn(__fsub_rn(low_log, v_log), boost_slope), strength), 18.0f);
+    if (v_log < k.low_log) {
+      const float d = fminf(__fmul_rn(__fmul_rn(__fsub_rn(k.low_log, v_log), k.boost_slope), k.strength), 18.0f);
       vb_delta = -to_i32(fast_round(d));
-    } else if (g.boost_only) {
+    } else if (k.boost_only) {
       vb_delta = 0;
     } else {
       const float anchor = ref_pick > 0.0f ? ref_pick : __fmul_rn(ref_act, 0.95f);
-      const float over = fmaxf(__fsub_rn(v_log, fmaxf(anchor, low_log)), 0.0f);
-      const float d = fminf(__fmul_rn(__fmul_rn(over, cut_slope), strength), 16.0f);
+      const float over = fmaxf(__fsub_rn(v_log, fmaxf(anchor, k.low_log)), 0.0f);
+      const float d = fminf(__fmul_rn(__fmul_rn(over, k.cut_slope), k.strength), 16.0f);
       vb_delta = to_i32(fast_round(d));
     }
     const int32_t flat_boost = max(-vb_delta, 0);
@@ -339,11 +353,7 @@ __device__ int32_t sb_target(const AqGeom& g, const SbStat& st, float ref_act, f
     if (vb_delta > 0 && dark > 0) delta = vb_delta - dark;
     else if (protection > 0) delta = -protection;
     else delta = vb_delta;
-    if (delta > 0) {
-      const float t = clampf(__fdiv_rn(__fsub_rn(20.0f, (float)base_q), 12.0f), 0.0f, 1.0f);
-      const float gate = __fsub_rn(1.0f, __fmul_rn(1.0f, t));
-      delta = to_i32(fast_round(__fmul_rn((float)delta, gate)));
-    }
+    if (delta > 0) delta = to_i32(fast_round(__fmul_rn((float)delta, k.ease)));
   } else {
     // aq_target_qidx (aq.rs:201-214): slope 5, max delta 28.
     const float dl = clampf(__fmul_rn(__fsub_rn(st.act, ref_act), 5.0f), -28.0f, 28.0f);
@@ -352,14 +362,15 @@ __device__ int32_t sb_target(const AqGeom& g, const SbStat& st, float ref_act, f
     const int32_t protection = max(max(-vb_delta, 0), dark);
     delta = protection > 0 ? -protection : vb_delta;
   }
-  delta = clamp_delta_relative(g, base_q, delta);
+  delta = clamp_delta_relative(acq, base_q, delta);
   return min(max(base_q + delta, 1), 255);
 }
 
 // One raster step of the delta-q chain (precompute_aq_grid): steps of 4 qindex,
-// at most 12, the decoder's Clip3(1, 255).
+// at most 12, the decoder's Clip3(1, 255).  (target - cur) / 4 is exact as a
+// product with 0.25.
 __device__ __forceinline__ int32_t chain_step(int32_t cur, int32_t target, int32_t* steps_out) {
-  const float st = clampf(fast_round(__fdiv_rn((float)(target - cur), 4.0f)), -12.0f, 12.0f);
+  const float st = clampf(fast_round(__fmul_rn((float)(target - cur), 0.25f)), -12.0f, 12.0f);
   const int32_t steps = to_i32(st);
   *steps_out = steps;
   return min(max(cur + steps * 4, 1), 255);
@@ -369,51 +380,54 @@ __global__ void __launch_bounds__(256) aq_tile_kernel(const AqGeom g, const SbSt
                                                       uint8_t* __restrict__ targets, uint8_t* __restrict__ maps,
                                                       uint32_t* __restrict__ counters, mt_aq_cell* __restrict__ cells,
                                                       float* __restrict__ tile_refs) {
+  __shared__ __align__(16) float s_val[2][kMaxTileSbs];  // per SB of the tile: act, pick_log (0 if unfilled)
+  __shared__ uint8_t s_tq[kMaxTileSbs];                  // target qindex per SB (last CTA)
+  __shared__ uint8_t s_map[kMaxChunks][256];
+  __shared__ uint16_t s_acq[256];
+  __shared__ int32_t s_entry[kMaxChunks];
   __shared__ float s_refs[2];
   __shared__ int32_t s_target[kChunk];
-  __shared__ int s_last;
-  __shared__ uint8_t s_map[kMaxChunks][256];
-  __shared__ int32_t s_entry[kMaxChunks];
+  __shared__ int s_filled, s_last;
   const int tid = threadIdx.x;
   const int tile = blockIdx.x / g.chunks_per_tile, chunk = blockIdx.x - tile * g.chunks_per_tile;
   const int tr = tile / g.tile_cols, tc = tile - tr * g.tile_cols;
+  const int sb_cols = g.sb_cols;
   const int sx0 = tc * g.tc_size, sy0 = tr * g.tr_size;
-  const int sw = min(g.tc_size, g.sb_cols - sx0), sh = min(g.tr_size, g.sb_rows - sy0);
+  const int sw = min(g.tc_size, sb_cols - sx0), sh = min(g.tr_size, g.sb_rows - sy0);
   const int n = sw * sh, nchunks = (n + kChunk - 1) / kChunk;
   if (chunk >= nchunks) return;
-  auto sb_of = [&](int i) {
+  s_acq[tid] = kAcQ[g.bd == 10 ? 1 : (g.bd == 12 ? 2 : 0)][tid];
+  if (tid == 0) s_filled = 0;
+  __syncthreads();
+  int filled = 0;
+  for (int i = tid; i < n; i += 256) {
     const int r = i / sw;
-    return (sy0 + r) * g.sb_cols + sx0 + (i - r * sw);
-  };
-  // Tile means in raster order: warp 0 sums the activities, warp 1 the picks.
+    const SbStat st = stats[(sy0 + r) * sb_cols + sx0 + (i - r * sw)];
+    s_val[0][i] = st.act;
+    s_val[1][i] = st.filled != 0 ? st.pick_log : 0.0f;
+    filled += st.filled != 0;
+  }
+  if (filled) atomicAdd(&s_filled, filled);
+  __syncthreads();
+  // Tile means in raster order (tile_ref_activity / tile_ref_picked): warp 0
+  // sums the activities, warp 1 the picks.  Adding the +0 of an unfilled SB
+  // leaves the sum unchanged (no value is -0), and the counts are exact.
   if (tid == 0 || tid == 32) {
-    const bool picks = tid == 32;
-    float sum = 0.0f, cnt = 0.0f;
+    const int which = tid >> 5;
+    const float4* v4 = reinterpret_cast<const float4*>(s_val[which]);
+    float sum = 0.0f;
     int i = 0;
-    for (; i + 8 <= n; i += 8) {
-      float v[8];
-      int32_t f[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) {
-        const SbStat* p = stats + sb_of(i + k);
-        v[k] = picks ? p->pick_log : p->act;
-        f[k] = p->filled;
-      }
-#pragma unroll
-      for (int k = 0; k < 8; k++)
-        if (!picks || f[k] != 0) {
-          sum = __fadd_rn(sum, v[k]);
-          cnt = __fadd_rn(cnt, 1.0f);
-        }
+#pragma unroll 4
+    for (; i + 4 <= n; i += 4) {
+      const float4 v = v4[i >> 2];
+      sum = __fadd_rn(sum, v.x);
+      sum = __fadd_rn(sum, v.y);
+      sum = __fadd_rn(sum, v.z);
+      sum = __fadd_rn(sum, v.w);
     }
-    for (; i < n; i++) {
-      const SbStat* p = stats + sb_of(i);
-      if (!picks || p->filled != 0) {
-        sum = __fadd_rn(sum, picks ? p->pick_log : p->act);
-        cnt = __fadd_rn(cnt, 1.0f);
-      }
-    }
-    s_refs[picks ? 1 : 0] = cnt > 0.0f ? __fdiv_rn(sum, cnt) : 5.0f;
+    for (; i < n; i++) sum = __fadd_rn(sum, s_val[which][i]);
+    const int cnt = which == 0 ? n : s_filled;
+    s_refs[which] = cnt > 0 ? __fdiv_rn(sum, (float)cnt) : 5.0f;
   }
   __syncthreads();
   const float ref_act = s_refs[0], ref_pick = s_refs[1];
@@ -423,10 +437,23 @@ __global__ void __launch_bounds__(256) aq_tile_kernel(const AqGeom g, const SbSt
   }
   const int first = chunk * kChunk, len = min(kChunk, n - first);
   if (tid < len) {
-    const int sb = sb_of(first + tid);
-    const int32_t t = sb_target(g, stats[sb], ref_act, ref_pick);
-    s_target[tid] = t;
-    targets[sb] = (uint8_t)t;
+    TargetConsts k;
+    k.base_q = g.base_q;
+    k.vb = g.vb;
+    k.boost_only = g.boost_only;
+    k.strength = fmaxf(g.strength, 0.0f);
+    k.mid_t = clampf(__fdiv_rn(__fsub_rn((float)g.base_q, 48.0f), 48.0f), 0.0f, 1.0f);
+    k.low_log = __fadd_rn(__fmul_rn(0.5f, k.mid_t), 5.549076f);
+    k.boost_slope = __fadd_rn(5.0f, __fmul_rn(1.5f, k.mid_t));
+    k.cut_slope = __fadd_rn(6.0f, __fmul_rn(2.0f, k.mid_t));
+    // top_ease_t (quant.rs:122-125): knee 20, width 12, top_ease 1.
+    const float t = clampf(__fdiv_rn(__fsub_rn(20.0f, (float)g.base_q), 12.0f), 0.0f, 1.0f);
+    k.ease = __fsub_rn(1.0f, __fmul_rn(1.0f, t));
+    const int i = first + tid, r = i / sw;
+    const int sb = (sy0 + r) * sb_cols + sx0 + (i - r * sw);
+    const int32_t tq = sb_target(k, s_acq, stats[sb], ref_act, ref_pick);
+    s_target[tid] = tq;
+    targets[sb] = (uint8_t)tq;
   }
   __syncthreads();
   // Exit qindex of this chunk for every entry qindex.
@@ -442,8 +469,13 @@ __global__ void __launch_bounds__(256) aq_tile_kernel(const AqGeom g, const SbSt
   if (!s_last) return;
   __threadfence();
   // Last CTA of the tile: compose the maps from base_q_idx, then walk every chunk.
-  for (int i = tid; i < nchunks * 256; i += 256)
-    s_map[i >> 8][i & 255] = __ldcg(maps + ((size_t)tile * g.chunks_per_tile) * 256 + i);
+  const uint8_t* tmaps = maps + (size_t)tile * g.chunks_per_tile * 256;
+  for (int i = tid; i < nchunks * 64; i += 256)
+    reinterpret_cast<uint32_t*>(&s_map[0][0])[i] = __ldcg(reinterpret_cast<const uint32_t*>(tmaps) + i);
+  for (int i = tid; i < n; i += 256) {
+    const int r = i / sw;
+    s_tq[i] = __ldcg(targets + (sy0 + r) * sb_cols + sx0 + (i - r * sw));
+  }
   __syncthreads();
   if (tid == 0) {
     int32_t cur = g.base_q;
@@ -456,9 +488,9 @@ __global__ void __launch_bounds__(256) aq_tile_kernel(const AqGeom g, const SbSt
   if (tid < nchunks) {
     int32_t cur = s_entry[tid];
     const int f = tid * kChunk, l = min(kChunk, n - f);
+    int r = f / sw, c = f - r * sw;
     for (int j = 0; j < l; j++) {
-      const int sb = sb_of(f + j);
-      const int32_t t = __ldcg(targets + sb);
+      const int32_t t = s_tq[f + j];
       int32_t steps;
       const int32_t nq = chain_step(cur, t, &steps);
       mt_aq_cell cell;
@@ -466,8 +498,12 @@ __global__ void __launch_bounds__(256) aq_tile_kernel(const AqGeom g, const SbSt
       cell.newq = (uint8_t)nq;
       cell.steps = (int8_t)steps;
       cell.target = (uint8_t)t;
-      cells[sb] = cell;
+      cells[(sy0 + r) * sb_cols + sx0 + c] = cell;
       cur = nq;
+      if (++c == sw) {
+        c = 0;
+        r++;
+      }
     }
   }
 }
@@ -510,8 +546,6 @@ int make_geom(const mt_aq_params* p, AqGeom* g) {
   g->octile = std::min(std::max(p->octile, 1), 8);
   g->boost_only = p->boost_only != 0;
   g->strength = p->strength;
-  const uint16_t* t = p->bd == 10 ? MT_AC_QLOOKUP_10 : (p->bd == 12 ? MT_AC_QLOOKUP_12 : MT_AC_QLOOKUP_8);
-  for (int i = 0; i < 256; i++) g->ac_q[i] = t[i];
   return MT_OK;
 }
 

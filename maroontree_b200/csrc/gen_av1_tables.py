@@ -80,6 +80,8 @@ def main():
         for k in range(0, len(nums), 24):
             lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
         lines.append("};")
+        if "QLOOKUP" in cname:  # also as an initialiser list, for device-side copies
+            lines.append(f"#define {cname}_LIST " + ",".join(str(v) for v in nums))
         lines.append("")
     open(out, "w").write("\n".join(lines))
     print("wrote", out)

@@ -86,6 +86,22 @@ def generate():
     for i in range(0, len(rows), 8):
         lines.append("  " + ",".join(f"0x{r:08x}" for _, r in rows[i:i + 8]) + ",")
     lines.append("};")
+    # Bucket index: entries of bucket b (x bits in [BASE + b * 4096, BASE + (b+1) * 4096))
+    # are kDarkPowX[kDarkPowB[b] .. kDarkPowB[b + 1]).
+    base, shift = 0x3F800000, 12
+    nb = ((0x40900000 - base) >> shift) + 1
+    starts, k = [], 0
+    for b_ in range(nb + 1):
+        while k < len(rows) and ((rows[k][0] - base) >> shift) < b_:
+            k += 1
+        starts.append(k)
+    lines.append(f"#define MT_DARK_POW_BASE 0x{base:08x}u")
+    lines.append(f"#define MT_DARK_POW_SHIFT {shift}")
+    lines.append(f"#define MT_DARK_POW_NB {nb}")
+    lines.append(f"__device__ const uint16_t kDarkPowB[{nb + 1}] = {{")
+    for i in range(0, len(starts), 16):
+        lines.append("  " + ",".join(str(v) for v in starts[i:i + 16]) + ",")
+    lines.append("};")
     with open(OUT, "w") as f:
         f.write("\n".join(lines) + "\n")
     return len(rows)

@@ -146,11 +146,18 @@ def test_dark_pow_table_pinned_to_this_c_library():
 
 def test_dark_pow_table_entries_match_oracle(oracle_lib):
     text = open(os.path.join(ROOT, "maroontree_b200", "csrc", "dark_pow_table.h")).read()
-    xs = np.array([int(v, 16) for v in re.findall(r"0x([0-9a-f]{8})", text.split("kDarkPowR")[0])], np.uint32)
-    rs = np.array([int(v, 16) for v in re.findall(r"0x([0-9a-f]{8})", text.split("kDarkPowR")[1])], np.uint32)
-    assert len(xs) == len(rs) > 1000 and np.all(np.diff(xs.astype(np.int64)) > 0)
-    got = oracle_lib.dark_pow(xs.view(np.float32)).view(np.uint32)
-    assert np.array_equal(got, rs)
+    def arr(name):
+        body = text.split(name)[1].split("{")[1].split("}")[0]
+        return np.array([int(v, 0) for v in re.findall(r"0x[0-9a-f]+|\d+", body)], np.int64)
+
+    xs, rs, bk = arr("kDarkPowX"), arr("kDarkPowR"), arr("kDarkPowB")
+    assert len(xs) == len(rs) > 1000 and np.all(np.diff(xs) > 0)
+    got = oracle_lib.dark_pow(xs.astype(np.uint32).view(np.float32)).view(np.uint32)
+    assert np.array_equal(got, rs.astype(np.uint32))
+    # the bucket index: entry i sits in bucket (x - 0x3f800000) >> 12
+    b = (xs - 0x3F800000) >> 12
+    assert np.array_equal(bk[b] <= np.arange(len(xs)), np.ones(len(xs), bool))
+    assert np.all(np.arange(len(xs)) < bk[b + 1]) and bk[-1] == len(xs) and bk[0] == 0
 
 
 # ---- CUDA parity (GPU) ---------------------------------------------------------
@@ -251,14 +258,18 @@ def test_aq_grid_device_api_matches_host(mt_lib, cuda):
 
 @pytest.mark.gpu
 def test_aq_grid_rejects_bad_input(mt_lib, cuda):
-    y = _case("serial")
-    for bad in (_params(200, 136, 60, bd=9), _params(201, 136, 60), _params(200, 136, 300),
-                _params(200, 136, 60, tiling=(7, 0))):
-        with pytest.raises(RuntimeError):
-            mt_lib.aq_grid(np.zeros((bad.h8, bad.w8), np.uint16) if bad.w8 % 8 == 0 else y, bad)
-    wide = _params(8192, 64, 60)  # one tile 128 superblocks wide
-    with pytest.raises(RuntimeError):
-        mt_lib.aq_grid(np.zeros((64, 8192), np.uint16), wide)
+    import ctypes as C
+
+    lib = mt_lib.load()
+    y = np.zeros((64, 8192), np.uint16)
+    cells = np.zeros(4096, abi.AQ_CELL_DTYPE)
+    refs = np.zeros(256, np.float32)
+    for bad in (_params(200, 64, 60, bd=9), _params(204, 64, 60), _params(200, 64, 300),
+                _params(200, 64, 60, tiling=(7, 0)),
+                _params(8192, 64, 60)):  # one tile 128 superblocks wide
+        assert lib.mt_aq_grid(y.ctypes.data, C.byref(bad), cells.ctypes.data, refs.ctypes.data) != 0
+    assert lib.mt_aq_grid(y.ctypes.data, C.byref(_params(8192, 64, 60, tiling=(1, 0))), cells.ctypes.data,
+                          refs.ctypes.data) == 0
 
 
 @pytest.mark.gpu
