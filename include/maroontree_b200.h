@@ -480,6 +480,50 @@ int mt_aq_grid(const uint16_t* luma, const mt_aq_params* prm, mt_aq_cell* cells,
  * elsewhere the binary64 power rounded once to binary32. */
 int mt_dark_pow_device(const float* d_x, float* d_out, int64_t n, void* stream);
 
+/* ---- Screen-content frame gate ----
+ * Replaces screen_frame_gate (src/coder/screen_gate.rs:64-273): per 16x16 luma
+ * block the distinct-value histogram (palette-exact / lenient counts,
+ * src/coder/palette.rs:651-690), the repeats among the hashes of the aligned
+ * non-flat 8x8 blocks, and, when that pre-screen passes, the IntraBC copy-gain
+ * model over the hash index of every 8x8 window on the chroma-parity grid
+ * (LossyIbcIndex, src/coder/block64.rs:92-330).  Shipped tuning: screen_few_share
+ * 0.10, ibc_gate_prescreen 0.02, ibc_gate_dv 1, ibc_gate_beta 32.  The luma
+ * plane is the padded source, w8 x h8 u16 row-major. */
+typedef struct mt_screen_gate_params {
+  int32_t w8, h8;          /* padded luma size, multiples of 8 */
+  int32_t sub_x, sub_y;    /* chroma subsampling shifts (the index grid's step) */
+  int32_t bd;              /* 8, 10 or 12 */
+  int32_t base_q_idx;      /* frame base qindex */
+} mt_screen_gate_params;
+
+typedef struct mt_screen_gate_result {
+  int32_t ibc_pays;        /* IntraBC is expected to save more than the loop filters it costs */
+  int32_t few_colour;      /* enough palette-exact 16x16 blocks for the text palette tools */
+  int32_t copy_stage;      /* 1: the pre-screen passed and the copy gains were measured */
+  uint32_t blocks16;       /* 16x16 blocks counted, (w8 / 16) * (h8 / 16) */
+  uint32_t few16;          /* palette-exact 16x16 blocks (2..8 values spanning >= 64 << (bd - 8)) */
+  uint32_t lenient16;      /* 16x16 blocks of 2..16 values with that span */
+  uint32_t nonflat8;       /* aligned non-flat 8x8 blocks inside the 16x16 grid */
+  uint32_t dup8;           /* of those, hashes already seen */
+  uint32_t copied;         /* 16x16 blocks whose best earlier copy gains */
+  uint32_t reserved;
+  uint64_t gain;           /* summed copy gain (gradient energy units) */
+  uint64_t photo;          /* photo-like 8x8 blocks priced as lost deblocking */
+} mt_screen_gate_result;
+
+/* At most this many index windows ((w8 - 7) x (h8 - 7) on the chroma-parity
+ * grid), else MT_ERR_TOO_LARGE. */
+#define MT_SCREEN_MAX_WINDOWS (1u << 26)
+/* Device working storage mt_screen_gate_device needs. */
+size_t mt_screen_gate_scratch_bytes(const mt_screen_gate_params* prm);
+/* The gate on the stream: the block pass, one read of its four counters (the
+ * stream is synchronised), the copy stage when the pre-screen passes (a second
+ * synchronisation), and the verdicts into the host struct *out. */
+int mt_screen_gate_device(const uint16_t* d_luma, const mt_screen_gate_params* prm, void* d_scratch,
+                          mt_screen_gate_result* out, void* stream);
+/* Host-buffer form. */
+int mt_screen_gate(const uint16_t* luma, const mt_screen_gate_params* prm, mt_screen_gate_result* out);
+
 /* Library version string. */
 const char* mt_version(void);
 

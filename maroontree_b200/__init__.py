@@ -279,6 +279,22 @@ def dark_pow_device(d_x, d_out, n, stream=0):
     _check(load().mt_dark_pow_device(ptr(d_x), ptr(d_out), n, stream or None), "mt_dark_pow_device")
 
 
+def screen_gate_params(w8, h8, sub_x, sub_y, base_q_idx, bd=8):
+    p = abi.ScreenGateParams()
+    p.w8, p.h8, p.sub_x, p.sub_y, p.bd, p.base_q_idx = w8, h8, sub_x, sub_y, bd, base_q_idx
+    return p
+
+
+def screen_gate(luma, sub_x, sub_y, base_q_idx, bd=8):
+    """``screen_frame_gate`` (src/coder/screen_gate.rs:64-273) of a padded luma
+    plane; returns the ``mt_screen_gate_result`` fields as a dict."""
+    luma = np.ascontiguousarray(luma, np.uint16)
+    prm = screen_gate_params(luma.shape[1], luma.shape[0], sub_x, sub_y, base_q_idx, bd)
+    r = abi.ScreenGateResult()
+    _check(load().mt_screen_gate(ptr(luma), C.byref(prm), C.byref(r)), "mt_screen_gate")
+    return r.as_dict()
+
+
 def loop_filter_levels(base_q_idx, sub_x, sub_y):
     """``loop_filter_levels`` / ``loop_filter_sharpness`` (src/obu.rs:306-334): (lvl_y, lvl_uv, sharp)."""
     a, b, c = C.c_int32(), C.c_int32(), C.c_int32()

@@ -99,6 +99,22 @@ assert C.sizeof(AqParams) == 44
 
 AQ_CELL_DTYPE = np.dtype([("prev", "u1"), ("newq", "u1"), ("steps", "i1"), ("target", "u1")])
 
+
+class ScreenGateParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "sub_x", "sub_y", "bd", "base_q_idx")]
+
+
+class ScreenGateResult(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("ibc_pays", "few_colour", "copy_stage")] + [
+        (n, C.c_uint32) for n in ("blocks16", "few16", "lenient16", "nonflat8", "dup8", "copied", "reserved")] + [
+        ("gain", C.c_uint64), ("photo", C.c_uint64)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_ if n != "reserved"}
+
+
+assert C.sizeof(ScreenGateParams) == 24 and C.sizeof(ScreenGateResult) == 56
+
 BLOCK8_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
     ("mode_bits", "<f4", (13,)),
@@ -168,6 +184,9 @@ def _bind(lib):
         "mt_aq_grid_device": (C.c_int, [_P, C.POINTER(AqParams), _P, _P, _P, _P]),
         "mt_aq_grid": (C.c_int, [_P, C.POINTER(AqParams), _P, _P]),
         "mt_dark_pow_device": (C.c_int, [_P, _P, C.c_int64, _P]),
+        "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
+        "mt_screen_gate_device": (C.c_int, [_P, C.POINTER(ScreenGateParams), _P, C.POINTER(ScreenGateResult), _P]),
+        "mt_screen_gate": (C.c_int, [_P, C.POINTER(ScreenGateParams), C.POINTER(ScreenGateResult)]),
         "mt_fwd_txfm_quant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P, _P]),
         "mt_inv_txfm_dequant_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.POINTER(Quant), _P, _P, _P]),
         "mt_trellis_optimize_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_float, _P]),
@@ -203,6 +222,7 @@ EXPORTED_SYMBOLS = (
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
+    "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate",
 )
 
 

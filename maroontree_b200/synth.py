@@ -407,3 +407,41 @@ def transform_maps(bw4, bh4, block_id, seed, split_p=0.4):
                     tv[r0:r1, c0] = 1
                     tt[r0, c0:c1] = 1
     return tw, th, tv, tt
+
+
+def screen_luma(w, h, seed, photo_frac=0.3, glyph_px=(8, 12), bd=8):
+    """Screen-content luma (u16, h x w): flat UI panels, rows of text drawn from a
+    small glyph alphabet (exact repeats at arbitrary offsets, with an
+    antialiasing level), and a photographic patch (the generator's luma)."""
+    rng = np.random.default_rng(seed)
+    top = (1 << bd) - 1
+    img = np.full((h, w), int(0.92 * top), np.int32)
+    # UI panels
+    for _ in range(6):
+        x0, y0 = rng.integers(0, w), rng.integers(0, h)
+        img[y0:y0 + rng.integers(16, h // 3 + 17), x0:x0 + rng.integers(16, w // 3 + 17)] = int(rng.integers(0, top + 1))
+    # glyph alphabet: binary masks with an antialiased edge level
+    gw, gh = glyph_px
+    glyphs = []
+    for _ in range(24):
+        m = (rng.random((gh, gw)) < 0.35).astype(np.int32)
+        aa = (rng.random((gh, gw)) < 0.15).astype(np.int32)
+        glyphs.append((m, aa))
+    ink, mid = int(0.1 * top), int(0.5 * top)
+    y = 4
+    while y + gh < h * (1 - photo_frac):
+        x = int(rng.integers(0, 24))
+        while x + gw < w:
+            if rng.random() < 0.8:
+                m, aa = glyphs[int(rng.integers(0, len(glyphs)))]
+                blk = img[y:y + gh, x:x + gw]
+                blk[aa == 1] = mid
+                blk[m == 1] = ink
+            x += gw + int(rng.integers(0, 3))
+        y += gh + int(rng.integers(2, 6))
+    # photographic patch at the bottom
+    ph = int(h * photo_frac)
+    if ph > 0:
+        lum = rgb_to_luma(generate_rgb(w, ph, int(seed) + 1)).astype(np.int32)
+        img[h - ph:, :] = lum << (bd - 8)
+    return np.clip(img, 0, top).astype(np.uint16)

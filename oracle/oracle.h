@@ -89,6 +89,9 @@ int32_t or_dark_protection(int32_t enabled, int32_t base_q, const uint16_t* yp, 
                            int32_t width, int32_t height, float scale);
 int or_tiling_spec_min(int32_t w8, int32_t h8, int32_t* cols_log2, int32_t* rows_log2);
 int or_aq_grid(const uint16_t* luma, const mt_aq_params* p, mt_aq_cell* cells, float* refs_out);
+/* screen_gate.rs screen_frame_gate; block64.rs hash8. */
+int or_screen_gate(const uint16_t* luma, const mt_screen_gate_params* p, mt_screen_gate_result* out);
+uint32_t or_hash8(const uint16_t* luma, int32_t w, int32_t x, int32_t y);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 

@@ -55,6 +55,8 @@ def load():
             "or_dark_protection": (C.c_int32, [C.c_int32, C.c_int32, _P] + [C.c_int32] * 5 + [C.c_float]),
             "or_tiling_spec_min": (C.c_int, [C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "or_aq_grid": (C.c_int, [_P, C.POINTER(abi.AqParams), _P, _P]),
+            "or_screen_gate": (C.c_int, [_P, C.POINTER(abi.ScreenGateParams), C.POINTER(abi.ScreenGateResult)]),
+            "or_hash8": (C.c_uint32, [_P, C.c_int32, C.c_int32, C.c_int32]),
             "or_candidate_chain": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), C.POINTER(abi.Quant), _P,
                                              C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
@@ -269,3 +271,18 @@ def aq_grid(luma, prm):
     refs = np.zeros((tc * tr, 2), np.float32)
     assert load().or_aq_grid(p(luma), C.byref(prm), p(cells), p(refs)) == 0
     return cells, refs
+
+
+def screen_gate(luma, sub_x, sub_y, base_q_idx, bd=8):
+    luma = np.ascontiguousarray(luma, np.uint16)
+    prm = abi.ScreenGateParams()
+    prm.h8, prm.w8 = luma.shape
+    prm.sub_x, prm.sub_y, prm.bd, prm.base_q_idx = sub_x, sub_y, bd, base_q_idx
+    r = abi.ScreenGateResult()
+    assert load().or_screen_gate(p(luma), C.byref(prm), C.byref(r)) == 0
+    return r.as_dict()
+
+
+def hash8(luma, x, y):
+    luma = np.ascontiguousarray(luma, np.uint16)
+    return load().or_hash8(p(luma), luma.shape[1], x, y)
