@@ -285,6 +285,19 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
                                                  ascr.data_ptr(), None))
         out[tag] = entry(ms, pw * ph * 2, "2 B luma read per sample")
         out[tag]["bound"] = "launch / per-tile serial means (two kernels; dark protection from qindex 90)"
+    # screen-content gate: the photo frame stops at the block pass; a mixed
+    # text / UI / photo frame of the same size runs the copy stage too
+    for tag, lum in (("screen_gate_photo", y), ("screen_gate_mixed",
+                     torch.from_numpy(synth.screen_luma(pw, ph, 5, photo_frac=0.3).view(np.int16)).to(dev))):
+        sp = mt.screen_gate_params(pw, ph, 1, 1, QIDX)
+        sscr = torch.empty(lib.mt_screen_gate_scratch_bytes(C.byref(sp)), dtype=torch.uint8, device=dev)
+        sres = abi.ScreenGateResult()
+        ms = timed(lambda: lib.mt_screen_gate_device(lum.data_ptr(), C.byref(sp), sscr.data_ptr(), C.byref(sres),
+                                                     None))
+        out[tag] = entry(ms, pw * ph * 2, "2 B luma read per sample (block pass; the copy stage re-reads windows)")
+        out[tag]["verdict"] = {"copy_stage": sres.copy_stage, "ibc_pays": sres.ibc_pays,
+                               "few_colour": sres.few_colour}
+        out[tag]["bound"] = "host synchronisation after the block pass (and after the copy stage)"
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)
