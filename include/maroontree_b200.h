@@ -125,6 +125,10 @@ typedef struct mt_candidate {
   uint8_t skip_ctx;      /* txb_skip context 0..12 */
   uint16_t reserved;
   float mode_bits;       /* LossyTile::mode_bits(px, py, mode) of the caller */
+  float extra_bits;      /* more signalling bits, added after mode_bits: bits = (luma_bits +
+                          * mode_bits) + extra_bits; the angle-delta symbol of the proxy's delta
+                          * pass, cdf_cost(angle_delta cdf of the mode, delta + 3)
+                          * (src/coder/partition_search.rs:576-578); 0 adds nothing */
 } mt_candidate;
 
 #define MT_CAND_HAVE_TR 1u
@@ -180,6 +184,7 @@ typedef struct mt_combo {
   int8_t angle_delta;
   uint8_t tx_type;
   uint8_t flags;          /* MT_COMBO_NO_TRELLIS */
+  float bits;             /* extra_bits of this combo's candidates (the angle-delta symbol) */
 } mt_combo;
 #define MT_COMBO_NO_TRELLIS 1u
 

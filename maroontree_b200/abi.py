@@ -119,22 +119,23 @@ BLOCK8_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "u1"),
     ("mode_bits", "<f4", (13,)),
 ])
-COMBO_DTYPE = np.dtype([("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"), ("flags", "u1")])
+COMBO_DTYPE = np.dtype([("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"), ("flags", "u1"), ("bits", "<f4")])
 BEST_DTYPE = np.dtype([
     ("combo", "<i4"), ("cost", "<f4"), ("distortion", "<f4"), ("bits", "<f4"), ("satd", "<u4"), ("eob", "<i4"),
     ("reserved", "<u4", (2,)),
 ])
-assert BLOCK8_DTYPE.itemsize == 60 and COMBO_DTYPE.itemsize == 4 and BEST_DTYPE.itemsize == 32
+assert BLOCK8_DTYPE.itemsize == 60 and COMBO_DTYPE.itemsize == 8 and BEST_DTYPE.itemsize == 32
 
 CANDIDATE_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("tx_type", "u1"),
     ("flags", "u1"), ("dcs_ctx", "u1"), ("skip_ctx", "u1"), ("reserved", "<u2"), ("mode_bits", "<f4"),
+    ("extra_bits", "<f4"),
 ])
 RESULT_DTYPE = np.dtype([
     ("distortion", "<f4"), ("bits", "<f4"), ("cost", "<f4"), ("satd", "<u4"), ("eob", "<i4"),
     ("reserved", "<u4", (3,)),
 ])
-assert CANDIDATE_DTYPE.itemsize == 16 and RESULT_DTYPE.itemsize == 32
+assert CANDIDATE_DTYPE.itemsize == 20 and RESULT_DTYPE.itemsize == 32
 
 _P = C.c_void_p
 

@@ -291,7 +291,8 @@ __device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, con
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
   const float cbits = rate4(cf, eob, T, cd.skip_ctx, cd.dcs_ctx, cd.mode, TX, p.use_skip_bits != 0, p.skip_bits[0],
                             p.skip_bits[1], reinterpret_cast<uint8_t*>(w.suf()));
-  const float bits = __fadd_rn(cbits, cd.mode_bits);
+  // (luma_bits + mode_bits) + extra_bits; adding 0 leaves the sum as is.
+  const float bits = __fadd_rn(__fadd_rn(cbits, cd.mode_bits), cd.extra_bits);
   r.distortion = price;
   r.bits = bits;
   r.cost = __fadd_rn(price, __fmul_rn(p.mode_lambda, bits));

@@ -49,6 +49,7 @@ __device__ __forceinline__ bool noalloc_candidate(const mt_block8& bk, const mt_
   cd.skip_ctx = bk.skip_ctx;
   cd.reserved = 0;
   cd.mode_bits = cb.mode <= MT_PAETH_PRED ? bk.mode_bits[cb.mode] : 0.0f;
+  cd.extra_bits = cb.bits;
   return true;
 }
 

@@ -183,23 +183,25 @@ def level_blocks(fw, fh, n=8, seed=0):
     return out
 
 
-def level_combos(modes, tx_types, deltas=(0,), no_trellis_types=()):
+def level_combos(modes, tx_types, deltas=(0,), no_trellis_types=(), delta_bits=None):
     """(mode, angle delta, tx type) combos in the reference's evaluation order
     (mode, then delta, then type); types in no_trellis_types carry
-    MT_COMBO_NO_TRELLIS."""
+    MT_COMBO_NO_TRELLIS.  delta_bits(mode, delta) -> the angle-delta symbol
+    cost of a nonzero delta (the proxy's delta pass); 0 for delta 0."""
     rows = []
     for m in modes:
         ds = deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)
         for d in ds:
+            extra = float(delta_bits(m, d)) if (delta_bits is not None and d != 0) else 0.0
             for t in tx_types:
-                rows.append((m, d, t, abi.COMBO_NO_TRELLIS if t in no_trellis_types else 0))
+                rows.append((m, d, t, abi.COMBO_NO_TRELLIS if t in no_trellis_types else 0, extra))
     return _combos(rows)
 
 
 def _combos(rows):
     out = np.zeros(len(rows), abi.COMBO_DTYPE)
-    for i, (m, d, t, f) in enumerate(rows):
-        out[i] = (m, d, t, f)
+    for i, row in enumerate(rows):
+        out[i] = tuple(row) + (0.0,) * (5 - len(row))
     return out
 
 
@@ -217,6 +219,7 @@ def candidates_of_level(blocks, combos):
     out["dcs_ctx"] = np.tile(blocks["dcs_ctx"], nc)
     out["skip_ctx"] = np.tile(blocks["skip_ctx"], nc)
     out["mode_bits"] = blocks["mode_bits"][np.tile(np.arange(nb), nc), np.repeat(combos["mode"], nb)]
+    out["extra_bits"] = np.repeat(combos["bits"], nb)
     return out
 
 

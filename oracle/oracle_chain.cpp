@@ -1247,7 +1247,7 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
   const int cls = n == 4 ? 0 : (n == 8 ? 1 : (n == 16 ? 2 : 3));
   float bits = or_real_block_bits(cf, scan, n, cls, cdfs, cd.skip_ctx, cd.dcs_ctx, cd.mode, cd.tx_type,
                                   p->use_skip_bits, p->skip_bits) +
-               cd.mode_bits;
+               cd.mode_bits + cd.extra_bits;
   r->distortion = price;
   r->bits = bits;
   r->cost = price + p->mode_lambda * bits;

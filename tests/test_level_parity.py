@@ -6,7 +6,7 @@ import pytest
 
 from maroontree_b200 import abi, synth
 
-pytestmark = pytest.mark.gpu
+
 
 
 def _setup(oracle_lib, w, h, seed, qidx, qm_level, types=abi.TX_2D_SCAN_TYPES, deltas=(0,)):
@@ -15,7 +15,8 @@ def _setup(oracle_lib, w, h, seed, qidx, qm_level, types=abi.TX_2D_SCAN_TYPES, d
     src = synth.rgb_to_luma(synth.generate_rgb(w, h, seed))
     rec = synth.synthetic_recon(src, seed + 7)
     blocks = synth.level_blocks(w, h, seed=seed)
-    combos = synth.level_combos(range(13), types, deltas)
+    # nonzero deltas carry an angle-delta symbol cost, as in the proxy's delta pass
+    combos = synth.level_combos(range(13), types, deltas, delta_bits=lambda m, d: 0.375 + 0.1 * m + 0.05 * abs(d))
     q = oracle_lib.quant_new(qidx, 8, qm_level)
     qm = oracle_lib.qm_row(qm_level, 0, 8)
     cdfs = synth.synthetic_cdfs(seed + 1)
@@ -23,6 +24,7 @@ def _setup(oracle_lib, w, h, seed, qidx, qm_level, types=abi.TX_2D_SCAN_TYPES, d
     return src, rec, blocks, combos, q, qm, cdfs, prm
 
 
+@pytest.mark.gpu
 @pytest.mark.parametrize("qidx,qm_level,deltas", [(70, 6, (0,)), (116, 1, (-3, 0, 3)), (30, 8, (-1, 0, 2))])
 def test_level_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, deltas):
     src, rec, blocks, combos, q, qm, cdfs, prm = _setup(oracle_lib, 160, 96, qidx, qidx, qm_level, deltas=deltas)
@@ -38,6 +40,7 @@ def test_level_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, deltas):
     assert np.array_equal(best["eob"], ref_w["eob"])
 
 
+@pytest.mark.gpu
 def test_level_ties_pick_first_combo(mt_lib, oracle_lib, cuda):
     """A flat source and reconstruction make many combos cost the same; the
     winner must be the first of them (strict < in evaluation order)."""
@@ -57,6 +60,7 @@ def test_level_ties_pick_first_combo(mt_lib, oracle_lib, cuda):
     assert np.array_equal(best["combo"], win)
 
 
+@pytest.mark.gpu
 def test_level_device_api_matches_host(mt_lib, oracle_lib, cuda):
     torch = cuda
     src, rec, blocks, combos, q, qm, cdfs, prm = _setup(oracle_lib, 96, 64, 5, 70, 6)
@@ -74,6 +78,7 @@ def test_level_device_api_matches_host(mt_lib, oracle_lib, cuda):
     assert d_res.cpu().numpy().tobytes() == host_res.tobytes()
 
 
+@pytest.mark.gpu
 def test_level_rejects_out_of_frame_blocks(mt_lib, oracle_lib, cuda):
     src, rec, blocks, combos, q, qm, cdfs, prm = _setup(oracle_lib, 64, 64, 6, 70, 6)
     blocks = blocks.copy()
@@ -83,3 +88,18 @@ def test_level_rejects_out_of_frame_blocks(mt_lib, oracle_lib, cuda):
     assert np.all(r[:, 3]["eob"] == abi.MT_EOB_INVALID)
     assert best["combo"][3] == -1
     assert np.all(best["combo"][np.arange(len(blocks)) != 3] >= 0)
+
+
+def test_extra_bits_follow_mode_bits_in_oracle(oracle_lib):
+    """bits = (luma_bits + mode_bits) + extra_bits, and extra_bits 0 changes nothing."""
+    src, rec, blocks, combos, q, qm, cdfs, prm = _setup(oracle_lib, 64, 64, 3, 70, 6, deltas=(-2, 0, 2))
+    cands = synth.candidates_of_level(blocks, combos)
+    with_bits, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, cands, threads=4)
+    plain = cands.copy()
+    plain["extra_bits"] = 0.0
+    without, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, plain, threads=4)
+    nz = cands["extra_bits"] != 0
+    assert nz.any() and (~nz).any()
+    assert np.array_equal(with_bits["bits"][~nz].view(np.uint32), without["bits"][~nz].view(np.uint32))
+    exp = (without["bits"][nz] + cands["extra_bits"][nz]).astype(np.float32)
+    assert np.array_equal(with_bits["bits"][nz].view(np.uint32), exp.view(np.uint32))

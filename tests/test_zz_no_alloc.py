@@ -25,7 +25,8 @@ def _level(oracle_lib, w, h, seed, qidx, qm_level):
     src = synth.rgb_to_luma(synth.generate_rgb(w, h, seed))
     rec = synth.synthetic_recon(src, seed + 3)
     blocks = synth.level_blocks(w, h, seed=seed)
-    combos = synth.level_combos(range(13), abi.TX_2D_SCAN_TYPES, deltas=(-3, 0, 3))
+    combos = synth.level_combos(range(13), abi.TX_2D_SCAN_TYPES, deltas=(-3, 0, 3),
+                                delta_bits=lambda m, d: 0.25 + 0.125 * abs(d))
     q = oracle_lib.quant_new(qidx, 8, qm_level)
     qm = oracle_lib.qm_row(qm_level, 0, 8)
     costs = mt.coef_costs(synth.synthetic_cdfs(seed))
