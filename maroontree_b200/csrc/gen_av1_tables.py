@@ -16,6 +16,7 @@ Source locations (reference paths):
   src/coef_q.rs     DC_QLOOKUP_8, AC_QLOOKUP_8/10/12, SCAN_16X16, SCAN_32X32
   src/tables.rs     SCAN_8X8, SCAN_4X4, LO_CTX_OFF, LO_CTX_OFF_WLH, LO_CTX_OFF_WGH
   src/qm_tables.rs  AV1_IQM  ([15][2][3344] u8)
+  src/dct.rs        ADST16_FWD_Q12 ([16][16] i16, the forward 16-point ADST in Q12)
 """
 import os
 import re
@@ -35,6 +36,7 @@ TABLES = [
     ("src/tables.rs", "LO_CTX_OFF_WLH", "MT_LO_CTX_OFF_WLH", "uint8_t"),
     ("src/tables.rs", "LO_CTX_OFF_WGH", "MT_LO_CTX_OFF_WGH", "uint8_t"),
     ("src/qm_tables.rs", "AV1_IQM", "MT_AV1_IQM", "uint8_t"),
+    ("src/dct.rs", "ADST16_FWD_Q12", "MT_ADST16_FWD_Q12", "int16_t"),
 ]
 
 

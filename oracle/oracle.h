@@ -27,6 +27,7 @@ const uint8_t* or_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h)
 const uint16_t* or_default_scan(int32_t n);
 
 /* dct.rs: forward transform + quantisation of one n x n block (n = 8). */
+void or_dct1d(int32_t* buf, int32_t n);
 void or_fwd_txfm_quant(const int32_t* resid, int32_t tx_type, int32_t n, const mt_quant* q,
                        const uint8_t* qm_row, int32_t* levels, float* targets);
 /* idct.rs: dequantisation + inverse transform of one block. */

@@ -257,6 +257,59 @@ void fwd_1d_4x4(const int32_t* in, bool vertical, int32_t mdc, int32_t mac, int3
     }
 }
 
+// dct.rs:224-238 WC16: the odd-half weights of the 16-point forward DCT (Q16).
+const int32_t WC16[8] = {32927, 34242, 37155, 42390, 51653, 69513, 112882, 334309};
+
+// dct.rs:241-276 dct1d_16_i32: even/odd split, 8-point DCTs on both halves (the
+// odd one after the WC16 weights), the odd-half running combine, interleave.
+void dct1d_16(int32_t* b) {
+  int32_t t[16];
+  for (int i = 0; i < 8; i++) {
+    t[i] = b[i] + b[15 - i];
+    t[8 + i] = b[i] - b[15 - i];
+  }
+  dct1d_8(t);
+  for (int i = 0; i < 8; i++) t[8 + i] = mul_q16(t[8 + i], WC16[i]);
+  dct1d_8(t + 8);
+  t[8] = fmla_sqrt2(t[8], t[9]);
+  for (int i = 9; i < 15; i++) t[i] += t[i + 1];
+  for (int i = 0; i < 8; i++) {
+    b[2 * i] = t[i];
+    b[2 * i + 1] = t[8 + i];
+  }
+}
+
+// dct.rs:513-523 fwd_adst16_1d: the Q12 matrix ADST16_FWD_Q12 (i64 sums).
+void fwd_adst16(int32_t* b) {
+  int32_t o[16];
+  for (int i = 0; i < 16; i++) {
+    int64_t acc = 0;
+    for (int j = 0; j < 16; j++) acc += (int64_t)MT_ADST16_FWD_Q12[i * 16 + j] * b[j];
+    o[i] = (int32_t)((acc + 2048) >> 12);
+  }
+  for (int i = 0; i < 16; i++) b[i] = o[i];
+}
+
+// dct.rs:557-580 dct16x16_quant_t_direct, :1295-1392 adst16x16 / adstdct16x16 /
+// dctadst16x16: columns, then rows, each output halved by mul_q16(x, 32768)
+// before store_quant_target (the Q16 multipliers are the quantiser's own).
+void fwd_2d_16x16(const int32_t* in, void (*colf)(int32_t*), void (*rowf)(int32_t*), int32_t mdc, int32_t mac,
+                  int32_t* cf, float* tf) {
+  int32_t tmp[256];
+  for (int u = 0; u < 16; u++) {
+    int32_t col[16];
+    for (int i = 0; i < 16; i++) col[i] = in[i * 16 + u];
+    colf(col);
+    for (int v = 0; v < 16; v++) tmp[v * 16 + u] = col[v];
+  }
+  for (int v = 0; v < 16; v++) {
+    int32_t row[16];
+    for (int u = 0; u < 16; u++) row[u] = tmp[v * 16 + u];
+    rowf(row);
+    for (int u = 0; u < 16; u++) store_quant_target(cf, tf, u * 16 + v, mul_q16(row[u], 32768), mdc, mac);
+  }
+}
+
 // dct.rs:1586-1611 identity_quant_t_direct (IDTX; QM never applied).
 void fwd_idtx(const int32_t* in, int w, int h, int32_t dc_q, int32_t ac_q, int32_t* cf, float* tf) {
   for (int y = 0; y < h; y++)
@@ -591,6 +644,8 @@ const uint16_t* or_default_scan(int32_t n) {
   return nullptr;
 }
 
+void inv_16x16(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* qm, int32_t* out);
+
 // DctDispatch::dct8x8_t / adst8x8_t / adstdct8x8_t / dctadst8x8_t (QM applied,
 // dct.rs:2751-2763, :2896-2909), fvdct8x8_t / fhdct8x8_t (flat, :2910-2920),
 // idtx8x8_t (dc/ac steps, :2918-2924).
@@ -615,6 +670,18 @@ void or_fwd_txfm_quant(const int32_t* resid, int32_t tx, int32_t n, const mt_qua
     if (qm_row) apply_qmatrix(cf, tf, qm_row, 16);
     return;
   }
+  if (n == 16) {
+    switch (tx) {
+      case MT_TX_IDTX: fwd_idtx(resid, 16, 16, q->dc_q, q->ac_q, cf, tf); return;
+      case MT_TX_DCT_DCT: fwd_2d_16x16(resid, dct1d_16, dct1d_16, q->q_mult_dc, q->q_mult_ac, cf, tf); break;
+      case MT_TX_ADST_ADST: fwd_2d_16x16(resid, fwd_adst16, fwd_adst16, q->q_mult_dc, q->q_mult_ac, cf, tf); break;
+      case MT_TX_ADST_DCT: fwd_2d_16x16(resid, fwd_adst16, dct1d_16, q->q_mult_dc, q->q_mult_ac, cf, tf); break;
+      case MT_TX_DCT_ADST: fwd_2d_16x16(resid, dct1d_16, fwd_adst16, q->q_mult_dc, q->q_mult_ac, cf, tf); break;
+      default: return;
+    }
+    if (qm_row) apply_qmatrix(cf, tf, qm_row, 256);
+    return;
+  }
   if (n != 8) return;
   switch (tx) {
     case MT_TX_IDTX: fwd_idtx(resid, 8, 8, q->dc_q, q->ac_q, cf, tf); return;
@@ -632,8 +699,143 @@ void or_fwd_txfm_quant(const int32_t* resid, int32_t tx, int32_t n, const mt_qua
 void or_inv_txfm_dequant(const int32_t* levels, int32_t tx, int32_t n, const mt_quant* q,
                          const uint8_t* qm_row, int32_t* resid) {
   if (n == 4) inv_4x4(levels, tx, q, qm_row, resid);
+  if (n == 16) inv_16x16(levels, tx, q, qm_row, resid);
   if (n != 8) return;
   inv_8x8(levels, tx, q, qm_row, resid);
+}
+
+// One dav1d rotation: (x * cx + y * cy + 2048) >> 12.  The reference writes
+// most of them with one constant minus 4096 and the input added back, and a
+// few with halved constants and >> 11; those equal this form exactly.
+inline int32_t rot12(int32_t x, int32_t cx, int32_t y, int32_t cy) { return (x * cx + y * cy + 2048) >> 12; }
+inline int32_t r181(int32_t v) { return (v * 181 + 128) >> 8; }
+
+// idct.rs:1871-1924 inv_dct16_1d: the 8-point inverse on the even inputs, the
+// odd half in four stages with the intermediate clip, the output butterflies.
+void inv_dct16(int32_t* c, int s, int32_t mn, int32_t mx) {
+  auto cl = [&](int32_t v) { return clampi(v, mn, mx); };
+  inv_dct8(c, 2 * s, mn, mx);
+  const int32_t in1 = c[s], in3 = c[3 * s], in5 = c[5 * s], in7 = c[7 * s];
+  const int32_t in9 = c[9 * s], in11 = c[11 * s], in13 = c[13 * s], in15 = c[15 * s];
+  const int32_t a8 = rot12(in1, 401, in15, -4076), a9 = rot12(in9, 3166, in7, -2598);
+  const int32_t a10 = rot12(in5, 1931, in11, -3612), a11 = rot12(in13, 3920, in3, -1189);
+  const int32_t a12 = rot12(in13, 1189, in3, 3920), a13 = rot12(in5, 3612, in11, 1931);
+  const int32_t a14 = rot12(in9, 2598, in7, 3166), a15 = rot12(in1, 4076, in15, 401);
+  const int32_t b8 = cl(a8 + a9), b9 = cl(a8 - a9), b10 = cl(a11 - a10), b11 = cl(a11 + a10);
+  const int32_t b12 = cl(a12 + a13), b13 = cl(a12 - a13), b14 = cl(a15 - a14), b15 = cl(a15 + a14);
+  const int32_t c9 = rot12(b14, 1567, b9, -3784), c14 = rot12(b14, 3784, b9, 1567);
+  const int32_t c10 = rot12(b13, -3784, b10, -1567), c13 = rot12(b13, 1567, b10, -3784);
+  const int32_t d8 = cl(b8 + b11), d9 = cl(c9 + c10), d10 = cl(c9 - c10), d11 = cl(b8 - b11);
+  const int32_t d12 = cl(b15 - b12), d13 = cl(c14 - c13), d14 = cl(c14 + c13), d15 = cl(b15 + b12);
+  const int32_t e10 = r181(d13 - d10), e13 = r181(d13 + d10), e11 = r181(d12 - d11), e12 = r181(d12 + d11);
+  const int32_t t0 = c[0], t1 = c[2 * s], t2 = c[4 * s], t3 = c[6 * s];
+  const int32_t t4 = c[8 * s], t5 = c[10 * s], t6 = c[12 * s], t7 = c[14 * s];
+  c[0] = cl(t0 + d15);
+  c[s] = cl(t1 + d14);
+  c[2 * s] = cl(t2 + e13);
+  c[3 * s] = cl(t3 + e12);
+  c[4 * s] = cl(t4 + e11);
+  c[5 * s] = cl(t5 + e10);
+  c[6 * s] = cl(t6 + d9);
+  c[7 * s] = cl(t7 + d8);
+  c[8 * s] = cl(t7 - d8);
+  c[9 * s] = cl(t6 - d9);
+  c[10 * s] = cl(t5 - e10);
+  c[11 * s] = cl(t4 - e11);
+  c[12 * s] = cl(t3 - e12);
+  c[13 * s] = cl(t2 - e13);
+  c[14 * s] = cl(t1 - d14);
+  c[15 * s] = cl(t0 - d15);
+}
+
+// idct.rs:1968-2062 inv_adst16_1d (dav1d): four rotation / butterfly stages
+// with the intermediate clip and the signed 181/256 outputs.
+void inv_adst16(int32_t* c, int s, int32_t mn, int32_t mx) {
+  auto cl = [&](int32_t v) { return clampi(v, mn, mx); };
+  int32_t in[16];
+  for (int i = 0; i < 16; i++) in[i] = c[i * s];
+  int32_t a[16];
+  a[0] = rot12(in[15], 4091, in[0], 201);
+  a[1] = rot12(in[15], 201, in[0], -4091);
+  a[2] = rot12(in[13], 3973, in[2], 995);
+  a[3] = rot12(in[13], 995, in[2], -3973);
+  a[4] = rot12(in[11], 3703, in[4], 1751);
+  a[5] = rot12(in[11], 1751, in[4], -3703);
+  a[6] = rot12(in[9], 3290, in[6], 2440);
+  a[7] = rot12(in[9], 2440, in[6], -3290);
+  a[8] = rot12(in[7], 2751, in[8], 3035);
+  a[9] = rot12(in[7], 3035, in[8], -2751);
+  a[10] = rot12(in[5], 2106, in[10], 3513);
+  a[11] = rot12(in[5], 3513, in[10], -2106);
+  a[12] = rot12(in[3], 1380, in[12], 3857);
+  a[13] = rot12(in[3], 3857, in[12], -1380);
+  a[14] = rot12(in[1], 601, in[14], 4052);
+  a[15] = rot12(in[1], 4052, in[14], -601);
+  int32_t b[16];
+  for (int i = 0; i < 8; i++) {
+    b[i] = cl(a[i] + a[i + 8]);
+    b[8 + i] = cl(a[i] - a[i + 8]);
+  }
+  const int32_t c8 = rot12(b[8], 4017, b[9], 799), c9 = rot12(b[8], 799, b[9], -4017);
+  const int32_t c10 = rot12(b[10], 2276, b[11], 3406), c11 = rot12(b[10], 3406, b[11], -2276);
+  const int32_t c12 = rot12(b[13], 4017, b[12], -799), c13 = rot12(b[13], 799, b[12], 4017);
+  const int32_t c14 = rot12(b[15], 2276, b[14], -3406), c15 = rot12(b[15], 3406, b[14], 2276);
+  const int32_t d0 = cl(b[0] + b[4]), d1 = cl(b[1] + b[5]), d2 = cl(b[2] + b[6]), d3 = cl(b[3] + b[7]);
+  const int32_t d4 = cl(b[0] - b[4]), d5 = cl(b[1] - b[5]), d6 = cl(b[2] - b[6]), d7 = cl(b[3] - b[7]);
+  const int32_t d8 = cl(c8 + c12), d9 = cl(c9 + c13), d10 = cl(c10 + c14), d11 = cl(c11 + c15);
+  const int32_t d12 = cl(c8 - c12), d13 = cl(c9 - c13), d14 = cl(c10 - c14), d15 = cl(c11 - c15);
+  const int32_t e4 = rot12(d4, 3784, d5, 1567), e5 = rot12(d4, 1567, d5, -3784);
+  const int32_t e6 = rot12(d7, 3784, d6, -1567), e7 = rot12(d7, 1567, d6, 3784);
+  const int32_t e12 = rot12(d12, 3784, d13, 1567), e13 = rot12(d12, 1567, d13, -3784);
+  const int32_t e14 = rot12(d15, 3784, d14, -1567), e15 = rot12(d15, 1567, d14, 3784);
+  const int32_t f2 = cl(d0 - d2), f3 = cl(d1 - d3), f6 = cl(e4 - e6), f7 = cl(e5 - e7);
+  const int32_t f10 = cl(d8 - d10), f11 = cl(d9 - d11), f14 = cl(e12 - e14), f15 = cl(e13 - e15);
+  c[0] = cl(d0 + d2);
+  c[15 * s] = -cl(d1 + d3);
+  c[3 * s] = -cl(e4 + e6);
+  c[12 * s] = cl(e5 + e7);
+  c[s] = -cl(d8 + d10);
+  c[14 * s] = cl(d9 + d11);
+  c[2 * s] = cl(e12 + e14);
+  c[13 * s] = -cl(e13 + e15);
+  c[7 * s] = -r181(f2 + f3);
+  c[8 * s] = r181(f2 - f3);
+  c[4 * s] = r181(f6 + f7);
+  c[11 * s] = -r181(f6 - f7);
+  c[6 * s] = r181(f10 + f11);
+  c[9 * s] = -r181(f10 - f11);
+  c[5 * s] = -r181(f14 + f15);
+  c[10 * s] = r181(f14 - f15);
+}
+
+// idct.rs:1926-1966 / :2067-2128 the 16x16 inverses: tmp[y*16 + x] =
+// coeff[y + x*16]; rows (row clip), (t+2)>>2 with the column clip, columns,
+// (t+8)>>4.  IDTX (idct.rs:1826-1869): identity16 2x + (x*1697 + 1024) >> 11
+// both passes, flat dequantisation.
+void inv_16x16(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* qm, int32_t* out) {
+  int32_t coeff[256], tmp[256];
+  const bool idtx = tx == MT_TX_IDTX;
+  dequant(levels, 256, 16, q, idtx ? nullptr : qm, coeff);
+  for (int y = 0; y < 16; y++)
+    for (int x = 0; x < 16; x++) tmp[y * 16 + x] = coeff[y + x * 16];
+  if (idtx) {
+    auto id16 = [](int32_t v) { return 2 * v + ((v * 1697 + 1024) >> 11); };
+    for (int i = 0; i < 256; i++) tmp[i] = clampi((id16(tmp[i]) + 2) >> 2, q->cmin, q->cmax);
+    for (int i = 0; i < 256; i++) out[i] = (id16(tmp[i]) + 8) >> 4;
+    return;
+  }
+  const bool row_adst = tx == MT_TX_ADST_ADST || tx == MT_TX_DCT_ADST;
+  const bool col_adst = tx == MT_TX_ADST_ADST || tx == MT_TX_ADST_DCT;
+  for (int y = 0; y < 16; y++) {
+    if (row_adst) inv_adst16(tmp + y * 16, 1, q->rmin, q->rmax);
+    else inv_dct16(tmp + y * 16, 1, q->rmin, q->rmax);
+  }
+  for (int i = 0; i < 256; i++) tmp[i] = clampi((tmp[i] + 2) >> 2, q->cmin, q->cmax);
+  for (int x = 0; x < 16; x++) {
+    if (col_adst) inv_adst16(tmp + x, 16, q->cmin, q->cmax);
+    else inv_dct16(tmp + x, 16, q->cmin, q->cmax);
+  }
+  for (int i = 0; i < 256; i++) out[i] = (tmp[i] + 8) >> 4;
 }
 
 // trellis.rs:944-1030 trellis_optimize with the AVX2 step A
@@ -1219,7 +1421,8 @@ void or_coef_costs_build(const mt_coef_cdfs* c, mt_coef_costs* o) {
     for (int s = 0; s < 16; s++) o->txtp[m][s] = or_cdf_cost(c->txtp[m], s);
 }
 
-// partition_search.rs:467-530: predict (DC via dc_pred_8x8, else predict_nd_ad)
+// partition_search.rs:467-530 (8x8) / :620-673 (16x16): predict (DC via
+// dc_pred_NxN, else predict_nd_ad)
 // -> residual_pred -> forward transform + quant (+QM) -> trellis_optimize ->
 // inverse -> luma_partition_distortion (lossy_state.rs:2385-2409) -> luma_bits
 // (lossy_state.rs:477-572) + mode_bits -> partition_rd::rd_cost.
@@ -1227,8 +1430,8 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
                       const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_candidate& cd, mt_candidate_result* r,
                       int32_t* lv_out, int32_t* rec_out) {
   const int n = p->tx_size, N = n * n;
-  int32_t pred[64], resid[64], cf[64], rr[64];
-  float tf[64];
+  int32_t pred[256], resid[256], cf[256], rr[256];
+  float tf[256];
   or_intra_predict(recon, p->stride, cd.px, cd.py, n, n, cd.mode, cd.angle_delta, (cd.flags & 1) != 0,
                    (cd.flags & 2) != 0, p->frame_w, p->frame_h, (cd.flags & 4) != 0, p->bd, pred);
   for (int y = 0; y < n; y++)
@@ -1265,10 +1468,17 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
     for (int i = 0; i < N; i++) rec_out[i] = clampi(pred[i] + rr[i], 0, maxv);
 }
 
+// The forward 1-D integer DCT of n = 4, 8 or 16 points in place (dct.rs:175-276).
+void or_dct1d(int32_t* buf, int32_t n) {
+  if (n == 4) dct1d_4(buf);
+  if (n == 8) dct1d_8(buf);
+  if (n == 16) dct1d_16(buf);
+}
+
 int or_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chain_params* p, const mt_quant* q,
                        const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_candidate* cands, int32_t n,
                        mt_candidate_result* results, int32_t* levels_out, int32_t* recon_out, int32_t threads) {
-  if (!p || (p->tx_size != 8 && p->tx_size != 4)) return MT_ERR_UNSUPPORTED;
+  if (!p || (p->tx_size != 8 && p->tx_size != 4 && p->tx_size != 16)) return MT_ERR_UNSUPPORTED;
   const int N = p->tx_size * p->tx_size;
   auto work = [&](int lo, int hi) {
     for (int i = lo; i < hi; i++)

@@ -50,6 +50,7 @@ def load():
                                            C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
             "or_fast_round": (C.c_float, [C.c_float]),
+            "or_dct1d": (None, [_P, C.c_int32]),
             "or_dirty_log1pf": (C.c_float, [C.c_float]),
             "or_dark_pow": (None, [_P, _P, C.c_int64]),
             "or_dark_protection": (C.c_int32, [C.c_int32, C.c_int32, _P] + [C.c_int32] * 5 + [C.c_float]),
@@ -286,3 +287,9 @@ def screen_gate(luma, sub_x, sub_y, base_q_idx, bd=8):
 def hash8(luma, x, y):
     luma = np.ascontiguousarray(luma, np.uint16)
     return load().or_hash8(p(luma), luma.shape[1], x, y)
+
+
+def dct1d(buf):
+    b = np.ascontiguousarray(buf, np.int32).copy()
+    load().or_dct1d(p(b), len(b))
+    return b
