@@ -140,7 +140,7 @@ typedef struct mt_candidate {
 
 /* Batch-wide parameters of the chain. */
 typedef struct mt_chain_params {
-  int32_t tx_size;        /* square luma transform size: 8, or 4 for the 4x4 level (16 reserved) */
+  int32_t tx_size;        /* square luma transform size: 8, or 4 / 16 for the 4x4 / 16x16 levels */
   int32_t bd;             /* bit depth (8) */
   int32_t frame_w, frame_h; /* padded plane size, also the prediction frame bounds */
   int32_t stride;         /* samples per row of src and recon */
@@ -278,6 +278,27 @@ int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const m
                          int32_t ncombos, mt_block_best* d_best, mt_candidate_result* d_results,
                          void* d_scratch, void* stream);
 size_t mt_rdo_level4_scratch_bytes(int32_t nblocks, int32_t ncombos);
+
+/* The batched 16x16 level: the 16x16 arm of rd_cost_square
+ * (src/coder/partition_search.rs:620-673 and its proxy_ad / ADST refinement
+ * passes) for every (block, combo) pair -- predict_nd (DC via dc_pred_16x16)
+ * -> dct16x16_t / adst16x16_t / adstdct16x16_t / dctadst16x16_t (+QM) or
+ * idtx16x16_t -> trellis_optimize over SCAN_16X16 -> the 16x16 inverse ->
+ * luma_partition_distortion -> TX_16X16 luma_bits + mode bits (+ the combo's
+ * bits) -> rd_cost.  prm->tx_size = 16; blocks are 16x16 at multiples of 16
+ * (an MT_CAND_* flags byte per block as for 8x8); qm_row is the 256-entry
+ * TX_16X16 row of the level (NULL: flat); costs is the TX_16X16 slice.
+ * Transform types DCT_DCT, ADST_ADST, ADST_DCT, DCT_ADST, IDTX (V/H_DCT give
+ * MT_EOB_INVALID). */
+int mt_rdo_level16(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
+                   const mt_combo* combos, int32_t ncombos, mt_block_best* best_out,
+                   mt_candidate_result* results_out);
+int mt_rdo_level16_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
+                          mt_block_best* d_best, mt_candidate_result* d_results, void* d_scratch, void* stream);
+size_t mt_rdo_level16_scratch_bytes(int32_t nblocks, int32_t ncombos);
 
 /* Allocation-free form of mt_rdo_level8_device.  No counterpart in the
  * reference: it exists for callers that cannot give this library device

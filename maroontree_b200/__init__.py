@@ -139,6 +139,24 @@ def rdo_level4(src, recon, prm, quant, qmrow, costs, blocks, combos, want_result
     return best, res
 
 
+def rdo_level16(src, recon, prm, quant, qmrow, costs, blocks, combos, want_results=False):
+    """The batched 16x16 level (``mt_rdo_level16``): blocks on the 16-sample
+    grid, prm.tx_size = 16, the 256-entry 16x16 QM row and the TX_16X16 cost
+    slice."""
+    lib = load()
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.BLOCK8_DTYPE)
+    combos = np.ascontiguousarray(combos, abi.COMBO_DTYPE)
+    best = np.zeros(len(blocks), abi.BEST_DTYPE)
+    res = np.zeros(len(blocks) * len(combos), RESULT_DTYPE) if want_results else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(lib.mt_rdo_level16(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                              ptr(blocks), len(blocks), ptr(combos), len(combos), ptr(best), ptr(res)),
+           "mt_rdo_level16")
+    return best, res
+
+
 def rdo_level8_scratch_bytes(nblocks, ncombos):
     """Device working storage ``mt_rdo_level8_device`` needs."""
     return load().mt_rdo_level8_scratch_bytes(nblocks, ncombos)

@@ -160,9 +160,14 @@ def _bind(lib):
         "mt_rdo_level8_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
         "mt_rdo_level4": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                     C.c_int32, _P, C.c_int32, _P, _P]),
+        "mt_rdo_level16": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                                     C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_rdo_level4_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
                                            _P, C.c_int32, _P, _P, _P, _P]),
+        "mt_rdo_level16_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P, C.c_int32,
+                                            _P, C.c_int32, _P, _P, _P, _P]),
         "mt_rdo_level4_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
+        "mt_rdo_level16_scratch_bytes": (C.c_size_t, [C.c_int32, C.c_int32]),
         "mt_rdo_level8_device_noalloc": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
                                                    C.c_int32, _P, C.c_int32, _P, _P]),
         "mt_padded_plane_dims": (C.c_int, [C.c_int32, C.c_int32, C.c_int32] + [C.POINTER(C.c_int32)] * 4),
@@ -218,6 +223,7 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",
+    "mt_rdo_level16", "mt_rdo_level16_device", "mt_rdo_level16_scratch_bytes",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
     "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",

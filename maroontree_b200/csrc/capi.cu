@@ -23,6 +23,10 @@ cudaError_t launch_level4(const uint16_t* src, const uint16_t* rec, const mt_cha
                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
                           mt_candidate_result* res, void* scratch, mt_block_best* best, cudaStream_t st);
+cudaError_t launch_level16(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
+                           mt_candidate_result* res, void* scratch, mt_block_best* best, cudaStream_t st);
 cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
@@ -279,16 +283,26 @@ int mt_rdo_level8(const uint16_t* src, const uint16_t* recon, const mt_chain_par
   return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
-size_t mt_rdo_level4_scratch_bytes(int32_t nblocks, int32_t ncombos) {
+}  // extern "C"
+
+namespace {
+
+using LevelLaunch = cudaError_t (*)(const uint16_t*, const uint16_t*, const mt_chain_params&, const mt_quant&, float,
+                                    const uint8_t*, const mt_coef_costs*, const mt_block8*, int, const mt_combo*, int,
+                                    mt_candidate_result*, void*, mt_block_best*, cudaStream_t);
+
+// The 4x4 and 16x16 levels: scratch is the per-block argmin keys.
+size_t small_level_scratch(int32_t nblocks, int32_t ncombos) {
   if (nblocks <= 0 || ncombos <= 0 || ncombos > MT_LEVEL_MAX_COMBOS) return 0;
   return (size_t)nblocks * 8;
 }
 
-int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
-                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
-                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
-                         mt_block_best* d_best, mt_candidate_result* d_results, void* d_scratch, void* stream) {
-  int rc = check_chain(prm, quant, 0, 4);
+int small_level_device(int tx, LevelLaunch launch, const uint16_t* d_src, const uint16_t* d_recon,
+                       const mt_chain_params* prm, const mt_quant* quant, const uint8_t* d_qm_row,
+                       const mt_coef_costs* d_costs, const mt_block8* d_blocks, int32_t nblocks,
+                       const mt_combo* d_combos, int32_t ncombos, mt_block_best* d_best,
+                       mt_candidate_result* d_results, void* d_scratch, void* stream) {
+  int rc = check_chain(prm, quant, 0, tx);
   if (rc != MT_OK) return rc;
   if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
   if (nblocks == 0 || ncombos == 0) return MT_OK;
@@ -297,15 +311,16 @@ int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const m
   if (!d_src || !d_recon || !d_costs || !d_blocks || !d_combos || !d_best || !d_results || !d_scratch)
     return MT_ERR_INVALID_INPUT;
   float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
-  cudaError_t e = mth::launch_level4(d_src, d_recon, *prm, *quant, tl, d_qm_row, d_costs, d_blocks, nblocks, d_combos,
-                                     ncombos, d_results, d_scratch, d_best, as_stream(stream));
+  cudaError_t e = launch(d_src, d_recon, *prm, *quant, tl, d_qm_row, d_costs, d_blocks, nblocks, d_combos, ncombos,
+                         d_results, d_scratch, d_best, as_stream(stream));
   return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
-int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
-                  const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
-                  const mt_combo* combos, int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out) {
-  int rc = check_chain(prm, quant, 0, 4);
+int small_level_host(int tx, LevelLaunch launch, const uint16_t* src, const uint16_t* recon,
+                     const mt_chain_params* prm, const mt_quant* quant, const uint8_t* qm_row,
+                     const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks, const mt_combo* combos,
+                     int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out) {
+  int rc = check_chain(prm, quant, 0, tx);
   if (rc != MT_OK) return rc;
   if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
   if (nblocks == 0 || ncombos == 0) return MT_OK;
@@ -314,6 +329,7 @@ int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_par
   if (!src || !recon || !costs || !blocks || !combos || !best_out) return MT_ERR_INVALID_INPUT;
   const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
   const size_t nres = (size_t)nblocks * ncombos;
+  const size_t qm_bytes = (size_t)tx * tx;
   size_t off_src = 0, off_rec = align256(plane), off_cost = off_rec + align256(plane);
   size_t off_qm = off_cost + align256(sizeof(mt_coef_costs));
   size_t off_blk = off_qm + 256;
@@ -333,22 +349,60 @@ int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_par
   cp(off_src, src, plane);
   cp(off_rec, recon, plane);
   cp(off_cost, costs, sizeof(mt_coef_costs));
-  if (qm_row) cp(off_qm, qm_row, 16);
+  if (qm_row) cp(off_qm, qm_row, qm_bytes);
   cp(off_blk, blocks, (size_t)nblocks * sizeof(mt_block8));
   cp(off_cmb, combos, (size_t)ncombos * sizeof(mt_combo));
   if (e != cudaSuccess) return MT_ERR_DEVICE;
   float tl = scaled_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
-  e = mth::launch_level4((const uint16_t*)(base + off_src), (const uint16_t*)(base + off_rec), *prm, *quant, tl,
-                         qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
-                         (const mt_block8*)(base + off_blk), nblocks, (const mt_combo*)(base + off_cmb), ncombos,
-                         (mt_candidate_result*)(base + off_res), base + off_key, (mt_block_best*)(base + off_best),
-                         st);
+  e = launch((const uint16_t*)(base + off_src), (const uint16_t*)(base + off_rec), *prm, *quant, tl,
+             qm_row ? (const uint8_t*)(base + off_qm) : nullptr, (const mt_coef_costs*)(base + off_cost),
+             (const mt_block8*)(base + off_blk), nblocks, (const mt_combo*)(base + off_cmb), ncombos,
+             (mt_candidate_result*)(base + off_res), base + off_key, (mt_block_best*)(base + off_best), st);
   if (e != cudaSuccess) return MT_ERR_DEVICE;
   e = cudaMemcpyAsync(best_out, base + off_best, (size_t)nblocks * sizeof(mt_block_best), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && results_out)
     e = cudaMemcpyAsync(results_out, base + off_res, nres * sizeof(mt_candidate_result), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t mt_rdo_level4_scratch_bytes(int32_t nblocks, int32_t ncombos) { return small_level_scratch(nblocks, ncombos); }
+
+int mt_rdo_level4_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
+                         mt_block_best* d_best, mt_candidate_result* d_results, void* d_scratch, void* stream) {
+  return small_level_device(4, mth::launch_level4, d_src, d_recon, prm, quant, d_qm_row, d_costs, d_blocks, nblocks,
+                            d_combos, ncombos, d_best, d_results, d_scratch, stream);
+}
+
+int mt_rdo_level4(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
+                  const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
+                  const mt_combo* combos, int32_t ncombos, mt_block_best* best_out, mt_candidate_result* results_out) {
+  return small_level_host(4, mth::launch_level4, src, recon, prm, quant, qm_row, costs, blocks, nblocks, combos,
+                          ncombos, best_out, results_out);
+}
+
+size_t mt_rdo_level16_scratch_bytes(int32_t nblocks, int32_t ncombos) { return small_level_scratch(nblocks, ncombos); }
+
+int mt_rdo_level16_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos, int32_t ncombos,
+                          mt_block_best* d_best, mt_candidate_result* d_results, void* d_scratch, void* stream) {
+  return small_level_device(16, mth::launch_level16, d_src, d_recon, prm, quant, d_qm_row, d_costs, d_blocks,
+                            nblocks, d_combos, ncombos, d_best, d_results, d_scratch, stream);
+}
+
+int mt_rdo_level16(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_block8* blocks, int32_t nblocks,
+                   const mt_combo* combos, int32_t ncombos, mt_block_best* best_out,
+                   mt_candidate_result* results_out) {
+  return small_level_host(16, mth::launch_level16, src, recon, prm, quant, qm_row, costs, blocks, nblocks, combos,
+                          ncombos, best_out, results_out);
 }
 
 int mt_candidate_chain(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_quant* quant,

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "chain16.cuh"
 #include "chain4.cuh"
 #include "chain8.cuh"
 
@@ -298,6 +299,54 @@ __global__ void __launch_bounds__(kThreads) level4_kernel(const uint16_t* __rest
   atomicMin(&best_key[b], key);
 }
 
+// The batched 16x16 level: thread t takes combo t / nblocks and block t %
+// nblocks, the whole chain per thread (prediction included) in a 3.6 KB
+// per-thread arena; the 256 QM weights and their forward scales are staged in
+// shared memory.
+__global__ void __launch_bounds__(kThreads) level16_kernel(const uint16_t* __restrict__ src,
+                                                           const uint16_t* __restrict__ rec, ChainArgs a,
+                                                           const uint8_t* __restrict__ qm_row,
+                                                           const mt_coef_costs* __restrict__ costs,
+                                                           const mt_block8* __restrict__ blocks, int nblocks,
+                                                           const mt_combo* __restrict__ combos, int ncombos,
+                                                           mt_candidate_result* __restrict__ res,
+                                                           unsigned long long* __restrict__ best_key) {
+  __shared__ mt_coef_costs sC;
+  __shared__ uint8_t sQm[256];
+  __shared__ float sQs[256];
+  __shared__ float sLut[64];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sC);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+      const int w = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)w;
+      sQs[i] = fwd_qm_scale(w);
+    }
+    if (threadIdx.x < 64) sLut[threadIdx.x] = kCoefRateLut[threadIdx.x];
+    __syncthreads();
+  }
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(t / nblocks), b = (int)(t - (long long)c * nblocks);
+  if (c >= ncombos) return;
+  const mt_candidate cd = level_candidate(blocks[b], combos[c]);
+  const size_t slot = (size_t)c * nblocks + b;
+  if (!cand16_ok(cd, a.p.frame_w, a.p.frame_h)) {
+    mt_candidate_result bad = {};
+    bad.eob = MT_EOB_INVALID;
+    res[slot] = bad;
+    return;
+  }
+  int32_t store[kWork16Words];
+  Work16 w{store};
+  mt_candidate_result r;
+  chain16_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  res[slot] = r;
+  const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c;
+  atomicMin(&best_key[b], key);
+}
+
 __global__ void level8_finalize_kernel(const unsigned long long* __restrict__ best_key, int nblocks,
                                        const mt_candidate_result* __restrict__ res, mt_block_best* __restrict__ best) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -484,6 +533,23 @@ cudaError_t launch_level4(const uint16_t* src, const uint16_t* rec, const mt_cha
   mtd::level4_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
                                                                qm_row, costs, blocks, nblocks, combos, ncombos, res,
                                                                keys);
+  mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_level16(const uint16_t* src, const uint16_t* rec, const mt_chain_params& p, const mt_quant& q,
+                           float trellis_lambda, const uint8_t* qm_row, const mt_coef_costs* costs,
+                           const mt_block8* blocks, int nblocks, const mt_combo* combos, int ncombos,
+                           mt_candidate_result* res, void* scratch, mt_block_best* best, cudaStream_t st) {
+  if (nblocks <= 0 || ncombos <= 0) return cudaSuccess;
+  unsigned long long* keys = static_cast<unsigned long long*>(scratch);
+  cudaError_t e = cudaMemsetAsync(keys, 0xff, (size_t)nblocks * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  const long long total = (long long)nblocks * ncombos;
+  const long long grid = (total + mtd::kThreads - 1) / mtd::kThreads;
+  mtd::level16_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+                                                                qm_row, costs, blocks, nblocks, combos, ncombos, res,
+                                                                keys);
   mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
   return cudaGetLastError();
 }

@@ -82,7 +82,7 @@ def main():
         for k in range(0, len(nums), 24):
             lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
         lines.append("};")
-        if "QLOOKUP" in cname:  # also as an initialiser list, for device-side copies
+        if "QLOOKUP" in cname or cname in ("MT_SCAN_16X16", "MT_ADST16_FWD_Q12"):  # initialiser lists for device copies
             lines.append(f"#define {cname}_LIST " + ",".join(str(v) for v in nums))
         lines.append("")
     open(out, "w").write("\n".join(lines))

@@ -16,10 +16,11 @@ __constant__ int16_t kDrDeriv[44] = {0,  1023, 0,  547, 372, 0,  0,  273, 215, 0
                                      35, 0,    31, 27,  0,   23, 19, 0,   15,  0,  11,  0,   7,  3};
 __constant__ int16_t kSmW8[8] = {255, 197, 146, 105, 73, 50, 37, 32};
 __constant__ int16_t kSmW4[4] = {255, 149, 85, 64};
+__constant__ int16_t kSmW16[16] = {255, 225, 196, 170, 145, 123, 102, 84, 68, 54, 43, 33, 26, 20, 17, 16};
 
 template <int N>
 __device__ __forceinline__ int32_t sm_weight(int i) {
-  return N == 4 ? kSmW4[i] : kSmW8[i];
+  return N == 4 ? kSmW4[i] : (N == 8 ? kSmW8[i] : kSmW16[i]);
 }
 
 constexpr int kEdgeOrigin = 2;
@@ -94,17 +95,17 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
   return 1 << (bd - 1);
 }
 
-// Prediction of an N x N block (N = 4 or 8) into out[N*N] (row-major).
+// Prediction of an N x N block (N = 4, 8 or 16) into out[N*N] (row-major).
 // `scratch` holds 3 * edge_cap<N>() words: the above and left edges and a
 // filter temporary.
 template <int N, typename O>
 __device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
                            int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out,
                            int32_t* __restrict__ scratch) {
-  static_assert(N == 4 || N == 8, "corner filtering (edge_len >= 24) is not built");
+  static_assert(N == 4 || N == 8 || N == 16, "square sizes 4, 8 and 16");
   constexpr int bw = N, bh = N, edge_len = 2 * N, cap = edge_cap<N>();
   if (mode == MT_DC_PRED) {
-    const int32_t d = dc_pred_sq(rec, stride, ox, oy, N, N == 4 ? 2 : 3, bd);
+    const int32_t d = dc_pred_sq(rec, stride, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : 4), bd);
     for (int i = 0; i < N * N; i++) out[i] = (O)(d);
     return;
   }
@@ -151,7 +152,13 @@ __device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw,
     const int angle = base_angle[mode] + delta * 3;
     int up_a = 0, up_l = 0;
     if (angle != 90 && angle != 180) {
-      // edge_len <= 16 < 24: no corner filter for 4x4 and 8x8.
+      // The corner filter (src/intrapred.rs:1014-1019) for edge_len >= 24,
+      // i.e. 16x16 here, before the edges are smoothed.
+      if (edge_len >= 24 && angle > 90 && angle < 180) {
+        const int32_t f = (5 * L[kEdgeOrigin] + 6 * A[kEdgeOrigin - 1] + 5 * A[kEdgeOrigin] + 8) >> 4;
+        A[kEdgeOrigin - 1] = f;
+        L[kEdgeOrigin - 1] = f;
+      }
       filter_edge(A, bw + 1 + (angle < 90 ? bh : 0), edge_strength(bw, bh, ft, angle - 90), tmp);
       filter_edge(L, bh + 1 + (angle > 180 ? bw : 0), edge_strength(bh, bw, ft, angle - 180), tmp);
       const int da = abs(angle - 90), dl = abs(angle - 180);
