@@ -12,11 +12,13 @@ coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
          block and combo lists copied in, per-block winners copied out, every
          step
 
-The line also carries ``frame_filters``: the frame-wide kernels of the same
-1080p 4:2:0 frame (colour conversion + padding, deblocking of the three
-planes, CDEF tables + strength search + apply) timed on the device with CUDA
-events after an L2 flush, with their algorithmic bytes against the measured
-HBM copy bandwidth.
+The line also carries ``level4`` / ``level16`` (the 4x4 and 16x16 levels of
+the same frame, device time and the oracle on the host cores) and
+``frame_filters``: the frame-wide kernels of the same
+1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
+grid, the screen-content gate, deblocking of the three planes, CDEF tables +
+strength search + apply) timed on the device with CUDA events after an L2
+flush, with their algorithmic bytes against the measured HBM copy bandwidth.
 
 ``--impl reference`` times the CPU restatement of the reference (the oracle;
 the Rust reference cannot be built here) on all host cores over a bounded
@@ -164,37 +166,47 @@ def run_reference(args):
     return 0
 
 
-def measure_level4(dev, wl, reps=5, cpu=True):
-    """The batched 4x4 level over the same 1080p luma (129,600 4x4 blocks x 13
-    modes x the SPLIT4 trial types DCT, ADST, IDTX-without-trellis, ADST_DCT,
-    DCT_ADST): device time with CUDA events after an L2 flush, and the oracle
-    on all host cores over the same candidates."""
+def measure_small_level(dev, wl, n, reps=5, cpu=True):
+    """The batched 4x4 or 16x16 level over the same 1080p luma: 4x4 -- 129,600
+    blocks x 13 modes x the SPLIT4 trial types DCT, ADST, IDTX-without-trellis,
+    ADST_DCT, DCT_ADST; 16x16 -- 8,040 blocks x 13 modes x the 16x16 proxy's
+    types DCT, ADST, IDTX.  Device time with CUDA events after an L2 flush, and
+    the oracle on all host cores over the same candidates."""
+    import ctypes as C
+
     import torch
     import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
     q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 4)
-    blocks = synth.level_blocks(W, H, n=4, seed=3)
-    combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX, abi.TX_ADST_DCT,
-                                        abi.TX_DCT_ADST), no_trellis_types=(abi.TX_IDTX,))
-    cdfs = synth.synthetic_cdfs(4, n_eob_bins=5)
+    qm = mt.qm_row(QM_LEVEL, 0, n)
+    blocks = synth.level_blocks(W, H, n=n, seed=3)
+    if n == 4:
+        combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX, abi.TX_ADST_DCT,
+                                            abi.TX_DCT_ADST), no_trellis_types=(abi.TX_IDTX,))
+        cdfs = synth.synthetic_cdfs(4, n_eob_bins=5)
+        entry, scratch_fn = "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes"
+        what = "rdo-level-4x4 1920x1080 luma, qindex 70, QM 6, 13 modes x 5 types (IDTX without trellis)"
+    else:
+        combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX))
+        cdfs = synth.synthetic_cdfs(4, n_eob_bins=9)
+        entry, scratch_fn = "mt_rdo_level16_device", "mt_rdo_level16_scratch_bytes"
+        what = "rdo-level-16x16 1920x1080 luma, qindex 70, QM 6, 13 modes x 3 types (DCT, ADST, IDTX)"
     costs = mt.coef_costs(cdfs)
-    prm = mt.chain_params(W, H, tx_size=4, trellis_lambda0=0.05, mode_lambda=wl["prm"].mode_lambda,
+    prm = mt.chain_params(W, H, tx_size=n, trellis_lambda0=0.05, mode_lambda=wl["prm"].mode_lambda,
                           satd_scale=wl["prm"].satd_scale, satd_bridge=wl["prm"].satd_bridge)
     nb, nc = len(blocks), len(combos)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d = [t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)), t(blocks), t(combos)]
     d_best = torch.empty(nb * abi.BEST_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     d_res = torch.empty(nb * nc * abi.RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
-    d_keys = torch.empty(mt.load().mt_rdo_level4_scratch_bytes(nb, nc), dtype=torch.uint8, device=dev)
+    d_keys = torch.empty(getattr(mt.load(), scratch_fn)(nb, nc), dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
-    import ctypes as C
+    fn = getattr(mt.load(), entry)
 
     def launch():
-        rc = mt.load().mt_rdo_level4_device(d[0].data_ptr(), d[1].data_ptr(), C.byref(prm), C.byref(q),
-                                            d[2].data_ptr(), d[3].data_ptr(), d[4].data_ptr(), nb, d[5].data_ptr(), nc,
-                                            d_best.data_ptr(), d_res.data_ptr(), d_keys.data_ptr(), None)
+        rc = fn(d[0].data_ptr(), d[1].data_ptr(), C.byref(prm), C.byref(q), d[2].data_ptr(), d[3].data_ptr(),
+                d[4].data_ptr(), nb, d[5].data_ptr(), nc, d_best.data_ptr(), d_res.data_ptr(), d_keys.data_ptr(), None)
         assert rc == 0, rc
 
     for _ in range(3):
@@ -210,8 +222,7 @@ def measure_level4(dev, wl, reps=5, cpu=True):
         torch.cuda.synchronize()
         ms.append(a.elapsed_time(b))
     step = float(np.median(ms))
-    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "candidates": nb * nc,
-           "workload": "rdo-level-4x4 1920x1080 luma, qindex 70, QM 6, 13 modes x 5 types (IDTX without trellis)"}
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "candidates": nb * nc, "workload": what}
     if cpu:
         from oracle import pyoracle as po
 
@@ -437,7 +448,8 @@ def run_ours(args):
     issue_rate = NCU_WARP_INSTS_PER_LAUNCH / (step_ms / 1e3)
 
     filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
-    level4 = measure_level4(dev, wl, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
+    level4 = measure_small_level(dev, wl, 4, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
+    level16 = measure_small_level(dev, wl, 16, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -468,6 +480,7 @@ def run_ours(args):
                            "inst_per_launch": NCU_WARP_INSTS_PER_LAUNCH, "sm_clock_mhz": clk_mhz},
         "frame_filters": filters,
         "level4": level4,
+        "level16": level16,
         # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
         "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),
