@@ -150,6 +150,9 @@ typedef struct mt_chain_params {
   float satd_bridge;      /* K_PART_LAMBDA / k_satd * proxy_luma_scale; 0 = bridge off */
   int32_t use_skip_bits;  /* 1: skip_bits below replace the txb_skip CDF cost */
   float skip_bits[2];     /* (all_zero = 1, all_zero = 0) */
+  int32_t vis_w, vis_h;   /* displayed luma size; samples past it carry no distortion (the
+                           * reference's SrcBlock masking, src/rd_sse.rs:61-167, :630-655);
+                           * 0 = frame_w / frame_h */
 } mt_chain_params;
 
 /* eob value of a candidate the kernel rejected (block outside the frame, or a

@@ -65,9 +65,11 @@ def coef_costs(cdfs):
 
 
 def chain_params(frame_w, frame_h, stride=None, tx_size=8, trellis_lambda0=0.05, mode_lambda=1.0,
-                 satd_scale=1.25, satd_bridge=0.0, skip_bits=None):
+                 satd_scale=1.25, satd_bridge=0.0, skip_bits=None, vis=None):
     p = ChainParams()
     p.tx_size, p.bd, p.frame_w, p.frame_h = tx_size, 8, frame_w, frame_h
+    if vis is not None:
+        p.vis_w, p.vis_h = vis
     p.stride = stride if stride is not None else frame_w
     p.trellis_lambda0, p.mode_lambda, p.satd_scale, p.satd_bridge = trellis_lambda0, mode_lambda, satd_scale, satd_bridge
     if skip_bits is not None:

@@ -66,7 +66,7 @@ class ChainParams(C.Structure):
         ("tx_size", C.c_int32), ("bd", C.c_int32), ("frame_w", C.c_int32), ("frame_h", C.c_int32),
         ("stride", C.c_int32), ("trellis_lambda0", C.c_float), ("mode_lambda", C.c_float),
         ("satd_scale", C.c_float), ("satd_bridge", C.c_float), ("use_skip_bits", C.c_int32),
-        ("skip_bits", C.c_float * 2),
+        ("skip_bits", C.c_float * 2), ("vis_w", C.c_int32), ("vis_h", C.c_int32),
     ]
 
 

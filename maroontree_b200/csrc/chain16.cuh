@@ -206,7 +206,7 @@ __device__ float rate16(const C* cf, int eob, const mt_coef_costs& T, int skip_c
 // block (src/partition_rd.rs:86-133).
 template <typename P, typename R>
 __device__ uint32_t satd16(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred, const R* rr,
-                           int32_t maxv) {
+                           int32_t maxv, int vw, int vh) {
   uint32_t satd = 0;
 #pragma unroll 1
   for (int tile = 0; tile < 16; tile++) {
@@ -218,7 +218,9 @@ __device__ uint32_t satd16(const uint16_t* __restrict__ src, int stride, int px,
 #pragma unroll
       for (int x = 0; x < 4; x++) {
         const int i = (ty + y) * 16 + tx + x;
-        d[x] = (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv);
+        d[x] = (tx + x < vw && ty + y < vh)
+                   ? (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv)
+                   : 0;
       }
       const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
       r[y][0] = e + g;
@@ -289,7 +291,8 @@ __device__ __forceinline__ void chain16_one(const uint16_t* __restrict__ src, co
       if (cf[kScan16[i]] != 0) eob = i;
   }
   inv16x16(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
-  const uint32_t satd = satd16(src, p.stride, cd.px, cd.py, pred, rr, maxv);
+  const uint32_t satd = satd16(src, p.stride, cd.px, cd.py, pred, rr, maxv, vis_extent(p.vis_w, p.frame_w, cd.px),
+                               vis_extent(p.vis_h, p.frame_h, cd.py));
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);

@@ -268,6 +268,11 @@ __device__ float rate8(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
   return bits;
 }
 
+// Visible columns (rows) of a block at p: the displayed size (0 = the padded
+// frame) minus the block origin; samples past it are masked to the
+// reconstruction (zero error), as the reference's SrcBlock does.
+__device__ __forceinline__ int vis_extent(int vis, int frame, int p) { return (vis > 0 ? vis : frame) - p; }
+
 #ifndef MT_SATD_UNROLL
 #define MT_SATD_UNROLL 1
 #endif
@@ -276,7 +281,7 @@ constexpr int kSatdUnroll = MT_SATD_UNROLL;
 // Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
 template <typename P, typename R>
 __device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
-                                          const R* rr, int32_t maxv) {
+                                          const R* rr, int32_t maxv, int vw, int vh) {
   uint32_t satd = 0;
 #pragma unroll kSatdUnroll
   for (int ty = 0; ty < 8; ty += 4)
@@ -289,7 +294,9 @@ __device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int 
 #pragma unroll
         for (int x = 0; x < 4; x++) {
           const int i = (ty + y) * 8 + tx + x;
-          d[x] = (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv);
+          d[x] = (tx + x < vw && ty + y < vh)
+                   ? (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv)
+                   : 0;
         }
         const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
         r[y][0] = e + g;
@@ -375,7 +382,8 @@ __device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, cons
       if (cf[kScan8[i]] != 0) eob = i;
   }
   inv8x8(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
-  const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv);
+  const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv, vis_extent(p.vis_w, p.frame_w, cd.px),
+                               vis_extent(p.vis_h, p.frame_h, cd.py));
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);

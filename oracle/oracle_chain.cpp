@@ -1194,14 +1194,24 @@ void or_intra_predict(const uint16_t* recon, int32_t stride, int32_t ox, int32_t
 }
 
 // partition_rd.rs:86-133 luma_satd_scalar.
+// rd_sse.rs:630-655 luma_satd: outside the visible window (vis_w x vis_h from
+// the block origin) the source is replaced by the reconstruction.
+static uint64_t luma_satd_vis(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w, int32_t h,
+                              int32_t maxv, const int32_t* pred, const int32_t* resid, int32_t vis_w, int32_t vis_h);
+
 uint64_t or_luma_satd(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w, int32_t h,
                       int32_t maxv, const int32_t* pred, const int32_t* resid) {
+  return luma_satd_vis(src, stride, px, py, w, h, maxv, pred, resid, w, h);
+}
+
+static uint64_t luma_satd_vis(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w, int32_t h,
+                              int32_t maxv, const int32_t* pred, const int32_t* resid, int32_t vis_w, int32_t vis_h) {
   std::vector<int32_t> err((size_t)w * h);
   for (int y = 0; y < h; y++)
     for (int x = 0; x < w; x++) {
       int i = y * w + x;
       int32_t r = pred[i] + (resid ? resid[i] : 0);
-      err[i] = (int32_t)src[(size_t)(py + y) * stride + px + x] - clampi(r, 0, maxv);
+      err[i] = (x < vis_w && y < vis_h) ? (int32_t)src[(size_t)(py + y) * stride + px + x] - clampi(r, 0, maxv) : 0;
     }
   uint64_t satd = 0;
   for (int ty = 0; ty < h; ty += 4)
@@ -1443,7 +1453,9 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
     or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, scan, N, p->trellis_lambda0);
   or_inv_txfm_dequant(cf, cd.tx_type, n, q, qm, rr);
   const int32_t maxv = (1 << p->bd) - 1;
-  uint64_t satd = or_luma_satd(src, p->stride, cd.px, cd.py, n, n, maxv, pred, rr);
+  const int32_t vis_w = (p->vis_w > 0 ? p->vis_w : p->frame_w) - cd.px;
+  const int32_t vis_h = (p->vis_h > 0 ? p->vis_h : p->frame_h) - cd.py;
+  uint64_t satd = luma_satd_vis(src, p->stride, cd.px, cd.py, n, n, maxv, pred, rr, vis_w, vis_h);
   float qstep = (float)q->ac_q;
   float price = (float)satd * (qstep > 1.0f ? qstep : 1.0f) * 0.25f * p->satd_scale;
   if (p->satd_bridge != 0.0f) price *= p->satd_bridge;

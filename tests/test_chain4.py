@@ -114,3 +114,13 @@ def test_oracle_level4_no_trellis_flag_changes_only_flagged(oracle_lib, mt_lib):
     flagged = (cands["flags"] & abi.CAND_NO_TRELLIS) != 0
     assert flagged.any() and np.array_equal(a[~flagged], b[~flagged])
     assert not np.array_equal(a[flagged]["cost"], b[flagged]["cost"])
+
+
+@pytest.mark.gpu
+def test_level4_masks_samples_past_the_displayed_frame(mt_lib, oracle_lib, cuda):
+    src, rec, blocks, combos, q, qm, cdfs, prm = _setup4(oracle_lib, 128, 72, 6, 70, 6)
+    prm.vis_w, prm.vis_h = 126, 69
+    best, res = mt_lib.rdo_level4(src, rec, prm, q, qm, mt_lib.coef_costs(cdfs), blocks, combos, want_results=True)
+    ref, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, synth.candidates_of_level(blocks, combos),
+                                           threads=8)
+    assert res.tobytes() == ref.tobytes()

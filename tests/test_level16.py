@@ -67,3 +67,13 @@ def test_level16_rejects_v_h_and_out_of_frame(mt_lib, oracle_lib, cuda):
     assert np.all(r[1]["eob"] == abi.MT_EOB_INVALID) and np.all(r[3]["eob"] == abi.MT_EOB_INVALID)
     assert np.all(r[:, 1]["eob"] == abi.MT_EOB_INVALID)
     assert best["combo"][1] == -1 and np.all(np.isin(best["combo"][np.arange(len(blocks)) != 1], (0, 2)))
+
+
+@pytest.mark.gpu
+def test_level16_masks_samples_past_the_displayed_frame(mt_lib, oracle_lib, cuda):
+    src, rec, blocks, combos, q, qm, cdfs, prm = _setup16(oracle_lib, 160, 96, 5, 70, 6)
+    prm.vis_w, prm.vis_h = 150, 90
+    best, res = mt_lib.rdo_level16(src, rec, prm, q, qm, mt_lib.coef_costs(cdfs), blocks, combos, want_results=True)
+    ref, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, synth.candidates_of_level(blocks, combos),
+                                           threads=8)
+    assert res.tobytes() == ref.tobytes()

@@ -103,3 +103,21 @@ def test_extra_bits_follow_mode_bits_in_oracle(oracle_lib):
     assert np.array_equal(with_bits["bits"][~nz].view(np.uint32), without["bits"][~nz].view(np.uint32))
     exp = (without["bits"][nz] + cands["extra_bits"][nz]).astype(np.float32)
     assert np.array_equal(with_bits["bits"][nz].view(np.uint32), exp.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_level_masks_samples_past_the_displayed_frame(mt_lib, oracle_lib, cuda):
+    """A frame displayed at 157x93 and coded at 160x96: the right / bottom
+    blocks price distortion over the displayed samples only (SrcBlock)."""
+    src, rec, blocks, combos, q, qm, cdfs, prm = _setup(oracle_lib, 160, 96, 9, 70, 6, deltas=(-2, 0, 2))
+    prm.vis_w, prm.vis_h = 157, 93
+    best, res = mt_lib.rdo_level8(src, rec, prm, q, qm, mt_lib.coef_costs(cdfs), blocks, combos, want_results=True)
+    cands = synth.candidates_of_level(blocks, combos)
+    ref, _, _ = oracle_lib.candidate_chain(src, rec, prm, q, qm, cdfs, cands, threads=8)
+    assert res.tobytes() == ref.tobytes()
+    full = prm.__class__.from_buffer_copy(prm)
+    full.vis_w = full.vis_h = 0
+    ref_full, _, _ = oracle_lib.candidate_chain(src, rec, full, q, qm, cdfs, cands, threads=8)
+    edge = (cands["px"] + 8 > 157) | (cands["py"] + 8 > 93)
+    assert (ref["satd"][edge] != ref_full["satd"][edge]).any()
+    assert np.array_equal(ref["satd"][~edge], ref_full["satd"][~edge])
