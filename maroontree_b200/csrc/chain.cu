@@ -97,6 +97,7 @@ __device__ __forceinline__ void store_blocks(Work8& w, int32_t maxv, int32_t* lv
   }
 }
 
+template <bool VIS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) chain8_kernel(const uint16_t* __restrict__ src,
                                                           const uint16_t* __restrict__ rec, ChainArgs a,
                                                           const uint8_t* __restrict__ qm_row,
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) chain8_kernel(const uint
   int32_t store[kWork8Words];
   Work8 w{store};
   mt_candidate_result r;
-  chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  chain8_one<VIS>(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[idx] = r;
   store_blocks(w, (1 << a.p.bd) - 1, lv_out, rec_out, (size_t)idx);
 }
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(kThreads) level8_pred_kernel(const uint16_t* _
   }
 }
 
+template <bool VIS>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint16_t* __restrict__ src, ChainArgs a,
                                                           const uint8_t* __restrict__ qm_row,
                                                           const mt_coef_costs* __restrict__ costs,
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint
     }
   }
   mt_candidate_result r;
-  chain8_tx(src, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  chain8_tx<VIS>(src, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[slot] = r;
   // Costs are non-negative finite floats, so their bit patterns order like
   // the values; ties go to the lower combo index (evaluated first in the
@@ -257,6 +259,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) level8_kernel(const uint
 // candidate (a 4x4 prediction is a few dozen operations).
 // 8 resident CTAs per SM requested (80 registers): measured 5 % faster than
 // the register allocator's free choice.
+template <bool VIS>
 __global__ void __launch_bounds__(kThreads, 8) level4_kernel(const uint16_t* __restrict__ src,
                                                           const uint16_t* __restrict__ rec, ChainArgs a,
                                                           const uint8_t* __restrict__ qm_row,
@@ -295,7 +298,7 @@ __global__ void __launch_bounds__(kThreads, 8) level4_kernel(const uint16_t* __r
   int32_t store[kWork4Words];
   Work4 w{store};
   mt_candidate_result r;
-  chain4_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  chain4_one<VIS>(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[slot] = r;
   const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c;
   atomicMin(&best_key[b], key);
@@ -308,6 +311,7 @@ __global__ void __launch_bounds__(kThreads, 8) level4_kernel(const uint16_t* __r
 // Full occupancy requested (16 CTAs of 128 threads, 32 registers): the kernel
 // waits on its local-memory arena, and more resident warps hide that better
 // (2.61 -> 2.26 ms on the 1080p level; a cap of 2-4 CTAs was slower).
+template <bool VIS>
 __global__ void __launch_bounds__(kThreads, 16) level16_kernel(const uint16_t* __restrict__ src,
                                                            const uint16_t* __restrict__ rec, ChainArgs a,
                                                            const uint8_t* __restrict__ qm_row,
@@ -346,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 16) level16_kernel(const uint16_t* _
   int32_t store[kWork16Words];
   Work16 w{store};
   mt_candidate_result r;
-  chain16_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  chain16_one<VIS>(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   res[slot] = r;
   const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c;
   atomicMin(&best_key[b], key);
@@ -448,6 +452,14 @@ __global__ void pred8_kernel(const uint16_t* __restrict__ rec, mt_chain_params p
 }  // namespace mtd
 
 // Host launchers used by the C ABI (capi.cu).
+namespace {
+// The displayed frame is smaller than the coded one: the distortion masks
+// samples past it (a separate instantiation, so coded-size frames pay nothing).
+bool clipped(const mt_chain_params& p) {
+  return (p.vis_w > 0 && p.vis_w < p.frame_w) || (p.vis_h > 0 && p.vis_h < p.frame_h);
+}
+}  // namespace
+
 namespace mth {
 static mtd::ChainArgs make_args(const mt_chain_params& p, const mt_quant& q, float tl, const uint8_t* qm) {
   mtd::ChainArgs a;
@@ -477,7 +489,11 @@ cudaError_t launch_chain8(const uint16_t* src, const uint16_t* rec, const mt_cha
     mtd::bucket_scan_kernel<<<1, mtd::kBuckets, 0, st>>>(hist, cursor);
     mtd::bucket_scatter_kernel<<<blocks, mtd::kThreads, 0, st>>>(cands, n, cursor, perm);
   }
-  mtd::chain8_kernel<<<blocks, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row), qm_row,
+  if (clipped(p))
+    mtd::chain8_kernel<true><<<blocks, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row), qm_row,
+                                                       costs, cands, perm, n, res, lv, ro);
+  else
+    mtd::chain8_kernel<false><<<blocks, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row), qm_row,
                                                        costs, cands, perm, n, res, lv, ro);
   return cudaGetLastError();
 }
@@ -519,7 +535,11 @@ cudaError_t launch_level8(const uint16_t* src, const uint16_t* rec, const mt_cha
   mtd::level8_runs_kernel<<<1, 32, 0, st>>>(combos, ncombos, runs);
   // At most ncombos runs: pred CTAs past the run count exit at once.
   mtd::level8_pred_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(rec, args, blocks, nblocks, combos, runs, preds);
-  mtd::level8_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, args, qm_row, costs, blocks, nblocks, combos,
+  if (clipped(p))
+    mtd::level8_kernel<true><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, args, qm_row, costs, blocks, nblocks, combos,
+                                                               ncombos, runs, preds, res, keys);
+  else
+    mtd::level8_kernel<false><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, args, qm_row, costs, blocks, nblocks, combos,
                                                                ncombos, runs, preds, res, keys);
   mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
   return cudaGetLastError();
@@ -535,7 +555,12 @@ cudaError_t launch_level4(const uint16_t* src, const uint16_t* rec, const mt_cha
   if (e != cudaSuccess) return e;
   const long long total = (long long)nblocks * ncombos;
   const long long grid = (total + mtd::kThreads - 1) / mtd::kThreads;
-  mtd::level4_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+  if (clipped(p))
+    mtd::level4_kernel<true><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+                                                               qm_row, costs, blocks, nblocks, combos, ncombos, res,
+                                                               keys);
+  else
+    mtd::level4_kernel<false><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
                                                                qm_row, costs, blocks, nblocks, combos, ncombos, res,
                                                                keys);
   mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);
@@ -552,7 +577,12 @@ cudaError_t launch_level16(const uint16_t* src, const uint16_t* rec, const mt_ch
   if (e != cudaSuccess) return e;
   const long long total = (long long)nblocks * ncombos;
   const long long grid = (total + mtd::kThreads - 1) / mtd::kThreads;
-  mtd::level16_kernel<<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+  if (clipped(p))
+    mtd::level16_kernel<true><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
+                                                                qm_row, costs, blocks, nblocks, combos, ncombos, res,
+                                                                keys);
+  else
+    mtd::level16_kernel<false><<<(unsigned)grid, mtd::kThreads, 0, st>>>(src, rec, make_args(p, q, trellis_lambda, qm_row),
                                                                 qm_row, costs, blocks, nblocks, combos, ncombos, res,
                                                                 keys);
   mtd::level8_finalize_kernel<<<(nblocks + 255) / 256, 256, 0, st>>>(keys, nblocks, res, best);

@@ -204,7 +204,7 @@ __device__ float rate16(const C* cf, int eob, const mt_coef_costs& T, int skip_c
 
 // Hadamard 4x4 SATD of src - clamp(pred + resid) over the 16 tiles of a 16x16
 // block (src/partition_rd.rs:86-133).
-template <typename P, typename R>
+template <bool MASK, typename P, typename R>
 __device__ uint32_t satd16(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred, const R* rr,
                            int32_t maxv, int vw, int vh) {
   uint32_t satd = 0;
@@ -218,7 +218,7 @@ __device__ uint32_t satd16(const uint16_t* __restrict__ src, int stride, int px,
 #pragma unroll
       for (int x = 0; x < 4; x++) {
         const int i = (ty + y) * 16 + tx + x;
-        d[x] = (tx + x < vw && ty + y < vh)
+        d[x] = (!MASK || (tx + x < vw && ty + y < vh))
                    ? (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv)
                    : 0;
       }
@@ -262,6 +262,7 @@ struct Work16 {
 };
 
 // One whole 16x16 candidate.  `qs` holds fwd_qm_scale of the 256 QM weights.
+template <bool VIS>
 __device__ __forceinline__ void chain16_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
                                             const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
                                             const uint8_t* qm, const float* qs, const float* lut,
@@ -291,8 +292,10 @@ __device__ __forceinline__ void chain16_one(const uint16_t* __restrict__ src, co
       if (cf[kScan16[i]] != 0) eob = i;
   }
   inv16x16(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
-  const uint32_t satd = satd16(src, p.stride, cd.px, cd.py, pred, rr, maxv, vis_extent(p.vis_w, p.frame_w, cd.px),
-                               vis_extent(p.vis_h, p.frame_h, cd.py));
+  const int vw = vis_extent(p.vis_w, p.frame_w, cd.px), vh = vis_extent(p.vis_h, p.frame_h, cd.py);
+  // VIS: the frame is displayed smaller than coded; samples past the
+  // displayed edge carry no distortion.
+  const uint32_t satd = satd16<VIS>(src, p.stride, cd.px, cd.py, pred, rr, maxv, vw, vh);
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);

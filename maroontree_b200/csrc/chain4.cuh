@@ -204,7 +204,7 @@ __device__ float rate4(const C* cf, int eob, const mt_coef_costs& T, int skip_ct
 }
 
 // Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
-template <typename P, typename R>
+template <bool MASK, typename P, typename R>
 __device__ __forceinline__ uint32_t satd4(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
                                           const R* rr, int32_t maxv, int vw, int vh) {
   int32_t r[4][4];
@@ -214,8 +214,9 @@ __device__ __forceinline__ uint32_t satd4(const uint16_t* __restrict__ src, int 
 #pragma unroll
     for (int x = 0; x < 4; x++) {
       const int i = y * 4 + x;
-      d[x] = (x < vw && y < vh) ? (int32_t)src[(size_t)(py + y) * stride + px + x] - clampi(pred[i] + rr[i], 0, maxv)
-                                : 0;
+      d[x] = (!MASK || (x < vw && y < vh))
+                 ? (int32_t)src[(size_t)(py + y) * stride + px + x] - clampi(pred[i] + rr[i], 0, maxv)
+                 : 0;
     }
     const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
     r[y][0] = e + g;
@@ -256,6 +257,7 @@ static_assert(kWork4Words >= 57, "4x4 arena too small");
 
 // Evaluate one 4x4 candidate; leaves the final levels in w.cf(), the
 // prediction in w.pred() and the inverse residual in w.rr().
+template <bool VIS>
 __device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
                                            const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
                                            const uint8_t* qm, const float* qs, const float* lut,
@@ -286,8 +288,10 @@ __device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, con
       if (cf[kScan4[i]] != 0) eob = i;
   }
   inv4x4(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
-  const uint32_t satd = satd4(src, p.stride, cd.px, cd.py, pred, rr, maxv, vis_extent(p.vis_w, p.frame_w, cd.px),
-                               vis_extent(p.vis_h, p.frame_h, cd.py));
+  const int vw = vis_extent(p.vis_w, p.frame_w, cd.px), vh = vis_extent(p.vis_h, p.frame_h, cd.py);
+  // VIS: the frame is displayed smaller than coded; samples past the
+  // displayed edge carry no distortion.
+  const uint32_t satd = satd4<VIS>(src, p.stride, cd.px, cd.py, pred, rr, maxv, vw, vh);
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);

@@ -279,7 +279,7 @@ __device__ __forceinline__ int vis_extent(int vis, int frame, int p) { return (v
 constexpr int kSatdUnroll = MT_SATD_UNROLL;
 
 // Hadamard 4x4 SATD of src - clamp(pred + resid) (src/partition_rd.rs:86-133).
-template <typename P, typename R>
+template <bool MASK, typename P, typename R>
 __device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int stride, int px, int py, const P* pred,
                                           const R* rr, int32_t maxv, int vw, int vh) {
   uint32_t satd = 0;
@@ -294,7 +294,7 @@ __device__ __forceinline__ uint32_t satd8(const uint16_t* __restrict__ src, int 
 #pragma unroll
         for (int x = 0; x < 4; x++) {
           const int i = (ty + y) * 8 + tx + x;
-          d[x] = (tx + x < vw && ty + y < vh)
+          d[x] = (!MASK || (tx + x < vw && ty + y < vh))
                    ? (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - clampi(pred[i] + rr[i], 0, maxv)
                    : 0;
         }
@@ -355,6 +355,7 @@ __device__ __forceinline__ void chain8_predict(const uint16_t* __restrict__ rec,
 
 // The rest of the chain for candidate cd from the prediction in w.pred()
 // (left intact, so several transform types can share one prediction).
+template <bool VIS>
 __device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, const mt_chain_params& p,
                                           const mt_quant& q, float trellis_lambda, const uint8_t* qm,
                                           const float* qs, const float* lut, const mt_coef_costs& T,
@@ -382,8 +383,10 @@ __device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, cons
       if (cf[kScan8[i]] != 0) eob = i;
   }
   inv8x8(cf, TX, q, qm, rr, reinterpret_cast<int32_t*>(w.suf()));
-  const uint32_t satd = satd8(src, p.stride, cd.px, cd.py, pred, rr, maxv, vis_extent(p.vis_w, p.frame_w, cd.px),
-                               vis_extent(p.vis_h, p.frame_h, cd.py));
+  const int vw = vis_extent(p.vis_w, p.frame_w, cd.px), vh = vis_extent(p.vis_h, p.frame_h, cd.py);
+  // VIS: the frame is displayed smaller than coded; samples past the
+  // displayed edge carry no distortion.
+  const uint32_t satd = satd8<VIS>(src, p.stride, cd.px, cd.py, pred, rr, maxv, vw, vh);
   const float qstep = (float)q.ac_q;
   float price = __fmul_rn(__fmul_rn(__fmul_rn((float)satd, fmaxf(qstep, 1.0f)), 0.25f), p.satd_scale);
   if (p.satd_bridge != 0.0f) price = __fmul_rn(price, p.satd_bridge);
@@ -399,13 +402,14 @@ __device__ __forceinline__ void chain8_tx(const uint16_t* __restrict__ src, cons
   r.reserved[0] = r.reserved[1] = r.reserved[2] = 0;
 }
 
+template <bool VIS>
 __device__ __forceinline__ void chain8_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
                                            const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
                                            const uint8_t* qm, const float* qs, const float* lut,
                                            const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
                                            Work8& w) {
   chain8_predict(rec, p, cd, w);
-  chain8_tx(src, p, q, trellis_lambda, qm, qs, lut, T, cd, r, w);
+  chain8_tx<VIS>(src, p, q, trellis_lambda, qm, qs, lut, T, cd, r, w);
 }
 
 }  // namespace mtd

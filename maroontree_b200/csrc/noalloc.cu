@@ -70,6 +70,7 @@ __device__ __forceinline__ void noalloc_tables(const mt_coef_costs* __restrict__
 
 // Pass 1: every (combo, block) candidate, folded into the block's key
 // (cost bits << 32 | combo), the same order as the level kernel's argmin.
+template <bool VIS>
 __global__ void __launch_bounds__(kNoAllocThreads) noalloc_keys_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, NoAllocArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs, const mt_block8* __restrict__ blocks,
@@ -88,11 +89,12 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_keys_kernel(
   int32_t store[mtd::kWork8Words];
   mtd::Work8 w{store};
   mt_candidate_result r;
-  mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+  mtd::chain8_one<VIS>(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
   atomicMin(&keys[b], ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)c);
 }
 
 // Pass 2: one thread per block re-evaluates its winning candidate.
+template <bool VIS>
 __global__ void __launch_bounds__(kNoAllocThreads) noalloc_winner_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, NoAllocArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs, const mt_block8* __restrict__ blocks,
@@ -117,7 +119,7 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_winner_kernel(
     int32_t store[mtd::kWork8Words];
   mtd::Work8 w{store};
     mt_candidate_result r;
-    mtd::chain8_one(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
+    mtd::chain8_one<VIS>(src, rec, a.p, a.q, a.trellis_lambda, a.has_qm ? sQm : nullptr, sQs, sLut, sC, cd, r, w);
     o.combo = c;
     o.cost = r.cost;
     o.distortion = r.distortion;
@@ -189,9 +191,19 @@ extern "C" int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_
     return MT_ERR_DEVICE;
   const long long total = (long long)nblocks * ncombos;
   const unsigned grid = (unsigned)((total + kNoAllocThreads - 1) / kNoAllocThreads);
-  noalloc_keys_kernel<<<grid, kNoAllocThreads, 0, st>>>(d_src, d_recon, a, d_qm_row, d_costs, d_blocks, nblocks,
+  // A frame displayed smaller than coded masks the samples past its edge.
+  const bool vis = (prm->vis_w > 0 && prm->vis_w < prm->frame_w) || (prm->vis_h > 0 && prm->vis_h < prm->frame_h);
+  if (vis)
+    noalloc_keys_kernel<true><<<grid, kNoAllocThreads, 0, st>>>(d_src, d_recon, a, d_qm_row, d_costs, d_blocks, nblocks,
                                                          d_combos, ncombos, keys);
-  noalloc_winner_kernel<<<(nblocks + kNoAllocThreads - 1) / kNoAllocThreads, kNoAllocThreads, 0, st>>>(
+  else
+    noalloc_keys_kernel<false><<<grid, kNoAllocThreads, 0, st>>>(d_src, d_recon, a, d_qm_row, d_costs, d_blocks, nblocks,
+                                                         d_combos, ncombos, keys);
+  if (vis)
+    noalloc_winner_kernel<true><<<(nblocks + kNoAllocThreads - 1) / kNoAllocThreads, kNoAllocThreads, 0, st>>>(
+      d_src, d_recon, a, d_qm_row, d_costs, d_blocks, nblocks, d_combos, keys, d_best);
+  else
+    noalloc_winner_kernel<false><<<(nblocks + kNoAllocThreads - 1) / kNoAllocThreads, kNoAllocThreads, 0, st>>>(
       d_src, d_recon, a, d_qm_row, d_costs, d_blocks, nblocks, d_combos, keys, d_best);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
