@@ -324,6 +324,25 @@ int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_t* d_recon,
                                  const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
                                  int32_t ncombos, mt_block_best* d_best, void* stream);
 
+/* ---- The proxy's mode beam ----
+ * proxy_mode_beam's ranking (src/coder/partition_search.rs:187-238): for every
+ * N x N block (N = prm->tx_size: 4, 8 or 16), the 11 nd_modes (DC, V, H, D45,
+ * D135, D113, D157, D203, D67, SMOOTH, PAETH; src/intrapred.rs:1712-1729)
+ * predicted at angle delta 0 from the reconstruction, each scored by
+ * satd_sad_proxy (SAD + SATD/4 over 4x4 Hadamard tiles of src - pred,
+ * src/rd_sse.rs:559-589, :1143-1176; samples past the displayed frame count as
+ * the prediction), sorted by (score, mode).  The caller keeps the first
+ * proxy_mode_beam_len of them (Slow 4:4:4 keeps {DC, PAETH} without ranking).
+ * scores / modes: nblocks x MT_BEAM_MODES, ascending.  A block outside the
+ * frame gets scores of all ones and mode 255. */
+#define MT_BEAM_MODES 11
+int mt_mode_beam_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_chain_params* prm,
+                        const mt_block8* d_blocks, int32_t nblocks, uint64_t* d_scores, uint8_t* d_modes,
+                        void* stream);
+/* Host-buffer form of mt_mode_beam_device (scores may be NULL). */
+int mt_mode_beam(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_block8* blocks,
+                 int32_t nblocks, uint64_t* scores, uint8_t* modes);
+
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and
  * f32 quantisation targets, with the QM applied as DctDispatch does. */

@@ -159,6 +159,23 @@ def rdo_level16(src, recon, prm, quant, qmrow, costs, blocks, combos, want_resul
     return best, res
 
 
+def mode_beam(src, recon, prm, blocks):
+    """``proxy_mode_beam``'s ranking (``mt_mode_beam``): (scores, modes), each
+    nblocks x 11 in ascending (score, mode) order; prm.tx_size is the block size."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.BLOCK8_DTYPE)
+    scores = np.zeros((len(blocks), abi_beam_modes()), np.uint64)
+    modes = np.zeros((len(blocks), abi_beam_modes()), np.uint8)
+    _check(load().mt_mode_beam(ptr(src), ptr(recon), C.byref(prm), ptr(blocks), len(blocks), ptr(scores), ptr(modes)),
+           "mt_mode_beam")
+    return scores, modes
+
+
+def abi_beam_modes():
+    return 11
+
+
 def rdo_level8_scratch_bytes(nblocks, ncombos):
     """Device working storage ``mt_rdo_level8_device`` needs."""
     return load().mt_rdo_level8_scratch_bytes(nblocks, ncombos)

@@ -190,6 +190,8 @@ def _bind(lib):
         "mt_aq_grid_device": (C.c_int, [_P, C.POINTER(AqParams), _P, _P, _P, _P]),
         "mt_aq_grid": (C.c_int, [_P, C.POINTER(AqParams), _P, _P]),
         "mt_dark_pow_device": (C.c_int, [_P, _P, C.c_int64, _P]),
+        "mt_mode_beam_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P, _P]),
+        "mt_mode_beam": (C.c_int, [_P, _P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
         "mt_screen_gate_device": (C.c_int, [_P, C.POINTER(ScreenGateParams), _P, C.POINTER(ScreenGateResult), _P]),
         "mt_screen_gate": (C.c_int, [_P, C.POINTER(ScreenGateParams), C.POINTER(ScreenGateResult)]),
@@ -229,7 +231,7 @@ EXPORTED_SYMBOLS = (
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
-    "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate",
+    "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate", "mt_mode_beam_device", "mt_mode_beam",
 )
 
 

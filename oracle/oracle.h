@@ -28,6 +28,9 @@ const uint16_t* or_default_scan(int32_t n);
 
 /* dct.rs: forward transform + quantisation of one n x n block (n = 8). */
 void or_dct1d(int32_t* buf, int32_t n);
+/* partition_search.rs proxy_mode_beam's ranking (11 nd_modes by satd_sad_proxy). */
+int or_mode_beam(const uint16_t* src, const uint16_t* recon, const mt_chain_params* p, const mt_block8* blocks,
+                 int32_t nblocks, uint64_t* scores, uint8_t* modes);
 void or_fwd_txfm_quant(const int32_t* resid, int32_t tx_type, int32_t n, const mt_quant* q,
                        const uint8_t* qm_row, int32_t* levels, float* targets);
 /* idct.rs: dequantisation + inverse transform of one block. */

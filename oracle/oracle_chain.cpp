@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <thread>
+#include <algorithm>
 #include <vector>
 
 #include "../maroontree_b200/csrc/av1_tables.h"
@@ -1478,6 +1479,67 @@ static void chain_one(const uint16_t* src, const uint16_t* recon, const mt_chain
   if (lv_out) memcpy(lv_out, cf, sizeof(int32_t) * N);
   if (rec_out)
     for (int i = 0; i < N; i++) rec_out[i] = clampi(pred[i] + rr[i], 0, maxv);
+}
+
+// partition_search.rs:187-238 proxy_mode_beam's ranking: the 11 nd_modes
+// (intrapred.rs:1712-1724) predicted at delta 0, scored by satd_sad_proxy
+// (rd_sse.rs:559-589, :1143-1176; samples past the displayed window taken as
+// the prediction), sorted by (score, mode).
+int or_mode_beam(const uint16_t* src, const uint16_t* recon, const mt_chain_params* p, const mt_block8* blocks,
+                 int32_t nblocks, uint64_t* scores, uint8_t* modes) {
+  static const int ND[11] = {MT_DC_PRED,   MT_V_PRED,    MT_H_PRED,    MT_D45_PRED,    MT_D135_PRED, MT_D113_PRED,
+                             MT_D157_PRED, MT_D203_PRED, MT_D67_PRED,  MT_SMOOTH_PRED, MT_PAETH_PRED};
+  const int n = p->tx_size;
+  std::vector<int32_t> pred((size_t)n * n);
+  for (int b = 0; b < nblocks; b++) {
+    const mt_block8& bk = blocks[b];
+    if (bk.px + n > p->frame_w || bk.py + n > p->frame_h) {
+      for (int k = 0; k < 11; k++) {
+        if (scores) scores[(size_t)b * 11 + k] = UINT64_MAX;
+        modes[(size_t)b * 11 + k] = 255;
+      }
+      continue;
+    }
+    const int vw = (p->vis_w > 0 ? p->vis_w : p->frame_w) - bk.px;
+    const int vh = (p->vis_h > 0 ? p->vis_h : p->frame_h) - bk.py;
+    std::vector<std::pair<uint64_t, int>> ranked;
+    for (int m : ND) {
+      or_intra_predict(recon, p->stride, bk.px, bk.py, n, n, m, 0, (bk.flags & 1) != 0, (bk.flags & 2) != 0,
+                       p->frame_w, p->frame_h, (bk.flags & 4) != 0, p->bd, pred.data());
+      uint64_t sad = 0, satd = 0;
+      for (int ty = 0; ty < n; ty += 4)
+        for (int tx = 0; tx < n; tx += 4) {
+          int32_t rows[4][4];
+          for (int r = 0; r < 4; r++) {
+            int32_t d[4];
+            for (int x = 0; x < 4; x++) {
+              const bool vis = tx + x < vw && ty + r < vh;
+              d[x] = vis ? (int32_t)src[(size_t)(bk.py + ty + r) * p->stride + bk.px + tx + x] -
+                               pred[(size_t)(ty + r) * n + tx + x]
+                         : 0;
+              sad += uabs(d[x]);
+            }
+            const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
+            rows[r][0] = e + g;
+            rows[r][1] = f + h;
+            rows[r][2] = f - h;
+            rows[r][3] = e - g;
+          }
+          for (int x = 0; x < 4; x++) {
+            const int32_t a = rows[0][x], bb = rows[1][x], c = rows[2][x], dd = rows[3][x];
+            const int32_t e = a + c, f = a - c, g = bb + dd, h = bb - dd;
+            satd += (uint64_t)uabs(e + g) + uabs(f + h) + uabs(f - h) + uabs(e - g);
+          }
+        }
+      ranked.emplace_back(sad + (satd >> 2), m);
+    }
+    std::sort(ranked.begin(), ranked.end());
+    for (int k = 0; k < 11; k++) {
+      if (scores) scores[(size_t)b * 11 + k] = ranked[k].first;
+      modes[(size_t)b * 11 + k] = (uint8_t)ranked[k].second;
+    }
+  }
+  return MT_OK;
 }
 
 // The forward 1-D integer DCT of n = 4, 8 or 16 points in place (dct.rs:175-276).

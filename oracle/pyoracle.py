@@ -51,6 +51,7 @@ def load():
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
             "or_fast_round": (C.c_float, [C.c_float]),
             "or_dct1d": (None, [_P, C.c_int32]),
+            "or_mode_beam": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), _P, C.c_int32, _P, _P]),
             "or_dirty_log1pf": (C.c_float, [C.c_float]),
             "or_dark_pow": (None, [_P, _P, C.c_int64]),
             "or_dark_protection": (C.c_int32, [C.c_int32, C.c_int32, _P] + [C.c_int32] * 5 + [C.c_float]),
@@ -293,3 +294,14 @@ def dct1d(buf):
     b = np.ascontiguousarray(buf, np.int32).copy()
     load().or_dct1d(p(b), len(b))
     return b
+
+
+def mode_beam(src, recon, prm, blocks):
+    """(scores, modes): nblocks x 11 each, ascending (score, mode)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.BLOCK8_DTYPE)
+    scores = np.zeros((len(blocks), 11), np.uint64)
+    modes = np.zeros((len(blocks), 11), np.uint8)
+    assert load().or_mode_beam(p(src), p(recon), C.byref(prm), p(blocks), len(blocks), p(scores), p(modes)) == 0
+    return scores, modes
