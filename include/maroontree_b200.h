@@ -343,6 +343,24 @@ int mt_mode_beam_device(const uint16_t* d_src, const uint16_t* d_recon, const mt
 int mt_mode_beam(const uint16_t* src, const uint16_t* recon, const mt_chain_params* prm, const mt_block8* blocks,
                  int32_t nblocks, uint64_t* scores, uint8_t* modes);
 
+/* ---- Decision distortion of reconstructed blocks ----
+ * sse_recon (src/rd_sse.rs:449-475) of n w x h luma blocks (w, h multiples of
+ * 4 up to 64): the error src - clamp(pred + resid, 0, 2^bd - 1) over the part
+ * of each block inside the displayed plane (vis_w x vis_h samples; a block
+ * wholly outside scores 0).  wsse_scale 0: the plain SSE; > 0: the reference's
+ * weighted decision distortion round(weighted_sse(err) * wsse_scale), half away
+ * from zero, err zero-padded to whole 4x4 tiles of the displayed part
+ * (src/rd_sse.rs:244-271; the 4x4-DCT weighted SSE in the pinned AVX2 order,
+ * src/avx/rd.rs:767-848).  pos: (px, py) u16 pairs; pred / resid: n blocks of
+ * w*h int32 packed row-major (resid may be NULL: zero). */
+int mt_sse_recon_device(const uint16_t* d_src, int32_t stride, int32_t vis_w, int32_t vis_h, int32_t bd,
+                        const uint16_t* d_pos, const int32_t* d_pred, const int32_t* d_resid, int32_t n, int32_t w,
+                        int32_t h, float wsse_scale, int64_t* d_out, void* stream);
+/* Host-buffer form (the source plane is stride x plane_h samples). */
+int mt_sse_recon(const uint16_t* src, int32_t stride, int32_t plane_h, int32_t vis_w, int32_t vis_h, int32_t bd,
+                 const uint16_t* pos, const int32_t* pred, const int32_t* resid, int32_t n, int32_t w, int32_t h,
+                 float wsse_scale, int64_t* out);
+
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and
  * f32 quantisation targets, with the QM applied as DctDispatch does. */

@@ -172,6 +172,19 @@ def mode_beam(src, recon, prm, blocks):
     return scores, modes
 
 
+def sse_recon(src, vis_w, vis_h, pos, pred, resid, w, h, wsse_scale=0.0, bd=8):
+    """``sse_recon`` decision distortion of n blocks (``mt_sse_recon``): plain SSE,
+    or with wsse_scale > 0 the scaled weighted SSE; returns int64[n]."""
+    src = np.ascontiguousarray(src, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    pred = np.ascontiguousarray(pred, np.int32)
+    resid = None if resid is None else np.ascontiguousarray(resid, np.int32)
+    out = np.zeros(len(pos), np.int64)
+    _check(load().mt_sse_recon(ptr(src), src.shape[1], src.shape[0], vis_w, vis_h, bd, ptr(pos), ptr(pred),
+                               ptr(resid), len(pos), w, h, wsse_scale, ptr(out)), "mt_sse_recon")
+    return out
+
+
 def abi_beam_modes():
     return 11
 

@@ -191,6 +191,8 @@ def _bind(lib):
         "mt_aq_grid": (C.c_int, [_P, C.POINTER(AqParams), _P, _P]),
         "mt_dark_pow_device": (C.c_int, [_P, _P, C.c_int64, _P]),
         "mt_mode_beam_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P, _P]),
+        "mt_sse_recon_device": (C.c_int, [_P] + [C.c_int32] * 4 + [_P, _P, _P] + [C.c_int32] * 3 + [C.c_float, _P, _P]),
+        "mt_sse_recon": (C.c_int, [_P] + [C.c_int32] * 5 + [_P, _P, _P] + [C.c_int32] * 3 + [C.c_float, _P]),
         "mt_mode_beam": (C.c_int, [_P, _P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
         "mt_screen_gate_device": (C.c_int, [_P, C.POINTER(ScreenGateParams), _P, C.POINTER(ScreenGateResult), _P]),
@@ -232,6 +234,7 @@ EXPORTED_SYMBOLS = (
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
     "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate", "mt_mode_beam_device", "mt_mode_beam",
+    "mt_sse_recon_device", "mt_sse_recon",
 )
 
 

@@ -85,6 +85,9 @@ int or_cdef_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint16_t* sy, con
                   int64_t* luma_tab, int64_t* u_tab, int64_t* v_tab, uint8_t* dirs, int32_t* vars);
 float or_weighted_sse(const int32_t* err, int32_t w, int32_t h);
 float or_cdef_frame_lambda(int32_t qidx, int32_t bd, int32_t sub_x, int32_t sub_y);
+/* rd_sse.rs sse_recon (plain or weighted decision distortion) of n blocks. */
+int or_sse_recon(const uint16_t* src, int32_t stride, int32_t vis_w, int32_t vis_h, int32_t bd, const uint16_t* pos,
+                 const int32_t* pred, const int32_t* resid, int32_t n, int32_t w, int32_t h, float scale, int64_t* out);
 /* aq_common.rs / coder/aq.rs / lossy_state.rs: the adaptive-quantisation grid and its pieces. */
 float or_fast_round(float x);
 float or_dirty_log1pf(float d);

@@ -675,6 +675,47 @@ extern "C" int or_cdef_frame(uint16_t* py, uint16_t* pu, uint16_t* pv, const uin
 }
 
 extern "C" float or_weighted_sse(const int32_t* err, int32_t w, int32_t h) { return wsse_avx2(err, w, h); }
+
+// rd_sse.rs:449-475 sse_recon with the SrcBlock visibility (rd_sse.rs:61-167)
+// and weighted_dist (rd_sse.rs:244-271): plain SSE, or round(wsse * scale)
+// over the displayed part padded to whole 4x4 tiles.
+extern "C" int or_sse_recon(const uint16_t* src, int32_t stride, int32_t vis_w, int32_t vis_h, int32_t bd,
+                            const uint16_t* pos, const int32_t* pred, const int32_t* resid, int32_t n, int32_t w,
+                            int32_t h, float scale, int64_t* out) {
+  const int32_t maxv = (1 << bd) - 1;
+  for (int b = 0; b < n; b++) {
+    const int px = pos[2 * b], py = pos[2 * b + 1];
+    const int vw = std::min(std::max(vis_w - px, 0), w), vh = std::min(std::max(vis_h - py, 0), h);
+    const int32_t* pr = pred + (size_t)b * w * h;
+    const int32_t* rs = resid ? resid + (size_t)b * w * h : nullptr;
+    auto err = [&](int x, int y) {
+      const int i = y * w + x;
+      return (int32_t)src[(size_t)(py + y) * stride + px + x] -
+             std::min(std::max(pr[i] + (rs ? rs[i] : 0), 0), maxv);
+    };
+    if (vw == 0 || vh == 0) {
+      out[b] = 0;
+      continue;
+    }
+    if (scale > 0.0f) {
+      const int pw = (vw + 3) & ~3, ph = (vh + 3) & ~3;
+      std::vector<int32_t> buf((size_t)pw * ph, 0);
+      for (int y = 0; y < vh; y++)
+        for (int x = 0; x < vw; x++) buf[(size_t)y * pw + x] = err(x, y);
+      const float d = wsse_avx2(buf.data(), pw, ph);
+      out[b] = (int64_t)roundf(d * scale);
+    } else {
+      int64_t s = 0;
+      for (int y = 0; y < vh; y++)
+        for (int x = 0; x < vw; x++) {
+          const int64_t v = err(x, y);
+          s += v * v;
+        }
+      out[b] = s;
+    }
+  }
+  return MT_OK;
+}
 extern "C" float or_cdef_frame_lambda(int32_t qidx, int32_t bd, int32_t sub_x, int32_t sub_y) {
   return frame_lambda_d(qidx, bd, sub_x, sub_y);
 }

@@ -51,6 +51,7 @@ def load():
             "or_coef_costs_build": (None, [C.POINTER(abi.CoefCdfs), C.POINTER(abi.CoefCosts)]),
             "or_fast_round": (C.c_float, [C.c_float]),
             "or_dct1d": (None, [_P, C.c_int32]),
+            "or_sse_recon": (C.c_int, [_P] + [C.c_int32] * 4 + [_P, _P, _P] + [C.c_int32] * 3 + [C.c_float, _P]),
             "or_mode_beam": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), _P, C.c_int32, _P, _P]),
             "or_dirty_log1pf": (C.c_float, [C.c_float]),
             "or_dark_pow": (None, [_P, _P, C.c_int64]),
@@ -305,3 +306,14 @@ def mode_beam(src, recon, prm, blocks):
     modes = np.zeros((len(blocks), 11), np.uint8)
     assert load().or_mode_beam(p(src), p(recon), C.byref(prm), p(blocks), len(blocks), p(scores), p(modes)) == 0
     return scores, modes
+
+
+def sse_recon(src, vis_w, vis_h, pos, pred, resid, w, h, scale=0.0, bd=8):
+    src = np.ascontiguousarray(src, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    pred = np.ascontiguousarray(pred, np.int32)
+    resid = None if resid is None else np.ascontiguousarray(resid, np.int32)
+    out = np.zeros(len(pos), np.int64)
+    assert load().or_sse_recon(p(src), src.shape[1], vis_w, vis_h, bd, p(pos), p(pred), p(resid), len(pos), w, h,
+                               scale, p(out)) == 0
+    return out
