@@ -121,6 +121,52 @@ def dist_env():
     return world, rank, local
 
 
+class Replicas:
+    """One process per GPU, each encoding its own frame (replicas: the path has
+    no exchange step, so nothing crosses ranks on the data path).  The process
+    group carries only the barriers around the timed region and the max-over-
+    ranks reduction of the step time; only rank 0 prints the JSON line."""
+
+    def __init__(self, backend="nccl", timeout_s=120):
+        self.world, self.rank, self.local = dist_env()
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, value, device="cpu"):
+        """The maximum of a per-rank float over all ranks."""
+        if self.dist is None:
+            return float(value)
+        import torch
+
+        t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def job_value(self, step_ms, units_per_rank=MPIX):
+        """Whole-job throughput: the units every rank processed over the slowest rank's step."""
+        return self.world * units_per_rank / (step_ms / 1e3)
+
+    def emit(self, line):
+        if self.rank == 0:
+            print(json.dumps(line), flush=True)
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 def cpu_rate(wl, sample, threads):
     """Oracle throughput (candidates/s) over a bounded slice of the candidates."""
     from oracle import pyoracle as po
@@ -368,12 +414,10 @@ def run_ours(args):
     import maroontree_b200 as mt
     from maroontree_b200 import abi
 
-    world, rank, local = dist_env()
-    if world > 1:
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    ranks = Replicas("nccl")
+    world, rank = ranks.world, ranks.rank
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     mt.load()
@@ -400,8 +444,7 @@ def run_ours(args):
     for _ in range(max(args.warmup, 3)):
         launch()
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    ranks.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
@@ -412,23 +455,20 @@ def run_ours(args):
             ev[i][1].record(stream)
         torch.cuda.synchronize()
     kernel_ms = [a.elapsed_time(b) for a, b in ev]
-    step_ms = float(np.mean(kernel_ms))
-    t = torch.tensor([step_ms], device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    step_ms = float(t.item())
-    value = world * MPIX / (step_ms / 1e3)
+    step_ms = ranks.max(float(np.mean(kernel_ms)), device=dev)
+    value = ranks.job_value(step_ms)
 
     # e2e through the host ABI (mt_rdo_level8): planes, block and combo lists
     # copied in and the per-block winners copied out inside the timed region
     src, rec = wl["src"], wl["rec"]
     e2e_times = []
+    ranks.barrier()
     for i in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         best, _ = mt.rdo_level8(src, rec, wl["prm"], wl["q"], wl["qm"], costs, blocks, combos)
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.median(e2e_times))
+    e2e_s = ranks.max(float(np.median(e2e_times)), device=dev)
     h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + blocks.nbytes + combos.nbytes
     d2h = nb * abi.BEST_DTYPE.itemsize
 
@@ -469,7 +509,7 @@ def run_ours(args):
         "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
                    "candidates": n, "blocks": nb, "combos": nc, "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed launches"},
-        "e2e": {"value": round(world * MPIX / e2e_s, 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
+        "e2e": {"value": round(ranks.job_value(e2e_s * 1e3), 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 5), "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
@@ -486,11 +526,8 @@ def run_ours(args):
         "clocks": clk.summary(),
         "cpu_baseline": cpu,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    ranks.emit(line)
+    ranks.close()
     return 0
 
 
