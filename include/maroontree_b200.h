@@ -97,6 +97,8 @@ typedef struct mt_coef_cdfs {
   uint16_t eob_bin[11];   /* eob_pt CDF of this size; unused tail = 0 */
   uint16_t dc_sign[3][2];
   uint16_t txtp[13][16];  /* intra tx-type CDF per y mode; unused tail = 0 */
+  uint16_t eob_bin_1d[11]; /* eob_pt CDF of the 1-D classes (V_DCT / H_DCT) of this size
+                            * (eob_bin_16_l1d / eob_bin_64_l1d); unused tail = 0 */
 } mt_coef_cdfs;
 
 /* Bit costs of the same slice, each entry cdf_cost_with_table(cdf, s)
@@ -111,6 +113,7 @@ typedef struct mt_coef_costs {
   float eob_bin[11];
   float dc_sign[3][2];
   float txtp[13][16];
+  float eob_bin_1d[11];
 } mt_coef_costs;
 
 /* One candidate of the batched chain: block position, intra mode (+ angle
@@ -360,6 +363,80 @@ int mt_sse_recon_device(const uint16_t* d_src, int32_t stride, int32_t vis_w, in
 int mt_sse_recon(const uint16_t* src, int32_t stride, int32_t plane_h, int32_t vis_w, int32_t vis_h, int32_t bd,
                  const uint16_t* pos, const int32_t* pred, const int32_t* resid, int32_t n, int32_t w, int32_t h,
                  float wsse_scale, int64_t* out);
+
+/* ---- Context-aware trellis ----
+ * trellis_optimize_ctx (src/trellis.rs:55-942) of n TX_8X8 luma blocks
+ * (class 1, plane 0) against the decision-CDF costs: the per-coefficient
+ * RD-best level in reverse scan order with the real base/range token costs,
+ * then the EOB position by the eob_pt / eob_base costs, with quantisation-
+ * matrix weighting (w/32, squared from QM level 5) and the tile's band tilt
+ * (distortion of coefficients with |target| < 2 divided by
+ * 1 + tilt * index / 64).  Shipped tuning: no dead zone, the DC-only terminal
+ * in context 0, skip priced at 1 bit.  d_levels (column-major int32, 64 per
+ * block) are updated in place; d_dcs_ctx: the dc_sign context of each block.
+ * lambda0 <= 0 leaves the levels unchanged. */
+int mt_trellis_optimize_ctx_device(int32_t* d_levels, const float* d_targets, const uint8_t* d_dcs_ctx, int32_t n,
+                                   const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                                   float lambda0, float band_tilt, void* stream);
+
+/* ---- The 16x16 leaf's TX_8X8 split trial ----
+ * split16_luma_try (src/coder/partition_search.rs:4235-4428) of a batch of
+ * (16x16 block, luma mode) jobs: the four 8x8 quadrants in raster order, each
+ * predicted from the reconstruction with the quadrants already trial-coded
+ * (edge flags (py > 0, px > 0), (have_tr, 0), (1, have_bl), (0, 0)), DCT_DCT
+ * with trellis_optimize_ctx, the dav1d inverse and sse_recon; with tx_search
+ * the 4:4:4 type trials ADST_ADST, ADST_DCT, DCT_ADST (trellised), IDTX,
+ * V_DCT, H_DCT (not trellised), each gated on its SSE (the ADST family within
+ * tx_guard of the DCT's) and priced only when the gate passes: the 2-D types by
+ * real_block_bits_bounded (src/rate.rs:149-291) in the quadrant's progressive
+ * txb_skip / dc_sign contexts, V/H by luma_bits_1d_8x8 (src/coder/
+ * lossy_state.rs:876-1008); the lowest rd_cost_i64 wins, ties to the earlier
+ * type.  The winner's coefficient result context (lossy_state.rs:630-648)
+ * feeds the next quadrant's contexts, its reconstruction the next quadrant's
+ * prediction. */
+typedef struct mt_split16_params {
+  int32_t frame_w, frame_h; /* padded plane size, also the prediction frame bounds */
+  int32_t stride;           /* samples per row of src and recon */
+  int32_t bd;               /* bit depth (8) */
+  int32_t vis_w, vis_h;     /* displayed luma size; 0 = frame_w / frame_h */
+  float trellis_lambda0;    /* lam of trellis_optimize_ctx; <= 0 disables */
+  float rd_lambda;          /* rd_lam of the type gates and the bits bound (the caller's mlam) */
+  float band_tilt;          /* Cdfs::band_tilt of the tile (src/coder/lossy_state.rs:351-359) */
+  float wsse_scale;         /* sse_recon: 0 plain SSE, > 0 the scaled weighted SSE */
+  int32_t tx_search;        /* 1: the 4:4:4 type search; 0: DCT_DCT only (4:2:0, 4:2:2, mono) */
+  int32_t tx_guard_shift;   /* Tuning::tx_guard_shift (4) / tx_guard_shift_444 (5); >= 63: no slack */
+  int32_t use_skip_bits;    /* 1: skip_bits replace the txb_skip CDF cost of the 2-D walks */
+  float skip_bits[13][2];   /* skip_price of class TX_8X8 per context: (all_zero = 1, all_zero = 0) */
+} mt_split16_params;
+
+typedef struct mt_split16_job {
+  uint16_t px, py;          /* 16x16 block origin (luma samples) */
+  uint8_t mode;             /* MT_*_PRED */
+  int8_t angle_delta;       /* -3..3, directional modes only */
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL / FILTER_TYPE of the 16x16 block */
+  uint8_t reserved;
+  uint8_t a_coef[4];        /* above coefficient contexts of the block's four 4-sample columns */
+  uint8_t l_coef[4];        /* left coefficient contexts of its four 4-sample rows */
+} mt_split16_job;
+
+typedef struct mt_split16_result {
+  int64_t sse;              /* sum of the quadrants' sse_recon */
+  float bits;               /* sum of the quadrants' coefficient bits, quadrant order */
+  uint8_t tx_types[4];      /* winning MT_TX_* per quadrant; all 255 for a rejected job */
+} mt_split16_result;
+
+/* Device form.  d_cf (optional): n x 256 int32, quadrant q's levels at
+ * [q*64, q*64 + 64) column-major; d_rec (optional): n x 256 u16, the 16x16
+ * trial reconstruction row-major.  A job outside the frame, or with a mode /
+ * delta out of range, is rejected (tx_types 255, sse 0, bits 0). */
+int mt_split16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                           const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                           const mt_split16_job* d_jobs, int32_t n, mt_split16_result* d_results, int32_t* d_cf,
+                           uint16_t* d_rec, void* stream);
+/* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
+int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                    const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                    mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
 
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and

@@ -185,6 +185,54 @@ def sse_recon(src, vis_w, vis_h, pos, pred, resid, w, h, wsse_scale=0.0, bd=8):
     return out
 
 
+def split16_params(frame_w, frame_h, stride=None, trellis_lambda0=0.05, rd_lambda=1.0, band_tilt=0.0,
+                   wsse_scale=0.0, tx_search=False, tx_guard_shift=4, skip_bits=None, vis=None, bd=8):
+    """``mt_split16_params``: skip_bits, when given, is 13 (all_zero = 1, all_zero = 0)
+    pairs of the TX_8X8 class (the reference's skip_price rows)."""
+    p = abi.Split16Params()
+    p.frame_w, p.frame_h, p.bd = frame_w, frame_h, bd
+    p.stride = stride if stride is not None else frame_w
+    if vis is not None:
+        p.vis_w, p.vis_h = vis
+    p.trellis_lambda0, p.rd_lambda, p.band_tilt, p.wsse_scale = trellis_lambda0, rd_lambda, band_tilt, wsse_scale
+    p.tx_search, p.tx_guard_shift = int(bool(tx_search)), tx_guard_shift
+    if skip_bits is not None:
+        p.use_skip_bits = 1
+        for k, (one, zero) in enumerate(skip_bits):
+            p.skip_bits[k][0], p.skip_bits[k][1] = one, zero
+    return p
+
+
+def split16_luma(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
+    """``split16_luma_try`` of a batch of (16x16 block, mode) jobs (``mt_split16_luma``):
+    returns (results, cf n x 256 or None, rec n x 16 x 16 or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_RESULT_DTYPE)
+    cf = np.zeros((n, 256), np.int32) if want_cf else None
+    rec = np.zeros((n, 16, 16), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_split16_luma(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                                  ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)), "mt_split16_luma")
+    return res, cf, rec
+
+
+def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
+                        stream=0):
+    _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),
+                                         ptr(d_costs), ptr(d_jobs), n, ptr(d_results), ptr(d_cf), ptr(d_rec),
+                                         stream), "mt_split16_luma_device")
+
+
+def trellis_optimize_ctx_device(d_levels, d_targets, d_dcs, n, quant, d_qm, d_costs, lambda0, band_tilt=0.0, stream=0):
+    """``trellis_optimize_ctx`` of n TX_8X8 luma blocks in place (``mt_trellis_optimize_ctx_device``)."""
+    _check(load().mt_trellis_optimize_ctx_device(ptr(d_levels), ptr(d_targets), ptr(d_dcs), n, C.byref(quant),
+                                                 ptr(d_qm), ptr(d_costs), lambda0, band_tilt, stream),
+           "mt_trellis_optimize_ctx_device")
+
+
 def abi_beam_modes():
     return 11
 

@@ -45,6 +45,7 @@ class CoefCdfs(C.Structure):
         ("eob_bin", C.c_uint16 * 11),
         ("dc_sign", (C.c_uint16 * 2) * 3),
         ("txtp", (C.c_uint16 * 16) * 13),
+        ("eob_bin_1d", C.c_uint16 * 11),
     ]
 
 
@@ -58,6 +59,7 @@ class CoefCosts(C.Structure):
         ("eob_bin", C.c_float * 11),
         ("dc_sign", (C.c_float * 2) * 3),
         ("txtp", (C.c_float * 16) * 13),
+        ("eob_bin_1d", C.c_float * 11),
     ]
 
 
@@ -68,6 +70,23 @@ class ChainParams(C.Structure):
         ("satd_scale", C.c_float), ("satd_bridge", C.c_float), ("use_skip_bits", C.c_int32),
         ("skip_bits", C.c_float * 2), ("vis_w", C.c_int32), ("vis_h", C.c_int32),
     ]
+
+
+class Split16Params(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("frame_w", "frame_h", "stride", "bd", "vis_w", "vis_h")] + [
+        (n, C.c_float) for n in ("trellis_lambda0", "rd_lambda", "band_tilt", "wsse_scale")] + [
+        (n, C.c_int32) for n in ("tx_search", "tx_guard_shift", "use_skip_bits")] + [
+        ("skip_bits", (C.c_float * 2) * 13)]
+
+
+assert C.sizeof(Split16Params) == 156
+
+SPLIT16_JOB_DTYPE = np.dtype([
+    ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"), ("reserved", "u1"),
+    ("a_coef", "u1", (4,)), ("l_coef", "u1", (4,)),
+])
+SPLIT16_RESULT_DTYPE = np.dtype([("sse", "<i8"), ("bits", "<f4"), ("tx_types", "u1", (4,))])
+assert SPLIT16_JOB_DTYPE.itemsize == 16 and SPLIT16_RESULT_DTYPE.itemsize == 16
 
 
 class DeblockFrameParams(C.Structure):
@@ -194,6 +213,12 @@ def _bind(lib):
         "mt_sse_recon_device": (C.c_int, [_P] + [C.c_int32] * 4 + [_P, _P, _P] + [C.c_int32] * 3 + [C.c_float, _P, _P]),
         "mt_sse_recon": (C.c_int, [_P] + [C.c_int32] * 5 + [_P, _P, _P] + [C.c_int32] * 3 + [C.c_float, _P]),
         "mt_mode_beam": (C.c_int, [_P, _P, C.POINTER(ChainParams), _P, C.c_int32, _P, _P]),
+        "mt_trellis_optimize_ctx_device": (C.c_int, [_P, _P, _P, C.c_int32, C.POINTER(Quant), _P, _P, C.c_float,
+                                                     C.c_float, _P]),
+        "mt_split16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                             C.c_int32, _P, _P, _P, _P]),
+        "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
+                                      _P, C.c_int32, _P, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
         "mt_screen_gate_device": (C.c_int, [_P, C.POINTER(ScreenGateParams), _P, C.POINTER(ScreenGateResult), _P]),
         "mt_screen_gate": (C.c_int, [_P, C.POINTER(ScreenGateParams), C.POINTER(ScreenGateResult)]),
@@ -234,7 +259,8 @@ EXPORTED_SYMBOLS = (
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
     "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate", "mt_mode_beam_device", "mt_mode_beam",
-    "mt_sse_recon_device", "mt_sse_recon",
+    "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
+    "mt_split16_luma",
 )
 
 

@@ -185,7 +185,15 @@ int mt_coef_costs_build(const mt_coef_cdfs* c, mt_coef_costs* o) {
     for (int s = 0; s < 2; s++) o->dc_sign[k][s] = cdf_cost(c->dc_sign[k], s);
   for (int m = 0; m < 13; m++)
     for (int s = 0; s < 16; s++) o->txtp[m][s] = cdf_cost(c->txtp[m], s);
+  for (int s = 0; s < 11; s++) o->eob_bin_1d[s] = cdf_cost(c->eob_bin_1d, s);
   return MT_OK;
+}
+
+extern "C++" {
+namespace mth {
+// scaled_trellis_lambda for the other translation units of the library.
+float scaled_trellis_lambda_host(float dc_q, float lambda0) { return scaled_trellis_lambda(dc_q, lambda0); }
+}  // namespace mth
 }
 
 static int check_chain(const mt_chain_params* prm, const mt_quant* q, int32_t n, int32_t tx_size = 8) {

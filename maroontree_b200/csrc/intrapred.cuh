@@ -81,31 +81,43 @@ __device__ __forceinline__ void upsample_edge(int32_t* e, int num_px, int32_t ma
   }
 }
 
+// Neighbour reads of the predictors: sample (x, y) of the reconstruction
+// plane.  Other readers (a plane with a trial-coded patch laid over it) supply
+// the same call.
+struct PlaneRead {
+  const uint16_t* __restrict__ p;
+  int stride;
+  __device__ __forceinline__ int32_t operator()(int x, int y) const { return p[(size_t)y * stride + x]; }
+};
+
 // DC predictor (src/intrapred.rs:1740-1789) for square power-of-two blocks.
-__device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, int stride, int ox, int oy, int n,
-                                              int log2n, int bd) {
+template <typename R>
+__device__ __forceinline__ int32_t dc_pred_sq_at(const R& rd, int ox, int oy, int n, int log2n, int bd) {
   const bool top = oy > 0, left = ox > 0;
   int32_t sum = 0;
   if (top)
-    for (int x = 0; x < n; x++) sum += rec[(size_t)(oy - 1) * stride + ox + x];
+    for (int x = 0; x < n; x++) sum += rd(ox + x, oy - 1);
   if (left)
-    for (int y = 0; y < n; y++) sum += rec[(size_t)(oy + y) * stride + ox - 1];
+    for (int y = 0; y < n; y++) sum += rd(ox - 1, oy + y);
   if (top && left) return (n + sum) >> (log2n + 1);
   if (top || left) return ((n >> 1) + sum) >> log2n;
   return 1 << (bd - 1);
 }
+__device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, int stride, int ox, int oy, int n,
+                                              int log2n, int bd) {
+  return dc_pred_sq_at(PlaneRead{rec, stride}, ox, oy, n, log2n, bd);
+}
 
-// Prediction of an N x N block (N = 4, 8 or 16) into out[N*N] (row-major).
-// `scratch` holds 3 * edge_cap<N>() words: the above and left edges and a
-// filter temporary.
-template <int N, typename O>
-__device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy, int mode,
-                           int delta, bool have_tr, bool have_bl, bool ft, int bd, O* __restrict__ out,
-                           int32_t* __restrict__ scratch) {
+// Prediction of an N x N block (N = 4, 8 or 16) into out[N*N] (row-major),
+// neighbours read through `rd`.  `scratch` holds 3 * edge_cap<N>() words: the
+// above and left edges and a filter temporary.
+template <int N, typename R, typename O>
+__device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int mode, int delta, bool have_tr,
+                              bool have_bl, bool ft, int bd, O* __restrict__ out, int32_t* __restrict__ scratch) {
   static_assert(N == 4 || N == 8 || N == 16, "square sizes 4, 8 and 16");
   constexpr int bw = N, bh = N, edge_len = 2 * N, cap = edge_cap<N>();
   if (mode == MT_DC_PRED) {
-    const int32_t d = dc_pred_sq(rec, stride, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : 4), bd);
+    const int32_t d = dc_pred_sq_at(rd, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : 4), bd);
     for (int i = 0; i < N * N; i++) out[i] = (O)(d);
     return;
   }
@@ -116,33 +128,33 @@ __device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw,
   int32_t* tmp = scratch + 2 * cap;
   const bool have_top = oy > 0, have_left = ox > 0;
   const int32_t base = 1 << (bd - 1);
-  const uint16_t* up = rec + (size_t)(oy - 1) * stride + ox;     // valid when have_top
-  const uint16_t* lf = rec + (size_t)oy * stride + ox - 1;       // valid when have_left
+  // above row at y = oy - 1 (valid when have_top), left column at x = ox - 1
+  // (valid when have_left)
   if (have_top) {
-    for (int i = 0; i < bw; i++) A[kEdgeOrigin + i] = up[i];
+    for (int i = 0; i < bw; i++) A[kEdgeOrigin + i] = rd(ox + i, oy - 1);
   } else {
-    const int32_t fill = have_left ? (int32_t)lf[0] : base - 1;
+    const int32_t fill = have_left ? rd(ox - 1, oy) : base - 1;
     for (int i = 0; i < edge_len; i++) A[kEdgeOrigin + i] = fill;
   }
   if (have_left) {
-    for (int j = 0; j < bh; j++) L[kEdgeOrigin + j] = lf[(size_t)j * stride];
+    for (int j = 0; j < bh; j++) L[kEdgeOrigin + j] = rd(ox - 1, oy + j);
   } else {
-    const int32_t fill = have_top ? (int32_t)up[0] : base + 1;
+    const int32_t fill = have_top ? rd(ox, oy - 1) : base + 1;
     for (int i = 0; i < edge_len; i++) L[kEdgeOrigin + i] = fill;
   }
   const int32_t corner =
-      have_left ? (have_top ? (int32_t)up[-1] : (int32_t)lf[0]) : (have_top ? (int32_t)up[0] : base);
+      have_left ? (have_top ? rd(ox - 1, oy - 1) : rd(ox - 1, oy)) : (have_top ? rd(ox, oy - 1) : base);
   A[kEdgeOrigin - 1] = corner;
   L[kEdgeOrigin - 1] = corner;
   if (have_top) {
     const int px_have = have_tr ? min(bw, max(fw - (ox + bw), 0)) : 0;
-    for (int i = 0; i < px_have; i++) A[kEdgeOrigin + bw + i] = up[bw + i];
+    for (int i = 0; i < px_have; i++) A[kEdgeOrigin + bw + i] = rd(ox + bw + i, oy - 1);
     const int32_t fill = A[kEdgeOrigin + bw + px_have - 1];
     for (int i = bw + px_have; i < edge_len; i++) A[kEdgeOrigin + i] = fill;
   }
   if (have_left) {
     const int px_have = have_bl ? min(bh, max(fh - (oy + bh), 0)) : 0;
-    for (int i = 0; i < px_have; i++) L[kEdgeOrigin + bh + i] = lf[(size_t)(bh + i) * stride];
+    for (int i = 0; i < px_have; i++) L[kEdgeOrigin + bh + i] = rd(ox - 1, oy + bh + i);
     const int32_t fill = L[kEdgeOrigin + bh + px_have - 1];
     for (int i = bh + px_have; i < edge_len; i++) L[kEdgeOrigin + i] = fill;
   }
@@ -253,6 +265,13 @@ __device__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw,
       for (int x = 0; x < bw; x++)
         out[y * bw + x] = (O)((sm_weight<N>(x) * l[y] + (256 - sm_weight<N>(x)) * right + 128) >> 8);
   }
+}
+
+template <int N, typename O>
+__device__ __forceinline__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy,
+                                           int mode, int delta, bool have_tr, bool have_bl, bool ft, int bd,
+                                           O* __restrict__ out, int32_t* __restrict__ scratch) {
+  predict_sq_at<N>(PlaneRead{rec, stride}, fw, fh, ox, oy, mode, delta, have_tr, have_bl, ft, bd, out, scratch);
 }
 
 template <typename O>

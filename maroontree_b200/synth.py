@@ -122,6 +122,8 @@ def synthetic_cdfs(seed, n_eob_bins=7, n_txtp=7):
     flat["eob_bin"] = _rand_cdf(rng, n_eob_bins, 11)
     flat["dc_sign"] = np.stack([_rand_cdf(rng, 2, 2) for _ in range(3)])
     flat["txtp"] = np.stack([_rand_cdf(rng, n_txtp, 16) for _ in range(13)])
+    # drawn last so the fields above keep their values for a given seed
+    flat["eob_bin_1d"] = _rand_cdf(rng, n_eob_bins, 11)
     for k, v in flat.items():
         arr = np.ctypeslib.as_array(getattr(c, k))
         arr[...] = v.reshape(arr.shape)
@@ -448,3 +450,32 @@ def screen_luma(w, h, seed, photo_frac=0.3, glyph_px=(8, 12), bd=8):
         lum = rgb_to_luma(generate_rgb(w, ph, int(seed) + 1)).astype(np.int32)
         img[h - ph:, :] = lum << (bd - 8)
     return np.clip(img, 0, top).astype(np.uint16)
+
+
+def coef_ctx_bytes(rng, n):
+    """Valid coefficient result context bytes (coef_res_ctx form): 0x40 for an
+    all-zero neighbour, else min(cumulative level, 63) | dc-sign marker."""
+    cul = rng.integers(1, 64, size=n)
+    dcb = rng.choice(np.array([0x00, 0x40, 0x80]), size=n)
+    zero = rng.random(n) < 0.3
+    return np.where(zero, 0x40, cul | dcb).astype(np.uint8)
+
+
+def split16_jobs(fw, fh, modes, deltas=(0,), seed=0):
+    """(16x16 block, mode, delta) jobs of split16_luma_try, mode-major (every
+    block for one (mode, delta), then the next), with deterministic neighbour
+    flags and random coefficient contexts per block."""
+    rng = np.random.default_rng(seed)
+    bys, bxs = np.meshgrid(np.arange(0, fh - 15, 16), np.arange(0, fw - 15, 16), indexing="ij")
+    px, py = bxs.ravel(), bys.ravel()
+    nb = len(px)
+    flags = np.array([block_flags(int(x), int(y), fw, fh, 16) for x, y in zip(px, py)], np.uint8)
+    flags |= np.where(rng.random(nb) < 0.5, abi.CAND_FILTER_TYPE, 0).astype(np.uint8)
+    a_coef = coef_ctx_bytes(rng, nb * 4).reshape(nb, 4)
+    l_coef = coef_ctx_bytes(rng, nb * 4).reshape(nb, 4)
+    rows = []
+    for m in modes:
+        for d in (deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)):
+            for b in range(nb):
+                rows.append((px[b], py[b], m, d, flags[b], 0, a_coef[b], l_coef[b]))
+    return np.array(rows, abi.SPLIT16_JOB_DTYPE)

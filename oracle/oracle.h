@@ -99,6 +99,24 @@ int or_aq_grid(const uint16_t* luma, const mt_aq_params* p, mt_aq_cell* cells, f
 /* screen_gate.rs screen_frame_gate; block64.rs hash8. */
 int or_screen_gate(const uint16_t* luma, const mt_screen_gate_params* p, mt_screen_gate_result* out);
 uint32_t or_hash8(const uint16_t* luma, int32_t w, int32_t x, int32_t y);
+/* trellis.rs:55 trellis_optimize_ctx (shipped tuning) of a square luma block. */
+void or_trellis_optimize_ctx(int32_t* cf, const float* tf, float dc_q, float ac_q, const uint16_t* scan, int32_t w,
+                             float lambda0, const mt_coef_cdfs* cdfs, int32_t dcs_ctx, const uint8_t* qm,
+                             int32_t qm_level, float band_tilt);
+/* rate.rs:149 real_block_bits_bounded with its exact abort bound. */
+float or_real_block_bits_bounded(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
+                                 const mt_coef_cdfs* cdfs, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
+                                 int32_t txtp, int32_t use_skip_bits, const float* skip_bits, float bound);
+/* lossy_state.rs:876 / :1010 luma_bits_1d_8x8 / _4x4 (V_DCT, H_DCT). */
+float or_luma_bits_1d(const int32_t* cf, int32_t w, int32_t vertical, const mt_coef_cdfs* cdfs, int32_t dcs,
+                      int32_t y_mode);
+/* lossy_state.rs:630 coef_res_ctx. */
+uint8_t or_coef_res_ctx(const int32_t* cf, const uint16_t* scan, int32_t n);
+/* partition_search.rs:4235 split16_luma_try over a batch of jobs. */
+int or_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                    const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
+                    mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out, int32_t threads);
+float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 

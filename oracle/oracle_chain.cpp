@@ -547,6 +547,11 @@ float scaled_trellis_lambda(float dc_q, float ac_q, float lambda0) {
   float aom = TRELLIS_AOM_CALIB * TRELLIS_CALIB * dc_q * dc_q * (3.3f + 0.0015f * dc_q);
   return aom * (lambda0 / TRELLIS_LAMBDA0);
 }
+}  // namespace
+extern "C" float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0) {
+  return scaled_trellis_lambda(dc_q, ac_q, lambda0);
+}
+namespace {
 
 // avx/trellis.rs:79-137 round_down_cost8/4 (FMA lanes) and :139-161
 // round_down_scalar_one; driver avx/trellis.rs:163-230.
@@ -1290,9 +1295,12 @@ extern "C" {
 // rate.rs:58-80 holds the same values).  txtp_mode < 0: no transform-type
 // symbol (chroma, TX_32X32).  Contexts: the square, w < h or w > h lo-context
 // offset table (src/tables.rs:354-360, :456-472).
-float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
-                            const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
-                            int32_t txtp, int32_t use_skip_bits, const float* skip_bits) {
+// `bound`: the exact abort of rate.rs:149-157 -- +inf once the running sum
+// passes it after the eob position (:208-210) or at every 16th interior index
+// (:234-236).
+float or_real_block_bits_bounded(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
+                                 const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
+                                 int32_t txtp, int32_t use_skip_bits, const float* skip_bits, float bound) {
   const int N = w * h;
   int eob = -1;
   for (int i = N - 1; i >= 0; i--)
@@ -1320,6 +1328,7 @@ float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, 
     bits += or_cdf_cost(c->eob_hi[eob_bin], (eob >> nbits) & 1);
     bits += (float)nbits;
   }
+  if (bits > bound) return INFINITY;
   static const uint8_t kOffWlh[25] = {0, 11, 11, 11, 11, 11, 11, 11, 11, 11, 6, 6, 21,
                                         21, 21, 6, 21, 21, 21, 21, 21, 21, 21, 21, 21};
   static const uint8_t kOffWgh[25] = {0, 16, 6, 6, 21, 16, 16, 6, 21, 21, 16, 16, 21,
@@ -1351,6 +1360,7 @@ float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, 
   }
   int ac_nonzero = 1;
   for (int i = eob - 1; i >= 1; i--) {
+    if ((i & 15) == 0 && bits > bound) return INFINITY;
     int rc = scan[i];
     int x = rc >> log2h, y = rc & (h - 1);
     uint32_t hi_mag;
@@ -1396,6 +1406,13 @@ float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, 
   return bits;
 }
 
+float or_real_block_bits_wh(const int32_t* cf, const uint16_t* scan, int32_t w, int32_t h,
+                            const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t txtp_mode,
+                            int32_t txtp, int32_t use_skip_bits, const float* skip_bits) {
+  return or_real_block_bits_bounded(cf, scan, w, h, c, skip_ctx, dcs_ctx, txtp_mode, txtp, use_skip_bits, skip_bits,
+                                    INFINITY);
+}
+
 // The square luma form the candidate chain prices (TX_32X32 codes no txtp).
 float or_real_block_bits(const int32_t* cf, const uint16_t* scan, int32_t n, int32_t cls,
                          const mt_coef_cdfs* c, int32_t skip_ctx, int32_t dcs_ctx, int32_t y_mode,
@@ -1430,6 +1447,7 @@ void or_coef_costs_build(const mt_coef_cdfs* c, mt_coef_costs* o) {
     for (int s = 0; s < 2; s++) o->dc_sign[k][s] = or_cdf_cost(c->dc_sign[k], s);
   for (int m = 0; m < 13; m++)
     for (int s = 0; s < 16; s++) o->txtp[m][s] = or_cdf_cost(c->txtp[m], s);
+  for (int s = 0; s < 11; s++) o->eob_bin_1d[s] = or_cdf_cost(c->eob_bin_1d, s);
 }
 
 // partition_search.rs:467-530 (8x8) / :620-673 (16x16): predict (DC via

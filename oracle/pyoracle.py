@@ -62,6 +62,14 @@ def load():
             "or_hash8": (C.c_uint32, [_P, C.c_int32, C.c_int32, C.c_int32]),
             "or_candidate_chain": (C.c_int, [_P, _P, C.POINTER(abi.ChainParams), C.POINTER(abi.Quant), _P,
                                              C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
+            "or_real_block_bits_bounded": (C.c_float, [_P, _P, C.c_int32, C.c_int32, C.POINTER(abi.CoefCdfs)] +
+                                           [C.c_int32] * 5 + [_P, C.c_float]),
+            "or_trellis_optimize_ctx": (None, [_P, _P, C.c_float, C.c_float, _P, C.c_int32, C.c_float,
+                                               C.POINTER(abi.CoefCdfs), C.c_int32, _P, C.c_int32, C.c_float]),
+            "or_luma_bits_1d": (C.c_float, [_P, C.c_int32, C.c_int32, C.POINTER(abi.CoefCdfs), C.c_int32, C.c_int32]),
+            "or_coef_res_ctx": (C.c_uint8, [_P, _P, C.c_int32]),
+            "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                          C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -317,3 +325,48 @@ def sse_recon(src, vis_w, vis_h, pos, pred, resid, w, h, scale=0.0, bd=8):
     assert load().or_sse_recon(p(src), src.shape[1], vis_w, vis_h, bd, p(pos), p(pred), p(resid), len(pos), w, h,
                                scale, p(out)) == 0
     return out
+
+
+def real_block_bits_bounded(cf, scan, w, h, cdfs, skip_ctx, dcs_ctx, txtp_mode, txtp, bound, skip_bits=None):
+    cf = np.ascontiguousarray(cf, np.int32)
+    scan = np.ascontiguousarray(scan, np.uint16)
+    sb = None if skip_bits is None else np.ascontiguousarray(skip_bits, np.float32)
+    return load().or_real_block_bits_bounded(p(cf), p(scan), w, h, C.byref(cdfs), skip_ctx, dcs_ctx, txtp_mode,
+                                             txtp, int(sb is not None), None if sb is None else p(sb), bound)
+
+
+def trellis_optimize_ctx(cf, tf, q, qm, cdfs, dcs_ctx, lambda0, band_tilt=0.0, n=8):
+    """trellis_optimize_ctx of one n x n luma block; returns the new levels."""
+    cf = np.array(cf, np.int32, copy=True)
+    tf = np.ascontiguousarray(tf, np.float32)
+    scan = default_scan(n)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    load().or_trellis_optimize_ctx(p(cf), p(tf), float(q.dc_q), float(q.ac_q), p(scan), n, lambda0, C.byref(cdfs),
+                                   dcs_ctx, p(qm), q.qm_level, band_tilt)
+    return cf
+
+
+def luma_bits_1d(cf, n, vertical, cdfs, dcs, y_mode):
+    cf = np.ascontiguousarray(cf, np.int32)
+    return load().or_luma_bits_1d(p(cf), n, int(vertical), C.byref(cdfs), dcs, y_mode)
+
+
+def coef_res_ctx(cf, n=8):
+    cf = np.ascontiguousarray(cf, np.int32)
+    scan = default_scan(n)
+    return load().or_coef_res_ctx(p(cf), p(scan), n * n)
+
+
+def split16_luma(src, recon, prm, q, qm, cdfs, jobs, threads=1):
+    """split16_luma_try of a batch of jobs: (results, cf n x 256, rec n x 16 x 16)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_RESULT_DTYPE)
+    cf = np.zeros((n, 256), np.int32)
+    rec = np.zeros((n, 16, 16), np.uint16)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    assert load().or_split16_luma(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
+                                  p(res), p(cf), p(rec), threads) == 0
+    return res, cf, rec
