@@ -13,7 +13,9 @@ coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
          step
 
 The line also carries ``level4`` / ``level16`` (the 4x4 and 16x16 levels of
-the same frame, device time and the oracle on the host cores) and
+the same frame, device time and the oracle on the host cores), ``split16``
+(the 16x16 leaf's TX_8X8 split trial over every block and mode, with and
+without the 4:4:4 type search) and
 ``frame_filters``: the frame-wide kernels of the same
 1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
 grid, the screen-content gate, deblocking of the three planes, CDEF tables +
@@ -282,6 +284,69 @@ def measure_small_level(dev, wl, n, reps=5, cpu=True):
     return out
 
 
+def measure_split16(dev, wl, search, reps=5, cpu=True):
+    """The 16x16 leaf's TX_8X8 split trial over the same 1080p luma: 8,040
+    blocks x 13 modes = 104,520 jobs of four quadrants each (DCT_DCT with
+    trellis_optimize_ctx, and with `search` the 4:4:4 type trials).  Device time
+    with CUDA events after an L2 flush; the oracle on all host cores over the
+    same jobs."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    q = mt.quant_new(QIDX, 8, QM_LEVEL)
+    qm = mt.qm_row(QM_LEVEL, 0, 8)
+    cdfs = synth.synthetic_cdfs(4)
+    costs = mt.coef_costs(cdfs)
+    jobs = synth.split16_jobs(W, H, MODES, seed=3)
+    n = len(jobs)
+    prm = mt.split16_params(W, H, trellis_lambda0=0.05, rd_lambda=wl["prm"].mode_lambda, band_tilt=1.9,
+                            tx_search=search, tx_guard_shift=5 if search else 4)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
+                                           t(jobs))
+    d_res = torch.empty(n * abi.SPLIT16_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    lib = mt.load()
+
+    def launch():
+        rc = lib.mt_split16_luma_device(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q),
+                                        d_qm.data_ptr(), d_costs.data_ptr(), d_jobs.data_ptr(), n,
+                                        d_res.data_ptr(), None, None, None)
+        assert rc == 0, rc
+
+    for _ in range(3):
+        launch()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(200_000)
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    step = float(np.median(ms))
+    what = (f"split16 leaf trial 1920x1080 luma, qindex 70, QM 6, 8,040 blocks x 13 modes, "
+            f"{'4:4:4 type search (7 types per quadrant)' if search else '4:2:0 (DCT_DCT per quadrant)'}")
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n,
+           "jobs_per_s": round(n / (step / 1e3)), "workload": what}
+    if cpu:
+        from oracle import pyoracle as po
+
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        po.split16_luma(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                               "sample": f"all {n} jobs ({dt:.2f} s)"}
+    return out
+
+
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -490,6 +555,8 @@ def run_ours(args):
     filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
     level4 = measure_small_level(dev, wl, 4, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
     level16 = measure_small_level(dev, wl, 16, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
+    split16 = {k: measure_split16(dev, wl, k == "search", cpu=world == 1 and not args.no_cpu)
+               for k in ("dct", "search")} if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -521,6 +588,7 @@ def run_ours(args):
         "frame_filters": filters,
         "level4": level4,
         "level16": level16,
+        "split16": split16,
         # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
         "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),

@@ -27,6 +27,10 @@ namespace {
 using namespace mtd;
 
 constexpr int kSplitThreads = 128;
+// Resident CTAs per SM each kernel is compiled for (measured on the 1080p
+// level: the DCT-only path is fastest at six, 85 registers a thread; the type
+// search, with far more live state, at three, no register cap).
+constexpr int kSplitMinBlocksDct = 6, kSplitMinBlocksSearch = 3;
 
 // Sample (x, y) of the reconstruction with the job's 16x16 trial patch at
 // (px, py) laid over it.
@@ -52,7 +56,8 @@ struct SplitArgs {
 // temporary (u[64, 128)).
 struct SplitWork {
   int32_t u[128];
-  int16_t pred[64], resid[64], cf[64], bcf[64], rr[64], brr[64];
+  int16_t pred[64], resid[64];
+  int16_t cfs[2][64], rrs[2][64];  // levels / inverse of the candidate and of the winner
   TrellisCtxScratch tr;
   uint8_t lv[160];
   uint8_t patch[256];
@@ -82,7 +87,10 @@ __device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate)
   return __fadd_rn((float)d, __fmul_rn(lam, rate));
 }
 
-__global__ void __launch_bounds__(kSplitThreads) split16_kernel(
+// SEARCH: the 4:4:4 type search is compiled in (a separate kernel keeps the
+// DCT-only path small for the instruction cache).
+template <bool SEARCH>
+__global__ void __launch_bounds__(kSplitThreads, SEARCH ? kSplitMinBlocksSearch : kSplitMinBlocksDct) split16_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, SplitArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_split16_job* __restrict__ jobs, int n, mt_split16_result* __restrict__ res, int32_t* __restrict__ cf_out,
@@ -159,68 +167,66 @@ __global__ void __launch_bounds__(kSplitThreads) split16_kernel(
     const float skip0 = p.use_skip_bits ? p.skip_bits[sk][1] : 0.0f;
     float* tf = reinterpret_cast<float*>(w.u);
     int32_t* tmp = w.u + 64;
-    // DCT_DCT with trellis_optimize_ctx, the reference every other type is
-    // gated against.
-    fwd8x8(w.resid, MT_TX_DCT_DCT, q, w.bcf, tf, tmp);
-    if (qm) apply_qm(w.bcf, tf, sQs, 64);
-    if (a.lambda > 0.0f) trellis_ctx8(w.bcf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
-    inv8x8(w.bcf, MT_TX_DCT_DCT, q, qm, w.brr, tmp);
-    eb.resid = w.brr;
-    const long long dct_sse = sse_recon_block(eb, p.wsse_scale);
-    float bbits = rate8_bounded(w.bcf, T, sk, ds, jb.mode, MT_TX_DCT_DCT, p.use_skip_bits != 0, skip1, skip0,
-                                __int_as_float(0x7f800000), w.lv);
-    long long bsse = dct_sse;
-    int btx = MT_TX_DCT_DCT;
-    if (p.tx_search) {
-      const long long guard = p.tx_guard_shift >= 63 ? 0 : (dct_sse >> p.tx_guard_shift);
-      // ADST_ADST, ADST_DCT, DCT_ADST (trellised), IDTX, V_DCT, H_DCT
-      const int kTypes[6] = {MT_TX_ADST_ADST, MT_TX_ADST_DCT, MT_TX_DCT_ADST, MT_TX_IDTX, MT_TX_V_DCT, MT_TX_H_DCT};
+    // The types in the reference's order: DCT_DCT (trellised; every other
+    // type is gated against it), then with SEARCH ADST_ADST, ADST_DCT,
+    // DCT_ADST (trellised), IDTX, V_DCT, H_DCT (not trellised).  One loop body
+    // keeps one copy of each stage in the code; the candidate and the current
+    // winner live in the two slots of cfs / rrs.
+    constexpr int kTypes = SEARCH ? 7 : 1;
+    constexpr uint32_t kTypeOrder = 0x3206541u;  // nibble k: the k-th type
+    int best = 0, btx = MT_TX_DCT_DCT;
+    long long bsse = 0, dct_sse = 0, guard = 0;
+    float bbits = 0.0f;
 #pragma unroll 1
-      for (int k = 0; k < 6; k++) {
-        const int t = kTypes[k];
-        fwd8x8(w.resid, t, q, w.cf, tf, tmp);
-        if (t >= MT_TX_ADST_ADST) {
-          if (qm) apply_qm(w.cf, tf, sQs, 64);
-          if (a.lambda > 0.0f) trellis_ctx8(w.cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
-        }
-        inv8x8(w.cf, t, q, qm, w.rr, tmp);
-        eb.resid = w.rr;
-        const long long asse = sse_recon_block(eb, p.wsse_scale);
-        const bool gate = t >= MT_TX_ADST_ADST ? asse <= dct_sse + guard : asse <= bsse;
-        if (!gate) continue;
-        const float best_rd = rd_cost_i64(bsse, rd_lam, bbits);
-        float abits;
-        if (t == MT_TX_V_DCT || t == MT_TX_H_DCT) {
-          abits = rate8_1d(w.cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
-        } else {
-          const float bound = __fdiv_rn(__fsub_rn(best_rd, (float)asse), rd_lam);
-          abits = rate8_bounded(w.cf, T, sk, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
-        }
-        if (rd_cost_i64(asse, rd_lam, abits) < best_rd) {
-#pragma unroll 8
-          for (int i = 0; i < 64; i++) {
-            w.bcf[i] = w.cf[i];
-            w.brr[i] = w.rr[i];
-          }
-          bsse = asse;
-          bbits = abits;
-          btx = t;
-        }
+    for (int k = 0; k < kTypes; k++) {
+      const int t = (int)((kTypeOrder >> (4 * k)) & 15u);
+      const int cur = k == 0 ? 0 : 1 - best;
+      int16_t* cf = w.cfs[cur];
+      int16_t* rr = w.rrs[cur];
+      fwd8x8(w.resid, t, q, cf, tf, tmp);
+      if (t == MT_TX_DCT_DCT || t >= MT_TX_ADST_ADST) {
+        if (qm) apply_qm(cf, tf, sQs, 64);
+        if (a.lambda > 0.0f) trellis_ctx8(cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
+      }
+      inv8x8(cf, t, q, qm, rr, tmp);
+      eb.resid = rr;
+      const long long asse = sse_recon_block(eb, p.wsse_scale);
+      if (k > 0 && !(t >= MT_TX_ADST_ADST ? asse <= dct_sse + guard : asse <= bsse)) continue;
+      const float best_rd = k == 0 ? 0.0f : rd_cost_i64(bsse, rd_lam, bbits);
+      float abits;
+      if (t == MT_TX_V_DCT || t == MT_TX_H_DCT) {
+        abits = rate8_1d(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
+      } else {
+        const float bound =
+            k == 0 ? __int_as_float(0x7f800000) : __fdiv_rn(__fsub_rn(best_rd, (float)asse), rd_lam);
+        abits = rate8_bounded(cf, T, sk, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
+      }
+      if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < best_rd) {
+        best = cur;
+        bsse = asse;
+        bbits = abits;
+        btx = t;
+      }
+      if (k == 0) {
+        dct_sse = asse;
+        guard = p.tx_guard_shift >= 63 ? 0 : (asse >> p.tx_guard_shift);
       }
     }
+    const int16_t* bcf = w.cfs[best];
+    const int16_t* brr = w.rrs[best];
     txtps |= (uint32_t)btx << (8 * qi);
     sse_sum += bsse;
     bits_sum = __fadd_rn(bits_sum, bbits);
-    const uint32_t res_ctx = coef_res_ctx8(w.bcf);
+    const uint32_t res_ctx = coef_res_ctx8(bcf);
     actx[ax] = actx[ax + 1] = res_ctx;
     lctx[ly] = lctx[ly + 1] = res_ctx;
 #pragma unroll 8
     for (int i = 0; i < 64; i++)
-      w.patch[(sy + (i >> 3)) * 16 + sx + (i & 7)] = (uint8_t)clampi((int32_t)w.pred[i] + w.brr[i], 0, maxv);
+      w.patch[(sy + (i >> 3)) * 16 + sx + (i & 7)] = (uint8_t)clampi((int32_t)w.pred[i] + brr[i], 0, maxv);
     if (cf_out) {
       int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * 256 + qi * 64);
 #pragma unroll
-      for (int i = 0; i < 16; i++) o[i] = make_int4(w.bcf[4 * i], w.bcf[4 * i + 1], w.bcf[4 * i + 2], w.bcf[4 * i + 3]);
+      for (int i = 0; i < 16; i++) o[i] = make_int4(bcf[4 * i], bcf[4 * i + 1], bcf[4 * i + 2], bcf[4 * i + 3]);
     }
   }
   r.sse = sse_sum;
@@ -311,9 +317,14 @@ int mt_split16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  split16_kernel<<<(n + kSplitThreads - 1) / kSplitThreads, kSplitThreads, 0,
-                   reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
-                                                             d_results, d_cf, d_rec);
+  const unsigned grid = (unsigned)((n + kSplitThreads - 1) / kSplitThreads);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (prm->tx_search)
+    split16_kernel<true><<<grid, kSplitThreads, 0, st>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n, d_results,
+                                                         d_cf, d_rec);
+  else
+    split16_kernel<false><<<grid, kSplitThreads, 0, st>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n, d_results,
+                                                          d_cf, d_rec);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
