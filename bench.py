@@ -15,7 +15,7 @@ coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
 The line also carries ``level4`` / ``level16`` (the 4x4 and 16x16 levels of
 the same frame, device time and the oracle on the host cores), ``split16``
 (the 16x16 leaf's TX_8X8 split trial over every block and mode, with and
-without the 4:4:4 type search) and
+without the 4:4:4 type search, and its depth-2 TX_4X4 trial) and
 ``frame_filters``: the frame-wide kernels of the same
 1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
 grid, the screen-content gate, deblocking of the three planes, CDEF tables +
@@ -284,12 +284,13 @@ def measure_small_level(dev, wl, n, reps=5, cpu=True):
     return out
 
 
-def measure_split16(dev, wl, search, reps=5, cpu=True):
+def measure_split16(dev, wl, search, reps=5, cpu=True, depth2=False):
     """The 16x16 leaf's TX_8X8 split trial over the same 1080p luma: 8,040
     blocks x 13 modes = 104,520 jobs of four quadrants each (DCT_DCT with
     trellis_optimize_ctx, and with `search` the 4:4:4 type trials).  Device time
     with CUDA events after an L2 flush; the oracle on all host cores over the
-    same jobs."""
+    same jobs.  depth2: the depth-2 trial instead (sixteen TX_4X4 per job, five
+    types each)."""
     import ctypes as C
 
     import torch
@@ -297,8 +298,8 @@ def measure_split16(dev, wl, search, reps=5, cpu=True):
     from maroontree_b200 import abi, synth
 
     q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 8)
-    cdfs = synth.synthetic_cdfs(4)
+    qm = mt.qm_row(QM_LEVEL, 0, 4 if depth2 else 8)
+    cdfs = synth.synthetic_cdfs(4, n_eob_bins=5) if depth2 else synth.synthetic_cdfs(4)
     costs = mt.coef_costs(cdfs)
     jobs = synth.split16_jobs(W, H, MODES, seed=3)
     n = len(jobs)
@@ -307,12 +308,14 @@ def measure_split16(dev, wl, search, reps=5, cpu=True):
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
                                            t(jobs))
-    d_res = torch.empty(n * abi.SPLIT16_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    rdt = abi.SPLIT16_D2_RESULT_DTYPE if depth2 else abi.SPLIT16_RESULT_DTYPE
+    d_res = torch.empty(n * rdt.itemsize, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lib = mt.load()
+    entry = lib.mt_split16_depth2_device if depth2 else lib.mt_split16_luma_device
 
     def launch():
-        rc = lib.mt_split16_luma_device(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q),
+        rc = entry(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q),
                                         d_qm.data_ptr(), d_costs.data_ptr(), d_jobs.data_ptr(), n,
                                         d_res.data_ptr(), None, None, None)
         assert rc == 0, rc
@@ -333,6 +336,9 @@ def measure_split16(dev, wl, search, reps=5, cpu=True):
     step = float(np.median(ms))
     what = (f"split16 leaf trial 1920x1080 luma, qindex 70, QM 6, 8,040 blocks x 13 modes, "
             f"{'4:4:4 type search (7 types per quadrant)' if search else '4:2:0 (DCT_DCT per quadrant)'}")
+    if depth2:
+        what = ("split16 depth-2 trial 1920x1080 luma, qindex 70, QM 6, 8,040 blocks x 13 modes, sixteen TX_4X4 "
+                "per job, 5 types each")
     out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n,
            "jobs_per_s": round(n / (step / 1e3)), "workload": what}
     if cpu:
@@ -340,7 +346,8 @@ def measure_split16(dev, wl, search, reps=5, cpu=True):
 
         threads = os.cpu_count() or 1
         t0 = time.perf_counter()
-        po.split16_luma(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, threads=threads)
+        (po.split16_depth2 if depth2 else po.split16_luma)(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs,
+                                                           threads=threads)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
                                "sample": f"all {n} jobs ({dt:.2f} s)"}
@@ -557,6 +564,8 @@ def run_ours(args):
     level16 = measure_small_level(dev, wl, 16, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
     split16 = {k: measure_split16(dev, wl, k == "search", cpu=world == 1 and not args.no_cpu)
                for k in ("dct", "search")} if rank == 0 else None
+    if split16 is not None:
+        split16["depth2"] = measure_split16(dev, wl, False, cpu=world == 1 and not args.no_cpu, depth2=True)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

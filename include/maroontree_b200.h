@@ -433,6 +433,40 @@ int mt_split16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const
                            const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                            const mt_split16_job* d_jobs, int32_t n, mt_split16_result* d_results, int32_t* d_cf,
                            uint16_t* d_rec, void* stream);
+/* ---- The 16x16 leaf's depth-2 trial: sixteen TX_4X4 ----
+ * split16_depth2_try (src/coder/partition_search.rs:4524-4642): the sixteen
+ * 4x4 transform blocks of each job in raster order, each predicted from the
+ * reconstruction with the blocks already trial-coded (edge flags: top row
+ * (py > 0 && (i < 3 || have_tr)), others (i < 3); left column
+ * (px > 0 && (j < 3 || have_bl)), others none), DCT_DCT with
+ * trellis_optimize, then ADST_ADST (trellised), IDTX, V_DCT, H_DCT, each taken
+ * when its sse_recon is within tx_guard of the DCT's and its rd cost is lower
+ * (ties keep the earlier type).  The 2-D types are priced by
+ * real_block_bits_bounded in txb_skip context 0 and the dc_sign context of the
+ * job's own above / left bytes for that column and row (the trial leaves the
+ * coefficient contexts alone), V / H by luma_bits_1d_4x4.  costs / qm_row:
+ * the TX_4X4 class slice and 4x4 row.  Of mt_split16_params, skip_bits[0]
+ * is the TX_4X4 class's context-0 pair (all_zero = 1, all_zero = 0) when
+ * use_skip_bits is set; tx_search and band_tilt are not used (this trial
+ * always tries its four types, with the plain trellis). */
+typedef struct mt_split16_d2_result {
+  int64_t sse;              /* sum of the sixteen sse_recon */
+  float bits;               /* sum of their coefficient bits, raster order */
+  uint8_t tx_types[16];     /* winning MT_TX_* per 4x4 in raster order; all 255 for a rejected job */
+  uint8_t reserved[4];
+} mt_split16_d2_result;
+
+/* d_cf (optional): n x 256 int32, 4x4 block t's levels at [t*16, t*16 + 16)
+ * column-major; d_rec (optional): n x 256 u16, the trial reconstruction
+ * row-major.  Rejected jobs as in mt_split16_luma_device. */
+int mt_split16_depth2_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                             const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                             const mt_split16_job* d_jobs, int32_t n, mt_split16_d2_result* d_results,
+                             int32_t* d_cf, uint16_t* d_rec, void* stream);
+int mt_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                      const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                      mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

@@ -219,6 +219,23 @@ def split16_luma(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want
     return res, cf, rec
 
 
+def split16_depth2(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
+    """``split16_depth2_try`` of a batch of jobs (``mt_split16_depth2``): sixteen TX_4X4
+    per job; qmrow / costs are the 4x4 row and the TX_4X4 slice.  Returns (results,
+    cf n x 256 or None, rec n x 16 x 16 or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_D2_RESULT_DTYPE)
+    cf = np.zeros((n, 256), np.int32) if want_cf else None
+    rec = np.zeros((n, 16, 16), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_split16_depth2(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                                    ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)), "mt_split16_depth2")
+    return res, cf, rec
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

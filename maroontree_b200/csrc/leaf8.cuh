@@ -14,6 +14,7 @@
 #pragma once
 #include <stdint.h>
 
+#include "chain4.cuh"
 #include "chain8.cuh"
 
 namespace mtd {
@@ -282,18 +283,25 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
   }
 }
 
-// real_block_bits_bounded of a TX_8X8 luma block in txb_skip context skip_ctx
-// and dc_sign context dcs with the tx-type symbol of (mode, tx): +inf once the
-// running sum passes `bound` after the eob position or at an interior scan
-// index divisible by 16.  lv: 80 bytes of scratch.
-template <typename C>
-__device__ float rate8_bounded(const C* __restrict__ cf, const mt_coef_costs& T, int skip_ctx, int dcs, int mode,
+// Default scan of a W x W block (scan index -> rc = x*W + y).
+template <int W>
+__device__ __forceinline__ int scan_rc(int i) {
+  return W == 4 ? kScan4[i] : kScan8[i];
+}
+
+// real_block_bits_bounded of a TX_WxW luma block (W = 4: class TX_4X4, 8:
+// TX_8X8) in txb_skip context skip_ctx and dc_sign context dcs with the
+// tx-type symbol of (mode, tx): +inf once the running sum passes `bound` after
+// the eob position or at an interior scan index divisible by 16.  lv:
+// (W + 2) * W bytes of scratch (the level map, stride W).
+template <int W, typename C>
+__device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, int skip_ctx, int dcs, int mode,
                                int tx, bool use_skip_bits, float skip1, float skip0, float bound,
                                uint8_t* __restrict__ lv) {
   const float kInf = __int_as_float(0x7f800000);
   int eob = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) {
+  for (int i = W * W - 1; i >= 0; i--)
+    if (cf[scan_rc<W>(i)] != 0) {
       eob = i;
       break;
     }
@@ -318,22 +326,23 @@ __device__ float rate8_bounded(const C* __restrict__ cf, const mt_coef_costs& T,
   if (bits > bound) return kInf;
   uint32_t* lv32 = reinterpret_cast<uint32_t*>(lv);
 #pragma unroll
-  for (int i = 0; i < 20; i++) lv32[i] = 0;
-  const int ctx_e = 1 + (eob > 8) + (eob > 16);
+  for (int i = 0; i < (W + 2) * W / 4; i++) lv32[i] = 0;
+  constexpr int L = W == 4 ? 2 : 3;
+  const int ctx_e = 1 + (eob > (W * W >> 3)) + (eob > (W * W >> 2));
   {
-    const int rc = kScan8[eob];
+    const int rc = scan_rc<W>(eob);
     const uint32_t m = uabs(cf[rc]);
     bits = __fadd_rn(bits, T.eob_base[ctx_e][min(m, 3u) - 1]);
-    if (m >= 3) bits = __fadd_rn(bits, hi_cost(T, m, ((rc >> 3) | (rc & 7)) > 1 ? 14 : 7));
+    if (m >= 3) bits = __fadd_rn(bits, hi_cost(T, m, ((rc >> L) | (rc & (W - 1))) > 1 ? 14 : 7));
     lv[rc] = (uint8_t)level_byte(m);
   }
   int ac_nz = 1;
   for (int i = eob - 1; i >= 1; i--) {
     if ((i & 15) == 0 && bits > bound) return kInf;
-    const int rc = kScan8[i];
-    const int x = rc >> 3, y = rc & 7;
-    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + 8] + lv[rc + 9];
-    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 16];
+    const int rc = scan_rc<W>(i);
+    const int x = rc >> L, y = rc & (W - 1);
+    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + W] + lv[rc + W + 1];
+    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 2 * W];
     const int ctx = kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
     const uint32_t m = uabs(cf[rc]);
     const uint32_t tok = min(m, 3u);
@@ -352,7 +361,7 @@ __device__ float rate8_bounded(const C* __restrict__ cf, const mt_coef_costs& T,
   const uint32_t dm = uabs(cf[0]);
   bits = __fadd_rn(bits, T.base_tok[0][min(dm, 3u)]);
   if (dm >= 3) {
-    const uint32_t mag = ((uint32_t)lv[1] + lv[8] + lv[9]) & 63;
+    const uint32_t mag = ((uint32_t)lv[1] + lv[W] + lv[W + 1]) & 63;
     bits = __fadd_rn(bits, hi_cost(T, dm, mag > 12 ? 6 : (int)((mag + 1) >> 1)));
   }
   if (cf[0] != 0) bits = __fadd_rn(bits, dcs_c[cf[0] < 0]);
@@ -360,16 +369,19 @@ __device__ float rate8_bounded(const C* __restrict__ cf, const mt_coef_costs& T,
   return bits;
 }
 
-// luma_bits_1d_8x8: the V_DCT (vertical) / H_DCT coefficient rate -- txb_skip
+// luma_bits_1d_8x8 / luma_bits_1d_4x4 (src/coder/lossy_state.rs:876-1143):
+// the V_DCT (vertical) / H_DCT coefficient rate of a W x W block -- txb_skip
 // context 0, tx-type symbol 2 / 3, the 1-D eob_pt CDF, the 1-D base contexts
-// (offset 26 + 0 / 5 / 10 by row) over (x, y) = (i & 7, i >> 3) of the scan
-// index, sign bits in place.  lv: 160 bytes of scratch (10 columns of 16).
-template <typename C>
-__device__ float rate8_1d(const C* __restrict__ cf, bool vertical, const mt_coef_costs& T, int dcs, int mode,
+// (offset 26 + 0 / 5 / 10 by row) over (x, y) = (i % W, i / W) of the scan
+// index, eob-coefficient context thresholds W*W/8 and W*W/4, sign bits in
+// place.  lv: 160 bytes of scratch (10 columns of 16).
+template <int W, typename C>
+__device__ float rate_1d(const C* __restrict__ cf, bool vertical, const mt_coef_costs& T, int dcs, int mode,
                           uint8_t* __restrict__ lv) {
-  auto pos_rc = [&](int i) -> int { return vertical ? ((i & 7) << 3) | (i >> 3) : i; };
+  constexpr int L = W == 4 ? 2 : 3;
+  auto pos_rc = [&](int i) -> int { return vertical ? ((i & (W - 1)) << L) | (i >> L) : i; };
   int eob = -1;
-  for (int i = 63; i >= 0; i--)
+  for (int i = W * W - 1; i >= 0; i--)
     if (cf[pos_rc(i)] != 0) {
       eob = i;
       break;
@@ -398,9 +410,9 @@ __device__ float rate8_1d(const C* __restrict__ cf, bool vertical, const mt_coef
     mag += (uint32_t)lv[x * 16 + y + 3] + lv[x * 16 + y + 4];
     return 26 + (y > 1 ? 10 : y * 5) + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
   };
-  const int ctx_e = 1 + (eob > 8) + (eob > 16);
+  const int ctx_e = 1 + (eob > (W * W >> 3)) + (eob > (W * W >> 2));
   {
-    const int x = eob & 7, y = eob >> 3;
+    const int x = eob & (W - 1), y = eob >> L;
     const uint32_t m = uabs(cf[pos_rc(eob)]);
     bits = __fadd_rn(bits, T.eob_base[ctx_e][min(m, 3u) - 1]);
     if (m >= 3) bits = __fadd_rn(bits, hi_cost(T, m, y != 0 ? 14 : 7));
@@ -408,7 +420,7 @@ __device__ float rate8_1d(const C* __restrict__ cf, bool vertical, const mt_coef
     lv[x * 16 + y] = (uint8_t)level_byte(m);
   }
   for (int i = eob - 1; i >= 1; i--) {
-    const int x = i & 7, y = i >> 3;
+    const int x = i & (W - 1), y = i >> L;
     const uint32_t m = uabs(cf[pos_rc(i)]);
     uint32_t hm;
     const int ctx = lo_ctx_1d(x, y, hm);

@@ -195,11 +195,11 @@ __global__ void __launch_bounds__(kSplitThreads, SEARCH ? kSplitMinBlocksSearch 
       const float best_rd = k == 0 ? 0.0f : rd_cost_i64(bsse, rd_lam, bbits);
       float abits;
       if (t == MT_TX_V_DCT || t == MT_TX_H_DCT) {
-        abits = rate8_1d(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
+        abits = rate_1d<8>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
       } else {
         const float bound =
             k == 0 ? __int_as_float(0x7f800000) : __fdiv_rn(__fsub_rn(best_rd, (float)asse), rd_lam);
-        abits = rate8_bounded(cf, T, sk, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
+        abits = rate_bounded<8>(cf, T, sk, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
       }
       if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < best_rd) {
         best = cur;
@@ -271,6 +271,161 @@ __global__ void __launch_bounds__(kSplitThreads) trellis_ctx_kernel(int32_t* __r
   trellis_ctx8(cf, tf, dc_q, ac_q, lambda, sT, dcs, has_qm ? sQm : nullptr, qm_full != 0, band_tilt, s);
 #pragma unroll 8
   for (int i = 0; i < 64; i++) levels[(size_t)b * 64 + i] = cf[i];
+}
+
+// split16_depth2_try: sixteen TX_4X4 per job in raster order, one thread per
+// job.  Per 4x4: prediction through PatchRead, DCT_DCT (+ QM, trellis), then
+// ADST_ADST (trellised), IDTX, V_DCT, H_DCT through one loop body, each kept
+// when its SSE is within tx_guard of the DCT's and its rd cost is lower.  The
+// rates use txb_skip context 0 and the dc_sign context of the job's own bytes
+// for the 4x4's column and row.
+struct Depth2Work {
+  int32_t u[128];  // prediction edges, then targets [0, 16) and the transform temporary [64, 128)
+  int16_t pred[16], resid[16];
+  int16_t cfs[2][16], rrs[2][16];
+  float suf[20];
+  uint8_t lv[160];
+  uint8_t patch[256];
+};
+
+__global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
+    const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, SplitArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_split16_job* __restrict__ jobs, int n, mt_split16_d2_result* __restrict__ res,
+    int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+  __shared__ mt_coef_costs sT;
+  __shared__ uint8_t sQm[16];
+  __shared__ float sQs[16];
+  __shared__ float sLut[64];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    if (threadIdx.x < 16) {
+      const int w = a.has_qm ? qm_row[threadIdx.x] : 32;
+      sQm[threadIdx.x] = (uint8_t)w;
+      sQs[threadIdx.x] = fwd_qm_scale(w);
+    }
+    if (threadIdx.x < 64) sLut[threadIdx.x] = kCoefRateLut[threadIdx.x];
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_quant& q = a.q;
+  const mt_coef_costs& T = sT;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const mt_split16_job jb = jobs[j];
+  mt_split16_d2_result& r = res[j];
+  if (!job_ok(jb, p.frame_w, p.frame_h)) {
+    r.sse = 0;
+    r.bits = 0.0f;
+    for (int i = 0; i < 4; i++) reinterpret_cast<uint32_t*>(r.tx_types)[i] = 0xffffffffu;
+    *reinterpret_cast<uint32_t*>(r.reserved) = 0;
+    if (cf_out)
+      for (int i = 0; i < 256; i++) cf_out[(size_t)j * 256 + i] = 0;
+    if (rec_out)
+      for (int i = 0; i < 256; i++) rec_out[(size_t)j * 256 + i] = 0;
+    return;
+  }
+  Depth2Work w;
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const bool ft = jb.flags & MT_CAND_FILTER_TYPE;
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float dcq = (float)q.dc_q, acq = (float)q.ac_q, rd_lam = p.rd_lambda;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  const float skip1 = p.use_skip_bits ? p.skip_bits[0][0] : 0.0f;
+  const float skip0 = p.use_skip_bits ? p.skip_bits[0][1] : 0.0f;
+  const PatchRead rd{rec, p.stride, jb.px, jb.py, w.patch};
+  long long sse_sum = 0;
+  float bits_sum = 0.0f;
+  uint8_t txtps[16];
+  for (int ti = 0; ti < 16; ti++) {
+    const int i = ti & 3, jr = ti >> 2, bx = jb.px + i * 4, by = jb.py + jr * 4;
+    const bool tr = jr == 0 ? (jb.py > 0 && (i < 3 || have_tr)) : i < 3;
+    const bool bl = i == 0 ? (jb.px > 0 && (jr < 3 || have_bl)) : false;
+    predict_sq_at<4>(rd, p.frame_w, p.frame_h, bx, by, jb.mode, jb.angle_delta, tr, bl, ft, p.bd, w.pred, w.u);
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      w.resid[k] = (int16_t)((int32_t)src[(size_t)(by + (k >> 2)) * p.stride + bx + (k & 3)] - w.pred[k]);
+    const int sgn = (int)(jb.a_coef[i] >> 6) + (int)(jb.l_coef[jr] >> 6) - 2;
+    const int ds = (sgn != 0) + (sgn > 0);
+    ErrBlock<int16_t, int16_t> eb;
+    eb.src = src + (size_t)by * p.stride + bx;
+    eb.stride = p.stride;
+    eb.pred = w.pred;
+    eb.w = 4;
+    eb.vw = min(max(vis_w - bx, 0), 4);
+    eb.vh = min(max(vis_h - by, 0), 4);
+    eb.maxv = maxv;
+    float* tf = reinterpret_cast<float*>(w.u);
+    int32_t* tmp = w.u + 64;
+    // DCT_DCT, ADST_ADST, IDTX, V_DCT, H_DCT (nibble k: the k-th type).
+    constexpr uint32_t kTypeOrder = 0x32041u;
+    int best = 0, btx = MT_TX_DCT_DCT;
+    long long bsse = 0, dct_sse = 0, guard = 0;
+    float bbits = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < 5; k++) {
+      const int t = (int)((kTypeOrder >> (4 * k)) & 15u);
+      const int cur = k == 0 ? 0 : 1 - best;
+      int16_t* cf = w.cfs[cur];
+      int16_t* rr = w.rrs[cur];
+      fwd4x4(w.resid, t, q, cf, tf, tmp);
+      if (t == MT_TX_DCT_DCT || t == MT_TX_ADST_ADST) {
+        if (qm) apply_qm(cf, tf, sQs, 16);
+        if (a.lambda > 0.0f) trellis4(cf, tf, w.suf, dcq, acq, a.lambda, sLut);
+      }
+      inv4x4(cf, t, q, qm, rr, tmp);
+      eb.resid = rr;
+      const long long asse = sse_recon_block(eb, p.wsse_scale);
+      if (k > 0 && !(asse <= dct_sse + guard)) continue;
+      const float best_rd = k == 0 ? 0.0f : rd_cost_i64(bsse, rd_lam, bbits);
+      float abits;
+      if (t == MT_TX_V_DCT || t == MT_TX_H_DCT) {
+        abits = rate_1d<4>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
+      } else {
+        const float bound =
+            k == 0 ? __int_as_float(0x7f800000) : __fdiv_rn(__fsub_rn(best_rd, (float)asse), rd_lam);
+        abits = rate_bounded<4>(cf, T, 0, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
+      }
+      if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < best_rd) {
+        best = cur;
+        bsse = asse;
+        bbits = abits;
+        btx = t;
+      }
+      if (k == 0) {
+        dct_sse = asse;
+        guard = p.tx_guard_shift >= 63 ? 0 : (asse >> p.tx_guard_shift);
+      }
+    }
+    const int16_t* bcf = w.cfs[best];
+    const int16_t* brr = w.rrs[best];
+    txtps[ti] = (uint8_t)btx;
+    sse_sum += bsse;
+    bits_sum = __fadd_rn(bits_sum, bbits);
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      w.patch[(jr * 4 + (k >> 2)) * 16 + i * 4 + (k & 3)] = (uint8_t)clampi((int32_t)w.pred[k] + brr[k], 0, maxv);
+    if (cf_out) {
+      int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * 256 + ti * 16);
+#pragma unroll
+      for (int k = 0; k < 4; k++) o[k] = make_int4(bcf[4 * k], bcf[4 * k + 1], bcf[4 * k + 2], bcf[4 * k + 3]);
+    }
+  }
+  r.sse = sse_sum;
+  r.bits = bits_sum;
+#pragma unroll
+  for (int k = 0; k < 16; k++) r.tx_types[k] = txtps[k];
+  *reinterpret_cast<uint32_t*>(r.reserved) = 0;
+  if (rec_out) {
+    uint2* o = reinterpret_cast<uint2*>(rec_out + (size_t)j * 256);
+#pragma unroll 4
+    for (int k = 0; k < 64; k++)
+      o[k] = make_uint2(w.patch[4 * k] | ((uint32_t)w.patch[4 * k + 1] << 16),
+                        w.patch[4 * k + 2] | ((uint32_t)w.patch[4 * k + 3] << 16));
+  }
 }
 
 int check_split(const mt_split16_params* p, const mt_quant* q, int32_t n) {
@@ -358,6 +513,70 @@ int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16
         cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr, rec_out ? reinterpret_cast<uint16_t*>(d + o_out) : nullptr,
         nullptr);
     if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_split16_result), cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 256 * 4, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && rec_out)
+      e = cudaMemcpy(rec_out, d + o_out, (size_t)n * 256 * 2, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int mt_split16_depth2_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                             const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                             const mt_split16_job* d_jobs, int32_t n, mt_split16_d2_result* d_results,
+                             int32_t* d_cf, uint16_t* d_rec, void* stream) {
+  int rc = check_split(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!d_src || !d_recon || !d_costs || !d_jobs || !d_results) return MT_ERR_INVALID_INPUT;
+  SplitArgs a;
+  a.p = *prm;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
+  depth2_kernel<<<(unsigned)((n + kSplitThreads - 1) / kSplitThreads), kSplitThreads, 0,
+                  reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
+                                                            d_results, d_cf, d_rec);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                      const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                      mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  int rc = check_split(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
+  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + 256;
+  const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
+  const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_split16_job));
+  const size_t o_cf = o_res + up256((size_t)n * sizeof(mt_split16_d2_result));
+  const size_t o_out = o_cf + (cf_out ? up256((size_t)n * 256 * 4) : 0);
+  const size_t total = o_out + (rec_out ? up256((size_t)n * 256 * 2) : 0);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_split16_job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = mt_split16_depth2_device(
+        reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant,
+        has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
+        reinterpret_cast<const mt_split16_job*>(d + o_jobs), n, reinterpret_cast<mt_split16_d2_result*>(d + o_res),
+        cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr, rec_out ? reinterpret_cast<uint16_t*>(d + o_out) : nullptr,
+        nullptr);
+    if (rc == MT_OK)
+      e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_split16_d2_result), cudaMemcpyDeviceToHost);
     if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 256 * 4, cudaMemcpyDeviceToHost);
     if (rc == MT_OK && e == cudaSuccess && rec_out)
       e = cudaMemcpy(rec_out, d + o_out, (size_t)n * 256 * 2, cudaMemcpyDeviceToHost);

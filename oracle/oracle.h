@@ -116,6 +116,10 @@ uint8_t or_coef_res_ctx(const int32_t* cf, const uint16_t* scan, int32_t n);
 int or_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                     const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
                     mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out, int32_t threads);
+/* partition_search.rs:4524 split16_depth2_try over a batch of jobs. */
+int or_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                      const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
+                      mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out, int32_t threads);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

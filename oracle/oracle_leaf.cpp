@@ -607,3 +607,149 @@ int or_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16
 }
 
 }  // extern "C"
+
+namespace {
+
+// One job of split16_depth2_try (partition_search.rs:4524-4642); `rec` as in
+// split16_one.
+void depth2_one(const uint16_t* src, uint16_t* rec, const mt_split16_params* p, const mt_quant* q, const uint8_t* qm,
+                const mt_coef_cdfs* cd, const mt_split16_job& jb, mt_split16_d2_result* r, int32_t* cf_out,
+                uint16_t* rec_out) {
+  const int px = jb.px, py = jb.py, stride = p->stride;
+  uint16_t saved[256], blk[256];
+  for (int y = 0; y < 16; y++)
+    for (int x = 0; x < 16; x++) saved[y * 16 + x] = rec[(size_t)(py + y) * stride + px + x];
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const int ft = (jb.flags & MT_CAND_FILTER_TYPE) != 0;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const uint16_t* scan = or_default_scan(4);
+  const float dcq = (float)q->dc_q, acq = (float)q->ac_q, rd_lam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  const float* skip = p->use_skip_bits ? p->skip_bits[0] : nullptr;
+  int64_t sse_sum = 0;
+  float bits_sum = 0.0f;
+  for (int j = 0; j < 4; j++)
+    for (int i = 0; i < 4; i++) {
+      const int ti = j * 4 + i, bx = px + i * 4, by = py + j * 4;
+      const bool tr = j == 0 ? (py > 0 && (i < 3 || have_tr)) : i < 3;
+      const bool bl = i == 0 ? (px > 0 && (j < 3 || have_bl)) : false;
+      int32_t pred[16];
+      if (jb.mode == MT_DC_PRED && jb.angle_delta == 0) {
+        const int32_t d = or_dc_pred(rec, stride, bx, by, 4, 4, p->bd);
+        for (int k = 0; k < 16; k++) pred[k] = d;
+      } else {
+        or_intra_predict(rec, stride, bx, by, 4, 4, jb.mode, jb.angle_delta, tr, bl, p->frame_w, p->frame_h, ft,
+                         p->bd, pred);
+      }
+      int32_t resid[16];
+      for (int y = 0; y < 4; y++)
+        for (int x = 0; x < 4; x++) resid[y * 4 + x] = (int32_t)src[(size_t)(by + y) * stride + bx + x] - pred[y * 4 + x];
+      // luma_bits' whole-block contexts (lossy_state.rs:495-513): txb_skip 0,
+      // dc_sign over this 4x4's own above / left bytes, left untouched by the trial.
+      int s = (jb.a_coef[i] >> 6) - 1 + (jb.l_coef[j] >> 6) - 1;
+      const int ds = (s != 0) + (s > 0);
+      const uint16_t pos[2] = {(uint16_t)bx, (uint16_t)by};
+      auto sse_of = [&](const int32_t* rr) -> int64_t {
+        int64_t d = 0;
+        or_sse_recon(src, stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, 4, 4, p->wsse_scale, &d);
+        return d;
+      };
+      int32_t bcf[16], brr[16];
+      float tf[16];
+      or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, 4, q, qm, bcf, tf);
+      or_trellis_optimize(bcf, tf, dcq, acq, scan, 16, p->trellis_lambda0);
+      or_inv_txfm_dequant(bcf, MT_TX_DCT_DCT, 4, q, qm, brr);
+      const int64_t dct_sse = sse_of(brr);
+      int64_t bsse = dct_sse;
+      float bbits = or_real_block_bits_bounded(bcf, scan, 4, 4, cd, 0, ds, jb.mode, MT_TX_DCT_DCT,
+                                               p->use_skip_bits, skip, INFINITY);
+      uint8_t btx = MT_TX_DCT_DCT;
+      const int64_t guard = p->tx_guard_shift >= 63 ? 0 : dct_sse >> p->tx_guard_shift;
+      static const int kTypes[4] = {MT_TX_ADST_ADST, MT_TX_IDTX, MT_TX_V_DCT, MT_TX_H_DCT};
+      for (int t : kTypes) {
+        int32_t acf[16], arr[16];
+        float atf[16];
+        or_fwd_txfm_quant(resid, t, 4, q, qm, acf, atf);
+        if (t == MT_TX_ADST_ADST) or_trellis_optimize(acf, atf, dcq, acq, scan, 16, p->trellis_lambda0);
+        or_inv_txfm_dequant(acf, t, 4, q, qm, arr);
+        const int64_t asse = sse_of(arr);
+        const float best_rd = rd_cost_i64(bsse, rd_lam, bbits);
+        const float bound = (best_rd - (float)asse) / rd_lam;
+        const float abits = (t == MT_TX_V_DCT || t == MT_TX_H_DCT)
+                                ? or_luma_bits_1d(acf, 4, t == MT_TX_V_DCT, cd, ds, jb.mode)
+                                : or_real_block_bits_bounded(acf, scan, 4, 4, cd, 0, ds, jb.mode, t, p->use_skip_bits,
+                                                             skip, bound);
+        if (asse <= dct_sse + guard && rd_cost_i64(asse, rd_lam, abits) < best_rd) {
+          memcpy(bcf, acf, sizeof(acf));
+          memcpy(brr, arr, sizeof(arr));
+          bsse = asse;
+          bbits = abits;
+          btx = (uint8_t)t;
+        }
+      }
+      r->tx_types[ti] = btx;
+      sse_sum += bsse;
+      bits_sum += bbits;
+      for (int y = 0; y < 4; y++)
+        for (int x = 0; x < 4; x++) {
+          const uint16_t v = (uint16_t)clampi(pred[y * 4 + x] + brr[y * 4 + x], 0, maxv);
+          rec[(size_t)(by + y) * stride + bx + x] = v;
+          blk[(j * 4 + y) * 16 + i * 4 + x] = v;
+        }
+      if (cf_out) memcpy(cf_out + ti * 16, bcf, sizeof(bcf));
+    }
+  for (int y = 0; y < 16; y++)
+    for (int x = 0; x < 16; x++) rec[(size_t)(py + y) * stride + px + x] = saved[y * 16 + x];
+  r->sse = sse_sum;
+  r->bits = bits_sum;
+  memset(r->reserved, 0, sizeof(r->reserved));
+  if (rec_out) memcpy(rec_out, blk, sizeof(blk));
+}
+
+}  // namespace
+
+extern "C" {
+
+// partition_search.rs:4524-4642 split16_depth2_try over a batch of jobs.
+int or_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                      const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
+                      mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out, int32_t threads) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const size_t plane = (size_t)p->stride * p->frame_h;
+  auto work = [&](int lo, int hi) {
+    std::vector<uint16_t> rec(recon, recon + plane);
+    for (int i = lo; i < hi; i++) {
+      const mt_split16_job& jb = jobs[i];
+      mt_split16_d2_result* r = &results[i];
+      const bool bad = jb.px + 16 > p->frame_w || jb.py + 16 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+                       jb.angle_delta < -3 || jb.angle_delta > 3 ||
+                       (jb.angle_delta != 0 && (jb.mode < MT_V_PRED || jb.mode > MT_D67_PRED));
+      if (bad) {
+        r->sse = 0;
+        r->bits = 0.0f;
+        memset(r->tx_types, 255, 16);
+        memset(r->reserved, 0, 4);
+        if (cf_out) memset(cf_out + (size_t)i * 256, 0, 256 * sizeof(int32_t));
+        if (rec_out) memset(rec_out + (size_t)i * 256, 0, 256 * sizeof(uint16_t));
+        continue;
+      }
+      depth2_one(src, rec.data(), p, q, qm, cdfs, jb, r, cf_out ? cf_out + (size_t)i * 256 : nullptr,
+                 rec_out ? rec_out + (size_t)i * 256 : nullptr);
+    }
+  };
+  if (threads <= 1 || n < 64) {
+    work(0, n);
+    return MT_OK;
+  }
+  std::vector<std::thread> pool;
+  const int per = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; t++) {
+    const int lo = t * per, hi = lo + per < n ? lo + per : n;
+    if (lo >= hi) break;
+    pool.emplace_back(work, lo, hi);
+  }
+  for (auto& th : pool) th.join();
+  return MT_OK;
+}
+
+}  // extern "C"

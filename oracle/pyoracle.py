@@ -68,6 +68,8 @@ def load():
                                                C.POINTER(abi.CoefCdfs), C.c_int32, _P, C.c_int32, C.c_float]),
             "or_luma_bits_1d": (C.c_float, [_P, C.c_int32, C.c_int32, C.POINTER(abi.CoefCdfs), C.c_int32, C.c_int32]),
             "or_coef_res_ctx": (C.c_uint8, [_P, _P, C.c_int32]),
+            "or_split16_depth2": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                            C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                           C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
@@ -369,4 +371,19 @@ def split16_luma(src, recon, prm, q, qm, cdfs, jobs, threads=1):
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
     assert load().or_split16_luma(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
                                   p(res), p(cf), p(rec), threads) == 0
+    return res, cf, rec
+
+
+def split16_depth2(src, recon, prm, q, qm, cdfs, jobs, threads=1):
+    """split16_depth2_try of a batch of jobs: (results, cf n x 256, rec n x 16 x 16)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_D2_RESULT_DTYPE)
+    cf = np.zeros((n, 256), np.int32)
+    rec = np.zeros((n, 16, 16), np.uint16)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    assert load().or_split16_depth2(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
+                                    p(res), p(cf), p(rec), threads) == 0
     return res, cf, rec

@@ -2,8 +2,9 @@
 reference's `Cdfs::new(0)` for the (TX_8X8 class, chroma) slice, the 4x8 / 8x4
 scans and lo-context offsets, and the golden rates of the reference's test
 `rectangular_orientations_use_their_own_contexts` (src/rate.rs:371-401); and
-cdfs_luma_tx8_qctx0.json: the (TX_8X8 class, luma) slice of the same snapshot
-with the 1-D eob_pt CDF and the intra tx-type CDFs.
+cdfs_luma_tx8_qctx0.json / cdfs_luma_tx4_qctx0.json: the (TX_8X8 / TX_4X4
+class, luma) slices of the same snapshot with the 1-D eob_pt CDF and the intra
+tx-type CDFs.
 
 Run in a checkout that has the reference next to it:
     python tests/golden/gen_rate_golden.py /path/to/maroontree
@@ -112,6 +113,25 @@ def main(ref):
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cdfs_luma_tx8_qctx0.json")
     with open(dst, "w") as f:
         json.dump(luma, f, indent=1)
+    print(dst)
+    # The luma TX_4X4 slice (class 0, plane 0) with its 1-D eob_pt CDF and the
+    # 4x4 intra tx-type CDFs.
+    luma4 = {
+        "source": "src/coef_q.rs, src/tables.rs (qctx 0, class 0 = TX_4X4, plane 0 = luma), "
+                  "src/coder/cdfs.rs:593-609 Cdfs::new field sources",
+        "skip": rust_array(q, "SKIP_TX4")[0],
+        "base_tok": rust_array(q, "BASE_TOK_TX4_LUMA_Q")[0],
+        "br_tok": rust_array(q, "BR_TOK_TX4_LUMA_Q")[0],
+        "eob_base": rust_array(q, "EOB_BASE_TX4_LUMA_Q")[0],
+        "eob_hi": rust_array(q, "EOB_HI_TX4_LUMA")[0],
+        "dc_sign": rust_array(q, "DC_SIGN_Q")[0][0],
+        "eob_bin": rust_array(q, "EOB_BIN_16_LUMA")[0],
+        "eob_bin_1d": rust_array(q, "EOB_BIN_16_LUMA_1D")[0],
+        "txtp": rust_array(t, "TXTP_INTRA1_TX4"),
+    }
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cdfs_luma_tx4_qctx0.json")
+    with open(dst, "w") as f:
+        json.dump(luma4, f, indent=1)
     print(dst)
 
 
