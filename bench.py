@@ -18,7 +18,8 @@ the same frame, device time and the oracle on the host cores), ``split16``
 without the 4:4:4 type search, and its depth-2 TX_4X4 trial) and
 ``frame_filters``: the frame-wide kernels of the same
 1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
-grid, the screen-content gate, deblocking of the three planes, CDEF tables +
+grid, the screen-content gate, the CfL alpha of every 8x8 chroma block,
+deblocking of the three planes, CDEF tables +
 strength search + apply) timed on the device with CUDA events after an L2
 flush, with their algorithmic bytes against the measured HBM copy bandwidth.
 
@@ -427,6 +428,17 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
         out[tag]["verdict"] = {"copy_stage": sres.copy_stage, "ibc_pays": sres.ibc_pays,
                                "few_colour": sres.few_colour}
         out[tag]["bound"] = "host synchronisation after the block pass (and after the copy stage)"
+    # chroma-from-luma alpha of every 8x8 chroma block (4:2:0), from the
+    # converted luma and chroma planes
+    cfl = np.zeros((pch // 8) * (pcw // 8), abi.CFL_BLOCK_DTYPE)
+    cys, cxs = np.meshgrid(np.arange(0, pch - 7, 8), np.arange(0, pcw - 7, 8), indexing="ij")
+    cfl["cx"], cfl["cy"], cfl["dc"] = cxs.ravel(), cys.ravel(), 128
+    d_cfl = torch.from_numpy(cfl.view(np.uint8).copy()).to(dev)
+    d_alpha = torch.empty(2 * len(cfl), dtype=torch.int8, device=dev)
+    ms = timed(lambda: lib.mt_cfl_alpha_device(y.data_ptr(), pw, cb.data_ptr(), cr.data_ptr(), pcw, 1, 1, 8, 8, 0, 0, 8,
+                                               d_cfl.data_ptr(), len(cfl), d_alpha.data_ptr(), None, None))
+    out["cfl_alpha"] = entry(ms, len(cfl) * 64 * (4 * 2 + 2 * 2), "4 luma + 2 chroma samples (2 B) per chroma sample")
+    out["cfl_alpha"]["blocks"] = len(cfl)
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)

@@ -472,6 +472,38 @@ int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
                     mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
 
+/* ---- Chroma-from-luma alpha search ----
+ * For n chroma blocks of cw x ch samples (4, 8, 16 or 32 each): the luma AC of
+ * the co-located reconstructed luma (cfl_ac_sub, src/intrapred.rs:1133-1172:
+ * each chroma position sums its 1, 2 or 4 luma samples, scaled to the <<3
+ * range, then the rounded block mean is removed; cfl_ac_444 is the unsampled
+ * case) and, for each of the U and V planes, the alpha of cfl_best_alpha
+ * (src/intrapred.rs:1211-1258): the analytic least-squares optimum
+ * round(64 num / den) clamped to [-16, 16], then the candidate in its +-3
+ * neighbourhood (inside [-16, 16]) with the lowest SSE of src - cfl_pred
+ * (dc + sign(alpha ac) ((|alpha ac| + 32) >> 6), clamped), first minimum; 0
+ * when the AC has no energy.  Only the displayed part of each block
+ * (vis_cw x vis_ch chroma samples of the plane; 0 = the whole block) is
+ * measured, as the reference's SrcBlock does.  sub_x / sub_y: the chroma
+ * subsampling (1, 1) 4:2:0, (1, 0) 4:2:2, (0, 0) 4:4:4.  dc: the DC_PRED value
+ * of the block in each plane, which the caller computes from its chroma
+ * reconstruction (dc_pred).  alpha: n x 2 (U, V); ac (optional): n x cw*ch
+ * int32 row-major, the AC the prediction uses. */
+typedef struct mt_cfl_block {
+  uint16_t cx, cy;          /* chroma sample position */
+  int16_t dc[2];            /* DC_PRED of the U and V planes at the block */
+} mt_cfl_block;
+int mt_cfl_alpha_device(const uint16_t* d_luma, int32_t luma_stride, const uint16_t* d_src_u, const uint16_t* d_src_v,
+                        int32_t chroma_stride, int32_t sub_x, int32_t sub_y, int32_t cw, int32_t ch, int32_t vis_cw,
+                        int32_t vis_ch, int32_t bd, const mt_cfl_block* d_blocks, int32_t n, int8_t* d_alpha,
+                        int32_t* d_ac, void* stream);
+/* Host-buffer form: luma is luma_stride x luma_h samples, the chroma planes
+ * chroma_stride x chroma_h. */
+int mt_cfl_alpha(const uint16_t* luma, int32_t luma_stride, int32_t luma_h, const uint16_t* src_u,
+                 const uint16_t* src_v, int32_t chroma_stride, int32_t chroma_h, int32_t sub_x, int32_t sub_y,
+                 int32_t cw, int32_t ch, int32_t vis_cw, int32_t vis_ch, int32_t bd, const mt_cfl_block* blocks,
+                 int32_t n, int8_t* alpha, int32_t* ac);
+
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and
  * f32 quantisation targets, with the QM applied as DctDispatch does. */

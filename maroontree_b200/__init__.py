@@ -236,6 +236,22 @@ def split16_depth2(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, wa
     return res, cf, rec
 
 
+def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8, want_ac=False):
+    """Chroma-from-luma alpha of n chroma blocks (``mt_cfl_alpha``): returns
+    (alpha n x 2 int8 for U and V, the AC n x ch x cw or None)."""
+    luma = np.ascontiguousarray(luma, np.uint16)
+    src_u = np.ascontiguousarray(src_u, np.uint16)
+    src_v = np.ascontiguousarray(src_v, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.CFL_BLOCK_DTYPE)
+    n = len(blocks)
+    alpha = np.zeros((n, 2), np.int8)
+    ac = np.zeros((n, ch, cw), np.int32) if want_ac else None
+    _check(load().mt_cfl_alpha(ptr(luma), luma.shape[1], luma.shape[0], ptr(src_u), ptr(src_v), src_u.shape[1],
+                               src_u.shape[0], sub_x, sub_y, cw, ch, vis[0], vis[1], bd, ptr(blocks), n, ptr(alpha),
+                               ptr(ac)), "mt_cfl_alpha")
+    return alpha, ac
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

@@ -90,6 +90,8 @@ SPLIT16_D2_RESULT_DTYPE = np.dtype([("sse", "<i8"), ("bits", "<f4"), ("tx_types"
                                     ("reserved", "u1", (4,))])
 assert SPLIT16_JOB_DTYPE.itemsize == 16 and SPLIT16_RESULT_DTYPE.itemsize == 16
 assert SPLIT16_D2_RESULT_DTYPE.itemsize == 32
+CFL_BLOCK_DTYPE = np.dtype([("cx", "<u2"), ("cy", "<u2"), ("dc", "<i2", (2,))])
+assert CFL_BLOCK_DTYPE.itemsize == 8
 
 
 class DeblockFrameParams(C.Structure):
@@ -224,6 +226,8 @@ def _bind(lib):
                                                C.c_int32, _P, _P, _P, _P]),
         "mt_split16_depth2": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P,
                                         C.POINTER(CoefCosts), _P, C.c_int32, _P, _P, _P]),
+        "mt_cfl_alpha_device": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P, _P]),
+        "mt_cfl_alpha": (C.c_int, [_P, C.c_int32, C.c_int32, _P, _P] + [C.c_int32] * 9 + [_P, C.c_int32, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                       _P, C.c_int32, _P, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
@@ -267,7 +271,7 @@ EXPORTED_SYMBOLS = (
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",
     "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate", "mt_mode_beam_device", "mt_mode_beam",
     "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
-    "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2",
+    "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
 )
 
 

@@ -120,6 +120,10 @@ int or_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16
 int or_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                       const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
                       mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out, int32_t threads);
+/* intrapred.rs:1112-1258 cfl_ac_sub / cfl_ac_444 + cfl_best_alpha over a batch of chroma blocks. */
+int or_cfl_alpha(const uint16_t* luma, int32_t luma_stride, const uint16_t* src_u, const uint16_t* src_v,
+                 int32_t chroma_stride, int32_t sub_x, int32_t sub_y, int32_t cw, int32_t ch, int32_t vis_cw,
+                 int32_t vis_ch, int32_t bd, const mt_cfl_block* blocks, int32_t n, int8_t* alpha, int32_t* ac_out);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

@@ -70,6 +70,7 @@ def load():
             "or_coef_res_ctx": (C.c_uint8, [_P, _P, C.c_int32]),
             "or_split16_depth2": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                             C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
+            "or_cfl_alpha": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                           C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
@@ -387,3 +388,17 @@ def split16_depth2(src, recon, prm, q, qm, cdfs, jobs, threads=1):
     assert load().or_split16_depth2(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
                                     p(res), p(cf), p(rec), threads) == 0
     return res, cf, rec
+
+
+def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8):
+    """cfl_ac + cfl_best_alpha of n chroma blocks: (alpha n x 2, ac n x ch x cw)."""
+    luma = np.ascontiguousarray(luma, np.uint16)
+    src_u = np.ascontiguousarray(src_u, np.uint16)
+    src_v = np.ascontiguousarray(src_v, np.uint16)
+    blocks = np.ascontiguousarray(blocks, abi.CFL_BLOCK_DTYPE)
+    n = len(blocks)
+    alpha = np.zeros((n, 2), np.int8)
+    ac = np.zeros((n, ch, cw), np.int32)
+    assert load().or_cfl_alpha(p(luma), luma.shape[1], p(src_u), p(src_v), src_u.shape[1], sub_x, sub_y, cw, ch,
+                               vis[0], vis[1], bd, p(blocks), n, p(alpha), p(ac)) == 0
+    return alpha, ac
