@@ -439,6 +439,19 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
                                                d_cfl.data_ptr(), len(cfl), d_alpha.data_ptr(), None, None))
     out["cfl_alpha"] = entry(ms, len(cfl) * 64 * (4 * 2 + 2 * 2), "4 luma + 2 chroma samples (2 B) per chroma sample")
     out["cfl_alpha"]["blocks"] = len(cfl)
+    # the filter-intra shortlist of every 16x16 luma block (five modes each)
+    fys, fxs = np.meshgrid(np.arange(0, H - 15, 16), np.arange(0, W - 15, 16), indexing="ij")
+    fpos = np.stack([fxs.ravel(), fys.ravel()], axis=1).astype(np.uint16)
+    d_fpos = torch.from_numpy(fpos.view(np.uint8).copy()).to(dev)
+    d_fsrc, d_frec = t16(wl["src"]), t16(wl["rec"])
+    d_fsc = torch.empty(len(fpos) * 5 * 8, dtype=torch.uint8, device=dev)
+    d_fmd = torch.empty(len(fpos) * 5, dtype=torch.uint8, device=dev)
+    ms = timed(lambda: lib.mt_filter_intra_beam_device(d_fsrc.data_ptr(), d_frec.data_ptr(), W, W, H, 0, 0, 8, 16, 16,
+                                                       d_fpos.data_ptr(), len(fpos), d_fsc.data_ptr(),
+                                                       d_fmd.data_ptr(), None, None))
+    out["filter_intra_beam16"] = entry(ms, len(fpos) * 5 * (256 * 2 + 33 * 2),
+                                       "per (block, mode): the 16x16 source (2 B / sample) and the 33 edge samples")
+    out["filter_intra_beam16"]["blocks"] = len(fpos)
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)

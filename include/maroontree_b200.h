@@ -472,6 +472,28 @@ int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
                     mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
 
+/* ---- Filter-intra shortlist ----
+ * rank_filter_intra_modes (src/coder/superblock.rs:356-400) over n luma blocks
+ * of w x h (4, 8, 16 or 32 each) at pos[2b], pos[2b+1]: each of the five
+ * filter-intra modes (DC, V, H, D157, PAETH in that order) predicted by the
+ * recursive 4x2-cell filter (filter_intra_predict, src/intrapred.rs:473-565:
+ * the above row of w samples, the left column of h samples and the corner,
+ * with the reference's fills when an edge is missing; no above-right), scored
+ * by satd_sad_proxy (samples past the displayed window count as the
+ * prediction), and sorted by (score, mode order); the caller keeps the first
+ * `budget`.  scores / modes: n x MT_FILTER_INTRA_MODES ascending; preds
+ * (optional): n x 5 x w*h int16, row-major, in mode order.  A block outside
+ * the frame gets scores of all ones and modes 255. */
+#define MT_FILTER_INTRA_MODES 5
+int mt_filter_intra_beam_device(const uint16_t* d_src, const uint16_t* d_recon, int32_t stride, int32_t frame_w,
+                                int32_t frame_h, int32_t vis_w, int32_t vis_h, int32_t bd, int32_t w, int32_t h,
+                                const uint16_t* d_pos, int32_t n, uint64_t* d_scores, uint8_t* d_modes,
+                                int16_t* d_preds, void* stream);
+/* Host-buffer form (planes stride x frame_h; scores and preds may be NULL). */
+int mt_filter_intra_beam(const uint16_t* src, const uint16_t* recon, int32_t stride, int32_t frame_w, int32_t frame_h,
+                         int32_t vis_w, int32_t vis_h, int32_t bd, int32_t w, int32_t h, const uint16_t* pos,
+                         int32_t n, uint64_t* scores, uint8_t* modes, int16_t* preds);
+
 /* ---- Chroma-from-luma alpha search ----
  * For n chroma blocks of cw x ch samples (4, 8, 16 or 32 each): the luma AC of
  * the co-located reconstructed luma (cfl_ac_sub, src/intrapred.rs:1133-1172:

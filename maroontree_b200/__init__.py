@@ -236,6 +236,22 @@ def split16_depth2(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, wa
     return res, cf, rec
 
 
+def filter_intra_beam(src, recon, w, h, pos, vis=(0, 0), bd=8, want_preds=False):
+    """The filter-intra shortlist ranking (``mt_filter_intra_beam``): (scores, modes),
+    each n x 5 ascending, and the five predictions n x 5 x h x w or None."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    scores = np.zeros((n, 5), np.uint64)
+    modes = np.zeros((n, 5), np.uint8)
+    preds = np.zeros((n, 5, h, w), np.int16) if want_preds else None
+    _check(load().mt_filter_intra_beam(ptr(src), ptr(recon), src.shape[1], src.shape[1], src.shape[0], vis[0], vis[1],
+                                       bd, w, h, ptr(pos), n, ptr(scores), ptr(modes), ptr(preds)),
+           "mt_filter_intra_beam")
+    return scores, modes, preds
+
+
 def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8, want_ac=False):
     """Chroma-from-luma alpha of n chroma blocks (``mt_cfl_alpha``): returns
     (alpha n x 2 int8 for U and V, the AC n x ch x cw or None)."""

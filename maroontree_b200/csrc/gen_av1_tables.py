@@ -17,6 +17,7 @@ Source locations (reference paths):
   src/tables.rs     SCAN_8X8, SCAN_4X4, LO_CTX_OFF, LO_CTX_OFF_WLH, LO_CTX_OFF_WGH
   src/qm_tables.rs  AV1_IQM  ([15][2][3344] u8)
   src/dct.rs        ADST16_FWD_Q12 ([16][16] i16, the forward 16-point ADST in Q12)
+  src/tables.rs     INTRA_FILTER_TAPS ([5][8][7] i8, the recursive filter-intra taps)
 """
 import os
 import re
@@ -37,6 +38,7 @@ TABLES = [
     ("src/tables.rs", "LO_CTX_OFF_WGH", "MT_LO_CTX_OFF_WGH", "uint8_t"),
     ("src/qm_tables.rs", "AV1_IQM", "MT_AV1_IQM", "uint8_t"),
     ("src/dct.rs", "ADST16_FWD_Q12", "MT_ADST16_FWD_Q12", "int16_t"),
+    ("src/tables.rs", "INTRA_FILTER_TAPS", "MT_INTRA_FILTER_TAPS", "int8_t"),
 ]
 
 
@@ -82,7 +84,7 @@ def main():
         for k in range(0, len(nums), 24):
             lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
         lines.append("};")
-        if "QLOOKUP" in cname or cname in ("MT_SCAN_16X16", "MT_ADST16_FWD_Q12"):  # initialiser lists for device copies
+        if "QLOOKUP" in cname or cname in ("MT_SCAN_16X16", "MT_ADST16_FWD_Q12", "MT_INTRA_FILTER_TAPS"):  # initialiser lists for device copies
             lines.append(f"#define {cname}_LIST " + ",".join(str(v) for v in nums))
         lines.append("")
     open(out, "w").write("\n".join(lines))

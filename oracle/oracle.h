@@ -124,6 +124,12 @@ int or_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split
 int or_cfl_alpha(const uint16_t* luma, int32_t luma_stride, const uint16_t* src_u, const uint16_t* src_v,
                  int32_t chroma_stride, int32_t sub_x, int32_t sub_y, int32_t cw, int32_t ch, int32_t vis_cw,
                  int32_t vis_ch, int32_t bd, const mt_cfl_block* blocks, int32_t n, int8_t* alpha, int32_t* ac_out);
+/* intrapred.rs:473-565 filter_intra_predict; superblock.rs:356-400 rank_filter_intra_modes. */
+void or_filter_intra_predict(const uint16_t* recon, int32_t stride, int32_t ox, int32_t oy, int32_t w, int32_t h,
+                             int32_t mode, int32_t bd, int32_t* out);
+int or_filter_intra_beam(const uint16_t* src, const uint16_t* recon, int32_t stride, int32_t frame_w, int32_t frame_h,
+                         int32_t vis_w, int32_t vis_h, int32_t bd, int32_t w, int32_t h, const uint16_t* pos,
+                         int32_t n, uint64_t* scores, uint8_t* modes, int16_t* preds);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

@@ -70,6 +70,8 @@ def load():
             "or_coef_res_ctx": (C.c_uint8, [_P, _P, C.c_int32]),
             "or_split16_depth2": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                             C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
+            "or_filter_intra_predict": (None, [_P] + [C.c_int32] * 7 + [_P]),
+            "or_filter_intra_beam": (C.c_int, [_P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P, _P]),
             "or_cfl_alpha": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                           C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
@@ -402,3 +404,24 @@ def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8
     assert load().or_cfl_alpha(p(luma), luma.shape[1], p(src_u), p(src_v), src_u.shape[1], sub_x, sub_y, cw, ch,
                                vis[0], vis[1], bd, p(blocks), n, p(alpha), p(ac)) == 0
     return alpha, ac
+
+
+def filter_intra_predict(recon, ox, oy, w, h, mode, bd=8):
+    recon = np.ascontiguousarray(recon, np.uint16)
+    out = np.zeros((h, w), np.int32)
+    load().or_filter_intra_predict(p(recon), recon.shape[1], ox, oy, w, h, mode, bd, p(out))
+    return out
+
+
+def filter_intra_beam(src, recon, w, h, pos, vis=(0, 0), bd=8):
+    """rank_filter_intra_modes of n blocks: (scores n x 5, modes n x 5, preds n x 5 x h x w)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    scores = np.zeros((n, 5), np.uint64)
+    modes = np.zeros((n, 5), np.uint8)
+    preds = np.zeros((n, 5, h, w), np.int16)
+    assert load().or_filter_intra_beam(p(src), p(recon), src.shape[1], src.shape[1], src.shape[0], vis[0], vis[1], bd,
+                                       w, h, p(pos), n, p(scores), p(modes), p(preds)) == 0
+    return scores, modes, preds
