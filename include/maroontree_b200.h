@@ -467,6 +467,25 @@ int mt_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split
                       const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
                       mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out);
 
+/* ---- The 8x8 leaf's TX_4X4 split trial ----
+ * split4tx_try (src/coder/block8.rs:157-286): the four 4x4 transform blocks of
+ * an 8x8 job in raster order (edge flags (py > 0, px > 0), (have_tr, 0),
+ * (1, have_bl), (0, 0)), DCT_DCT with trellis_optimize, then ADST_ADST
+ * (trellised) and IDTX, each taken when its sse_recon is within tx_guard of
+ * the DCT's and its rd cost is lower, priced like the depth-2 trial
+ * (real_block_bits_bounded in txb_skip context 0 and the dc_sign context of
+ * the job's bytes a_coef[i] / l_coef[j], i, j in 0..1).  The job's px, py
+ * address an 8x8 block; costs / qm_row: the TX_4X4 slice and 4x4 row; the
+ * params as for mt_split16_depth2.  d_cf (optional): n x 64 int32, 4x4 block
+ * q's levels at [q*16, q*16 + 16); d_rec (optional): n x 64 u16. */
+int mt_split4tx_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                       const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                       const mt_split16_job* d_jobs, int32_t n, mt_split16_result* d_results, int32_t* d_cf,
+                       uint16_t* d_rec, void* stream);
+int mt_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

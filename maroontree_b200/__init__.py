@@ -268,6 +268,22 @@ def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8
     return alpha, ac
 
 
+def split4tx(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
+    """The 8x8 leaf's ``split4tx_try`` (``mt_split4tx``): four TX_4X4 per 8x8 job;
+    returns (results, cf n x 64 or None, rec n x 8 x 8 or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_RESULT_DTYPE)
+    cf = np.zeros((n, 64), np.int32) if want_cf else None
+    rec = np.zeros((n, 8, 8), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_split4tx(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs), ptr(jobs),
+                              n, ptr(res), ptr(cf), ptr(rec)), "mt_split4tx")
+    return res, cf, rec
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

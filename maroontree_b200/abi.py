@@ -230,6 +230,10 @@ def _bind(lib):
         "mt_filter_intra_beam": (C.c_int, [_P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P, _P]),
         "mt_cfl_alpha_device": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P, _P]),
         "mt_cfl_alpha": (C.c_int, [_P, C.c_int32, C.c_int32, _P, _P] + [C.c_int32] * 9 + [_P, C.c_int32, _P, _P]),
+        "mt_split4tx_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                         C.c_int32, _P, _P, _P, _P]),
+        "mt_split4tx": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                                  C.c_int32, _P, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                       _P, C.c_int32, _P, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
@@ -274,7 +278,7 @@ EXPORTED_SYMBOLS = (
     "mt_screen_gate_scratch_bytes", "mt_screen_gate_device", "mt_screen_gate", "mt_mode_beam_device", "mt_mode_beam",
     "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
-    "mt_filter_intra_beam_device", "mt_filter_intra_beam",
+    "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
 )
 
 

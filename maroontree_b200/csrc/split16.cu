@@ -34,15 +34,18 @@ constexpr int kSplitMinBlocksDct = 6, kSplitMinBlocksSearch = 3;
 
 // Sample (x, y) of the reconstruction with the job's 16x16 trial patch at
 // (px, py) laid over it.
-struct PatchRead {
+template <int S>
+struct PatchReadS {
   const uint16_t* __restrict__ plane;
   int stride, px, py;
-  const uint8_t* patch;
+  const uint8_t* patch;  // S x S, row-major
   __device__ __forceinline__ int32_t operator()(int x, int y) const {
     const unsigned dx = (unsigned)(x - px), dy = (unsigned)(y - py);
-    return (dx < 16u && dy < 16u) ? (int32_t)patch[dy * 16 + dx] : (int32_t)plane[(size_t)y * stride + x];
+    return (dx < (unsigned)S && dy < (unsigned)S) ? (int32_t)patch[dy * S + dx]
+                                                  : (int32_t)plane[(size_t)y * stride + x];
   }
 };
+using PatchRead = PatchReadS<16>;
 
 struct SplitArgs {
   mt_split16_params p;
@@ -63,8 +66,9 @@ struct SplitWork {
   uint8_t patch[256];
 };
 
+template <int B = 16>
 __device__ __forceinline__ bool job_ok(const mt_split16_job& jb, int fw, int fh) {
-  if (jb.px + 16 > fw || jb.py + 16 > fh || jb.mode > MT_PAETH_PRED) return false;
+  if (jb.px + B > fw || jb.py + B > fh || jb.mode > MT_PAETH_PRED) return false;
   if (jb.angle_delta < -3 || jb.angle_delta > 3) return false;
   return jb.angle_delta == 0 || (jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED);
 }
@@ -273,12 +277,16 @@ __global__ void __launch_bounds__(kSplitThreads) trellis_ctx_kernel(int32_t* __r
   for (int i = 0; i < 64; i++) levels[(size_t)b * 64 + i] = cf[i];
 }
 
-// split16_depth2_try: sixteen TX_4X4 per job in raster order, one thread per
-// job.  Per 4x4: prediction through PatchRead, DCT_DCT (+ QM, trellis), then
-// ADST_ADST (trellised), IDTX, V_DCT, H_DCT through one loop body, each kept
-// when its SSE is within tx_guard of the DCT's and its rd cost is lower.  The
-// rates use txb_skip context 0 and the dc_sign context of the job's own bytes
-// for the 4x4's column and row.
+// The TX_4X4 split trials, one thread per job, the 4x4 blocks in raster
+// order: B = 16 is split16_depth2_try (sixteen 4x4, DCT_DCT, ADST_ADST, IDTX,
+// V_DCT, H_DCT), B = 8 is the 8x8 leaf's split4tx_try
+// (src/coder/block8.rs:157-286: four 4x4, DCT_DCT, ADST_ADST, IDTX, with the
+// quadrant edge flags (py > 0, px > 0), (have_tr, 0), (1, have_bl), (0, 0)).
+// Per 4x4: prediction through the B x B patch reader, DCT_DCT (+ QM,
+// trellis), then the other types through one loop body (ADST_ADST trellised),
+// each kept when its SSE is within tx_guard of the DCT's and its rd cost is
+// lower.  The rates use txb_skip context 0 and the dc_sign context of the job's
+// own bytes for the 4x4's column and row.
 struct Depth2Work {
   int32_t u[128];  // prediction edges, then targets [0, 16) and the transform temporary [64, 128)
   int16_t pred[16], resid[16];
@@ -288,11 +296,19 @@ struct Depth2Work {
   uint8_t patch[256];
 };
 
-__global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
+// tx_types of the B = 16 and B = 8 results.
+__device__ __forceinline__ uint8_t* result_types(mt_split16_d2_result& r) { return r.tx_types; }
+__device__ __forceinline__ uint8_t* result_types(mt_split16_result& r) { return r.tx_types; }
+__device__ __forceinline__ void clear_reserved(mt_split16_d2_result& r) { *reinterpret_cast<uint32_t*>(r.reserved) = 0; }
+__device__ __forceinline__ void clear_reserved(mt_split16_result&) {}
+
+template <int B, typename R>
+__global__ void __launch_bounds__(kSplitThreads) tx4_split_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, SplitArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
-    const mt_split16_job* __restrict__ jobs, int n, mt_split16_d2_result* __restrict__ res,
+    const mt_split16_job* __restrict__ jobs, int n, R* __restrict__ res,
     int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+  constexpr int G = B / 4, NB = G * G;  // 4x4 blocks per row / per job
   __shared__ mt_coef_costs sT;
   __shared__ uint8_t sQm[16];
   __shared__ float sQs[16];
@@ -316,16 +332,16 @@ __global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
   const mt_coef_costs& T = sT;
   const uint8_t* qm = a.has_qm ? sQm : nullptr;
   const mt_split16_job jb = jobs[j];
-  mt_split16_d2_result& r = res[j];
-  if (!job_ok(jb, p.frame_w, p.frame_h)) {
+  R& r = res[j];
+  if (!job_ok<B>(jb, p.frame_w, p.frame_h)) {
     r.sse = 0;
     r.bits = 0.0f;
-    for (int i = 0; i < 4; i++) reinterpret_cast<uint32_t*>(r.tx_types)[i] = 0xffffffffu;
-    *reinterpret_cast<uint32_t*>(r.reserved) = 0;
+    for (int i = 0; i < NB; i++) result_types(r)[i] = 0xff;
+    clear_reserved(r);
     if (cf_out)
-      for (int i = 0; i < 256; i++) cf_out[(size_t)j * 256 + i] = 0;
+      for (int i = 0; i < B * B; i++) cf_out[(size_t)j * B * B + i] = 0;
     if (rec_out)
-      for (int i = 0; i < 256; i++) rec_out[(size_t)j * 256 + i] = 0;
+      for (int i = 0; i < B * B; i++) rec_out[(size_t)j * B * B + i] = 0;
     return;
   }
   Depth2Work w;
@@ -336,14 +352,20 @@ __global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
   const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
   const float skip1 = p.use_skip_bits ? p.skip_bits[0][0] : 0.0f;
   const float skip0 = p.use_skip_bits ? p.skip_bits[0][1] : 0.0f;
-  const PatchRead rd{rec, p.stride, jb.px, jb.py, w.patch};
+  const PatchReadS<B> rd{rec, p.stride, jb.px, jb.py, w.patch};
   long long sse_sum = 0;
   float bits_sum = 0.0f;
-  uint8_t txtps[16];
-  for (int ti = 0; ti < 16; ti++) {
-    const int i = ti & 3, jr = ti >> 2, bx = jb.px + i * 4, by = jb.py + jr * 4;
-    const bool tr = jr == 0 ? (jb.py > 0 && (i < 3 || have_tr)) : i < 3;
-    const bool bl = i == 0 ? (jb.px > 0 && (jr < 3 || have_bl)) : false;
+  uint8_t txtps[NB];
+  for (int ti = 0; ti < NB; ti++) {
+    const int i = ti % G, jr = ti / G, bx = jb.px + i * 4, by = jb.py + jr * 4;
+    bool tr, bl;
+    if (B == 16) {
+      tr = jr == 0 ? (jb.py > 0 && (i < 3 || have_tr)) : i < 3;
+      bl = i == 0 ? (jb.px > 0 && (jr < 3 || have_bl)) : false;
+    } else {
+      tr = ti == 0 ? jb.py > 0 : (ti == 1 ? have_tr : ti == 2);
+      bl = ti == 0 ? jb.px > 0 : (ti == 2 ? have_bl : false);
+    }
     predict_sq_at<4>(rd, p.frame_w, p.frame_h, bx, by, jb.mode, jb.angle_delta, tr, bl, ft, p.bd, w.pred, w.u);
 #pragma unroll
     for (int k = 0; k < 16; k++)
@@ -360,13 +382,14 @@ __global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
     eb.maxv = maxv;
     float* tf = reinterpret_cast<float*>(w.u);
     int32_t* tmp = w.u + 64;
-    // DCT_DCT, ADST_ADST, IDTX, V_DCT, H_DCT (nibble k: the k-th type).
+    // DCT_DCT, ADST_ADST, IDTX[, V_DCT, H_DCT] (nibble k: the k-th type).
     constexpr uint32_t kTypeOrder = 0x32041u;
+    constexpr int kNumTypes = B == 16 ? 5 : 3;
     int best = 0, btx = MT_TX_DCT_DCT;
     long long bsse = 0, dct_sse = 0, guard = 0;
     float bbits = 0.0f;
 #pragma unroll 1
-    for (int k = 0; k < 5; k++) {
+    for (int k = 0; k < kNumTypes; k++) {
       const int t = (int)((kTypeOrder >> (4 * k)) & 15u);
       const int cur = k == 0 ? 0 : 1 - best;
       int16_t* cf = w.cfs[cur];
@@ -407,9 +430,9 @@ __global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
     bits_sum = __fadd_rn(bits_sum, bbits);
 #pragma unroll
     for (int k = 0; k < 16; k++)
-      w.patch[(jr * 4 + (k >> 2)) * 16 + i * 4 + (k & 3)] = (uint8_t)clampi((int32_t)w.pred[k] + brr[k], 0, maxv);
+      w.patch[(jr * 4 + (k >> 2)) * B + i * 4 + (k & 3)] = (uint8_t)clampi((int32_t)w.pred[k] + brr[k], 0, maxv);
     if (cf_out) {
-      int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * 256 + ti * 16);
+      int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * B * B + ti * 16);
 #pragma unroll
       for (int k = 0; k < 4; k++) o[k] = make_int4(bcf[4 * k], bcf[4 * k + 1], bcf[4 * k + 2], bcf[4 * k + 3]);
     }
@@ -417,12 +440,12 @@ __global__ void __launch_bounds__(kSplitThreads) depth2_kernel(
   r.sse = sse_sum;
   r.bits = bits_sum;
 #pragma unroll
-  for (int k = 0; k < 16; k++) r.tx_types[k] = txtps[k];
-  *reinterpret_cast<uint32_t*>(r.reserved) = 0;
+  for (int k = 0; k < NB; k++) result_types(r)[k] = txtps[k];
+  clear_reserved(r);
   if (rec_out) {
-    uint2* o = reinterpret_cast<uint2*>(rec_out + (size_t)j * 256);
+    uint2* o = reinterpret_cast<uint2*>(rec_out + (size_t)j * B * B);
 #pragma unroll 4
-    for (int k = 0; k < 64; k++)
+    for (int k = 0; k < B * B / 4; k++)
       o[k] = make_uint2(w.patch[4 * k] | ((uint32_t)w.patch[4 * k + 1] << 16),
                         w.patch[4 * k + 2] | ((uint32_t)w.patch[4 * k + 3] << 16));
   }
@@ -438,6 +461,68 @@ int check_split(const mt_split16_params* p, const mt_quant* q, int32_t n) {
 }
 
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Launch and host-buffer forms shared by the two TX_4X4 split trials.
+template <int B, typename R>
+int tx4_split_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                     const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                     const mt_split16_job* d_jobs, int32_t n, R* d_results, int32_t* d_cf, uint16_t* d_rec,
+                     void* stream) {
+  int rc = check_split(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!d_src || !d_recon || !d_costs || !d_jobs || !d_results) return MT_ERR_INVALID_INPUT;
+  SplitArgs a;
+  a.p = *prm;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
+  tx4_split_kernel<B, R><<<(unsigned)((n + kSplitThreads - 1) / kSplitThreads), kSplitThreads, 0,
+                           reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
+                                                                     d_results, d_cf, d_rec);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+template <int B, typename R>
+int tx4_split_host(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                   R* results, int32_t* cf_out, uint16_t* rec_out) {
+  int rc = check_split(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t), bb = (size_t)B * B;
+  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + 256;
+  const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
+  const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_split16_job));
+  const size_t o_cf = o_res + up256((size_t)n * sizeof(R));
+  const size_t o_out = o_cf + (cf_out ? up256((size_t)n * bb * 4) : 0);
+  const size_t total = o_out + (rec_out ? up256((size_t)n * bb * 2) : 0);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 16, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_split16_job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = tx4_split_device<B>(reinterpret_cast<const uint16_t*>(d + o_src),
+                             reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant, has_qm ? d + o_qm : nullptr,
+                             reinterpret_cast<const mt_coef_costs*>(d + o_cost),
+                             reinterpret_cast<const mt_split16_job*>(d + o_jobs), n, reinterpret_cast<R*>(d + o_res),
+                             cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr,
+                             rec_out ? reinterpret_cast<uint16_t*>(d + o_out) : nullptr, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(R), cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * bb * 4, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && rec_out)
+      e = cudaMemcpy(rec_out, d + o_out, (size_t)n * bb * 2, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
 
 }  // namespace
 
@@ -530,60 +615,28 @@ int mt_split16_depth2_device(const uint16_t* d_src, const uint16_t* d_recon, con
                              const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                              const mt_split16_job* d_jobs, int32_t n, mt_split16_d2_result* d_results,
                              int32_t* d_cf, uint16_t* d_rec, void* stream) {
-  int rc = check_split(prm, quant, n);
-  if (rc != MT_OK) return rc;
-  if (n == 0) return MT_OK;
-  if (!d_src || !d_recon || !d_costs || !d_jobs || !d_results) return MT_ERR_INVALID_INPUT;
-  SplitArgs a;
-  a.p = *prm;
-  a.q = *quant;
-  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
-                                         : 0.0f;
-  a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  depth2_kernel<<<(unsigned)((n + kSplitThreads - 1) / kSplitThreads), kSplitThreads, 0,
-                  reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
-                                                            d_results, d_cf, d_rec);
-  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+  return tx4_split_device<16>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec,
+                              stream);
 }
 
 int mt_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                       const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
                       mt_split16_d2_result* results, int32_t* cf_out, uint16_t* rec_out) {
-  int rc = check_split(prm, quant, n);
-  if (rc != MT_OK) return rc;
-  if (n == 0) return MT_OK;
-  if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
-  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
-  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + 256;
-  const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
-  const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_split16_job));
-  const size_t o_cf = o_res + up256((size_t)n * sizeof(mt_split16_d2_result));
-  const size_t o_out = o_cf + (cf_out ? up256((size_t)n * 256 * 4) : 0);
-  const size_t total = o_out + (rec_out ? up256((size_t)n * 256 * 2) : 0);
-  uint8_t* d = nullptr;
-  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
-  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
-  cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 16, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_split16_job), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    rc = mt_split16_depth2_device(
-        reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant,
-        has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
-        reinterpret_cast<const mt_split16_job*>(d + o_jobs), n, reinterpret_cast<mt_split16_d2_result*>(d + o_res),
-        cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr, rec_out ? reinterpret_cast<uint16_t*>(d + o_out) : nullptr,
-        nullptr);
-    if (rc == MT_OK)
-      e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_split16_d2_result), cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 256 * 4, cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && rec_out)
-      e = cudaMemcpy(rec_out, d + o_out, (size_t)n * 256 * 2, cudaMemcpyDeviceToHost);
-  }
-  cudaFree(d);
-  if (rc != MT_OK) return rc;
-  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+  return tx4_split_host<16>(src, recon, prm, quant, qm_row, costs, jobs, n, results, cf_out, rec_out);
+}
+
+int mt_split4tx_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                       const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                       const mt_split16_job* d_jobs, int32_t n, mt_split16_result* d_results, int32_t* d_cf,
+                       uint16_t* d_rec, void* stream) {
+  return tx4_split_device<8>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec,
+                             stream);
+}
+
+int mt_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
+                mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return tx4_split_host<8>(src, recon, prm, quant, qm_row, costs, jobs, n, results, cf_out, rec_out);
 }
 
 }  // extern "C"

@@ -461,15 +461,16 @@ def coef_ctx_bytes(rng, n):
     return np.where(zero, 0x40, cul | dcb).astype(np.uint8)
 
 
-def split16_jobs(fw, fh, modes, deltas=(0,), seed=0):
-    """(16x16 block, mode, delta) jobs of split16_luma_try, mode-major (every
+def split16_jobs(fw, fh, modes, deltas=(0,), seed=0, n=16):
+    """(n x n block, mode, delta) jobs of the split trials (n = 16:
+    split16_luma_try / split16_depth2_try, 8: split4tx_try), mode-major (every
     block for one (mode, delta), then the next), with deterministic neighbour
     flags and random coefficient contexts per block."""
     rng = np.random.default_rng(seed)
-    bys, bxs = np.meshgrid(np.arange(0, fh - 15, 16), np.arange(0, fw - 15, 16), indexing="ij")
+    bys, bxs = np.meshgrid(np.arange(0, fh - n + 1, n), np.arange(0, fw - n + 1, n), indexing="ij")
     px, py = bxs.ravel(), bys.ravel()
     nb = len(px)
-    flags = np.array([block_flags(int(x), int(y), fw, fh, 16) for x, y in zip(px, py)], np.uint8)
+    flags = np.array([block_flags(int(x), int(y), fw, fh, n) for x, y in zip(px, py)], np.uint8)
     flags |= np.where(rng.random(nb) < 0.5, abi.CAND_FILTER_TYPE, 0).astype(np.uint8)
     a_coef = coef_ctx_bytes(rng, nb * 4).reshape(nb, 4)
     l_coef = coef_ctx_bytes(rng, nb * 4).reshape(nb, 4)

@@ -130,6 +130,10 @@ void or_filter_intra_predict(const uint16_t* recon, int32_t stride, int32_t ox, 
 int or_filter_intra_beam(const uint16_t* src, const uint16_t* recon, int32_t stride, int32_t frame_w, int32_t frame_h,
                          int32_t vis_w, int32_t vis_h, int32_t bd, int32_t w, int32_t h, const uint16_t* pos,
                          int32_t n, uint64_t* scores, uint8_t* modes, int16_t* preds);
+/* block8.rs:157 split4tx_try over a batch of 8x8 jobs. */
+int or_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
+                mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

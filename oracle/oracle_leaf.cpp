@@ -753,3 +753,133 @@ int or_split16_depth2(const uint16_t* src, const uint16_t* recon, const mt_split
 }
 
 }  // extern "C"
+
+namespace {
+
+// One job of split4tx_try (block8.rs:157-286); `rec` as in split16_one.
+void split4tx_one(const uint16_t* src, uint16_t* rec, const mt_split16_params* p, const mt_quant* q, const uint8_t* qm,
+                  const mt_coef_cdfs* cd, const mt_split16_job& jb, mt_split16_result* r, int32_t* cf_out,
+                  uint16_t* rec_out) {
+  const int px = jb.px, py = jb.py, stride = p->stride;
+  uint16_t saved[64], blk[64];
+  for (int y = 0; y < 8; y++)
+    for (int x = 0; x < 8; x++) saved[y * 8 + x] = rec[(size_t)(py + y) * stride + px + x];
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const int ft = (jb.flags & MT_CAND_FILTER_TYPE) != 0;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const uint16_t* scan = or_default_scan(4);
+  const float dcq = (float)q->dc_q, acq = (float)q->ac_q, rd_lam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  const float* skip = p->use_skip_bits ? p->skip_bits[0] : nullptr;
+  static const int kQuad[4][2] = {{0, 0}, {4, 0}, {0, 4}, {4, 4}};
+  int64_t sse_sum = 0;
+  float bits_sum = 0.0f;
+  for (int qi = 0; qi < 4; qi++) {
+    const int sx = kQuad[qi][0], sy = kQuad[qi][1], bx = px + sx, by = py + sy;
+    bool tr, bl;
+    switch (qi) {
+      case 0: tr = py > 0; bl = px > 0; break;
+      case 1: tr = have_tr; bl = false; break;
+      case 2: tr = true; bl = have_bl; break;
+      default: tr = false; bl = false; break;
+    }
+    int32_t pred[16];
+    if (jb.mode == MT_DC_PRED) {
+      const int32_t d = or_dc_pred(rec, stride, bx, by, 4, 4, p->bd);
+      for (int k = 0; k < 16; k++) pred[k] = d;
+    } else {
+      or_intra_predict(rec, stride, bx, by, 4, 4, jb.mode, jb.angle_delta, tr, bl, p->frame_w, p->frame_h, ft, p->bd,
+                       pred);
+    }
+    int32_t resid[16];
+    for (int y = 0; y < 4; y++)
+      for (int x = 0; x < 4; x++) resid[y * 4 + x] = (int32_t)src[(size_t)(by + y) * stride + bx + x] - pred[y * 4 + x];
+    // luma_bits' whole-block contexts of this 4x4 (lossy_state.rs:495-513).
+    const int s = (jb.a_coef[sx / 4] >> 6) - 1 + (jb.l_coef[sy / 4] >> 6) - 1;
+    const int ds = (s != 0) + (s > 0);
+    const uint16_t pos[2] = {(uint16_t)bx, (uint16_t)by};
+    auto sse_of = [&](const int32_t* rr) -> int64_t {
+      int64_t d = 0;
+      or_sse_recon(src, stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, 4, 4, p->wsse_scale, &d);
+      return d;
+    };
+    int32_t bcf[16], brr[16];
+    float tf[16];
+    or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, 4, q, qm, bcf, tf);
+    or_trellis_optimize(bcf, tf, dcq, acq, scan, 16, p->trellis_lambda0);
+    or_inv_txfm_dequant(bcf, MT_TX_DCT_DCT, 4, q, qm, brr);
+    const int64_t dct_sse = sse_of(brr);
+    int64_t bsse = dct_sse;
+    float bbits = or_real_block_bits_bounded(bcf, scan, 4, 4, cd, 0, ds, jb.mode, MT_TX_DCT_DCT, p->use_skip_bits,
+                                             skip, INFINITY);
+    uint8_t btx = MT_TX_DCT_DCT;
+    const int64_t guard = p->tx_guard_shift >= 63 ? 0 : dct_sse >> p->tx_guard_shift;
+    for (int t : {MT_TX_ADST_ADST, MT_TX_IDTX}) {
+      int32_t acf[16], arr[16];
+      float atf[16];
+      or_fwd_txfm_quant(resid, t, 4, q, qm, acf, atf);
+      if (t == MT_TX_ADST_ADST) or_trellis_optimize(acf, atf, dcq, acq, scan, 16, p->trellis_lambda0);
+      or_inv_txfm_dequant(acf, t, 4, q, qm, arr);
+      const int64_t asse = sse_of(arr);
+      if (asse > dct_sse + guard) continue;
+      const float best_rd = rd_cost_i64(bsse, rd_lam, bbits);
+      const float bound = (best_rd - (float)asse) / rd_lam;
+      const float abits =
+          or_real_block_bits_bounded(acf, scan, 4, 4, cd, 0, ds, jb.mode, t, p->use_skip_bits, skip, bound);
+      if (rd_cost_i64(asse, rd_lam, abits) < best_rd) {
+        memcpy(bcf, acf, sizeof(acf));
+        memcpy(brr, arr, sizeof(arr));
+        bsse = asse;
+        bbits = abits;
+        btx = (uint8_t)t;
+      }
+    }
+    r->tx_types[qi] = btx;
+    sse_sum += bsse;
+    bits_sum += bbits;
+    for (int y = 0; y < 4; y++)
+      for (int x = 0; x < 4; x++) {
+        const uint16_t v = (uint16_t)clampi(pred[y * 4 + x] + brr[y * 4 + x], 0, maxv);
+        rec[(size_t)(by + y) * stride + bx + x] = v;
+        blk[(sy + y) * 8 + sx + x] = v;
+      }
+    if (cf_out) memcpy(cf_out + qi * 16, bcf, sizeof(bcf));
+  }
+  for (int y = 0; y < 8; y++)
+    for (int x = 0; x < 8; x++) rec[(size_t)(py + y) * stride + px + x] = saved[y * 8 + x];
+  r->sse = sse_sum;
+  r->bits = bits_sum;
+  if (rec_out) memcpy(rec_out, blk, sizeof(blk));
+}
+
+}  // namespace
+
+extern "C" {
+
+// block8.rs:157-286 split4tx_try over a batch of 8x8 jobs.
+int or_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
+                mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  std::vector<uint16_t> rec(recon, recon + (size_t)p->stride * p->frame_h);
+  for (int i = 0; i < n; i++) {
+    const mt_split16_job& jb = jobs[i];
+    mt_split16_result* r = &results[i];
+    const bool bad = jb.px + 8 > p->frame_w || jb.py + 8 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+                     jb.angle_delta < -3 || jb.angle_delta > 3 ||
+                     (jb.angle_delta != 0 && (jb.mode < MT_V_PRED || jb.mode > MT_D67_PRED));
+    if (bad) {
+      r->sse = 0;
+      r->bits = 0.0f;
+      memset(r->tx_types, 255, 4);
+      if (cf_out) memset(cf_out + (size_t)i * 64, 0, 64 * sizeof(int32_t));
+      if (rec_out) memset(rec_out + (size_t)i * 64, 0, 64 * sizeof(uint16_t));
+      continue;
+    }
+    split4tx_one(src, rec.data(), p, q, qm, cdfs, jb, r, cf_out ? cf_out + (size_t)i * 64 : nullptr,
+                 rec_out ? rec_out + (size_t)i * 64 : nullptr);
+  }
+  return MT_OK;
+}
+
+}  // extern "C"

@@ -73,6 +73,8 @@ def load():
             "or_filter_intra_predict": (None, [_P] + [C.c_int32] * 7 + [_P]),
             "or_filter_intra_beam": (C.c_int, [_P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P, _P]),
             "or_cfl_alpha": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P]),
+            "or_split4tx": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                      C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                           C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P, C.c_int32]),
         }
@@ -425,3 +427,18 @@ def filter_intra_beam(src, recon, w, h, pos, vis=(0, 0), bd=8):
     assert load().or_filter_intra_beam(p(src), p(recon), src.shape[1], src.shape[1], src.shape[0], vis[0], vis[1], bd,
                                        w, h, p(pos), n, p(scores), p(modes), p(preds)) == 0
     return scores, modes, preds
+
+
+def split4tx(src, recon, prm, q, qm, cdfs, jobs):
+    """split4tx_try of a batch of 8x8 jobs: (results, cf n x 64, rec n x 8 x 8)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.SPLIT16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.SPLIT16_RESULT_DTYPE)
+    cf = np.zeros((n, 64), np.int32)
+    rec = np.zeros((n, 8, 8), np.uint16)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+    assert load().or_split4tx(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n, p(res),
+                              p(cf), p(rec)) == 0
+    return res, cf, rec

@@ -187,3 +187,88 @@ def test_depth2_skip_bits_vis_and_rejects(mt_lib, oracle_lib, cuda):
     jobs["angle_delta"][4] = -1  # a delta on DC: rejected
     res = _check(mt_lib, oracle_lib, src, rec, prm, q, qm, luma_tx4_cdfs(), jobs)
     assert (res["tx_types"][2] == 255).all() and (res["tx_types"][4] == 255).all()
+
+
+def _compose4(oracle_lib, src, rec, prm, q, qm, c, jb):
+    """split4tx_try (src/coder/block8.rs:157-286) composed from the oracle's primitives."""
+    rec = rec.copy()
+    px, py = int(jb["px"]), int(jb["py"])
+    have_tr, have_bl = bool(jb["flags"] & abi.CAND_HAVE_TR), bool(jb["flags"] & abi.CAND_HAVE_BL)
+    ft = bool(jb["flags"] & abi.CAND_FILTER_TYPE)
+    mode, delta = int(jb["mode"]), int(jb["angle_delta"])
+    scan = oracle_lib.default_scan(4)
+    f32 = np.float32
+    rd = lambda d, b: f32(f32(d) + f32(f32(prm.rd_lambda) * f32(b)))
+    sse, bits, cf4, types = 0, f32(0), [], []
+    for qi, (sx, sy) in enumerate(((0, 0), (4, 0), (0, 4), (4, 4))):
+        bx, by = px + sx, py + sy
+        tr, bl = [(py > 0, px > 0), (have_tr, False), (True, have_bl), (False, False)][qi]
+        pred = oracle_lib.intra_predict(rec, bx, by, 4, 4, mode, delta, tr, bl, ft).ravel()
+        resid = src[by:by + 4, bx:bx + 4].astype(np.int32).ravel() - pred
+        s = (int(jb["a_coef"][sx // 4]) >> 6) - 1 + (int(jb["l_coef"][sy // 4]) >> 6) - 1
+        ds = int(s != 0) + int(s > 0)
+        best = None
+        for t in (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX):
+            cf, tf = oracle_lib.fwd_txfm_quant(resid, t, q, qm)
+            if t != abi.TX_IDTX:
+                cf = oracle_lib.trellis_optimize(cf, tf, float(q.dc_q), float(q.ac_q), scan, prm.trellis_lambda0)
+            rr = oracle_lib.inv_txfm_dequant(cf, t, q, qm)
+            d = int(oracle_lib.sse_recon(src, prm.frame_w, prm.frame_h, [(bx, by)], pred, rr, 4, 4)[0])
+            if best is None:
+                dct_sse = d
+                b = f32(oracle_lib.real_block_bits_bounded(cf, scan, 4, 4, c, 0, ds, mode, t, INF))
+                best = (cf, rr, d, b, t)
+                continue
+            if d > dct_sse + (dct_sse >> prm.tx_guard_shift):
+                continue
+            best_rd = rd(best[2], best[3])
+            bound = float(f32(f32(best_rd - f32(d)) / f32(prm.rd_lambda)))
+            b = f32(oracle_lib.real_block_bits_bounded(cf, scan, 4, 4, c, 0, ds, mode, t, bound))
+            if rd(d, b) < best_rd:
+                best = (cf, rr, d, b, t)
+        sse += best[2]
+        bits = f32(bits + best[3])
+        types.append(best[4])
+        cf4.append(best[0])
+        rec[by:by + 4, bx:bx + 4] = np.clip(pred.reshape(4, 4) + best[1].reshape(4, 4), 0, 255)
+    return sse, bits, np.concatenate(cf4), rec[py:py + 8, px:px + 8], types
+
+
+def test_split4tx_oracle_glue_matches_composition(oracle_lib):
+    import maroontree_b200 as mt
+
+    src, rec = _frame(48, 32, 41)
+    q = oracle_lib.quant_new(80, 8, 15)
+    c = luma_tx4_cdfs()
+    prm = mt.split16_params(48, 32, trellis_lambda0=0.05, rd_lambda=22.0, tx_guard_shift=4)
+    jobs = synth.split16_jobs(48, 32, (abi.DC_PRED, abi.H_PRED, abi.D45_PRED, abi.SMOOTH_PRED), deltas=(0, 2),
+                              seed=8, n=8)
+    res, cf, recs = oracle_lib.split4tx(src, rec, prm, q, None, c, jobs)
+    seen = set()
+    for i, jb in enumerate(jobs):
+        sse, bits, cf4, r8, types = _compose4(oracle_lib, src, rec, prm, q, None, c, jb)
+        assert res["sse"][i] == sse and np.float32(res["bits"][i]) == bits, i
+        assert list(res["tx_types"][i]) == types, i
+        assert np.array_equal(cf[i], cf4) and np.array_equal(recs[i], r8), i
+        seen.update(types)
+    assert len(seen) >= 2, seen
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qidx,qm_level,wsse", [(70, 6, 0.0), (116, 15, 1.0), (30, 3, 0.75)])
+def test_split4tx_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse):
+    import maroontree_b200 as mt
+
+    src, rec = _frame(160, 96, qidx + 3)
+    q = oracle_lib.quant_new(qidx, 8, qm_level)
+    qm = oracle_lib.qm_row(qm_level, 0, 4) if qm_level < 15 else None
+    jobs = synth.split16_jobs(160, 96, range(13), deltas=(-1, 0, 2), seed=qidx, n=8)
+    jobs["px"][5] = 156  # crosses the right edge: rejected
+    c = luma_tx4_cdfs()
+    prm = mt.split16_params(160, 96, trellis_lambda0=0.05, rd_lambda=0.3 * qidx + 2.0, wsse_scale=wsse,
+                            tx_guard_shift=4, skip_bits=[(1.5, 0.5)] + [(0.0, 0.0)] * 12, vis=(157, 93))
+    res, cf, recs = mt_lib.split4tx(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs, want_cf=True, want_rec=True)
+    want, wcf, wrec = oracle_lib.split4tx(src, rec, prm, q, qm, c, jobs)
+    assert res.tobytes() == want.tobytes()
+    assert np.array_equal(cf, wcf) and np.array_equal(recs, wrec)
+    assert (res["tx_types"][5] == 255).all() and len(np.unique(res["tx_types"])) >= 3
