@@ -15,7 +15,8 @@ coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
 The line also carries ``level4`` / ``level16`` (the 4x4 and 16x16 levels of
 the same frame, device time and the oracle on the host cores), ``split16``
 (the 16x16 leaf's TX_8X8 split trial over every block and mode, with and
-without the 4:4:4 type search, and its depth-2 TX_4X4 trial) and
+without the 4:4:4 type search, and its depth-2 TX_4X4 trial), ``leaf8`` (the
+8x8 leaf's mode-loop candidates and winner refinement) and
 ``frame_filters``: the frame-wide kernels of the same
 1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
 grid, the screen-content gate, the CfL alpha of every 8x8 chroma block,
@@ -355,6 +356,67 @@ def measure_split16(dev, wl, search, reps=5, cpu=True, depth2=False):
     return out
 
 
+def measure_leaf8(dev, wl, refine, reps=5, cpu=True):
+    """The 8x8 leaf's luma search over the same 1080p luma: the mode loop's
+    candidates (32,400 blocks x 13 modes, DCT_DCT with trellis_optimize_ctx and
+    sse_recon) or the winners' transform-type refinement (32,400 blocks, seven
+    types, 4:4:4 form).  Device time with CUDA events after an L2 flush; the
+    oracle on all host cores over the same jobs."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    q = mt.quant_new(QIDX, 8, QM_LEVEL)
+    qm = mt.qm_row(QM_LEVEL, 0, 8)
+    cdfs = synth.synthetic_cdfs(4)
+    costs = mt.coef_costs(cdfs)
+    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=3)
+    n = len(jobs)
+    prm = mt.split16_params(W, H, trellis_lambda0=0.05, rd_lambda=wl["prm"].mode_lambda, band_tilt=1.9,
+                            tx_search=refine, tx_guard_shift=5)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
+                                           t(jobs))
+    d_res = torch.empty(n * abi.LEAF8_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    lib = mt.load()
+    entry = lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device
+
+    def launch():
+        rc = entry(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q), d_qm.data_ptr(), d_costs.data_ptr(),
+                   d_jobs.data_ptr(), n, d_res.data_ptr(), None, None, None)
+        assert rc == 0, rc
+
+    for _ in range(3):
+        launch()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(200_000)
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    step = float(np.median(ms))
+    what = ("leaf8 winners' transform-type refinement 1920x1080 luma, 32,400 blocks, 7 types" if refine else
+            "leaf8 mode-loop candidates 1920x1080 luma, 32,400 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)")
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n, "workload": what}
+    if cpu:
+        from oracle import pyoracle as po
+
+        t0 = time.perf_counter()
+        po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": 1, "kind": "port",
+                               "sample": f"all {n} jobs ({dt:.2f} s)"}
+    return out
+
+
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -591,6 +653,8 @@ def run_ours(args):
                for k in ("dct", "search")} if rank == 0 else None
     if split16 is not None:
         split16["depth2"] = measure_split16(dev, wl, False, cpu=world == 1 and not args.no_cpu, depth2=True)
+    leaf8 = {k: measure_leaf8(dev, wl, k == "refine", cpu=world == 1 and not args.no_cpu)
+             for k in ("luma", "refine")} if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -623,6 +687,7 @@ def run_ours(args):
         "level4": level4,
         "level16": level16,
         "split16": split16,
+        "leaf8": leaf8,
         # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
         "gpu_launches": 4 * args.steps,
         "clocks": clk.summary(),

@@ -486,6 +486,55 @@ int mt_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_par
                 const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,
                 mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
 
+/* ---- The 8x8 leaf's luma search (pick_block8, src/coder/block8.rs:689-1420) ----
+ * mt_leaf8_luma: the Slow mode loop's candidates -- each (block, mode, delta)
+ * predicted from the reconstruction, DCT_DCT (+ QM) with the per-candidate
+ * trellis_optimize_ctx in the block's dc_sign context, the dav1d inverse,
+ * sse_recon, luma_bits in txb_skip context 0, and
+ * cost = rd_cost_i64(sse, rd_lambda, bits + syntax_bits) (block8.rs:738-808;
+ * syntax_bits is the caller's luma_intra_syntax_bits).  trellis_lambda0 <= 0
+ * prices the plain quantised levels (the Medium / Fast loop).
+ * mt_leaf8_tx_refine: the winner's transform-type refinement
+ * (block8.rs:1183-1404): the DCT baseline as above, then ADST_ADST (taken when
+ * within tx_guard of the DCT's SSE and below the DCT's rd cost), ADST_DCT and
+ * DCT_ADST (within tx_guard of the DCT's SSE, below the current best), IDTX
+ * (within tx_guard of the current best's SSE, unbounded rate), and unless
+ * tx_search is 0 (4:2:0) V_DCT and H_DCT (at most the current best's SSE);
+ * the ADST family trellised, priced by the bounded 2-D walk, V / H by the 1-D
+ * walk.  Params as mt_split16_params with skip_bits[0] the TX_8X8 class's
+ * context-0 pair; band_tilt the tile's.  Rejected jobs (outside the frame, a
+ * bad mode / delta / context) get sse 0, bits and cost +inf, tx_type 255. */
+typedef struct mt_leaf8_job {
+  uint16_t px, py;          /* 8x8 block origin */
+  uint8_t mode;             /* MT_*_PRED */
+  int8_t angle_delta;
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL / FILTER_TYPE */
+  uint8_t dcs_ctx;          /* dc_sign_ctx of the block, 0..2 */
+  float syntax_bits;        /* luma_intra_syntax_bits(px, py, 8, 8, mode, delta) */
+} mt_leaf8_job;
+typedef struct mt_leaf8_result {
+  int64_t sse;              /* sse_recon of the chosen levels */
+  float bits;               /* coefficient bits (without the syntax bits) */
+  float cost;               /* mt_leaf8_luma: rd_cost_i64(sse, rd_lambda, bits + syntax_bits);
+                             * mt_leaf8_tx_refine: rd_cost_i64(sse, rd_lambda, bits) */
+  uint8_t tx_type;          /* MT_TX_* (DCT_DCT from mt_leaf8_luma) */
+  uint8_t reserved[7];
+} mt_leaf8_result;
+/* d_cf (optional): n x 64 int32 levels column-major; d_rec (optional): n x 64
+ * u16 reconstruction. */
+int mt_leaf8_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                         const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                         const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                         uint16_t* d_rec, void* stream);
+int mt_leaf8_tx_refine_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                              const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                              const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                              uint16_t* d_rec, void* stream);
+/* Host-buffer forms; refine = 0: mt_leaf8_luma, 1: mt_leaf8_tx_refine. */
+int mt_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+             const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+             mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

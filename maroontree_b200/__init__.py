@@ -284,6 +284,23 @@ def split4tx(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec
     return res, cf, rec
 
 
+def leaf8(src, recon, prm, quant, qmrow, costs, jobs, refine=False, want_cf=False, want_rec=False):
+    """The 8x8 leaf's luma search (``mt_leaf8``): the mode loop's candidates, or with
+    refine the winners' transform-type refinement.  Returns (results, cf n x 64 or
+    None, rec n x 8 x 8 or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.LEAF8_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.LEAF8_RESULT_DTYPE)
+    cf = np.zeros((n, 64), np.int32) if want_cf else None
+    rec = np.zeros((n, 8, 8), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_leaf8(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs), ptr(jobs), n,
+                           int(bool(refine)), ptr(res), ptr(cf), ptr(rec)), "mt_leaf8")
+    return res, cf, rec
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

@@ -90,6 +90,11 @@ SPLIT16_D2_RESULT_DTYPE = np.dtype([("sse", "<i8"), ("bits", "<f4"), ("tx_types"
                                     ("reserved", "u1", (4,))])
 assert SPLIT16_JOB_DTYPE.itemsize == 16 and SPLIT16_RESULT_DTYPE.itemsize == 16
 assert SPLIT16_D2_RESULT_DTYPE.itemsize == 32
+LEAF8_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"),
+                            ("dcs_ctx", "u1"), ("syntax_bits", "<f4")])
+LEAF8_RESULT_DTYPE = np.dtype([("sse", "<i8"), ("bits", "<f4"), ("cost", "<f4"), ("tx_type", "u1"),
+                               ("reserved", "u1", (7,))])
+assert LEAF8_JOB_DTYPE.itemsize == 12 and LEAF8_RESULT_DTYPE.itemsize == 24
 CFL_BLOCK_DTYPE = np.dtype([("cx", "<u2"), ("cy", "<u2"), ("dc", "<i2", (2,))])
 assert CFL_BLOCK_DTYPE.itemsize == 8
 
@@ -234,6 +239,12 @@ def _bind(lib):
                                          C.c_int32, _P, _P, _P, _P]),
         "mt_split4tx": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                   C.c_int32, _P, _P, _P]),
+        "mt_leaf8_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                           C.c_int32, _P, _P, _P, _P]),
+        "mt_leaf8_tx_refine_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                                C.c_int32, _P, _P, _P, _P]),
+        "mt_leaf8": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                               C.c_int32, C.c_int32, _P, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                       _P, C.c_int32, _P, _P, _P]),
         "mt_screen_gate_scratch_bytes": (C.c_size_t, [C.POINTER(ScreenGateParams)]),
@@ -279,6 +290,7 @@ EXPORTED_SYMBOLS = (
     "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
+    "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8",
 )
 
 

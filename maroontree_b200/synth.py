@@ -480,3 +480,22 @@ def split16_jobs(fw, fh, modes, deltas=(0,), seed=0, n=16):
             for b in range(nb):
                 rows.append((px[b], py[b], m, d, flags[b], 0, a_coef[b], l_coef[b]))
     return np.array(rows, abi.SPLIT16_JOB_DTYPE)
+
+
+def leaf8_jobs(fw, fh, modes, deltas=(0,), seed=0):
+    """(8x8 block, mode, delta) jobs of the 8x8 leaf's luma search, mode-major,
+    with deterministic neighbour flags, random dc_sign contexts and syntax bits."""
+    rng = np.random.default_rng(seed)
+    bys, bxs = np.meshgrid(np.arange(0, fh - 7, 8), np.arange(0, fw - 7, 8), indexing="ij")
+    px, py = bxs.ravel(), bys.ravel()
+    nb = len(px)
+    flags = np.array([block_flags(int(x), int(y), fw, fh, 8) for x, y in zip(px, py)], np.uint8)
+    flags |= np.where(rng.random(nb) < 0.5, abi.CAND_FILTER_TYPE, 0).astype(np.uint8)
+    dcs = rng.integers(0, 3, size=nb)
+    rows = []
+    for m in modes:
+        for d in (deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)):
+            syn = (rng.random(nb) * 6 + 1).astype(np.float32)
+            for b in range(nb):
+                rows.append((px[b], py[b], m, d, flags[b], dcs[b], syn[b]))
+    return np.array(rows, abi.LEAF8_JOB_DTYPE)

@@ -134,6 +134,10 @@ int or_filter_intra_beam(const uint16_t* src, const uint16_t* recon, int32_t str
 int or_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                 const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_split16_job* jobs, int32_t n,
                 mt_split16_result* results, int32_t* cf_out, uint16_t* rec_out);
+/* block8.rs:689-1404 pick_block8: the mode loop's candidates (refine 0) or the winner's type refinement (1). */
+int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+             const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+             mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

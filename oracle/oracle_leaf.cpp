@@ -883,3 +883,141 @@ int or_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_par
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// block8.rs:738-808 (refine = 0: the Slow mode loop's candidate) and
+// :1183-1404 (refine = 1: the winner's transform-type refinement) of
+// pick_block8, over a batch of 8x8 jobs.
+int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+             const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+             mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const uint16_t* scan = or_default_scan(8);
+  const float dcq = (float)q->dc_q, acq = (float)q->ac_q, mlam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  const float* skip = p->use_skip_bits ? p->skip_bits[0] : nullptr;
+  auto guard = [&](int64_t d) -> int64_t { return p->tx_guard_shift >= 63 ? 0 : d >> p->tx_guard_shift; };
+  for (int i = 0; i < n; i++) {
+    const mt_leaf8_job& jb = jobs[i];
+    mt_leaf8_result* r = &results[i];
+    memset(r->reserved, 0, sizeof(r->reserved));
+    const bool bad = jb.px + 8 > p->frame_w || jb.py + 8 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+                     jb.angle_delta < -3 || jb.angle_delta > 3 ||
+                     (jb.angle_delta != 0 && (jb.mode < MT_V_PRED || jb.mode > MT_D67_PRED)) || jb.dcs_ctx > 2;
+    if (bad) {
+      r->sse = 0;
+      r->bits = r->cost = INFINITY;
+      r->tx_type = 255;
+      if (cf_out) memset(cf_out + (size_t)i * 64, 0, 256);
+      if (rec_out) memset(rec_out + (size_t)i * 64, 0, 128);
+      continue;
+    }
+    int32_t pred[64];
+    if (jb.mode == MT_DC_PRED) {
+      const int32_t d = or_dc_pred(recon, p->stride, jb.px, jb.py, 8, 8, p->bd);
+      for (int k = 0; k < 64; k++) pred[k] = d;
+    } else {
+      or_intra_predict(recon, p->stride, jb.px, jb.py, 8, 8, jb.mode, jb.angle_delta, jb.flags & 1,
+                       (jb.flags >> 1) & 1, p->frame_w, p->frame_h, (jb.flags >> 2) & 1, p->bd, pred);
+    }
+    int32_t resid[64];
+    for (int y = 0; y < 8; y++)
+      for (int x = 0; x < 8; x++)
+        resid[y * 8 + x] = (int32_t)src[(size_t)(jb.py + y) * p->stride + jb.px + x] - pred[y * 8 + x];
+    const int ds = jb.dcs_ctx;
+    const uint16_t pos[2] = {jb.px, jb.py};
+    auto sse_of = [&](const int32_t* rr) -> int64_t {
+      int64_t d = 0;
+      or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, 8, 8, p->wsse_scale, &d);
+      return d;
+    };
+    auto bits2d = [&](const int32_t* cf, int t, float bound) -> float {
+      return or_real_block_bits_bounded(cf, scan, 8, 8, cd, 0, ds, jb.mode, t, p->use_skip_bits, skip, bound);
+    };
+    // The DCT_DCT candidate with the per-candidate trellis (block8.rs:780-805).
+    int32_t lcf[64], lrr[64];
+    float tf[64];
+    or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, 8, q, qm, lcf, tf);
+    or_trellis_optimize_ctx(lcf, tf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level, p->band_tilt);
+    or_inv_txfm_dequant(lcf, MT_TX_DCT_DCT, 8, q, qm, lrr);
+    const int64_t dct_sse = sse_of(lrr);
+    const float dct_bits = bits2d(lcf, MT_TX_DCT_DCT, INFINITY);
+    int64_t bsse = dct_sse;
+    float bbits = dct_bits;
+    uint8_t btx = MT_TX_DCT_DCT;
+    if (refine) {
+      auto take = [&](const int32_t* cf, const int32_t* rr, int64_t s, float b, int t) {
+        memcpy(lcf, cf, sizeof(lcf));
+        memcpy(lrr, rr, sizeof(lrr));
+        bsse = s;
+        bbits = b;
+        btx = (uint8_t)t;
+      };
+      // ADST_ADST (block8.rs:1214-1262)
+      {
+        int32_t acf[64], arr[64];
+        float atf[64];
+        or_fwd_txfm_quant(resid, MT_TX_ADST_ADST, 8, q, qm, acf, atf);
+        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level,
+                                p->band_tilt);
+        or_inv_txfm_dequant(acf, MT_TX_ADST_ADST, 8, q, qm, arr);
+        const int64_t asse = sse_of(arr);
+        const float base_rd = rd_cost_i64(dct_sse, mlam, dct_bits);
+        const float abits = bits2d(acf, MT_TX_ADST_ADST, (base_rd - (float)asse) / mlam);
+        if (asse <= dct_sse + guard(dct_sse) && rd_cost_i64(asse, mlam, abits) < base_rd)
+          take(acf, arr, asse, abits, MT_TX_ADST_ADST);
+      }
+      // ADST_DCT, DCT_ADST (block8.rs:1264-1332)
+      for (int t : {MT_TX_ADST_DCT, MT_TX_DCT_ADST}) {
+        int32_t acf[64], arr[64];
+        float atf[64];
+        or_fwd_txfm_quant(resid, t, 8, q, qm, acf, atf);
+        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level,
+                                p->band_tilt);
+        or_inv_txfm_dequant(acf, t, 8, q, qm, arr);
+        const int64_t asse = sse_of(arr);
+        const float base_rd = rd_cost_i64(bsse, mlam, bbits);
+        const float abits = bits2d(acf, t, (base_rd - (float)asse) / mlam);
+        if (asse <= dct_sse + guard(dct_sse) && rd_cost_i64(asse, mlam, abits) < base_rd)
+          take(acf, arr, asse, abits, t);
+      }
+      // IDTX (block8.rs:1334-1361)
+      {
+        int32_t icf[64], irr[64];
+        float itf[64];
+        or_fwd_txfm_quant(resid, MT_TX_IDTX, 8, q, qm, icf, itf);
+        or_inv_txfm_dequant(icf, MT_TX_IDTX, 8, q, qm, irr);
+        const int64_t isse = sse_of(irr);
+        const float ibits = bits2d(icf, MT_TX_IDTX, INFINITY);
+        const float base_rd = rd_cost_i64(bsse, mlam, bbits);
+        if (isse <= bsse + guard(bsse) && rd_cost_i64(isse, mlam, ibits) < base_rd)
+          take(icf, irr, isse, ibits, MT_TX_IDTX);
+      }
+      // V_DCT, H_DCT unless 4:2:0 (block8.rs:1362-1396)
+      if (p->tx_search)
+        for (int vertical = 1; vertical >= 0; vertical--) {
+          const int t = vertical ? MT_TX_V_DCT : MT_TX_H_DCT;
+          int32_t vcf[64], vrr[64];
+          float vtf[64];
+          or_fwd_txfm_quant(resid, t, 8, q, qm, vcf, vtf);
+          or_inv_txfm_dequant(vcf, t, 8, q, qm, vrr);
+          const int64_t vsse = sse_of(vrr);
+          const float vbits = or_luma_bits_1d(vcf, 8, vertical, cd, ds, jb.mode);
+          const float base_rd = rd_cost_i64(bsse, mlam, bbits);
+          if (vsse <= bsse && rd_cost_i64(vsse, mlam, vbits) < base_rd) take(vcf, vrr, vsse, vbits, t);
+        }
+    }
+    r->sse = bsse;
+    r->bits = bbits;
+    r->cost = refine ? rd_cost_i64(bsse, mlam, bbits) : rd_cost_i64(bsse, mlam, bbits + jb.syntax_bits);
+    r->tx_type = btx;
+    if (cf_out) memcpy(cf_out + (size_t)i * 64, lcf, sizeof(lcf));
+    if (rec_out)
+      for (int k = 0; k < 64; k++) rec_out[(size_t)i * 64 + k] = (uint16_t)clampi(pred[k] + lrr[k], 0, maxv);
+  }
+  return MT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,109 @@
+"""The 8x8 leaf's luma search (pick_block8): the Slow mode loop's candidates and
+the winner's transform-type refinement.
+
+CPU tests pin the oracle's glue against a composition of its primitives (the
+candidate's DCT + trellis_optimize_ctx + sse_recon + luma_bits + syntax bits,
+and the refinement's gate sequence), with the default luma TX_8X8 CDFs of the
+reference's Cdfs::new(0).  GPU tests compare the CUDA kernels with the oracle
+bit for bit."""
+import numpy as np
+import pytest
+
+from maroontree_b200 import abi, synth
+from test_split16 import luma_tx8_cdfs
+
+INF = float("inf")
+
+
+def _frame(w, h, seed):
+    src = synth.rgb_to_luma(synth.generate_rgb(w, h, seed))
+    rec = synth.synthetic_recon(src, seed + 19)
+    return src, rec
+
+
+def _cand(oracle_lib, src, rec, prm, q, qm, c, jb, t):
+    px, py = int(jb["px"]), int(jb["py"])
+    fl = int(jb["flags"])
+    pred = oracle_lib.intra_predict(rec, px, py, 8, 8, int(jb["mode"]), int(jb["angle_delta"]), bool(fl & 1),
+                                    bool(fl & 2), bool(fl & 4)).ravel()
+    resid = src[py:py + 8, px:px + 8].astype(np.int32).ravel() - pred
+    cf, tf = oracle_lib.fwd_txfm_quant(resid, t, q, qm)
+    if t in (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_ADST_DCT, abi.TX_DCT_ADST):
+        cf = oracle_lib.trellis_optimize_ctx(cf, tf, q, qm, c, int(jb["dcs_ctx"]), prm.trellis_lambda0,
+                                             band_tilt=prm.band_tilt)
+    rr = oracle_lib.inv_txfm_dequant(cf, t, q, qm)
+    sse = int(oracle_lib.sse_recon(src, prm.frame_w, prm.frame_h, [(px, py)], pred, rr, 8, 8,
+                                   scale=prm.wsse_scale)[0])
+    return cf, sse
+
+
+def test_leaf8_oracle_glue(oracle_lib):
+    import maroontree_b200 as mt
+
+    src, rec = _frame(48, 40, 51)
+    q = oracle_lib.quant_new(70, 8, 15)
+    c = luma_tx8_cdfs()
+    prm = mt.split16_params(48, 40, trellis_lambda0=0.05, rd_lambda=18.0, band_tilt=1.9, tx_search=True,
+                            tx_guard_shift=5)
+    jobs = synth.leaf8_jobs(48, 40, (abi.DC_PRED, abi.V_PRED, abi.D203_PRED, abi.SMOOTH_V_PRED), deltas=(0, 1),
+                            seed=3)
+    scan = oracle_lib.default_scan(8)
+    f32 = np.float32
+    rd = lambda d, b: f32(f32(d) + f32(f32(prm.rd_lambda) * f32(b)))
+    res, _, _ = oracle_lib.leaf8(src, rec, prm, q, None, c, jobs)
+    ref, _, _ = oracle_lib.leaf8(src, rec, prm, q, None, c, jobs, refine=True)
+    seen = set()
+    for i, jb in enumerate(jobs):
+        m, ds = int(jb["mode"]), int(jb["dcs_ctx"])
+        cf, sse = _cand(oracle_lib, src, rec, prm, q, None, c, jb, abi.TX_DCT_DCT)
+        bits = f32(oracle_lib.real_block_bits_bounded(cf, scan, 8, 8, c, 0, ds, m, abi.TX_DCT_DCT, INF))
+        assert res["sse"][i] == sse and f32(res["bits"][i]) == bits
+        assert f32(res["cost"][i]) == rd(sse, f32(bits + f32(jb["syntax_bits"])))
+        # the refinement's sequence
+        dct = (sse, bits)
+        best = (sse, bits, abi.TX_DCT_DCT)
+        for t in (abi.TX_ADST_ADST, abi.TX_ADST_DCT, abi.TX_DCT_ADST, abi.TX_IDTX, abi.TX_V_DCT, abi.TX_H_DCT):
+            acf, asse = _cand(oracle_lib, src, rec, prm, q, None, c, jb, t)
+            base = rd(best[0], best[1])
+            if t in (abi.TX_V_DCT, abi.TX_H_DCT):
+                ab = f32(oracle_lib.luma_bits_1d(acf, 8, t == abi.TX_V_DCT, c, ds, m))
+                gate = asse <= best[0]
+            elif t == abi.TX_IDTX:
+                ab = f32(oracle_lib.real_block_bits_bounded(acf, scan, 8, 8, c, 0, ds, m, t, INF))
+                gate = asse <= best[0] + (best[0] >> prm.tx_guard_shift)
+            else:
+                bound = float(f32(f32(base - f32(asse)) / f32(prm.rd_lambda)))
+                ab = f32(oracle_lib.real_block_bits_bounded(acf, scan, 8, 8, c, 0, ds, m, t, bound))
+                gate = asse <= dct[0] + (dct[0] >> prm.tx_guard_shift)
+            if gate and rd(asse, ab) < base:
+                best = (asse, ab, t)
+        assert (ref["sse"][i], f32(ref["bits"][i]), ref["tx_type"][i]) == best, i
+        seen.add(best[2])
+    assert len(seen) >= 3, seen
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("refine", [False, True])
+@pytest.mark.parametrize("qidx,qm_level,search,wsse,cdfs", [
+    (70, 6, True, 0.0, "luma"), (116, 15, False, 1.0, "luma"), (30, 3, True, 0.75, "synthetic"),
+    (200, 8, True, 0.0, "synthetic")])
+def test_leaf8_gpu_matches_oracle(mt_lib, oracle_lib, cuda, refine, qidx, qm_level, search, wsse, cdfs):
+    import maroontree_b200 as mt
+
+    src, rec = _frame(160, 96, qidx)
+    q = oracle_lib.quant_new(qidx, 8, qm_level)
+    qm = oracle_lib.qm_row(qm_level, 0, 8) if qm_level < 15 else None
+    c = luma_tx8_cdfs() if cdfs == "luma" else synth.synthetic_cdfs(qidx + 5)
+    jobs = synth.leaf8_jobs(160, 96, range(13), deltas=(-2, 0, 3), seed=qidx)
+    jobs["px"][7] = 156  # crosses the right edge: rejected
+    prm = mt.split16_params(160, 96, trellis_lambda0=0.05, rd_lambda=0.3 * qidx + 2.0, band_tilt=1.9,
+                            wsse_scale=wsse, tx_search=search, tx_guard_shift=5 if search else 4,
+                            skip_bits=[(2.0, 0.3)] + [(0.0, 0.0)] * 12, vis=(157, 94))
+    res, cf, recs = mt_lib.leaf8(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs, refine=refine, want_cf=True,
+                                 want_rec=True)
+    want, wcf, wrec = oracle_lib.leaf8(src, rec, prm, q, qm, c, jobs, refine=refine)
+    assert res.tobytes() == want.tobytes()
+    assert np.array_equal(cf, wcf) and np.array_equal(recs, wrec)
+    assert res["tx_type"][7] == 255
+    if refine:
+        assert len(np.unique(res["tx_type"])) >= 4
