@@ -356,12 +356,14 @@ def measure_split16(dev, wl, search, reps=5, cpu=True, depth2=False):
     return out
 
 
-def measure_leaf8(dev, wl, refine, reps=5, cpu=True):
+def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     """The 8x8 leaf's luma search over the same 1080p luma: the mode loop's
     candidates (32,400 blocks x 13 modes, DCT_DCT with trellis_optimize_ctx and
     sse_recon) or the winners' transform-type refinement (32,400 blocks, seven
     types, 4:4:4 form).  Device time with CUDA events after an L2 flush; the
-    oracle on all host cores over the same jobs."""
+    oracle on all host cores over the same jobs.  n16: the 16x16 leaf's
+    mode-loop candidates (8,040 blocks x 13 modes, trellis_optimize_ctx at
+    TX_16X16)."""
     import ctypes as C
 
     import torch
@@ -369,10 +371,10 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True):
     from maroontree_b200 import abi, synth
 
     q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 8)
-    cdfs = synth.synthetic_cdfs(4)
+    qm = mt.qm_row(QM_LEVEL, 0, 16 if n16 else 8)
+    cdfs = synth.synthetic_cdfs(4, n_eob_bins=9) if n16 else synth.synthetic_cdfs(4)
     costs = mt.coef_costs(cdfs)
-    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=3)
+    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=3, n=16 if n16 else 8)
     n = len(jobs)
     prm = mt.split16_params(W, H, trellis_lambda0=0.05, rd_lambda=wl["prm"].mode_lambda, band_tilt=1.9,
                             tx_search=refine, tx_guard_shift=5)
@@ -382,7 +384,7 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True):
     d_res = torch.empty(n * abi.LEAF8_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lib = mt.load()
-    entry = lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device
+    entry = lib.mt_leaf16_luma_device if n16 else (lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device)
 
     def launch():
         rc = entry(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q), d_qm.data_ptr(), d_costs.data_ptr(),
@@ -405,12 +407,17 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True):
     step = float(np.median(ms))
     what = ("leaf8 winners' transform-type refinement 1920x1080 luma, 32,400 blocks, 7 types" if refine else
             "leaf8 mode-loop candidates 1920x1080 luma, 32,400 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)")
+    if n16:
+        what = "leaf16 mode-loop candidates 1920x1080 luma, 8,040 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)"
     out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n, "workload": what}
     if cpu:
         from oracle import pyoracle as po
 
         t0 = time.perf_counter()
-        po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
+        if n16:
+            po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs)
+        else:
+            po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": 1, "kind": "port",
                                "sample": f"all {n} jobs ({dt:.2f} s)"}
@@ -655,6 +662,8 @@ def run_ours(args):
         split16["depth2"] = measure_split16(dev, wl, False, cpu=world == 1 and not args.no_cpu, depth2=True)
     leaf8 = {k: measure_leaf8(dev, wl, k == "refine", cpu=world == 1 and not args.no_cpu)
              for k in ("luma", "refine")} if rank == 0 else None
+    if leaf8 is not None:
+        leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=world == 1 and not args.no_cpu, n16=True)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -1,6 +1,7 @@
-// The 8x8 leaf's luma search (pick_block8, src/coder/block8.rs:689-1420),
-// batched: the Slow mode loop's candidates (leaf8_kernel<false>) and the
-// winner's transform-type refinement (leaf8_kernel<true>), one thread per job.
+// The leaf luma searches, batched, one thread per job: pick_block8's
+// (src/coder/block8.rs:689-1420) Slow mode-loop candidates (leaf_kernel<8,
+// false>) and winner transform-type refinement (leaf_kernel<8, true>), and
+// pick_luma16's mode-loop candidates (leaf_kernel<16, false>).
 // The stages are the split trial's (leaf8.cuh): DCT_DCT + QM with
 // trellis_optimize_ctx, the dav1d inverse, sse_recon, the bounded 2-D and the
 // 1-D rate walks; every type runs through one loop body with the candidate and
@@ -29,35 +30,43 @@ struct LeafArgs {
   int has_qm;
 };
 
+// Per-thread working set of one N x N job.  u: the prediction edges, then the
+// targets [0, N*N) and the transform temporary [N*N, 2*N*N).
+template <int N>
 struct LeafWork {
-  int32_t u[128];  // prediction edges, then targets [0, 64) and the transform temporary [64, 128)
-  int16_t pred[64], resid[64];
-  int16_t cfs[2][64], rrs[2][64];
-  TrellisCtxScratch tr;
-  uint8_t lv[160];
+  int32_t u[2 * N * N];
+  int16_t pred[N * N], resid[N * N];
+  int16_t cfs[2][N * N], rrs[2][N * N];  // levels / inverse of the candidate and of the winner
+  TrellisCtxScratchW<N> tr;
+  uint8_t lv[N == 8 ? 160 : (N + 2) * N];  // rate walks' level maps
 };
 
 __device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate) {
   return __fadd_rn((float)d, __fmul_rn(lam, rate));
 }
 
-template <bool REFINE>
-__global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
+// N = 8: pick_block8's candidates (REFINE = false) and winner refinement
+// (REFINE = true); N = 16: pick_luma16's mode-loop candidates
+// (src/coder/partition_search.rs:4802-4880).
+template <int N, bool REFINE>
+__global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_leaf8_job* __restrict__ jobs, int n, mt_leaf8_result* __restrict__ res, int32_t* __restrict__ cf_out,
     uint16_t* __restrict__ rec_out) {
   __shared__ mt_coef_costs sT;
-  __shared__ uint8_t sQm[64];
-  __shared__ float sQs[64];
+  static_assert(N == 8 || (N == 16 && !REFINE), "8x8 candidates and refinement, 16x16 candidates");
+  constexpr int NN = N * N, L = N == 8 ? 3 : 4;
+  __shared__ uint8_t sQm[NN];
+  __shared__ float sQs[NN];
   {
     const float* g = reinterpret_cast<const float*>(costs);
     float* s = reinterpret_cast<float*>(&sT);
     for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
-    if (threadIdx.x < 64) {
-      const int w = a.has_qm ? qm_row[threadIdx.x] : 32;
-      sQm[threadIdx.x] = (uint8_t)w;
-      sQs[threadIdx.x] = fwd_qm_scale(w);
+    for (int i = threadIdx.x; i < NN; i += blockDim.x) {
+      const int w = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)w;
+      sQs[i] = fwd_qm_scale(w);
     }
     __syncthreads();
   }
@@ -69,7 +78,7 @@ __global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
   const uint8_t* qm = a.has_qm ? sQm : nullptr;
   const mt_leaf8_job jb = jobs[j];
   mt_leaf8_result& r = res[j];
-  const bool ok = jb.px + 8 <= p.frame_w && jb.py + 8 <= p.frame_h && jb.mode <= MT_PAETH_PRED &&
+  const bool ok = jb.px + N <= p.frame_w && jb.py + N <= p.frame_h && jb.mode <= MT_PAETH_PRED &&
                   jb.angle_delta >= -3 && jb.angle_delta <= 3 &&
                   (jb.angle_delta == 0 || (jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED)) && jb.dcs_ctx < 3;
   if (!ok) {
@@ -78,34 +87,34 @@ __global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
     r.tx_type = 255;
     for (int i = 0; i < 7; i++) r.reserved[i] = 0;
     if (cf_out)
-      for (int i = 0; i < 64; i++) cf_out[(size_t)j * 64 + i] = 0;
+      for (int i = 0; i < NN; i++) cf_out[(size_t)j * NN + i] = 0;
     if (rec_out)
-      for (int i = 0; i < 64; i++) rec_out[(size_t)j * 64 + i] = 0;
+      for (int i = 0; i < NN; i++) rec_out[(size_t)j * NN + i] = 0;
     return;
   }
-  LeafWork w;
+  LeafWork<N> w;
   const int32_t maxv = (1 << p.bd) - 1;
   const float dcq = (float)q.dc_q, acq = (float)q.ac_q, rd_lam = p.rd_lambda;
   const bool qm_full = q.qm_level >= 5;
   const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
-  predict_sq<8>(rec, p.stride, p.frame_w, p.frame_h, jb.px, jb.py, jb.mode, jb.angle_delta, jb.flags & 1,
+  predict_sq<N>(rec, p.stride, p.frame_w, p.frame_h, jb.px, jb.py, jb.mode, jb.angle_delta, jb.flags & 1,
                 (jb.flags >> 1) & 1, (jb.flags >> 2) & 1, p.bd, w.pred, w.u);
 #pragma unroll 8
-  for (int i = 0; i < 64; i++)
-    w.resid[i] = (int16_t)((int32_t)src[(size_t)(jb.py + (i >> 3)) * p.stride + jb.px + (i & 7)] - w.pred[i]);
+  for (int i = 0; i < NN; i++)
+    w.resid[i] = (int16_t)((int32_t)src[(size_t)(jb.py + (i >> L)) * p.stride + jb.px + (i & (N - 1))] - w.pred[i]);
   const int ds = jb.dcs_ctx;
   ErrBlock<int16_t, int16_t> eb;
   eb.src = src + (size_t)jb.py * p.stride + jb.px;
   eb.stride = p.stride;
   eb.pred = w.pred;
-  eb.w = 8;
-  eb.vw = min(max(vis_w - jb.px, 0), 8);
-  eb.vh = min(max(vis_h - jb.py, 0), 8);
+  eb.w = N;
+  eb.vw = min(max(vis_w - jb.px, 0), N);
+  eb.vh = min(max(vis_h - jb.py, 0), N);
   eb.maxv = maxv;
   const float skip1 = p.use_skip_bits ? p.skip_bits[0][0] : 0.0f;
   const float skip0 = p.use_skip_bits ? p.skip_bits[0][1] : 0.0f;
   float* tf = reinterpret_cast<float*>(w.u);
-  int32_t* tmp = w.u + 64;
+  int32_t* tmp = w.u + NN;
   // DCT_DCT, then (refinement) ADST_ADST, ADST_DCT, DCT_ADST, IDTX[, V_DCT,
   // H_DCT]; nibble k: the k-th type.
   constexpr uint32_t kTypeOrder = 0x3206541u;
@@ -119,12 +128,14 @@ __global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
     const int cur = k == 0 ? 0 : 1 - best;
     int16_t* cf = w.cfs[cur];
     int16_t* rr = w.rrs[cur];
-    fwd8x8(w.resid, t, q, cf, tf, tmp);
+    if (N == 8) fwd8x8(w.resid, t, q, cf, tf, tmp);
+    else fwd16x16(w.resid, t, q, cf, tf, tmp);
     if (t == MT_TX_DCT_DCT || t >= MT_TX_ADST_ADST) {
-      if (qm) apply_qm(cf, tf, sQs, 64);
-      if (a.lambda > 0.0f) trellis_ctx8(cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
+      if (qm) apply_qm(cf, tf, sQs, NN);
+      if (a.lambda > 0.0f) trellis_ctx<N>(cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
     }
-    inv8x8(cf, t, q, qm, rr, tmp);
+    if (N == 8) inv8x8(cf, t, q, qm, rr, tmp);
+    else inv16x16(cf, t, q, qm, rr, tmp);
     eb.resid = rr;
     const long long asse = sse_recon_block(eb, p.wsse_scale);
     if (k > 0) {
@@ -139,12 +150,12 @@ __global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
     }
     const float base_rd = k == 0 ? 0.0f : rd_cost_i64(bsse, rd_lam, bbits);
     float abits;
-    if (t == MT_TX_V_DCT || t == MT_TX_H_DCT) {
+    if (N == 8 && (t == MT_TX_V_DCT || t == MT_TX_H_DCT)) {
       abits = rate_1d<8>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
     } else {
       const float bound = (k == 0 || t == MT_TX_IDTX) ? __int_as_float(0x7f800000)
                                                       : __fdiv_rn(__fsub_rn(base_rd, (float)asse), rd_lam);
-      abits = rate_bounded<8>(cf, T, 0, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
+      abits = rate_bounded<N>(cf, T, 0, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
     }
     if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < base_rd) {
       best = cur;
@@ -165,21 +176,21 @@ __global__ void __launch_bounds__(kLeafThreads) leaf8_kernel(
   const int16_t* bcf = w.cfs[best];
   const int16_t* brr = w.rrs[best];
   if (cf_out) {
-    int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * 64);
-#pragma unroll
-    for (int i = 0; i < 16; i++) o[i] = make_int4(bcf[4 * i], bcf[4 * i + 1], bcf[4 * i + 2], bcf[4 * i + 3]);
+    int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * NN);
+#pragma unroll 4
+    for (int i = 0; i < NN / 4; i++) o[i] = make_int4(bcf[4 * i], bcf[4 * i + 1], bcf[4 * i + 2], bcf[4 * i + 3]);
   }
   if (rec_out) {
-    uint16_t* o = rec_out + (size_t)j * 64;
+    uint16_t* o = rec_out + (size_t)j * NN;
 #pragma unroll 8
-    for (int i = 0; i < 64; i++) o[i] = (uint16_t)clampi((int32_t)w.pred[i] + brr[i], 0, maxv);
+    for (int i = 0; i < NN; i++) o[i] = (uint16_t)clampi((int32_t)w.pred[i] + brr[i], 0, maxv);
   }
 }
 
 int check(const mt_split16_params* p, const mt_quant* q, int32_t n) {
   if (!p || !q || n < 0) return MT_ERR_INVALID_INPUT;
   if (p->bd != 8) return MT_ERR_UNSUPPORTED;
-  if (p->frame_w < 8 || p->frame_h < 8 || p->stride < p->frame_w || p->vis_w < 0 || p->vis_h < 0)
+  if (p->frame_w < 4 || p->frame_h < 4 || p->stride < p->frame_w || p->vis_w < 0 || p->vis_h < 0)
     return MT_ERR_INVALID_INPUT;
   if (!(p->rd_lambda > 0.0f) || !(p->wsse_scale >= 0.0f) || p->tx_guard_shift < 0) return MT_ERR_INVALID_INPUT;
   return MT_OK;
@@ -187,8 +198,8 @@ int check(const mt_split16_params* p, const mt_quant* q, int32_t n) {
 
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
 
-template <bool REFINE>
-int leaf8_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm, const mt_quant* quant,
+template <int N, bool REFINE>
+int leaf_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm, const mt_quant* quant,
                  const uint8_t* d_qm_row, const mt_coef_costs* d_costs, const mt_leaf8_job* d_jobs, int32_t n,
                  mt_leaf8_result* d_results, int32_t* d_cf, uint16_t* d_rec, void* stream) {
   const int rc = check(prm, quant, n);
@@ -201,11 +212,16 @@ int leaf8_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split1
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  leaf8_kernel<REFINE><<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+  leaf_kernel<N, REFINE><<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
                          reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
                                                                    d_results, d_cf, d_rec);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
+
+template <int N>
+int leaf_host(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 
 }  // namespace
 
@@ -215,52 +231,83 @@ int mt_leaf8_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const m
                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                          const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
                          uint16_t* d_rec, void* stream) {
-  return leaf8_device<false>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
+  return leaf_device<8, false>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
 }
 
 int mt_leaf8_tx_refine_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
                               const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                               const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
                               uint16_t* d_rec, void* stream) {
-  return leaf8_device<true>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
+  return leaf_device<8, true>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
 }
 
 int mt_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_host<8>(src, recon, prm, quant, qm_row, costs, jobs, n, refine, results, cf_out, rec_out);
+}
+
+int mt_leaf16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                          uint16_t* d_rec, void* stream) {
+  return leaf_device<16, false>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec,
+                                stream);
+}
+
+int mt_leaf16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
+                   mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_host<16>(src, recon, prm, quant, qm_row, costs, jobs, n, 0, results, cf_out, rec_out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Host-buffer form of the leaf searches.
+template <int N>
+int leaf_host(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  constexpr size_t NN = (size_t)N * N;
   int rc = check(prm, quant, n);
   if (rc != MT_OK) return rc;
   if (n == 0) return MT_OK;
   if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
   const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
-  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + 256;
+  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + up256(NN);
   const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
   const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_leaf8_job));
   const size_t o_cf = o_res + up256((size_t)n * sizeof(mt_leaf8_result));
-  const size_t o_out = o_cf + (cf_out ? up256((size_t)n * 64 * 4) : 0);
-  const size_t total = o_out + (rec_out ? up256((size_t)n * 64 * 2) : 0);
+  const size_t o_out = o_cf + (cf_out ? up256((size_t)n * NN * 4) : 0);
+  const size_t total = o_out + (rec_out ? up256((size_t)n * NN * 2) : 0);
   uint8_t* d = nullptr;
   if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
   const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
   cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 64, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, NN, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_leaf8_job), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    auto fn = refine ? leaf8_device<true> : leaf8_device<false>;
+    auto fn = (N == 8 && refine) ? leaf_device<8, true> : leaf_device<N, false>;
     rc = fn(reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant,
             has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
             reinterpret_cast<const mt_leaf8_job*>(d + o_jobs), n, reinterpret_cast<mt_leaf8_result*>(d + o_res),
             cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr,
             rec_out ? reinterpret_cast<uint16_t*>(d + o_out) : nullptr, nullptr);
     if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_leaf8_result), cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 256, cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && rec_out) e = cudaMemcpy(rec_out, d + o_out, (size_t)n * 128, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out) e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * NN * 4, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && rec_out) e = cudaMemcpy(rec_out, d + o_out, (size_t)n * NN * 2, cudaMemcpyDeviceToHost);
   }
   cudaFree(d);
   if (rc != MT_OK) return rc;
   return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
+
+}  // namespace
+
+extern "C" {
 
 }  // extern "C"

@@ -16,6 +16,7 @@
 
 #include "chain4.cuh"
 #include "chain8.cuh"
+#include "chain16.cuh"
 
 namespace mtd {
 
@@ -27,27 +28,37 @@ __device__ __forceinline__ float hi_cost(const mt_coef_costs& T, uint32_t m, int
   return h;
 }
 
-// Scratch of trellis_ctx8: the zero-distortion suffix sums and the level map
-// (stride 8 with the reference's two zero columns of padding).
-struct TrellisCtxScratch {
-  float suf0[65];
-  uint8_t lv[80];
-};
+// Default scan of a W x W block (scan index -> rc = x*W + y).
+template <int W>
+__device__ __forceinline__ int scan_rc(int i) {
+  return W == 4 ? kScan4[i] : (W == 8 ? kScan8[i] : kScan16[i]);
+}
 
-// trellis_optimize_ctx of one TX_8X8 luma block (class 1, plane 0) under the
+// Scratch of trellis_ctx<W>: the zero-distortion suffix sums and the level map
+// (stride W with the reference's two zero columns of padding).
+template <int W>
+struct TrellisCtxScratchW {
+  float suf0[W * W + 1];
+  uint8_t lv[(W + 2) * W];
+};
+using TrellisCtxScratch = TrellisCtxScratchW<8>;
+
+// trellis_optimize_ctx of one TX_WxW luma block (W = 8: class 1, 16: class 2;
+// plane 0; the cost slice of that class) under the
 // shipped tuning: trellis_aom / eob_reprice / eob_zero_term / pad_stride off,
 // dead zone 0, the DC-only terminal in eob_base context 0 with br context 0,
 // skip priced at trellis_zero_bits = 1, tilt magnitude cap 2.  `lambda` is
 // scaled_trellis_lambda (src/trellis.rs:50-53); qm (NULL = flat) the inverse
 // QM row, weighted w/32 and squared from QM level 5 (qm_full).
-template <typename C>
-__device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, float dc_q, float ac_q, float lambda,
-                             const mt_coef_costs& T, int dcs, const uint8_t* __restrict__ qm, bool qm_full,
-                             float band_t, TrellisCtxScratch& s) {
-  constexpr float kCap = 2.0f, kNInv = 1.0f / 64.0f;
+template <int W, typename C>
+__device__ void trellis_ctx(C* __restrict__ cf, const float* __restrict__ tf, float dc_q, float ac_q, float lambda,
+                            const mt_coef_costs& T, int dcs, const uint8_t* __restrict__ qm, bool qm_full,
+                            float band_t, TrellisCtxScratchW<W>& s) {
+  constexpr int N = W * W, L = W == 4 ? 2 : (W == 8 ? 3 : 4);
+  constexpr float kCap = 2.0f, kNInv = 1.0f / (float)N;
   int eob = -1;
-  for (int i = 63; i >= 0; i--)
-    if (cf[kScan8[i]] != 0) {
+  for (int i = N - 1; i >= 0; i--)
+    if (cf[scan_rc<W>(i)] != 0) {
       eob = i;
       break;
     }
@@ -68,29 +79,29 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
     return d;
   };
   uint8_t* lv = s.lv;
-#pragma unroll
-  for (int i = 0; i < 20; i++) reinterpret_cast<uint32_t*>(lv)[i] = 0;
+#pragma unroll 4
+  for (int i = 0; i < (W + 2) * W / 4; i++) reinterpret_cast<uint32_t*>(lv)[i] = 0;
   for (int i = 0; i <= eob; i++) {
-    const int rc = kScan8[i];
+    const int rc = scan_rc<W>(i);
     lv[rc] = (uint8_t)level_byte(uabs(cf[rc]));
   }
   auto interior_ctx = [&](int rc, int& bc) -> int {
-    const int x = rc >> 3, y = rc & 7;
-    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + 8] + lv[rc + 9];
-    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 16];
+    const int x = rc >> L, y = rc & (W - 1);
+    const uint32_t hm = (uint32_t)lv[rc + 1] + lv[rc + W] + lv[rc + W + 1];
+    const uint32_t mag = hm + lv[rc + 2] + lv[rc + 2 * W];
     const uint32_t hm6 = hm & 63;
     bc = ((y | x) > 1 ? 14 : 7) + (hm6 > 12 ? 6 : (int)((hm6 + 1) >> 1));
     return kLoCtxOff[min(y, 4) * 5 + min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
   };
   auto dc_brc = [&]() -> int {
-    const uint32_t mag = ((uint32_t)lv[1] + lv[8] + lv[9]) & 63;
+    const uint32_t mag = ((uint32_t)lv[1] + lv[W] + lv[W + 1]) & 63;
     return mag > 12 ? 6 : (int)((mag + 1) >> 1);
   };
 
   // Step A (src/trellis.rs:514-602): reverse-scan RD-best level per interior
   // coefficient below the last nonzero, then DC.
   for (int i = eob - 1; i >= 1; i--) {
-    const int rc = kScan8[i];
+    const int rc = scan_rc<W>(i);
     const uint32_t l = uabs(cf[rc]);
     if (l == 0) continue;
     int bc;
@@ -151,7 +162,7 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
   // the QM and multiplied by the reciprocal tilt factor.
   const int m = eob + 1;
   auto dist_pair = [&](int i, float& cur, float& zero) {
-    const int rc = kScan8[i];
+    const int rc = scan_rc<W>(i);
     const float dq2 = rc == 0 ? dq2_dc : dq2_ac;
     const float at = fabsf(tf[rc]);
     const float e = __fsub_rn(at, (float)uabs(cf[rc]));
@@ -186,12 +197,12 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
   uint32_t best_m = 0;
   float best_cost = __int_as_float(0x7f800000);
   auto eob_coeff_cost = [&](int e, uint32_t k) -> float {
-    const int ctx_e = 1 + (e > 8) + (e > 16);
+    const int ctx_e = 1 + (e > (N >> 3)) + (e > (N >> 2));
     const uint32_t tok = min(k, 3u);
     float c = T.eob_base[ctx_e][tok - 1];
     if (tok == 3) {
-      const int rc = kScan8[e];
-      c = __fadd_rn(c, hi_cost(T, k, ((rc >> 3) | (rc & 7)) > 1 ? 14 : 7));
+      const int rc = scan_rc<W>(e);
+      c = __fadd_rn(c, hi_cost(T, k, ((rc >> L) | (rc & (W - 1))) > 1 ? 14 : 7));
     }
     return __fadd_rn(c, 1.0f);
   };
@@ -206,7 +217,7 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
     return c;
   };
   auto eob_cand = [&](int e, uint32_t k) -> float {
-    return __fadd_rn(__fmul_rn(lambda, eob_coeff_cost(e, k)), distw(e, kScan8[e], k));
+    return __fadd_rn(__fmul_rn(lambda, eob_coeff_cost(e, k)), distw(e, scan_rc<W>(e), k));
   };
   {
     float dc_cost;
@@ -224,7 +235,7 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
     // running sum in the reference's order (src/trellis.rs:849-868).
     float acc = 0.0f;
     for (int e = 1; e < m; e++) {
-      const int rc = kScan8[e];
+      const int rc = scan_rc<W>(e);
       const uint32_t k = uabs(cf[rc]);
       if (k != 0) {
         const float base =
@@ -272,21 +283,23 @@ __device__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, f
   }
   const float skip_cost = __fadd_rn(__fadd_rn(suf0[1], dist_zero0), __fmul_rn(lambda, 1.0f));
   if (best_e < 0 || skip_cost < best_cost) {
-    for (int i = 0; i < m; i++) cf[kScan8[i]] = 0;
+    for (int i = 0; i < m; i++) cf[scan_rc<W>(i)] = 0;
   } else {
-    const int rc = kScan8[best_e];
+    const int rc = scan_rc<W>(best_e);
     if (best_m != uabs(cf[rc])) {
       const bool neg = cf[rc] != 0 ? cf[rc] < 0 : tf[rc] < 0.0f;
       cf[rc] = (C)(neg ? -(int32_t)best_m : (int32_t)best_m);
     }
-    for (int i = best_e + 1; i < m; i++) cf[kScan8[i]] = 0;
+    for (int i = best_e + 1; i < m; i++) cf[scan_rc<W>(i)] = 0;
   }
 }
 
-// Default scan of a W x W block (scan index -> rc = x*W + y).
-template <int W>
-__device__ __forceinline__ int scan_rc(int i) {
-  return W == 4 ? kScan4[i] : kScan8[i];
+template <typename C>
+__device__ __forceinline__ void trellis_ctx8(C* __restrict__ cf, const float* __restrict__ tf, float dc_q, float ac_q,
+                                             float lambda, const mt_coef_costs& T, int dcs,
+                                             const uint8_t* __restrict__ qm, bool qm_full, float band_t,
+                                             TrellisCtxScratch& s) {
+  trellis_ctx<8>(cf, tf, dc_q, ac_q, lambda, T, dcs, qm, qm_full, band_t, s);
 }
 
 // real_block_bits_bounded of a TX_WxW luma block (W = 4: class TX_4X4, 8:
@@ -327,7 +340,7 @@ __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, 
   uint32_t* lv32 = reinterpret_cast<uint32_t*>(lv);
 #pragma unroll
   for (int i = 0; i < (W + 2) * W / 4; i++) lv32[i] = 0;
-  constexpr int L = W == 4 ? 2 : 3;
+  constexpr int L = W == 4 ? 2 : (W == 8 ? 3 : 4);
   const int ctx_e = 1 + (eob > (W * W >> 3)) + (eob > (W * W >> 2));
   {
     const int rc = scan_rc<W>(eob);
@@ -378,7 +391,7 @@ __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, 
 template <int W, typename C>
 __device__ float rate_1d(const C* __restrict__ cf, bool vertical, const mt_coef_costs& T, int dcs, int mode,
                           uint8_t* __restrict__ lv) {
-  constexpr int L = W == 4 ? 2 : 3;
+  constexpr int L = W == 4 ? 2 : (W == 8 ? 3 : 4);
   auto pos_rc = [&](int i) -> int { return vertical ? ((i & (W - 1)) << L) | (i >> L) : i; };
   int eob = -1;
   for (int i = W * W - 1; i >= 0; i--)

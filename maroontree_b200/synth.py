@@ -482,14 +482,15 @@ def split16_jobs(fw, fh, modes, deltas=(0,), seed=0, n=16):
     return np.array(rows, abi.SPLIT16_JOB_DTYPE)
 
 
-def leaf8_jobs(fw, fh, modes, deltas=(0,), seed=0):
-    """(8x8 block, mode, delta) jobs of the 8x8 leaf's luma search, mode-major,
-    with deterministic neighbour flags, random dc_sign contexts and syntax bits."""
+def leaf8_jobs(fw, fh, modes, deltas=(0,), seed=0, n=8):
+    """(n x n block, mode, delta) jobs of the leaf luma searches (n = 8 or 16),
+    mode-major, with deterministic neighbour flags, random dc_sign contexts and
+    syntax bits."""
     rng = np.random.default_rng(seed)
-    bys, bxs = np.meshgrid(np.arange(0, fh - 7, 8), np.arange(0, fw - 7, 8), indexing="ij")
+    bys, bxs = np.meshgrid(np.arange(0, fh - n + 1, n), np.arange(0, fw - n + 1, n), indexing="ij")
     px, py = bxs.ravel(), bys.ravel()
     nb = len(px)
-    flags = np.array([block_flags(int(x), int(y), fw, fh, 8) for x, y in zip(px, py)], np.uint8)
+    flags = np.array([block_flags(int(x), int(y), fw, fh, n) for x, y in zip(px, py)], np.uint8)
     flags |= np.where(rng.random(nb) < 0.5, abi.CAND_FILTER_TYPE, 0).astype(np.uint8)
     dcs = rng.integers(0, 3, size=nb)
     rows = []

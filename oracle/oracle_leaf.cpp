@@ -889,12 +889,13 @@ extern "C" {
 // block8.rs:738-808 (refine = 0: the Slow mode loop's candidate) and
 // :1183-1404 (refine = 1: the winner's transform-type refinement) of
 // pick_block8, over a batch of 8x8 jobs.
-int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
-             const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
-             mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+                     mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
   if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int NN = N * N;
   const int32_t maxv = (1 << p->bd) - 1;
-  const uint16_t* scan = or_default_scan(8);
+  const uint16_t* scan = or_default_scan(N);
   const float dcq = (float)q->dc_q, acq = (float)q->ac_q, mlam = p->rd_lambda;
   const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
   const float* skip = p->use_skip_bits ? p->skip_bits[0] : nullptr;
@@ -903,54 +904,54 @@ int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params
     const mt_leaf8_job& jb = jobs[i];
     mt_leaf8_result* r = &results[i];
     memset(r->reserved, 0, sizeof(r->reserved));
-    const bool bad = jb.px + 8 > p->frame_w || jb.py + 8 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+    const bool bad = jb.px + N > p->frame_w || jb.py + N > p->frame_h || jb.mode > MT_PAETH_PRED ||
                      jb.angle_delta < -3 || jb.angle_delta > 3 ||
                      (jb.angle_delta != 0 && (jb.mode < MT_V_PRED || jb.mode > MT_D67_PRED)) || jb.dcs_ctx > 2;
     if (bad) {
       r->sse = 0;
       r->bits = r->cost = INFINITY;
       r->tx_type = 255;
-      if (cf_out) memset(cf_out + (size_t)i * 64, 0, 256);
-      if (rec_out) memset(rec_out + (size_t)i * 64, 0, 128);
+      if (cf_out) memset(cf_out + (size_t)i * NN, 0, NN * 4);
+      if (rec_out) memset(rec_out + (size_t)i * NN, 0, NN * 2);
       continue;
     }
-    int32_t pred[64];
+    int32_t pred[256];
     if (jb.mode == MT_DC_PRED) {
-      const int32_t d = or_dc_pred(recon, p->stride, jb.px, jb.py, 8, 8, p->bd);
-      for (int k = 0; k < 64; k++) pred[k] = d;
+      const int32_t d = or_dc_pred(recon, p->stride, jb.px, jb.py, N, N, p->bd);
+      for (int k = 0; k < NN; k++) pred[k] = d;
     } else {
-      or_intra_predict(recon, p->stride, jb.px, jb.py, 8, 8, jb.mode, jb.angle_delta, jb.flags & 1,
+      or_intra_predict(recon, p->stride, jb.px, jb.py, N, N, jb.mode, jb.angle_delta, jb.flags & 1,
                        (jb.flags >> 1) & 1, p->frame_w, p->frame_h, (jb.flags >> 2) & 1, p->bd, pred);
     }
-    int32_t resid[64];
-    for (int y = 0; y < 8; y++)
-      for (int x = 0; x < 8; x++)
-        resid[y * 8 + x] = (int32_t)src[(size_t)(jb.py + y) * p->stride + jb.px + x] - pred[y * 8 + x];
+    int32_t resid[256];
+    for (int y = 0; y < N; y++)
+      for (int x = 0; x < N; x++)
+        resid[y * N + x] = (int32_t)src[(size_t)(jb.py + y) * p->stride + jb.px + x] - pred[y * N + x];
     const int ds = jb.dcs_ctx;
     const uint16_t pos[2] = {jb.px, jb.py};
     auto sse_of = [&](const int32_t* rr) -> int64_t {
       int64_t d = 0;
-      or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, 8, 8, p->wsse_scale, &d);
+      or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, N, N, p->wsse_scale, &d);
       return d;
     };
     auto bits2d = [&](const int32_t* cf, int t, float bound) -> float {
-      return or_real_block_bits_bounded(cf, scan, 8, 8, cd, 0, ds, jb.mode, t, p->use_skip_bits, skip, bound);
+      return or_real_block_bits_bounded(cf, scan, N, N, cd, 0, ds, jb.mode, t, p->use_skip_bits, skip, bound);
     };
     // The DCT_DCT candidate with the per-candidate trellis (block8.rs:780-805).
-    int32_t lcf[64], lrr[64];
-    float tf[64];
-    or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, 8, q, qm, lcf, tf);
-    or_trellis_optimize_ctx(lcf, tf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level, p->band_tilt);
-    or_inv_txfm_dequant(lcf, MT_TX_DCT_DCT, 8, q, qm, lrr);
+    int32_t lcf[256], lrr[256];
+    float tf[256];
+    or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, N, q, qm, lcf, tf);
+    or_trellis_optimize_ctx(lcf, tf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level, p->band_tilt);
+    or_inv_txfm_dequant(lcf, MT_TX_DCT_DCT, N, q, qm, lrr);
     const int64_t dct_sse = sse_of(lrr);
     const float dct_bits = bits2d(lcf, MT_TX_DCT_DCT, INFINITY);
     int64_t bsse = dct_sse;
     float bbits = dct_bits;
     uint8_t btx = MT_TX_DCT_DCT;
-    if (refine) {
+    if (refine && N == 8) {
       auto take = [&](const int32_t* cf, const int32_t* rr, int64_t s, float b, int t) {
-        memcpy(lcf, cf, sizeof(lcf));
-        memcpy(lrr, rr, sizeof(lrr));
+        memcpy(lcf, cf, 64 * sizeof(int32_t));
+        memcpy(lrr, rr, 64 * sizeof(int32_t));
         bsse = s;
         bbits = b;
         btx = (uint8_t)t;
@@ -1013,11 +1014,24 @@ int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params
     r->bits = bbits;
     r->cost = refine ? rd_cost_i64(bsse, mlam, bbits) : rd_cost_i64(bsse, mlam, bbits + jb.syntax_bits);
     r->tx_type = btx;
-    if (cf_out) memcpy(cf_out + (size_t)i * 64, lcf, sizeof(lcf));
+    if (cf_out) memcpy(cf_out + (size_t)i * NN, lcf, NN * sizeof(int32_t));
     if (rec_out)
-      for (int k = 0; k < 64; k++) rec_out[(size_t)i * 64 + k] = (uint16_t)clampi(pred[k] + lrr[k], 0, maxv);
+      for (int k = 0; k < NN; k++) rec_out[(size_t)i * NN + k] = (uint16_t)clampi(pred[k] + lrr[k], 0, maxv);
   }
   return MT_OK;
+}
+
+int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+             const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+             mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_impl(8, src, recon, p, q, qm, cd, jobs, n, refine, results, cf_out, rec_out);
+}
+
+// partition_search.rs:4802-4880 pick_luma16's mode-loop candidates.
+int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+              const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_impl(16, src, recon, p, q, qm, cd, jobs, n, 0, results, cf_out, rec_out);
 }
 
 }  // extern "C"

@@ -107,3 +107,52 @@ def test_leaf8_gpu_matches_oracle(mt_lib, oracle_lib, cuda, refine, qidx, qm_lev
     assert res["tx_type"][7] == 255
     if refine:
         assert len(np.unique(res["tx_type"])) >= 4
+
+
+def test_leaf16_oracle_glue(oracle_lib):
+    """pick_luma16's candidate (partition_search.rs:4802-4880): DCT_DCT + QM,
+    trellis_optimize_ctx at TX_16X16, sse_recon, luma_bits + syntax bits."""
+    import maroontree_b200 as mt
+
+    src, rec = _frame(64, 48, 61)
+    q = oracle_lib.quant_new(90, 8, 7)
+    qm = oracle_lib.qm_row(7, 0, 16)
+    c = synth.synthetic_cdfs(12, n_eob_bins=9)
+    prm = mt.split16_params(64, 48, trellis_lambda0=0.05, rd_lambda=25.0, band_tilt=2.2)
+    jobs = synth.leaf8_jobs(64, 48, (abi.DC_PRED, abi.D113_PRED, abi.SMOOTH_PRED), deltas=(0, -2), seed=9, n=16)
+    scan = oracle_lib.default_scan(16)
+    f32 = np.float32
+    res, cf, recs = oracle_lib.leaf16(src, rec, prm, q, qm, c, jobs)
+    for i, jb in enumerate(jobs):
+        px, py, fl = int(jb["px"]), int(jb["py"]), int(jb["flags"])
+        pred = oracle_lib.intra_predict(rec, px, py, 16, 16, int(jb["mode"]), int(jb["angle_delta"]), bool(fl & 1),
+                                        bool(fl & 2), bool(fl & 4)).ravel()
+        resid = src[py:py + 16, px:px + 16].astype(np.int32).ravel() - pred
+        lv, tf = oracle_lib.fwd_txfm_quant(resid, abi.TX_DCT_DCT, q, qm)
+        lv = oracle_lib.trellis_optimize_ctx(lv, tf, q, qm, c, int(jb["dcs_ctx"]), 0.05, band_tilt=2.2, n=16)
+        rr = oracle_lib.inv_txfm_dequant(lv, abi.TX_DCT_DCT, q, qm)
+        sse = int(oracle_lib.sse_recon(src, 64, 48, [(px, py)], pred, rr, 16, 16)[0])
+        bits = f32(oracle_lib.real_block_bits_bounded(lv, scan, 16, 16, c, 0, int(jb["dcs_ctx"]), int(jb["mode"]),
+                                                      abi.TX_DCT_DCT, INF))
+        assert res["sse"][i] == sse and f32(res["bits"][i]) == bits and np.array_equal(cf[i], lv), i
+        assert f32(res["cost"][i]) == f32(f32(sse) + f32(f32(25.0) * f32(bits + f32(jb["syntax_bits"]))))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qidx,qm_level,wsse", [(70, 6, 0.0), (116, 15, 1.0), (30, 3, 0.75)])
+def test_leaf16_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse):
+    import maroontree_b200 as mt
+
+    src, rec = _frame(160, 96, qidx + 1)
+    q = oracle_lib.quant_new(qidx, 8, qm_level)
+    qm = oracle_lib.qm_row(qm_level, 0, 16) if qm_level < 15 else None
+    c = synth.synthetic_cdfs(qidx + 7, n_eob_bins=9)
+    jobs = synth.leaf8_jobs(160, 96, range(13), deltas=(-1, 0, 3), seed=qidx, n=16)
+    jobs["py"][4] = 88  # crosses the bottom edge: rejected
+    prm = mt.split16_params(160, 96, trellis_lambda0=0.05, rd_lambda=0.3 * qidx + 2.0, band_tilt=1.9,
+                            wsse_scale=wsse, skip_bits=[(2.0, 0.3)] + [(0.0, 0.0)] * 12, vis=(155, 91))
+    res, cf, recs = mt_lib.leaf16(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs, want_cf=True, want_rec=True)
+    want, wcf, wrec = oracle_lib.leaf16(src, rec, prm, q, qm, c, jobs)
+    assert res.tobytes() == want.tobytes()
+    assert np.array_equal(cf, wcf) and np.array_equal(recs, wrec)
+    assert res["tx_type"][4] == 255
