@@ -363,7 +363,7 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     types, 4:4:4 form).  Device time with CUDA events after an L2 flush; the
     oracle on all host cores over the same jobs.  n16: the 16x16 leaf's
     mode-loop candidates (8,040 blocks x 13 modes, trellis_optimize_ctx at
-    TX_16X16)."""
+    TX_16X16) or its winners' refinement (8,040 blocks, five types)."""
     import ctypes as C
 
     import torch
@@ -384,7 +384,10 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     d_res = torch.empty(n * abi.LEAF8_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lib = mt.load()
-    entry = lib.mt_leaf16_luma_device if n16 else (lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device)
+    if n16:
+        entry = lib.mt_leaf16_tx_refine_device if refine else lib.mt_leaf16_luma_device
+    else:
+        entry = lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device
 
     def launch():
         rc = entry(d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q), d_qm.data_ptr(), d_costs.data_ptr(),
@@ -408,14 +411,15 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     what = ("leaf8 winners' transform-type refinement 1920x1080 luma, 32,400 blocks, 7 types" if refine else
             "leaf8 mode-loop candidates 1920x1080 luma, 32,400 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)")
     if n16:
-        what = "leaf16 mode-loop candidates 1920x1080 luma, 8,040 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)"
+        what = ("leaf16 winners' transform-type refinement 1920x1080 luma, 8,040 blocks, 5 types" if refine else
+                "leaf16 mode-loop candidates 1920x1080 luma, 8,040 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)")
     out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n, "workload": what}
     if cpu:
         from oracle import pyoracle as po
 
         t0 = time.perf_counter()
         if n16:
-            po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs)
+            po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
         else:
             po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
         dt = time.perf_counter() - t0
@@ -664,6 +668,7 @@ def run_ours(args):
              for k in ("luma", "refine")} if rank == 0 else None
     if leaf8 is not None:
         leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=world == 1 and not args.no_cpu, n16=True)
+        leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=world == 1 and not args.no_cpu, n16=True)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -530,19 +530,27 @@ int mt_leaf8_tx_refine_device(const uint16_t* d_src, const uint16_t* d_recon, co
                               const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                               const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
                               uint16_t* d_rec, void* stream);
-/* The 16x16 leaf's mode loop (pick_luma16, src/coder/partition_search.rs:
- * 4802-4880): the same candidate as mt_leaf8_luma_device at 16x16 -- DCT_DCT
+/* The 16x16 leaf (pick_luma16, src/coder/partition_search.rs): the mode
+ * loop's candidates (:4802-4880) as mt_leaf8_luma_device at 16x16 -- DCT_DCT
  * (+ QM) with trellis_optimize_ctx of class TX_16X16, sse_recon, luma_bits in
- * txb_skip context 0 with the txtp16 symbol; jobs address 16x16 blocks, and
- * the costs / qm row are the TX_16X16 slice and 16x16 row; d_cf / d_rec are
- * n x 256. */
+ * txb_skip context 0 with the txtp16 symbol -- and the winner's refinement
+ * (:5252-5474): ADST_ADST (within tx_guard of the DCT's SSE, below the DCT's
+ * rd cost, bounded rate), ADST_DCT and DCT_ADST (within tx_guard of the DCT's
+ * SSE, below the current best, unbounded rate), IDTX (within tx_guard of the
+ * current best's SSE); no V / H.  Jobs address 16x16 blocks; the costs / qm
+ * row are the TX_16X16 slice and 16x16 row; d_cf / d_rec are n x 256. */
 int mt_leaf16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
                           const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                           const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
                           uint16_t* d_rec, void* stream);
-int mt_leaf16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
-                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
-                   mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+int mt_leaf16_tx_refine_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                               const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                               const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                               uint16_t* d_rec, void* stream);
+/* Host-buffer form; refine = 0: the candidates, 1: the refinement. */
+int mt_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 /* Host-buffer forms; refine = 0: mt_leaf8_luma, 1: mt_leaf8_tx_refine. */
 int mt_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,

@@ -301,10 +301,10 @@ def leaf8(src, recon, prm, quant, qmrow, costs, jobs, refine=False, want_cf=Fals
     return res, cf, rec
 
 
-def leaf16(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
-    """The 16x16 leaf's mode-loop candidates (``mt_leaf16_luma``); qmrow / costs are
-    the 16x16 row and the TX_16X16 slice.  Returns (results, cf n x 256 or None,
-    rec n x 16 x 16 or None)."""
+def leaf16(src, recon, prm, quant, qmrow, costs, jobs, refine=False, want_cf=False, want_rec=False):
+    """The 16x16 leaf's mode-loop candidates, or with refine the winners' transform-type
+    refinement (``mt_leaf16``); qmrow / costs are the 16x16 row and the TX_16X16
+    slice.  Returns (results, cf n x 256 or None, rec n x 16 x 16 or None)."""
     src = np.ascontiguousarray(src, np.uint16)
     recon = np.ascontiguousarray(recon, np.uint16)
     jobs = np.ascontiguousarray(jobs, abi.LEAF8_JOB_DTYPE)
@@ -313,8 +313,8 @@ def leaf16(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=F
     cf = np.zeros((n, 256), np.int32) if want_cf else None
     rec = np.zeros((n, 16, 16), np.uint16) if want_rec else None
     qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
-    _check(load().mt_leaf16_luma(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
-                                 ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)), "mt_leaf16_luma")
+    _check(load().mt_leaf16(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs), ptr(jobs),
+                            n, int(bool(refine)), ptr(res), ptr(cf), ptr(rec)), "mt_leaf16")
     return res, cf, rec
 
 

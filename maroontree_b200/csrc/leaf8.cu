@@ -47,7 +47,8 @@ __device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate)
 
 // N = 8: pick_block8's candidates (REFINE = false) and winner refinement
 // (REFINE = true); N = 16: pick_luma16's mode-loop candidates
-// (src/coder/partition_search.rs:4802-4880).
+// (src/coder/partition_search.rs:4802-4880) and winner refinement (:5252-5474:
+// ADST_ADST, ADST_DCT, DCT_ADST, IDTX with the 8x8 leaf's gates).
 template <int N, bool REFINE>
 __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const mt_leaf8_job* __restrict__ jobs, int n, mt_leaf8_result* __restrict__ res, int32_t* __restrict__ cf_out,
     uint16_t* __restrict__ rec_out) {
   __shared__ mt_coef_costs sT;
-  static_assert(N == 8 || (N == 16 && !REFINE), "8x8 candidates and refinement, 16x16 candidates");
+  static_assert(N == 8 || N == 16, "8x8 and 16x16 leaves");
   constexpr int NN = N * N, L = N == 8 ? 3 : 4;
   __shared__ uint8_t sQm[NN];
   __shared__ float sQs[NN];
@@ -118,7 +119,8 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
   // DCT_DCT, then (refinement) ADST_ADST, ADST_DCT, DCT_ADST, IDTX[, V_DCT,
   // H_DCT]; nibble k: the k-th type.
   constexpr uint32_t kTypeOrder = 0x3206541u;
-  const int ntypes = REFINE ? (p.tx_search ? 7 : 5) : 1;
+  // the 16x16 refinement has no V / H (transform set INTRA_2)
+  const int ntypes = REFINE ? ((N == 8 && p.tx_search) ? 7 : 5) : 1;
   int best = 0, btx = MT_TX_DCT_DCT;
   long long bsse = 0, dct_sse = 0, dct_guard = 0;
   float bbits = 0.0f;
@@ -139,9 +141,10 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     eb.resid = rr;
     const long long asse = sse_recon_block(eb, p.wsse_scale);
     if (k > 0) {
-      // the gates of block8.rs:1214-1396: the ADST family within tx_guard of
-      // the DCT's SSE, IDTX within tx_guard of the current best's, V / H at
-      // most the current best's
+      // the gates of block8.rs:1214-1396 (and partition_search.rs:5320-5470
+      // at 16x16): the ADST family within tx_guard of the DCT's SSE, IDTX
+      // within tx_guard of the current best's, V / H at most the current
+      // best's
       bool gate;
       if (t >= MT_TX_ADST_ADST) gate = asse <= dct_sse + dct_guard;
       else if (t == MT_TX_IDTX) gate = asse <= bsse + (p.tx_guard_shift >= 63 ? 0 : (bsse >> p.tx_guard_shift));
@@ -153,9 +156,14 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     if (N == 8 && (t == MT_TX_V_DCT || t == MT_TX_H_DCT)) {
       abits = rate_1d<8>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
     } else {
-      const float bound = (k == 0 || t == MT_TX_IDTX) ? __int_as_float(0x7f800000)
-                                                      : __fdiv_rn(__fsub_rn(base_rd, (float)asse), rd_lam);
-      abits = rate_bounded<N>(cf, T, 0, ds, jb.mode, t, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
+      // unbounded: the DCT, IDTX and, at 16x16, ADST_DCT / DCT_ADST (priced
+      // with luma_bits there, partition_search.rs:5396-5404)
+      const bool unbounded = k == 0 || t == MT_TX_IDTX || (N == 16 && t != MT_TX_ADST_ADST);
+      const float bound = unbounded ? __int_as_float(0x7f800000)
+                                    : __fdiv_rn(__fsub_rn(base_rd, (float)asse), rd_lam);
+      // tx-type symbol: the 5-type TX_16X16 intra set drops V_DCT / H_DCT
+      const int sym = N == 16 && t >= MT_TX_ADST_ADST ? t - 2 : t;
+      abits = rate_bounded<N>(cf, T, 0, ds, jb.mode, sym, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
     }
     if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < base_rd) {
       best = cur;
@@ -255,10 +263,18 @@ int mt_leaf16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const 
                                 stream);
 }
 
-int mt_leaf16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
-                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
-                   mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
-  return leaf_host<16>(src, recon, prm, quant, qm_row, costs, jobs, n, 0, results, cf_out, rec_out);
+int mt_leaf16_tx_refine_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                               const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                               const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                               uint16_t* d_rec, void* stream) {
+  return leaf_device<16, true>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec,
+                               stream);
+}
+
+int mt_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_host<16>(src, recon, prm, quant, qm_row, costs, jobs, n, refine, results, cf_out, rec_out);
 }
 
 }  // extern "C"
@@ -291,7 +307,7 @@ int leaf_host(const uint16_t* src, const uint16_t* recon, const mt_split16_param
   if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_leaf8_job), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    auto fn = (N == 8 && refine) ? leaf_device<8, true> : leaf_device<N, false>;
+    auto fn = refine ? leaf_device<N, true> : leaf_device<N, false>;
     rc = fn(reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant,
             has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
             reinterpret_cast<const mt_leaf8_job*>(d + o_jobs), n, reinterpret_cast<mt_leaf8_result*>(d + o_res),

@@ -138,9 +138,10 @@ int or_split4tx(const uint16_t* src, const uint16_t* recon, const mt_split16_par
 int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
              const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
-/* partition_search.rs:4802-4880 pick_luma16's mode-loop candidates. */
+/* partition_search.rs pick_luma16: the mode loop's candidates (refine 0, :4802-4880) or the winner's type
+ * refinement (1, :5252-5474). */
 int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
-              const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n,
+              const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);

@@ -888,7 +888,8 @@ extern "C" {
 
 // block8.rs:738-808 (refine = 0: the Slow mode loop's candidate) and
 // :1183-1404 (refine = 1: the winner's transform-type refinement) of
-// pick_block8, over a batch of 8x8 jobs.
+// pick_block8 over a batch of 8x8 jobs (N = 8), or the same two stages of
+// pick_luma16 over 16x16 jobs (N = 16).
 static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                      const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
                      mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
@@ -934,8 +935,12 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, N, N, p->wsse_scale, &d);
       return d;
     };
+    // The tx-type symbol: MT_TX_* is the 7-type TX_8X8 intra set's index;
+    // the 5-type TX_16X16 set (IDTX, DCT_DCT, ADST_ADST, ADST_DCT, DCT_ADST)
+    // drops V_DCT / H_DCT (cost.rs:95-108).
     auto bits2d = [&](const int32_t* cf, int t, float bound) -> float {
-      return or_real_block_bits_bounded(cf, scan, N, N, cd, 0, ds, jb.mode, t, p->use_skip_bits, skip, bound);
+      const int sym = N == 16 && t >= MT_TX_ADST_ADST ? t - 2 : t;
+      return or_real_block_bits_bounded(cf, scan, N, N, cd, 0, ds, jb.mode, sym, p->use_skip_bits, skip, bound);
     };
     // The DCT_DCT candidate with the per-candidate trellis (block8.rs:780-805).
     int32_t lcf[256], lrr[256];
@@ -948,56 +953,62 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
     int64_t bsse = dct_sse;
     float bbits = dct_bits;
     uint8_t btx = MT_TX_DCT_DCT;
-    if (refine && N == 8) {
+    if (refine) {
       auto take = [&](const int32_t* cf, const int32_t* rr, int64_t s, float b, int t) {
-        memcpy(lcf, cf, 64 * sizeof(int32_t));
-        memcpy(lrr, rr, 64 * sizeof(int32_t));
+        memcpy(lcf, cf, NN * sizeof(int32_t));
+        memcpy(lrr, rr, NN * sizeof(int32_t));
         bsse = s;
         bbits = b;
         btx = (uint8_t)t;
       };
-      // ADST_ADST (block8.rs:1214-1262)
+      // ADST_ADST (block8.rs:1214-1262; partition_search.rs:5276-5328): bounded
+      // by the DCT's rd cost.  An aborted rate is infinite, so an accepted
+      // one is exact.
       {
-        int32_t acf[64], arr[64];
-        float atf[64];
-        or_fwd_txfm_quant(resid, MT_TX_ADST_ADST, 8, q, qm, acf, atf);
-        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level,
+        int32_t acf[256], arr[256];
+        float atf[256];
+        or_fwd_txfm_quant(resid, MT_TX_ADST_ADST, N, q, qm, acf, atf);
+        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level,
                                 p->band_tilt);
-        or_inv_txfm_dequant(acf, MT_TX_ADST_ADST, 8, q, qm, arr);
+        or_inv_txfm_dequant(acf, MT_TX_ADST_ADST, N, q, qm, arr);
         const int64_t asse = sse_of(arr);
         const float base_rd = rd_cost_i64(dct_sse, mlam, dct_bits);
         const float abits = bits2d(acf, MT_TX_ADST_ADST, (base_rd - (float)asse) / mlam);
         if (asse <= dct_sse + guard(dct_sse) && rd_cost_i64(asse, mlam, abits) < base_rd)
           take(acf, arr, asse, abits, MT_TX_ADST_ADST);
       }
-      // ADST_DCT, DCT_ADST (block8.rs:1264-1332)
+      // ADST_DCT, DCT_ADST against the running winner (block8.rs:1264-1332,
+      // bounded rate; partition_search.rs:5331-5423, unbounded luma_bits, the
+      // ADST_ADST winner re-priced unbounded -- the same value).
       for (int t : {MT_TX_ADST_DCT, MT_TX_DCT_ADST}) {
-        int32_t acf[64], arr[64];
-        float atf[64];
-        or_fwd_txfm_quant(resid, t, 8, q, qm, acf, atf);
-        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, 8, p->trellis_lambda0, cd, ds, qm, q->qm_level,
+        int32_t acf[256], arr[256];
+        float atf[256];
+        or_fwd_txfm_quant(resid, t, N, q, qm, acf, atf);
+        or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level,
                                 p->band_tilt);
-        or_inv_txfm_dequant(acf, t, 8, q, qm, arr);
+        or_inv_txfm_dequant(acf, t, N, q, qm, arr);
         const int64_t asse = sse_of(arr);
         const float base_rd = rd_cost_i64(bsse, mlam, bbits);
-        const float abits = bits2d(acf, t, (base_rd - (float)asse) / mlam);
+        const float abits = bits2d(acf, t, N == 8 ? (base_rd - (float)asse) / mlam : INFINITY);
         if (asse <= dct_sse + guard(dct_sse) && rd_cost_i64(asse, mlam, abits) < base_rd)
           take(acf, arr, asse, abits, t);
       }
-      // IDTX (block8.rs:1334-1361)
+      // IDTX without the trellis, within tx_guard of the winner's SSE
+      // (block8.rs:1334-1361; partition_search.rs:5425-5474)
       {
-        int32_t icf[64], irr[64];
-        float itf[64];
-        or_fwd_txfm_quant(resid, MT_TX_IDTX, 8, q, qm, icf, itf);
-        or_inv_txfm_dequant(icf, MT_TX_IDTX, 8, q, qm, irr);
+        int32_t icf[256], irr[256];
+        float itf[256];
+        or_fwd_txfm_quant(resid, MT_TX_IDTX, N, q, qm, icf, itf);
+        or_inv_txfm_dequant(icf, MT_TX_IDTX, N, q, qm, irr);
         const int64_t isse = sse_of(irr);
         const float ibits = bits2d(icf, MT_TX_IDTX, INFINITY);
         const float base_rd = rd_cost_i64(bsse, mlam, bbits);
         if (isse <= bsse + guard(bsse) && rd_cost_i64(isse, mlam, ibits) < base_rd)
           take(icf, irr, isse, ibits, MT_TX_IDTX);
       }
-      // V_DCT, H_DCT unless 4:2:0 (block8.rs:1362-1396)
-      if (p->tx_search)
+      // V_DCT, H_DCT unless 4:2:0 (block8.rs:1362-1396); the 16x16 intra set
+      // has no 1-D types.
+      if (N == 8 && p->tx_search)
         for (int vertical = 1; vertical >= 0; vertical--) {
           const int t = vertical ? MT_TX_V_DCT : MT_TX_H_DCT;
           int32_t vcf[64], vrr[64];
@@ -1027,11 +1038,12 @@ int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params
   return leaf_impl(8, src, recon, p, q, qm, cd, jobs, n, refine, results, cf_out, rec_out);
 }
 
-// partition_search.rs:4802-4880 pick_luma16's mode-loop candidates.
+// partition_search.rs:4802-4880 pick_luma16's mode-loop candidates (refine 0)
+// and :5252-5474 the winner's transform-type refinement (refine 1).
 int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
-              const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n,
+              const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
-  return leaf_impl(16, src, recon, p, q, qm, cd, jobs, n, 0, results, cf_out, rec_out);
+  return leaf_impl(16, src, recon, p, q, qm, cd, jobs, n, refine, results, cf_out, rec_out);
 }
 
 }  // extern "C"

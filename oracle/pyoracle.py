@@ -76,7 +76,7 @@ def load():
             "or_split4tx": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                       C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_leaf16": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
-                                    C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
+                                    C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
             "or_leaf8": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                    C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -463,8 +463,8 @@ def leaf8(src, recon, prm, q, qm, cdfs, jobs, refine=False):
     return res, cf, rec
 
 
-def leaf16(src, recon, prm, q, qm, cdfs, jobs):
-    """pick_luma16's mode-loop candidates of n 16x16 jobs: (results, cf n x 256, rec n x 16 x 16)."""
+def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False):
+    """pick_luma16's mode-loop candidates / refinement of n 16x16 jobs: (results, cf n x 256, rec n x 16 x 16)."""
     src = np.ascontiguousarray(src, np.uint16)
     recon = np.ascontiguousarray(recon, np.uint16)
     jobs = np.ascontiguousarray(jobs, abi.LEAF8_JOB_DTYPE)
@@ -473,6 +473,6 @@ def leaf16(src, recon, prm, q, qm, cdfs, jobs):
     cf = np.zeros((n, 256), np.int32)
     rec = np.zeros((n, 16, 16), np.uint16)
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
-    assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n, p(res),
-                            p(cf), p(rec)) == 0
+    assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
+                            int(bool(refine)), p(res), p(cf), p(rec)) == 0
     return res, cf, rec

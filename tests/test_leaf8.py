@@ -1,5 +1,5 @@
-"""The 8x8 leaf's luma search (pick_block8): the Slow mode loop's candidates and
-the winner's transform-type refinement.
+"""The 8x8 leaf's luma search (pick_block8) and the 16x16 leaf's (pick_luma16):
+the Slow mode loop's candidates and the winner's transform-type refinement.
 
 CPU tests pin the oracle's glue against a composition of its primitives (the
 candidate's DCT + trellis_optimize_ctx + sse_recon + luma_bits + syntax bits,
@@ -21,18 +21,18 @@ def _frame(w, h, seed):
     return src, rec
 
 
-def _cand(oracle_lib, src, rec, prm, q, qm, c, jb, t):
+def _cand(oracle_lib, src, rec, prm, q, qm, c, jb, t, n=8):
     px, py = int(jb["px"]), int(jb["py"])
     fl = int(jb["flags"])
-    pred = oracle_lib.intra_predict(rec, px, py, 8, 8, int(jb["mode"]), int(jb["angle_delta"]), bool(fl & 1),
+    pred = oracle_lib.intra_predict(rec, px, py, n, n, int(jb["mode"]), int(jb["angle_delta"]), bool(fl & 1),
                                     bool(fl & 2), bool(fl & 4)).ravel()
-    resid = src[py:py + 8, px:px + 8].astype(np.int32).ravel() - pred
+    resid = src[py:py + n, px:px + n].astype(np.int32).ravel() - pred
     cf, tf = oracle_lib.fwd_txfm_quant(resid, t, q, qm)
     if t in (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_ADST_DCT, abi.TX_DCT_ADST):
         cf = oracle_lib.trellis_optimize_ctx(cf, tf, q, qm, c, int(jb["dcs_ctx"]), prm.trellis_lambda0,
-                                             band_tilt=prm.band_tilt)
+                                             band_tilt=prm.band_tilt, n=n)
     rr = oracle_lib.inv_txfm_dequant(cf, t, q, qm)
-    sse = int(oracle_lib.sse_recon(src, prm.frame_w, prm.frame_h, [(px, py)], pred, rr, 8, 8,
+    sse = int(oracle_lib.sse_recon(src, prm.frame_w, prm.frame_h, [(px, py)], pred, rr, n, n,
                                    scale=prm.wsse_scale)[0])
     return cf, sse
 
@@ -138,9 +138,62 @@ def test_leaf16_oracle_glue(oracle_lib):
         assert f32(res["cost"][i]) == f32(f32(sse) + f32(f32(25.0) * f32(bits + f32(jb["syntax_bits"]))))
 
 
+# The 5-type TX_16X16 intra set's symbol of each MT_TX_* (cost.rs:101-108).
+TX16_SYM = {abi.TX_IDTX: 0, abi.TX_DCT_DCT: 1, abi.TX_ADST_ADST: 2, abi.TX_ADST_DCT: 3, abi.TX_DCT_ADST: 4}
+
+
+def test_leaf16_refine_oracle_glue(oracle_lib):
+    """pick_luma16's winner refinement (partition_search.rs:5252-5474):
+    ADST_ADST with the rate bounded by the DCT's rd cost; ADST_DCT / DCT_ADST
+    priced unbounded against the running winner, gated on the DCT's SSE;
+    IDTX untrellised within tx_guard of the winner's SSE; the tx-type symbols
+    of the 5-type set; no V / H."""
+    import maroontree_b200 as mt
+
+    src, rec = _frame(64, 48, 71)
+    q = oracle_lib.quant_new(60, 8, 15)
+    c = synth.synthetic_cdfs(21, n_eob_bins=9)
+    prm = mt.split16_params(64, 48, trellis_lambda0=0.05, rd_lambda=14.0, band_tilt=1.9, tx_search=True,
+                            tx_guard_shift=4)
+    jobs = synth.leaf8_jobs(64, 48, (abi.DC_PRED, abi.H_PRED, abi.D157_PRED, abi.SMOOTH_H_PRED, abi.PAETH_PRED),
+                            deltas=(0, 2), seed=5, n=16)
+    scan = oracle_lib.default_scan(16)
+    f32 = np.float32
+    rd = lambda d, b: f32(f32(d) + f32(f32(prm.rd_lambda) * f32(b)))
+    bits = lambda cf, t, m, ds, bound: f32(oracle_lib.real_block_bits_bounded(cf, scan, 16, 16, c, 0, ds, m,
+                                                                             TX16_SYM[t], bound))
+    ref, rcf, _ = oracle_lib.leaf16(src, rec, prm, q, None, c, jobs, refine=True)
+    seen = set()
+    for i, jb in enumerate(jobs):
+        m, ds = int(jb["mode"]), int(jb["dcs_ctx"])
+        cf, sse = _cand(oracle_lib, src, rec, prm, q, None, c, jb, abi.TX_DCT_DCT, n=16)
+        dct = (sse, bits(cf, abi.TX_DCT_DCT, m, ds, INF))
+        best = dct + (abi.TX_DCT_DCT, cf)
+        guard = lambda d: d + (d >> prm.tx_guard_shift)
+        for t in (abi.TX_ADST_ADST, abi.TX_ADST_DCT, abi.TX_DCT_ADST, abi.TX_IDTX):
+            acf, asse = _cand(oracle_lib, src, rec, prm, q, None, c, jb, t, n=16)
+            base = rd(best[0], best[1])
+            if t == abi.TX_ADST_ADST:
+                ab = bits(acf, t, m, ds, float(f32(f32(base - f32(asse)) / f32(prm.rd_lambda))))
+                gate = asse <= guard(dct[0])
+            elif t == abi.TX_IDTX:
+                ab = bits(acf, t, m, ds, INF)
+                gate = asse <= guard(best[0])
+            else:
+                ab = bits(acf, t, m, ds, INF)
+                gate = asse <= guard(dct[0])
+            if gate and rd(asse, ab) < base:
+                best = (asse, ab, t, acf)
+        assert (ref["sse"][i], f32(ref["bits"][i]), ref["tx_type"][i]) == best[:3], i
+        assert np.array_equal(rcf[i], best[3])
+        seen.add(best[2])
+    assert len(seen) >= 3, seen
+
+
 @pytest.mark.gpu
+@pytest.mark.parametrize("refine", [False, True])
 @pytest.mark.parametrize("qidx,qm_level,wsse", [(70, 6, 0.0), (116, 15, 1.0), (30, 3, 0.75)])
-def test_leaf16_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse):
+def test_leaf16_gpu_matches_oracle(mt_lib, oracle_lib, cuda, refine, qidx, qm_level, wsse):
     import maroontree_b200 as mt
 
     src, rec = _frame(160, 96, qidx + 1)
@@ -150,9 +203,13 @@ def test_leaf16_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wss
     jobs = synth.leaf8_jobs(160, 96, range(13), deltas=(-1, 0, 3), seed=qidx, n=16)
     jobs["py"][4] = 88  # crosses the bottom edge: rejected
     prm = mt.split16_params(160, 96, trellis_lambda0=0.05, rd_lambda=0.3 * qidx + 2.0, band_tilt=1.9,
-                            wsse_scale=wsse, skip_bits=[(2.0, 0.3)] + [(0.0, 0.0)] * 12, vis=(155, 91))
-    res, cf, recs = mt_lib.leaf16(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs, want_cf=True, want_rec=True)
-    want, wcf, wrec = oracle_lib.leaf16(src, rec, prm, q, qm, c, jobs)
+                            wsse_scale=wsse, tx_guard_shift=4, skip_bits=[(2.0, 0.3)] + [(0.0, 0.0)] * 12,
+                            vis=(155, 91))
+    res, cf, recs = mt_lib.leaf16(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs, refine=refine, want_cf=True,
+                                  want_rec=True)
+    want, wcf, wrec = oracle_lib.leaf16(src, rec, prm, q, qm, c, jobs, refine=refine)
     assert res.tobytes() == want.tobytes()
     assert np.array_equal(cf, wcf) and np.array_equal(recs, wrec)
     assert res["tx_type"][4] == 255
+    if refine:
+        assert len(np.unique(res["tx_type"])) >= 4
