@@ -615,6 +615,49 @@ int mt_cfl_alpha(const uint16_t* luma, int32_t luma_stride, int32_t luma_h, cons
                  int32_t cw, int32_t ch, int32_t vis_cw, int32_t vis_ch, int32_t bd, const mt_cfl_block* blocks,
                  int32_t n, int8_t* alpha, int32_t* ac);
 
+/* ---- Lossy luma palette candidates (src/coder/palette.rs) ----
+ * Per w x h block (w, h in 4..64, powers of two): block_color_histogram
+ * (:651-706: distinct values ascending with counts; no candidate when the
+ * block has < 2 or > 64 distinct values), then fourteen candidate slots:
+ * slot s < 7 is sel = s + 2 colours with palette_centers' exact values
+ * (colours == distinct) or dp_palette_center_sets' optimal centres
+ * (:728-869, the shipped palette_dp_centers), slot s >= 7 is sel = s + 3
+ * (s - 5 colours) with top_palette_centers' dominant colours (:708-726, only
+ * when colours < distinct).  Each candidate's index map is built by
+ * lossy_luma_palette_from_centers (:1218-1265): the row Viterbi
+ * (viterbi_map_core, :1028-1172) when viterbi_lambda > 0, else
+ * luma_nearest_indices (src/kmeans.rs:71-101) + smooth_palette_map
+ * (:1173-1216) when smooth_t > 0; then palette_index_bits (:1911-1925). */
+#define MT_PALETTE_SLOTS 14
+
+typedef struct mt_palette_opts {
+  int32_t smooth_t;             /* palette_smooth tolerance in sample units; 0 = off */
+  int32_t smooth_guard;         /* palette_smooth_guard: keep samples the nearest centre hits exactly */
+  float viterbi_lambda;         /* > 0: the Viterbi map with this lambda (mlam x palette_viterbi_*) */
+  float color_costs[7][5][8];   /* palette_y_color bits [colours - 2][ctx][symbol] (pal_y_cost_tables) */
+} mt_palette_opts;
+
+typedef struct mt_palette_cand {
+  int16_t colors[8];  /* ascending centres, n_colors valid, the rest 0 */
+  uint8_t n_colors;   /* 0: no candidate in this slot */
+  uint8_t sel;        /* 2..8 (exact / optimal centres) or 10..16 (dominant colours) */
+  uint8_t hist_len;   /* the block's distinct values; 0 when the histogram gate rejects it */
+  uint8_t reserved;
+  float index_bits;   /* palette_index_bits of the map; 0 for an empty slot */
+} mt_palette_cand;
+
+/* d_pos: n (x, y) uint16 pairs; d_cands: n x MT_PALETTE_SLOTS; d_maps:
+ * n x MT_PALETTE_SLOTS x w x h indices (zero for an empty slot).  A block
+ * outside frame_w x frame_h, or with a sample above (1 << bd) - 1, gets
+ * empty slots. */
+int mt_luma_palette_device(const uint16_t* d_src, int32_t stride, int32_t frame_w, int32_t frame_h, int32_t bd,
+                           int32_t w, int32_t h, const uint16_t* d_pos, int32_t n, const mt_palette_opts* opts,
+                           mt_palette_cand* d_cands, uint8_t* d_maps, void* stream);
+/* Host-buffer form; maps may be NULL. */
+int mt_luma_palette(const uint16_t* src, int32_t stride, int32_t frame_w, int32_t frame_h, int32_t bd, int32_t w,
+                    int32_t h, const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_palette_cand* cands,
+                    uint8_t* maps);
+
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and
  * f32 quantisation targets, with the QM applied as DctDispatch does. */

@@ -268,6 +268,30 @@ def cfl_alpha(luma, src_u, src_v, sub_x, sub_y, cw, ch, blocks, vis=(0, 0), bd=8
     return alpha, ac
 
 
+def palette_opts(smooth_t=0, smooth_guard=True, viterbi_lambda=0.0, color_costs=None):
+    """``mt_palette_opts``: palette_smooth tolerance, its guard, the Viterbi lambda
+    (0 = nearest + smoothing) and the palette_y_color bits [size - 2][ctx][symbol]."""
+    o = abi.PaletteOpts()
+    o.smooth_t, o.smooth_guard, o.viterbi_lambda = int(smooth_t), int(bool(smooth_guard)), float(viterbi_lambda)
+    if color_costs is not None:
+        cc = np.ascontiguousarray(color_costs, np.float32).reshape(7, 5, 8)
+        C.memmove(C.addressof(o.color_costs), cc.ctypes.data, cc.nbytes)
+    return o
+
+
+def luma_palette(src, w, h, pos, opts, bd=8, want_maps=False):
+    """The lossy luma palette candidates of n w x h blocks (``mt_luma_palette``):
+    returns (candidates n x 14, maps n x 14 x h x w or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    cands = np.zeros((n, abi.PALETTE_SLOTS), abi.PALETTE_CAND_DTYPE)
+    maps = np.zeros((n, abi.PALETTE_SLOTS, h, w), np.uint8) if want_maps else None
+    _check(load().mt_luma_palette(ptr(src), src.shape[1], src.shape[1], src.shape[0], bd, w, h, ptr(pos), n,
+                                  C.byref(opts), ptr(cands), ptr(maps)), "mt_luma_palette")
+    return cands, maps
+
+
 def split4tx(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
     """The 8x8 leaf's ``split4tx_try`` (``mt_split4tx``): four TX_4X4 per 8x8 job;
     returns (results, cf n x 64 or None, rec n x 8 x 8 or None)."""

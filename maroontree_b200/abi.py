@@ -98,6 +98,18 @@ assert LEAF8_JOB_DTYPE.itemsize == 12 and LEAF8_RESULT_DTYPE.itemsize == 24
 CFL_BLOCK_DTYPE = np.dtype([("cx", "<u2"), ("cy", "<u2"), ("dc", "<i2", (2,))])
 assert CFL_BLOCK_DTYPE.itemsize == 8
 
+PALETTE_SLOTS = 14
+
+
+class PaletteOpts(C.Structure):
+    _fields_ = [("smooth_t", C.c_int32), ("smooth_guard", C.c_int32), ("viterbi_lambda", C.c_float),
+                ("color_costs", (C.c_float * 8) * 5 * 7)]
+
+
+PALETTE_CAND_DTYPE = np.dtype([("colors", "<i2", (8,)), ("n_colors", "u1"), ("sel", "u1"), ("hist_len", "u1"),
+                               ("reserved", "u1"), ("index_bits", "<f4")])
+assert PALETTE_CAND_DTYPE.itemsize == 24
+
 
 class DeblockFrameParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "disp_w", "disp_h", "sub_x", "sub_y", "mono", "bd")]
@@ -245,6 +257,10 @@ def _bind(lib):
                                                 C.c_int32, _P, _P, _P, _P]),
         "mt_leaf16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
                                             C.c_int32, _P, _P, _P, _P]),
+        "mt_luma_palette_device": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                             _P, C.c_int32, C.POINTER(PaletteOpts), _P, _P, _P]),
+        "mt_luma_palette": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P,
+                                      C.c_int32, C.POINTER(PaletteOpts), _P, _P]),
         "mt_leaf16_tx_refine_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
                                                  C.c_int32, _P, _P, _P, _P]),
         "mt_leaf16": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
@@ -296,7 +312,7 @@ EXPORTED_SYMBOLS = (
     "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
-    "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device",
+    "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
     "mt_leaf16",
 )
 

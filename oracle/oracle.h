@@ -147,6 +147,20 @@ float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);
 
+/* palette.rs / kmeans.rs lossy luma palette candidates and their parts (oracle_palette.cpp). */
+int or_luma_palette(const uint16_t* src, int32_t stride, int32_t frame_w, int32_t frame_h, int32_t bd, int32_t w,
+                    int32_t h, const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_palette_cand* cands,
+                    uint8_t* maps);
+void or_block_color_histogram(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w, int32_t h,
+                              int32_t* vals, uint32_t* counts, int32_t* n_out);
+void or_dp_palette_center_sets(const int32_t* vals, const uint32_t* counts, int32_t n, int32_t kmax, int32_t* sets,
+                               int32_t* lens);
+void or_luma_nearest_indices(const uint16_t* src, int32_t stride, int32_t px, int32_t py, int32_t w, int32_t h,
+                             const int32_t* centers, int32_t n, uint8_t* out);
+void or_palette_color_ctx_nb(int32_t l, int32_t u, int32_t ul, int32_t cur, int32_t* ctx, int32_t* sym);
+void or_palette_color_ctx(const uint8_t* map, int32_t stride, int32_t y, int32_t x, int32_t* ctx, int32_t* sym);
+float or_dirty_log2f(float d);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,14 @@ def load():
             "or_cfl_alpha": (C.c_int, [_P, C.c_int32, _P, _P] + [C.c_int32] * 8 + [_P, C.c_int32, _P, _P]),
             "or_split4tx": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                       C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
+            "or_luma_palette": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P,
+                                          C.c_int32, C.POINTER(abi.PaletteOpts), _P, _P]),
+            "or_block_color_histogram": (None, [_P] + [C.c_int32] * 5 + [_P, _P, _P]),
+            "or_dp_palette_center_sets": (None, [_P, _P, C.c_int32, C.c_int32, _P, _P]),
+            "or_luma_nearest_indices": (None, [_P] + [C.c_int32] * 5 + [_P, C.c_int32, _P]),
+            "or_palette_color_ctx_nb": (None, [C.c_int32] * 4 + [_P, _P]),
+            "or_palette_color_ctx": (None, [_P] + [C.c_int32] * 3 + [_P, _P]),
+            "or_dirty_log2f": (C.c_float, [C.c_float]),
             "or_leaf16": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                     C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
             "or_leaf8": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -476,3 +484,60 @@ def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False):
     assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
                             int(bool(refine)), p(res), p(cf), p(rec)) == 0
     return res, cf, rec
+
+
+def luma_palette(src, w, h, pos, opts, bd=8):
+    """Lossy luma palette candidates of n w x h blocks: (candidates n x 14, maps n x 14 x h x w)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    cands = np.zeros((n, abi.PALETTE_SLOTS), abi.PALETTE_CAND_DTYPE)
+    maps = np.zeros((n, abi.PALETTE_SLOTS, h, w), np.uint8)
+    assert load().or_luma_palette(p(src), src.shape[1], src.shape[1], src.shape[0], bd, w, h, p(pos), n,
+                                  C.byref(opts), p(cands), p(maps)) == 0
+    return cands, maps
+
+
+def block_color_histogram(src, px, py, w, h):
+    """(values, counts) ascending, or None when the block has < 2 or > 64 distinct values."""
+    src = np.ascontiguousarray(src, np.uint16)
+    vals = np.zeros(64, np.int32)
+    cnts = np.zeros(64, np.uint32)
+    nn = C.c_int32()
+    load().or_block_color_histogram(p(src), src.shape[1], px, py, w, h, p(vals), p(cnts), C.byref(nn))
+    return None if nn.value == 0 else (vals[:nn.value].copy(), cnts[:nn.value].copy())
+
+
+def dp_palette_center_sets(hist, kmax=8):
+    """Optimal centre sets for sizes 2..kmax of a [(value, count)] histogram: list of 7 lists."""
+    vals = np.ascontiguousarray([v for v, _ in hist], np.int32)
+    cnts = np.ascontiguousarray([c for _, c in hist], np.uint32)
+    sets = np.zeros((7, 8), np.int32)
+    lens = np.zeros(7, np.int32)
+    load().or_dp_palette_center_sets(p(vals), p(cnts), len(hist), kmax, p(sets), p(lens))
+    return [sets[k, :lens[k]].tolist() for k in range(7)]
+
+
+def luma_nearest_indices(src, px, py, w, h, centers):
+    src = np.ascontiguousarray(src, np.uint16)
+    c = np.ascontiguousarray(centers, np.int32)
+    out = np.zeros(w * h, np.uint8)
+    load().or_luma_nearest_indices(p(src), src.shape[1], px, py, w, h, p(c), len(c), p(out))
+    return out
+
+
+def palette_color_ctx_nb(l, u, ul, cur):
+    a, b = C.c_int32(), C.c_int32()
+    load().or_palette_color_ctx_nb(-1 if l is None else l, -1 if u is None else u, ul, cur, C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def palette_color_ctx(map_, stride, y, x):
+    m = np.ascontiguousarray(map_, np.uint8)
+    a, b = C.c_int32(), C.c_int32()
+    load().or_palette_color_ctx(p(m), stride, y, x, C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def dirty_log2f(d):
+    return load().or_dirty_log2f(d)
