@@ -525,6 +525,23 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     out["filter_intra_beam16"] = entry(ms, len(fpos) * 5 * (256 * 2 + 33 * 2),
                                        "per (block, mode): the 16x16 source (2 B / sample) and the 33 edge samples")
     out["filter_intra_beam16"]["blocks"] = len(fpos)
+    # the lossy luma palette candidates of every 16x16 block of a 1080p
+    # screen-content luma plane: histogram gate, 14 centre sets, Viterbi maps
+    # (the shipped screen-frame map, lambda = 0.35 x the mode lambda), index bits
+    scr = synth.screen_luma(W, H, 7)
+    d_scr = t16(scr)
+    popts = mt.palette_opts(viterbi_lambda=0.35 * wl["prm"].mode_lambda,
+                            color_costs=np.random.default_rng(5).uniform(0.15, 7.0, (7, 5, 8)))
+    d_pc = torch.empty(len(fpos) * abi.PALETTE_SLOTS * abi.PALETTE_CAND_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    d_pm = torch.empty(len(fpos) * abi.PALETTE_SLOTS * 256, dtype=torch.uint8, device=dev)
+    ms = timed(lambda: lib.mt_luma_palette_device(d_scr.data_ptr(), W, W, H, 8, 16, 16, d_fpos.data_ptr(), len(fpos),
+                                                  C.byref(popts), d_pc.data_ptr(), d_pm.data_ptr(), None))
+    out["luma_palette16"] = entry(ms, len(fpos) * (256 * 2 + abi.PALETTE_SLOTS * (256 + 24)),
+                                  "per block: the 16x16 source (2 B / sample), 14 maps (1 B / sample) and candidates")
+    out["luma_palette16"]["blocks"] = len(fpos)
+    out["luma_palette16"]["palette_blocks"] = None  # filled below from the candidates
+    pc = np.frombuffer(d_pc.cpu().numpy().tobytes(), abi.PALETTE_CAND_DTYPE).reshape(len(fpos), abi.PALETTE_SLOTS)
+    out["luma_palette16"]["palette_blocks"] = int((pc["hist_len"][:, 0] > 0).sum())
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)

@@ -11,8 +11,8 @@
 //
 // pal_map_kernel: one thread per (slot, block), slot-major so a warp runs one
 // palette size over 32 blocks.  lossy_luma_palette_from_centers
-// (:1218-1265): viterbi_map_core (:1078-1172; transition bits recomputed per
-// pixel from palette_color_ctx_nb, :980-1021, instead of the 16 KB table) or
+// (:1218-1265): viterbi_map_core (:1078-1172; the transition bits of
+// palette_color_ctx_nb, :980-1021, tabulated once per CTA in shared memory) or
 // luma_nearest_indices (src/kmeans.rs:71-101) + smooth_palette_map
 // (:1173-1216); then palette_index_bits (:1911-1925) in its diagonal order.
 // Float arithmetic is explicit round-to-nearest in the reference's order.
@@ -239,9 +239,46 @@ __global__ void __launch_bounds__(128) pal_map_kernel(const uint16_t* __restrict
                                                        const mt_palette_opts opt,
                                                        mt_palette_cand* __restrict__ cands,
                                                        uint8_t* __restrict__ maps) {
+  // The weighted transition bits lam x costs[ctx][sym] depend on the slot's
+  // palette size alone, so the CTA tabulates them once for the (at most two)
+  // slots its threads start in: [u][ul][j][i] interior, then top[j][i] (first
+  // row) and col[u][i] (first column), as viterbi_map_core does per block.
+  // Threads of a third slot (n < 64) price on the fly: the same products.
+  constexpr int kTab = 4096 + 128;
+  __shared__ float sTr[2][kTab];
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int slot = (int)(t / n), b = (int)(t - (long long)slot * n);
+  const int slot0 = (int)(((long long)blockIdx.x * blockDim.x) / n);
+  const float lam = opt.viterbi_lambda;
+  if (lam > 0.0f) {
+    for (int e = threadIdx.x; e < 2 * kTab; e += blockDim.x) {
+      const int k = e / kTab, r = e - k * kTab, s = slot0 + k;
+      if (s >= kSlots) continue;
+      const int ns = s < 7 ? s + 2 : s - 5;
+      int ctx = 0, sym = 0, i;
+      bool in;
+      if (r < 4096) {
+        const int u = r >> 9, ul = (r >> 6) & 7, j = (r >> 3) & 7;
+        i = r & 7;
+        in = u < ns && ul < ns && j < ns && i < ns;
+        if (in) color_ctx_nb(j, u, ul, i, ctx, sym);
+      } else if (r < 4096 + 64) {
+        const int j = (r - 4096) >> 3;
+        i = r & 7;
+        in = j < ns && i < ns;
+        if (in) color_ctx_nb(j, -1, 0, i, ctx, sym);
+      } else {
+        const int u = (r - 4160) >> 3;
+        i = r & 7;
+        in = u < ns && i < ns;
+        if (in) color_ctx_nb(-1, u, 0, i, ctx, sym);
+      }
+      sTr[k][r] = in ? __fmul_rn(lam, opt.color_costs[ns - 2][ctx][sym]) : 0.0f;
+    }
+    __syncthreads();
+  }
   if (slot >= kSlots) return;
+  const float* tab = slot - slot0 < 2 ? sTr[slot - slot0] : nullptr;
   mt_palette_cand& cd = cands[(size_t)b * kSlots + slot];
   uint8_t* map = maps + ((size_t)b * kSlots + slot) * w * h;
   const int nc = cd.n_colors;
@@ -255,10 +292,11 @@ __global__ void __launch_bounds__(128) pal_map_kernel(const uint16_t* __restrict
   const int px = pos[2 * b], py = pos[2 * b + 1];
   const uint16_t* blk = src + (size_t)py * stride + px;
   const float(*costs)[8] = opt.color_costs[nc - 2];
-  const float lam = opt.viterbi_lambda;
   if (lam > 0.0f) {
     uint8_t back[64 * 8];
     float prev[8], cur[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) prev[i] = cur[i] = 0.0f;
     for (int y = 0; y < h; y++) {
       for (int x = 0; x < w; x++) {
         const int v = blk[(size_t)y * stride + x];
@@ -271,24 +309,46 @@ __global__ void __launch_bounds__(128) pal_map_kernel(const uint16_t* __restrict
         if (x == 0) {
           if (y > 0) {
             const int u = map[(y - 1) * w];
-            for (int i = 0; i < nc; i++) {
-              int ctx, sym;
-              color_ctx_nb(-1, u, 0, i, ctx, sym);
-              cur[i] = __fadd_rn(dist[i], __fmul_rn(lam, costs[ctx][sym]));
+#pragma unroll
+            for (int i = 0; i < 8; i++) {
+              if (i >= nc) break;
+              float tc;
+              if (tab) {
+                tc = tab[4160 + u * 8 + i];
+              } else {
+                int ctx, sym;
+                color_ctx_nb(-1, u, 0, i, ctx, sym);
+                tc = __fmul_rn(lam, costs[ctx][sym]);
+              }
+              cur[i] = __fadd_rn(dist[i], tc);
             }
           } else {
-            for (int i = 0; i < nc; i++) cur[i] = dist[i];
+#pragma unroll
+            for (int i = 0; i < 8; i++) cur[i] = dist[i];
           }
         } else {
           const int u = y > 0 ? map[(y - 1) * w + x] : -1;
           const int ul = y > 0 ? map[(y - 1) * w + x - 1] : 0;
-          for (int i = 0; i < nc; i++) {
+          const float* tr = tab ? (y > 0 ? tab + (u * 8 + ul) * 64 : tab + 4096) : nullptr;
+          // states are unrolled to 8 and cut at nc so prev / cur / dist stay
+          // in registers
+#pragma unroll
+          for (int i = 0; i < 8; i++) {
+            if (i >= nc) break;
             float best = __int_as_float(0x7f800000);
             int arg = 0;
-            for (int j = 0; j < nc; j++) {
-              int ctx, sym;
-              color_ctx_nb(j, u, ul, i, ctx, sym);
-              const float cc = __fadd_rn(prev[j], __fmul_rn(lam, costs[ctx][sym]));
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              if (j >= nc) break;
+              float tc;
+              if (tr) {
+                tc = tr[j * 8 + i];
+              } else {
+                int ctx, sym;
+                color_ctx_nb(j, u, ul, i, ctx, sym);
+                tc = __fmul_rn(lam, costs[ctx][sym]);
+              }
+              const float cc = __fadd_rn(prev[j], tc);
               if (cc < best) {
                 best = cc;
                 arg = j;
@@ -298,12 +358,14 @@ __global__ void __launch_bounds__(128) pal_map_kernel(const uint16_t* __restrict
             back[x * 8 + i] = (uint8_t)arg;
           }
         }
-        for (int i = 0; i < nc; i++) prev[i] = cur[i];
+#pragma unroll
+        for (int i = 0; i < 8; i++) prev[i] = cur[i];
       }
       int bi = 0;
       float bc = __int_as_float(0x7f800000);
-      for (int i = 0; i < nc; i++)
-        if (prev[i] < bc) {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (i < nc && prev[i] < bc) {
           bc = prev[i];
           bi = i;
         }
