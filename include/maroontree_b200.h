@@ -13,6 +13,10 @@
  *                                         Quant::new_chroma_with_delta_qm
  *   mt_coef_costs_build                   src/rate.rs:58-80 CoefCostTables::build +
  *                                         src/cost.rs:156-190 cdf_cost_with_table
+ *   mt_qcat / mt_coef_cdfs_default        src/coef_q.rs:31-41 qcat, src/coder/cdfs.rs:401-629
+ *                                         Cdfs::new (the coefficient slices)
+ *   mt_quality_to_q / mt_qm_levels /      src/avif.rs:637-666 quality_to_q, src/quant.rs:122-167
+ *   mt_rd_lambdas_init                    QM level laws, src/cost.rs + src/partition_rd.rs lambdas
  *   mt_candidate_chain[_device]           the per-candidate chain of the luma mode
  *                                         search, src/coder/partition_search.rs:467-530
  *                                         (predict_nd -> residual_pred -> DctDispatch ->
@@ -218,6 +222,43 @@ const uint8_t* mt_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h)
 const uint16_t* mt_default_scan(int32_t n);
 /* CoefCostTables-style bit costs of one CDF slice. */
 int mt_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
+/* Decision lambdas of a frame (8-bit): the luma proxy's and the emitters'
+ * mode lambda mlam = mode_lambda_q(dc_q) x tune_weight (src/cost.rs:128-148,
+ * :286-292, src/coder/lossy_state.rs:1769-1771, :1864-1871), the decision
+ * lambda lambda_d = mlam / K_PART_LAMBDA (:1787-1789), the trellis lambda0
+ * (src/cost.rs:93, :110-112), and the SATD proxy's scale and bridge
+ * (src/partition_rd.rs:30-71, src/coder/lossy_state.rs:2396-2408:
+ * luma_satd_scale, K_PART_LAMBDA / k_satd x proxy_luma_scale). */
+typedef struct mt_rd_lambdas {
+  float mode_lambda;
+  float lambda_d;
+  float trellis_lambda0;
+  float satd_scale;
+  float satd_bridge;
+} mt_rd_lambdas;
+
+/* quality 0..100 -> base qindex (src/avif.rs:637-666 quality_to_q). */
+uint8_t mt_quality_to_q(uint8_t quality);
+/* Default quantisation-matrix levels of a base qindex: qm_level_law (luma) and
+ * qm_chroma_level_law (src/quant.rs:122-167); sub 0 = 4:4:4, 1 = 4:2:2,
+ * 2 = 4:2:0. */
+int mt_qm_levels(uint8_t base_q_idx, int32_t sub, uint8_t* y_level, uint8_t* uv_level);
+/* The lambdas above for base qindex base_q_idx (the frame's; the SATD laws
+ * read the AQ base qindex, equal to it without AQ), the DC quantiser step dc_q
+ * of the block's qindex, chroma subsampling sub (0 4:4:4, 1 4:2:2, 2 4:2:0)
+ * and bit depth bd (8 only: MT_ERR_UNSUPPORTED otherwise). */
+int mt_rd_lambdas_init(uint8_t base_q_idx, int32_t dc_q, int32_t sub, uint8_t bd, mt_rd_lambdas* out);
+/* Coefficient CDF q context of a base qindex: qcat (src/coef_q.rs:31-41). */
+int mt_qcat(int32_t base_q_idx);
+/* The (transform class, plane) slice of the default decision snapshot
+ * Cdfs::new(qctx) (src/coder/cdfs.rs:401-629) for a tx_w x tx_h transform
+ * (4..64, at most 1:4): skip / base / br / eob_base / eob_hi rows of the AV1
+ * class (the mean of the square sizes below and above), dc_sign of the plane,
+ * the eob_pt CDF of the transform's coefficient count (and the luma 1-D form
+ * at 16 / 64 / 128 coefficients), and for luma transforms without a 32-point
+ * side the intra tx-type CDFs per y mode (INTRA1 at TX_4X4 / TX_8X8, INTRA2 at
+ * TX_16X16).  plane: 0 luma, 1 chroma (no chroma 64-point class). */
+int mt_coef_cdfs_default(int32_t qctx, int32_t tx_w, int32_t tx_h, int32_t plane, mt_coef_cdfs* out);
 
 /* ---- batched kernels ------------------------------------------------------ */
 

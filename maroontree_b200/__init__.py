@@ -14,7 +14,7 @@ from .abi import (CANDIDATE_DTYPE, RESULT_DTYPE, ChainParams, CoefCdfs, CoefCost
 
 __all__ = [
     "abi", "load", "Quant", "CoefCdfs", "CoefCosts", "ChainParams", "CANDIDATE_DTYPE", "RESULT_DTYPE",
-    "quant_new", "quant_new_chroma", "qm_row", "default_scan", "coef_costs", "chain_params", "candidate_chain",
+    "quant_new", "quant_new_chroma", "qm_row", "default_scan", "qcat", "coef_cdfs_default", "quality_to_q", "qm_levels", "rd_lambdas", "coef_costs", "chain_params", "candidate_chain",
     "candidate_chain_device", "chain_scratch_bytes", "rdo_level8", "rdo_level8_device", "rdo_level8_scratch_bytes", "rdo_level4", "padded_plane_dims", "csc_rgb8", "deblock_plane", "loop_filter_levels", "deblock_frame", "cdef_params", "cdef_frame", "MtError",
 ]
 
@@ -56,6 +56,40 @@ def qm_row(level, chroma, n):
 def default_scan(n):
     p = load().mt_default_scan(n)
     return np.ctypeslib.as_array((C.c_uint16 * (n * n)).from_address(p)).copy()
+
+
+def quality_to_q(quality):
+    """``quality_to_q`` (src/avif.rs:637-666)."""
+    return load().mt_quality_to_q(quality)
+
+
+def qm_levels(base_q_idx, sub):
+    """(luma, chroma) quantisation-matrix levels of the QM level laws (src/quant.rs:138-167)."""
+    y, uv = C.c_uint8(), C.c_uint8()
+    _check(load().mt_qm_levels(base_q_idx, sub, C.byref(y), C.byref(uv)), "mt_qm_levels")
+    return y.value, uv.value
+
+
+def rd_lambdas(base_q_idx, dc_q, sub, bd=8):
+    """The frame's decision lambdas (``abi.RdLambdas``): mlam, lambda_d, trellis
+    lambda0, the SATD scale and bridge of the luma proxy."""
+    out = abi.RdLambdas()
+    _check(load().mt_rd_lambdas_init(base_q_idx, dc_q, sub, bd, C.byref(out)), "mt_rd_lambdas_init")
+    return out
+
+
+def qcat(base_q_idx):
+    """Coefficient CDF q context of a base qindex (``qcat``, src/coef_q.rs:31-41)."""
+    return load().mt_qcat(base_q_idx)
+
+
+def coef_cdfs_default(qctx, tx_w, tx_h=None, plane=0):
+    """The (class, plane) coefficient slice of the default decision snapshot
+    ``Cdfs::new(qctx)`` (src/coder/cdfs.rs:401-629) for a tx_w x tx_h transform."""
+    c = CoefCdfs()
+    _check(load().mt_coef_cdfs_default(qctx, tx_w, tx_w if tx_h is None else tx_h, plane, C.byref(c)),
+           "mt_coef_cdfs_default")
+    return c
 
 
 def coef_costs(cdfs):

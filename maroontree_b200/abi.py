@@ -181,6 +181,11 @@ assert CANDIDATE_DTYPE.itemsize == 20 and RESULT_DTYPE.itemsize == 32
 _P = C.c_void_p
 
 
+class RdLambdas(C.Structure):
+    _fields_ = [("mode_lambda", C.c_float), ("lambda_d", C.c_float), ("trellis_lambda0", C.c_float),
+                ("satd_scale", C.c_float), ("satd_bridge", C.c_float)]
+
+
 def _bind(lib):
     sig = {
         "mt_version": (C.c_char_p, []),
@@ -189,6 +194,11 @@ def _bind(lib):
         "mt_qm_row": (_P, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "mt_default_scan": (_P, [C.c_int32]),
         "mt_coef_costs_build": (C.c_int, [C.POINTER(CoefCdfs), C.POINTER(CoefCosts)]),
+        "mt_qcat": (C.c_int, [C.c_int32]),
+        "mt_quality_to_q": (C.c_uint8, [C.c_uint8]),
+        "mt_qm_levels": (C.c_int, [C.c_uint8, C.c_int32, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
+        "mt_rd_lambdas_init": (C.c_int, [C.c_uint8, C.c_int32, C.c_int32, C.c_uint8, C.POINTER(RdLambdas)]),
+        "mt_coef_cdfs_default": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(CoefCdfs)]),
         "mt_candidate_chain": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                          _P, C.c_int32, _P, _P, _P]),
         "mt_candidate_chain_device": (C.c_int, [_P, _P, C.POINTER(ChainParams), C.POINTER(Quant), _P, _P, _P,
@@ -299,7 +309,8 @@ def load():
 
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
-    "mt_coef_costs_build", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
+    "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_quality_to_q", "mt_qm_levels",
+    "mt_rd_lambdas_init", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",
     "mt_rdo_level16", "mt_rdo_level16_device", "mt_rdo_level16_scratch_bytes",

@@ -8,9 +8,15 @@ for byte parity, so this script reads them out of the reference's Rust sources
 once and writes a C header that is committed; nothing at run time reads the
 reference.
 
-Usage (from the repository root, with the reference checkout available)::
+Usage (from the repository root, with the reference checkout available; the
+reference root is a required argument)::
 
     python maroontree_b200/csrc/gen_av1_tables.py <reference-root>
+
+It also writes ``av1_cdfs.h``: the AV1 default coefficient CDFs of every
+coefficient q context (the arrays ``Cdfs::new(qctx)`` reads, src/coder/cdfs.rs:401-629)
+and the intra transform-type CDFs, in the AV1 cumulative form the reference
+stores (the inverse form is 32768 - v, src/tables.rs:31-35).
 
 Source locations (reference paths):
   src/coef_q.rs     DC_QLOOKUP_8, AC_QLOOKUP_8/10/12, SCAN_16X16, SCAN_32X32
@@ -18,6 +24,9 @@ Source locations (reference paths):
   src/qm_tables.rs  AV1_IQM  ([15][2][3344] u8)
   src/dct.rs        ADST16_FWD_Q12 ([16][16] i16, the forward 16-point ADST in Q12)
   src/tables.rs     INTRA_FILTER_TAPS ([5][8][7] i8, the recursive filter-intra taps)
+  src/coef_q.rs     SKIP_TX*, BASE_TOK_TX*_Q, BR_TOK_TX*_Q, EOB_BASE_TX*_Q, EOB_HI_TX*,
+                    DC_SIGN_Q, EOB_BIN_*  (av1_cdfs.h)
+  src/tables.rs     TXTP_INTRA1_TX4, TXTP_INTRA1_TX8, TXTP_INTRA2_TX16 (av1_cdfs.h)
 """
 import os
 import re
@@ -65,8 +74,49 @@ def extract(path, name):
     return nums, m.group(1).strip()
 
 
+CDF_TABLES = (
+    [("src/coef_q.rs", f"SKIP_TX{n}") for n in (4, 8, 16, 32, 64)]
+    + [("src/coef_q.rs", f"{k}_TX{n}_{p}_Q") for k in ("BASE_TOK", "BR_TOK", "EOB_BASE")
+       for n in (4, 8, 16, 32) for p in ("LUMA", "CHROMA")]
+    + [("src/coef_q.rs", "BASE_TOK_TX64_LUMA_Q"), ("src/coef_q.rs", "EOB_BASE_TX64_LUMA_Q")]
+    + [("src/coef_q.rs", f"EOB_HI_TX{n}_{p}") for n in (4, 8, 16, 32) for p in ("LUMA", "CHROMA")]
+    + [("src/coef_q.rs", "EOB_HI_TX64_LUMA"), ("src/coef_q.rs", "DC_SIGN_Q")]
+    + [("src/coef_q.rs", f"EOB_BIN_{a}_{p}") for a in (16, 32, 64, 128, 256, 512, 1024)
+       for p in ("LUMA", "CHROMA")]
+    + [("src/coef_q.rs", f"EOB_BIN_{a}_LUMA_1D") for a in (16, 64, 128)]
+    + [("src/tables.rs", "TXTP_INTRA1_TX4"), ("src/tables.rs", "TXTP_INTRA1_TX8"),
+       ("src/tables.rs", "TXTP_INTRA2_TX16")]
+)
+
+
+def write_cdfs(ref):
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "av1_cdfs.h")
+    lines = [
+        "/* Generated by gen_av1_tables.py: the AV1 default coefficient CDFs of every",
+        " * coefficient q context and the intra transform-type CDFs, in the cumulative",
+        " * form the reference stores (inverse form: 32768 - v).  Do not edit. */",
+        "#pragma once",
+        "#include <stdint.h>",
+        "",
+    ]
+    for rel, rname in CDF_TABLES:
+        nums, decl = extract(os.path.join(ref, rel), rname)
+        cname = "MT_CDF_" + rname
+        lines.append(f"/* {rel} {rname}: {decl} ({len(nums)} values) */")
+        lines.append(f"static const uint16_t {cname}[{len(nums)}] = {{")
+        for k in range(0, len(nums), 24):
+            lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
+        lines.append("};")
+        lines.append("")
+    open(out, "w").write("\n".join(lines))
+    print("wrote", out)
+
+
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: gen_av1_tables.py <reference-root>")
+    ref = sys.argv[1]
+    write_cdfs(ref)
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "av1_tables.h")
     lines = [
         "/* Generated by gen_av1_tables.py: normative AV1 tables (dequantiser lookups,",

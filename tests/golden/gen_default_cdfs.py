@@ -1,0 +1,48 @@
+"""Writes cdfs_default.json: every array the coefficient part of the
+reference's ``Cdfs::new(qctx)`` reads (src/coder/cdfs.rs:401-629), for all four
+coefficient q contexts, plus the intra tx-type CDF tables, parsed verbatim from
+the reference's Rust sources (src/coef_q.rs, src/tables.rs).  Nothing is
+computed; the tests assemble the per-(class, plane) slices from these arrays
+following Cdfs::new's field sources and compare them with the library's
+``mt_coef_cdfs_default``.
+
+Run in a checkout that has the reference next to it:
+    python tests/golden/gen_default_cdfs.py /path/to/maroontree
+"""
+import json
+import os
+import sys
+
+from gen_rate_golden import rust_array
+
+NAMES_COEF_Q = (
+    [f"SKIP_TX{n}" for n in (4, 8, 16, 32, 64)]
+    + [f"{k}_TX{n}_{p}_Q" for k in ("BASE_TOK", "BR_TOK", "EOB_BASE") for n in (4, 8, 16, 32)
+       for p in ("LUMA", "CHROMA")]
+    + ["BASE_TOK_TX64_LUMA_Q", "EOB_BASE_TX64_LUMA_Q"]
+    + [f"EOB_HI_TX{n}_{p}" for n in (4, 8, 16, 32) for p in ("LUMA", "CHROMA")]
+    + ["EOB_HI_TX64_LUMA", "DC_SIGN_Q"]
+    + [f"EOB_BIN_{a}_{p}" for a in (16, 32, 64, 128, 256, 512, 1024) for p in ("LUMA", "CHROMA")]
+    + [f"EOB_BIN_{a}_LUMA_1D" for a in (16, 64, 128)]
+)
+NAMES_TABLES = ["TXTP_INTRA1_TX4", "TXTP_INTRA1_TX8", "TXTP_INTRA2_TX16"]
+
+
+def main(ref):
+    q = os.path.join(ref, "src", "coef_q.rs")
+    t = os.path.join(ref, "src", "tables.rs")
+    out = {"source": "src/coef_q.rs, src/tables.rs; assembled as src/coder/cdfs.rs:401-629 Cdfs::new"}
+    for n in NAMES_COEF_Q:
+        out[n] = rust_array(q, n)
+    for n in NAMES_TABLES:
+        out[n] = rust_array(t, n)
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cdfs_default.json")
+    with open(dst, "w") as f:
+        json.dump(out, f, separators=(",", ":"))
+    print(dst)
+
+
+if __name__ == "__main__":
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: gen_default_cdfs.py <reference-root>")
+    main(sys.argv[1])

@@ -136,4 +136,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: gen_rate_golden.py <reference-root>")
+    main(sys.argv[1])
