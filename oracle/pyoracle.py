@@ -441,7 +441,22 @@ def filter_intra_beam(src, recon, w, h, pos, vis=(0, 0), bd=8):
     return scores, modes, preds
 
 
-def split4tx(src, recon, prm, q, qm, cdfs, jobs):
+def _chunked(n, threads, run):
+    """Runs run(lo, hi) over [0, n) in `threads` contiguous chunks on host
+    threads (each chunk is one foreign call; ctypes releases the GIL)."""
+    threads = max(1, min(int(threads), n)) if n else 1
+    if threads == 1:
+        run(0, n)
+        return
+    import concurrent.futures as cf
+
+    bounds = [(n * k // threads, n * (k + 1) // threads) for k in range(threads)]
+    with cf.ThreadPoolExecutor(threads) as ex:
+        for f in [ex.submit(run, lo, hi) for lo, hi in bounds if hi > lo]:
+            f.result()
+
+
+def split4tx(src, recon, prm, q, qm, cdfs, jobs, threads=1):
     """split4tx_try of a batch of 8x8 jobs: (results, cf n x 64, rec n x 8 x 8)."""
     src = np.ascontiguousarray(src, np.uint16)
     recon = np.ascontiguousarray(recon, np.uint16)
@@ -451,12 +466,16 @@ def split4tx(src, recon, prm, q, qm, cdfs, jobs):
     cf = np.zeros((n, 64), np.int32)
     rec = np.zeros((n, 8, 8), np.uint16)
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
-    assert load().or_split4tx(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n, p(res),
-                              p(cf), p(rec)) == 0
+
+    def run(lo, hi):
+        assert load().or_split4tx(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs[lo:hi]),
+                                  hi - lo, p(res[lo:hi]), p(cf[lo:hi]), p(rec[lo:hi])) == 0
+
+    _chunked(n, threads, run)
     return res, cf, rec
 
 
-def leaf8(src, recon, prm, q, qm, cdfs, jobs, refine=False):
+def leaf8(src, recon, prm, q, qm, cdfs, jobs, refine=False, threads=1):
     """pick_block8's luma candidates / refinement of n 8x8 jobs: (results, cf n x 64, rec n x 8 x 8)."""
     src = np.ascontiguousarray(src, np.uint16)
     recon = np.ascontiguousarray(recon, np.uint16)
@@ -466,12 +485,16 @@ def leaf8(src, recon, prm, q, qm, cdfs, jobs, refine=False):
     cf = np.zeros((n, 64), np.int32)
     rec = np.zeros((n, 8, 8), np.uint16)
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
-    assert load().or_leaf8(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
-                           int(bool(refine)), p(res), p(cf), p(rec)) == 0
+
+    def run(lo, hi):
+        assert load().or_leaf8(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs[lo:hi]),
+                           hi - lo, int(bool(refine)), p(res[lo:hi]), p(cf[lo:hi]), p(rec[lo:hi])) == 0
+
+    _chunked(n, threads, run)
     return res, cf, rec
 
 
-def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False):
+def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False, threads=1):
     """pick_luma16's mode-loop candidates / refinement of n 16x16 jobs: (results, cf n x 256, rec n x 16 x 16)."""
     src = np.ascontiguousarray(src, np.uint16)
     recon = np.ascontiguousarray(recon, np.uint16)
@@ -481,8 +504,12 @@ def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False):
     cf = np.zeros((n, 256), np.int32)
     rec = np.zeros((n, 16, 16), np.uint16)
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
-    assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs), n,
-                            int(bool(refine)), p(res), p(cf), p(rec)) == 0
+
+    def run(lo, hi):
+        assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs[lo:hi]),
+                           hi - lo, int(bool(refine)), p(res[lo:hi]), p(cf[lo:hi]), p(rec[lo:hi])) == 0
+
+    _chunked(n, threads, run)
     return res, cf, rec
 
 
@@ -541,3 +568,165 @@ def palette_color_ctx(map_, stride, y, x):
 
 def dirty_log2f(d):
     return load().or_dirty_log2f(d)
+
+
+# ---------------------------------------------------------------------------
+# The default decision snapshot and the frame laws, restated for the checker.
+
+GOLDEN_CDFS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden",
+                           "cdfs_default.json")
+_GOLDEN = None
+
+
+def _golden_cdfs():
+    global _GOLDEN
+    if _GOLDEN is None:
+        import json
+
+        _GOLDEN = json.load(open(GOLDEN_CDFS))
+    return _GOLDEN
+
+
+def _icdf(vals, width):
+    """src/tables.rs:31-35 icdf: 32768 - v per entry, then the terminal 0."""
+    out = np.zeros(width, np.uint16)
+    out[:len(vals)] = [32768 - v for v in vals]
+    return out
+
+
+def default_cdfs(qctx, w, h=None, plane=0):
+    """One (class, plane) coefficient slice of Cdfs::new(qctx)
+    (src/coder/cdfs.rs:401-629) from the reference's arrays
+    (tests/golden/cdfs_default.json): class by the AV1 txSzCtx of w x h, eob_pt
+    CDF by coefficient count (capped at 1024), the 1-D eob_pt CDF for luma
+    16 / 64 / 128, the tx-type CDFs for luma without a 32-point side (INTRA1
+    at square sizes 4 / 8, INTRA2 at 16)."""
+    h = w if h is None else h
+    g = _golden_cdfs()
+    lg = {4: 0, 8: 1, 16: 2, 32: 3, 64: 4}
+    sqr, up = min(lg[w], lg[h]), max(lg[w], lg[h])
+    n = (4, 8, 16, 32, 64)[(sqr + up + 1) >> 1]
+    pl = "CHROMA" if plane else "LUMA"
+    c = abi.CoefCdfs()
+    arr = lambda name: np.ctypeslib.as_array(getattr(c, name))
+    arr("txb_skip")[...] = np.stack([_icdf([v], 2) for v in g[f"SKIP_TX{n}"][qctx]])
+    bt = arr("base_tok")
+    for k, row in enumerate(g[f"BASE_TOK_TX{n}_{pl}_Q"][qctx]):
+        bt[k] = _icdf(row, 4)
+    br = arr("br_tok")
+    for k, row in enumerate(g[f"BR_TOK_TX{min(n, 32)}_{pl}_Q"][qctx]):
+        br[k] = _icdf(row, 4)
+    arr("eob_base")[...] = np.stack([_icdf(r, 3) for r in g[f"EOB_BASE_TX{n}_{pl}_Q"][qctx]])
+    arr("eob_hi")[...] = np.stack([_icdf([v], 2) for v in g[f"EOB_HI_TX{n}_{pl}"][qctx]])
+    arr("dc_sign")[...] = np.stack([_icdf([v], 2) for v in g["DC_SIGN_Q"][qctx][plane]])
+    area = min(w * h, 1024)
+    arr("eob_bin")[...] = _icdf(g[f"EOB_BIN_{area}_{pl}"][qctx], 11)
+    if plane == 0 and area in (16, 64, 128):
+        arr("eob_bin_1d")[...] = _icdf(g[f"EOB_BIN_{area}_LUMA_1D"][qctx], 11)
+    if plane == 0 and up <= 2:
+        tab = g[("TXTP_INTRA1_TX4", "TXTP_INTRA1_TX8", "TXTP_INTRA2_TX16")[sqr]]
+        tx = arr("txtp")
+        for m, row in enumerate(tab):
+            tx[m] = _icdf(row, 16)
+    return c
+
+
+def qcat(q):
+    """src/coef_q.rs:31-41."""
+    return 0 if q <= 20 else 1 if q <= 60 else 2 if q <= 120 else 3
+
+
+def quality_to_q(quality):
+    """src/avif.rs:637-666 quality_to_q."""
+    anchors = [(1, 215), (30, 140), (40, 116), (50, 91), (60, 70), (70, 53), (80, 35), (85, 28), (90, 17),
+               (93, 12), (96, 7), (98, 5), (99, 3), (100, 1)]
+    q = min(max(quality, 1), 100)
+    prev = anchors[0]
+    for l1, q1 in anchors[1:]:
+        if q <= l1:
+            l0, q0 = prev
+            t = q - l0
+            v = q0 + int((q1 - q0) * t / max(l1 - l0, 1))  # Rust i32 division truncates toward zero
+            return min(max(v, 1), 255)
+        prev = (l1, q1)
+    return 1
+
+
+_f32 = np.float32
+
+
+def _fast_round(v):
+    """src/util.rs:36-59 fast_round (x86-64)."""
+    b = np.array([v], _f32).view(np.uint32) + np.uint32(1)
+    u = b.view(_f32)[0]
+    magic = _f32((1 << 23) + (1 << 22))
+    return _f32(_f32(u + magic) - magic)
+
+
+def qm_level_law(q, sub):
+    """src/quant.rs:138-153."""
+    f = _f32
+    qi = f(q)
+    top = f(8.0) if sub else f(15.0)
+    if qi <= 20:
+        return 8 if sub else 15
+    if qi <= 48:
+        return int(_fast_round(f(top + f(f((f(8.0) - top) * f(qi - f(20.0))) / f(28.0)))))
+    if qi >= 128:
+        return 0
+    return int(_fast_round(f(f(f(8.0) * f(f(128.0) - qi)) / f(80.0))))
+
+
+def qm_chroma_level_law(q, sub):
+    """src/quant.rs:155-167 (top_ease 1, qm_hq knee 12 width 5)."""
+    f = _f32
+    if sub:
+        return qm_level_law(q, sub)
+    pinned = min(2, qm_level_law(q, sub))
+    t = f(np.clip(f(f(f(12.0) - f(q)) / f(5.0)), 0, 1))
+    if t > 0:
+        v = f(f(pinned) + f(f(f(15.0) - f(pinned)) * t))
+        return int(np.floor(v + 0.5))
+    return pinned
+
+
+def rd_lambdas(q, dc_q, sub):
+    """The frame's decision lambdas as abi.RdLambdas (8-bit): src/cost.rs:122-148
+    (aom_ssimulacra2_rdmult_weight, mode_lambda_weight), :286-292 (mode_lambda_q),
+    src/partition_rd.rs:30-71 (luma_satd_scale, k_satd),
+    src/coder/lossy_state.rs:1769-1789, :2396-2408, with the shipped tuning."""
+    f = _f32
+    scale = {2: f(0.8), 1: f(0.65), 0: f(0.6)}[sub]
+    w = f(f(min(max(((255 - q) * 3) // 4, 0), 72) + 128) * f(1.0 / 128.0))
+    if sub == 1:
+        weight = f(w * scale)
+    else:
+        r = f(np.clip(f(f(f(q) - f(0.0)) / f(72.0)), 0, 1))
+        weight = f(f(f(3.0) + f(f(w - f(3.0)) * r)) * scale)
+    dc = f(dc_q)
+    mult = f(f(3.3) + f(f(0.0015) * dc))
+    mlq = f(f(f(f(f(0.009005174719460433) * f(1.0)) * dc) * dc) * mult)
+    out = abi.RdLambdas()
+    out.mode_lambda = f(mlq * weight)
+    out.lambda_d = f(f(out.mode_lambda) / f(2.775))
+    out.trellis_lambda0 = f(0.05)
+    qi = f(q)
+    if sub:
+        out.satd_scale = f(1.25)
+    elif qi <= 20:
+        out.satd_scale = f(2.921556)
+    elif qi >= 48:
+        out.satd_scale = f(1.25)
+    else:
+        out.satd_scale = f(f(2.921556) + f(f(f(f(1.25) - f(2.921556)) * f(qi - f(20.0))) / f(28.0)))
+    k = [f(24.5), f(21.3), f(18.2)] if sub else [f(35.0), f(21.2), f(18.1)]
+    if qi <= 28:
+        ks = k[0]
+    elif qi >= 140:
+        ks = k[2]
+    elif qi <= 81:
+        ks = f(k[0] + f(f(f(k[1] - k[0]) * f(qi - f(28.0))) / f(53.0)))
+    else:
+        ks = f(k[1] + f(f(f(k[2] - k[1]) * f(qi - f(81.0))) / f(59.0)))
+    out.satd_bridge = f(f(f(2.775) / ks) * f(7.130643))
+    return out

@@ -1,7 +1,8 @@
 """The default decision snapshot of the library (mt_coef_cdfs_default, the
 coefficient slices of Cdfs::new(qctx), src/coder/cdfs.rs:401-629, and qcat,
 src/coef_q.rs:31-41) against the reference's own arrays parsed from its
-sources (tests/golden/cdfs_default.json), and against the qctx-0 luma slices
+sources (tests/golden/cdfs_default.json, assembled by the oracle's
+default_cdfs), and against the qctx-0 luma slices
 the leaf-trial parity tests were first pinned with.  No device call."""
 import json
 import os
@@ -9,14 +10,13 @@ import os
 import numpy as np
 import pytest
 
-from cdf_snapshot import slice_from_golden
 
 SIZES = [(w, h) for w in (4, 8, 16, 32, 64) for h in (4, 8, 16, 32, 64) if max(w, h) <= 4 * min(w, h)]
 
 
 @pytest.mark.parametrize("qctx", range(4))
 @pytest.mark.parametrize("plane", (0, 1))
-def test_default_slices_match_reference_arrays(mt_lib, qctx, plane):
+def test_default_slices_match_reference_arrays(mt_lib, oracle_lib, qctx, plane):
     for w, h in SIZES:
         cls = ({4: 0, 8: 1, 16: 2, 32: 3, 64: 4}[min(w, h)] + {4: 0, 8: 1, 16: 2, 32: 3, 64: 4}[max(w, h)] + 1) >> 1
         if plane == 1 and cls == 4:
@@ -26,12 +26,12 @@ def test_default_slices_match_reference_arrays(mt_lib, qctx, plane):
                 mt_lib.coef_cdfs_default(qctx, w, h, plane)
             continue
         got = mt_lib.coef_cdfs_default(qctx, w, h, plane)
-        want = slice_from_golden(qctx, w, h, plane)
+        want = oracle_lib.default_cdfs(qctx, w, h, plane)
         assert bytes(got) == bytes(want), (qctx, w, h, plane)
 
 
-def test_qcat_matches_reference_law(mt_lib):
-    want = [0 if q <= 20 else 1 if q <= 60 else 2 if q <= 120 else 3 for q in range(256)]
+def test_qcat_matches_reference_law(mt_lib, oracle_lib):
+    want = [oracle_lib.qcat(q) for q in range(256)]
     assert [mt_lib.qcat(q) for q in range(256)] == want
     # the configs' qindices: q40 -> 116, q60 -> 70, q80 -> 35
     assert (mt_lib.qcat(116), mt_lib.qcat(70), mt_lib.qcat(35)) == (2, 2, 1)
