@@ -356,11 +356,12 @@ size_t mt_rdo_level16_scratch_bytes(int32_t nblocks, int32_t ncombos);
  * file-scope device array of MT_NOALLOC_MAX_BLOCKS entries (1 MiB held on
  * every device that loads the library until exit), and each block's winner is
  * re-evaluated to fill d_best, which equals mt_rdo_level8_device's d_best.
- * More than MT_NOALLOC_MAX_BLOCKS blocks returns MT_ERR_TOO_LARGE.  The first
- * call on a device looks up that array's device address (once per device, with
- * the device current); make that first call before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must not be
- * issued. */
+ * Its input checks and error codes are mt_rdo_level8_device's; beyond them,
+ * more than MT_NOALLOC_MAX_BLOCKS blocks returns MT_ERR_TOO_LARGE.  Every call
+ * looks up that array's device address with the device current (the first
+ * call on a device may load the module, so make it before any stream
+ * capture).  All calls share the array: calls that overlap on the GPU race
+ * and must not be issued. */
 #define MT_NOALLOC_MAX_BLOCKS 131072
 int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_t* d_recon,
                                  const mt_chain_params* prm, const mt_quant* quant,

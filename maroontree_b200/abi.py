@@ -14,6 +14,7 @@ MT_ERR_INVALID_INPUT = -2
 MT_ERR_UNSUPPORTED = -3
 MT_ERR_TOO_LARGE = -4
 MT_NOALLOC_MAX_BLOCKS = 131072
+MT_LEVEL_MAX_COMBOS = 2048
 MT_ERR_DEVICE = -10
 MT_ERR_ALLOC = -11
 MT_EOB_INVALID = -2

@@ -20,9 +20,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <mutex>
-
 #include "chain8.cuh"
+
+namespace mth {
+float scaled_trellis_lambda_host(float dc_q, float lambda0);
+}
 
 namespace {
 
@@ -130,37 +132,16 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_winner_kernel(
   best[b] = o;
 }
 
-// Device address of g_noalloc_keys per device.  The symbol name is only a
-// host-side handle; the address must come from cudaGetSymbolAddress with the
-// device current, once per device.
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kMaxDevices] = {};
-
+// Device address of g_noalloc_keys in the current device's context.  The
+// symbol name is only a host-side handle; the address comes from
+// cudaGetSymbolAddress with the device current.  It is looked up on every call
+// (a table lookup once the module is loaded), so a context that was destroyed
+// and created again (cudaDeviceReset) gets its own array's address.
 int noalloc_keys_address(void** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MT_ERR_DEVICE;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_keys) != cudaSuccess || !p) return MT_ERR_DEVICE;
-    g_noalloc_addr[dev] = p;
-  }
-  *out = g_noalloc_addr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_keys) != cudaSuccess || !p) return MT_ERR_DEVICE;
+  *out = p;
   return MT_OK;
-}
-
-// scaled_trellis_lambda (src/trellis.rs:38-53) with trellis_calib = 1.15,
-// the same left-to-right f32 product the other entry points use.
-float noalloc_trellis_lambda(float dc_q, float lambda0) {
-  const float calib = 0.045025873597302174f * 0.5525f;
-  volatile float a = calib * 1.15f;
-  float aom = a * dc_q;
-  aom = aom * dc_q;
-  float k = 0.0015f * dc_q;
-  k = 3.3f + k;
-  aom = aom * k;
-  return aom * (lambda0 / 0.05f);
 }
 
 }  // namespace
@@ -170,12 +151,16 @@ extern "C" int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_
                                             const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
                                             const mt_block8* d_blocks, int32_t nblocks, const mt_combo* d_combos,
                                             int32_t ncombos, mt_block_best* d_best, void* stream) {
-  if (!prm || !quant || nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
+  // The checks and codes of mt_rdo_level8_device, then this entry point's own
+  // array bound.
+  if (!prm || !quant) return MT_ERR_INVALID_INPUT;
   if (prm->tx_size != 8 || prm->bd != 8) return MT_ERR_UNSUPPORTED;
   if (prm->frame_w <= 0 || prm->frame_h <= 0 || prm->stride < prm->frame_w) return MT_ERR_INVALID_INPUT;
-  if (nblocks > MT_NOALLOC_MAX_BLOCKS) return MT_ERR_TOO_LARGE;
-  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_TOO_LARGE;
+  if (nblocks < 0 || ncombos < 0) return MT_ERR_INVALID_INPUT;
   if (nblocks == 0 || ncombos == 0) return MT_OK;
+  if ((long long)nblocks * ncombos > 0x7fffffffLL) return MT_ERR_INVALID_INPUT;
+  if (ncombos > MT_LEVEL_MAX_COMBOS) return MT_ERR_TOO_LARGE;
+  if (nblocks > MT_NOALLOC_MAX_BLOCKS) return MT_ERR_TOO_LARGE;
   if (!d_src || !d_recon || !d_costs || !d_blocks || !d_combos || !d_best) return MT_ERR_INVALID_INPUT;
   void* keys_addr = nullptr;
   int rc = noalloc_keys_address(&keys_addr);
@@ -185,7 +170,7 @@ extern "C" int mt_rdo_level8_device_noalloc(const uint16_t* d_src, const uint16_
   NoAllocArgs a;
   a.p = *prm;
   a.q = *quant;
-  a.trellis_lambda = noalloc_trellis_lambda((float)quant->dc_q, prm->trellis_lambda0);
+  a.trellis_lambda = mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0);
   a.has_qm = d_qm_row != nullptr;
   if (cudaMemsetAsync(keys, 0xff, (size_t)nblocks * sizeof(unsigned long long), st) != cudaSuccess)
     return MT_ERR_DEVICE;

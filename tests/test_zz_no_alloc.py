@@ -19,7 +19,7 @@ from maroontree_b200 import abi, synth
 pytestmark = pytest.mark.gpu
 
 
-def _level(oracle_lib, w, h, seed, qidx, qm_level):
+def _level(oracle_lib, w, h, seed, qidx, qm_level, vis=None):
     import maroontree_b200 as mt
 
     src = synth.rgb_to_luma(synth.generate_rgb(w, h, seed))
@@ -30,7 +30,7 @@ def _level(oracle_lib, w, h, seed, qidx, qm_level):
     q = oracle_lib.quant_new(qidx, 8, qm_level)
     qm = oracle_lib.qm_row(qm_level, 0, 8)
     costs = mt.coef_costs(synth.synthetic_cdfs(seed))
-    prm = mt.chain_params(w, h, trellis_lambda0=0.05, mode_lambda=0.3 * qidx + 2.0, satd_bridge=0.8)
+    prm = mt.chain_params(w, h, trellis_lambda0=0.05, mode_lambda=0.3 * qidx + 2.0, satd_bridge=0.8, vis=vis)
     return src, rec, blocks, combos, q, qm, costs, prm
 
 
@@ -66,6 +66,24 @@ def test_noalloc_level_matches_level_entry_point_twice(mt_lib, oracle_lib, cuda)
         ref, got = _run_both(mt_lib, cuda, case)
         assert np.all(ref["combo"] >= 0)
         assert got.tobytes() == ref.tobytes()
+
+
+def test_noalloc_displayed_window_matches_level_entry_point(mt_lib, oracle_lib, cuda):
+    """A frame displayed smaller than it is coded takes the masked kernel form."""
+    case = _level(oracle_lib, 96, 64, 24, 70, 6, vis=(91, 59))
+    ref, got = _run_both(mt_lib, cuda, case)
+    assert np.all(ref["combo"] >= 0)
+    assert got.tobytes() == ref.tobytes()
+
+
+def test_noalloc_checks_match_level_entry_point(mt_lib, oracle_lib, cuda):
+    """Same input errors and codes as mt_rdo_level8_device (no device work)."""
+    src, rec, blocks, combos, q, qm, costs, prm = _level(oracle_lib, 64, 64, 25, 70, 6)
+    lib = mt_lib.load()
+    for nb, nc in ((70000, 40000), (4, abi.MT_LEVEL_MAX_COMBOS + 1), (-1, 3)):
+        a = lib.mt_rdo_level8_device(1, 1, C.byref(prm), C.byref(q), None, 1, 1, nb, 1, nc, 1, 1, 1, None)
+        b = lib.mt_rdo_level8_device_noalloc(1, 1, C.byref(prm), C.byref(q), None, 1, 1, nb, 1, nc, 1, None)
+        assert a == b != abi.MT_OK, (nb, nc, a, b)
 
 
 def test_noalloc_rejects_more_blocks_than_its_array(mt_lib, oracle_lib, cuda):
