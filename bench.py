@@ -41,37 +41,88 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-W, H, QIDX, QM_LEVEL = 1920, 1080, 70, 6
-# From one ncu capture of level8_kernel on this workload
-# (ncu --set full -k regex:"^level[48]_kernel$" ... python bench.py --steps 1 --warmup 3 --no-cpu):
-NCU_DRAM_BYTES_PER_LAUNCH = 198_752_000 + 1_367_270_000  # dram__bytes_read.sum + dram__bytes_write.sum
-NCU_WARP_INSTS_PER_LAUNCH = 1_224_376_834  # smsp__inst_executed.sum
-ISSUE_PEAK_PER_CLK = 148 * 4  # SMs x schedulers, one warp-instruction each per clock
+W, H, SEED, QUALITY, SUB = 1920, 1080, 3, 60, 2  # the 1080p 4:2:0 quality-60 frame
 MODES = list(range(13))
 MPIX = W * H / 1e6
+METRIC = "MPix/s (8x8 RDO level, 1080p luma)"
+SMS, LANES_PER_SM = 148, 128  # B200: SMs x INT32/FP32 lanes per SM
+# DRAM bytes of one level8_kernel launch on this workload, dram__bytes_read.sum
+# + dram__bytes_write.sum of the ncu capture in profiles/level8_kernel_1080p_q60.md
+NCU_DRAM_BYTES_PER_LAUNCH = 198_752_000 + 1_367_270_000
+
+# Algorithmic integer / FP32 operations of one 8x8 candidate chain, counted on
+# the oracle's scalar restatement (oracle/oracle_chain.cpp; one add, sub, mul,
+# shift, min, max, compare, select, convert or float op each; a clamp is two):
+#   prediction per mode (DC 40, V/H 0, directional 600 with the edge filter,
+#   SMOOTH 512, SMOOTH_V/H 256, PAETH 640), residual 64,
+#   forward 2-D (dct1d_8 = 62 ops, the Q12 ADST8 = 144 per 1-D pass; IDTX 256),
+#   quantisation + f32 targets 11 per coefficient (704), the QM re-rounding 8 per
+#   coefficient (512) on the 2-D types, dequantisation 192,
+#   inverse 2-D (inv_dct8 = 98, inv_adst8 = 140 per 1-D pass, plus the 256-op
+#   intermediate clip and the 128-op final rounding; IDTX 512),
+#   SATD bridge 770 (reconstruction difference 256, 8x8 Hadamard 384 + |.| and
+#   sum 127, scaling), RD cost 20,
+#   and per coefficient up to the end of block 22 (trellis round-down and EOB
+#   trim) + 12 (the rate walk's context and token costs).
+PRED_OPS = {0: 40, 1: 0, 2: 0, 9: 512, 10: 256, 11: 256, 12: 640}  # directional modes 3..8: 600
+FWD_OPS = {0: 256, 1: 992, 4: 2304, 5: 1648, 6: 1648}
+INV_OPS = {0: 512, 1: 1952, 4: 2624, 5: 2288, 6: 2288}
+QUANT_OPS, QM_OPS, DEQUANT_OPS, RESID_OPS, SATD_OPS, RD_OPS, PER_COEF_OPS = 704, 512, 192, 64, 770, 20, 34
 
 
-def make_workload(seed=3):
-    import maroontree_b200 as mt
+def chain_ops(combos, results, nblocks, qm_on):
+    """Algorithmic operations of every candidate of a level (combo-major
+    results): the fixed part by (mode, type) plus the per-coefficient part up to
+    each candidate's own end of block."""
+    fixed = np.array([PRED_OPS.get(int(m), 600) + RESID_OPS + FWD_OPS[int(t)] + QUANT_OPS
+                      + (QM_OPS if qm_on and int(t) != 0 else 0) + DEQUANT_OPS + INV_OPS[int(t)] + SATD_OPS + RD_OPS
+                      for m, t in zip(combos["mode"], combos["tx_type"])], np.int64)
+    eob = results["eob"].astype(np.int64).reshape(len(combos), nblocks)
+    coefs = np.where((eob >= 0) & (eob < 64), eob + 1, 0).sum(axis=1)
+    return int((fixed * nblocks).sum() + PER_COEF_OPS * coefs.sum())
+
+
+def config_line(nb, nc):
+    """The config object both arms print."""
+    return {"workload": "rdo-level-8x8 1920x1080 4:2:0 quality 60 (qindex 70, QM 6), seed 3: every 8x8 luma block "
+                        "x 13 intra modes x 5 transform types (IDTX, DCT_DCT, ADST_ADST, ADST_DCT, DCT_ADST)",
+            "cdfs": "default decision snapshot Cdfs::new(qctx 2)", "lambdas": "shipped Slow laws at qindex 70 4:2:0",
+            "candidates": nb * nc, "blocks": nb, "combos": nc, "l2": "inputs re-read after an L2 flush per step"}
+
+
+def make_workload(impl="ours"):
+    """The headline workload.  The quantiser, QM row, lambdas and default CDFs
+    come from the CUDA library's C ABI for our arm and from the oracle's
+    restatement for the reference arm (which must not load the library)."""
+    import maroontree_b200 as mt  # numpy / ctypes host helpers; the CUDA library loads on first call only
     from maroontree_b200 import abi, synth
 
-    rgb = synth.generate_rgb(W, H, seed, sigma=4.0, variant="1080p")
+    if impl == "ours":
+        qidx = mt.quality_to_q(QUALITY)
+        qm_level = mt.qm_levels(qidx, SUB)[0]
+        q = mt.quant_new(qidx, 8, qm_level)
+        qm = mt.qm_row(qm_level, 0, 8)
+        lam = mt.rd_lambdas(qidx, q.dc_q, SUB)
+        cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 0)
+    else:
+        from oracle import pyoracle as po
+
+        qidx = po.quality_to_q(QUALITY)
+        qm_level = po.qm_level_law(qidx, SUB)
+        q = po.quant_new(qidx, 8, qm_level)
+        qm = po.qm_row(qm_level, 0, 8)
+        lam = po.rd_lambdas(qidx, q.dc_q, SUB)
+        cdfs = po.default_cdfs(po.qcat(qidx), 8)
+    rgb = synth.generate_rgb(W, H, SEED, sigma=4.0, variant="1080p")
     src = synth.rgb_to_luma(rgb)
-    rec = synth.synthetic_recon(src, seed + 1000)
-    blocks = synth.level_blocks(W, H, seed=seed)
+    rec = synth.synthetic_recon(src, SEED + 1000)
+    blocks = synth.level_blocks(W, H, seed=SEED)
     combos = synth.level_combos(MODES, abi.TX_2D_SCAN_TYPES)
     cands = synth.candidates_of_level(blocks, combos)
-    cdfs = synth.synthetic_cdfs(seed)
-    q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 8)
-    # lambdas of the luma proxy at qindex 70 4:2:0 (mode_lambda_q(dc_q) x weight,
-    # luma_satd_scale = satd_base 1.25, bridge K_PART_LAMBDA / k_satd * 7.130643)
-    dcq = float(q.dc_q)
-    mlam = 0.009005174719460433 * dcq * dcq * (3.3 + 0.0015 * dcq) * 0.8
-    k_satd = 24.5 + (21.3 - 24.5) * (QIDX - 28.0) / (81.0 - 28.0)
-    prm = mt.chain_params(W, H, trellis_lambda0=0.05, mode_lambda=mlam, satd_scale=1.25,
-                          satd_bridge=2.775 / k_satd * 7.130643)
-    return dict(src=src, rec=rec, blocks=blocks, combos=combos, cands=cands, cdfs=cdfs, q=q, qm=qm, prm=prm, rgb=rgb)
+    prm = mt.chain_params(W, H, trellis_lambda0=lam.trellis_lambda0, mode_lambda=lam.mode_lambda,
+                          satd_scale=lam.satd_scale, satd_bridge=lam.satd_bridge)
+    return dict(src=src, rec=rec, blocks=blocks, combos=combos, cands=cands, cdfs=cdfs, q=q, qm=qm, prm=prm, rgb=rgb,
+                qidx=qidx, qm_level=qm_level, lam=lam)
 
 
 class ClockSampler:
@@ -171,45 +222,42 @@ class Replicas:
             self.dist = None
 
 
-def cpu_rate(wl, sample, threads):
-    """Oracle throughput (candidates/s) over a bounded slice of the candidates."""
+def cpu_level(wl, threads):
+    """The oracle over every candidate of the level on `threads` host cores:
+    (results, seconds)."""
     from oracle import pyoracle as po
 
-    cands = wl["cands"][:sample]
     t0 = time.perf_counter()
-    po.candidate_chain(wl["src"], wl["rec"], wl["prm"], wl["q"], wl["qm"], wl["cdfs"], cands, threads=threads)
-    dt = time.perf_counter() - t0
-    return len(cands) / dt, dt
+    res, _, _ = po.candidate_chain(wl["src"], wl["rec"], wl["prm"], wl["q"], wl["qm"], wl["cdfs"], wl["cands"],
+                                   threads=threads)
+    return res, time.perf_counter() - t0
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference (the oracle; the
+    Rust reference cannot be built here) over the same level on all host cores.
+    Its workload comes from the oracle alone; the CUDA library is never loaded."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
     from oracle import build as obuild
 
     obuild.build()
-    wl = make_workload()
+    wl = make_workload("reference")
     threads = os.cpu_count() or 1
-    n_all = len(wl["cands"])
-    sample = n_all  # the whole level: ~1.5 s on 8 cores
+    nb, nc = len(wl["blocks"]), len(wl["combos"])
     for _ in range(args.warmup):
-        cpu_rate(wl, min(sample, 50_000), threads)
-    times = []
-    for _ in range(args.steps):
-        rate, dt = cpu_rate(wl, sample, threads)
-        times.append(dt)
+        cpu_level(dict(wl, cands=wl["cands"][:50_000]), threads)
+    times = [cpu_level(wl, threads)[1] for _ in range(args.steps)]
     step_s = float(np.mean(times))
     value = MPIX / step_s
     line = {
-        "impl": "reference", "metric": "MPix/s (8x8 RDO level, 1080p luma)", "value": round(value, 4),
+        "impl": "reference", "metric": METRIC, "value": round(value, 4),
         "unit": "MPix/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int32+f32", "data": "synthetic",
-        "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
-                   "candidates": n_all},
+        "dtype": "int32+f32", "data": "synthetic", "config": config_line(nb, nc),
         "cpu_baseline": {"value": round(value, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
-                         "sample": f"all {n_all} candidates of the level per step"},
+                         "sample": f"every candidate of the level ({nb * nc}) per step"},
         "e2e": {"value": round(value, 4), "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -228,22 +276,22 @@ def measure_small_level(dev, wl, n, reps=5, cpu=True):
     import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
-    q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, n)
-    blocks = synth.level_blocks(W, H, n=n, seed=3)
+    q = wl["q"]
+    qm = mt.qm_row(wl["qm_level"], 0, n)
+    blocks = synth.level_blocks(W, H, n=n, seed=SEED)
     if n == 4:
         combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX, abi.TX_ADST_DCT,
                                             abi.TX_DCT_ADST), no_trellis_types=(abi.TX_IDTX,))
-        cdfs = synth.synthetic_cdfs(4, n_eob_bins=5)
+        cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), 4, 4, 0)
         entry, scratch_fn = "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes"
         what = "rdo-level-4x4 1920x1080 luma, qindex 70, QM 6, 13 modes x 5 types (IDTX without trellis)"
     else:
         combos = synth.level_combos(MODES, (abi.TX_DCT_DCT, abi.TX_ADST_ADST, abi.TX_IDTX))
-        cdfs = synth.synthetic_cdfs(4, n_eob_bins=9)
+        cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), 16, 16, 0)
         entry, scratch_fn = "mt_rdo_level16_device", "mt_rdo_level16_scratch_bytes"
         what = "rdo-level-16x16 1920x1080 luma, qindex 70, QM 6, 13 modes x 3 types (DCT, ADST, IDTX)"
     costs = mt.coef_costs(cdfs)
-    prm = mt.chain_params(W, H, tx_size=n, trellis_lambda0=0.05, mode_lambda=wl["prm"].mode_lambda,
+    prm = mt.chain_params(W, H, tx_size=n, trellis_lambda0=wl["lam"].trellis_lambda0, mode_lambda=wl["prm"].mode_lambda,
                           satd_scale=wl["prm"].satd_scale, satd_bridge=wl["prm"].satd_bridge)
     nb, nc = len(blocks), len(combos)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
@@ -299,13 +347,13 @@ def measure_split16(dev, wl, search, reps=5, cpu=True, depth2=False):
     import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
-    q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 4 if depth2 else 8)
-    cdfs = synth.synthetic_cdfs(4, n_eob_bins=5) if depth2 else synth.synthetic_cdfs(4)
+    q = wl["q"]
+    qm = mt.qm_row(wl["qm_level"], 0, 4 if depth2 else 8)
+    cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), 4 if depth2 else 8, 4 if depth2 else 8, 0)
     costs = mt.coef_costs(cdfs)
-    jobs = synth.split16_jobs(W, H, MODES, seed=3)
+    jobs = synth.split16_jobs(W, H, MODES, seed=SEED)
     n = len(jobs)
-    prm = mt.split16_params(W, H, trellis_lambda0=0.05, rd_lambda=wl["prm"].mode_lambda, band_tilt=1.9,
+    prm = mt.split16_params(W, H, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].lambda_d, band_tilt=1.9,
                             tx_search=search, tx_guard_shift=5 if search else 4)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
@@ -370,13 +418,13 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
-    q = mt.quant_new(QIDX, 8, QM_LEVEL)
-    qm = mt.qm_row(QM_LEVEL, 0, 16 if n16 else 8)
-    cdfs = synth.synthetic_cdfs(4, n_eob_bins=9) if n16 else synth.synthetic_cdfs(4)
+    q = wl["q"]
+    qm = mt.qm_row(wl["qm_level"], 0, 16 if n16 else 8)
+    cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), 16 if n16 else 8, 16 if n16 else 8, 0)
     costs = mt.coef_costs(cdfs)
-    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=3, n=16 if n16 else 8)
+    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=SEED, n=16 if n16 else 8)
     n = len(jobs)
-    prm = mt.split16_params(W, H, trellis_lambda0=0.05, rd_lambda=wl["prm"].mode_lambda, band_tilt=1.9,
+    prm = mt.split16_params(W, H, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].lambda_d, band_tilt=1.9,
                             tx_search=refine, tx_guard_shift=5)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
@@ -417,13 +465,14 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     if cpu:
         from oracle import pyoracle as po
 
+        threads = os.cpu_count() or 1
         t0 = time.perf_counter()
         if n16:
-            po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
+            po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine, threads=threads)
         else:
-            po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine)
+            po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine, threads=threads)
         dt = time.perf_counter() - t0
-        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": 1, "kind": "port",
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
                                "sample": f"all {n} jobs ({dt:.2f} s)"}
     return out
 
@@ -481,7 +530,7 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     nsb = ((pw + 63) // 64) * ((ph + 63) // 64)
     cells = torch.empty(nsb * 4, dtype=torch.uint8, device=dev)
     refs = torch.empty(2 * 64, dtype=torch.float32, device=dev)
-    for tag, q in (("aq_grid", QIDX), ("aq_grid_q116", 116)):
+    for tag, q in (("aq_grid", wl["qidx"]), ("aq_grid_q116", 116)):
         ap = mt.aq_params(pw, ph, q)
         ascr = torch.empty(lib.mt_aq_grid_scratch_bytes(C.byref(ap)), dtype=torch.uint8, device=dev)
         ms = timed(lambda: lib.mt_aq_grid_device(y.data_ptr(), C.byref(ap), cells.data_ptr(), refs.data_ptr(),
@@ -492,7 +541,7 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     # text / UI / photo frame of the same size runs the copy stage too
     for tag, lum in (("screen_gate_photo", y), ("screen_gate_mixed",
                      torch.from_numpy(synth.screen_luma(pw, ph, 5, photo_frac=0.3).view(np.int16)).to(dev))):
-        sp = mt.screen_gate_params(pw, ph, 1, 1, QIDX)
+        sp = mt.screen_gate_params(pw, ph, 1, 1, wl["qidx"])
         sscr = torch.empty(lib.mt_screen_gate_scratch_bytes(C.byref(sp)), dtype=torch.uint8, device=dev)
         sres = abi.ScreenGateResult()
         ms = timed(lambda: lib.mt_screen_gate_device(lum.data_ptr(), C.byref(sp), sscr.data_ptr(), C.byref(sres),
@@ -553,7 +602,7 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     g = abi.DeblockFrameParams()
     g.w8, g.h8, g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = pw, ph, W, H, 1, 1, 0, 8
     scr = torch.empty(max(1, lib.mt_deblock_frame_scratch_bytes(C.byref(g))), dtype=torch.uint8, device=dev)
-    ly, luv, _ = mt.loop_filter_levels(QIDX, 1, 1)
+    ly, luv, _ = mt.loop_filter_levels(wl["qidx"], 1, 1)
 
     def reset_db():
         for a, b in zip(dp, d0):
@@ -566,7 +615,7 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     out["deblock"]["levels"] = [ly, luv, luv]
     # CDEF: the table pass alone (device events) and the whole frame (host search inside)
     src, rec, skip = synth.cdef_inputs(W, H, 1, 1, False, 3)
-    prm = mt.cdef_params(W, H, 1, 1, QIDX)
+    prm = mt.cdef_params(W, H, 1, 1, wl["qidx"])
     r0 = [t16(p) for p in rec]
     rr = [p.clone() for p in r0]
     ss = [t16(p) for p in src]
@@ -659,20 +708,27 @@ def run_ours(args):
     h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + blocks.nbytes + combos.nbytes
     d2h = nb * abi.BEST_DTYPE.itemsize
 
-    # roofline of the level kernel against HBM: algorithmic bytes per launch =
-    # per candidate the result record (32 B) + source block (64 x 2 B) +
-    # neighbour edges (up to 33 x 2 B); per block its record (60 B)
-    alg_bytes = n * (32 + 128 + 66) + nb * 60
+    # roofline of the level (four launches; level8_kernel is ~99 % of them in
+    # profiles/bench_launch_list_1080p_q60.md) against the SMs' INT32/FP32 issue
+    # rate: algorithmic operations of every candidate (chain_ops: the per-stage
+    # table above, the per-coefficient part up to each candidate's own end of
+    # block, read from this run's results) over the mean device time.
+    res_gpu = d_res.cpu().numpy().view(abi.RESULT_DTYPE)
+    ops = chain_ops(combos, res_gpu, nb, wl["qm"] is not None)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    achieved = alg_bytes / (step_ms / 1e3) / 1e9
-    clk_mhz = peaks.get("sm_max_mhz", 1965.0)
-    issue_peak = ISSUE_PEAK_PER_CLK * clk_mhz * 1e6
-    issue_rate = NCU_WARP_INSTS_PER_LAUNCH / (step_ms / 1e3)
+    clocks = clk.summary()
+    clk_mhz = clocks.get("sm_mhz") or 1965.0
+    op_peak = SMS * LANES_PER_SM * clk_mhz * 1e6  # thread operations per second at the sampled SM clock
+    achieved = ops / (step_ms / 1e3)
+    # HBM view of the same launch: per candidate the result record (32 B) +
+    # source block (64 x 2 B) + neighbour edges (up to 33 x 2 B); per block its
+    # record (60 B)
+    alg_bytes = n * (32 + 128 + 66) + nb * 60
 
     filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
     level4 = measure_small_level(dev, wl, 4, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
@@ -687,33 +743,37 @@ def run_ours(args):
         leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=world == 1 and not args.no_cpu, n16=True)
         leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=world == 1 and not args.no_cpu, n16=True)
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import build as obuild
 
         obuild.build()
         threads = os.cpu_count() or 1
-        rate, dt = cpu_rate(wl, n, threads)  # the same candidates, combo-major
+        ref, dt = cpu_level(wl, threads)  # the same candidates, combo-major
         cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
                "sample": f"the whole level, {n} candidates ({dt:.2f} s)"}
+        # the timed level's results must be the oracle's, bit for bit
+        parity = {"results_equal_oracle": res_gpu.tobytes() == ref.tobytes(), "candidates": n}
+        if not parity["results_equal_oracle"]:
+            raise SystemExit("bench: the GPU level's results differ from the oracle's")
 
     line = {
-        "metric": "MPix/s (8x8 RDO level, 1080p luma)", "value": round(value, 3), "unit": "MPix/s",
+        "metric": METRIC, "value": round(value, 3), "unit": "MPix/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f32",
-        "data": "synthetic",
-        "config": {"workload": "rdo-level-8x8 1920x1080 4:2:0 q60 (qindex 70, QM 6), 13 modes x 5 tx types",
-                   "candidates": n, "blocks": nb, "combos": nc, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between timed launches"},
+        "data": "synthetic", "config": config_line(nb, nc),
+        "parallelism": f"replicas x{world}",
         "e2e": {"value": round(ranks.job_value(e2e_s * 1e3), 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm_peak, "unit": "GB/s",
-                     "frac": round(achieved / hbm_peak, 5), "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
-                     "kernel": "level8_kernel", "alg_bytes_per_launch": alg_bytes,
-                     "note": "integer/FP32 issue-bound kernel; see issue_roofline"},
-        "issue_roofline": {"achieved_ginst_s": round(issue_rate / 1e9, 1),
-                           "peak_ginst_s": round(issue_peak / 1e9, 1), "frac": round(issue_rate / issue_peak, 4),
-                           "inst_per_launch": NCU_WARP_INSTS_PER_LAUNCH, "sm_clock_mhz": clk_mhz},
+        "roofline": {"bound": "int32/fp32 issue", "achieved": round(achieved / 1e12, 3),
+                     "peak": round(op_peak / 1e12, 3), "unit": "Tops/s", "frac": round(achieved / op_peak, 4),
+                     "traffic": NCU_DRAM_BYTES_PER_LAUNCH, "kernel": "level8_kernel (+ its run/pred/finalize launches)",
+                     "ops_per_launch": ops, "alg_bytes_per_launch": alg_bytes,
+                     "hbm": {"achieved_gbs": round(alg_bytes / (step_ms / 1e3) / 1e9, 1), "peak_gbs": hbm_peak,
+                             "frac": round(alg_bytes / (step_ms / 1e3) / 1e9 / hbm_peak, 4)},
+                     "peak_basis": f"{SMS} SMs x {LANES_PER_SM} INT32/FP32 lanes x the sampled SM clock "
+                                   f"({clk_mhz:.0f} MHz); no measured integer peak exists"},
+        "parity": parity,
         "frame_filters": filters,
         "level4": level4,
         "level16": level16,
@@ -721,7 +781,7 @@ def run_ours(args):
         "leaf8": leaf8,
         # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
         "gpu_launches": 4 * args.steps,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "cpu_baseline": cpu,
     }
     ranks.emit(line)
