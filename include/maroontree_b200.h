@@ -15,6 +15,9 @@
  *                                         src/cost.rs:156-190 cdf_cost_with_table
  *   mt_qcat / mt_coef_cdfs_default        src/coef_q.rs:31-41 qcat, src/coder/cdfs.rs:401-629
  *                                         Cdfs::new (the coefficient slices)
+ *   mt_range_encoder_* / mt_cdfs_default  src/odec.rs:35-615 OdEcEncoder, src/coder/cdfs.rs:193-629
+ *   mt_pack_tile                          src/coder/wavefront.rs:617-657 pack_wavefront_tile
+ *   mt_replay_tile_with_filters           src/coder/tile_encode.rs:404-466 replay_tile_with_filters
  *   mt_quality_to_q / mt_qm_levels /      src/avif.rs:637-666 quality_to_q, src/quant.rs:122-167
  *   mt_rd_lambdas_init                    QM level laws, src/cost.rs + src/partition_rd.rs lambdas
  *   mt_candidate_chain[_device]           the per-candidate chain of the luma mode
@@ -931,6 +934,62 @@ int mt_screen_gate(const uint16_t* luma, const mt_screen_gate_params* prm, mt_sc
 
 /* Library version string. */
 const char* mt_version(void);
+
+
+/* ---- Entropy coding, tile packing and filter replay (host) ----------------
+ * The AV1 multi-symbol range coder of src/odec.rs:35-615 (OdEcEncoder): CDFs
+ * are inverse-form u16 arrays whose last entry is the adaptation counter
+ * (src/tables.rs:31-35 icdf); a CDF of len entries codes len symbols.
+ * mt_range_encoder_* replace OdEcEncoder::{new, encode_bool, encode_symbol,
+ * encode_symbol_noupdate, encode_literal, encode_signed_subexp_with_ref, done}
+ * (src/odec.rs:236-253, :427-600). */
+typedef struct mt_range_encoder mt_range_encoder;
+mt_range_encoder* mt_range_encoder_new(int32_t updating_cdf);
+void mt_range_encoder_free(mt_range_encoder* e);
+int mt_range_encode_bool(mt_range_encoder* e, int32_t value, uint16_t f);
+/* adapt != 0: encode_symbol (adapts cdf in place when the encoder updates
+ * CDFs); adapt == 0: encode_symbol_noupdate. */
+int mt_range_encode_symbol(mt_range_encoder* e, int32_t s, uint16_t* cdf, int32_t len, int32_t adapt);
+int mt_range_encode_literal(mt_range_encoder* e, uint32_t value, uint32_t bits);
+int mt_range_encode_signed_subexp_with_ref(mt_range_encoder* e, int32_t v, int32_t low, int32_t high, uint32_t k,
+                                           int32_t r);
+/* Flushes, returns the bytes (free with mt_free) and frees the encoder. */
+int mt_range_encoder_done(mt_range_encoder* e, uint8_t** out, size_t* out_len);
+
+/* The frame-initial CDF set Cdfs::new(qctx) (src/coder/cdfs.rs:401-629) as
+ * slots in Cdfs::semantic_slots order (src/coder/cdfs.rs:193-355): slot i is
+ * data[offsets[i] .. offsets[i] + lens[i]).  With all three arrays NULL only
+ * the sizes are returned. */
+int32_t mt_cdf_slot_count(void);
+int mt_cdfs_default(int32_t qctx, uint16_t* data, size_t data_cap, uint32_t* offsets, uint16_t* lens,
+                    int32_t slots_cap, size_t* data_len, int32_t* nslots);
+
+/* One tile's packer: pack_wavefront_tile (src/coder/wavefront.rs:617-657).
+ * The superblocks' semantic token streams (EntropyTokens, src/odec.rs:96-108:
+ * two tag bits, adaptive symbol (slot << 8 | s), bool (f << 1 | v), gathered
+ * partition bool (slot << 2 | split << 1 | top), non-adapting symbol) are
+ * replayed in raster order against Cdfs::new(qcat(base_q_idx)) (replay_semantic,
+ * src/odec.rs:315-360).  Superblock i's tokens are ops[sb_start[i] ..
+ * sb_start[i + 1]) (sb_start has nsb + 1 entries); sb_cdef_point[i] is the
+ * index within them of its read_cdef() point, or -1 (NULL: none).  Returns
+ * the payload (free with mt_free) and, when trace is non-NULL, the symbol
+ * trace the filter replay needs (free with mt_tile_trace_free).  A token that
+ * names no slot or a symbol outside its CDF returns MT_ERR_INVALID_INPUT. */
+typedef struct mt_tile_trace mt_tile_trace;
+int mt_pack_tile(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, const uint32_t* sb_start,
+                 const int32_t* sb_cdef_point, int32_t nsb, uint8_t** payload, size_t* payload_len,
+                 mt_tile_trace** trace);
+void mt_tile_trace_free(mt_tile_trace* t);
+/* replay_tile_with_filters (src/coder/tile_encode.rs:404-466) without loop
+ * restoration: the trace re-emitted superblock by superblock in raster order
+ * over the tile (x0, y0, w, h), with the 64x64 unit's cdef_idx (cdef_grid,
+ * unit_cols per row, cdef_bits wide) as a raw literal at each recorded
+ * read_cdef() point; cdef_grid NULL replays the trace as is. */
+int mt_replay_tile_with_filters(const mt_tile_trace* t, int32_t tile_x0, int32_t tile_y0, int32_t tile_w,
+                                int32_t tile_h, const uint8_t* cdef_grid, int32_t unit_cols, int32_t grid_len,
+                                int32_t cdef_bits, int32_t updating_cdf, uint8_t** out, size_t* out_len);
+/* Frees a buffer this library returned. */
+void mt_free(void* p);
 
 #ifdef __cplusplus
 }

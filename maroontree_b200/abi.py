@@ -196,6 +196,24 @@ def _bind(lib):
         "mt_default_scan": (_P, [C.c_int32]),
         "mt_coef_costs_build": (C.c_int, [C.POINTER(CoefCdfs), C.POINTER(CoefCosts)]),
         "mt_qcat": (C.c_int, [C.c_int32]),
+        "mt_range_encoder_new": (_P, [C.c_int32]),
+        "mt_range_encoder_free": (None, [_P]),
+        "mt_range_encode_bool": (C.c_int, [_P, C.c_int32, C.c_uint16]),
+        "mt_range_encode_symbol": (C.c_int, [_P, C.c_int32, _P, C.c_int32, C.c_int32]),
+        "mt_range_encode_literal": (C.c_int, [_P, C.c_uint32, C.c_uint32]),
+        "mt_range_encode_signed_subexp_with_ref": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_uint32,
+                                                             C.c_int32]),
+        "mt_range_encoder_done": (C.c_int, [_P, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+        "mt_cdf_slot_count": (C.c_int32, []),
+        "mt_cdfs_default": (C.c_int, [C.c_int32, _P, C.c_size_t, _P, _P, C.c_int32, C.POINTER(C.c_size_t),
+                                      C.POINTER(C.c_int32)]),
+        "mt_pack_tile": (C.c_int, [C.c_uint8, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(_P),
+                                   C.POINTER(C.c_size_t), C.POINTER(_P)]),
+        "mt_tile_trace_free": (None, [_P]),
+        "mt_replay_tile_with_filters": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
+                                                  C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P),
+                                                  C.POINTER(C.c_size_t)]),
+        "mt_free": (None, [_P]),
         "mt_quality_to_q": (C.c_uint8, [C.c_uint8]),
         "mt_qm_levels": (C.c_int, [C.c_uint8, C.c_int32, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
         "mt_rd_lambdas_init": (C.c_int, [C.c_uint8, C.c_int32, C.c_int32, C.c_uint8, C.POINTER(RdLambdas)]),
@@ -310,7 +328,10 @@ def load():
 
 EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
-    "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_quality_to_q", "mt_qm_levels",
+    "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_range_encoder_new", "mt_range_encoder_free",
+    "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
+    "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default",
+    "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free", "mt_quality_to_q", "mt_qm_levels",
     "mt_rd_lambdas_init", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",

@@ -86,7 +86,60 @@ CDF_TABLES = (
     + [("src/coef_q.rs", f"EOB_BIN_{a}_LUMA_1D") for a in (16, 64, 128)]
     + [("src/tables.rs", "TXTP_INTRA1_TX4"), ("src/tables.rs", "TXTP_INTRA1_TX8"),
        ("src/tables.rs", "TXTP_INTRA2_TX16")]
+    # the mode / partition / tool CDFs of Cdfs::new (src/coder/cdfs.rs:506-627)
+    + [("src/tables.rs", n) for n in ("SKIP_CDF", "FILTER_INTRA_MODE_CDF", "FILTER_INTRA_CDF", "KF_Y_MODE_CDF",
+                                      "UV_MODE_NOCFL_CDF", "UV_MODE_CFL_CDF", "ANGLE_DELTA_CDF", "PART_SPLIT_CDF",
+                                      "PART_BL8_CDF", "TXSZ_CAT0_CDF", "TXSZ_CAT1_CDF", "TXSZ_CAT2_CDF",
+                                      "TXSZ_CAT3_CDF")]
+    + [("src/intrapred.rs", "CFL_SIGN_CDF"), ("src/intrapred.rs", "CFL_ALPHA_CDF")]
 )
+
+
+def extract_fn_static(path, fn_name, static_name):
+    """The values of `static static_name` (or `const`) declared inside fn_name."""
+    text = open(path, encoding="utf-8").read()
+    i = text.index("fn " + fn_name + "(")
+    j = text.index("\n}\n", i)
+    body = text[i:j]
+    m = re.search(r"(?:static|const)\s+" + re.escape(static_name) + r"\s*:\s*([^=]+)=\s*\[", body)
+    k = m.end() - 1
+    depth, e = 0, k
+    while True:
+        if body[e] == "[":
+            depth += 1
+        elif body[e] == "]":
+            depth -= 1
+            if depth == 0:
+                break
+        e += 1
+    vals = re.sub(r"//[^\n]*", "", body[k:e + 1])
+    return [int(v) for v in re.findall(r"-?\d+", vals)], m.group(1).strip()
+
+
+def extract_palette_y_color(path):
+    """palette_y_color_raw's (size, ctx) => &[..] arms, sizes 2..8 x 5 contexts,
+    concatenated in (size, ctx) order (size - 1 values each)."""
+    text = open(path, encoding="utf-8").read()
+    i = text.index("fn palette_y_color_raw(")
+    j = text.index("\n}\n", i)
+    arms = re.findall(r"\((\d+),\s*(\d+)\)\s*=>\s*&\[([^\]]*)\]", text[i:j])
+    got = {(int(a), int(b)): [int(v) for v in re.findall(r"\d+", c)] for a, b, c in arms}
+    out = []
+    for n in range(2, 9):
+        for ctx in range(5):
+            assert len(got[(n, ctx)]) == n - 1
+            out += got[(n, ctx)]
+    return out
+
+
+def extract_palette_uv_color(path):
+    """palette_uv_color_raw's S2..S8 tables ([5][size - 1]) in size order."""
+    out = []
+    for n in range(2, 9):
+        vals, _ = extract_fn_static(path, "palette_uv_color_raw", f"S{n}")
+        assert len(vals) == 5 * (n - 1)
+        out += vals
+    return out
 
 
 def write_cdfs(ref):
@@ -103,6 +156,26 @@ def write_cdfs(ref):
         nums, decl = extract(os.path.join(ref, rel), rname)
         cname = "MT_CDF_" + rname
         lines.append(f"/* {rel} {rname}: {decl} ({len(nums)} values) */")
+        lines.append(f"static const uint16_t {cname}[{len(nums)}] = {{")
+        for k in range(0, len(nums), 24):
+            lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
+        lines.append("};")
+        lines.append("")
+    pal = os.path.join(ref, "src/coder/palette.rs")
+    extra = [
+        ("MT_CDF_PALETTE_Y_MODE", extract_fn_static(pal, "palette_y_mode_cdfs", "RAW")[0],
+         "src/coder/palette.rs palette_y_mode_cdfs RAW [7][3]"),
+        ("MT_CDF_PALETTE_Y_SIZE", extract_fn_static(pal, "palette_y_size_cdfs", "RAW")[0],
+         "src/coder/palette.rs palette_y_size_cdfs RAW [7][6]"),
+        ("MT_CDF_PALETTE_UV_SIZE", extract_fn_static(pal, "palette_uv_size_cdfs", "RAW")[0],
+         "src/coder/palette.rs palette_uv_size_cdfs RAW [7][6]"),
+        ("MT_CDF_PALETTE_Y_COLOR", extract_palette_y_color(pal),
+         "src/coder/palette.rs palette_y_color_raw, sizes 2..8 x 5 contexts, size-1 values each"),
+        ("MT_CDF_PALETTE_UV_COLOR", extract_palette_uv_color(pal),
+         "src/coder/palette.rs palette_uv_color_raw S2..S8, sizes 2..8 x 5 contexts, size-1 values each"),
+    ]
+    for cname, nums, what in extra:
+        lines.append(f"/* {what} ({len(nums)} values) */")
         lines.append(f"static const uint16_t {cname}[{len(nums)}] = {{")
         for k in range(0, len(nums), 24):
             lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")

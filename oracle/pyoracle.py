@@ -730,3 +730,146 @@ def rd_lambdas(q, dc_q, sub):
         ks = f(k[1] + f(f(f(k[2] - k[1]) * f(qi - f(81.0))) / f(59.0)))
     out.satd_bridge = f(f(f(2.775) / ks) * f(7.130643))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Entropy path checker: the range decoder (oracle_entropy.cpp) and Cdfs::new
+# assembled in semantic-slot order from the reference's arrays.
+
+class RangeDecoder:
+    """OdEcDecoder (src/odec.rs:615-760) over a byte string."""
+
+    def __init__(self, data):
+        self._buf = C.create_string_buffer(bytes(data), max(1, len(data)))
+        lib = load()
+        lib.or_dec_new.restype = C.c_void_p
+        lib.or_dec_new.argtypes = [C.c_void_p, C.c_size_t]
+        lib.or_dec_free.argtypes = [C.c_void_p]
+        lib.or_dec_bool.argtypes = [C.c_void_p, C.c_uint16]
+        lib.or_dec_literal.restype = C.c_uint32
+        lib.or_dec_literal.argtypes = [C.c_void_p, C.c_uint32]
+        lib.or_dec_symbol.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        lib.or_dec_signed_subexp_with_ref.restype = C.c_int32
+        lib.or_dec_signed_subexp_with_ref.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_uint32, C.c_int32]
+        self._d = lib.or_dec_new(C.addressof(self._buf), len(data))
+
+    def bool(self, f):
+        return bool(load().or_dec_bool(self._d, f))
+
+    def literal(self, bits):
+        return load().or_dec_literal(self._d, bits)
+
+    def symbol(self, cdf, adapt=True):
+        assert cdf.dtype == np.uint16 and cdf.flags.c_contiguous
+        return load().or_dec_symbol(self._d, cdf.ctypes.data, len(cdf), int(bool(adapt)))
+
+    def signed_subexp_with_ref(self, low, high, k, r):
+        return load().or_dec_signed_subexp_with_ref(self._d, low, high, k, r)
+
+    def __del__(self):
+        if getattr(self, "_d", None):
+            load().or_dec_free(self._d)
+            self._d = None
+
+
+def cdfs_new_slots(qctx):
+    """Cdfs::new(qctx) (src/coder/cdfs.rs:401-629) as a list of np.uint16 inverse
+    CDFs (counter last) in Cdfs::semantic_slots order (src/coder/cdfs.rs:193-355),
+    from the reference's arrays (tests/golden/cdfs_default.json); the values
+    Cdfs::new writes inline are listed with their source lines."""
+    g = _golden_cdfs()
+    out = []
+
+    def one(vals):
+        out.append(np.array([32768 - v for v in vals] + [0], np.uint16))
+
+    def rows(t):
+        for r in t:
+            one(r)
+
+    def singles(t):
+        for v in t:
+            one([v])
+
+    def flat(t):
+        while isinstance(t[0], list):
+            t = [x for row in t for x in row]
+        return t
+
+    singles(g["SKIP_CDF"])
+    one([30531])  # intrabc (cdfs.rs:508)
+    singles([28581, 23846, 20847, 24315, 18196, 12133, 18791, 10887, 11005, 27179, 20004, 11281, 26549, 19308,
+             14224, 28015, 21546, 14400, 28165, 22401, 16088])  # TXPART_CDF (cdfs.rs:71-79)
+    one([770, 2421, 5225, 12907, 15819, 18927, 21561, 24089, 26595, 28526, 30529])  # txtp_inter2 (:513-515)
+    singles([16384, 4167, 1998, 748])  # txtp_inter3 (:516-519)
+    one([4096, 11264, 19328])  # mv_joint
+    for _ in range(2):
+        one([16384])  # mv_sign
+    for _ in range(2):
+        one([28672, 30976, 31858, 32320, 32551, 32656, 32740, 32757, 32762, 32767])  # mv_classes
+    for _ in range(2):
+        one([27648])  # mv_class0
+    for _ in range(2):
+        singles([17408, 17920, 18944, 20480, 22528, 24576, 28672, 29952, 29952, 30720])  # mv_class_n
+    rows(g["PART_BL8_CDF"])
+    for lvl in g["PART_SPLIT_CDF"]:
+        rows(lvl)
+    for a in g["KF_Y_MODE_CDF"]:
+        rows(a)
+    rows(g["UV_MODE_NOCFL_CDF"])
+    rows(g["UV_MODE_CFL_CDF"])
+    rows(g["ANGLE_DELTA_CDF"])
+    singles(g["FILTER_INTRA_CDF"])
+    one(g["FILTER_INTRA_MODE_CDF"])
+    singles(flat(g["PALETTE_Y_MODE"]))
+    ys = g["PALETTE_Y_SIZE"]
+    rows([ys[k * 6:(k + 1) * 6] for k in range(7)])
+    singles([32461, 21488])  # palette_uv_mode (cdfs.rs:573)
+    for n in range(2, 9):
+        for ctx in range(5):
+            one(g["PALETTE_Y_COLOR"][f"{n},{ctx}"])
+    us = g["PALETTE_UV_SIZE"]
+    rows([us[k * 6:(k + 1) * 6] for k in range(7)])
+    for n in range(2, 9):
+        t = g["PALETTE_UV_COLOR"][str(n)]
+        rows([t[c * (n - 1):(c + 1) * (n - 1)] for c in range(5)])
+    one(g["CFL_SIGN_CDF"])
+    rows(g["CFL_ALPHA_CDF"])
+    for k in range(4):
+        rows(g[f"TXSZ_CAT{k}_CDF"])
+    rows(g["TXTP_INTRA1_TX8"])
+    rows(g["TXTP_INTRA1_TX4"])
+    rows(g["TXTP_INTRA2_TX16"])
+    for n in (4, 8, 16, 32, 64):
+        singles(g[f"SKIP_TX{n}"][qctx])
+    for n in (4, 8, 16, 32):
+        for p in ("LUMA", "CHROMA"):
+            rows(g[f"BASE_TOK_TX{n}_{p}_Q"][qctx])
+    rows(g["BASE_TOK_TX64_LUMA_Q"][qctx])
+    for n in (4, 8, 16, 32):
+        for p in ("LUMA", "CHROMA"):
+            rows(g[f"BR_TOK_TX{n}_{p}_Q"][qctx])
+    for n in (4, 8, 16, 32):
+        for p in ("LUMA", "CHROMA"):
+            rows(g[f"EOB_BASE_TX{n}_{p}_Q"][qctx])
+    rows(g["EOB_BASE_TX64_LUMA_Q"][qctx])
+    for n in (4, 8, 16, 32):
+        for p in ("LUMA", "CHROMA"):
+            singles(g[f"EOB_HI_TX{n}_{p}"][qctx])
+    singles(g["EOB_HI_TX64_LUMA"][qctx])
+    for p in range(2):
+        singles(g["DC_SIGN_Q"][qctx][p])
+    for name in ("16_CHROMA", "16_LUMA", "32_CHROMA", "32_LUMA", "64_LUMA", "16_LUMA_1D", "64_LUMA_1D",
+                 "128_LUMA_1D", "64_CHROMA", "256_LUMA", "256_CHROMA", "128_CHROMA", "128_LUMA", "1024_LUMA",
+                 "1024_CHROMA", "512_CHROMA", "512_LUMA"):
+        one(g[f"EOB_BIN_{name}"][qctx])
+    one([28160, 32120, 32677])  # delta_q (cdfs.rs:621)
+    one([11570])  # wiener_restore (tile_encode.rs:34-36)
+    return out
+
+
+def gather_split_prob(cdf, top):
+    """gather_split_prob_icdf (src/coeffs.rs:2927-2935)."""
+    v = [int(x) for x in cdf]
+    out = (v[1] - v[4]) + v[5] + (v[8] - v[7]) if top else (v[0] - v[1]) + (v[2] - v[6]) + (v[7] - v[8])
+    return min(max(out, 1), 32767)

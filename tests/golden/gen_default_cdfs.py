@@ -25,7 +25,47 @@ NAMES_COEF_Q = (
     + [f"EOB_BIN_{a}_{p}" for a in (16, 32, 64, 128, 256, 512, 1024) for p in ("LUMA", "CHROMA")]
     + [f"EOB_BIN_{a}_LUMA_1D" for a in (16, 64, 128)]
 )
-NAMES_TABLES = ["TXTP_INTRA1_TX4", "TXTP_INTRA1_TX8", "TXTP_INTRA2_TX16"]
+NAMES_TABLES = ["TXTP_INTRA1_TX4", "TXTP_INTRA1_TX8", "TXTP_INTRA2_TX16", "SKIP_CDF", "FILTER_INTRA_MODE_CDF",
+                "FILTER_INTRA_CDF", "KF_Y_MODE_CDF", "UV_MODE_NOCFL_CDF", "UV_MODE_CFL_CDF", "ANGLE_DELTA_CDF",
+                "PART_SPLIT_CDF", "PART_BL8_CDF", "TXSZ_CAT0_CDF", "TXSZ_CAT1_CDF", "TXSZ_CAT2_CDF", "TXSZ_CAT3_CDF"]
+NAMES_INTRAPRED = ["CFL_SIGN_CDF", "CFL_ALPHA_CDF"]
+
+
+def palette_tables(path):
+    """The palette CDFs of src/coder/palette.rs: the function-local RAW tables of
+    palette_y_mode_cdfs / palette_y_size_cdfs / palette_uv_size_cdfs, the
+    (size, ctx) arms of palette_y_color_raw and palette_uv_color_raw's S2..S8."""
+    import re
+
+    src = open(path).read()
+
+    def fn_body(name):
+        i = src.index("fn " + name + "(")
+        return src[i:src.index("\n}\n", i)]
+
+    def nums(text):
+        return [int(v) for v in re.findall(r"\d+", re.sub(r"//[^\n]*", "", text))]
+
+    def table(name, static):
+        b = fn_body(name)
+        i = b.index(static + ":")
+        j = b.index("= [", i) + 2
+        depth, k = 0, j
+        while True:
+            depth += {"[": 1, "]": -1}.get(b[k], 0)
+            if depth == 0:
+                break
+            k += 1
+        return nums(b[j:k + 1])
+
+    yc = {}
+    for a, c, body in re.findall(r"\((\d+),\s*(\d+)\)\s*=>\s*&\[([^\]]*)\]", fn_body("palette_y_color_raw")):
+        yc[f"{a},{c}"] = nums(body)
+    uvc = {str(n): table("palette_uv_color_raw", f"S{n}") for n in range(2, 9)}
+    return {"PALETTE_Y_MODE": table("palette_y_mode_cdfs", "RAW"),
+            "PALETTE_Y_SIZE": table("palette_y_size_cdfs", "RAW"),
+            "PALETTE_UV_SIZE": table("palette_uv_size_cdfs", "RAW"),
+            "PALETTE_Y_COLOR": yc, "PALETTE_UV_COLOR": uvc}
 
 
 def main(ref):
@@ -36,6 +76,9 @@ def main(ref):
         out[n] = rust_array(q, n)
     for n in NAMES_TABLES:
         out[n] = rust_array(t, n)
+    for n in NAMES_INTRAPRED:
+        out[n] = rust_array(os.path.join(ref, "src", "intrapred.rs"), n)
+    out.update(palette_tables(os.path.join(ref, "src", "coder", "palette.rs")))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cdfs_default.json")
     with open(dst, "w") as f:
         json.dump(out, f, separators=(",", ":"))
