@@ -18,6 +18,9 @@
  *   mt_range_encoder_* / mt_cdfs_default  src/odec.rs:35-615 OdEcEncoder, src/coder/cdfs.rs:193-629
  *   mt_pack_tile                          src/coder/wavefront.rs:617-657 pack_wavefront_tile
  *   mt_replay_tile_with_filters           src/coder/tile_encode.rs:404-466 replay_tile_with_filters
+ *   mt_sequence_header / mt_frame_header  src/obu.rs:46-771 sequence / frame headers, OBU framing
+ *   mt_assemble_frame_obus / mt_av1_stream src/coder/frame_encode.rs:436-525, src/dispatch.rs:239-256
+ *   mt_wrap_av1_image                     src/isobmff.rs:210-494 wrap_av1_image, src/avif.rs:676-740
  *   mt_quality_to_q / mt_qm_levels /      src/avif.rs:637-666 quality_to_q, src/quant.rs:122-167
  *   mt_rd_lambdas_init                    QM level laws, src/cost.rs + src/partition_rd.rs lambdas
  *   mt_candidate_chain[_device]           the per-candidate chain of the luma mode
@@ -990,6 +993,84 @@ int mt_replay_tile_with_filters(const mt_tile_trace* t, int32_t tile_x0, int32_t
                                 int32_t cdef_bits, int32_t updating_cdf, uint8_t** out, size_t* out_len);
 /* Frees a buffer this library returned. */
 void mt_free(void* p);
+
+
+/* ---- Headers and container (host) ----------------------------------------
+ * src/bitwriter.rs leb128, src/obu.rs wrap_obu / sequence_header_cicp(_ss) /
+ * sequence_header_mono / frame_header_lossy_multitile(_th),
+ * src/coder/frame_encode.rs:436-525 assemble_tilegroup / assemble_frame_obus,
+ * src/coder/tiling.rs:63-136 the increment bits of a tiling, and
+ * src/isobmff.rs:68-494 wrap_av1_image with src/avif.rs:676-740 make_av1c. */
+typedef struct mt_sequence_header_params {
+  uint32_t width, height;          /* displayed frame size */
+  uint32_t profile;                /* 0 (4:2:0 / mono), 1 (4:4:4), 2 (4:2:2 or 12-bit) */
+  uint32_t bit_depth;              /* 8, 10, 12 */
+  int32_t monochrome;              /* 1: the monochrome header (sequence_header_mono) */
+  int32_t color_present;           /* CICP colour description present */
+  uint32_t primaries, transfer, matrix; /* CICP code points (matrix 0 = identity / RGB) */
+  int32_t full_range;
+  uint32_t chroma_sample_position; /* coded for 4:2:0 */
+  uint32_t ss_x, ss_y;             /* chroma subsampling */
+  int32_t enable_filter_intra, enable_intra_edge_filter;
+} mt_sequence_header_params;
+
+typedef struct mt_frame_header_params {
+  int32_t w8, h8;                  /* padded frame size (for the tiling's increment bits) */
+  int32_t tile_cols_log2, tile_rows_log2;
+  uint32_t base_q_idx;             /* 1..255 (lossy) */
+  uint32_t qm_y, qm_u, qm_v;       /* 0..15; all 15 = no quantisation matrices */
+  int32_t uac_delta, udc_delta;    /* chroma AC / DC qindex deltas */
+  int32_t monochrome;
+  int32_t aq;                      /* superblock delta-q present */
+  uint32_t delta_q_res_log2;
+  int32_t allow_intrabc;
+  int32_t updating_cdf;            /* 0: disable_cdf_update */
+  int32_t lf_y, lf_u, lf_v, lf_sharpness; /* loop-filter levels and sharpness */
+  int32_t cdef_bits;               /* -1: CDEF off (the no-op parameter set) */
+  int32_t cdef_damping;            /* 3..6 */
+  uint8_t cdef_strengths[8][4];    /* (y pri, y sec, uv pri, uv sec); sec 0, 1, 2 or 4 */
+  int32_t lr_luma_wiener;          /* 1: luma RESTORE_WIENER */
+} mt_frame_header_params;
+
+typedef struct mt_avif_item_params {
+  uint32_t width, height;
+  uint8_t bit_depth, channels;     /* channels 3 colour, 1 monochrome */
+  uint8_t seq_profile, seq_level_idx; /* av1C (mt_av1_level_for) */
+  int32_t monochrome, chroma_sub_x, chroma_sub_y;
+  int32_t color_present;           /* nclx colr box */
+  uint16_t primaries, transfer, matrix;
+  int32_t full_range;
+  const uint8_t* icc; size_t icc_len;   /* prof colr box, or NULL */
+  const uint8_t* exif; size_t exif_len; /* Exif item (TIFF bytes), or NULL */
+  uint8_t irot_steps;              /* 0..3 anti-clockwise quarter turns */
+  int32_t imir_axis;               /* -1 none, 0 vertical axis, 1 horizontal axis */
+  int32_t clli_present;
+  uint16_t max_content_light_level, max_pic_average_light_level;
+} mt_avif_item_params;
+
+/* leb128 bytes of value (out NULL: only the length). */
+int mt_leb128(uint64_t value, uint8_t* out, size_t cap, size_t* len);
+/* An OBU with obu_has_size_field = 1 around payload. */
+int mt_wrap_obu(int32_t obu_type, const uint8_t* payload, size_t n, uint8_t** out, size_t* out_len);
+/* The increment_tile_{cols,rows}_log2 bits (each at most 8) that signal a tiling. */
+int mt_tiling_increments(int32_t w8, int32_t h8, int32_t tile_cols_log2, int32_t tile_rows_log2, uint8_t* cols_incr,
+                         int32_t* ncols, uint8_t* rows_incr, int32_t* nrows);
+/* The sequence header OBU. */
+int mt_sequence_header(const mt_sequence_header_params* p, uint8_t** out, size_t* out_len);
+/* The uncompressed frame header bits (with trailing bits when trailing != 0). */
+int mt_frame_header(const mt_frame_header_params* p, int32_t trailing, uint8_t** out, size_t* out_len);
+/* One OBU_FRAME for a single tile, else OBU_FRAME_HEADER + OBU_TILE_GROUP
+ * (tile sizes as 4-byte little-endian tile_size_minus_1). */
+int mt_assemble_frame_obus(const mt_frame_header_params* p, const uint8_t* const* tiles, const size_t* tile_lens,
+                           int32_t ntiles, uint8_t** out, size_t* out_len);
+/* temporal delimiter + sequence header + frame OBUs (src/dispatch.rs:239-256). */
+int mt_av1_stream(const mt_sequence_header_params* sp, const mt_frame_header_params* fp, const uint8_t* const* tiles,
+                  const size_t* tile_lens, int32_t ntiles, uint8_t** out, size_t* out_len);
+/* seq_level_idx for a picture size (AV1 Table A.2 thresholds). */
+uint8_t mt_av1_level_for(uint32_t width, uint32_t height);
+/* The AVIF file around an AV1 stream (free with mt_free). */
+int mt_wrap_av1_image(const uint8_t* obu, size_t obu_len, const mt_avif_item_params* p, uint8_t** out,
+                      size_t* out_len);
 
 #ifdef __cplusplus
 }

@@ -187,6 +187,35 @@ class RdLambdas(C.Structure):
                 ("satd_scale", C.c_float), ("satd_bridge", C.c_float)]
 
 
+class SequenceHeaderParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("profile", C.c_uint32), ("bit_depth", C.c_uint32),
+                ("monochrome", C.c_int32), ("color_present", C.c_int32), ("primaries", C.c_uint32),
+                ("transfer", C.c_uint32), ("matrix", C.c_uint32), ("full_range", C.c_int32),
+                ("chroma_sample_position", C.c_uint32), ("ss_x", C.c_uint32), ("ss_y", C.c_uint32),
+                ("enable_filter_intra", C.c_int32), ("enable_intra_edge_filter", C.c_int32)]
+
+
+class FrameHeaderParams(C.Structure):
+    _fields_ = [("w8", C.c_int32), ("h8", C.c_int32), ("tile_cols_log2", C.c_int32), ("tile_rows_log2", C.c_int32),
+                ("base_q_idx", C.c_uint32), ("qm_y", C.c_uint32), ("qm_u", C.c_uint32), ("qm_v", C.c_uint32),
+                ("uac_delta", C.c_int32), ("udc_delta", C.c_int32), ("monochrome", C.c_int32), ("aq", C.c_int32),
+                ("delta_q_res_log2", C.c_uint32), ("allow_intrabc", C.c_int32), ("updating_cdf", C.c_int32),
+                ("lf_y", C.c_int32), ("lf_u", C.c_int32), ("lf_v", C.c_int32), ("lf_sharpness", C.c_int32),
+                ("cdef_bits", C.c_int32), ("cdef_damping", C.c_int32), ("cdef_strengths", (C.c_uint8 * 4) * 8),
+                ("lr_luma_wiener", C.c_int32)]
+
+
+class AvifItemParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("bit_depth", C.c_uint8), ("channels", C.c_uint8),
+                ("seq_profile", C.c_uint8), ("seq_level_idx", C.c_uint8), ("monochrome", C.c_int32),
+                ("chroma_sub_x", C.c_int32), ("chroma_sub_y", C.c_int32), ("color_present", C.c_int32),
+                ("primaries", C.c_uint16), ("transfer", C.c_uint16), ("matrix", C.c_uint16),
+                ("full_range", C.c_int32), ("icc", C.c_void_p), ("icc_len", C.c_size_t), ("exif", C.c_void_p),
+                ("exif_len", C.c_size_t), ("irot_steps", C.c_uint8), ("imir_axis", C.c_int32),
+                ("clli_present", C.c_int32), ("max_content_light_level", C.c_uint16),
+                ("max_pic_average_light_level", C.c_uint16)]
+
+
 def _bind(lib):
     sig = {
         "mt_version": (C.c_char_p, []),
@@ -214,6 +243,19 @@ def _bind(lib):
                                                   C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P),
                                                   C.POINTER(C.c_size_t)]),
         "mt_free": (None, [_P]),
+        "mt_leb128": (C.c_int, [C.c_uint64, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "mt_wrap_obu": (C.c_int, [C.c_int32, _P, C.c_size_t, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+        "mt_tiling_increments": (C.c_int, [C.c_int32] * 4 + [_P, C.POINTER(C.c_int32), _P, C.POINTER(C.c_int32)]),
+        "mt_sequence_header": (C.c_int, [C.POINTER(SequenceHeaderParams), C.POINTER(_P), C.POINTER(C.c_size_t)]),
+        "mt_frame_header": (C.c_int, [C.POINTER(FrameHeaderParams), C.c_int32, C.POINTER(_P),
+                                      C.POINTER(C.c_size_t)]),
+        "mt_assemble_frame_obus": (C.c_int, [C.POINTER(FrameHeaderParams), _P, _P, C.c_int32, C.POINTER(_P),
+                                             C.POINTER(C.c_size_t)]),
+        "mt_av1_stream": (C.c_int, [C.POINTER(SequenceHeaderParams), C.POINTER(FrameHeaderParams), _P, _P,
+                                    C.c_int32, C.POINTER(_P), C.POINTER(C.c_size_t)]),
+        "mt_av1_level_for": (C.c_uint8, [C.c_uint32, C.c_uint32]),
+        "mt_wrap_av1_image": (C.c_int, [_P, C.c_size_t, C.POINTER(AvifItemParams), C.POINTER(_P),
+                                        C.POINTER(C.c_size_t)]),
         "mt_quality_to_q": (C.c_uint8, [C.c_uint8]),
         "mt_qm_levels": (C.c_int, [C.c_uint8, C.c_int32, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
         "mt_rd_lambdas_init": (C.c_int, [C.c_uint8, C.c_int32, C.c_int32, C.c_uint8, C.POINTER(RdLambdas)]),
@@ -331,7 +373,9 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_range_encoder_new", "mt_range_encoder_free",
     "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
     "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default",
-    "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free", "mt_quality_to_q", "mt_qm_levels",
+    "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
+    "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
+    "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image", "mt_quality_to_q", "mt_qm_levels",
     "mt_rd_lambdas_init", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",

@@ -772,7 +772,7 @@ class RangeDecoder:
             self._d = None
 
 
-def cdfs_new_slots(qctx):
+def cdfs_new_slots(qctx, sections=None):
     """Cdfs::new(qctx) (src/coder/cdfs.rs:401-629) as a list of np.uint16 inverse
     CDFs (counter last) in Cdfs::semantic_slots order (src/coder/cdfs.rs:193-355),
     from the reference's arrays (tests/golden/cdfs_default.json); the values
@@ -796,6 +796,8 @@ def cdfs_new_slots(qctx):
             t = [x for row in t for x in row]
         return t
 
+    sec = sections if sections is not None else {}
+    sec["skip"] = len(out)
     singles(g["SKIP_CDF"])
     one([30531])  # intrabc (cdfs.rs:508)
     singles([28581, 23846, 20847, 24315, 18196, 12133, 18791, 10887, 11005, 27179, 20004, 11281, 26549, 19308,
@@ -811,19 +813,25 @@ def cdfs_new_slots(qctx):
         one([27648])  # mv_class0
     for _ in range(2):
         singles([17408, 17920, 18944, 20480, 22528, 24576, 28672, 29952, 29952, 30720])  # mv_class_n
+    sec["part_bl8"] = len(out)
     rows(g["PART_BL8_CDF"])
+    sec["part_split"] = len(out)
     for lvl in g["PART_SPLIT_CDF"]:
         rows(lvl)
+    sec["kf_y"] = len(out)
     for a in g["KF_Y_MODE_CDF"]:
         rows(a)
+    sec["uv_mode"] = len(out)
     rows(g["UV_MODE_NOCFL_CDF"])
     rows(g["UV_MODE_CFL_CDF"])
     rows(g["ANGLE_DELTA_CDF"])
     singles(g["FILTER_INTRA_CDF"])
     one(g["FILTER_INTRA_MODE_CDF"])
+    sec["palette_y_mode"] = len(out)
     singles(flat(g["PALETTE_Y_MODE"]))
     ys = g["PALETTE_Y_SIZE"]
     rows([ys[k * 6:(k + 1) * 6] for k in range(7)])
+    sec["palette_uv_mode"] = len(out)
     singles([32461, 21488])  # palette_uv_mode (cdfs.rs:573)
     for n in range(2, 9):
         for ctx in range(5):
@@ -835,6 +843,7 @@ def cdfs_new_slots(qctx):
         rows([t[c * (n - 1):(c + 1) * (n - 1)] for c in range(5)])
     one(g["CFL_SIGN_CDF"])
     rows(g["CFL_ALPHA_CDF"])
+    sec["txsz"] = len(out)
     for k in range(4):
         rows(g[f"TXSZ_CAT{k}_CDF"])
     rows(g["TXTP_INTRA1_TX8"])
