@@ -21,6 +21,7 @@
  *   mt_sequence_header / mt_frame_header  src/obu.rs:46-771 sequence / frame headers, OBU framing
  *   mt_assemble_frame_obus / mt_av1_stream src/coder/frame_encode.rs:436-525, src/dispatch.rs:239-256
  *   mt_wrap_av1_image                     src/isobmff.rs:210-494 wrap_av1_image, src/avif.rs:676-740
+ *   mt_encode_config_* / mt_validate_rgb8_input  src/avif.rs:257-344 EncodeConfig, :577-635, :915-923
  *   mt_quality_to_q / mt_qm_levels /      src/avif.rs:637-666 quality_to_q, src/quant.rs:122-167
  *   mt_rd_lambdas_init                    QM level laws, src/cost.rs + src/partition_rd.rs lambdas
  *   mt_candidate_chain[_device]           the per-candidate chain of the luma mode
@@ -58,6 +59,12 @@ extern "C" {
 #define MT_ERR_TOO_LARGE (-4)
 #define MT_ERR_DEVICE (-10)
 #define MT_ERR_ALLOC (-11)
+/* The EncodeError variants of the encode boundary (src/err.rs:33-62). */
+#define MT_ERR_INVALID_DIMENSIONS (-20)    /* InvalidDimensions: not 1..=16383 */
+#define MT_ERR_DIMENSION_TOO_LARGE (-21)   /* DimensionTooLarge: buffer size overflows */
+#define MT_ERR_INVALID_QUALITY (-22)       /* InvalidQuality: quality > 100, QM level > 15 */
+#define MT_ERR_UNSUPPORTED_CHROMA_FORMAT (-23)
+#define MT_ERR_UNSUPPORTED_BIT_DEPTH (-24) /* UnsupportedChromaBitDepth */
 
 /* Intra prediction modes, AV1 numbering (src/intrapred.rs:54-79). */
 #define MT_DC_PRED 0
@@ -1071,6 +1078,62 @@ uint8_t mt_av1_level_for(uint32_t width, uint32_t height);
 /* The AVIF file around an AV1 stream (free with mt_free). */
 int mt_wrap_av1_image(const uint8_t* obu, size_t obu_len, const mt_avif_item_params* p, uint8_t** out,
                       size_t* out_len);
+
+
+/* ---- Encode configuration (the drop-in boundary's EncodeConfig) -----------
+ * Every EncodeConfig field (src/avif.rs:257-316) except the gain map;
+ * mt_encode_config_default gives EncodeConfig::default() (src/avif.rs:318-344:
+ * quality 80, 4:2:0, sRGB-YCbCr CICP, all cores, Slow, adaptive CDFs, AQ with
+ * Variance Boost and dark protection, CDEF flag off (Slow forces it on),
+ * Wiener off, quantisation matrices on, screen content and IntraBC allowed). */
+#define MT_CHROMA_420 0
+#define MT_CHROMA_422 1
+#define MT_CHROMA_444 2
+#define MT_CHROMA_MONO 3
+#define MT_SPEED_EXTRA_SLOW 0
+#define MT_SPEED_SLOW 1
+#define MT_SPEED_MEDIUM 2
+#define MT_SPEED_FAST 3
+typedef struct mt_encode_config {
+  int32_t quality;                 /* 0..100 */
+  int32_t chroma;                  /* MT_CHROMA_* */
+  int32_t color_present;           /* color_encoding: Some(Cicp) */
+  uint32_t primaries, transfer, matrix;
+  int32_t full_range;
+  uint32_t chroma_sample_position;
+  const uint8_t* icc; size_t icc_len;
+  int32_t orientation;             /* metadata: EXIF orientation 1..8 */
+  int32_t clli_present;            /* metadata: content light level */
+  uint16_t max_content_light_level, max_pic_average_light_level;
+  const uint8_t* exif; size_t exif_len;
+  int32_t threads;                 /* 0 = all cores */
+  int32_t speed;                   /* MT_SPEED_* */
+  int32_t updating_cdf, adaptive_quant, variance_boost, dark_aq, cdef, wiener;
+  int32_t quantization_matrices, screen_content, intrabc;
+  int32_t qmatrix_level;           /* -1 = None, else 0..15 */
+  int32_t alpha_quality;           /* -1 = None, else 0..100 */
+} mt_encode_config;
+
+/* The frame-level settings a validated config resolves to: quality_to_q, the
+ * QM levels of EncodeConfig::vb (src/avif.rs:543-575), cdef_enabled
+ * (src/avif.rs:449-451), the AQ switches. */
+typedef struct mt_encode_plan {
+  uint8_t base_q_idx;
+  uint8_t qm_y, qm_u, qm_v;
+  int32_t sub;                     /* 0 4:4:4 / mono, 1 4:2:2, 2 4:2:0 */
+  int32_t cdef, aq, variance_boost, dark_aq;
+} mt_encode_plan;
+
+int mt_encode_config_default(mt_encode_config* cfg);
+/* EncodeConfig::validate (src/avif.rs:577-592): MT_ERR_INVALID_QUALITY for a
+ * quality or alpha quality above 100 or a QM level above 15. */
+int mt_encode_config_validate(const mt_encode_config* cfg);
+/* encode_rgb8's input checks (src/avif.rs:915-923, :593-635): dimensions
+ * 1..=16383 (MT_ERR_INVALID_DIMENSIONS), a buffer size that does not overflow
+ * (MT_ERR_DIMENSION_TOO_LARGE), rgb_len == width * height * 3
+ * (MT_ERR_INVALID_INPUT). */
+int mt_validate_rgb8_input(uint32_t width, uint32_t height, size_t rgb_len);
+int mt_encode_config_effective(const mt_encode_config* cfg, mt_encode_plan* out);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,9 @@ MT_ERR_UNSUPPORTED = -3
 MT_ERR_TOO_LARGE = -4
 MT_NOALLOC_MAX_BLOCKS = 131072
 MT_LEVEL_MAX_COMBOS = 2048
+MT_ERR_INVALID_QUALITY = -22
+MT_ERR_DIMENSION_TOO_LARGE = -21
+MT_ERR_INVALID_DIMENSIONS = -20
 MT_ERR_DEVICE = -10
 MT_ERR_ALLOC = -11
 MT_EOB_INVALID = -2
@@ -216,6 +219,25 @@ class AvifItemParams(C.Structure):
                 ("max_pic_average_light_level", C.c_uint16)]
 
 
+class EncodeConfig(C.Structure):
+    _fields_ = [("quality", C.c_int32), ("chroma", C.c_int32), ("color_present", C.c_int32),
+                ("primaries", C.c_uint32), ("transfer", C.c_uint32), ("matrix", C.c_uint32),
+                ("full_range", C.c_int32), ("chroma_sample_position", C.c_uint32), ("icc", C.c_void_p),
+                ("icc_len", C.c_size_t), ("orientation", C.c_int32), ("clli_present", C.c_int32),
+                ("max_content_light_level", C.c_uint16), ("max_pic_average_light_level", C.c_uint16),
+                ("exif", C.c_void_p), ("exif_len", C.c_size_t), ("threads", C.c_int32), ("speed", C.c_int32),
+                ("updating_cdf", C.c_int32), ("adaptive_quant", C.c_int32), ("variance_boost", C.c_int32),
+                ("dark_aq", C.c_int32), ("cdef", C.c_int32), ("wiener", C.c_int32),
+                ("quantization_matrices", C.c_int32), ("screen_content", C.c_int32), ("intrabc", C.c_int32),
+                ("qmatrix_level", C.c_int32), ("alpha_quality", C.c_int32)]
+
+
+class EncodePlan(C.Structure):
+    _fields_ = [("base_q_idx", C.c_uint8), ("qm_y", C.c_uint8), ("qm_u", C.c_uint8), ("qm_v", C.c_uint8),
+                ("sub", C.c_int32), ("cdef", C.c_int32), ("aq", C.c_int32), ("variance_boost", C.c_int32),
+                ("dark_aq", C.c_int32)]
+
+
 def _bind(lib):
     sig = {
         "mt_version": (C.c_char_p, []),
@@ -243,6 +265,10 @@ def _bind(lib):
                                                   C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P),
                                                   C.POINTER(C.c_size_t)]),
         "mt_free": (None, [_P]),
+        "mt_encode_config_default": (C.c_int, [C.POINTER(EncodeConfig)]),
+        "mt_encode_config_validate": (C.c_int, [C.POINTER(EncodeConfig)]),
+        "mt_validate_rgb8_input": (C.c_int, [C.c_uint32, C.c_uint32, C.c_size_t]),
+        "mt_encode_config_effective": (C.c_int, [C.POINTER(EncodeConfig), C.POINTER(EncodePlan)]),
         "mt_leb128": (C.c_int, [C.c_uint64, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "mt_wrap_obu": (C.c_int, [C.c_int32, _P, C.c_size_t, C.POINTER(_P), C.POINTER(C.c_size_t)]),
         "mt_tiling_increments": (C.c_int, [C.c_int32] * 4 + [_P, C.POINTER(C.c_int32), _P, C.POINTER(C.c_int32)]),
@@ -375,7 +401,8 @@ EXPORTED_SYMBOLS = (
     "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default",
     "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
     "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
-    "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image", "mt_quality_to_q", "mt_qm_levels",
+    "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image",
+    "mt_encode_config_default", "mt_encode_config_validate", "mt_validate_rgb8_input", "mt_encode_config_effective", "mt_quality_to_q", "mt_qm_levels",
     "mt_rd_lambdas_init", "mt_candidate_chain", "mt_candidate_chain_device", "mt_candidate_chain_scratch_bytes",
     "mt_rdo_level8", "mt_rdo_level8_device", "mt_rdo_level8_scratch_bytes", "mt_rdo_level8_device_noalloc",
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",
