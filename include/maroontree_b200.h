@@ -17,6 +17,7 @@
  *                                         Cdfs::new (the coefficient slices)
  *   mt_range_encoder_* / mt_cdfs_default  src/odec.rs:35-615 OdEcEncoder, src/coder/cdfs.rs:193-629
  *   mt_pack_tile                          src/coder/wavefront.rs:617-657 pack_wavefront_tile
+ *   mt_emit_coeffs[_device] / mt_cdf_layout  src/coeffs.rs:34-2520 the square coefficient coders
  *   mt_replay_tile_with_filters           src/coder/tile_encode.rs:404-466 replay_tile_with_filters
  *   mt_sequence_header / mt_frame_header  src/obu.rs:46-771 sequence / frame headers, OBU framing
  *   mt_assemble_frame_obus / mt_av1_stream src/coder/frame_encode.rs:436-525, src/dispatch.rs:239-256
@@ -971,6 +972,21 @@ int mt_range_encoder_done(mt_range_encoder* e, uint8_t** out, size_t* out_len);
  * data[offsets[i] .. offsets[i] + lens[i]).  With all three arrays NULL only
  * the sizes are returned. */
 int32_t mt_cdf_slot_count(void);
+/* First slot of each CDF group in that order: a CDF with context k of group g
+ * is slot g + k (two-level groups row-major, e.g. kf_y + above * 5 + left,
+ * part_split + level * 4 + ctx, uv_mode + cfl_allowed * 13 + y_mode,
+ * txsz + cat * 3 + ctx).  Groups a class or plane lacks are -1.  eob_bin is
+ * the first of the seventeen eob_pt CDFs in the order 16c 16l 32c 32l 64l
+ * 16l1d 64l1d 128l1d 64c 256l 256c 128c 128l 1024l 1024c 512c 512l. */
+typedef struct mt_cdf_slot_layout {
+  int32_t skip, intrabc, part_bl8, part_split, kf_y, uv_mode, angle_delta, filter_intra, filter_intra_mode;
+  int32_t palette_y_mode, palette_y_size, palette_uv_mode, cfl_sign, cfl_alpha, txsz, txtp8, txtp4, txtp16;
+  int32_t txb_skip[5];
+  int32_t base_tok[5][2], br_tok[4][2], eob_base[5][2], eob_hi[5][2];
+  int32_t dc_sign[2];
+  int32_t eob_bin, delta_q, wiener_restore, nslots;
+} mt_cdf_slot_layout;
+int mt_cdf_layout(mt_cdf_slot_layout* out);
 int mt_cdfs_default(int32_t qctx, uint16_t* data, size_t data_cap, uint32_t* offsets, uint16_t* lens,
                     int32_t slots_cap, size_t* data_len, int32_t* nslots);
 
@@ -1134,6 +1150,36 @@ int mt_encode_config_validate(const mt_encode_config* cfg);
  * (MT_ERR_INVALID_INPUT). */
 int mt_validate_rgb8_input(uint32_t width, uint32_t height, size_t rgb_len);
 int mt_encode_config_effective(const mt_encode_config* cfg, mt_encode_plan* out);
+
+
+/* ---- Coefficient token emission (device) ----------------------------------
+ * The square 2-D coefficient coders of src/coeffs.rs (encode_tx4_luma_coeffs_adapt
+ * :2414, encode_4x4_chroma_coeffs :2310, encode_tx8_coeffs_adapt :583,
+ * encode_tx16_coeffs_adapt :707) batched over transform blocks, writing the
+ * semantic tokens mt_pack_tile replays (slots of mt_cdf_layout).  A block's
+ * levels are cf[x * n + y] (column-major, the reference's layout) at
+ * levels + cf_offset. */
+typedef struct mt_coef_block {
+  uint32_t cf_offset;   /* first of the n * n levels */
+  uint8_t log2n;        /* 2, 3, 4: TX_4X4, TX_8X8, TX_16X16 */
+  uint8_t plane;        /* 0 luma, 1 chroma */
+  uint8_t skip_ctx;     /* txb_skip context 0..12 */
+  uint8_t dcs_ctx;      /* dc_sign context 0..2 */
+  uint8_t y_mode;       /* luma: the tx-type CDF row */
+  uint8_t txtp;         /* luma: tx-type symbol in the class's intra set */
+  uint8_t code_txtp;    /* luma: 1 codes the tx-type symbol */
+  uint8_t reserved;
+} mt_coef_block;
+/* Device form, two calls on the stream: with d_tokens NULL it counts each
+ * block's tokens into d_counts and writes the n + 1 exclusive offsets
+ * (d_offsets[n] = total); with d_tokens (>= total entries) it writes the
+ * tokens of block i at d_tokens + d_offsets[i] and its coefficient context
+ * byte (cul | dc-sign bits, 0x40 for an all-zero block) to d_res_ctx[i]. */
+int mt_emit_coeffs_device(const int32_t* d_levels, const mt_coef_block* d_blocks, int32_t n, uint32_t* d_counts,
+                          uint32_t* d_offsets, uint32_t* d_tokens, uint8_t* d_res_ctx, void* stream);
+/* Host form: *tokens (free with mt_free) and offsets (n + 1 entries). */
+int mt_emit_coeffs(const int32_t* levels, size_t nlevels, const mt_coef_block* blocks, int32_t n, uint32_t** tokens,
+                   uint32_t* offsets, uint8_t* res_ctx);
 
 #ifdef __cplusplus
 }

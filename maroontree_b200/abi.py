@@ -238,6 +238,22 @@ class EncodePlan(C.Structure):
                 ("dark_aq", C.c_int32)]
 
 
+COEF_BLOCK_DTYPE = np.dtype([("cf_offset", "<u4"), ("log2n", "u1"), ("plane", "u1"), ("skip_ctx", "u1"),
+                              ("dcs_ctx", "u1"), ("y_mode", "u1"), ("txtp", "u1"), ("code_txtp", "u1"),
+                              ("reserved", "u1")])
+assert COEF_BLOCK_DTYPE.itemsize == 12
+
+
+class CdfSlotLayout(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in ("skip", "intrabc", "part_bl8", "part_split", "kf_y", "uv_mode",
+                                          "angle_delta", "filter_intra", "filter_intra_mode", "palette_y_mode",
+                                          "palette_y_size", "palette_uv_mode", "cfl_sign", "cfl_alpha", "txsz",
+                                          "txtp8", "txtp4", "txtp16")] + [
+        ("txb_skip", C.c_int32 * 5), ("base_tok", (C.c_int32 * 2) * 5), ("br_tok", (C.c_int32 * 2) * 4),
+        ("eob_base", (C.c_int32 * 2) * 5), ("eob_hi", (C.c_int32 * 2) * 5), ("dc_sign", C.c_int32 * 2),
+        ("eob_bin", C.c_int32), ("delta_q", C.c_int32), ("wiener_restore", C.c_int32), ("nslots", C.c_int32)]
+
+
 def _bind(lib):
     sig = {
         "mt_version": (C.c_char_p, []),
@@ -265,6 +281,9 @@ def _bind(lib):
                                                   C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P),
                                                   C.POINTER(C.c_size_t)]),
         "mt_free": (None, [_P]),
+        "mt_cdf_layout": (C.c_int, [C.POINTER(CdfSlotLayout)]),
+        "mt_emit_coeffs_device": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
+        "mt_emit_coeffs": (C.c_int, [_P, C.c_size_t, _P, C.c_int32, C.POINTER(_P), _P, _P]),
         "mt_encode_config_default": (C.c_int, [C.POINTER(EncodeConfig)]),
         "mt_encode_config_validate": (C.c_int, [C.POINTER(EncodeConfig)]),
         "mt_validate_rgb8_input": (C.c_int, [C.c_uint32, C.c_uint32, C.c_size_t]),
@@ -398,7 +417,8 @@ EXPORTED_SYMBOLS = (
     "mt_version", "mt_quant_init", "mt_quant_init_chroma", "mt_qm_row", "mt_default_scan",
     "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_range_encoder_new", "mt_range_encoder_free",
     "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
-    "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default",
+    "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default", "mt_cdf_layout",
+    "mt_emit_coeffs_device", "mt_emit_coeffs",
     "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
     "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
     "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image",

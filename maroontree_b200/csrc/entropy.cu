@@ -229,7 +229,10 @@ struct CdfSet {
   }
 };
 
-void build_cdfs(int q, CdfSet& c) {
+void build_cdfs(int q, CdfSet& c, mt_cdf_slot_layout* L = nullptr) {
+  mt_cdf_slot_layout dummy;
+  if (!L) L = &dummy;
+  auto at = [&]() { return (int32_t)c.off.size(); };
   static const uint16_t kTxpart[7][3] = {{28581, 23846, 20847}, {24315, 18196, 12133}, {18791, 10887, 11005},
                                          {27179, 20004, 11281}, {26549, 19308, 14224}, {28015, 21546, 14400},
                                          {28165, 22401, 16088}};
@@ -242,7 +245,9 @@ void build_cdfs(int q, CdfSet& c) {
   static const uint16_t kDeltaQ[3] = {28160, 32120, 32677};
   static const uint16_t kWienerRestore = 11570;
 
+  L->skip = at();
   c.singles(MT_CDF_SKIP_CDF, 3);                     // skip [3 ctx]
+  L->intrabc = at();
   c.push1(30531);                                    // intrabc
   c.singles(&kTxpart[0][0], 21);                     // txpart [7][3]
   c.push(kTxtpInter2, 11);                           // txtp_inter2
@@ -252,16 +257,26 @@ void build_cdfs(int q, CdfSet& c) {
   for (int k = 0; k < 2; ++k) c.push(kMvClasses, 10);  // mv_classes [2]
   for (int k = 0; k < 2; ++k) c.push1(27648);        // mv_class0 [2]
   for (int k = 0; k < 2; ++k) c.singles(kMvClassN, 10);  // mv_class_n [2][10]
+  L->part_bl8 = at();
   c.rows(MT_CDF_PART_BL8_CDF, 4, 3);                 // part_bl8 [4 ctx]
+  L->part_split = at();
   c.rows(MT_CDF_PART_SPLIT_CDF, 12, 9);              // part_split [3 levels][4 ctx]
+  L->kf_y = at();
   c.rows(MT_CDF_KF_Y_MODE_CDF, 25, 12);              // kf_y [above * 5 + left]
+  L->uv_mode = at();
   c.rows(MT_CDF_UV_MODE_NOCFL_CDF, 13, 12);          // uv_mode, CfL not allowed [13]
   c.rows(MT_CDF_UV_MODE_CFL_CDF, 13, 13);            // uv_mode, CfL allowed [13]
+  L->angle_delta = at();
   c.rows(MT_CDF_ANGLE_DELTA_CDF, 8, 6);              // angle_delta [8]
+  L->filter_intra = at();
   c.singles(MT_CDF_FILTER_INTRA_CDF, 22);            // filter_intra [22 block sizes]
+  L->filter_intra_mode = at();
   c.push(MT_CDF_FILTER_INTRA_MODE_CDF, 4);           // filter_intra_mode
+  L->palette_y_mode = at();
   c.singles(MT_CDF_PALETTE_Y_MODE, 21);              // palette_y_mode [7][3]
+  L->palette_y_size = at();
   c.rows(MT_CDF_PALETTE_Y_SIZE, 7, 6);               // palette_y_size [7]
+  L->palette_uv_mode = at();
   c.singles(kPaletteUvMode, 2);                      // palette_uv_mode [2]
   {
     const uint16_t* p = MT_CDF_PALETTE_Y_COLOR;      // palette_y_color [size 2..8][5 ctx]
@@ -274,17 +289,26 @@ void build_cdfs(int q, CdfSet& c) {
     for (int n = 2; n <= 8; ++n)
       for (int ctx = 0; ctx < 5; ++ctx, p += n - 1) c.push(p, n - 1);
   }
+  L->cfl_sign = at();
   c.push(MT_CDF_CFL_SIGN_CDF, 7);                    // cfl_sign
+  L->cfl_alpha = at();
   c.rows(MT_CDF_CFL_ALPHA_CDF, 6, 15);               // cfl_alpha [6]
+  L->txsz = at();
   c.rows(MT_CDF_TXSZ_CAT0_CDF, 3, 1);                // txsz [4 cats][3 ctx]
   c.rows(MT_CDF_TXSZ_CAT1_CDF, 3, 2);
   c.rows(MT_CDF_TXSZ_CAT2_CDF, 3, 2);
   c.rows(MT_CDF_TXSZ_CAT3_CDF, 3, 2);
+  L->txtp8 = at();
   c.rows(MT_CDF_TXTP_INTRA1_TX8, 13, 6);             // txtp (TX_8X8) [13 y modes]
+  L->txtp4 = at();
   c.rows(MT_CDF_TXTP_INTRA1_TX4, 13, 6);             // txtp4
+  L->txtp16 = at();
   c.rows(MT_CDF_TXTP_INTRA2_TX16, 13, 4);            // txtp16
   const uint16_t* skip[5] = {MT_CDF_SKIP_TX4, MT_CDF_SKIP_TX8, MT_CDF_SKIP_TX16, MT_CDF_SKIP_TX32, MT_CDF_SKIP_TX64};
-  for (int k = 0; k < 5; ++k) c.singles(skip[k] + q * 13, 13);  // txb_skip [5 classes][13]
+  for (int k = 0; k < 5; ++k) {
+    L->txb_skip[k] = at();
+    c.singles(skip[k] + q * 13, 13);  // txb_skip [5 classes][13]
+  }
   struct Pl { const uint16_t* t; int rows; };
   const Pl base[5][2] = {{{MT_CDF_BASE_TOK_TX4_LUMA_Q, 41}, {MT_CDF_BASE_TOK_TX4_CHROMA_Q, 41}},
                          {{MT_CDF_BASE_TOK_TX8_LUMA_Q, 41}, {MT_CDF_BASE_TOK_TX8_CHROMA_Q, 41}},
@@ -292,32 +316,45 @@ void build_cdfs(int q, CdfSet& c) {
                          {{MT_CDF_BASE_TOK_TX32_LUMA_Q, 42}, {MT_CDF_BASE_TOK_TX32_CHROMA_Q, 42}},
                          {{MT_CDF_BASE_TOK_TX64_LUMA_Q, 42}, {nullptr, 0}}};
   for (int k = 0; k < 5; ++k)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
+      L->base_tok[k][p] = base[k][p].t ? at() : -1;
       if (base[k][p].t) c.rows(base[k][p].t + q * base[k][p].rows * 3, base[k][p].rows, 3);
+    }
   const uint16_t* br[4][2] = {{MT_CDF_BR_TOK_TX4_LUMA_Q, MT_CDF_BR_TOK_TX4_CHROMA_Q},
                               {MT_CDF_BR_TOK_TX8_LUMA_Q, MT_CDF_BR_TOK_TX8_CHROMA_Q},
                               {MT_CDF_BR_TOK_TX16_LUMA_Q, MT_CDF_BR_TOK_TX16_CHROMA_Q},
                               {MT_CDF_BR_TOK_TX32_LUMA_Q, MT_CDF_BR_TOK_TX32_CHROMA_Q}};
   for (int k = 0; k < 4; ++k)
-    for (int p = 0; p < 2; ++p) c.rows(br[k][p] + q * 21 * 3, 21, 3);
+    for (int p = 0; p < 2; ++p) {
+      L->br_tok[k][p] = at();
+      c.rows(br[k][p] + q * 21 * 3, 21, 3);
+    }
   const uint16_t* eb[5][2] = {{MT_CDF_EOB_BASE_TX4_LUMA_Q, MT_CDF_EOB_BASE_TX4_CHROMA_Q},
                               {MT_CDF_EOB_BASE_TX8_LUMA_Q, MT_CDF_EOB_BASE_TX8_CHROMA_Q},
                               {MT_CDF_EOB_BASE_TX16_LUMA_Q, MT_CDF_EOB_BASE_TX16_CHROMA_Q},
                               {MT_CDF_EOB_BASE_TX32_LUMA_Q, MT_CDF_EOB_BASE_TX32_CHROMA_Q},
                               {MT_CDF_EOB_BASE_TX64_LUMA_Q, nullptr}};
   for (int k = 0; k < 5; ++k)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
+      L->eob_base[k][p] = eb[k][p] ? at() : -1;
       if (eb[k][p]) c.rows(eb[k][p] + q * 4 * 2, 4, 2);
+    }
   const uint16_t* eh[5][2] = {{MT_CDF_EOB_HI_TX4_LUMA, MT_CDF_EOB_HI_TX4_CHROMA},
                               {MT_CDF_EOB_HI_TX8_LUMA, MT_CDF_EOB_HI_TX8_CHROMA},
                               {MT_CDF_EOB_HI_TX16_LUMA, MT_CDF_EOB_HI_TX16_CHROMA},
                               {MT_CDF_EOB_HI_TX32_LUMA, MT_CDF_EOB_HI_TX32_CHROMA},
                               {MT_CDF_EOB_HI_TX64_LUMA, nullptr}};
   for (int k = 0; k < 5; ++k)
-    for (int p = 0; p < 2; ++p)
+    for (int p = 0; p < 2; ++p) {
+      L->eob_hi[k][p] = eh[k][p] ? at() : -1;
       if (eh[k][p]) c.singles(eh[k][p] + q * 11, 11);
+    }
+  L->dc_sign[0] = at();
   c.singles(MT_CDF_DC_SIGN_Q + (q * 2 + 0) * 3, 3);  // dc_sign [plane][3]
+  L->dc_sign[1] = at();
   c.singles(MT_CDF_DC_SIGN_Q + (q * 2 + 1) * 3, 3);
+  L->eob_bin = at();  // 16_c, 16_l, 32_c, 32_l, 64_l, 16_l1d, 64_l1d, 128_l1d, 64_c, 256_l, 256_c,
+                      // 128_c, 128_l, 1024_l, 1024_c, 512_c, 512_l
   c.push(MT_CDF_EOB_BIN_16_CHROMA + q * 4, 4);
   c.push(MT_CDF_EOB_BIN_16_LUMA + q * 4, 4);
   c.push(MT_CDF_EOB_BIN_32_CHROMA + q * 5, 5);
@@ -335,8 +372,11 @@ void build_cdfs(int q, CdfSet& c) {
   c.push(MT_CDF_EOB_BIN_1024_CHROMA + q * 10, 10);
   c.push(MT_CDF_EOB_BIN_512_CHROMA + q * 9, 9);
   c.push(MT_CDF_EOB_BIN_512_LUMA + q * 9, 9);
+  L->delta_q = at();
   c.push(kDeltaQ, 3);          // delta_q
+  L->wiener_restore = at();
   c.push1(kWienerRestore);     // wiener_restore
+  L->nslots = at();
 }
 
 // gather_split_prob_icdf (src/coeffs.rs:2927-2935): the edge partition's
@@ -438,6 +478,13 @@ int mt_range_encoder_done(mt_range_encoder* e, uint8_t** out, size_t* out_len) {
   int rc = out_bytes(e->done(), out, out_len);
   delete e;
   return rc;
+}
+
+int mt_cdf_layout(mt_cdf_slot_layout* out) {
+  if (!out) return MT_ERR_INVALID_INPUT;
+  CdfSet c;
+  build_cdfs(0, c, out);
+  return MT_OK;
 }
 
 int32_t mt_cdf_slot_count(void) {

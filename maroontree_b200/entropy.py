@@ -112,3 +112,30 @@ def replay_tile_with_filters(trace, rect, cdef_grid=None, unit_cols=0, cdef_bits
                                               0 if grid is None else len(grid), cdef_bits, int(bool(updating_cdf)),
                                               C.byref(out), C.byref(n)), "mt_replay_tile_with_filters")
     return _take(out, n.value)
+
+
+def cdf_layout():
+    """First slot of every CDF group (``abi.CdfSlotLayout``)."""
+    out = abi.CdfSlotLayout()
+    _check(load().mt_cdf_layout(C.byref(out)), "mt_cdf_layout")
+    return out
+
+
+def emit_coeffs(levels, blocks):
+    """Coefficient tokens of transform blocks (``mt_emit_coeffs``): levels is an
+    int32 array, blocks COEF_BLOCK_DTYPE records; returns (tokens u32, offsets
+    (n + 1), res_ctx u8)."""
+    levels = np.ascontiguousarray(levels, np.int32).ravel()
+    blocks = np.ascontiguousarray(blocks, abi.COEF_BLOCK_DTYPE)
+    n = len(blocks)
+    offsets = np.zeros(n + 1, np.uint32)
+    res = np.zeros(max(n, 1), np.uint8)
+    tok = C.c_void_p()
+    _check(load().mt_emit_coeffs(ptr(levels), len(levels), ptr(blocks), n, C.byref(tok), ptr(offsets), ptr(res)),
+           "mt_emit_coeffs")
+    total = int(offsets[n])
+    try:
+        toks = np.frombuffer(C.string_at(tok, total * 4), np.uint32).copy() if total else np.zeros(0, np.uint32)
+    finally:
+        load().mt_free(tok)
+    return toks, offsets, res[:n]

@@ -846,28 +846,41 @@ def cdfs_new_slots(qctx, sections=None):
     sec["txsz"] = len(out)
     for k in range(4):
         rows(g[f"TXSZ_CAT{k}_CDF"])
+    sec["txtp8"] = len(out)
     rows(g["TXTP_INTRA1_TX8"])
+    sec["txtp4"] = len(out)
     rows(g["TXTP_INTRA1_TX4"])
+    sec["txtp16"] = len(out)
     rows(g["TXTP_INTRA2_TX16"])
-    for n in (4, 8, 16, 32, 64):
+    for k, n in enumerate((4, 8, 16, 32, 64)):
+        sec[f"txb_skip{k}"] = len(out)
         singles(g[f"SKIP_TX{n}"][qctx])
-    for n in (4, 8, 16, 32):
-        for p in ("LUMA", "CHROMA"):
+    for k, n in enumerate((4, 8, 16, 32)):
+        for pi, p in enumerate(("LUMA", "CHROMA")):
+            sec[f"base_tok{k}{pi}"] = len(out)
             rows(g[f"BASE_TOK_TX{n}_{p}_Q"][qctx])
+    sec["base_tok40"] = len(out)
     rows(g["BASE_TOK_TX64_LUMA_Q"][qctx])
-    for n in (4, 8, 16, 32):
-        for p in ("LUMA", "CHROMA"):
+    for k, n in enumerate((4, 8, 16, 32)):
+        for pi, p in enumerate(("LUMA", "CHROMA")):
+            sec[f"br_tok{k}{pi}"] = len(out)
             rows(g[f"BR_TOK_TX{n}_{p}_Q"][qctx])
-    for n in (4, 8, 16, 32):
-        for p in ("LUMA", "CHROMA"):
+    for k, n in enumerate((4, 8, 16, 32)):
+        for pi, p in enumerate(("LUMA", "CHROMA")):
+            sec[f"eob_base{k}{pi}"] = len(out)
             rows(g[f"EOB_BASE_TX{n}_{p}_Q"][qctx])
+    sec["eob_base40"] = len(out)
     rows(g["EOB_BASE_TX64_LUMA_Q"][qctx])
-    for n in (4, 8, 16, 32):
-        for p in ("LUMA", "CHROMA"):
+    for k, n in enumerate((4, 8, 16, 32)):
+        for pi, p in enumerate(("LUMA", "CHROMA")):
+            sec[f"eob_hi{k}{pi}"] = len(out)
             singles(g[f"EOB_HI_TX{n}_{p}"][qctx])
+    sec["eob_hi40"] = len(out)
     singles(g["EOB_HI_TX64_LUMA"][qctx])
     for p in range(2):
+        sec[f"dc_sign{p}"] = len(out)
         singles(g["DC_SIGN_Q"][qctx][p])
+    sec["eob_bin"] = len(out)
     for name in ("16_CHROMA", "16_LUMA", "32_CHROMA", "32_LUMA", "64_LUMA", "16_LUMA_1D", "64_LUMA_1D",
                  "128_LUMA_1D", "64_CHROMA", "256_LUMA", "256_CHROMA", "128_CHROMA", "128_LUMA", "1024_LUMA",
                  "1024_CHROMA", "512_CHROMA", "512_LUMA"):
@@ -882,3 +895,44 @@ def gather_split_prob(cdf, top):
     v = [int(x) for x in cdf]
     out = (v[1] - v[4]) + v[5] + (v[8] - v[7]) if top else (v[0] - v[1]) + (v[2] - v[6]) + (v[7] - v[8])
     return min(max(out, 1), 32767)
+
+
+class EmitSlots(C.Structure):
+    """The CDF groups the coefficient coders touch, as slot numbers."""
+    _fields_ = [("txb_skip", C.c_int32 * 4), ("base_tok", (C.c_int32 * 2) * 4), ("br_tok", (C.c_int32 * 2) * 4),
+                ("eob_base", (C.c_int32 * 2) * 4), ("eob_hi", (C.c_int32 * 2) * 4), ("dc_sign", C.c_int32 * 2),
+                ("eob_bin", C.c_int32), ("txtp4", C.c_int32), ("txtp8", C.c_int32), ("txtp16", C.c_int32)]
+
+
+def emit_slots(qctx=0):
+    sec = {}
+    cdfs_new_slots(qctx, sec)
+    e = EmitSlots()
+    for k in range(4):
+        e.txb_skip[k] = sec[f"txb_skip{k}"]
+        for p in range(2):
+            e.base_tok[k][p] = sec[f"base_tok{k}{p}"]
+            e.br_tok[k][p] = sec[f"br_tok{k}{p}"]
+            e.eob_base[k][p] = sec[f"eob_base{k}{p}"]
+            e.eob_hi[k][p] = sec[f"eob_hi{k}{p}"]
+    e.dc_sign[0], e.dc_sign[1] = sec["dc_sign0"], sec["dc_sign1"]
+    e.eob_bin, e.txtp4, e.txtp8, e.txtp16 = sec["eob_bin"], sec["txtp4"], sec["txtp8"], sec["txtp16"]
+    return e, sec
+
+
+def emit_coeffs(levels, blocks):
+    """The oracle's coefficient coders over a block list: (tokens, offsets, res_ctx)."""
+    levels = np.ascontiguousarray(levels, np.int32).ravel()
+    blocks = np.ascontiguousarray(blocks, abi.COEF_BLOCK_DTYPE)
+    n = len(blocks)
+    e, _ = emit_slots()
+    cap = int(sum(8 + 40 * (1 << (2 * int(b))) for b in blocks["log2n"])) + 1
+    toks = np.zeros(cap, np.uint32)
+    offsets = np.zeros(n + 1, np.uint32)
+    res = np.zeros(max(n, 1), np.uint8)
+    lib = load()
+    lib.or_emit_coeffs.restype = C.c_int
+    lib.or_emit_coeffs.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                   C.c_void_p]
+    assert lib.or_emit_coeffs(p(levels), p(blocks), n, C.addressof(e), p(toks), cap, p(offsets), p(res)) == 0
+    return toks[:offsets[n]].copy(), offsets, res[:n]
