@@ -1167,8 +1167,9 @@ typedef struct mt_coef_block {
   uint8_t dcs_ctx;      /* dc_sign context 0..2 */
   uint8_t y_mode;       /* luma: the tx-type CDF row */
   uint8_t txtp;         /* luma: tx-type symbol in the class's intra set */
-  uint8_t code_txtp;    /* luma: 1 codes the tx-type symbol */
-  uint8_t reserved;
+  uint8_t code_txtp;    /* luma: 1 codes the tx-type symbol (the 2-D class's) */
+  uint8_t tx_class;     /* 0 the 2-D class; 1 V_DCT, 2 H_DCT (luma TX_4X4 / TX_8X8: encode_tx{4,8}_coeffs_1d,
+                         * src/coeffs.rs:109-420, their own scan, contexts and eob CDF) */
 } mt_coef_block;
 /* Device form, two calls on the stream: with d_tokens NULL it counts each
  * block's tokens into d_counts and writes the n + 1 exclusive offsets

@@ -240,7 +240,7 @@ class EncodePlan(C.Structure):
 
 COEF_BLOCK_DTYPE = np.dtype([("cf_offset", "<u4"), ("log2n", "u1"), ("plane", "u1"), ("skip_ctx", "u1"),
                               ("dcs_ctx", "u1"), ("y_mode", "u1"), ("txtp", "u1"), ("code_txtp", "u1"),
-                              ("reserved", "u1")])
+                              ("tx_class", "u1")])
 assert COEF_BLOCK_DTYPE.itemsize == 12
 
 

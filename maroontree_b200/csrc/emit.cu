@@ -74,6 +74,104 @@ __device__ __forceinline__ int scan_at(int lg, int i) {
   return lg == 2 ? eScan4[i] : (lg == 3 ? eScan8[i] : eScan16[i]);
 }
 
+// The 1-D classes (V_DCT vertical, H_DCT horizontal) at TX_4X4 / TX_8X8:
+// encode_tx4_coeffs_1d / encode_tx8_coeffs_1d (src/coeffs.rs:264-420, :109-262).
+// Class coordinates (x, y) = (i mod n, i / n); the coefficient at class index
+// i is cf[(x << lg) | y] for the vertical class and cf[i] for the horizontal.
+__device__ void emit_block_1d(const int32_t* __restrict__ cf, const mt_coef_block& b, const mt_cdf_slot_layout& L,
+                              Sink& k, uint8_t* res_ctx) {
+  const int lg = b.log2n, n = 1 << lg, area = n * n;
+  const int cls = lg - 2;
+  const bool vertical = b.tx_class == 1;
+  auto pos_rc = [&](int i) { return vertical ? (((i & (n - 1)) << lg) | (i >> lg)) : i; };
+  int eob = -1;
+  for (int i = area - 1; i >= 0; --i)
+    if (cf[pos_rc(i)] != 0) {
+      eob = i;
+      break;
+    }
+  if (eob < 0) {
+    k.sym(L.txb_skip[cls] + b.skip_ctx, 1);
+    *res_ctx = 0x40;
+    return;
+  }
+  uint32_t cul = 0;
+  for (int i = 0; i <= eob; ++i) cul += (uint32_t)abs(cf[pos_rc(i)]);
+  k.sym(L.txb_skip[cls] + b.skip_ctx, 0);
+  k.sym((cls == 0 ? L.txtp4 : L.txtp8) + b.y_mode, vertical ? 2 : 3);
+  const uint8_t dcb = cf[0] == 0 ? (1 << 6) : (cf[0] < 0 ? 0 : (2 << 6));
+  *res_ctx = (uint8_t)(min(cul, 63u) | dcb);
+  const int32_t eb = L.eob_bin + (cls == 0 ? 5 : 6);  // eob_bin_16_l1d / eob_bin_64_l1d
+  const int32_t base = L.base_tok[cls][0], br = L.br_tok[cls][0], ebase = L.eob_base[cls][0];
+  if (eob == 0) {
+    k.sym(eb, 0);
+    const uint32_t m = (uint32_t)abs(cf[0]);
+    const uint32_t bs = min(m, 3u);
+    k.sym(ebase + 0, bs - 1);
+    if (bs == 3) k.hi_tok(m, br + 0);
+    k.sym(L.dc_sign[0] + b.dcs_ctx, cf[0] < 0 ? 1 : 0);
+    if (m >= 15) k.golomb(m - 15);
+    return;
+  }
+  const int eob_bin = eob < 2 ? eob : 32 - __clz((uint32_t)eob);
+  k.sym(eb, (uint32_t)eob_bin);
+  if (eob_bin > 1) {
+    const int nbits = eob_bin - 2;
+    k.sym(L.eob_hi[cls][0] + eob_bin, (uint32_t)((eob >> nbits) & 1));
+    for (int bb = nbits - 1; bb >= 0; --bb) k.bit(((eob >> bb) & 1) != 0);
+  }
+  uint8_t levels[160];  // stride 16, zero-padded: the 1-D context reaches (x, y + 4)
+  for (int i = 0; i < 160; ++i) levels[i] = 0;
+  auto lo_ctx = [&](int x, int y, uint32_t* hi) {
+    uint32_t mag = (uint32_t)levels[x * 16 + y + 1] + levels[(x + 1) * 16 + y] + levels[x * 16 + y + 2];
+    *hi = mag;
+    mag += (uint32_t)levels[x * 16 + y + 3] + levels[x * 16 + y + 4];
+    return 26u + (y > 1 ? 10u : (uint32_t)y * 5u) + (mag > 512 ? 4u : (mag + 64) >> 7);
+  };
+  const int ctx_e = 1 + (eob > (area >> 3)) + (eob > (area >> 2));
+  {
+    const int x = eob & (n - 1), y = eob >> lg;
+    const uint32_t m = (uint32_t)abs(cf[pos_rc(eob)]);
+    const uint32_t et = min(m, 3u) - 1;
+    k.sym(ebase + ctx_e, et);
+    if (et == 2) k.hi_tok(m, br + (y != 0 ? 14 : 7));
+    levels[x * 16 + y] = level_byte(m);
+  }
+  for (int i = eob - 1; i >= 1; --i) {
+    const int x = i & (n - 1), y = i >> lg;
+    uint32_t hi;
+    const uint32_t ctx = lo_ctx(x, y, &hi);
+    const uint32_t m = (uint32_t)abs(cf[pos_rc(i)]);
+    const uint32_t tok = min(m, 3u);
+    k.sym(base + (int32_t)ctx, tok);
+    if (tok == 3) {
+      const uint32_t mg = hi & 63;
+      k.hi_tok(m, br + (int32_t)((y != 0 ? 14 : 7) + (mg > 12 ? 6 : (mg + 1) >> 1)));
+    }
+    levels[x * 16 + y] = level_byte(m);
+  }
+  uint32_t dhi;
+  const uint32_t dctx = lo_ctx(0, 0, &dhi);
+  const uint32_t dm = (uint32_t)abs(cf[0]);
+  const uint32_t dt = min(dm, 3u);
+  k.sym(base + (int32_t)dctx, dt);
+  if (dt == 3) {
+    const uint32_t mg = dhi & 63;
+    k.hi_tok(dm, br + (int32_t)(mg > 12 ? 6 : (mg + 1) >> 1));
+  }
+  if (cf[0] != 0) {
+    k.sym(L.dc_sign[0] + b.dcs_ctx, cf[0] < 0 ? 1 : 0);
+    if (dm >= 15) k.golomb(dm - 15);
+  }
+  for (int i = 1; i <= eob; ++i) {
+    const int32_t c = cf[pos_rc(i)];
+    if (c != 0) {
+      k.bit(c < 0);
+      if ((uint32_t)abs(c) >= 15) k.golomb((uint32_t)abs(c) - 15);
+    }
+  }
+}
+
 // One block's tokens (and its coefficient context byte).
 __device__ void emit_block(const int32_t* __restrict__ cf, const mt_coef_block& b, const mt_cdf_slot_layout& L,
                            Sink& k, uint8_t* res_ctx) {
@@ -180,7 +278,10 @@ __global__ void __launch_bounds__(128) emit_kernel(const int32_t* __restrict__ l
   const mt_coef_block b = blocks[i];
   Sink k{WRITE ? tokens + offsets[i] : nullptr, 0};
   uint8_t rc = 0;
-  emit_block(levels + b.cf_offset, b, a.L, k, &rc);
+  if (b.tx_class)
+    emit_block_1d(levels + b.cf_offset, b, a.L, k, &rc);
+  else
+    emit_block(levels + b.cf_offset, b, a.L, k, &rc);
   if (!WRITE) counts[i] = k.n;
   if (WRITE && res_ctx) res_ctx[i] = rc;
 }
@@ -218,6 +319,7 @@ bool check_blocks_host(const mt_coef_block* b, int32_t n) {
     const int cls = b[i].log2n - 2;
     const int ntx = cls == 2 ? 5 : 7;  // INTRA2 at TX_16X16, INTRA1 below
     if (!b[i].plane && b[i].code_txtp && b[i].txtp >= ntx) return false;
+    if (b[i].tx_class > 2 || (b[i].tx_class && (b[i].plane || b[i].log2n > 3))) return false;
   }
   return true;
 }

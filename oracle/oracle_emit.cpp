@@ -155,6 +155,106 @@ uint8_t encode_square(Toks& t, const EmitSlots& S, const int32_t* cf, int n, boo
   return res_ctx;
 }
 
+// encode_tx4_coeffs_1d / encode_tx8_coeffs_1d (src/coeffs.rs:264-420, :109-262).
+uint8_t encode_1d(Toks& t, const EmitSlots& S, const int32_t* cf, int n, bool vertical, int skip_ctx, int dcs_ctx,
+                  int y_mode) {
+  const int cls = n == 4 ? 0 : 1, pl = 0, sh = n == 4 ? 2 : 3;
+  auto pos_rc = [&](int i) -> int {
+    const int x = i & (n - 1), y = i >> sh;
+    return vertical ? ((x << sh) | y) : i;
+  };
+  int eob = -1;
+  for (int i = n * n - 1; i >= 0; --i)
+    if (cf[pos_rc(i)] != 0) {
+      eob = i;
+      break;
+    }
+  if (eob < 0) {
+    t.symbol(S.txb_skip[cls] + skip_ctx, 1);
+    return 0x40;
+  }
+  uint32_t cul = 0;
+  for (int i = 0; i <= eob; ++i) cul += (uint32_t)abs(cf[pos_rc(i)]);
+  t.symbol(S.txb_skip[cls] + skip_ctx, 0);
+  t.symbol((cls == 0 ? S.txtp4 : S.txtp8) + y_mode, vertical ? 2 : 3);
+  const uint8_t dc_sign_bits = cf[0] == 0 ? (1 << 6) : (cf[0] < 0 ? 0 : (2 << 6));
+  const uint8_t res_ctx = (uint8_t)((cul < 63 ? cul : 63) | dc_sign_bits);
+  const int32_t eb = S.eob_bin + (cls == 0 ? 5 : 6);  // eob_bin_16_l1d, eob_bin_64_l1d
+  if (eob == 0) {
+    t.symbol(eb, 0);
+    const uint32_t m = (uint32_t)abs(cf[0]);
+    const uint32_t base = m < 3 ? m : 3;
+    t.symbol(S.eob_base[cls][pl] + 0, base - 1);
+    if (base == 3) encode_hi_tok(t, m, S.br_tok[cls][pl] + 0);
+    t.symbol(S.dc_sign[pl] + dcs_ctx, cf[0] < 0 ? 1 : 0);
+    if (m >= 15) encode_golomb(t, m - 15);
+    return res_ctx;
+  }
+  int eob_bin = eob;
+  if (eob >= 2) {
+    eob_bin = 0;
+    while ((1u << eob_bin) <= (uint32_t)eob) ++eob_bin;
+  }
+  t.symbol(eb, (uint32_t)eob_bin);
+  if (eob_bin > 1) {
+    const int nbits = eob_bin - 2;
+    t.symbol(S.eob_hi[cls][pl] + eob_bin, (uint32_t)((eob >> nbits) & 1));
+    for (int b = nbits - 1; b >= 0; --b) t.boolean(((eob >> b) & 1) == 1);
+  }
+  uint8_t levels[16 * 10] = {};
+  auto lvl = [&](int x, int y) { return (uint32_t)levels[x * 16 + y]; };
+  auto lo_ctx_1d = [&](int x, int y, uint32_t* hi_mag) {
+    uint32_t mag = lvl(x, y + 1) + lvl(x + 1, y) + lvl(x, y + 2);
+    *hi_mag = mag;
+    mag += lvl(x, y + 3) + lvl(x, y + 4);
+    const uint32_t offset = 26 + (y > 1 ? 10 : (uint32_t)y * 5);
+    return offset + (mag > 512 ? 4 : (mag + 64) >> 7);
+  };
+  const int ctx_e = 1 + (eob > (n * n) / 8 ? 1 : 0) + (eob > (n * n) / 4 ? 1 : 0);
+  {
+    const int x = eob & (n - 1), y = eob >> sh;
+    const uint32_t m = (uint32_t)abs(cf[pos_rc(eob)]);
+    const uint32_t eob_tok = (m < 3 ? m : 3) - 1;
+    t.symbol(S.eob_base[cls][pl] + ctx_e, eob_tok);
+    if (eob_tok == 2) encode_hi_tok(t, m, S.br_tok[cls][pl] + (y != 0 ? 14 : 7));
+    levels[x * 16 + y] = level_byte(m);
+  }
+  for (int i = eob - 1; i >= 1; --i) {
+    const int x = i & (n - 1), y = i >> sh;
+    uint32_t hi_mag;
+    const uint32_t ctx = lo_ctx_1d(x, y, &hi_mag);
+    const uint32_t m = (uint32_t)abs(cf[pos_rc(i)]);
+    const uint32_t tok = m < 3 ? m : 3;
+    t.symbol(S.base_tok[cls][pl] + (int32_t)ctx, tok);
+    if (tok == 3) {
+      const uint32_t mg = hi_mag & 63;
+      encode_hi_tok(t, m, S.br_tok[cls][pl] + (int32_t)((y != 0 ? 14 : 7) + (mg > 12 ? 6 : (mg + 1) >> 1)));
+    }
+    levels[x * 16 + y] = level_byte(m);
+  }
+  uint32_t dc_hi;
+  const uint32_t dc_ctx = lo_ctx_1d(0, 0, &dc_hi);
+  const uint32_t dm = (uint32_t)abs(cf[0]);
+  const uint32_t dc_tok = dm < 3 ? dm : 3;
+  t.symbol(S.base_tok[cls][pl] + (int32_t)dc_ctx, dc_tok);
+  if (dc_tok == 3) {
+    const uint32_t mg = dc_hi & 63;
+    encode_hi_tok(t, dm, S.br_tok[cls][pl] + (int32_t)(mg > 12 ? 6 : (mg + 1) >> 1));
+  }
+  if (cf[0] != 0) {
+    t.symbol(S.dc_sign[pl] + dcs_ctx, cf[0] < 0 ? 1 : 0);
+    if (dm >= 15) encode_golomb(t, dm - 15);
+  }
+  for (int i = 1; i <= eob; ++i) {
+    const int32_t c = cf[pos_rc(i)];
+    if (c != 0) {
+      t.boolean(c < 0);
+      if ((uint32_t)abs(c) >= 15) encode_golomb(t, (uint32_t)abs(c) - 15);
+    }
+  }
+  return res_ctx;
+}
+
 }  // namespace
 
 extern "C" int or_emit_coeffs(const int32_t* levels, const mt_coef_block* blocks, int32_t n, const EmitSlots* S,
@@ -163,8 +263,12 @@ extern "C" int or_emit_coeffs(const int32_t* levels, const mt_coef_block* blocks
   for (int32_t i = 0; i < n; ++i) {
     Toks t;
     const mt_coef_block& b = blocks[i];
-    res_ctx[i] = encode_square(t, *S, levels + b.cf_offset, 1 << b.log2n, b.plane != 0, b.skip_ctx, b.dcs_ctx,
-                               b.y_mode, b.txtp, b.code_txtp != 0);
+    if (b.tx_class)
+      res_ctx[i] = encode_1d(t, *S, levels + b.cf_offset, 1 << b.log2n, b.tx_class == 1, b.skip_ctx, b.dcs_ctx,
+                             b.y_mode);
+    else
+      res_ctx[i] = encode_square(t, *S, levels + b.cf_offset, 1 << b.log2n, b.plane != 0, b.skip_ctx, b.dcs_ctx,
+                                 b.y_mode, b.txtp, b.code_txtp != 0);
     offsets[i] = (uint32_t)at;
     if (at + t.v.size() > cap) return -1;
     memcpy(tokens + at, t.v.data(), t.v.size() * 4);
