@@ -11,8 +11,11 @@ src/coder/block8.rs:2620-2700, src/coder/lossy_state.rs:1408-1415,
 :4021-4051, src/coeffs.rs:2917-2920).
 
 The picture is coded with the identity matrix (RGB as G, B, R planes), full
-range, so the decoder's RGB output is the reconstruction itself; the loop
-filter and CDEF are left off so nothing after the reconstruction changes it.
+range, so the decoder's RGB output is the reconstruction itself.  With
+filters=True the frame also carries the shipped loop-filter levels and the
+oracle's CDEF decision (strengths in the frame header, each superblock's
+cdef_idx inserted at its read_cdef() point by the library's filter replay), and
+the expected output is the oracle's deblocked and CDEF-filtered planes.
 """
 import io
 
@@ -54,8 +57,8 @@ SCAN8 = [0, 8, 1, 2, 9, 16, 24, 17, 10, 3, 4, 11, 18, 25, 32, 40, 33, 26, 19, 12
 
 
 class Coder:
-    def __init__(self, mt, po, rgb, qidx, qm_level, gpu, seed=0):
-        self.mt, self.po, self.gpu = mt, po, gpu
+    def __init__(self, mt, po, rgb, qidx, qm_level, gpu, seed=0, filters=False, pick="random"):
+        self.mt, self.po, self.gpu, self.filters, self.pick = mt, po, gpu, filters, pick
         self.h, self.w = rgb.shape[:2]
         assert self.w % 64 == 0 and self.h % 64 == 0
         # identity matrix: Y = G, U = B, V = R
@@ -101,6 +104,16 @@ class Coder:
         self.rec[plane][py:py + 8, px:px + 8] = ro[0].reshape(8, 8)
         return lv[0]
 
+    def best(self, px, py, flags):
+        prm = self.mt.chain_params(self.w, self.h, tx_size=8, mode_lambda=20.0, satd_bridge=0.7)
+        cands = np.zeros(13 * 7, abi.CANDIDATE_DTYPE)
+        cands["px"], cands["py"], cands["flags"] = px, py, flags
+        cands["mode"] = np.repeat(np.arange(13), 7)
+        cands["tx_type"] = np.tile(np.array(TYPES), 13)
+        res, _, _ = self.po.candidate_chain(self.src[0], self.rec[0], prm, self.q[0], self.qm, self.cdfs, cands)
+        k = int(np.argmin(res["cost"]))
+        return int(cands["mode"][k]), 0, int(cands["tx_type"][k])
+
     def block8(self, out, x8, y8, thr, lhb):
         px, py = x8 * 8, y8 * 8
         bx4, by4 = px // 4, py // 4
@@ -109,6 +122,10 @@ class Coder:
         mode = int(self.rng.integers(0, 13))
         delta = int(self.rng.integers(-3, 4)) if 1 <= mode <= 8 else 0
         tx = int(TYPES[int(self.rng.integers(0, 7))])
+        ft = (py > 0 and self.a_mode[bx4] in SMOOTH) or (px > 0 and self.l_mode[by4] in SMOOTH)
+        flags = (abi.CAND_HAVE_TR if have_tr else 0) | (abi.CAND_HAVE_BL if have_bl else 0)
+        if self.pick == "best":  # the lowest-cost (mode, type) of the chain at delta 0
+            mode, delta, tx = self.best(px, py, flags | (abi.CAND_FILTER_TYPE if ft else 0))
         L = self.L
         out.append(self.tok(L.skip + int(self.a_skip[bx4]) + int(self.l_skip[by4]), 0))  # skip = 0
         self.a_skip[bx4:bx4 + 2] = 0
@@ -127,8 +144,6 @@ class Coder:
         out.append(self.tok(L.txsz + 0 * 3 + ctx, 0))  # tx_depth 0: TX_8X8
         self.a_tx[bx4:bx4 + 2] = 1
         self.l_tx[by4:by4 + 2] = 1
-        ft = (py > 0 and self.a_mode[bx4] in SMOOTH) or (px > 0 and self.l_mode[by4] in SMOOTH)
-        flags = (abi.CAND_HAVE_TR if have_tr else 0) | (abi.CAND_HAVE_BL if have_bl else 0)
         for plane in range(3):
             lv = self.chain(plane, px, py, mode if plane == 0 else 0, delta if plane == 0 else 0,
                             tx if plane == 0 else abi.TX_DCT_DCT,
@@ -184,20 +199,60 @@ class Coder:
                 else:
                     s.append(t)
             streams.append(np.array(s, np.uint32))
-        tile = en.pack_tile(self.qidx, streams)
-        sp = ct.SequenceHeaderParams()
-        sp.width, sp.height, sp.profile, sp.bit_depth = self.w, self.h, 1, 8
-        sp.color_present, sp.primaries, sp.transfer, sp.matrix, sp.full_range = 1, 1, 13, 0, 1
-        sp.enable_filter_intra = sp.enable_intra_edge_filter = 1
         fp = ct.FrameHeaderParams()
         fp.w8, fp.h8, fp.base_q_idx = self.w, self.h, self.qidx
         fp.qm_y = fp.qm_u = fp.qm_v = self.qm_level
         fp.updating_cdf = 1
         fp.cdef_bits, fp.cdef_damping = -1, 3
+        self.out = [p.copy() for p in self.rec]
+        if not self.filters:
+            tile = en.pack_tile(self.qidx, streams)
+        else:
+            self.out, fp = self.loop_filters(fp)
+            # every superblock's first block is coded (skip = 0): its read_cdef()
+            # point follows that block's skip flag, the fifth token of the SB
+            points = [5] * len(streams) if fp.cdef_bits >= 0 else None
+            _, trace = en.pack_tile(self.qidx, streams, points, want_trace=True)
+            if fp.cdef_bits > 0:
+                tile = en.replay_tile_with_filters(trace, (0, 0, self.w, self.h), self.cdef["grid"],
+                                                   unit_cols=self.w // 64, cdef_bits=fp.cdef_bits)
+            else:
+                tile = en.replay_tile_with_filters(trace, (0, 0, self.w, self.h))
+        sp = ct.SequenceHeaderParams()
+        sp.width, sp.height, sp.profile, sp.bit_depth = self.w, self.h, 1, 8
+        sp.color_present, sp.primaries, sp.transfer, sp.matrix, sp.full_range = 1, 1, 13, 0, 1
+        sp.enable_filter_intra = sp.enable_intra_edge_filter = 1
         obu = ct.av1_stream(sp, fp, [tile])
         item = ct.srgb_item(self.w, self.h, "444")
         item.matrix = 0
         return ct.wrap_av1_image(obu, item)
+
+
+def _loop_filters(self, fp):
+    """Deblocking with the shipped levels (uniform 8x8 blocks and transforms)
+    and the oracle's CDEF decision over the deblocked planes."""
+    n4r, n4c = self.h // 4, self.w // 4
+    two = np.full((n4r, n4c), 2, np.uint8)
+    tv = np.zeros((n4r, n4c), np.uint8)
+    tv[:, ::2] = 1
+    tt = np.zeros((n4r, n4c), np.uint8)
+    tt[::2, :] = 1
+    ly, luv, sharp = self.mt.loop_filter_levels(self.qidx, 0, 0)
+    fp.lf_y, fp.lf_u, fp.lf_v, fp.lf_sharpness = ly, luv, luv, sharp
+    planes = self.po.deblock_frame(self.rec, self.w, self.h, 0, 0, (two, two, tv, tt), (two, two), ly, luv, luv)
+    prm = self.mt.cdef_params(self.w, self.h, 0, 0, self.qidx)
+    skip8 = np.zeros((self.h // 8, self.w // 8), np.uint8)
+    out, dec, _ = self.po.cdef_frame(planes, self.src, skip8, prm)
+    self.cdef = dec
+    if dec["bits"] >= 0:
+        fp.cdef_bits, fp.cdef_damping = dec["bits"], dec["damping"]
+        for e, st in enumerate(dec["strengths"]):
+            for k in range(4):
+                fp.cdef_strengths[e][k] = st[k]
+    return out, fp
+
+
+Coder.loop_filters = _loop_filters
 
 
 def decode_rgb(avif):
@@ -208,8 +263,8 @@ def decode_rgb(avif):
     return np.asarray(im.convert("RGB"))
 
 
-def encode_and_decode(mt, po, w, h, seed, qidx, qm_level, gpu):
-    rgb = synth.generate_rgb(w, h, seed)
-    c = Coder(mt, po, rgb, qidx, qm_level, gpu, seed)
+def encode_and_decode(mt, po, w, h, seed, qidx, qm_level, gpu, filters=False, pick="random", sigma=4.0):
+    rgb = synth.generate_rgb(w, h, seed, sigma=sigma)
+    c = Coder(mt, po, rgb, qidx, qm_level, gpu, seed, filters, pick)
     avif = c.encode()
     return c, decode_rgb(avif), avif
