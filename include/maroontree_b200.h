@@ -1182,6 +1182,31 @@ int mt_emit_coeffs_device(const int32_t* d_levels, const mt_coef_block* d_blocks
 int mt_emit_coeffs(const int32_t* levels, size_t nlevels, const mt_coef_block* blocks, int32_t n, uint32_t** tokens,
                    uint32_t* offsets, uint8_t* res_ctx);
 
+
+/* ---- End-to-end encode ------------------------------------------------------
+ * encode_rgb8 (src/avif.rs:915-940) for 8-bit RGB: the encode_rgb8 input
+ * checks and EncodeConfig validation, Q13 colour conversion and padding, the
+ * decisions below on the device, and the reference's coefficient and block
+ * syntax, adaptive range coder, loop-filter levels, CDEF strength search with
+ * its cdef_idx replay, sequence / frame headers and AVIF container.  The
+ * decisions are NOT the reference's decode_sb search: every superblock is
+ * split down to 8x8 blocks, each taking the lowest-RD-cost (13 intra modes at
+ * angle delta 0) x (7 intra transform types) luma candidate of the candidate
+ * chain, chroma UV_DC_PRED / DCT_DCT; the output is therefore a valid AVIF
+ * with this library's own decisions, not the reference's bytes.  4:2:0 and
+ * 4:4:4 (else MT_ERR_UNSUPPORTED_CHROMA_FORMAT).  *out is freed with mt_free. */
+int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
+                   size_t* out_len);
+/* The same, also returning the decoder's output planes (padded sizes of
+ * mt_padded_plane_dims, after deblocking and CDEF) when recon_out is non-NULL. */
+int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
+                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3]);
+/* The same encode from 8-bit Y, U, V planes (chroma at ((w + sx) >> sx) x
+ * ((h + sy) >> sy)), without colour conversion: the planes are coded as
+ * given and described by the config's CICP (e.g. identity for G, B, R). */
+int mt_encode_yuv8(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t width, uint32_t height,
+                   const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,748 @@
+// mt_encode_rgb8: an end-to-end AVIF encode on the device with this library's
+// kernels and the reference's bitstream, entropy coder and container.
+//
+// What it decides, and what it does not: the reference's superblock decision
+// engine (src/coder/superblock.rs:813 decode_sb and its partition / leaf
+// searches) is not restated here.  This encoder codes every 64x64 superblock
+// as a full split down to 8x8 blocks; each 8x8 luma block takes the lowest RD
+// cost (strict <, first in (mode, type) order) of the 13 intra modes at angle
+// delta 0 times the seven 8x8 intra transform types, as priced by the batched
+// candidate chain (prediction, forward transform, quantisation and QM,
+// trellis, inverse, SATD bridge, coefficient rate); chroma is UV_DC_PRED with
+// DCT_DCT (8x8 in 4:4:4, 4x4 in 4:2:0).  Everything after the decisions is the
+// reference's: the coefficient coders and block syntax with their contexts,
+// the adaptive range coder and tile packer, the shipped loop-filter levels,
+// the CDEF strength search with its per-unit cdef_idx replay, the sequence and
+// frame headers and the AVIF container.  The result decodes under any AV1
+// decoder to the reconstruction this encoder computed.
+//
+// Schedule: superblocks in the d = 2 * row + col wavefront (each needs its
+// left, top and top-right neighbours), one launch per diagonal and one CTA
+// per superblock; inside a CTA the 8x8 blocks go in z-order, the 91 luma
+// candidates of a block one per thread, the CTA minimum picks the winner.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/maroontree_b200.h"
+#include "av1_tables.h"
+#include "chain4.cuh"
+#include "chain8.cuh"
+
+namespace mth {
+float scaled_trellis_lambda_host(float dc_q, float lambda0);
+}
+
+namespace {
+
+constexpr int kEncThreads = 128;
+constexpr int kCands = 13 * 7;
+__constant__ uint8_t kEncTypes[7] = {MT_TX_IDTX,      MT_TX_DCT_DCT,   MT_TX_V_DCT,  MT_TX_H_DCT,
+                                     MT_TX_ADST_ADST, MT_TX_ADST_DCT, MT_TX_DCT_ADST};
+
+struct EncArgs {
+  const uint16_t* src[3];
+  uint16_t* rec[3];
+  mt_chain_params py, pc;  // luma / chroma plane parameters
+  mt_quant qy, qc;
+  float tly, tlc;          // scaled trellis lambdas
+  int has_qm_y, has_qm_c;  // a QM row for luma / chroma (level < 15)
+  int sub;                 // 0 4:4:4, 2 4:2:0
+  int sb_cols;
+  int w8, h8;
+  uint8_t* mode;           // per 8x8 block (frame raster of 8x8 blocks)
+  uint8_t* tx;
+  int32_t* lv_y;           // 64 per block
+  int32_t* lv_u;           // 64 (4:4:4) or 16 (4:2:0) per block
+  int32_t* lv_v;
+};
+
+// The z-order position of the k-th 8x8 block of a superblock and its
+// intra-edge flags down the quadtree (src/coder/superblock.rs:958-987: root
+// (top-right 1, bottom-left 0); children TL (1, 1), TR (parent's, 0),
+// BL (1, parent's), BR (0, 0)).
+__device__ __forceinline__ void zorder(int k, int* bx, int* by, bool* thr, bool* lhb) {
+  int x = 0, y = 0;
+  bool t = true, l = false;
+  for (int lvl = 2; lvl >= 0; --lvl) {
+    const int c = (k >> (2 * lvl)) & 3;
+    const int h = 1 << lvl;
+    if (c == 0) {
+      t = true;
+      l = true;
+    } else if (c == 1) {
+      x += h;
+      l = false;
+    } else if (c == 2) {
+      y += h;
+      t = true;
+    } else {
+      x += h;
+      y += h;
+      t = false;
+      l = false;
+    }
+  }
+  *bx = x;
+  *by = y;
+  *thr = t;
+  *lhb = l;
+}
+
+// Coefficient bit costs, QM weights and their forward scales into shared
+// memory (n QM entries: 64 for an 8x8 transform, 16 for a 4x4 one).
+__device__ __forceinline__ void enc_stage(const mt_coef_costs* __restrict__ costs, const uint8_t* __restrict__ qm_row,
+                                          int nqm, int has_qm, mt_coef_costs& sC, uint8_t* sQm, float* sQs, float* sLut) {
+  const float* g = reinterpret_cast<const float*>(costs);
+  float* s = reinterpret_cast<float*>(&sC);
+  for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+  if (threadIdx.x < 64) {
+    const int w = (has_qm && (int)threadIdx.x < nqm) ? qm_row[threadIdx.x] : 32;
+    sQm[threadIdx.x] = (uint8_t)w;
+    sQs[threadIdx.x] = mtd::fwd_qm_scale(w);
+    sLut[threadIdx.x] = mtd::kCoefRateLut[threadIdx.x];
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool is_smooth(int m) { return m == MT_SMOOTH_PRED || m == MT_SMOOTH_V_PRED || m == MT_SMOOTH_H_PRED; }
+
+__global__ void __launch_bounds__(kEncThreads) encode_sb_kernel(EncArgs a, const mt_coef_costs* __restrict__ costs_y,
+                                                                 const mt_coef_costs* __restrict__ costs_c,
+                                                                 const uint8_t* __restrict__ qm_y,
+                                                                 const uint8_t* __restrict__ qm_c, int d) {
+  __shared__ mt_coef_costs sCy;
+  __shared__ mt_coef_costs sCc;
+  __shared__ uint8_t sQmY[64], sQmC[64];
+  __shared__ float sQsY[64], sQsC[64], sLut[64];
+  __shared__ unsigned long long sBest;
+  enc_stage(costs_y, qm_y, 64, a.has_qm_y, sCy, sQmY, sQsY, sLut);
+  enc_stage(costs_c, qm_c, a.sub ? 16 : 64, a.has_qm_c, sCc, sQmC, sQsC, sLut);
+  // the b-th superblock on diagonal d = 2 * row + col
+  const int sb_rows = (a.h8 + 63) / 64;
+  int row = 0, col = 0, found = 0;
+  for (int r = 0, seen = 0; r < sb_rows; ++r) {
+    const int c = d - 2 * r;
+    if (c < 0 || c >= a.sb_cols) continue;
+    if (seen++ == (int)blockIdx.x) {
+      row = r;
+      col = c;
+      found = 1;
+      break;
+    }
+  }
+  if (!found) return;
+  const int nbx = a.w8 / 8;
+  int32_t store[mtd::kWork8Words];
+  mtd::Work8 w{store};
+  for (int k = 0; k < 64; ++k) {
+    int bx, by;
+    bool thr, lhb;
+    zorder(k, &bx, &by, &thr, &lhb);
+    const int px = col * 64 + bx * 8, py = row * 64 + by * 8;
+    if (px >= a.w8 || py >= a.h8) continue;  // uniform across the CTA
+    const int b = (py / 8) * nbx + px / 8;
+    const bool have_tr = thr && py > 0 && px + 8 < a.w8;
+    const bool have_bl = lhb && px > 0 && py + 8 < a.h8;
+    const bool ft = (py > 0 && is_smooth(a.mode[b - nbx])) || (px > 0 && is_smooth(a.mode[b - 1]));
+    const uint8_t flags = (have_tr ? 1 : 0) | (have_bl ? 2 : 0);
+    if (threadIdx.x == 0) sBest = ~0ull;
+    __syncthreads();
+    const int t = threadIdx.x;
+    mt_candidate cd = {};
+    cd.px = (uint16_t)px;
+    cd.py = (uint16_t)py;
+    cd.flags = flags | (ft ? 4 : 0);
+    if (t < kCands) {
+      cd.mode = (uint8_t)(t / 7);
+      cd.tx_type = kEncTypes[t % 7];
+      mt_candidate_result r;
+      mtd::chain8_predict(a.rec[0], a.py, cd, w);
+      mtd::chain8_tx<false>(a.src[0], a.py, a.qy, a.tly, a.has_qm_y ? sQmY : nullptr, sQsY, sLut, sCy, cd, r, w);
+      const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)t;
+      atomicMin(&sBest, key);
+    }
+    __syncthreads();
+    const int win = (int)(sBest & 0xffffffffu);
+    if (t == win) {  // the winner still holds its levels, prediction and inverse residual
+      const int16_t* cf = w.cf();
+      const int16_t* pr = w.pred();
+      const int16_t* rr = w.rr();
+      for (int i = 0; i < 64; ++i) a.lv_y[(size_t)b * 64 + i] = cf[i];
+      for (int y = 0; y < 8; ++y)
+        for (int x = 0; x < 8; ++x)
+          a.rec[0][(size_t)(py + y) * a.py.stride + px + x] =
+              (uint16_t)min(max((int)pr[y * 8 + x] + rr[y * 8 + x], 0), 255);
+      a.mode[b] = cd.mode;
+      a.tx[b] = cd.tx_type;
+    }
+    // chroma: UV_DC_PRED, DCT_DCT, one thread per plane
+    if (t < 2) {
+      mt_candidate cc = {};
+      cc.mode = MT_DC_PRED;
+      cc.tx_type = MT_TX_DCT_DCT;
+      mt_candidate_result r;
+      int32_t* lv = t == 0 ? a.lv_u : a.lv_v;
+      if (a.sub == 0) {
+        cc.px = (uint16_t)px;
+        cc.py = (uint16_t)py;
+        cc.flags = flags;
+        mtd::chain8_predict(a.rec[1 + t], a.pc, cc, w);
+        mtd::chain8_tx<false>(a.src[1 + t], a.pc, a.qc, a.tlc, a.has_qm_c ? sQmC : nullptr, sQsC, sLut, sCc, cc, r,
+                              w);
+        const int16_t* cf = w.cf();
+        const int16_t* pr = w.pred();
+        const int16_t* rr = w.rr();
+        for (int i = 0; i < 64; ++i) lv[(size_t)b * 64 + i] = cf[i];
+        for (int y = 0; y < 8; ++y)
+          for (int x = 0; x < 8; ++x)
+            a.rec[1 + t][(size_t)(py + y) * a.pc.stride + px + x] =
+                (uint16_t)min(max((int)pr[y * 8 + x] + rr[y * 8 + x], 0), 255);
+      } else {
+        cc.px = (uint16_t)(px / 2);
+        cc.py = (uint16_t)(py / 2);
+        int32_t st4[mtd::kWork4Words];
+        mtd::Work4 w4{st4};
+        mtd::chain4_one<false>(a.src[1 + t], a.rec[1 + t], a.pc, a.qc, a.tlc, a.has_qm_c ? sQmC : nullptr, sQsC,
+                               sLut, sCc, cc, r, w4);
+        const int16_t* cf = w4.cf();
+        const int16_t* pr = w4.pred();
+        const int16_t* rr = w4.rr();
+        for (int i = 0; i < 16; ++i) lv[(size_t)b * 16 + i] = cf[i];
+        for (int y = 0; y < 4; ++y)
+          for (int x = 0; x < 4; ++x)
+            a.rec[1 + t][(size_t)(cc.py + y) * a.pc.stride + cc.px + x] =
+                (uint16_t)min(max((int)pr[y * 4 + x] + rr[y * 4 + x], 0), 255);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// One plane of 8-bit samples into the coder's padded u16 plane, edge samples
+// replicated past the displayed size (pad_to_mult8_u16, src/dispatch.rs:113-131).
+__global__ void pad_plane_kernel(const uint8_t* __restrict__ in, int w, int h, uint16_t* __restrict__ out, int pw,
+                                 int ph) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  if (x >= pw || y >= ph) return;
+  out[(size_t)y * pw + x] = in[(size_t)min(y, h - 1) * w + min(x, w - 1)];
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+namespace {
+
+const int kIntraModeCtx[13] = {0, 1, 2, 3, 4, 4, 4, 4, 3, 0, 1, 2, 0};  // src/intrapred.rs:1088
+
+struct BlockSyntax {
+  const mt_cdf_slot_layout& L;
+  int w8, h8, sub, nbx;
+  const uint8_t* mode;
+  const uint8_t* tx;
+  std::vector<uint8_t> a_part, l_part, a_skip, l_skip, a_mode, l_mode;
+  std::vector<int8_t> a_tx, l_tx;
+  std::vector<uint8_t> a_coef[3], l_coef[3];
+  const uint8_t* res_ctx;  // per coefficient block, in coding order: (Y, U, V) per 8x8 block
+  std::vector<mt_coef_block>* blocks;
+  std::vector<std::vector<uint32_t>> sbs;  // tokens with coefficient placeholders
+  std::vector<int32_t> cdef_points;
+
+  static constexpr uint32_t kCoef = 0xFFFFFFFFu;  // placeholder: next coefficient block's tokens
+  std::vector<uint32_t>* out;
+
+  void tok(int32_t slot, uint32_t s) { out->push_back(((uint32_t)slot << 8) | s); }
+  int part_ctx(int bl, int x8, int y8) const {
+    const int sh = 4 - bl;
+    return ((a_part[x8] >> sh) & 1) + (((l_part[y8] >> sh) & 1) << 1);
+  }
+
+  void block8(int x8, int y8, int* cdef_point) {
+    const int px = x8 * 8, py = y8 * 8, bx4 = px / 4, by4 = py / 4;
+    const int b = y8 * nbx + x8;
+    const int m = mode[b], t = tx[b];
+    tok(L.skip + a_skip[bx4] + l_skip[by4], 0);
+    if (*cdef_point < 0) *cdef_point = (int)out->size();  // read_cdef() follows the SB's first coded skip flag
+    a_skip[bx4] = a_skip[bx4 + 1] = 0;
+    l_skip[by4] = l_skip[by4 + 1] = 0;
+    tok(L.kf_y + kIntraModeCtx[a_mode[bx4]] * 5 + kIntraModeCtx[l_mode[by4]], (uint32_t)m);
+    if (m >= MT_V_PRED && m <= MT_D67_PRED) tok(L.angle_delta + m - MT_V_PRED, 3);  // delta 0
+    tok(L.uv_mode + 13 + m, MT_DC_PRED);  // CfL allowed at 8x8
+    if (m == MT_DC_PRED) tok(L.palette_y_mode + 0, 0);
+    tok(L.palette_uv_mode + 0, 0);
+    if (m == MT_DC_PRED) tok(L.filter_intra + 3, 0);  // BLOCK_8X8
+    tok(L.txsz + 0 * 3 + (l_tx[by4] >= 1) + (a_tx[bx4] >= 1), 0);
+    a_tx[bx4] = a_tx[bx4 + 1] = 1;
+    l_tx[by4] = l_tx[by4 + 1] = 1;
+    // residual: Y (TX_8X8), then U and V (TX_8X8 in 4:4:4, TX_4X4 in 4:2:0)
+    for (int p = 0; p < 3; ++p) {
+      const int u = (p == 0 || sub == 0) ? 2 : 1;  // 4x4 units the transform spans
+      const int cx = (p == 0 || sub == 0) ? bx4 : bx4 / 2, cy = (p == 0 || sub == 0) ? by4 : by4 / 2;
+      std::vector<uint8_t>& A = a_coef[p];
+      std::vector<uint8_t>& Ll = l_coef[p];
+      int s = -2 * u, anz = 0, lnz = 0;
+      for (int k = 0; k < u; ++k) {
+        s += (A[cx + k] >> 6) + (Ll[cy + k] >> 6);
+        anz |= A[cx + k] != 0x40;
+        lnz |= Ll[cy + k] != 0x40;
+      }
+      mt_coef_block cb = {};
+      cb.log2n = u == 2 ? 3 : 2;
+      cb.plane = p ? 1 : 0;
+      cb.skip_ctx = (uint8_t)(p == 0 ? 0 : 7 + anz + lnz);
+      cb.dcs_ctx = (uint8_t)((s != 0) + (s > 0));
+      cb.y_mode = (uint8_t)m;
+      cb.txtp = (uint8_t)(p == 0 ? t : MT_TX_DCT_DCT);
+      cb.code_txtp = p == 0;
+      cb.tx_class = (uint8_t)(p == 0 && t == MT_TX_V_DCT ? 1 : (p == 0 && t == MT_TX_H_DCT ? 2 : 0));
+      blocks->push_back(cb);
+      out->push_back(kCoef);
+    }
+    a_mode[bx4] = a_mode[bx4 + 1] = (uint8_t)m;
+    l_mode[by4] = l_mode[by4 + 1] = (uint8_t)m;
+  }
+
+  // After a block's coefficient contexts are known: its res_ctx bytes.
+  void commit_res(int x8, int y8, const uint8_t r[3]) {
+    const int bx4 = x8 * 2, by4 = y8 * 2;
+    for (int p = 0; p < 3; ++p) {
+      const int u = (p == 0 || sub == 0) ? 2 : 1;
+      const int cx = (p == 0 || sub == 0) ? bx4 : bx4 / 2, cy = (p == 0 || sub == 0) ? by4 : by4 / 2;
+      for (int k = 0; k < u; ++k) {
+        a_coef[p][cx + k] = r[p];
+        l_coef[p][cy + k] = r[p];
+      }
+    }
+  }
+
+  // code_split (src/coder/superblock.rs:950-990) always taking SPLIT, down to
+  // 8x8 PARTITION_NONE leaves.
+  template <class F>
+  void node(int bl, int x8, int y8, int sz8, int* cdef_point, F&& leaf) {
+    if (sz8 == 1) {
+      tok(L.part_bl8 + part_ctx(4, x8, y8), 0);
+      leaf(x8, y8);
+      a_part[x8] = 0x1E;
+      l_part[y8] = 0x1E;
+      return;
+    }
+    const int hh = sz8 / 2;
+    const bool have_h = (x8 + hh) * 8 < w8, have_v = (y8 + hh) * 8 < h8;
+    const int32_t slot = L.part_split + (bl - 1) * 4 + part_ctx(bl, x8, y8);
+    if (have_h && have_v)
+      tok(slot, 3);
+    else if (have_h)
+      out->push_back((2u << 30) | ((uint32_t)slot << 2) | (1u << 1) | 1u);  // gathered: split, top
+    else if (have_v)
+      out->push_back((2u << 30) | ((uint32_t)slot << 2) | (1u << 1) | 0u);  // gathered: split, left
+    const int cx[4] = {x8, x8 + hh, x8, x8 + hh}, cy[4] = {y8, y8, y8 + hh, y8 + hh};
+    for (int c = 0; c < 4; ++c)
+      if (cx[c] * 8 < w8 && cy[c] * 8 < h8) node(bl + 1, cx[c], cy[c], hh, cdef_point, leaf);
+  }
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { cudaFree(p); }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+  bool alloc(size_t n) { return cudaMalloc(&p, n ? n : 1) == cudaSuccess; }
+};
+
+}  // namespace
+
+extern "C" {
+
+int mt_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
+const uint8_t* mt_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h);
+int mt_emit_coeffs_device(const int32_t* d_levels, const mt_coef_block* d_blocks, int32_t n, uint32_t* d_counts,
+                          uint32_t* d_offsets, uint32_t* d_tokens, uint8_t* d_res_ctx, void* stream);
+
+// The encode from the input planes: rgb (interleaved, converted by the Q13
+// colour conversion) or yuv (three 8-bit planes at their displayed sizes).
+static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t width, uint32_t height,
+                       const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
+  if (!out || !out_len) return MT_ERR_INVALID_INPUT;
+  *out = nullptr;
+  *out_len = 0;
+  int rc = mt_encode_config_validate(cfg);
+  if (rc != MT_OK) return rc;
+  rc = mt_validate_rgb8_input(width, height, (size_t)width * height * 3);
+  if (rc != MT_OK) return rc;
+  if (!rgb && (!yuv || !yuv[0] || !yuv[1] || !yuv[2])) return MT_ERR_INVALID_INPUT;
+  if (cfg->chroma != MT_CHROMA_420 && cfg->chroma != MT_CHROMA_444) return MT_ERR_UNSUPPORTED_CHROMA_FORMAT;
+  mt_encode_plan plan;
+  if ((rc = mt_encode_config_effective(cfg, &plan)) != MT_OK) return rc;
+  if (plan.base_q_idx == 0) return MT_ERR_UNSUPPORTED;  // lossless is a separate encoder
+  const int sub = cfg->chroma == MT_CHROMA_420 ? 2 : 0;
+  const int sx = sub ? 1 : 0;
+  int32_t pw, ph, pcw, pch;
+  if ((rc = mt_padded_plane_dims((int)width, (int)height, sub, &pw, &ph, &pcw, &pch)) != MT_OK) return rc;
+  const int nbx = pw / 8, nby = ph / 8, nb = nbx * nby;
+  const int sb_cols = (pw + 63) / 64, sb_rows = (ph + 63) / 64;
+  const int cl = sub ? 16 : 64;  // chroma levels per block
+  // quantisers, QM rows, default CDF slices and their bit costs, lambdas
+  mt_quant qy, qc;
+  if (mt_quant_init(plan.base_q_idx, 8, plan.qm_y, &qy) != MT_OK) return MT_ERR_INVALID_INPUT;
+  if (mt_quant_init_chroma(plan.base_q_idx, 0, 0, 8, plan.qm_u, &qc) != MT_OK) return MT_ERR_INVALID_INPUT;
+  mt_coef_cdfs cdy, cdc;
+  mt_coef_costs cy, cc;
+  const int qctx = mt_qcat(plan.base_q_idx);
+  mt_coef_cdfs_default(qctx, 8, 8, 0, &cdy);
+  mt_coef_cdfs_default(qctx, sub ? 4 : 8, sub ? 4 : 8, 1, &cdc);
+  mt_coef_costs_build(&cdy, &cy);
+  mt_coef_costs_build(&cdc, &cc);
+  mt_rd_lambdas lam;
+  if (mt_rd_lambdas_init(plan.base_q_idx, qy.dc_q, sub, 8, &lam) != MT_OK) return MT_ERR_INVALID_INPUT;
+  const uint8_t* qmy = mt_qm_row(plan.qm_y, 0, 8, 8);
+  const uint8_t* qmc = mt_qm_row(plan.qm_u, 1, sub ? 4 : 8, sub ? 4 : 8);
+  // device buffers
+  const size_t ny = (size_t)pw * ph, nc = (size_t)pcw * pch;
+  DevBuf d_rgb, d_pl, d_tab, d_dec, d_lv, d_emit, d_maps, d_skip8;
+  const size_t in_bytes = rgb ? (size_t)width * height * 3
+                              : (size_t)width * height + 2 * (size_t)((width + sx) >> sx) * ((height + sx) >> sx);
+  if (!d_rgb.alloc(in_bytes) || !d_pl.alloc((ny + 2 * nc) * 2 * 2) ||
+      !d_tab.alloc(2 * sizeof(mt_coef_costs) + 128) || !d_dec.alloc((size_t)nb * 2) ||
+      !d_lv.alloc((size_t)nb * (64 + 2 * cl) * 4))
+    return MT_ERR_DEVICE;
+  uint16_t* src[3] = {d_pl.as<uint16_t>(), d_pl.as<uint16_t>() + ny, d_pl.as<uint16_t>() + ny + nc};
+  uint16_t* rec[3] = {src[2] + nc, src[2] + nc + ny, src[2] + nc + ny + nc};
+  mt_coef_costs* d_cy = d_tab.as<mt_coef_costs>();
+  mt_coef_costs* d_cc = d_cy + 1;
+  uint8_t* d_qmy = reinterpret_cast<uint8_t*>(d_cc + 1);
+  uint8_t* d_qmc = d_qmy + 64;
+  cudaStream_t st = nullptr;
+  if (rgb) {
+    if (cudaMemcpy(d_rgb.p, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+    if ((rc = mt_csc_rgb8_device(d_rgb.as<uint8_t>(), (int)width, (int)height, sub, src[0], src[1], src[2], st)) !=
+        MT_OK)
+      return rc;
+  } else {
+    const int cw = (int)((width + sx) >> sx), ch = (int)((height + sx) >> sx);
+    uint8_t* d_in = d_rgb.as<uint8_t>();
+    const size_t n0 = (size_t)width * height, n1 = (size_t)cw * ch;
+    if (cudaMemcpy(d_in, yuv[0], n0, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_in + n0, yuv[1], n1, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(d_in + n0 + n1, yuv[2], n1, cudaMemcpyHostToDevice) != cudaSuccess)
+      return MT_ERR_DEVICE;
+    pad_plane_kernel<<<dim3((pw + 127) / 128, ph), 128, 0, st>>>(d_in, (int)width, (int)height, src[0], pw, ph);
+    pad_plane_kernel<<<dim3((pcw + 127) / 128, pch), 128, 0, st>>>(d_in + n0, cw, ch, src[1], pcw, pch);
+    pad_plane_kernel<<<dim3((pcw + 127) / 128, pch), 128, 0, st>>>(d_in + n0 + n1, cw, ch, src[2], pcw, pch);
+  }
+  cudaMemsetAsync(d_tab.p, 32, 2 * sizeof(mt_coef_costs) + 128, st);  // flat QM weights past a 4x4 row
+  cudaMemcpyAsync(d_cy, &cy, sizeof(cy), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_cc, &cc, sizeof(cc), cudaMemcpyHostToDevice, st);
+  if (qmy) cudaMemcpyAsync(d_qmy, qmy, 64, cudaMemcpyHostToDevice, st);
+  if (qmc) cudaMemcpyAsync(d_qmc, qmc, sub ? 16 : 64, cudaMemcpyHostToDevice, st);
+  EncArgs a = {};
+  for (int p = 0; p < 3; ++p) {
+    a.src[p] = src[p];
+    a.rec[p] = rec[p];
+  }
+  a.py = {};
+  a.py.tx_size = 8;
+  a.py.bd = 8;
+  a.py.frame_w = pw;
+  a.py.frame_h = ph;
+  a.py.stride = pw;
+  a.py.trellis_lambda0 = lam.trellis_lambda0;
+  a.py.mode_lambda = lam.mode_lambda;
+  a.py.satd_scale = lam.satd_scale;
+  a.py.satd_bridge = lam.satd_bridge;
+  a.pc = a.py;
+  a.pc.tx_size = sub ? 4 : 8;
+  a.pc.frame_w = pcw;
+  a.pc.frame_h = pch;
+  a.pc.stride = pcw;
+  a.qy = qy;
+  a.qc = qc;
+  a.tly = mth::scaled_trellis_lambda_host((float)qy.dc_q, lam.trellis_lambda0);
+  a.tlc = mth::scaled_trellis_lambda_host((float)qc.dc_q, lam.trellis_lambda0);
+  a.has_qm_y = qmy != nullptr;
+  a.has_qm_c = qmc != nullptr;
+  a.sub = sub;
+  a.sb_cols = sb_cols;
+  a.w8 = pw;
+  a.h8 = ph;
+  a.mode = d_dec.as<uint8_t>();
+  a.tx = a.mode + nb;
+  a.lv_y = d_lv.as<int32_t>();
+  a.lv_u = a.lv_y + (size_t)nb * 64;
+  a.lv_v = a.lv_u + (size_t)nb * cl;
+  if (cudaMemsetAsync(a.mode, 0, (size_t)nb * 2, st) != cudaSuccess) return MT_ERR_DEVICE;
+  // the superblock wavefront
+  const int ndiag = 2 * (sb_rows - 1) + sb_cols;
+  for (int d = 0; d < ndiag; ++d) {
+    int n = 0;
+    for (int r = 0; r < sb_rows; ++r) {
+      const int c = d - 2 * r;
+      n += c >= 0 && c < sb_cols;
+    }
+    if (n) encode_sb_kernel<<<n, kEncThreads, 0, st>>>(a, d_cy, d_cc, d_qmy, d_qmc, d);
+  }
+  if (cudaGetLastError() != cudaSuccess) return MT_ERR_DEVICE;
+  std::vector<uint8_t> mode(nb), tx(nb);
+  if (cudaMemcpy(mode.data(), a.mode, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  if (cudaMemcpy(tx.data(), a.tx, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  // block syntax in coding order, with the coefficient blocks it carries
+  mt_cdf_slot_layout L;
+  mt_cdf_layout(&L);
+  std::vector<mt_coef_block> blocks;
+  blocks.reserve((size_t)nb * 3);
+  BlockSyntax bs{L, pw, ph, sub, nbx, mode.data(), tx.data()};
+  bs.a_part.assign(nbx, 0);
+  bs.l_part.assign(nby, 0);
+  bs.a_skip.assign(nbx * 2, 0);
+  bs.l_skip.assign(nby * 2, 0);
+  bs.a_mode.assign(nbx * 2, 0);
+  bs.l_mode.assign(nby * 2, 0);
+  bs.a_tx.assign(nbx * 2, -1);
+  bs.l_tx.assign(nby * 2, -1);
+  for (int p = 0; p < 3; ++p) {
+    bs.a_coef[p].assign(nbx * 2, 0x40);
+    bs.l_coef[p].assign(nby * 2, 0x40);
+  }
+  bs.blocks = &blocks;
+  // The coefficient contexts of a block depend on its neighbours' res_ctx
+  // bytes, which depend on their levels only: compute them on the host from
+  // the levels as the syntax walk reaches each block.
+  std::vector<int32_t> lv((size_t)nb * (64 + 2 * cl));
+  if (cudaMemcpy(lv.data(), a.lv_y, lv.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  auto res_ctx_of = [&](const int32_t* cf, int n, int cls) -> uint8_t {
+    static const uint8_t s4[16] = {0, 4, 1, 2, 5, 8, 12, 9, 6, 3, 7, 10, 13, 14, 11, 15};
+    int eob = -1;
+    auto at = [&](int i) -> int {
+      if (cls == 1) return ((i & (n - 1)) * n) + i / n;  // vertical class order
+      if (cls == 2) return i;
+      return n == 4 ? s4[i] : MT_SCAN_8X8[i];
+    };
+    for (int i = 0; i < n * n; ++i)
+      if (cf[at(i)]) eob = i;
+    if (eob < 0) return 0x40;
+    uint32_t cul = 0;
+    for (int i = 0; i <= eob; ++i) cul += (uint32_t)abs(cf[at(i)]);
+    const uint8_t dcb = cf[0] == 0 ? 0x40 : (cf[0] < 0 ? 0 : 0x80);
+    return (uint8_t)((cul < 63 ? cul : 63) | dcb);
+  };
+  std::vector<uint32_t> coef_off;  // per coefficient block: offset of its levels in lv
+  for (int sr = 0; sr < sb_rows; ++sr)
+    for (int sc = 0; sc < sb_cols; ++sc) {
+      bs.sbs.emplace_back();
+      bs.out = &bs.sbs.back();
+      int cp = -1;
+      bs.node(1, sc * 8, sr * 8, 8, &cp, [&](int x8, int y8) {
+        const size_t first = blocks.size();
+        bs.block8(x8, y8, &cp);
+        const int b = y8 * nbx + x8;
+        const uint32_t off[3] = {(uint32_t)((size_t)b * 64), (uint32_t)((size_t)nb * 64 + (size_t)b * cl),
+                                 (uint32_t)((size_t)nb * (64 + cl) + (size_t)b * cl)};
+        uint8_t r[3];
+        for (int p = 0; p < 3; ++p) {
+          blocks[first + p].cf_offset = off[p];
+          r[p] = res_ctx_of(&lv[off[p]], p == 0 || sub == 0 ? 8 : 4, blocks[first + p].tx_class);
+        }
+        bs.commit_res(x8, y8, r);
+      });
+      bs.cdef_points.push_back(cp);
+    }
+  // coefficient tokens of every block in one launch
+  const int ncb = (int)blocks.size();
+  if (!d_emit.alloc((size_t)ncb * (sizeof(mt_coef_block) + 8) + 8)) return MT_ERR_DEVICE;
+  mt_coef_block* d_blocks = d_emit.as<mt_coef_block>();
+  uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d_blocks + ncb);
+  uint32_t* d_off = d_cnt + ncb;
+  if (cudaMemcpy(d_blocks, blocks.data(), (size_t)ncb * sizeof(mt_coef_block), cudaMemcpyHostToDevice) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, nullptr, nullptr, st)) != MT_OK) return rc;
+  uint32_t total = 0;
+  if (cudaMemcpy(&total, d_off + ncb, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  DevBuf d_tok;
+  if (!d_tok.alloc((size_t)total * 4)) return MT_ERR_DEVICE;
+  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok.as<uint32_t>(), nullptr, st)) != MT_OK)
+    return rc;
+  std::vector<uint32_t> toks(total), offs((size_t)ncb + 1);
+  if (cudaMemcpy(toks.data(), d_tok.p, (size_t)total * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  if (cudaMemcpy(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  // splice the coefficient tokens into the superblock streams
+  std::vector<uint32_t> ops, sb_start(1, 0);
+  std::vector<int32_t> cdef_pt;
+  size_t k = 0;
+  for (size_t s = 0; s < bs.sbs.size(); ++s) {
+    const size_t base = ops.size();
+    int32_t cp_spliced = -1;
+    for (size_t i = 0; i < bs.sbs[s].size(); ++i) {
+      if ((int)i == bs.cdef_points[s]) cp_spliced = (int32_t)(ops.size() - base);
+      const uint32_t t = bs.sbs[s][i];
+      if (t == BlockSyntax::kCoef) {
+        ops.insert(ops.end(), toks.begin() + offs[k], toks.begin() + offs[k + 1]);
+        ++k;
+      } else {
+        ops.push_back(t);
+      }
+    }
+    sb_start.push_back((uint32_t)ops.size());
+    cdef_pt.push_back(cp_spliced);
+  }
+  // deblocking (uniform 8x8 blocks and transforms) and the CDEF decision
+  int32_t ly, luv, sharp;
+  mt_loop_filter_levels(plan.base_q_idx, sx, sx, &ly, &luv, &sharp);
+  const int n4 = (pw / 4) * (ph / 4);
+  std::vector<uint8_t> maps((size_t)n4 * 6);
+  for (int r = 0; r < ph / 4; ++r)
+    for (int c = 0; c < pw / 4; ++c) {
+      const size_t i = (size_t)r * (pw / 4) + c;
+      maps[i] = 2;
+      maps[n4 + i] = 2;
+      maps[2 * (size_t)n4 + i] = (c % 2) == 0;
+      maps[3 * (size_t)n4 + i] = (r % 2) == 0;
+      maps[4 * (size_t)n4 + i] = 2;
+      maps[5 * (size_t)n4 + i] = 2;
+    }
+  mt_deblock_frame_params g = {};
+  g.w8 = pw;
+  g.h8 = ph;
+  g.disp_w = (int)width;
+  g.disp_h = (int)height;
+  g.sub_x = g.sub_y = sx;
+  g.bd = 8;
+  DevBuf d_db;
+  const size_t dbs = mt_deblock_frame_scratch_bytes(&g);
+  if (!d_maps.alloc(maps.size()) || !d_db.alloc(dbs)) return MT_ERR_DEVICE;
+  if (cudaMemcpy(d_maps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+  // the recon planes are kept: the filters run on a copy
+  DevBuf d_flt;
+  if (!d_flt.alloc((ny + 2 * nc) * 2)) return MT_ERR_DEVICE;
+  uint16_t* flt[3] = {d_flt.as<uint16_t>(), d_flt.as<uint16_t>() + ny, d_flt.as<uint16_t>() + ny + nc};
+  if (cudaMemcpyAsync(flt[0], rec[0], (ny + 2 * nc) * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  const uint8_t* m0 = d_maps.as<uint8_t>();
+  if ((rc = mt_deblock_frame_device(flt[0], flt[1], flt[2], m0, m0 + n4, m0 + 2 * (size_t)n4, m0 + 3 * (size_t)n4,
+                                    m0 + 4 * (size_t)n4, m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db.p, st)) != MT_OK)
+    return rc;
+  mt_cdef_params cp = {};
+  cp.w8 = pw;
+  cp.h8 = ph;
+  cp.disp_w = (int)width;
+  cp.disp_h = (int)height;
+  cp.sub_x = cp.sub_y = sx;
+  cp.base_q_idx = plan.base_q_idx;
+  cp.bd = 8;
+  cp.slow = cfg->speed <= MT_SPEED_SLOW;
+  DevBuf d_cs;
+  const int unit_cols = (pw + 63) / 64, unit_rows = (ph + 63) / 64;
+  if (!d_skip8.alloc((size_t)nb) || !d_cs.alloc(mt_cdef_scratch_bytes(&cp))) return MT_ERR_DEVICE;
+  if (cudaMemsetAsync(d_skip8.p, 0, (size_t)nb, st) != cudaSuccess) return MT_ERR_DEVICE;
+  mt_cdef_decision dec = {};
+  std::vector<uint8_t> grid((size_t)unit_cols * unit_rows);
+  if (plan.cdef) {
+    if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8.as<uint8_t>(), &cp, d_cs.p,
+                                   &dec, grid.data(), st)) != MT_OK)
+      return rc;
+  } else {
+    dec.bits = -1;
+  }
+  if (recon_out) {  // the decoder's output: deblocked and CDEF-filtered
+    if (cudaMemcpy(recon_out[0], flt[0], ny * 2, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(recon_out[1], flt[1], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(recon_out[2], flt[2], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return MT_ERR_DEVICE;
+  }
+  // the tile: pack, then re-emit with each unit's cdef_idx
+  uint8_t* tile = nullptr;
+  size_t tile_len = 0;
+  mt_tile_trace* trace = nullptr;
+  if ((rc = mt_pack_tile(plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
+                         (int32_t)bs.sbs.size(), &tile, &tile_len, &trace)) != MT_OK)
+    return rc;
+  if (dec.bits > 0) {
+    free(tile);
+    rc = mt_replay_tile_with_filters(trace, 0, 0, pw, ph, grid.data(), unit_cols, (int32_t)grid.size(), dec.bits,
+                                     cfg->updating_cdf, &tile, &tile_len);
+  }
+  mt_tile_trace_free(trace);
+  if (rc != MT_OK) return rc;
+  // headers and container
+  mt_sequence_header_params sp = {};
+  sp.width = width;
+  sp.height = height;
+  sp.profile = sub ? 0 : 1;
+  sp.bit_depth = 8;
+  sp.color_present = cfg->color_present;
+  sp.primaries = cfg->primaries;
+  sp.transfer = cfg->transfer;
+  sp.matrix = cfg->matrix;
+  sp.full_range = cfg->full_range;
+  sp.chroma_sample_position = cfg->chroma_sample_position;
+  sp.ss_x = sp.ss_y = (uint32_t)sx;
+  sp.enable_filter_intra = sp.enable_intra_edge_filter = 1;
+  mt_frame_header_params fp = {};
+  fp.w8 = pw;
+  fp.h8 = ph;
+  fp.base_q_idx = plan.base_q_idx;
+  fp.qm_y = plan.qm_y;
+  fp.qm_u = fp.qm_v = plan.qm_u;
+  fp.updating_cdf = cfg->updating_cdf;
+  fp.lf_y = ly;
+  fp.lf_u = fp.lf_v = luv;
+  fp.lf_sharpness = sharp;
+  fp.cdef_bits = dec.bits;
+  fp.cdef_damping = dec.bits >= 0 ? dec.damping : 3;
+  for (int e = 0; e < dec.n_strengths && e < 8; ++e)
+    for (int q = 0; q < 4; ++q) fp.cdef_strengths[e][q] = dec.strengths[e][q];
+  const uint8_t* tiles[1] = {tile};
+  const size_t tl[1] = {tile_len};
+  uint8_t* obu = nullptr;
+  size_t obu_len = 0;
+  rc = mt_av1_stream(&sp, &fp, tiles, tl, 1, &obu, &obu_len);
+  free(tile);
+  if (rc != MT_OK) return rc;
+  mt_avif_item_params ip = {};
+  ip.width = width;
+  ip.height = height;
+  ip.bit_depth = 8;
+  ip.channels = 3;
+  ip.seq_profile = (uint8_t)sp.profile;
+  ip.seq_level_idx = mt_av1_level_for(width, height);
+  ip.chroma_sub_x = ip.chroma_sub_y = sx;
+  ip.color_present = cfg->color_present;
+  ip.primaries = (uint16_t)cfg->primaries;
+  ip.transfer = (uint16_t)cfg->transfer;
+  ip.matrix = (uint16_t)cfg->matrix;
+  ip.full_range = cfg->full_range;
+  ip.icc = cfg->icc;
+  ip.icc_len = cfg->icc_len;
+  ip.exif = cfg->exif;
+  ip.exif_len = cfg->exif_len;
+  ip.imir_axis = -1;
+  ip.clli_present = cfg->clli_present;
+  ip.max_content_light_level = cfg->max_content_light_level;
+  ip.max_pic_average_light_level = cfg->max_pic_average_light_level;
+  rc = mt_wrap_av1_image(obu, obu_len, &ip, out, out_len);
+  free(obu);
+  return rc;
+}
+
+int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
+                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
+  if (!rgb) return MT_ERR_INVALID_INPUT;
+  return encode_impl(rgb, nullptr, width, height, cfg, out, out_len, recon_out);
+}
+
+int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
+                   size_t* out_len) {
+  return mt_encode_rgb8_ex(rgb, width, height, cfg, out, out_len, nullptr);
+}
+
+int mt_encode_yuv8(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t width, uint32_t height,
+                   const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
+  const uint8_t* planes[3] = {y, u, v};
+  if (!y || !u || !v) return MT_ERR_INVALID_INPUT;
+  return encode_impl(nullptr, planes, width, height, cfg, out, out_len, recon_out);
+}
+
+}  // extern "C"

@@ -1,0 +1,51 @@
+"""encode_rgb8 over the C ABI (``mt_encode_rgb8``): an 8-bit RGB image in, AVIF
+bytes out, with ``EncodeConfig``'s fields (``abi.EncodeConfig``)."""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .abi import load, ptr
+from .entropy import _check, _take
+
+
+def config(**kw):
+    """EncodeConfig::default() with fields overridden by keyword."""
+    c = abi.EncodeConfig()
+    _check(load().mt_encode_config_default(C.byref(c)), "mt_encode_config_default")
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
+def _planes_out(w, h, sub):
+    pw, ph = (w + 7) & ~7, (h + 7) & ~7
+    pcw, pch = (pw >> 1, ph >> 1) if sub else (pw, ph)
+    return [np.zeros((ph, pw), np.uint16), np.zeros((pch, pcw), np.uint16), np.zeros((pch, pcw), np.uint16)]
+
+
+def encode_rgb8(rgb, cfg=None, want_recon=False):
+    """rgb: (h, w, 3) uint8.  Returns the AVIF bytes (and the decoder's output
+    planes, padded, when want_recon)."""
+    rgb = np.ascontiguousarray(rgb, np.uint8)
+    h, w = rgb.shape[:2]
+    cfg = cfg if cfg is not None else config()
+    out, n = C.c_void_p(), C.c_size_t()
+    planes = _planes_out(w, h, cfg.chroma == 0) if want_recon else None
+    arr = (C.c_void_p * 3)(*[p.ctypes.data for p in planes]) if want_recon else None
+    _check(load().mt_encode_rgb8_ex(ptr(rgb), w, h, C.byref(cfg), C.byref(out), C.byref(n), arr), "mt_encode_rgb8")
+    data = _take(out, n.value)
+    return (data, planes) if want_recon else data
+
+
+def encode_yuv8(y, u, v, cfg, want_recon=False):
+    """8-bit planes at their displayed sizes, coded as given (no colour conversion)."""
+    y, u, v = [np.ascontiguousarray(p, np.uint8) for p in (y, u, v)]
+    h, w = y.shape
+    out, n = C.c_void_p(), C.c_size_t()
+    planes = _planes_out(w, h, cfg.chroma == 0) if want_recon else None
+    arr = (C.c_void_p * 3)(*[p.ctypes.data for p in planes]) if want_recon else None
+    _check(load().mt_encode_yuv8(ptr(y), ptr(u), ptr(v), w, h, C.byref(cfg), C.byref(out), C.byref(n), arr),
+           "mt_encode_yuv8")
+    data = _take(out, n.value)
+    return (data, planes) if want_recon else data

@@ -57,17 +57,19 @@ SCAN8 = [0, 8, 1, 2, 9, 16, 24, 17, 10, 3, 4, 11, 18, 25, 32, 40, 33, 26, 19, 12
 
 
 class Coder:
-    def __init__(self, mt, po, rgb, qidx, qm_level, gpu, seed=0, filters=False, pick="random"):
+    def __init__(self, mt, po, rgb, qidx, qm_level, gpu, seed=0, filters=False, pick="random", qm_uv=None):
         self.mt, self.po, self.gpu, self.filters, self.pick = mt, po, gpu, filters, pick
+        self.qm_uv = qm_level if qm_uv is None else qm_uv
         self.h, self.w = rgb.shape[:2]
         assert self.w % 64 == 0 and self.h % 64 == 0
         # identity matrix: Y = G, U = B, V = R
         self.src = [rgb[..., 1].astype(np.uint16), rgb[..., 2].astype(np.uint16), rgb[..., 0].astype(np.uint16)]
         self.rec = [np.zeros((self.h, self.w), np.uint16) for _ in range(3)]
         self.qidx, self.qm_level = qidx, qm_level
-        self.q = [mt.quant_new(qidx, 8, qm_level)] + [mt.quant_new_chroma(qidx, 0, 0, 8, qm_level)] * 2
+        self.q = [mt.quant_new(qidx, 8, qm_level)] + [mt.quant_new_chroma(qidx, 0, 0, 8, self.qm_uv)] * 2
         self.qm = mt.qm_row(qm_level, 0, 8) if qm_level < 15 else None
-        self.qmc = mt.qm_row(qm_level, 1, 8) if qm_level < 15 else None
+        self.qmc = mt.qm_row(self.qm_uv, 1, 8) if (qm_level < 15 or self.qm_uv < 15) else None
+        self.lam = mt.rd_lambdas(qidx, self.q[0].dc_q, 0)
         self.costs = mt.coef_costs(mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 0))
         self.cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 0)
         self.rng = np.random.default_rng(seed)
@@ -105,7 +107,9 @@ class Coder:
         return lv[0]
 
     def best(self, px, py, flags):
-        prm = self.mt.chain_params(self.w, self.h, tx_size=8, mode_lambda=20.0, satd_bridge=0.7)
+        lam = self.lam
+        prm = self.mt.chain_params(self.w, self.h, tx_size=8, trellis_lambda0=lam.trellis_lambda0,
+                                   mode_lambda=lam.mode_lambda, satd_scale=lam.satd_scale, satd_bridge=lam.satd_bridge)
         cands = np.zeros(13 * 7, abi.CANDIDATE_DTYPE)
         cands["px"], cands["py"], cands["flags"] = px, py, flags
         cands["mode"] = np.repeat(np.arange(13), 7)
@@ -201,7 +205,7 @@ class Coder:
             streams.append(np.array(s, np.uint32))
         fp = ct.FrameHeaderParams()
         fp.w8, fp.h8, fp.base_q_idx = self.w, self.h, self.qidx
-        fp.qm_y = fp.qm_u = fp.qm_v = self.qm_level
+        fp.qm_y, fp.qm_u, fp.qm_v = self.qm_level, self.qm_uv, self.qm_uv
         fp.updating_cdf = 1
         fp.cdef_bits, fp.cdef_damping = -1, 3
         self.out = [p.copy() for p in self.rec]
