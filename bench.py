@@ -477,6 +477,42 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     return out
 
 
+def measure_encode(wl, reps=3):
+    """The whole-file encode of the same 1080p 4:2:0 quality-60 frame through
+    mt_encode_rgb8 (host RGB in, AVIF bytes out; colour conversion, the 8x8
+    decision wavefront, token emission, packing, filters and container inside
+    the timed call).  Its decisions are the library's own 8x8 search, not the
+    reference's decode_sb, so the bytes are not the reference's; the file is a
+    valid AVIF that AV1 decoders reproduce exactly (tests/test_encode.py)."""
+    import io
+
+    from maroontree_b200 import encoder as enc
+
+    rgb = wl["rgb"]
+    cfg = enc.config(quality=QUALITY)
+    avif = enc.encode_rgb8(rgb, cfg)  # warm-up (module load, first allocations)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        avif = enc.encode_rgb8(rgb, cfg)
+        times.append(time.perf_counter() - t0)
+    step = float(np.median(times))
+    out = {"ms": round(step * 1e3, 2), "mpix_s": round(MPIX / step, 3), "bytes": len(avif),
+           "workload": "mt_encode_rgb8 1920x1080 4:2:0 quality 60: 8x8 blocks, 13 modes x 7 types per luma block",
+           "decisions": "the library's 8x8 search (not the reference's decode_sb)"}
+    try:
+        from PIL import Image
+
+        im = Image.open(io.BytesIO(avif))
+        im.load()
+        dec = np.asarray(im.convert("RGB")).astype(np.float64)
+        mse = float(np.mean((dec - rgb.astype(np.float64)) ** 2))
+        out["psnr_rgb_db"] = round(10 * np.log10(255.0 ** 2 / mse), 3)
+    except Exception as e:  # decoding is a check, not part of the measurement
+        out["decode_error"] = str(e)[:200]
+    return out
+
+
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -731,6 +767,7 @@ def run_ours(args):
     alg_bytes = n * (32 + 128 + 66) + nb * 60
 
     filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
+    encode = measure_encode(wl) if rank == 0 else None
     level4 = measure_small_level(dev, wl, 4, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
     level16 = measure_small_level(dev, wl, 16, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
     split16 = {k: measure_split16(dev, wl, k == "search", cpu=world == 1 and not args.no_cpu)
@@ -775,6 +812,7 @@ def run_ours(args):
                                    f"({clk_mhz:.0f} MHz); no measured integer peak exists"},
         "parity": parity,
         "frame_filters": filters,
+        "encode": encode,
         "level4": level4,
         "level16": level16,
         "split16": split16,
