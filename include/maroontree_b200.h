@@ -17,6 +17,7 @@
  *                                         Cdfs::new (the coefficient slices)
  *   mt_range_encoder_* / mt_cdfs_default  src/odec.rs:35-615 OdEcEncoder, src/coder/cdfs.rs:193-629
  *   mt_pack_tile                          src/coder/wavefront.rs:617-657 pack_wavefront_tile
+ *   mt_pack_tile_filtered                 the same, with replay_tile_with_filters folded in
  *   mt_emit_coeffs[_device] / mt_cdf_layout  src/coeffs.rs:34-2520 the square coefficient coders
  *   mt_replay_tile_with_filters           src/coder/tile_encode.rs:404-466 replay_tile_with_filters
  *   mt_sequence_header / mt_frame_header  src/obu.rs:46-771 sequence / frame headers, OBU framing
@@ -1014,6 +1015,16 @@ void mt_tile_trace_free(mt_tile_trace* t);
 int mt_replay_tile_with_filters(const mt_tile_trace* t, int32_t tile_x0, int32_t tile_y0, int32_t tile_w,
                                 int32_t tile_h, const uint8_t* cdef_grid, int32_t unit_cols, int32_t grid_len,
                                 int32_t cdef_bits, int32_t updating_cdf, uint8_t** out, size_t* out_len);
+/* mt_pack_tile followed by mt_replay_tile_with_filters in one pass, for a
+ * caller that knows each superblock's cdef_idx before packing (the frame's
+ * filters already decided): superblock i's sb_cdef_idx[i] (< 2^cdef_bits) is
+ * coded as a raw literal at its read_cdef() point, the symbol sequence
+ * replay_tile_with_filters would produce over a tile whose 64x64 units are
+ * its superblocks (same bytes), with no trace kept.  cdef_bits 0 packs as
+ * mt_pack_tile does. */
+int mt_pack_tile_filtered(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, const uint32_t* sb_start,
+                          const int32_t* sb_cdef_point, int32_t nsb, const uint8_t* sb_cdef_idx, int32_t cdef_bits,
+                          uint8_t** payload, size_t* payload_len);
 /* Frees a buffer this library returned. */
 void mt_free(void* p);
 

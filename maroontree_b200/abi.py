@@ -276,6 +276,8 @@ def _bind(lib):
                                       C.POINTER(C.c_int32)]),
         "mt_pack_tile": (C.c_int, [C.c_uint8, C.c_int32, _P, _P, _P, C.c_int32, C.POINTER(_P),
                                    C.POINTER(C.c_size_t), C.POINTER(_P)]),
+        "mt_pack_tile_filtered": (C.c_int, [C.c_uint8, C.c_int32, _P, _P, _P, C.c_int32, _P, C.c_int32,
+                                            C.POINTER(_P), C.POINTER(C.c_size_t)]),
         "mt_tile_trace_free": (None, [_P]),
         "mt_replay_tile_with_filters": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
                                                   C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P),
@@ -425,7 +427,7 @@ EXPORTED_SYMBOLS = (
     "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
     "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default", "mt_cdf_layout",
     "mt_emit_coeffs_device", "mt_emit_coeffs", "mt_encode_rgb8", "mt_encode_rgb8_ex", "mt_encode_yuv8",
-    "mt_pack_tile", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
+    "mt_pack_tile", "mt_pack_tile_filtered", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
     "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
     "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image",
     "mt_encode_config_default", "mt_encode_config_validate", "mt_validate_rgb8_input", "mt_encode_config_effective", "mt_quality_to_q", "mt_qm_levels",

@@ -256,20 +256,21 @@ struct Work4 {
 static_assert(kWork4Words >= 57, "4x4 arena too small");
 
 // Evaluate one 4x4 candidate; leaves the final levels in w.cf(), the
-// prediction in w.pred() and the inverse residual in w.rr().
-template <bool VIS>
-__device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
-                                           const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
-                                           const uint8_t* qm, const float* qs, const float* lut,
-                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
-                                           Work4& w) {
+// prediction in w.pred() and the inverse residual in w.rr().  The
+// neighbouring reconstruction is read through `rd` (chain4_one: the plane).
+template <bool VIS, typename R>
+__device__ __forceinline__ void chain4_one_rd(const uint16_t* __restrict__ src, const R& rd,
+                                              const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
+                                              const uint8_t* qm, const float* qs, const float* lut,
+                                              const mt_coef_costs& T, const mt_candidate& cd,
+                                              mt_candidate_result& r, Work4& w) {
   const int32_t maxv = (1 << p.bd) - 1;
   int16_t* pred = w.pred();
   int16_t* cf = w.cf();
   int16_t* rr = w.rr();
   float* tf = w.tf();
-  predict_sq<4>(rec, p.stride, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
-                (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, w.edges());
+  predict_sq_at<4>(rd, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
+                   (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, w.edges());
 #pragma unroll
   for (int y = 0; y < 4; y++)
 #pragma unroll
@@ -305,6 +306,15 @@ __device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, con
   r.satd = satd;
   r.eob = eob;
   r.reserved[0] = r.reserved[1] = r.reserved[2] = 0;
+}
+
+template <bool VIS>
+__device__ __forceinline__ void chain4_one(const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec,
+                                           const mt_chain_params& p, const mt_quant& q, float trellis_lambda,
+                                           const uint8_t* qm, const float* qs, const float* lut,
+                                           const mt_coef_costs& T, const mt_candidate& cd, mt_candidate_result& r,
+                                           Work4& w) {
+  chain4_one_rd<VIS>(src, PlaneRead{rec, p.stride}, p, q, trellis_lambda, qm, qs, lut, T, cd, r, w);
 }
 
 }  // namespace mtd

@@ -20,17 +20,20 @@
 // left, top and top-right neighbours), one launch per diagonal and one CTA
 // per superblock; inside a CTA the 8x8 blocks go in z-order, the 91 luma
 // candidates of a block one per thread, the CTA minimum picks the winner.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/maroontree_b200.h"
 #include "av1_tables.h"
 #include "chain4.cuh"
 #include "chain8.cuh"
+#include "coop8.cuh"
 
 namespace mth {
 float scaled_trellis_lambda_host(float dc_q, float lambda0);
@@ -38,7 +41,8 @@ float scaled_trellis_lambda_host(float dc_q, float lambda0);
 
 namespace {
 
-constexpr int kEncThreads = 128;
+namespace cg = cooperative_groups;
+
 constexpr int kCands = 13 * 7;
 __constant__ uint8_t kEncTypes[7] = {MT_TX_IDTX,      MT_TX_DCT_DCT,   MT_TX_V_DCT,  MT_TX_H_DCT,
                                      MT_TX_ADST_ADST, MT_TX_ADST_DCT, MT_TX_DCT_ADST};
@@ -64,7 +68,7 @@ struct EncArgs {
 // intra-edge flags down the quadtree (src/coder/superblock.rs:958-987: root
 // (top-right 1, bottom-left 0); children TL (1, 1), TR (parent's, 0),
 // BL (1, parent's), BR (0, 0)).
-__device__ __forceinline__ void zorder(int k, int* bx, int* by, bool* thr, bool* lhb) {
+__host__ __device__ inline void zorder(int k, int* bx, int* by, bool* thr, bool* lhb) {
   int x = 0, y = 0;
   bool t = true, l = false;
   for (int lvl = 2; lvl >= 0; --lvl) {
@@ -92,134 +96,280 @@ __device__ __forceinline__ void zorder(int k, int* bx, int* by, bool* thr, bool*
   *lhb = l;
 }
 
-// Coefficient bit costs, QM weights and their forward scales into shared
-// memory (n QM entries: 64 for an 8x8 transform, 16 for a 4x4 one).
-__device__ __forceinline__ void enc_stage(const mt_coef_costs* __restrict__ costs, const uint8_t* __restrict__ qm_row,
-                                          int nqm, int has_qm, mt_coef_costs& sC, uint8_t* sQm, float* sQs, float* sLut) {
-  const float* g = reinterpret_cast<const float*>(costs);
-  float* s = reinterpret_cast<float*>(&sC);
-  for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
-  if (threadIdx.x < 64) {
-    const int w = (has_qm && (int)threadIdx.x < nqm) ? qm_row[threadIdx.x] : 32;
-    sQm[threadIdx.x] = (uint8_t)w;
-    sQs[threadIdx.x] = mtd::fwd_qm_scale(w);
-    sLut[threadIdx.x] = mtd::kCoefRateLut[threadIdx.x];
-  }
-  __syncthreads();
-}
-
 __device__ __forceinline__ bool is_smooth(int m) { return m == MT_SMOOTH_PRED || m == MT_SMOOTH_V_PRED || m == MT_SMOOTH_H_PRED; }
 
-__global__ void __launch_bounds__(kEncThreads) encode_sb_kernel(EncArgs a, const mt_coef_costs* __restrict__ costs_y,
-                                                                 const mt_coef_costs* __restrict__ costs_c,
-                                                                 const uint8_t* __restrict__ qm_y,
-                                                                 const uint8_t* __restrict__ qm_c, int d) {
-  __shared__ mt_coef_costs sCy;
-  __shared__ mt_coef_costs sCc;
-  __shared__ uint8_t sQmY[64], sQmC[64];
-  __shared__ float sQsY[64], sQsC[64], sLut[64];
-  __shared__ unsigned long long sBest;
-  enc_stage(costs_y, qm_y, 64, a.has_qm_y, sCy, sQmY, sQsY, sLut);
-  enc_stage(costs_c, qm_c, a.sub ? 16 : 64, a.has_qm_c, sCc, sQmC, sQsC, sLut);
-  // the b-th superblock on diagonal d = 2 * row + col
-  const int sb_rows = (a.h8 + 63) / 64;
-  int row = 0, col = 0, found = 0;
-  for (int r = 0, seen = 0; r < sb_rows; ++r) {
-    const int c = d - 2 * r;
-    if (c < 0 || c >= a.sb_cols) continue;
-    if (seen++ == (int)blockIdx.x) {
-      row = r;
-      col = c;
-      found = 1;
-      break;
+// The 91 candidates of a block are split over a cluster of kClusterCtas CTAs
+// (on as many SMs): CTA r takes candidate indices [23r, 23r + 23) (index =
+// mode * 7 + type, the order ties are broken in) and runs them type by type,
+// so the four octets of a warp mostly share a transform path.
+constexpr int kClusterCtas = 4;
+constexpr int kCandPerCta = 23;
+constexpr int kLumaThreads = 192;  // 23 octets, rounded up to whole warps
+constexpr int kStepThreads = kLumaThreads + 32;
+
+struct CandOrder {
+  int8_t t[kClusterCtas][kLumaThreads / 8];  // candidate index per octet, -1 none
+};
+constexpr CandOrder make_order() {
+  CandOrder o{};
+  for (int r = 0; r < kClusterCtas; ++r) {
+    const int lo = r * kCandPerCta, hi = lo + kCandPerCta < kCands ? lo + kCandPerCta : kCands;
+    int k = 0;
+    for (int ti = 0; ti < 7; ++ti)
+      for (int m = 0; m < 13; ++m)
+        if (m * 7 + ti >= lo && m * 7 + ti < hi) o.t[r][k++] = (int8_t)(m * 7 + ti);
+    for (; k < kLumaThreads / 8; ++k) o.t[r][k] = -1;
+  }
+  return o;
+}
+__constant__ CandOrder kOrder = make_order();
+
+// Everything one CTA keeps in shared memory.
+struct StepShared {
+  mt_coef_costs cy, cc;
+  float qsY[64], qsC[64], lut[64];
+  uint8_t qmY[64], qmC[64];
+  mtd::CoopTabs tabs;
+  int16_t pred[4][64];              // the predictions of this CTA's four modes (angle delta 0)
+  int16_t cpred[64];                // the chroma DC prediction (4:4:4)
+  uint16_t src[64], csrc[64];       // the block's luma and chroma source samples
+  int16_t above[2][17], left[2][16];  // the block's luma / chroma neighbours (mtd::EdgeRead)
+  unsigned long long best;
+  uint32_t ticket, abort;
+  mtd::Oct8 oct[kLumaThreads / 8 + 1];  // one per candidate octet, then the chroma plane's
+};
+
+__device__ __forceinline__ void luma_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kLumaThreads) : "memory"); }
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Writes of a winning 8x8 chain: levels, and prediction + inverse residual
+// into the reconstruction plane (lane j: row j, and levels [8j, 8j+8)).
+__device__ __forceinline__ void put8(const mtd::Oct8& o, const int16_t* pred, int32_t* lv, uint16_t* rec, int stride,
+                                     int px, int py, int j) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) lv[j * 8 + i] = o.cf[j * 8 + i];
+#pragma unroll
+  for (int x = 0; x < 8; ++x)
+    rec[(size_t)(py + j) * stride + px + x] = (uint16_t)min(max((int)pred[j * 8 + x] + o.rr[j * 8 + x], 0), 255);
+}
+
+// A block's neighbours (above run of 17 from (ox - 1, oy - 1), left run of 16
+// from (ox - 1, oy)) into shared memory for lanes k in [0, 33), read past L1
+// (they were written by other SMs); positions outside the plane are clamped
+// (never read by the predictor).
+__device__ __forceinline__ void stage_edges(const uint16_t* rec, int stride, int fw, int fh, int ox, int oy,
+                                            int16_t* above, int16_t* left, int k) {
+  if (k < 17) {
+    if (oy > 0) above[k] = (int16_t)__ldcg(rec + (size_t)(oy - 1) * stride + min(max(ox - 1 + k, 0), fw - 1));
+  } else if (k < 33) {
+    if (ox > 0) left[k - 17] = (int16_t)__ldcg(rec + (size_t)min(oy + k - 17, fh - 1) * stride + ox - 1);
+  }
+}
+
+constexpr uint32_t kDonePerBlock = kClusterCtas;  // each CTA of the coding cluster publishes once
+constexpr int kMaxPolls = 1 << 20;               // a dependency wait gives up after this many polls
+
+// The 8x8 blocks of the frame in dependency order, coded by persistent
+// clusters (one block per cluster at a time).  A cluster takes the next block
+// from the ticket counter, waits until the block's left, top, top-left and,
+// where its intra edges use them, top-right and bottom-left neighbours are
+// published (done[] == kDonePerBlock), stages the neighbours and the source
+// block in shared memory, and evaluates the block: in each CTA the luma warps
+// run its share of the 91 candidates (the first four octets also build the
+// four predictions the share needs), the last warp codes a chroma plane in
+// CTAs 2 (U) and 3 (V).  The cluster's winner is the minimum of the CTAs'
+// keys (cost, candidate index), read through distributed shared memory; the
+// CTA holding it writes it out; then every CTA publishes.  Tickets follow the
+// dependency levels, so a block waits only on blocks that running clusters
+// took earlier.  A wait that runs out of polls sets *err; once *err is set
+// the remaining waits stop and every cluster leaves at its next ticket.
+// list[i] = block index | have-top-right (bit 30) | left-has-bottom (bit 31).
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThreads)
+    encode_blocks_kernel(EncArgs a, const uint32_t* __restrict__ list, int nlist, uint32_t* done,
+                         uint32_t* ticket_ctr, uint32_t* err, const mt_coef_costs* __restrict__ costs_y,
+                         const mt_coef_costs* __restrict__ costs_c, const uint8_t* __restrict__ qm_y,
+                         const uint8_t* __restrict__ qm_c) {
+  __shared__ StepShared S;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int t = threadIdx.x;
+  {
+    const float* gy = reinterpret_cast<const float*>(costs_y);
+    const float* gc = reinterpret_cast<const float*>(costs_c);
+    float* sy = reinterpret_cast<float*>(&S.cy);
+    float* sc = reinterpret_cast<float*>(&S.cc);
+    for (int i = t; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) {
+      sy[i] = gy[i];
+      sc[i] = gc[i];
+    }
+    if (t < 64) {
+      const int w = a.has_qm_y ? qm_y[t] : 32;
+      S.qmY[t] = (uint8_t)w;
+      S.qsY[t] = mtd::fwd_qm_scale(w);
+      S.lut[t] = mtd::kCoefRateLut[t];
+    } else if (t < 128) {
+      const int i = t - 64;
+      const int w = (a.has_qm_c && i < (a.sub ? 16 : 64)) ? qm_c[i] : 32;
+      S.qmC[i] = (uint8_t)w;
+      S.qsC[i] = mtd::fwd_qm_scale(w);
+    } else if (t < 192) {
+      S.tabs.load(t - 128, 64);
+    } else if (t == 192) {
+      S.best = ~0ull;
     }
   }
-  if (!found) return;
+  __syncthreads();
   const int nbx = a.w8 / 8;
-  int32_t store[mtd::kWork8Words];
-  mtd::Work8 w{store};
-  for (int k = 0; k < 64; ++k) {
-    int bx, by;
-    bool thr, lhb;
-    zorder(k, &bx, &by, &thr, &lhb);
-    const int px = col * 64 + bx * 8, py = row * 64 + by * 8;
-    if (px >= a.w8 || py >= a.h8) continue;  // uniform across the CTA
-    const int b = (py / 8) * nbx + px / 8;
+  const int mlo = rank * kCandPerCta / 7;  // first mode of this CTA's share
+  const int c = t - kLumaThreads;          // lane of the chroma warp
+  const int pl = rank - 2;                 // its plane (CTAs 2 and 3)
+  for (;;) {
+    if (rank == 0 && t == 0) {
+      S.ticket = atomicAdd(ticket_ctr, 1u);
+      S.abort = *(volatile uint32_t*)err;
+    }
+    cluster.sync();
+    const uint32_t tk = *cluster.map_shared_rank(&S.ticket, 0);
+    const uint32_t ab = *cluster.map_shared_rank(&S.abort, 0);
+    if (ab || tk >= (uint32_t)nlist) break;  // the same for every CTA of the cluster
+    const uint32_t e = list[tk];
+    const int b = (int)(e & 0x3fffffffu);
+    const int bx = b % nbx, by = b / nbx;
+    const int px = bx * 8, py = by * 8;
+    const bool thr = (e >> 30) & 1, lhb = (e >> 31) & 1;
     const bool have_tr = thr && py > 0 && px + 8 < a.w8;
     const bool have_bl = lhb && px > 0 && py + 8 < a.h8;
-    const bool ft = (py > 0 && is_smooth(a.mode[b - nbx])) || (px > 0 && is_smooth(a.mode[b - 1]));
     const uint8_t flags = (have_tr ? 1 : 0) | (have_bl ? 2 : 0);
-    if (threadIdx.x == 0) sBest = ~0ull;
-    __syncthreads();
-    const int t = threadIdx.x;
-    mt_candidate cd = {};
-    cd.px = (uint16_t)px;
-    cd.py = (uint16_t)py;
-    cd.flags = flags | (ft ? 4 : 0);
-    if (t < kCands) {
-      cd.mode = (uint8_t)(t / 7);
-      cd.tx_type = kEncTypes[t % 7];
-      mt_candidate_result r;
-      mtd::chain8_predict(a.rec[0], a.py, cd, w);
-      mtd::chain8_tx<false>(a.src[0], a.py, a.qy, a.tly, a.has_qm_y ? sQmY : nullptr, sQsY, sLut, sCy, cd, r, w);
-      const unsigned long long key = ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)t;
-      atomicMin(&sBest, key);
-    }
-    __syncthreads();
-    const int win = (int)(sBest & 0xffffffffu);
-    if (t == win) {  // the winner still holds its levels, prediction and inverse residual
-      const int16_t* cf = w.cf();
-      const int16_t* pr = w.pred();
-      const int16_t* rr = w.rr();
-      for (int i = 0; i < 64; ++i) a.lv_y[(size_t)b * 64 + i] = cf[i];
-      for (int y = 0; y < 8; ++y)
-        for (int x = 0; x < 8; ++x)
-          a.rec[0][(size_t)(py + y) * a.py.stride + px + x] =
-              (uint16_t)min(max((int)pr[y * 8 + x] + rr[y * 8 + x], 0), 255);
-      a.mode[b] = cd.mode;
-      a.tx[b] = cd.tx_type;
-    }
-    // chroma: UV_DC_PRED, DCT_DCT, one thread per plane
-    if (t < 2) {
-      mt_candidate cc = {};
-      cc.mode = MT_DC_PRED;
-      cc.tx_type = MT_TX_DCT_DCT;
-      mt_candidate_result r;
-      int32_t* lv = t == 0 ? a.lv_u : a.lv_v;
-      if (a.sub == 0) {
-        cc.px = (uint16_t)px;
-        cc.py = (uint16_t)py;
-        cc.flags = flags;
-        mtd::chain8_predict(a.rec[1 + t], a.pc, cc, w);
-        mtd::chain8_tx<false>(a.src[1 + t], a.pc, a.qc, a.tlc, a.has_qm_c ? sQmC : nullptr, sQsC, sLut, sCc, cc, r,
-                              w);
-        const int16_t* cf = w.cf();
-        const int16_t* pr = w.pred();
-        const int16_t* rr = w.rr();
-        for (int i = 0; i < 64; ++i) lv[(size_t)b * 64 + i] = cf[i];
-        for (int y = 0; y < 8; ++y)
-          for (int x = 0; x < 8; ++x)
-            a.rec[1 + t][(size_t)(py + y) * a.pc.stride + px + x] =
-                (uint16_t)min(max((int)pr[y * 8 + x] + rr[y * 8 + x], 0), 255);
-      } else {
-        cc.px = (uint16_t)(px / 2);
-        cc.py = (uint16_t)(py / 2);
-        int32_t st4[mtd::kWork4Words];
-        mtd::Work4 w4{st4};
-        mtd::chain4_one<false>(a.src[1 + t], a.rec[1 + t], a.pc, a.qc, a.tlc, a.has_qm_c ? sQmC : nullptr, sQsC,
-                               sLut, sCc, cc, r, w4);
-        const int16_t* cf = w4.cf();
-        const int16_t* pr = w4.pred();
-        const int16_t* rr = w4.rr();
-        for (int i = 0; i < 16; ++i) lv[(size_t)b * 16 + i] = cf[i];
-        for (int y = 0; y < 4; ++y)
-          for (int x = 0; x < 4; ++x)
-            a.rec[1 + t][(size_t)(cc.py + y) * a.pc.stride + cc.px + x] =
-                (uint16_t)min(max((int)pr[y * 4 + x] + rr[y * 4 + x], 0), 255);
+    if (t < 5) {  // one thread per dependency
+      int dep = -1;
+      if (t == 0 && bx > 0) dep = b - 1;
+      if (t == 1 && by > 0) dep = b - nbx;
+      if (t == 2 && bx > 0 && by > 0) dep = b - nbx - 1;
+      if (t == 3 && have_tr) dep = b - nbx + 1;
+      if (t == 4 && have_bl) dep = b + nbx - 1;
+      if (dep >= 0) {
+        int it = 0;
+        while (ld_acquire(done + dep) < kDonePerBlock) {
+          if (*(volatile uint32_t*)err) break;
+          if (++it > kMaxPolls) {
+            atomicExch(err, 1u);
+            break;
+          }
+          __nanosleep(64);
+        }
       }
     }
     __syncthreads();
+    // the block's neighbours and source samples
+    if (t < 33) {
+      stage_edges(a.rec[0], a.py.stride, a.w8, a.h8, px, py, S.above[0], S.left[0], t);
+    } else if (t >= 64 && t < 128) {
+      const int i = t - 64;
+      S.src[i] = a.src[0][(size_t)(py + (i >> 3)) * a.py.stride + px + (i & 7)];
+    } else if (rank >= 2 && c >= 0) {
+      const int cx = a.sub ? px / 2 : px, cy = a.sub ? py / 2 : py, n = a.sub ? 4 : 8;
+      stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, S.above[1], S.left[1], c);
+      if (c == 0)
+        stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, S.above[1], S.left[1], 32);
+      if (n == 8)
+        for (int i = c; i < 64; i += 32) S.csrc[i] = a.src[1 + pl][(size_t)(cy + i / 8) * a.pc.stride + cx + (i % 8)];
+    }
+    __syncthreads();
+    if (t < kLumaThreads) {
+      const mtd::Octet g;
+      const int o = t >> 3;
+      const bool ft = (py > 0 && is_smooth(__ldcg(a.mode + b - nbx))) || (px > 0 && is_smooth(__ldcg(a.mode + b - 1)));
+      mt_candidate cd = {};
+      cd.px = (uint16_t)px;
+      cd.py = (uint16_t)py;
+      cd.flags = flags | (ft ? 4 : 0);
+      const mtd::EdgeRead rd{S.above[0], S.left[0], px, py};
+      if (o < 4 && mlo + o < 13) {
+        int32_t scratch[3 * mtd::kEdgeCap8];
+        cd.mode = (uint8_t)(mlo + o);
+        mtd::coop8_predict_row(rd, a.py, cd, S.pred[o], scratch, g);
+      }
+      luma_bar();
+      const int ci = kOrder.t[rank][o];
+      if (ci >= 0) {
+        cd.mode = (uint8_t)(ci / 7);
+        cd.tx_type = kEncTypes[ci % 7];
+        mt_candidate_result r;
+        mtd::coop8_tx(S.src, 8, 0, 0, a.py, a.qy, a.tly, a.has_qm_y ? S.qmY : nullptr, S.qsY, S.lut, S.cy, cd,
+                      S.pred[cd.mode - mlo], r, S.oct[o], S.tabs, g);
+        if (g.j == 0) atomicMin(&S.best, ((unsigned long long)__float_as_uint(r.cost) << 32) | (unsigned)ci);
+      }
+    } else if (rank >= 2) {  // chroma: UV_DC_PRED with DCT_DCT, U in CTA 2, V in CTA 3
+      int32_t* lvc = pl == 0 ? a.lv_u : a.lv_v;
+      if (a.sub == 0 && c < 8) {
+        const mtd::Octet g;
+        mt_candidate cc = {};
+        cc.px = (uint16_t)px;
+        cc.py = (uint16_t)py;
+        cc.flags = flags;
+        cc.mode = MT_DC_PRED;
+        cc.tx_type = MT_TX_DCT_DCT;
+        int32_t scratch[3 * mtd::kEdgeCap8];
+        mtd::coop8_predict_row(mtd::EdgeRead{S.above[1], S.left[1], px, py}, a.pc, cc, S.cpred, scratch, g);
+        g.sync();
+        mt_candidate_result r;
+        mtd::Oct8& oc = S.oct[kLumaThreads / 8];
+        mtd::coop8_tx(S.csrc, 8, 0, 0, a.pc, a.qc, a.tlc, a.has_qm_c ? S.qmC : nullptr, S.qsC, S.lut, S.cc, cc,
+                      S.cpred, r, oc, S.tabs, g);
+        put8(oc, S.cpred, lvc + (size_t)b * 64, a.rec[1 + pl], a.pc.stride, px, py, g.j);
+      } else if (a.sub != 0 && c == 0) {
+        mt_candidate cc = {};
+        cc.mode = MT_DC_PRED;
+        cc.tx_type = MT_TX_DCT_DCT;
+        cc.px = (uint16_t)(px / 2);
+        cc.py = (uint16_t)(py / 2);
+        mt_candidate_result r;
+        int32_t st4[mtd::kWork4Words];
+        mtd::Work4 w4{st4};
+        mtd::chain4_one_rd<false>(a.src[1 + pl], mtd::EdgeRead{S.above[1], S.left[1], cc.px, cc.py}, a.pc, a.qc,
+                                  a.tlc, a.has_qm_c ? S.qmC : nullptr, S.qsC, S.lut, S.cc, cc, r, w4);
+        const int16_t* cf = w4.cf();
+        const int16_t* pr = w4.pred();
+        const int16_t* rr = w4.rr();
+        int32_t* lv = lvc + (size_t)b * 16;
+        for (int i = 0; i < 16; ++i) lv[i] = cf[i];
+        for (int y = 0; y < 4; ++y)
+          for (int x = 0; x < 4; ++x)
+            a.rec[1 + pl][(size_t)(cc.py + y) * a.pc.stride + cc.px + x] =
+                (uint16_t)min(max((int)pr[y * 4 + x] + rr[y * 4 + x], 0), 255);
+      }
+    }
+    cluster.sync();  // every CTA's key is final
+    unsigned long long w = ~0ull;
+    for (int q = 0; q < kClusterCtas; ++q) {
+      const unsigned long long k = *cluster.map_shared_rank(&S.best, q);
+      w = k < w ? k : w;
+    }
+    const int wi = (int)(w & 0xffffffffu);
+    if (t < kLumaThreads && rank == wi / kCandPerCta && kOrder.t[rank][t >> 3] == wi) {
+      const int j = t & 7;
+      put8(S.oct[t >> 3], S.pred[wi / 7 - mlo], a.lv_y + (size_t)b * 64, a.rec[0], a.py.stride, px, py, j);
+      if (j == 0) {
+        a.mode[b] = (uint8_t)(wi / 7);
+        a.tx[b] = kEncTypes[wi % 7];
+      }
+    }
+    __syncthreads();  // this CTA's writes of the block are issued
+    if (t == 0) {
+      __threadfence();
+      atomicAdd(done + b, 1u);
+    }
+    cluster.sync();  // every CTA has read the keys
+    if (t == 0) S.best = ~0ull;
   }
+  // The last ticket was read from CTA 0's shared memory by the other CTAs:
+  // none may leave while such a read can still be in flight.
+  cluster.sync();
 }
 
 // One plane of 8-bit samples into the coder's padded u16 plane, edge samples
@@ -475,16 +625,75 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   a.lv_u = a.lv_y + (size_t)nb * 64;
   a.lv_v = a.lv_u + (size_t)nb * cl;
   if (cudaMemsetAsync(a.mode, 0, (size_t)nb * 2, st) != cudaSuccess) return MT_ERR_DEVICE;
-  // the superblock wavefront
-  const int ndiag = 2 * (sb_rows - 1) + sb_cols;
-  for (int d = 0; d < ndiag; ++d) {
-    int n = 0;
-    for (int r = 0; r < sb_rows; ++r) {
-      const int c = d - 2 * r;
-      n += c >= 0 && c < sb_cols;
-    }
-    if (n) encode_sb_kernel<<<n, kEncThreads, 0, st>>>(a, d_cy, d_cc, d_qmy, d_qmc, d);
+  // Dependency levels of the 8x8 blocks: a block needs its left, top,
+  // top-left neighbours and, where the intra edge uses them, its top-right and
+  // bottom-left ones; blocks of one level run as one launch.
+  std::vector<uint32_t> sched;
+  std::vector<int> lstart;
+  {
+    std::vector<int32_t> T((size_t)nb, -1);
+    std::vector<uint32_t> entry((size_t)nb);
+    std::vector<int> cnt;
+    for (int sr = 0; sr < sb_rows; ++sr)
+      for (int sc = 0; sc < sb_cols; ++sc)
+        for (int k = 0; k < 64; ++k) {
+          int bx, by;
+          bool thr, lhb;
+          zorder(k, &bx, &by, &thr, &lhb);
+          const int x = sc * 8 + bx, y = sr * 8 + by;
+          if (x >= nbx || y >= nby) continue;
+          const bool tr = thr && y > 0 && (x + 1) * 8 < pw;
+          const bool bl = lhb && x > 0 && (y + 1) * 8 < ph;
+          int lv = 0;
+          auto dep = [&](int xx, int yy) { lv = std::max(lv, T[(size_t)yy * nbx + xx] + 1); };
+          if (x > 0) dep(x - 1, y);
+          if (y > 0) dep(x, y - 1);
+          if (x > 0 && y > 0) dep(x - 1, y - 1);
+          if (tr) dep(x + 1, y - 1);
+          if (bl) dep(x - 1, y + 1);
+          const size_t bi = (size_t)y * nbx + x;
+          T[bi] = lv;
+          entry[bi] = (uint32_t)bi | (thr ? 1u << 30 : 0u) | (lhb ? 1u << 31 : 0u);
+          if ((int)cnt.size() <= lv) cnt.resize(lv + 1, 0);
+          ++cnt[lv];
+        }
+    lstart.assign(cnt.size() + 1, 0);
+    for (size_t l = 0; l < cnt.size(); ++l) lstart[l + 1] = lstart[l] + cnt[l];
+    sched.resize((size_t)nb);
+    std::vector<int> fill(lstart.begin(), lstart.end() - 1);
+    for (int sr = 0; sr < sb_rows; ++sr)  // coding order inside a level
+      for (int sc = 0; sc < sb_cols; ++sc)
+        for (int k = 0; k < 64; ++k) {
+          int bx, by;
+          bool thr, lhb;
+          zorder(k, &bx, &by, &thr, &lhb);
+          const int x = sc * 8 + bx, y = sr * 8 + by;
+          if (x >= nbx || y >= nby) continue;
+          const size_t bi = (size_t)y * nbx + x;
+          sched[fill[T[bi]]++] = entry[bi];
+        }
   }
+  // the dependency-ordered block list, the per-block done counts, the ticket
+  // counter and the wait-timeout flag
+  int width_max = 1;
+  for (size_t l = 0; l + 1 < lstart.size(); ++l) width_max = std::max(width_max, lstart[l + 1] - lstart[l]);
+  DevBuf d_sched;
+  if (!d_sched.alloc(sched.size() * 4 + ((size_t)nb + 2) * 4)) return MT_ERR_DEVICE;
+  uint32_t* d_done = d_sched.as<uint32_t>() + sched.size();
+  uint32_t* d_ctl = d_done + nb;  // [0] ticket counter, [1] timeout flag
+  if (cudaMemcpyAsync(d_sched.p, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemsetAsync(d_done, 0, ((size_t)nb + 2) * 4, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  // one cluster per block that can run at once (the widest dependency level),
+  // at most 64 clusters (two CTAs per SM)
+  const int nclusters = std::min(width_max, 64);
+  encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, st>>>(a, d_sched.as<uint32_t>(), nb, d_done,
+                                                                           d_ctl, d_ctl + 1, d_cy, d_cc, d_qmy, d_qmc);
+  uint32_t timed_out = 0;
+  if (cudaMemcpyAsync(&timed_out, d_ctl + 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  if (timed_out) return MT_ERR_DEVICE;
   if (cudaGetLastError() != cudaSuccess) return MT_ERR_DEVICE;
   std::vector<uint8_t> mode(nb), tx(nb);
   if (cudaMemcpy(mode.data(), a.mode, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
@@ -652,20 +861,14 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
         cudaMemcpy(recon_out[2], flt[2], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
       return MT_ERR_DEVICE;
   }
-  // the tile: pack, then re-emit with each unit's cdef_idx
+  // the tile, in one pass with each superblock's cdef_idx at its read_cdef()
+  // point (the 64x64 CDEF units are the superblocks of the one tile)
   uint8_t* tile = nullptr;
   size_t tile_len = 0;
-  mt_tile_trace* trace = nullptr;
-  if ((rc = mt_pack_tile(plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
-                         (int32_t)bs.sbs.size(), &tile, &tile_len, &trace)) != MT_OK)
+  if ((rc = mt_pack_tile_filtered(plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
+                                  (int32_t)bs.sbs.size(), dec.bits > 0 ? grid.data() : nullptr,
+                                  dec.bits > 0 ? dec.bits : 0, &tile, &tile_len)) != MT_OK)
     return rc;
-  if (dec.bits > 0) {
-    free(tile);
-    rc = mt_replay_tile_with_filters(trace, 0, 0, pw, ph, grid.data(), unit_cols, (int32_t)grid.size(), dec.bits,
-                                     cfg->updating_cdf, &tile, &tile_len);
-  }
-  mt_tile_trace_free(trace);
-  if (rc != MT_OK) return rc;
   // headers and container
   mt_sequence_header_params sp = {};
   sp.width = width;

@@ -28,11 +28,7 @@ constexpr uint32_t kTagMask = 3u << kTagShift;
 constexpr uint32_t kTagBool = 1u << kTagShift;
 constexpr uint32_t kTagNoUpdate = 3u << kTagShift;
 
-int clz16(uint32_t r) {  // leading zeros of a 16-bit value (0..16)
-  int n = 0;
-  for (uint32_t b = 0x8000; b && !(r & b); b >>= 1) ++n;
-  return n;
-}
+inline int clz16(uint32_t r) { return r ? __builtin_clz(r) - 16 : 16; }  // leading zeros of a 16-bit value
 
 }  // namespace
 
@@ -101,11 +97,11 @@ struct mt_range_encoder {
     const uint32_t count = cdf[n - 1];
     const uint32_t rate = 3 + (uint32_t)((n >> 1) < 2 ? (n >> 1) : 2) + (count >> 4);
     cdf[n - 1] = (uint16_t)(count + 1 - (count >> 5));
+    // entries below val move up towards 32768, the others down towards 0
     for (int i = 0; i < n - 1; ++i) {
-      if (i >= val)
-        cdf[i] = (uint16_t)(cdf[i] - (cdf[i] >> rate));
-      else
-        cdf[i] = (uint16_t)(cdf[i] + ((32768u - cdf[i]) >> rate));
+      const uint32_t c = cdf[i];
+      const uint32_t up = c + ((32768u - c) >> rate), dn = c - (c >> rate);
+      cdf[i] = (uint16_t)(i < val ? up : dn);
     }
   }
 
@@ -390,31 +386,43 @@ uint16_t gather_split_prob(const uint16_t* cdf, bool top) {
 }
 
 // One superblock's semantic stream against the live CDF set
-// (src/odec.rs:315-360).  Returns false on a malformed token.
-bool replay_tokens(mt_range_encoder& enc, CdfSet& c, const uint32_t* ops, uint32_t n, int32_t cdef_point) {
+// (src/odec.rs:315-360).  At the read_cdef() point the trace is marked and,
+// when cdef_bits > 0, the unit's cdef_idx is coded there as a raw literal.
+// Returns false on a malformed token.
+bool replay_tokens(mt_range_encoder& enc, CdfSet& c, const uint32_t* ops, uint32_t n, int32_t cdef_point,
+                   int cdef_bits = 0, uint32_t cdef_idx = 0) {
   const size_t nslots = c.off.size();
+  uint16_t* const data = c.data.data();
+  const uint32_t* const off = c.off.data();
+  const uint16_t* const lens = c.len.data();
   for (uint32_t i = 0; i < n; ++i) {
-    if (cdef_point >= 0 && (uint32_t)cdef_point == i) enc.mark_cdef();
+    if (cdef_point >= 0 && (uint32_t)cdef_point == i) {
+      enc.mark_cdef();
+      if (cdef_bits > 0) enc.encode_literal(cdef_idx, (uint32_t)cdef_bits);
+    }
     const uint32_t t = ops[i];
     const uint32_t tag = t & kTagMask;
     if (tag == 0 || tag == kTagNoUpdate) {
       const uint32_t slot = (t >> 8) & 0xffff, s = t & 0xff;
-      if (slot >= nslots || s >= c.len[slot]) return false;
-      uint16_t* cdf = &c.data[c.off[slot]];
+      if (slot >= nslots || s >= lens[slot]) return false;
+      uint16_t* cdf = data + off[slot];
       if (tag == 0)
-        enc.encode_symbol((int)s, cdf, c.len[slot]);
+        enc.encode_symbol((int)s, cdf, lens[slot]);
       else
-        enc.encode_symbol_noupdate((int)s, cdf, c.len[slot]);
+        enc.encode_symbol_noupdate((int)s, cdf, lens[slot]);
     } else if (tag == kTagBool) {
       enc.encode_bool((t & 1) != 0, (uint16_t)((t >> 1) & 0xffff));
     } else {  // gathered partition bool (tag 2)
       const uint32_t slot = (t >> 2) & 0xffff;
-      if (slot >= nslots || c.len[slot] != 10) return false;
-      const uint16_t p = gather_split_prob(&c.data[c.off[slot]], (t & 1) != 0);
+      if (slot >= nslots || lens[slot] != 10) return false;
+      const uint16_t p = gather_split_prob(data + off[slot], (t & 1) != 0);
       enc.encode_bool((t & 2) != 0, p);
     }
   }
-  if (cdef_point >= 0 && (uint32_t)cdef_point == n) enc.mark_cdef();
+  if (cdef_point >= 0 && (uint32_t)cdef_point == n) {
+    enc.mark_cdef();
+    if (cdef_bits > 0) enc.encode_literal(cdef_idx, (uint32_t)cdef_bits);
+  }
   return true;
 }
 
@@ -520,7 +528,8 @@ int mt_pack_tile(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, 
   build_cdfs(q, c);
   mt_range_encoder enc;
   enc.updating_cdf = updating_cdf != 0;
-  enc.tracing = true;
+  enc.tracing = trace != nullptr;
+  if (nsb > 0) enc.precarry.reserve(sb_start[nsb] / 2 + 64);
   for (int32_t i = 0; i < nsb; ++i) {
     enc.mark_sb();
     const int32_t cp = sb_cdef_point ? sb_cdef_point[i] : -1;
@@ -533,6 +542,31 @@ int mt_pack_tile(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, 
     t->marks.swap(enc.trace_marks);
     t->cdef.swap(enc.trace_cdef);
     *trace = t;
+  }
+  return out_bytes(enc.done(), payload, payload_len);
+}
+
+int mt_pack_tile_filtered(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, const uint32_t* sb_start,
+                          const int32_t* sb_cdef_point, int32_t nsb, const uint8_t* sb_cdef_idx, int32_t cdef_bits,
+                          uint8_t** payload, size_t* payload_len) {
+  if (!payload || !payload_len || nsb < 0 || (nsb > 0 && (!ops || !sb_start))) return MT_ERR_INVALID_INPUT;
+  if (cdef_bits < 0 || cdef_bits > 3 || (cdef_bits > 0 && (!sb_cdef_idx || !sb_cdef_point)))
+    return MT_ERR_INVALID_INPUT;
+  for (int32_t i = 0; i < nsb; ++i) {
+    if (sb_start[i + 1] < sb_start[i]) return MT_ERR_INVALID_INPUT;
+    if (cdef_bits > 0 && sb_cdef_point[i] >= 0 && sb_cdef_idx[i] >= (1u << cdef_bits)) return MT_ERR_INVALID_INPUT;
+  }
+  const int q = base_q_idx <= 20 ? 0 : base_q_idx <= 60 ? 1 : base_q_idx <= 120 ? 2 : 3;  // qcat
+  CdfSet c;
+  build_cdfs(q, c);
+  mt_range_encoder enc;
+  enc.updating_cdf = updating_cdf != 0;
+  if (nsb > 0) enc.precarry.reserve(sb_start[nsb] / 2 + 64);
+  for (int32_t i = 0; i < nsb; ++i) {
+    const int32_t cp = sb_cdef_point ? sb_cdef_point[i] : -1;
+    if (!replay_tokens(enc, c, ops + sb_start[i], sb_start[i + 1] - sb_start[i], cp, cdef_bits,
+                       cdef_bits > 0 ? sb_cdef_idx[i] : 0))
+      return MT_ERR_INVALID_INPUT;
   }
   return out_bytes(enc.done(), payload, payload_len);
 }

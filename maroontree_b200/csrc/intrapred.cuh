@@ -110,15 +110,18 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
 
 // Prediction of an N x N block (N = 4, 8 or 16) into out[N*N] (row-major),
 // neighbours read through `rd`.  `scratch` holds 3 * edge_cap<N>() words: the
-// above and left edges and a filter temporary.
+// above and left edges and a filter temporary.  Only rows [y0, y1) of out are
+// written (the edges are always built whole), so several threads can share
+// one block's rows.
 template <int N, typename R, typename O>
 __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int mode, int delta, bool have_tr,
-                              bool have_bl, bool ft, int bd, O* __restrict__ out, int32_t* __restrict__ scratch) {
+                              bool have_bl, bool ft, int bd, O* __restrict__ out, int32_t* __restrict__ scratch,
+                              int y0 = 0, int y1 = N) {
   static_assert(N == 4 || N == 8 || N == 16, "square sizes 4, 8 and 16");
   constexpr int bw = N, bh = N, edge_len = 2 * N, cap = edge_cap<N>();
   if (mode == MT_DC_PRED) {
     const int32_t d = dc_pred_sq_at(rd, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : 4), bd);
-    for (int i = 0; i < N * N; i++) out[i] = (O)(d);
+    for (int i = y0 * N; i < y1 * N; i++) out[i] = (O)(d);
     return;
   }
   // Every edge entry the predictor reads is written below (logical -1 ..
@@ -184,16 +187,16 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
     const int32_t* a = A + kEdgeOrigin;  // logical index 0
     const int32_t* l = L + kEdgeOrigin;
     if (angle == 90) {
-      for (int y = 0; y < bh; y++)
+      for (int y = y0; y < y1; y++)
         for (int x = 0; x < bw; x++) out[y * bw + x] = (O)(a[x]);
     } else if (angle == 180) {
-      for (int y = 0; y < bh; y++)
+      for (int y = y0; y < y1; y++)
         for (int x = 0; x < bw; x++) out[y * bw + x] = (O)(l[y]);
     } else if (angle < 90) {
       const int dx = kDrDeriv[angle >> 1];
       const int max_base_x = (edge_len - 1) << up_a;
       const int frac_bits = 6 - up_a, inc = 1 << up_a;
-      for (int y = 0; y < bh; y++) {
+      for (int y = y0; y < y1; y++) {
         const int xpos = dx * (y + 1);
         const int shift = ((xpos << up_a) & 0x3f) >> 1;
         const int b0 = xpos >> frac_bits;
@@ -206,7 +209,7 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
       const int dy = kDrDeriv[(270 - angle) >> 1];
       const int max_base_y = (edge_len - 1) << up_l;
       const int frac_bits = 6 - up_l, inc = 1 << up_l;
-      for (int y = 0; y < bh; y++)
+      for (int y = y0; y < y1; y++)
         for (int x = 0; x < bw; x++) {
           const int ypos = dy * (x + 1);
           const int shift = ((ypos << up_l) & 0x3f) >> 1;
@@ -216,7 +219,7 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
     } else {
       const int dy = kDrDeriv[(angle - 90) >> 1];
       const int dx = kDrDeriv[(180 - angle) >> 1];
-      for (int y = 0; y < bh; y++) {
+      for (int y = y0; y < y1; y++) {
         const int t = (y + 1) * dx - 64;
         const int x0 = t <= 0 ? 0 : min((t + 63) >> 6, bw);
         const int xpos0 = (x0 << 6) - (y + 1) * dx;
@@ -240,7 +243,7 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
   const int32_t* a = A + kEdgeOrigin;
   const int32_t* l = L + kEdgeOrigin;
   if (mode == MT_PAETH_PRED) {
-    for (int y = 0; y < bh; y++)
+    for (int y = y0; y < y1; y++)
       for (int x = 0; x < bw; x++) {
         const int32_t lv = l[y], tv = a[x], b = lv + tv - corner;
         const int32_t ld = abs(lv - b), td = abs(tv - b), cd = abs(corner - b);
@@ -248,7 +251,7 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
       }
   } else if (mode == MT_SMOOTH_PRED) {
     const int32_t right = a[bw - 1], bottom = l[bh - 1];
-    for (int y = 0; y < bh; y++)
+    for (int y = y0; y < y1; y++)
       for (int x = 0; x < bw; x++) {
         const int32_t wv = sm_weight<N>(y), wh = sm_weight<N>(x);
         const int32_t p = wv * a[x] + (256 - wv) * bottom + wh * l[y] + (256 - wh) * right;
@@ -256,12 +259,12 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
       }
   } else if (mode == MT_SMOOTH_V_PRED) {
     const int32_t bottom = l[bh - 1];
-    for (int y = 0; y < bh; y++)
+    for (int y = y0; y < y1; y++)
       for (int x = 0; x < bw; x++)
         out[y * bw + x] = (O)((sm_weight<N>(y) * a[x] + (256 - sm_weight<N>(y)) * bottom + 128) >> 8);
   } else {  // SMOOTH_H
     const int32_t right = a[bw - 1];
-    for (int y = 0; y < bh; y++)
+    for (int y = y0; y < y1; y++)
       for (int x = 0; x < bw; x++)
         out[y * bw + x] = (O)((sm_weight<N>(x) * l[y] + (256 - sm_weight<N>(x)) * right + 128) >> 8);
   }
@@ -270,8 +273,10 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
 template <int N, typename O>
 __device__ __forceinline__ void predict_sq(const uint16_t* __restrict__ rec, int stride, int fw, int fh, int ox, int oy,
                                            int mode, int delta, bool have_tr, bool have_bl, bool ft, int bd,
-                                           O* __restrict__ out, int32_t* __restrict__ scratch) {
-  predict_sq_at<N>(PlaneRead{rec, stride}, fw, fh, ox, oy, mode, delta, have_tr, have_bl, ft, bd, out, scratch);
+                                           O* __restrict__ out, int32_t* __restrict__ scratch, int y0 = 0,
+                                           int y1 = N) {
+  predict_sq_at<N>(PlaneRead{rec, stride}, fw, fh, ox, oy, mode, delta, have_tr, have_bl, ft, bd, out, scratch, y0,
+                   y1);
 }
 
 template <typename O>

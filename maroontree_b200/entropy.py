@@ -104,6 +104,22 @@ def pack_tile(base_q_idx, sb_tokens, cdef_points=None, updating_cdf=True, want_t
     return (payload, TileTrace(tr.value)) if want_trace else payload
 
 
+def pack_tile_filtered(base_q_idx, sb_tokens, cdef_points, sb_cdef_idx=None, cdef_bits=0, updating_cdf=True):
+    """pack_tile + replay_tile_with_filters in one pass (``mt_pack_tile_filtered``):
+    superblock i's cdef_idx literal coded at its read_cdef() point."""
+    starts = np.zeros(len(sb_tokens) + 1, np.uint32)
+    starts[1:] = np.cumsum([len(t) for t in sb_tokens])
+    ops = np.concatenate([np.asarray(t, np.uint32) for t in sb_tokens]) if sb_tokens else np.zeros(1, np.uint32)
+    ops = np.ascontiguousarray(ops, np.uint32)
+    cp = np.ascontiguousarray(cdef_points, np.int32)
+    idx = None if sb_cdef_idx is None else np.ascontiguousarray(sb_cdef_idx, np.uint8)
+    out, n = C.c_void_p(), C.c_size_t()
+    _check(load().mt_pack_tile_filtered(base_q_idx, int(bool(updating_cdf)), ptr(ops), ptr(starts), ptr(cp),
+                                        len(sb_tokens), ptr(idx), cdef_bits, C.byref(out), C.byref(n)),
+           "mt_pack_tile_filtered")
+    return _take(out, n.value)
+
+
 def replay_tile_with_filters(trace, rect, cdef_grid=None, unit_cols=0, cdef_bits=0, updating_cdf=True):
     """replay_tile_with_filters without loop restoration; rect = (x0, y0, w, h)."""
     grid = None if cdef_grid is None else np.ascontiguousarray(cdef_grid, np.uint8).ravel()

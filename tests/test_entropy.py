@@ -223,6 +223,23 @@ def test_filter_replay_inserts_cdef_literals(mt_lib, oracle_lib):
         _decode_tokens(oracle_lib, d, slots, toks, points[k], bits if points[k] >= 0 else 0, int(grid[k]))
 
 
+@pytest.mark.parametrize("bits,updating", [(0, True), (1, True), (2, False), (3, True)])
+def test_single_pass_filtered_pack_equals_pack_then_replay(mt_lib, oracle_lib, bits, updating):
+    """mt_pack_tile_filtered gives the bytes of pack_tile followed by
+    replay_tile_with_filters on a tile whose units are its superblocks."""
+    slots = oracle_lib.cdfs_new_slots(1)
+    w, h = 64 * 5, 64 * 3
+    sbs, points = _random_tokens(oracle_lib, slots, XorShift(31 + bits), 15, 120)
+    grid = np.array([(5 * k + 1) % (1 << max(bits, 1)) for k in range(15)], np.uint8)
+    payload, trace = en.pack_tile(60, sbs, points, updating_cdf=updating, want_trace=True)
+    want = en.replay_tile_with_filters(trace, (0, 0, w, h), grid if bits else None, unit_cols=5, cdef_bits=bits,
+                                       updating_cdf=updating)
+    got = en.pack_tile_filtered(60, sbs, points, grid if bits else None, bits, updating_cdf=updating)
+    assert got == want
+    if bits == 0:
+        assert got == payload
+
+
 def test_packer_rejects_bad_tokens(mt_lib, oracle_lib):
     from maroontree_b200 import MtError
 
