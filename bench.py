@@ -1,32 +1,38 @@
-"""Benchmark of the B200 intra RD core.
+"""Benchmark of the B200 intra encoder: the AVIF encode through mt_encode_rgb8.
 
-Default workload (1080p 4:2:0 luma, quality 60 -> qindex 70, QM level 6): one
-step is one batched RDO level over the whole frame -- every 8x8 luma block x
-13 intra modes x 5 transform types (the 2-D-scan set IDTX, DCT_DCT, ADST_ADST,
-ADST_DCT, DCT_ADST) = 2,106,000 candidate chains (predict -> residual ->
-forward transform + quant + QM -> trellis -> inverse -> SATD distortion ->
-coefficient rate -> RD cost), neighbours taken from a reconstruction snapshot.
+Default workload: the 1920x1080 generator image (seed 3: sinusoids, rectangles,
+noise sigma 4, the 64-px texture band and the gradient quadrant), 4:2:0,
+quality 60 (qindex 70, QM level 6).  One step is one whole encode: colour
+conversion and padding, the 8x8 decisions over the dependency wavefront of
+the frame (every 8x8 luma block x 13 intra modes x 7 transform types, each
+candidate predicted, transformed, quantised with the QM, trellised,
+reconstructed, priced by SATD distortion and coefficient rate; chroma UV DC),
+coefficient token emission, block syntax, deblocking, the CDEF decision, range
+coding with the cdef_idx literals, headers and the AVIF container.  The
+decisions are this library's 8x8 rule, not the reference's decode_sb, and the
+file is byte for byte the oracle encode's (oracle/oracle_avif.py), which is
+checked in every default run.
 
-  value  MPix/s of the device-resident launch (inputs already in HBM)
-  e2e    MPix/s through the public host C ABI (mt_rdo_level8): host planes,
-         block and combo lists copied in, per-block winners copied out, every
-         step
+  value  MPix/s with the RGB already in device memory (mt_encode_rgb8_device),
+         the whole call between CUDA events on its stream, L2 flushed before
+         each step
+  e2e    MPix/s through mt_encode_rgb8 with host RGB (pinned), the copies of the
+         call inside the timed region; the bytes both ways are the library's
+         count of its own copies
 
-The line also carries ``level4`` / ``level16`` (the 4x4 and 16x16 levels of
-the same frame, device time and the oracle on the host cores), ``split16``
-(the 16x16 leaf's TX_8X8 split trial over every block and mode, with and
-without the 4:4:4 type search, and its depth-2 TX_4X4 trial), ``leaf8`` (the
-8x8 leaf's mode-loop candidates and winner refinement) and
-``frame_filters``: the frame-wide kernels of the same
-1080p 4:2:0 frame (colour conversion + padding, the adaptive-quantisation
-grid, the screen-content gate, the CfL alpha of every 8x8 chroma block,
-deblocking of the three planes, CDEF tables +
-strength search + apply) timed on the device with CUDA events after an L2
-flush, with their algorithmic bytes against the measured HBM copy bandwidth.
+The roofline is the dominant kernel's (encode_blocks_kernel: the persistent
+decision kernel): its algorithmic integer/FP32 operations over its device time
+against the SMs' issue rate, and the dependency view that bounds it (levels of
+the 8x8 dependency graph and the time per level).
 
-``--impl reference`` times the CPU restatement of the reference (the oracle;
-the Rust reference cannot be built here) on all host cores over a bounded
-sample of the same workload.
+The line also carries the earlier kernel-level measurements of the same frame
+as secondary entries: ``level8`` (one batched 8x8 RDO level over a
+reconstruction snapshot, the oracle's results asserted equal), ``level4`` /
+``level16``, ``split16``, ``leaf8`` and ``frame_filters``.
+
+``--impl reference`` times the oracle encode (the CPU restatement of the same
+encode; the Rust reference cannot be built here) on all host cores, one whole
+encode per step; it never loads the CUDA library.
 """
 import argparse
 import json
@@ -44,7 +50,8 @@ sys.path.insert(0, ROOT)
 W, H, SEED, QUALITY, SUB = 1920, 1080, 3, 60, 2  # the 1080p 4:2:0 quality-60 frame
 MODES = list(range(13))
 MPIX = W * H / 1e6
-METRIC = "MPix/s (8x8 RDO level, 1080p luma)"
+METRIC = "MPix/s (AVIF encode, mt_encode_rgb8 1920x1080 4:2:0 quality 60)"
+LEVEL_METRIC = "MPix/s (8x8 RDO level, 1080p luma)"
 SMS, LANES_PER_SM = 148, 128  # B200: SMs x INT32/FP32 lanes per SM
 # DRAM bytes of one level8_kernel launch on this workload, dram__bytes_read.sum
 # + dram__bytes_write.sum of the ncu capture in profiles/level8_kernel_1080p_q60.md
@@ -82,37 +89,71 @@ def chain_ops(combos, results, nblocks, qm_on):
     return int((fixed * nblocks).sum() + PER_COEF_OPS * coefs.sum())
 
 
-def config_line(nb, nc):
+def config_line():
     """The config object both arms print."""
+    return {"workload": "encode_rgb8 1920x1080 4:2:0 quality 60 (qindex 70, QM 6), generator image seed 3: every "
+                        "64x64 superblock split to 8x8 blocks, each luma block the lowest RD cost of 13 intra modes x "
+                        "7 transform types (91 candidates), chroma UV_DC_PRED + DCT_DCT, deblocking, CDEF decision, "
+                        "range coding, AVIF container",
+            "decisions": "the library's 8x8 rule (not the reference's decode_sb search)",
+            "config": "EncodeConfig defaults (Slow: CDEF on, updating CDFs, sRGB-YCbCr CICP) with quality 60",
+            "blocks": (W // 8) * ((H + 7) // 8), "candidates_per_block": 91,
+            "l2": "256 MB buffer written before each timed step"}
+
+
+def level_config(nb, nc):
+    """The config of the secondary 8x8-level measurement."""
     return {"workload": "rdo-level-8x8 1920x1080 4:2:0 quality 60 (qindex 70, QM 6), seed 3: every 8x8 luma block "
                         "x 13 intra modes x 5 transform types (IDTX, DCT_DCT, ADST_ADST, ADST_DCT, DCT_ADST)",
             "cdfs": "default decision snapshot Cdfs::new(qctx 2)", "lambdas": "shipped Slow laws at qindex 70 4:2:0",
             "candidates": nb * nc, "blocks": nb, "combos": nc, "l2": "inputs re-read after an L2 flush per step"}
 
 
-def make_workload(impl="ours"):
-    """The headline workload.  The quantiser, QM row, lambdas and default CDFs
-    come from the CUDA library's C ABI for our arm and from the oracle's
-    restatement for the reference arm (which must not load the library)."""
-    import maroontree_b200 as mt  # numpy / ctypes host helpers; the CUDA library loads on first call only
+def encode_rgb():
+    from maroontree_b200 import synth
+
+    return synth.generate_rgb(W, H, SEED, sigma=4.0, variant="1080p")
+
+
+def oracle_encode(rgb, threads):
+    """The oracle encode of the frame on `threads` host cores: (bytes, seconds)."""
+    from oracle import oracle_avif as oa
+
+    t0 = time.perf_counter()
+    avif = oa.encode_rgb8(rgb, QUALITY, 0, threads=threads)
+    return avif, time.perf_counter() - t0
+
+
+# Algorithmic operations of one block's decision (the roofline's work unit),
+# from the per-stage table above with every coefficient up to the end of block
+# counted (an upper bound of the per-coefficient part): the 13 predictions, and
+# per (mode, type) the rest of the chain (V_DCT / H_DCT counted as DCT_DCT, an
+# upper bound: one 1-D pass each); chroma adds two DC_PRED + DCT_DCT chains (8x8
+# in 4:4:4; in 4:2:0 a 4x4 chain, counted as a quarter of the 8x8 one).
+def block_ops(sub):
+    per_type = (0, 1, 1, 1, 4, 5, 6)  # IDTX, DCT_DCT, V_DCT, H_DCT, ADST_ADST, ADST_DCT, DCT_ADST
+    chain = sum(RESID_OPS + FWD_OPS[t] + QUANT_OPS + (QM_OPS if t != 0 else 0) + DEQUANT_OPS + INV_OPS[t] + SATD_OPS
+                + RD_OPS + 64 * PER_COEF_OPS for t in per_type)
+    luma = len(MODES) * chain + sum(PRED_OPS.get(m, 600) for m in MODES)
+    chroma = PRED_OPS[0] + RESID_OPS + FWD_OPS[1] + QUANT_OPS + QM_OPS + DEQUANT_OPS + INV_OPS[1] + SATD_OPS + RD_OPS + \
+        64 * PER_COEF_OPS
+    return luma + (2 * chroma if sub == 0 else chroma // 2)
+
+
+def make_workload():
+    """The workload of the secondary kernel-level measurements: the frame's
+    luma, a seeded reconstruction snapshot (source plus +-3 coding error), the
+    8x8 level's blocks and (mode, type) combos, and the frame laws' quantiser,
+    QM row, lambdas and default CDF slice from the library's C ABI."""
+    import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
-    if impl == "ours":
-        qidx = mt.quality_to_q(QUALITY)
-        qm_level = mt.qm_levels(qidx, SUB)[0]
-        q = mt.quant_new(qidx, 8, qm_level)
-        qm = mt.qm_row(qm_level, 0, 8)
-        lam = mt.rd_lambdas(qidx, q.dc_q, SUB)
-        cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 0)
-    else:
-        from oracle import pyoracle as po
-
-        qidx = po.quality_to_q(QUALITY)
-        qm_level = po.qm_level_law(qidx, SUB)
-        q = po.quant_new(qidx, 8, qm_level)
-        qm = po.qm_row(qm_level, 0, 8)
-        lam = po.rd_lambdas(qidx, q.dc_q, SUB)
-        cdfs = po.default_cdfs(po.qcat(qidx), 8)
+    qidx = mt.quality_to_q(QUALITY)
+    qm_level = mt.qm_levels(qidx, SUB)[0]
+    q = mt.quant_new(qidx, 8, qm_level)
+    qm = mt.qm_row(qm_level, 0, 8)
+    lam = mt.rd_lambdas(qidx, q.dc_q, SUB)
+    cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 0)
     rgb = synth.generate_rgb(W, H, SEED, sigma=4.0, variant="1080p")
     src = synth.rgb_to_luma(rgb)
     rec = synth.synthetic_recon(src, SEED + 1000)
@@ -234,30 +275,30 @@ def cpu_level(wl, threads):
 
 
 def run_reference(args):
-    """The reference arm: the CPU restatement of the reference (the oracle; the
-    Rust reference cannot be built here) over the same level on all host cores.
-    Its workload comes from the oracle alone; the CUDA library is never loaded."""
+    """The reference arm: the oracle encode (the CPU restatement of the same
+    encode; the Rust reference cannot be built here), one whole encode per
+    step on all host cores.  Its inputs come from the oracle and the shared
+    image generator alone; the CUDA library is never loaded."""
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
     from oracle import build as obuild
 
     obuild.build()
-    wl = make_workload("reference")
+    rgb = encode_rgb()
     threads = os.cpu_count() or 1
-    nb, nc = len(wl["blocks"]), len(wl["combos"])
     for _ in range(args.warmup):
-        cpu_level(dict(wl, cands=wl["cands"][:50_000]), threads)
-    times = [cpu_level(wl, threads)[1] for _ in range(args.steps)]
+        oracle_encode(rgb, threads)
+    times = [oracle_encode(rgb, threads)[1] for _ in range(args.steps)]
     step_s = float(np.mean(times))
     value = MPIX / step_s
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4),
         "unit": "MPix/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(step_s * 1e3, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int32+f32", "data": "synthetic", "config": config_line(nb, nc),
+        "dtype": "int32+f32", "data": "synthetic", "config": config_line(),
         "cpu_baseline": {"value": round(value, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
-                         "sample": f"every candidate of the level ({nb * nc}) per step"},
+                         "sample": "one whole 1920x1080 encode per step (the oracle's restatement, all host cores)"},
         "e2e": {"value": round(value, 4), "unit": "MPix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -477,42 +518,6 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     return out
 
 
-def measure_encode(wl, reps=3):
-    """The whole-file encode of the same 1080p 4:2:0 quality-60 frame through
-    mt_encode_rgb8 (host RGB in, AVIF bytes out; colour conversion, the 8x8
-    decision wavefront, token emission, packing, filters and container inside
-    the timed call).  Its decisions are the library's own 8x8 search, not the
-    reference's decode_sb, so the bytes are not the reference's; the file is a
-    valid AVIF that AV1 decoders reproduce exactly (tests/test_encode.py)."""
-    import io
-
-    from maroontree_b200 import encoder as enc
-
-    rgb = wl["rgb"]
-    cfg = enc.config(quality=QUALITY)
-    avif = enc.encode_rgb8(rgb, cfg)  # warm-up (module load, first allocations)
-    times = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        avif = enc.encode_rgb8(rgb, cfg)
-        times.append(time.perf_counter() - t0)
-    step = float(np.median(times))
-    out = {"ms": round(step * 1e3, 2), "mpix_s": round(MPIX / step, 3), "bytes": len(avif),
-           "workload": "mt_encode_rgb8 1920x1080 4:2:0 quality 60: 8x8 blocks, 13 modes x 7 types per luma block",
-           "decisions": "the library's 8x8 search (not the reference's decode_sb)"}
-    try:
-        from PIL import Image
-
-        im = Image.open(io.BytesIO(avif))
-        im.load()
-        dec = np.asarray(im.convert("RGB")).astype(np.float64)
-        mse = float(np.mean((dec - rgb.astype(np.float64)) ** 2))
-        out["psnr_rgb_db"] = round(10 * np.log10(255.0 ** 2 / mse), 3)
-    except Exception as e:  # decoding is a check, not part of the measurement
-        out["decode_error"] = str(e)[:200]
-    return out
-
-
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -681,24 +686,19 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     return out
 
 
-def run_ours(args):
+def measure_level8(dev, wl, steps, warmup, op_peak, hbm_peak, cpu):
+    """The batched 8x8 RDO level over a reconstruction snapshot of the frame
+    (every block x 13 modes x 5 types): device time after an L2 flush, the
+    host ABI call, the integer-op roofline, and the oracle over the same
+    candidates on all host cores with its results asserted equal."""
     import torch
     import maroontree_b200 as mt
     from maroontree_b200 import abi
 
-    _, _, local = dist_env()
-    torch.cuda.set_device(local)
-    ranks = Replicas("nccl")
-    world, rank = ranks.world, ranks.rank
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    mt.load()
-    wl = make_workload()
     blocks, combos = wl["blocks"], wl["combos"]
     nb, nc = len(blocks), len(combos)
     n = nb * nc
     costs = mt.coef_costs(wl["cdfs"])
-    # device-resident inputs (replicas: every rank encodes its own frame; no collective on the data path)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_src, d_rec, d_qm = t(wl["src"]), t(wl["rec"]), t(wl["qm"])
     d_costs = t(np.frombuffer(bytes(costs), np.uint8))
@@ -713,44 +713,101 @@ def run_ours(args):
         mt.rdo_level8_device(d_src, d_rec, wl["prm"], wl["q"], d_qm, d_costs, d_blocks, nb, d_combos, nc, d_best,
                              d_res, d_keys, stream=stream.cuda_stream)
 
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(max(warmup, 3)):
         launch()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for i in range(steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        launch()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    step_ms = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    src, rec = wl["src"], wl["rec"]
+    e2e = []
+    for _ in range(max(1, steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mt.rdo_level8(src, rec, wl["prm"], wl["q"], wl["qm"], costs, blocks, combos)
+        e2e.append(time.perf_counter() - t0)
+    res_gpu = d_res.cpu().numpy().view(abi.RESULT_DTYPE)
+    ops = chain_ops(combos, res_gpu, nb, wl["qm"] is not None)
+    achieved = ops / (step_ms / 1e3)
+    alg_bytes = n * (32 + 128 + 66) + nb * 60
+    out = {"metric": LEVEL_METRIC, "value": round(MPIX / (step_ms / 1e3), 3), "ms": round(step_ms, 4),
+           "e2e_mpix_s": round(MPIX / float(np.median(e2e)), 3), "config": level_config(nb, nc),
+           "roofline": {"bound": "int32/fp32 issue", "achieved_tops": round(achieved / 1e12, 3),
+                        "peak_tops": round(op_peak / 1e12, 3), "frac": round(achieved / op_peak, 4),
+                        "traffic": NCU_DRAM_BYTES_PER_LAUNCH, "ops_per_launch": ops,
+                        "hbm_frac": round(alg_bytes / (step_ms / 1e3) / 1e9 / hbm_peak, 4)},
+           "gpu_launches": 4 * steps}
+    if cpu:
+        threads = os.cpu_count() or 1
+        ref, dt = cpu_level(wl, threads)
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                               "sample": f"the whole level, {n} candidates ({dt:.2f} s)"}
+        out["results_equal_oracle"] = res_gpu.tobytes() == ref.tobytes()
+        if not out["results_equal_oracle"]:
+            raise SystemExit("bench: the GPU level's results differ from the oracle's")
+    return out
+
+
+def run_ours(args):
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi
+    from maroontree_b200 import encoder as enc
+
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    ranks = Replicas("nccl")
+    world, rank = ranks.world, ranks.rank
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    mt.load()
+    rgb = encode_rgb()
+    cfg = enc.config(quality=QUALITY, chroma=0)  # MT_CHROMA_420
+    # replicas: every rank encodes its own copy of the frame, no collective on the data path
+    d_rgb = torch.from_numpy(np.ascontiguousarray(rgb).reshape(-1)).to(dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)  # the legacy default stream, the library's stream
+
+    def step(stats=None):
+        return enc.encode_rgb8_device(d_rgb.data_ptr(), W, H, cfg, stats=stats)
+
+    for _ in range(max(args.warmup, 3)):
+        avif = step()
     torch.cuda.synchronize()
     ranks.barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    stats = [abi.EncodeStats() for _ in range(args.steps)]
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         for i in range(args.steps):
-            flush.zero_()  # L2 flush between timed launches (outside the events)
+            flush.zero_()  # L2 flush between timed steps (outside the events)
             ev[i][0].record(stream)
-            launch()
+            avif = step(stats[i])
             ev[i][1].record(stream)
         torch.cuda.synchronize()
-    kernel_ms = [a.elapsed_time(b) for a, b in ev]
-    step_ms = ranks.max(float(np.mean(kernel_ms)), device=dev)
+    step_ms = ranks.max(float(np.mean([a.elapsed_time(b) for a, b in ev])), device=dev)
     value = ranks.job_value(step_ms)
 
-    # e2e through the host ABI (mt_rdo_level8): planes, block and combo lists
-    # copied in and the per-block winners copied out inside the timed region
-    src, rec = wl["src"], wl["rec"]
-    e2e_times = []
+    # e2e through mt_encode_rgb8: host RGB (pinned) in, AVIF bytes out
+    pinned = torch.empty(rgb.nbytes, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = np.ascontiguousarray(rgb).reshape(-1)
+    host_rgb = pinned.numpy().reshape(rgb.shape)
+    e2e_times, e2e_stats = [], abi.EncodeStats()
     ranks.barrier()
-    for i in range(max(1, args.steps)):
+    for _ in range(max(1, args.steps)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        best, _ = mt.rdo_level8(src, rec, wl["prm"], wl["q"], wl["qm"], costs, blocks, combos)
+        avif_e2e = enc.encode_rgb8(host_rgb, cfg, stats=e2e_stats)
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = ranks.max(float(np.median(e2e_times)), device=dev)
-    h2d = 2 * src.nbytes + len(bytes(costs)) + 64 + blocks.nbytes + combos.nbytes
-    d2h = nb * abi.BEST_DTYPE.itemsize
+    if avif_e2e != avif:
+        raise SystemExit("bench: the host and device entry points gave different files")
 
-    # roofline of the level (four launches; level8_kernel is ~99 % of them in
-    # profiles/bench_launch_list_1080p_q60.md) against the SMs' INT32/FP32 issue
-    # rate: algorithmic operations of every candidate (chain_ops: the per-stage
-    # table above, the per-coefficient part up to each candidate's own end of
-    # block, read from this run's results) over the mean device time.
-    res_gpu = d_res.cpu().numpy().view(abi.RESULT_DTYPE)
-    ops = chain_ops(combos, res_gpu, nb, wl["qm"] is not None)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -760,68 +817,70 @@ def run_ours(args):
     clocks = clk.summary()
     clk_mhz = clocks.get("sm_mhz") or 1965.0
     op_peak = SMS * LANES_PER_SM * clk_mhz * 1e6  # thread operations per second at the sampled SM clock
-    achieved = ops / (step_ms / 1e3)
-    # HBM view of the same launch: per candidate the result record (32 B) +
-    # source block (64 x 2 B) + neighbour edges (up to 33 x 2 B); per block its
-    # record (60 B)
-    alg_bytes = n * (32 + 128 + 66) + nb * 60
+    blocks_ms = float(np.mean([st.blocks_ms for st in stats]))
+    nblocks, nlevels = stats[0].blocks, stats[0].levels
+    ops = nblocks * block_ops(SUB)
+    achieved = ops / (blocks_ms / 1e3)
 
-    filters = measure_filters(dev, wl, hbm_peak) if rank == 0 else None
-    encode = measure_encode(wl) if rank == 0 else None
-    level4 = measure_small_level(dev, wl, 4, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
-    level16 = measure_small_level(dev, wl, 16, cpu=world == 1 and not args.no_cpu) if rank == 0 else None
-    split16 = {k: measure_split16(dev, wl, k == "search", cpu=world == 1 and not args.no_cpu)
-               for k in ("dct", "search")} if rank == 0 else None
-    if split16 is not None:
-        split16["depth2"] = measure_split16(dev, wl, False, cpu=world == 1 and not args.no_cpu, depth2=True)
-    leaf8 = {k: measure_leaf8(dev, wl, k == "refine", cpu=world == 1 and not args.no_cpu)
-             for k in ("luma", "refine")} if rank == 0 else None
-    if leaf8 is not None:
-        leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=world == 1 and not args.no_cpu, n16=True)
-        leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=world == 1 and not args.no_cpu, n16=True)
-
+    secondary = {}
     cpu = parity = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        from oracle import build as obuild
+    if rank == 0:
+        wl = make_workload()
+        nocpu = world > 1 or args.no_cpu
+        secondary["level8"] = measure_level8(dev, wl, args.steps, args.warmup, op_peak, hbm_peak, not nocpu)
+        secondary["frame_filters"] = measure_filters(dev, wl, hbm_peak)
+        secondary["level4"] = measure_small_level(dev, wl, 4, cpu=not nocpu)
+        secondary["level16"] = measure_small_level(dev, wl, 16, cpu=not nocpu)
+        split16 = {k: measure_split16(dev, wl, k == "search", cpu=not nocpu) for k in ("dct", "search")}
+        split16["depth2"] = measure_split16(dev, wl, False, cpu=not nocpu, depth2=True)
+        secondary["split16"] = split16
+        leaf8 = {k: measure_leaf8(dev, wl, k == "refine", cpu=not nocpu) for k in ("luma", "refine")}
+        leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n16=True)
+        leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=not nocpu, n16=True)
+        secondary["leaf8"] = leaf8
+        if not nocpu:
+            from oracle import build as obuild
 
-        obuild.build()
-        threads = os.cpu_count() or 1
-        ref, dt = cpu_level(wl, threads)  # the same candidates, combo-major
-        cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
-               "sample": f"the whole level, {n} candidates ({dt:.2f} s)"}
-        # the timed level's results must be the oracle's, bit for bit
-        parity = {"results_equal_oracle": res_gpu.tobytes() == ref.tobytes(), "candidates": n}
-        if not parity["results_equal_oracle"]:
-            raise SystemExit("bench: the GPU level's results differ from the oracle's")
+            obuild.build()
+            threads = os.cpu_count() or 1
+            want, dt = oracle_encode(rgb, threads)
+            cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                   "sample": f"one whole 1920x1080 encode by the oracle ({dt:.2f} s)"}
+            # the timed encode's file must be the oracle encode's, byte for byte
+            parity = {"avif_bytes_equal_oracle": avif == want, "bytes": len(avif)}
+            if avif != want:
+                raise SystemExit("bench: the GPU encode's file differs from the oracle encode's")
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "MPix/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32+f32",
-        "data": "synthetic", "config": config_line(nb, nc),
+        "data": "synthetic", "config": config_line(),
         "parallelism": f"replicas x{world}",
-        "e2e": {"value": round(ranks.job_value(e2e_s * 1e3), 3), "unit": "MPix/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "int32/fp32 issue", "achieved": round(achieved / 1e12, 3),
+        "e2e": {"value": round(ranks.job_value(e2e_s * 1e3), 3), "unit": "MPix/s",
+                "h2d_bytes_per_step": int(e2e_stats.h2d_bytes), "d2h_bytes_per_step": int(e2e_stats.d2h_bytes)},
+        "roofline": {"bound": "int32/fp32 issue", "achieved": round(achieved / 1e12, 4),
                      "peak": round(op_peak / 1e12, 3), "unit": "Tops/s", "frac": round(achieved / op_peak, 4),
-                     "traffic": NCU_DRAM_BYTES_PER_LAUNCH, "kernel": "level8_kernel (+ its run/pred/finalize launches)",
-                     "ops_per_launch": ops, "alg_bytes_per_launch": alg_bytes,
-                     "hbm": {"achieved_gbs": round(alg_bytes / (step_ms / 1e3) / 1e9, 1), "peak_gbs": hbm_peak,
-                             "frac": round(alg_bytes / (step_ms / 1e3) / 1e9 / hbm_peak, 4)},
+                     "traffic": None, "kernel": "encode_blocks_kernel",
+                     "ops_per_launch": int(ops), "kernel_ms": round(blocks_ms, 4),
+                     "ops_basis": "per 8x8 block: 13 predictions + 91 (mode, type) chains with every coefficient "
+                                  "counted + two chroma chains, by the per-stage operation table of the oracle",
                      "peak_basis": f"{SMS} SMs x {LANES_PER_SM} INT32/FP32 lanes x the sampled SM clock "
-                                   f"({clk_mhz:.0f} MHz); no measured integer peak exists"},
+                                   f"({clk_mhz:.0f} MHz); no measured integer peak exists",
+                     "dependency": {"levels": int(nlevels), "blocks": int(nblocks),
+                                    "us_per_level": round(blocks_ms * 1e3 / max(nlevels, 1), 3),
+                                    "note": "the kernel is bound by its chain of dependent 8x8 blocks (a block "
+                                            "needs its left, top, top-left and, where its edges use them, "
+                                            "top-right and bottom-left neighbours), not by issue or HBM"}},
+        "host": {"call_ms": round(float(np.mean([st.call_ms for st in stats])), 4),
+                 "blocks_kernel_ms": round(blocks_ms, 4), "tokens": int(stats[0].tokens),
+                 "avif_bytes": len(avif)},
         "parity": parity,
-        "frame_filters": filters,
-        "encode": encode,
-        "level4": level4,
-        "level16": level16,
-        "split16": split16,
-        "leaf8": leaf8,
-        # per step: level8_runs_kernel, level8_pred_kernel, level8_kernel, level8_finalize_kernel
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": int(sum(st.kernel_launches for st in stats)),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    line.update(secondary)
     ranks.emit(line)
     ranks.close()
     return 0

@@ -1208,10 +1208,32 @@ int mt_emit_coeffs(const int32_t* levels, size_t nlevels, const mt_coef_block* b
  * 4:4:4 (else MT_ERR_UNSUPPORTED_CHROMA_FORMAT).  *out is freed with mt_free. */
 int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
                    size_t* out_len);
+/* What one encode call did, for measurement: the bytes it copied between the
+ * host and the device in each direction, the kernels of this library it
+ * launched, the semantic tokens it range coded, and device times (CUDA events
+ * on its stream) of the block-decision kernel and of the whole call. */
+typedef struct mt_encode_stats {
+  uint64_t h2d_bytes;
+  uint64_t d2h_bytes;
+  uint32_t kernel_launches;
+  uint32_t tokens;
+  uint32_t blocks;          /* 8x8 blocks decided */
+  uint32_t levels;          /* dependency levels of those blocks (the critical path) */
+  float blocks_ms;
+  float call_ms;
+} mt_encode_stats;
+
 /* The same, also returning the decoder's output planes (padded sizes of
- * mt_padded_plane_dims, after deblocking and CDEF) when recon_out is non-NULL. */
+ * mt_padded_plane_dims, after deblocking and CDEF) when recon_out is non-NULL
+ * and the call's measurements when stats is non-NULL. */
 int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
-                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3]);
+                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3], mt_encode_stats* stats);
+/* mt_encode_rgb8 with the interleaved RGB already in device memory (d_rgb,
+ * width * height * 3 bytes); the AVIF comes back in host memory as from
+ * mt_encode_rgb8.  No counterpart in the reference, whose input is always in
+ * host memory. */
+int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
+                          uint8_t** out, size_t* out_len, mt_encode_stats* stats);
 /* The same encode from 8-bit Y, U, V planes (chroma at ((w + sx) >> sx) x
  * ((h + sy) >> sy)), without colour conversion: the planes are coded as
  * given and described by the config's CICP (e.g. identity for G, B, R). */

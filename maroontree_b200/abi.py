@@ -238,6 +238,13 @@ class EncodePlan(C.Structure):
                 ("dark_aq", C.c_int32)]
 
 
+class EncodeStats(C.Structure):
+    """mt_encode_stats: what one encode call did."""
+    _fields_ = [("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("kernel_launches", C.c_uint32),
+                ("tokens", C.c_uint32), ("blocks", C.c_uint32), ("levels", C.c_uint32), ("blocks_ms", C.c_float),
+                ("call_ms", C.c_float)]
+
+
 COEF_BLOCK_DTYPE = np.dtype([("cf_offset", "<u4"), ("log2n", "u1"), ("plane", "u1"), ("skip_ctx", "u1"),
                               ("dcs_ctx", "u1"), ("y_mode", "u1"), ("txtp", "u1"), ("code_txtp", "u1"),
                               ("tx_class", "u1")])
@@ -287,7 +294,9 @@ def _bind(lib):
         "mt_encode_rgb8": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
                                      C.POINTER(C.c_size_t)]),
         "mt_encode_rgb8_ex": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
-                                        C.POINTER(C.c_size_t), _P]),
+                                        C.POINTER(C.c_size_t), _P, C.POINTER(EncodeStats)]),
+        "mt_encode_rgb8_device": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
+                                            C.POINTER(C.c_size_t), C.POINTER(EncodeStats)]),
         "mt_encode_yuv8": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
                                      C.POINTER(C.c_size_t), _P]),
         "mt_emit_coeffs_device": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
@@ -426,7 +435,7 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_range_encoder_new", "mt_range_encoder_free",
     "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
     "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default", "mt_cdf_layout",
-    "mt_emit_coeffs_device", "mt_emit_coeffs", "mt_encode_rgb8", "mt_encode_rgb8_ex", "mt_encode_yuv8",
+    "mt_emit_coeffs_device", "mt_emit_coeffs", "mt_encode_rgb8", "mt_encode_rgb8_ex", "mt_encode_rgb8_device", "mt_encode_yuv8",
     "mt_pack_tile", "mt_pack_tile_filtered", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
     "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
     "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image",

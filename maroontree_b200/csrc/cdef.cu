@@ -580,6 +580,25 @@ Layout make_layout(const Geo& g, bool mono) {
   return L;
 }
 
+}  // namespace
+
+namespace mth {
+// Kernels the calling thread's last mt_cdef_frame_device launched (the
+// direction and table kernels, and the apply kernel when a unit filters).
+thread_local int cdef_last_launches = 0;
+// Bytes mt_cdef_frame_device moves between the device and the host: the
+// per-unit tables read back for the strength search (d2h) and the chosen
+// per-unit strengths sent back (h2d, only when the apply kernel runs).
+void cdef_frame_transfer_bytes(const mt_cdef_params* p, size_t* d2h, size_t* h2d) {
+  const Geo g = make_geo(p);
+  const Layout L = make_layout(g, p->mono != 0);
+  *d2h = L.read_bytes;
+  *h2d = (size_t)g.uc * g.ur * 4;
+}
+}  // namespace mth
+
+namespace {
+
 int launch_tables(const uint16_t* y, const uint16_t* u, const uint16_t* v, const uint16_t* sy, const uint16_t* su,
                   const uint16_t* sv, const uint8_t* skip8, const Geo& g, bool mono, uint8_t* dirs, int32_t* vars,
                   int64_t* ltab, int64_t* utab, int64_t* vtab, unsigned long long* dv_sum, int* dv_cnt,
@@ -934,9 +953,11 @@ int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint
   int64_t* tabs = reinterpret_cast<int64_t*>(s + L.tabs);
   unsigned long long* dv_sum = reinterpret_cast<unsigned long long*>(s + L.dv_sum);
   int* dv_cnt = reinterpret_cast<int*>(s + L.dv_cnt);
+  mth::cdef_last_launches = 0;
   rc = launch_tables(d_y, d_u, d_v, d_src_y, d_src_u, d_src_v, d_skip8, g, mono, dirs, vars, tabs, tabs + nu * kNCand,
                      tabs + 2 * nu * kNCand, dv_sum, dv_cnt, st);
   if (rc != MT_OK) return rc;
+  mth::cdef_last_launches = 2;
   // Read the tables back (one copy) for the host search.
   std::vector<uint8_t> host(L.read_bytes);
   if (cudaMemcpyAsync(host.data(), s + L.tabs, L.read_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
@@ -973,6 +994,7 @@ int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint
     if (cudaMemcpyAsync(s + L.snap_v, d_v, nc, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MT_ERR_DEVICE;
   }
   cdef_apply_kernel<<<dim3(g.nbx, g.nby, mono ? 1 : 3), 64, 0, st>>>(aa, g, d_skip8, dirs, vars, s + L.ustr);
+  mth::cdef_last_launches = 3;
   // The strengths were staged from pageable host memory; keep the buffer alive
   // until the copy has been consumed.
   if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;

@@ -504,7 +504,46 @@ struct DevBuf {
   bool alloc(size_t n) { return cudaMalloc(&p, n ? n : 1) == cudaSuccess; }
 };
 
+// The stats of one call: copies, launches and CUDA-event times (the events
+// exist only when the caller asked for stats).
+struct CallStats {
+  mt_encode_stats* s;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start, blocks start, blocks end, call end
+  explicit CallStats(mt_encode_stats* st) : s(st) {
+    if (!s) return;
+    memset(s, 0, sizeof(*s));
+    for (auto& e : ev) cudaEventCreate(&e);
+  }
+  ~CallStats() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  void h2d(size_t n) {
+    if (s) s->h2d_bytes += n;
+  }
+  void d2h(size_t n) {
+    if (s) s->d2h_bytes += n;
+  }
+  void launches(int n) {
+    if (s) s->kernel_launches += (uint32_t)n;
+  }
+  void mark(int k, cudaStream_t st) {
+    if (s) cudaEventRecord(ev[k], st);
+  }
+  void finish() {
+    if (!s) return;
+    cudaEventSynchronize(ev[3]);
+    cudaEventElapsedTime(&s->blocks_ms, ev[1], ev[2]);
+    cudaEventElapsedTime(&s->call_ms, ev[0], ev[3]);
+  }
+};
+
 }  // namespace
+
+namespace mth {
+void cdef_frame_transfer_bytes(const mt_cdef_params* p, size_t* d2h, size_t* h2d);
+extern thread_local int cdef_last_launches;
+}  // namespace mth
 
 extern "C" {
 
@@ -515,8 +554,9 @@ int mt_emit_coeffs_device(const int32_t* d_levels, const mt_coef_block* d_blocks
 
 // The encode from the input planes: rgb (interleaved, converted by the Q13
 // colour conversion) or yuv (three 8-bit planes at their displayed sizes).
-static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t width, uint32_t height,
-                       const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
+static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* const* yuv, uint32_t width,
+                       uint32_t height, const mt_encode_config* cfg, uint8_t** out, size_t* out_len,
+                       uint16_t* recon_out[3], mt_encode_stats* stats) {
   if (!out || !out_len) return MT_ERR_INVALID_INPUT;
   *out = nullptr;
   *out_len = 0;
@@ -535,6 +575,8 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   if ((rc = mt_padded_plane_dims((int)width, (int)height, sub, &pw, &ph, &pcw, &pch)) != MT_OK) return rc;
   const int nbx = pw / 8, nby = ph / 8, nb = nbx * nby;
   const int sb_cols = (pw + 63) / 64, sb_rows = (ph + 63) / 64;
+  // one tile: the AV1 maximum tile width (64 superblocks) and area (2304)
+  if (sb_cols > 64 || sb_cols * sb_rows > 2304) return MT_ERR_UNSUPPORTED;
   const int cl = sub ? 16 : 64;  // chroma levels per block
   // quantisers, QM rows, default CDF slices and their bit costs, lambdas
   mt_quant qy, qc;
@@ -556,7 +598,7 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   DevBuf d_rgb, d_pl, d_tab, d_dec, d_lv, d_emit, d_maps, d_skip8;
   const size_t in_bytes = rgb ? (size_t)width * height * 3
                               : (size_t)width * height + 2 * (size_t)((width + sx) >> sx) * ((height + sx) >> sx);
-  if (!d_rgb.alloc(in_bytes) || !d_pl.alloc((ny + 2 * nc) * 2 * 2) ||
+  if (!d_rgb.alloc(rgb_on_device ? 1 : in_bytes) || !d_pl.alloc((ny + 2 * nc) * 2 * 2) ||
       !d_tab.alloc(2 * sizeof(mt_coef_costs) + 128) || !d_dec.alloc((size_t)nb * 2) ||
       !d_lv.alloc((size_t)nb * (64 + 2 * cl) * 4))
     return MT_ERR_DEVICE;
@@ -567,11 +609,17 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   uint8_t* d_qmy = reinterpret_cast<uint8_t*>(d_cc + 1);
   uint8_t* d_qmc = d_qmy + 64;
   cudaStream_t st = nullptr;
+  CallStats cs(stats);
+  cs.mark(0, st);
   if (rgb) {
-    if (cudaMemcpy(d_rgb.p, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
-    if ((rc = mt_csc_rgb8_device(d_rgb.as<uint8_t>(), (int)width, (int)height, sub, src[0], src[1], src[2], st)) !=
-        MT_OK)
-      return rc;
+    const uint8_t* d_in = rgb;
+    if (!rgb_on_device) {
+      if (cudaMemcpy(d_rgb.p, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+      cs.h2d(in_bytes);
+      d_in = d_rgb.as<uint8_t>();
+    }
+    if ((rc = mt_csc_rgb8_device(d_in, (int)width, (int)height, sub, src[0], src[1], src[2], st)) != MT_OK) return rc;
+    cs.launches(2);
   } else {
     const int cw = (int)((width + sx) >> sx), ch = (int)((height + sx) >> sx);
     uint8_t* d_in = d_rgb.as<uint8_t>();
@@ -583,12 +631,15 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
     pad_plane_kernel<<<dim3((pw + 127) / 128, ph), 128, 0, st>>>(d_in, (int)width, (int)height, src[0], pw, ph);
     pad_plane_kernel<<<dim3((pcw + 127) / 128, pch), 128, 0, st>>>(d_in + n0, cw, ch, src[1], pcw, pch);
     pad_plane_kernel<<<dim3((pcw + 127) / 128, pch), 128, 0, st>>>(d_in + n0 + n1, cw, ch, src[2], pcw, pch);
+    cs.h2d(n0 + 2 * n1);
+    cs.launches(3);
   }
   cudaMemsetAsync(d_tab.p, 32, 2 * sizeof(mt_coef_costs) + 128, st);  // flat QM weights past a 4x4 row
   cudaMemcpyAsync(d_cy, &cy, sizeof(cy), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_cc, &cc, sizeof(cc), cudaMemcpyHostToDevice, st);
   if (qmy) cudaMemcpyAsync(d_qmy, qmy, 64, cudaMemcpyHostToDevice, st);
   if (qmc) cudaMemcpyAsync(d_qmc, qmc, sub ? 16 : 64, cudaMemcpyHostToDevice, st);
+  cs.h2d(2 * sizeof(mt_coef_costs) + (qmy ? 64 : 0) + (qmc ? (sub ? 16 : 64) : 0));
   EncArgs a = {};
   for (int p = 0; p < 3; ++p) {
     a.src[p] = src[p];
@@ -687,8 +738,17 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   // one cluster per block that can run at once (the widest dependency level),
   // at most 64 clusters (two CTAs per SM)
   const int nclusters = std::min(width_max, 64);
+  cs.h2d(sched.size() * 4);
+  cs.mark(1, st);
   encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, st>>>(a, d_sched.as<uint32_t>(), nb, d_done,
                                                                            d_ctl, d_ctl + 1, d_cy, d_cc, d_qmy, d_qmc);
+  cs.mark(2, st);
+  cs.launches(1);
+  cs.d2h(4);
+  if (stats) {
+    stats->blocks = (uint32_t)nb;
+    stats->levels = (uint32_t)(lstart.size() - 1);
+  }
   uint32_t timed_out = 0;
   if (cudaMemcpyAsync(&timed_out, d_ctl + 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
@@ -698,6 +758,7 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   std::vector<uint8_t> mode(nb), tx(nb);
   if (cudaMemcpy(mode.data(), a.mode, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
   if (cudaMemcpy(tx.data(), a.tx, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.d2h(2 * (size_t)nb);
   // block syntax in coding order, with the coefficient blocks it carries
   mt_cdf_slot_layout L;
   mt_cdf_layout(&L);
@@ -722,6 +783,7 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   // the levels as the syntax walk reaches each block.
   std::vector<int32_t> lv((size_t)nb * (64 + 2 * cl));
   if (cudaMemcpy(lv.data(), a.lv_y, lv.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.d2h(lv.size() * 4);
   auto res_ctx_of = [&](const int32_t* cf, int n, int cls) -> uint8_t {
     static const uint8_t s4[16] = {0, 4, 1, 2, 5, 8, 12, 9, 6, 3, 7, 10, 13, 14, 11, 15};
     int eob = -1;
@@ -768,15 +830,19 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   if (cudaMemcpy(d_blocks, blocks.data(), (size_t)ncb * sizeof(mt_coef_block), cudaMemcpyHostToDevice) != cudaSuccess)
     return MT_ERR_DEVICE;
   if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, nullptr, nullptr, st)) != MT_OK) return rc;
+  cs.h2d((size_t)ncb * sizeof(mt_coef_block));
+  cs.launches(2);
   uint32_t total = 0;
   if (cudaMemcpy(&total, d_off + ncb, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
   DevBuf d_tok;
   if (!d_tok.alloc((size_t)total * 4)) return MT_ERR_DEVICE;
   if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok.as<uint32_t>(), nullptr, st)) != MT_OK)
     return rc;
+  cs.launches(1);
   std::vector<uint32_t> toks(total), offs((size_t)ncb + 1);
   if (cudaMemcpy(toks.data(), d_tok.p, (size_t)total * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
   if (cudaMemcpy(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.d2h(4 + (size_t)total * 4 + offs.size() * 4);
   // splice the coefficient tokens into the superblock streams
   std::vector<uint32_t> ops, sb_start(1, 0);
   std::vector<int32_t> cdef_pt;
@@ -823,6 +889,7 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   const size_t dbs = mt_deblock_frame_scratch_bytes(&g);
   if (!d_maps.alloc(maps.size()) || !d_db.alloc(dbs)) return MT_ERR_DEVICE;
   if (cudaMemcpy(d_maps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.h2d(maps.size());
   // the recon planes are kept: the filters run on a copy
   DevBuf d_flt;
   if (!d_flt.alloc((ny + 2 * nc) * 2)) return MT_ERR_DEVICE;
@@ -833,6 +900,13 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   if ((rc = mt_deblock_frame_device(flt[0], flt[1], flt[2], m0, m0 + n4, m0 + 2 * (size_t)n4, m0 + 3 * (size_t)n4,
                                     m0 + 4 * (size_t)n4, m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db.p, st)) != MT_OK)
     return rc;
+  {  // the deblocking launches: vertical and horizontal edges per filtered plane, the chroma geometry
+    const int vw4 = ((int)width + 3) / 4, vh4 = ((int)height + 3) / 4;
+    const int cw4 = (((int)width + sx) >> sx) / 4 + ((((int)width + sx) >> sx) % 4 != 0);
+    const int ch4 = (((int)height + sx) >> sx) / 4 + ((((int)height + sx) >> sx) % 4 != 0);
+    if (ly > 0) cs.launches((vw4 > 1) + (vh4 > 1));
+    if (ly > 0 && luv > 0) cs.launches(1 + 2 * ((cw4 > 1) + (ch4 > 1)));
+  }
   mt_cdef_params cp = {};
   cp.w8 = pw;
   cp.h8 = ph;
@@ -852,6 +926,11 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
     if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8.as<uint8_t>(), &cp, d_cs.p,
                                    &dec, grid.data(), st)) != MT_OK)
       return rc;
+    size_t cd2h = 0, ch2d = 0;
+    mth::cdef_frame_transfer_bytes(&cp, &cd2h, &ch2d);
+    cs.launches(mth::cdef_last_launches);
+    cs.d2h(cd2h);
+    if (mth::cdef_last_launches == 3) cs.h2d(ch2d);
   } else {
     dec.bits = -1;
   }
@@ -860,6 +939,7 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
         cudaMemcpy(recon_out[1], flt[1], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(recon_out[2], flt[2], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
       return MT_ERR_DEVICE;
+    cs.d2h((ny + 2 * nc) * 2);
   }
   // the tile, in one pass with each superblock's cdef_idx at its read_cdef()
   // point (the 64x64 CDEF units are the superblocks of the one tile)
@@ -927,25 +1007,34 @@ static int encode_impl(const uint8_t* rgb, const uint8_t* const* yuv, uint32_t w
   ip.max_pic_average_light_level = cfg->max_pic_average_light_level;
   rc = mt_wrap_av1_image(obu, obu_len, &ip, out, out_len);
   free(obu);
+  if (stats) stats->tokens = (uint32_t)ops.size();
+  cs.mark(3, st);
+  cs.finish();
   return rc;
 }
 
 int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
-                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
+                      uint8_t** out, size_t* out_len, uint16_t* recon_out[3], mt_encode_stats* stats) {
   if (!rgb) return MT_ERR_INVALID_INPUT;
-  return encode_impl(rgb, nullptr, width, height, cfg, out, out_len, recon_out);
+  return encode_impl(rgb, false, nullptr, width, height, cfg, out, out_len, recon_out, stats);
 }
 
 int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
                    size_t* out_len) {
-  return mt_encode_rgb8_ex(rgb, width, height, cfg, out, out_len, nullptr);
+  return mt_encode_rgb8_ex(rgb, width, height, cfg, out, out_len, nullptr, nullptr);
+}
+
+int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
+                          uint8_t** out, size_t* out_len, mt_encode_stats* stats) {
+  if (!d_rgb) return MT_ERR_INVALID_INPUT;
+  return encode_impl(d_rgb, true, nullptr, width, height, cfg, out, out_len, nullptr, stats);
 }
 
 int mt_encode_yuv8(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t width, uint32_t height,
                    const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
   const uint8_t* planes[3] = {y, u, v};
   if (!y || !u || !v) return MT_ERR_INVALID_INPUT;
-  return encode_impl(nullptr, planes, width, height, cfg, out, out_len, recon_out);
+  return encode_impl(nullptr, false, planes, width, height, cfg, out, out_len, recon_out, nullptr);
 }
 
 }  // extern "C"

@@ -24,18 +24,30 @@ def _planes_out(w, h, sub):
     return [np.zeros((ph, pw), np.uint16), np.zeros((pch, pcw), np.uint16), np.zeros((pch, pcw), np.uint16)]
 
 
-def encode_rgb8(rgb, cfg=None, want_recon=False):
+def encode_rgb8(rgb, cfg=None, want_recon=False, stats=None):
     """rgb: (h, w, 3) uint8.  Returns the AVIF bytes (and the decoder's output
-    planes, padded, when want_recon)."""
+    planes, padded, when want_recon); fills ``stats`` (abi.EncodeStats) when
+    given."""
     rgb = np.ascontiguousarray(rgb, np.uint8)
     h, w = rgb.shape[:2]
     cfg = cfg if cfg is not None else config()
     out, n = C.c_void_p(), C.c_size_t()
     planes = _planes_out(w, h, cfg.chroma == 0) if want_recon else None
     arr = (C.c_void_p * 3)(*[p.ctypes.data for p in planes]) if want_recon else None
-    _check(load().mt_encode_rgb8_ex(ptr(rgb), w, h, C.byref(cfg), C.byref(out), C.byref(n), arr), "mt_encode_rgb8")
+    _check(load().mt_encode_rgb8_ex(ptr(rgb), w, h, C.byref(cfg), C.byref(out), C.byref(n), arr,
+                                    C.byref(stats) if stats is not None else None), "mt_encode_rgb8")
     data = _take(out, n.value)
     return (data, planes) if want_recon else data
+
+
+def encode_rgb8_device(d_rgb, w, h, cfg=None, stats=None):
+    """The encode of interleaved RGB already in device memory (d_rgb: a device
+    pointer as an int, w * h * 3 bytes).  Returns the AVIF bytes."""
+    cfg = cfg if cfg is not None else config()
+    out, n = C.c_void_p(), C.c_size_t()
+    _check(load().mt_encode_rgb8_device(C.c_void_p(d_rgb), w, h, C.byref(cfg), C.byref(out), C.byref(n),
+                                        C.byref(stats) if stats is not None else None), "mt_encode_rgb8_device")
+    return _take(out, n.value)
 
 
 def encode_yuv8(y, u, v, cfg, want_recon=False):

@@ -20,6 +20,15 @@
 extern "C" {
 #endif
 
+/* The CDF groups the coefficient coders touch, as semantic slot numbers. */
+typedef struct or_emit_slots {
+  int32_t txb_skip[4], base_tok[4][2], br_tok[4][2], eob_base[4][2], eob_hi[4][2], dc_sign[2];
+  int32_t eob_bin, txtp4, txtp8, txtp16;
+} or_emit_slots;
+/* src/coeffs.rs coefficient coders over a block list (tokens of src/odec.rs:96-108). */
+int or_emit_coeffs(const int32_t* levels, const mt_coef_block* blocks, int32_t n, const or_emit_slots* S,
+                   uint32_t* tokens, size_t cap, uint32_t* offsets, uint8_t* res_ctx);
+
 int or_quant_init(uint8_t base_q_idx, uint8_t bd, uint8_t qm_level, mt_quant* out);
 int or_quant_init_chroma(uint8_t base_q_idx, int32_t dc_delta, int32_t ac_delta, uint8_t bd,
                          uint8_t qm_level, mt_quant* out);

@@ -14,13 +14,11 @@
 
 #include "../include/maroontree_b200.h"
 #include "../maroontree_b200/csrc/av1_tables.h"
+#include "oracle.h"
 
 namespace {
 
-struct EmitSlots {
-  int32_t txb_skip[4], base_tok[4][2], br_tok[4][2], eob_base[4][2], eob_hi[4][2], dc_sign[2];
-  int32_t eob_bin, txtp4, txtp8, txtp16;
-};
+using EmitSlots = or_emit_slots;
 
 struct Toks {
   std::vector<uint32_t> v;

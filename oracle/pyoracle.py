@@ -824,7 +824,9 @@ def cdfs_new_slots(qctx, sections=None):
     sec["uv_mode"] = len(out)
     rows(g["UV_MODE_NOCFL_CDF"])
     rows(g["UV_MODE_CFL_CDF"])
+    sec["angle_delta"] = len(out)
     rows(g["ANGLE_DELTA_CDF"])
+    sec["filter_intra"] = len(out)
     singles(g["FILTER_INTRA_CDF"])
     one(g["FILTER_INTRA_MODE_CDF"])
     sec["palette_y_mode"] = len(out)
