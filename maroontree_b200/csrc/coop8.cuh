@@ -43,11 +43,21 @@ struct CoopTabs {
   uint8_t scan[64];   // kScan8
   uint8_t iscan[64];  // kIScan8
   uint8_t loctx[32];  // kLoCtxOff
+  // vmask[rc] bit k: the rate walk's neighbour rc + {1, 8, 9, 2, 16}[k] lies in
+  // the block and comes later in the scan (so the reverse walk has already
+  // entered its level when it reaches rc)
+  uint8_t vmask[64];
   __device__ __forceinline__ void load(int t, int nthreads) {
     for (int i = t; i < 64; i += nthreads) {
       scan[i] = kScan8[i];
       iscan[i] = kIScan8[i];
       if (i < 25) loctx[i] = kLoCtxOff[i];
+      const int off[5] = {1, 8, 9, 2, 16};
+      uint8_t m = 0;
+#pragma unroll
+      for (int k = 0; k < 5; k++)
+        if (i + off[k] < 64 && kIScan8[i + off[k]] > kIScan8[i]) m |= (uint8_t)(1 << k);
+      vmask[i] = m;
     }
   }
 };
@@ -90,6 +100,208 @@ __device__ __forceinline__ void coop8_predict_row(const R& rd, const mt_chain_pa
                                                   int16_t* pred, int32_t* scratch, const Octet& g) {
   predict_sq_at<8>(rd, p.frame_w, p.frame_h, cd.px, cd.py, cd.mode, cd.angle_delta, cd.flags & 1,
                    (cd.flags >> 1) & 1, (cd.flags >> 2) & 1, p.bd, pred, scratch, g.j, g.j + 1);
+}
+
+// Shared scratch of the lane-parallel 8x8 predictor: the above and left edges
+// (logical index -2 .. 33 at offset 2, predict_sq_at's IntraEdge layout) and
+// their copies, which the edge filter and the upsampler read.
+struct Edge8 {
+  int32_t a[40], l[40], ca[40], cl[40];
+};
+
+// One output of filter_edge (src/intrapred.rs:977-1012) at position o of an
+// edge of `size` entries, from the unfiltered copy src[k] = e[k - 1].
+__device__ __forceinline__ int32_t edge_tap(const int32_t* src, int o, int size, int strength) {
+  const int32_t k0 = strength == 3 ? 2 : 0, k1 = strength == 1 ? 4 : (strength == 2 ? 5 : 4),
+                k2 = strength == 1 ? 8 : (strength == 2 ? 6 : 4);
+  const int last = size - 1;
+  const int32_t a = src[::max(o - 1, 0)], b = src[::min(::max(o, 0), last)], c = src[::min(o + 1, last)];
+  const int32_t d = src[::min(o + 2, last)], f = src[::min(o + 3, last)];
+  return (k0 * a + k1 * b + k2 * c + k1 * d + k0 * f + 8) >> 4;
+}
+
+// predict_sq_at<8> (intrapred.cuh) split over the octet: the edges are built,
+// filtered and upsampled position by position in E (each lane a few
+// positions from copies taken before the step), then lane j writes row j of
+// the prediction into pred (shared, row-major).  Same values as
+// predict_sq_at<8> for every mode, angle delta and availability.
+template <typename R>
+__device__ void coop8_predict(const R& rd, const mt_chain_params& p, const mt_candidate& cd, int16_t* pred, Edge8& E,
+                              const Octet& g) {
+  constexpr int bw = 8, bh = 8, edge_len = 16;
+  const int j = g.j, y = j;
+  const int ox = cd.px, oy = cd.py, mode = cd.mode;
+  const bool have_tr = cd.flags & 1, have_bl = (cd.flags >> 1) & 1, ft = (cd.flags >> 2) & 1;
+  const int bd = p.bd;
+  const bool have_top = oy > 0, have_left = ox > 0;
+  const int32_t base = 1 << (bd - 1);
+  int16_t* out = pred + y * 8;
+  if (mode == MT_DC_PRED) {  // dc_pred_sq_at: (n + sum) >> (log2n + 1), or one side >> log2n
+    const int32_t s = (have_top ? rd(ox + j, oy - 1) : 0) + (have_left ? rd(ox - 1, oy + j) : 0);
+    const int32_t sum = (int32_t)g.sum((unsigned)s);
+    const int32_t d = (have_top && have_left) ? (8 + sum) >> 4 : ((have_top || have_left) ? (4 + sum) >> 3 : base);
+#pragma unroll
+    for (int x = 0; x < 8; x++) out[x] = (int16_t)d;
+    return;
+  }
+  int32_t* A = E.a + 2;
+  int32_t* L = E.l + 2;
+  // edges: lane j fills positions j and 8 + j of each
+  if (have_top) {
+    const int px_have = have_tr ? ::min(bw, ::max(p.frame_w - (ox + bw), 0)) : 0;
+    A[j] = rd(ox + j, oy - 1);
+    A[8 + j] = rd(ox + 8 + (j < px_have ? j : px_have - 1), oy - 1);  // the last available sample repeated
+  } else {
+    const int32_t fill = have_left ? rd(ox - 1, oy) : base - 1;
+    A[j] = fill;
+    A[8 + j] = fill;
+  }
+  if (have_left) {
+    const int px_have = have_bl ? ::min(bh, ::max(p.frame_h - (oy + bh), 0)) : 0;
+    L[j] = rd(ox - 1, oy + j);
+    L[8 + j] = rd(ox - 1, oy + 8 + (j < px_have ? j : px_have - 1));
+  } else {
+    const int32_t fill = have_top ? rd(ox, oy - 1) : base + 1;
+    L[j] = fill;
+    L[8 + j] = fill;
+  }
+  const int32_t corner =
+      have_left ? (have_top ? rd(ox - 1, oy - 1) : rd(ox - 1, oy)) : (have_top ? rd(ox, oy - 1) : base);
+  if (j == 0) A[-1] = L[-1] = corner;
+  g.sync();
+  const bool directional = mode >= MT_V_PRED && mode <= MT_D67_PRED;
+  if (directional) {
+    const int base_angle = mode == MT_V_PRED ? 90 : mode == MT_H_PRED ? 180 : mode == MT_D45_PRED ? 45
+                         : mode == MT_D135_PRED ? 135 : mode == MT_D113_PRED ? 113 : mode == MT_D157_PRED ? 157
+                         : mode == MT_D203_PRED ? 203 : 67;
+    const int angle = base_angle + cd.angle_delta * 3;
+    int up_a = 0, up_l = 0;
+    if (angle != 90 && angle != 180) {  // (the corner filter needs edges of 24 or more)
+      const int sa = edge_strength(bw, bh, ft, angle - 90), sl = edge_strength(bh, bw, ft, angle - 180);
+      const int na = bw + 1 + (angle < 90 ? bh : 0), nl = bh + 1 + (angle > 180 ? bw : 0);
+      for (int k = j; k < 18; k += 8) {  // copies src[k] = e[k - 1]
+        E.ca[k] = A[k - 1];
+        E.cl[k] = L[k - 1];
+      }
+      g.sync();
+      if (sa)
+        for (int o = j; o < na - 1; o += 8) A[o] = edge_tap(E.ca, o, na, sa);
+      if (sl)
+        for (int o = j; o < nl - 1; o += 8) L[o] = edge_tap(E.cl, o, nl, sl);
+      g.sync();
+      const int da = abs(angle - 90), dl = abs(angle - 180), lim = ft ? 8 : 16;
+      up_a = (da != 0 && da < 40 && bw + bh <= lim);
+      up_l = (dl != 0 && dl < 40 && bw + bh <= lim);
+      if (up_a || up_l) {  // upsample_edge (src/intrapred.rs:1026-1048)
+        const int32_t maxv = (1 << bd) - 1;
+        const int numa = bw + (angle < 90 ? bh : 0), numl = bh + (angle > 180 ? bw : 0);
+        for (int k = j; k < 18; k += 8) {  // copies c[m] = e[m - 1], m = 0 .. num
+          if (up_a && k <= numa) E.ca[k] = A[k - 1];
+          if (up_l && k <= numl) E.cl[k] = L[k - 1];
+        }
+        g.sync();
+        auto in = [](const int32_t* c, int k, int num) { return c[k <= 1 ? 0 : ::min(k - 1, num)]; };
+        if (up_a) {
+          if (j == 0) A[-2] = E.ca[0];
+          for (int i = j; i < numa; i += 8) {
+            const int32_t v = -in(E.ca, i, numa) + 9 * in(E.ca, i + 1, numa) + 9 * in(E.ca, i + 2, numa) -
+                              in(E.ca, i + 3, numa);
+            A[2 * i - 1] = clampi((v + 8) >> 4, 0, maxv);
+            A[2 * i] = in(E.ca, i + 2, numa);
+          }
+        }
+        if (up_l) {
+          if (j == 0) L[-2] = E.cl[0];
+          for (int i = j; i < numl; i += 8) {
+            const int32_t v = -in(E.cl, i, numl) + 9 * in(E.cl, i + 1, numl) + 9 * in(E.cl, i + 2, numl) -
+                              in(E.cl, i + 3, numl);
+            L[2 * i - 1] = clampi((v + 8) >> 4, 0, maxv);
+            L[2 * i] = in(E.cl, i + 2, numl);
+          }
+        }
+        g.sync();
+      }
+    }
+    const int32_t* a = A;
+    const int32_t* l = L;
+    if (angle == 90) {
+#pragma unroll
+      for (int x = 0; x < 8; x++) out[x] = (int16_t)a[x];
+    } else if (angle == 180) {
+#pragma unroll
+      for (int x = 0; x < 8; x++) out[x] = (int16_t)l[y];
+    } else if (angle < 90) {
+      const int dx = kDrDeriv[angle >> 1];
+      const int max_base_x = (edge_len - 1) << up_a;
+      const int frac_bits = 6 - up_a, inc = 1 << up_a;
+      const int xpos = dx * (y + 1);
+      const int shift = ((xpos << up_a) & 0x3f) >> 1;
+      const int b0 = xpos >> frac_bits;
+#pragma unroll
+      for (int x = 0; x < 8; x++) {
+        const int b = b0 + x * inc;
+        out[x] = (int16_t)(b < max_base_x ? (a[b] * (32 - shift) + a[b + 1] * shift + 16) >> 5 : a[max_base_x]);
+      }
+    } else if (angle > 180) {
+      const int dy = kDrDeriv[(270 - angle) >> 1];
+      const int max_base_y = (edge_len - 1) << up_l;
+      const int frac_bits = 6 - up_l, inc = 1 << up_l;
+#pragma unroll
+      for (int x = 0; x < 8; x++) {
+        const int ypos = dy * (x + 1);
+        const int shift = ((ypos << up_l) & 0x3f) >> 1;
+        const int b = (ypos >> frac_bits) + y * inc;
+        out[x] = (int16_t)(b >= max_base_y ? l[max_base_y] : (l[b] * (32 - shift) + l[b + 1] * shift + 16) >> 5);
+      }
+    } else {
+      const int dy = kDrDeriv[(angle - 90) >> 1];
+      const int dx = kDrDeriv[(180 - angle) >> 1];
+      const int t = (y + 1) * dx - 64;
+      const int x0 = t <= 0 ? 0 : ::min((t + 63) >> 6, bw);
+      const int xpos0 = (x0 << 6) - (y + 1) * dx;
+      const int ba0 = xpos0 >> (6 - up_a);
+      const int sha = ((xpos0 * (1 << up_a)) & 0x3f) >> 1;
+#pragma unroll
+      for (int x = 0; x < 8; x++) {
+        if (x < x0) {
+          const int ypos = (y << 6) - (x + 1) * dy;
+          const int b = ypos >> (6 - up_l);
+          const int sh = ((ypos * (1 << up_l)) & 0x3f) >> 1;
+          out[x] = (int16_t)((l[b] * (32 - sh) + l[b + 1] * sh + 16) >> 5);
+        } else {
+          const int b = ba0 + (x - x0) * (1 << up_a);
+          out[x] = (int16_t)((a[b] * (32 - sha) + a[b + 1] * sha + 16) >> 5);
+        }
+      }
+    }
+    return;
+  }
+  const int32_t* a = A;
+  const int32_t* l = L;
+  if (mode == MT_PAETH_PRED) {
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+      const int32_t lv = l[y], tv = a[x], b = lv + tv - corner;
+      const int32_t ld = abs(lv - b), td = abs(tv - b), cdd = abs(corner - b);
+      out[x] = (int16_t)((ld <= td && ld <= cdd) ? lv : (td <= cdd ? tv : corner));
+    }
+  } else if (mode == MT_SMOOTH_PRED) {
+    const int32_t right = a[bw - 1], bottom = l[bh - 1];
+#pragma unroll
+    for (int x = 0; x < 8; x++) {
+      const int32_t wv = kSmW8[y], wh = kSmW8[x];
+      const int32_t pp = wv * a[x] + (256 - wv) * bottom + wh * l[y] + (256 - wh) * right;
+      out[x] = (int16_t)((pp + 256) >> 9);
+    }
+  } else if (mode == MT_SMOOTH_V_PRED) {
+    const int32_t bottom = l[bh - 1];
+#pragma unroll
+    for (int x = 0; x < 8; x++) out[x] = (int16_t)((kSmW8[y] * a[x] + (256 - kSmW8[y]) * bottom + 128) >> 8);
+  } else {  // SMOOTH_H
+    const int32_t right = a[bw - 1];
+#pragma unroll
+    for (int x = 0; x < 8; x++) out[x] = (int16_t)((kSmW8[x] * l[y] + (256 - kSmW8[x]) * right + 128) >> 8);
+  }
 }
 
 // Forward transform + quantisation (+ QM for the 2-D types) of src - pred
@@ -178,44 +390,68 @@ __device__ __forceinline__ void coop8_fwd(const uint16_t* __restrict__ src, int 
 __device__ __forceinline__ int coop8_eob(const Oct8& o, const CoopTabs& tb, const Octet& g) {
   int e1 = 0;
 #pragma unroll
-  for (int k = 0; k < 8; k++)
-    if (o.cf[tb.scan[k * 8 + g.j]] != 0) e1 = k * 8 + g.j + 1;
+  for (int y = 0; y < 8; y++) {
+    const int rc = g.j * 8 + y;
+    if (o.cf[rc] != 0) e1 = ::max(e1, (int)tb.iscan[rc] + 1);
+  }
   return g.max(e1) - 1;
 }
 
-// trellis8 over the octet.  Returns the final EOB scan index.
+// trellis8 over the octet, lane j holding column j of the block (positions
+// rc = 8j + y, y = 0..7, in registers).  Returns the final EOB scan index.
 __device__ __forceinline__ int coop8_trellis(Oct8& o, float dc_q, float ac_q, float lambda, const float* lut,
                                              const CoopTabs& tb, const Octet& g) {
   const int j = g.j;
   const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
-  const int m = coop8_eob(o, tb, g) + 1;
+  int32_t c[8];
+  float at[8];
+  int e[8];
+  int e1 = 0;
+#pragma unroll
+  for (int y = 0; y < 8; y++) {
+    const int rc = j * 8 + y;
+    c[y] = o.cf[rc];
+    at[y] = fabsf(o.tf[rc]);
+    e[y] = tb.iscan[rc];
+    if (c[y] != 0) e1 = ::max(e1, e[y] + 1);
+  }
+  const int m = g.max(e1);
   if (m == 0) return -1;
   const int full8 = m & ~7;
   const bool has4 = (m - full8) >= 4;
-  // step A: lane j decides scan position 8k + j of chunk k
-  for (int base = 0; base < m; base += 8) {
-    const int e = base + j;
-    const int rc = tb.scan[e];
-    const int32_t c = o.cf[rc];
-    const float at = fabsf(o.tf[rc]);
-    const bool in_chunk = base < full8 || (has4 && j < 4);  // an 8-wide or the 4-wide chunk
-    const bool big = g.any(in_chunk && uabs(c) > 63u);
-    bool dn = false;
-    if (e < m && c != 0) {
-      const float q2 = rc == 0 ? dq2 : aq2;
-      if (in_chunk && !big) {
-        const int32_t li = (int32_t)uabs(c), ldi = ::max(li - 1, 0);
-        const float el = __fsub_rn(at, (float)li), ed = __fsub_rn(at, (float)ldi);
+  // step A.  The reference decides each position of a chunk from the chunk's
+  // starting values, in the AVX2 FMA form unless the chunk holds a level
+  // above 63 (then, and in the scalar tail, the plain form): positions are
+  // independent given each chunk's flag (bits 0-7: the 8-wide chunks, bit 8:
+  // the 4-wide one).
+  unsigned bigb = 0;
+#pragma unroll
+  for (int y = 0; y < 8; y++) {
+    if (uabs(c[y]) > 63u && e[y] < m) {
+      if (e[y] < full8) bigb |= 1u << (e[y] >> 3);
+      else if (has4 && e[y] < full8 + 4) bigb |= 1u << 8;
+    }
+  }
+  const unsigned big = __reduce_or_sync(g.mask, bigb);
+#pragma unroll
+  for (int y = 0; y < 8; y++) {
+    if (e[y] < m && c[y] != 0) {
+      const float q2 = (j == 0 && y == 0) ? dq2 : aq2;
+      const bool fma_form = e[y] < full8 ? !((big >> (e[y] >> 3)) & 1) : (has4 && e[y] < full8 + 4 && !((big >> 8) & 1));
+      bool dn;
+      if (fma_form) {
+        const int32_t li = (int32_t)uabs(c[y]), ldi = ::max(li - 1, 0);
+        const float el = __fsub_rn(at[y], (float)li), ed = __fsub_rn(at[y], (float)ldi);
         const float cl = __fmaf_rn(q2, __fmul_rn(el, el), __fmul_rn(lambda, lut[li]));
         const float cd = __fmaf_rn(q2, __fmul_rn(ed, ed), __fmul_rn(lambda, lut[ldi]));
         dn = cd < cl;
       } else {
-        dn = round_down_plain(at, uabs(c), q2, lambda);
+        dn = round_down_plain(at[y], uabs(c[y]), q2, lambda);
       }
+      if (dn) c[y] = c[y] < 0 ? c[y] + 1 : c[y] - 1;
     }
-    if (dn) o.cf[rc] = (int16_t)(c < 0 ? c + 1 : c - 1);
   }
-  g.sync();
+  g.sync();  // every lane has read tf before R overwrites it
   // Terms of the two ordered float chains, by scan position e < m:
   //   S[e] = q2 * at^2 (the zeroing distortion; becomes the suffix sums),
   //   B[e] = q2 * (at - l)^2 (becomes the running prefix cost base_c),
@@ -223,41 +459,49 @@ __device__ __forceinline__ int coop8_trellis(Oct8& o, float dc_q, float ac_q, fl
   float* S = reinterpret_cast<float*>(o.t);
   float* B = o.x;
   float* R = o.tf;
-  float at_k[8];
-  uint32_t l_k[8];
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int e = k * 8 + j;
-    const int rc = tb.scan[e];
-    at_k[k] = fabsf(o.tf[rc]);
-    l_k[k] = uabs(o.cf[rc]);
-  }
-  g.sync();  // tf is overwritten by R below
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int e = k * 8 + j;
-    if (e < m) {
-      const float q2 = tb.scan[e] == 0 ? dq2 : aq2;
-      S[e] = __fmul_rn(q2, __fmul_rn(at_k[k], at_k[k]));
-      const float ecur = __fsub_rn(at_k[k], (float)l_k[k]);
-      B[e] = __fmul_rn(q2, __fmul_rn(ecur, ecur));
-      R[e] = __fmul_rn(lambda, l_k[k] < 64 ? lut[l_k[k]] : coef_rate_bits(l_k[k]));
+  for (int y = 0; y < 8; y++) {
+    if (e[y] < m) {
+      const float q2 = (j == 0 && y == 0) ? dq2 : aq2;
+      const uint32_t l = uabs(c[y]);
+      S[e[y]] = __fmul_rn(q2, __fmul_rn(at[y], at[y]));
+      const float ecur = __fsub_rn(at[y], (float)l);
+      B[e[y]] = __fmul_rn(q2, __fmul_rn(ecur, ecur));
+      R[e[y]] = __fmul_rn(lambda, l < 64 ? lut[l] : coef_rate_bits(l));
     }
   }
   g.sync();
   // Two ordered chains in one loop: lane 0 the suffix sums right to left
   // (acc += S[e]; S[e] = acc), lane 1 the prefix cost left to right
   // (base_c = pre + B[e]; B[e] = base_c; pre = base_c + R[e]).  Lane 0 adds
-  // +0 in the second step, which leaves its non-negative sum unchanged.
+  // +0 in the second step, which leaves its non-negative sum unchanged.  The
+  // terms are loaded eight at a time ahead of the ordered additions.
   if (j < 2) {
     if (j == 0) S[m] = 0.0f;
     float* arr = j == 0 ? S : B;
     float acc = 0.0f;
-    for (int s = 0; s < m; s++) {
-      const int e = j == 0 ? m - 1 - s : s;
-      const float r = __fadd_rn(acc, arr[e]);
-      arr[e] = r;
-      acc = __fadd_rn(r, j == 0 ? 0.0f : R[e]);
+    int s = 0;
+    for (; s + 8 <= m; s += 8) {
+      float v[8], r[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int ee = j == 0 ? m - 1 - (s + u) : s + u;
+        v[u] = arr[ee];
+        r[u] = j == 0 ? 0.0f : R[ee];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const int ee = j == 0 ? m - 1 - (s + u) : s + u;
+        const float x = __fadd_rn(acc, v[u]);
+        arr[ee] = x;
+        acc = __fadd_rn(x, r[u]);
+      }
+    }
+    for (; s < m; s++) {
+      const int ee = j == 0 ? m - 1 - s : s;
+      const float x = __fadd_rn(acc, arr[ee]);
+      arr[ee] = x;
+      acc = __fadd_rn(x, j == 0 ? 0.0f : R[ee]);
     }
   }
   g.sync();
@@ -265,23 +509,23 @@ __device__ __forceinline__ int coop8_trellis(Oct8& o, float dc_q, float ac_q, fl
   float best = __int_as_float(0x7f800000);
   int best_e = 64;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int e = k * 8 + j;
-    if (e < m && l_k[k] != 0) {
-      const int bin = e < 2 ? e : 32 - __clz(e);
+  for (int y = 0; y < 8; y++) {
+    if (e[y] < m && c[y] != 0) {
+      const int ee = e[y];
+      const int bin = ee < 2 ? ee : 32 - __clz(ee);
       const int extra = bin > 1 ? bin - 2 : 0;
       const float sig = __fadd_rn(__fmul_rn((float)bin, 0.9f), __fadd_rn((float)extra, 2.0f));
-      const float c = __fadd_rn(__fadd_rn(B[e], __fmul_rn(lambda, sig)), S[e + 1]);
-      if (c < best) {
-        best = c;
-        best_e = e;
+      const float cst = __fadd_rn(__fadd_rn(B[ee], __fmul_rn(lambda, sig)), S[ee + 1]);
+      if (cst < best || (cst == best && ee < best_e)) {
+        best = cst;
+        best_e = ee;
       }
     }
   }
 #pragma unroll
-  for (int s = 1; s < 8; s <<= 1) {
-    const float ob = __shfl_xor_sync(g.mask, best, s);
-    const int oe = __shfl_xor_sync(g.mask, best_e, s);
+  for (int sh = 1; sh < 8; sh <<= 1) {
+    const float ob = __shfl_xor_sync(g.mask, best, sh);
+    const int oe = __shfl_xor_sync(g.mask, best_e, sh);
     if (ob < best || (ob == best && oe < best_e)) {
       best = ob;
       best_e = oe;
@@ -290,10 +534,7 @@ __device__ __forceinline__ int coop8_trellis(Oct8& o, float dc_q, float ac_q, fl
   const float skip = __fadd_rn(S[0], lambda);
   const int keep = (best_e == 64 || skip < best) ? 0 : best_e + 1;
 #pragma unroll
-  for (int k = 0; k < 8; k++) {
-    const int e = k * 8 + j;
-    if (e >= keep && e < m) o.cf[tb.scan[e]] = 0;
-  }
+  for (int y = 0; y < 8; y++) o.cf[j * 8 + y] = (int16_t)((e[y] >= keep && e[y] < m) ? 0 : c[y]);
   g.sync();
   return keep - 1;
 }
@@ -372,13 +613,16 @@ __device__ __forceinline__ uint32_t coop8_satd(const uint16_t* __restrict__ src,
   return g.sum(satd);
 }
 
-// rate8 over the octet.  The level map the reference fills as its reverse
-// walk goes holds, at scan index i, level_byte(|level|) of exactly the
-// positions of scan index > i, so every position's context is known from the
-// final levels; the per-position terms go to shared memory and lane 0 adds
-// them in the walk's order (base token, then the br cost, then the golomb
-// cost; an absent term is +0, which leaves the positive sum unchanged).
-// Every lane returns the bits.
+// rate8 over the octet, lane j holding column j.  The level map the
+// reference fills as its reverse walk goes holds, at scan index i,
+// level_byte(|level|) of exactly the positions of scan index > i (its
+// neighbours are entered before it when they come later in the scan:
+// CoopTabs::vmask), so every position's context is known from the final
+// levels; the neighbours' level bytes come from the lanes of columns j + 1
+// and j + 2.  The per-position terms go to shared memory and lane 0 adds them
+// in the walk's order (base token, then the br cost, then the golomb cost; an
+// absent term is +0, which leaves the positive sum unchanged).  Every lane
+// returns the bits.
 __device__ __forceinline__ float coop8_rate(Oct8& o, int eob, const mt_coef_costs& T, int skip_ctx, int dcs,
                                             int mode, int tx, bool use_skip_bits, float skip1, float skip0,
                                             const CoopTabs& tb, const Octet& g) {
@@ -388,36 +632,52 @@ __device__ __forceinline__ float coop8_rate(Oct8& o, int eob, const mt_coef_cost
   float* T2 = o.x;
   float* T3 = reinterpret_cast<float*>(o.t);
   unsigned nz = 0;
-  if (eob > 0) {
-    auto lvb = [&](int p, int i) -> uint32_t {
-      return (p < 64 && (int)tb.iscan[p] > i) ? level_byte(uabs(o.cf[p])) : 0u;
-    };
+  uint32_t m[8], lb[8], lb1[8], lb2[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const int i = k * 8 + j;
+  for (int y = 0; y < 8; y++) {
+    m[y] = uabs(o.cf[j * 8 + y]);
+    lb[y] = level_byte(m[y]);
+  }
+#pragma unroll
+  for (int y = 0; y < 8; y++) {  // columns j + 1 and j + 2 (none past column 7)
+    const uint32_t v1 = __shfl_down_sync(g.mask, lb[y], 1, 8), v2 = __shfl_down_sync(g.mask, lb[y], 2, 8);
+    lb1[y] = j + 1 < 8 ? v1 : 0u;
+    lb2[y] = j + 2 < 8 ? v2 : 0u;
+  }
+  if (eob > 0) {
+#pragma unroll
+    for (int y = 0; y < 8; y++) {
+      const int rc = j * 8 + y;
+      const int i = tb.iscan[rc];
       if (i >= 1 && i < eob) {
-        const int rc = tb.scan[i];
-        const int x = rc >> 3, y = rc & 7;
-        const uint32_t hm = lvb(rc + 1, i) + lvb(rc + 8, i) + lvb(rc + 9, i);
-        const uint32_t mag = hm + lvb(rc + 2, i) + lvb(rc + 16, i);
-        const int ctx = tb.loctx[::min(y, 4) * 5 + ::min(x, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
-        const uint32_t m = uabs(o.cf[rc]);
-        const uint32_t tok = ::min(m, 3u);
+        const unsigned vm = tb.vmask[rc];
+        // neighbours rc + 1, + 8, + 9, + 2, + 16 (rc + 1 and + 2 run on into the next column)
+        const uint32_t n1 = y < 7 ? lb[y + 1] : lb1[0];
+        const uint32_t n8 = lb1[y];
+        const uint32_t n9 = y < 7 ? lb1[y + 1] : lb2[0];
+        const uint32_t n2 = y < 6 ? lb[y + 2] : lb1[y - 6];
+        const uint32_t n16 = lb2[y];
+        const uint32_t hm = ((vm & 1) ? n1 : 0u) + ((vm & 2) ? n8 : 0u) + ((vm & 4) ? n9 : 0u);
+        const uint32_t mag = hm + ((vm & 8) ? n2 : 0u) + ((vm & 16) ? n16 : 0u);
+        const int ctx = tb.loctx[::min(y, 4) * 5 + ::min(j, 4)] + (mag > 512 ? 4 : (int)((mag + 64) >> 7));
+        const uint32_t tok = ::min(m[y], 3u);
         T1[i] = T.base_tok[ctx][tok];
         float t2 = 0.0f, t3 = 0.0f;
         if (tok == 3) {
           const uint32_t hmag = hm & 63;
-          const int bc = ((y | x) > 1 ? 14 : 7) + (hmag > 12 ? 6 : (int)((hmag + 1) >> 1));
-          t2 = T.br_cum[bc][::min((int32_t)m - 3, 12)];
-          if (m >= 15) t3 = golomb_cost(m - 15);
+          const int bc = ((y | j) > 1 ? 14 : 7) + (hmag > 12 ? 6 : (int)((hmag + 1) >> 1));
+          t2 = T.br_cum[bc][::min((int32_t)m[y] - 3, 12)];
+          if (m[y] >= 15) t3 = golomb_cost(m[y] - 15);
         }
         T2[i] = t2;
         T3[i] = t3;
-        nz += m != 0;
+        nz += m[y] != 0;
       }
     }
     nz = g.sum(nz);
   }
+  // the DC context's neighbours (0, 1), (1, 0), (1, 1): lane 0's column and lane 1's
+  const uint32_t dcmag = (lb[1] + lb1[0] + lb1[1]) & 63;
   g.sync();
   float bits = 0.0f;
   if (j == 0) {
@@ -425,12 +685,12 @@ __device__ __forceinline__ float coop8_rate(Oct8& o, int eob, const mt_coef_cost
     bits = __fadd_rn(bits, T.txtp[mode][tx]);
     const float* dcs_c = T.dc_sign[dcs];
     if (eob == 0) {
-      const uint32_t m = uabs(o.cf[0]), mm = ::min(m, 3u);
+      const uint32_t mm = ::min(m[0], 3u);
       bits = __fadd_rn(bits, T.eob_bin[0]);
       bits = __fadd_rn(bits, T.eob_base[0][mm - 1]);
       if (mm == 3) {
-        float h = T.br_cum[0][::min((int32_t)m - 3, 12)];
-        if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+        float h = T.br_cum[0][::min((int32_t)m[0] - 3, 12)];
+        if (m[0] >= 15) h = __fadd_rn(h, golomb_cost(m[0] - 15));
         bits = __fadd_rn(bits, h);
       }
       bits = __fadd_rn(bits, dcs_c[o.cf[0] < 0]);
@@ -446,26 +706,26 @@ __device__ __forceinline__ float coop8_rate(Oct8& o, int eob, const mt_coef_cost
       {
         const int rc = tb.scan[eob];
         const int ex = rc >> 3, ey = rc & 7;
-        const uint32_t m = uabs(o.cf[rc]);
-        const uint32_t tok = ::min(m, 3u) - 1;
+        const uint32_t me = uabs(o.cf[rc]);
+        const uint32_t tok = ::min(me, 3u) - 1;
         bits = __fadd_rn(bits, T.eob_base[ctx_e][tok]);
         if (tok == 2) {
-          float h = T.br_cum[(ex | ey) > 1 ? 14 : 7][::min((int32_t)m - 3, 12)];
-          if (m >= 15) h = __fadd_rn(h, golomb_cost(m - 15));
+          float h = T.br_cum[(ex | ey) > 1 ? 14 : 7][::min((int32_t)me - 3, 12)];
+          if (me >= 15) h = __fadd_rn(h, golomb_cost(me - 15));
           bits = __fadd_rn(bits, h);
         }
       }
       int i = eob - 1;
-      for (; i >= 4; i -= 4) {  // loads ahead of the ordered additions
-        float a[4], b2[4], c3[4];
+      for (; i >= 8; i -= 8) {  // loads ahead of the ordered additions
+        float a[8], b2[8], c3[8];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < 8; u++) {
           a[u] = T1[i - u];
           b2[u] = T2[i - u];
           c3[u] = T3[i - u];
         }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < 8; u++) {
           bits = __fadd_rn(bits, a[u]);
           bits = __fadd_rn(bits, b2[u]);
           bits = __fadd_rn(bits, c3[u]);
@@ -476,11 +736,10 @@ __device__ __forceinline__ float coop8_rate(Oct8& o, int eob, const mt_coef_cost
         bits = __fadd_rn(bits, T2[i]);
         bits = __fadd_rn(bits, T3[i]);
       }
-      const uint32_t dm = uabs(o.cf[0]), dtok = ::min(dm, 3u);
+      const uint32_t dm = m[0], dtok = ::min(dm, 3u);
       bits = __fadd_rn(bits, T.base_tok[0][dtok]);
       if (dtok == 3) {
-        const uint32_t mag = (level_byte(uabs(o.cf[1])) + level_byte(uabs(o.cf[8])) + level_byte(uabs(o.cf[9]))) & 63;
-        float h = T.br_cum[mag > 12 ? 6 : (int)((mag + 1) >> 1)][::min((int32_t)dm - 3, 12)];
+        float h = T.br_cum[dcmag > 12 ? 6 : (int)((dcmag + 1) >> 1)][::min((int32_t)dm - 3, 12)];
         if (dm >= 15) h = __fadd_rn(h, golomb_cost(dm - 15));
         bits = __fadd_rn(bits, h);
       }

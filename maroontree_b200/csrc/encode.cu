@@ -134,6 +134,7 @@ struct StepShared {
   int16_t cpred[64];                // the chroma DC prediction (4:4:4)
   uint16_t src[64], csrc[64];       // the block's luma and chroma source samples
   int16_t above[2][17], left[2][16];  // the block's luma / chroma neighbours (mtd::EdgeRead)
+  mtd::Edge8 edge[5];                 // the edges of the four luma predictions and the chroma one
   unsigned long long best;
   uint32_t ticket, abort;
   mtd::Oct8 oct[kLumaThreads / 8 + 1];  // one per candidate octet, then the chroma plane's
@@ -290,9 +291,8 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
       cd.flags = flags | (ft ? 4 : 0);
       const mtd::EdgeRead rd{S.above[0], S.left[0], px, py};
       if (o < 4 && mlo + o < 13) {
-        int32_t scratch[3 * mtd::kEdgeCap8];
         cd.mode = (uint8_t)(mlo + o);
-        mtd::coop8_predict_row(rd, a.py, cd, S.pred[o], scratch, g);
+        mtd::coop8_predict(rd, a.py, cd, S.pred[o], S.edge[o], g);
       }
       luma_bar();
       const int ci = kOrder.t[rank][o];
@@ -314,8 +314,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
         cc.flags = flags;
         cc.mode = MT_DC_PRED;
         cc.tx_type = MT_TX_DCT_DCT;
-        int32_t scratch[3 * mtd::kEdgeCap8];
-        mtd::coop8_predict_row(mtd::EdgeRead{S.above[1], S.left[1], px, py}, a.pc, cc, S.cpred, scratch, g);
+        mtd::coop8_predict(mtd::EdgeRead{S.above[1], S.left[1], px, py}, a.pc, cc, S.cpred, S.edge[4], g);
         g.sync();
         mt_candidate_result r;
         mtd::Oct8& oc = S.oct[kLumaThreads / 8];
