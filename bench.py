@@ -824,9 +824,9 @@ def run_ours(args):
 
     secondary = {}
     cpu = parity = None
-    if rank == 0:
+    nocpu = world > 1 or args.no_cpu
+    if rank == 0 and not args.headline_only:
         wl = make_workload()
-        nocpu = world > 1 or args.no_cpu
         secondary["level8"] = measure_level8(dev, wl, args.steps, args.warmup, op_peak, hbm_peak, not nocpu)
         secondary["frame_filters"] = measure_filters(dev, wl, hbm_peak)
         secondary["level4"] = measure_small_level(dev, wl, 4, cpu=not nocpu)
@@ -838,18 +838,18 @@ def run_ours(args):
         leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n16=True)
         leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=not nocpu, n16=True)
         secondary["leaf8"] = leaf8
-        if not nocpu:
-            from oracle import build as obuild
+    if rank == 0 and not nocpu:
+        from oracle import build as obuild
 
-            obuild.build()
-            threads = os.cpu_count() or 1
-            want, dt = oracle_encode(rgb, threads)
-            cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
-                   "sample": f"one whole 1920x1080 encode by the oracle ({dt:.2f} s)"}
-            # the timed encode's file must be the oracle encode's, byte for byte
-            parity = {"avif_bytes_equal_oracle": avif == want, "bytes": len(avif)}
-            if avif != want:
-                raise SystemExit("bench: the GPU encode's file differs from the oracle encode's")
+        obuild.build()
+        threads = os.cpu_count() or 1
+        want, dt = oracle_encode(rgb, threads)
+        cpu = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+               "sample": f"one whole 1920x1080 encode by the oracle ({dt:.2f} s)"}
+        # the timed encode's file must be the oracle encode's, byte for byte
+        parity = {"avif_bytes_equal_oracle": avif == want, "bytes": len(avif)}
+        if avif != want:
+            raise SystemExit("bench: the GPU encode's file differs from the oracle encode's")
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "MPix/s",
@@ -893,6 +893,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--headline-only", action="store_true", help="skip the secondary kernel-level measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

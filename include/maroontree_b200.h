@@ -1234,6 +1234,12 @@ int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const
  * host memory. */
 int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
                           uint8_t** out, size_t* out_len, mt_encode_stats* stats);
+/* The encode calls of a device reuse one set of device buffers (grown to the
+ * largest frame seen; a call that finds the set taken by another thread's
+ * call allocates its own).  This frees every device's set; the next call
+ * allocates again.  No counterpart in the reference, whose buffers are host
+ * memory freed per call. */
+void mt_encode_release_buffers(void);
 /* The same encode from 8-bit Y, U, V planes (chroma at ((w + sx) >> sx) x
  * ((h + sy) >> sy)), without colour conversion: the planes are coded as
  * given and described by the config's CICP (e.g. identity for G, B, R). */

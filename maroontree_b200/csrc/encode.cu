@@ -27,6 +27,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "../../include/maroontree_b200.h"
@@ -380,6 +381,38 @@ __global__ void pad_plane_kernel(const uint8_t* __restrict__ in, int w, int h, u
   out[(size_t)y * pw + x] = in[(size_t)min(y, h - 1) * w + min(x, w - 1)];
 }
 
+// The coefficient context byte each transform block leaves for its
+// neighbours (src/coeffs.rs eob_and_cul): min(sum of |levels| up to the end
+// of block, 63) | the DC sign bits, 0x40 when all levels are zero; the sum
+// runs in the block's coding order (the 2-D scan, or the 1-D classes' row /
+// column order).  res[3 b + p] for 8x8 block b and plane p.
+__global__ void res_ctx_kernel(const int32_t* __restrict__ lv_y, const int32_t* __restrict__ lv_u,
+                               const int32_t* __restrict__ lv_v, const uint8_t* __restrict__ tx, int nb, int sub,
+                               uint8_t* __restrict__ res) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * nb) return;
+  const int b = i / 3, p = i % 3;
+  const int n = (p == 0 || sub == 0) ? 8 : 4, cl = sub ? 16 : 64;
+  const int32_t* cf = p == 0 ? lv_y + (size_t)b * 64 : (p == 1 ? lv_u : lv_v) + (size_t)b * cl;
+  const int cls = p == 0 ? (tx[b] == MT_TX_V_DCT ? 1 : (tx[b] == MT_TX_H_DCT ? 2 : 0)) : 0;
+  auto at = [&](int k) -> int {
+    if (cls == 1) return ((k & (n - 1)) * n) + k / n;  // vertical class order
+    if (cls == 2) return k;
+    return n == 4 ? mtd::kScan4[k] : mtd::kScan8[k];
+  };
+  int eob = -1;
+  for (int k = 0; k < n * n; ++k)
+    if (cf[at(k)]) eob = k;
+  if (eob < 0) {
+    res[i] = 0x40;
+    return;
+  }
+  uint32_t cul = 0;
+  for (int k = 0; k <= eob; ++k) cul += (uint32_t)abs(cf[at(k)]);
+  const uint8_t dcb = cf[0] == 0 ? 0x40 : (cf[0] < 0 ? 0 : 0x80);
+  res[i] = (uint8_t)((cul < 63 ? cul : 63) | dcb);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -495,12 +528,48 @@ struct BlockSyntax {
   }
 };
 
-struct DevBuf {
-  void* p = nullptr;
-  ~DevBuf() { cudaFree(p); }
+// The device buffers of an encode call.  Each device keeps one set (grown to
+// the largest frame seen, held until mt_encode_release_buffers or exit) that a
+// call uses when no other call on that device holds it; a call that finds it
+// taken allocates its own.  Every call's device work is ordered on the legacy
+// default stream, so a set is reused only after the previous call's work.
+constexpr int kSlots = 16;
+enum Slot { kRgb, kPlanes, kTables, kDecisions, kLevels, kSched, kEmit, kTokens, kMaps, kDeblock, kFiltered, kSkip8,
+            kCdef, kRes };
+struct Arena {
+  std::mutex mu;
+  void* p[kSlots] = {};
+  size_t cap[kSlots] = {};
+};
+Arena g_arenas[16];
+
+struct Buffers {
+  Arena* ar = nullptr;
+  void* own[kSlots] = {};
+  Buffers() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 16 && g_arenas[dev].mu.try_lock()) ar = &g_arenas[dev];
+  }
+  ~Buffers() {
+    if (ar) ar->mu.unlock();
+    for (void* q : own) cudaFree(q);
+  }
   template <class T>
-  T* as() const { return reinterpret_cast<T*>(p); }
-  bool alloc(size_t n) { return cudaMalloc(&p, n ? n : 1) == cudaSuccess; }
+  T* get(Slot s, size_t n) {
+    n = n ? n : 1;
+    if (ar) {
+      if (ar->cap[s] < n) {
+        cudaFree(ar->p[s]);
+        ar->p[s] = nullptr;
+        ar->cap[s] = 0;
+        if (cudaMalloc(&ar->p[s], n) != cudaSuccess) return nullptr;
+        ar->cap[s] = n;
+      }
+      return reinterpret_cast<T*>(ar->p[s]);
+    }
+    if (cudaMalloc(&own[s], n) != cudaSuccess) return nullptr;
+    return reinterpret_cast<T*>(own[s]);
+  }
 };
 
 // The stats of one call: copies, launches and CUDA-event times (the events
@@ -594,16 +663,19 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   const uint8_t* qmc = mt_qm_row(plan.qm_u, 1, sub ? 4 : 8, sub ? 4 : 8);
   // device buffers
   const size_t ny = (size_t)pw * ph, nc = (size_t)pcw * pch;
-  DevBuf d_rgb, d_pl, d_tab, d_dec, d_lv, d_emit, d_maps, d_skip8;
+  Buffers buf;
   const size_t in_bytes = rgb ? (size_t)width * height * 3
                               : (size_t)width * height + 2 * (size_t)((width + sx) >> sx) * ((height + sx) >> sx);
-  if (!d_rgb.alloc(rgb_on_device ? 1 : in_bytes) || !d_pl.alloc((ny + 2 * nc) * 2 * 2) ||
-      !d_tab.alloc(2 * sizeof(mt_coef_costs) + 128) || !d_dec.alloc((size_t)nb * 2) ||
-      !d_lv.alloc((size_t)nb * (64 + 2 * cl) * 4))
-    return MT_ERR_DEVICE;
-  uint16_t* src[3] = {d_pl.as<uint16_t>(), d_pl.as<uint16_t>() + ny, d_pl.as<uint16_t>() + ny + nc};
+  uint8_t* d_rgbbuf = buf.get<uint8_t>(kRgb, rgb_on_device ? 1 : in_bytes);
+  uint16_t* d_planes = buf.get<uint16_t>(kPlanes, (ny + 2 * nc) * 2 * 2);
+  uint8_t* d_tabs = buf.get<uint8_t>(kTables, 2 * sizeof(mt_coef_costs) + 128);
+  uint8_t* d_decs = buf.get<uint8_t>(kDecisions, (size_t)nb * 2);
+  int32_t* d_levels = buf.get<int32_t>(kLevels, (size_t)nb * (64 + 2 * cl) * 4);
+  uint8_t* d_res = buf.get<uint8_t>(kRes, (size_t)nb * 3);
+  if (!d_rgbbuf || !d_planes || !d_tabs || !d_decs || !d_levels || !d_res) return MT_ERR_DEVICE;
+  uint16_t* src[3] = {d_planes, d_planes + ny, d_planes + ny + nc};
   uint16_t* rec[3] = {src[2] + nc, src[2] + nc + ny, src[2] + nc + ny + nc};
-  mt_coef_costs* d_cy = d_tab.as<mt_coef_costs>();
+  mt_coef_costs* d_cy = reinterpret_cast<mt_coef_costs*>(d_tabs);
   mt_coef_costs* d_cc = d_cy + 1;
   uint8_t* d_qmy = reinterpret_cast<uint8_t*>(d_cc + 1);
   uint8_t* d_qmc = d_qmy + 64;
@@ -613,15 +685,15 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   if (rgb) {
     const uint8_t* d_in = rgb;
     if (!rgb_on_device) {
-      if (cudaMemcpy(d_rgb.p, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+      if (cudaMemcpy(d_rgbbuf, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
       cs.h2d(in_bytes);
-      d_in = d_rgb.as<uint8_t>();
+      d_in = d_rgbbuf;
     }
     if ((rc = mt_csc_rgb8_device(d_in, (int)width, (int)height, sub, src[0], src[1], src[2], st)) != MT_OK) return rc;
     cs.launches(2);
   } else {
     const int cw = (int)((width + sx) >> sx), ch = (int)((height + sx) >> sx);
-    uint8_t* d_in = d_rgb.as<uint8_t>();
+    uint8_t* d_in = d_rgbbuf;
     const size_t n0 = (size_t)width * height, n1 = (size_t)cw * ch;
     if (cudaMemcpy(d_in, yuv[0], n0, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(d_in + n0, yuv[1], n1, cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -633,7 +705,7 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     cs.h2d(n0 + 2 * n1);
     cs.launches(3);
   }
-  cudaMemsetAsync(d_tab.p, 32, 2 * sizeof(mt_coef_costs) + 128, st);  // flat QM weights past a 4x4 row
+  cudaMemsetAsync(d_tabs, 32, 2 * sizeof(mt_coef_costs) + 128, st);  // flat QM weights past a 4x4 row
   cudaMemcpyAsync(d_cy, &cy, sizeof(cy), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_cc, &cc, sizeof(cc), cudaMemcpyHostToDevice, st);
   if (qmy) cudaMemcpyAsync(d_qmy, qmy, 64, cudaMemcpyHostToDevice, st);
@@ -669,9 +741,9 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   a.sb_cols = sb_cols;
   a.w8 = pw;
   a.h8 = ph;
-  a.mode = d_dec.as<uint8_t>();
+  a.mode = d_decs;
   a.tx = a.mode + nb;
-  a.lv_y = d_lv.as<int32_t>();
+  a.lv_y = d_levels;
   a.lv_u = a.lv_y + (size_t)nb * 64;
   a.lv_v = a.lv_u + (size_t)nb * cl;
   if (cudaMemsetAsync(a.mode, 0, (size_t)nb * 2, st) != cudaSuccess) return MT_ERR_DEVICE;
@@ -727,11 +799,11 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   // counter and the wait-timeout flag
   int width_max = 1;
   for (size_t l = 0; l + 1 < lstart.size(); ++l) width_max = std::max(width_max, lstart[l + 1] - lstart[l]);
-  DevBuf d_sched;
-  if (!d_sched.alloc(sched.size() * 4 + ((size_t)nb + 2) * 4)) return MT_ERR_DEVICE;
-  uint32_t* d_done = d_sched.as<uint32_t>() + sched.size();
+  uint32_t* d_sched = buf.get<uint32_t>(kSched, sched.size() * 4 + ((size_t)nb + 2) * 4);
+  if (!d_sched) return MT_ERR_DEVICE;
+  uint32_t* d_done = d_sched + sched.size();
   uint32_t* d_ctl = d_done + nb;  // [0] ticket counter, [1] timeout flag
-  if (cudaMemcpyAsync(d_sched.p, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+  if (cudaMemcpyAsync(d_sched, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemsetAsync(d_done, 0, ((size_t)nb + 2) * 4, st) != cudaSuccess)
     return MT_ERR_DEVICE;
   // one cluster per block that can run at once (the widest dependency level),
@@ -739,7 +811,7 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   const int nclusters = std::min(width_max, 64);
   cs.h2d(sched.size() * 4);
   cs.mark(1, st);
-  encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, st>>>(a, d_sched.as<uint32_t>(), nb, d_done,
+  encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, st>>>(a, d_sched, nb, d_done,
                                                                            d_ctl, d_ctl + 1, d_cy, d_cc, d_qmy, d_qmc);
   cs.mark(2, st);
   cs.launches(1);
@@ -777,29 +849,15 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     bs.l_coef[p].assign(nby * 2, 0x40);
   }
   bs.blocks = &blocks;
-  // The coefficient contexts of a block depend on its neighbours' res_ctx
-  // bytes, which depend on their levels only: compute them on the host from
-  // the levels as the syntax walk reaches each block.
-  std::vector<int32_t> lv((size_t)nb * (64 + 2 * cl));
-  if (cudaMemcpy(lv.data(), a.lv_y, lv.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  cs.d2h(lv.size() * 4);
-  auto res_ctx_of = [&](const int32_t* cf, int n, int cls) -> uint8_t {
-    static const uint8_t s4[16] = {0, 4, 1, 2, 5, 8, 12, 9, 6, 3, 7, 10, 13, 14, 11, 15};
-    int eob = -1;
-    auto at = [&](int i) -> int {
-      if (cls == 1) return ((i & (n - 1)) * n) + i / n;  // vertical class order
-      if (cls == 2) return i;
-      return n == 4 ? s4[i] : MT_SCAN_8X8[i];
-    };
-    for (int i = 0; i < n * n; ++i)
-      if (cf[at(i)]) eob = i;
-    if (eob < 0) return 0x40;
-    uint32_t cul = 0;
-    for (int i = 0; i <= eob; ++i) cul += (uint32_t)abs(cf[at(i)]);
-    const uint8_t dcb = cf[0] == 0 ? 0x40 : (cf[0] < 0 ? 0 : 0x80);
-    return (uint8_t)((cul < 63 ? cul : 63) | dcb);
-  };
-  std::vector<uint32_t> coef_off;  // per coefficient block: offset of its levels in lv
+  // The coefficient contexts of a block depend on its neighbours' context
+  // bytes, which depend on their levels only: computed on the device for
+  // every transform block, read back as three bytes per 8x8 block.
+  res_ctx_kernel<<<(unsigned)((3 * (size_t)nb + 255) / 256), 256, 0, st>>>(a.lv_y, a.lv_u, a.lv_v, a.tx, nb, sub,
+                                                                           d_res);
+  cs.launches(1);
+  std::vector<uint8_t> resb((size_t)nb * 3);
+  if (cudaMemcpy(resb.data(), d_res, resb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.d2h(resb.size());
   for (int sr = 0; sr < sb_rows; ++sr)
     for (int sc = 0; sc < sb_cols; ++sc) {
       bs.sbs.emplace_back();
@@ -811,19 +869,15 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
         const int b = y8 * nbx + x8;
         const uint32_t off[3] = {(uint32_t)((size_t)b * 64), (uint32_t)((size_t)nb * 64 + (size_t)b * cl),
                                  (uint32_t)((size_t)nb * (64 + cl) + (size_t)b * cl)};
-        uint8_t r[3];
-        for (int p = 0; p < 3; ++p) {
-          blocks[first + p].cf_offset = off[p];
-          r[p] = res_ctx_of(&lv[off[p]], p == 0 || sub == 0 ? 8 : 4, blocks[first + p].tx_class);
-        }
-        bs.commit_res(x8, y8, r);
+        for (int p = 0; p < 3; ++p) blocks[first + p].cf_offset = off[p];
+        bs.commit_res(x8, y8, &resb[(size_t)b * 3]);
       });
       bs.cdef_points.push_back(cp);
     }
   // coefficient tokens of every block in one launch
   const int ncb = (int)blocks.size();
-  if (!d_emit.alloc((size_t)ncb * (sizeof(mt_coef_block) + 8) + 8)) return MT_ERR_DEVICE;
-  mt_coef_block* d_blocks = d_emit.as<mt_coef_block>();
+  mt_coef_block* d_blocks = buf.get<mt_coef_block>(kEmit, (size_t)ncb * (sizeof(mt_coef_block) + 8) + 8);
+  if (!d_blocks) return MT_ERR_DEVICE;
   uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d_blocks + ncb);
   uint32_t* d_off = d_cnt + ncb;
   if (cudaMemcpy(d_blocks, blocks.data(), (size_t)ncb * sizeof(mt_coef_block), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -833,13 +887,13 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   cs.launches(2);
   uint32_t total = 0;
   if (cudaMemcpy(&total, d_off + ncb, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  DevBuf d_tok;
-  if (!d_tok.alloc((size_t)total * 4)) return MT_ERR_DEVICE;
-  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok.as<uint32_t>(), nullptr, st)) != MT_OK)
+  uint32_t* d_tok = buf.get<uint32_t>(kTokens, (size_t)total * 4);
+  if (!d_tok) return MT_ERR_DEVICE;
+  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok, nullptr, st)) != MT_OK)
     return rc;
   cs.launches(1);
   std::vector<uint32_t> toks(total), offs((size_t)ncb + 1);
-  if (cudaMemcpy(toks.data(), d_tok.p, (size_t)total * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
+  if (cudaMemcpy(toks.data(), d_tok, (size_t)total * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
   if (cudaMemcpy(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
   cs.d2h(4 + (size_t)total * 4 + offs.size() * 4);
   // splice the coefficient tokens into the superblock streams
@@ -884,20 +938,22 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   g.disp_h = (int)height;
   g.sub_x = g.sub_y = sx;
   g.bd = 8;
-  DevBuf d_db;
+
   const size_t dbs = mt_deblock_frame_scratch_bytes(&g);
-  if (!d_maps.alloc(maps.size()) || !d_db.alloc(dbs)) return MT_ERR_DEVICE;
-  if (cudaMemcpy(d_maps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+  uint8_t* d_maps = buf.get<uint8_t>(kMaps, maps.size());
+  void* d_db = buf.get<void>(kDeblock, dbs);
+  if (!d_maps || !d_db) return MT_ERR_DEVICE;
+  if (cudaMemcpy(d_maps, maps.data(), maps.size(), cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
   cs.h2d(maps.size());
   // the recon planes are kept: the filters run on a copy
-  DevBuf d_flt;
-  if (!d_flt.alloc((ny + 2 * nc) * 2)) return MT_ERR_DEVICE;
-  uint16_t* flt[3] = {d_flt.as<uint16_t>(), d_flt.as<uint16_t>() + ny, d_flt.as<uint16_t>() + ny + nc};
+  uint16_t* d_flt = buf.get<uint16_t>(kFiltered, (ny + 2 * nc) * 2);
+  if (!d_flt) return MT_ERR_DEVICE;
+  uint16_t* flt[3] = {d_flt, d_flt + ny, d_flt + ny + nc};
   if (cudaMemcpyAsync(flt[0], rec[0], (ny + 2 * nc) * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     return MT_ERR_DEVICE;
-  const uint8_t* m0 = d_maps.as<uint8_t>();
+  const uint8_t* m0 = d_maps;
   if ((rc = mt_deblock_frame_device(flt[0], flt[1], flt[2], m0, m0 + n4, m0 + 2 * (size_t)n4, m0 + 3 * (size_t)n4,
-                                    m0 + 4 * (size_t)n4, m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db.p, st)) != MT_OK)
+                                    m0 + 4 * (size_t)n4, m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db, st)) != MT_OK)
     return rc;
   {  // the deblocking launches: vertical and horizontal edges per filtered plane, the chroma geometry
     const int vw4 = ((int)width + 3) / 4, vh4 = ((int)height + 3) / 4;
@@ -915,14 +971,16 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   cp.base_q_idx = plan.base_q_idx;
   cp.bd = 8;
   cp.slow = cfg->speed <= MT_SPEED_SLOW;
-  DevBuf d_cs;
+
   const int unit_cols = (pw + 63) / 64, unit_rows = (ph + 63) / 64;
-  if (!d_skip8.alloc((size_t)nb) || !d_cs.alloc(mt_cdef_scratch_bytes(&cp))) return MT_ERR_DEVICE;
-  if (cudaMemsetAsync(d_skip8.p, 0, (size_t)nb, st) != cudaSuccess) return MT_ERR_DEVICE;
+  uint8_t* d_skip8 = buf.get<uint8_t>(kSkip8, (size_t)nb);
+  void* d_cs = buf.get<void>(kCdef, mt_cdef_scratch_bytes(&cp));
+  if (!d_skip8 || !d_cs) return MT_ERR_DEVICE;
+  if (cudaMemsetAsync(d_skip8, 0, (size_t)nb, st) != cudaSuccess) return MT_ERR_DEVICE;
   mt_cdef_decision dec = {};
   std::vector<uint8_t> grid((size_t)unit_cols * unit_rows);
   if (plan.cdef) {
-    if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8.as<uint8_t>(), &cp, d_cs.p,
+    if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8, &cp, d_cs,
                                    &dec, grid.data(), st)) != MT_OK)
       return rc;
     size_t cd2h = 0, ch2d = 0;
@@ -1027,6 +1085,25 @@ int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height,
                           uint8_t** out, size_t* out_len, mt_encode_stats* stats) {
   if (!d_rgb) return MT_ERR_INVALID_INPUT;
   return encode_impl(d_rgb, true, nullptr, width, height, cfg, out, out_len, nullptr, stats);
+}
+
+void mt_encode_release_buffers(void) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (int d = 0; d < 16; ++d) {
+    Arena& ar = g_arenas[d];
+    std::lock_guard<std::mutex> lock(ar.mu);
+    bool any = false;
+    for (int s = 0; s < kSlots; ++s) any |= ar.p[s] != nullptr;
+    if (!any) continue;
+    cudaSetDevice(d);
+    for (int s = 0; s < kSlots; ++s) {
+      cudaFree(ar.p[s]);
+      ar.p[s] = nullptr;
+      ar.cap[s] = 0;
+    }
+  }
+  cudaSetDevice(cur);
 }
 
 int mt_encode_yuv8(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_t width, uint32_t height,

@@ -112,3 +112,17 @@ def test_encoder_bytes_equal_the_oracle_encode_at_ragged_sizes(mt_lib, oracle_li
     rgb = synth.generate_rgb(w, h, w * 3 + h)
     got = enc.encode_rgb8(rgb, enc.config(quality=quality, chroma=chroma))
     assert got == oa.encode_rgb8(rgb, quality, chroma)
+
+
+def test_reused_device_buffers_give_the_same_bytes(mt_lib, cuda):
+    """Calls of one device share a set of device buffers, grown to the largest
+    frame: a small frame after a large one, the large one again, and a call
+    after the set is released all give the bytes of the first calls."""
+    from maroontree_b200 import encoder as enc
+
+    big, small = synth.generate_rgb(640, 360, 21), synth.generate_rgb(136, 72, 22)
+    cfg = enc.config(quality=55)
+    a, b = enc.encode_rgb8(big, cfg), enc.encode_rgb8(small, cfg)
+    assert enc.encode_rgb8(big, cfg) == a and enc.encode_rgb8(small, cfg) == b
+    mt_lib.load().mt_encode_release_buffers()
+    assert enc.encode_rgb8(small, cfg) == b and enc.encode_rgb8(big, cfg) == a
