@@ -1234,9 +1234,21 @@ int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const
  * host memory. */
 int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
                           uint8_t** out, size_t* out_len, mt_encode_stats* stats);
-/* The encode calls of a device reuse one set of device buffers (grown to the
- * largest frame seen; a call that finds the set taken by another thread's
- * call allocates its own).  This frees every device's set; the next call
+/* mt_encode_rgb8 of n images (1..64) in one call: each image set up on a
+ * stream of its own, the 8x8 decisions of all of them in ONE persistent launch
+ * (their blocks merged level by level into one dependency-ordered ticket
+ * queue, so blocks of different images run side by side), then each image's
+ * syntax, filters, range coding and container on a host thread of its own.
+ * Image i's bytes are those of encoding it alone; rcs[i] (when non-NULL)
+ * receives its code, and the call returns the first failing code or MT_OK.
+ * Images may differ in size and configuration.  No counterpart in the
+ * reference, which encodes one image per call. */
+int mt_encode_rgb8_batch(int32_t n, const uint8_t* const* rgb, const uint32_t* widths, const uint32_t* heights,
+                         const mt_encode_config* cfgs, uint8_t** outs, size_t* out_lens, int32_t* rcs,
+                         mt_encode_stats* stats);
+/* The encode calls of a device reuse its device buffers (one set per image
+ * of the largest batch seen, each grown to the largest frame it carried; a
+ * call that finds them taken by another thread's call allocates its own).  This frees every device's set; the next call
  * allocates again.  No counterpart in the reference, whose buffers are host
  * memory freed per call. */
 void mt_encode_release_buffers(void);

@@ -298,6 +298,8 @@ def _bind(lib):
         "mt_encode_rgb8_device": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
                                             C.POINTER(C.c_size_t), C.POINTER(EncodeStats)]),
         "mt_encode_release_buffers": (None, []),
+        "mt_encode_rgb8_batch": (C.c_int, [C.c_int32, _P, _P, _P, C.POINTER(EncodeConfig), _P, _P, _P,
+                                           C.POINTER(EncodeStats)]),
         "mt_encode_yuv8": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(EncodeConfig), C.POINTER(_P),
                                      C.POINTER(C.c_size_t), _P]),
         "mt_emit_coeffs_device": (C.c_int, [_P, _P, C.c_int32, _P, _P, _P, _P, _P]),
@@ -436,7 +438,7 @@ EXPORTED_SYMBOLS = (
     "mt_coef_costs_build", "mt_qcat", "mt_coef_cdfs_default", "mt_range_encoder_new", "mt_range_encoder_free",
     "mt_range_encode_bool", "mt_range_encode_symbol", "mt_range_encode_literal",
     "mt_range_encode_signed_subexp_with_ref", "mt_range_encoder_done", "mt_cdf_slot_count", "mt_cdfs_default", "mt_cdf_layout",
-    "mt_emit_coeffs_device", "mt_emit_coeffs", "mt_encode_rgb8", "mt_encode_rgb8_ex", "mt_encode_rgb8_device", "mt_encode_release_buffers", "mt_encode_yuv8",
+    "mt_emit_coeffs_device", "mt_emit_coeffs", "mt_encode_rgb8", "mt_encode_rgb8_ex", "mt_encode_rgb8_device", "mt_encode_release_buffers", "mt_encode_rgb8_batch", "mt_encode_yuv8",
     "mt_pack_tile", "mt_pack_tile_filtered", "mt_tile_trace_free", "mt_replay_tile_with_filters", "mt_free",
     "mt_leb128", "mt_wrap_obu", "mt_tiling_increments", "mt_sequence_header", "mt_frame_header",
     "mt_assemble_frame_obus", "mt_av1_stream", "mt_av1_level_for", "mt_wrap_av1_image",

@@ -27,7 +27,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/maroontree_b200.h"
@@ -63,6 +65,17 @@ struct EncArgs {
   int32_t* lv_y;           // 64 per block
   int32_t* lv_u;           // 64 (4:4:4) or 16 (4:2:0) per block
   int32_t* lv_v;
+};
+
+// One image of a launch: its arguments, its tables and its per-block done
+// counts.
+struct JobDesc {
+  EncArgs a;
+  const mt_coef_costs* cy;
+  const mt_coef_costs* cc;
+  const uint8_t* qmy;
+  const uint8_t* qmc;
+  uint32_t* done;
 };
 
 // The z-order position of the k-th 8x8 block of a superblock and its
@@ -138,6 +151,8 @@ struct StepShared {
   mtd::Edge8 edge[5];                 // the edges of the four luma predictions and the chroma one
   unsigned long long best;
   uint32_t ticket, abort;
+  int cur;                            // the image whose tables are staged (-1: none)
+  JobDesc job;                        // its descriptor
   mtd::Oct8 oct[kLumaThreads / 8 + 1];  // one per candidate octet, then the chroma plane's
 };
 
@@ -192,41 +207,21 @@ constexpr int kMaxPolls = 1 << 20;               // a dependency wait gives up a
 // the remaining waits stop and every cluster leaves at its next ticket.
 // list[i] = block index | have-top-right (bit 30) | left-has-bottom (bit 31).
 __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThreads)
-    encode_blocks_kernel(EncArgs a, const uint32_t* __restrict__ list, int nlist, uint32_t* done,
-                         uint32_t* ticket_ctr, uint32_t* err, const mt_coef_costs* __restrict__ costs_y,
-                         const mt_coef_costs* __restrict__ costs_c, const uint8_t* __restrict__ qm_y,
-                         const uint8_t* __restrict__ qm_c) {
+    encode_blocks_kernel(const JobDesc* __restrict__ jobs, const uint2* __restrict__ list, int nlist,
+                         uint32_t* ticket_ctr, uint32_t* err) {
   __shared__ StepShared S;
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int t = threadIdx.x;
-  {
-    const float* gy = reinterpret_cast<const float*>(costs_y);
-    const float* gc = reinterpret_cast<const float*>(costs_c);
-    float* sy = reinterpret_cast<float*>(&S.cy);
-    float* sc = reinterpret_cast<float*>(&S.cc);
-    for (int i = t; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) {
-      sy[i] = gy[i];
-      sc[i] = gc[i];
-    }
-    if (t < 64) {
-      const int w = a.has_qm_y ? qm_y[t] : 32;
-      S.qmY[t] = (uint8_t)w;
-      S.qsY[t] = mtd::fwd_qm_scale(w);
-      S.lut[t] = mtd::kCoefRateLut[t];
-    } else if (t < 128) {
-      const int i = t - 64;
-      const int w = (a.has_qm_c && i < (a.sub ? 16 : 64)) ? qm_c[i] : 32;
-      S.qmC[i] = (uint8_t)w;
-      S.qsC[i] = mtd::fwd_qm_scale(w);
-    } else if (t < 192) {
-      S.tabs.load(t - 128, 64);
-    } else if (t == 192) {
-      S.best = ~0ull;
-    }
+  if (t < 64) {
+    S.lut[t] = mtd::kCoefRateLut[t];
+    S.tabs.load(t, 64);
+  } else if (t == 64) {
+    S.best = ~0ull;
+    S.cur = -1;
   }
   __syncthreads();
-  const int nbx = a.w8 / 8;
+  const EncArgs& a = S.job.a;
   const int mlo = rank * kCandPerCta / 7;  // first mode of this CTA's share
   const int c = t - kLumaThreads;          // lane of the chroma warp
   const int pl = rank - 2;                 // its plane (CTAs 2 and 3)
@@ -239,7 +234,37 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
     const uint32_t tk = *cluster.map_shared_rank(&S.ticket, 0);
     const uint32_t ab = *cluster.map_shared_rank(&S.abort, 0);
     if (ab || tk >= (uint32_t)nlist) break;  // the same for every CTA of the cluster
-    const uint32_t e = list[tk];
+    const uint2 ent = list[tk];
+    const int img = (int)ent.y;
+    if (img != S.cur) {  // another image: its descriptor, then its cost and QM tables
+      const int* gj = reinterpret_cast<const int*>(jobs + img);
+      int* sj = reinterpret_cast<int*>(&S.job);
+      for (int i = t; i < (int)(sizeof(JobDesc) / 4); i += blockDim.x) sj[i] = gj[i];
+      __syncthreads();
+      const float* gy = reinterpret_cast<const float*>(S.job.cy);
+      const float* gc = reinterpret_cast<const float*>(S.job.cc);
+      float* sy = reinterpret_cast<float*>(&S.cy);
+      float* sc = reinterpret_cast<float*>(&S.cc);
+      for (int i = t; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) {
+        sy[i] = gy[i];
+        sc[i] = gc[i];
+      }
+      if (t < 64) {
+        const int w = a.has_qm_y ? S.job.qmy[t] : 32;
+        S.qmY[t] = (uint8_t)w;
+        S.qsY[t] = mtd::fwd_qm_scale(w);
+      } else if (t < 128) {
+        const int i = t - 64;
+        const int w = (a.has_qm_c && i < (a.sub ? 16 : 64)) ? S.job.qmc[i] : 32;
+        S.qmC[i] = (uint8_t)w;
+        S.qsC[i] = mtd::fwd_qm_scale(w);
+      }
+      __syncthreads();
+      if (t == 0) S.cur = img;
+    }
+    uint32_t* const done = S.job.done;
+    const int nbx = a.w8 / 8;
+    const uint32_t e = ent.x;
     const int b = (int)(e & 0x3fffffffu);
     const int bx = b % nbx, by = b / nbx;
     const int px = bx * 8, py = by * 8;
@@ -528,48 +553,64 @@ struct BlockSyntax {
   }
 };
 
-// The device buffers of an encode call.  Each device keeps one set (grown to
-// the largest frame seen, held until mt_encode_release_buffers or exit) that a
-// call uses when no other call on that device holds it; a call that finds it
-// taken allocates its own.  Every call's device work is ordered on the legacy
-// default stream, so a set is reused only after the previous call's work.
+// The device buffers of the images of an encode call.  Each device keeps
+// sets of them -- one per image of the largest batch seen, each grown to the
+// largest frame it carried, each with a stream -- until
+// mt_encode_release_buffers or exit.  A call uses them when no other call on
+// that device holds them; otherwise it allocates its own for the call.
 constexpr int kSlots = 16;
 enum Slot { kRgb, kPlanes, kTables, kDecisions, kLevels, kSched, kEmit, kTokens, kMaps, kDeblock, kFiltered, kSkip8,
-            kCdef, kRes };
-struct Arena {
-  std::mutex mu;
+            kCdef, kRes, kList, kJobs };
+struct BufSet {
   void* p[kSlots] = {};
   size_t cap[kSlots] = {};
+  cudaStream_t st = nullptr;
+};
+struct Arena {
+  std::mutex mu;
+  std::vector<BufSet> sets;
 };
 Arena g_arenas[16];
 
-struct Buffers {
-  Arena* ar = nullptr;
-  void* own[kSlots] = {};
-  Buffers() {
+class Buffers {
+ public:
+  explicit Buffers(int n) : own_((size_t)n) {
     int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 16 && g_arenas[dev].mu.try_lock()) ar = &g_arenas[dev];
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 16 && g_arenas[dev].mu.try_lock()) {
+      ar_ = &g_arenas[dev];
+      if ((int)ar_->sets.size() < n) ar_->sets.resize((size_t)n);
+    }
   }
   ~Buffers() {
-    if (ar) ar->mu.unlock();
-    for (void* q : own) cudaFree(q);
+    if (ar_) ar_->mu.unlock();
+    for (BufSet& b : own_) {
+      for (void* q : b.p) cudaFree(q);
+      if (b.st) cudaStreamDestroy(b.st);
+    }
   }
   template <class T>
-  T* get(Slot s, size_t n) {
+  T* get(int i, Slot s, size_t n) {
+    BufSet& b = set(i);
     n = n ? n : 1;
-    if (ar) {
-      if (ar->cap[s] < n) {
-        cudaFree(ar->p[s]);
-        ar->p[s] = nullptr;
-        ar->cap[s] = 0;
-        if (cudaMalloc(&ar->p[s], n) != cudaSuccess) return nullptr;
-        ar->cap[s] = n;
-      }
-      return reinterpret_cast<T*>(ar->p[s]);
+    if (b.cap[s] < n) {
+      cudaFree(b.p[s]);
+      b.p[s] = nullptr;
+      b.cap[s] = 0;
+      if (cudaMalloc(&b.p[s], n) != cudaSuccess) return nullptr;
+      b.cap[s] = n;
     }
-    if (cudaMalloc(&own[s], n) != cudaSuccess) return nullptr;
-    return reinterpret_cast<T*>(own[s]);
+    return reinterpret_cast<T*>(b.p[s]);
   }
+  cudaStream_t stream(int i) {
+    BufSet& b = set(i);
+    if (!b.st && cudaStreamCreateWithFlags(&b.st, cudaStreamNonBlocking) != cudaSuccess) b.st = nullptr;
+    return b.st;
+  }
+
+ private:
+  BufSet& set(int i) { return ar_ ? ar_->sets[(size_t)i] : own_[(size_t)i]; }
+  Arena* ar_ = nullptr;
+  std::vector<BufSet> own_;
 };
 
 // The stats of one call: copies, launches and CUDA-event times (the events
@@ -606,6 +647,36 @@ struct CallStats {
   }
 };
 
+
+// One image of an encode call, through its three phases.
+struct Job {
+  // the call's inputs
+  const uint8_t* rgb = nullptr;
+  bool rgb_on_device = false;
+  const uint8_t* const* yuv = nullptr;
+  uint32_t width = 0, height = 0;
+  const mt_encode_config* cfg = nullptr;
+  uint8_t** out = nullptr;
+  size_t* out_len = nullptr;
+  uint16_t** recon_out = nullptr;
+  mt_encode_stats* stats = nullptr;
+  // the frame
+  mt_encode_plan plan = {};
+  int sub = 0, sx = 0, nbx = 0, nby = 0, nb = 0, sb_cols = 0, sb_rows = 0, cl = 0;
+  int32_t pw = 0, ph = 0, pcw = 0, pch = 0;
+  size_t ny = 0, nc = 0;
+  EncArgs a = {};
+  JobDesc desc = {};
+  uint16_t* src[3] = {};
+  uint16_t* rec[3] = {};
+  uint8_t* d_res = nullptr;
+  std::vector<uint32_t> sched;  // blocks in dependency-level order
+  std::vector<int> lstart;      // first entry of each level
+  cudaStream_t st = nullptr;
+  std::unique_ptr<CallStats> cs;
+  int rc = MT_OK;
+};
+
 }  // namespace
 
 namespace mth {
@@ -614,78 +685,84 @@ extern thread_local int cdef_last_launches;
 }  // namespace mth
 
 extern "C" {
-
 int mt_coef_costs_build(const mt_coef_cdfs* cdfs, mt_coef_costs* out);
 const uint8_t* mt_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h);
 int mt_emit_coeffs_device(const int32_t* d_levels, const mt_coef_block* d_blocks, int32_t n, uint32_t* d_counts,
                           uint32_t* d_offsets, uint32_t* d_tokens, uint8_t* d_res_ctx, void* stream);
+}
 
-// The encode from the input planes: rgb (interleaved, converted by the Q13
-// colour conversion) or yuv (three 8-bit planes at their displayed sizes).
-static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* const* yuv, uint32_t width,
-                       uint32_t height, const mt_encode_config* cfg, uint8_t** out, size_t* out_len,
-                       uint16_t* recon_out[3], mt_encode_stats* stats) {
-  if (!out || !out_len) return MT_ERR_INVALID_INPUT;
-  *out = nullptr;
-  *out_len = 0;
-  int rc = mt_encode_config_validate(cfg);
+namespace {
+
+// Validation, device buffers, the input on the device (colour conversion or
+// padding), the frame laws' tables, the kernel arguments and the dependency
+// schedule of image i.
+int job_setup(Job& j, Buffers& buf, int i) {
+  if (!j.out || !j.out_len) return MT_ERR_INVALID_INPUT;
+  *j.out = nullptr;
+  *j.out_len = 0;
+  int rc = mt_encode_config_validate(j.cfg);
   if (rc != MT_OK) return rc;
+  const mt_encode_config* cfg = j.cfg;
+  const uint32_t width = j.width, height = j.height;
   rc = mt_validate_rgb8_input(width, height, (size_t)width * height * 3);
   if (rc != MT_OK) return rc;
-  if (!rgb && (!yuv || !yuv[0] || !yuv[1] || !yuv[2])) return MT_ERR_INVALID_INPUT;
+  if (!j.rgb && (!j.yuv || !j.yuv[0] || !j.yuv[1] || !j.yuv[2])) return MT_ERR_INVALID_INPUT;
   if (cfg->chroma != MT_CHROMA_420 && cfg->chroma != MT_CHROMA_444) return MT_ERR_UNSUPPORTED_CHROMA_FORMAT;
-  mt_encode_plan plan;
-  if ((rc = mt_encode_config_effective(cfg, &plan)) != MT_OK) return rc;
-  if (plan.base_q_idx == 0) return MT_ERR_UNSUPPORTED;  // lossless is a separate encoder
-  const int sub = cfg->chroma == MT_CHROMA_420 ? 2 : 0;
-  const int sx = sub ? 1 : 0;
-  int32_t pw, ph, pcw, pch;
-  if ((rc = mt_padded_plane_dims((int)width, (int)height, sub, &pw, &ph, &pcw, &pch)) != MT_OK) return rc;
-  const int nbx = pw / 8, nby = ph / 8, nb = nbx * nby;
-  const int sb_cols = (pw + 63) / 64, sb_rows = (ph + 63) / 64;
+  if ((rc = mt_encode_config_effective(cfg, &j.plan)) != MT_OK) return rc;
+  if (j.plan.base_q_idx == 0) return MT_ERR_UNSUPPORTED;  // lossless is a separate encoder
+  const int sub = j.sub = cfg->chroma == MT_CHROMA_420 ? 2 : 0;
+  const int sx = j.sx = sub ? 1 : 0;
+  if ((rc = mt_padded_plane_dims((int)width, (int)height, sub, &j.pw, &j.ph, &j.pcw, &j.pch)) != MT_OK) return rc;
+  const int32_t pw = j.pw, ph = j.ph, pcw = j.pcw, pch = j.pch;
+  const int nbx = j.nbx = pw / 8, nby = j.nby = ph / 8, nb = j.nb = nbx * nby;
+  const int sb_cols = j.sb_cols = (pw + 63) / 64, sb_rows = j.sb_rows = (ph + 63) / 64;
   // one tile: the AV1 maximum tile width (64 superblocks) and area (2304)
   if (sb_cols > 64 || sb_cols * sb_rows > 2304) return MT_ERR_UNSUPPORTED;
-  const int cl = sub ? 16 : 64;  // chroma levels per block
+  const int cl = j.cl = sub ? 16 : 64;  // chroma levels per block
   // quantisers, QM rows, default CDF slices and their bit costs, lambdas
   mt_quant qy, qc;
-  if (mt_quant_init(plan.base_q_idx, 8, plan.qm_y, &qy) != MT_OK) return MT_ERR_INVALID_INPUT;
-  if (mt_quant_init_chroma(plan.base_q_idx, 0, 0, 8, plan.qm_u, &qc) != MT_OK) return MT_ERR_INVALID_INPUT;
+  if (mt_quant_init(j.plan.base_q_idx, 8, j.plan.qm_y, &qy) != MT_OK) return MT_ERR_INVALID_INPUT;
+  if (mt_quant_init_chroma(j.plan.base_q_idx, 0, 0, 8, j.plan.qm_u, &qc) != MT_OK) return MT_ERR_INVALID_INPUT;
   mt_coef_cdfs cdy, cdc;
   mt_coef_costs cy, cc;
-  const int qctx = mt_qcat(plan.base_q_idx);
+  const int qctx = mt_qcat(j.plan.base_q_idx);
   mt_coef_cdfs_default(qctx, 8, 8, 0, &cdy);
   mt_coef_cdfs_default(qctx, sub ? 4 : 8, sub ? 4 : 8, 1, &cdc);
   mt_coef_costs_build(&cdy, &cy);
   mt_coef_costs_build(&cdc, &cc);
   mt_rd_lambdas lam;
-  if (mt_rd_lambdas_init(plan.base_q_idx, qy.dc_q, sub, 8, &lam) != MT_OK) return MT_ERR_INVALID_INPUT;
-  const uint8_t* qmy = mt_qm_row(plan.qm_y, 0, 8, 8);
-  const uint8_t* qmc = mt_qm_row(plan.qm_u, 1, sub ? 4 : 8, sub ? 4 : 8);
+  if (mt_rd_lambdas_init(j.plan.base_q_idx, qy.dc_q, sub, 8, &lam) != MT_OK) return MT_ERR_INVALID_INPUT;
+  const uint8_t* qmy = mt_qm_row(j.plan.qm_y, 0, 8, 8);
+  const uint8_t* qmc = mt_qm_row(j.plan.qm_u, 1, sub ? 4 : 8, sub ? 4 : 8);
   // device buffers
-  const size_t ny = (size_t)pw * ph, nc = (size_t)pcw * pch;
-  Buffers buf;
-  const size_t in_bytes = rgb ? (size_t)width * height * 3
-                              : (size_t)width * height + 2 * (size_t)((width + sx) >> sx) * ((height + sx) >> sx);
-  uint8_t* d_rgbbuf = buf.get<uint8_t>(kRgb, rgb_on_device ? 1 : in_bytes);
-  uint16_t* d_planes = buf.get<uint16_t>(kPlanes, (ny + 2 * nc) * 2 * 2);
-  uint8_t* d_tabs = buf.get<uint8_t>(kTables, 2 * sizeof(mt_coef_costs) + 128);
-  uint8_t* d_decs = buf.get<uint8_t>(kDecisions, (size_t)nb * 2);
-  int32_t* d_levels = buf.get<int32_t>(kLevels, (size_t)nb * (64 + 2 * cl) * 4);
-  uint8_t* d_res = buf.get<uint8_t>(kRes, (size_t)nb * 3);
-  if (!d_rgbbuf || !d_planes || !d_tabs || !d_decs || !d_levels || !d_res) return MT_ERR_DEVICE;
-  uint16_t* src[3] = {d_planes, d_planes + ny, d_planes + ny + nc};
-  uint16_t* rec[3] = {src[2] + nc, src[2] + nc + ny, src[2] + nc + ny + nc};
+  const size_t ny = j.ny = (size_t)pw * ph, nc = j.nc = (size_t)pcw * pch;
+  const size_t in_bytes = j.rgb ? (size_t)width * height * 3
+                                : (size_t)width * height + 2 * (size_t)((width + sx) >> sx) * ((height + sx) >> sx);
+  uint8_t* d_rgbbuf = buf.get<uint8_t>(i, kRgb, j.rgb_on_device ? 1 : in_bytes);
+  uint16_t* d_planes = buf.get<uint16_t>(i, kPlanes, (ny + 2 * nc) * 2 * 2);
+  uint8_t* d_tabs = buf.get<uint8_t>(i, kTables, 2 * sizeof(mt_coef_costs) + 128);
+  uint8_t* d_decs = buf.get<uint8_t>(i, kDecisions, (size_t)nb * 2);
+  int32_t* d_levels = buf.get<int32_t>(i, kLevels, (size_t)nb * (64 + 2 * cl) * 4);
+  j.d_res = buf.get<uint8_t>(i, kRes, (size_t)nb * 3);
+  uint32_t* d_done = buf.get<uint32_t>(i, kSched, (size_t)nb * 4);
+  const cudaStream_t st = j.st = buf.stream(i);
+  if (!d_rgbbuf || !d_planes || !d_tabs || !d_decs || !d_levels || !j.d_res || !d_done || !st) return MT_ERR_DEVICE;
+  uint16_t* const* src = j.src;
+  for (int p = 0; p < 3; ++p) {
+    j.src[p] = d_planes + (p == 0 ? 0 : ny + (size_t)(p - 1) * nc);
+    j.rec[p] = d_planes + ny + 2 * nc + (p == 0 ? 0 : ny + (size_t)(p - 1) * nc);
+  }
   mt_coef_costs* d_cy = reinterpret_cast<mt_coef_costs*>(d_tabs);
   mt_coef_costs* d_cc = d_cy + 1;
   uint8_t* d_qmy = reinterpret_cast<uint8_t*>(d_cc + 1);
   uint8_t* d_qmc = d_qmy + 64;
-  cudaStream_t st = nullptr;
-  CallStats cs(stats);
+  j.cs.reset(new CallStats(j.stats));
+  CallStats& cs = *j.cs;
   cs.mark(0, st);
-  if (rgb) {
-    const uint8_t* d_in = rgb;
-    if (!rgb_on_device) {
-      if (cudaMemcpy(d_rgbbuf, rgb, in_bytes, cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+  if (j.rgb) {
+    const uint8_t* d_in = j.rgb;
+    if (!j.rgb_on_device) {
+      if (cudaMemcpyAsync(d_rgbbuf, j.rgb, in_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return MT_ERR_DEVICE;
       cs.h2d(in_bytes);
       d_in = d_rgbbuf;
     }
@@ -695,9 +772,9 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     const int cw = (int)((width + sx) >> sx), ch = (int)((height + sx) >> sx);
     uint8_t* d_in = d_rgbbuf;
     const size_t n0 = (size_t)width * height, n1 = (size_t)cw * ch;
-    if (cudaMemcpy(d_in, yuv[0], n0, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d_in + n0, yuv[1], n1, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(d_in + n0 + n1, yuv[2], n1, cudaMemcpyHostToDevice) != cudaSuccess)
+    if (cudaMemcpyAsync(d_in, j.yuv[0], n0, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_in + n0, j.yuv[1], n1, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(d_in + n0 + n1, j.yuv[2], n1, cudaMemcpyHostToDevice, st) != cudaSuccess)
       return MT_ERR_DEVICE;
     pad_plane_kernel<<<dim3((pw + 127) / 128, ph), 128, 0, st>>>(d_in, (int)width, (int)height, src[0], pw, ph);
     pad_plane_kernel<<<dim3((pcw + 127) / 128, pch), 128, 0, st>>>(d_in + n0, cw, ch, src[1], pcw, pch);
@@ -711,10 +788,11 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   if (qmy) cudaMemcpyAsync(d_qmy, qmy, 64, cudaMemcpyHostToDevice, st);
   if (qmc) cudaMemcpyAsync(d_qmc, qmc, sub ? 16 : 64, cudaMemcpyHostToDevice, st);
   cs.h2d(2 * sizeof(mt_coef_costs) + (qmy ? 64 : 0) + (qmc ? (sub ? 16 : 64) : 0));
-  EncArgs a = {};
+  EncArgs& a = j.a;
+  a = EncArgs{};
   for (int p = 0; p < 3; ++p) {
-    a.src[p] = src[p];
-    a.rec[p] = rec[p];
+    a.src[p] = j.src[p];
+    a.rec[p] = j.rec[p];
   }
   a.py = {};
   a.py.tx_size = 8;
@@ -746,90 +824,170 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   a.lv_y = d_levels;
   a.lv_u = a.lv_y + (size_t)nb * 64;
   a.lv_v = a.lv_u + (size_t)nb * cl;
-  if (cudaMemsetAsync(a.mode, 0, (size_t)nb * 2, st) != cudaSuccess) return MT_ERR_DEVICE;
+  j.desc.a = a;
+  j.desc.cy = d_cy;
+  j.desc.cc = d_cc;
+  j.desc.qmy = d_qmy;
+  j.desc.qmc = d_qmc;
+  j.desc.done = d_done;
+  if (cudaMemsetAsync(a.mode, 0, (size_t)nb * 2, st) != cudaSuccess ||
+      cudaMemsetAsync(d_done, 0, (size_t)nb * 4, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
   // Dependency levels of the 8x8 blocks: a block needs its left, top,
   // top-left neighbours and, where the intra edge uses them, its top-right and
-  // bottom-left ones; blocks of one level run as one launch.
-  std::vector<uint32_t> sched;
-  std::vector<int> lstart;
-  {
-    std::vector<int32_t> T((size_t)nb, -1);
-    std::vector<uint32_t> entry((size_t)nb);
-    std::vector<int> cnt;
-    for (int sr = 0; sr < sb_rows; ++sr)
-      for (int sc = 0; sc < sb_cols; ++sc)
-        for (int k = 0; k < 64; ++k) {
-          int bx, by;
-          bool thr, lhb;
-          zorder(k, &bx, &by, &thr, &lhb);
-          const int x = sc * 8 + bx, y = sr * 8 + by;
-          if (x >= nbx || y >= nby) continue;
-          const bool tr = thr && y > 0 && (x + 1) * 8 < pw;
-          const bool bl = lhb && x > 0 && (y + 1) * 8 < ph;
-          int lv = 0;
-          auto dep = [&](int xx, int yy) { lv = std::max(lv, T[(size_t)yy * nbx + xx] + 1); };
-          if (x > 0) dep(x - 1, y);
-          if (y > 0) dep(x, y - 1);
-          if (x > 0 && y > 0) dep(x - 1, y - 1);
-          if (tr) dep(x + 1, y - 1);
-          if (bl) dep(x - 1, y + 1);
-          const size_t bi = (size_t)y * nbx + x;
-          T[bi] = lv;
-          entry[bi] = (uint32_t)bi | (thr ? 1u << 30 : 0u) | (lhb ? 1u << 31 : 0u);
-          if ((int)cnt.size() <= lv) cnt.resize(lv + 1, 0);
-          ++cnt[lv];
-        }
-    lstart.assign(cnt.size() + 1, 0);
-    for (size_t l = 0; l < cnt.size(); ++l) lstart[l + 1] = lstart[l] + cnt[l];
-    sched.resize((size_t)nb);
-    std::vector<int> fill(lstart.begin(), lstart.end() - 1);
-    for (int sr = 0; sr < sb_rows; ++sr)  // coding order inside a level
-      for (int sc = 0; sc < sb_cols; ++sc)
-        for (int k = 0; k < 64; ++k) {
-          int bx, by;
-          bool thr, lhb;
-          zorder(k, &bx, &by, &thr, &lhb);
-          const int x = sc * 8 + bx, y = sr * 8 + by;
-          if (x >= nbx || y >= nby) continue;
-          const size_t bi = (size_t)y * nbx + x;
-          sched[fill[T[bi]]++] = entry[bi];
-        }
+  // bottom-left ones.
+  std::vector<int32_t> T((size_t)nb, -1);
+  std::vector<uint32_t> entry((size_t)nb);
+  std::vector<int> cnt;
+  for (int sr = 0; sr < sb_rows; ++sr)
+    for (int sc = 0; sc < sb_cols; ++sc)
+      for (int k = 0; k < 64; ++k) {
+        int bx, by;
+        bool thr, lhb;
+        zorder(k, &bx, &by, &thr, &lhb);
+        const int x = sc * 8 + bx, y = sr * 8 + by;
+        if (x >= nbx || y >= nby) continue;
+        const bool tr = thr && y > 0 && (x + 1) * 8 < pw;
+        const bool bl = lhb && x > 0 && (y + 1) * 8 < ph;
+        int lv = 0;
+        auto dep = [&](int xx, int yy) { lv = std::max(lv, T[(size_t)yy * nbx + xx] + 1); };
+        if (x > 0) dep(x - 1, y);
+        if (y > 0) dep(x, y - 1);
+        if (x > 0 && y > 0) dep(x - 1, y - 1);
+        if (tr) dep(x + 1, y - 1);
+        if (bl) dep(x - 1, y + 1);
+        const size_t bi = (size_t)y * nbx + x;
+        T[bi] = lv;
+        entry[bi] = (uint32_t)bi | (thr ? 1u << 30 : 0u) | (lhb ? 1u << 31 : 0u);
+        if ((int)cnt.size() <= lv) cnt.resize(lv + 1, 0);
+        ++cnt[lv];
+      }
+  j.lstart.assign(cnt.size() + 1, 0);
+  for (size_t l = 0; l < cnt.size(); ++l) j.lstart[l + 1] = j.lstart[l] + cnt[l];
+  j.sched.resize((size_t)nb);
+  std::vector<int> fill(j.lstart.begin(), j.lstart.end() - 1);
+  for (int sr = 0; sr < sb_rows; ++sr)  // coding order inside a level
+    for (int sc = 0; sc < sb_cols; ++sc)
+      for (int k = 0; k < 64; ++k) {
+        int bx, by;
+        bool thr, lhb;
+        zorder(k, &bx, &by, &thr, &lhb);
+        const int x = sc * 8 + bx, y = sr * 8 + by;
+        if (x >= nbx || y >= nby) continue;
+        const size_t bi = (size_t)y * nbx + x;
+        j.sched[fill[T[bi]]++] = entry[bi];
+      }
+  if (j.stats) {
+    j.stats->blocks = (uint32_t)nb;
+    j.stats->levels = (uint32_t)(j.lstart.size() - 1);
   }
-  // the dependency-ordered block list, the per-block done counts, the ticket
-  // counter and the wait-timeout flag
+  return MT_OK;
+}
+
+// The decisions of every image that set up, in one launch: the images'
+// blocks merged level by level into one ticket list (each image's order is
+// still a dependency order), the persistent clusters taking tickets across
+// images.
+int decide_all(std::vector<Job>& jobs, Buffers& buf) {
+  std::vector<uint2> list;
+  std::vector<JobDesc> descs;
+  std::vector<int> slot;  // job index per descriptor
+  int levels = 0;
+  for (size_t i = 0; i < jobs.size(); ++i)
+    if (jobs[i].rc == MT_OK) {
+      slot.push_back((int)i);
+      descs.push_back(jobs[i].desc);
+      levels = std::max(levels, (int)jobs[i].lstart.size() - 1);
+    }
+  if (slot.empty()) return MT_OK;
   int width_max = 1;
-  for (size_t l = 0; l + 1 < lstart.size(); ++l) width_max = std::max(width_max, lstart[l + 1] - lstart[l]);
-  uint32_t* d_sched = buf.get<uint32_t>(kSched, sched.size() * 4 + ((size_t)nb + 2) * 4);
-  if (!d_sched) return MT_ERR_DEVICE;
-  uint32_t* d_done = d_sched + sched.size();
-  uint32_t* d_ctl = d_done + nb;  // [0] ticket counter, [1] timeout flag
-  if (cudaMemcpyAsync(d_sched, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-      cudaMemsetAsync(d_done, 0, ((size_t)nb + 2) * 4, st) != cudaSuccess)
-    return MT_ERR_DEVICE;
-  // one cluster per block that can run at once (the widest dependency level),
-  // at most 64 clusters (two CTAs per SM)
-  const int nclusters = std::min(width_max, 64);
-  cs.h2d(sched.size() * 4);
-  cs.mark(1, st);
-  encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, st>>>(a, d_sched, nb, d_done,
-                                                                           d_ctl, d_ctl + 1, d_cy, d_cc, d_qmy, d_qmc);
-  cs.mark(2, st);
-  cs.launches(1);
-  cs.d2h(4);
-  if (stats) {
-    stats->blocks = (uint32_t)nb;
-    stats->levels = (uint32_t)(lstart.size() - 1);
+  for (int l = 0; l < levels; ++l) {
+    const size_t before = list.size();
+    for (size_t d = 0; d < slot.size(); ++d) {
+      const Job& j = jobs[(size_t)slot[d]];
+      if (l + 1 >= (int)j.lstart.size()) continue;
+      for (int k = j.lstart[l]; k < j.lstart[l + 1]; ++k) list.push_back(make_uint2(j.sched[(size_t)k], (unsigned)d));
+    }
+    width_max = std::max(width_max, (int)(list.size() - before));
   }
+  const int i0 = slot[0];
+  const cudaStream_t ks = jobs[(size_t)i0].st;
+  uint2* d_list = buf.get<uint2>(i0, kList, list.size() * sizeof(uint2) + 16);
+  JobDesc* d_jobs = buf.get<JobDesc>(i0, kJobs, descs.size() * sizeof(JobDesc));
+  if (!d_list || !d_jobs) return MT_ERR_DEVICE;
+  uint32_t* d_ctl = reinterpret_cast<uint32_t*>(d_list + list.size());  // [0] ticket counter, [1] timeout flag
+  // the launch waits for every image's set-up on its own stream
+  std::vector<cudaEvent_t> evs;
+  for (size_t d = 1; d < slot.size(); ++d) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return MT_ERR_DEVICE;
+    evs.push_back(e);
+    cudaEventRecord(e, jobs[(size_t)slot[d]].st);
+    cudaStreamWaitEvent(ks, e, 0);
+  }
+  if (cudaMemcpyAsync(d_list, list.data(), list.size() * sizeof(uint2), cudaMemcpyHostToDevice, ks) != cudaSuccess ||
+      cudaMemcpyAsync(d_jobs, descs.data(), descs.size() * sizeof(JobDesc), cudaMemcpyHostToDevice, ks) !=
+          cudaSuccess ||
+      cudaMemsetAsync(d_ctl, 0, 8, ks) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  // one cluster per block that can run at once (the widest merged level), at
+  // most 74 clusters (two CTAs on each of the 148 SMs)
+  const int nclusters = std::min(width_max, 74);
+  for (int d : slot) {
+    jobs[(size_t)d].cs->h2d(jobs[(size_t)d].sched.size() * 8 + sizeof(JobDesc));
+    jobs[(size_t)d].cs->mark(1, ks);
+  }
+  encode_blocks_kernel<<<nclusters * kClusterCtas, kStepThreads, 0, ks>>>(d_jobs, d_list, (int)list.size(), d_ctl,
+                                                                          d_ctl + 1);
+  for (int d : slot) {
+    jobs[(size_t)d].cs->mark(2, ks);
+    jobs[(size_t)d].cs->launches(1);
+    jobs[(size_t)d].cs->d2h(4);
+  }
+  // every image's finishing work waits for the launch
+  cudaEvent_t done_ev;
+  if (cudaEventCreateWithFlags(&done_ev, cudaEventDisableTiming) != cudaSuccess) return MT_ERR_DEVICE;
+  evs.push_back(done_ev);
+  cudaEventRecord(done_ev, ks);
+  for (int d : slot) cudaStreamWaitEvent(jobs[(size_t)d].st, done_ev, 0);
   uint32_t timed_out = 0;
-  if (cudaMemcpyAsync(&timed_out, d_ctl + 1, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+  const bool ok = cudaMemcpyAsync(&timed_out, d_ctl + 1, 4, cudaMemcpyDeviceToHost, ks) == cudaSuccess &&
+                  cudaStreamSynchronize(ks) == cudaSuccess && cudaGetLastError() == cudaSuccess;
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  if (!ok || timed_out) return MT_ERR_DEVICE;
+  return MT_OK;
+}
+
+// Everything after the decisions for image i: the context bytes, the block
+// syntax walk, the coefficient tokens, the filters, range coding, headers
+// and container.
+int job_finish(Job& j, Buffers& buf, int i) {
+  int rc = MT_OK;
+  const cudaStream_t st = j.st;
+  CallStats& cs = *j.cs;
+  const mt_encode_config* cfg = j.cfg;
+  const uint32_t width = j.width, height = j.height;
+  const int sub = j.sub, sx = j.sx, nbx = j.nbx, nby = j.nby, nb = j.nb, sb_cols = j.sb_cols, sb_rows = j.sb_rows,
+            cl = j.cl;
+  const int32_t pw = j.pw, ph = j.ph;
+  const size_t ny = j.ny, nc = j.nc;
+  const EncArgs& a = j.a;
+  uint16_t* const* src = j.src;
+  uint16_t* const* rec = j.rec;
+  std::vector<uint8_t> mode(nb), tx(nb);
+  // The coefficient contexts of a block depend on its neighbours' context
+  // bytes, which depend on their levels only: computed on the device for
+  // every transform block, read back as three bytes per 8x8 block.
+  res_ctx_kernel<<<(unsigned)((3 * (size_t)nb + 255) / 256), 256, 0, st>>>(a.lv_y, a.lv_u, a.lv_v, a.tx, nb, sub,
+                                                                           j.d_res);
+  cs.launches(1);
+  std::vector<uint8_t> resb((size_t)nb * 3);
+  if (cudaMemcpyAsync(mode.data(), a.mode, nb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(tx.data(), a.tx, nb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(resb.data(), j.d_res, resb.size(), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return MT_ERR_DEVICE;
-  if (timed_out) return MT_ERR_DEVICE;
-  if (cudaGetLastError() != cudaSuccess) return MT_ERR_DEVICE;
-  std::vector<uint8_t> mode(nb), tx(nb);
-  if (cudaMemcpy(mode.data(), a.mode, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  if (cudaMemcpy(tx.data(), a.tx, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  cs.d2h(2 * (size_t)nb);
+  cs.d2h(2 * (size_t)nb + resb.size());
   // block syntax in coding order, with the coefficient blocks it carries
   mt_cdf_slot_layout L;
   mt_cdf_layout(&L);
@@ -849,15 +1007,6 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     bs.l_coef[p].assign(nby * 2, 0x40);
   }
   bs.blocks = &blocks;
-  // The coefficient contexts of a block depend on its neighbours' context
-  // bytes, which depend on their levels only: computed on the device for
-  // every transform block, read back as three bytes per 8x8 block.
-  res_ctx_kernel<<<(unsigned)((3 * (size_t)nb + 255) / 256), 256, 0, st>>>(a.lv_y, a.lv_u, a.lv_v, a.tx, nb, sub,
-                                                                           d_res);
-  cs.launches(1);
-  std::vector<uint8_t> resb((size_t)nb * 3);
-  if (cudaMemcpy(resb.data(), d_res, resb.size(), cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  cs.d2h(resb.size());
   for (int sr = 0; sr < sb_rows; ++sr)
     for (int sc = 0; sc < sb_cols; ++sc) {
       bs.sbs.emplace_back();
@@ -876,60 +1025,43 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     }
   // coefficient tokens of every block in one launch
   const int ncb = (int)blocks.size();
-  mt_coef_block* d_blocks = buf.get<mt_coef_block>(kEmit, (size_t)ncb * (sizeof(mt_coef_block) + 8) + 8);
+  mt_coef_block* d_blocks = buf.get<mt_coef_block>(i, kEmit, (size_t)ncb * (sizeof(mt_coef_block) + 8) + 8);
   if (!d_blocks) return MT_ERR_DEVICE;
   uint32_t* d_cnt = reinterpret_cast<uint32_t*>(d_blocks + ncb);
   uint32_t* d_off = d_cnt + ncb;
-  if (cudaMemcpy(d_blocks, blocks.data(), (size_t)ncb * sizeof(mt_coef_block), cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(d_blocks, blocks.data(), (size_t)ncb * sizeof(mt_coef_block), cudaMemcpyHostToDevice, st) !=
+      cudaSuccess)
     return MT_ERR_DEVICE;
   if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, nullptr, nullptr, st)) != MT_OK) return rc;
   cs.h2d((size_t)ncb * sizeof(mt_coef_block));
   cs.launches(2);
   uint32_t total = 0;
-  if (cudaMemcpy(&total, d_off + ncb, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  uint32_t* d_tok = buf.get<uint32_t>(kTokens, (size_t)total * 4);
+  if (cudaMemcpyAsync(&total, d_off + ncb, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  uint32_t* d_tok = buf.get<uint32_t>(i, kTokens, (size_t)total * 4);
   if (!d_tok) return MT_ERR_DEVICE;
-  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok, nullptr, st)) != MT_OK)
-    return rc;
+  if ((rc = mt_emit_coeffs_device(a.lv_y, d_blocks, ncb, d_cnt, d_off, d_tok, nullptr, st)) != MT_OK) return rc;
   cs.launches(1);
   std::vector<uint32_t> toks(total), offs((size_t)ncb + 1);
-  if (cudaMemcpy(toks.data(), d_tok, (size_t)total * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  if (cudaMemcpy(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return MT_ERR_DEVICE;
-  cs.d2h(4 + (size_t)total * 4 + offs.size() * 4);
-  // splice the coefficient tokens into the superblock streams
-  std::vector<uint32_t> ops, sb_start(1, 0);
-  std::vector<int32_t> cdef_pt;
-  size_t k = 0;
-  for (size_t s = 0; s < bs.sbs.size(); ++s) {
-    const size_t base = ops.size();
-    int32_t cp_spliced = -1;
-    for (size_t i = 0; i < bs.sbs[s].size(); ++i) {
-      if ((int)i == bs.cdef_points[s]) cp_spliced = (int32_t)(ops.size() - base);
-      const uint32_t t = bs.sbs[s][i];
-      if (t == BlockSyntax::kCoef) {
-        ops.insert(ops.end(), toks.begin() + offs[k], toks.begin() + offs[k + 1]);
-        ++k;
-      } else {
-        ops.push_back(t);
-      }
-    }
-    sb_start.push_back((uint32_t)ops.size());
-    cdef_pt.push_back(cp_spliced);
-  }
-  // deblocking (uniform 8x8 blocks and transforms) and the CDEF decision
+  if (cudaMemcpyAsync(toks.data(), d_tok, (size_t)total * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  // deblocking (uniform 8x8 blocks and transforms) and the CDEF decision,
+  // enqueued before the host splices the tokens
   int32_t ly, luv, sharp;
-  mt_loop_filter_levels(plan.base_q_idx, sx, sx, &ly, &luv, &sharp);
+  mt_loop_filter_levels(j.plan.base_q_idx, sx, sx, &ly, &luv, &sharp);
   const int n4 = (pw / 4) * (ph / 4);
   std::vector<uint8_t> maps((size_t)n4 * 6);
   for (int r = 0; r < ph / 4; ++r)
     for (int c = 0; c < pw / 4; ++c) {
-      const size_t i = (size_t)r * (pw / 4) + c;
-      maps[i] = 2;
-      maps[n4 + i] = 2;
-      maps[2 * (size_t)n4 + i] = (c % 2) == 0;
-      maps[3 * (size_t)n4 + i] = (r % 2) == 0;
-      maps[4 * (size_t)n4 + i] = 2;
-      maps[5 * (size_t)n4 + i] = 2;
+      const size_t k = (size_t)r * (pw / 4) + c;
+      maps[k] = 2;
+      maps[n4 + k] = 2;
+      maps[2 * (size_t)n4 + k] = (c % 2) == 0;
+      maps[3 * (size_t)n4 + k] = (r % 2) == 0;
+      maps[4 * (size_t)n4 + k] = 2;
+      maps[5 * (size_t)n4 + k] = 2;
     }
   mt_deblock_frame_params g = {};
   g.w8 = pw;
@@ -938,15 +1070,15 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   g.disp_h = (int)height;
   g.sub_x = g.sub_y = sx;
   g.bd = 8;
-
   const size_t dbs = mt_deblock_frame_scratch_bytes(&g);
-  uint8_t* d_maps = buf.get<uint8_t>(kMaps, maps.size());
-  void* d_db = buf.get<void>(kDeblock, dbs);
+  uint8_t* d_maps = buf.get<uint8_t>(i, kMaps, maps.size());
+  void* d_db = buf.get<void>(i, kDeblock, dbs);
   if (!d_maps || !d_db) return MT_ERR_DEVICE;
-  if (cudaMemcpy(d_maps, maps.data(), maps.size(), cudaMemcpyHostToDevice) != cudaSuccess) return MT_ERR_DEVICE;
+  if (cudaMemcpyAsync(d_maps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
   cs.h2d(maps.size());
   // the recon planes are kept: the filters run on a copy
-  uint16_t* d_flt = buf.get<uint16_t>(kFiltered, (ny + 2 * nc) * 2);
+  uint16_t* d_flt = buf.get<uint16_t>(i, kFiltered, (ny + 2 * nc) * 2);
   if (!d_flt) return MT_ERR_DEVICE;
   uint16_t* flt[3] = {d_flt, d_flt + ny, d_flt + ny + nc};
   if (cudaMemcpyAsync(flt[0], rec[0], (ny + 2 * nc) * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
@@ -962,26 +1094,49 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
     if (ly > 0) cs.launches((vw4 > 1) + (vh4 > 1));
     if (ly > 0 && luv > 0) cs.launches(1 + 2 * ((cw4 > 1) + (ch4 > 1)));
   }
+  // splice the coefficient tokens into the superblock streams (the token copy
+  // has completed once the stream reaches the filters' first sync)
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;
+  cs.d2h(4 + (size_t)total * 4 + offs.size() * 4);
+  std::vector<uint32_t> ops, sb_start(1, 0);
+  std::vector<int32_t> cdef_pt;
+  ops.reserve((size_t)total + (size_t)nb * 12);
+  size_t k = 0;
+  for (size_t sbi = 0; sbi < bs.sbs.size(); ++sbi) {
+    const size_t base = ops.size();
+    int32_t cp_spliced = -1;
+    for (size_t t = 0; t < bs.sbs[sbi].size(); ++t) {
+      if ((int)t == bs.cdef_points[sbi]) cp_spliced = (int32_t)(ops.size() - base);
+      const uint32_t tok = bs.sbs[sbi][t];
+      if (tok == BlockSyntax::kCoef) {
+        ops.insert(ops.end(), toks.begin() + offs[k], toks.begin() + offs[k + 1]);
+        ++k;
+      } else {
+        ops.push_back(tok);
+      }
+    }
+    sb_start.push_back((uint32_t)ops.size());
+    cdef_pt.push_back(cp_spliced);
+  }
   mt_cdef_params cp = {};
   cp.w8 = pw;
   cp.h8 = ph;
   cp.disp_w = (int)width;
   cp.disp_h = (int)height;
   cp.sub_x = cp.sub_y = sx;
-  cp.base_q_idx = plan.base_q_idx;
+  cp.base_q_idx = j.plan.base_q_idx;
   cp.bd = 8;
   cp.slow = cfg->speed <= MT_SPEED_SLOW;
-
   const int unit_cols = (pw + 63) / 64, unit_rows = (ph + 63) / 64;
-  uint8_t* d_skip8 = buf.get<uint8_t>(kSkip8, (size_t)nb);
-  void* d_cs = buf.get<void>(kCdef, mt_cdef_scratch_bytes(&cp));
+  uint8_t* d_skip8 = buf.get<uint8_t>(i, kSkip8, (size_t)nb);
+  void* d_cs = buf.get<void>(i, kCdef, mt_cdef_scratch_bytes(&cp));
   if (!d_skip8 || !d_cs) return MT_ERR_DEVICE;
   if (cudaMemsetAsync(d_skip8, 0, (size_t)nb, st) != cudaSuccess) return MT_ERR_DEVICE;
   mt_cdef_decision dec = {};
   std::vector<uint8_t> grid((size_t)unit_cols * unit_rows);
-  if (plan.cdef) {
-    if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8, &cp, d_cs,
-                                   &dec, grid.data(), st)) != MT_OK)
+  if (j.plan.cdef) {
+    if ((rc = mt_cdef_frame_device(flt[0], flt[1], flt[2], src[0], src[1], src[2], d_skip8, &cp, d_cs, &dec,
+                                   grid.data(), st)) != MT_OK)
       return rc;
     size_t cd2h = 0, ch2d = 0;
     mth::cdef_frame_transfer_bytes(&cp, &cd2h, &ch2d);
@@ -991,10 +1146,11 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   } else {
     dec.bits = -1;
   }
-  if (recon_out) {  // the decoder's output: deblocked and CDEF-filtered
-    if (cudaMemcpy(recon_out[0], flt[0], ny * 2, cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(recon_out[1], flt[1], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(recon_out[2], flt[2], nc * 2, cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (j.recon_out) {  // the decoder's output: deblocked and CDEF-filtered
+    if (cudaMemcpyAsync(j.recon_out[0], flt[0], ny * 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(j.recon_out[1], flt[1], nc * 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(j.recon_out[2], flt[2], nc * 2, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
       return MT_ERR_DEVICE;
     cs.d2h((ny + 2 * nc) * 2);
   }
@@ -1002,7 +1158,7 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   // point (the 64x64 CDEF units are the superblocks of the one tile)
   uint8_t* tile = nullptr;
   size_t tile_len = 0;
-  if ((rc = mt_pack_tile_filtered(plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
+  if ((rc = mt_pack_tile_filtered(j.plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
                                   (int32_t)bs.sbs.size(), dec.bits > 0 ? grid.data() : nullptr,
                                   dec.bits > 0 ? dec.bits : 0, &tile, &tile_len)) != MT_OK)
     return rc;
@@ -1023,9 +1179,9 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   mt_frame_header_params fp = {};
   fp.w8 = pw;
   fp.h8 = ph;
-  fp.base_q_idx = plan.base_q_idx;
-  fp.qm_y = plan.qm_y;
-  fp.qm_u = fp.qm_v = plan.qm_u;
+  fp.base_q_idx = j.plan.base_q_idx;
+  fp.qm_y = j.plan.qm_y;
+  fp.qm_u = fp.qm_v = j.plan.qm_u;
   fp.updating_cdf = cfg->updating_cdf;
   fp.lf_y = ly;
   fp.lf_u = fp.lf_v = luv;
@@ -1062,18 +1218,63 @@ static int encode_impl(const uint8_t* rgb, bool rgb_on_device, const uint8_t* co
   ip.clli_present = cfg->clli_present;
   ip.max_content_light_level = cfg->max_content_light_level;
   ip.max_pic_average_light_level = cfg->max_pic_average_light_level;
-  rc = mt_wrap_av1_image(obu, obu_len, &ip, out, out_len);
+  rc = mt_wrap_av1_image(obu, obu_len, &ip, j.out, j.out_len);
   free(obu);
-  if (stats) stats->tokens = (uint32_t)ops.size();
+  if (j.stats) j.stats->tokens = (uint32_t)ops.size();
   cs.mark(3, st);
   cs.finish();
   return rc;
 }
 
+// The encode of a batch of images: set-up per image, one launch for all
+// their decisions, then each image's finishing work on a host thread of its
+// own (the calling thread for one image).  Every image's bytes are those of
+// encoding it alone.
+void encode_jobs(std::vector<Job>& jobs) {
+  const int n = (int)jobs.size();
+  Buffers buf(n);
+  for (int i = 0; i < n; ++i) jobs[(size_t)i].rc = job_setup(jobs[(size_t)i], buf, i);
+  const int rc = decide_all(jobs, buf);
+  for (Job& j : jobs)
+    if (j.rc == MT_OK && rc != MT_OK) j.rc = rc;
+  if (n == 1) {
+    if (jobs[0].rc == MT_OK) jobs[0].rc = job_finish(jobs[0], buf, 0);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int i = 0; i < n; ++i)
+    if (jobs[(size_t)i].rc == MT_OK)
+      pool.emplace_back([&jobs, &buf, i]() { jobs[(size_t)i].rc = job_finish(jobs[(size_t)i], buf, i); });
+  for (std::thread& t : pool) t.join();
+}
+
+int encode_one(const uint8_t* rgb, bool rgb_on_device, const uint8_t* const* yuv, uint32_t width, uint32_t height,
+               const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3],
+               mt_encode_stats* stats) {
+  std::vector<Job> jobs(1);
+  Job& j = jobs[0];
+  j.rgb = rgb;
+  j.rgb_on_device = rgb_on_device;
+  j.yuv = yuv;
+  j.width = width;
+  j.height = height;
+  j.cfg = cfg;
+  j.out = out;
+  j.out_len = out_len;
+  j.recon_out = recon_out;
+  j.stats = stats;
+  encode_jobs(jobs);
+  return j.rc;
+}
+
+}  // namespace
+
+extern "C" {
+
 int mt_encode_rgb8_ex(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
                       uint8_t** out, size_t* out_len, uint16_t* recon_out[3], mt_encode_stats* stats) {
   if (!rgb) return MT_ERR_INVALID_INPUT;
-  return encode_impl(rgb, false, nullptr, width, height, cfg, out, out_len, recon_out, stats);
+  return encode_one(rgb, false, nullptr, width, height, cfg, out, out_len, recon_out, stats);
 }
 
 int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
@@ -1084,7 +1285,42 @@ int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt
 int mt_encode_rgb8_device(const uint8_t* d_rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg,
                           uint8_t** out, size_t* out_len, mt_encode_stats* stats) {
   if (!d_rgb) return MT_ERR_INVALID_INPUT;
-  return encode_impl(d_rgb, true, nullptr, width, height, cfg, out, out_len, nullptr, stats);
+  return encode_one(d_rgb, true, nullptr, width, height, cfg, out, out_len, nullptr, stats);
+}
+
+int mt_encode_rgb8_batch(int32_t n, const uint8_t* const* rgb, const uint32_t* widths, const uint32_t* heights,
+                         const mt_encode_config* cfgs, uint8_t** outs, size_t* out_lens, int32_t* rcs,
+                         mt_encode_stats* stats) {
+  if (n < 1 || n > 64 || !rgb || !widths || !heights || !cfgs || !outs || !out_lens) return MT_ERR_INVALID_INPUT;
+  std::vector<Job> jobs((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    Job& j = jobs[(size_t)i];
+    outs[i] = nullptr;
+    out_lens[i] = 0;
+    j.rgb = rgb[i];
+    j.width = widths[i];
+    j.height = heights[i];
+    j.cfg = &cfgs[i];
+    j.out = &outs[i];
+    j.out_len = &out_lens[i];
+    j.stats = stats ? &stats[i] : nullptr;
+    if (!rgb[i]) j.rc = MT_ERR_INVALID_INPUT;
+  }
+  std::vector<Job> live;  // images with an input: the others keep their code
+  std::vector<int> idx;
+  for (int i = 0; i < n; ++i)
+    if (jobs[(size_t)i].rgb) {
+      idx.push_back(i);
+      live.push_back(std::move(jobs[(size_t)i]));
+    }
+  encode_jobs(live);
+  int first = MT_OK;
+  for (size_t k = 0; k < live.size(); ++k) jobs[(size_t)idx[k]].rc = live[k].rc;
+  for (int i = 0; i < n; ++i) {
+    if (rcs) rcs[i] = jobs[(size_t)i].rc;
+    if (first == MT_OK && jobs[(size_t)i].rc != MT_OK) first = jobs[(size_t)i].rc;
+  }
+  return first;
 }
 
 void mt_encode_release_buffers(void) {
@@ -1093,15 +1329,16 @@ void mt_encode_release_buffers(void) {
   for (int d = 0; d < 16; ++d) {
     Arena& ar = g_arenas[d];
     std::lock_guard<std::mutex> lock(ar.mu);
-    bool any = false;
-    for (int s = 0; s < kSlots; ++s) any |= ar.p[s] != nullptr;
-    if (!any) continue;
+    if (ar.sets.empty()) continue;
     cudaSetDevice(d);
-    for (int s = 0; s < kSlots; ++s) {
-      cudaFree(ar.p[s]);
-      ar.p[s] = nullptr;
-      ar.cap[s] = 0;
+    for (BufSet& b : ar.sets) {
+      for (void*& q : b.p) {
+        cudaFree(q);
+        q = nullptr;
+      }
+      if (b.st) cudaStreamDestroy(b.st);
     }
+    ar.sets.clear();
   }
   cudaSetDevice(cur);
 }
@@ -1110,7 +1347,7 @@ int mt_encode_yuv8(const uint8_t* y, const uint8_t* u, const uint8_t* v, uint32_
                    const mt_encode_config* cfg, uint8_t** out, size_t* out_len, uint16_t* recon_out[3]) {
   const uint8_t* planes[3] = {y, u, v};
   if (!y || !u || !v) return MT_ERR_INVALID_INPUT;
-  return encode_impl(nullptr, false, planes, width, height, cfg, out, out_len, recon_out, nullptr);
+  return encode_one(nullptr, false, planes, width, height, cfg, out, out_len, recon_out, nullptr);
 }
 
 }  // extern "C"

@@ -61,3 +61,31 @@ def encode_yuv8(y, u, v, cfg, want_recon=False):
            "mt_encode_yuv8")
     data = _take(out, n.value)
     return (data, planes) if want_recon else data
+
+
+def encode_rgb8_batch(images, cfgs=None, stats=None):
+    """mt_encode_rgb8_batch: a list of (h, w, 3) uint8 images (and one config
+    per image, or one for all) encoded in one call.  Returns the list of AVIF
+    bytes; raises on the first failing image.  ``stats``: a list of
+    abi.EncodeStats to fill, one per image."""
+    n = len(images)
+    imgs = [np.ascontiguousarray(im, np.uint8) for im in images]
+    if cfgs is None or isinstance(cfgs, abi.EncodeConfig):
+        cfgs = [cfgs if cfgs is not None else config()] * n
+    carr = (abi.EncodeConfig * n)(*cfgs)
+    ptrs = (C.c_void_p * n)(*[im.ctypes.data for im in imgs])
+    ws = (C.c_uint32 * n)(*[im.shape[1] for im in imgs])
+    hs = (C.c_uint32 * n)(*[im.shape[0] for im in imgs])
+    outs = (C.c_void_p * n)()
+    lens = (C.c_size_t * n)()
+    rcs = (C.c_int32 * n)()
+    st = (abi.EncodeStats * n)() if stats is not None else None
+    rc = load().mt_encode_rgb8_batch(n, ptrs, ws, hs, carr, outs, lens, rcs, st)
+    res = []
+    for i in range(n):
+        res.append(_take(C.c_void_p(outs[i]), lens[i]) if outs[i] else None)
+    if stats is not None:
+        for i in range(n):
+            C.memmove(C.byref(stats[i]), C.byref(st[i]), C.sizeof(abi.EncodeStats))
+    _check(rc, "mt_encode_rgb8_batch")
+    return res

@@ -126,3 +126,18 @@ def test_reused_device_buffers_give_the_same_bytes(mt_lib, cuda):
     assert enc.encode_rgb8(big, cfg) == a and enc.encode_rgb8(small, cfg) == b
     mt_lib.load().mt_encode_release_buffers()
     assert enc.encode_rgb8(small, cfg) == b and enc.encode_rgb8(big, cfg) == a
+
+
+def test_batch_encode_equals_each_image_alone(mt_lib, cuda):
+    """mt_encode_rgb8_batch: images of different sizes, chroma formats and
+    qualities decided in one persistent launch give, each, the bytes of
+    encoding it alone (and a batch of one is the single call)."""
+    from maroontree_b200 import encoder as enc
+
+    shapes = [(640, 360, 60, 0), (203, 117, 80, 0), (512, 512, 40, 2), (136, 72, 55, 2), (64, 64, 90, 0)]
+    imgs = [synth.generate_rgb(w, h, 30 + k) for k, (w, h, _, _) in enumerate(shapes)]
+    cfgs = [enc.config(quality=q, chroma=c) for (_, _, q, c) in shapes]
+    batch = enc.encode_rgb8_batch(imgs, cfgs)
+    alone = [enc.encode_rgb8(im, c) for im, c in zip(imgs, cfgs)]
+    assert batch == alone
+    assert enc.encode_rgb8_batch(imgs[:1], cfgs[0]) == alone[:1]
