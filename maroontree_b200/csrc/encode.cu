@@ -117,6 +117,10 @@ __device__ __forceinline__ bool is_smooth(int m) { return m == MT_SMOOTH_PRED ||
 // mode * 7 + type, the order ties are broken in) and runs them type by type,
 // so the four octets of a warp mostly share a transform path.
 constexpr int kClusterCtas = 4;
+// CTAs of the decision kernel resident per SM (its register budget follows).
+#ifndef MT_ENC_CTAS_PER_SM
+#define MT_ENC_CTAS_PER_SM 2
+#endif
 constexpr int kCandPerCta = 23;
 constexpr int kLumaThreads = 192;  // 23 octets, rounded up to whole warps
 constexpr int kStepThreads = kLumaThreads + 32;
@@ -206,7 +210,7 @@ constexpr int kMaxPolls = 1 << 20;               // a dependency wait gives up a
 // took earlier.  A wait that runs out of polls sets *err; once *err is set
 // the remaining waits stop and every cluster leaves at its next ticket.
 // list[i] = block index | have-top-right (bit 30) | left-has-bottom (bit 31).
-__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThreads)
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThreads, MT_ENC_CTAS_PER_SM)
     encode_blocks_kernel(const JobDesc* __restrict__ jobs, const uint2* __restrict__ list, int nlist,
                          uint32_t* ticket_ctr, uint32_t* err) {
   __shared__ StepShared S;
@@ -931,8 +935,8 @@ int decide_all(std::vector<Job>& jobs, Buffers& buf) {
       cudaMemsetAsync(d_ctl, 0, 8, ks) != cudaSuccess)
     return MT_ERR_DEVICE;
   // one cluster per block that can run at once (the widest merged level), at
-  // most 74 clusters (two CTAs on each of the 148 SMs)
-  const int nclusters = std::min(width_max, 74);
+  // most as many as the SMs hold
+  const int nclusters = std::min(width_max, 148 * MT_ENC_CTAS_PER_SM / kClusterCtas);
   for (int d : slot) {
     jobs[(size_t)d].cs->h2d(jobs[(size_t)d].sched.size() * 8 + sizeof(JobDesc));
     jobs[(size_t)d].cs->mark(1, ks);
