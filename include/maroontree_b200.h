@@ -1205,7 +1205,10 @@ int mt_emit_coeffs(const int32_t* levels, size_t nlevels, const mt_coef_block* b
  * angle delta 0) x (7 intra transform types) luma candidate of the candidate
  * chain, chroma UV_DC_PRED / DCT_DCT; the output is therefore a valid AVIF
  * with this library's own decisions, not the reference's bytes.  4:2:0 and
- * 4:4:4 (else MT_ERR_UNSUPPORTED_CHROMA_FORMAT).  *out is freed with mt_free. */
+ * 4:4:4 (else MT_ERR_UNSUPPORTED_CHROMA_FORMAT).  The frame is coded in the
+ * reference's spec-minimum uniform tiling (mt_tiling_spec_min: one tile up to
+ * 64 superblocks wide and 2304 in area, e.g. 1 x 2 tiles at 4096x4096), the
+ * tiles' decisions and range coding independent.  *out is freed with mt_free. */
 int mt_encode_rgb8(const uint8_t* rgb, uint32_t width, uint32_t height, const mt_encode_config* cfg, uint8_t** out,
                    size_t* out_len);
 /* What one encode call did, for measurement: the bytes it copied between the

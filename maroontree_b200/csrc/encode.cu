@@ -16,10 +16,14 @@
 // frame headers and the AVIF container.  The result decodes under any AV1
 // decoder to the reconstruction this encoder computed.
 //
-// Schedule: superblocks in the d = 2 * row + col wavefront (each needs its
-// left, top and top-right neighbours), one launch per diagonal and one CTA
-// per superblock; inside a CTA the 8x8 blocks go in z-order, the 91 luma
-// candidates of a block one per thread, the CTA minimum picks the winner.
+// Schedule: one persistent launch of 4-CTA clusters takes the frame's 8x8
+// blocks from a ticket counter in dependency-level order (a block after its
+// left, top, top-left and, where its edges use them, top-right and
+// bottom-left neighbours inside its tile) and waits on those neighbours'
+// done counts with bounded polls.  The 91 luma candidates of a block are
+// split over the cluster's CTAs, each evaluated by eight lanes; the cluster
+// minimum picks the winner.  Frames code in the spec-minimum uniform tiling
+// (one tile up to 64 superblocks wide and 2304 in area), tiles independent.
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -60,6 +64,7 @@ struct EncArgs {
   int sub;                 // 0 4:4:4, 2 4:2:0
   int sb_cols;
   int w8, h8;
+  int tile_w8, tile_h8;    // the uniform tile size in 8x8 blocks (the last tile may be smaller)
   uint8_t* mode;           // per 8x8 block (frame raster of 8x8 blocks)
   uint8_t* tx;
   int32_t* lv_y;           // 64 per block
@@ -181,14 +186,15 @@ __device__ __forceinline__ void put8(const mtd::Oct8& o, const int16_t* pred, in
 
 // A block's neighbours (above run of 17 from (ox - 1, oy - 1), left run of 16
 // from (ox - 1, oy)) into shared memory for lanes k in [0, 33), read past L1
-// (they were written by other SMs); positions outside the plane are clamped
-// (never read by the predictor).
-__device__ __forceinline__ void stage_edges(const uint16_t* rec, int stride, int fw, int fh, int ox, int oy,
-                                            int16_t* above, int16_t* left, int k) {
+// (they were written by other SMs); only the sides inside the block's tile are
+// read, and positions outside the plane are clamped (never read by the
+// predictor).
+__device__ __forceinline__ void stage_edges(const uint16_t* rec, int stride, int fw, int fh, int ox, int oy, bool top,
+                                            bool lft, int16_t* above, int16_t* left, int k) {
   if (k < 17) {
-    if (oy > 0) above[k] = (int16_t)__ldcg(rec + (size_t)(oy - 1) * stride + min(max(ox - 1 + k, 0), fw - 1));
+    if (top) above[k] = (int16_t)__ldcg(rec + (size_t)(oy - 1) * stride + min(max(ox - 1 + k, 0), fw - 1));
   } else if (k < 33) {
-    if (ox > 0) left[k - 17] = (int16_t)__ldcg(rec + (size_t)min(oy + k - 17, fh - 1) * stride + ox - 1);
+    if (lft) left[k - 17] = (int16_t)__ldcg(rec + (size_t)min(oy + k - 17, fh - 1) * stride + ox - 1);
   }
 }
 
@@ -273,14 +279,20 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
     const int bx = b % nbx, by = b / nbx;
     const int px = bx * 8, py = by * 8;
     const bool thr = (e >> 30) & 1, lhb = (e >> 31) & 1;
-    const bool have_tr = thr && py > 0 && px + 8 < a.w8;
-    const bool have_bl = lhb && px > 0 && py + 8 < a.h8;
+    // the block's tile: neighbours outside it are unavailable (AV1 intra edges
+    // and contexts stop at tile edges); the predictor works in tile coordinates
+    const int tx0 = bx - bx % a.tile_w8, ty0 = by - by % a.tile_h8;
+    const int tx1 = min(tx0 + a.tile_w8, nbx), ty1 = min(ty0 + a.tile_h8, a.h8 / 8);
+    const bool has_l = bx > tx0, has_t = by > ty0;
+    const bool have_tr = thr && has_t && bx + 1 < tx1;
+    const bool have_bl = lhb && has_l && by + 1 < ty1;
     const uint8_t flags = (have_tr ? 1 : 0) | (have_bl ? 2 : 0);
+    const int rx = px - tx0 * 8, ry = py - ty0 * 8;  // tile-relative position
     if (t < 5) {  // one thread per dependency
       int dep = -1;
-      if (t == 0 && bx > 0) dep = b - 1;
-      if (t == 1 && by > 0) dep = b - nbx;
-      if (t == 2 && bx > 0 && by > 0) dep = b - nbx - 1;
+      if (t == 0 && has_l) dep = b - 1;
+      if (t == 1 && has_t) dep = b - nbx;
+      if (t == 2 && has_l && has_t) dep = b - nbx - 1;
       if (t == 3 && have_tr) dep = b - nbx + 1;
       if (t == 4 && have_bl) dep = b + nbx - 1;
       if (dep >= 0) {
@@ -298,15 +310,17 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
     __syncthreads();
     // the block's neighbours and source samples
     if (t < 33) {
-      stage_edges(a.rec[0], a.py.stride, a.w8, a.h8, px, py, S.above[0], S.left[0], t);
+      stage_edges(a.rec[0], a.py.stride, a.w8, a.h8, px, py, has_t, has_l, S.above[0], S.left[0], t);
     } else if (t >= 64 && t < 128) {
       const int i = t - 64;
       S.src[i] = a.src[0][(size_t)(py + (i >> 3)) * a.py.stride + px + (i & 7)];
     } else if (rank >= 2 && c >= 0) {
       const int cx = a.sub ? px / 2 : px, cy = a.sub ? py / 2 : py, n = a.sub ? 4 : 8;
-      stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, S.above[1], S.left[1], c);
+      stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, has_t, has_l, S.above[1],
+                  S.left[1], c);
       if (c == 0)
-        stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, S.above[1], S.left[1], 32);
+        stage_edges(a.rec[1 + pl], a.pc.stride, a.pc.frame_w, a.pc.frame_h, cx, cy, has_t, has_l, S.above[1],
+                    S.left[1], 32);
       if (n == 8)
         for (int i = c; i < 64; i += 32) S.csrc[i] = a.src[1 + pl][(size_t)(cy + i / 8) * a.pc.stride + cx + (i % 8)];
     }
@@ -314,12 +328,12 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
     if (t < kLumaThreads) {
       const mtd::Octet g;
       const int o = t >> 3;
-      const bool ft = (py > 0 && is_smooth(__ldcg(a.mode + b - nbx))) || (px > 0 && is_smooth(__ldcg(a.mode + b - 1)));
+      const bool ft = (has_t && is_smooth(__ldcg(a.mode + b - nbx))) || (has_l && is_smooth(__ldcg(a.mode + b - 1)));
       mt_candidate cd = {};
-      cd.px = (uint16_t)px;
-      cd.py = (uint16_t)py;
+      cd.px = (uint16_t)rx;
+      cd.py = (uint16_t)ry;
       cd.flags = flags | (ft ? 4 : 0);
-      const mtd::EdgeRead rd{S.above[0], S.left[0], px, py};
+      const mtd::EdgeRead rd{S.above[0], S.left[0], rx, ry};
       if (o < 4 && mlo + o < 13) {
         cd.mode = (uint8_t)(mlo + o);
         mtd::coop8_predict(rd, a.py, cd, S.pred[o], S.edge[o], g);
@@ -339,12 +353,12 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
       if (a.sub == 0 && c < 8) {
         const mtd::Octet g;
         mt_candidate cc = {};
-        cc.px = (uint16_t)px;
-        cc.py = (uint16_t)py;
+        cc.px = (uint16_t)rx;
+        cc.py = (uint16_t)ry;
         cc.flags = flags;
         cc.mode = MT_DC_PRED;
         cc.tx_type = MT_TX_DCT_DCT;
-        mtd::coop8_predict(mtd::EdgeRead{S.above[1], S.left[1], px, py}, a.pc, cc, S.cpred, S.edge[4], g);
+        mtd::coop8_predict(mtd::EdgeRead{S.above[1], S.left[1], rx, ry}, a.pc, cc, S.cpred, S.edge[4], g);
         g.sync();
         mt_candidate_result r;
         mtd::Oct8& oc = S.oct[kLumaThreads / 8];
@@ -355,13 +369,15 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
         mt_candidate cc = {};
         cc.mode = MT_DC_PRED;
         cc.tx_type = MT_TX_DCT_DCT;
-        cc.px = (uint16_t)(px / 2);
-        cc.py = (uint16_t)(py / 2);
+        cc.px = (uint16_t)(rx / 2);
+        cc.py = (uint16_t)(ry / 2);
         mt_candidate_result r;
         int32_t st4[mtd::kWork4Words];
         mtd::Work4 w4{st4};
-        mtd::chain4_one_rd<false>(a.src[1 + pl], mtd::EdgeRead{S.above[1], S.left[1], cc.px, cc.py}, a.pc, a.qc,
-                                  a.tlc, a.has_qm_c ? S.qmC : nullptr, S.qsC, S.lut, S.cc, cc, r, w4);
+        // the source plane from the tile's origin, so that tile coordinates address it
+        const uint16_t* tsrc = a.src[1 + pl] + (size_t)(ty0 * 4) * a.pc.stride + tx0 * 4;
+        mtd::chain4_one_rd<false>(tsrc, mtd::EdgeRead{S.above[1], S.left[1], cc.px, cc.py}, a.pc, a.qc, a.tlc,
+                                  a.has_qm_c ? S.qmC : nullptr, S.qsC, S.lut, S.cc, cc, r, w4);
         const int16_t* cf = w4.cf();
         const int16_t* pr = w4.pred();
         const int16_t* rr = w4.rr();
@@ -369,7 +385,7 @@ __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kStepThre
         for (int i = 0; i < 16; ++i) lv[i] = cf[i];
         for (int y = 0; y < 4; ++y)
           for (int x = 0; x < 4; ++x)
-            a.rec[1 + pl][(size_t)(cc.py + y) * a.pc.stride + cc.px + x] =
+            a.rec[1 + pl][(size_t)(py / 2 + y) * a.pc.stride + px / 2 + x] =
                 (uint16_t)min(max((int)pr[y * 4 + x] + rr[y * 4 + x], 0), 255);
       }
     }
@@ -516,6 +532,32 @@ struct BlockSyntax {
     }
     a_mode[bx4] = a_mode[bx4 + 1] = (uint8_t)m;
     l_mode[by4] = l_mode[by4 + 1] = (uint8_t)m;
+  }
+
+  // clear_above_context at a tile's start for its 8x8 columns [x0, x1), and
+  // clear_left_context at each superblock row of a tile for rows [y0, y1):
+  // the values of an unavailable neighbour.
+  void clear_above(int x0, int x1) {
+    for (int x = x0; x < x1; ++x) a_part[x] = 0;
+    for (int x = 2 * x0; x < 2 * x1; ++x) {
+      a_skip[x] = a_mode[x] = 0;
+      a_tx[x] = -1;
+    }
+    for (int p = 0; p < 3; ++p) {
+      const int k = (p == 0 || sub == 0) ? 2 : 1;
+      for (int x = k * x0; x < k * x1; ++x) a_coef[p][x] = 0x40;
+    }
+  }
+  void clear_left(int y0, int y1) {
+    for (int y = y0; y < y1; ++y) l_part[y] = 0;
+    for (int y = 2 * y0; y < 2 * y1; ++y) {
+      l_skip[y] = l_mode[y] = 0;
+      l_tx[y] = -1;
+    }
+    for (int p = 0; p < 3; ++p) {
+      const int k = (p == 0 || sub == 0) ? 2 : 1;
+      for (int y = k * y0; y < k * y1; ++y) l_coef[p][y] = 0x40;
+    }
   }
 
   // After a block's coefficient contexts are known: its res_ctx bytes.
@@ -667,6 +709,8 @@ struct Job {
   // the frame
   mt_encode_plan plan = {};
   int sub = 0, sx = 0, nbx = 0, nby = 0, nb = 0, sb_cols = 0, sb_rows = 0, cl = 0;
+  int32_t tcl = 0, trl = 0;      // TileColsLog2, TileRowsLog2
+  int tile_sb_w = 0, tile_sb_h = 0;  // the uniform tile size in superblocks
   int32_t pw = 0, ph = 0, pcw = 0, pch = 0;
   size_t ny = 0, nc = 0;
   EncArgs a = {};
@@ -720,8 +764,12 @@ int job_setup(Job& j, Buffers& buf, int i) {
   const int32_t pw = j.pw, ph = j.ph, pcw = j.pcw, pch = j.pch;
   const int nbx = j.nbx = pw / 8, nby = j.nby = ph / 8, nb = j.nb = nbx * nby;
   const int sb_cols = j.sb_cols = (pw + 63) / 64, sb_rows = j.sb_rows = (ph + 63) / 64;
-  // one tile: the AV1 maximum tile width (64 superblocks) and area (2304)
-  if (sb_cols > 64 || sb_cols * sb_rows > 2304) return MT_ERR_UNSUPPORTED;
+  // the spec-minimum uniform tiling (src/coder/frame_encode.rs:75-80): one
+  // tile unless the frame exceeds the AV1 maximum tile width (64 superblocks)
+  // or area (2304 superblocks)
+  if ((rc = mt_tiling_spec_min(pw, ph, &j.tcl, &j.trl)) != MT_OK) return rc;
+  j.tile_sb_w = (sb_cols + (1 << j.tcl) - 1) >> j.tcl;
+  j.tile_sb_h = (sb_rows + (1 << j.trl) - 1) >> j.trl;
   const int cl = j.cl = sub ? 16 : 64;  // chroma levels per block
   // quantisers, QM rows, default CDF slices and their bit costs, lambdas
   mt_quant qy, qc;
@@ -823,6 +871,8 @@ int job_setup(Job& j, Buffers& buf, int i) {
   a.sb_cols = sb_cols;
   a.w8 = pw;
   a.h8 = ph;
+  a.tile_w8 = j.tile_sb_w * 8;
+  a.tile_h8 = j.tile_sb_h * 8;
   a.mode = d_decs;
   a.tx = a.mode + nb;
   a.lv_y = d_levels;
@@ -839,7 +889,7 @@ int job_setup(Job& j, Buffers& buf, int i) {
     return MT_ERR_DEVICE;
   // Dependency levels of the 8x8 blocks: a block needs its left, top,
   // top-left neighbours and, where the intra edge uses them, its top-right and
-  // bottom-left ones.
+  // bottom-left ones, all inside its tile (tiles are independent).
   std::vector<int32_t> T((size_t)nb, -1);
   std::vector<uint32_t> entry((size_t)nb);
   std::vector<int> cnt;
@@ -851,13 +901,16 @@ int job_setup(Job& j, Buffers& buf, int i) {
         zorder(k, &bx, &by, &thr, &lhb);
         const int x = sc * 8 + bx, y = sr * 8 + by;
         if (x >= nbx || y >= nby) continue;
-        const bool tr = thr && y > 0 && (x + 1) * 8 < pw;
-        const bool bl = lhb && x > 0 && (y + 1) * 8 < ph;
+        const int tx0 = x - x % a.tile_w8, ty0 = y - y % a.tile_h8;
+        const int tx1 = std::min(tx0 + a.tile_w8, nbx), ty1 = std::min(ty0 + a.tile_h8, nby);
+        const bool has_l = x > tx0, has_t = y > ty0;
+        const bool tr = thr && has_t && x + 1 < tx1;
+        const bool bl = lhb && has_l && y + 1 < ty1;
         int lv = 0;
         auto dep = [&](int xx, int yy) { lv = std::max(lv, T[(size_t)yy * nbx + xx] + 1); };
-        if (x > 0) dep(x - 1, y);
-        if (y > 0) dep(x, y - 1);
-        if (x > 0 && y > 0) dep(x - 1, y - 1);
+        if (has_l) dep(x - 1, y);
+        if (has_t) dep(x, y - 1);
+        if (has_l && has_t) dep(x - 1, y - 1);
         if (tr) dep(x + 1, y - 1);
         if (bl) dep(x - 1, y + 1);
         const size_t bi = (size_t)y * nbx + x;
@@ -936,7 +989,11 @@ int decide_all(std::vector<Job>& jobs, Buffers& buf) {
     return MT_ERR_DEVICE;
   // one cluster per block that can run at once (the widest merged level), at
   // most as many as the SMs hold
-  const int nclusters = std::min(width_max, 148 * MT_ENC_CTAS_PER_SM / kClusterCtas);
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+    return MT_ERR_DEVICE;
+  const int nclusters = std::max(1, std::min(width_max, sms * MT_ENC_CTAS_PER_SM / kClusterCtas));
   for (int d : slot) {
     jobs[(size_t)d].cs->h2d(jobs[(size_t)d].sched.size() * 8 + sizeof(JobDesc));
     jobs[(size_t)d].cs->mark(1, ks);
@@ -1011,22 +1068,36 @@ int job_finish(Job& j, Buffers& buf, int i) {
     bs.l_coef[p].assign(nby * 2, 0x40);
   }
   bs.blocks = &blocks;
-  for (int sr = 0; sr < sb_rows; ++sr)
-    for (int sc = 0; sc < sb_cols; ++sc) {
-      bs.sbs.emplace_back();
-      bs.out = &bs.sbs.back();
-      int cp = -1;
-      bs.node(1, sc * 8, sr * 8, 8, &cp, [&](int x8, int y8) {
-        const size_t first = blocks.size();
-        bs.block8(x8, y8, &cp);
-        const int b = y8 * nbx + x8;
-        const uint32_t off[3] = {(uint32_t)((size_t)b * 64), (uint32_t)((size_t)nb * 64 + (size_t)b * cl),
-                                 (uint32_t)((size_t)nb * (64 + cl) + (size_t)b * cl)};
-        for (int p = 0; p < 3; ++p) blocks[first + p].cf_offset = off[p];
-        bs.commit_res(x8, y8, &resb[(size_t)b * 3]);
-      });
-      bs.cdef_points.push_back(cp);
+  // tiles in raster order, superblocks in raster order inside each tile
+  // (decode_tile: the above context cleared per tile, the left per SB row)
+  std::vector<int> tile_first;  // first coded superblock of each tile
+  std::vector<int> sb_unit;     // frame-raster 64x64 unit of each coded superblock
+  for (int r0 = 0; r0 < sb_rows; r0 += j.tile_sb_h)
+    for (int c0 = 0; c0 < sb_cols; c0 += j.tile_sb_w) {
+      const int r1 = std::min(r0 + j.tile_sb_h, sb_rows), c1 = std::min(c0 + j.tile_sb_w, sb_cols);
+      tile_first.push_back((int)bs.sbs.size());
+      bs.clear_above(c0 * 8, std::min(c1 * 8, nbx));
+      for (int sr = r0; sr < r1; ++sr) {
+        bs.clear_left(sr * 8, std::min(sr * 8 + 8, nby));
+        for (int sc = c0; sc < c1; ++sc) {
+          bs.sbs.emplace_back();
+          bs.out = &bs.sbs.back();
+          sb_unit.push_back(sr * sb_cols + sc);
+          int cp = -1;
+          bs.node(1, sc * 8, sr * 8, 8, &cp, [&](int x8, int y8) {
+            const size_t first = blocks.size();
+            bs.block8(x8, y8, &cp);
+            const int b = y8 * nbx + x8;
+            const uint32_t off[3] = {(uint32_t)((size_t)b * 64), (uint32_t)((size_t)nb * 64 + (size_t)b * cl),
+                                     (uint32_t)((size_t)nb * (64 + cl) + (size_t)b * cl)};
+            for (int p = 0; p < 3; ++p) blocks[first + p].cf_offset = off[p];
+            bs.commit_res(x8, y8, &resb[(size_t)b * 3]);
+          });
+          bs.cdef_points.push_back(cp);
+        }
+      }
     }
+  tile_first.push_back((int)bs.sbs.size());
   // coefficient tokens of every block in one launch
   const int ncb = (int)blocks.size();
   mt_coef_block* d_blocks = buf.get<mt_coef_block>(i, kEmit, (size_t)ncb * (sizeof(mt_coef_block) + 8) + 8);
@@ -1158,14 +1229,36 @@ int job_finish(Job& j, Buffers& buf, int i) {
       return MT_ERR_DEVICE;
     cs.d2h((ny + 2 * nc) * 2);
   }
-  // the tile, in one pass with each superblock's cdef_idx at its read_cdef()
-  // point (the 64x64 CDEF units are the superblocks of the one tile)
-  uint8_t* tile = nullptr;
-  size_t tile_len = 0;
-  if ((rc = mt_pack_tile_filtered(j.plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data(), cdef_pt.data(),
-                                  (int32_t)bs.sbs.size(), dec.bits > 0 ? grid.data() : nullptr,
-                                  dec.bits > 0 ? dec.bits : 0, &tile, &tile_len)) != MT_OK)
-    return rc;
+  // each tile in one pass of its range coder, with each superblock's
+  // cdef_idx (its 64x64 unit's) at its read_cdef() point; tiles are coded
+  // independently, on threads of their own when there are several
+  const int ntiles = (int)tile_first.size() - 1;
+  std::vector<uint8_t> sb_idx(sb_unit.size());
+  for (size_t k2 = 0; k2 < sb_unit.size(); ++k2) sb_idx[k2] = grid[(size_t)sb_unit[k2]];
+  std::vector<uint8_t*> tiles((size_t)ntiles, nullptr);
+  std::vector<size_t> tile_lens((size_t)ntiles, 0);
+  std::vector<int> tile_rc((size_t)ntiles, MT_OK);
+  auto pack = [&](int t) {
+    const int f = tile_first[(size_t)t], n = tile_first[(size_t)t + 1] - f;
+    tile_rc[(size_t)t] = mt_pack_tile_filtered(j.plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data() + f,
+                                               cdef_pt.data() + f, n, dec.bits > 0 ? sb_idx.data() + f : nullptr,
+                                               dec.bits > 0 ? dec.bits : 0, &tiles[(size_t)t], &tile_lens[(size_t)t]);
+  };
+  if (ntiles == 1) {
+    pack(0);
+  } else {
+    std::vector<std::thread> workers;
+    for (int t = 0; t < ntiles; ++t) workers.emplace_back(pack, t);
+    for (std::thread& w : workers) w.join();
+  }
+  auto free_tiles = [&]() {
+    for (uint8_t* t : tiles) free(t);
+  };
+  for (int r2 : tile_rc)
+    if (r2 != MT_OK) {
+      free_tiles();
+      return r2;
+    }
   // headers and container
   mt_sequence_header_params sp = {};
   sp.width = width;
@@ -1194,12 +1287,13 @@ int job_finish(Job& j, Buffers& buf, int i) {
   fp.cdef_damping = dec.bits >= 0 ? dec.damping : 3;
   for (int e = 0; e < dec.n_strengths && e < 8; ++e)
     for (int q = 0; q < 4; ++q) fp.cdef_strengths[e][q] = dec.strengths[e][q];
-  const uint8_t* tiles[1] = {tile};
-  const size_t tl[1] = {tile_len};
+  fp.tile_cols_log2 = j.tcl;
+  fp.tile_rows_log2 = j.trl;
+  std::vector<const uint8_t*> ctiles(tiles.begin(), tiles.end());
   uint8_t* obu = nullptr;
   size_t obu_len = 0;
-  rc = mt_av1_stream(&sp, &fp, tiles, tl, 1, &obu, &obu_len);
-  free(tile);
+  rc = mt_av1_stream(&sp, &fp, ctiles.data(), tile_lens.data(), ntiles, &obu, &obu_len);
+  free_tiles();
   if (rc != MT_OK) return rc;
   mt_avif_item_params ip = {};
   ip.width = width;

@@ -6,7 +6,10 @@ a sum of six 2-D sinusoids (1-40 cycles/image, random phase, amplitude <= 60)
 over mid-grey, twelve hard-edged rectangles (six axis-aligned, six rotated)
 in uniform colours, then Gaussian noise, rounded half away from zero and
 clamped to 0..255.  The 1080p variant adds a 64-px-period texture band and a
-smooth gradient quadrant.  A xoshiro128** stream drives every draw.
+smooth gradient quadrant.  The large variant (the 4096x4096 frame) keeps the
+noise to the left half and makes the right half piecewise constant: a grid
+of cells with seeded cut positions, each in one uniform colour.  A
+xoshiro128** stream drives every draw.
 """
 import numpy as np
 
@@ -80,8 +83,22 @@ def generate_rgb(w, h, seed, sigma=4.0, variant="plain"):
         g = 255.0 * ((xx - w // 2) + (yy - h // 2)) / (w / 2 + h / 2)
         for c in range(3):
             img[c][q] = g[q]
+    half = None
+    if variant == "large":
+        half = xx >= w // 2
+        xs = np.sort(np.array([w // 2] + [int(rng.uniform(w // 2, w)) for _ in range(15)] + [w]))
+        ys = np.sort(np.array([0] + [int(rng.uniform(0, h)) for _ in range(15)] + [h]))
+        cx = np.searchsorted(xs, xx[0], side="right") - 1
+        cy = np.searchsorted(ys, yy[:, 0], side="right") - 1
+        cols = np.array([[rng.randint(0, 255) for _ in range(3)] for _ in range(len(xs) * len(ys))], np.float64)
+        cell = cy[:, None] * len(xs) + cx[None, :]
+        for c in range(3):
+            img[c][half] = cols[cell, c][half]
     noise_rng = np.random.default_rng(rng.next_u32())
-    img = img + noise_rng.normal(0.0, sigma, size=img.shape)
+    noise = noise_rng.normal(0.0, sigma, size=img.shape)
+    if half is not None:
+        noise[:, half] = 0.0
+    img = img + noise
     img = np.where(img >= 0, np.floor(img + 0.5), np.ceil(img - 0.5))
     return np.clip(img, 0, 255).astype(np.uint8).transpose(1, 2, 0).copy()
 

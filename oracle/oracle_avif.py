@@ -8,11 +8,11 @@ encode.
     wavefront on host threads);
   * deblocking with the shipped levels and the CDEF decision: the oracle's
     frame filters;
-  * block syntax, coefficient tokens and the tile's range coding with the
+  * block syntax, coefficient tokens and each tile's range coding with the
     cdef_idx literals: or_encode_pack;
   * headers and the AVIF container, restated here from src/bitwriter.rs,
-    src/obu.rs and src/isobmff.rs for the subset the encoder writes (one tile,
-    reduced still-picture header, lossy frame header without segmentation,
+    src/obu.rs and src/isobmff.rs for the subset the encoder writes (the
+    spec-minimum uniform tiling, reduced still-picture header, lossy frame header without segmentation,
     delta-q, IntraBC or restoration; a colour item with ispe, pixi, av1C and
     an nclx colr).
 """
@@ -34,13 +34,13 @@ def _lib():
     lib = po.load()
     if not _bound:
         lib.or_encode_decide.restype = C.c_int
-        lib.or_encode_decide.argtypes = [C.c_int32] * 3 + [C.POINTER(abi.ChainParams)] * 2 + \
+        lib.or_encode_decide.argtypes = [C.c_int32] * 5 + [C.POINTER(abi.ChainParams)] * 2 + \
             [C.POINTER(abi.Quant)] * 2 + [_P, _P] + [C.POINTER(abi.CoefCdfs)] * 2 + [_P] * 11 + [C.c_int32]
         lib.or_encode_pack.restype = C.c_int
-        lib.or_encode_pack.argtypes = [C.c_int32] * 3 + [_P] * 5 + [_P, C.POINTER(po.EmitSlots), _P, _P, _P,
+        lib.or_encode_pack.argtypes = [C.c_int32] * 5 + [_P] * 5 + [_P, C.POINTER(po.EmitSlots), _P, _P, _P,
                                                                    C.c_int32, C.c_size_t, _P, C.c_int32,
-                                                                   C.c_int32, _P, C.c_size_t,
-                                                                   C.POINTER(C.c_size_t)]
+                                                                   C.c_int32, _P, C.c_size_t, _P, C.c_int32,
+                                                                   C.POINTER(C.c_int32), C.POINTER(C.c_size_t)]
         _bound = True
     return lib
 
@@ -156,12 +156,28 @@ def _increments(lo, hi, target):
     return v
 
 
+def tiling(w8, h8):
+    """plan_tiling(sb_cols, sb_rows, 1) (src/coder/tiling.rs:92-136): the
+    spec-minimum (TileColsLog2, TileRowsLog2) with the increment bits that
+    signal them, and the uniform tile size in superblocks
+    (tile_starts_sb, :140-152)."""
+    sbc, sbr = (w8 + 63) // 64, (h8 + 63) // 64
+    min_c, max_c = _tile_log2(64, sbc), _tile_log2(1, min(sbc, 64))
+    max_r = _tile_log2(1, min(sbr, 64))
+    min_t = max(min_c, _tile_log2(2304, sbr * sbc))
+    tcl = min(min_c, max_c)
+    trl = min(max(min_t - tcl, 0), max_r)
+    incr = _increments(min_c, max_c, tcl) + _increments(max(min_t - tcl, 0), max_r, trl)
+    return tcl, trl, incr, -(-sbc // (1 << tcl)), -(-sbr // (1 << trl))
+
+
 def frame_header(w8, h8, q, qm, lf, sharp, cdef, updating_cdf=True):
-    """frame_header_lossy_impl (src/obu.rs:396-527) for one tile at the spec
-    minimum, no delta-q or IntraBC, the luma DC delta of -8
-    (src/quant.rs:350-352), no chroma deltas; cdef = (damping, bits, strengths)
-    or None (the no-op parameters); restoration off.  Byte aligned without
-    trailing bits (the header of an OBU_FRAME)."""
+    """frame_header_lossy_impl (src/obu.rs:396-527) in the spec-minimum tiling,
+    no delta-q or IntraBC, the luma DC delta of -8 (src/quant.rs:350-352), no
+    chroma deltas; cdef = (damping, bits, strengths) or None (the no-op
+    parameters); restoration off.  For one tile: byte aligned without trailing
+    bits (the header of an OBU_FRAME); for several: with trailing bits (an
+    OBU_FRAME_HEADER)."""
     b = _Bits()
     b.flag(not updating_cdf)
     b.flag(True)   # allow_screen_content_tools
@@ -169,13 +185,12 @@ def frame_header(w8, h8, q, qm, lf, sharp, cdef, updating_cdf=True):
     b.flag(False)  # render_and_frame_size_different
     b.flag(False)  # allow_intrabc
     b.flag(True)   # uniform_tile_spacing_flag
-    sbc, sbr = (w8 + 63) // 64, (h8 + 63) // 64
-    min_c, max_c = _tile_log2(64, sbc), _tile_log2(1, min(sbc, 64))
-    max_r = _tile_log2(1, min(sbr, 64))
-    min_t = max(min_c, _tile_log2(2304, sbr * sbc))
-    assert min_t == 0, "one tile"
-    for v in _increments(min_c, max_c, 0) + _increments(min_t, max_r, 0):
+    tcl, trl, incr, _, _ = tiling(w8, h8)
+    for v in incr:
         b.flag(v)
+    if tcl + trl > 0:
+        b.f(0, tcl + trl)  # context_update_tile_id
+        b.f(3, 2)          # tile_size_bytes_minus_1: TileSizeBytes 4
     b.f(q, 8)
     b.flag(True)
     b.f(-8 & 0x7F, 7)  # DeltaQYDc
@@ -210,7 +225,20 @@ def frame_header(w8, h8, q, qm, lf, sharp, cdef, updating_cdf=True):
         b.f(0, 2)
     b.flag(True)   # tx_mode_select
     b.flag(False)  # reduced_tx_set
+    if tcl + trl > 0:
+        b.trailing()
     return b.bytes()
+
+
+def frame_obus(fh, tiles):
+    """assemble_frame_obus (src/coder/frame_encode.rs:444-525): one tile as an
+    OBU_FRAME; several as an OBU_FRAME_HEADER and an OBU_TILE_GROUP whose
+    tiles but the last carry their size less one in 4 little-endian bytes
+    (src/obu.rs:296-300).  fh is frame_header()'s output for the tiling."""
+    if len(tiles) == 1:
+        return obu(6, fh + tiles[0])
+    tg = b"\0" + b"".join((len(t) - 1).to_bytes(4, "little") + t for t in tiles[:-1]) + tiles[-1]
+    return obu(3, fh) + obu(4, tg)
 
 
 def level_for(w, h):
@@ -300,7 +328,8 @@ def encode(planes, w, h, sub, quality, threads=None, cicp=SRGB_YCBCR, want_recon
     mode, tx = np.zeros(nb, np.uint8), np.zeros(nb, np.uint8)
     lv = [np.zeros(nb * 64, np.int32), np.zeros(nb * nc * nc, np.int32), np.zeros(nb * nc * nc, np.int32)]
     p = po.p
-    rc = lib.or_encode_decide(pw, ph, sub, C.byref(py), C.byref(pc), C.byref(qy), C.byref(qc), p(qmy), p(qmc),
+    _, _, _, tsw, tsh = tiling(pw, ph)
+    rc = lib.or_encode_decide(pw, ph, sub, tsw, tsh, C.byref(py), C.byref(pc), C.byref(qy), C.byref(qc), p(qmy), p(qmc),
                               C.byref(cdy), C.byref(cdc), *[p(x) for x in src], *[p(x) for x in rec], p(mode),
                               p(tx), *[p(x) for x in lv], threads)
     assert rc == 0, rc
@@ -330,15 +359,20 @@ def encode(planes, w, h, sub, quality, threads=None, cicp=SRGB_YCBCR, want_recon
     grid = np.ascontiguousarray(dec["grid"], np.uint8)
     cap = nb * 1024 + 4096
     out = np.zeros(cap, np.uint8)
-    n = C.c_size_t()
-    rc = lib.or_encode_pack(pw, ph, sub, p(mode), p(tx), *[p(x) for x in lv], p(syn), C.byref(es), p(data), p(offs),
-                            p(lens), len(slots), len(data), p(grid), bits, 1, p(out), cap, C.byref(n))
+    n, nt = C.c_size_t(), C.c_int32()
+    tl = np.zeros(4096, np.uint64)
+    rc = lib.or_encode_pack(pw, ph, sub, tsw, tsh, p(mode), p(tx), *[p(x) for x in lv], p(syn), C.byref(es), p(data),
+                            p(offs), p(lens), len(slots), len(data), p(grid), bits, 1, p(out), cap, p(tl), len(tl),
+                            C.byref(nt), C.byref(n))
     assert rc == 0, rc
-    tile = out[:n.value].tobytes()
+    tiles, at = [], 0
+    for t in range(nt.value):
+        tiles.append(out[at:at + int(tl[t])].tobytes())
+        at += int(tl[t])
     cdef = (dec["damping"], dec["bits"], dec["strengths"]) if dec["bits"] >= 0 else None
     fh = frame_header(pw, ph, q, (qm_y, qm_uv), (ly, luv), sharp, cdef)
     profile = 0 if sub else 1
-    av1 = obu(2, b"") + sequence_header(w, h, profile, bool(sub), cicp) + obu(6, fh + tile)
+    av1 = obu(2, b"") + sequence_header(w, h, profile, bool(sub), cicp) + frame_obus(fh, tiles)
     avif = wrap_av1_image(av1, w, h, profile, bool(sub), cicp)
     return (avif, flt) if want_recon else avif
 

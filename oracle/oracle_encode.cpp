@@ -20,15 +20,19 @@
 //                     src/coder/lossy_state.rs:1408-1415, :4021-4051), the
 //                     coefficient tokens of the oracle's coders with their
 //                     txb_skip / dc_sign contexts (src/coeffs.rs:2917-2920),
-//                     and the tile's range coding (src/odec.rs:35-615
+//                     and each tile's range coding (src/odec.rs:35-615
 //                     OdEcEncoder, src/coder/wavefront.rs:617-657
 //                     pack_wavefront_tile) with each superblock's cdef_idx
 //                     literal at its read_cdef() point
 //                     (src/coder/tile_encode.rs:404-466).
+// Both work in the uniform tiling the caller gives (the spec minimum,
+// src/coder/frame_encode.rs:75-103): each tile is coded as a frame of its own,
+// with its own contexts and range coder.
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <atomic>
 #include <thread>
 #include <vector>
@@ -76,6 +80,7 @@ bool smooth(int m) { return m == MT_SMOOTH_PRED || m == MT_SMOOTH_V_PRED || m ==
 
 struct Frame {
   int pw, ph, pcw, pch, sub, nbx, nby;
+  int tw8, th8;  // the uniform tile size in 8x8 blocks
   const mt_chain_params* py;
   const mt_chain_params* pc;
   const mt_quant* qy;
@@ -91,11 +96,22 @@ struct Frame {
   int32_t* lv[3];
 };
 
-// One 8x8 block: the luma decision and the chroma blocks.
+// One 8x8 block: the luma decision and the chroma blocks.  The block's tile
+// is coded as a frame of its own, as the reference codes a cropped tile
+// (src/coder/frame_encode.rs:82-103, src/coder/tiling.rs crop_plane): tile
+// coordinates, the tile's size as the frame size, the planes from the tile's
+// origin.
 void code_block(const Frame& f, int x8, int y8, bool thr, bool lhb) {
-  const int px = x8 * 8, py = y8 * 8, b = y8 * f.nbx + x8;
-  const bool have_tr = thr && py > 0 && px + 8 < f.pw;
-  const bool have_bl = lhb && px > 0 && py + 8 < f.ph;
+  const int b = y8 * f.nbx + x8;
+  const int tx0 = x8 - x8 % f.tw8, ty0 = y8 - y8 % f.th8;
+  const int tw = (std::min(tx0 + f.tw8, f.nbx) - tx0) * 8, th = (std::min(ty0 + f.th8, f.nby) - ty0) * 8;
+  const int px = (x8 - tx0) * 8, py = (y8 - ty0) * 8;
+  mt_chain_params ply = *f.py;
+  ply.frame_w = tw;
+  ply.frame_h = th;
+  const size_t oy = (size_t)ty0 * 8 * f.pw + (size_t)tx0 * 8;
+  const bool have_tr = thr && py > 0 && px + 8 < tw;
+  const bool have_bl = lhb && px > 0 && py + 8 < th;
   const bool ft = (py > 0 && smooth(f.mode[b - f.nbx])) || (px > 0 && smooth(f.mode[b - 1]));
   mt_candidate cands[91];
   memset(cands, 0, sizeof(cands));
@@ -108,30 +124,34 @@ void code_block(const Frame& f, int x8, int y8, bool thr, bool lhb) {
   }
   mt_candidate_result res[91];
   std::vector<int32_t> lv(91 * 64), rc(91 * 64);
-  or_candidate_chain(f.src[0], f.rec[0], f.py, f.qy, f.qmy, f.cdy, cands, 91, res, lv.data(), rc.data(), 1);
+  or_candidate_chain(f.src[0] + oy, f.rec[0] + oy, &ply, f.qy, f.qmy, f.cdy, cands, 91, res, lv.data(), rc.data(), 1);
   int best = 0;
   for (int t = 1; t < 91; ++t)
     if (res[t].cost < res[best].cost) best = t;
   for (int y = 0; y < 8; ++y)
-    for (int x = 0; x < 8; ++x) f.rec[0][(size_t)(py + y) * f.pw + px + x] = (uint16_t)rc[best * 64 + y * 8 + x];
+    for (int x = 0; x < 8; ++x) f.rec[0][oy + (size_t)(py + y) * f.pw + px + x] = (uint16_t)rc[best * 64 + y * 8 + x];
   memcpy(f.lv[0] + (size_t)b * 64, &lv[best * 64], 64 * sizeof(int32_t));
   f.mode[b] = (uint8_t)(best / 7);
   f.tx[b] = kTypes[best % 7];
   // chroma: UV_DC_PRED, DCT_DCT
-  const int n = f.sub ? 4 : 8;
+  const int n = f.sub ? 4 : 8, sh = f.sub ? 1 : 0;
+  mt_chain_params plc = *f.pc;
+  plc.frame_w = tw >> sh;
+  plc.frame_h = th >> sh;
+  const size_t oc = (size_t)(ty0 * 8 >> sh) * f.pcw + (size_t)(tx0 * 8 >> sh);
   for (int p = 1; p < 3; ++p) {
     mt_candidate c;
     memset(&c, 0, sizeof(c));
-    c.px = (uint16_t)(f.sub ? px / 2 : px);
-    c.py = (uint16_t)(f.sub ? py / 2 : py);
+    c.px = (uint16_t)(px >> sh);
+    c.py = (uint16_t)(py >> sh);
     c.mode = MT_DC_PRED;
     c.tx_type = MT_TX_DCT_DCT;
     c.flags = (uint8_t)(f.sub ? 0 : ((have_tr ? 1 : 0) | (have_bl ? 2 : 0)));
     mt_candidate_result r;
     int32_t l[64], o[64];
-    or_candidate_chain(f.src[p], f.rec[p], f.pc, f.qc, f.qmc, f.cdc, &c, 1, &r, l, o, 1);
+    or_candidate_chain(f.src[p] + oc, f.rec[p] + oc, &plc, f.qc, f.qmc, f.cdc, &c, 1, &r, l, o, 1);
     for (int y = 0; y < n; ++y)
-      for (int x = 0; x < n; ++x) f.rec[p][(size_t)(c.py + y) * f.pcw + c.px + x] = (uint16_t)o[y * n + x];
+      for (int x = 0; x < n; ++x) f.rec[p][oc + (size_t)(c.py + y) * f.pcw + c.px + x] = (uint16_t)o[y * n + x];
     memcpy(f.lv[p] + (size_t)b * n * n, l, (size_t)n * n * sizeof(int32_t));
   }
 }
@@ -246,6 +266,26 @@ struct Syntax {
     }
   }
   void sym(int32_t slot, uint32_t s) { out->push_back(((uint32_t)slot << 8) | s); }
+  // clear_above_context for a tile's 8x8 columns [x0, x1) and
+  // clear_left_context for a superblock row's 8x8 rows [y0, y1) (decode_tile)
+  void clear_above(int x0, int x1) {
+    for (int x = x0; x < x1; ++x) a_part[x] = 0;
+    for (int x = 2 * x0; x < 2 * x1; ++x) {
+      a_skip[x] = a_mode[x] = 0;
+      a_tx[x] = -1;
+    }
+    for (int p = 0; p < 3; ++p)
+      for (int x = (p && f.sub ? 1 : 2) * x0; x < (p && f.sub ? 1 : 2) * x1; ++x) a_coef[p][x] = 0x40;
+  }
+  void clear_left(int y0, int y1) {
+    for (int y = y0; y < y1; ++y) l_part[y] = 0;
+    for (int y = 2 * y0; y < 2 * y1; ++y) {
+      l_skip[y] = l_mode[y] = 0;
+      l_tx[y] = -1;
+    }
+    for (int p = 0; p < 3; ++p)
+      for (int y = (p && f.sub ? 1 : 2) * y0; y < (p && f.sub ? 1 : 2) * y1; ++y) l_coef[p][y] = 0x40;
+  }
   int part_ctx(int bl, int x8, int y8) const {
     return ((a_part[x8] >> (4 - bl)) & 1) + (((l_part[y8] >> (4 - bl)) & 1) << 1);
   }
@@ -332,14 +372,19 @@ extern "C" {
 
 // The decisions, reconstruction and levels of a frame (planes padded to x8:
 // luma pw x ph, chroma pcw x pch; levels: 64 per block for luma and 64 / 16
-// per block for chroma).  threads <= 1 codes the superblocks serially.
-int or_encode_decide(int32_t pw, int32_t ph, int32_t sub, const mt_chain_params* py, const mt_chain_params* pc,
-                     const mt_quant* qy, const mt_quant* qc, const uint8_t* qmy, const uint8_t* qmc,
-                     const mt_coef_cdfs* cdy, const mt_coef_cdfs* cdc, const uint16_t* src_y, const uint16_t* src_u,
-                     const uint16_t* src_v, uint16_t* rec_y, uint16_t* rec_u, uint16_t* rec_v, uint8_t* mode,
-                     uint8_t* tx, int32_t* lv_y, int32_t* lv_u, int32_t* lv_v, int32_t threads) {
-  if (pw <= 0 || ph <= 0 || (pw & 7) || (ph & 7) || (sub != 0 && sub != 2)) return MT_ERR_INVALID_INPUT;
+// per block for chroma) in uniform tiles of tile_sb_w x tile_sb_h
+// superblocks.  threads <= 1 codes the superblocks serially.
+int or_encode_decide(int32_t pw, int32_t ph, int32_t sub, int32_t tile_sb_w, int32_t tile_sb_h,
+                     const mt_chain_params* py, const mt_chain_params* pc, const mt_quant* qy, const mt_quant* qc,
+                     const uint8_t* qmy, const uint8_t* qmc, const mt_coef_cdfs* cdy, const mt_coef_cdfs* cdc,
+                     const uint16_t* src_y, const uint16_t* src_u, const uint16_t* src_v, uint16_t* rec_y,
+                     uint16_t* rec_u, uint16_t* rec_v, uint8_t* mode, uint8_t* tx, int32_t* lv_y, int32_t* lv_u,
+                     int32_t* lv_v, int32_t threads) {
+  if (pw <= 0 || ph <= 0 || (pw & 7) || (ph & 7) || (sub != 0 && sub != 2) || tile_sb_w <= 0 || tile_sb_h <= 0)
+    return MT_ERR_INVALID_INPUT;
   Frame f;
+  f.tw8 = tile_sb_w * 8;
+  f.th8 = tile_sb_h * 8;
   f.pw = pw;
   f.ph = ph;
   f.pcw = sub ? pw / 2 : pw;
@@ -402,18 +447,25 @@ int or_encode_decide(int32_t pw, int32_t ph, int32_t sub, const mt_chain_params*
   return MT_OK;
 }
 
-// The tile payload of a decided frame: block syntax and coefficient tokens in
-// coding order, range coded against the frame-initial CDF set (cdf_data /
-// cdf_off / cdf_len, Cdfs::new in semantic-slot order, copied here), with
-// superblock i's cdef_idx (sb_cdef_idx[i], cdef_bits wide; 0 bits: none) at
-// its read_cdef() point.  slots: skip, part_bl8, part_split, kf_y, uv_mode,
+// The tile payloads of a decided frame in uniform tiles of tile_sb_w x
+// tile_sb_h superblocks (raster order, concatenated in out; tile_lens[t] the
+// length of tile t): block syntax and coefficient tokens in coding order
+// (each tile's superblocks in raster order, the above contexts cleared per
+// tile and the left per superblock row), each tile range coded against the
+// frame-initial CDF set (cdf_data / cdf_off / cdf_len, Cdfs::new in
+// semantic-slot order, copied per tile), with superblock i's cdef_idx
+// (sb_cdef_idx[i], frame raster; cdef_bits wide, 0 bits: none) at its
+// read_cdef() point.  slots: skip, part_bl8, part_split, kf_y, uv_mode,
 // angle_delta, filter_intra, palette_y_mode, palette_uv_mode, txsz.
-int or_encode_pack(int32_t pw, int32_t ph, int32_t sub, const uint8_t* mode, const uint8_t* tx, const int32_t* lv_y,
-                   const int32_t* lv_u, const int32_t* lv_v, const int32_t* slots, const or_emit_slots* E,
-                   const uint16_t* cdf_data, const uint32_t* cdf_off, const uint16_t* cdf_len, int32_t nslots,
-                   size_t ndata, const uint8_t* sb_cdef_idx, int32_t cdef_bits, int32_t updating_cdf, uint8_t* out,
-                   size_t cap, size_t* out_len) {
-  if (pw <= 0 || ph <= 0 || (pw & 7) || (ph & 7) || !slots || !E || !out_len) return MT_ERR_INVALID_INPUT;
+int or_encode_pack(int32_t pw, int32_t ph, int32_t sub, int32_t tile_sb_w, int32_t tile_sb_h, const uint8_t* mode,
+                   const uint8_t* tx, const int32_t* lv_y, const int32_t* lv_u, const int32_t* lv_v,
+                   const int32_t* slots, const or_emit_slots* E, const uint16_t* cdf_data, const uint32_t* cdf_off,
+                   const uint16_t* cdf_len, int32_t nslots, size_t ndata, const uint8_t* sb_cdef_idx,
+                   int32_t cdef_bits, int32_t updating_cdf, uint8_t* out, size_t cap, size_t* tile_lens,
+                   int32_t max_tiles, int32_t* ntiles, size_t* out_len) {
+  if (pw <= 0 || ph <= 0 || (pw & 7) || (ph & 7) || !slots || !E || !out_len || !ntiles || tile_sb_w <= 0 ||
+      tile_sb_h <= 0)
+    return MT_ERR_INVALID_INPUT;
   Frame f;
   memset(&f, 0, sizeof(f));
   f.pw = pw;
@@ -429,38 +481,52 @@ int or_encode_pack(int32_t pw, int32_t ph, int32_t sub, const uint8_t* mode, con
   SyntaxSlots L;
   memcpy(&L, slots, sizeof(L));
   Syntax syn(f, L, *E);
-  std::vector<uint16_t> cdf(cdf_data, cdf_data + ndata);
-  RangeCoder rc;
   const int sbc = (pw + 63) / 64, sbr = (ph + 63) / 64;
+  std::vector<uint8_t> all;
+  std::vector<size_t> lens;
   std::vector<uint32_t> toks;
-  for (int r = 0; r < sbr; ++r)
-    for (int c = 0; c < sbc; ++c) {
-      toks.clear();
-      syn.out = &toks;
-      syn.cdef_point = -1;
-      syn.node(1, c * 8, r * 8, 8);
-      const int i = r * sbc + c;
-      for (size_t k = 0; k <= toks.size(); ++k) {
-        if (cdef_bits > 0 && (int)k == syn.cdef_point) rc.literal(sb_cdef_idx[i], cdef_bits);
-        if (k == toks.size()) break;
-        const uint32_t t = toks[k], tag = t >> 30;
-        if (tag == 0 || tag == 3) {
-          const uint32_t slot = (t >> 8) & 0xffff, s = t & 0xff;
-          if ((int32_t)slot >= nslots || s >= cdf_len[slot]) return MT_ERR_INVALID_INPUT;
-          rc.symbol((int)s, &cdf[cdf_off[slot]], cdf_len[slot], tag == 0 && updating_cdf);
-        } else if (tag == 1) {
-          rc.boolean((t & 1) != 0, (t >> 1) & 0xffff);
-        } else {
-          const uint32_t slot = (t >> 2) & 0xffff;
-          if ((int32_t)slot >= nslots || cdf_len[slot] != 10) return MT_ERR_INVALID_INPUT;
-          rc.boolean((t & 2) != 0, gather(&cdf[cdf_off[slot]], (t & 1) != 0));
+  for (int r0 = 0; r0 < sbr; r0 += tile_sb_h)
+    for (int c0 = 0; c0 < sbc; c0 += tile_sb_w) {
+      const int r1 = std::min(r0 + tile_sb_h, sbr), c1 = std::min(c0 + tile_sb_w, sbc);
+      std::vector<uint16_t> cdf(cdf_data, cdf_data + ndata);
+      RangeCoder rc;
+      syn.clear_above(c0 * 8, std::min(c1 * 8, f.nbx));
+      for (int r = r0; r < r1; ++r) {
+        syn.clear_left(r * 8, std::min(r * 8 + 8, f.nby));
+        for (int c = c0; c < c1; ++c) {
+          toks.clear();
+          syn.out = &toks;
+          syn.cdef_point = -1;
+          syn.node(1, c * 8, r * 8, 8);
+          const int i = r * sbc + c;
+          for (size_t k = 0; k <= toks.size(); ++k) {
+            if (cdef_bits > 0 && (int)k == syn.cdef_point) rc.literal(sb_cdef_idx[i], cdef_bits);
+            if (k == toks.size()) break;
+            const uint32_t t = toks[k], tag = t >> 30;
+            if (tag == 0 || tag == 3) {
+              const uint32_t slot = (t >> 8) & 0xffff, s = t & 0xff;
+              if ((int32_t)slot >= nslots || s >= cdf_len[slot]) return MT_ERR_INVALID_INPUT;
+              rc.symbol((int)s, &cdf[cdf_off[slot]], cdf_len[slot], tag == 0 && updating_cdf);
+            } else if (tag == 1) {
+              rc.boolean((t & 1) != 0, (t >> 1) & 0xffff);
+            } else {
+              const uint32_t slot = (t >> 2) & 0xffff;
+              if ((int32_t)slot >= nslots || cdf_len[slot] != 10) return MT_ERR_INVALID_INPUT;
+              rc.boolean((t & 2) != 0, gather(&cdf[cdf_off[slot]], (t & 1) != 0));
+            }
+          }
         }
       }
+      const std::vector<uint8_t> bytes = rc.done();
+      lens.push_back(bytes.size());
+      all.insert(all.end(), bytes.begin(), bytes.end());
     }
-  const std::vector<uint8_t> bytes = rc.done();
-  *out_len = bytes.size();
-  if (!out || cap < bytes.size()) return out ? MT_ERR_TOO_LARGE : MT_OK;
-  memcpy(out, bytes.data(), bytes.size());
+  *ntiles = (int32_t)lens.size();
+  *out_len = all.size();
+  if (!tile_lens || (int32_t)lens.size() > max_tiles) return MT_ERR_TOO_LARGE;
+  for (size_t t = 0; t < lens.size(); ++t) tile_lens[t] = lens[t];
+  if (!out || cap < all.size()) return out ? MT_ERR_TOO_LARGE : MT_OK;
+  memcpy(out, all.data(), all.size());
   return MT_OK;
 }
 

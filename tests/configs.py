@@ -7,6 +7,9 @@ CDF snapshot of the frame's coefficient q context.
          quality 40 (qindex 116)
   C2q60  the same at seed 3, quality 60 (qindex 70)
   C2q80  the same at seed 4, quality 80 (qindex 35)
+  C3     4096x4096, seed 5, sigma 8 noise on the left half, piecewise-constant
+         cells on the right half, 4:4:4, quality 60 (qindex 70): two tiles
+         (the whole-frame encode only)
 
 The reconstruction snapshot the candidates predict from is the source plus a
 seeded +-3 coding error (the decision engine that would supply the real one
@@ -24,8 +27,9 @@ CONFIGS = {
     "C2q40": dict(w=1920, h=1080, seed=2, variant="1080p", quality=40, sub=2),
     "C2q60": dict(w=1920, h=1080, seed=3, variant="1080p", quality=60, sub=2),
     "C2q80": dict(w=1920, h=1080, seed=4, variant="1080p", quality=80, sub=2),
+    "C3": dict(w=4096, h=4096, seed=5, variant="large", quality=60, sub=0, sigma=8.0),
 }
-NAMES = list(CONFIGS)
+NAMES = ["C1", "C2q40", "C2q60", "C2q80"]  # the kernel-family parity workloads
 THREADS = os.cpu_count() or 1
 
 
@@ -34,7 +38,7 @@ def workload(name):
     import maroontree_b200 as mt
 
     c = CONFIGS[name]
-    rgb = synth.generate_rgb(c["w"], c["h"], c["seed"], sigma=4.0, variant=c["variant"])
+    rgb = synth.generate_rgb(c["w"], c["h"], c["seed"], sigma=c.get("sigma", 4.0), variant=c["variant"])
     src = synth.rgb_to_luma(rgb)
     rec = synth.synthetic_recon(src, c["seed"] + 1000)
     qidx = mt.quality_to_q(c["quality"])

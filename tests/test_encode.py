@@ -87,24 +87,28 @@ def test_420_rgb_encode_decodes(mt_lib, cuda, w, h, quality, seed):
         assert 10 * np.log10(255.0 ** 2 / mse) > 28.0
 
 
-@pytest.mark.parametrize("name", ["C1", "C2q40", "C2q60", "C2q80"])
+@pytest.mark.parametrize("name", ["C1", "C2q40", "C2q60", "C2q80", "C3"])
 def test_encoder_bytes_equal_the_oracle_encode_at_the_benchmark_configs(mt_lib, oracle_lib, cuda, name):
     """mt_encode_rgb8 on the benchmark configurations (512x512 4:4:4 quality
-    60; 1920x1080 4:2:0 at quality 40 / 60 / 80) gives the oracle encode's file
-    byte for byte: the same decisions, reconstruction, filters, syntax, range
-    coding, headers and container."""
+    60; 1920x1080 4:2:0 at quality 40 / 60 / 80; 4096x4096 4:4:4 quality 60 in
+    two tiles) gives the oracle encode's file byte for byte: the same
+    decisions, reconstruction, filters, syntax, range coding, headers and
+    container."""
     import configs
     from maroontree_b200 import encoder as enc
     from oracle import oracle_avif as oa
 
     c = configs.CONFIGS[name]
-    rgb = synth.generate_rgb(c["w"], c["h"], c["seed"], sigma=4.0, variant=c["variant"])
+    rgb = synth.generate_rgb(c["w"], c["h"], c["seed"], sigma=c.get("sigma", 4.0), variant=c["variant"])
     chroma = 2 if c["sub"] == 0 else 0
     got = enc.encode_rgb8(rgb, enc.config(quality=c["quality"], chroma=chroma))
     assert got == oa.encode_rgb8(rgb, c["quality"], chroma, threads=configs.THREADS)
 
 
-@pytest.mark.parametrize("w,h,quality,chroma", [(203, 117, 80, 0), (200, 136, 40, 2), (72, 520, 60, 0)])
+# 4160x64, 4163x72 and 4100x131: two tile columns (65 superblock columns;
+# the C3 frame has two tile rows)
+@pytest.mark.parametrize("w,h,quality,chroma", [(203, 117, 80, 0), (200, 136, 40, 2), (72, 520, 60, 0),
+                                                (4160, 64, 60, 2), (4163, 72, 80, 0), (4100, 131, 50, 0)])
 def test_encoder_bytes_equal_the_oracle_encode_at_ragged_sizes(mt_lib, oracle_lib, cuda, w, h, quality, chroma):
     from maroontree_b200 import encoder as enc
     from oracle import oracle_avif as oa

@@ -30,7 +30,9 @@ def _decode(avif):
 IDENTITY = (1, 13, 0, 1, 0)
 
 
-@pytest.mark.parametrize("w,h,quality", [(128, 64, 60), (200, 136, 40), (72, 200, 80)])
+# 4160x64 is the smallest kind of frame in two tiles (65 superblock columns:
+# over the 64-column maximum tile width)
+@pytest.mark.parametrize("w,h,quality", [(128, 64, 60), (200, 136, 40), (72, 200, 80), (4160, 64, 60)])
 def test_identity_444_oracle_encode_decodes_exactly(oracle_lib, w, h, quality):
     from oracle import oracle_avif as oa
 
@@ -43,7 +45,7 @@ def test_identity_444_oracle_encode_decodes_exactly(oracle_lib, w, h, quality):
     assert np.array_equal(dec[..., 0], rec[2][:h, :w])
 
 
-@pytest.mark.parametrize("w,h,quality", [(203, 117, 80), (128, 128, 40)])
+@pytest.mark.parametrize("w,h,quality", [(203, 117, 80), (128, 128, 40), (4163, 72, 80)])
 def test_420_oracle_encode_decodes_to_its_luma(oracle_lib, w, h, quality):
     from oracle import oracle_avif as oa
 
@@ -91,3 +93,33 @@ def test_oracle_headers_and_container_equal_the_library_writers(mt_lib, oracle_l
     ip.seq_profile = 0 if sub else 1
     ip.seq_level_idx = ct.level_for(w, h)
     assert oa.wrap_av1_image(payload, w, h, ip.seq_profile, bool(sub), cicp) == ct.wrap_av1_image(payload, ip)
+
+
+@pytest.mark.parametrize("w,h", [(1920, 1080), (4096, 4096), (4160, 64), (4104, 2400), (8200, 64), (4096, 2368)])
+def test_oracle_tiling_and_frame_obus_equal_the_library(mt_lib, oracle_lib, w, h):
+    """The spec-minimum tiling, the frame header with its tile info and the
+    frame OBUs (one OBU_FRAME, or OBU_FRAME_HEADER + OBU_TILE_GROUP) against
+    the library's writers."""
+    from maroontree_b200 import abi
+    from maroontree_b200 import container as ct
+    from oracle import oracle_avif as oa
+
+    pw, ph = (w + 7) & ~7, (h + 7) & ~7
+    tcl, trl, _, tsw, tsh = oa.tiling(pw, ph)
+    assert (tcl, trl) == mt_lib.tiling_spec_min(pw, ph)
+    sbc, sbr = (pw + 63) // 64, (ph + 63) // 64
+    assert tsw <= 64 and tsw * tsh <= 2304  # the AV1 tile limits
+    ntiles = -(-sbc // tsw) * -(-sbr // tsh)
+    fp = abi.FrameHeaderParams()
+    fp.w8, fp.h8, fp.base_q_idx, fp.qm_y, fp.qm_u, fp.qm_v = pw, ph, 70, 6, 6, 6
+    fp.updating_cdf, fp.lf_y, fp.lf_u, fp.lf_v, fp.lf_sharpness = 1, 8, 3, 3, 0
+    fp.cdef_bits, fp.cdef_damping = 1, 4
+    fp.tile_cols_log2, fp.tile_rows_log2 = tcl, trl
+    cdef = (4, 1, [(3, 1, 2, 4), (0, 0, 1, 2)])
+    for e, st in enumerate(cdef[2]):
+        for k in range(4):
+            fp.cdef_strengths[e][k] = st[k]
+    fh = oa.frame_header(pw, ph, 70, (6, 6), (8, 3), 0, cdef)
+    assert fh == ct.frame_header(fp, trailing=ntiles > 1)
+    tiles = [bytes([(7 * t + k) & 0xFF for k in range(50 + 13 * t)]) for t in range(ntiles)]
+    assert oa.frame_obus(fh, tiles) == ct.assemble_frame_obus(fp, tiles)
