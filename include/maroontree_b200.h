@@ -831,11 +831,11 @@ int mt_cdef_tables_device(const uint16_t* d_y, const uint16_t* d_u, const uint16
                           int64_t* d_u_tab, int64_t* d_v_tab, void* stream);
 /* Device working storage mt_cdef_frame_device needs. */
 size_t mt_cdef_scratch_bytes(const mt_cdef_params* prm);
-/* The whole frame CDEF: tables on the device, the strength search on the host
- * (the stream is synchronised once to read the tables), then the filter
- * applied to the recon planes on the stream.  grid: host buffer of
- * unit_cols * unit_rows bytes (the per-unit strength index; zeros unless bits
- * > 0), may be NULL. */
+/* The whole frame CDEF on the stream: tables, the strength search and the
+ * filter applied to the recon planes, back to back on the device; the stream
+ * is synchronised once, at the end, to read the decision.  grid: host buffer
+ * of unit_cols * unit_rows bytes (the per-unit strength index; zeros unless
+ * bits > 0), may be NULL. */
 int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint16_t* d_src_y,
                          const uint16_t* d_src_u, const uint16_t* d_src_v, const uint8_t* d_skip8,
                          const mt_cdef_params* prm, void* d_scratch, mt_cdef_decision* out, uint8_t* grid,

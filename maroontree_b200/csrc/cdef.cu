@@ -17,9 +17,13 @@
 //   cdef_apply_kernel    one 64-thread CTA per (plane, luma 8x8): the chosen
 //                        strengths filtered from a pre-CDEF snapshot into the
 //                        reconstruction (src/coder/frame_cdef.rs:960-1125).
-// Host side: the staged strength search over the unit tables
-// (src/coder/frame_cdef.rs:116-520), a few hundred kilobytes of integers.
+//   the strength search   the staged search over the unit tables
+//                        (src/coder/frame_cdef.rs:116-520) as a chain of small
+//                        kernels, so that tables, search and apply run back to
+//                        back on the stream and the host reads the decision
+//                        once at the end.
 #include <cuda_runtime.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
@@ -539,11 +543,34 @@ Geo make_geo(const mt_cdef_params* p) {
   return g;
 }
 
+constexpr int kMaxPairs = 144;  // 12 luma x 12 chroma candidates
+constexpr long long kMargin = 40, kGate = 15000;
+constexpr int kGreedySteps = 7;  // entries 2 .. 8
+constexpr int kSearchThreads = 256;
+
+struct SearchState {
+  // the decision
+  int32_t bits, n_strengths;
+  uint8_t strengths[8][4];
+  // unit statistics: signalling units, trusted units, distortion sums
+  unsigned long long n_sig, n_trusted, total_off, unsig_off, gsum[3];
+  // candidates: (pri, sec) and the table column of each
+  int32_t nl, nc, np;
+  uint8_t cand[12][2];
+  int8_t col[12];
+  // pass totals: [0] the single-entry pass, [1] and [2] alternate in the greedy passes
+  unsigned long long tot[3][kMaxPairs];
+  long long prefix[4];
+  int32_t global_entry, nentries;
+  int32_t entries[8];
+  unsigned long long assign_total[4];  // the 2-, 4- and 8-entry sets at [1..3]
+};
+
 // Scratch layout of mt_cdef_frame_device (256-byte aligned pieces).
 struct Layout {
   size_t dirs, vars, tabs, dv_sum, dv_cnt, ustr, snap_y, snap_u, snap_v, total;
+  size_t state, d_off, thr, cm, sig, grids, grid;  // the strength search
   size_t tab_bytes;  // one plane's table
-  size_t read_bytes; // tabs .. dv_cnt end (the block read back to the host)
 };
 
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -563,10 +590,23 @@ Layout make_layout(const Geo& g, bool mono) {
   o += nu * 8;
   L.dv_cnt = o;
   o += nu * 4;
-  L.read_bytes = o - L.tabs;
   o = up256(o);
   L.ustr = o;
   o += up256(nu * 4);
+  L.state = o;
+  o += up256(sizeof(SearchState));
+  L.d_off = o;
+  o += up256(nu * 8);
+  L.thr = o;
+  o += up256(nu * 8);
+  L.cm = o;
+  o += up256(nu * 8);
+  L.sig = o;
+  o += up256(nu);
+  L.grids = o;
+  o += up256(3 * nu);
+  L.grid = o;
+  o += up256(nu);
   L.snap_y = o;
   o += up256((size_t)g.w8 * g.h8 * 2);
   L.snap_u = o;
@@ -584,16 +624,15 @@ Layout make_layout(const Geo& g, bool mono) {
 
 namespace mth {
 // Kernels the calling thread's last mt_cdef_frame_device launched (the
-// direction and table kernels, and the apply kernel when a unit filters).
+// direction and table kernels, the strength search's kernels and the apply
+// kernel).
 thread_local int cdef_last_launches = 0;
-// Bytes mt_cdef_frame_device moves between the device and the host: the
-// per-unit tables read back for the strength search (d2h) and the chosen
-// per-unit strengths sent back (h2d, only when the apply kernel runs).
+// Bytes mt_cdef_frame_device reads back to the host: the search's state
+// (decision and statistics) and, when asked for, the per-unit grid.
 void cdef_frame_transfer_bytes(const mt_cdef_params* p, size_t* d2h, size_t* h2d) {
   const Geo g = make_geo(p);
-  const Layout L = make_layout(g, p->mono != 0);
-  *d2h = L.read_bytes;
-  *h2d = (size_t)g.uc * g.ur * 4;
+  *d2h = sizeof(SearchState) + (size_t)g.uc * g.ur;
+  *h2d = 0;
 }
 }  // namespace mth
 
@@ -657,256 +696,376 @@ float frame_lambda_d(int qidx, int bd, int sub_x, int sub_y, float dc_q) {
   return num / 2.775f;
 }
 
-int64_t sat_mul(int64_t a, int64_t b) {
-  __int128 r = (__int128)a * b;
-  if (r > INT64_MAX) return INT64_MAX;
-  if (r < INT64_MIN) return INT64_MIN;
-  return (int64_t)r;
+// ---------------------------------------------------------------------------
+// The staged strength search (src/coder/frame_cdef.rs:116-520) on the device,
+// as a chain of small kernels on the stream (no host round trip): the unit
+// statistics, the candidate list, the single-entry pass, seven greedy entry
+// passes, the assignment of the 2-, 4- and 8-entry sets to the units, the rate
+// decision and the per-unit strengths the apply kernel reads.  Integer sums
+// are 64-bit atomics (order-free, exact); every choice is the first minimum in
+// the reference's order, and the rate arithmetic is the reference's f32
+// operations one by one.
+
+struct SearchArgs {
+  const long long* ltab;
+  const long long* utab;
+  const long long* vtab;
+  const unsigned long long* dv_sum;
+  const int* dv_cnt;
+  int nu, mono, slow;
+  float lambda;      // the frame lambda_d pricing the CDEF bits
+  SearchState* S;
+  long long* d_off;  // distortion with CDEF off, per unit
+  long long* thr;    // its margin threshold
+  long long* cm;     // the greedy set's best distortion so far
+  uint8_t* sig;      // the unit signals a strength index (a non-skip block)
+  uint8_t* grids;    // 3 x nu: the entry of each unit for the 2-, 4- and 8-entry sets
+  uint8_t* grid;     // nu: the chosen set's entry per unit (0 unless bits > 0)
+  uint8_t* ustr;     // nu x 4: the unit's strengths for the apply kernel
+};
+
+__host__ __device__ __forceinline__ long long sat_mul_pos(long long a, long long b) {  // b > 0
+  if (a > LLONG_MAX / b) return LLONG_MAX;
+  if (a < LLONG_MIN / b) return LLONG_MIN;
+  return a * b;
+}
+__host__ __device__ __forceinline__ long long off_of(long long off) { return off - sat_mul_pos(off, kMargin) / 1000; }
+__host__ __device__ __forceinline__ int cand_col(int pri, int sec) {  // sec_idx * 4 + pri_idx
+  return sec * 4 + (pri == 4 ? 3 : pri);
 }
 
-// The staged strength search (src/coder/frame_cdef.rs:116-520) over the unit
-// tables.  Returns the decision; ustr receives per-unit strengths.
-void decide(const mt_cdef_params* p, const Geo& g, const int64_t* ltab, const int64_t* utab, const int64_t* vtab,
-            const int64_t* dv_sum, const int32_t* dv_cnt, float dc_q, mt_cdef_decision* out, uint8_t* grid_out,
-            std::vector<uint8_t>& ustr) {
-  static const int kPri[4] = {0, 1, 2, 4};
-  static const int kSec[3] = {0, 1, 2};
-  const bool mono = p->mono != 0;
-  const int nu = g.uc * g.ur;
-  const int64_t margin = 40, gate = 15000;
-  out->bits = -1;
-  out->damping = 3 + std::min(p->base_q_idx / 64, 3);
-  out->n_strengths = 0;
-  out->unit_cols = g.uc;
-  out->unit_rows = g.ur;
-  memset(out->strengths, 0, sizeof(out->strengths));
-  ustr.assign((size_t)nu * 4, 0);
-  if (grid_out) memset(grid_out, 0, nu);
-  std::vector<char> signaled(nu);
-  int n_sig = 0, n_trusted = 0;
-  for (int u = 0; u < nu; u++) {
-    signaled[u] = dv_cnt[u] > 0;
-    n_sig += signaled[u];
-    if (gate == 0 || dv_sum[u] / std::max<int64_t>(dv_cnt[u], 1) >= gate) n_trusted++;
+__device__ __forceinline__ long long d_pair(const SearchArgs& a, const SearchState& S, int pp, int u) {
+  long long d = a.ltab[(size_t)u * kNCand + S.col[pp / S.nc]];
+  if (!a.mono) {
+    const int c = S.col[pp % S.nc];
+    d += a.utab[(size_t)u * kNCand + c] + a.vtab[(size_t)u * kNCand + c];
   }
-  if (n_sig == 0) return;
-  auto col = [](int pri, int sec) {
-    int pi = 0, si = 0;
-    for (int i = 0; i < 4; i++)
-      if (kPri[i] == pri) pi = i;
-    for (int i = 0; i < 3; i++)
-      if (kSec[i] == sec) si = i;
-    return si * 4 + pi;
-  };
-  auto off_of = [&](int64_t off) { return off - sat_mul(off, margin) / 1000; };
-  // Candidate list.
-  std::vector<std::pair<int, int>> cands = {{0, 0}};
-  if (p->slow) {
-    const int pri_list[3] = {1, 2, 4};
-    std::vector<std::pair<int64_t, int>> ranked;
-    for (int i = 0; i < 3; i++) {
-      int64_t gsum = 0;
-      const int c = col(pri_list[i], 0), c0 = col(0, 0);
-      for (int u = 0; u < nu; u++) {
-        const int64_t off = ltab[u * kNCand + c0], on = ltab[u * kNCand + c];
-        gsum += on < off_of(off) ? off - on : 0;
-      }
-      ranked.push_back({gsum, i});
-      cands.push_back({pri_list[i], 0});
+  return d;
+}
+
+// The four strengths of pair pp (luma pri, sec, chroma pri, sec).
+__device__ __forceinline__ void pair_strengths(const SearchState& S, int mono, int pp, int s[4]) {
+  s[0] = S.cand[pp / S.nc][0];
+  s[1] = S.cand[pp / S.nc][1];
+  s[2] = mono ? 0 : S.cand[pp % S.nc][0];
+  s[3] = mono ? 0 : S.cand[pp % S.nc][1];
+}
+
+__device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sums of v[0..N) over the CTA into dst[0..N) with one atomic each
+// (kSearchThreads threads).
+template <int N>
+__device__ __forceinline__ void block_add(unsigned long long (&v)[N], unsigned long long* const (&dst)[N]) {
+  __shared__ unsigned long long part[N][kSearchThreads / 32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    const unsigned long long s = warp_sum(v[k]);
+    if (l == 0) part[k][w] = s;
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      unsigned long long s = l < kSearchThreads / 32 ? part[k][l] : 0ull;
+      s = warp_sum(s);
+      if (l == 0 && s) atomicAdd(dst[k], s);
     }
-    std::stable_sort(ranked.begin(), ranked.end(), [](const std::pair<int64_t, int>& a, const std::pair<int64_t, int>& b) {
-      return a.first != b.first ? a.first > b.first : a.second < b.second;
-    });
-    for (int sec : {1, 2}) {
-      cands.push_back({0, sec});
-      for (size_t r = 0; r < ranked.size() && r < 4; r++)
-        if (ranked[r].first > 0) cands.push_back({pri_list[ranked[r].second], sec});
+  }
+}
+
+// Per unit: the signalling and trust flags (directional-variance gate), the
+// CDEF-off distortion and its threshold, and the luma gains of pri 1 / 2 / 4
+// that rank the Slow candidate list.
+__global__ void __launch_bounds__(kSearchThreads) cdef_unit_stats_kernel(SearchArgs a) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  SearchState& S = *a.S;
+  unsigned long long v[7] = {0, 0, 0, 0, 0, 0, 0};  // n_sig, n_trusted, total_off, unsig_off, gsum[3]
+  if (u < a.nu) {
+    const bool sg = a.dv_cnt[u] > 0;
+    const long long cnt = a.dv_cnt[u] > 1 ? a.dv_cnt[u] : 1;
+    const long long* lt = a.ltab + (size_t)u * kNCand;
+    const long long lo = lt[0];
+    const long long off = lo + (a.mono ? 0 : a.utab[(size_t)u * kNCand] + a.vtab[(size_t)u * kNCand]);
+    a.d_off[u] = off;
+    a.thr[u] = off_of(off);
+    a.cm[u] = off;
+    a.sig[u] = sg;
+    v[0] = sg;
+    v[1] = (long long)a.dv_sum[u] / cnt >= kGate;
+    v[2] = (unsigned long long)off;
+    v[3] = sg ? 0ull : (unsigned long long)off;
+    const long long lim = off_of(lo);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {  // pri 1, 2, 4 at sec 0: columns 1..3
+      const long long on = lt[1 + i];
+      v[4 + i] = on < lim ? (unsigned long long)(lo - on) : 0ull;
+    }
+  }
+  unsigned long long* const dst[7] = {&S.n_sig, &S.n_trusted, &S.total_off, &S.unsig_off,
+                                      &S.gsum[0], &S.gsum[1], &S.gsum[2]};
+  block_add<7>(v, dst);
+}
+
+// The candidate list (one thread): Slow ranks pri 1 / 2 / 4 by their gains
+// and pairs the useful ones with sec 1 and 2; otherwise all 12.
+__global__ void cdef_plan_kernel(SearchArgs a) {
+  SearchState& S = *a.S;
+  int n = 0;
+  auto push = [&](int pri, int sec) {
+    S.cand[n][0] = (uint8_t)pri;
+    S.cand[n][1] = (uint8_t)sec;
+    S.col[n] = (int8_t)cand_col(pri, sec);
+    ++n;
+  };
+  push(0, 0);
+  if (a.slow) {
+    const int pri_list[3] = {1, 2, 4};
+    int r[3] = {0, 1, 2};  // stable: larger gain first, then list order
+    for (int i = 1; i < 3; i++)
+      for (int j = i; j > 0 && S.gsum[r[j]] > S.gsum[r[j - 1]]; j--) {
+        const int t = r[j];
+        r[j] = r[j - 1];
+        r[j - 1] = t;
+      }
+    for (int i = 0; i < 3; i++) push(pri_list[i], 0);
+    for (int sec = 1; sec <= 2; sec++) {
+      push(0, sec);
+      for (int k = 0; k < 3; k++)
+        if (S.gsum[r[k]] > 0) push(pri_list[r[k]], sec);
     }
   } else {
-    for (int pri : {0, 1, 2, 4})
-      for (int sec : {0, 1, 2})
-        if (pri || sec) cands.push_back({pri, sec});
+    const int pl[4] = {0, 1, 2, 4};
+    for (int i = 0; i < 4; i++)
+      for (int sec = 0; sec <= 2; sec++)
+        if (pl[i] || sec) push(pl[i], sec);
   }
-  const size_t nl = cands.size();
-  const size_t nc = mono ? 1 : nl;
-  // ly[i][u], lc[i][u] flattened.
-  std::vector<int64_t> ly(nl * nu), lc(nc * nu);
-  for (size_t i = 0; i < nl; i++) {
-    const int c = col(cands[i].first, cands[i].second);
-    for (int u = 0; u < nu; u++) ly[i * nu + u] = ltab[u * kNCand + c];
-  }
-  for (size_t i = 0; i < nc; i++) {
-    if (mono) {
-      for (int u = 0; u < nu; u++) lc[u] = 0;
-      break;
-    }
-    const int c = col(cands[i].first, cands[i].second);
-    for (int u = 0; u < nu; u++) lc[i * nu + u] = utab[u * kNCand + c] + vtab[u * kNCand + c];
-  }
-  std::vector<int64_t> d_off(nu), thr(nu);
-  int64_t total_off = 0;
-  for (int u = 0; u < nu; u++) {
-    d_off[u] = ly[u] + lc[u];
-    thr[u] = off_of(d_off[u]);
-    total_off += d_off[u];
-  }
-  const size_t n_pairs = nl * nc;
-  // d_pair(p, u) for every pair, row-major by pair (n_pairs x nu).
-  std::vector<int64_t> dp(n_pairs * nu);
-  for (size_t pp = 0; pp < n_pairs; pp++) {
-    const int64_t* a = &ly[(pp / nc) * nu];
-    const int64_t* b = &lc[(pp % nc) * nu];
-    int64_t* r = &dp[pp * nu];
-    for (int u = 0; u < nu; u++) r[u] = a[u] + b[u];
-  }
-  auto d_pair = [&](size_t pp, int u) { return dp[pp * nu + u]; };
-  // Units that never signal contribute d_off whatever the entry.
-  std::vector<int> sig_units;
-  int64_t unsig_off = 0;
-  for (int u = 0; u < nu; u++) {
-    if (signaled[u])
-      sig_units.push_back(u);
-    else
-      unsig_off += d_off[u];
-  }
-  size_t global_entry = 0;
-  int64_t prefix[4] = {INT64_MAX, INT64_MAX, INT64_MAX, INT64_MAX};
-  for (size_t pp = 0; pp < n_pairs; pp++) {
-    const int64_t* r = &dp[pp * nu];
-    int64_t t = unsig_off;
-    for (int u : sig_units) t += r[u];
-    if (t < prefix[0]) {
-      prefix[0] = t;
-      global_entry = pp;
+  S.nl = n;
+  S.nc = a.mono ? 1 : n;
+  S.np = n * S.nc;
+  for (int k = 0; k < 4; k++) S.prefix[k] = LLONG_MAX;
+  S.entries[0] = 0;
+  S.nentries = 1;
+}
+
+// Per (pair, chunk of units): the pair's total over the signalling units.
+// Pass 0 (the single-entry pass): its distortion.  Greedy passes: the set
+// extended by the pair, each unit at the better of the set and the pair, or
+// at CDEF off when that is within the margin.
+__global__ void __launch_bounds__(kSearchThreads) cdef_pair_sum_kernel(SearchArgs a, int buf) {
+  const SearchState& S = *a.S;
+  const int pp = blockIdx.y;
+  if (S.n_sig == 0 || pp >= S.np) return;
+  unsigned long long v[1] = {0};
+  for (int u = blockIdx.x * kSearchThreads + threadIdx.x; u < a.nu; u += gridDim.x * kSearchThreads) {
+    if (!a.sig[u]) continue;
+    const long long r = d_pair(a, S, pp, u);
+    if (buf == 0) {
+      v[0] += (unsigned long long)r;
+    } else {
+      const long long b = a.cm[u] < r ? a.cm[u] : r;
+      v[0] += (unsigned long long)(b >= a.thr[u] ? a.d_off[u] : b);
     }
   }
-  // Greedy set construction on the signalled units (compacted copies).
-  const size_t ns = sig_units.size();
-  std::vector<int64_t> cm(ns), th(ns), off(ns), dps(n_pairs * ns);
-  for (size_t k = 0; k < ns; k++) {
-    const int u = sig_units[k];
-    cm[k] = d_off[u];
-    th[k] = thr[u];
-    off[k] = d_off[u];
-  }
-  for (size_t pp = 0; pp < n_pairs; pp++)
-    for (size_t k = 0; k < ns; k++) dps[pp * ns + k] = dp[pp * nu + sig_units[k]];
-  std::vector<size_t> entries = {0};
-  while (entries.size() < 8) {
-    size_t best_p = 0;
-    int64_t best_tot = INT64_MAX;
-    for (size_t pp = 0; pp < n_pairs; pp++) {
-      const int64_t* r = &dps[pp * ns];
-      int64_t tot = unsig_off;
-      for (size_t k = 0; k < ns; k++) {
-        const int64_t b = cm[k] < r[k] ? cm[k] : r[k];
-        tot += b >= th[k] ? off[k] : b;
-      }
-      if (tot < best_tot) {
-        best_tot = tot;
-        best_p = pp;
-      }
+  unsigned long long* const dst[1] = {&a.S->tot[buf][pp]};
+  block_add<1>(v, dst);
+}
+
+// First minimum over the pairs of unsig_off + tot[buf][pair].
+__device__ __forceinline__ int first_min(const SearchState& S, int buf, long long* best) {
+  int bp = 0;
+  long long bt = LLONG_MAX;
+  for (int pp = 0; pp < S.np; pp++) {
+    const long long t = (long long)(S.unsig_off + S.tot[buf][pp]);
+    if (t < bt) {
+      bt = t;
+      bp = pp;
     }
-    entries.push_back(best_p);
-    const int64_t* r = &dps[best_p * ns];
-    for (size_t k = 0; k < ns; k++) cm[k] = std::min(cm[k], r[k]);
-    const size_t n = entries.size();
-    if ((n & (n - 1)) == 0) prefix[__builtin_ctzll(n)] = best_tot;
   }
-  auto pair_strengths = [&](size_t pp, int s[4]) {
-    s[0] = cands[pp / nc].first;
-    s[1] = cands[pp / nc].second;
-    s[2] = mono ? 0 : cands[pp % nc].first;
-    s[3] = mono ? 0 : cands[pp % nc].second;
-  };
-  auto assign = [&](const size_t* set, size_t nset, std::vector<uint8_t>& grid) -> int64_t {
-    int z = -1;
-    for (size_t e = 0; e < nset; e++)
-      if (set[e] == 0) {
-        z = (int)e;
-        break;
-      }
-    int64_t total = 0;
-    grid.assign(nu, 0);
-    for (int u = 0; u < nu; u++) {
-      if (!signaled[u]) {
-        total += d_off[u];
-        continue;
-      }
-      bool have = false;
-      int pm = 0;
-      int64_t pd = 0, rb_d = INT64_MAX;
-      size_t pe = 0, rb_e = 0;
-      for (size_t e = 0; e < nset; e++) {
-        const int64_t d = d_pair(set[e], u);
-        if (d < rb_d) {
-          rb_d = d;
-          rb_e = e;
-        }
-        if (d < thr[u]) {
-          int s[4];
-          pair_strengths(set[e], s);
-          const int mag = s[0] + s[1] + s[2] + s[3];
-          if (!have || mag < pm || (mag == pm && d < pd)) {
-            have = true;
-            pm = mag;
-            pd = d;
-            pe = e;
+  *best = bt;
+  return bp;
+}
+
+// The single-entry pass's best pair (one thread).
+__global__ void cdef_global_entry_kernel(SearchArgs a) {
+  SearchState& S = *a.S;
+  if (S.n_sig == 0) return;
+  long long bt;
+  S.global_entry = first_min(S, 0, &bt);
+  S.prefix[0] = bt;
+}
+
+// One greedy step: every CTA finds the pass's best pair (the same one) and
+// lowers its units' set distortion to it; CTA 0 records the entry and clears
+// the other pass buffer for the next step.
+__global__ void __launch_bounds__(kSearchThreads) cdef_greedy_step_kernel(SearchArgs a, int buf) {
+  SearchState& S = *a.S;
+  if (S.n_sig == 0) return;
+  __shared__ int s_best;
+  __shared__ long long s_tot;
+  if (threadIdx.x == 0) {
+    long long bt;
+    s_best = first_min(S, buf, &bt);
+    s_tot = bt;
+  }
+  __syncthreads();
+  const int bp = s_best;
+  if (blockIdx.x == 0) {
+    const int other = buf == 1 ? 2 : 1;
+    for (int pp = threadIdx.x; pp < kMaxPairs; pp += blockDim.x) S.tot[other][pp] = 0;
+    if (threadIdx.x == 0) {
+      const int n = S.nentries + 1;
+      S.entries[n - 1] = bp;
+      S.nentries = n;
+      if ((n & (n - 1)) == 0) S.prefix[__ffs(n) - 1] = s_tot;
+    }
+  }
+  for (int u = blockIdx.x * kSearchThreads + threadIdx.x; u < a.nu; u += gridDim.x * kSearchThreads) {
+    if (!a.sig[u]) continue;
+    const long long r = d_pair(a, S, bp, u);
+    if (r < a.cm[u]) a.cm[u] = r;
+  }
+}
+
+// The 2-, 4- and 8-entry sets' per-unit entries and totals: a unit takes the
+// smallest-magnitude entry within its margin (ties by distortion, then list
+// order), else the zero entry at CDEF off, else its best entry.
+__global__ void __launch_bounds__(kSearchThreads) cdef_assign_kernel(SearchArgs a) {
+  const SearchState& S = *a.S;
+  if (S.n_sig == 0) return;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long v[3] = {0, 0, 0};
+  if (u < a.nu) {
+    for (int b = 1; b <= 3; b++) {
+      const int nset = 1 << b;
+      uint8_t g = 0;
+      if (!a.sig[u]) {
+        v[b - 1] = (unsigned long long)a.d_off[u];
+      } else {
+        int z = -1;
+        for (int e = 0; e < nset; e++)
+          if (S.entries[e] == 0) {
+            z = e;
+            break;
+          }
+        bool have = false;
+        int pm = 0, pe = 0, rb_e = 0;
+        long long pd = 0, rb_d = LLONG_MAX;
+        for (int e = 0; e < nset; e++) {
+          const long long d = d_pair(a, S, S.entries[e], u);
+          if (d < rb_d) {
+            rb_d = d;
+            rb_e = e;
+          }
+          if (d < a.thr[u]) {
+            int s[4];
+            pair_strengths(S, a.mono, S.entries[e], s);
+            const int mag = s[0] + s[1] + s[2] + s[3];
+            if (!have || mag < pm || (mag == pm && d < pd)) {
+              have = true;
+              pm = mag;
+              pd = d;
+              pe = e;
+            }
           }
         }
+        long long t;
+        if (have) {
+          t = pd;
+          g = (uint8_t)pe;
+        } else if (z >= 0) {
+          t = a.d_off[u];
+          g = (uint8_t)z;
+        } else {
+          t = rb_d;
+          g = (uint8_t)rb_e;
+        }
+        v[b - 1] = (unsigned long long)t;
       }
-      if (have) {
-        total += pd;
-        grid[u] = (uint8_t)pe;
-      } else if (z >= 0) {
-        total += d_off[u];
-        grid[u] = (uint8_t)z;
-      } else {
-        total += rb_d;
-        grid[u] = (uint8_t)rb_e;
-      }
+      a.grids[(size_t)(b - 1) * a.nu + u] = g;
     }
-    return total;
-  };
-  const float lambda = frame_lambda_d(p->base_q_idx, p->bd, p->sub_x, p->sub_y, dc_q);
-  const float cost_off = (float)total_off;
-  const float per_entry_bits = mono ? 6.0f : 12.0f;
+  }
+  unsigned long long* const dst[3] = {&a.S->assign_total[1], &a.S->assign_total[2], &a.S->assign_total[3]};
+  block_add<3>(v, dst);
+}
+
+// The rate decision (one thread): CDEF off, the single entry, or 2 / 4 / 8
+// entries, each priced as distortion + lambda_d x (entry bits + index bits).
+__global__ void cdef_decide_kernel(SearchArgs a) {
+  SearchState& S = *a.S;
+  S.bits = -1;
+  S.n_strengths = 0;
+  for (int e = 0; e < 8; e++)
+    for (int k = 0; k < 4; k++) S.strengths[e][k] = 0;
+  if (S.n_sig == 0) return;
+  const long long total_off = (long long)S.total_off;
+  const float per_entry_bits = a.mono ? 6.0f : 12.0f;
+  const int n_sig = (int)S.n_sig, n_trusted = (int)S.n_trusted;
   int best_bits = -1;
-  float best_cost = cost_off;
-  std::vector<uint8_t> grid;
+  float best_cost = __ll2float_rn(total_off);
   for (int b = 0; b <= 3; b++) {
     const int nb = 1 << b;
-    const int64_t total = b == 0 ? prefix[0] : assign(entries.data(), nb, grid);
-    if (total == INT64_MAX) continue;
-    if (b == 0 && (global_entry == 0 || n_trusted * 4 < n_sig * 3 || total >= off_of(total_off))) continue;
-    volatile float e_bits = per_entry_bits * (float)(nb - 1);
-    volatile float u_bits = (float)b * (float)n_sig;
-    volatile float bits_f = e_bits + u_bits;
-    volatile float lb = lambda * bits_f;
-    const float cost = (float)total + lb;
+    const long long total = b == 0 ? S.prefix[0] : (long long)S.assign_total[b];
+    if (total == LLONG_MAX) continue;
+    if (b == 0 && (S.global_entry == 0 || n_trusted * 4 < n_sig * 3 || total >= off_of(total_off))) continue;
+    const float e_bits = __fmul_rn(per_entry_bits, __int2float_rn(nb - 1));
+    const float u_bits = __fmul_rn(__int2float_rn(b), __int2float_rn(n_sig));
+    const float bits_f = __fadd_rn(e_bits, u_bits);
+    const float lb = __fmul_rn(a.lambda, bits_f);
+    const float cost = __fadd_rn(__ll2float_rn(total), lb);
     if (cost < best_cost) {
       best_cost = cost;
       best_bits = b;
     }
   }
   if (best_bits < 0) return;
-  std::vector<size_t> set;
-  if (best_bits == 0)
-    set = {global_entry};
-  else
-    set.assign(entries.begin(), entries.begin() + (1 << best_bits));
-  grid.assign(nu, 0);
-  if (best_bits > 0) assign(set.data(), set.size(), grid);
-  out->bits = best_bits;
-  out->n_strengths = (int)set.size();
-  for (size_t e = 0; e < set.size(); e++) {
+  const int n = 1 << best_bits;
+  S.bits = best_bits;
+  S.n_strengths = n;
+  for (int e = 0; e < n; e++) {
     int s[4];
-    pair_strengths(set[e], s);
-    for (int k = 0; k < 4; k++) out->strengths[e][k] = (uint8_t)s[k];
+    pair_strengths(S, a.mono, best_bits == 0 ? S.global_entry : S.entries[e], s);
+    for (int k = 0; k < 4; k++) S.strengths[e][k] = (uint8_t)s[k];
   }
-  if (grid_out && best_bits > 0) memcpy(grid_out, grid.data(), nu);
-  for (int u = 0; u < nu; u++)
-    for (int k = 0; k < 4; k++) ustr[(size_t)u * 4 + k] = out->strengths[grid[u]][k];
+}
+
+// Each unit's entry and strengths under the decision (all zero when CDEF is
+// off: the apply kernel then leaves the planes as they are).
+__global__ void __launch_bounds__(kSearchThreads) cdef_unit_strengths_kernel(SearchArgs a) {
+  const SearchState& S = *a.S;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= a.nu) return;
+  const int g = S.bits > 0 ? a.grids[(size_t)(S.bits - 1) * a.nu + u] : 0;
+  a.grid[u] = (uint8_t)g;
+#pragma unroll
+  for (int k = 0; k < 4; k++) a.ustr[(size_t)u * 4 + k] = S.bits >= 0 ? S.strengths[g][k] : 0;
+}
+
+// The search's launches on the stream, after the tables.
+constexpr int kSearchLaunches = 7 + 2 * kGreedySteps;
+
+int launch_search(const SearchArgs& a, cudaStream_t st) {
+  if (cudaMemsetAsync(a.S, 0, sizeof(SearchState), st) != cudaSuccess) return MT_ERR_DEVICE;
+  const int ublocks = (a.nu + kSearchThreads - 1) / kSearchThreads;
+  const int chunks = std::min(ublocks, 16);  // unit chunks per pair in the pass sums
+  cdef_unit_stats_kernel<<<ublocks, kSearchThreads, 0, st>>>(a);
+  cdef_plan_kernel<<<1, 1, 0, st>>>(a);
+  cdef_pair_sum_kernel<<<dim3(chunks, kMaxPairs), kSearchThreads, 0, st>>>(a, 0);
+  cdef_global_entry_kernel<<<1, 1, 0, st>>>(a);
+  for (int k = 0; k < kGreedySteps; k++) {
+    const int buf = 1 + (k & 1);
+    cdef_pair_sum_kernel<<<dim3(chunks, kMaxPairs), kSearchThreads, 0, st>>>(a, buf);
+    cdef_greedy_step_kernel<<<std::min(ublocks, 64), kSearchThreads, 0, st>>>(a, buf);
+  }
+  cdef_assign_kernel<<<ublocks, kSearchThreads, 0, st>>>(a);
+  cdef_decide_kernel<<<1, 1, 0, st>>>(a);
+  cdef_unit_strengths_kernel<<<ublocks, kSearchThreads, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
 }  // namespace
@@ -958,28 +1117,31 @@ int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint
                      tabs + 2 * nu * kNCand, dv_sum, dv_cnt, st);
   if (rc != MT_OK) return rc;
   mth::cdef_last_launches = 2;
-  // Read the tables back (one copy) for the host search.
-  std::vector<uint8_t> host(L.read_bytes);
-  if (cudaMemcpyAsync(host.data(), s + L.tabs, L.read_bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
-    return MT_ERR_DEVICE;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;
-  const int64_t* h_tabs = reinterpret_cast<const int64_t*>(host.data());
-  const int64_t* h_dv_sum = reinterpret_cast<const int64_t*>(host.data() + (L.dv_sum - L.tabs));
-  const int32_t* h_dv_cnt = reinterpret_cast<const int32_t*>(host.data() + (L.dv_cnt - L.tabs));
+  // the strength search on the stream
   mt_quant q;
   if (mt_quant_init((uint8_t)prm->base_q_idx, (uint8_t)prm->bd, 15, &q) != MT_OK) return MT_ERR_INVALID_INPUT;
-  std::vector<uint8_t> ustr;
-  decide(prm, g, h_tabs, h_tabs + nu * kNCand, h_tabs + 2 * nu * kNCand, h_dv_sum, h_dv_cnt, (float)q.dc_q, out, grid,
-         ustr);
-  if (out->bits < 0) return MT_OK;
-  bool any_y = false, any_uv = false;
-  for (size_t u = 0; u < nu; u++) {
-    any_y |= (ustr[u * 4] | ustr[u * 4 + 1]) != 0;
-    any_uv |= (ustr[u * 4 + 2] | ustr[u * 4 + 3]) != 0;
-  }
-  if (!any_y && (mono || !any_uv)) return MT_OK;
-  if (cudaMemcpyAsync(s + L.ustr, ustr.data(), nu * 4, cudaMemcpyHostToDevice, st) != cudaSuccess)
-    return MT_ERR_DEVICE;
+  SearchArgs sa;
+  sa.ltab = reinterpret_cast<const long long*>(tabs);
+  sa.utab = reinterpret_cast<const long long*>(tabs + nu * kNCand);
+  sa.vtab = reinterpret_cast<const long long*>(tabs + 2 * nu * kNCand);
+  sa.dv_sum = dv_sum;
+  sa.dv_cnt = dv_cnt;
+  sa.nu = (int)nu;
+  sa.mono = mono;
+  sa.slow = prm->slow != 0;
+  sa.lambda = frame_lambda_d(prm->base_q_idx, prm->bd, prm->sub_x, prm->sub_y, (float)q.dc_q);
+  sa.S = reinterpret_cast<SearchState*>(s + L.state);
+  sa.d_off = reinterpret_cast<long long*>(s + L.d_off);
+  sa.thr = reinterpret_cast<long long*>(s + L.thr);
+  sa.cm = reinterpret_cast<long long*>(s + L.cm);
+  sa.sig = s + L.sig;
+  sa.grids = s + L.grids;
+  sa.grid = s + L.grid;
+  sa.ustr = s + L.ustr;
+  if ((rc = launch_search(sa, st)) != MT_OK) return rc;
+  mth::cdef_last_launches += kSearchLaunches;
+  // the filter from a pre-CDEF snapshot, with each unit's strengths (all zero:
+  // the planes stay as they are)
   ApplyArgs aa;
   aa.rec[0] = d_y;
   aa.rec[1] = d_u;
@@ -994,10 +1156,18 @@ int mt_cdef_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint
     if (cudaMemcpyAsync(s + L.snap_v, d_v, nc, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MT_ERR_DEVICE;
   }
   cdef_apply_kernel<<<dim3(g.nbx, g.nby, mono ? 1 : 3), 64, 0, st>>>(aa, g, d_skip8, dirs, vars, s + L.ustr);
-  mth::cdef_last_launches = 3;
-  // The strengths were staged from pageable host memory; keep the buffer alive
-  // until the copy has been consumed.
+  mth::cdef_last_launches += 1;
+  // the decision back to the host, once, at the end
+  SearchState hs;
+  if (cudaMemcpyAsync(&hs, s + L.state, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess) return MT_ERR_DEVICE;
+  if (grid && cudaMemcpyAsync(grid, s + L.grid, nu, cudaMemcpyDeviceToHost, st) != cudaSuccess) return MT_ERR_DEVICE;
   if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;
+  out->bits = hs.bits;
+  out->damping = 3 + std::min(prm->base_q_idx / 64, 3);
+  out->n_strengths = hs.n_strengths;
+  out->unit_cols = g.uc;
+  out->unit_rows = g.ur;
+  memcpy(out->strengths, hs.strengths, sizeof(out->strengths));
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 

@@ -107,6 +107,7 @@ CASES = [
     (640, 480, (1, 1), False, 20, True, 20),  # 3
     (640, 480, (0, 0), False, 10, True, 24),  # 2
     (1920, 1080, (1, 1), False, 70, True, 3),
+    (1280, 720, (0, 0), False, 50, True, 26),
 ]
 
 
