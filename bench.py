@@ -783,6 +783,122 @@ def measure_batch(steps, avif_alone, reps=3):
                         f"{SEED}..{SEED + BATCH - 1}), host RGB in, AVIF bytes out, wall time of the call"}
 
 
+C3_W = C3_H = 4096  # the 4096x4096 4:4:4 quality-60 frame: two tiles
+
+
+def measure_c3(dev, hbm_peak, steps, reps=5):
+    """The 4096x4096 frame (generator seed 5, sigma 8 noise on the left half,
+    piecewise-constant cells on the right), 4:4:4 quality 60: the whole encode
+    through mt_encode_rgb8 (host RGB in, AVIF out; two tiles), and the frame
+    filters at that size against the HBM roofline -- deblocking of the three
+    planes with the encoder's uniform 8x8 geometry and with random AV1-shaped
+    geometry, the CDEF tables and the whole frame CDEF (tables, strength
+    search, apply) -- each timed with CUDA events after an L2 flush."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+    from maroontree_b200 import encoder as enc
+
+    lib = mt.load()
+    rgb = synth.generate_rgb(C3_W, C3_H, 5, sigma=8.0, variant="large")
+    cfg = enc.config(quality=60, chroma=2)
+    first = enc.encode_rgb8(rgb, cfg)  # warm-up (buffers, module)
+    times, st = [], abi.EncodeStats()
+    for _ in range(max(steps, 3)):
+        t0 = time.perf_counter()
+        out = enc.encode_rgb8(rgb, cfg, stats=st)
+        times.append(time.perf_counter() - t0)
+        if out != first:
+            raise SystemExit("bench: the 4096x4096 encode is not repeatable")
+    dt = float(np.median(times))
+    res = {"workload": "mt_encode_rgb8 of the 4096x4096 4:4:4 quality-60 frame (two tiles), host RGB in, AVIF out, "
+                       "median wall time",
+           "ms": round(dt * 1e3, 2), "mpix_s": round(C3_W * C3_H / dt / 1e6, 2), "avif_bytes": len(first),
+           "blocks_kernel_ms": round(st.blocks_ms, 3), "levels": int(st.levels), "blocks": int(st.blocks),
+           "tokens": int(st.tokens)}
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    t16 = lambda a: torch.from_numpy(np.ascontiguousarray(a).astype(np.int16)).to(dev)
+    t8 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.uint8)).to(dev)
+
+    def timed(fn, reset):
+        ms = []
+        for i in range(reps + 2):
+            reset()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            flush.zero_()
+            torch.cuda._sleep(200_000)
+            a.record()
+            rc = fn()
+            b.record()
+            torch.cuda.synchronize()
+            assert rc == 0, rc
+            if i >= 2:
+                ms.append(a.elapsed_time(b))
+        return float(np.median(ms))
+
+    def entry(ms, nbytes, what):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        return {"ms": round(ms, 4), "alg_bytes": int(nbytes), "achieved_gbs": round(gbs, 1),
+                "frac_hbm": round(gbs / hbm_peak, 4), "bytes": what}
+
+    src, rec, skip = synth.cdef_inputs(C3_W, C3_H, 0, 0, False, 5, rgb=rgb)
+    samples = 3 * C3_W * C3_H
+    r0 = [t16(p) for p in rec]
+    rr = [p.clone() for p in r0]
+    ss = [t16(p) for p in src]
+
+    def reset():
+        for a, b in zip(rr, r0):
+            a.copy_(b)
+
+    g = abi.DeblockFrameParams()
+    g.w8, g.h8, g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = C3_W, C3_H, C3_W, C3_H, 0, 0, 0, 8
+    scr = torch.empty(max(1, lib.mt_deblock_frame_scratch_bytes(C.byref(g))), dtype=torch.uint8, device=dev)
+    ly, luv, _ = mt.loop_filter_levels(70, 0, 0)
+    n4r, n4c = C3_H // 4, C3_W // 4
+    two = np.full((n4r, n4c), 2, np.uint8)
+    uniform = [two, two, np.tile((np.arange(n4c) % 2 == 0).astype(np.uint8), (n4r, 1)),
+               np.tile((np.arange(n4r) % 2 == 0).astype(np.uint8)[:, None], (1, n4c)), two, two]
+    pwm, phm, _, _, bid = synth.partition_maps(n4c, n4r, 7)
+    random_maps = list(synth.transform_maps(pwm, phm, bid, 8)) + [pwm, phm]
+    outp = [torch.empty_like(p) for p in rr]
+    for tag, mp in (("deblock_uniform8", uniform), ("deblock_random", random_maps)):
+        maps = [t8(m) for m in mp]
+        # the encoder's entry: unfiltered planes in, filtered planes out
+        ms = timed(lambda: lib.mt_deblock_frame_device_to(*[p.data_ptr() for p in rr], *[p.data_ptr() for p in outp],
+                                                          *[m.data_ptr() for m in maps], C.byref(g), ly, luv, luv,
+                                                          scr.data_ptr(), None), reset)
+        res[tag] = entry(ms, 4 * samples, "2 B read + 2 B write per sample (3 planes, both edge directions)")
+        # the in-place entry (a snapshot copy of the planes first)
+        ms = timed(lambda: lib.mt_deblock_frame_device(*[p.data_ptr() for p in rr], *[m.data_ptr() for m in maps],
+                                                       C.byref(g), ly, luv, luv, scr.data_ptr(), None), reset)
+        res[tag]["in_place_ms"] = round(ms, 4)
+    prm = mt.cdef_params(C3_W, C3_H, 0, 0, 70)
+    sk = t8(skip)
+    nu = (C3_W // 64) * (C3_H // 64)
+    dirs = torch.empty(skip.size, dtype=torch.uint8, device=dev)
+    vars_ = torch.empty(skip.size, dtype=torch.int32, device=dev)
+    tabs = [torch.empty((nu, 12), dtype=torch.int64, device=dev) for _ in range(3)]
+    ms = timed(lambda: lib.mt_cdef_tables_device(*[p.data_ptr() for p in rr], *[p.data_ptr() for p in ss],
+                                                 sk.data_ptr(), C.byref(prm), dirs.data_ptr(), vars_.data_ptr(),
+                                                 *[t.data_ptr() for t in tabs], None), reset)
+    res["cdef_tables"] = entry(ms, 4 * samples, "2 B recon + 2 B source read per sample")
+    res["cdef_tables"]["bound"] = "issue (12 candidate filters + weighted SSE per sample)"
+    cscr = torch.empty(lib.mt_cdef_scratch_bytes(C.byref(prm)), dtype=torch.uint8, device=dev)
+    dec = abi.CdefDecision()
+    ms = timed(lambda: lib.mt_cdef_frame_device(*[p.data_ptr() for p in rr], *[p.data_ptr() for p in ss],
+                                                sk.data_ptr(), C.byref(prm), cscr.data_ptr(), C.byref(dec), None,
+                                                None), reset)
+    res["cdef_frame"] = entry(ms, 6 * samples, "tables + apply: 2 B recon + 2 B source + 2 B write per sample")
+    res["cdef_frame"]["cdef_bits"] = dec.bits
+    res["filters_workload"] = ("4096x4096 4:4:4 planes of the same frame (luma, contrast-reduced chroma copies) with "
+                               "seeded per-unit coding error; qindex 70; L2 flushed before each timed call")
+    return res
+
+
 def run_ours(args):
     import torch
     import maroontree_b200 as mt
@@ -856,6 +972,7 @@ def run_ours(args):
     cpu = parity = None
     if rank == 0:
         secondary["batch"] = measure_batch(args.steps, avif)
+        secondary["c3"] = measure_c3(dev, hbm_peak, args.steps)
     nocpu = world > 1 or args.no_cpu
     if rank == 0 and not args.headline_only:
         wl = make_workload()

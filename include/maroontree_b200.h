@@ -781,11 +781,27 @@ typedef struct mt_deblock_frame_params {
  * tuning): the frame's luma and chroma levels and the sharpness. */
 int mt_loop_filter_levels(int32_t base_q_idx, int32_t sub_x, int32_t sub_y, int32_t* lvl_y, int32_t* lvl_uv,
                           int32_t* sharp);
+/* Device working storage of the two device entries below (edge widths per
+ * cell, the chroma geometry, and room for the unfiltered planes of an
+ * in-place call). */
 size_t mt_deblock_frame_scratch_bytes(const mt_deblock_frame_params* prm);
+/* The frame deblocked in place on the stream: the planes are snapshotted into
+ * the scratch, then each 64x64 tile is filtered from the snapshot (all
+ * vertical, then all horizontal edges, in shared memory) and written once.
+ * Maps whose edges have overlapping taps (no AV1 geometry has them) are
+ * filtered by two frame-wide passes that keep the reference's order. */
 int mt_deblock_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const uint8_t* d_blk4,
                             const uint8_t* d_blk4h, const uint8_t* d_blk4v, const uint8_t* d_blk4t,
                             const uint8_t* d_pblk4, const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm,
                             int32_t lvl_y, int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream);
+/* The same from unfiltered planes d_in_* (left unchanged) into the planes
+ * d_* (same sizes, separate buffers), without the snapshot.  No counterpart in
+ * the reference, which filters in place. */
+int mt_deblock_frame_device_to(const uint16_t* d_in_y, const uint16_t* d_in_u, const uint16_t* d_in_v, uint16_t* d_y,
+                               uint16_t* d_u, uint16_t* d_v, const uint8_t* d_blk4, const uint8_t* d_blk4h,
+                               const uint8_t* d_blk4v, const uint8_t* d_blk4t, const uint8_t* d_pblk4,
+                               const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm, int32_t lvl_y,
+                               int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream);
 int mt_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,
                      const uint8_t* blk4v, const uint8_t* blk4t, const uint8_t* pblk4, const uint8_t* pblk4h,
                      const mt_deblock_frame_params* prm, int32_t lvl_y, int32_t lvl_u, int32_t lvl_v);

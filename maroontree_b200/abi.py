@@ -357,6 +357,8 @@ def _bind(lib):
         "mt_loop_filter_levels": (C.c_int, [C.c_int32] * 3 + [C.POINTER(C.c_int32)] * 3),
         "mt_deblock_frame_scratch_bytes": (C.c_size_t, [C.POINTER(DeblockFrameParams)]),
         "mt_deblock_frame_device": (C.c_int, [_P] * 9 + [C.POINTER(DeblockFrameParams)] + [C.c_int32] * 3 + [_P, _P]),
+        "mt_deblock_frame_device_to": (C.c_int, [_P] * 12 + [C.POINTER(DeblockFrameParams)] + [C.c_int32] * 3 +
+                                       [_P, _P]),
         "mt_deblock_frame": (C.c_int, [_P] * 9 + [C.POINTER(DeblockFrameParams)] + [C.c_int32] * 3),
         "mt_cdef_tables_device": (C.c_int, [_P] * 7 + [C.POINTER(CdefParams)] + [_P] * 6),
         "mt_cdef_scratch_bytes": (C.c_size_t, [C.POINTER(CdefParams)]),
@@ -448,7 +450,7 @@ EXPORTED_SYMBOLS = (
     "mt_rdo_level4", "mt_rdo_level4_device", "mt_rdo_level4_scratch_bytes", "mt_fwd_txfm_quant_device",
     "mt_rdo_level16", "mt_rdo_level16_device", "mt_rdo_level16_scratch_bytes",
     "mt_padded_plane_dims", "mt_csc_rgb8", "mt_csc_rgb8_device", "mt_deblock_plane", "mt_deblock_plane_device",
-    "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame",
+    "mt_loop_filter_levels", "mt_deblock_frame_scratch_bytes", "mt_deblock_frame_device", "mt_deblock_frame_device_to", "mt_deblock_frame",
     "mt_cdef_tables_device", "mt_cdef_scratch_bytes", "mt_cdef_frame_device", "mt_cdef_frame",
     "mt_inv_txfm_dequant_device", "mt_trellis_optimize_device", "mt_intra_predict_device",
     "mt_tiling_spec_min", "mt_aq_grid_scratch_bytes", "mt_aq_grid_device", "mt_aq_grid", "mt_dark_pow_device",

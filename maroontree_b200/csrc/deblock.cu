@@ -353,6 +353,280 @@ __global__ void __launch_bounds__(128) lf_horz_kernel(uint16_t* __restrict__ px,
   }
 }
 
+// ---------------------------------------------------------------------------
+// The frame path.  The fused kernel filters each 64x64 tile in shared memory:
+// the tile's region (a 16-sample halo holds every tap its samples depend on)
+// and the block maps of the region's cells are loaded once, the edge widths
+// computed there, then all vertical edges and all horizontal edges filtered,
+// reading the unfiltered plane and writing the tile once into the filtered
+// plane (a separate buffer: neighbouring tiles read their halos while others
+// are being written) -- the samples of the frame-wide two-pass order.  Each
+// tile also checks whether an edge of its own cells has taps overlapping one
+// of the next three edges of its line (never with AV1 block geometry); if any
+// tile finds one, it raises a flag, the unfiltered planes are copied over the
+// filtered ones, and the two-pass kernels above (which keep overlapping runs
+// in the reference's order) filter them in place.
+
+struct FramePlane {
+  const uint16_t* in;  // the unfiltered plane (never written while the fused kernel runs)
+  uint16_t* px;        // the filtered plane
+  const uint8_t* bw4;
+  const uint8_t* bh4;
+  const uint8_t* vedge4;
+  const uint8_t* hedge4;
+  PlaneArgs a;
+  int nr4;  // map rows
+  int on;
+};
+struct FrameArgs {
+  FramePlane p[3];
+};
+
+// One line across a horizontal edge in shared memory (col: the sample on the
+// edge's lower side, rows pitch apart).
+template <int WD>
+__device__ __forceinline__ void lf_col(uint16_t* col, int pitch, const LfLimits L, int bd) {
+  using R = Reach<WD>;
+  int v[14];
+#pragma unroll
+  for (int k = -R::RLO; k <= R::RHI; k++) v[7 + k] = col[k * pitch];
+  lf_core<WD>(v, L, bd);
+#pragma unroll
+  for (int k = -R::WLO; k <= R::WHI; k++) col[k * pitch] = (uint16_t)v[7 + k];
+}
+
+constexpr int kFT = 64;              // output tile
+constexpr int kFH = 16;              // halo: every tap of an edge that writes the tile
+constexpr int kFR = kFT + 2 * kFH;   // region side, samples
+constexpr int kFP = kFR + 2;         // row pitch (odd in 4-byte words: column walks are conflict-free)
+constexpr int kFC = kFR / 4;         // region side, cells
+constexpr int kFM = kFC + 1;         // map block side: the region's cells and the cells before them
+constexpr int kFE0 = 3, kFE1 = 21;   // region cells whose edges write the tile (4c - 6 <= 79, 4c + 5 >= 16)
+constexpr int kFThreads = 256;
+
+// edge_wd on the map block in shared memory: the edge before map cell (mr, mc)
+// along a line (dv = 1: vertical edge, the previous cell to the left; else
+// horizontal, the previous cell above), i its cell index along the line.
+__device__ __forceinline__ int smem_edge_wd(const uint8_t* dim, const uint8_t* flag, bool has_flag, int mr, int mc,
+                                            bool vert, int i, int n4, int len, bool luma) {
+  if (i < 1 || i >= n4) return 0;
+  const int cur = dim[mr * kFM + mc];
+  if (cur == 0) return 0;
+  const bool present = has_flag ? flag[mr * kFM + mc] != 0 : (i % cur == 0);
+  if (!present) return 0;
+  const int prev = vert ? dim[mr * kFM + mc - 1] : dim[(mr - 1) * kFM + mc];
+  const int a = lf_cls(cur, luma), b = lf_cls(prev, luma);
+  const int wd = lf_wd(a < b ? a : b, luma);
+  if (4 * i - lf_reach_lo(wd) < 0 || 4 * i + lf_reach_hi(wd) >= len) return 0;
+  return wd;
+}
+
+// Width class of a filter width (4, 6, 8, 16 -> 0..3).
+__device__ __forceinline__ int wd_class(int wd) { return wd == 4 ? 0 : (wd == 6 ? 1 : (wd == 8 ? 2 : 3)); }
+
+constexpr int kFMaxV = (kFC - 2) * (kFE1 - kFE0 + 1);  // vertical edges filtered: cell rows 1..kFC-2
+constexpr int kFMaxH = (kFE1 - kFE0 + 1) * (kFT / 4);  // horizontal edges filtered: the tile's cell columns
+
+__global__ void __launch_bounds__(kFThreads) lf_fused_kernel(FrameArgs fa, int* __restrict__ overlap) {
+  const FramePlane& P = fa.p[blockIdx.z];
+  if (!P.px || (!P.on && P.in == P.px)) return;  // no plane, or unfiltered in place
+  const PlaneArgs& a = P.a;
+  const int x0 = blockIdx.x * kFT, y0 = blockIdx.y * kFT;
+  if (x0 >= a.w || y0 >= a.h) return;
+  __shared__ __align__(16) uint16_t S[kFR * kFP];
+  __shared__ uint8_t vw[kFC * kFC], hw[kFC * kFC];
+  __shared__ uint8_t mb[4][kFM * kFM];  // bw4, bh4, vedge4, hedge4 of the map block
+  __shared__ uint16_t vlist[4][kFMaxV], hlist[4][kFMaxH];  // active edges by width class: cell row << 8 | col
+  __shared__ int nv[4], nh[4], bad;
+  const int rx0 = x0 - kFH, ry0 = y0 - kFH, c0 = rx0 / 4, r0 = ry0 / 4;
+  const int t = threadIdx.x;
+  const bool on = P.on;  // an unfiltered plane is copied through
+  if (t < 4) {
+    nv[t] = 0;
+    nh[t] = 0;
+  }
+  if (t == 0) bad = 0;
+  // the region's samples, 4 at a time (8-byte loads: rx0, the plane width and
+  // the row starts are multiples of 4 samples)
+  for (int i = t; i < kFR * (kFR / 4); i += kFThreads) {
+    const int r = i / (kFR / 4), c4 = (i - r * (kFR / 4)) * 4;
+    const int gy = ry0 + r, gx = rx0 + c4;
+    uint2 v = make_uint2(0, 0);
+    if (gy >= 0 && gy < a.h && gx >= 0 && gx < a.w)
+      v = *reinterpret_cast<const uint2*>(P.in + (size_t)gy * a.w + gx);
+    uint32_t* d = reinterpret_cast<uint32_t*>(&S[r * kFP + c4]);
+    d[0] = v.x;
+    d[1] = v.y;
+  }
+  // the map block: cells (r0 - 1 .. r0 + kFC - 1) x (c0 - 1 .. c0 + kFC - 1)
+  if (on)
+    for (int i = t; i < kFM * kFM; i += kFThreads) {
+      const int mr = i / kFM, mc = i - mr * kFM;
+      const int gr = r0 - 1 + mr, gc = c0 - 1 + mc;
+      const bool in = gr >= 0 && gr < P.nr4 && gc >= 0 && gc < a.nc4;
+      const long idx = (long)gr * a.nc4 + gc;
+      mb[0][i] = in ? P.bw4[idx] : 0;
+      mb[1][i] = in ? P.bh4[idx] : 0;
+      mb[2][i] = in && P.vedge4 ? P.vedge4[idx] : 0;
+      mb[3][i] = in && P.hedge4 ? P.hedge4[idx] : 0;
+    }
+  __syncthreads();
+  // the region's edge widths (none outside the visible cells), and the lists
+  // of the edges this tile filters
+  if (on)
+    for (int i = t; i < kFC * kFC; i += kFThreads) {
+      const int cr = i / kFC, cc = i - cr * kFC;
+      const int gr = r0 + cr, gc = c0 + cc;
+      const bool in = gr >= 0 && gr < a.h4 && gc >= 0 && gc < a.w4;
+      const int v = in ? smem_edge_wd(mb[0], mb[2], P.vedge4 != nullptr, cr + 1, cc + 1, true, gc, a.w4, a.w, a.luma)
+                       : 0;
+      const int h = in ? smem_edge_wd(mb[1], mb[3], P.hedge4 != nullptr, cr + 1, cc + 1, false, gr, a.h4, a.h, a.luma)
+                       : 0;
+      vw[i] = (uint8_t)v;
+      hw[i] = (uint8_t)h;
+      if (v && cr >= 1 && cr <= kFC - 2 && cc >= kFE0 && cc <= kFE1) {
+        const int k = wd_class(v);
+        vlist[k][atomicAdd(&nv[k], 1)] = (uint16_t)(cr << 8 | cc);
+      }
+      if (h && cr >= kFE0 && cr <= kFE1 && cc >= kFH / 4 && cc < (kFH + kFT) / 4) {
+        const int k = wd_class(h);
+        hlist[k][atomicAdd(&nh[k], 1)] = (uint16_t)(cr << 8 | cc);
+      }
+    }
+  __syncthreads();
+  // overlapping taps between an edge of the tile's own cells and the next
+  // three edges of its line (every such pair has its first edge in exactly
+  // one tile): the two-pass kernels then redo the whole frame
+  if (on) {
+    bool o = false;
+    for (int i = t; i < 2 * (kFT / 4) * (kFT / 4); i += kFThreads) {
+      const bool vert = i < (kFT / 4) * (kFT / 4);
+      const int j = vert ? i : i - (kFT / 4) * (kFT / 4);
+      const int ar = kFH / 4 + j / (kFT / 4), ac = kFH / 4 + j % (kFT / 4);  // line, and position along it
+      const uint8_t* w = vert ? vw : hw;
+      const int cell = vert ? ar * kFC + ac : ac * kFC + ar;
+      const int wd = w[cell];
+      if (!wd) continue;
+      const int gi = vert ? c0 + ac : r0 + ac;
+      for (int k = 1; k <= 3; k++) {
+        const int wk = w[vert ? cell + k : cell + k * kFC];
+        if (wk && taps_overlap(gi, wd, gi + k, wk)) o = true;
+      }
+    }
+    if (o) bad = 1;
+  }
+  __syncthreads();
+  if (bad) {
+    if (t == 0) atomicExch(overlap, 1);
+    return;
+  }
+  // vertical edges, width class by class (four rows per edge; the rows of
+  // cell rows 1 .. kFC-2 cover every row the horizontal pass reads)
+  if (on) {
+    int base = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int n = 4 * nv[k];
+      for (int i = (t - base) & (kFThreads - 1); i < n; i += kFThreads) {
+        const int e = vlist[k][i >> 2];
+        uint16_t* row = &S[(4 * (e >> 8) + (i & 3)) * kFP + 4 * (e & 255)];
+        switch (k) {  // 8-bit samples: the entry accepts no other depth
+          case 0: lf_row<4>(row, a.L, 8); break;
+          case 1: lf_row<6>(row, a.L, 8); break;
+          case 2: lf_row<8>(row, a.L, 8); break;
+          default: lf_row<16>(row, a.L, 8); break;
+        }
+      }
+      base = (base + n) & (kFThreads - 1);
+    }
+  }
+  __syncthreads();
+  // horizontal edges on the tile's columns, width class by class
+  if (on) {
+    int base = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int n = 4 * nh[k];
+      for (int i = (t - base) & (kFThreads - 1); i < n; i += kFThreads) {
+        const int e = hlist[k][i >> 2];
+        uint16_t* cp = &S[(4 * (e >> 8)) * kFP + 4 * (e & 255) + (i & 3)];
+        switch (k) {
+          case 0: lf_col<4>(cp, kFP, a.L, 8); break;
+          case 1: lf_col<6>(cp, kFP, a.L, 8); break;
+          case 2: lf_col<8>(cp, kFP, a.L, 8); break;
+          default: lf_col<16>(cp, kFP, a.L, 8); break;
+        }
+      }
+      base = (base + n) & (kFThreads - 1);
+    }
+  }
+  __syncthreads();
+  for (int i = t; i < kFT * (kFT / 4); i += kFThreads) {
+    const int r = i / (kFT / 4), c4 = (i - r * (kFT / 4)) * 4;
+    const int gy = y0 + r, gx = x0 + c4;
+    if (gy < a.h && gx < a.w) {
+      const uint32_t* sp = reinterpret_cast<const uint32_t*>(&S[(kFH + r) * kFP + kFH + c4]);
+      *reinterpret_cast<uint2*>(P.px + (size_t)gy * a.w + gx) = make_uint2(sp[0], sp[1]);
+    }
+  }
+}
+
+// With overlapping taps: the unfiltered planes into the filtered ones (where
+// they are separate buffers), for the two-pass kernels to filter in place.
+__global__ void __launch_bounds__(256) lf_copy_frame_kernel(FrameArgs fa, const int* __restrict__ overlap) {
+  if (!*overlap) return;
+  const FramePlane& P = fa.p[blockIdx.z];
+  if (!P.px || P.in == P.px) return;
+  const long n = (long)P.a.w * P.a.h / 2;  // sample pairs
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(P.in);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(P.px);
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
+// The two-pass kernels over all planes of the frame, run only when the
+// classify pass found overlapping taps.
+__global__ void __launch_bounds__(128) lf_vert_frame_kernel(FrameArgs fa, const int* __restrict__ overlap) {
+  if (!*overlap) return;
+  const FramePlane& P = fa.p[blockIdx.z];
+  if (!P.on) return;
+  const PlaneArgs& a = P.a;
+  const long n = (long)a.w4 * a.h4;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int r4 = (int)(i / a.w4), c4 = (int)(i - (long)r4 * a.w4);
+    const EdgeLine e{P.bw4, P.vedge4, (long)r4 * a.nc4, 1, a.w4, a.w, a.luma != 0};
+    bool run;
+    int wd = own_edge(e, c4, &run);
+    int cur = c4;
+    while (wd) {
+      vert_cell(P.px, a, r4, cur, wd);
+      if (!run) break;
+      cur = run_next(e, cur, &wd);
+      if (!cur) break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128) lf_horz_frame_kernel(FrameArgs fa, const int* __restrict__ overlap) {
+  if (!*overlap) return;
+  const FramePlane& P = fa.p[blockIdx.z];
+  if (!P.on) return;
+  const PlaneArgs& a = P.a;
+  const long n = (long)a.w4 * a.h4;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int r4 = (int)(i / a.w4), c4 = (int)(i - (long)r4 * a.w4);
+    const EdgeLine e{P.bh4, P.hedge4, (long)c4, a.nc4, a.h4, a.h, a.luma != 0};
+    bool run;
+    int wd = own_edge(e, r4, &run);
+    int cur = r4;
+    while (wd) {
+      horz_cell(P.px, a, cur, c4, wd);
+      if (!run) break;
+      cur = run_next(e, cur, &wd);
+      if (!cur) break;
+    }
+  }
+}
+
 int check_plane(int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, int32_t nc4, int32_t level, int32_t sharp,
                 int32_t bd) {
   if (w <= 0 || h <= 0 || (w & 3) || (h & 3)) return MT_ERR_INVALID_INPUT;
@@ -401,6 +675,147 @@ int check_frame(const mt_deblock_frame_params* p) {
   return MT_OK;
 }
 
+// Scratch of the frame entries: the chroma block maps, the overlap flag and
+// the unfiltered planes of an in-place call.
+struct FrameLayout {
+  size_t cbw4, cbh4, flag, snap[3], total;
+};
+
+FrameLayout frame_layout(const mt_deblock_frame_params& p) {
+  auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+  const size_t nch = (size_t)((p.w8 >> p.sub_x) / 4) * ((p.h8 >> p.sub_y) / 4);
+  FrameLayout L;
+  size_t o = 0;
+  L.cbw4 = o;
+  o += up(nch);
+  L.cbh4 = o;
+  o += up(nch);
+  L.flag = o;
+  o += 256;
+  const size_t ny = (size_t)p.w8 * p.h8 * 2, nc = (size_t)(p.w8 >> p.sub_x) * (p.h8 >> p.sub_y) * 2;
+  for (int pl = 0; pl < 3; pl++) {  // the unfiltered planes of an in-place call
+    L.snap[pl] = o;
+    o += up(pl ? (p.mono ? 0 : nc) : ny);
+  }
+  L.total = o;
+  return L;
+}
+
+}  // namespace
+
+namespace mth {
+// Kernels the calling thread's last mt_deblock_frame_device launched.
+thread_local int deblock_last_launches = 0;
+}  // namespace mth
+
+namespace {
+
+// The frame deblocking from the unfiltered planes in_* (null: the filtered
+// planes themselves, snapshotted into the scratch first) into the filtered
+// planes d_*.
+int deblock_frame(const uint16_t* in_y, const uint16_t* in_u, const uint16_t* in_v, uint16_t* d_y, uint16_t* d_u,
+                  uint16_t* d_v, const uint8_t* d_blk4, const uint8_t* d_blk4h, const uint8_t* d_blk4v,
+                  const uint8_t* d_blk4t, const uint8_t* d_pblk4, const uint8_t* d_pblk4h,
+                  const mt_deblock_frame_params* prm, int32_t lvl_y, int32_t lvl_u, int32_t lvl_v, void* d_scratch,
+                  void* stream) {
+  mth::deblock_last_launches = 0;
+  int rc = check_frame(prm);
+  if (rc != MT_OK) return rc;
+  if (lvl_y < 0 || lvl_y > 63 || lvl_u < 0 || lvl_u > 63 || lvl_v < 0 || lvl_v > 63) return MT_ERR_INVALID_INPUT;
+  const bool in_place = in_y == nullptr;
+  if (in_place && lvl_y == 0) return MT_OK;  // chroma is filtered only with luma
+  const bool want_uv = !prm->mono && lvl_y > 0 && (lvl_u > 0 || lvl_v > 0);  // chroma is filtered
+  if (!d_y || !d_scratch) return MT_ERR_INVALID_INPUT;
+  if (want_uv && (!d_u || !d_v || (!in_place && (!in_u || !in_v)))) return MT_ERR_INVALID_INPUT;
+  // chroma planes to carry (filtered, or copied through by an out-of-place call)
+  const bool planes_uv = !prm->mono && d_u && d_v && (in_place || (in_u && in_v));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int cw8 = prm->w8 >> prm->sub_x, ch8 = prm->h8 >> prm->sub_y;
+  const size_t ny = (size_t)prm->w8 * prm->h8 * 2, nc = (size_t)cw8 * ch8 * 2;
+  if (lvl_y == 0) {  // the planes as they are
+    if (cudaMemcpyAsync(d_y, in_y, ny, cudaMemcpyDeviceToDevice, st) != cudaSuccess) return MT_ERR_DEVICE;
+    if (planes_uv && (cudaMemcpyAsync(d_u, in_u, nc, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+                      cudaMemcpyAsync(d_v, in_v, nc, cudaMemcpyDeviceToDevice, st) != cudaSuccess))
+      return MT_ERR_DEVICE;
+    return MT_OK;
+  }
+  const int sharp = 7;
+  const int nc4 = prm->w8 / 4;
+  const bool chroma = want_uv;
+  if (!d_blk4 || !d_blk4h) return MT_ERR_INVALID_INPUT;
+  if (chroma && (!d_pblk4 || !d_pblk4h)) return MT_ERR_INVALID_INPUT;
+  const FrameLayout L = frame_layout(*prm);
+  uint8_t* s = static_cast<uint8_t*>(d_scratch);
+  FrameArgs fa = {};
+  int launches = 0;
+  auto plane = [&](int k, const uint16_t* in, uint16_t* px, int w, int h, int vis_w, int vis_h, const uint8_t* bw4,
+                   const uint8_t* bh4, const uint8_t* ve, const uint8_t* he, int pnc4, int level, bool luma) -> int {
+    const int r = check_plane(w, h, vis_w, vis_h, pnc4, level, sharp, prm->bd);
+    if (r != MT_OK) return r;
+    if ((reinterpret_cast<uintptr_t>(px) | reinterpret_cast<uintptr_t>(in)) & 7)
+      return MT_ERR_INVALID_INPUT;  // paired and 8-byte row accesses
+    FramePlane& P = fa.p[k];
+    P.in = in;
+    P.px = px;
+    P.bw4 = bw4;
+    P.bh4 = bh4;
+    P.vedge4 = ve;
+    P.hedge4 = he;
+    P.nr4 = h / 4;
+    P.a.w = w;
+    P.a.h = h;
+    P.a.w4 = (vis_w + 3) / 4;
+    P.a.h4 = (vis_h + 3) / 4;
+    P.a.nc4 = pnc4;
+    P.a.bd = prm->bd;
+    P.a.luma = luma;
+    P.a.L = lf_limits(level, sharp);
+    P.on = level > 0;
+    if (in_place && P.on) {  // the unfiltered plane, read by the fused kernel
+      uint16_t* snap = reinterpret_cast<uint16_t*>(s + L.snap[k]);
+      if (cudaMemcpyAsync(snap, px, (size_t)w * h * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return MT_ERR_DEVICE;
+      P.in = snap;
+    }
+    return MT_OK;
+  };
+  if ((rc = plane(0, in_y, d_y, prm->w8, prm->h8, prm->disp_w, prm->disp_h, d_blk4, d_blk4h, d_blk4v, d_blk4t, nc4,
+                  lvl_y, true)) != MT_OK)
+    return rc;
+  if (planes_uv) {
+    const int cnc4 = cw8 / 4, cnr4 = ch8 / 4;
+    uint8_t* cbw4 = s + L.cbw4;
+    uint8_t* cbh4 = s + L.cbh4;
+    if (chroma) {
+      const size_t n = (size_t)cnc4 * cnr4;
+      chroma_geom_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pblk4, d_pblk4h, nc4, cnc4, cnr4, prm->sub_x,
+                                                                      prm->sub_y, cbw4, cbh4);
+      ++launches;
+    }
+    const int vis_w = (prm->disp_w + (1 << prm->sub_x) - 1) >> prm->sub_x;
+    const int vis_h = (prm->disp_h + (1 << prm->sub_y) - 1) >> prm->sub_y;
+    if ((rc = plane(1, in_place ? d_u : in_u, d_u, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4,
+                    chroma ? lvl_u : 0, false)) != MT_OK ||
+        (rc = plane(2, in_place ? d_v : in_v, d_v, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4,
+                    chroma ? lvl_v : 0, false)) != MT_OK)
+      return rc;
+  }
+  int* flag = reinterpret_cast<int*>(s + L.flag);
+  if (cudaMemsetAsync(flag, 0, sizeof(int), st) != cudaSuccess) return MT_ERR_DEVICE;
+  const long cells = (long)fa.p[0].a.w4 * fa.p[0].a.h4;  // the largest plane
+  lf_fused_kernel<<<dim3((prm->w8 + kFT - 1) / kFT, (prm->h8 + kFT - 1) / kFT, 3), kFThreads, 0, st>>>(fa, flag);
+  // the fallback, gated on the flag (small grids: they return at once without it)
+  const int gs = (int)std::min<long>((cells + 255) / 256, 296);
+  lf_copy_frame_kernel<<<dim3(gs, 1, 3), 256, 0, st>>>(fa, flag);
+  launches += 2;
+  const int g2 = (int)std::min<long>((cells + 127) / 128, 592);
+  lf_vert_frame_kernel<<<dim3(g2, 1, 3), 128, 0, st>>>(fa, flag);
+  lf_horz_frame_kernel<<<dim3(g2, 1, 3), 128, 0, st>>>(fa, flag);
+  launches += 2;
+  mth::deblock_last_launches = launches;
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
 }  // namespace
 
 extern "C" {
@@ -423,8 +838,7 @@ int mt_loop_filter_levels(int32_t base_q_idx, int32_t sub_x, int32_t sub_y, int3
 
 size_t mt_deblock_frame_scratch_bytes(const mt_deblock_frame_params* prm) {
   if (check_frame(prm) != MT_OK) return 0;
-  const size_t n = (size_t)((prm->w8 >> prm->sub_x) / 4) * ((prm->h8 >> prm->sub_y) / 4);
-  return 2 * ((n + 255) & ~(size_t)255);
+  return frame_layout(*prm).total;
 }
 
 int mt_deblock_plane_device(uint16_t* d_px, int32_t w, int32_t h, int32_t vis_w, int32_t vis_h, const uint8_t* d_bw4,
@@ -455,38 +869,18 @@ int mt_deblock_frame_device(uint16_t* d_y, uint16_t* d_u, uint16_t* d_v, const u
                             const uint8_t* d_blk4h, const uint8_t* d_blk4v, const uint8_t* d_blk4t,
                             const uint8_t* d_pblk4, const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm,
                             int32_t lvl_y, int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream) {
-  int rc = check_frame(prm);
-  if (rc != MT_OK) return rc;
-  if (lvl_y < 0 || lvl_y > 63 || lvl_u < 0 || lvl_u > 63 || lvl_v < 0 || lvl_v > 63) return MT_ERR_INVALID_INPUT;
-  const int sharp = 7;
-  const int nc4 = prm->w8 / 4;
-  if (lvl_y > 0) {
-    rc = mt_deblock_plane_device(d_y, prm->w8, prm->h8, prm->disp_w, prm->disp_h, d_blk4, d_blk4h, d_blk4v, d_blk4t,
-                                 nc4, lvl_y, sharp, 1, prm->bd, stream);
-    if (rc != MT_OK) return rc;
-  }
-  if (prm->mono || lvl_y <= 0 || (lvl_u <= 0 && lvl_v <= 0)) return MT_OK;
-  if (!d_pblk4 || !d_pblk4h || !d_scratch || !d_u || !d_v) return MT_ERR_INVALID_INPUT;
-  const int cw8 = prm->w8 >> prm->sub_x, ch8 = prm->h8 >> prm->sub_y;
-  const int cnc4 = cw8 / 4, cnr4 = ch8 / 4;
-  const size_t n = (size_t)cnc4 * cnr4;
-  uint8_t* cbw4 = static_cast<uint8_t*>(d_scratch);
-  uint8_t* cbh4 = cbw4 + ((n + 255) & ~(size_t)255);
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  chroma_geom_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_pblk4, d_pblk4h, nc4, cnc4, cnr4, prm->sub_x,
-                                                                  prm->sub_y, cbw4, cbh4);
-  if (cudaGetLastError() != cudaSuccess) return MT_ERR_DEVICE;
-  const int vis_w = (prm->disp_w + (1 << prm->sub_x) - 1) >> prm->sub_x;
-  const int vis_h = (prm->disp_h + (1 << prm->sub_y) - 1) >> prm->sub_y;
-  if (lvl_u > 0) {
-    rc = mt_deblock_plane_device(d_u, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4, lvl_u, sharp, 0,
-                                 prm->bd, stream);
-    if (rc != MT_OK) return rc;
-  }
-  if (lvl_v > 0)
-    rc = mt_deblock_plane_device(d_v, cw8, ch8, vis_w, vis_h, cbw4, cbh4, nullptr, nullptr, cnc4, lvl_v, sharp, 0,
-                                 prm->bd, stream);
-  return rc;
+  return deblock_frame(nullptr, nullptr, nullptr, d_y, d_u, d_v, d_blk4, d_blk4h, d_blk4v, d_blk4t, d_pblk4, d_pblk4h,
+                       prm, lvl_y, lvl_u, lvl_v, d_scratch, stream);
+}
+
+int mt_deblock_frame_device_to(const uint16_t* d_in_y, const uint16_t* d_in_u, const uint16_t* d_in_v, uint16_t* d_y,
+                               uint16_t* d_u, uint16_t* d_v, const uint8_t* d_blk4, const uint8_t* d_blk4h,
+                               const uint8_t* d_blk4v, const uint8_t* d_blk4t, const uint8_t* d_pblk4,
+                               const uint8_t* d_pblk4h, const mt_deblock_frame_params* prm, int32_t lvl_y,
+                               int32_t lvl_u, int32_t lvl_v, void* d_scratch, void* stream) {
+  if (!prm || !d_in_y) return MT_ERR_INVALID_INPUT;
+  return deblock_frame(d_in_y, d_in_u, d_in_v, d_y, d_u, d_v, d_blk4, d_blk4h, d_blk4v, d_blk4t, d_pblk4, d_pblk4h,
+                       prm, lvl_y, lvl_u, lvl_v, d_scratch, stream);
 }
 
 int mt_deblock_frame(uint16_t* y, uint16_t* u, uint16_t* v, const uint8_t* blk4, const uint8_t* blk4h,

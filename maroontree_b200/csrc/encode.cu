@@ -730,6 +730,7 @@ struct Job {
 namespace mth {
 void cdef_frame_transfer_bytes(const mt_cdef_params* p, size_t* d2h, size_t* h2d);
 extern thread_local int cdef_last_launches;
+extern thread_local int deblock_last_launches;
 }  // namespace mth
 
 extern "C" {
@@ -1152,23 +1153,16 @@ int job_finish(Job& j, Buffers& buf, int i) {
   if (cudaMemcpyAsync(d_maps, maps.data(), maps.size(), cudaMemcpyHostToDevice, st) != cudaSuccess)
     return MT_ERR_DEVICE;
   cs.h2d(maps.size());
-  // the recon planes are kept: the filters run on a copy
+  // the recon planes are kept: the filters write planes of their own
   uint16_t* d_flt = buf.get<uint16_t>(i, kFiltered, (ny + 2 * nc) * 2);
   if (!d_flt) return MT_ERR_DEVICE;
   uint16_t* flt[3] = {d_flt, d_flt + ny, d_flt + ny + nc};
-  if (cudaMemcpyAsync(flt[0], rec[0], (ny + 2 * nc) * 2, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-    return MT_ERR_DEVICE;
   const uint8_t* m0 = d_maps;
-  if ((rc = mt_deblock_frame_device(flt[0], flt[1], flt[2], m0, m0 + n4, m0 + 2 * (size_t)n4, m0 + 3 * (size_t)n4,
-                                    m0 + 4 * (size_t)n4, m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db, st)) != MT_OK)
+  if ((rc = mt_deblock_frame_device_to(rec[0], rec[1], rec[2], flt[0], flt[1], flt[2], m0, m0 + n4,
+                                       m0 + 2 * (size_t)n4, m0 + 3 * (size_t)n4, m0 + 4 * (size_t)n4,
+                                       m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db, st)) != MT_OK)
     return rc;
-  {  // the deblocking launches: vertical and horizontal edges per filtered plane, the chroma geometry
-    const int vw4 = ((int)width + 3) / 4, vh4 = ((int)height + 3) / 4;
-    const int cw4 = (((int)width + sx) >> sx) / 4 + ((((int)width + sx) >> sx) % 4 != 0);
-    const int ch4 = (((int)height + sx) >> sx) / 4 + ((((int)height + sx) >> sx) % 4 != 0);
-    if (ly > 0) cs.launches((vw4 > 1) + (vh4 > 1));
-    if (ly > 0 && luv > 0) cs.launches(1 + 2 * ((cw4 > 1) + (ch4 > 1)));
-  }
+  cs.launches(mth::deblock_last_launches);
   // splice the coefficient tokens into the superblock streams (the token copy
   // has completed once the stream reaches the filters' first sync)
   if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;

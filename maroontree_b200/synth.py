@@ -362,15 +362,16 @@ def blocky_plane(w, h, block_id, seed, maxv=255):
     return full.astype(np.uint16)
 
 
-def cdef_inputs(disp_w, disp_h, sub_x, sub_y, mono, seed, skip_frac=0.3):
+def cdef_inputs(disp_w, disp_h, sub_x, sub_y, mono, seed, skip_frac=0.3, rgb=None):
     """Source and reconstruction planes plus a per-8x8 skip map for the frame
-    CDEF: luma from the synthetic RGB image, chroma a contrast-reduced copy of
-    it; the reconstruction adds seeded error whose amplitude varies per 64x64
-    unit (0 .. 12, with or without block-edge ringing), so that CDEF helps some units and
-    not others.  Planes are edge-padded to multiples of 8."""
+    CDEF: luma from the synthetic RGB image (or the given disp_h x disp_w
+    image), chroma a contrast-reduced copy of it; the reconstruction adds
+    seeded error whose amplitude varies per 64x64 unit (0 .. 12, with or
+    without block-edge ringing), so that CDEF helps some units and not others.
+    Planes are edge-padded to multiples of 8."""
     w8, h8 = (disp_w + 7) & ~7, (disp_h + 7) & ~7
     rng = np.random.default_rng(seed)
-    y = rgb_to_luma(generate_rgb(disp_w, disp_h, seed)).astype(np.int32)
+    y = rgb_to_luma(generate_rgb(disp_w, disp_h, seed) if rgb is None else rgb).astype(np.int32)
     y = np.pad(y, ((0, h8 - disp_h), (0, w8 - disp_w)), mode="edge")
     planes = [y]
     if not mono:

@@ -219,3 +219,87 @@ def test_deblock_frame_matches_oracle(mt_lib, oracle_lib, cuda, disp_w, disp_h, 
     for a, b, c in zip(got, want, planes):
         assert np.array_equal(a, b)
         assert not np.array_equal(b, c)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mono", [True, False])
+def test_deblock_frame_overlapping_taps_match_oracle(mt_lib, oracle_lib, cuda, mono):
+    """The frame entry on the reference's mixed-geometry maps (edges whose
+    taps overlap): the classify pass sends the frame to the two-pass kernels,
+    which keep each run in the reference's order."""
+    W, H, bw, bh, ve, he, img = _mixed_geometry()
+    tx = (bw, bh, ve, he)
+    pred = (np.full_like(bw, 2), np.full_like(bh, 2))
+    planes = [img]
+    if not mono:
+        planes += [img[::2, ::2].copy(), (255 - img[::2, ::2]).astype(np.uint16)]
+    for q in (60, 200):
+        ly, luv, _ = mt_lib.loop_filter_levels(q, 1, 1)
+        want = oracle_lib.deblock_frame(planes, W, H, 1, 1, tx, pred, ly, luv, luv, mono)
+        got = mt_lib.deblock_frame(planes, W, H, 1, 1, tx, pred, ly, luv, luv, mono)
+        for a, b, c in zip(got, want, planes):
+            assert np.array_equal(a, b)
+        assert not np.array_equal(want[0], planes[0])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("disp_w,disp_h,sx,sy", [(1031, 517, 0, 0), (4096, 256, 1, 1)])
+def test_deblock_frame_tiles_match_oracle(mt_lib, oracle_lib, cuda, disp_w, disp_h, sx, sy):
+    """The fused tile kernel across many 64x64 tiles and ragged frame edges,
+    against the oracle's frame-wide two-pass deblocking."""
+    planes, tx, pred = _frame_inputs(disp_w, disp_h, sx, sy, False, disp_w + disp_h)
+    ly, luv, _ = mt_lib.loop_filter_levels(150, sx, sy)
+    want = oracle_lib.deblock_frame(planes, disp_w, disp_h, sx, sy, tx, pred, ly, luv, luv, False)
+    got = mt_lib.deblock_frame(planes, disp_w, disp_h, sx, sy, tx, pred, ly, luv, luv, False)
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+
+
+def _device_deblock(mt_lib, planes, disp_w, disp_h, sx, sy, tx, pred, lv, to):
+    """mt_deblock_frame_device (in place) or mt_deblock_frame_device_to (from
+    separate input planes, which must come back unchanged) on the GPU."""
+    import torch
+    from maroontree_b200 import abi
+
+    lib = mt_lib.load()
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a).astype(np.int16)).cuda()
+    src = [dev(p) for p in planes]
+    out = [torch.zeros_like(p) for p in src] if to else [p.clone() for p in src]
+    maps = [torch.from_numpy(np.ascontiguousarray(m, np.uint8)).cuda() for m in list(tx) + list(pred)]
+    g = abi.DeblockFrameParams()
+    g.w8, g.h8 = planes[0].shape[1], planes[0].shape[0]
+    g.disp_w, g.disp_h, g.sub_x, g.sub_y, g.mono, g.bd = disp_w, disp_h, sx, sy, 0, 8
+    scr = torch.empty(lib.mt_deblock_frame_scratch_bytes(C.byref(g)), dtype=torch.uint8, device="cuda")
+    args = [m.data_ptr() for m in maps] + [C.byref(g), *lv, scr.data_ptr(), None]
+    if to:
+        rc = lib.mt_deblock_frame_device_to(*[p.data_ptr() for p in src], *[p.data_ptr() for p in out], *args)
+    else:
+        rc = lib.mt_deblock_frame_device(*[p.data_ptr() for p in out], *args)
+    torch.cuda.synchronize()
+    assert rc == 0
+    if to:
+        for a, b in zip(src, planes):
+            assert np.array_equal(a.cpu().numpy().view(np.uint16), b)
+    return [p.cpu().numpy().view(np.uint16) for p in out]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mixed", [False, True])
+def test_deblock_frame_device_to_equals_in_place(mt_lib, oracle_lib, cuda, mixed):
+    """The out-of-place entry gives the in-place entry's planes and leaves its
+    input planes as they were, on the fused path and on the two-pass path of
+    maps with overlapping taps."""
+    if mixed:
+        W, H, bw, bh, ve, he, img = _mixed_geometry()
+        planes, tx, pred = [img, img[::2, ::2].copy(), img[::2, ::2].copy()], (bw, bh, ve, he), (bw, bh)
+        dw, dh = W, H
+    else:
+        dw, dh = 515, 333
+        planes, tx, pred = _frame_inputs(dw, dh, 1, 1, False, 5)
+    lv = mt_lib.loop_filter_levels(120, 1, 1)[:2]
+    lv = (lv[0], lv[1], lv[1])
+    a = _device_deblock(mt_lib, planes, dw, dh, 1, 1, tx, pred, lv, to=False)
+    b = _device_deblock(mt_lib, planes, dw, dh, 1, 1, tx, pred, lv, to=True)
+    want = oracle_lib.deblock_frame(planes, dw, dh, 1, 1, tx, pred, *lv, False)
+    for x, y, z in zip(a, b, want):
+        assert np.array_equal(x, y) and np.array_equal(x, z)
