@@ -612,6 +612,25 @@ int mt_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_param
 int mt_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+/* The 32x32 leaf (pick_luma32, src/coder/block32.rs:728-836): the mode loop's
+ * candidates as mt_leaf8_luma_device at 32x32 -- the prediction at 32x32, the
+ * TX_32X32 DCT_DCT (the only intra type of that size; the reference's 64-bit
+ * rounded forward transform, src/dct.rs:589-736) with the 32x32 QM,
+ * trellis_optimize_ctx of class TX_32X32, the dav1d inverse with the TX_32X32
+ * dequantisation (src/idct.rs:2130-2320), sse_recon, luma_bits in txb_skip
+ * context 0 with no tx-type symbol, and
+ * cost = rd_cost_i64(sse, rd_lambda, bits + syntax_bits).  Jobs address 32x32
+ * blocks; the costs / qm row are the TX_32X32 slice and 32x32 row (1024
+ * weights); skip_bits[0] the TX_32X32 class's context-0 pair; d_cf / d_rec
+ * are n x 1024. */
+int mt_leaf32_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                          uint16_t* d_rec, void* stream);
+/* Host-buffer form of mt_leaf32_luma_device. */
+int mt_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,

@@ -376,6 +376,23 @@ def leaf16(src, recon, prm, quant, qmrow, costs, jobs, refine=False, want_cf=Fal
     return res, cf, rec
 
 
+def leaf32(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
+    """The 32x32 leaf's mode-loop candidates (``mt_leaf32``); qmrow / costs are the
+    32x32 row and the TX_32X32 slice.  Returns (results, cf n x 1024 or None,
+    rec n x 32 x 32 or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.LEAF8_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.LEAF8_RESULT_DTYPE)
+    cf = np.zeros((n, 1024), np.int32) if want_cf else None
+    rec = np.zeros((n, 32, 32), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_leaf32(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs), ptr(jobs),
+                            n, ptr(res), ptr(cf), ptr(rec)), "mt_leaf32")
+    return res, cf, rec
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

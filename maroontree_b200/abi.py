@@ -403,6 +403,10 @@ def _bind(lib):
                                                  C.c_int32, _P, _P, _P, _P]),
         "mt_leaf16": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                 C.c_int32, C.c_int32, _P, _P, _P]),
+        "mt_leaf32_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                            C.c_int32, _P, _P, _P, _P]),
+        "mt_leaf32": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
+                                C.c_int32, _P, _P, _P]),
         "mt_leaf8": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                C.c_int32, C.c_int32, _P, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
@@ -459,7 +463,7 @@ EXPORTED_SYMBOLS = (
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
     "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
-    "mt_leaf16",
+    "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32",
 )
 
 

@@ -207,7 +207,8 @@ def main():
         for k in range(0, len(nums), 24):
             lines.append("  " + ",".join(str(v) for v in nums[k : k + 24]) + ",")
         lines.append("};")
-        if "QLOOKUP" in cname or cname in ("MT_SCAN_16X16", "MT_ADST16_FWD_Q12", "MT_INTRA_FILTER_TAPS"):  # initialiser lists for device copies
+        if "QLOOKUP" in cname or cname in ("MT_SCAN_16X16", "MT_SCAN_32X32", "MT_ADST16_FWD_Q12",
+                                           "MT_INTRA_FILTER_TAPS"):  # initialiser lists for device copies
             lines.append(f"#define {cname}_LIST " + ",".join(str(v) for v in nums))
         lines.append("")
     open(out, "w").write("\n".join(lines))

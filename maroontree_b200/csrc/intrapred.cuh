@@ -17,10 +17,12 @@ __constant__ int16_t kDrDeriv[44] = {0,  1023, 0,  547, 372, 0,  0,  273, 215, 0
 __constant__ int16_t kSmW8[8] = {255, 197, 146, 105, 73, 50, 37, 32};
 __constant__ int16_t kSmW4[4] = {255, 149, 85, 64};
 __constant__ int16_t kSmW16[16] = {255, 225, 196, 170, 145, 123, 102, 84, 68, 54, 43, 33, 26, 20, 17, 16};
+__constant__ int16_t kSmW32[32] = {255, 240, 225, 210, 196, 182, 169, 157, 145, 133, 122, 111, 101, 92, 83, 74,
+                                   66,  59,  52,  45,  39,  34,  29,  25,  21,  17,  14,  12,  10,  9,  8,  8};
 
 template <int N>
 __device__ __forceinline__ int32_t sm_weight(int i) {
-  return N == 4 ? kSmW4[i] : (N == 8 ? kSmW8[i] : kSmW16[i]);
+  return N == 4 ? kSmW4[i] : (N == 8 ? kSmW8[i] : (N == 16 ? kSmW16[i] : kSmW32[i]));
 }
 
 constexpr int kEdgeOrigin = 2;
@@ -108,7 +110,7 @@ __device__ __forceinline__ int32_t dc_pred_sq(const uint16_t* __restrict__ rec, 
   return dc_pred_sq_at(PlaneRead{rec, stride}, ox, oy, n, log2n, bd);
 }
 
-// Prediction of an N x N block (N = 4, 8 or 16) into out[N*N] (row-major),
+// Prediction of an N x N block (N = 4, 8, 16 or 32) into out[N*N] (row-major),
 // neighbours read through `rd`.  `scratch` holds 3 * edge_cap<N>() words: the
 // above and left edges and a filter temporary.  Only rows [y0, y1) of out are
 // written (the edges are always built whole), so several threads can share
@@ -117,10 +119,10 @@ template <int N, typename R, typename O>
 __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int mode, int delta, bool have_tr,
                               bool have_bl, bool ft, int bd, O* __restrict__ out, int32_t* __restrict__ scratch,
                               int y0 = 0, int y1 = N) {
-  static_assert(N == 4 || N == 8 || N == 16, "square sizes 4, 8 and 16");
+  static_assert(N == 4 || N == 8 || N == 16 || N == 32, "square sizes 4, 8, 16 and 32");
   constexpr int bw = N, bh = N, edge_len = 2 * N, cap = edge_cap<N>();
   if (mode == MT_DC_PRED) {
-    const int32_t d = dc_pred_sq_at(rd, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : 4), bd);
+    const int32_t d = dc_pred_sq_at(rd, ox, oy, N, N == 4 ? 2 : (N == 8 ? 3 : (N == 16 ? 4 : 5)), bd);
     for (int i = y0 * N; i < y1 * N; i++) out[i] = (O)(d);
     return;
   }
@@ -168,7 +170,7 @@ __device__ void predict_sq_at(const R& rd, int fw, int fh, int ox, int oy, int m
     int up_a = 0, up_l = 0;
     if (angle != 90 && angle != 180) {
       // The corner filter (src/intrapred.rs:1014-1019) for edge_len >= 24,
-      // i.e. 16x16 here, before the edges are smoothed.
+      // i.e. 16x16 and 32x32 here, before the edges are smoothed.
       if (edge_len >= 24 && angle > 90 && angle < 180) {
         const int32_t f = (5 * L[kEdgeOrigin] + 6 * A[kEdgeOrigin - 1] + 5 * A[kEdgeOrigin] + 8) >> 4;
         A[kEdgeOrigin - 1] = f;

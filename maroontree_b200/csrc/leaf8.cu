@@ -9,8 +9,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/maroontree_b200.h"
 #include "leaf8.cuh"
+#include "txfm32.cuh"
 #include "wsse.cuh"
 
 namespace mth {
@@ -31,12 +34,17 @@ struct LeafArgs {
 };
 
 // Per-thread working set of one N x N job.  u: the prediction edges, then the
-// targets [0, N*N) and the transform temporary [N*N, 2*N*N).
+// targets [0, N*N) and the transform temporary [N*N, 2*N*N).  Levels are
+// 32-bit at 32x32 (a full-scale DC at the smallest steps passes 16 bits);
+// 32x32 has one transform type, so one slot.
 template <int N>
 struct LeafWork {
+  using Coef = std::conditional_t<N == 32, int32_t, int16_t>;
+  static constexpr int kSlots = N == 32 ? 1 : 2;
   int32_t u[2 * N * N];
   int16_t pred[N * N], resid[N * N];
-  int16_t cfs[2][N * N], rrs[2][N * N];  // levels / inverse of the candidate and of the winner
+  Coef cfs[kSlots][N * N];                // levels of the candidate and of the winner
+  int16_t rrs[kSlots][N * N];             // their inverses
   TrellisCtxScratchW<N> tr;
   uint8_t lv[N == 8 ? 160 : (N + 2) * N];  // rate walks' level maps
 };
@@ -48,7 +56,10 @@ __device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate)
 // N = 8: pick_block8's candidates (REFINE = false) and winner refinement
 // (REFINE = true); N = 16: pick_luma16's mode-loop candidates
 // (src/coder/partition_search.rs:4802-4880) and winner refinement (:5252-5474:
-// ADST_ADST, ADST_DCT, DCT_ADST, IDTX with the 8x8 leaf's gates).
+// ADST_ADST, ADST_DCT, DCT_ADST, IDTX with the 8x8 leaf's gates); N = 32:
+// pick_luma32's mode-loop candidates (src/coder/block32.rs:776-836: TX_32X32
+// DCT_DCT, the only intra type of that size, trellis_optimize_ctx of class 3,
+// no tx-type symbol in the rate).
 template <int N, bool REFINE>
 __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
@@ -56,8 +67,8 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const mt_leaf8_job* __restrict__ jobs, int n, mt_leaf8_result* __restrict__ res, int32_t* __restrict__ cf_out,
     uint16_t* __restrict__ rec_out) {
   __shared__ mt_coef_costs sT;
-  static_assert(N == 8 || N == 16, "8x8 and 16x16 leaves");
-  constexpr int NN = N * N, L = N == 8 ? 3 : 4;
+  static_assert(N == 8 || N == 16 || (N == 32 && !REFINE), "8x8 and 16x16 leaves, the 32x32 mode loop");
+  constexpr int NN = N * N, L = log2w<N>();
   __shared__ uint8_t sQm[NN];
   __shared__ float sQs[NN];
   {
@@ -128,16 +139,18 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
   for (int k = 0; k < ntypes; k++) {
     const int t = (int)((kTypeOrder >> (4 * k)) & 15u);
     const int cur = k == 0 ? 0 : 1 - best;
-    int16_t* cf = w.cfs[cur];
+    auto* cf = w.cfs[cur];
     int16_t* rr = w.rrs[cur];
-    if (N == 8) fwd8x8(w.resid, t, q, cf, tf, tmp);
-    else fwd16x16(w.resid, t, q, cf, tf, tmp);
+    if constexpr (N == 8) fwd8x8(w.resid, t, q, cf, tf, tmp);
+    else if constexpr (N == 16) fwd16x16(w.resid, t, q, cf, tf, tmp);
+    else fwd32x32(w.resid, q, cf, tf, tmp);
     if (t == MT_TX_DCT_DCT || t >= MT_TX_ADST_ADST) {
       if (qm) apply_qm(cf, tf, sQs, NN);
       if (a.lambda > 0.0f) trellis_ctx<N>(cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
     }
-    if (N == 8) inv8x8(cf, t, q, qm, rr, tmp);
-    else inv16x16(cf, t, q, qm, rr, tmp);
+    if constexpr (N == 8) inv8x8(cf, t, q, qm, rr, tmp);
+    else if constexpr (N == 16) inv16x16(cf, t, q, qm, rr, tmp);
+    else inv32x32(cf, q, qm, rr, tmp);
     eb.resid = rr;
     const long long asse = sse_recon_block(eb, p.wsse_scale);
     if (k > 0) {
@@ -154,15 +167,16 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
     const float base_rd = k == 0 ? 0.0f : rd_cost_i64(bsse, rd_lam, bbits);
     float abits;
     if (N == 8 && (t == MT_TX_V_DCT || t == MT_TX_H_DCT)) {
-      abits = rate_1d<8>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
+      if constexpr (N == 8) abits = rate_1d<8>(cf, t == MT_TX_V_DCT, T, ds, jb.mode, w.lv);
     } else {
       // unbounded: the DCT, IDTX and, at 16x16, ADST_DCT / DCT_ADST (priced
       // with luma_bits there, partition_search.rs:5396-5404)
       const bool unbounded = k == 0 || t == MT_TX_IDTX || (N == 16 && t != MT_TX_ADST_ADST);
       const float bound = unbounded ? __int_as_float(0x7f800000)
                                     : __fdiv_rn(__fsub_rn(base_rd, (float)asse), rd_lam);
-      // tx-type symbol: the 5-type TX_16X16 intra set drops V_DCT / H_DCT
-      const int sym = N == 16 && t >= MT_TX_ADST_ADST ? t - 2 : t;
+      // tx-type symbol: the 5-type TX_16X16 intra set drops V_DCT / H_DCT;
+      // TX_32X32 codes none
+      const int sym = N == 32 ? -1 : (N == 16 && t >= MT_TX_ADST_ADST ? t - 2 : t);
       abits = rate_bounded<N>(cf, T, 0, ds, jb.mode, sym, p.use_skip_bits != 0, skip1, skip0, bound, w.lv);
     }
     if (k == 0 || rd_cost_i64(asse, rd_lam, abits) < base_rd) {
@@ -181,7 +195,7 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
   r.cost = REFINE ? rd_cost_i64(bsse, rd_lam, bbits) : rd_cost_i64(bsse, rd_lam, __fadd_rn(bbits, jb.syntax_bits));
   r.tx_type = (uint8_t)btx;
   for (int i = 0; i < 7; i++) r.reserved[i] = 0;
-  const int16_t* bcf = w.cfs[best];
+  const auto* bcf = w.cfs[best];
   const int16_t* brr = w.rrs[best];
   if (cf_out) {
     int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * NN);
@@ -277,6 +291,20 @@ int mt_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_param
   return leaf_host<16>(src, recon, prm, quant, qm_row, costs, jobs, n, refine, results, cf_out, rec_out);
 }
 
+int mt_leaf32_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_leaf8_job* d_jobs, int32_t n, mt_leaf8_result* d_results, int32_t* d_cf,
+                          uint16_t* d_rec, void* stream) {
+  return leaf_device<32, false>(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, d_rec,
+                                stream);
+}
+
+int mt_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+              const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_host<32>(src, recon, prm, quant, qm_row, costs, jobs, n, 0, results, cf_out, rec_out);
+}
+
 }  // extern "C"
 
 namespace {
@@ -307,7 +335,7 @@ int leaf_host(const uint16_t* src, const uint16_t* recon, const mt_split16_param
   if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_leaf8_job), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    auto fn = refine ? leaf_device<N, true> : leaf_device<N, false>;
+    auto fn = refine ? leaf_device<N, N != 32> : leaf_device<N, false>;
     rc = fn(reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec), prm, quant,
             has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
             reinterpret_cast<const mt_leaf8_job*>(d + o_jobs), n, reinterpret_cast<mt_leaf8_result*>(d + o_res),

@@ -28,10 +28,18 @@ __device__ __forceinline__ float hi_cost(const mt_coef_costs& T, uint32_t m, int
   return h;
 }
 
+__constant__ uint16_t kScan32[1024] = {MT_SCAN_32X32_LIST};
+
 // Default scan of a W x W block (scan index -> rc = x*W + y).
 template <int W>
 __device__ __forceinline__ int scan_rc(int i) {
-  return W == 4 ? kScan4[i] : (W == 8 ? kScan8[i] : kScan16[i]);
+  return W == 4 ? kScan4[i] : (W == 8 ? kScan8[i] : (W == 16 ? kScan16[i] : kScan32[i]));
+}
+
+// log2 of a block side 4 .. 32.
+template <int W>
+__host__ __device__ constexpr int log2w() {
+  return W == 4 ? 2 : (W == 8 ? 3 : (W == 16 ? 4 : 5));
 }
 
 // Scratch of trellis_ctx<W>: the zero-distortion suffix sums and the level map
@@ -43,8 +51,8 @@ struct TrellisCtxScratchW {
 };
 using TrellisCtxScratch = TrellisCtxScratchW<8>;
 
-// trellis_optimize_ctx of one TX_WxW luma block (W = 8: class 1, 16: class 2;
-// plane 0; the cost slice of that class) under the
+// trellis_optimize_ctx of one TX_WxW luma block (W = 8: class 1, 16: class 2,
+// 32: class 3; plane 0; the cost slice of that class) under the
 // shipped tuning: trellis_aom / eob_reprice / eob_zero_term / pad_stride off,
 // dead zone 0, the DC-only terminal in eob_base context 0 with br context 0,
 // skip priced at trellis_zero_bits = 1, tilt magnitude cap 2.  `lambda` is
@@ -54,7 +62,7 @@ template <int W, typename C>
 __device__ void trellis_ctx(C* __restrict__ cf, const float* __restrict__ tf, float dc_q, float ac_q, float lambda,
                             const mt_coef_costs& T, int dcs, const uint8_t* __restrict__ qm, bool qm_full,
                             float band_t, TrellisCtxScratchW<W>& s) {
-  constexpr int N = W * W, L = W == 4 ? 2 : (W == 8 ? 3 : 4);
+  constexpr int N = W * W, L = log2w<W>();
   constexpr float kCap = 2.0f, kNInv = 1.0f / (float)N;
   int eob = -1;
   for (int i = N - 1; i >= 0; i--)
@@ -302,11 +310,12 @@ __device__ __forceinline__ void trellis_ctx8(C* __restrict__ cf, const float* __
   trellis_ctx<8>(cf, tf, dc_q, ac_q, lambda, T, dcs, qm, qm_full, band_t, s);
 }
 
-// real_block_bits_bounded of a TX_WxW luma block (W = 4: class TX_4X4, 8:
-// TX_8X8) in txb_skip context skip_ctx and dc_sign context dcs with the
-// tx-type symbol of (mode, tx): +inf once the running sum passes `bound` after
-// the eob position or at an interior scan index divisible by 16.  lv:
-// (W + 2) * W bytes of scratch (the level map, stride W).
+// real_block_bits_bounded of a TX_WxW luma block (W = 4, 8, 16, 32: classes
+// TX_4X4 .. TX_32X32) in txb_skip context skip_ctx and dc_sign context dcs
+// with the tx-type symbol of (mode, tx) (tx < 0: none, the DCT-only TX_32X32
+// set): +inf once the running sum passes `bound` after the eob position or at
+// an interior scan index divisible by 16.  lv: (W + 2) * W bytes of scratch
+// (the level map, stride W).
 template <int W, typename C>
 __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, int skip_ctx, int dcs, int mode,
                                int tx, bool use_skip_bits, float skip1, float skip0, float bound,
@@ -320,7 +329,7 @@ __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, 
     }
   if (eob < 0) return use_skip_bits ? skip1 : T.txb_skip[skip_ctx][1];
   float bits = use_skip_bits ? skip0 : T.txb_skip[skip_ctx][0];
-  bits = __fadd_rn(bits, T.txtp[mode][tx]);
+  if (tx >= 0) bits = __fadd_rn(bits, T.txtp[mode][tx]);
   const float* dcs_c = T.dc_sign[dcs];
   if (eob == 0) {
     const uint32_t m = uabs(cf[0]);
@@ -340,7 +349,7 @@ __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, 
   uint32_t* lv32 = reinterpret_cast<uint32_t*>(lv);
 #pragma unroll
   for (int i = 0; i < (W + 2) * W / 4; i++) lv32[i] = 0;
-  constexpr int L = W == 4 ? 2 : (W == 8 ? 3 : 4);
+  constexpr int L = log2w<W>();
   const int ctx_e = 1 + (eob > (W * W >> 3)) + (eob > (W * W >> 2));
   {
     const int rc = scan_rc<W>(eob);
@@ -391,7 +400,7 @@ __device__ float rate_bounded(const C* __restrict__ cf, const mt_coef_costs& T, 
 template <int W, typename C>
 __device__ float rate_1d(const C* __restrict__ cf, bool vertical, const mt_coef_costs& T, int dcs, int mode,
                           uint8_t* __restrict__ lv) {
-  constexpr int L = W == 4 ? 2 : (W == 8 ? 3 : 4);
+  constexpr int L = log2w<W>();
   auto pos_rc = [&](int i) -> int { return vertical ? ((i & (W - 1)) << L) | (i >> L) : i; };
   int eob = -1;
   for (int i = W * W - 1; i >= 0; i--)

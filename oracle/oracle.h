@@ -152,6 +152,12 @@ int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params
 int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
               const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+/* dct1d_32_i32 in place on 32 values. */
+void or_dct1d_32(int32_t* buf);
+/* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */
+int or_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+              const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n,
+              mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 float or_scaled_trellis_lambda(float dc_q, float ac_q, float lambda0);
 int or_edge_filter_strength(int w, int h, int filter_type, int delta);
 int or_use_edge_upsample(int w, int h, int filter_type, int delta);

@@ -311,6 +311,51 @@ void fwd_2d_16x16(const int32_t* in, void (*colf)(int32_t*), void (*rowf)(int32_
   }
 }
 
+// dct.rs:589-631 WC32 (the odd-half weights of the 32-point forward DCT) and
+// dct1d_32_i32: even/odd split, the 16-point DCT of both halves (the odd one
+// after the WC32 weights), the odd-half running combine, interleave.
+const int32_t WC32[16] = {32808, 33127, 33780, 34802, 36248,  38203,  40796,  44224,
+                          48794, 55008, 63738, 76640, 97266, 134859, 223321, 667812};
+void dct1d_32(int32_t* b) {
+  int32_t t[32];
+  for (int i = 0; i < 16; i++) {
+    t[i] = b[i] + b[31 - i];
+    t[16 + i] = b[i] - b[31 - i];
+  }
+  dct1d_16(t);
+  for (int i = 0; i < 16; i++) t[16 + i] = mul_q16(t[16 + i], WC32[i]);
+  dct1d_16(t + 16);
+  t[16] = mul_q16(t[16], 92682) + t[17];  // fmla_sqrt2 (dct.rs:158-160)
+  for (int i = 17; i < 31; i++) t[i] += t[i + 1];
+  for (int i = 0; i < 16; i++) {
+    b[2 * i] = t[i];
+    b[2 * i + 1] = t[16 + i];
+  }
+}
+
+// dct.rs:705-736 dct32x32_quant_t_direct: the residual shifted left by B = 6,
+// columns then rows, each output (x * 16384 + 2^(15+B)) >> (16+B) in i64,
+// quantised into the levels at u*32 + v.
+void fwd_2d_32x32(const int32_t* in, int32_t mdc, int32_t mac, int32_t* cf, float* tf) {
+  const int B = 6;
+  std::vector<int32_t> tmp(1024);
+  for (int u = 0; u < 32; u++) {
+    int32_t col[32];
+    for (int i = 0; i < 32; i++) col[i] = in[i * 32 + u] * (1 << B);
+    dct1d_32(col);
+    for (int v = 0; v < 32; v++) tmp[(size_t)v * 32 + u] = col[v];
+  }
+  for (int v = 0; v < 32; v++) {
+    int32_t row[32];
+    for (int u = 0; u < 32; u++) row[u] = tmp[(size_t)v * 32 + u];
+    dct1d_32(row);
+    for (int u = 0; u < 32; u++) {
+      const int64_t prod = (int64_t)row[u] * 16384;
+      store_quant_target(cf, tf, u * 32 + v, (int32_t)((prod + (1ll << (15 + B))) >> (16 + B)), mdc, mac);
+    }
+  }
+}
+
 // dct.rs:1586-1611 identity_quant_t_direct (IDTX; QM never applied).
 void fwd_idtx(const int32_t* in, int w, int h, int32_t dc_q, int32_t ac_q, int32_t* cf, float* tf) {
   for (int y = 0; y < h; y++)
@@ -640,6 +685,9 @@ const uint8_t* or_qm_row(int32_t qm_level, int32_t chroma, int32_t w, int32_t h)
   return &MT_AV1_IQM[((size_t)qm_level * 2 + (chroma ? 1 : 0)) * 3344 + off];
 }
 
+// dct1d_32_i32 on one buffer of 32 (for the property tests of dct.rs:4091-4125).
+void or_dct1d_32(int32_t* buf) { dct1d_32(buf); }
+
 const uint16_t* or_default_scan(int32_t n) {
   switch (n) {
     case 4: return MT_SCAN_4X4;
@@ -651,6 +699,7 @@ const uint16_t* or_default_scan(int32_t n) {
 }
 
 void inv_16x16(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* qm, int32_t* out);
+void inv_32x32(const int32_t* levels, const mt_quant* q, const uint8_t* qm, int32_t* out);
 
 // DctDispatch::dct8x8_t / adst8x8_t / adstdct8x8_t / dctadst8x8_t (QM applied,
 // dct.rs:2751-2763, :2896-2909), fvdct8x8_t / fhdct8x8_t (flat, :2910-2920),
@@ -674,6 +723,12 @@ void or_fwd_txfm_quant(const int32_t* resid, int32_t tx, int32_t n, const mt_qua
       default: return;
     }
     if (qm_row) apply_qmatrix(cf, tf, qm_row, 16);
+    return;
+  }
+  if (n == 32) {  // TX_32X32: DCT_DCT only (dct.rs:2862-2873, QM applied)
+    if (tx != MT_TX_DCT_DCT) return;
+    fwd_2d_32x32(resid, q->q_mult_dc, q->q_mult_ac, cf, tf);
+    if (qm_row) apply_qmatrix(cf, tf, qm_row, 1024);
     return;
   }
   if (n == 16) {
@@ -706,6 +761,7 @@ void or_inv_txfm_dequant(const int32_t* levels, int32_t tx, int32_t n, const mt_
                          const uint8_t* qm_row, int32_t* resid) {
   if (n == 4) inv_4x4(levels, tx, q, qm_row, resid);
   if (n == 16) inv_16x16(levels, tx, q, qm_row, resid);
+  if (n == 32 && tx == MT_TX_DCT_DCT) inv_32x32(levels, q, qm_row, resid);
   if (n != 8) return;
   inv_8x8(levels, tx, q, qm_row, resid);
 }
@@ -842,6 +898,121 @@ void inv_16x16(const int32_t* levels, int tx, const mt_quant* q, const uint8_t* 
     else inv_dct16(tmp + x, 16, q->cmin, q->cmax);
   }
   for (int i = 0; i < 256; i++) out[i] = (tmp[i] + 8) >> 4;
+}
+
+// idct.rs:2130-2279 inv_dct32_1d (dav1d), in the reference's own forms: the
+// 16-point inverse on the even inputs, seven stages on the odd half.
+void inv_dct32(int32_t* c, int s, int32_t mn, int32_t mx) {
+  auto cl = [&](int32_t v) { return clampi(v, mn, mx); };
+  inv_dct16(c, 2 * s, mn, mx);
+  const int32_t in1 = c[s], in3 = c[3 * s], in5 = c[5 * s], in7 = c[7 * s];
+  const int32_t in9 = c[9 * s], in11 = c[11 * s], in13 = c[13 * s], in15 = c[15 * s];
+  const int32_t in17 = c[17 * s], in19 = c[19 * s], in21 = c[21 * s], in23 = c[23 * s];
+  const int32_t in25 = c[25 * s], in27 = c[27 * s], in29 = c[29 * s], in31 = c[31 * s];
+  int32_t t16a = ((in1 * 201 - in31 * (4091 - 4096) + 2048) >> 12) - in31;
+  int32_t t17a = ((in17 * (3035 - 4096) - in15 * 2751 + 2048) >> 12) + in17;
+  int32_t t18a = ((in9 * 1751 - in23 * (3703 - 4096) + 2048) >> 12) - in23;
+  int32_t t19a = ((in25 * (3857 - 4096) - in7 * 1380 + 2048) >> 12) + in25;
+  int32_t t20a = ((in5 * 995 - in27 * (3973 - 4096) + 2048) >> 12) - in27;
+  int32_t t21a = ((in21 * (3513 - 4096) - in11 * 2106 + 2048) >> 12) + in21;
+  int32_t t22a = (in13 * 1220 - in19 * 1645 + 1024) >> 11;
+  int32_t t23a = ((in29 * (4052 - 4096) - in3 * 601 + 2048) >> 12) + in29;
+  int32_t t24a = ((in29 * 601 + in3 * (4052 - 4096) + 2048) >> 12) + in3;
+  int32_t t25a = (in13 * 1645 + in19 * 1220 + 1024) >> 11;
+  int32_t t26a = ((in21 * 2106 + in11 * (3513 - 4096) + 2048) >> 12) + in11;
+  int32_t t27a = ((in5 * (3973 - 4096) + in27 * 995 + 2048) >> 12) + in5;
+  int32_t t28a = ((in25 * 1380 + in7 * (3857 - 4096) + 2048) >> 12) + in7;
+  int32_t t29a = ((in9 * (3703 - 4096) + in23 * 1751 + 2048) >> 12) + in9;
+  int32_t t30a = ((in17 * 2751 + in15 * (3035 - 4096) + 2048) >> 12) + in15;
+  int32_t t31a = ((in1 * (4091 - 4096) + in31 * 201 + 2048) >> 12) + in1;
+  int32_t t16 = cl(t16a + t17a), t17 = cl(t16a - t17a), t18 = cl(t19a - t18a), t19 = cl(t19a + t18a);
+  int32_t t20 = cl(t20a + t21a), t21 = cl(t20a - t21a), t22 = cl(t23a - t22a), t23 = cl(t23a + t22a);
+  int32_t t24 = cl(t24a + t25a), t25 = cl(t24a - t25a), t26 = cl(t27a - t26a), t27 = cl(t27a + t26a);
+  int32_t t28 = cl(t28a + t29a), t29 = cl(t28a - t29a), t30 = cl(t31a - t30a), t31 = cl(t31a + t30a);
+  t17a = ((t30 * 799 - t17 * (4017 - 4096) + 2048) >> 12) - t17;
+  t30a = ((t30 * (4017 - 4096) + t17 * 799 + 2048) >> 12) + t30;
+  t18a = ((-(t29 * (4017 - 4096) + t18 * 799) + 2048) >> 12) - t29;
+  t29a = ((t29 * 799 - t18 * (4017 - 4096) + 2048) >> 12) - t18;
+  t21a = (t26 * 1703 - t21 * 1138 + 1024) >> 11;
+  t26a = (t26 * 1138 + t21 * 1703 + 1024) >> 11;
+  t22a = (-(t25 * 1138 + t22 * 1703) + 1024) >> 11;
+  t25a = (t25 * 1703 - t22 * 1138 + 1024) >> 11;
+  t16a = cl(t16 + t19);
+  t17 = cl(t17a + t18a);
+  t18 = cl(t17a - t18a);
+  t19a = cl(t16 - t19);
+  t20a = cl(t23 - t20);
+  t21 = cl(t22a - t21a);
+  t22 = cl(t22a + t21a);
+  t23a = cl(t23 + t20);
+  t24a = cl(t24 + t27);
+  t25 = cl(t25a + t26a);
+  t26 = cl(t25a - t26a);
+  t27a = cl(t24 - t27);
+  t28a = cl(t31 - t28);
+  t29 = cl(t30a - t29a);
+  t30 = cl(t30a + t29a);
+  t31a = cl(t31 + t28);
+  t18a = ((t29 * 1567 - t18 * (3784 - 4096) + 2048) >> 12) - t18;
+  t29a = ((t29 * (3784 - 4096) + t18 * 1567 + 2048) >> 12) + t29;
+  t19 = ((t28a * 1567 - t19a * (3784 - 4096) + 2048) >> 12) - t19a;
+  t28 = ((t28a * (3784 - 4096) + t19a * 1567 + 2048) >> 12) + t28a;
+  t20 = ((-(t27a * (3784 - 4096) + t20a * 1567) + 2048) >> 12) - t27a;
+  t27 = ((t27a * 1567 - t20a * (3784 - 4096) + 2048) >> 12) - t20a;
+  t21a = ((-(t26 * (3784 - 4096) + t21 * 1567) + 2048) >> 12) - t26;
+  t26a = ((t26 * 1567 - t21 * (3784 - 4096) + 2048) >> 12) - t21;
+  t16 = cl(t16a + t23a);
+  t17a = cl(t17 + t22);
+  t18 = cl(t18a + t21a);
+  t19a = cl(t19 + t20);
+  t20a = cl(t19 - t20);
+  t21 = cl(t18a - t21a);
+  t22a = cl(t17 - t22);
+  t23 = cl(t16a - t23a);
+  t24 = cl(t31a - t24a);
+  t25a = cl(t30 - t25);
+  t26 = cl(t29a - t26a);
+  t27a = cl(t28 - t27);
+  t28a = cl(t28 + t27);
+  t29 = cl(t29a + t26a);
+  t30a = cl(t30 + t25);
+  t31 = cl(t31a + t24a);
+  t20 = ((t27a - t20a) * 181 + 128) >> 8;
+  t27 = ((t27a + t20a) * 181 + 128) >> 8;
+  t21a = ((t26 - t21) * 181 + 128) >> 8;
+  t26a = ((t26 + t21) * 181 + 128) >> 8;
+  t22 = ((t25a - t22a) * 181 + 128) >> 8;
+  t25 = ((t25a + t22a) * 181 + 128) >> 8;
+  t23a = ((t24 - t23) * 181 + 128) >> 8;
+  t24a = ((t24 + t23) * 181 + 128) >> 8;
+  const int32_t odd[16] = {t31, t30a, t29, t28a, t27, t26a, t25, t24a, t23a, t22, t21a, t20, t19a, t18, t17a, t16};
+  int32_t even[16];
+  for (int k = 0; k < 16; k++) even[k] = c[2 * k * s];
+  for (int k = 0; k < 16; k++) {
+    c[k * s] = cl(even[k] + odd[k]);
+    c[(31 - k) * s] = cl(even[k] - odd[k]);
+  }
+}
+
+// idct.rs:2281-2320 idct_dequant_32x32_scalar: the dequantised product masked
+// to 24 bits and halved (dq_shift 1), clamped to cf_max; rows with the row
+// clip, (t+2)>>2 with the column clip, columns, (t+8)>>4.
+void inv_32x32(const int32_t* levels, const mt_quant* q, const uint8_t* qm, int32_t* out) {
+  std::vector<int32_t> tmp(1024, 0);
+  for (int rc = 0; rc < 1024; rc++) {
+    const int32_t l = levels[rc];
+    if (l == 0) continue;
+    const int32_t base = rc == 0 ? q->dc_q : q->ac_q;
+    const int32_t step = qm ? ((base * (int32_t)qm[rc] + 16) >> 5) : base;
+    int32_t mag = (int32_t)((((uint64_t)uabs(l) * (uint64_t)(uint32_t)step) & 0xffffffULL) >> 1);
+    const int32_t cap = q->cf_max + (l < 0 ? 1 : 0);
+    if (mag > cap) mag = cap;
+    tmp[(size_t)(rc & 31) * 32 + (rc >> 5)] = l < 0 ? -mag : mag;
+  }
+  for (int y = 0; y < 32; y++) inv_dct32(&tmp[(size_t)y * 32], 1, q->rmin, q->rmax);
+  for (int i = 0; i < 1024; i++) tmp[i] = clampi((tmp[i] + 2) >> 2, q->cmin, q->cmax);
+  for (int x = 0; x < 32; x++) inv_dct32(&tmp[x], 32, q->cmin, q->cmax);
+  for (int i = 0; i < 1024; i++) out[i] = (tmp[i] + 8) >> 4;
 }
 
 // trellis.rs:944-1030 trellis_optimize with the AVX2 step A

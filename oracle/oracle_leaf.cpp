@@ -888,8 +888,9 @@ extern "C" {
 
 // block8.rs:738-808 (refine = 0: the Slow mode loop's candidate) and
 // :1183-1404 (refine = 1: the winner's transform-type refinement) of
-// pick_block8 over a batch of 8x8 jobs (N = 8), or the same two stages of
-// pick_luma16 over 16x16 jobs (N = 16).
+// pick_block8 over a batch of 8x8 jobs (N = 8), the same two stages of
+// pick_luma16 over 16x16 jobs (N = 16), or pick_luma32's mode-loop candidates
+// over 32x32 jobs (N = 32, refine 0: block32.rs:776-836, TX_32X32 DCT_DCT).
 static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                      const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
                      mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
@@ -916,7 +917,7 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       if (rec_out) memset(rec_out + (size_t)i * NN, 0, NN * 2);
       continue;
     }
-    int32_t pred[256];
+    int32_t pred[1024];
     if (jb.mode == MT_DC_PRED) {
       const int32_t d = or_dc_pred(recon, p->stride, jb.px, jb.py, N, N, p->bd);
       for (int k = 0; k < NN; k++) pred[k] = d;
@@ -924,7 +925,7 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       or_intra_predict(recon, p->stride, jb.px, jb.py, N, N, jb.mode, jb.angle_delta, jb.flags & 1,
                        (jb.flags >> 1) & 1, p->frame_w, p->frame_h, (jb.flags >> 2) & 1, p->bd, pred);
     }
-    int32_t resid[256];
+    int32_t resid[1024];
     for (int y = 0; y < N; y++)
       for (int x = 0; x < N; x++)
         resid[y * N + x] = (int32_t)src[(size_t)(jb.py + y) * p->stride + jb.px + x] - pred[y * N + x];
@@ -940,11 +941,13 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
     // drops V_DCT / H_DCT (cost.rs:95-108).
     auto bits2d = [&](const int32_t* cf, int t, float bound) -> float {
       const int sym = N == 16 && t >= MT_TX_ADST_ADST ? t - 2 : t;
-      return or_real_block_bits_bounded(cf, scan, N, N, cd, 0, ds, jb.mode, sym, p->use_skip_bits, skip, bound);
+      // TX_32X32 intra codes no tx-type symbol (lossy_state.rs:533-539)
+      return or_real_block_bits_bounded(cf, scan, N, N, cd, 0, ds, N == 32 ? -1 : jb.mode, sym, p->use_skip_bits,
+                                        skip, bound);
     };
     // The DCT_DCT candidate with the per-candidate trellis (block8.rs:780-805).
-    int32_t lcf[256], lrr[256];
-    float tf[256];
+    int32_t lcf[1024], lrr[1024];
+    float tf[1024];
     or_fwd_txfm_quant(resid, MT_TX_DCT_DCT, N, q, qm, lcf, tf);
     or_trellis_optimize_ctx(lcf, tf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level, p->band_tilt);
     or_inv_txfm_dequant(lcf, MT_TX_DCT_DCT, N, q, qm, lrr);
@@ -965,8 +968,8 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       // by the DCT's rd cost.  An aborted rate is infinite, so an accepted
       // one is exact.
       {
-        int32_t acf[256], arr[256];
-        float atf[256];
+        int32_t acf[1024], arr[1024];
+        float atf[1024];
         or_fwd_txfm_quant(resid, MT_TX_ADST_ADST, N, q, qm, acf, atf);
         or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level,
                                 p->band_tilt);
@@ -981,8 +984,8 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       // bounded rate; partition_search.rs:5331-5423, unbounded luma_bits, the
       // ADST_ADST winner re-priced unbounded -- the same value).
       for (int t : {MT_TX_ADST_DCT, MT_TX_DCT_ADST}) {
-        int32_t acf[256], arr[256];
-        float atf[256];
+        int32_t acf[1024], arr[1024];
+        float atf[1024];
         or_fwd_txfm_quant(resid, t, N, q, qm, acf, atf);
         or_trellis_optimize_ctx(acf, atf, dcq, acq, scan, N, p->trellis_lambda0, cd, ds, qm, q->qm_level,
                                 p->band_tilt);
@@ -996,8 +999,8 @@ static int leaf_impl(int N, const uint16_t* src, const uint16_t* recon, const mt
       // IDTX without the trellis, within tx_guard of the winner's SSE
       // (block8.rs:1334-1361; partition_search.rs:5425-5474)
       {
-        int32_t icf[256], irr[256];
-        float itf[256];
+        int32_t icf[1024], irr[1024];
+        float itf[1024];
         or_fwd_txfm_quant(resid, MT_TX_IDTX, N, q, qm, icf, itf);
         or_inv_txfm_dequant(icf, MT_TX_IDTX, N, q, qm, irr);
         const int64_t isse = sse_of(irr);
@@ -1044,6 +1047,13 @@ int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_param
               const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
   return leaf_impl(16, src, recon, p, q, qm, cd, jobs, n, refine, results, cf_out, rec_out);
+}
+
+// block32.rs:776-836 pick_luma32's mode-loop candidates.
+int or_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+              const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, mt_leaf8_result* results,
+              int32_t* cf_out, uint16_t* rec_out) {
+  return leaf_impl(32, src, recon, p, q, qm, cd, jobs, n, 0, results, cf_out, rec_out);
 }
 
 }  // extern "C"

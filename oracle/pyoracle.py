@@ -85,6 +85,9 @@ def load():
             "or_dirty_log2f": (C.c_float, [C.c_float]),
             "or_leaf16": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                     C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
+            "or_dct1d_32": (None, [_P]),
+            "or_leaf32": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                    C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_leaf8": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                    C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
             "or_split16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -508,6 +511,32 @@ def leaf16(src, recon, prm, q, qm, cdfs, jobs, refine=False, threads=1):
     def run(lo, hi):
         assert load().or_leaf16(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs[lo:hi]),
                            hi - lo, int(bool(refine)), p(res[lo:hi]), p(cf[lo:hi]), p(rec[lo:hi])) == 0
+
+    _chunked(n, threads, run)
+    return res, cf, rec
+
+
+def dct1d_32(buf):
+    """dct1d_32_i32 of 32 integers."""
+    b = np.ascontiguousarray(buf, np.int32).copy()
+    load().or_dct1d_32(p(b))
+    return b
+
+
+def leaf32(src, recon, prm, q, qm, cdfs, jobs, threads=1):
+    """pick_luma32's mode-loop candidates of n 32x32 jobs: (results, cf n x 1024, rec n x 32 x 32)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.LEAF8_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.LEAF8_RESULT_DTYPE)
+    cf = np.zeros((n, 1024), np.int32)
+    rec = np.zeros((n, 32, 32), np.uint16)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+
+    def run(lo, hi):
+        assert load().or_leaf32(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs), p(jobs[lo:hi]),
+                                hi - lo, p(res[lo:hi]), p(cf[lo:hi]), p(rec[lo:hi])) == 0
 
     _chunked(n, threads, run)
     return res, cf, rec
