@@ -445,14 +445,16 @@ def measure_split16(dev, wl, search, reps=5, cpu=True, depth2=False):
     return out
 
 
-def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
+def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False, n32=False):
     """The 8x8 leaf's luma search over the same 1080p luma: the mode loop's
     candidates (32,400 blocks x 13 modes, DCT_DCT with trellis_optimize_ctx and
     sse_recon) or the winners' transform-type refinement (32,400 blocks, seven
     types, 4:4:4 form).  Device time with CUDA events after an L2 flush; the
     oracle on all host cores over the same jobs.  n16: the 16x16 leaf's
     mode-loop candidates (8,040 blocks x 13 modes, trellis_optimize_ctx at
-    TX_16X16) or its winners' refinement (8,040 blocks, five types)."""
+    TX_16X16) or its winners' refinement (8,040 blocks, five types).  n32: the
+    32x32 leaf's mode-loop candidates (1,980 blocks x 13 modes, TX_32X32
+    DCT_DCT with trellis_optimize_ctx)."""
     import ctypes as C
 
     import torch
@@ -460,10 +462,11 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     from maroontree_b200 import abi, synth
 
     q = wl["q"]
-    qm = mt.qm_row(wl["qm_level"], 0, 16 if n16 else 8)
-    cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), 16 if n16 else 8, 16 if n16 else 8, 0)
+    size = 32 if n32 else (16 if n16 else 8)
+    qm = mt.qm_row(wl["qm_level"], 0, size)
+    cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), size, size, 0)
     costs = mt.coef_costs(cdfs)
-    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=SEED, n=16 if n16 else 8)
+    jobs = synth.leaf8_jobs(W, H, [abi.PAETH_PRED] if refine else MODES, seed=SEED, n=size)
     n = len(jobs)
     prm = mt.split16_params(W, H, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].lambda_d, band_tilt=1.9,
                             tx_search=refine, tx_guard_shift=5)
@@ -473,7 +476,9 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     d_res = torch.empty(n * abi.LEAF8_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     lib = mt.load()
-    if n16:
+    if n32:
+        entry = lib.mt_leaf32_luma_device
+    elif n16:
         entry = lib.mt_leaf16_tx_refine_device if refine else lib.mt_leaf16_luma_device
     else:
         entry = lib.mt_leaf8_tx_refine_device if refine else lib.mt_leaf8_luma_device
@@ -502,13 +507,18 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False):
     if n16:
         what = ("leaf16 winners' transform-type refinement 1920x1080 luma, 8,040 blocks, 5 types" if refine else
                 "leaf16 mode-loop candidates 1920x1080 luma, 8,040 blocks x 13 modes (DCT_DCT + trellis_optimize_ctx)")
+    if n32:
+        what = "leaf32 mode-loop candidates 1920x1080 luma, 1,980 blocks x 13 modes (TX_32X32 DCT_DCT + " \
+               "trellis_optimize_ctx)"
     out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n, "workload": what}
     if cpu:
         from oracle import pyoracle as po
 
         threads = os.cpu_count() or 1
         t0 = time.perf_counter()
-        if n16:
+        if n32:
+            po.leaf32(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, threads=threads)
+        elif n16:
             po.leaf16(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine, threads=threads)
         else:
             po.leaf8(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, refine=refine, threads=threads)
@@ -986,6 +996,7 @@ def run_ours(args):
         leaf8 = {k: measure_leaf8(dev, wl, k == "refine", cpu=not nocpu) for k in ("luma", "refine")}
         leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n16=True)
         leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=not nocpu, n16=True)
+        leaf8["luma32"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n32=True)
         secondary["leaf8"] = leaf8
     if rank == 0 and not nocpu:
         from oracle import build as obuild
