@@ -632,6 +632,47 @@ int mt_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_param
               const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
 
+/* The 64x64 leaf's four-TX_32X32 leg (rd_pick_luma64's candidate loop,
+ * src/coder/block64.rs:1906-1958; the shipped tuning leaves TX_64X64 off): for
+ * each (64x64 block, mode, delta) the four quadrants in raster order, each
+ * predicted at 32x32 from the block's running reconstruction with the
+ * per-transform edge flags (quad_edges, :2731-2745: the first from the rows /
+ * columns around the block, the second with the block's top-right flag, the
+ * third with top-right and the block's bottom-left flag, the fourth with
+ * neither), TX_32X32 DCT_DCT with the QM and trellis_optimize_ctx in the
+ * quadrant's dc_sign context, the inverse, the decision distortion sse_recon
+ * x K_PART_LAMBDA (luma64_wsse, src/coder/lossy_state.rs:2363-2382) and
+ * luma_bits in txb_skip context 0; the quadrant's reconstruction is written
+ * back before the next.  total = rd_lambda x mode_bits (+ rd_lambda x
+ * delta_bits for a directional mode) + the quadrants' sse x 2.775 +
+ * rd_lambda x bits, f32 in that order.  Params as for the 32x32 leaf
+ * (trellis_lambda0: the trellis lambda with the perceptual scale;
+ * rd_lambda: mlam x prdo).  Rejected jobs (outside the frame, a bad mode /
+ * delta / context) get total and bits +inf, sse 0. */
+typedef struct mt_quad32_job {
+  uint16_t px, py;          /* 64x64 block origin */
+  uint8_t mode;             /* MT_*_PRED */
+  int8_t angle_delta;       /* -3..3, directional modes only */
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL of the 64x64 block, MT_CAND_FILTER_TYPE */
+  uint8_t reserved;
+  uint8_t dcs_ctx[4];       /* dc_sign_ctx_32 of each quadrant, raster order */
+  float mode_bits;          /* mode_bits(px, py, mode) */
+  float delta_bits;         /* the angle-delta symbol's bits (read for directional modes) */
+} mt_quad32_job;
+typedef struct mt_quad32_result {
+  float total;              /* the candidate's total cost */
+  float bits[4];            /* each quadrant's coefficient bits */
+  uint32_t reserved;
+  int64_t sse[4];           /* each quadrant's sse_recon */
+} mt_quad32_result;
+int mt_quad32_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_quad32_job* d_jobs, int32_t n, mt_quad32_result* d_results, void* stream);
+/* Host-buffer form of mt_quad32_luma_device. */
+int mt_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_quad32_job* jobs, int32_t n,
+                   mt_quad32_result* results);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

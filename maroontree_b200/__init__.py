@@ -393,6 +393,20 @@ def leaf32(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=F
     return res, cf, rec
 
 
+def quad32_luma(src, recon, prm, quant, qmrow, costs, jobs):
+    """The 64x64 leaf's four-TX_32X32 leg (``mt_quad32_luma``); qmrow / costs are
+    the 32x32 row and the TX_32X32 slice.  Returns the results."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.QUAD32_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.QUAD32_RESULT_DTYPE)
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_quad32_luma(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                                 ptr(jobs), n, ptr(res)), "mt_quad32_luma")
+    return res
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

@@ -99,6 +99,13 @@ LEAF8_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angl
 LEAF8_RESULT_DTYPE = np.dtype([("sse", "<i8"), ("bits", "<f4"), ("cost", "<f4"), ("tx_type", "u1"),
                                ("reserved", "u1", (7,))])
 assert LEAF8_JOB_DTYPE.itemsize == 12 and LEAF8_RESULT_DTYPE.itemsize == 24
+# mt_quad32_job / mt_quad32_result.
+QUAD32_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"),
+                             ("reserved", "u1"), ("dcs_ctx", "u1", (4,)), ("mode_bits", "<f4"),
+                             ("delta_bits", "<f4")], align=True)
+QUAD32_RESULT_DTYPE = np.dtype([("total", "<f4"), ("bits", "<f4", (4,)), ("reserved", "<u4"), ("sse", "<i8", (4,))],
+                               align=True)
+assert QUAD32_JOB_DTYPE.itemsize == 20 and QUAD32_RESULT_DTYPE.itemsize == 56
 CFL_BLOCK_DTYPE = np.dtype([("cx", "<u2"), ("cy", "<u2"), ("dc", "<i2", (2,))])
 assert CFL_BLOCK_DTYPE.itemsize == 8
 
@@ -407,6 +414,10 @@ def _bind(lib):
                                             C.c_int32, _P, _P, _P, _P]),
         "mt_leaf32": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                 C.c_int32, _P, _P, _P]),
+        "mt_quad32_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                            C.c_int32, _P, _P]),
+        "mt_quad32_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
+                                     _P, C.c_int32, _P]),
         "mt_leaf8": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                C.c_int32, C.c_int32, _P, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
@@ -463,7 +474,7 @@ EXPORTED_SYMBOLS = (
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
     "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
-    "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32",
+    "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
 )
 
 

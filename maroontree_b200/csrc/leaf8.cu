@@ -209,6 +209,122 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
   }
 }
 
+// The 64x64 leaf's four-TX_32X32 leg (rd_pick_luma64's candidate loop,
+// src/coder/block64.rs:1906-1958): for a (64x64 block, mode, delta), the
+// quadrants in raster order (Q64, :328), each predicted at 32x32 from the
+// running reconstruction with the per-transform edge flags (quad_edges,
+// :2731-2745), TX_32X32 DCT_DCT with the QM and trellis_optimize_ctx in the
+// quadrant's dc_sign context, the inverse, the decision distortion
+// (luma_pick_distortion with luma64_wsse: chroma_sse's value, i.e. sse_recon,
+// times K_PART_LAMBDA, src/coder/lossy_state.rs:2363-2382), luma_bits, and the
+// reconstruction written back before the next quadrant.  total =
+// mlam * mode_bits (+ mlam * delta_bits) + sum of (dist + mlam * bits), f32 in
+// that order.
+struct Patch64Read {
+  const uint16_t* __restrict__ rec;
+  int stride, px, py;
+  const uint16_t* patch;
+  __device__ __forceinline__ int32_t operator()(int x, int y) const {
+    const int dx = x - px, dy = y - py;
+    if ((unsigned)dx < 64u && (unsigned)dy < 64u) return patch[dy * 64 + dx];
+    return rec[(size_t)y * stride + x];
+  }
+};
+
+__global__ void __launch_bounds__(kLeafThreads) quad32_kernel(
+    const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_quad32_job* __restrict__ jobs, int n, mt_quad32_result* __restrict__ res) {
+  __shared__ mt_coef_costs sT;
+  constexpr int NN = 1024;
+  __shared__ uint8_t sQm[NN];
+  __shared__ float sQs[NN];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    for (int i = threadIdx.x; i < NN; i += blockDim.x) {
+      const int w = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)w;
+      sQs[i] = fwd_qm_scale(w);
+    }
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_quant& q = a.q;
+  const mt_coef_costs& T = sT;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const mt_quad32_job jb = jobs[j];
+  mt_quad32_result& r = res[j];
+  const bool directional = jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED;
+  const bool ok = jb.px + 64 <= p.frame_w && jb.py + 64 <= p.frame_h && jb.mode <= MT_PAETH_PRED &&
+                  jb.angle_delta >= -3 && jb.angle_delta <= 3 && (jb.angle_delta == 0 || directional) &&
+                  jb.dcs_ctx[0] < 3 && jb.dcs_ctx[1] < 3 && jb.dcs_ctx[2] < 3 && jb.dcs_ctx[3] < 3;
+  r.reserved = 0;
+  if (!ok) {
+    r.total = __int_as_float(0x7f800000);
+    for (int k = 0; k < 4; k++) {
+      r.bits[k] = __int_as_float(0x7f800000);
+      r.sse[k] = 0;
+    }
+    return;
+  }
+  LeafWork<32> w;
+  uint16_t patch[64 * 64];
+  for (int y = 0; y < 64; y++)
+    for (int x = 0; x < 64; x++) patch[y * 64 + x] = rec[(size_t)(jb.py + y) * p.stride + jb.px + x];
+  const Patch64Read rd{rec, p.stride, jb.px, jb.py, patch};
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float dcq = (float)q.dc_q, acq = (float)q.ac_q, mlam = p.rd_lambda;
+  const bool qm_full = q.qm_level >= 5;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  const float skip1 = p.use_skip_bits ? p.skip_bits[0][0] : 0.0f;
+  const float skip0 = p.use_skip_bits ? p.skip_bits[0][1] : 0.0f;
+  const bool have_tr = jb.flags & 1, have_bl = (jb.flags >> 1) & 1, ft = (jb.flags >> 2) & 1;
+  float total = __fmul_rn(mlam, jb.mode_bits);
+  if (directional) total = __fadd_rn(total, __fmul_rn(mlam, jb.delta_bits));
+  float* tf = reinterpret_cast<float*>(w.u);
+  int32_t* tmp = w.u + NN;
+  auto* cf = w.cfs[0];
+  int16_t* rr = w.rrs[0];
+#pragma unroll 1
+  for (int k = 0; k < 4; k++) {
+    const int sx = (k & 1) * 32, sy = (k >> 1) * 32;
+    const int bx = jb.px + sx, by = jb.py + sy;
+    const bool tr = k == 0 ? jb.py > 0 : (k == 1 ? have_tr : k == 2);
+    const bool bl = k == 0 ? jb.px > 0 : (k == 2 ? have_bl : false);
+    predict_sq_at<32>(rd, p.frame_w, p.frame_h, bx, by, jb.mode, jb.angle_delta, tr, bl, ft, p.bd, w.pred, w.u);
+#pragma unroll 8
+    for (int i = 0; i < NN; i++)
+      w.resid[i] = (int16_t)((int32_t)src[(size_t)(by + (i >> 5)) * p.stride + bx + (i & 31)] - w.pred[i]);
+    fwd32x32(w.resid, q, cf, tf, tmp);
+    if (qm) apply_qm(cf, tf, sQs, NN);
+    if (a.lambda > 0.0f) trellis_ctx<32>(cf, tf, dcq, acq, a.lambda, T, jb.dcs_ctx[k], qm, qm_full, p.band_tilt, w.tr);
+    inv32x32(cf, q, qm, rr, tmp);
+    ErrBlock<int16_t, int16_t> eb;
+    eb.src = src + (size_t)by * p.stride + bx;
+    eb.stride = p.stride;
+    eb.pred = w.pred;
+    eb.resid = rr;
+    eb.w = 32;
+    eb.vw = min(max(vis_w - bx, 0), 32);
+    eb.vh = min(max(vis_h - by, 0), 32);
+    eb.maxv = maxv;
+    const long long sse = sse_recon_block(eb, p.wsse_scale);
+    const float dist = __fmul_rn(__ll2float_rn(sse), 2.775f);  // proxy_wsse: K_PART_LAMBDA
+    const float bits = rate_bounded<32>(cf, T, 0, jb.dcs_ctx[k], jb.mode, -1, p.use_skip_bits != 0, skip1, skip0,
+                                        __int_as_float(0x7f800000), w.lv);
+    total = __fadd_rn(total, __fadd_rn(dist, __fmul_rn(mlam, bits)));
+    r.bits[k] = bits;
+    r.sse[k] = sse;
+    for (int i = 0; i < NN; i++)
+      patch[(sy + (i >> 5)) * 64 + sx + (i & 31)] = (uint16_t)clampi((int32_t)w.pred[i] + rr[i], 0, maxv);
+  }
+  r.total = total;
+}
+
 int check(const mt_split16_params* p, const mt_quant* q, int32_t n) {
   if (!p || !q || n < 0) return MT_ERR_INVALID_INPUT;
   if (p->bd != 8) return MT_ERR_UNSUPPORTED;
@@ -244,6 +360,25 @@ template <int N>
 int leaf_host(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
               const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+
+int quad32_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm, const mt_quant* quant,
+                  const uint8_t* d_qm_row, const mt_coef_costs* d_costs, const mt_quad32_job* d_jobs, int32_t n,
+                  mt_quad32_result* d_results, void* stream) {
+  const int rc = check(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!d_src || !d_recon || !d_costs || !d_jobs || !d_results) return MT_ERR_INVALID_INPUT;
+  LeafArgs a;
+  a.p = *prm;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
+  quad32_kernel<<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+                  reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
+                                                            d_results);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
 
 }  // namespace
 
@@ -303,6 +438,44 @@ int mt_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_param
               const uint8_t* qm_row, const mt_coef_costs* costs, const mt_leaf8_job* jobs, int32_t n,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out) {
   return leaf_host<32>(src, recon, prm, quant, qm_row, costs, jobs, n, 0, results, cf_out, rec_out);
+}
+
+int mt_quad32_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_quad32_job* d_jobs, int32_t n, mt_quad32_result* d_results, void* stream) {
+  return quad32_device(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, stream);
+}
+
+int mt_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_quad32_job* jobs, int32_t n,
+                   mt_quad32_result* results) {
+  int rc = check(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
+  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + up256(1024);
+  const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
+  const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_quad32_job));
+  const size_t total = o_res + up256((size_t)n * sizeof(mt_quad32_result));
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 1024, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_quad32_job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = quad32_device(reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec),
+                       prm, quant, has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
+                       reinterpret_cast<const mt_quad32_job*>(d + o_jobs), n,
+                       reinterpret_cast<mt_quad32_result*>(d + o_res), nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_quad32_result), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
 }  // extern "C"

@@ -152,6 +152,10 @@ int or_leaf8(const uint16_t* src, const uint16_t* recon, const mt_split16_params
 int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
               const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_leaf8_job* jobs, int32_t n, int32_t refine,
               mt_leaf8_result* results, int32_t* cf_out, uint16_t* rec_out);
+/* block64.rs rd_pick_luma64's four-TX_32X32 leg (:1906-1958) per (64x64 block, mode, delta). */
+int or_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                   const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_quad32_job* jobs, int32_t n,
+                   mt_quad32_result* results);
 /* dct1d_32_i32 in place on 32 values. */
 void or_dct1d_32(int32_t* buf);
 /* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */

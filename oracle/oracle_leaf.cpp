@@ -1049,6 +1049,98 @@ int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_param
   return leaf_impl(16, src, recon, p, q, qm, cd, jobs, n, refine, results, cf_out, rec_out);
 }
 
+// block64.rs:1906-1958 rd_pick_luma64's four-TX_32X32 leg (Quad32) of each
+// (64x64 block, mode, delta) job: the quadrants in Q64 order (:328), each
+// predicted at 32x32 from the running reconstruction with quad_edges'
+// flags (:2731-2745), DCT_DCT + QM, trellis_optimize_ctx in the quadrant's
+// dc_sign context, the inverse, luma_pick_distortion's Wsse metric
+// (chroma_sse's value x K_PART_LAMBDA, lossy_state.rs:2363-2382, :1804-1806),
+// luma_bits, recon_add_pred back into the reconstruction; total =
+// rate_cost(mlam, mode_bits) [+ rate_cost(mlam, delta_bits)] + the quadrants'
+// rd_cost (partition_rd.rs:140-142).  Each job starts from the block's
+// reconstruction as given (the reference restores it per candidate).
+int or_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                   const uint8_t* qm, const mt_coef_cdfs* cd, const mt_quad32_job* jobs, int32_t n,
+                   mt_quad32_result* results) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const uint16_t* scan = or_default_scan(32);
+  const float dcq = (float)q->dc_q, acq = (float)q->ac_q, mlam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  const float* skip = p->use_skip_bits ? p->skip_bits[0] : nullptr;
+  std::vector<uint16_t> work(recon, recon + (size_t)p->stride * p->frame_h);
+  std::vector<int32_t> pred(1024), resid(1024), cf(1024), rr(1024);
+  std::vector<float> tf(1024);
+  for (int i = 0; i < n; i++) {
+    const mt_quad32_job& jb = jobs[i];
+    mt_quad32_result* r = &results[i];
+    r->reserved = 0;
+    const bool directional = jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED;
+    const bool bad = jb.px + 64 > p->frame_w || jb.py + 64 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+                     jb.angle_delta < -3 || jb.angle_delta > 3 || (jb.angle_delta != 0 && !directional) ||
+                     jb.dcs_ctx[0] > 2 || jb.dcs_ctx[1] > 2 || jb.dcs_ctx[2] > 2 || jb.dcs_ctx[3] > 2;
+    if (bad) {
+      r->total = INFINITY;
+      for (int k = 0; k < 4; k++) {
+        r->bits[k] = INFINITY;
+        r->sse[k] = 0;
+      }
+      continue;
+    }
+    const bool have_tr = jb.flags & 1, have_bl = (jb.flags >> 1) & 1, ft = (jb.flags >> 2) & 1;
+    float total = mlam * jb.mode_bits;
+    if (directional) total += mlam * jb.delta_bits;
+    static const int kQ64[4][2] = {{0, 0}, {32, 0}, {0, 32}, {32, 32}};
+    for (int k = 0; k < 4; k++) {
+      const int sx = kQ64[k][0], sy = kQ64[k][1];
+      const int bx = jb.px + sx, by = jb.py + sy;
+      bool tr, bl;  // quad_edges
+      if (sx == 0 && sy == 0) {
+        tr = jb.py > 0;
+        bl = jb.px > 0;
+      } else if (sy == 0) {
+        tr = have_tr;
+        bl = false;
+      } else if (sx == 0) {
+        tr = true;
+        bl = have_bl;
+      } else {
+        tr = bl = false;
+      }
+      if (jb.mode == MT_DC_PRED) {
+        const int32_t d = or_dc_pred(work.data(), p->stride, bx, by, 32, 32, p->bd);
+        for (int t = 0; t < 1024; t++) pred[t] = d;
+      } else {
+        or_intra_predict(work.data(), p->stride, bx, by, 32, 32, jb.mode, jb.angle_delta, tr, bl, p->frame_w,
+                         p->frame_h, ft, p->bd, pred.data());
+      }
+      for (int y = 0; y < 32; y++)
+        for (int x = 0; x < 32; x++)
+          resid[y * 32 + x] = (int32_t)src[(size_t)(by + y) * p->stride + bx + x] - pred[y * 32 + x];
+      or_fwd_txfm_quant(resid.data(), MT_TX_DCT_DCT, 32, q, qm, cf.data(), tf.data());
+      or_trellis_optimize_ctx(cf.data(), tf.data(), dcq, acq, scan, 32, p->trellis_lambda0, cd, jb.dcs_ctx[k], qm,
+                              q->qm_level, p->band_tilt);
+      or_inv_txfm_dequant(cf.data(), MT_TX_DCT_DCT, 32, q, qm, rr.data());
+      const uint16_t pos[2] = {(uint16_t)bx, (uint16_t)by};
+      int64_t sse = 0;
+      or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred.data(), rr.data(), 1, 32, 32, p->wsse_scale, &sse);
+      const float dist = (float)sse * 2.775f;
+      const float bits = or_real_block_bits_bounded(cf.data(), scan, 32, 32, cd, 0, jb.dcs_ctx[k], -1, 0,
+                                                    p->use_skip_bits, skip, INFINITY);
+      total += dist + mlam * bits;
+      r->bits[k] = bits;
+      r->sse[k] = sse;
+      for (int y = 0; y < 32; y++)
+        for (int x = 0; x < 32; x++)
+          work[(size_t)(by + y) * p->stride + bx + x] = (uint16_t)clampi(pred[y * 32 + x] + rr[y * 32 + x], 0, maxv);
+    }
+    r->total = total;
+    for (int y = 0; y < 64; y++)  // the next job predicts from the input reconstruction
+      memcpy(&work[(size_t)(jb.py + y) * p->stride + jb.px], &recon[(size_t)(jb.py + y) * p->stride + jb.px], 128);
+  }
+  return MT_OK;
+}
+
 // block32.rs:776-836 pick_luma32's mode-loop candidates.
 int or_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
               const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, mt_leaf8_result* results,

@@ -86,6 +86,8 @@ def load():
             "or_leaf16": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                     C.POINTER(abi.CoefCdfs), _P, C.c_int32, C.c_int32, _P, _P, _P]),
             "or_dct1d_32": (None, [_P]),
+            "or_quad32_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                         C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P]),
             "or_leaf32": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                     C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_leaf8": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -540,6 +542,23 @@ def leaf32(src, recon, prm, q, qm, cdfs, jobs, threads=1):
 
     _chunked(n, threads, run)
     return res, cf, rec
+
+
+def quad32_luma(src, recon, prm, q, qm, cdfs, jobs, threads=1):
+    """rd_pick_luma64's four-TX_32X32 leg of n (64x64 block, mode, delta) jobs: the results."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.QUAD32_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.QUAD32_RESULT_DTYPE)
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+
+    def run(lo, hi):
+        assert load().or_quad32_luma(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs),
+                                     p(jobs[lo:hi]), hi - lo, p(res[lo:hi])) == 0
+
+    _chunked(n, threads, run)
+    return res
 
 
 def luma_palette(src, w, h, pos, opts, bd=8):
