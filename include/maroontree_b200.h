@@ -673,6 +673,57 @@ int mt_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_
                    const uint8_t* qm_row, const mt_coef_costs* costs, const mt_quad32_job* jobs, int32_t n,
                    mt_quad32_result* results);
 
+/* The 64x64 leaf's sixteen-TX_16X16 leg (rd_pick_luma64's tx_depth-2 trial,
+ * src/coder/block64.rs:1983-2010, on in the shipped tuning as tx64_depth2,
+ * through grid16_luma_pass, :1670-1805): for the winning (mode, delta) of a
+ * 64x64 block, the sixteen 16x16 transforms in raster order, each predicted at
+ * 16x16 from the block's running reconstruction with the per-transform edge
+ * flags (first row: top-right when the block has a row above and the
+ * transform is not the last column or the block has its top-right; other
+ * rows: not the last column; first column: bottom-left when the block has a
+ * column on its left and the transform is not the last row or the block has
+ * its bottom-left; other columns: none), TX_16X16 DCT_DCT with the QM and
+ * trellis_optimize_ctx in the dc_sign context of the transform's four above
+ * and four left coefficient-context bytes (dc_sign_ctx_span), the inverse,
+ * the distortion sse_recon x K_PART_LAMBDA, and luma_bits_ctx_bounded in the
+ * txb_skip context skip_ctx_split of the same bytes with the DCT_DCT symbol
+ * (1 in the TX_16X16 intra set) of the mode's tx-type CDF; the transform's
+ * coef_res_ctx then fills its four above and four left bytes.  dist and bits
+ * are f32 sums in raster order; total = (rd_lambda x mode_bits [+ rd_lambda x
+ * delta_bits]) + (dist + rd_lambda x bits) + rd_lambda x depth_bits.  Costs /
+ * qm row: the TX_16X16 slice and 16x16 row; skip_bits[ctx]: the TX_16X16
+ * class's pair per txb_skip context.  Rejected jobs (outside the frame, a bad
+ * mode / delta) get total, dist and bits +inf, sse 0. */
+typedef struct mt_grid16_job {
+  uint16_t px, py;          /* 64x64 block origin */
+  uint8_t mode;             /* MT_*_PRED */
+  int8_t angle_delta;       /* -3..3, directional modes only */
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL of the 64x64 block, MT_CAND_FILTER_TYPE */
+  uint8_t reserved;
+  uint8_t a_coef[16];       /* above coefficient contexts of the block's sixteen 4-sample columns */
+  uint8_t l_coef[16];       /* left coefficient contexts of its sixteen 4-sample rows */
+  float mode_bits;          /* mode_bits(px, py, mode) */
+  float delta_bits;         /* the angle-delta symbol's bits (read for directional modes) */
+  float depth_bits;         /* tx_depth64_bits(2) - tx_depth64_bits(1) */
+} mt_grid16_job;
+typedef struct mt_grid16_result {
+  float total;              /* the tx_depth-2 total */
+  float dist;               /* sum of the transforms' sse x K_PART_LAMBDA */
+  float bits;               /* sum of their coefficient bits */
+  uint32_t reserved;
+  int64_t sse;              /* sum of their sse_recon */
+} mt_grid16_result;
+/* Device form.  d_cf (optional): n x 4096 int32, transform t's levels
+ * (column-major, as the 16x16 leaf's) at t * 256, raster order. */
+int mt_grid16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_grid16_job* d_jobs, int32_t n, mt_grid16_result* d_results, int32_t* d_cf,
+                          void* stream);
+/* Host-buffer form of mt_grid16_luma_device. */
+int mt_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_grid16_job* jobs, int32_t n,
+                   mt_grid16_result* results, int32_t* cf_out);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

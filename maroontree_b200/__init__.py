@@ -407,6 +407,22 @@ def quad32_luma(src, recon, prm, quant, qmrow, costs, jobs):
     return res
 
 
+def grid16_luma(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False):
+    """The 64x64 leaf's sixteen-TX_16X16 leg (``mt_grid16_luma``); qmrow / costs
+    are the 16x16 row and the TX_16X16 slice.  Returns (results, levels or None),
+    levels n x 4096 with transform t at t * 256."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.GRID16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.GRID16_RESULT_DTYPE)
+    cf = np.zeros((n, 4096), np.int32) if want_cf else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_grid16_luma(ptr(src), ptr(recon), C.byref(prm), C.byref(quant), ptr(qm), C.byref(costs),
+                                 ptr(jobs), n, ptr(res), ptr(cf)), "mt_grid16_luma")
+    return res, cf
+
+
 def split16_luma_device(d_src, d_recon, prm, quant, d_qm, d_costs, d_jobs, n, d_results, d_cf=None, d_rec=None,
                         stream=0):
     _check(load().mt_split16_luma_device(ptr(d_src), ptr(d_recon), C.byref(prm), C.byref(quant), ptr(d_qm),

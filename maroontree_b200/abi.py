@@ -106,6 +106,13 @@ QUAD32_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("ang
 QUAD32_RESULT_DTYPE = np.dtype([("total", "<f4"), ("bits", "<f4", (4,)), ("reserved", "<u4"), ("sse", "<i8", (4,))],
                                align=True)
 assert QUAD32_JOB_DTYPE.itemsize == 20 and QUAD32_RESULT_DTYPE.itemsize == 56
+# mt_grid16_job / mt_grid16_result.
+GRID16_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"),
+                             ("reserved", "u1"), ("a_coef", "u1", (16,)), ("l_coef", "u1", (16,)),
+                             ("mode_bits", "<f4"), ("delta_bits", "<f4"), ("depth_bits", "<f4")], align=True)
+GRID16_RESULT_DTYPE = np.dtype([("total", "<f4"), ("dist", "<f4"), ("bits", "<f4"), ("reserved", "<u4"),
+                                ("sse", "<i8")], align=True)
+assert GRID16_JOB_DTYPE.itemsize == 52 and GRID16_RESULT_DTYPE.itemsize == 24
 CFL_BLOCK_DTYPE = np.dtype([("cx", "<u2"), ("cy", "<u2"), ("dc", "<i2", (2,))])
 assert CFL_BLOCK_DTYPE.itemsize == 8
 
@@ -418,6 +425,10 @@ def _bind(lib):
                                             C.c_int32, _P, _P]),
         "mt_quad32_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                      _P, C.c_int32, _P]),
+        "mt_grid16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
+                                            C.c_int32, _P, _P, _P]),
+        "mt_grid16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
+                                     _P, C.c_int32, _P, _P]),
         "mt_leaf8": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
                                C.c_int32, C.c_int32, _P, _P, _P]),
         "mt_split16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
@@ -475,6 +486,7 @@ EXPORTED_SYMBOLS = (
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
     "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
     "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
+    "mt_grid16_luma_device", "mt_grid16_luma",
 )
 
 

@@ -325,6 +325,141 @@ __global__ void __launch_bounds__(kLeafThreads) quad32_kernel(
   r.total = total;
 }
 
+// The 64x64 leaf's sixteen-TX_16X16 leg (rd_pick_luma64's tx_depth-2 trial,
+// src/coder/block64.rs:1983-2010, through grid16_luma_pass, :1670-1805): the
+// transforms in raster order, each predicted at 16x16 through the job's 64x64
+// patch with the per-transform edge flags, TX_16X16 DCT_DCT with the QM and
+// trellis_optimize_ctx in the dc_sign context of its four above / four left
+// context bytes, the inverse, sse_recon x K_PART_LAMBDA, and the bounded rate
+// walk in the txb_skip context skip_ctx_split of the same bytes with the
+// DCT_DCT symbol (1) of the mode's TX_16X16 tx-type CDF; coef_res_ctx then
+// fills the transform's context bytes.  total = mode cost + (dist + mlam x
+// bits) + mlam x depth_bits, f32 in that order.
+__global__ void __launch_bounds__(kLeafThreads) grid16_kernel(
+    const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_grid16_job* __restrict__ jobs, int n, mt_grid16_result* __restrict__ res, int32_t* __restrict__ cf_out) {
+  __shared__ mt_coef_costs sT;
+  constexpr int NN = 256;
+  __shared__ uint8_t sQm[NN];
+  __shared__ float sQs[NN];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    for (int i = threadIdx.x; i < NN; i += blockDim.x) {
+      const int w = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)w;
+      sQs[i] = fwd_qm_scale(w);
+    }
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_quant& q = a.q;
+  const mt_coef_costs& T = sT;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const mt_grid16_job jb = jobs[j];
+  mt_grid16_result& r = res[j];
+  const bool directional = jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED;
+  const bool ok = jb.px + 64 <= p.frame_w && jb.py + 64 <= p.frame_h && jb.mode <= MT_PAETH_PRED &&
+                  jb.angle_delta >= -3 && jb.angle_delta <= 3 && (jb.angle_delta == 0 || directional);
+  r.reserved = 0;
+  if (!ok) {
+    r.total = r.dist = r.bits = __int_as_float(0x7f800000);
+    r.sse = 0;
+    if (cf_out)
+      for (int i = 0; i < 4096; i++) cf_out[(size_t)j * 4096 + i] = 0;
+    return;
+  }
+  LeafWork<16> w;
+  uint16_t patch[64 * 64];
+  for (int y = 0; y < 64; y++)
+    for (int x = 0; x < 64; x++) patch[y * 64 + x] = rec[(size_t)(jb.py + y) * p.stride + jb.px + x];
+  const Patch64Read rd{rec, p.stride, jb.px, jb.py, patch};
+  uint8_t actx[16], lctx[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    actx[i] = jb.a_coef[i];
+    lctx[i] = jb.l_coef[i];
+  }
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float dcq = (float)q.dc_q, acq = (float)q.ac_q, mlam = p.rd_lambda;
+  const bool qm_full = q.qm_level >= 5;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const bool ft = jb.flags & MT_CAND_FILTER_TYPE;
+  float* tf = reinterpret_cast<float*>(w.u);
+  int32_t* tmp = w.u + NN;
+  int16_t* cf = w.cfs[0];
+  int16_t* rr = w.rrs[0];
+  float dist = 0.0f, bits = 0.0f;
+  long long sse_sum = 0;
+#pragma unroll 1
+  for (int t = 0; t < 16; t++) {
+    const int tx = t & 3, ty = t >> 2;
+    const int sx = tx * 16, sy = ty * 16, bx = jb.px + sx, by = jb.py + sy;
+    const bool tr = ty == 0 ? (jb.py > 0 && (tx < 3 || have_tr)) : tx < 3;
+    const bool bl = tx == 0 && jb.px > 0 && (ty < 3 || have_bl);
+    predict_sq_at<16>(rd, p.frame_w, p.frame_h, bx, by, jb.mode, jb.angle_delta, tr, bl, ft, p.bd, w.pred, w.u);
+#pragma unroll 8
+    for (int i = 0; i < NN; i++)
+      w.resid[i] = (int16_t)((int32_t)src[(size_t)(by + (i >> 4)) * p.stride + bx + (i & 15)] - w.pred[i]);
+    uint32_t la = 0, ll = 0;
+    int s = -8;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      la |= actx[tx * 4 + k];
+      ll |= lctx[ty * 4 + k];
+      s += (actx[tx * 4 + k] >> 6) + (lctx[ty * 4 + k] >> 6);
+    }
+    const int sk = kSkipCtxTbl[min(la & 0x3fu, 4u)][min(ll & 0x3fu, 4u)];
+    const int ds = (s != 0) + (s > 0);
+    fwd16x16(w.resid, MT_TX_DCT_DCT, q, cf, tf, tmp);
+    if (qm) apply_qm(cf, tf, sQs, NN);
+    if (a.lambda > 0.0f) trellis_ctx<16>(cf, tf, dcq, acq, a.lambda, T, ds, qm, qm_full, p.band_tilt, w.tr);
+    inv16x16(cf, MT_TX_DCT_DCT, q, qm, rr, tmp);
+    ErrBlock<int16_t, int16_t> eb;
+    eb.src = src + (size_t)by * p.stride + bx;
+    eb.stride = p.stride;
+    eb.pred = w.pred;
+    eb.resid = rr;
+    eb.w = 16;
+    eb.vw = min(max(vis_w - bx, 0), 16);
+    eb.vh = min(max(vis_h - by, 0), 16);
+    eb.maxv = maxv;
+    const long long sse = sse_recon_block(eb, p.wsse_scale);
+    dist = __fadd_rn(dist, __fmul_rn(__ll2float_rn(sse), 2.775f));  // proxy_wsse: K_PART_LAMBDA
+    sse_sum += sse;
+    const float skip1 = p.use_skip_bits ? p.skip_bits[sk][0] : 0.0f;
+    const float skip0 = p.use_skip_bits ? p.skip_bits[sk][1] : 0.0f;
+    bits = __fadd_rn(bits, rate_bounded<16>(cf, T, sk, ds, jb.mode, 1, p.use_skip_bits != 0, skip1, skip0,
+                                            __int_as_float(0x7f800000), w.lv));
+    const uint8_t rc = coef_res_ctx_w<16>(cf);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      actx[tx * 4 + k] = rc;
+      lctx[ty * 4 + k] = rc;
+    }
+#pragma unroll 8
+    for (int i = 0; i < NN; i++)
+      patch[(sy + (i >> 4)) * 64 + sx + (i & 15)] = (uint16_t)clampi((int32_t)w.pred[i] + rr[i], 0, maxv);
+    if (cf_out) {
+      int4* o = reinterpret_cast<int4*>(cf_out + (size_t)j * 4096 + t * NN);
+#pragma unroll 4
+      for (int i = 0; i < NN / 4; i++) o[i] = make_int4(cf[4 * i], cf[4 * i + 1], cf[4 * i + 2], cf[4 * i + 3]);
+    }
+  }
+  float total = __fmul_rn(mlam, jb.mode_bits);
+  if (directional) total = __fadd_rn(total, __fmul_rn(mlam, jb.delta_bits));
+  total = __fadd_rn(total, __fadd_rn(dist, __fmul_rn(mlam, bits)));
+  r.total = __fadd_rn(total, __fmul_rn(mlam, jb.depth_bits));
+  r.dist = dist;
+  r.bits = bits;
+  r.sse = sse_sum;
+}
+
 int check(const mt_split16_params* p, const mt_quant* q, int32_t n) {
   if (!p || !q || n < 0) return MT_ERR_INVALID_INPUT;
   if (p->bd != 8) return MT_ERR_UNSUPPORTED;
@@ -377,6 +512,25 @@ int quad32_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split
   quad32_kernel<<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
                   reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
                                                             d_results);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int grid16_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm, const mt_quant* quant,
+                  const uint8_t* d_qm_row, const mt_coef_costs* d_costs, const mt_grid16_job* d_jobs, int32_t n,
+                  mt_grid16_result* d_results, int32_t* d_cf, void* stream) {
+  const int rc = check(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!d_src || !d_recon || !d_costs || !d_jobs || !d_results) return MT_ERR_INVALID_INPUT;
+  LeafArgs a;
+  a.p = *prm;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
+  grid16_kernel<<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+                  reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
+                                                            d_results, d_cf);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
@@ -472,6 +626,49 @@ int mt_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_
                        reinterpret_cast<const mt_quad32_job*>(d + o_jobs), n,
                        reinterpret_cast<mt_quad32_result*>(d + o_res), nullptr);
     if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_quad32_result), cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_grid16_luma_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16_params* prm,
+                          const mt_quant* quant, const uint8_t* d_qm_row, const mt_coef_costs* d_costs,
+                          const mt_grid16_job* d_jobs, int32_t n, mt_grid16_result* d_results, int32_t* d_cf,
+                          void* stream) {
+  return grid16_device(d_src, d_recon, prm, quant, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, stream);
+}
+
+int mt_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
+                   const uint8_t* qm_row, const mt_coef_costs* costs, const mt_grid16_job* jobs, int32_t n,
+                   mt_grid16_result* results, int32_t* cf_out) {
+  int rc = check(prm, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!src || !recon || !costs || !jobs || !results) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * sizeof(uint16_t);
+  const size_t o_src = 0, o_rec = up256(plane), o_qm = o_rec + up256(plane), o_cost = o_qm + up256(256);
+  const size_t o_jobs = o_cost + up256(sizeof(mt_coef_costs));
+  const size_t o_res = o_jobs + up256((size_t)n * sizeof(mt_grid16_job));
+  const size_t o_cf = o_res + up256((size_t)n * sizeof(mt_grid16_result));
+  const size_t total = o_cf + (cf_out ? up256((size_t)n * 4096 * 4) : 0);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_src, src, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rec, recon, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 256, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_cost, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_jobs, jobs, (size_t)n * sizeof(mt_grid16_job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    rc = grid16_device(reinterpret_cast<const uint16_t*>(d + o_src), reinterpret_cast<const uint16_t*>(d + o_rec),
+                       prm, quant, has_qm ? d + o_qm : nullptr, reinterpret_cast<const mt_coef_costs*>(d + o_cost),
+                       reinterpret_cast<const mt_grid16_job*>(d + o_jobs), n,
+                       reinterpret_cast<mt_grid16_result*>(d + o_res),
+                       cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(results, d + o_res, (size_t)n * sizeof(mt_grid16_result), cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out)
+      e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 4096 * 4, cudaMemcpyDeviceToHost);
   }
   cudaFree(d);
   if (rc != MT_OK) return rc;

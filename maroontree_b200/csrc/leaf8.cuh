@@ -466,6 +466,28 @@ __device__ float rate_1d(const C* __restrict__ cf, bool vertical, const mt_coef_
   return bits;
 }
 
+// The dav1d txb_skip context table of skip_ctx_split
+// (src/coder/lossy_state.rs:1367-1386), indexed by the capped ORs of the above
+// and left coefficient-context bytes.
+__constant__ uint8_t kSkipCtxTbl[5][5] = {
+    {1, 2, 2, 2, 3}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {3, 5, 5, 5, 6}};
+
+// coef_res_ctx of a W x W transform (levels column-major, the default scan).
+template <int W, typename C>
+__device__ __forceinline__ uint8_t coef_res_ctx_w(const C* __restrict__ cf) {
+  int eob = -1;
+  for (int i = W * W - 1; i >= 0; i--)
+    if (cf[scan_rc<W>(i)] != 0) {
+      eob = i;
+      break;
+    }
+  if (eob < 0) return 0x40;
+  uint32_t cul = 0;
+  for (int i = 0; i <= eob && cul < 63u; i++) cul += uabs(cf[scan_rc<W>(i)]);
+  const uint32_t dcb = cf[0] == 0 ? 0x40u : (cf[0] < 0 ? 0u : 0x80u);
+  return (uint8_t)(min(cul, 63u) | dcb);
+}
+
 // coef_res_ctx: min(cumulative level, 63) | the dc-sign marker (0x40 zero,
 // 0x00 negative, 0x80 positive), or 0x40 for an all-zero block.
 template <typename C>

@@ -73,11 +73,9 @@ __device__ __forceinline__ bool job_ok(const mt_split16_job& jb, int fw, int fh)
   return jb.angle_delta == 0 || (jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED);
 }
 
-// lossy_state.rs:1367-1386 skip_ctx_split (2 x 2 span, the dav1d skip_ctx
-// table indexed by the OR of the above / left context bytes without the
-// dc-sign bits, each capped at 4) and :1388-1405 dc_sign_ctx_span.
-__constant__ uint8_t kSkipCtxTbl[5][5] = {
-    {1, 2, 2, 2, 3}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {3, 5, 5, 5, 6}};
+// lossy_state.rs:1367-1386 skip_ctx_split (2 x 2 span; kSkipCtxTbl indexed
+// by the OR of the above / left context bytes without the dc-sign bits, each
+// capped at 4) and :1388-1405 dc_sign_ctx_span.
 __device__ __forceinline__ int skip_ctx_split2(uint32_t a0, uint32_t a1, uint32_t l0, uint32_t l1) {
   const uint32_t la = (a0 | a1) & 0x3f, ll = (l0 | l1) & 0x3f;
   return kSkipCtxTbl[min(la, 4u)][min(ll, 4u)];

@@ -156,6 +156,11 @@ int or_leaf16(const uint16_t* src, const uint16_t* recon, const mt_split16_param
 int or_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                    const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_quad32_job* jobs, int32_t n,
                    mt_quad32_result* results);
+/* block64.rs rd_pick_luma64's tx_depth-2 trial (:1983-2010, grid16_luma_pass :1670-1805) per (64x64 block,
+ * mode, delta); cf_out (optional): n x 4096, transform t's levels at t * 256. */
+int or_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                   const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_grid16_job* jobs, int32_t n,
+                   mt_grid16_result* results, int32_t* cf_out);
 /* dct1d_32_i32 in place on 32 values. */
 void or_dct1d_32(int32_t* buf);
 /* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */

@@ -1141,6 +1141,102 @@ int or_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_
   return MT_OK;
 }
 
+// rd_pick_luma64's tx_depth-2 trial (src/coder/block64.rs:1983-2010) through
+// grid16_luma_pass (:1670-1805): sixteen TX_16X16 in raster order on one
+// (mode, delta), the coefficient contexts carried between transforms.
+int or_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
+                   const uint8_t* qm, const mt_coef_cdfs* cd, const mt_grid16_job* jobs, int32_t n,
+                   mt_grid16_result* results, int32_t* cf_out) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const uint16_t* scan = or_default_scan(16);
+  const float dcq = (float)q->dc_q, acq = (float)q->ac_q, mlam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  std::vector<uint16_t> work(recon, recon + (size_t)p->stride * p->frame_h);
+  std::vector<int32_t> pred(256), resid(256), cf(256), rr(256);
+  std::vector<float> tf(256);
+  for (int i = 0; i < n; i++) {
+    const mt_grid16_job& jb = jobs[i];
+    mt_grid16_result* r = &results[i];
+    r->reserved = 0;
+    const bool directional = jb.mode >= MT_V_PRED && jb.mode <= MT_D67_PRED;
+    const bool bad = jb.px + 64 > p->frame_w || jb.py + 64 > p->frame_h || jb.mode > MT_PAETH_PRED ||
+                     jb.angle_delta < -3 || jb.angle_delta > 3 || (jb.angle_delta != 0 && !directional);
+    if (bad) {
+      r->total = r->dist = r->bits = INFINITY;
+      r->sse = 0;
+      if (cf_out) memset(cf_out + (size_t)i * 4096, 0, 4096 * sizeof(int32_t));
+      continue;
+    }
+    uint8_t a[16], l[16];
+    memcpy(a, jb.a_coef, 16);
+    memcpy(l, jb.l_coef, 16);
+    const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+    const int ft = (jb.flags & MT_CAND_FILTER_TYPE) != 0;
+    float dist = 0.0f, bits = 0.0f;
+    int64_t sse_sum = 0;
+    for (int ty = 0; ty < 4; ty++)
+      for (int tx = 0; tx < 4; tx++) {
+        const int bx = jb.px + tx * 16, by = jb.py + ty * 16;
+        const bool tr = ty == 0 ? (jb.py > 0 && (tx < 3 || have_tr)) : tx < 3;
+        const bool bl = tx == 0 ? (jb.px > 0 && (ty < 3 || have_bl)) : false;
+        if (jb.mode == MT_DC_PRED) {
+          const int32_t d = or_dc_pred(work.data(), p->stride, bx, by, 16, 16, p->bd);
+          for (int t = 0; t < 256; t++) pred[t] = d;
+        } else {
+          or_intra_predict(work.data(), p->stride, bx, by, 16, 16, jb.mode, jb.angle_delta, tr, bl, p->frame_w,
+                           p->frame_h, ft, p->bd, pred.data());
+        }
+        for (int y = 0; y < 16; y++)
+          for (int x = 0; x < 16; x++)
+            resid[y * 16 + x] = (int32_t)src[(size_t)(by + y) * p->stride + bx + x] - pred[y * 16 + x];
+        // skip_ctx_split / dc_sign_ctx_span over the transform's four above
+        // and four left context bytes
+        uint8_t la = 0, ll = 0;
+        int s = 0;
+        for (int k = 0; k < 4; k++) {
+          la |= a[tx * 4 + k];
+          ll |= l[ty * 4 + k];
+          s += (a[tx * 4 + k] >> 6) - 1 + (l[ty * 4 + k] >> 6) - 1;
+        }
+        static const uint8_t kTbl[5][5] = {
+            {1, 2, 2, 2, 3}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {2, 4, 4, 4, 5}, {3, 5, 5, 5, 6}};
+        const int sk = kTbl[(la & 0x3f) < 4 ? (la & 0x3f) : 4][(ll & 0x3f) < 4 ? (ll & 0x3f) : 4];
+        const int ds = (s != 0) + (s > 0);
+        or_fwd_txfm_quant(resid.data(), MT_TX_DCT_DCT, 16, q, qm, cf.data(), tf.data());
+        or_trellis_optimize_ctx(cf.data(), tf.data(), dcq, acq, scan, 16, p->trellis_lambda0, cd, ds, qm,
+                                q->qm_level, p->band_tilt);
+        or_inv_txfm_dequant(cf.data(), MT_TX_DCT_DCT, 16, q, qm, rr.data());
+        const uint16_t pos[2] = {(uint16_t)bx, (uint16_t)by};
+        int64_t sse = 0;
+        or_sse_recon(src, p->stride, vis_w, vis_h, p->bd, pos, pred.data(), rr.data(), 1, 16, 16, p->wsse_scale, &sse);
+        dist += (float)sse * 2.775f;
+        sse_sum += sse;
+        // the DCT_DCT symbol of the TX_16X16 intra set is 1
+        bits += or_real_block_bits_bounded(cf.data(), scan, 16, 16, cd, sk, ds, jb.mode, 1, p->use_skip_bits,
+                                           p->skip_bits[sk], INFINITY);
+        const uint8_t rc = or_coef_res_ctx(cf.data(), scan, 256);
+        memset(a + tx * 4, rc, 4);
+        memset(l + ty * 4, rc, 4);
+        for (int y = 0; y < 16; y++)
+          for (int x = 0; x < 16; x++)
+            work[(size_t)(by + y) * p->stride + bx + x] = (uint16_t)clampi(pred[y * 16 + x] + rr[y * 16 + x], 0, maxv);
+        if (cf_out) memcpy(cf_out + (size_t)i * 4096 + (ty * 4 + tx) * 256, cf.data(), 256 * sizeof(int32_t));
+      }
+    float total = mlam * jb.mode_bits;
+    if (directional) total += mlam * jb.delta_bits;
+    total = total + (dist + mlam * bits);
+    total = total + mlam * jb.depth_bits;
+    r->total = total;
+    r->dist = dist;
+    r->bits = bits;
+    r->sse = sse_sum;
+    for (int y = 0; y < 64; y++)  // the next job predicts from the input reconstruction
+      memcpy(&work[(size_t)(jb.py + y) * p->stride + jb.px], &recon[(size_t)(jb.py + y) * p->stride + jb.px], 128);
+  }
+  return MT_OK;
+}
+
 // block32.rs:776-836 pick_luma32's mode-loop candidates.
 int or_leaf32(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
               const uint8_t* qm, const mt_coef_cdfs* cd, const mt_leaf8_job* jobs, int32_t n, mt_leaf8_result* results,

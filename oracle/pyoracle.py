@@ -88,6 +88,8 @@ def load():
             "or_dct1d_32": (None, [_P]),
             "or_quad32_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                          C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P]),
+            "or_grid16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
+                                         C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P]),
             "or_leaf32": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                     C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_leaf8": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -986,3 +988,23 @@ def emit_coeffs(levels, blocks):
                                    C.c_void_p]
     assert lib.or_emit_coeffs(p(levels), p(blocks), n, C.addressof(e), p(toks), cap, p(offsets), p(res)) == 0
     return toks[:offsets[n]].copy(), offsets, res[:n]
+
+
+def grid16_luma(src, recon, prm, q, qm, cdfs, jobs, threads=1, want_cf=False):
+    """rd_pick_luma64's sixteen-TX_16X16 leg of n (64x64 block, mode, delta) jobs:
+    (results, levels or None)."""
+    src = np.ascontiguousarray(src, np.uint16)
+    recon = np.ascontiguousarray(recon, np.uint16)
+    jobs = np.ascontiguousarray(jobs, abi.GRID16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.GRID16_RESULT_DTYPE)
+    cf = np.zeros((n, 4096), np.int32) if want_cf else None
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+
+    def run(lo, hi):
+        assert load().or_grid16_luma(p(src), p(recon), C.byref(prm), C.byref(q), p(qm), C.byref(cdfs),
+                                     p(jobs[lo:hi]), hi - lo, p(res[lo:hi]),
+                                     None if cf is None else p(cf[lo:hi])) == 0
+
+    _chunked(n, threads, run)
+    return res, cf

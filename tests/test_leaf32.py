@@ -152,95 +152,3 @@ def test_leaf32_at_config(mt_lib, oracle_lib, cuda, name):
     assert res.tobytes() == want.tobytes()
     assert np.array_equal(cf, wcf)
 
-
-def quad32_jobs(fw, fh, modes, deltas=(0,), seed=0):
-    """(64x64 block, mode, delta) jobs of the 64x64 leaf's four-TX_32X32 leg:
-    the 64-grid blocks, neighbour flags, random filter types, per-quadrant
-    dc_sign contexts and mode / delta bits."""
-    rng = np.random.default_rng(seed)
-    rows = []
-    for py in range(0, fh - 63, 64):
-        for px in range(0, fw - 63, 64):
-            fl = synth.block_flags(px, py, fw, fh, 64) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
-            dcs = rng.integers(0, 3, size=4)
-            for m in modes:
-                for d in (deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)):
-                    rows.append((px, py, m, d, fl, 0, tuple(int(v) for v in dcs), np.float32(rng.random() * 6 + 1),
-                                 np.float32(rng.random() * 3 + 0.5)))
-    return np.array(rows, abi.QUAD32_JOB_DTYPE)
-
-
-def test_quad32_oracle_glue(oracle_lib):
-    """rd_pick_luma64's four-TX_32X32 leg (block64.rs:1906-1958): quadrants in
-    raster order from the running reconstruction with quad_edges' flags, the
-    32x32 chain in each quadrant's dc_sign context, sse x K_PART_LAMBDA, and
-    the f32 total in the reference's order."""
-    import maroontree_b200 as mt
-
-    src, rec = _frame(128, 128, 51)
-    q = oracle_lib.quant_new(80, 8, 5)
-    qm = oracle_lib.qm_row(5, 0, 32)
-    c = oracle_lib.default_cdfs(oracle_lib.qcat(80), 32)
-    prm = mt.split16_params(128, 128, trellis_lambda0=0.05, rd_lambda=18.0, band_tilt=1.3, wsse_scale=1.0)
-    jobs = quad32_jobs(128, 128, (abi.DC_PRED, abi.V_PRED, abi.D157_PRED, abi.SMOOTH_PRED), deltas=(0, -2), seed=3)
-    scan = oracle_lib.default_scan(32)
-    f32 = np.float32
-    res = oracle_lib.quad32_luma(src, rec, prm, q, qm, c, jobs)
-    for i, jb in enumerate(jobs):
-        px, py, fl, m, d = int(jb["px"]), int(jb["py"]), int(jb["flags"]), int(jb["mode"]), int(jb["angle_delta"])
-        work = rec.copy()
-        total = f32(f32(18.0) * jb["mode_bits"])
-        if abi.V_PRED <= m <= abi.D67_PRED:
-            total = f32(total + f32(f32(18.0) * jb["delta_bits"]))
-        edges = [(py > 0, px > 0), (bool(fl & 1), False), (True, bool(fl & 2)), (False, False)]
-        for k, (sx, sy) in enumerate(((0, 0), (32, 0), (0, 32), (32, 32))):
-            bx, by = px + sx, py + sy
-            pred = oracle_lib.intra_predict(work, bx, by, 32, 32, m, d, edges[k][0], edges[k][1], bool(fl & 4)).ravel()
-            resid = src[by:by + 32, bx:bx + 32].astype(np.int32).ravel() - pred
-            lv, tf = oracle_lib.fwd_txfm_quant(resid, abi.TX_DCT_DCT, q, qm)
-            lv = oracle_lib.trellis_optimize_ctx(lv, tf, q, qm, c, int(jb["dcs_ctx"][k]), 0.05, band_tilt=1.3, n=32)
-            rr = oracle_lib.inv_txfm_dequant(lv, abi.TX_DCT_DCT, q, qm)
-            sse = int(oracle_lib.sse_recon(src, 128, 128, [(bx, by)], pred, rr, 32, 32, scale=1.0)[0])
-            bits = f32(oracle_lib.real_block_bits_bounded(lv, scan, 32, 32, c, 0, int(jb["dcs_ctx"][k]), -1, 0, INF))
-            assert res["sse"][i][k] == sse and f32(res["bits"][i][k]) == bits, (i, k)
-            total = f32(total + f32(f32(f32(sse) * f32(2.775)) + f32(f32(18.0) * bits)))
-            work[by:by + 32, bx:bx + 32] = np.clip(pred + rr, 0, 255).reshape(32, 32)
-        assert f32(res["total"][i]) == total, i
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("qidx,qm_level,wsse", [(70, 6, 1.0), (116, 15, 0.0), (30, 3, 0.75)])
-def test_quad32_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse):
-    import maroontree_b200 as mt
-
-    src, rec = _frame(320, 192, qidx + 9)
-    q = oracle_lib.quant_new(qidx, 8, qm_level)
-    qm = oracle_lib.qm_row(qm_level, 0, 32) if qm_level < 15 else None
-    c = oracle_lib.default_cdfs(oracle_lib.qcat(qidx), 32)
-    jobs = quad32_jobs(320, 192, range(13), deltas=(-3, 0, 1), seed=qidx)
-    jobs["px"][3] = 280  # crosses the right edge: rejected
-    prm = mt.split16_params(320, 192, trellis_lambda0=0.05, rd_lambda=0.3 * qidx + 2.0, band_tilt=1.9,
-                            wsse_scale=wsse, vis=(311, 190))
-    res = mt_lib.quad32_luma(src, rec, prm, q, qm, mt_lib.coef_costs(c), jobs)
-    want = oracle_lib.quad32_luma(src, rec, prm, q, qm, c, jobs, threads=os.cpu_count() or 1)
-    assert res.tobytes() == want.tobytes()
-    assert np.isinf(res["total"][3]) and np.isfinite(res["total"][0])
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("name", ["C1", "C2q40", "C2q60", "C2q80"])
-def test_quad32_at_config(mt_lib, oracle_lib, cuda, name):
-    """Every 64x64 block of the benchmark frames with the 13 modes (angle
-    deltas -3 / 0 / 3), the configuration's quantiser, QM and lambdas and the
-    default TX_32X32 CDFs."""
-    import configs
-
-    wl = configs.workload(name)
-    qm = configs.qm(mt_lib, wl, 32)
-    c = configs.cdfs(mt_lib, wl, 32)
-    jobs = quad32_jobs(wl.w, wl.h, range(13), deltas=(-3, 0, 3), seed=wl.qidx)
-    prm = mt_lib.split16_params(wl.w, wl.h, trellis_lambda0=wl.lam.trellis_lambda0, rd_lambda=wl.lam.mode_lambda,
-                                band_tilt=0.0, wsse_scale=1.0)
-    res = mt_lib.quad32_luma(wl.src, wl.rec, prm, wl.q, qm, mt_lib.coef_costs(c), jobs)
-    want = oracle_lib.quad32_luma(wl.src, wl.rec, prm, wl.q, qm, c, jobs, threads=configs.THREADS)
-    assert res.tobytes() == want.tobytes()
