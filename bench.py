@@ -528,6 +528,77 @@ def measure_leaf8(dev, wl, refine, reps=5, cpu=True, n16=False, n32=False):
     return out
 
 
+def measure_leaf64(dev, wl, grid, reps=5, cpu=True):
+    """The 64x64 leaf's luma legs over the same 1080p luma: the four-TX_32X32
+    candidate leg (480 blocks x 13 modes, four TX_32X32 with
+    trellis_optimize_ctx each) or the sixteen-TX_16X16 tx_depth-2 leg on one
+    mode per block (480 blocks, sixteen TX_16X16 each, the modes spread over
+    the blocks).  Device time with CUDA events after an L2 flush; the oracle on
+    all host cores over the same jobs."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    q = wl["q"]
+    size = 16 if grid else 32
+    qm = mt.qm_row(wl["qm_level"], 0, size)
+    cdfs = mt.coef_cdfs_default(mt.qcat(wl["qidx"]), size, size, 0)
+    costs = mt.coef_costs(cdfs)
+    jobs = synth.leaf64_jobs(W, H, MODES, seed=SEED, grid=grid)
+    if grid:  # one (winning) mode per block
+        nb = len(jobs) // len(MODES)
+        jobs = jobs[np.arange(nb) + nb * (np.arange(nb) % len(MODES))]
+    n = len(jobs)
+    prm = mt.split16_params(W, H, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].lambda_d,
+                            band_tilt=1.9, wsse_scale=1.0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d_src, d_rec, d_qm, d_costs, d_jobs = (t(wl["src"]), t(wl["rec"]), t(qm), t(np.frombuffer(bytes(costs), np.uint8)),
+                                           t(jobs))
+    rdt = abi.GRID16_RESULT_DTYPE if grid else abi.QUAD32_RESULT_DTYPE
+    d_res = torch.empty(n * rdt.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    lib = mt.load()
+
+    def launch():
+        args = [d_src.data_ptr(), d_rec.data_ptr(), C.byref(prm), C.byref(q), d_qm.data_ptr(), d_costs.data_ptr(),
+                d_jobs.data_ptr(), n, d_res.data_ptr()]
+        rc = lib.mt_grid16_luma_device(*args, None, None) if grid else lib.mt_quad32_luma_device(*args, None)
+        assert rc == 0, rc
+
+    for _ in range(3):
+        launch()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(200_000)
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    step = float(np.median(ms))
+    what = ("leaf64 tx_depth-2 leg 1920x1080 luma, 480 blocks x 1 mode (sixteen TX_16X16)" if grid else
+            "leaf64 four-TX_32X32 leg 1920x1080 luma, 480 blocks x 13 modes")
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n, "workload": what}
+    if cpu:
+        from oracle import pyoracle as po
+
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        if grid:
+            po.grid16_luma(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, threads=threads)
+        else:
+            po.quad32_luma(wl["src"], wl["rec"], prm, q, qm, cdfs, jobs, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                               "sample": f"all {n} jobs ({dt:.2f} s)"}
+    return out
+
+
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -997,6 +1068,8 @@ def run_ours(args):
         leaf8["luma16"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n16=True)
         leaf8["refine16"] = measure_leaf8(dev, wl, True, cpu=not nocpu, n16=True)
         leaf8["luma32"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n32=True)
+        leaf8["quad32_64"] = measure_leaf64(dev, wl, False, cpu=not nocpu)
+        leaf8["grid16_64"] = measure_leaf64(dev, wl, True, cpu=not nocpu)
         secondary["leaf8"] = leaf8
     if rank == 0 and not nocpu:
         from oracle import build as obuild

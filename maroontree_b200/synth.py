@@ -500,6 +500,38 @@ def split16_jobs(fw, fh, modes, deltas=(0,), seed=0, n=16):
     return np.array(rows, abi.SPLIT16_JOB_DTYPE)
 
 
+def leaf64_jobs(fw, fh, modes, deltas=(0,), seed=0, grid=False):
+    """(64x64 block, mode, delta) jobs of the 64x64 leaf's legs, mode-major:
+    the four-TX_32X32 leg (mt_quad32_job: random per-quadrant dc_sign contexts)
+    or, grid=True, the sixteen-TX_16X16 leg (mt_grid16_job: above / left
+    coefficient-context bytes shaped like coef_res_ctx's, tx_depth bits)."""
+    rng = np.random.default_rng(seed)
+    bys, bxs = np.meshgrid(np.arange(0, fh - 63, 64), np.arange(0, fw - 63, 64), indexing="ij")
+    px, py = bxs.ravel(), bys.ravel()
+    nb = len(px)
+    flags = np.array([block_flags(int(x), int(y), fw, fh, 64) for x, y in zip(px, py)], np.uint8)
+    flags |= np.where(rng.random(nb) < 0.5, abi.CAND_FILTER_TYPE, 0).astype(np.uint8)
+
+    def ctx_bytes():
+        b = rng.integers(0, 64, size=(nb, 16)) | rng.choice([0x00, 0x40, 0x80], size=(nb, 16))
+        return np.where(rng.random((nb, 16)) < 0.3, 0x40, b).astype(np.uint8)
+
+    a, l = ctx_bytes(), ctx_bytes()
+    dcs = rng.integers(0, 3, size=(nb, 4)).astype(np.uint8)
+    rows = []
+    for m in modes:
+        for d in (deltas if abi.V_PRED <= m <= abi.D67_PRED else (0,)):
+            mb = (rng.random(nb) * 6 + 1).astype(np.float32)
+            db = (rng.random(nb) * 3 + 0.5).astype(np.float32)
+            xb = (rng.random(nb) * 4 - 1).astype(np.float32)
+            for b in range(nb):
+                if grid:
+                    rows.append((px[b], py[b], m, d, flags[b], 0, a[b], l[b], mb[b], db[b], xb[b]))
+                else:
+                    rows.append((px[b], py[b], m, d, flags[b], 0, dcs[b], mb[b], db[b]))
+    return np.array(rows, abi.GRID16_JOB_DTYPE if grid else abi.QUAD32_JOB_DTYPE)
+
+
 def leaf8_jobs(fw, fh, modes, deltas=(0,), seed=0, n=8):
     """(n x n block, mode, delta) jobs of the leaf luma searches (n = 8 or 16),
     mode-major, with deterministic neighbour flags, random dc_sign contexts and
