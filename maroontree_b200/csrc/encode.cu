@@ -41,6 +41,7 @@
 #include "chain4.cuh"
 #include "chain8.cuh"
 #include "coop8.cuh"
+#include "pack.h"
 
 namespace mth {
 float scaled_trellis_lambda_host(float dc_q, float lambda0);
@@ -1023,6 +1024,25 @@ int decide_all(std::vector<Job>& jobs, Buffers& buf) {
 // Everything after the decisions for image i: the context bytes, the block
 // syntax walk, the coefficient tokens, the filters, range coding, headers
 // and container.
+// A CUDA event destroyed with its scope.
+struct EventGuard {
+  cudaEvent_t e = nullptr;
+  ~EventGuard() {
+    if (e) cudaEventDestroy(e);
+  }
+};
+
+// Host threads joined when their scope ends, on every return path.
+struct ThreadGroup {
+  std::vector<std::thread> v;
+  ~ThreadGroup() { join(); }
+  void join() {
+    for (std::thread& w : v)
+      if (w.joinable()) w.join();
+    v.clear();
+  }
+};
+
 int job_finish(Job& j, Buffers& buf, int i) {
   int rc = MT_OK;
   const cudaStream_t st = j.st;
@@ -1073,6 +1093,7 @@ int job_finish(Job& j, Buffers& buf, int i) {
   // (decode_tile: the above context cleared per tile, the left per SB row)
   std::vector<int> tile_first;  // first coded superblock of each tile
   std::vector<int> sb_unit;     // frame-raster 64x64 unit of each coded superblock
+  std::vector<size_t> sb_coef_first;  // first coefficient block of each coded superblock
   for (int r0 = 0; r0 < sb_rows; r0 += j.tile_sb_h)
     for (int c0 = 0; c0 < sb_cols; c0 += j.tile_sb_w) {
       const int r1 = std::min(r0 + j.tile_sb_h, sb_rows), c1 = std::min(c0 + j.tile_sb_w, sb_cols);
@@ -1083,6 +1104,7 @@ int job_finish(Job& j, Buffers& buf, int i) {
         for (int sc = c0; sc < c1; ++sc) {
           bs.sbs.emplace_back();
           bs.out = &bs.sbs.back();
+          sb_coef_first.push_back(blocks.size());
           sb_unit.push_back(sr * sb_cols + sc);
           int cp = -1;
           bs.node(1, sc * 8, sr * 8, 8, &cp, [&](int x8, int y8) {
@@ -1099,6 +1121,7 @@ int job_finish(Job& j, Buffers& buf, int i) {
       }
     }
   tile_first.push_back((int)bs.sbs.size());
+  sb_coef_first.push_back(blocks.size());
   // coefficient tokens of every block in one launch
   const int ncb = (int)blocks.size();
   mt_coef_block* d_blocks = buf.get<mt_coef_block>(i, kEmit, (size_t)ncb * (sizeof(mt_coef_block) + 8) + 8);
@@ -1122,6 +1145,12 @@ int job_finish(Job& j, Buffers& buf, int i) {
   std::vector<uint32_t> toks(total), offs((size_t)ncb + 1);
   if (cudaMemcpyAsync(toks.data(), d_tok, (size_t)total * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaMemcpyAsync(offs.data(), d_off, offs.size() * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return MT_ERR_DEVICE;
+  // the tokens are on the host once this event has passed; the filters
+  // carry on behind it on the stream
+  EventGuard tok_ev;
+  if (cudaEventCreateWithFlags(&tok_ev.e, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(tok_ev.e, st) != cudaSuccess)
     return MT_ERR_DEVICE;
   // deblocking (uniform 8x8 blocks and transforms) and the CDEF decision,
   // enqueued before the host splices the tokens
@@ -1163,29 +1192,33 @@ int job_finish(Job& j, Buffers& buf, int i) {
                                        m0 + 5 * (size_t)n4, &g, ly, luv, luv, d_db, st)) != MT_OK)
     return rc;
   cs.launches(mth::deblock_last_launches);
-  // splice the coefficient tokens into the superblock streams (the token copy
-  // has completed once the stream reaches the filters' first sync)
-  if (cudaStreamSynchronize(st) != cudaSuccess) return MT_ERR_DEVICE;
+  // phase 1 of the range coding (each token's store, with the CDF
+  // adaptation), one host thread per tile, reading the superblocks' syntax
+  // tokens and the coefficient blocks in place while the filters run
+  if (cudaEventSynchronize(tok_ev.e) != cudaSuccess) return MT_ERR_DEVICE;
   cs.d2h(4 + (size_t)total * 4 + offs.size() * 4);
-  std::vector<uint32_t> ops, sb_start(1, 0);
-  std::vector<int32_t> cdef_pt;
-  ops.reserve((size_t)total + (size_t)nb * 12);
-  size_t k = 0;
-  for (size_t sbi = 0; sbi < bs.sbs.size(); ++sbi) {
-    const size_t base = ops.size();
-    int32_t cp_spliced = -1;
-    for (size_t t = 0; t < bs.sbs[sbi].size(); ++t) {
-      if ((int)t == bs.cdef_points[sbi]) cp_spliced = (int32_t)(ops.size() - base);
-      const uint32_t tok = bs.sbs[sbi][t];
-      if (tok == BlockSyntax::kCoef) {
-        ops.insert(ops.end(), toks.begin() + offs[k], toks.begin() + offs[k + 1]);
-        ++k;
-      } else {
-        ops.push_back(tok);
-      }
-    }
-    sb_start.push_back((uint32_t)ops.size());
-    cdef_pt.push_back(cp_spliced);
+  const int ntiles = (int)tile_first.size() - 1;
+  std::vector<std::unique_ptr<mth::TileStores>> stores((size_t)ntiles);
+  size_t nstores = 0;
+  for (int t = 0; t < ntiles; ++t) {
+    const int f = tile_first[(size_t)t], l = tile_first[(size_t)t + 1];
+    const size_t k0 = sb_coef_first[(size_t)f], k1 = sb_coef_first[(size_t)l];
+    size_t n = (size_t)offs[k1] - offs[k0];
+    for (int sb = f; sb < l; ++sb) n += bs.sbs[(size_t)sb].size();
+    n -= k1 - k0;  // the placeholders
+    auto ts = std::make_unique<mth::TileStores>();
+    ts->st.resize(n);
+    ts->sb_end.assign((size_t)(l - f), 0);
+    ts->cdef_at.assign((size_t)(l - f), UINT32_MAX);
+    stores[(size_t)t] = std::move(ts);
+    nstores += n;
+  }
+  ThreadGroup tracers;  // joined on every return path
+  for (int t = 0; t < ntiles; ++t) {
+    const int f = tile_first[(size_t)t];
+    tracers.v.emplace_back(mth::trace_tile_stores, j.plan.base_q_idx, cfg->updating_cdf, &bs.sbs[(size_t)f],
+                         tile_first[(size_t)t + 1] - f, bs.cdef_points.data() + f, toks.data(), offs.data(),
+                         sb_coef_first[(size_t)f], stores[(size_t)t].get());
   }
   mt_cdef_params cp = {};
   cp.w8 = pw;
@@ -1223,28 +1256,28 @@ int job_finish(Job& j, Buffers& buf, int i) {
       return MT_ERR_DEVICE;
     cs.d2h((ny + 2 * nc) * 2);
   }
-  // each tile in one pass of its range coder, with each superblock's
-  // cdef_idx (its 64x64 unit's) at its read_cdef() point; tiles are coded
-  // independently, on threads of their own when there are several
-  const int ntiles = (int)tile_first.size() - 1;
+  // phase 2: each tile's coder over its stores, following phase 1, with each
+  // superblock's cdef_idx (its 64x64 unit's) at its read_cdef() point; tiles
+  // are coded independently, on threads of their own when there are several
   std::vector<uint8_t> sb_idx(sb_unit.size());
   for (size_t k2 = 0; k2 < sb_unit.size(); ++k2) sb_idx[k2] = grid[(size_t)sb_unit[k2]];
   std::vector<uint8_t*> tiles((size_t)ntiles, nullptr);
   std::vector<size_t> tile_lens((size_t)ntiles, 0);
   std::vector<int> tile_rc((size_t)ntiles, MT_OK);
-  auto pack = [&](int t) {
+  auto code = [&](int t) {
     const int f = tile_first[(size_t)t], n = tile_first[(size_t)t + 1] - f;
-    tile_rc[(size_t)t] = mt_pack_tile_filtered(j.plan.base_q_idx, cfg->updating_cdf, ops.data(), sb_start.data() + f,
-                                               cdef_pt.data() + f, n, dec.bits > 0 ? sb_idx.data() + f : nullptr,
-                                               dec.bits > 0 ? dec.bits : 0, &tiles[(size_t)t], &tile_lens[(size_t)t]);
+    tile_rc[(size_t)t] = mth::code_tile_stores(stores[(size_t)t].get(), n, cfg->updating_cdf,
+                                               dec.bits > 0 ? sb_idx.data() + f : nullptr, dec.bits > 0 ? dec.bits : 0,
+                                               &tiles[(size_t)t], &tile_lens[(size_t)t]);
   };
   if (ntiles == 1) {
-    pack(0);
+    code(0);
   } else {
-    std::vector<std::thread> workers;
-    for (int t = 0; t < ntiles; ++t) workers.emplace_back(pack, t);
-    for (std::thread& w : workers) w.join();
+    ThreadGroup coders;
+    for (int t = 0; t < ntiles; ++t) coders.v.emplace_back(code, t);
+    coders.join();
   }
+  tracers.join();
   auto free_tiles = [&]() {
     for (uint8_t* t : tiles) free(t);
   };
@@ -1312,7 +1345,7 @@ int job_finish(Job& j, Buffers& buf, int i) {
   ip.max_pic_average_light_level = cfg->max_pic_average_light_level;
   rc = mt_wrap_av1_image(obu, obu_len, &ip, j.out, j.out_len);
   free(obu);
-  if (j.stats) j.stats->tokens = (uint32_t)ops.size();
+  if (j.stats) j.stats->tokens = (uint32_t)nstores;
   cs.mark(3, st);
   cs.finish();
   return rc;

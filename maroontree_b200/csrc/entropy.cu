@@ -13,11 +13,18 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/maroontree_b200.h"
 #include "av1_cdfs.h"
+#include "pack.h"
+
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 namespace {
 
@@ -164,9 +171,52 @@ struct mt_range_encoder {
     trace_cdef.back() = (uint32_t)trace_ops.size();
   }
 
+  // store() over n recorded stores, with the coder state in locals and the
+  // output written through a raw pointer (each store emits at most two
+  // entries): the same arithmetic without the member round trips.
   void replay(const uint64_t* ops, size_t n) {
-    for (size_t i = 0; i < n; ++i)
-      store((uint32_t)(ops[i] >> 24), (uint32_t)((ops[i] >> 8) & 0xffff), (uint32_t)(ops[i] & 0xff));
+    if (tracing) {
+      for (size_t i = 0; i < n; ++i)
+        store((uint32_t)(ops[i] >> 24), (uint32_t)((ops[i] >> 8) & 0xffff), (uint32_t)(ops[i] & 0xff));
+      return;
+    }
+    const size_t base = precarry.size();
+    precarry.resize(base + 2 * n);
+    uint16_t* pc = precarry.data() + base;
+    uint32_t lo_s = low, r = rng;
+    int c_s = cnt;
+    for (size_t i = 0; i < n; ++i) {
+      const uint64_t op = ops[i];
+      const uint32_t fl = (uint32_t)(op >> 24), fh = (uint32_t)((op >> 8) & 0xffff), nms = (uint32_t)(op & 0xff);
+      uint32_t u = (((r >> 8) * (fl >> kProbShift)) >> (7 - kProbShift)) + kMinProb * nms;
+      u = fl >= 32768 ? r : u;
+      const uint32_t v = (((r >> 8) * (fh >> kProbShift)) >> (7 - kProbShift)) + kMinProb * (nms - 1);
+      const uint32_t nr = (u - v) & 0xffff;
+      uint32_t lo = (r - u) + lo_s;
+      int c = c_s;
+      const int d = clz16(nr);
+      int sh = c + d;
+      if (sh >= 0) {
+        c += 16;
+        uint32_t m = (1u << c) - 1;
+        if (sh >= 8) {
+          *pc++ = (uint16_t)(lo >> c);
+          lo &= m;
+          c -= 8;
+          m >>= 8;
+        }
+        *pc++ = (uint16_t)(lo >> c);
+        sh = c + d - 24;
+        lo &= m;
+      }
+      lo_s = lo << d;
+      r = (nr << d) & 0xffff;
+      c_s = sh;
+    }
+    precarry.resize((size_t)(pc - precarry.data()));
+    low = lo_s;
+    rng = (uint16_t)r;
+    cnt = (int16_t)c_s;
   }
 
   std::vector<uint8_t> done() {
@@ -375,6 +425,40 @@ void build_cdfs(int q, CdfSet& c, mt_cdf_slot_layout* L = nullptr) {
   L->nslots = at();
 }
 
+// The packers' CdfSet carries this many spare entries past its last CDF, so
+// that every CDF can be read and written back eight entries at a time.
+constexpr size_t kCdfPad = 16;
+
+// update_cdf on a CDF of the padded CdfSet: the same per-entry arithmetic
+// (entries below val move up towards 32768 by (32768 - c) >> rate, the others
+// down by c >> rate), eight 16-bit lanes at a time; lanes at or past the
+// counter are written back unchanged, and the counter is updated last.
+inline void update_cdf_padded(uint16_t* cdf, int n, int val) {
+#if defined(__SSE2__)
+  const uint32_t count = cdf[n - 1];
+  const uint32_t rate = 3 + (uint32_t)((n >> 1) < 2 ? (n >> 1) : 2) + (count >> 4);
+  const __m128i sh = _mm_cvtsi32_si128((int)rate);
+  const __m128i top = _mm_set1_epi16((short)0x8000);
+  const __m128i vv = _mm_set1_epi16((short)val), nn = _mm_set1_epi16((short)(n - 1));
+  __m128i idx = _mm_setr_epi16(0, 1, 2, 3, 4, 5, 6, 7);
+  for (int b = 0; b < n - 1; b += 8) {
+    __m128i* p = reinterpret_cast<__m128i*>(cdf + b);
+    const __m128i c = _mm_loadu_si128(p);
+    const __m128i up = _mm_add_epi16(c, _mm_srl_epi16(_mm_sub_epi16(top, c), sh));
+    const __m128i dn = _mm_sub_epi16(c, _mm_srl_epi16(c, sh));
+    const __m128i is_up = _mm_cmplt_epi16(idx, vv);
+    const __m128i live = _mm_cmplt_epi16(idx, nn);
+    __m128i r = _mm_or_si128(_mm_and_si128(is_up, up), _mm_andnot_si128(is_up, dn));
+    r = _mm_or_si128(_mm_and_si128(live, r), _mm_andnot_si128(live, c));
+    _mm_storeu_si128(p, r);
+    idx = _mm_add_epi16(idx, _mm_set1_epi16(8));
+  }
+  cdf[n - 1] = (uint16_t)(count + 1 - (count >> 5));
+#else
+  mt_range_encoder::update_cdf(cdf, n, val);
+#endif
+}
+
 // gather_split_prob_icdf (src/coeffs.rs:2927-2935): the edge partition's
 // split probability read from a live 10-symbol partition CDF.
 uint16_t gather_split_prob(const uint16_t* cdf, bool top) {
@@ -406,10 +490,8 @@ bool replay_tokens(mt_range_encoder& enc, CdfSet& c, const uint32_t* ops, uint32
       const uint32_t slot = (t >> 8) & 0xffff, s = t & 0xff;
       if (slot >= nslots || s >= lens[slot]) return false;
       uint16_t* cdf = data + off[slot];
-      if (tag == 0)
-        enc.encode_symbol((int)s, cdf, lens[slot]);
-      else
-        enc.encode_symbol_noupdate((int)s, cdf, lens[slot]);
+      enc.encode_symbol_noupdate((int)s, cdf, lens[slot]);
+      if (tag == 0 && enc.updating_cdf) update_cdf_padded(cdf, lens[slot], (int)s);
     } else if (tag == kTagBool) {
       enc.encode_bool((t & 1) != 0, (uint16_t)((t >> 1) & 0xffff));
     } else {  // gathered partition bool (tag 2)
@@ -526,6 +608,7 @@ int mt_pack_tile(uint8_t base_q_idx, int32_t updating_cdf, const uint32_t* ops, 
   int q = base_q_idx <= 20 ? 0 : base_q_idx <= 60 ? 1 : base_q_idx <= 120 ? 2 : 3;  // qcat
   CdfSet c;
   build_cdfs(q, c);
+  c.data.resize(c.data.size() + kCdfPad, 0);
   mt_range_encoder enc;
   enc.updating_cdf = updating_cdf != 0;
   enc.tracing = trace != nullptr;
@@ -559,6 +642,7 @@ int mt_pack_tile_filtered(uint8_t base_q_idx, int32_t updating_cdf, const uint32
   const int q = base_q_idx <= 20 ? 0 : base_q_idx <= 60 ? 1 : base_q_idx <= 120 ? 2 : 3;  // qcat
   CdfSet c;
   build_cdfs(q, c);
+  c.data.resize(c.data.size() + kCdfPad, 0);
   mt_range_encoder enc;
   enc.updating_cdf = updating_cdf != 0;
   if (nsb > 0) enc.precarry.reserve(sb_start[nsb] / 2 + 64);
@@ -606,3 +690,117 @@ int mt_replay_tile_with_filters(const mt_tile_trace* t, int32_t tile_x0, int32_t
 void mt_free(void* p) { free(p); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The tile packer in two phases for the encoder.  Every token is one store of
+// the range coder, and which store it is depends only on the token and the
+// adapted CDFs, never on the coder's state or on the cdef_idx literals (raw
+// bits, no CDF).  Phase 1 turns the superblocks' tokens into their stores
+// (fl, fh, nms, as the tile trace holds them) with the CDF adaptation, reading
+// the syntax tokens and the coefficient blocks they point to in place; phase 2
+// runs the coder over the stores with each superblock's cdef_idx inserted at
+// its read_cdef() point.  Phase 1 can start as soon as the tokens exist, before
+// the CDEF decision is made, and phase 2 follows it superblock by superblock
+// on another thread.  The bytes are those of mt_pack_tile_filtered over the
+// spliced token stream.
+
+namespace mth {
+
+constexpr uint32_t kCoefMarker = 0xFFFFFFFFu;
+
+// The store of one token against the live CDFs, with the CDF update; false
+// for a malformed token.
+inline bool token_store(uint32_t t, uint16_t* data, const uint32_t* off, const uint16_t* lens, size_t nslots,
+                        bool updating, uint64_t& st) {
+  const uint32_t tag = t & kTagMask;
+  if (tag == 0 || tag == kTagNoUpdate) {
+    const uint32_t slot = (t >> 8) & 0xffff, s = t & 0xff;
+    if (slot >= nslots || s >= lens[slot]) return false;
+    uint16_t* cdf = data + off[slot];
+    const uint32_t fl = s > 0 ? cdf[s - 1] : 32768u;
+    st = ((uint64_t)fl << 24) | ((uint64_t)cdf[s] << 8) | (uint64_t)(lens[slot] - s);
+    if (tag == 0 && updating) update_cdf_padded(cdf, lens[slot], (int)s);
+  } else {
+    uint32_t b, p;
+    if (tag == kTagBool) {
+      b = t & 1;
+      p = (t >> 1) & 0xffff;
+    } else {  // gathered partition bool
+      const uint32_t slot = (t >> 2) & 0xffff;
+      if (slot >= nslots || lens[slot] != 10) return false;
+      b = (t >> 1) & 1;
+      p = gather_split_prob(data + off[slot], (t & 1) != 0);
+    }
+    st = b ? (((uint64_t)p << 24) | 1u) : (((uint64_t)32768u << 24) | ((uint64_t)p << 8) | 2u);
+  }
+  return true;
+}
+
+void trace_tile_stores(uint8_t base_q_idx, int32_t updating_cdf, const std::vector<uint32_t>* sbs, int nsb,
+                       const int32_t* cdef_point, const uint32_t* toks, const uint32_t* offs, size_t first_coef,
+                       TileStores* out) {
+  const int q = base_q_idx <= 20 ? 0 : base_q_idx <= 60 ? 1 : base_q_idx <= 120 ? 2 : 3;  // qcat
+  CdfSet c;
+  build_cdfs(q, c);
+  c.data.resize(c.data.size() + kCdfPad, 0);
+  uint16_t* const data = c.data.data();
+  const uint32_t* const off = c.off.data();
+  const uint16_t* const lens = c.len.data();
+  const size_t nslots = c.off.size(), cap = out->st.size();
+  const bool upd = updating_cdf != 0;
+  uint64_t* const w = out->st.data();
+  size_t n = 0, k = first_coef;
+  for (int i = 0; i < nsb; ++i) {
+    const std::vector<uint32_t>& syn = sbs[i];
+    uint32_t at = UINT32_MAX;
+    bool ok = true;
+    for (size_t t = 0; t < syn.size() && ok; ++t) {
+      if ((int32_t)t == cdef_point[i]) at = (uint32_t)n;
+      const uint32_t tok = syn[t];
+      if (tok == kCoefMarker) {
+        const uint32_t a = offs[k], b = offs[k + 1];
+        ++k;
+        if (n + (b - a) > cap) ok = false;
+        for (uint32_t e = a; e < b && ok; ++e) ok = token_store(toks[e], data, off, lens, nslots, upd, w[n++]);
+      } else {
+        ok = n < cap && token_store(tok, data, off, lens, nslots, upd, w[n++]);
+      }
+    }
+    if (cdef_point[i] >= 0 && (size_t)cdef_point[i] == syn.size()) at = (uint32_t)n;
+    if (!ok) {
+      out->failed.store(true, std::memory_order_release);
+      out->done.store(nsb, std::memory_order_release);
+      return;
+    }
+    out->sb_end[(size_t)i] = (uint32_t)n;
+    out->cdef_at[(size_t)i] = at;
+    out->done.store(i + 1, std::memory_order_release);
+  }
+}
+
+int code_tile_stores(TileStores* in, int nsb, int32_t updating_cdf, const uint8_t* cdef_idx, int32_t cdef_bits,
+                     uint8_t** payload, size_t* payload_len) {
+  mt_range_encoder enc;
+  enc.updating_cdf = updating_cdf != 0;
+  enc.precarry.reserve(in->st.size() / 2 + 64);
+  const uint64_t* const st = in->st.data();
+  size_t a = 0;
+  for (int i = 0; i < nsb; ++i) {
+    // phase 1 always reaches nsb (failure included): the wait ends
+    while (in->done.load(std::memory_order_acquire) <= i) std::this_thread::yield();
+    if (in->failed.load(std::memory_order_acquire)) return MT_ERR_INVALID_INPUT;
+    const size_t b = in->sb_end[(size_t)i], p = in->cdef_at[(size_t)i];
+    if (p == UINT32_MAX || cdef_bits <= 0) {
+      enc.replay(st + a, b - a);
+    } else {
+      enc.replay(st + a, p - a);
+      enc.encode_literal(cdef_idx[i], (uint32_t)cdef_bits);
+      enc.replay(st + p, b - p);
+    }
+    a = b;
+  }
+  return out_bytes(enc.done(), payload, payload_len);
+}
+
+}  // namespace mth
+
