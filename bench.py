@@ -599,6 +599,78 @@ def measure_leaf64(dev, wl, grid, reps=5, cpu=True):
     return out
 
 
+def measure_uv16(dev, wl, reps=5, cpu=True):
+    """The 16x16 leaf's 4:2:0 chroma search (pick_uv16_420) over every 16x16
+    leaf of the 1080p frame (8,040 leaves: DC, CfL, 60 shortlist predictions
+    per plane, the 4 best priced in full) with the frame's chroma quantiser
+    and QM, the default chroma TX_8X8 and mode CDFs.  Device time with CUDA
+    events after an L2 flush; the oracle on all host cores over the same
+    leaves."""
+    import ctypes as C
+
+    import torch
+    import maroontree_b200 as mt
+    from maroontree_b200 import abi, synth
+
+    qidx = wl["qidx"]
+    qm_uv = mt.qm_levels(qidx, SUB)[1]
+    q = mt.quant_new_chroma(qidx, 0, 0, 8, qm_uv)
+    qm = mt.qm_row(qm_uv, 1, 8) if qm_uv < 15 else None
+    cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 1)
+    costs = mt.coef_costs(cdfs)
+    mcdfs = mt.uv_mode_cdfs_default()
+    mcost = mt.uv_mode_costs(mcdfs)
+    src, rec = synth.planes420(wl["rgb"], SEED)
+    cw, ch = src[1].shape[1], src[1].shape[0]
+    prm = mt.split16_params(cw, ch, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].mode_lambda,
+                            wsse_scale=1.0, vis=(W // 2, H // 2))
+    uvp = mt.uv16_params(src[0].shape[1], joint_k=4, angle_deltas=True)
+    jobs = synth.uv16_jobs(W, H, SEED)
+    n = len(jobs)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
+    d_p = [t(a) for a in (src[1], src[2], rec[1], rec[2], rec[0])]
+    d_qm = t(qm) if qm is not None else None
+    d_costs, d_mc, d_jobs = t(np.frombuffer(bytes(costs), np.uint8)), t(np.frombuffer(bytes(mcost), np.uint8)), t(jobs)
+    d_res = torch.empty(n * abi.UV16_RESULT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    lib = mt.load()
+
+    def launch():
+        rc = lib.mt_pick_uv16_420_device(*[a.data_ptr() for a in d_p], C.byref(prm), C.byref(uvp), C.byref(q),
+                                         None if d_qm is None else d_qm.data_ptr(), d_costs.data_ptr(),
+                                         d_mc.data_ptr(), d_jobs.data_ptr(), n, d_res.data_ptr(), None, None, None)
+        assert rc == 0, rc
+
+    for _ in range(3):
+        launch()
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(200_000)
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    step = float(np.median(ms))
+    out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n,
+           "workload": "pick_uv16_420 1920x1080 4:2:0, 8,040 16x16 leaves (DC, CfL, 60-entry SATD shortlist, 4 "
+                       "priced), frame chroma quantiser and QM"}
+    if cpu:
+        from oracle import pyoracle as po
+
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        po.pick_uv16_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, po.default_cdfs(mt.qcat(qidx), 8,
+                         plane=1), po.uv_mode_cdfs(), jobs, threads=threads)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
+                               "sample": f"all {n} leaves ({dt:.2f} s)"}
+    return out
+
+
 def measure_filters(dev, wl, hbm_peak, reps=5):
     """Device time of the frame-wide kernels on the 1080p 4:2:0 frame."""
     import ctypes as C
@@ -1070,6 +1142,7 @@ def run_ours(args):
         leaf8["luma32"] = measure_leaf8(dev, wl, False, cpu=not nocpu, n32=True)
         leaf8["quad32_64"] = measure_leaf64(dev, wl, False, cpu=not nocpu)
         leaf8["grid16_64"] = measure_leaf64(dev, wl, True, cpu=not nocpu)
+        secondary["uv16_420"] = measure_uv16(dev, wl, cpu=not nocpu)
         secondary["leaf8"] = leaf8
     if rank == 0 and not nocpu:
         from oracle import build as obuild

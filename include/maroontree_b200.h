@@ -724,6 +724,109 @@ int mt_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_
                    const uint8_t* qm_row, const mt_coef_costs* costs, const mt_grid16_job* jobs, int32_t n,
                    mt_grid16_result* results, int32_t* cf_out);
 
+/* ---- Chroma RD ----
+ * uv_mode_bits (src/coder/lossy_state.rs:1302-1349) prices a chroma mode from
+ * the decision CDFs: the CfL-allowed uv_mode CDF of the luma mode, the
+ * angle-delta CDF at delta 0 for a directional mode, and for CfL the joint
+ * sign and the per-plane alpha magnitudes (contexts by the other plane's
+ * sign); CfL with both alphas 0 is priced as DC.  CDFs in the inverse form of
+ * mt_coef_cdfs (one entry per symbol, the last 0). */
+#define MT_UV_CFL_PRED 13
+typedef struct mt_uv_mode_cdfs {
+  uint16_t uv_mode[13][14];    /* uv_mode with CfL allowed, per y mode */
+  uint16_t angle_delta[8][7];  /* per directional mode, V_PRED..D67_PRED */
+  uint16_t cfl_sign[8];
+  uint16_t cfl_alpha[6][16];
+} mt_uv_mode_cdfs;
+typedef struct mt_uv_mode_costs {  /* cdf_cost_with_table of every symbol of the same CDFs */
+  float uv_mode[13][14];
+  float angle_delta[8][7];
+  float cfl_sign[8];
+  float cfl_alpha[6][16];
+} mt_uv_mode_costs;
+/* The decision snapshot's CDFs (Cdfs::new, src/coder/cdfs.rs; the mode CDFs
+ * do not depend on the quantiser). */
+int mt_uv_mode_cdfs_default(mt_uv_mode_cdfs* out);
+int mt_uv_mode_costs_build(const mt_uv_mode_cdfs* cdfs, mt_uv_mode_costs* out);
+/* uv_mode_bits(y_mode, uv_mode, cfl ? Some([alpha_u, alpha_v]) : None). */
+float mt_uv_mode_bits(const mt_uv_mode_costs* costs, int32_t y_mode, int32_t uv_mode, int32_t cfl, int32_t alpha_u,
+                      int32_t alpha_v);
+
+/* The 16x16 leaf's 4:2:0 chroma search (pick_uv16_420,
+ * src/coder/block16.rs:980-1381, with the shipped tuning: uv16_joint on,
+ * uv8_joint_k 4, cfl_alpha_rd_steps 0) over n 16x16 leaves, each with an 8x8
+ * chroma block at (px / 2, py / 2):
+ *   1. DC: per plane the DC prediction, DCT_DCT with the QM, the chroma
+ *      trellis (trellis_optimize_ctx, coefficient class TX_8X8, chroma CDFs,
+ *      the dc_sign context of the plane's two above / two left bytes),
+ *      preserve_dc, the inverse, sse_recon and chroma_bits (txb_skip context
+ *      7 + above non-zero + left non-zero, no tx-type symbol); total = the
+ *      planes' rd_cost_i64 in f32, with no mode bits;
+ *   2. CfL: the AC of the 16x16 luma reconstruction (cfl_ac_sub 4:2:0), each
+ *      plane's closed-form alpha (cfl_best_alpha over the displayed part),
+ *      its prediction through DCT_DCT, trellis, inverse, sse and bits (no
+ *      preserve_dc); total = the planes' costs + rd_lambda x
+ *      uv_mode_bits(CfL, alphas) - rd_lambda x uv_mode_bits(DC); taken when an
+ *      alpha is non-zero and the total is below the best;
+ *   3. the joint shortlist: SMOOTH_V, PAETH, SMOOTH, SMOOTH_H, V, H, D135,
+ *      D113, D157, D45, D67, D203, the directional ones at deltas -3..3 when
+ *      angle_deltas is set, each scored by the two planes' satd_sad_proxy,
+ *      sorted by (score, mode, delta); the first joint_k are priced: rd_lambda
+ *      x (uv_mode_bits + the delta's angle-delta bits over delta 0's), then
+ *      per plane the prediction with the leaf's edge flags, the mode's
+ *      transform (dav1d's uv-mode map: ADST_ADST, ADST_DCT, DCT_ADST or
+ *      DCT_DCT) with the QM, trellis, preserve_dc, inverse, sse and bits,
+ *      stopping after U when the total already reaches the best; taken when
+ *      below the best.
+ * Params: mt_split16_params of the chroma planes (frame_w / frame_h the
+ * chroma plane's size, stride its stride, vis_w / vis_h its displayed size,
+ * trellis_lambda0 the trellis lambda, rd_lambda the chroma mode lambda
+ * (emit_mlam_c), band_tilt of the chroma quantiser, wsse_scale, skip_bits[ctx]
+ * the TX_8X8 class's chroma pairs when use_skip_bits); quant the chroma
+ * quantiser; qm row the 8x8 chroma weights (NULL: flat); costs the chroma
+ * TX_8X8 slice (mt_coef_cdfs_default(qctx, 8, 8, 1)). */
+typedef struct mt_uv16_params {
+  int32_t luma_stride;   /* stride of the luma reconstruction the CfL AC reads */
+  int32_t joint_k;       /* shortlist length, clamped to 1..12 (uv8_joint_k) */
+  int32_t angle_deltas;  /* try_angle_deltas_av1(16, base_q_idx) */
+  int32_t reserved;
+} mt_uv16_params;
+typedef struct mt_uv16_job {
+  uint16_t px, py;          /* 16x16 luma leaf origin */
+  uint8_t y_mode;           /* the luma winner's mode */
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL of the leaf, MT_CAND_FILTER_TYPE: chroma filter type */
+  uint8_t a_coef[2][2];     /* above coefficient contexts of the chroma block's two 4-sample columns, U then V */
+  uint8_t l_coef[2][2];     /* left contexts of its two 4-sample rows */
+  uint8_t reserved[2];
+} mt_uv16_job;
+typedef struct mt_uv16_result {
+  float total;              /* the winner's total (the picker's best_total) */
+  float dc_total;           /* the DC path's total */
+  float cfl_total;          /* the CfL path's total */
+  uint8_t uv_mode;          /* MT_*_PRED or MT_UV_CFL_PRED; 255 for a rejected job */
+  int8_t angle_delta;
+  int8_t cfl_alpha[2];      /* the closed-form alphas (U, V) */
+} mt_uv16_result;
+/* Device form.  d_luma: the luma reconstruction (luma_stride); d_src_u /
+ * d_src_v and d_rec_u / d_rec_v: the chroma source and reconstruction planes
+ * (prm->stride).  d_cf (optional): n x 128 int32, the winner's U then V
+ * levels; d_rec (optional): n x 128 uint16, its U then V reconstruction
+ * (clamp(prediction + inverse)).  Rejected jobs (chroma block outside the
+ * plane, a bad mode) get uv_mode 255 and total +inf. */
+int mt_pick_uv16_420_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv16_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream);
+/* Host-buffer form: chroma planes prm->stride x prm->frame_h, the luma
+ * reconstruction luma_stride x 2 frame_h. */
+int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv16_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
+
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */
 int mt_split16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* prm, const mt_quant* quant,
                     const uint8_t* qm_row, const mt_coef_costs* costs, const mt_split16_job* jobs, int32_t n,

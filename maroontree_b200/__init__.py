@@ -219,6 +219,48 @@ def sse_recon(src, vis_w, vis_h, pos, pred, resid, w, h, wsse_scale=0.0, bd=8):
     return out
 
 
+def uv_mode_cdfs_default():
+    """The mode CDFs uv_mode_bits reads, from the default decision snapshot."""
+    c = abi.UvModeCdfs()
+    _check(load().mt_uv_mode_cdfs_default(C.byref(c)), "mt_uv_mode_cdfs_default")
+    return c
+
+
+def uv_mode_costs(cdfs):
+    out = abi.UvModeCosts()
+    _check(load().mt_uv_mode_costs_build(C.byref(cdfs), C.byref(out)), "mt_uv_mode_costs_build")
+    return out
+
+
+def uv_mode_bits(costs, y_mode, uv_mode, cfl=None):
+    """uv_mode_bits(y_mode, uv_mode, cfl) on the host; cfl: (alpha_u, alpha_v) or None."""
+    au, av = cfl if cfl is not None else (0, 0)
+    return load().mt_uv_mode_bits(C.byref(costs), y_mode, uv_mode, int(cfl is not None), au, av)
+
+
+def uv16_params(luma_stride, joint_k=4, angle_deltas=True):
+    u = abi.Uv16Params()
+    u.luma_stride, u.joint_k, u.angle_deltas = luma_stride, joint_k, int(bool(angle_deltas))
+    return u
+
+
+def pick_uv16_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs, jobs, want_cf=False,
+                  want_rec=False):
+    """pick_uv16_420 over (16x16 leaf) jobs (``mt_pick_uv16_420``): (results,
+    levels n x 128 or None, reconstruction n x 128 or None), U then V."""
+    planes = [np.ascontiguousarray(a, np.uint16) for a in (src_u, src_v, rec_u, rec_v, luma)]
+    jobs = np.ascontiguousarray(jobs, abi.UV16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.UV16_RESULT_DTYPE)
+    cf = np.zeros((n, 128), np.int32) if want_cf else None
+    rec = np.zeros((n, 128), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(load().mt_pick_uv16_420(*[ptr(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(quant), ptr(qm),
+                                   C.byref(costs), C.byref(mode_costs), ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)),
+           "mt_pick_uv16_420")
+    return res, cf, rec
+
+
 def split16_params(frame_w, frame_h, stride=None, trellis_lambda0=0.05, rd_lambda=1.0, band_tilt=0.0,
                    wsse_scale=0.0, tx_search=False, tx_guard_shift=4, skip_bits=None, vis=None, bd=8):
     """``mt_split16_params``: skip_bits, when given, is 13 (all_zero = 1, all_zero = 0)

@@ -85,6 +85,32 @@ class Split16Params(C.Structure):
 
 assert C.sizeof(Split16Params) == 156
 
+
+class UvModeCdfs(C.Structure):
+    """mt_uv_mode_cdfs."""
+    _fields_ = [("uv_mode", (C.c_uint16 * 14) * 13), ("angle_delta", (C.c_uint16 * 7) * 8),
+                ("cfl_sign", C.c_uint16 * 8), ("cfl_alpha", (C.c_uint16 * 16) * 6)]
+
+
+class UvModeCosts(C.Structure):
+    """mt_uv_mode_costs."""
+    _fields_ = [("uv_mode", (C.c_float * 14) * 13), ("angle_delta", (C.c_float * 7) * 8),
+                ("cfl_sign", C.c_float * 8), ("cfl_alpha", (C.c_float * 16) * 6)]
+
+
+class Uv16Params(C.Structure):
+    """mt_uv16_params."""
+    _fields_ = [(n, C.c_int32) for n in ("luma_stride", "joint_k", "angle_deltas", "reserved")]
+
+
+UV_CFL_PRED = 13
+UV16_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("y_mode", "u1"), ("flags", "u1"),
+                           ("a_coef", "u1", (2, 2)), ("l_coef", "u1", (2, 2)), ("reserved", "u1", (2,))])
+UV16_RESULT_DTYPE = np.dtype([("total", "<f4"), ("dc_total", "<f4"), ("cfl_total", "<f4"), ("uv_mode", "u1"),
+                              ("angle_delta", "i1"), ("cfl_alpha", "i1", (2,))])
+assert C.sizeof(UvModeCdfs) == 2 * (13 * 14 + 8 * 7 + 8 + 6 * 16) and C.sizeof(UvModeCosts) == 4 * (13 * 14 + 8 * 7 + 8 + 6 * 16)
+assert UV16_JOB_DTYPE.itemsize == 16 and UV16_RESULT_DTYPE.itemsize == 16
+
 SPLIT16_JOB_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"), ("reserved", "u1"),
     ("a_coef", "u1", (4,)), ("l_coef", "u1", (4,)),
@@ -425,6 +451,15 @@ def _bind(lib):
                                             C.c_int32, _P, _P]),
         "mt_quad32_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
                                      _P, C.c_int32, _P]),
+        "mt_uv_mode_cdfs_default": (C.c_int, [C.POINTER(UvModeCdfs)]),
+        "mt_uv_mode_costs_build": (C.c_int, [C.POINTER(UvModeCdfs), C.POINTER(UvModeCosts)]),
+        "mt_uv_mode_bits": (C.c_float, [C.POINTER(UvModeCosts), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                        C.c_int32]),
+        "mt_pick_uv16_420_device": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                              C.POINTER(Quant), _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
+        "mt_pick_uv16_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                       C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
+                                       C.c_int32, _P, _P, _P]),
         "mt_grid16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
                                             C.c_int32, _P, _P, _P]),
         "mt_grid16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
@@ -486,7 +521,8 @@ EXPORTED_SYMBOLS = (
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
     "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
     "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
-    "mt_grid16_luma_device", "mt_grid16_luma",
+    "mt_grid16_luma_device", "mt_grid16_luma", "mt_uv_mode_cdfs_default", "mt_uv_mode_costs_build",
+    "mt_uv_mode_bits", "mt_pick_uv16_420_device", "mt_pick_uv16_420",
 )
 
 

@@ -17,6 +17,8 @@
 
 namespace {
 
+using namespace mtd;
+
 using mtd::clampi;
 using mtd::uabs;
 
@@ -25,41 +27,6 @@ constexpr int kBeamModes = MT_BEAM_MODES;
 __constant__ uint8_t kNdModes[kBeamModes] = {MT_DC_PRED,    MT_V_PRED,      MT_H_PRED,    MT_D45_PRED,
                                              MT_D135_PRED,  MT_D113_PRED,   MT_D157_PRED, MT_D203_PRED,
                                              MT_D67_PRED,   MT_SMOOTH_PRED, MT_PAETH_PRED};
-
-// satd_sad_proxy_scalar (src/rd_sse.rs:1143-1176): SAD + (SATD >> 2) of
-// src - pred over 4x4 tiles, with the samples past the displayed window
-// (vw x vh from the block origin) taken as the prediction.
-template <int N>
-__device__ uint64_t satd_sad_proxy(const uint16_t* __restrict__ src, int stride, int px, int py,
-                                   const int16_t* __restrict__ pred, int vw, int vh) {
-  uint64_t sad = 0, satd = 0;
-#pragma unroll 1
-  for (int tile = 0; tile < (N / 4) * (N / 4); tile++) {
-    const int ty = (tile / (N / 4)) * 4, tx = (tile % (N / 4)) * 4;
-    int32_t r[4][4];
-#pragma unroll
-    for (int y = 0; y < 4; y++) {
-      int32_t d[4];
-#pragma unroll
-      for (int x = 0; x < 4; x++) {
-        const bool vis = tx + x < vw && ty + y < vh;
-        d[x] = vis ? (int32_t)src[(size_t)(py + ty + y) * stride + px + tx + x] - pred[(ty + y) * N + tx + x] : 0;
-        sad += uabs(d[x]);
-      }
-      const int32_t e = d[0] + d[2], f = d[0] - d[2], g = d[1] + d[3], h = d[1] - d[3];
-      r[y][0] = e + g;
-      r[y][1] = f + h;
-      r[y][2] = f - h;
-      r[y][3] = e - g;
-    }
-#pragma unroll
-    for (int x = 0; x < 4; x++) {
-      const int32_t e = r[0][x] + r[2][x], f = r[0][x] - r[2][x], g = r[1][x] + r[3][x], h = r[1][x] - r[3][x];
-      satd += (uint64_t)uabs(e + g) + uabs(f + h) + uabs(f - h) + uabs(e - g);
-    }
-  }
-  return sad + (satd >> 2);
-}
 
 template <int N>
 __global__ void __launch_bounds__(128) beam_score_kernel(const uint16_t* __restrict__ src,

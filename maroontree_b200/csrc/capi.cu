@@ -189,6 +189,37 @@ int mt_coef_costs_build(const mt_coef_cdfs* c, mt_coef_costs* o) {
   return MT_OK;
 }
 
+int mt_uv_mode_costs_build(const mt_uv_mode_cdfs* c, mt_uv_mode_costs* o) {
+  if (!c || !o) return MT_ERR_INVALID_INPUT;
+  for (int m = 0; m < 13; m++)
+    for (int s = 0; s < 14; s++) o->uv_mode[m][s] = cdf_cost(c->uv_mode[m], s);
+  for (int m = 0; m < 8; m++)
+    for (int s = 0; s < 7; s++) o->angle_delta[m][s] = cdf_cost(c->angle_delta[m], s);
+  for (int s = 0; s < 8; s++) o->cfl_sign[s] = cdf_cost(c->cfl_sign, s);
+  for (int k = 0; k < 6; k++)
+    for (int s = 0; s < 16; s++) o->cfl_alpha[k][s] = cdf_cost(c->cfl_alpha[k], s);
+  return MT_OK;
+}
+
+// uv_mode_bits (src/coder/lossy_state.rs:1302-1349); the same sums as the
+// device's uv_mode_bits_dev.
+float mt_uv_mode_bits(const mt_uv_mode_costs* c, int32_t y_mode, int32_t uv_mode, int32_t cfl, int32_t au, int32_t av) {
+  if (!c || y_mode < 0 || y_mode > 12 || uv_mode < 0 || uv_mode > 13) return INFINITY;
+  if (!cfl) {
+    float bits = c->uv_mode[y_mode][uv_mode];
+    if (uv_mode >= MT_V_PRED && uv_mode <= MT_D67_PRED) bits += c->angle_delta[uv_mode - MT_V_PRED][3];
+    return bits;
+  }
+  if (au < -16 || au > 16 || av < -16 || av > 16) return INFINITY;
+  const int su = au == 0 ? 0 : (au < 0 ? 1 : 2), sv = av == 0 ? 0 : (av < 0 ? 1 : 2);
+  const int sign = su * 3 + sv;
+  if (sign == 0) return c->uv_mode[y_mode][MT_DC_PRED];
+  float bits = c->uv_mode[y_mode][MT_UV_CFL_PRED] + c->cfl_sign[sign - 1];
+  if (su != 0) bits += c->cfl_alpha[(su == 2) * 3 + sv][(au < 0 ? -au : au) - 1];
+  if (sv != 0) bits += c->cfl_alpha[(sv == 2) * 3 + su][(av < 0 ? -av : av) - 1];
+  return bits;
+}
+
 extern "C++" {
 namespace mth {
 // scaled_trellis_lambda for the other translation units of the library.

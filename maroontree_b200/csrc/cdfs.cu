@@ -150,3 +150,16 @@ extern "C" int mt_coef_cdfs_default(int32_t qctx, int32_t tx_w, int32_t tx_h, in
   }
   return MT_OK;
 }
+
+// The mode CDFs uv_mode_bits reads (src/coder/lossy_state.rs:1302-1349) from
+// the decision snapshot: uv_mode with CfL allowed per y mode, angle_delta per
+// directional mode, cfl_sign, cfl_alpha per context.
+extern "C" int mt_uv_mode_cdfs_default(mt_uv_mode_cdfs* out) {
+  if (!out) return MT_ERR_INVALID_INPUT;
+  memset(out, 0, sizeof(*out));
+  for (int m = 0; m < 13; ++m) row(out->uv_mode[m], &MT_CDF_UV_MODE_CFL_CDF[m * 13], 13);
+  for (int m = 0; m < 8; ++m) row(out->angle_delta[m], &MT_CDF_ANGLE_DELTA_CDF[m * 6], 6);
+  row(out->cfl_sign, MT_CDF_CFL_SIGN_CDF, 7);
+  for (int c = 0; c < 6; ++c) row(out->cfl_alpha[c], &MT_CDF_CFL_ALPHA_CDF[c * 15], 15);
+  return MT_OK;
+}

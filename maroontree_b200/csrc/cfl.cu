@@ -10,8 +10,11 @@
 #include <stdint.h>
 
 #include "../../include/maroontree_b200.h"
+#include "common.cuh"
 
 namespace {
+
+using namespace mtd;
 
 constexpr int kCflWarps = 4;
 constexpr int kCflMaxSamples = 32 * 32;
@@ -20,13 +23,6 @@ __device__ __forceinline__ long long warp_sum64(long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
-}
-
-// cfl_pred_pixel (src/intrapred.rs:1194-1199).
-__device__ __forceinline__ int32_t cfl_pred_pixel(int32_t dc, int32_t ac, int32_t alpha, int32_t maxv) {
-  const int32_t diff = alpha * ac;
-  const int32_t mag = (abs(diff) + 32) >> 6;
-  return min(max(dc + (diff < 0 ? -mag : mag), 0), maxv);
 }
 
 __global__ void __launch_bounds__(32 * kCflWarps) cfl_kernel(

@@ -1,0 +1,458 @@
+// The 16x16 leaf's 4:2:0 chroma search (pick_uv16_420,
+// src/coder/block16.rs:980-1381) with the shipped tuning (uv16_joint on,
+// uv8_joint_k 4, cfl_alpha_rd_steps 0), batched over leaves, one thread per
+// leaf.  The 8x8 chroma block of each leaf runs the DC path, the CfL path
+// (the AC of the 16x16 luma reconstruction, the closed-form alphas) and the
+// joint (mode, delta) SATD shortlist, whose first joint_k entries are priced
+// in full; every priced candidate goes through the same per-plane chain:
+// prediction, the transform (DCT_DCT, or the uv mode's type for the
+// shortlist) with the QM, the chroma trellis (trellis_optimize_ctx against
+// the chroma TX_8X8 costs), preserve_dc where the reference applies it, the
+// inverse, sse_recon and chroma_bits.  The candidate and the winner live in
+// the two slots of UvWork; a candidate that wins swaps them.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/maroontree_b200.h"
+#include "common.cuh"
+#include "leaf8.cuh"
+#include "wsse.cuh"
+
+namespace mth {
+float scaled_trellis_lambda_host(float dc_q, float lambda0);
+}
+
+namespace {
+
+using namespace mtd;
+
+constexpr int kUvThreads = 64;
+constexpr int kJointModes = 12;
+constexpr int kMaxJoint = 12;
+
+struct UvArgs {
+  mt_split16_params p;  // the chroma planes
+  mt_uv16_params u;
+  mt_quant q;           // the chroma quantiser
+  float lambda;         // scaled_trellis_lambda of the chroma trellis (0: off)
+  int has_qm;
+};
+
+// Both planes of one candidate: predictions, levels and inverses.
+struct UvSlot {
+  int16_t pred[2][64];
+  int16_t cf[2][64];
+  int16_t rr[2][64];
+};
+
+struct UvWork {
+  UvSlot s[2];     // the candidate and the winner
+  int32_t u[128];  // prediction edges, then the targets [0, 64) and the transform temporary [64, 128)
+  int16_t resid[64];
+  int16_t ac[64];  // CfL AC of the leaf's luma
+  TrellisCtxScratch tr;
+  uint8_t lv[160];
+};
+
+// The shortlist's modes in the reference's order (block16.rs:1143-1156).
+__constant__ uint8_t kJointList[kJointModes] = {MT_SMOOTH_V_PRED, MT_PAETH_PRED, MT_SMOOTH_PRED, MT_SMOOTH_H_PRED,
+                                                MT_V_PRED,        MT_H_PRED,     MT_D135_PRED,   MT_D113_PRED,
+                                                MT_D157_PRED,     MT_D45_PRED,   MT_D67_PRED,    MT_D203_PRED};
+
+__device__ __forceinline__ bool directional(int m) { return m >= MT_V_PRED && m <= MT_D67_PRED; }
+
+// chroma_tx_for_mode (src/coder/chroma_tx.rs:46-66): dav1d's uv-mode map.
+__device__ __forceinline__ int chroma_tx(int m) {
+  if (m == MT_PAETH_PRED || m == MT_SMOOTH_PRED || m == MT_D135_PRED) return MT_TX_ADST_ADST;
+  if (m == MT_SMOOTH_V_PRED || m == MT_V_PRED || m == MT_D113_PRED || m == MT_D67_PRED) return MT_TX_ADST_DCT;
+  if (m == MT_SMOOTH_H_PRED || m == MT_H_PRED || m == MT_D157_PRED || m == MT_D203_PRED) return MT_TX_DCT_ADST;
+  return MT_TX_DCT_DCT;
+}
+
+__device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate) {
+  return __fadd_rn((float)d, __fmul_rn(lam, rate));
+}
+
+// uv_mode_bits (src/coder/lossy_state.rs:1302-1349); cfl: the alphas' form.
+__device__ float uv_mode_bits(const mt_uv_mode_costs& C, int y_mode, int uv, bool cfl, int au, int av) {
+  if (!cfl) {
+    float bits = C.uv_mode[y_mode][uv];
+    if (directional(uv)) bits = __fadd_rn(bits, C.angle_delta[uv - MT_V_PRED][3]);
+    return bits;
+  }
+  const int su = au == 0 ? 0 : (au < 0 ? 1 : 2), sv = av == 0 ? 0 : (av < 0 ? 1 : 2);
+  const int sign = su * 3 + sv;
+  if (sign == 0) return C.uv_mode[y_mode][MT_DC_PRED];
+  float bits = __fadd_rn(C.uv_mode[y_mode][MT_UV_CFL_PRED], C.cfl_sign[sign - 1]);
+  if (su != 0) bits = __fadd_rn(bits, C.cfl_alpha[(su == 2) * 3 + sv][abs(au) - 1]);
+  if (sv != 0) bits = __fadd_rn(bits, C.cfl_alpha[(sv == 2) * 3 + su][abs(av) - 1]);
+  return bits;
+}
+
+// Per-plane constants of a job: source / reconstruction origins, displayed
+// extent, coefficient contexts.
+struct UvPlane {
+  const uint16_t* src;  // block origin
+  const uint16_t* rec;  // plane base
+  int vw, vh;
+  int sk, ds;           // txb_skip context 7 + above nz + left nz, dc_sign_ctx_span
+  float skip1, skip0;
+};
+
+// One plane of a candidate after its prediction: residual, transform with
+// the QM, trellis, preserve_dc (src/rd_sse.rs:759-765) when `keep_dc`,
+// inverse, sse_recon and the rate.  Returns the plane's rd_cost_i64.
+__device__ float plane_chain(const UvArgs& a, const UvPlane& P, const mt_coef_costs& T, const uint8_t* qm,
+                             const float* sQs, int tx, bool keep_dc, int16_t* pred, int16_t* cf, int16_t* rr,
+                             UvWork& w) {
+  const mt_split16_params& p = a.p;
+  const mt_quant& q = a.q;
+  int32_t sum = 0;
+#pragma unroll 8
+  for (int i = 0; i < 64; i++) {
+    const int32_t r = (int32_t)P.src[(size_t)(i >> 3) * p.stride + (i & 7)] - pred[i];
+    w.resid[i] = (int16_t)r;
+    sum += r;
+  }
+  float* tf = reinterpret_cast<float*>(w.u);
+  int32_t* tmp = w.u + 64;
+  fwd8x8(w.resid, tx, q, cf, tf, tmp);
+  if (qm) apply_qm(cf, tf, sQs, 64);
+  if (a.lambda > 0.0f)
+    trellis_ctx8(cf, tf, (float)q.dc_q, (float)q.ac_q, a.lambda, T, P.ds, qm, q.qm_level >= 5, p.band_tilt, w.tr);
+  if (keep_dc) {
+    const int32_t mean = sum / 64;  // truncating, as the reference's i32 division
+    if (cf[0] == 0 && abs(mean) >= 8) cf[0] = (int16_t)(mean > 0 ? 1 : -1);
+  }
+  inv8x8(cf, tx, q, qm, rr, tmp);
+  ErrBlock<int16_t, int16_t> eb;
+  eb.src = P.src;
+  eb.stride = p.stride;
+  eb.pred = pred;
+  eb.resid = rr;
+  eb.w = 8;
+  eb.vw = P.vw;
+  eb.vh = P.vh;
+  eb.maxv = (1 << p.bd) - 1;
+  const long long sse = sse_recon_block(eb, p.wsse_scale);
+  const float bits = rate_bounded<8>(cf, T, P.sk, P.ds, 0, -1, p.use_skip_bits != 0, P.skip1, P.skip0,
+                                     __int_as_float(0x7f800000), w.lv);
+  return rd_cost_i64(sse, p.rd_lambda, bits);
+}
+
+// cfl_best_alpha (src/intrapred.rs:1211-1258) over the displayed part: the
+// closed-form alpha, then the first minimum of the prediction's SSE over
+// alpha - 3 .. alpha + 3 within +-16.
+__device__ int cfl_alpha(const int16_t* ac, const UvPlane& P, int stride, int32_t dc, int32_t maxv) {
+  long long num = 0, den = 0;
+  for (int y = 0; y < P.vh; y++)
+    for (int x = 0; x < P.vw; x++) {
+      const long long v = ac[y * 8 + x];
+      num += (long long)((int32_t)P.src[(size_t)y * stride + x] - dc) * v;
+      den += v * v;
+    }
+  if (den == 0) return 0;
+  const long long sg = num > 0 ? 1 : (num < 0 ? -1 : 0);
+  long long a0 = (64 * num + (den >> 1) * sg) / den;
+  a0 = a0 < -16 ? -16 : (a0 > 16 ? 16 : a0);
+  long long best_e = 0x7fffffffffffffffLL;
+  int best_a = 0;
+  for (int c = (int)a0 - 3; c <= (int)a0 + 3; c++) {
+    if (c < -16 || c > 16) continue;
+    long long e = 0;
+    for (int y = 0; y < P.vh; y++)
+      for (int x = 0; x < P.vw; x++) {
+        const long long d = (int32_t)P.src[(size_t)y * stride + x] - cfl_pred_pixel(dc, ac[y * 8 + x], c, maxv);
+        e += d * d;
+      }
+    if (e < best_e) {
+      best_e = e;
+      best_a = c;
+    }
+  }
+  return best_a;
+}
+
+__global__ void __launch_bounds__(kUvThreads) uv16_420_kernel(
+    const uint16_t* __restrict__ src_u, const uint16_t* __restrict__ src_v, const uint16_t* __restrict__ rec_u,
+    const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_job* __restrict__ jobs, int n,
+    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+  __shared__ mt_coef_costs sT;
+  __shared__ mt_uv_mode_costs sM;
+  __shared__ uint8_t sQm[64];
+  __shared__ float sQs[64];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    const float* gm = reinterpret_cast<const float*>(mode_costs);
+    float* sm = reinterpret_cast<float*>(&sM);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_uv_mode_costs) / 4); i += blockDim.x) sm[i] = gm[i];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+      const int wq = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)wq;
+      sQs[i] = fwd_qm_scale(wq);
+    }
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_uv16_job jb = jobs[j];
+  mt_uv16_result& r = res[j];
+  const int cx = jb.px >> 1, cy = jb.py >> 1;
+  const float kInf = __int_as_float(0x7f800000);
+  const bool ok = (jb.px & 15) == 0 && (jb.py & 15) == 0 && cx + 8 <= p.frame_w && cy + 8 <= p.frame_h &&
+                  jb.y_mode <= MT_PAETH_PRED;
+  if (!ok) {
+    r.total = r.dc_total = r.cfl_total = kInf;
+    r.uv_mode = 255;
+    r.angle_delta = 0;
+    r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
+    if (cf_out)
+      for (int i = 0; i < 128; i++) cf_out[(size_t)j * 128 + i] = 0;
+    if (rec_out)
+      for (int i = 0; i < 128; i++) rec_out[(size_t)j * 128 + i] = 0;
+    return;
+  }
+  const mt_coef_costs& T = sT;
+  const mt_uv_mode_costs& M = sM;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float mlam = p.rd_lambda;
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const bool ft = jb.flags & MT_CAND_FILTER_TYPE;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  UvPlane P[2];
+  for (int pl = 0; pl < 2; pl++) {
+    UvPlane& q = P[pl];
+    q.src = (pl ? src_v : src_u) + (size_t)cy * p.stride + cx;
+    q.rec = pl ? rec_v : rec_u;
+    q.vw = min(max(vis_w - cx, 0), 8);
+    q.vh = min(max(vis_h - cy, 0), 8);
+    const uint32_t a0 = jb.a_coef[pl][0], a1 = jb.a_coef[pl][1], l0 = jb.l_coef[pl][0], l1 = jb.l_coef[pl][1];
+    q.sk = 7 + (a0 != 0x40 || a1 != 0x40) + (l0 != 0x40 || l1 != 0x40);
+    const int s = (int)(a0 >> 6) + (int)(a1 >> 6) + (int)(l0 >> 6) + (int)(l1 >> 6) - 4;
+    q.ds = (s != 0) + (s > 0);
+    q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
+    q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
+  }
+  UvWork w;
+  int best = 0;
+  // 1. DC on both planes (block16.rs:999-1046): no mode bits in its total
+  int32_t dc[2];
+  float dc_total = 0.0f;
+  for (int pl = 0; pl < 2; pl++) {
+    predict_sq<8>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
+                  w.s[0].pred[pl], w.u);
+    dc[pl] = w.s[0].pred[pl][0];
+    dc_total = __fadd_rn(dc_total, plane_chain(a, P[pl], T, qm, sQs, MT_TX_DCT_DCT, true, w.s[0].pred[pl],
+                                               w.s[0].cf[pl], w.s[0].rr[pl], w));
+  }
+  float best_total = dc_total;
+  int mode = MT_DC_PRED, delta = 0;
+  // 2. CfL (:1058-1128): the AC of the 16x16 luma reconstruction, the
+  // closed-form alphas, each plane's prediction through the DCT chain
+  {
+    const int ls = a.u.luma_stride;
+    const uint16_t* l = luma + (size_t)jb.py * ls + jb.px;
+    int32_t sum = 32;
+    for (int i = 0; i < 64; i++) {
+      const int y = i >> 3, x = i & 7;
+      const uint16_t* q = l + (size_t)(2 * y) * ls + 2 * x;
+      const int32_t v = ((int32_t)q[0] + q[1] + q[ls] + q[ls + 1]) << 1;
+      w.ac[i] = (int16_t)v;
+      sum += v;
+    }
+    const int32_t mean = sum >> 6;
+    for (int i = 0; i < 64; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
+  }
+  int alpha[2];
+  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha(w.ac, P[pl], p.stride, dc[pl], maxv);
+  {
+    UvSlot& c = w.s[1 - best];
+    float body = 0.0f;
+    for (int pl = 0; pl < 2; pl++) {
+      for (int i = 0; i < 64; i++) c.pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
+      body = __fadd_rn(body, plane_chain(a, P[pl], T, qm, sQs, MT_TX_DCT_DCT, false, c.pred[pl], c.cf[pl],
+                                         c.rr[pl], w));
+    }
+    const float cfl_total =
+        __fsub_rn(__fadd_rn(body, __fmul_rn(mlam, uv_mode_bits(M, jb.y_mode, MT_UV_CFL_PRED, true, alpha[0], alpha[1]))),
+                  __fmul_rn(mlam, uv_mode_bits(M, jb.y_mode, MT_DC_PRED, false, 0, 0)));
+    r.cfl_total = cfl_total;
+    if ((alpha[0] != 0 || alpha[1] != 0) && cfl_total < best_total) {
+      best_total = cfl_total;
+      mode = MT_UV_CFL_PRED;
+      best = 1 - best;
+    }
+  }
+  // 3. the joint (mode, delta) shortlist (:1157-1240): the two planes'
+  // satd_sad_proxy per candidate, the first joint_k by (score, mode, delta)
+  const int k = min(max(a.u.joint_k, 1), kMaxJoint);
+  unsigned long long ks[kMaxJoint];
+  uint8_t km[kMaxJoint];
+  int8_t kd[kMaxJoint];
+  int nk = 0;
+  int16_t* sp = w.s[1 - best].pred[0];  // scratch prediction
+  for (int ci = 0; ci < kJointModes; ci++) {
+    const int m = kJointList[ci];
+    const bool dir = directional(m) && a.u.angle_deltas;
+    for (int d = dir ? -3 : 0; d <= (dir ? 3 : 0); d++) {
+      unsigned long long sc = 0;
+      for (int pl = 0; pl < 2; pl++) {
+        predict_sq<8>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, have_tr, have_bl, ft, p.bd, sp, w.u);
+        sc += satd_sad_proxy<8>(pl ? src_v : src_u, p.stride, cx, cy, sp, P[pl].vw, P[pl].vh);
+      }
+      // insert (sc, m, d) into the ascending list of at most k entries
+      auto less = [&](int e) {
+        return sc < ks[e] || (sc == ks[e] && (m < km[e] || (m == km[e] && d < kd[e])));
+      };
+      if (nk == k && !less(nk - 1)) continue;
+      int e = nk < k ? nk++ : nk - 1;
+      while (e > 0 && less(e - 1)) {
+        ks[e] = ks[e - 1];
+        km[e] = km[e - 1];
+        kd[e] = kd[e - 1];
+        e--;
+      }
+      ks[e] = sc;
+      km[e] = (uint8_t)m;
+      kd[e] = (int8_t)d;
+    }
+  }
+  for (int e = 0; e < nk; e++) {
+    const int m = km[e], d = kd[e], tx = chroma_tx(m);
+    float ad_bits = 0.0f;
+    if (directional(m)) ad_bits = __fsub_rn(M.angle_delta[m - MT_V_PRED][d + 3], M.angle_delta[m - MT_V_PRED][3]);
+    float total = __fmul_rn(mlam, __fadd_rn(uv_mode_bits(M, jb.y_mode, m, false, 0, 0), ad_bits));
+    UvSlot& c = w.s[1 - best];
+    for (int pl = 0; pl < 2; pl++) {
+      predict_sq<8>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, have_tr, have_bl, ft, p.bd, c.pred[pl],
+                    w.u);
+      total = __fadd_rn(total, plane_chain(a, P[pl], T, qm, sQs, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w));
+      if (pl == 0 && total >= best_total) break;  // cannot win: the second plane is skipped
+    }
+    if (total < best_total) {
+      best_total = total;
+      mode = m;
+      delta = d;
+      best = 1 - best;
+    }
+  }
+  r.total = best_total;
+  r.dc_total = dc_total;
+  r.uv_mode = (uint8_t)mode;
+  r.angle_delta = (int8_t)delta;
+  r.cfl_alpha[0] = (int8_t)alpha[0];
+  r.cfl_alpha[1] = (int8_t)alpha[1];
+  const UvSlot& b = w.s[best];
+  if (cf_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 64; i++) cf_out[(size_t)j * 128 + pl * 64 + i] = b.cf[pl][i];
+  if (rec_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 64; i++)
+        rec_out[(size_t)j * 128 + pl * 64 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
+}
+
+int uv_check(const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q, int32_t n) {
+  if (!p || !u || !q || n < 0) return MT_ERR_INVALID_INPUT;
+  if (p->bd != 8) return MT_ERR_UNSUPPORTED;
+  if (p->frame_w < 8 || p->frame_h < 8 || p->stride < p->frame_w || p->vis_w < 0 || p->vis_h < 0)
+    return MT_ERR_INVALID_INPUT;
+  if (u->luma_stride < 2 * p->frame_w) return MT_ERR_INVALID_INPUT;
+  if (!(p->rd_lambda > 0.0f) || !(p->wsse_scale >= 0.0f)) return MT_ERR_INVALID_INPUT;
+  return MT_OK;
+}
+
+size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int uv16_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* luma,
+                const mt_split16_params* prm, const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm,
+                const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mc, const mt_uv16_job* d_jobs, int32_t n,
+                mt_uv16_result* d_res, int32_t* d_cf, uint16_t* d_rec, void* stream) {
+  const int rc = uv_check(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!su || !sv || !ru || !rv || !luma || !d_costs || !d_mc || !d_jobs || !d_res) return MT_ERR_INVALID_INPUT;
+  UvArgs a;
+  a.p = *prm;
+  a.u = *uvp;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
+  uv16_420_kernel<<<(unsigned)((n + kUvThreads - 1) / kUvThreads), kUvThreads, 0,
+                    reinterpret_cast<cudaStream_t>(stream)>>>(su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs,
+                                                              n, d_res, d_cf, d_rec);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mt_pick_uv16_420_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv16_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream) {
+  return uv16_device(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs, d_mode_costs,
+                     d_jobs, n, d_results, d_cf, d_rec, stream);
+}
+
+int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv16_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  int rc = uv_check(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!src_u || !src_v || !rec_u || !rec_v || !luma || !costs || !mode_costs || !jobs || !results)
+    return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * 2;
+  const size_t lplane = (size_t)uvp->luma_stride * 2 * prm->frame_h * 2;
+  size_t o = 0;
+  const size_t o_su = o, o_sv = (o += up256(plane)), o_ru = (o += up256(plane)), o_rv = (o += up256(plane));
+  const size_t o_l = (o += up256(plane)), o_qm = (o += up256(lplane)), o_c = (o += up256(64));
+  const size_t o_mc = (o += up256(sizeof(mt_coef_costs))), o_j = (o += up256(sizeof(mt_uv_mode_costs)));
+  const size_t o_r = (o += up256((size_t)n * sizeof(mt_uv16_job)));
+  const size_t o_cf = (o += up256((size_t)n * sizeof(mt_uv16_result)));
+  const size_t o_rec = (o += cf_out ? up256((size_t)n * 128 * 4) : 0);
+  const size_t total = o + (rec_out ? up256((size_t)n * 128 * 2) : 0);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_su, src_u, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_sv, src_v, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_ru, rec_u, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rv, rec_v, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_l, luma, lplane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 64, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_c, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_mc, mode_costs, sizeof(mt_uv_mode_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_j, jobs, (size_t)n * sizeof(mt_uv16_job), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    auto U = [&](size_t off) { return reinterpret_cast<const uint16_t*>(d + off); };
+    rc = uv16_device(U(o_su), U(o_sv), U(o_ru), U(o_rv), U(o_l), prm, uvp, quant, has_qm ? d + o_qm : nullptr,
+                     reinterpret_cast<const mt_coef_costs*>(d + o_c),
+                     reinterpret_cast<const mt_uv_mode_costs*>(d + o_mc), reinterpret_cast<const mt_uv16_job*>(d + o_j),
+                     n, reinterpret_cast<mt_uv16_result*>(d + o_r), cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr,
+                     rec_out ? reinterpret_cast<uint16_t*>(d + o_rec) : nullptr, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(results, d + o_r, (size_t)n * sizeof(mt_uv16_result), cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out)
+      e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 128 * 4, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && rec_out)
+      e = cudaMemcpy(rec_out, d + o_rec, (size_t)n * 128 * 2, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+}  // extern "C"

@@ -500,6 +500,38 @@ def split16_jobs(fw, fh, modes, deltas=(0,), seed=0, n=16):
     return np.array(rows, abi.SPLIT16_JOB_DTYPE)
 
 
+def planes420(rgb, seed):
+    """Source and reconstruction planes of a 4:2:0 frame from an RGB image:
+    luma by rgb_to_luma, U and V the blue and red channels averaged over each
+    2x2 cell's diagonal pair (textured chroma with real edges, so every kind
+    of chroma mode can win); each reconstruction is the plane plus a seeded
+    +-3 coding error.  Returns ([Y, U, V], [Y', U', V'])."""
+    c = np.asarray(rgb).astype(np.int32)
+    y = rgb_to_luma(np.asarray(rgb, np.uint8))
+    u = ((c[0::2, 0::2, 2] + c[1::2, 1::2, 2] + 1) >> 1).astype(np.uint16)
+    v = ((c[0::2, 0::2, 0] + c[1::2, 1::2, 0] + 1) >> 1).astype(np.uint16)
+    src = [y, u, v]
+    rec = [synthetic_recon(p, seed + 7 + k) for k, p in enumerate(src)]
+    return src, rec
+
+
+def uv16_jobs(w, h, seed, every=1):
+    """16x16-leaf jobs of the 4:2:0 chroma search (mt_uv16_job): every
+    16x16 leaf of a w x h frame (or about one in `every`), a random luma
+    winner mode, deterministic neighbour flags with a random chroma filter
+    type, coefficient-context bytes shaped like coef_res_ctx's."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for py in range(0, h - 15, 16):
+        for px in range(0, w - 15, 16):
+            if rng.random() > 1.0 / every:
+                continue
+            fl = block_flags(px, py, w, h, 16) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
+            ctx = coef_ctx_bytes(rng, 8)
+            rows.append((px, py, int(rng.integers(0, 13)), fl, ctx[:4].reshape(2, 2), ctx[4:].reshape(2, 2), (0, 0)))
+    return np.array(rows, abi.UV16_JOB_DTYPE)
+
+
 def leaf64_jobs(fw, fh, modes, deltas=(0,), seed=0, grid=False):
     """(64x64 block, mode, delta) jobs of the 64x64 leaf's legs, mode-major:
     the four-TX_32X32 leg (mt_quad32_job: random per-quadrant dc_sign contexts)

@@ -161,6 +161,14 @@ int or_quad32_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_
 int or_grid16_luma(const uint16_t* src, const uint16_t* recon, const mt_split16_params* p, const mt_quant* q,
                    const uint8_t* qm, const mt_coef_cdfs* cdfs, const mt_grid16_job* jobs, int32_t n,
                    mt_grid16_result* results, int32_t* cf_out);
+/* lossy_state.rs uv_mode_bits (:1302-1349) from the mode CDFs. */
+float or_uv_mode_bits(const mt_uv_mode_cdfs* c, int32_t y_mode, int32_t uv_mode, int32_t cfl, int32_t alpha_u,
+                      int32_t alpha_v);
+/* block16.rs pick_uv16_420 (:980-1381) with the shipped tuning, per 16x16 leaf. */
+int or_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc, const mt_uv16_job* jobs,
+                     int32_t n, mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
 /* dct1d_32_i32 in place on 32 values. */
 void or_dct1d_32(int32_t* buf);
 /* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */

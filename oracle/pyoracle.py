@@ -88,6 +88,11 @@ def load():
             "or_dct1d_32": (None, [_P]),
             "or_quad32_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                          C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P]),
+            "or_uv_mode_bits": (C.c_float, [C.POINTER(abi.UvModeCdfs), C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                            C.c_int32]),
+            "or_pick_uv16_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
+                                           C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
+                                           C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_grid16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                          C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P]),
             "or_leaf32": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -1008,3 +1013,47 @@ def grid16_luma(src, recon, prm, q, qm, cdfs, jobs, threads=1, want_cf=False):
 
     _chunked(n, threads, run)
     return res, cf
+
+
+def uv_mode_cdfs():
+    """The mode CDFs uv_mode_bits reads, from the reference's default arrays
+    (tests/golden/cdfs_default.json): uv_mode with CfL allowed per y mode,
+    angle_delta per directional mode, cfl_sign, cfl_alpha."""
+    g = _golden_cdfs()
+    c = abi.UvModeCdfs()
+    arr = lambda name: np.ctypeslib.as_array(getattr(c, name))
+    um = np.asarray(g["UV_MODE_CFL_CDF"]).reshape(13, 13)
+    arr("uv_mode")[...] = np.stack([_icdf(r, 14) for r in um])
+    ad = np.asarray(g["ANGLE_DELTA_CDF"]).reshape(8, 6)
+    arr("angle_delta")[...] = np.stack([_icdf(r, 7) for r in ad])
+    arr("cfl_sign")[...] = _icdf(np.asarray(g["CFL_SIGN_CDF"]).reshape(-1), 8)
+    ca = np.asarray(g["CFL_ALPHA_CDF"]).reshape(6, 15)
+    arr("cfl_alpha")[...] = np.stack([_icdf(r, 16) for r in ca])
+    return c
+
+
+def uv_mode_bits(cdfs, y_mode, uv_mode, cfl=None):
+    au, av = cfl if cfl is not None else (0, 0)
+    return load().or_uv_mode_bits(C.byref(cdfs), y_mode, uv_mode, int(cfl is not None), au, av)
+
+
+def pick_uv16_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs, threads=1,
+                  want_cf=False, want_rec=False):
+    """pick_uv16_420 of n 16x16 leaves: (results, levels or None, reconstruction or None)."""
+    planes = [np.ascontiguousarray(a, np.uint16) for a in (src_u, src_v, rec_u, rec_v, luma)]
+    jobs = np.ascontiguousarray(jobs, abi.UV16_JOB_DTYPE)
+    n = len(jobs)
+    res = np.zeros(n, abi.UV16_RESULT_DTYPE)
+    cf = np.zeros((n, 128), np.int32) if want_cf else None
+    rec = np.zeros((n, 128), np.uint16) if want_rec else None
+    qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
+
+    def run(lo, hi):
+        assert load().or_pick_uv16_420(*[p(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(q), p(qm),
+                                       C.byref(cdfs), C.byref(mode_cdfs), p(jobs[lo:hi]), hi - lo, p(res[lo:hi]),
+                                       None if cf is None else p(cf[lo:hi]),
+                                       None if rec is None else p(rec[lo:hi])) == 0
+
+    _chunked(n, threads, run)
+    return res, cf, rec
+
