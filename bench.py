@@ -939,7 +939,7 @@ def measure_batch(steps, avif_alone, reps=3):
 C3_W = C3_H = 4096  # the 4096x4096 4:4:4 quality-60 frame: two tiles
 
 
-def measure_c3(dev, hbm_peak, steps, reps=5):
+def measure_c3(dev, hbm_peak, steps, reps=5, encode=True):
     """The 4096x4096 frame (generator seed 5, sigma 8 noise on the left half,
     piecewise-constant cells on the right), 4:4:4 quality 60: the whole encode
     through mt_encode_rgb8 (host RGB in, AVIF out; two tiles), and the frame
@@ -956,21 +956,23 @@ def measure_c3(dev, hbm_peak, steps, reps=5):
 
     lib = mt.load()
     rgb = synth.generate_rgb(C3_W, C3_H, 5, sigma=8.0, variant="large")
-    cfg = enc.config(quality=60, chroma=2)
-    first = enc.encode_rgb8(rgb, cfg)  # warm-up (buffers, module)
-    times, st = [], abi.EncodeStats()
-    for _ in range(max(steps, 3)):
-        t0 = time.perf_counter()
-        out = enc.encode_rgb8(rgb, cfg, stats=st)
-        times.append(time.perf_counter() - t0)
-        if out != first:
-            raise SystemExit("bench: the 4096x4096 encode is not repeatable")
-    dt = float(np.median(times))
-    res = {"workload": "mt_encode_rgb8 of the 4096x4096 4:4:4 quality-60 frame (two tiles), host RGB in, AVIF out, "
-                       "median wall time",
-           "ms": round(dt * 1e3, 2), "mpix_s": round(C3_W * C3_H / dt / 1e6, 2), "avif_bytes": len(first),
-           "blocks_kernel_ms": round(st.blocks_ms, 3), "levels": int(st.levels), "blocks": int(st.blocks),
-           "tokens": int(st.tokens)}
+    res = {}
+    if encode:
+        cfg = enc.config(quality=60, chroma=2)
+        first = enc.encode_rgb8(rgb, cfg)  # warm-up (buffers, module)
+        times, st = [], abi.EncodeStats()
+        for _ in range(max(steps, 3)):
+            t0 = time.perf_counter()
+            out = enc.encode_rgb8(rgb, cfg, stats=st)
+            times.append(time.perf_counter() - t0)
+            if out != first:
+                raise SystemExit("bench: the 4096x4096 encode is not repeatable")
+        dt = float(np.median(times))
+        res = {"workload": "mt_encode_rgb8 of the 4096x4096 4:4:4 quality-60 frame (two tiles), host RGB in, AVIF "
+                           "out, median wall time",
+               "ms": round(dt * 1e3, 2), "mpix_s": round(C3_W * C3_H / dt / 1e6, 2), "avif_bytes": len(first),
+               "blocks_kernel_ms": round(st.blocks_ms, 3), "levels": int(st.levels), "blocks": int(st.blocks),
+               "tokens": int(st.tokens)}
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
     t16 = lambda a: torch.from_numpy(np.ascontiguousarray(a).astype(np.int16)).to(dev)
     t8 = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.uint8)).to(dev)
@@ -1192,6 +1194,40 @@ def run_ours(args):
     return 0
 
 
+# The single measurements of --only: name -> (what it runs).
+ONLY = {
+    "uv16": "pick_uv16_420 over the 8,040 16x16 leaves of the 1080p frame (uv16_420_kernel)",
+    "quad32": "the 64x64 leaf's four-TX_32X32 leg, 480 blocks x 13 modes (quad32_kernel)",
+    "grid16": "the 64x64 leaf's sixteen-TX_16X16 leg, 480 blocks (grid16_kernel)",
+    "leaf32": "the 32x32 leaf's mode-loop candidates, 1,980 blocks x 13 modes (leaf_kernel<32>)",
+    "c3_filters": "the 4096x4096 4:4:4 frame filters: deblocking and CDEF (lf_fused_kernel, the CDEF search)",
+}
+
+
+def run_only(args):
+    import torch
+    import maroontree_b200 as mt
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    mt.load()
+    if args.only == "c3_filters":
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            peaks = {}
+        out = measure_c3(dev, peaks.get("hbm_gbs", 6650.0), 1, reps=1, encode=False)
+    else:
+        wl = make_workload()
+        run = {"uv16": lambda: measure_uv16(dev, wl, reps=1, cpu=False),
+               "quad32": lambda: measure_leaf64(dev, wl, False, reps=1, cpu=False),
+               "grid16": lambda: measure_leaf64(dev, wl, True, reps=1, cpu=False),
+               "leaf32": lambda: measure_leaf8(dev, wl, False, reps=1, cpu=False, n32=True)}[args.only]
+        out = run()
+    print(json.dumps({"only": args.only, "what": ONLY[args.only], **out}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1200,9 +1236,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--headline-only", action="store_true", help="skip the secondary kernel-level measurements")
+    ap.add_argument("--only", choices=sorted(ONLY),
+                    help="run one secondary measurement alone (one timed call after the warm-up calls, no CPU leg) "
+                         "and print its JSON; the kernel profiles are taken on these runs")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only:
+        return run_only(args)
     return run_ours(args)
 
 
