@@ -787,9 +787,9 @@ float mt_uv_mode_bits(const mt_uv_mode_costs* costs, int32_t y_mode, int32_t uv_
  * TX_8X8 slice (mt_coef_cdfs_default(qctx, 8, 8, 1)). */
 typedef struct mt_uv16_params {
   int32_t luma_stride;   /* stride of the luma reconstruction the CfL AC reads */
-  int32_t joint_k;       /* shortlist length, clamped to 1..12 (uv8_joint_k) */
+  int32_t joint_k;       /* 4:2:0: shortlist length, clamped to 1..12 (uv8_joint_k) */
   int32_t angle_deltas;  /* try_angle_deltas_av1(16, base_q_idx) */
-  int32_t reserved;
+  float dir_lambda;      /* 4:4:4: the directional stage's lambda (emit_mlam: uv16_444_mlam_c is off) */
 } mt_uv16_params;
 typedef struct mt_uv16_job {
   uint16_t px, py;          /* 16x16 luma leaf origin */
@@ -825,6 +825,50 @@ int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                      const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
                      const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
                      const mt_uv_mode_costs* mode_costs, const mt_uv16_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
+
+/* The 16x16 leaf's 4:4:4 chroma search (pick_uv16_444,
+ * src/coder/block16.rs:437-978, shipped tuning: no palette outside screen
+ * content, uv16_444_mlam_c off, cfl_alpha_rd_steps 0) on the leaf's 16x16
+ * chroma blocks (the luma position):
+ *   1. DC: per plane DCT_DCT with the QM, the plain trellis_optimize (the
+ *      4:4:4 chroma_rect_trellis), preserve_dc, the inverse, sse_recon and
+ *      chroma_bits (coefficient class TX_16X16, txb_skip context 7 + above
+ *      non-zero + left non-zero over four bytes each, dc_sign over 4 + 4);
+ *   2. CfL: the 4:4:4 AC of the leaf's luma reconstruction, each plane's
+ *      cfl_best_alpha, the same chain without preserve_dc; taken when an
+ *      alpha is non-zero and rd_cost_i64(sse_u + sse_v, rd_lambda, bits_u +
+ *      bits_v + uv_mode_bits(CfL)) is below DC's (with uv_mode_bits(DC));
+ *   3. with dir_lambda: the current choice's total rd_lambda' x mode bits +
+ *      the planes' rd_cost_i64, then the 12 modes at delta 0 ranked by the two
+ *      planes' satd_sad_proxy, the 3 best (DirectionalTopK: strict insertion,
+ *      ties to the earlier mode) priced in list order with the mode's
+ *      transform, the trellis, preserve_dc; a winner that is directional with
+ *      angle_deltas set then tries its zone-2 deltas (V: 1..3, H: -3..-1,
+ *      D113 / D135 / D157: +-1..3) predicted with no top-right / bottom-left.
+ * Params as for mt_pick_uv16_420 with the chroma planes at the luma size
+ * (luma_stride may equal prm->stride), the 16x16 chroma QM row (256 weights)
+ * and the chroma TX_16X16 cost slice (mt_coef_cdfs_default(qctx, 16, 16, 1));
+ * rd_lambda is emit_mlam_c, uvp->dir_lambda emit_mlam.  d_cf / d_rec: n x
+ * 512, U then V. */
+typedef struct mt_uv16_444_job {
+  uint16_t px, py;          /* 16x16 leaf origin (luma and chroma) */
+  uint8_t y_mode;
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL of the leaf, MT_CAND_FILTER_TYPE: chroma filter type */
+  uint8_t a_coef[2][4];     /* above coefficient contexts of the block's four 4-sample columns, U then V */
+  uint8_t l_coef[2][4];
+  uint8_t reserved[2];
+} mt_uv16_444_job;
+int mt_pick_uv16_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv16_444_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream);
+int mt_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv16_444_job* jobs, int32_t n,
                      mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
 
 /* Host-buffer form (planes stride x frame_h; costs and qm row on the host). */

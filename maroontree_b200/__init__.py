@@ -238,27 +238,42 @@ def uv_mode_bits(costs, y_mode, uv_mode, cfl=None):
     return load().mt_uv_mode_bits(C.byref(costs), y_mode, uv_mode, int(cfl is not None), au, av)
 
 
-def uv16_params(luma_stride, joint_k=4, angle_deltas=True):
+def uv16_params(luma_stride, joint_k=4, angle_deltas=True, dir_lambda=0.0):
+    """``mt_uv16_params``: dir_lambda is the 4:4:4 search's directional-stage lambda."""
     u = abi.Uv16Params()
-    u.luma_stride, u.joint_k, u.angle_deltas = luma_stride, joint_k, int(bool(angle_deltas))
+    u.luma_stride, u.joint_k, u.angle_deltas, u.dir_lambda = luma_stride, joint_k, int(bool(angle_deltas)), dir_lambda
     return u
+
+
+def _pick_uv16(entry, dtype, per_job, src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs,
+               jobs, want_cf, want_rec):
+    planes = [np.ascontiguousarray(a, np.uint16) for a in (src_u, src_v, rec_u, rec_v, luma)]
+    jobs = np.ascontiguousarray(jobs, dtype)
+    n = len(jobs)
+    res = np.zeros(n, abi.UV16_RESULT_DTYPE)
+    cf = np.zeros((n, per_job), np.int32) if want_cf else None
+    rec = np.zeros((n, per_job), np.uint16) if want_rec else None
+    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
+    _check(getattr(load(), entry)(*[ptr(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(quant), ptr(qm),
+                                  C.byref(costs), C.byref(mode_costs), ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)),
+           entry)
+    return res, cf, rec
 
 
 def pick_uv16_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs, jobs, want_cf=False,
                   want_rec=False):
     """pick_uv16_420 over (16x16 leaf) jobs (``mt_pick_uv16_420``): (results,
     levels n x 128 or None, reconstruction n x 128 or None), U then V."""
-    planes = [np.ascontiguousarray(a, np.uint16) for a in (src_u, src_v, rec_u, rec_v, luma)]
-    jobs = np.ascontiguousarray(jobs, abi.UV16_JOB_DTYPE)
-    n = len(jobs)
-    res = np.zeros(n, abi.UV16_RESULT_DTYPE)
-    cf = np.zeros((n, 128), np.int32) if want_cf else None
-    rec = np.zeros((n, 128), np.uint16) if want_rec else None
-    qm = None if qmrow is None else np.ascontiguousarray(qmrow, np.uint8)
-    _check(load().mt_pick_uv16_420(*[ptr(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(quant), ptr(qm),
-                                   C.byref(costs), C.byref(mode_costs), ptr(jobs), n, ptr(res), ptr(cf), ptr(rec)),
-           "mt_pick_uv16_420")
-    return res, cf, rec
+    return _pick_uv16("mt_pick_uv16_420", abi.UV16_JOB_DTYPE, 128, src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant,
+                      qmrow, costs, mode_costs, jobs, want_cf, want_rec)
+
+
+def pick_uv16_444(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs, jobs, want_cf=False,
+                  want_rec=False):
+    """pick_uv16_444 over (16x16 leaf) jobs (``mt_pick_uv16_444``): (results,
+    levels n x 512 or None, reconstruction n x 512 or None), U then V."""
+    return _pick_uv16("mt_pick_uv16_444", abi.UV16_444_JOB_DTYPE, 512, src_u, src_v, rec_u, rec_v, luma, prm, uvp,
+                      quant, qmrow, costs, mode_costs, jobs, want_cf, want_rec)
 
 
 def split16_params(frame_w, frame_h, stride=None, trellis_lambda0=0.05, rd_lambda=1.0, band_tilt=0.0,

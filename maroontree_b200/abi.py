@@ -100,7 +100,7 @@ class UvModeCosts(C.Structure):
 
 class Uv16Params(C.Structure):
     """mt_uv16_params."""
-    _fields_ = [(n, C.c_int32) for n in ("luma_stride", "joint_k", "angle_deltas", "reserved")]
+    _fields_ = [(n, C.c_int32) for n in ("luma_stride", "joint_k", "angle_deltas")] + [("dir_lambda", C.c_float)]
 
 
 UV_CFL_PRED = 13
@@ -110,6 +110,9 @@ UV16_RESULT_DTYPE = np.dtype([("total", "<f4"), ("dc_total", "<f4"), ("cfl_total
                               ("angle_delta", "i1"), ("cfl_alpha", "i1", (2,))])
 assert C.sizeof(UvModeCdfs) == 2 * (13 * 14 + 8 * 7 + 8 + 6 * 16) and C.sizeof(UvModeCosts) == 4 * (13 * 14 + 8 * 7 + 8 + 6 * 16)
 assert UV16_JOB_DTYPE.itemsize == 16 and UV16_RESULT_DTYPE.itemsize == 16
+UV16_444_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("y_mode", "u1"), ("flags", "u1"),
+                               ("a_coef", "u1", (2, 4)), ("l_coef", "u1", (2, 4)), ("reserved", "u1", (2,))])
+assert UV16_444_JOB_DTYPE.itemsize == 24
 
 SPLIT16_JOB_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"), ("reserved", "u1"),
@@ -460,6 +463,11 @@ def _bind(lib):
         "mt_pick_uv16_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
                                        C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
                                        C.c_int32, _P, _P, _P]),
+        "mt_pick_uv16_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                       C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
+                                       C.c_int32, _P, _P, _P]),
+        "mt_pick_uv16_444_device": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                              C.POINTER(Quant), _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
         "mt_grid16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
                                             C.c_int32, _P, _P, _P]),
         "mt_grid16_luma": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts),
@@ -523,6 +531,7 @@ EXPORTED_SYMBOLS = (
     "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
     "mt_grid16_luma_device", "mt_grid16_luma", "mt_uv_mode_cdfs_default", "mt_uv_mode_costs_build",
     "mt_uv_mode_bits", "mt_pick_uv16_420_device", "mt_pick_uv16_420",
+    "mt_pick_uv16_444_device", "mt_pick_uv16_444",
 )
 
 

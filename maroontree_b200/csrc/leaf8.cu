@@ -25,6 +25,14 @@ namespace {
 using namespace mtd;
 
 constexpr int kLeafThreads = 128;
+// The 32x32 and 64x64 searches have few jobs per frame (1,980 32x32 blocks x 13
+// modes, 480 64x64 blocks at 1080p) and long serial chains per job: one warp
+// per CTA spreads them over every SM instead of a few.
+constexpr int kBigThreads = 32;
+template <int N>
+constexpr int leaf_threads() {
+  return N == 32 ? kBigThreads : kLeafThreads;
+}
 
 struct LeafArgs {
   mt_split16_params p;
@@ -61,7 +69,7 @@ __device__ __forceinline__ float rd_cost_i64(long long d, float lam, float rate)
 // DCT_DCT, the only intra type of that size, trellis_optimize_ctx of class 3,
 // no tx-type symbol in the rate).
 template <int N, bool REFINE>
-__global__ void __launch_bounds__(kLeafThreads) leaf_kernel(
+__global__ void __launch_bounds__(leaf_threads<N>()) leaf_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_leaf8_job* __restrict__ jobs, int n, mt_leaf8_result* __restrict__ res, int32_t* __restrict__ cf_out,
@@ -231,7 +239,7 @@ struct Patch64Read {
   }
 };
 
-__global__ void __launch_bounds__(kLeafThreads) quad32_kernel(
+__global__ void __launch_bounds__(kBigThreads) quad32_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_quad32_job* __restrict__ jobs, int n, mt_quad32_result* __restrict__ res) {
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(kLeafThreads) quad32_kernel(
 // DCT_DCT symbol (1) of the mode's TX_16X16 tx-type CDF; coef_res_ctx then
 // fills the transform's context bytes.  total = mode cost + (dist + mlam x
 // bits) + mlam x depth_bits, f32 in that order.
-__global__ void __launch_bounds__(kLeafThreads) grid16_kernel(
+__global__ void __launch_bounds__(kBigThreads) grid16_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_grid16_job* __restrict__ jobs, int n, mt_grid16_result* __restrict__ res, int32_t* __restrict__ cf_out) {
@@ -485,7 +493,8 @@ int leaf_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split16
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  leaf_kernel<N, REFINE><<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+  constexpr int T = leaf_threads<N>();
+  leaf_kernel<N, REFINE><<<(unsigned)((n + T - 1) / T), T, 0,
                          reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
                                                                    d_results, d_cf, d_rec);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
@@ -509,7 +518,7 @@ int quad32_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  quad32_kernel<<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+  quad32_kernel<<<(unsigned)((n + kBigThreads - 1) / kBigThreads), kBigThreads, 0,
                   reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
                                                             d_results);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
@@ -528,7 +537,7 @@ int grid16_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  grid16_kernel<<<(unsigned)((n + kLeafThreads - 1) / kLeafThreads), kLeafThreads, 0,
+  grid16_kernel<<<(unsigned)((n + kBigThreads - 1) / kBigThreads), kBigThreads, 0,
                   reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
                                                             d_results, d_cf);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;

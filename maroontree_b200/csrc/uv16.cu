@@ -26,7 +26,7 @@ namespace {
 
 using namespace mtd;
 
-constexpr int kUvThreads = 64;
+constexpr int kUvThreads = 32;  // one warp per CTA: 8,040 leaves at 1080p reach every SM
 constexpr int kJointModes = 12;
 constexpr int kMaxJoint = 12;
 
@@ -358,6 +358,300 @@ __global__ void __launch_bounds__(kUvThreads) uv16_420_kernel(
         rec_out[(size_t)j * 128 + pl * 64 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
 }
 
+// ---- 4:4:4: pick_uv16_444 ----
+
+struct Uv444Slot {
+  int16_t pred[2][256];
+  int16_t cf[2][256];
+  int16_t rr[2][256];
+};
+
+struct Uv444Work {
+  Uv444Slot s[2];  // the current choice and the candidate
+  int32_t u[512];  // prediction edges, then the targets [0, 256) and the transform temporary [256, 512)
+  int16_t resid[256];
+  int16_t ac[256];
+  float suf[257];  // trellis16 scratch
+  uint8_t lv[288];
+};
+
+struct PlaneCost {
+  long long sse;
+  float bits;
+};
+
+// One 16x16 plane of a candidate after its prediction: the transform with
+// the QM, the plain trellis_optimize (4:4:4's chroma_rect_trellis),
+// preserve_dc when `keep_dc`, the inverse, sse_recon and chroma_bits.
+__device__ PlaneCost plane_chain16(const UvArgs& a, const UvPlane& P, const mt_coef_costs& T, const uint8_t* qm,
+                                   const float* sQs, const float* lut, int tx, bool keep_dc, int16_t* pred,
+                                   int16_t* cf, int16_t* rr, Uv444Work& w) {
+  const mt_split16_params& p = a.p;
+  const mt_quant& q = a.q;
+  int32_t sum = 0;
+#pragma unroll 8
+  for (int i = 0; i < 256; i++) {
+    const int32_t r = (int32_t)P.src[(size_t)(i >> 4) * p.stride + (i & 15)] - pred[i];
+    w.resid[i] = (int16_t)r;
+    sum += r;
+  }
+  float* tf = reinterpret_cast<float*>(w.u);
+  int32_t* tmp = w.u + 256;
+  fwd16x16(w.resid, tx, q, cf, tf, tmp);
+  if (qm) apply_qm(cf, tf, sQs, 256);
+  if (a.lambda > 0.0f) trellis16(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut);
+  if (keep_dc) {
+    const int32_t mean = sum / 256;
+    if (cf[0] == 0 && abs(mean) >= 8) cf[0] = (int16_t)(mean > 0 ? 1 : -1);
+  }
+  inv16x16(cf, tx, q, qm, rr, tmp);
+  ErrBlock<int16_t, int16_t> eb;
+  eb.src = P.src;
+  eb.stride = p.stride;
+  eb.pred = pred;
+  eb.resid = rr;
+  eb.w = 16;
+  eb.vw = P.vw;
+  eb.vh = P.vh;
+  eb.maxv = (1 << p.bd) - 1;
+  PlaneCost c;
+  c.sse = sse_recon_block(eb, p.wsse_scale);
+  c.bits = rate_bounded<16>(cf, T, P.sk, P.ds, 0, -1, p.use_skip_bits != 0, P.skip1, P.skip0,
+                            __int_as_float(0x7f800000), w.lv);
+  return c;
+}
+
+// cfl_best_alpha over a 16x16 block's displayed part (as cfl_alpha).
+__device__ int cfl_alpha16(const int16_t* ac, const UvPlane& P, int stride, int32_t dc, int32_t maxv) {
+  long long num = 0, den = 0;
+  for (int y = 0; y < P.vh; y++)
+    for (int x = 0; x < P.vw; x++) {
+      const long long v = ac[y * 16 + x];
+      num += (long long)((int32_t)P.src[(size_t)y * stride + x] - dc) * v;
+      den += v * v;
+    }
+  if (den == 0) return 0;
+  const long long sg = num > 0 ? 1 : (num < 0 ? -1 : 0);
+  long long a0 = (64 * num + (den >> 1) * sg) / den;
+  a0 = a0 < -16 ? -16 : (a0 > 16 ? 16 : a0);
+  long long best_e = 0x7fffffffffffffffLL;
+  int best_a = 0;
+  for (int c = (int)a0 - 3; c <= (int)a0 + 3; c++) {
+    if (c < -16 || c > 16) continue;
+    long long e = 0;
+    for (int y = 0; y < P.vh; y++)
+      for (int x = 0; x < P.vw; x++) {
+        const long long d = (int32_t)P.src[(size_t)y * stride + x] - cfl_pred_pixel(dc, ac[y * 16 + x], c, maxv);
+        e += d * d;
+      }
+    if (e < best_e) {
+      best_e = e;
+      best_a = c;
+    }
+  }
+  return best_a;
+}
+
+__global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
+    const uint16_t* __restrict__ src_u, const uint16_t* __restrict__ src_v, const uint16_t* __restrict__ rec_u,
+    const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_444_job* __restrict__ jobs, int n,
+    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+  __shared__ mt_coef_costs sT;
+  __shared__ mt_uv_mode_costs sM;
+  __shared__ uint8_t sQm[256];
+  __shared__ float sQs[256];
+  __shared__ float sLut[64];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    const float* gm = reinterpret_cast<const float*>(mode_costs);
+    float* sm = reinterpret_cast<float*>(&sM);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_uv_mode_costs) / 4); i += blockDim.x) sm[i] = gm[i];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+      const int wq = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)wq;
+      sQs[i] = fwd_qm_scale(wq);
+    }
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) sLut[i] = kCoefRateLut[i];
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_uv16_444_job jb = jobs[j];
+  mt_uv16_result& r = res[j];
+  const int cx = jb.px, cy = jb.py;
+  const float kInf = __int_as_float(0x7f800000);
+  const bool ok = (cx & 15) == 0 && (cy & 15) == 0 && cx + 16 <= p.frame_w && cy + 16 <= p.frame_h &&
+                  jb.y_mode <= MT_PAETH_PRED;
+  if (!ok) {
+    r.total = r.dc_total = r.cfl_total = kInf;
+    r.uv_mode = 255;
+    r.angle_delta = 0;
+    r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
+    if (cf_out)
+      for (int i = 0; i < 512; i++) cf_out[(size_t)j * 512 + i] = 0;
+    if (rec_out)
+      for (int i = 0; i < 512; i++) rec_out[(size_t)j * 512 + i] = 0;
+    return;
+  }
+  const mt_coef_costs& T = sT;
+  const mt_uv_mode_costs& M = sM;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float mlam = p.rd_lambda, dlam = a.u.dir_lambda;
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const bool ft = jb.flags & MT_CAND_FILTER_TYPE;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  UvPlane P[2];
+  for (int pl = 0; pl < 2; pl++) {
+    UvPlane& q = P[pl];
+    q.src = (pl ? src_v : src_u) + (size_t)cy * p.stride + cx;
+    q.rec = pl ? rec_v : rec_u;
+    q.vw = min(max(vis_w - cx, 0), 16);
+    q.vh = min(max(vis_h - cy, 0), 16);
+    bool anz = false, lnz = false;
+    int s = -8;
+    for (int k = 0; k < 4; k++) {
+      anz |= jb.a_coef[pl][k] != 0x40;
+      lnz |= jb.l_coef[pl][k] != 0x40;
+      s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
+    }
+    q.sk = 7 + anz + lnz;  // skip_ctx_16
+    q.ds = (s != 0) + (s > 0);  // dc_sign_ctx_16
+    q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
+    q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
+  }
+  Uv444Work w;
+  // 1. DC (block16.rs:451-479), slot 0
+  int32_t dc[2];
+  PlaneCost dcc[2], cfc[2];
+  for (int pl = 0; pl < 2; pl++) {
+    predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
+                   w.s[0].pred[pl], w.u);
+    dc[pl] = w.s[0].pred[pl][0];
+    dcc[pl] = plane_chain16(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, true, w.s[0].pred[pl], w.s[0].cf[pl],
+                            w.s[0].rr[pl], w);
+  }
+  // 2. CfL against DC (:480-597), slot 1
+  {
+    const int ls = a.u.luma_stride;
+    const uint16_t* l = luma + (size_t)cy * ls + cx;
+    int32_t sum = 128;
+    for (int i = 0; i < 256; i++) {
+      const int32_t v = (int32_t)l[(size_t)(i >> 4) * ls + (i & 15)] << 3;
+      w.ac[i] = (int16_t)v;
+      sum += v;
+    }
+    const int32_t mean = sum >> 8;
+    for (int i = 0; i < 256; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
+  }
+  int alpha[2];
+  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha16(w.ac, P[pl], p.stride, dc[pl], maxv);
+  for (int pl = 0; pl < 2; pl++) {
+    for (int i = 0; i < 256; i++) w.s[1].pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
+    cfc[pl] = plane_chain16(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, false, w.s[1].pred[pl], w.s[1].cf[pl],
+                            w.s[1].rr[pl], w);
+  }
+  const float sig = uv_mode_bits(M, jb.y_mode, MT_UV_CFL_PRED, true, alpha[0], alpha[1]);
+  const float dc_bits = uv_mode_bits(M, jb.y_mode, MT_DC_PRED, false, 0, 0);
+  const float dc_total = rd_cost_i64(dcc[0].sse + dcc[1].sse, mlam, __fadd_rn(__fadd_rn(dcc[0].bits, dcc[1].bits), dc_bits));
+  const float cfl_total = rd_cost_i64(cfc[0].sse + cfc[1].sse, mlam, __fadd_rn(__fadd_rn(cfc[0].bits, cfc[1].bits), sig));
+  const bool use_cfl = cfl_total < dc_total && (alpha[0] != 0 || alpha[1] != 0);
+  int best = use_cfl ? 1 : 0;
+  const PlaneCost* cur = use_cfl ? cfc : dcc;
+  // 3. the directional stage on dir_lambda (:598-772): the current choice's
+  // total, then the ranked modes
+  float best_total = __fmul_rn(dlam, use_cfl ? sig : dc_bits);
+  for (int pl = 0; pl < 2; pl++) best_total = __fadd_rn(best_total, rd_cost_i64(cur[pl].sse, dlam, cur[pl].bits));
+  int mode = MT_DC_PRED, delta = 0;
+  // rank_chroma_modes (superblock.rs:469-513) into DirectionalTopK (coder.rs:326-365), K = 3
+  unsigned long long tc[3];
+  int tm[3], tn = 0;
+  int16_t* sp = w.s[1 - best].pred[0];
+  for (int ci = 0; ci < kJointModes; ci++) {
+    const int m = kJointList[ci];
+    unsigned long long sc = 0;
+    for (int pl = 0; pl < 2; pl++) {
+      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd, sp, w.u);
+      sc += satd_sad_proxy<16>(pl ? src_v : src_u, p.stride, cx, cy, sp, P[pl].vw, P[pl].vh);
+    }
+    int pos = tn < 3 ? tn : 2;
+    if (tn == 3 && sc >= tc[pos]) continue;
+    if (tn < 3) pos = tn++;
+    while (pos > 0 && sc < tc[pos - 1]) {
+      tc[pos] = tc[pos - 1];
+      tm[pos] = tm[pos - 1];
+      pos--;
+    }
+    tc[pos] = sc;
+    tm[pos] = m;
+  }
+  for (int ci = 0; ci < kJointModes; ci++) {
+    const int m = kJointList[ci];
+    bool in = false;
+    for (int e = 0; e < tn; e++) in |= tm[e] == m;
+    if (!in) continue;
+    const int tx = chroma_tx(m);
+    float total = __fmul_rn(dlam, uv_mode_bits(M, jb.y_mode, m, false, 0, 0));
+    Uv444Slot& c = w.s[1 - best];
+    for (int pl = 0; pl < 2; pl++) {
+      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd,
+                     c.pred[pl], w.u);
+      const PlaneCost pc = plane_chain16(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+      total = __fadd_rn(total, rd_cost_i64(pc.sse, dlam, pc.bits));
+    }
+    if (total < best_total) {
+      best_total = total;
+      mode = m;
+      best = 1 - best;
+    }
+  }
+  // the zone-2 angle deltas of a directional winner (uv_ad, :743-778)
+  if (a.u.angle_deltas && directional(mode)) {
+    const int m = mode, tx = chroma_tx(m);
+    int lo = 0, hi = -1;
+    if (m == MT_V_PRED) lo = 1, hi = 3;
+    else if (m == MT_H_PRED) lo = -3, hi = -1;
+    else if (m == MT_D113_PRED || m == MT_D135_PRED || m == MT_D157_PRED) lo = -3, hi = 3;
+    const float base_sig = __fsub_rn(uv_mode_bits(M, jb.y_mode, m, false, 0, 0), M.angle_delta[m - MT_V_PRED][3]);
+    for (int d = lo; d <= hi; d++) {
+      if (d == 0) continue;
+      float total = __fmul_rn(dlam, __fadd_rn(base_sig, M.angle_delta[m - MT_V_PRED][d + 3]));
+      Uv444Slot& c = w.s[1 - best];
+      for (int pl = 0; pl < 2; pl++) {
+        predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, false, false, ft, p.bd, c.pred[pl],
+                       w.u);
+        const PlaneCost pc = plane_chain16(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+        total = __fadd_rn(total, rd_cost_i64(pc.sse, dlam, pc.bits));
+      }
+      if (total < best_total) {
+        best_total = total;
+        delta = d;
+        best = 1 - best;
+      }
+    }
+  }
+  r.total = best_total;
+  r.dc_total = dc_total;
+  r.cfl_total = cfl_total;
+  r.uv_mode = (uint8_t)(mode != MT_DC_PRED ? mode : (use_cfl ? MT_UV_CFL_PRED : MT_DC_PRED));
+  r.angle_delta = (int8_t)delta;
+  r.cfl_alpha[0] = (int8_t)alpha[0];
+  r.cfl_alpha[1] = (int8_t)alpha[1];
+  const Uv444Slot& b = w.s[best];
+  if (cf_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 256; i++) cf_out[(size_t)j * 512 + pl * 256 + i] = b.cf[pl][i];
+  if (rec_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 256; i++)
+        rec_out[(size_t)j * 512 + pl * 256 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
+}
+
 int uv_check(const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q, int32_t n) {
   if (!p || !u || !q || n < 0) return MT_ERR_INVALID_INPUT;
   if (p->bd != 8) return MT_ERR_UNSUPPORTED;
@@ -368,7 +662,41 @@ int uv_check(const mt_split16_params* p, const mt_uv16_params* u, const mt_quant
   return MT_OK;
 }
 
+// 4:4:4: the chroma planes have the luma size, so the luma stride needs only
+// the frame width.
+int uv_check_444(const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q, int32_t n) {
+  if (!p || !u || !q || n < 0) return MT_ERR_INVALID_INPUT;
+  if (p->bd != 8) return MT_ERR_UNSUPPORTED;
+  if (p->frame_w < 16 || p->frame_h < 16 || p->stride < p->frame_w || p->vis_w < 0 || p->vis_h < 0)
+    return MT_ERR_INVALID_INPUT;
+  if (u->luma_stride < p->frame_w) return MT_ERR_INVALID_INPUT;
+  if (!(p->rd_lambda > 0.0f) || !(p->wsse_scale >= 0.0f)) return MT_ERR_INVALID_INPUT;
+  return MT_OK;
+}
+
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+int uv444_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* luma,
+                 const mt_split16_params* prm, const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm,
+                 const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mc, const mt_uv16_444_job* d_jobs, int32_t n,
+                 mt_uv16_result* d_res, int32_t* d_cf, uint16_t* d_rec, void* stream) {
+  const int rc = uv_check_444(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!su || !sv || !ru || !rv || !luma || !d_costs || !d_mc || !d_jobs || !d_res) return MT_ERR_INVALID_INPUT;
+  if (!(uvp->dir_lambda > 0.0f)) return MT_ERR_INVALID_INPUT;
+  UvArgs a;
+  a.p = *prm;
+  a.u = *uvp;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
+  uv16_444_kernel<<<(unsigned)((n + kUvThreads - 1) / kUvThreads), kUvThreads, 0,
+                    reinterpret_cast<cudaStream_t>(stream)>>>(su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs,
+                                                              n, d_res, d_cf, d_rec);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
 
 int uv16_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* luma,
                 const mt_split16_params* prm, const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm,
@@ -391,6 +719,61 @@ int uv16_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, cons
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
+// Host-buffer form of either search: the planes, tables and jobs copied to one
+// device allocation, the launch, the results (and levels / reconstruction,
+// per_job entries each) copied back.
+template <typename J, typename L>
+int uv_host(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+            const uint16_t* luma, size_t luma_rows, const mt_split16_params* prm, const mt_uv16_params* uvp,
+            const mt_quant* quant, const uint8_t* qm_row, size_t qm_len, const mt_coef_costs* costs,
+            const mt_uv_mode_costs* mode_costs, const J* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
+            uint16_t* rec_out, size_t per_job, L launch) {
+  if (!prm || !uvp || !quant || n < 0) return MT_ERR_INVALID_INPUT;
+  if (n == 0) return MT_OK;
+  if (!src_u || !src_v || !rec_u || !rec_v || !luma || !costs || !mode_costs || !jobs || !results)
+    return MT_ERR_INVALID_INPUT;
+  if (prm->stride <= 0 || prm->frame_h <= 0 || uvp->luma_stride <= 0) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)prm->stride * prm->frame_h * 2;
+  const size_t lplane = (size_t)uvp->luma_stride * luma_rows * 2;
+  size_t o = 0;
+  const size_t o_su = o, o_sv = (o += up256(plane)), o_ru = (o += up256(plane)), o_rv = (o += up256(plane));
+  const size_t o_l = (o += up256(plane)), o_qm = (o += up256(lplane)), o_c = (o += up256(qm_len));
+  const size_t o_mc = (o += up256(sizeof(mt_coef_costs))), o_j = (o += up256(sizeof(mt_uv_mode_costs)));
+  const size_t o_r = (o += up256((size_t)n * sizeof(J)));
+  const size_t o_cf = (o += up256((size_t)n * sizeof(mt_uv16_result)));
+  const size_t o_rec = (o += cf_out ? up256((size_t)n * per_job * 4) : 0);
+  const size_t total = o + (rec_out ? up256((size_t)n * per_job * 2) : 0);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
+  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
+  cudaError_t e = cudaMemcpy(d + o_su, src_u, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_sv, src_v, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_ru, rec_u, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_rv, rec_v, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_l, luma, lplane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, qm_len, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_c, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_mc, mode_costs, sizeof(mt_uv_mode_costs), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_j, jobs, (size_t)n * sizeof(J), cudaMemcpyHostToDevice);
+  int rc = MT_OK;
+  if (e == cudaSuccess) {
+    auto U = [&](size_t off) { return reinterpret_cast<const uint16_t*>(d + off); };
+    rc = launch(U(o_su), U(o_sv), U(o_ru), U(o_rv), U(o_l), has_qm ? d + o_qm : nullptr,
+                reinterpret_cast<const mt_coef_costs*>(d + o_c), reinterpret_cast<const mt_uv_mode_costs*>(d + o_mc),
+                reinterpret_cast<const J*>(d + o_j), reinterpret_cast<mt_uv16_result*>(d + o_r),
+                cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr,
+                rec_out ? reinterpret_cast<uint16_t*>(d + o_rec) : nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(results, d + o_r, (size_t)n * sizeof(mt_uv16_result), cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && cf_out)
+      e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * per_job * 4, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && rec_out)
+      e = cudaMemcpy(rec_out, d + o_rec, (size_t)n * per_job * 2, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
 }  // namespace
 
 extern "C" {
@@ -410,49 +793,42 @@ int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                      const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
                      const mt_uv_mode_costs* mode_costs, const mt_uv16_job* jobs, int32_t n,
                      mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
-  int rc = uv_check(prm, uvp, quant, n);
+  const int rc = uv_check(prm, uvp, quant, n);
   if (rc != MT_OK) return rc;
-  if (n == 0) return MT_OK;
-  if (!src_u || !src_v || !rec_u || !rec_v || !luma || !costs || !mode_costs || !jobs || !results)
-    return MT_ERR_INVALID_INPUT;
-  const size_t plane = (size_t)prm->stride * prm->frame_h * 2;
-  const size_t lplane = (size_t)uvp->luma_stride * 2 * prm->frame_h * 2;
-  size_t o = 0;
-  const size_t o_su = o, o_sv = (o += up256(plane)), o_ru = (o += up256(plane)), o_rv = (o += up256(plane));
-  const size_t o_l = (o += up256(plane)), o_qm = (o += up256(lplane)), o_c = (o += up256(64));
-  const size_t o_mc = (o += up256(sizeof(mt_coef_costs))), o_j = (o += up256(sizeof(mt_uv_mode_costs)));
-  const size_t o_r = (o += up256((size_t)n * sizeof(mt_uv16_job)));
-  const size_t o_cf = (o += up256((size_t)n * sizeof(mt_uv16_result)));
-  const size_t o_rec = (o += cf_out ? up256((size_t)n * 128 * 4) : 0);
-  const size_t total = o + (rec_out ? up256((size_t)n * 128 * 2) : 0);
-  uint8_t* d = nullptr;
-  if (cudaMalloc(&d, total) != cudaSuccess) return MT_ERR_ALLOC;
-  const bool has_qm = quant->qm_level < 15 && qm_row != nullptr;
-  cudaError_t e = cudaMemcpy(d + o_su, src_u, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_sv, src_v, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_ru, rec_u, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_rv, rec_v, plane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_l, luma, lplane, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && has_qm) e = cudaMemcpy(d + o_qm, qm_row, 64, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_c, costs, sizeof(mt_coef_costs), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_mc, mode_costs, sizeof(mt_uv_mode_costs), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d + o_j, jobs, (size_t)n * sizeof(mt_uv16_job), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) {
-    auto U = [&](size_t off) { return reinterpret_cast<const uint16_t*>(d + off); };
-    rc = uv16_device(U(o_su), U(o_sv), U(o_ru), U(o_rv), U(o_l), prm, uvp, quant, has_qm ? d + o_qm : nullptr,
-                     reinterpret_cast<const mt_coef_costs*>(d + o_c),
-                     reinterpret_cast<const mt_uv_mode_costs*>(d + o_mc), reinterpret_cast<const mt_uv16_job*>(d + o_j),
-                     n, reinterpret_cast<mt_uv16_result*>(d + o_r), cf_out ? reinterpret_cast<int32_t*>(d + o_cf) : nullptr,
-                     rec_out ? reinterpret_cast<uint16_t*>(d + o_rec) : nullptr, nullptr);
-    if (rc == MT_OK) e = cudaMemcpy(results, d + o_r, (size_t)n * sizeof(mt_uv16_result), cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && cf_out)
-      e = cudaMemcpy(cf_out, d + o_cf, (size_t)n * 128 * 4, cudaMemcpyDeviceToHost);
-    if (rc == MT_OK && e == cudaSuccess && rec_out)
-      e = cudaMemcpy(rec_out, d + o_rec, (size_t)n * 128 * 2, cudaMemcpyDeviceToHost);
-  }
-  cudaFree(d);
+  return uv_host(src_u, src_v, rec_u, rec_v, luma, 2 * (size_t)prm->frame_h, prm, uvp, quant, qm_row, 64, costs,
+                 mode_costs, jobs, n, results, cf_out, rec_out, 128,
+                 [&](const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* l,
+                     const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc, const mt_uv16_job* j,
+                     mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
+                   return uv16_device(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
+                 });
+}
+
+int mt_pick_uv16_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv16_444_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream) {
+  return uv444_device(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs, d_mode_costs,
+                      d_jobs, n, d_results, d_cf, d_rec, stream);
+}
+
+int mt_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv16_444_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  const int rc = uv_check_444(prm, uvp, quant, n);
   if (rc != MT_OK) return rc;
-  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+  if (n > 0 && !(uvp->dir_lambda > 0.0f)) return MT_ERR_INVALID_INPUT;
+  return uv_host(src_u, src_v, rec_u, rec_v, luma, (size_t)prm->frame_h, prm, uvp, quant, qm_row, 256, costs,
+                 mode_costs, jobs, n, results, cf_out, rec_out, 512,
+                 [&](const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* l,
+                     const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc,
+                     const mt_uv16_444_job* j, mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
+                   return uv444_device(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
+                 });
 }
 
 }  // extern "C"

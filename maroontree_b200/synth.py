@@ -515,6 +515,31 @@ def planes420(rgb, seed):
     return src, rec
 
 
+def planes444(rgb, seed):
+    """Source and reconstruction planes of a 4:4:4 frame from an RGB image:
+    luma by rgb_to_luma, U the blue and V the red channel, each reconstruction
+    the plane plus a seeded +-3 coding error."""
+    c = np.asarray(rgb)
+    src = [rgb_to_luma(np.asarray(rgb, np.uint8)), c[:, :, 2].astype(np.uint16), c[:, :, 0].astype(np.uint16)]
+    rec = [synthetic_recon(p, seed + 7 + k) for k, p in enumerate(src)]
+    return src, rec
+
+
+def uv16_444_jobs(w, h, seed, every=1):
+    """16x16-leaf jobs of the 4:4:4 chroma search (mt_uv16_444_job), as
+    uv16_jobs with four coefficient-context bytes per plane and side."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for py in range(0, h - 15, 16):
+        for px in range(0, w - 15, 16):
+            if rng.random() > 1.0 / every:
+                continue
+            fl = block_flags(px, py, w, h, 16) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
+            ctx = coef_ctx_bytes(rng, 16)
+            rows.append((px, py, int(rng.integers(0, 13)), fl, ctx[:8].reshape(2, 4), ctx[8:].reshape(2, 4), (0, 0)))
+    return np.array(rows, abi.UV16_444_JOB_DTYPE)
+
+
 def uv16_jobs(w, h, seed, every=1):
     """16x16-leaf jobs of the 4:2:0 chroma search (mt_uv16_job): every
     16x16 leaf of a w x h frame (or about one in `every`), a random luma

@@ -93,6 +93,9 @@ def load():
             "or_pick_uv16_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
                                            C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
                                            C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
+            "or_pick_uv16_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
+                                           C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
+                                           C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_grid16_luma": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
                                          C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P]),
             "or_leaf32": (C.c_int, [_P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Quant), _P,
@@ -1037,23 +1040,36 @@ def uv_mode_bits(cdfs, y_mode, uv_mode, cfl=None):
     return load().or_uv_mode_bits(C.byref(cdfs), y_mode, uv_mode, int(cfl is not None), au, av)
 
 
-def pick_uv16_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs, threads=1,
-                  want_cf=False, want_rec=False):
-    """pick_uv16_420 of n 16x16 leaves: (results, levels or None, reconstruction or None)."""
+def _pick_uv16(entry, dtype, per_job, src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs,
+               threads, want_cf, want_rec):
     planes = [np.ascontiguousarray(a, np.uint16) for a in (src_u, src_v, rec_u, rec_v, luma)]
-    jobs = np.ascontiguousarray(jobs, abi.UV16_JOB_DTYPE)
+    jobs = np.ascontiguousarray(jobs, dtype)
     n = len(jobs)
     res = np.zeros(n, abi.UV16_RESULT_DTYPE)
-    cf = np.zeros((n, 128), np.int32) if want_cf else None
-    rec = np.zeros((n, 128), np.uint16) if want_rec else None
+    cf = np.zeros((n, per_job), np.int32) if want_cf else None
+    rec = np.zeros((n, per_job), np.uint16) if want_rec else None
     qm = None if qm is None else np.ascontiguousarray(qm, np.uint8)
 
     def run(lo, hi):
-        assert load().or_pick_uv16_420(*[p(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(q), p(qm),
-                                       C.byref(cdfs), C.byref(mode_cdfs), p(jobs[lo:hi]), hi - lo, p(res[lo:hi]),
-                                       None if cf is None else p(cf[lo:hi]),
-                                       None if rec is None else p(rec[lo:hi])) == 0
+        assert getattr(load(), entry)(*[p(a) for a in planes], C.byref(prm), C.byref(uvp), C.byref(q), p(qm),
+                                      C.byref(cdfs), C.byref(mode_cdfs), p(jobs[lo:hi]), hi - lo, p(res[lo:hi]),
+                                      None if cf is None else p(cf[lo:hi]),
+                                      None if rec is None else p(rec[lo:hi])) == 0
 
     _chunked(n, threads, run)
     return res, cf, rec
+
+
+def pick_uv16_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs, threads=1,
+                  want_cf=False, want_rec=False):
+    """pick_uv16_420 of n 16x16 leaves: (results, levels or None, reconstruction or None)."""
+    return _pick_uv16("or_pick_uv16_420", abi.UV16_JOB_DTYPE, 128, src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm,
+                      cdfs, mode_cdfs, jobs, threads, want_cf, want_rec)
+
+
+def pick_uv16_444(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs, threads=1,
+                  want_cf=False, want_rec=False):
+    """pick_uv16_444 of n 16x16 leaves: (results, levels or None, reconstruction or None)."""
+    return _pick_uv16("or_pick_uv16_444", abi.UV16_444_JOB_DTYPE, 512, src_u, src_v, rec_u, rec_v, luma, prm, uvp, q,
+                      qm, cdfs, mode_cdfs, jobs, threads, want_cf, want_rec)
 

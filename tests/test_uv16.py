@@ -222,3 +222,187 @@ def test_uv16_at_config(mt_lib, oracle_lib, cuda, name):
     uvp = mt_lib.uv16_params(src[0].shape[1], joint_k=4, angle_deltas=True)
     jobs = synth.uv16_jobs(wl.w, wl.h, wl.qidx)
     _gpu_case(mt_lib, oracle_lib, src, rec, prm, uvp, q, qm, wl.qctx, jobs, configs.THREADS)
+
+
+# ---- 4:4:4 (pick_uv16_444) ----
+
+def _glue_444(op, src, rec, prm, uvp, q, qm, cd, mc, jb):
+    """pick_uv16_444 of one leaf from the oracle's primitives."""
+    f32 = np.float32
+    cx, cy = int(jb["px"]), int(jb["py"])
+    fl = int(jb["flags"])
+    tr, bl, ft = bool(fl & 1), bool(fl & 2), bool(fl & 4)
+    mlam, dlam = f32(prm.rd_lambda), f32(uvp.dir_lambda)
+    scan = op.default_scan(16)
+    fw, fh = src[1].shape[1], src[1].shape[0]
+    vw, vh = min(max(prm.vis_w - cx, 0), 16), min(max(prm.vis_h - cy, 0), 16)
+    ctx = []
+    for pl in range(2):
+        a, l = [int(v) for v in jb["a_coef"][pl]], [int(v) for v in jb["l_coef"][pl]]
+        sk = 7 + int(any(v != 0x40 for v in a)) + int(any(v != 0x40 for v in l))
+        s = sum(v >> 6 for v in a + l) - 8
+        ctx.append((sk, int(s != 0) + int(s > 0)))
+
+    def plane(pl, pred, tx, keep_dc):
+        s = src[1 + pl][cy:cy + 16, cx:cx + 16].astype(np.int32).ravel()
+        resid = s - pred.ravel()
+        lv, tf = op.fwd_txfm_quant(resid, tx, q, qm)
+        lv = op.trellis_optimize(lv, tf, float(q.dc_q), float(q.ac_q), scan, prm.trellis_lambda0)
+        if keep_dc:
+            mean = int(np.trunc(resid.sum() / 256))
+            if lv[0] == 0 and abs(mean) >= 8:
+                lv[0] = 1 if mean > 0 else -1
+        rr = op.inv_txfm_dequant(lv, tx, q, qm)
+        sse = int(op.sse_recon(src[1 + pl], prm.vis_w, prm.vis_h, [(cx, cy)], pred.ravel(), rr, 16, 16,
+                               scale=prm.wsse_scale)[0])
+        return sse, f32(op.real_block_bits_bounded(lv, scan, 16, 16, cd, ctx[pl][0], ctx[pl][1], -1, 0, INF))
+
+    ym = int(jb["y_mode"])
+    dc = [int(op.intra_predict(rec[1 + pl], cx, cy, 16, 16, abi.DC_PRED)[0, 0]) for pl in range(2)]
+    dcp = [plane(pl, np.full((16, 16), dc[pl]), abi.TX_DCT_DCT, True) for pl in range(2)]
+    blk = np.array([(cx, cy, (dc[0], dc[1]))], abi.CFL_BLOCK_DTYPE)
+    alpha, ac = op.cfl_alpha(rec[0], src[1], src[2], 0, 0, 16, 16, blk, vis=(prm.vis_w, prm.vis_h))
+    al = (int(alpha[0][0]), int(alpha[0][1]))
+    cfp = []
+    for pl in range(2):
+        diff = al[pl] * ac[0]
+        mag = (np.abs(diff) + 32) >> 6
+        cfp.append(plane(pl, np.clip(dc[pl] + np.where(diff < 0, -mag, mag), 0, 255), abi.TX_DCT_DCT, False))
+    sig = f32(op.uv_mode_bits(mc, ym, abi.UV_CFL_PRED, al))
+    dcb = f32(op.uv_mode_bits(mc, ym, abi.DC_PRED))
+    dc_total = f32(f32(dcp[0][0] + dcp[1][0]) + f32(mlam * f32(f32(dcp[0][1] + dcp[1][1]) + dcb)))
+    cfl_total = f32(f32(cfp[0][0] + cfp[1][0]) + f32(mlam * f32(f32(cfp[0][1] + cfp[1][1]) + sig)))
+    use_cfl = cfl_total < dc_total and any(al)
+    cur = cfp if use_cfl else dcp
+    best = f32(dlam * (sig if use_cfl else dcb))
+    for pl in range(2):
+        best = f32(best + f32(f32(cur[pl][0]) + f32(dlam * cur[pl][1])))
+    mode, delta = abi.DC_PRED, 0
+    top = []  # DirectionalTopK, K = 3
+    for m in JOINT:
+        sc = 0
+        for pl in range(2):
+            pp = op.intra_predict(rec[1 + pl], cx, cy, 16, 16, m, 0, tr, bl, ft, fw=fw, fh=fh)
+            d = np.where((np.arange(16)[None, :] < vw) & (np.arange(16)[:, None] < vh),
+                         src[1 + pl][cy:cy + 16, cx:cx + 16].astype(np.int64) - pp, 0)
+            h4 = np.array([[1, 1, 1, 1], [1, -1, 1, -1], [1, 1, -1, -1], [1, -1, -1, 1]])
+            satd = sum(int(np.abs(h4 @ d[ty:ty + 4, tx:tx + 4] @ h4.T).sum()) for ty in range(0, 16, 4)
+                       for tx in range(0, 16, 4))
+            sc += int(np.abs(d).sum()) + (satd >> 2)
+        if len(top) == 3 and sc >= top[-1][0]:
+            continue
+        pos = len(top) if len(top) < 3 else 2
+        if len(top) < 3:
+            top.append(None)
+        while pos > 0 and sc < top[pos - 1][0]:
+            top[pos] = top[pos - 1]
+            pos -= 1
+        top[pos] = (sc, m)
+    txmap = {abi.PAETH_PRED: abi.TX_ADST_ADST, abi.SMOOTH_PRED: abi.TX_ADST_ADST, abi.D135_PRED: abi.TX_ADST_ADST,
+             abi.SMOOTH_V_PRED: abi.TX_ADST_DCT, abi.V_PRED: abi.TX_ADST_DCT, abi.D113_PRED: abi.TX_ADST_DCT,
+             abi.D67_PRED: abi.TX_ADST_DCT, abi.SMOOTH_H_PRED: abi.TX_DCT_ADST, abi.H_PRED: abi.TX_DCT_ADST,
+             abi.D157_PRED: abi.TX_DCT_ADST, abi.D203_PRED: abi.TX_DCT_ADST}
+
+    def price(m, d, etr, ebl, bits):
+        total = f32(dlam * f32(bits))
+        for pl in range(2):
+            pp = op.intra_predict(rec[1 + pl], cx, cy, 16, 16, m, d, etr, ebl, ft, fw=fw, fh=fh)
+            sse, b = plane(pl, pp, txmap.get(m, abi.TX_DCT_DCT), True)
+            total = f32(total + f32(f32(sse) + f32(dlam * b)))
+        return total
+
+    ranked = {m for _, m in top}
+    for m in JOINT:
+        if m in ranked:
+            t = price(m, 0, tr, bl, op.uv_mode_bits(mc, ym, m))
+            if t < best:
+                best, mode = t, m
+    adc = np.ctypeslib.as_array(mc.angle_delta)
+    zone2 = {abi.V_PRED: (1, 2, 3), abi.H_PRED: (-3, -2, -1), abi.D113_PRED: (-3, -2, -1, 1, 2, 3),
+             abi.D135_PRED: (-3, -2, -1, 1, 2, 3), abi.D157_PRED: (-3, -2, -1, 1, 2, 3)}
+    if uvp.angle_deltas and abi.V_PRED <= mode <= abi.D67_PRED:
+        m = mode
+        base = f32(f32(op.uv_mode_bits(mc, ym, m)) - f32(op.cdf_cost(adc[m - abi.V_PRED], 3)))
+        for d in zone2.get(m, ()):
+            t = price(m, d, False, False, f32(base + f32(op.cdf_cost(adc[m - abi.V_PRED], d + 3))))
+            if t < best:
+                best, delta = t, d
+    um = mode if mode != abi.DC_PRED else (abi.UV_CFL_PRED if use_cfl else abi.DC_PRED)
+    return best, dc_total, cfl_total, um, delta, al
+
+
+def _case444(mt, op, w, h, seed, qidx, qm_level, wsse, vis_cut=(0, 0), skip=False, ad=True):
+    src, rec = synth.planes444(synth.generate_rgb(w, h, seed, sigma=4.0, variant="1080p"), seed)
+    q = op.quant_new_chroma(qidx, 0, 0, 8, qm_level)
+    qm = op.qm_row(qm_level, 1, 16) if qm_level < 15 else None
+    sb = [(float(np.float32(1.5 + 0.1 * k)), float(np.float32(0.2 + 0.05 * k))) for k in range(13)] if skip else None
+    prm = mt.split16_params(w, h, trellis_lambda0=0.05, rd_lambda=0.2 * qidx + 3, wsse_scale=wsse,
+                            vis=(w - vis_cut[0], h - vis_cut[1]), skip_bits=sb)
+    uvp = mt.uv16_params(w, angle_deltas=ad, dir_lambda=0.15 * qidx + 2)
+    return src, rec, q, qm, prm, uvp
+
+
+@pytest.mark.parametrize("qidx,qm_level,wsse", [(90, 6, 1.0), (40, 15, 0.0)])
+def test_uv16_444_oracle_glue(oracle_lib, qidx, qm_level, wsse):
+    import maroontree_b200 as mt
+
+    op = oracle_lib
+    src, rec, q, qm, prm, uvp = _case444(mt, op, 96, 64, qidx + 1, qidx, qm_level, wsse, vis_cut=(3, 1))
+    cd = op.default_cdfs(op.qcat(qidx), 16, plane=1)
+    mc = op.uv_mode_cdfs()
+    jobs = synth.uv16_444_jobs(96, 64, qidx)
+    res, _, _ = op.pick_uv16_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd, mc, jobs)
+    f32 = np.float32
+    for i, jb in enumerate(jobs):
+        best, dct, cflt, mode, delta, al = _glue_444(op, src, rec, prm, uvp, q, qm, cd, mc, jb)
+        r = res[i]
+        assert (f32(r["total"]), f32(r["dc_total"]), f32(r["cfl_total"])) == (best, dct, cflt), i
+        assert (int(r["uv_mode"]), int(r["angle_delta"]), tuple(int(v) for v in r["cfl_alpha"])) == (mode, delta, al)
+
+
+def _gpu444(mt, op, src, rec, prm, uvp, q, qm, qctx, jobs, threads):
+    cd = op.default_cdfs(qctx, 16, plane=1)
+    mc = op.uv_mode_cdfs()
+    costs = mt.coef_costs(mt.coef_cdfs_default(qctx, 16, 16, 1))
+    mcost = mt.uv_mode_costs(mt.uv_mode_cdfs_default())
+    got = mt.pick_uv16_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, costs, mcost, jobs, want_cf=True,
+                           want_rec=True)
+    want = op.pick_uv16_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd, mc, jobs, threads=threads,
+                            want_cf=True, want_rec=True)
+    assert got[0].tobytes() == want[0].tobytes()
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2])
+    return got[0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qidx,qm_level,wsse,skip,ad", [(70, 6, 1.0, False, True), (116, 15, 0.0, True, True),
+                                                         (30, 3, 0.75, False, False), (200, 10, 0.0, False, True)])
+def test_uv16_444_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse, skip, ad):
+    src, rec, q, qm, prm, uvp = _case444(mt_lib, oracle_lib, 320, 192, qidx + 5, qidx, qm_level, wsse,
+                                         vis_cut=(5, 2), skip=skip, ad=ad)
+    jobs = synth.uv16_444_jobs(320, 192, qidx)
+    jobs = np.concatenate([jobs, jobs[:2]])
+    jobs["px"][-2] = 312  # leaves the plane: rejected
+    jobs["y_mode"][-1] = 13
+    res = _gpu444(mt_lib, oracle_lib, src, rec, prm, uvp, q, qm, oracle_lib.qcat(qidx), jobs, os.cpu_count() or 1)
+    assert (res["uv_mode"][-2:] == 255).all() and (res["uv_mode"][:-2] != 255).all()
+    kinds = set(int(m) for m in res["uv_mode"][:-2])
+    assert abi.DC_PRED in kinds and len(kinds) >= 4, kinds
+
+
+@pytest.mark.gpu
+def test_uv16_444_at_config(mt_lib, oracle_lib, cuda):
+    """Every 16x16 leaf of the 4:4:4 benchmark frame C1 (512x512, qindex 70):
+    its chroma quantiser and QM level, the chroma TX_16X16 CDFs of its q
+    context, the luma and chroma lambdas of its laws."""
+    import configs
+
+    wl = configs.workload("C1")
+    src, rec = synth.planes444(wl.rgb, wl.qidx)
+    q = mt_lib.quant_new_chroma(wl.qidx, 0, 0, 8, wl.qm_uv)
+    qm = mt_lib.qm_row(wl.qm_uv, 1, 16) if wl.qm_uv < 15 else None
+    prm = mt_lib.split16_params(wl.w, wl.h, trellis_lambda0=wl.lam.trellis_lambda0, rd_lambda=wl.lam.mode_lambda,
+                                wsse_scale=1.0)
+    uvp = mt_lib.uv16_params(wl.w, angle_deltas=True, dir_lambda=wl.lam.lambda_d)
+    jobs = synth.uv16_444_jobs(wl.w, wl.h, wl.qidx)
+    _gpu444(mt_lib, oracle_lib, src, rec, prm, uvp, q, qm, wl.qctx, jobs, configs.THREADS)
