@@ -343,10 +343,17 @@ __global__ void __launch_bounds__(kBigThreads) quad32_kernel(
 // DCT_DCT symbol (1) of the mode's TX_16X16 tx-type CDF; coef_res_ctx then
 // fills the transform's context bytes.  total = mode cost + (dist + mlam x
 // bits) + mlam x depth_bits, f32 in that order.
+// grid16_kernel's per-job working set (in shared memory, see smem_arena).
+struct Grid16Arena {
+  LeafWork<16> w;
+  uint16_t patch[64 * 64];
+};
+
 __global__ void __launch_bounds__(kBigThreads) grid16_kernel(
     const uint16_t* __restrict__ src, const uint16_t* __restrict__ rec, LeafArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
-    const mt_grid16_job* __restrict__ jobs, int n, mt_grid16_result* __restrict__ res, int32_t* __restrict__ cf_out) {
+    const mt_grid16_job* __restrict__ jobs, int n, mt_grid16_result* __restrict__ res, int32_t* __restrict__ cf_out,
+    int arena) {
   __shared__ mt_coef_costs sT;
   constexpr int NN = 256;
   __shared__ uint8_t sQm[NN];
@@ -381,8 +388,9 @@ __global__ void __launch_bounds__(kBigThreads) grid16_kernel(
       for (int i = 0; i < 4096; i++) cf_out[(size_t)j * 4096 + i] = 0;
     return;
   }
-  LeafWork<16> w;
-  uint16_t patch[64 * 64];
+  Grid16Arena& A = smem_arena<Grid16Arena>(arena);
+  LeafWork<16>& w = A.w;
+  uint16_t* patch = A.patch;
   for (int y = 0; y < 64; y++)
     for (int x = 0; x < 64; x++) patch[y * 64 + x] = rec[(size_t)(jb.py + y) * p.stride + jb.px + x];
   const Patch64Read rd{rec, p.stride, jb.px, jb.py, patch};
@@ -537,9 +545,12 @@ int grid16_device(const uint16_t* d_src, const uint16_t* d_recon, const mt_split
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm_row != nullptr;
-  grid16_kernel<<<(unsigned)((n + kBigThreads - 1) / kBigThreads), kBigThreads, 0,
-                  reinterpret_cast<cudaStream_t>(stream)>>>(d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n,
-                                                            d_results, d_cf);
+  const int stride = arena_stride(sizeof(Grid16Arena));
+  int threads = 0;
+  size_t dyn = 0;
+  if (!arena_launch_shape(grid16_kernel, n, stride, kBigThreads, &threads, &dyn)) return MT_ERR_DEVICE;
+  grid16_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+      d_src, d_recon, a, d_qm_row, d_costs, d_jobs, n, d_results, d_cf, stride);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 

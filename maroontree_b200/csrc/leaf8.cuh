@@ -12,6 +12,7 @@
 // cdf_cost_with_table of the same symbol, br_cum the base-range ladder of
 // src/cost.rs:214-241 (equal term for term to hi_tok_cost_with_table).
 #pragma once
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "chain4.cuh"
@@ -464,6 +465,40 @@ __device__ float rate_1d(const C* __restrict__ cf, bool vertical, const mt_coef_
   }
   if (dm != 0) bits = __fadd_rn(bits, T.dc_sign[dcs][cf[0] < 0]);
   return bits;
+}
+
+// A one-thread-per-job kernel's working set in the CTA's dynamic shared
+// memory instead of local memory: thread t's copy at t * stride bytes.
+// arena_stride rounds the size up to 128 bytes and adds 16, so consecutive
+// threads' copies start 4 banks apart and every copy stays 16-byte aligned.
+constexpr int arena_stride(size_t bytes) { return (int)(((bytes + 127) & ~(size_t)127) + 16); }
+
+template <typename A>
+__device__ __forceinline__ A& smem_arena(int stride) {
+  extern __shared__ __align__(16) unsigned char mt_arena_smem[];
+  return *reinterpret_cast<A*>(mt_arena_smem + (size_t)threadIdx.x * stride);
+}
+
+// Launch shape of an arena kernel: n jobs spread over the SMs (one CTA per
+// SM while they fit), at most `cap` threads per CTA and as many copies as fit
+// beside the kernel's static shared memory.  False when not even one fits.
+template <typename K>
+__host__ bool arena_launch_shape(K kernel, int n, int stride, int cap, int* threads, size_t* dyn) {
+  cudaFuncAttributes fa;
+  int dev = 0, sms = 0, optin = 0;
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return false;
+  const long fit = ((long)optin - (long)fa.sharedSizeBytes) / stride;
+  if (fit < 1 || sms < 1) return false;
+  long t = (n + sms - 1) / sms;
+  t = t < 1 ? 1 : t;
+  t = t > cap ? cap : t;
+  t = t > fit ? fit : t;
+  *threads = (int)t;
+  *dyn = (size_t)t * stride;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*dyn) == cudaSuccess;
 }
 
 // The dav1d txb_skip context table of skip_ctx_split

@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kUvThreads) uv16_420_kernel(
     const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_job* __restrict__ jobs, int n,
-    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out, int arena) {
   __shared__ mt_coef_costs sT;
   __shared__ mt_uv_mode_costs sM;
   __shared__ uint8_t sQm[64];
@@ -239,7 +239,7 @@ __global__ void __launch_bounds__(kUvThreads) uv16_420_kernel(
     q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
     q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
   }
-  UvWork w;
+  UvWork& w = smem_arena<UvWork>(arena);
   int best = 0;
   // 1. DC on both planes (block16.rs:999-1046): no mode bits in its total
   int32_t dc[2];
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
     const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_444_job* __restrict__ jobs, int n,
-    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out) {
+    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out, int arena) {
   __shared__ mt_coef_costs sT;
   __shared__ mt_uv_mode_costs sM;
   __shared__ uint8_t sQm[256];
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
     q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
   }
-  Uv444Work w;
+  Uv444Work& w = smem_arena<Uv444Work>(arena);
   // 1. DC (block16.rs:451-479), slot 0
   int32_t dc[2];
   PlaneCost dcc[2], cfc[2];
@@ -692,9 +692,12 @@ int uv444_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, con
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
-  uv16_444_kernel<<<(unsigned)((n + kUvThreads - 1) / kUvThreads), kUvThreads, 0,
-                    reinterpret_cast<cudaStream_t>(stream)>>>(su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs,
-                                                              n, d_res, d_cf, d_rec);
+  const int stride = arena_stride(sizeof(Uv444Work));
+  int threads = 0;
+  size_t dyn = 0;
+  if (!arena_launch_shape(uv16_444_kernel, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
+  uv16_444_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+      su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs, n, d_res, d_cf, d_rec, stride);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
@@ -713,9 +716,12 @@ int uv16_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, cons
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
-  uv16_420_kernel<<<(unsigned)((n + kUvThreads - 1) / kUvThreads), kUvThreads, 0,
-                    reinterpret_cast<cudaStream_t>(stream)>>>(su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs,
-                                                              n, d_res, d_cf, d_rec);
+  const int stride = arena_stride(sizeof(UvWork));
+  int threads = 0;
+  size_t dyn = 0;
+  if (!arena_launch_shape(uv16_420_kernel, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
+  uv16_420_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+      su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs, n, d_res, d_cf, d_rec, stride);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
