@@ -859,6 +859,34 @@ typedef struct mt_uv16_444_job {
   uint8_t l_coef[2][4];
   uint8_t reserved[2];
 } mt_uv16_444_job;
+/* The 32x32 leaf's 4:2:0 chroma search (pick_uv32_420,
+ * src/coder/block32.rs:2797-3120, shipped tuning: uv_ad and uv_ad32 on,
+ * cfl_alpha_rd_steps 0) on the leaf's 16x16 chroma blocks at (px / 2, py / 2):
+ * DC (DCT_DCT with the QM, trellis_optimize_ctx of the chroma TX_16X16 class
+ * in the dc_sign context of the plane's four above / four left bytes,
+ * preserve_dc); CfL from the 4:2:0 AC of the 32x32 luma reconstruction,
+ * taken when an alpha is non-zero and body + rd_lambda x (uv_mode_bits(CfL) -
+ * uv_mode_bits(DC)), f32 as the reference orders it, is below DC's; the 12
+ * modes at delta 0 ranked by SATD into a top-3 priced in list order (each
+ * winner clearing CfL); when CfL did not win and angle_deltas is set, a
+ * directional winner's zone-2 deltas with no top-right / bottom-left.  Every
+ * total on rd_lambda (emit_mlam_c at 32).  Jobs: mt_uv16_444_job's layout
+ * with px / py the 32x32 leaf origin and the contexts those of the 16x16
+ * chroma block.  Params, QM row and costs as for the 4:4:4 search (16x16 chroma
+ * weights, the chroma TX_16X16 slice); the luma reconstruction luma_stride x
+ * 2 frame_h.  d_cf / d_rec: n x 512, U then V. */
+typedef mt_uv16_444_job mt_uv32_420_job;
+int mt_pick_uv32_420_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv32_420_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream);
+int mt_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv32_420_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
 int mt_pick_uv16_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
                             const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
                             const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,

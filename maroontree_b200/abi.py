@@ -466,6 +466,11 @@ def _bind(lib):
         "mt_pick_uv16_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
                                        C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
                                        C.c_int32, _P, _P, _P]),
+        "mt_pick_uv32_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                       C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
+                                       C.c_int32, _P, _P, _P]),
+        "mt_pick_uv32_420_device": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                              C.POINTER(Quant), _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
         "mt_pick_uv16_444_device": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
                                               C.POINTER(Quant), _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
         "mt_grid16_luma_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
@@ -531,7 +536,7 @@ EXPORTED_SYMBOLS = (
     "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
     "mt_grid16_luma_device", "mt_grid16_luma", "mt_uv_mode_cdfs_default", "mt_uv_mode_costs_build",
     "mt_uv_mode_bits", "mt_pick_uv16_420_device", "mt_pick_uv16_420",
-    "mt_pick_uv16_444_device", "mt_pick_uv16_444",
+    "mt_pick_uv16_444_device", "mt_pick_uv16_444", "mt_pick_uv32_420_device", "mt_pick_uv32_420",
 )
 
 

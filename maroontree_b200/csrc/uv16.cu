@@ -372,6 +372,7 @@ struct Uv444Work {
   int16_t resid[256];
   int16_t ac[256];
   float suf[257];  // trellis16 scratch
+  TrellisCtxScratchW<16> trc;  // trellis_ctx<16> scratch (4:2:0 at 16x16)
   uint8_t lv[288];
 };
 
@@ -383,6 +384,9 @@ struct PlaneCost {
 // One 16x16 plane of a candidate after its prediction: the transform with
 // the QM, the plain trellis_optimize (4:4:4's chroma_rect_trellis),
 // preserve_dc when `keep_dc`, the inverse, sse_recon and chroma_bits.
+// CTX: the 4:2:0 chroma_rect_trellis, trellis_optimize_ctx against the
+// chroma TX_16X16 costs in the plane's dc_sign context, instead.
+template <bool CTX = false>
 __device__ PlaneCost plane_chain16(const UvArgs& a, const UvPlane& P, const mt_coef_costs& T, const uint8_t* qm,
                                    const float* sQs, const float* lut, int tx, bool keep_dc, int16_t* pred,
                                    int16_t* cf, int16_t* rr, Uv444Work& w) {
@@ -399,7 +403,13 @@ __device__ PlaneCost plane_chain16(const UvArgs& a, const UvPlane& P, const mt_c
   int32_t* tmp = w.u + 256;
   fwd16x16(w.resid, tx, q, cf, tf, tmp);
   if (qm) apply_qm(cf, tf, sQs, 256);
-  if (a.lambda > 0.0f) trellis16(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut);
+  if (a.lambda > 0.0f) {
+    if constexpr (CTX)
+      trellis_ctx<16>(cf, tf, (float)q.dc_q, (float)q.ac_q, a.lambda, T, P.ds, qm, q.qm_level >= 5, p.band_tilt,
+                      w.trc);
+    else
+      trellis16(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut);
+  }
   if (keep_dc) {
     const int32_t mean = sum / 256;
     if (cf[0] == 0 && abs(mean) >= 8) cf[0] = (int16_t)(mean > 0 ? 1 : -1);
@@ -652,6 +662,221 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
         rec_out[(size_t)j * 512 + pl * 256 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
 }
 
+// ---- the 32x32 leaf at 4:2:0: pick_uv32_420 ----
+
+// pick_uv32_420 (src/coder/block32.rs:2797-3120) with the shipped tuning on
+// the 32x32 leaf's 16x16 chroma blocks: DC (the 4:2:0 context trellis,
+// preserve_dc), CfL from the AC of the 32x32 luma reconstruction against
+// DC, the 12 modes ranked by SATD into a top-3 priced in list order, then a
+// directional winner's zone-2 deltas (uv_ad, uv_ad32; not after CfL); every
+// total on the one chroma lambda.
+__global__ void __launch_bounds__(kUvThreads) uv32_420_kernel(
+    const uint16_t* __restrict__ src_u, const uint16_t* __restrict__ src_v, const uint16_t* __restrict__ rec_u,
+    const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
+    const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
+    const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_444_job* __restrict__ jobs, int n,
+    mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out, int arena) {
+  __shared__ mt_coef_costs sT;
+  __shared__ mt_uv_mode_costs sM;
+  __shared__ uint8_t sQm[256];
+  __shared__ float sQs[256];
+  {
+    const float* g = reinterpret_cast<const float*>(costs);
+    float* s = reinterpret_cast<float*>(&sT);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_coef_costs) / 4); i += blockDim.x) s[i] = g[i];
+    const float* gm = reinterpret_cast<const float*>(mode_costs);
+    float* sm = reinterpret_cast<float*>(&sM);
+    for (int i = threadIdx.x; i < (int)(sizeof(mt_uv_mode_costs) / 4); i += blockDim.x) sm[i] = gm[i];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+      const int wq = a.has_qm ? qm_row[i] : 32;
+      sQm[i] = (uint8_t)wq;
+      sQs[i] = fwd_qm_scale(wq);
+    }
+    __syncthreads();
+  }
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const mt_split16_params& p = a.p;
+  const mt_uv16_444_job jb = jobs[j];
+  mt_uv16_result& r = res[j];
+  const int cx = jb.px >> 1, cy = jb.py >> 1;
+  const float kInf = __int_as_float(0x7f800000);
+  const bool ok = (jb.px & 31) == 0 && (jb.py & 31) == 0 && cx + 16 <= p.frame_w && cy + 16 <= p.frame_h &&
+                  jb.y_mode <= MT_PAETH_PRED;
+  if (!ok) {
+    r.total = r.dc_total = r.cfl_total = kInf;
+    r.uv_mode = 255;
+    r.angle_delta = 0;
+    r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
+    if (cf_out)
+      for (int i = 0; i < 512; i++) cf_out[(size_t)j * 512 + i] = 0;
+    if (rec_out)
+      for (int i = 0; i < 512; i++) rec_out[(size_t)j * 512 + i] = 0;
+    return;
+  }
+  const mt_coef_costs& T = sT;
+  const mt_uv_mode_costs& M = sM;
+  const uint8_t* qm = a.has_qm ? sQm : nullptr;
+  const int32_t maxv = (1 << p.bd) - 1;
+  const float mlam = p.rd_lambda;
+  const bool have_tr = jb.flags & MT_CAND_HAVE_TR, have_bl = jb.flags & MT_CAND_HAVE_BL;
+  const bool ft = jb.flags & MT_CAND_FILTER_TYPE;
+  const int vis_w = p.vis_w > 0 ? p.vis_w : p.frame_w, vis_h = p.vis_h > 0 ? p.vis_h : p.frame_h;
+  UvPlane P[2];
+  for (int pl = 0; pl < 2; pl++) {
+    UvPlane& q = P[pl];
+    q.src = (pl ? src_v : src_u) + (size_t)cy * p.stride + cx;
+    q.rec = pl ? rec_v : rec_u;
+    q.vw = min(max(vis_w - cx, 0), 16);
+    q.vh = min(max(vis_h - cy, 0), 16);
+    bool anz = false, lnz = false;
+    int s = -8;
+    for (int k = 0; k < 4; k++) {
+      anz |= jb.a_coef[pl][k] != 0x40;
+      lnz |= jb.l_coef[pl][k] != 0x40;
+      s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
+    }
+    q.sk = 7 + anz + lnz;
+    q.ds = (s != 0) + (s > 0);
+    q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
+    q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
+  }
+  Uv444Work& w = smem_arena<Uv444Work>(arena);
+  int best = 0;
+  int32_t dc[2];
+  float dc_total = 0.0f;
+  for (int pl = 0; pl < 2; pl++) {
+    predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
+                   w.s[0].pred[pl], w.u);
+    dc[pl] = w.s[0].pred[pl][0];
+    const PlaneCost c = plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, true, w.s[0].pred[pl],
+                                           w.s[0].cf[pl], w.s[0].rr[pl], w);
+    dc_total = __fadd_rn(dc_total, rd_cost_i64(c.sse, mlam, c.bits));
+  }
+  float best_total = dc_total;
+  int mode = MT_DC_PRED, delta = 0;
+  bool use_cfl = false;
+  // CfL: cfl_ac_sub of the 32x32 luma into 16x16
+  {
+    const int ls = a.u.luma_stride;
+    const uint16_t* l = luma + (size_t)jb.py * ls + jb.px;
+    int32_t sum = 128;
+    for (int i = 0; i < 256; i++) {
+      const int y = i >> 4, x = i & 15;
+      const uint16_t* q = l + (size_t)(2 * y) * ls + 2 * x;
+      const int32_t v = ((int32_t)q[0] + q[1] + q[ls] + q[ls + 1]) << 1;
+      w.ac[i] = (int16_t)v;
+      sum += v;
+    }
+    const int32_t mean = sum >> 8;
+    for (int i = 0; i < 256; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
+  }
+  int alpha[2];
+  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha16(w.ac, P[pl], p.stride, dc[pl], maxv);
+  {
+    Uv444Slot& c = w.s[1 - best];
+    float body = 0.0f;
+    for (int pl = 0; pl < 2; pl++) {
+      for (int i = 0; i < 256; i++) c.pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
+      const PlaneCost pc = plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, false, c.pred[pl],
+                                               c.cf[pl], c.rr[pl], w);
+      body = __fadd_rn(body, rd_cost_i64(pc.sse, mlam, pc.bits));
+    }
+    const float cfl_total =
+        __fsub_rn(__fadd_rn(body, __fmul_rn(mlam, uv_mode_bits(M, jb.y_mode, MT_UV_CFL_PRED, true, alpha[0], alpha[1]))),
+                  __fmul_rn(mlam, uv_mode_bits(M, jb.y_mode, MT_DC_PRED, false, 0, 0)));
+    r.cfl_total = cfl_total;
+    if ((alpha[0] != 0 || alpha[1] != 0) && cfl_total < best_total) {
+      best_total = cfl_total;
+      use_cfl = true;
+      best = 1 - best;
+    }
+  }
+  // rank_chroma_modes into DirectionalTopK (K = 3), then the ranked modes in list order
+  unsigned long long tc[3];
+  int tm[3], tn = 0;
+  int16_t* sp = w.s[1 - best].pred[0];
+  for (int ci = 0; ci < kJointModes; ci++) {
+    const int m = kJointList[ci];
+    unsigned long long sc = 0;
+    for (int pl = 0; pl < 2; pl++) {
+      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd, sp, w.u);
+      sc += satd_sad_proxy<16>(pl ? src_v : src_u, p.stride, cx, cy, sp, P[pl].vw, P[pl].vh);
+    }
+    int pos = tn < 3 ? tn : 2;
+    if (tn == 3 && sc >= tc[pos]) continue;
+    if (tn < 3) pos = tn++;
+    while (pos > 0 && sc < tc[pos - 1]) {
+      tc[pos] = tc[pos - 1];
+      tm[pos] = tm[pos - 1];
+      pos--;
+    }
+    tc[pos] = sc;
+    tm[pos] = m;
+  }
+  for (int ci = 0; ci < kJointModes; ci++) {
+    const int m = kJointList[ci];
+    bool in = false;
+    for (int e = 0; e < tn; e++) in |= tm[e] == m;
+    if (!in) continue;
+    const int tx = chroma_tx(m);
+    float total = __fmul_rn(mlam, uv_mode_bits(M, jb.y_mode, m, false, 0, 0));
+    Uv444Slot& c = w.s[1 - best];
+    for (int pl = 0; pl < 2; pl++) {
+      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd,
+                     c.pred[pl], w.u);
+      const PlaneCost pc =
+          plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+      total = __fadd_rn(total, rd_cost_i64(pc.sse, mlam, pc.bits));
+    }
+    if (total < best_total) {
+      best_total = total;
+      mode = m;
+      use_cfl = false;
+      best = 1 - best;
+    }
+  }
+  if (!use_cfl && a.u.angle_deltas && directional(mode)) {
+    const int m = mode, tx = chroma_tx(m);
+    int lo = 0, hi = -1;
+    if (m == MT_V_PRED) lo = 1, hi = 3;
+    else if (m == MT_H_PRED) lo = -3, hi = -1;
+    else if (m == MT_D113_PRED || m == MT_D135_PRED || m == MT_D157_PRED) lo = -3, hi = 3;
+    const float base_sig = __fsub_rn(uv_mode_bits(M, jb.y_mode, m, false, 0, 0), M.angle_delta[m - MT_V_PRED][3]);
+    for (int d = lo; d <= hi; d++) {
+      if (d == 0) continue;
+      float total = __fmul_rn(mlam, __fadd_rn(base_sig, M.angle_delta[m - MT_V_PRED][d + 3]));
+      Uv444Slot& c = w.s[1 - best];
+      for (int pl = 0; pl < 2; pl++) {
+        predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, false, false, ft, p.bd, c.pred[pl],
+                       w.u);
+        const PlaneCost pc =
+            plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+        total = __fadd_rn(total, rd_cost_i64(pc.sse, mlam, pc.bits));
+      }
+      if (total < best_total) {
+        best_total = total;
+        delta = d;
+        best = 1 - best;
+      }
+    }
+  }
+  r.total = best_total;
+  r.dc_total = dc_total;
+  r.uv_mode = (uint8_t)(use_cfl ? MT_UV_CFL_PRED : mode);
+  r.angle_delta = (int8_t)delta;
+  r.cfl_alpha[0] = (int8_t)alpha[0];
+  r.cfl_alpha[1] = (int8_t)alpha[1];
+  const Uv444Slot& b = w.s[best];
+  if (cf_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 256; i++) cf_out[(size_t)j * 512 + pl * 256 + i] = b.cf[pl][i];
+  if (rec_out)
+    for (int pl = 0; pl < 2; pl++)
+      for (int i = 0; i < 256; i++)
+        rec_out[(size_t)j * 512 + pl * 256 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
+}
+
 int uv_check(const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q, int32_t n) {
   if (!p || !u || !q || n < 0) return MT_ERR_INVALID_INPUT;
   if (p->bd != 8) return MT_ERR_UNSUPPORTED;
@@ -697,6 +922,30 @@ int uv444_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, con
   size_t dyn = 0;
   if (!arena_launch_shape(uv16_444_kernel, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
   uv16_444_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+      su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs, n, d_res, d_cf, d_rec, stride);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int uv32_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* luma,
+                const mt_split16_params* prm, const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm,
+                const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mc, const mt_uv16_444_job* d_jobs, int32_t n,
+                mt_uv16_result* d_res, int32_t* d_cf, uint16_t* d_rec, void* stream) {
+  const int rc = uv_check(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n == 0) return MT_OK;
+  if (!su || !sv || !ru || !rv || !luma || !d_costs || !d_mc || !d_jobs || !d_res) return MT_ERR_INVALID_INPUT;
+  UvArgs a;
+  a.p = *prm;
+  a.u = *uvp;
+  a.q = *quant;
+  a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
+                                         : 0.0f;
+  a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
+  const int stride = arena_stride(sizeof(Uv444Work));
+  int threads = 0;
+  size_t dyn = 0;
+  if (!arena_launch_shape(uv32_420_kernel, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
+  uv32_420_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
       su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs, n, d_res, d_cf, d_rec, stride);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
@@ -807,6 +1056,32 @@ int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                      const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc, const mt_uv16_job* j,
                      mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
                    return uv16_device(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
+                 });
+}
+
+int mt_pick_uv32_420_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv32_420_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream) {
+  return uv32_device(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs, d_mode_costs,
+                     d_jobs, n, d_results, d_cf, d_rec, stream);
+}
+
+int mt_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv32_420_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  const int rc = uv_check(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  return uv_host(src_u, src_v, rec_u, rec_v, luma, 2 * (size_t)prm->frame_h, prm, uvp, quant, qm_row, 256, costs,
+                 mode_costs, jobs, n, results, cf_out, rec_out, 512,
+                 [&](const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* l,
+                     const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc,
+                     const mt_uv32_420_job* j, mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
+                   return uv32_device(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
                  });
 }
 

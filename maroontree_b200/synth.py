@@ -525,16 +525,17 @@ def planes444(rgb, seed):
     return src, rec
 
 
-def uv16_444_jobs(w, h, seed, every=1):
+def uv16_444_jobs(w, h, seed, every=1, leaf=16):
     """16x16-leaf jobs of the 4:4:4 chroma search (mt_uv16_444_job), as
-    uv16_jobs with four coefficient-context bytes per plane and side."""
+    uv16_jobs with four coefficient-context bytes per plane and side; leaf=32:
+    the 32x32 leaves of the 4:2:0 search pick_uv32_420 (same layout)."""
     rng = np.random.default_rng(seed)
     rows = []
-    for py in range(0, h - 15, 16):
-        for px in range(0, w - 15, 16):
+    for py in range(0, h - leaf + 1, leaf):
+        for px in range(0, w - leaf + 1, leaf):
             if rng.random() > 1.0 / every:
                 continue
-            fl = block_flags(px, py, w, h, 16) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
+            fl = block_flags(px, py, w, h, leaf) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
             ctx = coef_ctx_bytes(rng, 16)
             rows.append((px, py, int(rng.integers(0, 13)), fl, ctx[:8].reshape(2, 4), ctx[8:].reshape(2, 4), (0, 0)))
     return np.array(rows, abi.UV16_444_JOB_DTYPE)

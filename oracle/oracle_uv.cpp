@@ -2,7 +2,8 @@
 // searches with the shipped tuning -- pick_uv16_420
 // (src/coder/block16.rs:980-1381: uv16_joint on, uv8_joint_k from the params)
 // and pick_uv16_444 (:437-978: no palette outside screen content,
-// uv16_444_mlam_c off), both with cfl_alpha_rd_steps 0 so cfl_alpha_rd_refine
+// uv16_444_mlam_c off), and the 32x32 leaf's pick_uv32_420
+// (src/coder/block32.rs:2797-3120), both with cfl_alpha_rd_steps 0 so cfl_alpha_rd_refine
 // returns the closed-form alpha (src/cost.rs:332-341) -- and uv_mode_bits
 // (src/coder/lossy_state.rs:1302-1349) priced straight from the CDFs with
 // cdf_cost.  Composed of the oracle's own
@@ -114,13 +115,13 @@ float plane_cost(const mt_split16_params* p, const mt_quant* q, const uint8_t* q
   return (float)sse + p->rd_lambda * bits;
 }
 
-// One 16x16 plane of a 4:4:4 candidate: the transform with the QM, the plain
+// One 16x16 plane of a chroma candidate: the transform with the QM, the plain
 // trellis_optimize (chroma_rect_trellis outside 4:2:0 / 4:2:2,
-// lossy_state.rs:834-838), preserve_dc when keep_dc, the inverse, sse_recon
+// lossy_state.rs:834-838) or, ctx, trellis_optimize_ctx (4:2:0), preserve_dc when keep_dc, the inverse, sse_recon
 // and chroma_bits at TX_16X16 (lossy_state.rs:749-811); sse and bits apart.
 void plane_cost16(const mt_split16_params* p, const mt_quant* q, const uint8_t* qm, const mt_coef_cdfs* cd,
                   const Plane& P, int cx, int cy, int tx, bool keep_dc, const int32_t* pred, int32_t* cf, int32_t* rr,
-                  int64_t* sse, float* bits) {
+                  int64_t* sse, float* bits, bool ctx = false) {
   int32_t resid[256];
   float tf[256];
   int32_t sum = 0;
@@ -129,7 +130,11 @@ void plane_cost16(const mt_split16_params* p, const mt_quant* q, const uint8_t* 
     sum += resid[i];
   }
   or_fwd_txfm_quant(resid, tx, 16, q, qm, cf, tf);
-  or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, or_default_scan(16), 256, p->trellis_lambda0);
+  if (ctx)  // the 4:2:0 chroma_rect_trellis (lossy_state.rs:821-870)
+    or_trellis_optimize_ctx(cf, tf, (float)q->dc_q, (float)q->ac_q, or_default_scan(16), 16, p->trellis_lambda0, cd,
+                            P.ds, qm, q->qm_level, p->band_tilt);
+  else
+    or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, or_default_scan(16), 256, p->trellis_lambda0);
   if (keep_dc) {
     const int32_t mean = sum / 256;
     if (cf[0] == 0 && (mean < 0 ? -mean : mean) >= 8) cf[0] = mean > 0 ? 1 : -1;
@@ -465,6 +470,181 @@ int or_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_
     r.dc_total = dc_total;
     r.cfl_total = cfl_total;
     r.uv_mode = (uint8_t)(mode != MT_DC_PRED ? mode : (use_cfl ? MT_UV_CFL_PRED : MT_DC_PRED));
+    r.angle_delta = (int8_t)delta;
+    r.cfl_alpha[0] = alpha[0];
+    r.cfl_alpha[1] = alpha[1];
+    for (int i = 0; i < 512; i++) {
+      if (cf_out) cf_out[(size_t)j * 512 + i] = bcf[(size_t)i];
+      if (rec_out) {
+        const int32_t v = bpred[(size_t)i] + brr[(size_t)i];
+        rec_out[(size_t)j * 512 + i] = (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
+      }
+    }
+  }
+  return MT_OK;
+}
+
+int or_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
+                     const mt_uv16_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
+                     uint16_t* rec_out) {
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const float mlam = p->rd_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  static const int kList[12] = {MT_SMOOTH_V_PRED, MT_PAETH_PRED, MT_SMOOTH_PRED, MT_SMOOTH_H_PRED,
+                                MT_V_PRED,        MT_H_PRED,     MT_D135_PRED,   MT_D113_PRED,
+                                MT_D157_PRED,     MT_D45_PRED,   MT_D67_PRED,    MT_D203_PRED};
+  for (int j = 0; j < n; j++) {
+    const mt_uv16_444_job& jb = jobs[j];
+    mt_uv16_result& r = results[j];
+    const int cx = jb.px / 2, cy = jb.py / 2;
+    if ((jb.px & 31) || (jb.py & 31) || cx + 16 > p->frame_w || cy + 16 > p->frame_h || jb.y_mode > MT_PAETH_PRED) {
+      r.total = r.dc_total = r.cfl_total = INFINITY;
+      r.uv_mode = 255;
+      r.angle_delta = 0;
+      r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
+      if (cf_out) memset(cf_out + (size_t)j * 512, 0, 512 * sizeof(int32_t));
+      if (rec_out) memset(rec_out + (size_t)j * 512, 0, 512 * sizeof(uint16_t));
+      continue;
+    }
+    const bool tr = jb.flags & MT_CAND_HAVE_TR, bl = jb.flags & MT_CAND_HAVE_BL, ft = jb.flags & MT_CAND_FILTER_TYPE;
+    Plane P[2];
+    for (int pl = 0; pl < 2; pl++) {
+      P[pl].src = pl ? src_v : src_u;
+      P[pl].rec = pl ? rec_v : rec_u;
+      bool anz = false, lnz = false;
+      int s = -8;
+      for (int k = 0; k < 4; k++) {
+        anz |= jb.a_coef[pl][k] != 0x40;
+        lnz |= jb.l_coef[pl][k] != 0x40;
+        s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
+      }
+      P[pl].sk = 7 + anz + lnz;
+      P[pl].ds = (s != 0) + (s > 0);
+    }
+    std::vector<int32_t> bpred(512), bcf(512), brr(512), npred(512), ncf(512), nrr(512);
+    int32_t dc[2];
+    float dc_total = 0.0f;
+    for (int pl = 0; pl < 2; pl++) {
+      dc[pl] = or_dc_pred(P[pl].rec, p->stride, cx, cy, 16, 16, p->bd);
+      for (int i = 0; i < 256; i++) bpred[(size_t)pl * 256 + i] = dc[pl];
+      int64_t sse;
+      float bits;
+      plane_cost16(p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, true, &bpred[(size_t)pl * 256], &bcf[(size_t)pl * 256],
+                   &brr[(size_t)pl * 256], &sse, &bits, true);
+      dc_total += (float)sse + mlam * bits;
+    }
+    float best_total = dc_total;
+    int mode = MT_DC_PRED, delta = 0;
+    bool use_cfl = false;
+    // CfL: cfl_ac_sub of the 32x32 luma (4:2:0) and cfl_best_alpha
+    mt_cfl_block cb = {};
+    cb.cx = (uint16_t)cx;
+    cb.cy = (uint16_t)cy;
+    cb.dc[0] = (int16_t)dc[0];
+    cb.dc[1] = (int16_t)dc[1];
+    int8_t alpha[2];
+    std::vector<int32_t> ac(256);
+    or_cfl_alpha(luma, u->luma_stride, src_u, src_v, p->stride, 1, 1, 16, 16, vis_w, vis_h, p->bd, &cb, 1, alpha,
+                 ac.data());
+    float body = 0.0f;
+    for (int pl = 0; pl < 2; pl++) {
+      for (int i = 0; i < 256; i++) {
+        const int32_t diff = alpha[pl] * ac[(size_t)i];
+        const int32_t mag = ((diff < 0 ? -diff : diff) + 32) >> 6;
+        const int32_t v = dc[pl] + (diff < 0 ? -mag : mag);
+        npred[(size_t)pl * 256 + i] = v < 0 ? 0 : (v > maxv ? maxv : v);
+      }
+      int64_t sse;
+      float bits;
+      plane_cost16(p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, false, &npred[(size_t)pl * 256], &ncf[(size_t)pl * 256],
+                   &nrr[(size_t)pl * 256], &sse, &bits, true);
+      body += (float)sse + mlam * bits;
+    }
+    const float cfl_total = body + mlam * or_uv_mode_bits(mc, jb.y_mode, MT_UV_CFL_PRED, 1, alpha[0], alpha[1]) -
+                            mlam * or_uv_mode_bits(mc, jb.y_mode, MT_DC_PRED, 0, 0, 0);
+    if ((alpha[0] != 0 || alpha[1] != 0) && cfl_total < best_total) {
+      best_total = cfl_total;
+      use_cfl = true;
+      bpred = npred;
+      bcf = ncf;
+      brr = nrr;
+    }
+    // rank_chroma_modes + DirectionalTopK (K = 3)
+    uint64_t tc[3];
+    int tm[3], tn = 0;
+    int32_t pp[256];
+    for (int m : kList) {
+      uint64_t cost = 0;
+      for (int pl = 0; pl < 2; pl++) {
+        or_intra_predict(P[pl].rec, p->stride, cx, cy, 16, 16, m, 0, tr, bl, p->frame_w, p->frame_h, ft, p->bd, pp);
+        const int vw = std::min(std::max(vis_w - cx, 0), 16), vh = std::min(std::max(vis_h - cy, 0), 16);
+        cost += satd_sad_proxy_n(P[pl].src + (size_t)cy * p->stride + cx, p->stride, pp, 16, vw, vh);
+      }
+      int pos = tn < 3 ? tn : 2;
+      if (tn == 3 && cost >= tc[pos]) continue;
+      if (tn < 3) pos = tn++;
+      while (pos > 0 && cost < tc[pos - 1]) {
+        tc[pos] = tc[pos - 1];
+        tm[pos] = tm[pos - 1];
+        pos--;
+      }
+      tc[pos] = cost;
+      tm[pos] = m;
+    }
+    auto price = [&](int m, int d, bool etr, bool ebl, float rate_bits) {
+      const int tx = chroma_tx(m);
+      float total = mlam * rate_bits;
+      for (int pl = 0; pl < 2; pl++) {
+        or_intra_predict(P[pl].rec, p->stride, cx, cy, 16, 16, m, d, etr, ebl, p->frame_w, p->frame_h, ft, p->bd,
+                         &npred[(size_t)pl * 256]);
+        int64_t sse;
+        float bits;
+        plane_cost16(p, q, qm, cd, P[pl], cx, cy, tx, true, &npred[(size_t)pl * 256], &ncf[(size_t)pl * 256],
+                     &nrr[(size_t)pl * 256], &sse, &bits, true);
+        total += (float)sse + mlam * bits;
+      }
+      return total;
+    };
+    for (int m : kList) {
+      bool in = false;
+      for (int e = 0; e < tn; e++) in |= tm[e] == m;
+      if (!in) continue;
+      const float total = price(m, 0, tr, bl, or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0));
+      if (total < best_total) {
+        best_total = total;
+        mode = m;
+        use_cfl = false;
+        bpred = npred;
+        bcf = ncf;
+        brr = nrr;
+      }
+    }
+    // uv_ad / uv_ad32 (block32.rs:3054-3110)
+    if (!use_cfl && u->angle_deltas && directional(mode)) {
+      const int m = mode;
+      std::vector<int> ds;
+      if (m == MT_V_PRED) ds = {1, 2, 3};
+      else if (m == MT_H_PRED) ds = {-3, -2, -1};
+      else if (m == MT_D113_PRED || m == MT_D135_PRED || m == MT_D157_PRED) ds = {-3, -2, -1, 1, 2, 3};
+      const float base_sig = or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0) - or_cdf_cost(mc->angle_delta[m - MT_V_PRED], 3);
+      for (int d : ds) {
+        const float total = price(m, d, false, false, base_sig + or_cdf_cost(mc->angle_delta[m - MT_V_PRED], d + 3));
+        if (total < best_total) {
+          best_total = total;
+          delta = d;
+          bpred = npred;
+          bcf = ncf;
+          brr = nrr;
+        }
+      }
+    }
+    r.total = best_total;
+    r.dc_total = dc_total;
+    r.cfl_total = cfl_total;
+    r.uv_mode = (uint8_t)(use_cfl ? MT_UV_CFL_PRED : mode);
     r.angle_delta = (int8_t)delta;
     r.cfl_alpha[0] = alpha[0];
     r.cfl_alpha[1] = alpha[1];

@@ -406,3 +406,144 @@ def test_uv16_444_at_config(mt_lib, oracle_lib, cuda):
     uvp = mt_lib.uv16_params(wl.w, angle_deltas=True, dir_lambda=wl.lam.lambda_d)
     jobs = synth.uv16_444_jobs(wl.w, wl.h, wl.qidx)
     _gpu444(mt_lib, oracle_lib, src, rec, prm, uvp, q, qm, wl.qctx, jobs, configs.THREADS)
+
+
+# ---- the 32x32 leaf at 4:2:0 (pick_uv32_420) ----
+
+def _case32(mt, op, w, h, seed, qidx, qm_level, wsse, skip=False, ad=True):
+    src, rec = _planes(w, h, seed)
+    cw, ch = src[1].shape[1], src[1].shape[0]
+    q = op.quant_new_chroma(qidx, 0, 0, 8, qm_level)
+    qm = op.qm_row(qm_level, 1, 16) if qm_level < 15 else None
+    sb = [(float(np.float32(1.5 + 0.1 * k)), float(np.float32(0.2 + 0.05 * k))) for k in range(13)] if skip else None
+    prm = mt.split16_params(cw, ch, trellis_lambda0=0.05, rd_lambda=0.2 * qidx + 3, band_tilt=0.6, wsse_scale=wsse,
+                            vis=(cw - 3, ch - 1), skip_bits=sb)
+    uvp = mt.uv16_params(src[0].shape[1], angle_deltas=ad)
+    return src, rec, q, qm, prm, uvp
+
+
+@pytest.mark.parametrize("qidx,qm_level,wsse", [(90, 6, 1.0), (40, 15, 0.0)])
+def test_uv32_oracle_accounting(oracle_lib, qidx, qm_level, wsse):
+    """The oracle's DC and CfL totals and its winner's total equal the costs
+    recomputed from the oracle's primitives (the 4:2:0 context trellis on
+    16x16 chroma, the CfL AC of the 32x32 luma); the winner is no worse than
+    DC and, unless CfL was refused, CfL."""
+    import maroontree_b200 as mt
+
+    op = oracle_lib
+    src, rec, q, qm, prm, uvp = _case32(mt, op, 128, 96, qidx + 2, qidx, qm_level, wsse)
+    cd = op.default_cdfs(op.qcat(qidx), 16, plane=1)
+    mc = op.uv_mode_cdfs()
+    jobs = synth.uv16_444_jobs(128, 96, qidx, leaf=32)
+    res, _, _ = op.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd, mc, jobs)
+    f32 = np.float32
+    lam = f32(prm.rd_lambda)
+    scan = op.default_scan(16)
+    adc = np.ctypeslib.as_array(mc.angle_delta)
+    txmap = {abi.PAETH_PRED: abi.TX_ADST_ADST, abi.SMOOTH_PRED: abi.TX_ADST_ADST, abi.D135_PRED: abi.TX_ADST_ADST,
+             abi.SMOOTH_V_PRED: abi.TX_ADST_DCT, abi.V_PRED: abi.TX_ADST_DCT, abi.D113_PRED: abi.TX_ADST_DCT,
+             abi.D67_PRED: abi.TX_ADST_DCT, abi.SMOOTH_H_PRED: abi.TX_DCT_ADST, abi.H_PRED: abi.TX_DCT_ADST,
+             abi.D157_PRED: abi.TX_DCT_ADST, abi.D203_PRED: abi.TX_DCT_ADST}
+    cw, ch = src[1].shape[1], src[1].shape[0]
+    for i, jb in enumerate(jobs):
+        cx, cy, fl, ym = int(jb["px"]) // 2, int(jb["py"]) // 2, int(jb["flags"]), int(jb["y_mode"])
+        ctx = []
+        for pl in range(2):
+            a, l = [int(v) for v in jb["a_coef"][pl]], [int(v) for v in jb["l_coef"][pl]]
+            s = sum(v >> 6 for v in a + l) - 8
+            ctx.append((7 + int(any(v != 0x40 for v in a)) + int(any(v != 0x40 for v in l)),
+                        int(s != 0) + int(s > 0)))
+
+        def plane(pl, pred, tx, keep_dc):
+            resid = src[1 + pl][cy:cy + 16, cx:cx + 16].astype(np.int32).ravel() - pred.ravel()
+            lv, tf = op.fwd_txfm_quant(resid, tx, q, qm)
+            lv = op.trellis_optimize_ctx(lv, tf, q, qm, cd, ctx[pl][1], prm.trellis_lambda0, band_tilt=prm.band_tilt,
+                                         n=16)
+            if keep_dc:
+                mean = int(np.trunc(resid.sum() / 256))
+                if lv[0] == 0 and abs(mean) >= 8:
+                    lv[0] = 1 if mean > 0 else -1
+            rr = op.inv_txfm_dequant(lv, tx, q, qm)
+            sse = int(op.sse_recon(src[1 + pl], prm.vis_w, prm.vis_h, [(cx, cy)], pred.ravel(), rr, 16, 16,
+                                   scale=prm.wsse_scale)[0])
+            bits = f32(op.real_block_bits_bounded(lv, scan, 16, 16, cd, ctx[pl][0], ctx[pl][1], -1, 0, INF))
+            return f32(f32(sse) + f32(lam * bits))
+
+        dc = [int(op.intra_predict(rec[1 + pl], cx, cy, 16, 16, abi.DC_PRED)[0, 0]) for pl in range(2)]
+        dct = f32(0)
+        for pl in range(2):
+            dct = f32(dct + plane(pl, np.full((16, 16), dc[pl]), abi.TX_DCT_DCT, True))
+        blk = np.array([(cx, cy, (dc[0], dc[1]))], abi.CFL_BLOCK_DTYPE)
+        alpha, ac = op.cfl_alpha(rec[0], src[1], src[2], 1, 1, 16, 16, blk, vis=(prm.vis_w, prm.vis_h))
+        body = f32(0)
+        for pl in range(2):
+            diff = int(alpha[0][pl]) * ac[0]
+            mag = (np.abs(diff) + 32) >> 6
+            body = f32(body + plane(pl, np.clip(dc[pl] + np.where(diff < 0, -mag, mag), 0, 255), abi.TX_DCT_DCT, False))
+        cflt = f32(f32(body + f32(lam * f32(op.uv_mode_bits(mc, ym, abi.UV_CFL_PRED, tuple(int(v) for v in alpha[0])))))
+                   - f32(lam * f32(op.uv_mode_bits(mc, ym, abi.DC_PRED))))
+        r = res[i]
+        assert (f32(r["dc_total"]), f32(r["cfl_total"])) == (dct, cflt), i
+        assert tuple(int(v) for v in r["cfl_alpha"]) == tuple(int(v) for v in alpha[0])
+        m, d = int(r["uv_mode"]), int(r["angle_delta"])
+        assert f32(r["total"]) <= dct
+        if m == abi.DC_PRED:
+            want = dct
+        elif m == abi.UV_CFL_PRED:
+            want = cflt
+        else:
+            bits = f32(op.uv_mode_bits(mc, ym, m))
+            if d != 0:
+                bits = f32(f32(bits - f32(op.cdf_cost(adc[m - abi.V_PRED], 3))) +
+                           f32(op.cdf_cost(adc[m - abi.V_PRED], d + 3)))
+            want = f32(lam * bits)
+            tr, bl = (bool(fl & 1), bool(fl & 2)) if d == 0 else (False, False)
+            for pl in range(2):
+                pp = op.intra_predict(rec[1 + pl], cx, cy, 16, 16, m, d, tr, bl, bool(fl & 4), fw=cw, fh=ch)
+                want = f32(want + plane(pl, pp, txmap.get(m, abi.TX_DCT_DCT), True))
+        assert f32(r["total"]) == want, (i, m, d)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qidx,qm_level,wsse,skip,ad", [(70, 6, 1.0, False, True), (116, 15, 0.0, True, True),
+                                                         (30, 3, 0.75, False, False)])
+def test_uv32_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse, skip, ad):
+    src, rec, q, qm, prm, uvp = _case32(mt_lib, oracle_lib, 320, 192, qidx + 9, qidx, qm_level, wsse, skip=skip, ad=ad)
+    jobs = synth.uv16_444_jobs(320, 192, qidx, leaf=32)
+    jobs = np.concatenate([jobs, jobs[:2]])
+    jobs["px"][-2] = 304  # leaves the plane: rejected
+    jobs["y_mode"][-1] = 13
+    cd = oracle_lib.default_cdfs(oracle_lib.qcat(qidx), 16, plane=1)
+    mc = oracle_lib.uv_mode_cdfs()
+    costs = mt_lib.coef_costs(mt_lib.coef_cdfs_default(oracle_lib.qcat(qidx), 16, 16, 1))
+    mcost = mt_lib.uv_mode_costs(mt_lib.uv_mode_cdfs_default())
+    got = mt_lib.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, costs, mcost, jobs,
+                               want_cf=True, want_rec=True)
+    want = oracle_lib.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd, mc, jobs,
+                                    threads=os.cpu_count() or 1, want_cf=True, want_rec=True)
+    assert got[0].tobytes() == want[0].tobytes()
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2])
+    assert (got[0]["uv_mode"][-2:] == 255).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["C2q40", "C2q80"])
+def test_uv32_at_config(mt_lib, oracle_lib, cuda, name):
+    import configs
+
+    wl = configs.workload(name)
+    src, rec = synth.planes420(wl.rgb, wl.qidx)
+    cw, ch = src[1].shape[1], src[1].shape[0]
+    q = mt_lib.quant_new_chroma(wl.qidx, 0, 0, 8, wl.qm_uv)
+    qm = mt_lib.qm_row(wl.qm_uv, 1, 16) if wl.qm_uv < 15 else None
+    prm = mt_lib.split16_params(cw, ch, trellis_lambda0=wl.lam.trellis_lambda0, rd_lambda=wl.lam.mode_lambda,
+                                wsse_scale=1.0, vis=(wl.w // 2, wl.h // 2))
+    uvp = mt_lib.uv16_params(src[0].shape[1], angle_deltas=True)
+    jobs = synth.uv16_444_jobs(wl.w, wl.h, wl.qidx, leaf=32)
+    cd = oracle_lib.default_cdfs(wl.qctx, 16, plane=1)
+    got = mt_lib.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm,
+                               mt_lib.coef_costs(mt_lib.coef_cdfs_default(wl.qctx, 16, 16, 1)),
+                               mt_lib.uv_mode_costs(mt_lib.uv_mode_cdfs_default()), jobs)
+    want = oracle_lib.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd,
+                                    oracle_lib.uv_mode_cdfs(), jobs, threads=configs.THREADS)
+    assert got[0].tobytes() == want[0].tobytes()
