@@ -1216,9 +1216,10 @@ int job_finish(Job& j, Buffers& buf, int i) {
   ThreadGroup tracers;  // joined on every return path
   for (int t = 0; t < ntiles; ++t) {
     const int f = tile_first[(size_t)t];
-    tracers.v.emplace_back(mth::trace_tile_stores, j.plan.base_q_idx, cfg->updating_cdf, &bs.sbs[(size_t)f],
-                         tile_first[(size_t)t + 1] - f, bs.cdef_points.data() + f, toks.data(), offs.data(),
-                         sb_coef_first[(size_t)f], stores[(size_t)t].get());
+    for (int part = 0; part < mth::kTracers; ++part)
+      tracers.v.emplace_back(mth::trace_tile_stores, j.plan.base_q_idx, cfg->updating_cdf, &bs.sbs[(size_t)f],
+                             tile_first[(size_t)t + 1] - f, bs.cdef_points.data() + f, toks.data(), offs.data(),
+                             sb_coef_first[(size_t)f], stores[(size_t)t].get(), part);
   }
   mt_cdef_params cp = {};
   cp.w8 = pw;

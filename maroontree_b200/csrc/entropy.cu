@@ -736,9 +736,18 @@ inline bool token_store(uint32_t t, uint16_t* data, const uint32_t* off, const u
   return true;
 }
 
+// Which phase-1 worker codes token t: symbols and gathered bools by their
+// CDF slot's parity, raw-bit bools on worker 0.
+inline int token_part(uint32_t t) {
+  const uint32_t tag = t & kTagMask;
+  if (tag == kTagBool) return 0;
+  const uint32_t slot = tag == 0 || tag == kTagNoUpdate ? (t >> 8) & 0xffff : (t >> 2) & 0xffff;
+  return (int)(slot % (uint32_t)kTracers);
+}
+
 void trace_tile_stores(uint8_t base_q_idx, int32_t updating_cdf, const std::vector<uint32_t>* sbs, int nsb,
                        const int32_t* cdef_point, const uint32_t* toks, const uint32_t* offs, size_t first_coef,
-                       TileStores* out) {
+                       TileStores* out, int part) {
   const int q = base_q_idx <= 20 ? 0 : base_q_idx <= 60 ? 1 : base_q_idx <= 120 ? 2 : 3;  // qcat
   CdfSet c;
   build_cdfs(q, c);
@@ -761,20 +770,25 @@ void trace_tile_stores(uint8_t base_q_idx, int32_t updating_cdf, const std::vect
         const uint32_t a = offs[k], b = offs[k + 1];
         ++k;
         if (n + (b - a) > cap) ok = false;
-        for (uint32_t e = a; e < b && ok; ++e) ok = token_store(toks[e], data, off, lens, nslots, upd, w[n++]);
+        for (uint32_t e = a; e < b && ok; ++e, ++n)
+          if (token_part(toks[e]) == part) ok = token_store(toks[e], data, off, lens, nslots, upd, w[n]);
       } else {
-        ok = n < cap && token_store(tok, data, off, lens, nslots, upd, w[n++]);
+        ok = n < cap;
+        if (ok && token_part(tok) == part) ok = token_store(tok, data, off, lens, nslots, upd, w[n]);
+        ++n;
       }
     }
     if (cdef_point[i] >= 0 && (size_t)cdef_point[i] == syn.size()) at = (uint32_t)n;
     if (!ok) {
       out->failed.store(true, std::memory_order_release);
-      out->done.store(nsb, std::memory_order_release);
+      out->done[part].store(nsb, std::memory_order_release);
       return;
     }
-    out->sb_end[(size_t)i] = (uint32_t)n;
-    out->cdef_at[(size_t)i] = at;
-    out->done.store(i + 1, std::memory_order_release);
+    if (part == 0) {
+      out->sb_end[(size_t)i] = (uint32_t)n;
+      out->cdef_at[(size_t)i] = at;
+    }
+    out->done[part].store(i + 1, std::memory_order_release);
   }
 }
 
@@ -786,8 +800,9 @@ int code_tile_stores(TileStores* in, int nsb, int32_t updating_cdf, const uint8_
   const uint64_t* const st = in->st.data();
   size_t a = 0;
   for (int i = 0; i < nsb; ++i) {
-    // phase 1 always reaches nsb (failure included): the wait ends
-    while (in->done.load(std::memory_order_acquire) <= i) std::this_thread::yield();
+    // every phase-1 worker always reaches nsb (failure included): the wait ends
+    for (int p = 0; p < kTracers; ++p)
+      while (in->done[p].load(std::memory_order_acquire) <= i) std::this_thread::yield();
     if (in->failed.load(std::memory_order_acquire)) return MT_ERR_INVALID_INPUT;
     const size_t b = in->sb_end[(size_t)i], p = in->cdef_at[(size_t)i];
     if (p == UINT32_MAX || cdef_bits <= 0) {
