@@ -859,6 +859,36 @@ typedef struct mt_uv16_444_job {
   uint8_t l_coef[2][4];
   uint8_t reserved[2];
 } mt_uv16_444_job;
+/* The 32x32 leaf's 4:4:4 chroma search (pick_uv32_444,
+ * src/coder/block32.rs:2264-2720, shipped tuning) on its 32x32 chroma blocks:
+ * as mt_pick_uv16_444 at 32x32, with every transform DCT_DCT (forced at
+ * TX_32X32), the plain trellis_optimize over the 1024-entry scan, chroma_bits
+ * of the chroma TX_32X32 class (contexts over eight above / eight left
+ * bytes), and CfL taken when the planes' rd_cost_i64 summed plus rd_lambda x
+ * uv_mode_bits(CfL) is below DC's sum plus rd_lambda x uv_mode_bits(DC).
+ * uvp->dir_lambda is mlam_c x (emit_mlam / mlam) at 32.  QM row: the 32x32
+ * chroma weights; costs: the chroma TX_32X32 slice (mt_coef_cdfs_default(qctx,
+ * 32, 32, 1)).  d_cf / d_rec: n x 2048, U then V. */
+typedef struct mt_uv32_444_job {
+  uint16_t px, py;          /* 32x32 leaf origin (luma and chroma) */
+  uint8_t y_mode;
+  uint8_t flags;            /* MT_CAND_HAVE_TR / HAVE_BL of the leaf, MT_CAND_FILTER_TYPE: chroma filter type */
+  uint8_t a_coef[2][8];     /* above coefficient contexts of the block's eight 4-sample columns, U then V */
+  uint8_t l_coef[2][8];
+  uint8_t reserved[2];
+} mt_uv32_444_job;
+int mt_pick_uv32_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv32_444_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream);
+int mt_pick_uv32_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv32_444_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out);
+
 /* The 32x32 leaf's 4:2:0 chroma search (pick_uv32_420,
  * src/coder/block32.rs:2797-3120, shipped tuning: uv_ad and uv_ad32 on,
  * cfl_alpha_rd_steps 0) on the leaf's 16x16 chroma blocks at (px / 2, py / 2):

@@ -276,6 +276,14 @@ def pick_uv32_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, cost
                       quant, qmrow, costs, mode_costs, jobs, want_cf, want_rec)
 
 
+def pick_uv32_444(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs, jobs, want_cf=False,
+                  want_rec=False):
+    """pick_uv32_444 over (32x32 leaf) jobs (``mt_pick_uv32_444``): (results,
+    levels n x 2048 or None, reconstruction n x 2048 or None), U then V."""
+    return _pick_uv16("mt_pick_uv32_444", abi.UV32_444_JOB_DTYPE, 2048, src_u, src_v, rec_u, rec_v, luma, prm, uvp,
+                      quant, qmrow, costs, mode_costs, jobs, want_cf, want_rec)
+
+
 def pick_uv16_444(src_u, src_v, rec_u, rec_v, luma, prm, uvp, quant, qmrow, costs, mode_costs, jobs, want_cf=False,
                   want_rec=False):
     """pick_uv16_444 over (16x16 leaf) jobs (``mt_pick_uv16_444``): (results,

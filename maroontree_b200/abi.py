@@ -113,6 +113,9 @@ assert UV16_JOB_DTYPE.itemsize == 16 and UV16_RESULT_DTYPE.itemsize == 16
 UV16_444_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("y_mode", "u1"), ("flags", "u1"),
                                ("a_coef", "u1", (2, 4)), ("l_coef", "u1", (2, 4)), ("reserved", "u1", (2,))])
 assert UV16_444_JOB_DTYPE.itemsize == 24
+UV32_444_JOB_DTYPE = np.dtype([("px", "<u2"), ("py", "<u2"), ("y_mode", "u1"), ("flags", "u1"),
+                               ("a_coef", "u1", (2, 8)), ("l_coef", "u1", (2, 8)), ("reserved", "u1", (2,))])
+assert UV32_444_JOB_DTYPE.itemsize == 40
 
 SPLIT16_JOB_DTYPE = np.dtype([
     ("px", "<u2"), ("py", "<u2"), ("mode", "u1"), ("angle_delta", "i1"), ("flags", "u1"), ("reserved", "u1"),
@@ -466,6 +469,11 @@ def _bind(lib):
         "mt_pick_uv16_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
                                        C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
                                        C.c_int32, _P, _P, _P]),
+        "mt_pick_uv32_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                       C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
+                                       C.c_int32, _P, _P, _P]),
+        "mt_pick_uv32_444_device": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
+                                              C.POINTER(Quant), _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P]),
         "mt_pick_uv32_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Split16Params), C.POINTER(Uv16Params),
                                        C.POINTER(Quant), _P, C.POINTER(CoefCosts), C.POINTER(UvModeCosts), _P,
                                        C.c_int32, _P, _P, _P]),
@@ -537,6 +545,7 @@ EXPORTED_SYMBOLS = (
     "mt_grid16_luma_device", "mt_grid16_luma", "mt_uv_mode_cdfs_default", "mt_uv_mode_costs_build",
     "mt_uv_mode_bits", "mt_pick_uv16_420_device", "mt_pick_uv16_420",
     "mt_pick_uv16_444_device", "mt_pick_uv16_444", "mt_pick_uv32_420_device", "mt_pick_uv32_420",
+    "mt_pick_uv32_444_device", "mt_pick_uv32_444",
 )
 
 

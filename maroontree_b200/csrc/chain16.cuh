@@ -16,19 +16,20 @@ namespace mtd {
 // are column-major (rc = y + 16 x).
 __constant__ uint16_t kScan16[256] = {MT_SCAN_16X16_LIST};
 
-// trellis_optimize (src/trellis.rs:944-1030) over the 16x16 scan: step A in
+// trellis_optimize (src/trellis.rs:944-1030) over an N-coefficient scan
+// (scan(i): the coefficient index of scan position i): step A in
 // the pinned AVX2 chunking (8-wide chunks, one 4-wide chunk, scalar tail; a
 // chunk holding a level >= 64 takes the scalar form in all lanes), the exact
 // right-to-left suffix sums of the zeroing distortion, and the EOB search.
-// `suf` is scratch for 257 floats.  Returns the final EOB scan index.
-template <typename C>
-__device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda, const float* lut) {
-  constexpr int N = 256;
+// `suf` is scratch for N + 1 floats.  Returns the final EOB scan index.
+template <int N, typename S, typename C>
+__device__ int trellis_sq(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda, const float* lut,
+                          S scan) {
   const float dq2 = __fmul_rn(dc_q, dc_q), aq2 = __fmul_rn(ac_q, ac_q);
   int eob_idx = -1;
 #pragma unroll 8
   for (int i = 0; i < N; i++)
-    if (cf[kScan16[i]] != 0) eob_idx = i;
+    if (cf[scan(i)] != 0) eob_idx = i;
   const int m = eob_idx + 1;
   const int M = warp_max(m);
   if (m == 0) return -1;
@@ -47,7 +48,7 @@ __device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float a
 #pragma unroll
       for (int k = 0; k < 8; k++) {
         if (k < W) {
-          rc[k] = kScan16[base + k];
+          rc[k] = scan(base + k);
           c[k] = cf[rc[k]];
           at[k] = fabsf(tf[rc[k]]);
           big |= uabs(c[k]) > 63u;
@@ -76,7 +77,7 @@ __device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float a
       for (int k = 0; k < 4; k++) {
         const int e = s + k;
         if (e >= m) break;
-        const int r = kScan16[e];
+        const int r = scan(e);
         const int32_t v = cf[r];
         if (v != 0 && round_down_plain(fabsf(tf[r]), uabs(v), r == 0 ? dq2 : aq2, lambda))
           cf[r] = (C)(v < 0 ? v + 1 : v - 1);
@@ -87,7 +88,7 @@ __device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float a
   float acc = 0.0f;
   for (int e = M - 1; e >= 0; e--) {
     if (e >= m) continue;
-    const int rc = kScan16[e];
+    const int rc = scan(e);
     const float at = fabsf(tf[rc]);
     acc = __fadd_rn(acc, __fmul_rn(rc == 0 ? dq2 : aq2, __fmul_rn(at, at)));
     suf[e] = acc;
@@ -97,7 +98,7 @@ __device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float a
   float pre = 0.0f;
   for (int e = 0; e < M; e++) {
     if (e >= m) continue;
-    const int rc = kScan16[e];
+    const int rc = scan(e);
     const float at = fabsf(tf[rc]);
     const uint32_t l = uabs(cf[rc]);
     const float ecur = __fsub_rn(at, (float)l);
@@ -118,8 +119,20 @@ __device__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float a
   const float skip = __fadd_rn(suf[0], lambda);
   const int keep = (best_e < 0 || skip < best) ? 0 : best_e + 1;
   for (int e = 0; e < M; e++)
-    if (e >= keep && e < m) cf[kScan16[e]] = 0;
+    if (e >= keep && e < m) cf[scan(e)] = 0;
   return keep - 1;
+}
+
+// The 16x16 default scan as trellis_sq's accessor.
+struct Scan16 {
+  __device__ __forceinline__ int operator()(int i) const { return kScan16[i]; }
+};
+
+// trellis_optimize over the 16x16 scan; `suf` is scratch for 257 floats.
+template <typename C>
+__device__ __forceinline__ int trellis16(C* cf, const float* tf, float* suf, float dc_q, float ac_q, float lambda,
+                                         const float* lut) {
+  return trellis_sq<256>(cf, tf, suf, dc_q, ac_q, lambda, lut, Scan16{});
 }
 
 // Coefficient bits of a 16x16 luma block (src/rate.rs:149-291), float

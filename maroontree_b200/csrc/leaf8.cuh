@@ -30,6 +30,10 @@ __device__ __forceinline__ float hi_cost(const mt_coef_costs& T, uint32_t m, int
 }
 
 __constant__ uint16_t kScan32[1024] = {MT_SCAN_32X32_LIST};
+// The 32x32 default scan as trellis_sq's accessor.
+struct Scan32 {
+  __device__ __forceinline__ int operator()(int i) const { return kScan32[i]; }
+};
 
 // Default scan of a W x W block (scan index -> rc = x*W + y).
 template <int W>

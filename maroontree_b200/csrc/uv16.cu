@@ -13,9 +13,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/maroontree_b200.h"
 #include "common.cuh"
 #include "leaf8.cuh"
+#include "txfm32.cuh"
 #include "wsse.cuh"
 
 namespace mth {
@@ -51,7 +54,7 @@ struct UvWork {
   int16_t resid[64];
   int16_t ac[64];  // CfL AC of the leaf's luma
   TrellisCtxScratch tr;
-  uint8_t lv[160];
+  alignas(16) uint8_t lv[160];  // the rate walk stores it as 32-bit words
 };
 
 // The shortlist's modes in the reference's order (block16.rs:1143-1156).
@@ -358,85 +361,100 @@ __global__ void __launch_bounds__(kUvThreads) uv16_420_kernel(
         rec_out[(size_t)j * 128 + pl * 64 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
 }
 
-// ---- 4:4:4: pick_uv16_444 ----
+// ---- 4:4:4: pick_uv16_444 and pick_uv32_444 ----
 
-struct Uv444Slot {
-  int16_t pred[2][256];
-  int16_t cf[2][256];
-  int16_t rr[2][256];
+// Both planes of one N x N candidate: predictions, levels (32-bit at 32x32,
+// where a full-scale DC passes 16 bits) and inverses.
+template <int N>
+struct UvBigSlot {
+  using Coef = std::conditional_t<N == 32, int32_t, int16_t>;
+  int16_t pred[2][N * N];
+  Coef cf[2][N * N];
+  int16_t rr[2][N * N];
 };
 
-struct Uv444Work {
-  Uv444Slot s[2];  // the current choice and the candidate
-  int32_t u[512];  // prediction edges, then the targets [0, 256) and the transform temporary [256, 512)
-  int16_t resid[256];
-  int16_t ac[256];
-  float suf[257];  // trellis16 scratch
-  TrellisCtxScratchW<16> trc;  // trellis_ctx<16> scratch (4:2:0 at 16x16)
-  uint8_t lv[288];
+template <int N>
+struct UvBigWork {
+  UvBigSlot<N> s[2];   // the current choice and the candidate
+  int32_t u[2 * N * N];  // prediction edges, then the targets [0, N*N) and the transform temporary [N*N, 2N*N)
+  int16_t resid[N * N];
+  int16_t ac[N * N];
+  float suf[N * N + 1];  // trellis_sq scratch
+  std::conditional_t<N == 16, TrellisCtxScratchW<16>, char> trc;  // trellis_ctx<16> scratch (4:2:0 at 16x16)
+  alignas(16) uint8_t lv[(N + 2) * N];  // the rate walk stores it as 32-bit words
 };
+using Uv444Slot = UvBigSlot<16>;
+using Uv444Work = UvBigWork<16>;
 
 struct PlaneCost {
   long long sse;
   float bits;
 };
 
-// One 16x16 plane of a candidate after its prediction: the transform with
-// the QM, the plain trellis_optimize (4:4:4's chroma_rect_trellis),
-// preserve_dc when `keep_dc`, the inverse, sse_recon and chroma_bits.
-// CTX: the 4:2:0 chroma_rect_trellis, trellis_optimize_ctx against the
-// chroma TX_16X16 costs in the plane's dc_sign context, instead.
-template <bool CTX = false>
-__device__ PlaneCost plane_chain16(const UvArgs& a, const UvPlane& P, const mt_coef_costs& T, const uint8_t* qm,
-                                   const float* sQs, const float* lut, int tx, bool keep_dc, int16_t* pred,
-                                   int16_t* cf, int16_t* rr, Uv444Work& w) {
+// One N x N plane of a candidate after its prediction: the transform with
+// the QM (DCT_DCT only at 32x32), the plain trellis_optimize (the 4:4:4
+// chroma_rect_trellis) or, CTX, trellis_optimize_ctx against the chroma
+// costs in the plane's dc_sign context (4:2:0), preserve_dc when `keep_dc`,
+// the inverse, sse_recon and chroma_bits.
+template <int N, bool CTX = false>
+__device__ PlaneCost plane_chain(const UvArgs& a, const UvPlane& P, const mt_coef_costs& T, const uint8_t* qm,
+                                 const float* sQs, const float* lut, int tx, bool keep_dc, int16_t* pred,
+                                 typename UvBigSlot<N>::Coef* cf, int16_t* rr, UvBigWork<N>& w) {
+  static_assert(N == 16 || N == 32, "16x16 and 32x32 chroma blocks");
+  static_assert(!CTX || N == 16, "the context trellis runs at 16x16 here");
+  constexpr int NN = N * N, L = log2w<N>();
   const mt_split16_params& p = a.p;
   const mt_quant& q = a.q;
   int32_t sum = 0;
 #pragma unroll 8
-  for (int i = 0; i < 256; i++) {
-    const int32_t r = (int32_t)P.src[(size_t)(i >> 4) * p.stride + (i & 15)] - pred[i];
+  for (int i = 0; i < NN; i++) {
+    const int32_t r = (int32_t)P.src[(size_t)(i >> L) * p.stride + (i & (N - 1))] - pred[i];
     w.resid[i] = (int16_t)r;
     sum += r;
   }
   float* tf = reinterpret_cast<float*>(w.u);
-  int32_t* tmp = w.u + 256;
-  fwd16x16(w.resid, tx, q, cf, tf, tmp);
-  if (qm) apply_qm(cf, tf, sQs, 256);
+  int32_t* tmp = w.u + NN;
+  if constexpr (N == 16) fwd16x16(w.resid, tx, q, cf, tf, tmp);
+  else fwd32x32(w.resid, q, cf, tf, tmp);
+  if (qm) apply_qm(cf, tf, sQs, NN);
   if (a.lambda > 0.0f) {
     if constexpr (CTX)
       trellis_ctx<16>(cf, tf, (float)q.dc_q, (float)q.ac_q, a.lambda, T, P.ds, qm, q.qm_level >= 5, p.band_tilt,
                       w.trc);
+    else if constexpr (N == 16)
+      trellis_sq<NN>(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut, Scan16{});
     else
-      trellis16(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut);
+      trellis_sq<NN>(cf, tf, w.suf, (float)q.dc_q, (float)q.ac_q, a.lambda, lut, Scan32{});
   }
   if (keep_dc) {
-    const int32_t mean = sum / 256;
-    if (cf[0] == 0 && abs(mean) >= 8) cf[0] = (int16_t)(mean > 0 ? 1 : -1);
+    const int32_t mean = sum / NN;
+    if (cf[0] == 0 && abs(mean) >= 8) cf[0] = mean > 0 ? 1 : -1;
   }
-  inv16x16(cf, tx, q, qm, rr, tmp);
+  if constexpr (N == 16) inv16x16(cf, tx, q, qm, rr, tmp);
+  else inv32x32(cf, q, qm, rr, tmp);
   ErrBlock<int16_t, int16_t> eb;
   eb.src = P.src;
   eb.stride = p.stride;
   eb.pred = pred;
   eb.resid = rr;
-  eb.w = 16;
+  eb.w = N;
   eb.vw = P.vw;
   eb.vh = P.vh;
   eb.maxv = (1 << p.bd) - 1;
   PlaneCost c;
   c.sse = sse_recon_block(eb, p.wsse_scale);
-  c.bits = rate_bounded<16>(cf, T, P.sk, P.ds, 0, -1, p.use_skip_bits != 0, P.skip1, P.skip0,
-                            __int_as_float(0x7f800000), w.lv);
+  c.bits = rate_bounded<N>(cf, T, P.sk, P.ds, 0, -1, p.use_skip_bits != 0, P.skip1, P.skip0,
+                           __int_as_float(0x7f800000), w.lv);
   return c;
 }
 
-// cfl_best_alpha over a 16x16 block's displayed part (as cfl_alpha).
-__device__ int cfl_alpha16(const int16_t* ac, const UvPlane& P, int stride, int32_t dc, int32_t maxv) {
+// cfl_best_alpha over an N x N block's displayed part (as cfl_alpha).
+template <int N>
+__device__ int cfl_alpha_n(const int16_t* ac, const UvPlane& P, int stride, int32_t dc, int32_t maxv) {
   long long num = 0, den = 0;
   for (int y = 0; y < P.vh; y++)
     for (int x = 0; x < P.vw; x++) {
-      const long long v = ac[y * 16 + x];
+      const long long v = ac[y * N + x];
       num += (long long)((int32_t)P.src[(size_t)y * stride + x] - dc) * v;
       den += v * v;
     }
@@ -451,7 +469,7 @@ __device__ int cfl_alpha16(const int16_t* ac, const UvPlane& P, int stride, int3
     long long e = 0;
     for (int y = 0; y < P.vh; y++)
       for (int x = 0; x < P.vw; x++) {
-        const long long d = (int32_t)P.src[(size_t)y * stride + x] - cfl_pred_pixel(dc, ac[y * 16 + x], c, maxv);
+        const long long d = (int32_t)P.src[(size_t)y * stride + x] - cfl_pred_pixel(dc, ac[y * N + x], c, maxv);
         e += d * d;
       }
     if (e < best_e) {
@@ -462,16 +480,21 @@ __device__ int cfl_alpha16(const int16_t* ac, const UvPlane& P, int stride, int3
   return best_a;
 }
 
-__global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
+// The 4:4:4 leaf searches: N = 16 is pick_uv16_444 (block16.rs:437-978), N =
+// 32 pick_uv32_444 (block32.rs:2264-2720).  J: the job (four or eight
+// context bytes per plane and side).
+template <int N, typename J>
+__global__ void __launch_bounds__(kUvThreads) uv444_kernel(
     const uint16_t* __restrict__ src_u, const uint16_t* __restrict__ src_v, const uint16_t* __restrict__ rec_u,
     const uint16_t* __restrict__ rec_v, const uint16_t* __restrict__ luma, UvArgs a,
     const uint8_t* __restrict__ qm_row, const mt_coef_costs* __restrict__ costs,
-    const mt_uv_mode_costs* __restrict__ mode_costs, const mt_uv16_444_job* __restrict__ jobs, int n,
+    const mt_uv_mode_costs* __restrict__ mode_costs, const J* __restrict__ jobs, int n,
     mt_uv16_result* __restrict__ res, int32_t* __restrict__ cf_out, uint16_t* __restrict__ rec_out, int arena) {
+  constexpr int NN = N * N, U = N / 4, L = log2w<N>();
   __shared__ mt_coef_costs sT;
   __shared__ mt_uv_mode_costs sM;
-  __shared__ uint8_t sQm[256];
-  __shared__ float sQs[256];
+  __shared__ uint8_t sQm[NN];
+  __shared__ float sQs[NN];
   __shared__ float sLut[64];
   {
     const float* g = reinterpret_cast<const float*>(costs);
@@ -480,7 +503,7 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     const float* gm = reinterpret_cast<const float*>(mode_costs);
     float* sm = reinterpret_cast<float*>(&sM);
     for (int i = threadIdx.x; i < (int)(sizeof(mt_uv_mode_costs) / 4); i += blockDim.x) sm[i] = gm[i];
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    for (int i = threadIdx.x; i < NN; i += blockDim.x) {
       const int wq = a.has_qm ? qm_row[i] : 32;
       sQm[i] = (uint8_t)wq;
       sQs[i] = fwd_qm_scale(wq);
@@ -491,11 +514,11 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const mt_split16_params& p = a.p;
-  const mt_uv16_444_job jb = jobs[j];
+  const J jb = jobs[j];
   mt_uv16_result& r = res[j];
   const int cx = jb.px, cy = jb.py;
   const float kInf = __int_as_float(0x7f800000);
-  const bool ok = (cx & 15) == 0 && (cy & 15) == 0 && cx + 16 <= p.frame_w && cy + 16 <= p.frame_h &&
+  const bool ok = (cx & (N - 1)) == 0 && (cy & (N - 1)) == 0 && cx + N <= p.frame_w && cy + N <= p.frame_h &&
                   jb.y_mode <= MT_PAETH_PRED;
   if (!ok) {
     r.total = r.dc_total = r.cfl_total = kInf;
@@ -503,9 +526,9 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     r.angle_delta = 0;
     r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
     if (cf_out)
-      for (int i = 0; i < 512; i++) cf_out[(size_t)j * 512 + i] = 0;
+      for (int i = 0; i < 2 * NN; i++) cf_out[(size_t)j * 2 * NN + i] = 0;
     if (rec_out)
-      for (int i = 0; i < 512; i++) rec_out[(size_t)j * 512 + i] = 0;
+      for (int i = 0; i < 2 * NN; i++) rec_out[(size_t)j * 2 * NN + i] = 0;
     return;
   }
   const mt_coef_costs& T = sT;
@@ -521,60 +544,69 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     UvPlane& q = P[pl];
     q.src = (pl ? src_v : src_u) + (size_t)cy * p.stride + cx;
     q.rec = pl ? rec_v : rec_u;
-    q.vw = min(max(vis_w - cx, 0), 16);
-    q.vh = min(max(vis_h - cy, 0), 16);
+    q.vw = min(max(vis_w - cx, 0), N);
+    q.vh = min(max(vis_h - cy, 0), N);
     bool anz = false, lnz = false;
-    int s = -8;
-    for (int k = 0; k < 4; k++) {
+    int s = -2 * U;
+    for (int k = 0; k < U; k++) {
       anz |= jb.a_coef[pl][k] != 0x40;
       lnz |= jb.l_coef[pl][k] != 0x40;
       s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
     }
-    q.sk = 7 + anz + lnz;  // skip_ctx_16
-    q.ds = (s != 0) + (s > 0);  // dc_sign_ctx_16
+    q.sk = 7 + anz + lnz;       // the chroma txb_skip context over the block's units
+    q.ds = (s != 0) + (s > 0);  // dc_sign_ctx_span over U + U units
     q.skip1 = p.use_skip_bits ? p.skip_bits[q.sk][0] : 0.0f;
     q.skip0 = p.use_skip_bits ? p.skip_bits[q.sk][1] : 0.0f;
   }
-  Uv444Work& w = smem_arena<Uv444Work>(arena);
-  // 1. DC (block16.rs:451-479), slot 0
+  UvBigWork<N>& w = smem_arena<UvBigWork<N>>(arena);
+  // DC, slot 0
   int32_t dc[2];
   PlaneCost dcc[2], cfc[2];
   for (int pl = 0; pl < 2; pl++) {
-    predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
-                   w.s[0].pred[pl], w.u);
+    predict_sq<N>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
+                  w.s[0].pred[pl], w.u);
     dc[pl] = w.s[0].pred[pl][0];
-    dcc[pl] = plane_chain16(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, true, w.s[0].pred[pl], w.s[0].cf[pl],
-                            w.s[0].rr[pl], w);
+    dcc[pl] = plane_chain<N>(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, true, w.s[0].pred[pl], w.s[0].cf[pl],
+                             w.s[0].rr[pl], w);
   }
-  // 2. CfL against DC (:480-597), slot 1
+  // CfL against DC, slot 1: cfl_ac_444 (each luma sample << 3, less the rounded mean)
   {
     const int ls = a.u.luma_stride;
     const uint16_t* l = luma + (size_t)cy * ls + cx;
-    int32_t sum = 128;
-    for (int i = 0; i < 256; i++) {
-      const int32_t v = (int32_t)l[(size_t)(i >> 4) * ls + (i & 15)] << 3;
+    int32_t sum = NN / 2;
+    for (int i = 0; i < NN; i++) {
+      const int32_t v = (int32_t)l[(size_t)(i >> L) * ls + (i & (N - 1))] << 3;
       w.ac[i] = (int16_t)v;
       sum += v;
     }
-    const int32_t mean = sum >> 8;
-    for (int i = 0; i < 256; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
+    const int32_t mean = sum >> (2 * L);
+    for (int i = 0; i < NN; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
   }
   int alpha[2];
-  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha16(w.ac, P[pl], p.stride, dc[pl], maxv);
+  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha_n<N>(w.ac, P[pl], p.stride, dc[pl], maxv);
   for (int pl = 0; pl < 2; pl++) {
-    for (int i = 0; i < 256; i++) w.s[1].pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
-    cfc[pl] = plane_chain16(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, false, w.s[1].pred[pl], w.s[1].cf[pl],
-                            w.s[1].rr[pl], w);
+    for (int i = 0; i < NN; i++) w.s[1].pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
+    cfc[pl] = plane_chain<N>(a, P[pl], T, qm, sQs, sLut, MT_TX_DCT_DCT, false, w.s[1].pred[pl], w.s[1].cf[pl],
+                             w.s[1].rr[pl], w);
   }
   const float sig = uv_mode_bits(M, jb.y_mode, MT_UV_CFL_PRED, true, alpha[0], alpha[1]);
   const float dc_bits = uv_mode_bits(M, jb.y_mode, MT_DC_PRED, false, 0, 0);
-  const float dc_total = rd_cost_i64(dcc[0].sse + dcc[1].sse, mlam, __fadd_rn(__fadd_rn(dcc[0].bits, dcc[1].bits), dc_bits));
-  const float cfl_total = rd_cost_i64(cfc[0].sse + cfc[1].sse, mlam, __fadd_rn(__fadd_rn(cfc[0].bits, cfc[1].bits), sig));
+  float dc_total, cfl_total;
+  if constexpr (N == 16) {
+    // rd_cost_i64 of the summed SSE and bits (block16.rs:587-597)
+    dc_total = rd_cost_i64(dcc[0].sse + dcc[1].sse, mlam, __fadd_rn(__fadd_rn(dcc[0].bits, dcc[1].bits), dc_bits));
+    cfl_total = rd_cost_i64(cfc[0].sse + cfc[1].sse, mlam, __fadd_rn(__fadd_rn(cfc[0].bits, cfc[1].bits), sig));
+  } else {
+    // the planes' rd_cost_i64 summed, then the mode bits (block32.rs:2399-2404)
+    dc_total = __fadd_rn(__fadd_rn(rd_cost_i64(dcc[0].sse, mlam, dcc[0].bits), rd_cost_i64(dcc[1].sse, mlam, dcc[1].bits)),
+                         __fmul_rn(mlam, dc_bits));
+    cfl_total = __fadd_rn(__fadd_rn(rd_cost_i64(cfc[0].sse, mlam, cfc[0].bits), rd_cost_i64(cfc[1].sse, mlam, cfc[1].bits)),
+                          __fmul_rn(mlam, sig));
+  }
   const bool use_cfl = cfl_total < dc_total && (alpha[0] != 0 || alpha[1] != 0);
   int best = use_cfl ? 1 : 0;
   const PlaneCost* cur = use_cfl ? cfc : dcc;
-  // 3. the directional stage on dir_lambda (:598-772): the current choice's
-  // total, then the ranked modes
+  // the directional stage on dir_lambda: the current choice's total, then the ranked modes
   float best_total = __fmul_rn(dlam, use_cfl ? sig : dc_bits);
   for (int pl = 0; pl < 2; pl++) best_total = __fadd_rn(best_total, rd_cost_i64(cur[pl].sse, dlam, cur[pl].bits));
   int mode = MT_DC_PRED, delta = 0;
@@ -586,8 +618,8 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     const int m = kJointList[ci];
     unsigned long long sc = 0;
     for (int pl = 0; pl < 2; pl++) {
-      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd, sp, w.u);
-      sc += satd_sad_proxy<16>(pl ? src_v : src_u, p.stride, cx, cy, sp, P[pl].vw, P[pl].vh);
+      predict_sq<N>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd, sp, w.u);
+      sc += satd_sad_proxy<N>(pl ? src_v : src_u, p.stride, cx, cy, sp, P[pl].vw, P[pl].vh);
     }
     int pos = tn < 3 ? tn : 2;
     if (tn == 3 && sc >= tc[pos]) continue;
@@ -605,13 +637,13 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     bool in = false;
     for (int e = 0; e < tn; e++) in |= tm[e] == m;
     if (!in) continue;
-    const int tx = chroma_tx(m);
+    const int tx = N == 32 ? MT_TX_DCT_DCT : chroma_tx(m);  // forced DCT_DCT at TX_32X32
     float total = __fmul_rn(dlam, uv_mode_bits(M, jb.y_mode, m, false, 0, 0));
-    Uv444Slot& c = w.s[1 - best];
+    UvBigSlot<N>& c = w.s[1 - best];
     for (int pl = 0; pl < 2; pl++) {
-      predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd,
-                     c.pred[pl], w.u);
-      const PlaneCost pc = plane_chain16(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+      predict_sq<N>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd,
+                    c.pred[pl], w.u);
+      const PlaneCost pc = plane_chain<N>(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
       total = __fadd_rn(total, rd_cost_i64(pc.sse, dlam, pc.bits));
     }
     if (total < best_total) {
@@ -620,9 +652,9 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
       best = 1 - best;
     }
   }
-  // the zone-2 angle deltas of a directional winner (uv_ad, :743-778)
+  // the zone-2 angle deltas of a directional winner (uv_ad; uv_ad32 at 32x32)
   if (a.u.angle_deltas && directional(mode)) {
-    const int m = mode, tx = chroma_tx(m);
+    const int m = mode, tx = N == 32 ? MT_TX_DCT_DCT : chroma_tx(m);
     int lo = 0, hi = -1;
     if (m == MT_V_PRED) lo = 1, hi = 3;
     else if (m == MT_H_PRED) lo = -3, hi = -1;
@@ -631,11 +663,11 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
     for (int d = lo; d <= hi; d++) {
       if (d == 0) continue;
       float total = __fmul_rn(dlam, __fadd_rn(base_sig, M.angle_delta[m - MT_V_PRED][d + 3]));
-      Uv444Slot& c = w.s[1 - best];
+      UvBigSlot<N>& c = w.s[1 - best];
       for (int pl = 0; pl < 2; pl++) {
-        predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, false, false, ft, p.bd, c.pred[pl],
-                       w.u);
-        const PlaneCost pc = plane_chain16(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+        predict_sq<N>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, false, false, ft, p.bd, c.pred[pl],
+                      w.u);
+        const PlaneCost pc = plane_chain<N>(a, P[pl], T, qm, sQs, sLut, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
         total = __fadd_rn(total, rd_cost_i64(pc.sse, dlam, pc.bits));
       }
       if (total < best_total) {
@@ -652,14 +684,14 @@ __global__ void __launch_bounds__(kUvThreads) uv16_444_kernel(
   r.angle_delta = (int8_t)delta;
   r.cfl_alpha[0] = (int8_t)alpha[0];
   r.cfl_alpha[1] = (int8_t)alpha[1];
-  const Uv444Slot& b = w.s[best];
+  const UvBigSlot<N>& b = w.s[best];
   if (cf_out)
     for (int pl = 0; pl < 2; pl++)
-      for (int i = 0; i < 256; i++) cf_out[(size_t)j * 512 + pl * 256 + i] = b.cf[pl][i];
+      for (int i = 0; i < NN; i++) cf_out[(size_t)j * 2 * NN + pl * NN + i] = b.cf[pl][i];
   if (rec_out)
     for (int pl = 0; pl < 2; pl++)
-      for (int i = 0; i < 256; i++)
-        rec_out[(size_t)j * 512 + pl * 256 + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
+      for (int i = 0; i < NN; i++)
+        rec_out[(size_t)j * 2 * NN + pl * NN + i] = (uint16_t)clampi((int32_t)b.pred[pl][i] + b.rr[pl][i], 0, maxv);
 }
 
 // ---- the 32x32 leaf at 4:2:0: pick_uv32_420 ----
@@ -749,7 +781,7 @@ __global__ void __launch_bounds__(kUvThreads) uv32_420_kernel(
     predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, MT_DC_PRED, 0, have_tr, have_bl, ft, p.bd,
                    w.s[0].pred[pl], w.u);
     dc[pl] = w.s[0].pred[pl][0];
-    const PlaneCost c = plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, true, w.s[0].pred[pl],
+    const PlaneCost c = plane_chain<16, true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, true, w.s[0].pred[pl],
                                            w.s[0].cf[pl], w.s[0].rr[pl], w);
     dc_total = __fadd_rn(dc_total, rd_cost_i64(c.sse, mlam, c.bits));
   }
@@ -772,13 +804,13 @@ __global__ void __launch_bounds__(kUvThreads) uv32_420_kernel(
     for (int i = 0; i < 256; i++) w.ac[i] = (int16_t)(w.ac[i] - mean);
   }
   int alpha[2];
-  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha16(w.ac, P[pl], p.stride, dc[pl], maxv);
+  for (int pl = 0; pl < 2; pl++) alpha[pl] = cfl_alpha_n<16>(w.ac, P[pl], p.stride, dc[pl], maxv);
   {
     Uv444Slot& c = w.s[1 - best];
     float body = 0.0f;
     for (int pl = 0; pl < 2; pl++) {
       for (int i = 0; i < 256; i++) c.pred[pl][i] = (int16_t)cfl_pred_pixel(dc[pl], w.ac[i], alpha[pl], maxv);
-      const PlaneCost pc = plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, false, c.pred[pl],
+      const PlaneCost pc = plane_chain<16, true>(a, P[pl], T, qm, sQs, nullptr, MT_TX_DCT_DCT, false, c.pred[pl],
                                                c.cf[pl], c.rr[pl], w);
       body = __fadd_rn(body, rd_cost_i64(pc.sse, mlam, pc.bits));
     }
@@ -826,7 +858,7 @@ __global__ void __launch_bounds__(kUvThreads) uv32_420_kernel(
       predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, 0, have_tr, have_bl, ft, p.bd,
                      c.pred[pl], w.u);
       const PlaneCost pc =
-          plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+          plane_chain<16, true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
       total = __fadd_rn(total, rd_cost_i64(pc.sse, mlam, pc.bits));
     }
     if (total < best_total) {
@@ -851,7 +883,7 @@ __global__ void __launch_bounds__(kUvThreads) uv32_420_kernel(
         predict_sq<16>(P[pl].rec, p.stride, p.frame_w, p.frame_h, cx, cy, m, d, false, false, ft, p.bd, c.pred[pl],
                        w.u);
         const PlaneCost pc =
-            plane_chain16<true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
+            plane_chain<16, true>(a, P[pl], T, qm, sQs, nullptr, tx, true, c.pred[pl], c.cf[pl], c.rr[pl], w);
         total = __fadd_rn(total, rd_cost_i64(pc.sse, mlam, pc.bits));
       }
       if (total < best_total) {
@@ -901,15 +933,16 @@ int uv_check_444(const mt_split16_params* p, const mt_uv16_params* u, const mt_q
 
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+template <int N, typename J>
 int uv444_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* luma,
                  const mt_split16_params* prm, const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm,
-                 const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mc, const mt_uv16_444_job* d_jobs, int32_t n,
+                 const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mc, const J* d_jobs, int32_t n,
                  mt_uv16_result* d_res, int32_t* d_cf, uint16_t* d_rec, void* stream) {
   const int rc = uv_check_444(prm, uvp, quant, n);
   if (rc != MT_OK) return rc;
   if (n == 0) return MT_OK;
   if (!su || !sv || !ru || !rv || !luma || !d_costs || !d_mc || !d_jobs || !d_res) return MT_ERR_INVALID_INPUT;
-  if (!(uvp->dir_lambda > 0.0f)) return MT_ERR_INVALID_INPUT;
+  if (!(uvp->dir_lambda > 0.0f) || prm->frame_w < N || prm->frame_h < N) return MT_ERR_INVALID_INPUT;
   UvArgs a;
   a.p = *prm;
   a.u = *uvp;
@@ -917,11 +950,12 @@ int uv444_device(const uint16_t* su, const uint16_t* sv, const uint16_t* ru, con
   a.lambda = prm->trellis_lambda0 > 0.0f ? mth::scaled_trellis_lambda_host((float)quant->dc_q, prm->trellis_lambda0)
                                          : 0.0f;
   a.has_qm = quant->qm_level < 15 && d_qm != nullptr;
-  const int stride = arena_stride(sizeof(Uv444Work));
+  const int stride = arena_stride(sizeof(UvBigWork<N>));
+  auto* kern = uv444_kernel<N, J>;
   int threads = 0;
   size_t dyn = 0;
-  if (!arena_launch_shape(uv16_444_kernel, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
-  uv16_444_kernel<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+  if (!arena_launch_shape(kern, n, stride, kUvThreads, &threads, &dyn)) return MT_ERR_DEVICE;
+  kern<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
       su, sv, ru, rv, luma, a, d_qm, d_costs, d_mc, d_jobs, n, d_res, d_cf, d_rec, stride);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
@@ -1059,6 +1093,33 @@ int mt_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                  });
 }
 
+int mt_pick_uv32_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
+                            const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
+                            const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
+                            const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
+                            const mt_uv32_444_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
+                            uint16_t* d_rec, void* stream) {
+  return uv444_device<32>(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs,
+                          d_mode_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
+}
+
+int mt_pick_uv32_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* prm, const mt_uv16_params* uvp,
+                     const mt_quant* quant, const uint8_t* qm_row, const mt_coef_costs* costs,
+                     const mt_uv_mode_costs* mode_costs, const mt_uv32_444_job* jobs, int32_t n,
+                     mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  const int rc = uv_check_444(prm, uvp, quant, n);
+  if (rc != MT_OK) return rc;
+  if (n > 0 && !(uvp->dir_lambda > 0.0f)) return MT_ERR_INVALID_INPUT;
+  return uv_host(src_u, src_v, rec_u, rec_v, luma, (size_t)prm->frame_h, prm, uvp, quant, qm_row, 1024, costs,
+                 mode_costs, jobs, n, results, cf_out, rec_out, 2048,
+                 [&](const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* l,
+                     const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc,
+                     const mt_uv32_444_job* j, mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
+                   return uv444_device<32>(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
+                 });
+}
+
 int mt_pick_uv32_420_device(const uint16_t* d_src_u, const uint16_t* d_src_v, const uint16_t* d_rec_u,
                             const uint16_t* d_rec_v, const uint16_t* d_luma, const mt_split16_params* prm,
                             const mt_uv16_params* uvp, const mt_quant* quant, const uint8_t* d_qm_row,
@@ -1091,8 +1152,8 @@ int mt_pick_uv16_444_device(const uint16_t* d_src_u, const uint16_t* d_src_v, co
                             const mt_coef_costs* d_costs, const mt_uv_mode_costs* d_mode_costs,
                             const mt_uv16_444_job* d_jobs, int32_t n, mt_uv16_result* d_results, int32_t* d_cf,
                             uint16_t* d_rec, void* stream) {
-  return uv444_device(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs, d_mode_costs,
-                      d_jobs, n, d_results, d_cf, d_rec, stream);
+  return uv444_device<16>(d_src_u, d_src_v, d_rec_u, d_rec_v, d_luma, prm, uvp, quant, d_qm_row, d_costs,
+                          d_mode_costs, d_jobs, n, d_results, d_cf, d_rec, stream);
 }
 
 int mt_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
@@ -1108,7 +1169,7 @@ int mt_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                  [&](const uint16_t* su, const uint16_t* sv, const uint16_t* ru, const uint16_t* rv, const uint16_t* l,
                      const uint8_t* qm, const mt_coef_costs* c, const mt_uv_mode_costs* mc,
                      const mt_uv16_444_job* j, mt_uv16_result* r, int32_t* cf, uint16_t* rec) {
-                   return uv444_device(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
+                   return uv444_device<16>(su, sv, ru, rv, l, prm, uvp, quant, qm, c, mc, j, n, r, cf, rec, nullptr);
                  });
 }
 

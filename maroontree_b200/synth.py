@@ -541,6 +541,19 @@ def uv16_444_jobs(w, h, seed, every=1, leaf=16):
     return np.array(rows, abi.UV16_444_JOB_DTYPE)
 
 
+def uv32_444_jobs(w, h, seed):
+    """32x32-leaf jobs of the 4:4:4 chroma search (mt_uv32_444_job): eight
+    coefficient-context bytes per plane and side."""
+    rng = np.random.default_rng(seed)
+    rows = []
+    for py in range(0, h - 31, 32):
+        for px in range(0, w - 31, 32):
+            fl = block_flags(px, py, w, h, 32) | (abi.CAND_FILTER_TYPE if rng.random() < 0.5 else 0)
+            ctx = coef_ctx_bytes(rng, 32)
+            rows.append((px, py, int(rng.integers(0, 13)), fl, ctx[:16].reshape(2, 8), ctx[16:].reshape(2, 8), (0, 0)))
+    return np.array(rows, abi.UV32_444_JOB_DTYPE)
+
+
 def uv16_jobs(w, h, seed, every=1):
     """16x16-leaf jobs of the 4:2:0 chroma search (mt_uv16_job): every
     16x16 leaf of a w x h frame (or about one in `every`), a random luma

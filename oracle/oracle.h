@@ -181,6 +181,12 @@ int or_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                      const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
                      const mt_uv16_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
                      uint16_t* rec_out);
+/* block32.rs pick_uv32_444 (:2264-2720) with the shipped tuning, per 32x32 leaf. */
+int or_pick_uv32_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
+                     const mt_uv32_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
+                     uint16_t* rec_out);
 /* dct1d_32_i32 in place on 32 values. */
 void or_dct1d_32(int32_t* buf);
 /* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */

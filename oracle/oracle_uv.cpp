@@ -115,37 +115,236 @@ float plane_cost(const mt_split16_params* p, const mt_quant* q, const uint8_t* q
   return (float)sse + p->rd_lambda * bits;
 }
 
-// One 16x16 plane of a chroma candidate: the transform with the QM, the plain
+// One N x N plane of a chroma candidate: the transform with the QM, the plain
 // trellis_optimize (chroma_rect_trellis outside 4:2:0 / 4:2:2,
 // lossy_state.rs:834-838) or, ctx, trellis_optimize_ctx (4:2:0), preserve_dc when keep_dc, the inverse, sse_recon
 // and chroma_bits at TX_16X16 (lossy_state.rs:749-811); sse and bits apart.
-void plane_cost16(const mt_split16_params* p, const mt_quant* q, const uint8_t* qm, const mt_coef_cdfs* cd,
+void plane_cost_n(int N, const mt_split16_params* p, const mt_quant* q, const uint8_t* qm, const mt_coef_cdfs* cd,
                   const Plane& P, int cx, int cy, int tx, bool keep_dc, const int32_t* pred, int32_t* cf, int32_t* rr,
                   int64_t* sse, float* bits, bool ctx = false) {
-  int32_t resid[256];
-  float tf[256];
+  const int NN = N * N;
+  std::vector<int32_t> resid((size_t)NN);
+  std::vector<float> tf((size_t)NN);
   int32_t sum = 0;
-  for (int i = 0; i < 256; i++) {
-    resid[i] = (int32_t)P.src[(size_t)(cy + i / 16) * p->stride + cx + i % 16] - pred[i];
-    sum += resid[i];
+  for (int i = 0; i < NN; i++) {
+    resid[(size_t)i] = (int32_t)P.src[(size_t)(cy + i / N) * p->stride + cx + i % N] - pred[i];
+    sum += resid[(size_t)i];
   }
-  or_fwd_txfm_quant(resid, tx, 16, q, qm, cf, tf);
+  or_fwd_txfm_quant(resid.data(), tx, N, q, qm, cf, tf.data());
   if (ctx)  // the 4:2:0 chroma_rect_trellis (lossy_state.rs:821-870)
-    or_trellis_optimize_ctx(cf, tf, (float)q->dc_q, (float)q->ac_q, or_default_scan(16), 16, p->trellis_lambda0, cd,
-                            P.ds, qm, q->qm_level, p->band_tilt);
+    or_trellis_optimize_ctx(cf, tf.data(), (float)q->dc_q, (float)q->ac_q, or_default_scan(N), N, p->trellis_lambda0,
+                            cd, P.ds, qm, q->qm_level, p->band_tilt);
   else
-    or_trellis_optimize(cf, tf, (float)q->dc_q, (float)q->ac_q, or_default_scan(16), 256, p->trellis_lambda0);
+    or_trellis_optimize(cf, tf.data(), (float)q->dc_q, (float)q->ac_q, or_default_scan(N), NN, p->trellis_lambda0);
   if (keep_dc) {
-    const int32_t mean = sum / 256;
+    const int32_t mean = sum / NN;
     if (cf[0] == 0 && (mean < 0 ? -mean : mean) >= 8) cf[0] = mean > 0 ? 1 : -1;
   }
-  or_inv_txfm_dequant(cf, tx, 16, q, qm, rr);
+  or_inv_txfm_dequant(cf, tx, N, q, qm, rr);
   const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
   const uint16_t pos[2] = {(uint16_t)cx, (uint16_t)cy};
   *sse = 0;
-  or_sse_recon(P.src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, 16, 16, p->wsse_scale, sse);
-  *bits = or_real_block_bits_bounded(cf, or_default_scan(16), 16, 16, cd, P.sk, P.ds, -1, 0, p->use_skip_bits,
+  or_sse_recon(P.src, p->stride, vis_w, vis_h, p->bd, pos, pred, rr, 1, N, N, p->wsse_scale, sse);
+  *bits = or_real_block_bits_bounded(cf, or_default_scan(N), N, N, cd, P.sk, P.ds, -1, 0, p->use_skip_bits,
                                      p->skip_bits[P.sk], INFINITY);
+}
+
+inline void plane_cost16(const mt_split16_params* p, const mt_quant* q, const uint8_t* qm, const mt_coef_cdfs* cd,
+                         const Plane& P, int cx, int cy, int tx, bool keep_dc, const int32_t* pred, int32_t* cf,
+                         int32_t* rr, int64_t* sse, float* bits, bool ctx = false) {
+  plane_cost_n(16, p, q, qm, cd, P, cx, cy, tx, keep_dc, pred, cf, rr, sse, bits, ctx);
+}
+
+template <int N, typename J>
+int pick444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+            const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+            const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc, const J* jobs, int32_t n,
+            mt_uv16_result* results, int32_t* cf_out, uint16_t* rec_out) {
+  constexpr int NN = N * N, U = N / 4;
+  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
+  const int32_t maxv = (1 << p->bd) - 1;
+  const float mlam = p->rd_lambda, dlam = u->dir_lambda;
+  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
+  static const int kList[12] = {MT_SMOOTH_V_PRED, MT_PAETH_PRED, MT_SMOOTH_PRED, MT_SMOOTH_H_PRED,
+                                MT_V_PRED,        MT_H_PRED,     MT_D135_PRED,   MT_D113_PRED,
+                                MT_D157_PRED,     MT_D45_PRED,   MT_D67_PRED,    MT_D203_PRED};
+  std::vector<int32_t> bufs(12 * NN);
+  for (int j = 0; j < n; j++) {
+    const J& jb = jobs[j];
+    mt_uv16_result& r = results[j];
+    const int cx = jb.px, cy = jb.py;
+    if ((cx & (N - 1)) || (cy & (N - 1)) || cx + N > p->frame_w || cy + N > p->frame_h || jb.y_mode > MT_PAETH_PRED) {
+      r.total = r.dc_total = r.cfl_total = INFINITY;
+      r.uv_mode = 255;
+      r.angle_delta = 0;
+      r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
+      if (cf_out) memset(cf_out + (size_t)j * 2 * NN, 0, 2 * NN * sizeof(int32_t));
+      if (rec_out) memset(rec_out + (size_t)j * 2 * NN, 0, 2 * NN * sizeof(uint16_t));
+      continue;
+    }
+    const bool tr = jb.flags & MT_CAND_HAVE_TR, bl = jb.flags & MT_CAND_HAVE_BL, ft = jb.flags & MT_CAND_FILTER_TYPE;
+    Plane P[2];
+    for (int pl = 0; pl < 2; pl++) {
+      P[pl].src = pl ? src_v : src_u;
+      P[pl].rec = pl ? rec_v : rec_u;
+      // the chroma txb_skip context and dc_sign span over the block's U + U units
+      // (skip_ctx_16 / dc_sign_ctx_16 at 16x16, lossy_state.rs:1420-1440)
+      bool anz = false, lnz = false;
+      int s = -2 * U;
+      for (int k = 0; k < U; k++) {
+        anz |= jb.a_coef[pl][k] != 0x40;
+        lnz |= jb.l_coef[pl][k] != 0x40;
+        s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
+      }
+      P[pl].sk = 7 + anz + lnz;
+      P[pl].ds = (s != 0) + (s > 0);
+    }
+    int32_t* dpred = &bufs[0];  // [2][NN]
+    int32_t* dcf = &bufs[2 * NN];
+    int32_t* drr = &bufs[4 * NN];
+    int32_t* cpred = &bufs[6 * NN];
+    int32_t* ccf = &bufs[8 * NN];
+    int32_t* crr = &bufs[10 * NN];
+    // 1. DC
+    int32_t dc[2];
+    int64_t dsse[2], csse[2];
+    float dbits[2], cbits[2];
+    for (int pl = 0; pl < 2; pl++) {
+      dc[pl] = or_dc_pred(P[pl].rec, p->stride, cx, cy, N, N, p->bd);
+      for (int i = 0; i < NN; i++) dpred[pl * NN + i] = dc[pl];
+      plane_cost_n(N, p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, true, dpred + pl * NN, dcf + pl * NN,
+                   drr + pl * NN, &dsse[pl], &dbits[pl]);
+    }
+    // 2. CfL: cfl_ac_444 and cfl_best_alpha (or_cfl_alpha without subsampling)
+    mt_cfl_block cb = {};
+    cb.cx = (uint16_t)cx;
+    cb.cy = (uint16_t)cy;
+    cb.dc[0] = (int16_t)dc[0];
+    cb.dc[1] = (int16_t)dc[1];
+    int8_t alpha[2];
+    std::vector<int32_t> ac(NN);
+    or_cfl_alpha(luma, u->luma_stride, src_u, src_v, p->stride, 0, 0, N, N, vis_w, vis_h, p->bd, &cb, 1, alpha,
+                 ac.data());
+    for (int pl = 0; pl < 2; pl++) {
+      for (int i = 0; i < NN; i++) {
+        const int32_t diff = alpha[pl] * ac[i];
+        const int32_t mag = ((diff < 0 ? -diff : diff) + 32) >> 6;
+        const int32_t v = dc[pl] + (diff < 0 ? -mag : mag);
+        cpred[pl * NN + i] = v < 0 ? 0 : (v > maxv ? maxv : v);
+      }
+      plane_cost_n(N, p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, false, cpred + pl * NN, ccf + pl * NN,
+                   crr + pl * NN, &csse[pl], &cbits[pl]);
+    }
+    const float sig = or_uv_mode_bits(mc, jb.y_mode, MT_UV_CFL_PRED, 1, alpha[0], alpha[1]);
+    const float dcb = or_uv_mode_bits(mc, jb.y_mode, MT_DC_PRED, 0, 0, 0);
+    float dc_total, cfl_total;
+    if (N == 16) {  // block16.rs:587-597
+      dc_total = (float)(dsse[0] + dsse[1]) + mlam * (dbits[0] + dbits[1] + dcb);
+      cfl_total = (float)(csse[0] + csse[1]) + mlam * (cbits[0] + cbits[1] + sig);
+    } else {  // block32.rs:2399-2404: the planes' costs summed, then the mode bits
+      dc_total = ((float)dsse[0] + mlam * dbits[0]) + ((float)dsse[1] + mlam * dbits[1]) + mlam * dcb;
+      cfl_total = ((float)csse[0] + mlam * cbits[0]) + ((float)csse[1] + mlam * cbits[1]) + mlam * sig;
+    }
+    const bool use_cfl = cfl_total < dc_total && (alpha[0] != 0 || alpha[1] != 0);
+    // the winner so far: prediction, levels, inverse
+    std::vector<int32_t> bpred(use_cfl ? cpred : dpred, (use_cfl ? cpred : dpred) + 2 * NN);
+    std::vector<int32_t> bcf(use_cfl ? ccf : dcf, (use_cfl ? ccf : dcf) + 2 * NN);
+    std::vector<int32_t> brr(use_cfl ? crr : drr, (use_cfl ? crr : drr) + 2 * NN);
+    // 3. the directional stage on dir_lambda
+    float best_total = dlam * (use_cfl ? sig : dcb);
+    for (int pl = 0; pl < 2; pl++)
+      best_total += (float)(use_cfl ? csse[pl] : dsse[pl]) + dlam * (use_cfl ? cbits[pl] : dbits[pl]);
+    int mode = MT_DC_PRED, delta = 0;
+    // rank_chroma_modes + DirectionalTopK (K = 3)
+    uint64_t tc[3];
+    int tm[3], tn = 0;
+    std::vector<int32_t> ppv(NN);
+    int32_t* pp = ppv.data();
+    for (int m : kList) {
+      uint64_t cost = 0;
+      for (int pl = 0; pl < 2; pl++) {
+        or_intra_predict(P[pl].rec, p->stride, cx, cy, N, N, m, 0, tr, bl, p->frame_w, p->frame_h, ft, p->bd, pp);
+        const int vw = std::min(std::max(vis_w - cx, 0), N), vh = std::min(std::max(vis_h - cy, 0), N);
+        cost += satd_sad_proxy_n(P[pl].src + (size_t)cy * p->stride + cx, p->stride, pp, N, vw, vh);
+      }
+      int pos = tn < 3 ? tn : 2;
+      if (tn == 3 && cost >= tc[pos]) continue;
+      if (tn < 3) pos = tn++;
+      while (pos > 0 && cost < tc[pos - 1]) {
+        tc[pos] = tc[pos - 1];
+        tm[pos] = tm[pos - 1];
+        pos--;
+      }
+      tc[pos] = cost;
+      tm[pos] = m;
+    }
+    std::vector<int32_t> nbuf(6 * NN);
+    int32_t* npred = nbuf.data();
+    int32_t* ncf = npred + 2 * NN;
+    int32_t* nrr = ncf + 2 * NN;
+    auto price = [&](int m, int d, bool etr, bool ebl, float rate_bits) {
+      const int tx = N == 32 ? MT_TX_DCT_DCT : chroma_tx(m);  // forced DCT_DCT at TX_32X32
+      float total = dlam * rate_bits;
+      for (int pl = 0; pl < 2; pl++) {
+        or_intra_predict(P[pl].rec, p->stride, cx, cy, N, N, m, d, etr, ebl, p->frame_w, p->frame_h, ft, p->bd,
+                         npred + pl * NN);
+        int64_t sse;
+        float bits;
+        plane_cost_n(N, p, q, qm, cd, P[pl], cx, cy, tx, true, npred + pl * NN, ncf + pl * NN, nrr + pl * NN, &sse,
+                     &bits);
+        total += (float)sse + dlam * bits;
+      }
+      return total;
+    };
+    auto take = [&]() {
+      std::copy(npred, npred + 2 * NN, bpred.begin());
+      std::copy(ncf, ncf + 2 * NN, bcf.begin());
+      std::copy(nrr, nrr + 2 * NN, brr.begin());
+    };
+    for (int m : kList) {
+      bool in = false;
+      for (int e = 0; e < tn; e++) in |= tm[e] == m;
+      if (!in) continue;
+      const float total = price(m, 0, tr, bl, or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0));
+      if (total < best_total) {
+        best_total = total;
+        mode = m;
+        take();
+      }
+    }
+    // uv_ad: the zone-2 deltas of a directional winner (block16.rs:743-778, :2342-2349)
+    if (u->angle_deltas && directional(mode)) {
+      const int m = mode;
+      std::vector<int> ds;
+      if (m == MT_V_PRED) ds = {1, 2, 3};
+      else if (m == MT_H_PRED) ds = {-3, -2, -1};
+      else if (m == MT_D113_PRED || m == MT_D135_PRED || m == MT_D157_PRED) ds = {-3, -2, -1, 1, 2, 3};
+      const float base_sig = or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0) - or_cdf_cost(mc->angle_delta[m - MT_V_PRED], 3);
+      for (int d : ds) {
+        const float total = price(m, d, false, false, base_sig + or_cdf_cost(mc->angle_delta[m - MT_V_PRED], d + 3));
+        if (total < best_total) {
+          best_total = total;
+          delta = d;
+          take();
+        }
+      }
+    }
+    r.total = best_total;
+    r.dc_total = dc_total;
+    r.cfl_total = cfl_total;
+    r.uv_mode = (uint8_t)(mode != MT_DC_PRED ? mode : (use_cfl ? MT_UV_CFL_PRED : MT_DC_PRED));
+    r.angle_delta = (int8_t)delta;
+    r.cfl_alpha[0] = alpha[0];
+    r.cfl_alpha[1] = alpha[1];
+    for (int i = 0; i < 2 * NN; i++) {
+      if (cf_out) cf_out[(size_t)j * 2 * NN + i] = bcf[(size_t)i];
+      if (rec_out) {
+        const int32_t v = bpred[(size_t)i] + brr[(size_t)i];
+        rec_out[(size_t)j * 2 * NN + i] = (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
+      }
+    }
+  }
+  return MT_OK;
 }
 
 }  // namespace
@@ -304,185 +503,6 @@ int or_pick_uv16_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
   return MT_OK;
 }
 
-int or_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
-                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
-                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
-                     const mt_uv16_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
-                     uint16_t* rec_out) {
-  if (!p || p->bd != 8) return MT_ERR_UNSUPPORTED;
-  const int32_t maxv = (1 << p->bd) - 1;
-  const float mlam = p->rd_lambda, dlam = u->dir_lambda;
-  const int vis_w = p->vis_w > 0 ? p->vis_w : p->frame_w, vis_h = p->vis_h > 0 ? p->vis_h : p->frame_h;
-  static const int kList[12] = {MT_SMOOTH_V_PRED, MT_PAETH_PRED, MT_SMOOTH_PRED, MT_SMOOTH_H_PRED,
-                                MT_V_PRED,        MT_H_PRED,     MT_D135_PRED,   MT_D113_PRED,
-                                MT_D157_PRED,     MT_D45_PRED,   MT_D67_PRED,    MT_D203_PRED};
-  std::vector<int32_t> bufs(12 * 256);
-  for (int j = 0; j < n; j++) {
-    const mt_uv16_444_job& jb = jobs[j];
-    mt_uv16_result& r = results[j];
-    const int cx = jb.px, cy = jb.py;
-    if ((cx & 15) || (cy & 15) || cx + 16 > p->frame_w || cy + 16 > p->frame_h || jb.y_mode > MT_PAETH_PRED) {
-      r.total = r.dc_total = r.cfl_total = INFINITY;
-      r.uv_mode = 255;
-      r.angle_delta = 0;
-      r.cfl_alpha[0] = r.cfl_alpha[1] = 0;
-      if (cf_out) memset(cf_out + (size_t)j * 512, 0, 512 * sizeof(int32_t));
-      if (rec_out) memset(rec_out + (size_t)j * 512, 0, 512 * sizeof(uint16_t));
-      continue;
-    }
-    const bool tr = jb.flags & MT_CAND_HAVE_TR, bl = jb.flags & MT_CAND_HAVE_BL, ft = jb.flags & MT_CAND_FILTER_TYPE;
-    Plane P[2];
-    for (int pl = 0; pl < 2; pl++) {
-      P[pl].src = pl ? src_v : src_u;
-      P[pl].rec = pl ? rec_v : rec_u;
-      // skip_ctx_16 / dc_sign_ctx_16 (lossy_state.rs:1420-1440)
-      bool anz = false, lnz = false;
-      int s = -8;
-      for (int k = 0; k < 4; k++) {
-        anz |= jb.a_coef[pl][k] != 0x40;
-        lnz |= jb.l_coef[pl][k] != 0x40;
-        s += (jb.a_coef[pl][k] >> 6) + (jb.l_coef[pl][k] >> 6);
-      }
-      P[pl].sk = 7 + anz + lnz;
-      P[pl].ds = (s != 0) + (s > 0);
-    }
-    int32_t* dpred = &bufs[0];  // [2][256]
-    int32_t* dcf = &bufs[512];
-    int32_t* drr = &bufs[1024];
-    int32_t* cpred = &bufs[1536];
-    int32_t* ccf = &bufs[2048];
-    int32_t* crr = &bufs[2560];
-    // 1. DC
-    int32_t dc[2];
-    int64_t dsse[2], csse[2];
-    float dbits[2], cbits[2];
-    for (int pl = 0; pl < 2; pl++) {
-      dc[pl] = or_dc_pred(P[pl].rec, p->stride, cx, cy, 16, 16, p->bd);
-      for (int i = 0; i < 256; i++) dpred[pl * 256 + i] = dc[pl];
-      plane_cost16(p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, true, dpred + pl * 256, dcf + pl * 256,
-                   drr + pl * 256, &dsse[pl], &dbits[pl]);
-    }
-    // 2. CfL: cfl_ac_444 and cfl_best_alpha (or_cfl_alpha without subsampling)
-    mt_cfl_block cb = {};
-    cb.cx = (uint16_t)cx;
-    cb.cy = (uint16_t)cy;
-    cb.dc[0] = (int16_t)dc[0];
-    cb.dc[1] = (int16_t)dc[1];
-    int8_t alpha[2];
-    std::vector<int32_t> ac(256);
-    or_cfl_alpha(luma, u->luma_stride, src_u, src_v, p->stride, 0, 0, 16, 16, vis_w, vis_h, p->bd, &cb, 1, alpha,
-                 ac.data());
-    for (int pl = 0; pl < 2; pl++) {
-      for (int i = 0; i < 256; i++) {
-        const int32_t diff = alpha[pl] * ac[i];
-        const int32_t mag = ((diff < 0 ? -diff : diff) + 32) >> 6;
-        const int32_t v = dc[pl] + (diff < 0 ? -mag : mag);
-        cpred[pl * 256 + i] = v < 0 ? 0 : (v > maxv ? maxv : v);
-      }
-      plane_cost16(p, q, qm, cd, P[pl], cx, cy, MT_TX_DCT_DCT, false, cpred + pl * 256, ccf + pl * 256,
-                   crr + pl * 256, &csse[pl], &cbits[pl]);
-    }
-    const float sig = or_uv_mode_bits(mc, jb.y_mode, MT_UV_CFL_PRED, 1, alpha[0], alpha[1]);
-    const float dcb = or_uv_mode_bits(mc, jb.y_mode, MT_DC_PRED, 0, 0, 0);
-    const float dc_total = (float)(dsse[0] + dsse[1]) + mlam * (dbits[0] + dbits[1] + dcb);
-    const float cfl_total = (float)(csse[0] + csse[1]) + mlam * (cbits[0] + cbits[1] + sig);
-    const bool use_cfl = cfl_total < dc_total && (alpha[0] != 0 || alpha[1] != 0);
-    // the winner so far: prediction, levels, inverse
-    std::vector<int32_t> bpred(use_cfl ? cpred : dpred, (use_cfl ? cpred : dpred) + 512);
-    std::vector<int32_t> bcf(use_cfl ? ccf : dcf, (use_cfl ? ccf : dcf) + 512);
-    std::vector<int32_t> brr(use_cfl ? crr : drr, (use_cfl ? crr : drr) + 512);
-    // 3. the directional stage on dir_lambda
-    float best_total = dlam * (use_cfl ? sig : dcb);
-    for (int pl = 0; pl < 2; pl++)
-      best_total += (float)(use_cfl ? csse[pl] : dsse[pl]) + dlam * (use_cfl ? cbits[pl] : dbits[pl]);
-    int mode = MT_DC_PRED, delta = 0;
-    // rank_chroma_modes + DirectionalTopK (K = 3)
-    uint64_t tc[3];
-    int tm[3], tn = 0;
-    int32_t pp[256];
-    for (int m : kList) {
-      uint64_t cost = 0;
-      for (int pl = 0; pl < 2; pl++) {
-        or_intra_predict(P[pl].rec, p->stride, cx, cy, 16, 16, m, 0, tr, bl, p->frame_w, p->frame_h, ft, p->bd, pp);
-        const int vw = std::min(std::max(vis_w - cx, 0), 16), vh = std::min(std::max(vis_h - cy, 0), 16);
-        cost += satd_sad_proxy_n(P[pl].src + (size_t)cy * p->stride + cx, p->stride, pp, 16, vw, vh);
-      }
-      int pos = tn < 3 ? tn : 2;
-      if (tn == 3 && cost >= tc[pos]) continue;
-      if (tn < 3) pos = tn++;
-      while (pos > 0 && cost < tc[pos - 1]) {
-        tc[pos] = tc[pos - 1];
-        tm[pos] = tm[pos - 1];
-        pos--;
-      }
-      tc[pos] = cost;
-      tm[pos] = m;
-    }
-    int32_t npred[512], ncf[512], nrr[512];
-    auto price = [&](int m, int d, bool etr, bool ebl, float rate_bits) {
-      const int tx = chroma_tx(m);
-      float total = dlam * rate_bits;
-      for (int pl = 0; pl < 2; pl++) {
-        or_intra_predict(P[pl].rec, p->stride, cx, cy, 16, 16, m, d, etr, ebl, p->frame_w, p->frame_h, ft, p->bd,
-                         npred + pl * 256);
-        int64_t sse;
-        float bits;
-        plane_cost16(p, q, qm, cd, P[pl], cx, cy, tx, true, npred + pl * 256, ncf + pl * 256, nrr + pl * 256, &sse,
-                     &bits);
-        total += (float)sse + dlam * bits;
-      }
-      return total;
-    };
-    auto take = [&]() {
-      std::copy(npred, npred + 512, bpred.begin());
-      std::copy(ncf, ncf + 512, bcf.begin());
-      std::copy(nrr, nrr + 512, brr.begin());
-    };
-    for (int m : kList) {
-      bool in = false;
-      for (int e = 0; e < tn; e++) in |= tm[e] == m;
-      if (!in) continue;
-      const float total = price(m, 0, tr, bl, or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0));
-      if (total < best_total) {
-        best_total = total;
-        mode = m;
-        take();
-      }
-    }
-    // uv_ad: the zone-2 deltas of a directional winner (block16.rs:743-778, :2342-2349)
-    if (u->angle_deltas && directional(mode)) {
-      const int m = mode;
-      std::vector<int> ds;
-      if (m == MT_V_PRED) ds = {1, 2, 3};
-      else if (m == MT_H_PRED) ds = {-3, -2, -1};
-      else if (m == MT_D113_PRED || m == MT_D135_PRED || m == MT_D157_PRED) ds = {-3, -2, -1, 1, 2, 3};
-      const float base_sig = or_uv_mode_bits(mc, jb.y_mode, m, 0, 0, 0) - or_cdf_cost(mc->angle_delta[m - MT_V_PRED], 3);
-      for (int d : ds) {
-        const float total = price(m, d, false, false, base_sig + or_cdf_cost(mc->angle_delta[m - MT_V_PRED], d + 3));
-        if (total < best_total) {
-          best_total = total;
-          delta = d;
-          take();
-        }
-      }
-    }
-    r.total = best_total;
-    r.dc_total = dc_total;
-    r.cfl_total = cfl_total;
-    r.uv_mode = (uint8_t)(mode != MT_DC_PRED ? mode : (use_cfl ? MT_UV_CFL_PRED : MT_DC_PRED));
-    r.angle_delta = (int8_t)delta;
-    r.cfl_alpha[0] = alpha[0];
-    r.cfl_alpha[1] = alpha[1];
-    for (int i = 0; i < 512; i++) {
-      if (cf_out) cf_out[(size_t)j * 512 + i] = bcf[(size_t)i];
-      if (rec_out) {
-        const int32_t v = bpred[(size_t)i] + brr[(size_t)i];
-        rec_out[(size_t)j * 512 + i] = (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
-      }
-    }
-  }
-  return MT_OK;
-}
 
 int or_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
                      const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
@@ -657,6 +677,23 @@ int or_pick_uv32_420(const uint16_t* src_u, const uint16_t* src_v, const uint16_
     }
   }
   return MT_OK;
+}
+
+int or_pick_uv16_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
+                     const mt_uv16_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
+                     uint16_t* rec_out) {
+  return pick444<16>(src_u, src_v, rec_u, rec_v, luma, p, u, q, qm, cd, mc, jobs, n, results, cf_out, rec_out);
+}
+
+// block32.rs pick_uv32_444 (:2264-2720).
+int or_pick_uv32_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_t* rec_u, const uint16_t* rec_v,
+                     const uint16_t* luma, const mt_split16_params* p, const mt_uv16_params* u, const mt_quant* q,
+                     const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
+                     const mt_uv32_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
+                     uint16_t* rec_out) {
+  return pick444<32>(src_u, src_v, rec_u, rec_v, luma, p, u, q, qm, cd, mc, jobs, n, results, cf_out, rec_out);
 }
 
 }  // extern "C"

@@ -93,6 +93,9 @@ def load():
             "or_pick_uv16_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
                                            C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
                                            C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
+            "or_pick_uv32_444": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
+                                           C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
+                                           C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_pick_uv32_420": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(abi.Split16Params), C.POINTER(abi.Uv16Params),
                                            C.POINTER(abi.Quant), _P, C.POINTER(abi.CoefCdfs),
                                            C.POINTER(abi.UvModeCdfs), _P, C.c_int32, _P, _P, _P]),
@@ -1081,5 +1084,12 @@ def pick_uv32_420(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_
                   want_cf=False, want_rec=False):
     """pick_uv32_420 of n 32x32 leaves: (results, levels or None, reconstruction or None)."""
     return _pick_uv16("or_pick_uv32_420", abi.UV16_444_JOB_DTYPE, 512, src_u, src_v, rec_u, rec_v, luma, prm, uvp, q,
+                      qm, cdfs, mode_cdfs, jobs, threads, want_cf, want_rec)
+
+
+def pick_uv32_444(src_u, src_v, rec_u, rec_v, luma, prm, uvp, q, qm, cdfs, mode_cdfs, jobs, threads=1,
+                  want_cf=False, want_rec=False):
+    """pick_uv32_444 of n 32x32 leaves: (results, levels or None, reconstruction or None)."""
+    return _pick_uv16("or_pick_uv32_444", abi.UV32_444_JOB_DTYPE, 2048, src_u, src_v, rec_u, rec_v, luma, prm, uvp, q,
                       qm, cdfs, mode_cdfs, jobs, threads, want_cf, want_rec)
 

@@ -547,3 +547,143 @@ def test_uv32_at_config(mt_lib, oracle_lib, cuda, name):
     want = oracle_lib.pick_uv32_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd,
                                     oracle_lib.uv_mode_cdfs(), jobs, threads=configs.THREADS)
     assert got[0].tobytes() == want[0].tobytes()
+
+
+# ---- the 32x32 leaf at 4:4:4 (pick_uv32_444) ----
+
+def _case32_444(mt, op, w, h, seed, qidx, qm_level, wsse, skip=False, ad=True):
+    src, rec = synth.planes444(synth.generate_rgb(w, h, seed, sigma=4.0, variant="1080p"), seed)
+    q = op.quant_new_chroma(qidx, 0, 0, 8, qm_level)
+    qm = op.qm_row(qm_level, 1, 32) if qm_level < 15 else None
+    sb = [(float(np.float32(1.5 + 0.1 * k)), float(np.float32(0.2 + 0.05 * k))) for k in range(13)] if skip else None
+    prm = mt.split16_params(w, h, trellis_lambda0=0.05, rd_lambda=0.2 * qidx + 3, wsse_scale=wsse,
+                            vis=(w - 5, h - 2), skip_bits=sb)
+    uvp = mt.uv16_params(w, angle_deltas=ad, dir_lambda=0.15 * qidx + 2)
+    return src, rec, q, qm, prm, uvp
+
+
+@pytest.mark.parametrize("qidx,qm_level,wsse", [(90, 6, 1.0), (40, 15, 0.0)])
+def test_uv32_444_oracle_accounting(oracle_lib, qidx, qm_level, wsse):
+    """The oracle's DC and CfL totals (the planes' costs summed, then the mode
+    bits), its winner's total and levels recomputed from primitives: the plain
+    trellis over the 1024-entry scan, DCT_DCT for every mode, contexts over
+    eight bytes per side."""
+    import maroontree_b200 as mt
+
+    op = oracle_lib
+    src, rec, q, qm, prm, uvp = _case32_444(mt, op, 128, 96, qidx + 4, qidx, qm_level, wsse)
+    cd = op.default_cdfs(op.qcat(qidx), 32, plane=1)
+    mc = op.uv_mode_cdfs()
+    jobs = synth.uv32_444_jobs(128, 96, qidx)
+    res, cfo, _ = op.pick_uv32_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd, mc, jobs, want_cf=True)
+    f32 = np.float32
+    mlam, dlam = f32(prm.rd_lambda), f32(uvp.dir_lambda)
+    scan = op.default_scan(32)
+    adc = np.ctypeslib.as_array(mc.angle_delta)
+    for i, jb in enumerate(jobs):
+        cx, cy, fl, ym = int(jb["px"]), int(jb["py"]), int(jb["flags"]), int(jb["y_mode"])
+        ctx = []
+        for pl in range(2):
+            a, l = [int(v) for v in jb["a_coef"][pl]], [int(v) for v in jb["l_coef"][pl]]
+            s = sum(v >> 6 for v in a + l) - 16
+            ctx.append((7 + int(any(v != 0x40 for v in a)) + int(any(v != 0x40 for v in l)),
+                        int(s != 0) + int(s > 0)))
+
+        def plane(pl, pred, keep_dc):
+            resid = src[1 + pl][cy:cy + 32, cx:cx + 32].astype(np.int32).ravel() - pred.ravel()
+            lv, tf = op.fwd_txfm_quant(resid, abi.TX_DCT_DCT, q, qm)
+            lv = op.trellis_optimize(lv, tf, float(q.dc_q), float(q.ac_q), scan, prm.trellis_lambda0)
+            if keep_dc:
+                mean = int(np.trunc(resid.sum() / 1024))
+                if lv[0] == 0 and abs(mean) >= 8:
+                    lv[0] = 1 if mean > 0 else -1
+            rr = op.inv_txfm_dequant(lv, abi.TX_DCT_DCT, q, qm)
+            sse = int(op.sse_recon(src[1 + pl], prm.vis_w, prm.vis_h, [(cx, cy)], pred.ravel(), rr, 32, 32,
+                                   scale=prm.wsse_scale)[0])
+            return sse, f32(op.real_block_bits_bounded(lv, scan, 32, 32, cd, ctx[pl][0], ctx[pl][1], -1, 0, INF)), lv
+
+        dc = [int(op.intra_predict(rec[1 + pl], cx, cy, 32, 32, abi.DC_PRED)[0, 0]) for pl in range(2)]
+        dcp = [plane(pl, np.full((32, 32), dc[pl]), True) for pl in range(2)]
+        blk = np.array([(cx, cy, (dc[0], dc[1]))], abi.CFL_BLOCK_DTYPE)
+        alpha, ac = op.cfl_alpha(rec[0], src[1], src[2], 0, 0, 32, 32, blk, vis=(prm.vis_w, prm.vis_h))
+        al = (int(alpha[0][0]), int(alpha[0][1]))
+        cfp = []
+        for pl in range(2):
+            diff = al[pl] * ac[0]
+            mag = (np.abs(diff) + 32) >> 6
+            cfp.append(plane(pl, np.clip(dc[pl] + np.where(diff < 0, -mag, mag), 0, 255), False))
+        cost = lambda c: f32(f32(c[0]) + f32(mlam * c[1]))
+        dct = f32(f32(f32(cost(dcp[0]) + cost(dcp[1])) + f32(mlam * f32(op.uv_mode_bits(mc, ym, abi.DC_PRED)))))
+        cflt = f32(f32(f32(cost(cfp[0]) + cost(cfp[1])) + f32(mlam * f32(op.uv_mode_bits(mc, ym, abi.UV_CFL_PRED, al)))))
+        r = res[i]
+        assert (f32(r["dc_total"]), f32(r["cfl_total"])) == (dct, cflt), i
+        m, d = int(r["uv_mode"]), int(r["angle_delta"])
+        if m in (abi.DC_PRED, abi.UV_CFL_PRED):
+            cur = cfp if m == abi.UV_CFL_PRED else dcp
+            bits = f32(op.uv_mode_bits(mc, ym, abi.UV_CFL_PRED, al) if m == abi.UV_CFL_PRED else
+                       op.uv_mode_bits(mc, ym, abi.DC_PRED))
+            want = f32(dlam * bits)
+            for pl in range(2):
+                want = f32(want + f32(f32(cur[pl][0]) + f32(dlam * cur[pl][1])))
+            levels = [cur[0][2], cur[1][2]]
+        else:
+            bits = f32(op.uv_mode_bits(mc, ym, m))
+            if d != 0:
+                bits = f32(f32(bits - f32(op.cdf_cost(adc[m - abi.V_PRED], 3))) +
+                           f32(op.cdf_cost(adc[m - abi.V_PRED], d + 3)))
+            want = f32(dlam * bits)
+            tr, bl = (bool(fl & 1), bool(fl & 2)) if d == 0 else (False, False)
+            levels = []
+            for pl in range(2):
+                pp = op.intra_predict(rec[1 + pl], cx, cy, 32, 32, m, d, tr, bl, bool(fl & 4), fw=128, fh=96)
+                sse, b, lv = plane(pl, pp, True)
+                want = f32(want + f32(f32(sse) + f32(dlam * b)))
+                levels.append(lv)
+        assert f32(r["total"]) == want, (i, m, d)
+        assert np.array_equal(cfo[i], np.concatenate(levels)), i
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qidx,qm_level,wsse,skip,ad", [(70, 6, 1.0, False, True), (116, 15, 0.0, True, True),
+                                                         (30, 3, 0.75, False, False)])
+def test_uv32_444_gpu_matches_oracle(mt_lib, oracle_lib, cuda, qidx, qm_level, wsse, skip, ad):
+    src, rec, q, qm, prm, uvp = _case32_444(mt_lib, oracle_lib, 320, 192, qidx + 11, qidx, qm_level, wsse,
+                                            skip=skip, ad=ad)
+    jobs = synth.uv32_444_jobs(320, 192, qidx)
+    jobs = np.concatenate([jobs, jobs[:2]])
+    jobs["px"][-2] = 304  # leaves the plane: rejected
+    jobs["y_mode"][-1] = 13
+    cd = oracle_lib.default_cdfs(oracle_lib.qcat(qidx), 32, plane=1)
+    costs = mt_lib.coef_costs(mt_lib.coef_cdfs_default(oracle_lib.qcat(qidx), 32, 32, 1))
+    mcost = mt_lib.uv_mode_costs(mt_lib.uv_mode_cdfs_default())
+    got = mt_lib.pick_uv32_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, costs, mcost, jobs,
+                               want_cf=True, want_rec=True)
+    want = oracle_lib.pick_uv32_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd,
+                                    oracle_lib.uv_mode_cdfs(), jobs, threads=os.cpu_count() or 1, want_cf=True,
+                                    want_rec=True)
+    assert got[0].tobytes() == want[0].tobytes()
+    assert np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2])
+    assert (got[0]["uv_mode"][-2:] == 255).all()
+
+
+@pytest.mark.gpu
+def test_uv32_444_at_config(mt_lib, oracle_lib, cuda):
+    """Every 32x32 leaf of C1 (512x512 4:4:4, qindex 70) with its chroma
+    quantiser, QM and lambdas and the chroma TX_32X32 CDFs of its q context."""
+    import configs
+
+    wl = configs.workload("C1")
+    src, rec = synth.planes444(wl.rgb, wl.qidx)
+    q = mt_lib.quant_new_chroma(wl.qidx, 0, 0, 8, wl.qm_uv)
+    qm = mt_lib.qm_row(wl.qm_uv, 1, 32) if wl.qm_uv < 15 else None
+    prm = mt_lib.split16_params(wl.w, wl.h, trellis_lambda0=wl.lam.trellis_lambda0, rd_lambda=wl.lam.mode_lambda,
+                                wsse_scale=1.0)
+    uvp = mt_lib.uv16_params(wl.w, angle_deltas=True, dir_lambda=wl.lam.lambda_d)
+    jobs = synth.uv32_444_jobs(wl.w, wl.h, wl.qidx)
+    cd = oracle_lib.default_cdfs(wl.qctx, 32, plane=1)
+    got = mt_lib.pick_uv32_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm,
+                               mt_lib.coef_costs(mt_lib.coef_cdfs_default(wl.qctx, 32, 32, 1)),
+                               mt_lib.uv_mode_costs(mt_lib.uv_mode_cdfs_default()), jobs)
+    want = oracle_lib.pick_uv32_444(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, cd,
+                                    oracle_lib.uv_mode_cdfs(), jobs, threads=configs.THREADS)
+    assert got[0].tobytes() == want[0].tobytes()
