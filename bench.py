@@ -599,7 +599,7 @@ def measure_leaf64(dev, wl, grid, reps=5, cpu=True):
     return out
 
 
-def measure_uv16(dev, wl, reps=5, cpu=True):
+def measure_uv16(dev, wl, reps=5, cpu=True, form="420"):
     """The 16x16 leaf's 4:2:0 chroma search (pick_uv16_420) over every 16x16
     leaf of the 1080p frame (8,040 leaves: DC, CfL, 60 shortlist predictions
     per plane, the 4 best priced in full) with the frame's chroma quantiser
@@ -612,20 +612,35 @@ def measure_uv16(dev, wl, reps=5, cpu=True):
     import maroontree_b200 as mt
     from maroontree_b200 import abi, synth
 
+    # form: "420" pick_uv16_420, "444" pick_uv16_444, "420_32" pick_uv32_420, "444_32" pick_uv32_444
     qidx = wl["qidx"]
-    qm_uv = mt.qm_levels(qidx, SUB)[1]
+    sub = 0 if form.startswith("444") else SUB
+    tx = 32 if form.endswith("_32") else (16 if form == "444" else 8)
+    qm_uv = mt.qm_levels(qidx, sub)[1]
     q = mt.quant_new_chroma(qidx, 0, 0, 8, qm_uv)
-    qm = mt.qm_row(qm_uv, 1, 8) if qm_uv < 15 else None
-    cdfs = mt.coef_cdfs_default(mt.qcat(qidx), 8, 8, 1)
+    qm = mt.qm_row(qm_uv, 1, tx) if qm_uv < 15 else None
+    cdfs = mt.coef_cdfs_default(mt.qcat(qidx), tx, tx, 1)
     costs = mt.coef_costs(cdfs)
     mcdfs = mt.uv_mode_cdfs_default()
     mcost = mt.uv_mode_costs(mcdfs)
-    src, rec = synth.planes420(wl["rgb"], SEED)
+    if sub:
+        src, rec = synth.planes420(wl["rgb"], SEED)
+    else:
+        src, rec = synth.planes444(wl["rgb"], SEED)
     cw, ch = src[1].shape[1], src[1].shape[0]
     prm = mt.split16_params(cw, ch, trellis_lambda0=wl["lam"].trellis_lambda0, rd_lambda=wl["lam"].mode_lambda,
-                            wsse_scale=1.0, vis=(W // 2, H // 2))
-    uvp = mt.uv16_params(src[0].shape[1], joint_k=4, angle_deltas=True)
-    jobs = synth.uv16_jobs(W, H, SEED)
+                            wsse_scale=1.0, vis=(W >> (1 if sub else 0), H >> (1 if sub else 0)))
+    uvp = mt.uv16_params(src[0].shape[1], joint_k=4, angle_deltas=True, dir_lambda=wl["lam"].lambda_d)
+    entry, po_entry, jobs, what = {
+        "420": ("mt_pick_uv16_420_device", "pick_uv16_420", synth.uv16_jobs(W, H, SEED),
+                "pick_uv16_420 1920x1080 4:2:0, 8,040 16x16 leaves (DC, CfL, 60-entry SATD shortlist, 4 priced)"),
+        "444": ("mt_pick_uv16_444_device", "pick_uv16_444", synth.uv16_444_jobs(W, H, SEED),
+                "pick_uv16_444 1920x1080 4:4:4, 8,040 16x16 leaves (DC, CfL, SATD top-3, zone-2 deltas)"),
+        "420_32": ("mt_pick_uv32_420_device", "pick_uv32_420", synth.uv16_444_jobs(W, H, SEED, leaf=32),
+                   "pick_uv32_420 1920x1080 4:2:0, 1,980 32x32 leaves (16x16 chroma: DC, CfL, SATD top-3, deltas)"),
+        "444_32": ("mt_pick_uv32_444_device", "pick_uv32_444", synth.uv32_444_jobs(W, H, SEED),
+                   "pick_uv32_444 1920x1080 4:4:4, 1,980 32x32 leaves (32x32 chroma: DC, CfL, SATD top-3, deltas)"),
+    }[form]
     n = len(jobs)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).to(dev)
     d_p = [t(a) for a in (src[1], src[2], rec[1], rec[2], rec[0])]
@@ -636,7 +651,7 @@ def measure_uv16(dev, wl, reps=5, cpu=True):
     lib = mt.load()
 
     def launch():
-        rc = lib.mt_pick_uv16_420_device(*[a.data_ptr() for a in d_p], C.byref(prm), C.byref(uvp), C.byref(q),
+        rc = getattr(lib, entry)(*[a.data_ptr() for a in d_p], C.byref(prm), C.byref(uvp), C.byref(q),
                                          None if d_qm is None else d_qm.data_ptr(), d_costs.data_ptr(),
                                          d_mc.data_ptr(), d_jobs.data_ptr(), n, d_res.data_ptr(), None, None, None)
         assert rc == 0, rc
@@ -656,15 +671,14 @@ def measure_uv16(dev, wl, reps=5, cpu=True):
         ms.append(a.elapsed_time(b))
     step = float(np.median(ms))
     out = {"ms": round(step, 4), "mpix_s": round(MPIX / (step / 1e3), 2), "jobs": n,
-           "workload": "pick_uv16_420 1920x1080 4:2:0, 8,040 16x16 leaves (DC, CfL, 60-entry SATD shortlist, 4 "
-                       "priced), frame chroma quantiser and QM"}
+           "workload": what + ", frame chroma quantiser and QM"}
     if cpu:
         from oracle import pyoracle as po
 
         threads = os.cpu_count() or 1
         t0 = time.perf_counter()
-        po.pick_uv16_420(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm, po.default_cdfs(mt.qcat(qidx), 8,
-                         plane=1), po.uv_mode_cdfs(), jobs, threads=threads)
+        getattr(po, po_entry)(src[1], src[2], rec[1], rec[2], rec[0], prm, uvp, q, qm,
+                              po.default_cdfs(mt.qcat(qidx), tx, plane=1), po.uv_mode_cdfs(), jobs, threads=threads)
         dt = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": round(MPIX / dt, 4), "unit": "MPix/s", "cores": threads, "kind": "port",
                                "sample": f"all {n} leaves ({dt:.2f} s)"}
@@ -1145,6 +1159,7 @@ def run_ours(args):
         leaf8["quad32_64"] = measure_leaf64(dev, wl, False, cpu=not nocpu)
         leaf8["grid16_64"] = measure_leaf64(dev, wl, True, cpu=not nocpu)
         secondary["uv16_420"] = measure_uv16(dev, wl, cpu=not nocpu)
+        secondary["uv_search"] = {f: measure_uv16(dev, wl, cpu=not nocpu, form=f) for f in ("444", "420_32", "444_32")}
         secondary["leaf8"] = leaf8
     if rank == 0 and not nocpu:
         from oracle import build as obuild
@@ -1201,6 +1216,9 @@ ONLY = {
     "grid16": "the 64x64 leaf's sixteen-TX_16X16 leg, 480 blocks (grid16_kernel)",
     "leaf32": "the 32x32 leaf's mode-loop candidates, 1,980 blocks x 13 modes (leaf_kernel<32>)",
     "c3_filters": "the 4096x4096 4:4:4 frame filters: deblocking and CDEF (lf_fused_kernel, the CDEF search)",
+    "uv444": "pick_uv16_444 over the 8,040 16x16 leaves of the 1080p frame at 4:4:4 (uv444_kernel<16>)",
+    "uv32_420": "pick_uv32_420 over the 1,980 32x32 leaves of the 1080p frame (uv32_420_kernel)",
+    "uv32_444": "pick_uv32_444 over the 1,980 32x32 leaves of the 1080p frame at 4:4:4 (uv444_kernel<32>)",
 }
 
 
@@ -1220,6 +1238,9 @@ def run_only(args):
     else:
         wl = make_workload()
         run = {"uv16": lambda: measure_uv16(dev, wl, reps=1, cpu=False),
+               "uv444": lambda: measure_uv16(dev, wl, reps=1, cpu=False, form="444"),
+               "uv32_420": lambda: measure_uv16(dev, wl, reps=1, cpu=False, form="420_32"),
+               "uv32_444": lambda: measure_uv16(dev, wl, reps=1, cpu=False, form="444_32"),
                "quad32": lambda: measure_leaf64(dev, wl, False, reps=1, cpu=False),
                "grid16": lambda: measure_leaf64(dev, wl, True, reps=1, cpu=False),
                "leaf32": lambda: measure_leaf8(dev, wl, False, reps=1, cpu=False, n32=True)}[args.only]
