@@ -1031,6 +1031,41 @@ int mt_luma_palette(const uint16_t* src, int32_t stride, int32_t frame_w, int32_
                     int32_t h, const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_palette_cand* cands,
                     uint8_t* maps);
 
+/* ---- UV palette candidates (4:4:4 screen content: the palette leg of
+ * pick_uv16_444 / pick_uv32_444, src/coder/block16.rs:813-860) ----
+ * Per w x h chroma block (w, h in 4..32): exact_uv_palette
+ * (src/coder/palette.rs:199-262) when the block holds 2..8 distinct (U, V)
+ * pairs -- slot 0, exact = 1, the pairs in lexicographic order and the map
+ * of each sample's pair; otherwise lossy_uv_palette_from_hist (:315-431) over
+ * uv_pair_histogram (:264-309, the block's pairs sorted and counted) in
+ * slots 0..3 for (8 colours, k-means), (4, k-means), (8, dominant pairs),
+ * (4, dominant pairs): all pairs when the histogram holds exactly that many,
+ * the most frequent pairs (count descending, pair ascending), or eight Lloyd
+ * passes from weighted-quantile starts with integer rounded means, a slot
+ * left empty when the centres collapse or the histogram is too small.  The
+ * centres are sorted; the index map is viterbi_uv_palette_map (:1053-1076:
+ * the row Viterbi on the squared (U, V) distance with opts->color_costs, the
+ * palette_uv_color bits, and opts->viterbi_lambda) when viterbi_lambda > 0,
+ * else uv_nearest_indices (src/kmeans.rs:37-68). */
+#define MT_UV_PALETTE_SLOTS 4
+typedef struct mt_uv_palette_cand {
+  uint8_t n_colors;   /* 0: no candidate in this slot */
+  uint8_t exact;      /* 1: exact_uv_palette's */
+  uint8_t reserved[2];
+  int16_t u[8];       /* the centres in (U, V) lexicographic order, n_colors valid */
+  int16_t v[8];
+} mt_uv_palette_cand;
+/* d_pos: n (x, y) uint16 block origins in the chroma planes (stride);
+ * d_cands: n x MT_UV_PALETTE_SLOTS; d_maps: n x MT_UV_PALETTE_SLOTS x w x h
+ * (zero for an empty slot).  opts->smooth_t is not used. */
+int mt_uv_palette_device(const uint16_t* d_src_u, const uint16_t* d_src_v, int32_t stride, int32_t w, int32_t h,
+                         const uint16_t* d_pos, int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* d_cands,
+                         uint8_t* d_maps, void* stream);
+/* Host-buffer form: planes stride x rows (rows covering every block). */
+int mt_uv_palette(const uint16_t* src_u, const uint16_t* src_v, int32_t stride, int32_t rows, int32_t w, int32_t h,
+                  const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* cands,
+                  uint8_t* maps);
+
 /* Forward transform + quantisation of n residual blocks (row-major int32,
  * tx_size^2 each) with one tx type per block: levels (column-major int32) and
  * f32 quantisation targets, with the QM applied as DctDispatch does. */

@@ -399,6 +399,25 @@ def luma_palette(src, w, h, pos, opts, bd=8, want_maps=False):
     return cands, maps
 
 
+def uv_palette(src_u, src_v, w, h, pos, opts, want_maps=False):
+    """The UV palette candidates of n w x h chroma blocks (``mt_uv_palette``):
+    exact_uv_palette in slot 0, or the four lossy_uv_palette_from_hist
+    candidates (8 / 4 colours by k-means, 8 / 4 dominant pairs); ``opts`` carries
+    the Viterbi lambda and the palette_uv_color bits.  Returns (candidates n x 4,
+    maps n x 4 x h x w or None)."""
+    src_u = np.ascontiguousarray(src_u, np.uint16)
+    src_v = np.ascontiguousarray(src_v, np.uint16)
+    if src_u.shape != src_v.shape:
+        raise ValueError("U and V planes differ in shape")
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    cands = np.zeros((n, abi.UV_PALETTE_SLOTS), abi.UV_PALETTE_CAND_DTYPE)
+    maps = np.zeros((n, abi.UV_PALETTE_SLOTS, h, w), np.uint8) if want_maps else None
+    _check(load().mt_uv_palette(ptr(src_u), ptr(src_v), src_u.shape[1], src_u.shape[0], w, h, ptr(pos), n,
+                                C.byref(opts), ptr(cands), ptr(maps)), "mt_uv_palette")
+    return cands, maps
+
+
 def split4tx(src, recon, prm, quant, qmrow, costs, jobs, want_cf=False, want_rec=False):
     """The 8x8 leaf's ``split4tx_try`` (``mt_split4tx``): four TX_4X4 per 8x8 job;
     returns (results, cf n x 64 or None, rec n x 8 x 8 or None)."""

@@ -160,6 +160,11 @@ PALETTE_CAND_DTYPE = np.dtype([("colors", "<i2", (8,)), ("n_colors", "u1"), ("se
                                ("reserved", "u1"), ("index_bits", "<f4")])
 assert PALETTE_CAND_DTYPE.itemsize == 24
 
+UV_PALETTE_SLOTS = 4
+UV_PALETTE_CAND_DTYPE = np.dtype([("n_colors", "u1"), ("exact", "u1"), ("reserved", "u1", (2,)),
+                                  ("u", "<i2", (8,)), ("v", "<i2", (8,))])
+assert UV_PALETTE_CAND_DTYPE.itemsize == 36
+
 
 class DeblockFrameParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in ("w8", "h8", "disp_w", "disp_h", "sub_x", "sub_y", "mono", "bd")]
@@ -445,6 +450,10 @@ def _bind(lib):
                                              _P, C.c_int32, C.POINTER(PaletteOpts), _P, _P, _P]),
         "mt_luma_palette": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P,
                                       C.c_int32, C.POINTER(PaletteOpts), _P, _P]),
+        "mt_uv_palette_device": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
+                                           C.POINTER(PaletteOpts), _P, _P, _P]),
+        "mt_uv_palette": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
+                                    C.POINTER(PaletteOpts), _P, _P]),
         "mt_leaf16_tx_refine_device": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, _P, _P,
                                                  C.c_int32, _P, _P, _P, _P]),
         "mt_leaf16": (C.c_int, [_P, _P, C.POINTER(Split16Params), C.POINTER(Quant), _P, C.POINTER(CoefCosts), _P,
@@ -540,7 +549,7 @@ EXPORTED_SYMBOLS = (
     "mt_sse_recon_device", "mt_sse_recon", "mt_trellis_optimize_ctx_device", "mt_split16_luma_device",
     "mt_split16_luma", "mt_split16_depth2_device", "mt_split16_depth2", "mt_cfl_alpha_device", "mt_cfl_alpha",
     "mt_filter_intra_beam_device", "mt_filter_intra_beam", "mt_split4tx_device", "mt_split4tx",
-    "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette",
+    "mt_leaf8_luma_device", "mt_leaf8_tx_refine_device", "mt_leaf8", "mt_leaf16_luma_device", "mt_leaf16_tx_refine_device", "mt_luma_palette_device", "mt_luma_palette", "mt_uv_palette_device", "mt_uv_palette",
     "mt_leaf16", "mt_leaf32_luma_device", "mt_leaf32", "mt_quad32_luma_device", "mt_quad32_luma",
     "mt_grid16_luma_device", "mt_grid16_luma", "mt_uv_mode_cdfs_default", "mt_uv_mode_costs_build",
     "mt_uv_mode_bits", "mt_pick_uv16_420_device", "mt_pick_uv16_420",

@@ -443,6 +443,280 @@ int check(int32_t stride, int32_t fw, int32_t fh, int32_t bd, int32_t w, int32_t
 
 size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
 
+// ---- UV palette candidates (exact_uv_palette, uv_pair_histogram,
+// lossy_uv_palette_from_hist, src/coder/palette.rs:199-431; the index map by
+// viterbi_uv_palette_map, :1053-1076, or uv_nearest_indices,
+// src/kmeans.rs:37-68) ----
+//
+// One thread per block.  The (U, V) pairs are sorted as u << 16 | v keys (the
+// reference's lexicographic pair order) with a Shell sort in local memory,
+// counted into the histogram, then the exact palette (2..8 distinct pairs:
+// the histogram itself) or the four lossy candidates; each candidate's map
+// is written straight to its slot.
+
+constexpr int kUvMaxSamples = 32 * 32;
+
+// The histogram is compacted into the sorted keys in place (entry e's key in
+// key[e], its count in cnt[e]): 6 KB of local memory per thread.
+struct UvPalScratch {
+  uint32_t key[kUvMaxSamples];
+  uint16_t cnt[kUvMaxSamples];
+};
+
+__device__ __forceinline__ int32_t key_u(uint32_t k) { return (int32_t)(k >> 16); }
+__device__ __forceinline__ int32_t key_v(uint32_t k) { return (int32_t)(k & 0xffffu); }
+
+// lossy_uv_palette_from_hist's centres (ascending keys); false: None.
+__device__ bool uv_lossy_centers(const uint32_t* hk, const uint16_t* hc, int hn, int colors, bool top,
+                                 uint32_t* out) {
+  if (hn < 2 || colors > hn) return false;
+  if (colors == hn) {
+    for (int i = 0; i < colors; i++) out[i] = hk[i];
+    return true;  // already ascending
+  }
+  if (top) {
+    // the `colors` most frequent pairs, count descending then pair ascending
+    int n = 0;
+    while (n < colors) {
+      int best = -1;
+      for (int i = 0; i < hn; i++) {
+        bool used = false;
+        for (int k = 0; k < n; k++) used |= out[k] == hk[i];
+        if (used) continue;
+        if (best < 0 || hc[i] > hc[best]) best = i;  // ties keep the smaller pair (earlier in the sorted list)
+      }
+      out[n++] = hk[best];
+    }
+  } else {
+    unsigned long long total = 0;
+    for (int i = 0; i < hn; i++) total += hc[i];
+    uint32_t init[8];
+    int m = 0;
+    for (int i = 0; i < colors; i++) {
+      const uint32_t target = (uint32_t)((unsigned long long)(2 * i + 1) * total / (unsigned long long)(2 * colors));
+      uint32_t acc = 0, pick = hk[hn - 1];
+      for (int e = 0; e < hn; e++) {
+        acc += hc[e];
+        if (acc > target) {
+          pick = hk[e];
+          break;
+        }
+      }
+      if (m == 0 || init[m - 1] != pick) init[m++] = pick;  // dedup of consecutive equal starts
+    }
+    if (m != colors) return false;
+    for (int it = 0; it < 8; it++) {
+      long long su[8] = {}, sv[8] = {}, cnt[8] = {};
+      for (int e = 0; e < hn; e++) {
+        const int32_t u = key_u(hk[e]), v = key_v(hk[e]);
+        int best = 0;
+        long long bd = 0x7fffffffffffffffLL;
+        for (int i = 0; i < m; i++) {
+          const long long du = u - key_u(init[i]), dv = v - key_v(init[i]);
+          const long long d = du * du + dv * dv;
+          if (d < bd) {
+            bd = d;
+            best = i;
+          }
+        }
+        su[best] += (long long)u * hc[e];
+        sv[best] += (long long)v * hc[e];
+        cnt[best] += hc[e];
+      }
+      for (int i = 0; i < m; i++)
+        if (cnt[i] != 0)
+          init[i] = ((uint32_t)((su[i] + cnt[i] / 2) / cnt[i]) << 16) | (uint32_t)((sv[i] + cnt[i] / 2) / cnt[i]);
+      // sort (at most eight) and drop consecutive duplicates
+      for (int a = 1; a < m; a++) {
+        const uint32_t x = init[a];
+        int b = a - 1;
+        while (b >= 0 && init[b] > x) {
+          init[b + 1] = init[b];
+          b--;
+        }
+        init[b + 1] = x;
+      }
+      int k = 0;
+      for (int i = 0; i < m; i++)
+        if (k == 0 || init[k - 1] != init[i]) init[k++] = init[i];
+      m = k;
+      if (m != colors) return false;
+    }
+    for (int i = 0; i < colors; i++) out[i] = init[i];
+  }
+  for (int a = 1; a < colors; a++) {  // centres.sort_unstable()
+    const uint32_t x = out[a];
+    int b = a - 1;
+    while (b >= 0 && out[b] > x) {
+      out[b + 1] = out[b];
+      b--;
+    }
+    out[b + 1] = x;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(64) uv_pal_kernel(const uint16_t* __restrict__ su, const uint16_t* __restrict__ sv,
+                                                    int stride, int w, int h, const uint16_t* __restrict__ pos, int n,
+                                                    const mt_palette_opts opt, mt_uv_palette_cand* __restrict__ cands,
+                                                    uint8_t* __restrict__ maps) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  const int wh = w * h, cx = pos[2 * b], cy = pos[2 * b + 1];
+  mt_uv_palette_cand* cb = cands + (size_t)b * MT_UV_PALETTE_SLOTS;
+  uint8_t* mb = maps ? maps + (size_t)b * MT_UV_PALETTE_SLOTS * wh : nullptr;
+  for (int k = 0; k < MT_UV_PALETTE_SLOTS; k++) {
+    cb[k].n_colors = 0;
+    cb[k].exact = 0;
+    cb[k].reserved[0] = cb[k].reserved[1] = 0;
+    for (int i = 0; i < 8; i++) cb[k].u[i] = cb[k].v[i] = 0;
+  }
+  if (mb)
+    for (int i = 0; i < MT_UV_PALETTE_SLOTS * wh; i++) mb[i] = 0;
+  UvPalScratch S;
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      const size_t o = (size_t)(cy + y) * stride + cx + x;
+      S.key[y * w + x] = ((uint32_t)su[o] << 16) | sv[o];
+    }
+  // Shell sort (gaps 701, 301, 132, 57, 23, 10, 4, 1)
+  const int gaps[8] = {701, 301, 132, 57, 23, 10, 4, 1};
+  for (int g = 0; g < 8; g++) {
+    const int gap = gaps[g];
+    for (int i = gap; i < wh; i++) {
+      const uint32_t x = S.key[i];
+      int j = i;
+      while (j >= gap && S.key[j - gap] > x) {
+        S.key[j] = S.key[j - gap];
+        j -= gap;
+      }
+      S.key[j] = x;
+    }
+  }
+  int hn = 0;  // uv_pair_histogram: hn <= i, so the compaction never overtakes the read
+  for (int i = 0; i < wh; i++) {
+    if (hn > 0 && S.key[hn - 1] == S.key[i]) {
+      S.cnt[hn - 1]++;
+    } else {
+      S.key[hn] = S.key[i];
+      S.cnt[hn] = 1;
+      hn++;
+    }
+  }
+  uint32_t centers[8];
+  const int kColors[4] = {8, 4, 8, 4};
+  for (int k = 0; k < MT_UV_PALETTE_SLOTS; k++) {
+    int nc;
+    if (hn >= 2 && hn <= 8) {  // exact_uv_palette: slot 0 only
+      if (k > 0) break;
+      nc = hn;
+      for (int i = 0; i < nc; i++) centers[i] = S.key[i];
+      cb[0].exact = 1;
+    } else {
+      if (!uv_lossy_centers(S.key, S.cnt, hn, kColors[k], k >= 2, centers)) continue;
+      nc = kColors[k];
+    }
+    cb[k].n_colors = (uint8_t)nc;
+    int32_t cu[8] = {}, cvv[8] = {};
+    for (int i = 0; i < nc; i++) {
+      cu[i] = key_u(centers[i]);
+      cvv[i] = key_v(centers[i]);
+      cb[k].u[i] = (int16_t)cu[i];
+      cb[k].v[i] = (int16_t)cvv[i];
+    }
+    if (!mb) continue;
+    uint8_t* map = mb + (size_t)k * wh;
+    const bool exact = hn >= 2 && hn <= 8;
+    if (exact) {
+      for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+          const size_t o = (size_t)(cy + y) * stride + cx + x;
+          const uint32_t key = ((uint32_t)su[o] << 16) | sv[o];
+          int idx = 0;
+          for (int i = 0; i < nc; i++)
+            if (centers[i] == key) idx = i;
+          map[y * w + x] = (uint8_t)idx;
+        }
+    } else if (opt.viterbi_lambda > 0.0f) {
+      const float lam = opt.viterbi_lambda;
+      const float(*costs)[8] = opt.color_costs[nc - 2];
+      uint8_t back[32 * 8];
+      float prev[8], cur[8];
+      for (int i = 0; i < 8; i++) prev[i] = cur[i] = 0.0f;
+      for (int y = 0; y < h; y++) {
+        for (int x = 0; x < w; x++) {
+          const size_t o = (size_t)(cy + y) * stride + cx + x;
+          const int32_t u = su[o], v = sv[o];
+          float dist[8];
+          for (int i = 0; i < nc; i++) {
+            const float eu = (float)(u - cu[i]), ev = (float)(v - cvv[i]);
+            dist[i] = __fadd_rn(__fmul_rn(eu, eu), __fmul_rn(ev, ev));
+          }
+          if (x == 0) {
+            if (y > 0) {
+              const int up = map[(y - 1) * w];
+              for (int i = 0; i < nc; i++) {
+                int ctx, sym;
+                color_ctx_nb(-1, up, 0, i, ctx, sym);
+                cur[i] = __fadd_rn(dist[i], __fmul_rn(lam, costs[ctx][sym]));
+              }
+            } else {
+              for (int i = 0; i < nc; i++) cur[i] = dist[i];
+            }
+          } else {
+            const int up = y > 0 ? map[(y - 1) * w + x] : -1;
+            const int ul = y > 0 ? map[(y - 1) * w + x - 1] : 0;
+            for (int i = 0; i < nc; i++) {
+              float best = __int_as_float(0x7f800000);
+              int arg = 0;
+              for (int j = 0; j < nc; j++) {
+                int ctx, sym;
+                color_ctx_nb(j, up, ul, i, ctx, sym);
+                const float cc = __fadd_rn(prev[j], __fmul_rn(lam, costs[ctx][sym]));
+                if (cc < best) {
+                  best = cc;
+                  arg = j;
+                }
+              }
+              cur[i] = __fadd_rn(best, dist[i]);
+              back[x * 8 + i] = (uint8_t)arg;
+            }
+          }
+          for (int i = 0; i < 8; i++) prev[i] = cur[i];
+        }
+        int bi = 0;
+        float bc = __int_as_float(0x7f800000);
+        for (int i = 0; i < nc; i++)
+          if (prev[i] < bc) {
+            bc = prev[i];
+            bi = i;
+          }
+        for (int x = w - 1; x >= 0; x--) {
+          map[y * w + x] = (uint8_t)bi;
+          if (x > 0) bi = back[x * 8 + bi];
+        }
+      }
+    } else {
+      for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+          const size_t o = (size_t)(cy + y) * stride + cx + x;
+          const int32_t u = su[o], v = sv[o];
+          long long bd = 0x7fffffffffffffffLL;
+          int bi = 0;
+          for (int i = 0; i < nc; i++) {
+            const long long du = u - cu[i], dv = v - cvv[i];
+            const long long d = du * du + dv * dv;
+            if (d < bd) {
+              bd = d;
+              bi = i;
+            }
+          }
+          map[y * w + x] = (uint8_t)bi;
+        }
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -483,6 +757,48 @@ int mt_luma_palette(const uint16_t* src, int32_t stride, int32_t frame_w, int32_
                                 reinterpret_cast<mt_palette_cand*>(d + o_c), d + o_m, nullptr);
     if (rc == MT_OK) e = cudaMemcpy(cands, d + o_c, ncand * sizeof(mt_palette_cand), cudaMemcpyDeviceToHost);
     if (rc == MT_OK && e == cudaSuccess && maps) e = cudaMemcpy(maps, d + o_m, nmap, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (rc != MT_OK) return rc;
+  return e == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_uv_palette_device(const uint16_t* d_src_u, const uint16_t* d_src_v, int32_t stride, int32_t w, int32_t h,
+                         const uint16_t* d_pos, int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* d_cands,
+                         uint8_t* d_maps, void* stream) {
+  if (!opts || n < 0 || w < 4 || h < 4 || w > 32 || h > 32 || stride < w) return MT_ERR_INVALID_INPUT;
+  if (!(opts->viterbi_lambda >= 0.0f)) return MT_ERR_INVALID_INPUT;
+  if (n == 0) return MT_OK;
+  if (!d_src_u || !d_src_v || !d_pos || !d_cands) return MT_ERR_INVALID_INPUT;
+  uv_pal_kernel<<<(unsigned)((n + 63) / 64), 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
+      d_src_u, d_src_v, stride, w, h, d_pos, n, *opts, d_cands, d_maps);
+  return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
+}
+
+int mt_uv_palette(const uint16_t* src_u, const uint16_t* src_v, int32_t stride, int32_t rows, int32_t w, int32_t h,
+                  const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* cands,
+                  uint8_t* maps) {
+  if (!opts || n < 0 || rows <= 0 || stride <= 0) return MT_ERR_INVALID_INPUT;
+  if (n == 0) return MT_OK;
+  if (!src_u || !src_v || !pos || !cands) return MT_ERR_INVALID_INPUT;
+  for (int32_t b = 0; b < n; b++)  // every block inside the planes
+    if ((int64_t)pos[2 * b] + w > stride || (int64_t)pos[2 * b + 1] + h > rows) return MT_ERR_INVALID_INPUT;
+  const size_t plane = (size_t)stride * rows * 2, pb = (size_t)n * 4, cb = (size_t)n * MT_UV_PALETTE_SLOTS *
+                                                                           sizeof(mt_uv_palette_cand);
+  const size_t mbytes = maps ? (size_t)n * MT_UV_PALETTE_SLOTS * w * h : 0;
+  const size_t o_u = 0, o_v = up256(plane), o_p = o_v + up256(plane), o_c = o_p + up256(pb), o_m = o_c + up256(cb);
+  uint8_t* d = nullptr;
+  if (cudaMalloc(&d, o_m + up256(mbytes ? mbytes : 1)) != cudaSuccess) return MT_ERR_ALLOC;
+  cudaError_t e = cudaMemcpy(d + o_u, src_u, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_v, src_v, plane, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d + o_p, pos, pb, cudaMemcpyHostToDevice);
+  int rc = MT_OK;
+  if (e == cudaSuccess) {
+    rc = mt_uv_palette_device(reinterpret_cast<const uint16_t*>(d + o_u), reinterpret_cast<const uint16_t*>(d + o_v),
+                              stride, w, h, reinterpret_cast<const uint16_t*>(d + o_p), n, opts,
+                              reinterpret_cast<mt_uv_palette_cand*>(d + o_c), maps ? d + o_m : nullptr, nullptr);
+    if (rc == MT_OK) e = cudaMemcpy(cands, d + o_c, cb, cudaMemcpyDeviceToHost);
+    if (rc == MT_OK && e == cudaSuccess && maps) e = cudaMemcpy(maps, d + o_m, mbytes, cudaMemcpyDeviceToHost);
   }
   cudaFree(d);
   if (rc != MT_OK) return rc;

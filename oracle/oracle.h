@@ -187,6 +187,9 @@ int or_pick_uv32_444(const uint16_t* src_u, const uint16_t* src_v, const uint16_
                      const uint8_t* qm, const mt_coef_cdfs* cd, const mt_uv_mode_cdfs* mc,
                      const mt_uv32_444_job* jobs, int32_t n, mt_uv16_result* results, int32_t* cf_out,
                      uint16_t* rec_out);
+/* palette.rs exact_uv_palette / uv_pair_histogram / lossy_uv_palette_from_hist + the UV index map. */
+int or_uv_palette(const uint16_t* su, const uint16_t* sv, int32_t stride, int32_t w, int32_t h, const uint16_t* pos,
+                  int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* cands, uint8_t* maps);
 /* dct1d_32_i32 in place on 32 values. */
 void or_dct1d_32(int32_t* buf);
 /* block32.rs pick_luma32: the mode loop's candidates (:776-836, TX_32X32 DCT_DCT). */

@@ -131,8 +131,10 @@ void ctx_nb(int l, int u, int ul, int cur, int& ctx, int& sym) {
   else sym = n + cur - ((r0 < cur) + (n >= 2 && r1 < cur) + (n >= 3 && r2 < cur));
 }
 
-void viterbi(uint8_t* map, const uint16_t* src, int stride, int px, int py, int w, int h, const int32_t* c, int n,
-             const float costs[5][8], float lam) {
+// viterbi_map_core over n palette entries; dist(x, y, d) fills the squared
+// error of every entry at map position (x, y).
+template <typename D>
+void viterbi_core(uint8_t* map, int w, int h, int n, const float costs[5][8], float lam, D dist_at) {
   std::vector<float> trans(8 * 8 * 8 * 8, 0.0f);
   float top[8][8] = {}, col[8][8] = {};
   for (int i = 0; i < n; i++)
@@ -152,11 +154,7 @@ void viterbi(uint8_t* map, const uint16_t* src, int stride, int px, int py, int 
   std::vector<uint8_t> back((size_t)w * 8, 0);
   for (int y = 0; y < h; y++) {
     for (int x = 0; x < w; x++) {
-      const int v = src[(size_t)(py + y) * stride + px + x];
-      for (int i = 0; i < n; i++) {
-        const float e = (float)(v - c[i]);
-        dist[i] = e * e;
-      }
+      dist_at(x, y, dist);
       if (x == 0) {
         if (y > 0) {
           const int u = map[(y - 1) * w];
@@ -195,6 +193,18 @@ void viterbi(uint8_t* map, const uint16_t* src, int stride, int px, int py, int 
       if (x > 0) bi = back[(size_t)x * 8 + bi];
     }
   }
+}
+
+// viterbi_palette_map (palette.rs:1028-1052): the luma distance.
+void viterbi(uint8_t* map, const uint16_t* src, int stride, int px, int py, int w, int h, const int32_t* c, int n,
+             const float costs[5][8], float lam) {
+  viterbi_core(map, w, h, n, costs, lam, [&](int x, int y, float* d) {
+    const int v = src[(size_t)(py + y) * stride + px + x];
+    for (int i = 0; i < n; i++) {
+      const float e = (float)(v - c[i]);
+      d[i] = e * e;
+    }
+  });
 }
 
 void smooth(uint8_t* map, const uint16_t* src, int stride, int px, int py, int w, int h, const int32_t* c, int t,
@@ -367,3 +377,175 @@ int or_luma_palette(const uint16_t* src, int32_t stride, int32_t frame_w, int32_
 }
 
 }  // extern "C"
+
+// ---- UV palette candidates ----
+
+namespace {
+
+using Pair = std::pair<int32_t, int32_t>;
+
+// exact_uv_palette (palette.rs:199-262).
+bool exact_uv(const uint16_t* su, const uint16_t* sv, int stride, int cx, int cy, int w, int h, std::vector<Pair>& pairs,
+              uint8_t* map) {
+  pairs.clear();
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      const Pair p((int32_t)su[(size_t)(cy + y) * stride + cx + x], (int32_t)sv[(size_t)(cy + y) * stride + cx + x]);
+      if (std::find(pairs.begin(), pairs.end(), p) == pairs.end()) {
+        if (pairs.size() == 8) return false;
+        pairs.push_back(p);
+      }
+    }
+  if (pairs.size() < 2) return false;
+  std::sort(pairs.begin(), pairs.end());
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      const Pair p((int32_t)su[(size_t)(cy + y) * stride + cx + x], (int32_t)sv[(size_t)(cy + y) * stride + cx + x]);
+      map[y * w + x] = (uint8_t)(std::find(pairs.begin(), pairs.end(), p) - pairs.begin());
+    }
+  return true;
+}
+
+// lossy_uv_palette_from_hist's centres (palette.rs:315-410); false: None.
+bool lossy_uv_centers(const std::vector<std::pair<Pair, uint32_t>>& hist, int colors, bool top,
+                      std::vector<Pair>& out) {
+  if (hist.size() < 2 || (size_t)colors > hist.size()) return false;
+  out.clear();
+  if ((size_t)colors == hist.size()) {
+    for (auto& e : hist) out.push_back(e.first);
+  } else if (top) {
+    std::vector<size_t> idx(hist.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+      if (hist[a].second != hist[b].second) return hist[a].second > hist[b].second;
+      return hist[a].first < hist[b].first;
+    });
+    for (int i = 0; i < colors; i++) out.push_back(hist[idx[(size_t)i]].first);
+  } else {
+    uint64_t total = 0;
+    for (auto& e : hist) total += e.second;
+    std::vector<Pair> init;
+    for (int i = 0; i < colors; i++) {
+      const uint32_t target = (uint32_t)((uint64_t)(2 * i + 1) * total / (uint64_t)(2 * colors));
+      uint32_t acc = 0;
+      Pair pick = hist.back().first;
+      for (auto& e : hist) {
+        acc += e.second;
+        if (acc > target) {
+          pick = e.first;
+          break;
+        }
+      }
+      init.push_back(pick);
+    }
+    init.erase(std::unique(init.begin(), init.end()), init.end());
+    if ((int)init.size() != colors) return false;
+    for (int it = 0; it < 8; it++) {
+      int64_t su[8] = {}, sv[8] = {}, cnt[8] = {};
+      for (auto& e : hist) {
+        const int32_t u = e.first.first, v = e.first.second;
+        int best = 0;
+        int64_t bd = INT64_MAX;
+        for (int i = 0; i < (int)init.size(); i++) {
+          const int64_t du = u - init[(size_t)i].first, dv = v - init[(size_t)i].second;
+          const int64_t d = du * du + dv * dv;
+          if (d < bd) {
+            bd = d;
+            best = i;
+          }
+        }
+        su[best] += (int64_t)u * e.second;
+        sv[best] += (int64_t)v * e.second;
+        cnt[best] += e.second;
+      }
+      for (int i = 0; i < (int)init.size(); i++)
+        if (cnt[i] != 0)
+          init[(size_t)i] = Pair((int32_t)((su[i] + cnt[i] / 2) / cnt[i]), (int32_t)((sv[i] + cnt[i] / 2) / cnt[i]));
+      std::sort(init.begin(), init.end());
+      init.erase(std::unique(init.begin(), init.end()), init.end());
+      if ((int)init.size() != colors) return false;
+    }
+    out = init;
+  }
+  std::sort(out.begin(), out.end());
+  return true;
+}
+
+}  // namespace
+
+extern "C" int or_uv_palette(const uint16_t* su, const uint16_t* sv, int32_t stride, int32_t w, int32_t h,
+                             const uint16_t* pos, int32_t n, const mt_palette_opts* opts, mt_uv_palette_cand* cands,
+                             uint8_t* maps) {
+  const size_t wh = (size_t)w * h;
+  static const int kList[4][2] = {{8, 0}, {4, 0}, {8, 1}, {4, 1}};
+  std::vector<Pair> pairs, centers;
+  for (int b = 0; b < n; b++) {
+    const int cx = pos[2 * b], cy = pos[2 * b + 1];
+    mt_uv_palette_cand* cb = cands + (size_t)b * 4;
+    uint8_t* mb = maps ? maps + (size_t)b * 4 * wh : nullptr;
+    memset(cb, 0, 4 * sizeof(mt_uv_palette_cand));
+    if (mb) memset(mb, 0, 4 * wh);
+    std::vector<uint8_t> scratch(wh);
+    if (exact_uv(su, sv, stride, cx, cy, w, h, pairs, mb ? mb : scratch.data())) {
+      cb[0].n_colors = (uint8_t)pairs.size();
+      cb[0].exact = 1;
+      for (size_t i = 0; i < pairs.size(); i++) {
+        cb[0].u[i] = (int16_t)pairs[i].first;
+        cb[0].v[i] = (int16_t)pairs[i].second;
+      }
+      continue;
+    }
+    // uv_pair_histogram (palette.rs:264-309)
+    std::vector<Pair> all;
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++)
+        all.emplace_back((int32_t)su[(size_t)(cy + y) * stride + cx + x], (int32_t)sv[(size_t)(cy + y) * stride + cx + x]);
+    std::sort(all.begin(), all.end());
+    std::vector<std::pair<Pair, uint32_t>> hist;
+    for (auto& p : all) {
+      if (!hist.empty() && hist.back().first == p) hist.back().second++;
+      else hist.emplace_back(p, 1u);
+    }
+    for (int k = 0; k < 4; k++) {
+      if (!lossy_uv_centers(hist, kList[k][0], kList[k][1] != 0, centers)) continue;
+      const int nc = (int)centers.size();
+      cb[k].n_colors = (uint8_t)nc;
+      int32_t cu[8] = {}, cv[8] = {};
+      for (int i = 0; i < nc; i++) {
+        cu[i] = centers[(size_t)i].first;
+        cv[i] = centers[(size_t)i].second;
+        cb[k].u[i] = (int16_t)cu[i];
+        cb[k].v[i] = (int16_t)cv[i];
+      }
+      uint8_t* map = mb ? mb + (size_t)k * wh : scratch.data();
+      if (opts->viterbi_lambda > 0.0f) {
+        viterbi_core(map, w, h, nc, opts->color_costs[nc - 2], opts->viterbi_lambda, [&](int x, int y, float* d) {
+          const size_t o = (size_t)(cy + y) * stride + cx + x;
+          const int32_t u = su[o], v = sv[o];
+          for (int i = 0; i < nc; i++) {
+            const float eu = (float)(u - cu[i]), ev = (float)(v - cv[i]);
+            d[i] = eu * eu + ev * ev;
+          }
+        });
+      } else {
+        for (int y = 0; y < h; y++)  // uv_nearest_indices (kmeans.rs:37-68)
+          for (int x = 0; x < w; x++) {
+            const size_t o = (size_t)(cy + y) * stride + cx + x;
+            const int32_t u = su[o], v = sv[o];
+            int64_t bd = INT64_MAX;
+            int bi = 0;
+            for (int i = 0; i < nc; i++) {
+              const int64_t du = u - cu[i], dv = v - cv[i];
+              const int64_t d = du * du + dv * dv;
+              if (d < bd) {
+                bd = d;
+                bi = i;
+              }
+            }
+            map[y * w + x] = (uint8_t)bi;
+          }
+      }
+    }
+  }
+  return MT_OK;
+}

@@ -77,6 +77,8 @@ def load():
                                       C.POINTER(abi.CoefCdfs), _P, C.c_int32, _P, _P, _P]),
             "or_luma_palette": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P,
                                           C.c_int32, C.POINTER(abi.PaletteOpts), _P, _P]),
+            "or_uv_palette": (C.c_int, [_P, _P, C.c_int32, C.c_int32, C.c_int32, _P, C.c_int32,
+                                        C.POINTER(abi.PaletteOpts), _P, _P]),
             "or_block_color_histogram": (None, [_P] + [C.c_int32] * 5 + [_P, _P, _P]),
             "or_dp_palette_center_sets": (None, [_P, _P, C.c_int32, C.c_int32, _P, _P]),
             "or_luma_nearest_indices": (None, [_P] + [C.c_int32] * 5 + [_P, C.c_int32, _P]),
@@ -586,6 +588,19 @@ def luma_palette(src, w, h, pos, opts, bd=8):
     maps = np.zeros((n, abi.PALETTE_SLOTS, h, w), np.uint8)
     assert load().or_luma_palette(p(src), src.shape[1], src.shape[1], src.shape[0], bd, w, h, p(pos), n,
                                   C.byref(opts), p(cands), p(maps)) == 0
+    return cands, maps
+
+
+def uv_palette(src_u, src_v, w, h, pos, opts):
+    """UV palette candidates of n w x h chroma blocks: (candidates n x 4, maps n x 4 x h x w)."""
+    src_u = np.ascontiguousarray(src_u, np.uint16)
+    src_v = np.ascontiguousarray(src_v, np.uint16)
+    pos = np.ascontiguousarray(pos, np.uint16).reshape(-1, 2)
+    n = len(pos)
+    cands = np.zeros((n, abi.UV_PALETTE_SLOTS), abi.UV_PALETTE_CAND_DTYPE)
+    maps = np.zeros((n, abi.UV_PALETTE_SLOTS, h, w), np.uint8)
+    assert load().or_uv_palette(p(src_u), p(src_v), src_u.shape[1], w, h, p(pos), n, C.byref(opts), p(cands),
+                                p(maps)) == 0
     return cands, maps
 
 
