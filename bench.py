@@ -799,6 +799,21 @@ def measure_filters(dev, wl, hbm_peak, reps=5):
     out["luma_palette16"]["palette_blocks"] = None  # filled below from the candidates
     pc = np.frombuffer(d_pc.cpu().numpy().tobytes(), abi.PALETTE_CAND_DTYPE).reshape(len(fpos), abi.PALETTE_SLOTS)
     out["luma_palette16"]["palette_blocks"] = int((pc["hist_len"][:, 0] > 0).sum())
+    # the UV palette candidates of every 16x16 block of 1080p 4:4:4
+    # screen-content chroma planes: exact palette or the four lossy candidates,
+    # Viterbi UV maps at the same lambda
+    d_su, d_sv = t16(synth.screen_luma(W, H, 11)), t16(synth.screen_luma(W, H, 12))
+    d_uc = torch.empty(len(fpos) * abi.UV_PALETTE_SLOTS * abi.UV_PALETTE_CAND_DTYPE.itemsize, dtype=torch.uint8,
+                       device=dev)
+    d_um = torch.empty(len(fpos) * abi.UV_PALETTE_SLOTS * 256, dtype=torch.uint8, device=dev)
+    ms = timed(lambda: lib.mt_uv_palette_device(d_su.data_ptr(), d_sv.data_ptr(), W, 16, 16, d_fpos.data_ptr(),
+                                                len(fpos), C.byref(popts), d_uc.data_ptr(), d_um.data_ptr(), None))
+    out["uv_palette16"] = entry(ms, len(fpos) * (256 * 2 * 2 + abi.UV_PALETTE_SLOTS * (256 + 36)),
+                                "per block: the 16x16 U and V source (2 B / sample), 4 maps (1 B / sample), candidates")
+    out["uv_palette16"]["blocks"] = len(fpos)
+    uc = np.frombuffer(d_uc.cpu().numpy().tobytes(), abi.UV_PALETTE_CAND_DTYPE).reshape(len(fpos), -1)
+    out["uv_palette16"]["exact_blocks"] = int((uc["exact"][:, 0] == 1).sum())
+    out["uv_palette16"]["lossy_blocks"] = int(((uc["exact"][:, 0] == 0) & (uc["n_colors"].max(1) > 0)).sum())
     # deblocking of the three planes (frame_deblock at the shipped levels)
     pwm, phm, _, _, bid = synth.partition_maps(pw // 4, ph // 4, 7)
     tx = synth.transform_maps(pwm, phm, bid, 8)

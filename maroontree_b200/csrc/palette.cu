@@ -20,8 +20,13 @@
 #include <stdint.h>
 
 #include "../../include/maroontree_b200.h"
+#include "leaf8.cuh"
 
 namespace {
+
+using mtd::arena_launch_shape;
+using mtd::arena_stride;
+using mtd::smem_arena;
 
 constexpr int kSlots = MT_PALETTE_SLOTS;
 constexpr int kWarps = 4;
@@ -457,10 +462,16 @@ size_t up256(size_t v) { return (v + 255) & ~(size_t)255; }
 constexpr int kUvMaxSamples = 32 * 32;
 
 // The histogram is compacted into the sorted keys in place (entry e's key in
-// key[e], its count in cnt[e]): 6 KB of local memory per thread.
+// key[e], its count in cnt[e]).  Each thread's copy sits in the CTA's dynamic
+// shared memory (1.5 KB for blocks up to 16x16, 6 KB up to 32x32), which keeps
+// the per-thread local allocation under 1 KB.  The kernel's time goes to each
+// thread's serial work, not to this scratch: the 8-colour Viterbi derives n^2
+// palette contexts per sample, and a warp's lanes diverge between exact and
+// lossy blocks.
+template <int MAXS>
 struct UvPalScratch {
-  uint32_t key[kUvMaxSamples];
-  uint16_t cnt[kUvMaxSamples];
+  uint32_t key[MAXS];
+  uint16_t cnt[MAXS];
 };
 
 __device__ __forceinline__ int32_t key_u(uint32_t k) { return (int32_t)(k >> 16); }
@@ -556,10 +567,11 @@ __device__ bool uv_lossy_centers(const uint32_t* hk, const uint16_t* hc, int hn,
   return true;
 }
 
+template <int MAXS>
 __global__ void __launch_bounds__(64) uv_pal_kernel(const uint16_t* __restrict__ su, const uint16_t* __restrict__ sv,
                                                     int stride, int w, int h, const uint16_t* __restrict__ pos, int n,
                                                     const mt_palette_opts opt, mt_uv_palette_cand* __restrict__ cands,
-                                                    uint8_t* __restrict__ maps) {
+                                                    uint8_t* __restrict__ maps, int arena) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
   const int wh = w * h, cx = pos[2 * b], cy = pos[2 * b + 1];
@@ -573,7 +585,7 @@ __global__ void __launch_bounds__(64) uv_pal_kernel(const uint16_t* __restrict__
   }
   if (mb)
     for (int i = 0; i < MT_UV_PALETTE_SLOTS * wh; i++) mb[i] = 0;
-  UvPalScratch S;
+  UvPalScratch<MAXS>& S = smem_arena<UvPalScratch<MAXS>>(arena);
   for (int y = 0; y < h; y++)
     for (int x = 0; x < w; x++) {
       const size_t o = (size_t)(cy + y) * stride + cx + x;
@@ -770,8 +782,14 @@ int mt_uv_palette_device(const uint16_t* d_src_u, const uint16_t* d_src_v, int32
   if (!(opts->viterbi_lambda >= 0.0f)) return MT_ERR_INVALID_INPUT;
   if (n == 0) return MT_OK;
   if (!d_src_u || !d_src_v || !d_pos || !d_cands) return MT_ERR_INVALID_INPUT;
-  uv_pal_kernel<<<(unsigned)((n + 63) / 64), 64, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
-      d_src_u, d_src_v, stride, w, h, d_pos, n, *opts, d_cands, d_maps);
+  auto* kern = w * h <= 256 ? uv_pal_kernel<256> : uv_pal_kernel<kUvMaxSamples>;
+  const int arena = w * h <= 256 ? arena_stride(sizeof(UvPalScratch<256>))
+                                 : arena_stride(sizeof(UvPalScratch<kUvMaxSamples>));
+  int threads = 0;
+  size_t dyn = 0;
+  if (!arena_launch_shape(kern, n, arena, 64, &threads, &dyn)) return MT_ERR_DEVICE;
+  kern<<<(unsigned)((n + threads - 1) / threads), threads, dyn, reinterpret_cast<cudaStream_t>(stream)>>>(
+      d_src_u, d_src_v, stride, w, h, d_pos, n, *opts, d_cands, d_maps, arena);
   return cudaGetLastError() == cudaSuccess ? MT_OK : MT_ERR_DEVICE;
 }
 
